@@ -1,0 +1,65 @@
+"""Build recipe of the CUDA library athenak_b200/libdustb.so (sm_100a, in-tree).
+
+Every .cu under csrc/ is compiled by nvcc for sm_100a and linked into one shared library
+with C linkage entry points (include/dustb.h).  The FP64 translation units are compiled with
+--fmad=false so their per-particle arithmetic rounds as the CPU oracle's does.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libdustb.so")
+BUILD = os.path.join(HERE, "_build")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# translation units and their extra flags
+UNITS = {
+    "dustb_fp64.cu": ["--fmad=false"],
+    "dustb_sort.cu": [],
+    "dustb_mixed.cu": [],
+}
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    deps.append(os.path.join(HERE, "..", "include", "dustb.h"))
+    newest = max(os.path.getmtime(p) for p in deps)
+    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= newest:
+        return OUT
+    objs = []
+    for unit, extra in UNITS.items():
+        src = os.path.join(CSRC, unit)
+        if not os.path.exists(src):
+            continue
+        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+               "-Xptxas", "-v" if verbose else "-O3", "-rdc=false", "-c", src, "-o", obj, *extra]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"nvcc failed on {unit}")
+        if verbose:
+            sys.stderr.write(r.stderr)
+        objs.append(obj)
+    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", OUT, *objs]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("link failed")
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -1,0 +1,81 @@
+// dustb_common.cuh -- device-side layout helpers shared by the dust drag kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/dustb.h"
+
+namespace dustb {
+
+// RegionSize field order (src/mesh/mesh.hpp:25-29)
+enum { X1MIN = 0, X2MIN = 1, X3MIN = 2, X1MAX = 3, X2MAX = 4, X3MAX = 5, DX1 = 6, DX2 = 7,
+       DX3 = 8 };
+
+// index ranges of one MeshBlock's padded arrays (mb_indcs, src/mesh/mesh.cpp:320-360)
+struct Ind {
+  int n1, n2, n3, is, ie, js, je, ks, ke;
+  int nx1, nx2, nx3, ng, nmb, three_d, multi_d;
+  __host__ __device__ long long cells() const { return (long long)n1 * n2 * n3; }
+  __host__ __device__ long long at(int m, int nvar, int v, int k, int j, int i) const {
+    return ((((long long)m * nvar + v) * n3 + k) * n2 + j) * (long long)n1 + i;
+  }
+};
+
+inline Ind make_ind(const dustb_mesh &ms) {
+  Ind d;
+  d.nx1 = ms.nx1; d.nx2 = ms.multi_d ? ms.nx2 : 1; d.nx3 = ms.three_d ? ms.nx3 : 1;
+  d.ng = ms.ng; d.nmb = ms.nmb; d.three_d = ms.three_d; d.multi_d = ms.multi_d;
+  d.n1 = ms.nx1 + 2 * ms.ng;
+  d.n2 = ms.multi_d ? ms.nx2 + 2 * ms.ng : 1;
+  d.n3 = ms.three_d ? ms.nx3 + 2 * ms.ng : 1;
+  d.is = ms.ng; d.ie = d.is + d.nx1 - 1;
+  d.js = ms.multi_d ? ms.ng : 0; d.je = d.js + d.nx2 - 1;
+  d.ks = ms.three_d ? ms.ng : 0; d.ke = d.ks + d.nx3 - 1;
+  return d;
+}
+
+// PMWeights (src/dust/dust.hpp:1088-1111), FP64, operation for operation.
+__device__ __forceinline__ void pm_weights(double x, double xmin, double xmax, int nx, int is,
+                                           int scheme, int &ip, double w[3]) {
+  double cell = (x - xmin) * ((double)nx / (xmax - xmin));
+  int ig = (int)(cell + 1.0) - 1;
+  double del = cell - ((double)ig + 0.5);
+  ip = ig + is;
+  if (scheme == 0) {
+    w[0] = 0.0; w[1] = 1.0; w[2] = 0.0;
+  } else if (scheme == 1) {
+    w[0] = fmax(0.0, -del); w[1] = 1.0 - fabs(del); w[2] = fmax(0.0, del);
+  } else {
+    w[0] = 0.5 * ((0.5 - del) * (0.5 - del));
+    w[1] = 0.75 - del * del;
+    w[2] = 0.5 * ((0.5 + del) * (0.5 + del));
+  }
+}
+
+__device__ __forceinline__ void report(unsigned int *err, unsigned int bit) {
+  if (err) atomicOr(err, bit);
+}
+
+// the 26 same-level directions in NeighborIndex(ox1,ox2,ox3,0,0) order
+// (src/mesh/nghbr_index.hpp:29-55): the order RecvAndSumDeposit sums its buffers in
+__constant__ const signed char kDirOrder[26][3] = {
+  {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0},
+  {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 1, 0},
+  {0, 0, -1}, {0, 0, 1},
+  {-1, 0, -1}, {1, 0, -1}, {-1, 0, 1}, {1, 0, 1},
+  {0, -1, -1}, {0, 1, -1}, {0, -1, 1}, {0, 1, 1},
+  {-1, -1, -1}, {1, -1, -1}, {-1, 1, -1}, {1, 1, -1},
+  {-1, -1, 1}, {1, -1, 1}, {-1, 1, 1}, {1, 1, 1}};
+
+__host__ __device__ inline int dir_slot(int o1, int o2, int o3) {
+  return (o3 + 1) * 9 + (o2 + 1) * 3 + (o1 + 1);
+}
+
+}  // namespace dustb
+
+// host-side error bookkeeping shared by the translation units
+namespace dustb_host {
+void set_error(const char *what, cudaError_t e);
+int launch_status(const char *what);
+}  // namespace dustb_host

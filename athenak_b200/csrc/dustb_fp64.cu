@@ -1,0 +1,1039 @@
+// dustb_fp64.cu -- the FP64 form of the dust drag step: one kernel per reference kernel,
+// one thread per particle or per cell, FP64 global atomics for the deposits.  This is the
+// straightforward GPU form of the reference's Kokkos kernels (the "plain FP64" baseline of
+// the mixed-precision form in dustb_mixed.cu).  Compiled with --fmad=false so that the
+// per-particle arithmetic rounds exactly as the CPU oracle's does.
+#include <cfloat>
+#include <cstdio>
+#include <cstring>
+
+#include "dustb_common.cuh"
+
+using namespace dustb;
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned blocks_for(long long n) {
+  long long b = (n + kThreads - 1) / kThreads;
+  return (unsigned)(b < 1 ? 1 : b);
+}
+inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+struct PCtx {            // particle view passed by value into kernels
+  double *pr;
+  int *pi;
+  long long stride;
+  int npart;
+  __device__ double &r(int c, int p) const { return pr[(long long)c * stride + p]; }
+  __device__ int &i(int c, int p) const { return pi[(long long)c * stride + p]; }
+};
+
+struct MCtx {            // mesh view
+  const double *mb;
+  const int *nghbr;
+  int gids, scheme, three_d, multi_d;
+  double x1min, x1max, x2min, x2max, x3min, x3max;
+  __device__ double s(int m, int f) const { return mb[(long long)m * 9 + f]; }
+};
+
+PCtx pview(const dustb_ctx *c) {
+  return PCtx{c->part.pr, c->part.pi, c->part.stride, c->part.npart};
+}
+MCtx mview(const dustb_ctx *c) {
+  const dustb_mesh &ms = c->mesh;
+  return MCtx{ms.mb_size, ms.nghbr, ms.gids, c->phys.scheme, ms.three_d, ms.multi_d,
+              ms.x1min, ms.x1max, ms.x2min, ms.x2max, ms.x3min, ms.x3max};
+}
+
+__device__ __forceinline__ void weights3(const MCtx &M, const Ind &d, int m, double x,
+                                         double y, double z, int &ip, int &jp, int &kp,
+                                         double wx[3], double wy[3], double wz[3]) {
+  pm_weights(x, M.s(m, X1MIN), M.s(m, X1MAX), d.nx1, d.is, M.scheme, ip, wx);
+  pm_weights(y, M.s(m, X2MIN), M.s(m, X2MAX), d.nx2, d.js, M.scheme, jp, wy);
+  if (d.three_d) {
+    pm_weights(z, M.s(m, X3MIN), M.s(m, X3MAX), d.nx3, d.ks, M.scheme, kp, wz);
+  } else {
+    kp = d.ks; wz[0] = 0.0; wz[1] = 1.0; wz[2] = 0.0;
+  }
+}
+
+__device__ __forceinline__ bool halo_ok(const Ind &d, int ip, int jp, int kp) {
+  if (ip < d.is - 1 || ip > d.is + d.nx1) return false;
+  if (jp < d.js - 1 || jp > d.js + d.nx2) return false;
+  if (d.three_d && (kp < d.ks - 1 || kp > d.ks + d.nx3)) return false;
+  return true;
+}
+
+__device__ __forceinline__ double cell_vol(const MCtx &M, const Ind &d, int m) {
+  double v = M.s(m, DX1) * M.s(m, DX2);
+  if (d.three_d) v *= M.s(m, DX3);
+  return v;
+}
+
+__device__ __forceinline__ bool block_ok(const Ind &d, int m) { return m >= 0 && m < d.nmb; }
+
+// ---- register copy / gas stand-in / history ------------------------------------------
+__global__ void k_reg_copy(PCtx P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  P.r(DUSTB_IPX1, p) = P.r(DUSTB_IPX, p);
+  P.r(DUSTB_IPVX1, p) = P.r(DUSTB_IPVX, p);
+  P.r(DUSTB_IPY1, p) = P.r(DUSTB_IPY, p);
+  P.r(DUSTB_IPVY1, p) = P.r(DUSTB_IPVY, p);
+  P.r(DUSTB_IPZ1, p) = P.r(DUSTB_IPZ, p);
+  P.r(DUSTB_IPVZ1, p) = P.r(DUSTB_IPVZ, p);
+}
+
+// active-cell loop helper: idx over nmb*nx3*nx2*nx1
+__device__ __forceinline__ bool active_cell(const Ind &d, long long idx, int &m, int &k, int &j,
+                                            int &i) {
+  long long n = (long long)d.nmb * d.nx3 * d.nx2 * d.nx1;
+  if (idx >= n) return false;
+  i = (int)(idx % d.nx1) + d.is; idx /= d.nx1;
+  j = (int)(idx % d.nx2) + d.js; idx /= d.nx2;
+  k = (int)(idx % d.nx3) + d.ks; idx /= d.nx3;
+  m = (int)idx;
+  return true;
+}
+
+__global__ void k_gas_rk(Ind d, double *u0, const double *u1, int nv, double g0, double g1) {
+  int m, k, j, i;
+  if (!active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i)) return;
+  for (int v = 0; v < nv; ++v) {
+    long long a = d.at(m, nv, v, k, j, i);
+    u0[a] = g0 * u0[a] + g1 * u1[a];
+  }
+}
+
+__global__ void k_history(Ind d, double *u0, int nv, const double *dmom, double atw_dt) {
+  int m, k, j, i;
+  if (!active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i)) return;
+  for (int v = 0; v < 3; ++v) u0[d.at(m, nv, 1 + v, k, j, i)] += atw_dt * dmom[d.at(m, 3, v, k, j, i)];
+}
+
+// ---- ExplicitPush imex, src/dust/dust_push.cpp:262-297 ----------------------------------
+__global__ void k_push_imex(PCtx P, int three_d, int sbox, int strat, double q, double om,
+                            double gam0, double gam1, double beta_dt, double atw_dt) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  double x_old = P.r(DUSTB_IPX, p), y_old = P.r(DUSTB_IPY, p), z_old = P.r(DUSTB_IPZ, p);
+  double vx_old = P.r(DUSTB_IPVX, p), vy_old = P.r(DUSTB_IPVY, p), vz_old = P.r(DUSTB_IPVZ, p);
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  if (sbox) {
+    if (three_d) {
+      fx = 2.0 * om * vy_old;
+      fy = -(2.0 - q) * om * vx_old;
+      if (strat) fz = -(om * om) * z_old;
+    } else {
+      fx = 2.0 * om * vz_old;
+      fz = -(2.0 - q) * om * vx_old;
+    }
+  }
+  P.r(DUSTB_IPVX, p) = gam0 * vx_old + gam1 * P.r(DUSTB_IPVX1, p) + beta_dt * fx + atw_dt * P.r(DUSTB_IPRX, p);
+  P.r(DUSTB_IPVY, p) = gam0 * vy_old + gam1 * P.r(DUSTB_IPVY1, p) + beta_dt * fy + atw_dt * P.r(DUSTB_IPRY, p);
+  P.r(DUSTB_IPVZ, p) = gam0 * vz_old + gam1 * P.r(DUSTB_IPVZ1, p) + beta_dt * fz + atw_dt * P.r(DUSTB_IPRZ, p);
+  double ydot = vy_old;
+  if (sbox && three_d) ydot -= q * om * x_old;
+  P.r(DUSTB_IPX, p) = gam0 * x_old + gam1 * P.r(DUSTB_IPX1, p) + beta_dt * vx_old;
+  P.r(DUSTB_IPY, p) = gam0 * y_old + gam1 * P.r(DUSTB_IPY1, p) + beta_dt * ydot;
+  if (three_d) P.r(DUSTB_IPZ, p) = gam0 * z_old + gam1 * P.r(DUSTB_IPZ1, p) + beta_dt * vz_old;
+}
+
+// ---- SetNewPrtclGID, src/bvals/bvals_part.cpp:159-429 (single level, no shear x1) -------
+__global__ void k_route(PCtx P, MCtx M, Ind d, int x3bc, double *x3rem, unsigned *err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  int m = P.i(DUSTB_PGID, p) - M.gids;
+  if (!block_ok(d, m)) { report(err, DUSTB_ERR_PGID); return; }
+  const double z3a = M.x3min, z3b = M.x3max;
+  if (x3bc != 0 && (P.r(DUSTB_IPZ, p) < z3a || P.r(DUSTB_IPZ, p) >= z3b)) {
+    const bool lo = (P.r(DUSTB_IPZ, p) < z3a);
+    if (x3bc == 1) {
+      const double zf = lo ? z3a : z3b;
+      double z = 2.0 * zf - P.r(DUSTB_IPZ, p);
+      if (z >= z3b) z = z3b - 1.0e-12 * (z3b - z3a);
+      if (z < z3a) z = z3a;
+      P.r(DUSTB_IPZ, p) = z;
+      P.r(DUSTB_IPVZ, p) = -P.r(DUSTB_IPVZ, p);
+      P.r(DUSTB_IPZ1, p) = 2.0 * zf - P.r(DUSTB_IPZ1, p);
+      P.r(DUSTB_IPVZ1, p) = -P.r(DUSTB_IPVZ1, p);
+    } else {
+      if (x3rem) { atomicAdd(&x3rem[0], P.r(DUSTB_IPM, p)); atomicAdd(&x3rem[1], 1.0); }
+      P.r(DUSTB_IPM, p) = 0.0;
+      const double dz = M.s(m, DX3);
+      const double z = lo ? (M.s(m, X3MIN) + 0.5 * dz) : (M.s(m, X3MAX) - 0.5 * dz);
+      P.r(DUSTB_IPZ, p) = z;
+      P.r(DUSTB_IPVX, p) = 0.0; P.r(DUSTB_IPVY, p) = 0.0; P.r(DUSTB_IPVZ, p) = 0.0;
+      P.r(DUSTB_IPX1, p) = P.r(DUSTB_IPX, p); P.r(DUSTB_IPY1, p) = P.r(DUSTB_IPY, p);
+      P.r(DUSTB_IPZ1, p) = z;
+      P.r(DUSTB_IPVX1, p) = 0.0; P.r(DUSTB_IPVY1, p) = 0.0; P.r(DUSTB_IPVZ1, p) = 0.0;
+    }
+  }
+  double x1 = P.r(DUSTB_IPX, p), x2 = P.r(DUSTB_IPY, p), x3 = P.r(DUSTB_IPZ, p);
+  const double lx = M.s(m, X1MAX) - M.s(m, X1MIN);
+  const double ly = M.s(m, X2MAX) - M.s(m, X2MIN);
+  const double lz = M.s(m, X3MAX) - M.s(m, X3MIN);
+  int ix = (int)((x1 - M.s(m, X1MIN) + lx) / lx) - 1;
+  int iy = (int)((x2 - M.s(m, X2MIN) + ly) / ly) - 1;
+  int iz = (int)((x3 - M.s(m, X3MIN) + lz) / lz) - 1;
+  auto snap = [&](int off, double &x, double xa, double xb, int ipx, int irx) {
+    if (off != 0) return;
+    double xs = x;
+    if (x < xa) xs = xa;
+    else if (x >= xb) xs = nextafter(xb, xa);
+    if (xs != x) { P.r(irx, p) += xs - x; P.r(ipx, p) = xs; x = xs; }
+  };
+  snap(ix, x1, M.s(m, X1MIN), M.s(m, X1MAX), DUSTB_IPX, DUSTB_IPX1);
+  if (M.multi_d) snap(iy, x2, M.s(m, X2MIN), M.s(m, X2MAX), DUSTB_IPY, DUSTB_IPY1);
+  if (M.three_d) snap(iz, x3, M.s(m, X3MIN), M.s(m, X3MAX), DUSTB_IPZ, DUSTB_IPZ1);
+  if (!M.multi_d) iy = 0;
+  if (!M.three_d) iz = 0;
+  if (abs(ix) > 1 || abs(iy) > 1 || abs(iz) > 1) { report(err, DUSTB_ERR_ROUTE); return; }
+  if (ix == 0 && iy == 0 && iz == 0) return;
+  const bool lo1 = (ix < 0) && (M.s(m, X1MIN) < M.x1min + 0.5 * lx);
+  const bool hi1 = (ix > 0) && (M.s(m, X1MAX) > M.x1max - 0.5 * lx);
+  const bool lo2 = (iy < 0) && (M.s(m, X2MIN) < M.x2min + 0.5 * ly);
+  const bool hi2 = (iy > 0) && (M.s(m, X2MAX) > M.x2max - 0.5 * ly);
+  const bool lo3 = (iz < 0) && (M.s(m, X3MIN) < M.x3min + 0.5 * lz);
+  const bool hi3 = (iz > 0) && (M.s(m, X3MAX) > M.x3max - 0.5 * lz);
+  const int gid = M.nghbr[(long long)m * 27 + dir_slot(ix, iy, iz)];
+  if (gid < 0) { report(err, DUSTB_ERR_NGHBR); return; }
+  P.i(DUSTB_PGID, p) = gid;
+  const double Lx = M.x1max - M.x1min, Ly = M.x2max - M.x2min, Lz = M.x3max - M.x3min;
+  if (lo1) { P.r(DUSTB_IPX, p) += Lx; P.r(DUSTB_IPX1, p) += Lx; }
+  else if (hi1) { P.r(DUSTB_IPX, p) -= Lx; P.r(DUSTB_IPX1, p) -= Lx; }
+  if (lo2) { P.r(DUSTB_IPY, p) += Ly; P.r(DUSTB_IPY1, p) += Ly; }
+  else if (hi2) { P.r(DUSTB_IPY, p) -= Ly; P.r(DUSTB_IPY1, p) -= Ly; }
+  if (lo3) { P.r(DUSTB_IPZ, p) += Lz; P.r(DUSTB_IPZ1, p) += Lz; }
+  else if (hi3) { P.r(DUSTB_IPZ, p) -= Lz; P.r(DUSTB_IPZ1, p) -= Lz; }
+}
+
+// ---- DepositDrag imex scatter, src/dust/dust_pm.cpp:225-274 ------------------------------
+__global__ void k_scatter(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, double sh,
+                          unsigned *err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  int m = P.i(DUSTB_PGID, p) - M.gids;
+  if (!block_ok(d, m)) { report(err, DUSTB_ERR_PGID); return; }
+  int ip, jp, kp; double wx[3], wy[3], wz[3];
+  weights3(M, d, m, P.r(DUSTB_IPX, p), P.r(DUSTB_IPY, p) + sh * P.r(DUSTB_IPX, p),
+           P.r(DUSTB_IPZ, p), ip, jp, kp, wx, wy, wz);
+  if (!halo_ok(d, ip, jp, kp)) { report(err, DUSTB_ERR_HALO); return; }
+  double vol = cell_vol(M, d, m);
+  double cj = a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
+  double muc = P.r(DUSTB_IPM, p) * cj / vol;
+  double vx = P.r(DUSTB_IPVX, p), vy = P.r(DUSTB_IPVY, p), vz = P.r(DUSTB_IPVZ, p);
+  int clo = d.three_d ? 0 : 1, chi = d.three_d ? 2 : 1;
+  for (int c = clo; c <= chi; ++c)
+    for (int b = 0; b < 3; ++b) {
+      double wcb = wz[c] * wy[b] * muc;
+      if (wcb == 0.0) continue;
+      for (int a = 0; a < 3; ++a) {
+        double w = wcb * wx[a];
+        int kk = kp + c - 1, jj = jp + b - 1, ii = ip + a - 1;
+        atomicAdd(&qdep[d.at(m, 5, 0, kk, jj, ii)], w);
+        atomicAdd(&qdep[d.at(m, 5, 1, kk, jj, ii)], w * vx);
+        atomicAdd(&qdep[d.at(m, 5, 2, kk, jj, ii)], w * vy);
+        atomicAdd(&qdep[d.at(m, 5, 3, kk, jj, ii)], w * vz);
+      }
+    }
+}
+
+// ---- ghost exchanges (pull form, one thread per destination cell) -----------------------
+// RecvAndSumDeposit (src/bvals/bvals_dep.cpp:457-560): receiver active strips on side o
+// (InitRecvIndices :281-297) += the neighbour's ghost cells at index - o*nx, in
+// NeighborIndex order.
+__global__ void k_ghost_add(Ind d, const int *nghbr, int gids, double *a, int nvar) {
+  int m, k, j, i;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long ncell = (long long)d.nmb * d.nx3 * d.nx2 * d.nx1;
+  int v = (int)(idx / ncell);
+  if (v >= nvar) return;
+  if (!active_cell(d, idx - (long long)v * ncell, m, k, j, i)) return;
+  const int ng1 = d.ng - 1;
+  const bool near = (i <= d.is + ng1) || (i >= d.ie - ng1) || (j <= d.js + ng1 && d.multi_d) ||
+                    (j >= d.je - ng1 && d.multi_d) || (d.three_d && (k <= d.ks + ng1 || k >= d.ke - ng1));
+  if (!near) return;
+  const int ndir = d.three_d ? 26 : (d.multi_d ? 8 : 2);
+  const long long at = d.at(m, nvar, v, k, j, i);
+  double val = a[at];
+  for (int n = 0; n < ndir; ++n) {
+    const int o1 = kDirOrder[n][0], o2 = kDirOrder[n][1], o3 = kDirOrder[n][2];
+    if (o1 > 0 && i < d.ie - ng1) continue;
+    if (o1 < 0 && i > d.is + ng1) continue;
+    if (o2 > 0 && j < d.je - ng1) continue;
+    if (o2 < 0 && j > d.js + ng1) continue;
+    if (o3 > 0 && k < d.ke - ng1) continue;
+    if (o3 < 0 && k > d.ks + ng1) continue;
+    const int src = nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)] - gids;
+    if (src < 0 || src >= d.nmb) continue;
+    val += a[d.at(src, nvar, v, k - o3 * d.nx3, j - o2 * d.nx2, i - o1 * d.nx1)];
+  }
+  a[at] = val;
+}
+
+// copy exchange: every ghost cell <- the neighbour's active cell at index - o*nx
+__global__ void k_ghost_copy(Ind d, const int *nghbr, int gids, double *a, int nvar) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long per = d.cells();
+  long long tot = per * d.nmb;
+  if (idx >= tot) return;
+  int m = (int)(idx / per);
+  long long r = idx - (long long)m * per;
+  int i = (int)(r % d.n1); r /= d.n1;
+  int j = (int)(r % d.n2);
+  int k = (int)(r / d.n2);
+  int o1 = (i < d.is) ? -1 : ((i > d.ie) ? 1 : 0);
+  int o2 = (j < d.js) ? -1 : ((j > d.je) ? 1 : 0);
+  int o3 = (k < d.ks) ? -1 : ((k > d.ke) ? 1 : 0);
+  if (o1 == 0 && o2 == 0 && o3 == 0) return;
+  const int src = nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)] - gids;
+  if (src < 0 || src >= d.nmb) return;
+  for (int v = 0; v < nvar; ++v)
+    a[d.at(m, nvar, v, k, j, i)] = a[d.at(src, nvar, v, k - o3 * d.nx3, j - o2 * d.nx2, i - o1 * d.nx1)];
+}
+
+// UstarX3BCs, src/dust/dust_tasks.cpp:445-469
+__global__ void k_x3_bcs(Ind d, const int *nghbr, double *a, int refl) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long per = (long long)d.ng * d.n2 * d.n1;
+  if (idx >= per * d.nmb) return;
+  int m = (int)(idx / per);
+  long long r = idx - (long long)m * per;
+  int i = (int)(r % d.n1); r /= d.n1;
+  int j = (int)(r % d.n2);
+  int g = (int)(r / d.n2);
+  const bool lo_face = nghbr[(long long)m * 27 + dir_slot(0, 0, -1)] < 0;
+  const bool hi_face = nghbr[(long long)m * 27 + dir_slot(0, 0, 1)] < 0;
+  if (lo_face) {
+    int kg = d.ks - 1 - g, kc = refl ? (d.ks + g) : d.ks;
+    for (int v = 0; v < 3; ++v)
+      a[d.at(m, 3, v, kg, j, i)] = (refl && v == 2) ? -a[d.at(m, 3, v, kc, j, i)] : a[d.at(m, 3, v, kc, j, i)];
+  }
+  if (hi_face) {
+    int kg = d.ke + 1 + g, kc = refl ? (d.ke - g) : d.ke;
+    for (int v = 0; v < 3; ++v)
+      a[d.at(m, 3, v, kg, j, i)] = (refl && v == 2) ? -a[d.at(m, 3, v, kc, j, i)] : a[d.at(m, 3, v, kc, j, i)];
+  }
+}
+
+// ---- solve (dust_pm.cpp:426-436) --------------------------------------------------------
+__global__ void k_solve_ustar(Ind d, const double *u0, int nv, const double *qdep, double *us,
+                              int br) {
+  int m, k, j, i;
+  if (!active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i)) return;
+  double q0 = br ? qdep[d.at(m, 5, 0, k, j, i)] : 0.0;
+  double denom = 1.0 / (u0[d.at(m, nv, 0, k, j, i)] + q0);
+  for (int v = 0; v < 3; ++v) {
+    double qv = br ? qdep[d.at(m, 5, 1 + v, k, j, i)] : 0.0;
+    us[d.at(m, 3, v, k, j, i)] = (u0[d.at(m, nv, 1 + v, k, j, i)] + qv) * denom;
+  }
+}
+
+// ---- PointOperatorParticles, src/dust/dust_solver.cpp:151-201 ---------------------------
+__global__ void k_operator(PCtx P, MCtx M, Ind d, const double *field, double *result,
+                           double a_dt, double sh, unsigned *err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  int m = P.i(DUSTB_PGID, p) - M.gids;
+  if (!block_ok(d, m)) { report(err, DUSTB_ERR_PGID); return; }
+  int ip, jp, kp; double wx[3], wy[3], wz[3];
+  weights3(M, d, m, P.r(DUSTB_IPX, p), P.r(DUSTB_IPY, p) + sh * P.r(DUSTB_IPX, p),
+           P.r(DUSTB_IPZ, p), ip, jp, kp, wx, wy, wz);
+  if (!halo_ok(d, ip, jp, kp)) { report(err, DUSTB_ERR_HALO); return; }
+  double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+  int clo = d.three_d ? 0 : 1, chi = d.three_d ? 2 : 1;
+  for (int c = clo; c <= chi; ++c)
+    for (int b = 0; b < 3; ++b) {
+      double wcb = wz[c] * wy[b];
+      if (wcb == 0.0) continue;
+      for (int a = 0; a < 3; ++a) {
+        double w = wcb * wx[a];
+        int kk = kp + c - 1, jj = jp + b - 1, ii = ip + a - 1;
+        g0 += w * field[d.at(m, 3, 0, kk, jj, ii)];
+        g1 += w * field[d.at(m, 3, 1, kk, jj, ii)];
+        g2 += w * field[d.at(m, 3, 2, kk, jj, ii)];
+      }
+    }
+  double vol = cell_vol(M, d, m);
+  double cj = a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
+  double fac = P.r(DUSTB_IPM, p) * cj / vol;
+  for (int c = clo; c <= chi; ++c)
+    for (int b = 0; b < 3; ++b) {
+      double wcb = wz[c] * wy[b] * fac;
+      if (wcb == 0.0) continue;
+      for (int a = 0; a < 3; ++a) {
+        double w = wcb * wx[a];
+        int kk = kp + c - 1, jj = jp + b - 1, ii = ip + a - 1;
+        atomicAdd(&result[d.at(m, 3, 0, kk, jj, ii)], w * g0);
+        atomicAdd(&result[d.at(m, 3, 1, kk, jj, ii)], w * g1);
+        atomicAdd(&result[d.at(m, 3, 2, kk, jj, ii)], w * g2);
+      }
+    }
+}
+
+// dust_applya_dc, src/dust/dust_solver.cpp:243-252
+__global__ void k_dc_correct(Ind d, const double *u0, int nv, const double *qdep,
+                             const double *result, double *field) {
+  int m, k, j, i;
+  if (!active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i)) return;
+  double rho = u0[d.at(m, nv, 0, k, j, i)];
+  double pinv = 1.0 / (rho + qdep[d.at(m, 5, 0, k, j, i)]);
+  for (int v = 0; v < 3; ++v) {
+    long long a = d.at(m, 3, v, k, j, i);
+    double av = result[a] + rho * field[a];
+    double rv = u0[d.at(m, nv, 1 + v, k, j, i)] + qdep[d.at(m, 5, 1 + v, k, j, i)] - av;
+    field[a] += pinv * rv;
+  }
+}
+
+// ---- GatherKickPMBR, src/dust/dust_pm.cpp:500-564 ----------------------------------------
+__global__ void k_gather_kick(PCtx P, MCtx M, Ind d, const double *us, double *dmom, double a_dt,
+                              double sh, int br, unsigned *err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  int m = P.i(DUSTB_PGID, p) - M.gids;
+  if (!block_ok(d, m)) { report(err, DUSTB_ERR_PGID); return; }
+  int ip, jp, kp; double wx[3], wy[3], wz[3];
+  weights3(M, d, m, P.r(DUSTB_IPX, p), P.r(DUSTB_IPY, p) + sh * P.r(DUSTB_IPX, p),
+           P.r(DUSTB_IPZ, p), ip, jp, kp, wx, wy, wz);
+  if (!halo_ok(d, ip, jp, kp)) { report(err, DUSTB_ERR_HALO); return; }
+  double ux = 0.0, uy = 0.0, uz = 0.0;
+  int clo = d.three_d ? 0 : 1, chi = d.three_d ? 2 : 1;
+  for (int c = clo; c <= chi; ++c)
+    for (int b = 0; b < 3; ++b) {
+      double wcb = wz[c] * wy[b];
+      if (wcb == 0.0) continue;
+      for (int a = 0; a < 3; ++a) {
+        double w = wcb * wx[a];
+        int kk = kp + c - 1, jj = jp + b - 1, ii = ip + a - 1;
+        ux += w * us[d.at(m, 3, 0, kk, jj, ii)];
+        uy += w * us[d.at(m, 3, 1, kk, jj, ii)];
+        uz += w * us[d.at(m, 3, 2, kk, jj, ii)];
+      }
+    }
+  double cj = a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
+  double dvx = cj * (ux - P.r(DUSTB_IPVX, p));
+  double dvy = cj * (uy - P.r(DUSTB_IPVY, p));
+  double dvz = cj * (uz - P.r(DUSTB_IPVZ, p));
+  P.r(DUSTB_IPVX, p) += dvx; P.r(DUSTB_IPVY, p) += dvy; P.r(DUSTB_IPVZ, p) += dvz;
+  P.r(DUSTB_IPRX, p) = dvx / a_dt; P.r(DUSTB_IPRY, p) = dvy / a_dt; P.r(DUSTB_IPRZ, p) = dvz / a_dt;
+  if (!br) return;
+  double vol = cell_vol(M, d, m);
+  double fac = -P.r(DUSTB_IPM, p) / vol;
+  for (int c = clo; c <= chi; ++c)
+    for (int b = 0; b < 3; ++b) {
+      double wcb = wz[c] * wy[b] * fac;
+      if (wcb == 0.0) continue;
+      for (int a = 0; a < 3; ++a) {
+        double w = wcb * wx[a];
+        int kk = kp + c - 1, jj = jp + b - 1, ii = ip + a - 1;
+        atomicAdd(&dmom[d.at(m, 3, 0, kk, jj, ii)], w * dvx);
+        atomicAdd(&dmom[d.at(m, 3, 1, kk, jj, ii)], w * dvy);
+        atomicAdd(&dmom[d.at(m, 3, 2, kk, jj, ii)], w * dvz);
+      }
+    }
+}
+
+// ---- ApplyPMBR, src/dust/dust_pm.cpp:649-708 ---------------------------------------------
+__device__ __forceinline__ bool center_cell(const PCtx &P, const MCtx &M, const Ind &d, int p,
+                                            int &m, int &ip, int &jp, int &kp) {
+  m = P.i(DUSTB_PGID, p) - M.gids;
+  if (!block_ok(d, m)) return false;
+  double w[3];
+  pm_weights(P.r(DUSTB_IPX, p), M.s(m, X1MIN), M.s(m, X1MAX), d.nx1, d.is, M.scheme, ip, w);
+  pm_weights(P.r(DUSTB_IPY, p), M.s(m, X2MIN), M.s(m, X2MAX), d.nx2, d.js, M.scheme, jp, w);
+  if (d.three_d) pm_weights(P.r(DUSTB_IPZ, p), M.s(m, X3MIN), M.s(m, X3MAX), d.nx3, d.ks, M.scheme, kp, w);
+  else kp = d.ks;
+  return halo_ok(d, ip, jp, kp);
+}
+
+__global__ void k_center_mass(PCtx P, MCtx M, Ind d, double *res, double a_dt, unsigned *err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  if (P.r(DUSTB_IPM, p) <= 0.0) return;
+  int m, ip, jp, kp;
+  if (!center_cell(P, M, d, p, m, ip, jp, kp)) { report(err, DUSTB_ERR_HALO); return; }
+  double vol = cell_vol(M, d, m);
+  atomicAdd(&res[d.at(m, 4, 3, kp, jp, ip)],
+            P.r(DUSTB_IPM, p) * (a_dt / (P.r(DUSTB_IPTS, p) + a_dt)) / vol);
+}
+
+__global__ void k_consistent_gas(Ind d, double *u0, int nv, const double *us, const double *qdep,
+                                 double *dmom, double *res, double inv_adt) {
+  int m, k, j, i;
+  if (!active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i)) return;
+  const double rho = u0[d.at(m, nv, 0, k, j, i)], qt = res[d.at(m, 4, 3, k, j, i)];
+  const double q = qdep[d.at(m, 5, 0, k, j, i)];
+  for (int v = 0; v < 3; ++v) {
+    long long a3 = d.at(m, 3, v, k, j, i);
+    long long au = d.at(m, nv, 1 + v, k, j, i);
+    double dgas = dmom[a3];
+    if (qt > 0.0) {
+      const double g = rho * us[a3] - u0[au];
+      const double r = (dmom[a3] - g) / (rho + q);
+      dgas = g + rho * r;
+      res[d.at(m, 4, v, k, j, i)] = r * q / qt;
+    }
+    u0[au] += dgas;
+    dmom[a3] = dgas * inv_adt;
+  }
+}
+
+__global__ void k_consistent_dust(PCtx P, MCtx M, Ind d, const double *res, double a_dt) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  if (P.r(DUSTB_IPM, p) <= 0.0) return;
+  int m, ip, jp, kp;
+  if (!center_cell(P, M, d, p, m, ip, jp, kp)) return;
+  const double cj = a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
+  for (int v = 0; v < 3; ++v) {
+    const double dv = cj * res[d.at(m, 4, v, kp, jp, ip)];
+    P.r(DUSTB_IPVX + 2 * v, p) += dv;
+    P.r(DUSTB_IPRX + v, p) += dv / a_dt;
+  }
+}
+
+__global__ void k_pmbr(Ind d, double *u0, int nv, double *dmom, double inv_adt) {
+  int m, k, j, i;
+  if (!active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i)) return;
+  for (int v = 0; v < 3; ++v) {
+    long long a3 = d.at(m, 3, v, k, j, i);
+    u0[d.at(m, nv, 1 + v, k, j, i)] += dmom[a3];
+    dmom[a3] *= inv_adt;
+  }
+}
+
+// ---- reductions: newdt, stopping times ---------------------------------------------------
+__device__ __forceinline__ void atomic_min_pos(double *a, double v) {
+  atomicMin((unsigned long long *)a, (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void atomic_max_pos(double *a, double v) {
+  atomicMax((unsigned long long *)a, (unsigned long long)__double_as_longlong(v));
+}
+
+__global__ void k_set(double *a, double v0, int two, double v1) {
+  a[0] = v0;
+  if (two) a[1] = v1;
+}
+
+__global__ void k_newdt(PCtx P, MCtx M, Ind d, int shear3d, double qo, double *out) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  double t = (double)FLT_MAX;
+  if (p < P.npart) {
+    int m = P.i(DUSTB_PGID, p) - M.gids;
+    if (block_ok(d, m)) {
+      double vy = P.r(DUSTB_IPVY, p);
+      if (shear3d) vy -= qo * P.r(DUSTB_IPX, p);
+      t = fmin(M.s(m, DX1) / fmax(fabs(P.r(DUSTB_IPVX, p)), 1.0e-30), t);
+      t = fmin(M.s(m, DX2) / fmax(fabs(vy), 1.0e-30), t);
+      if (d.three_d) t = fmin(M.s(m, DX3) / fmax(fabs(P.r(DUSTB_IPVZ, p)), 1.0e-30), t);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) t = fmin(t, __shfl_xor_sync(0xffffffffu, t, o));
+  if ((threadIdx.x & 31) == 0) atomic_min_pos(out, t);
+}
+
+__global__ void k_scale(double *a, double s) { a[0] = s * a[0]; }
+
+__global__ void k_tstop(PCtx P, double *out, unsigned *err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  double mx = 0.0, mn = DBL_MAX;
+  if (p < P.npart) {
+    double ts = P.r(DUSTB_IPTS, p);
+    int s = P.i(DUSTB_PSP, p);
+    bool bad = (s < 0 || !isfinite(ts) || !(ts > 0.0));
+    if (bad) report(err, DUSTB_ERR_TSTOP);
+    mx = bad ? DBL_MAX : ts;
+    mn = (ts > 0.0) ? ts : DBL_MAX;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+  }
+  if ((threadIdx.x & 31) == 0) { atomic_max_pos(&out[0], mx); atomic_min_pos(&out[1], mn); }
+}
+
+// ---- pc2 ---------------------------------------------------------------------------------
+// DepositDrag pc2 predictor, src/dust/dust_pm.cpp:141-193
+__global__ void k_pc2_predictor(PCtx P, MCtx M, Ind d, const double *uold, int nv, double *qdep,
+                                double dt, int rate_dep, unsigned *err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  int m = P.i(DUSTB_PGID, p) - M.gids;
+  if (!block_ok(d, m)) { report(err, DUSTB_ERR_PGID); return; }
+  int ip, jp, kp; double wx[3], wy[3], wz[3];
+  weights3(M, d, m, P.r(DUSTB_IPX, p), P.r(DUSTB_IPY, p), P.r(DUSTB_IPZ, p), ip, jp, kp, wx, wy, wz);
+  if (!halo_ok(d, ip, jp, kp)) { report(err, DUSTB_ERR_HALO); return; }
+  double ugx = 0.0, ugy = 0.0, ugz = 0.0;
+  int clo = d.three_d ? 0 : 1, chi = d.three_d ? 2 : 1;
+  for (int c = clo; c <= chi; ++c)
+    for (int b = 0; b < 3; ++b) {
+      double wcb = wz[c] * wy[b];
+      if (wcb == 0.0) continue;
+      for (int a = 0; a < 3; ++a) {
+        double w = wcb * wx[a];
+        int kk = kp + c - 1, jj = jp + b - 1, ii = ip + a - 1;
+        double invrho = 1.0 / uold[d.at(m, nv, 0, kk, jj, ii)];
+        ugx += w * uold[d.at(m, nv, 1, kk, jj, ii)] * invrho;
+        ugy += w * uold[d.at(m, nv, 2, kk, jj, ii)] * invrho;
+        ugz += w * uold[d.at(m, nv, 3, kk, jj, ii)] * invrho;
+      }
+    }
+  double vol = cell_vol(M, d, m);
+  double rate = P.r(DUSTB_IPM, p) / (P.r(DUSTB_IPTS, p) * vol);
+  double gx = -dt * rate * (ugx - P.r(DUSTB_IPVX, p));
+  double gy = -dt * rate * (ugy - P.r(DUSTB_IPVY, p));
+  double gz = -dt * rate * (ugz - P.r(DUSTB_IPVZ, p));
+  for (int c = clo; c <= chi; ++c)
+    for (int b = 0; b < 3; ++b) {
+      double wcb = wz[c] * wy[b];
+      if (wcb == 0.0) continue;
+      for (int a = 0; a < 3; ++a) {
+        double w = wcb * wx[a];
+        int kk = kp + c - 1, jj = jp + b - 1, ii = ip + a - 1;
+        atomicAdd(&qdep[d.at(m, 5, 1, kk, jj, ii)], w * gx);
+        atomicAdd(&qdep[d.at(m, 5, 2, kk, jj, ii)], w * gy);
+        atomicAdd(&qdep[d.at(m, 5, 3, kk, jj, ii)], w * gz);
+        if (rate_dep) atomicAdd(&qdep[d.at(m, 5, 4, kk, jj, ii)], w * rate);
+      }
+    }
+}
+
+// UpdateStiffness's maximum of qdep4/rho (dust_pm.cpp:295-301), before the damping
+__global__ void k_pc2_rate_max(Ind d, const double *u0, int nv, const double *qdep, double *out) {
+  int m, k, j, i;
+  double r = 0.0;
+  if (active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i))
+    r = qdep[d.at(m, 5, 4, k, j, i)] / u0[d.at(m, nv, 0, k, j, i)];
+  for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+  if ((threadIdx.x & 31) == 0 && r > 0.0) atomic_max_pos(out, r);
+}
+
+// dust_pc2_apply_predictor, dust_pm.cpp:387-402
+__global__ void k_pc2_apply(Ind d, double *u0, int nv, double *qdep, double dt, int damp) {
+  int m, k, j, i;
+  if (!active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i)) return;
+  if (damp) {
+    const double chi = dt * qdep[d.at(m, 5, 4, k, j, i)] / u0[d.at(m, nv, 0, k, j, i)];
+    if (chi > 1.0) {
+      const double s = 1.0 / chi;
+      for (int v = 1; v <= 3; ++v) qdep[d.at(m, 5, v, k, j, i)] *= s;
+    }
+  }
+  for (int v = 1; v <= 3; ++v) u0[d.at(m, nv, v, k, j, i)] += qdep[d.at(m, 5, v, k, j, i)];
+}
+
+// dust_gas_midpoint, dust_push.cpp:53-59 (ghosts included)
+__global__ void k_pc2_midpoint(Ind d, const double *u0, const double *u1, int nv, double *us) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long per = d.cells();
+  if (idx >= per * d.nmb) return;
+  int m = (int)(idx / per);
+  long long c = idx - (long long)m * per;
+  const long long b0 = ((long long)m * nv) * per + c;
+  double inv = 1.0 / (u1[b0] + u0[b0]);
+  for (int v = 0; v < 3; ++v) {
+    long long bv = ((long long)m * nv + 1 + v) * per + c;
+    us[((long long)m * 3 + v) * per + c] = (u1[bv] + u0[bv]) * inv;
+  }
+}
+
+// dust_pc2_advance, src/dust/dust_push.cpp:132-245
+__global__ void k_pc2_advance(PCtx P, MCtx M, Ind d, const double *us, double *dmom, double dt,
+                              int br, int sbox, int strat, double q, double om, double aphi,
+                              unsigned *err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  int m = P.i(DUSTB_PGID, p) - M.gids;
+  if (!block_ok(d, m)) { report(err, DUSTB_ERR_PGID); return; }
+  const bool three_d = d.three_d;
+  double x0 = P.r(DUSTB_IPX1, p), y0 = P.r(DUSTB_IPY1, p), z0 = P.r(DUSTB_IPZ1, p);
+  double vx0 = P.r(DUSTB_IPVX1, p), vy0 = P.r(DUSTB_IPVY1, p), vz0 = P.r(DUSTB_IPVZ1, p);
+  double xh = x0 + 0.5 * dt * vx0;
+  double yh = y0 + 0.5 * dt * (vy0 - ((sbox && three_d) ? q * om * x0 : 0.0));
+  double zh = three_d ? z0 + 0.5 * dt * vz0 : z0;
+  double yg = yh + ((sbox && three_d) ? q * om * xh * 0.5 * dt : 0.0);
+  int ip, jp, kp; double wx[3], wy[3], wz[3];
+  weights3(M, d, m, xh, yg, zh, ip, jp, kp, wx, wy, wz);
+  if (!halo_ok(d, ip, jp, kp)) { report(err, DUSTB_ERR_HALO); return; }
+  double ugx = 0.0, ugy = 0.0, ugz = 0.0;
+  int clo = three_d ? 0 : 1, chi = three_d ? 2 : 1;
+  for (int c = clo; c <= chi; ++c)
+    for (int b = 0; b < 3; ++b) {
+      double wcb = wz[c] * wy[b];
+      if (wcb == 0.0) continue;
+      for (int a = 0; a < 3; ++a) {
+        double w = wcb * wx[a];
+        int kk = kp + c - 1, jj = jp + b - 1, ii = ip + a - 1;
+        ugx += w * us[d.at(m, 3, 0, kk, jj, ii)];
+        ugy += w * us[d.at(m, 3, 1, kk, jj, ii)];
+        ugz += w * us[d.at(m, 3, 2, kk, jj, ii)];
+      }
+    }
+  double h = 0.5 * dt;
+  double lambda = h / P.r(DUSTB_IPTS, p);
+  double aa = 1.0 + lambda;
+  double rx = vx0 + lambda * ugx, ry = vy0 + lambda * ugy, rz = vz0 + lambda * ugz;
+  double vxh, vyh, vzh;
+  if (sbox && three_d) {
+    double cxy = 2.0 * h * om, cyx = h * (2.0 - q) * om;
+    double det = aa * aa + cxy * cyx;
+    vxh = (aa * rx + cxy * ry) / det;
+    vyh = (aa * ry - cyx * rx) / det;
+    if (strat) rz -= h * (om * om) * zh;
+    vzh = rz / aa;
+  } else if (sbox) {
+    double cxz = 2.0 * h * om, czx = h * (2.0 - q) * om;
+    double det = aa * aa + cxz * czx;
+    if (aphi != 0.0) rz += h * aphi;
+    vxh = (aa * rx + cxz * rz) / det;
+    vzh = (aa * rz - czx * rx) / det;
+    vyh = ry / aa;
+  } else {
+    vxh = rx / aa; vyh = ry / aa; vzh = rz / aa;
+  }
+  P.r(DUSTB_IPVX, p) = 2.0 * vxh - vx0;
+  P.r(DUSTB_IPVY, p) = 2.0 * vyh - vy0;
+  P.r(DUSTB_IPVZ, p) = 2.0 * vzh - vz0;
+  P.r(DUSTB_IPX, p) = x0 + dt * vxh;
+  P.r(DUSTB_IPY, p) = y0 + dt * (vyh - ((sbox && three_d) ? q * om * xh : 0.0));
+  if (three_d) P.r(DUSTB_IPZ, p) = z0 + dt * vzh;
+  P.r(DUSTB_IPX1, p) = xh; P.r(DUSTB_IPY1, p) = yh; P.r(DUSTB_IPZ1, p) = zh;
+  double dvx = dt * (ugx - vxh) / P.r(DUSTB_IPTS, p);
+  double dvy = dt * (ugy - vyh) / P.r(DUSTB_IPTS, p);
+  double dvz = dt * (ugz - vzh) / P.r(DUSTB_IPTS, p);
+  P.r(DUSTB_IPRX, p) = dvx; P.r(DUSTB_IPRY, p) = dvy; P.r(DUSTB_IPRZ, p) = dvz;
+  if (!br) return;
+  double vol = cell_vol(M, d, m);
+  double fac = -P.r(DUSTB_IPM, p) / vol;
+  for (int c = clo; c <= chi; ++c)
+    for (int b = 0; b < 3; ++b) {
+      double wcb = wz[c] * wy[b] * fac;
+      if (wcb == 0.0) continue;
+      for (int a = 0; a < 3; ++a) {
+        double w = wcb * wx[a];
+        int kk = kp + c - 1, jj = jp + b - 1, ii = ip + a - 1;
+        atomicAdd(&dmom[d.at(m, 3, 0, kk, jj, ii)], w * dvx);
+        atomicAdd(&dmom[d.at(m, 3, 1, kk, jj, ii)], w * dvy);
+        atomicAdd(&dmom[d.at(m, 3, 2, kk, jj, ii)], w * dvz);
+      }
+    }
+}
+
+// dust_pc2_commit, dust_pm.cpp:596-601
+__global__ void k_pc2_commit(Ind d, double *u0, int nv, const double *dmom, const double *qdep,
+                             double wpred) {
+  int m, k, j, i;
+  if (!active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i)) return;
+  for (int v = 0; v < 3; ++v)
+    u0[d.at(m, nv, 1 + v, k, j, i)] += dmom[d.at(m, 3, v, k, j, i)] - wpred * qdep[d.at(m, 5, 1 + v, k, j, i)];
+}
+
+long long n_active(const Ind &d) { return (long long)d.nmb * d.nx3 * d.nx2 * d.nx1; }
+long long n_all(const Ind &d) { return d.cells() * d.nmb; }
+
+bool ctx_ok(const dustb_ctx *c) {
+  if (!c) return false;
+  const dustb_mesh &m = c->mesh;
+  if (m.nmb <= 0 || m.nx1 <= 0 || m.ng < 2 || !m.mb_size || !m.nghbr || !m.multi_d) return false;
+  if (m.three_d && m.nx3 <= 0) return false;
+  // every ghost cell must map to an active cell of one neighbour
+  if (m.nx1 < m.ng || (m.multi_d && m.nx2 < m.ng) || (m.three_d && m.nx3 < m.ng)) return false;
+  if (c->part.npart < 0 || (c->part.npart > 0 && (!c->part.pr || !c->part.pi))) return false;
+  if (c->part.npart > c->part.stride) return false;
+  if (c->f.nvar_gas < 4) return false;
+  return true;
+}
+
+}  // namespace
+
+// ---- host error bookkeeping --------------------------------------------------------------
+namespace dustb_host {
+static char g_err[256] = "";
+void set_error(const char *what, cudaError_t e) {
+  snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
+}
+int launch_status(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { set_error(what, e); return DUSTB_ELAUNCH; }
+  return DUSTB_OK;
+}
+}  // namespace dustb_host
+
+using dustb_host::launch_status;
+
+#define CHECK_CTX(c) do { if (!ctx_ok(c)) { return DUSTB_EINVAL; } } while (0)
+#define PGRID(c) blocks_for((c)->part.npart), kThreads, 0, S(stream)
+
+extern "C" {
+
+int dustb_version(void) { return 1; }
+const char *dustb_last_error(void) { return dustb_host::g_err; }
+
+int dustb_register_copy(const dustb_ctx *c, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  size_t bytes = (size_t)n_all(d) * c->f.nvar_gas * sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(c->f.u1, c->f.u0, bytes, cudaMemcpyDeviceToDevice, S(stream));
+  if (e != cudaSuccess) { dustb_host::set_error("register_copy", e); return DUSTB_ELAUNCH; }
+  if (c->part.npart > 0) k_reg_copy<<<PGRID(c)>>>(pview(c));
+  return launch_status("register_copy");
+}
+
+int dustb_gas_rk_noflux(const dustb_ctx *c, double gam0, double gam1, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  k_gas_rk<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.u1, c->f.nvar_gas, gam0, gam1);
+  return launch_status("gas_rk_noflux");
+}
+
+int dustb_history_gas(const dustb_ctx *c, double atw_dt, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  k_history<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, atw_dt);
+  return launch_status("history_gas");
+}
+
+int dustb_push_imex(const dustb_ctx *c, double gam0, double gam1, double beta_dt, double atw_dt,
+                    void *stream) {
+  CHECK_CTX(c);
+  if (c->part.npart == 0) return DUSTB_OK;
+  k_push_imex<<<PGRID(c)>>>(pview(c), c->mesh.three_d, c->phys.shearing_box, c->phys.stratified,
+                            c->phys.qshear, c->phys.omega0, gam0, gam1, beta_dt, atw_dt);
+  return launch_status("push_imex");
+}
+
+int dustb_route(const dustb_ctx *c, double *x3_removed, void *stream) {
+  CHECK_CTX(c);
+  if (c->mesh.x3bc == DUSTB_X3_OUTFLOW && !x3_removed) return DUSTB_EINVAL;
+  if (c->part.npart == 0) return DUSTB_OK;
+  Ind d = make_ind(c->mesh);
+  k_route<<<PGRID(c)>>>(pview(c), mview(c), d, c->mesh.x3bc, x3_removed, c->err);
+  return launch_status("route");
+}
+
+int dustb_deposit_qp(const dustb_ctx *c, double a_dt, double sh, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  cudaMemsetAsync(c->f.qdep, 0, (size_t)n_all(d) * 5 * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_scatter<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, c->err);
+  return launch_status("deposit_qp");
+}
+
+int dustb_ghost_add(const dustb_ctx *c, double *field, int nvar, void *stream) {
+  CHECK_CTX(c);
+  if (!field || nvar <= 0) return DUSTB_EINVAL;
+  Ind d = make_ind(c->mesh);
+  k_ghost_add<<<blocks_for(n_active(d) * nvar), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar);
+  return launch_status("ghost_add");
+}
+
+int dustb_ghost_copy(const dustb_ctx *c, double *field, int nvar, int x3_bcs, void *stream) {
+  CHECK_CTX(c);
+  if (!field || nvar <= 0) return DUSTB_EINVAL;
+  Ind d = make_ind(c->mesh);
+  k_ghost_copy<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar);
+  if (x3_bcs && nvar == 3 && d.three_d && c->mesh.x3bc != DUSTB_X3_PERIODIC)
+    k_x3_bcs<<<blocks_for((long long)d.ng * d.n2 * d.n1 * d.nmb), kThreads, 0, S(stream)>>>(
+        d, c->mesh.nghbr, field, c->mesh.x3bc == DUSTB_X3_REFLECT);
+  return launch_status("ghost_copy");
+}
+
+int dustb_solve_ustar(const dustb_ctx *c, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  k_solve_ustar<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.qdep,
+                                                                     c->f.ustar, c->phys.back_reaction);
+  return launch_status("solve_ustar");
+}
+
+int dustb_dc1_sweep(const dustb_ctx *c, double a_dt, double sh, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  int rc = dustb_ghost_copy(c, c->f.ustar, 3, 1, stream);
+  if (rc) return rc;
+  cudaMemsetAsync(c->f.work, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_operator<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.ustar, c->f.work, a_dt, sh, c->err);
+  rc = dustb_ghost_add(c, c->f.work, 3, stream);
+  if (rc) return rc;
+  k_dc_correct<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.qdep,
+                                                                    c->f.work, c->f.ustar);
+  return launch_status("dc1_sweep");
+}
+
+int dustb_gather_kick_pmbr(const dustb_ctx *c, double a_dt, double sh, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  const int br = c->phys.back_reaction;
+  if (br) cudaMemsetAsync(c->f.dmom, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_gather_kick<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.ustar, c->f.dmom, a_dt, sh, br, c->err);
+  return launch_status("gather_kick_pmbr");
+}
+
+int dustb_apply_pmbr(const dustb_ctx *c, double a_dt, void *stream) {
+  CHECK_CTX(c);
+  if (!c->phys.back_reaction) return DUSTB_OK;
+  Ind d = make_ind(c->mesh);
+  const double inv_adt = 1.0 / a_dt;
+  if (!c->phys.consistent_gas) {
+    k_pmbr<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, inv_adt);
+    return launch_status("apply_pmbr");
+  }
+  cudaMemsetAsync(c->f.resid, 0, (size_t)n_all(d) * 4 * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_center_mass<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, c->err);
+  k_consistent_gas<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(
+      d, c->f.u0, c->f.nvar_gas, c->f.ustar, c->f.qdep, c->f.dmom, c->f.resid, inv_adt);
+  if (c->part.npart > 0)
+    k_consistent_dust<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt);
+  return launch_status("apply_pmbr");
+}
+
+int dustb_newdt(const dustb_ctx *c, double dt_cfl, double *dt_out, void *stream) {
+  CHECK_CTX(c);
+  if (!dt_out) return DUSTB_EINVAL;
+  Ind d = make_ind(c->mesh);
+  k_set<<<1, 1, 0, S(stream)>>>(dt_out, (double)FLT_MAX, 0, 0.0);
+  if (c->part.npart > 0)
+    k_newdt<<<PGRID(c)>>>(pview(c), mview(c), d, c->phys.shearing_box && d.three_d,
+                          c->phys.qshear * c->phys.omega0, dt_out);
+  k_scale<<<1, 1, 0, S(stream)>>>(dt_out, dt_cfl);
+  return launch_status("newdt");
+}
+
+int dustb_tstop_extrema(const dustb_ctx *c, double *out, void *stream) {
+  CHECK_CTX(c);
+  if (!out) return DUSTB_EINVAL;
+  k_set<<<1, 1, 0, S(stream)>>>(out, 0.0, 1, DBL_MAX);
+  if (c->part.npart > 0) k_tstop<<<PGRID(c)>>>(pview(c), out, c->err);
+  return launch_status("tstop_extrema");
+}
+
+int dustb_pc2_predictor(const dustb_ctx *c, double dt, int rate_dep, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  cudaMemsetAsync(c->f.qdep, 0, (size_t)n_all(d) * 5 * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_pc2_predictor<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.u1, c->f.nvar_gas, c->f.qdep, dt,
+                                  rate_dep, c->err);
+  return launch_status("pc2_predictor");
+}
+
+int dustb_pc2_apply_predictor(const dustb_ctx *c, double dt, double *chi_max, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  if (chi_max) {
+    k_set<<<1, 1, 0, S(stream)>>>(chi_max, 0.0, 0, 0.0);
+    k_pc2_rate_max<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.qdep, chi_max);
+    k_scale<<<1, 1, 0, S(stream)>>>(chi_max, dt);
+  }
+  k_pc2_apply<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.qdep, dt,
+                                                                   c->phys.pc2_feedback_damping);
+  return launch_status("pc2_apply_predictor");
+}
+
+int dustb_pc2_midpoint(const dustb_ctx *c, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  k_pc2_midpoint<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.u1, c->f.nvar_gas, c->f.ustar);
+  return launch_status("pc2_midpoint");
+}
+
+int dustb_pc2_advance(const dustb_ctx *c, double dt, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  const int br = c->phys.back_reaction;
+  if (br) cudaMemsetAsync(c->f.dmom, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_pc2_advance<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.ustar, c->f.dmom, dt, br,
+                                c->phys.shearing_box, c->phys.stratified, c->phys.qshear,
+                                c->phys.omega0, c->phys.const_accel_phi, c->err);
+  return launch_status("pc2_advance");
+}
+
+int dustb_pc2_commit(const dustb_ctx *c, double wpred, void *stream) {
+  CHECK_CTX(c);
+  Ind d = make_ind(c->mesh);
+  k_pc2_commit<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom,
+                                                                    c->f.qdep, wpred);
+  return launch_status("pc2_commit");
+}
+
+// one imex2+ cycle in the task order of src/dust/dust_tasks.cpp:38-120 (stage 3 dormant,
+// dust.cpp:1646-1649); tableau src/driver/driver.cpp:278-300
+int dustb_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co, double *x3_removed,
+                     void *stream) {
+  CHECK_CTX(c);
+  if (!co || !(co->dt > 0.0)) return DUSTB_EINVAL;
+  const double g = co->gamma, dt = co->dt;
+  const double gam0[2] = {1.0, (2.0 * g - 1.0) / (2.0 * g * g)};
+  const double gam1[2] = {0.0, 1.0 - (2.0 * g - 1.0) / (2.0 * g * g)};
+  const double beta[2] = {g, 1.0 / (2.0 * g)};
+  const double atw22 = (1.0 - 2.0 * g * g) / 2.0 / g;
+  const double a_dt = g * dt;
+  const int br = c->phys.back_reaction;
+  int rc;
+#define RUN(x) do { rc = (x); if (rc) return rc; } while (0)
+  for (int stage = 1; stage <= 2; ++stage) {
+    if (stage == 1) RUN(dustb_register_copy(c, stream));
+    RUN(dustb_gas_rk_noflux(c, gam0[stage - 1], gam1[stage - 1], stream));
+    if (stage == 2 && br) RUN(dustb_history_gas(c, atw22 * dt, stream));
+    RUN(dustb_push_imex(c, gam0[stage - 1], gam1[stage - 1], beta[stage - 1] * dt,
+                        (stage == 2) ? atw22 * dt : 0.0, stream));
+    RUN(dustb_route(c, x3_removed, stream));
+    const double sh = co->sh[stage - 1];
+    if (br) {
+      RUN(dustb_deposit_qp(c, a_dt, sh, stream));
+      RUN(dustb_ghost_add(c, c->f.qdep, 5, stream));
+    }
+    RUN(dustb_solve_ustar(c, stream));
+    if (br && c->phys.drag_solver >= DUSTB_SOLVER_DC1) {
+      int nsw = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
+      for (int w = 0; w < nsw; ++w) RUN(dustb_dc1_sweep(c, a_dt, sh, stream));
+    }
+    RUN(dustb_ghost_copy(c, c->f.ustar, 3, 1, stream));
+    RUN(dustb_gather_kick_pmbr(c, a_dt, sh, stream));
+    if (br) {
+      RUN(dustb_ghost_add(c, c->f.dmom, 3, stream));
+      RUN(dustb_apply_pmbr(c, a_dt, stream));
+    }
+    RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, stream));
+  }
+  return DUSTB_OK;
+}
+
+// one pc2 cycle (integrator rk2): stage 1 predictor, stage 2 midpoint advance and commit
+int dustb_pc2_cycle(const dustb_ctx *c, double dt, double *chi_max, double *x3_removed,
+                    void *stream) {
+  CHECK_CTX(c);
+  if (!(dt > 0.0)) return DUSTB_EINVAL;
+  const int br = c->phys.back_reaction;
+  int rc;
+  RUN(dustb_register_copy(c, stream));
+  RUN(dustb_gas_rk_noflux(c, 1.0, 0.0, stream));
+  if (br) {
+    RUN(dustb_pc2_predictor(c, dt, 1, stream));
+    RUN(dustb_ghost_add(c, c->f.qdep, 5, stream));
+    RUN(dustb_pc2_apply_predictor(c, dt, chi_max, stream));
+  }
+  RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, stream));
+  RUN(dustb_pc2_midpoint(c, stream));
+  RUN(dustb_gas_rk_noflux(c, 0.5, 0.5, stream));
+  RUN(dustb_pc2_advance(c, dt, stream));
+  RUN(dustb_route(c, x3_removed, stream));
+  if (br) {
+    RUN(dustb_ghost_add(c, c->f.dmom, 3, stream));
+    RUN(dustb_pc2_commit(c, 0.5, stream));
+  }
+  RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, stream));
+#undef RUN
+  return DUSTB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,267 @@
+// dustb_sort.cu -- particle cell index (a CSR over cells) and the cell sort of the
+// particle SoA (DustGasDrag::SortParticles, src/dust/dust_cloud_device.cpp:1881-1977).
+//
+// The reference sorts 64-bit keys (block*ncell + cell)*npart + p with thrust::sort.  The same
+// permutation comes from a counting sort over the cell key (one bucket per cell: the bucket
+// count fits the mesh arrays anyway), followed by ordering each bucket by particle index.
+// Steps: key + histogram (atomics on the cell counters), exclusive scan of the counters,
+// scatter of the particle indices with per-cell cursors, per-cell sort of the (short)
+// index runs.  Every result is deterministic.
+#include <cstdint>
+
+#include "dustb_common.cuh"
+#include "dustb_sort.cuh"
+
+using namespace dustb;
+
+namespace {
+
+constexpr int kT = 256;
+constexpr int kScanT = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanT * kScanItems;
+
+inline unsigned nblk(long long n, int t = kT) {
+  long long b = (n + t - 1) / t;
+  return (unsigned)(b < 1 ? 1 : b);
+}
+
+// SortParticles' key of particle p (dust_cloud_device.cpp:1900-1916)
+__global__ void k_keys(const double *pr, const int *pi, long long stride, int npart,
+                       const double *mb, int gids, int nmb, int nx1, int nx2, int nx3, int z3,
+                       int *key, int *count) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npart) return;
+  int m = pi[(long long)DUSTB_PGID * stride + p] - gids;
+  m = (m < 0) ? 0 : ((m >= nmb) ? nmb - 1 : m);
+  const double *s = mb + (long long)m * 9;
+  int i = (int)floor((pr[(long long)DUSTB_IPX * stride + p] - s[X1MIN]) / s[DX1]);
+  int j = (int)floor((pr[(long long)DUSTB_IPY * stride + p] - s[X2MIN]) / s[DX2]);
+  i = (i < 0) ? 0 : ((i >= nx1) ? nx1 - 1 : i);
+  j = (j < 0) ? 0 : ((j >= nx2) ? nx2 - 1 : j);
+  int k = 0;
+  if (z3) {
+    k = (int)floor((pr[(long long)DUSTB_IPZ * stride + p] - s[X3MIN]) / s[DX3]);
+    k = (k < 0) ? 0 : ((k >= nx3) ? nx3 - 1 : k);
+  }
+  const int c = m * (nx1 * nx2 * nx3) + (k * nx2 + j) * nx1 + i;
+  key[p] = c;
+  atomicAdd(&count[c], 1);
+}
+
+// ---- exclusive scan of n ints in place (three kernels) ---------------------------------
+__device__ __forceinline__ int block_excl_scan(int v, int *sh, int &total) {
+  // warp inclusive scan
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    sh[lane] = w;    // inclusive warp totals
+  }
+  __syncthreads();
+  total = sh[(blockDim.x >> 5) - 1];
+  int base = (warp > 0) ? sh[warp - 1] : 0;
+  __syncthreads();
+  return base + x - v;
+}
+
+__global__ void k_scan_reduce(const int *a, long long n, int *bsum) {
+  __shared__ int sh[32];
+  long long base = (long long)blockIdx.x * kScanTile;
+  int s = 0;
+  for (int r = 0; r < kScanItems; ++r) {
+    long long idx = base + (long long)r * kScanT + threadIdx.x;
+    if (idx < n) s += a[idx];
+  }
+  int total;
+  block_excl_scan(s, sh, total);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+// one block: exclusive scan of nb block sums, chunk after chunk with a carry
+__global__ void k_scan_sums(int *bsum, int nb) {
+  __shared__ int sh[32];
+  int carry = 0;
+  for (int base = 0; base < nb; base += kScanT) {
+    int idx = base + threadIdx.x;
+    int v = (idx < nb) ? bsum[idx] : 0;
+    int total;
+    int ex = block_excl_scan(v, sh, total);
+    if (idx < nb) bsum[idx] = carry + ex;
+    carry += total;
+    __syncthreads();
+  }
+}
+
+__global__ void k_scan_apply(int *a, long long n, const int *bsum) {
+  __shared__ int sh[32];
+  long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int s = 0;
+  for (int r = 0; r < kScanItems; ++r) {
+    long long idx = base + r;
+    v[r] = (idx < n) ? a[idx] : 0;
+    s += v[r];
+  }
+  int total;
+  int ex = block_excl_scan(s, sh, total) + bsum[blockIdx.x];
+  for (int r = 0; r < kScanItems; ++r) {
+    long long idx = base + r;
+    if (idx < n) a[idx] = ex;
+    ex += v[r];
+  }
+}
+
+__global__ void k_fill(const int *key, int npart, int *cursor, int *order) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npart) return;
+  int slot = atomicAdd(&cursor[key[p]], 1);
+  order[slot] = p;
+}
+
+// order every cell's run by particle index: insertion sort for short runs, heap sort
+// for long ones (both in place, deterministic)
+__device__ void sift_down(int *a, int root, int n) {
+  while (true) {
+    int child = 2 * root + 1;
+    if (child >= n) return;
+    if (child + 1 < n && a[child] < a[child + 1]) ++child;
+    if (a[root] >= a[child]) return;
+    int t = a[root]; a[root] = a[child]; a[child] = t;
+    root = child;
+  }
+}
+
+__global__ void k_sort_runs(const int *cstart, long long ncell, int *order) {
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int b = cstart[c], e = cstart[c + 1];
+  int n = e - b;
+  if (n < 2) return;
+  int *a = order + b;
+  if (n <= 48) {
+    for (int x = 1; x < n; ++x) {
+      int v = a[x];
+      int y = x - 1;
+      while (y >= 0 && a[y] > v) { a[y + 1] = a[y]; --y; }
+      a[y + 1] = v;
+    }
+    return;
+  }
+  for (int r = n / 2 - 1; r >= 0; --r) sift_down(a, r, n);
+  for (int x = n - 1; x > 0; --x) {
+    int t = a[0]; a[0] = a[x]; a[x] = t;
+    sift_down(a, 0, x);
+  }
+}
+
+// every row of particle order[k] into slot k of the spare arrays
+__global__ void k_move(const double *pr, const int *pi, long long stride, int npart,
+                       const int *order, double *npr, int *npi) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npart) return;
+  int p = order[k];
+  for (int r = 0; r < DUSTB_NREAL; ++r) npr[(long long)r * stride + k] = pr[(long long)r * stride + p];
+  for (int r = 0; r < DUSTB_NINT; ++r) npi[(long long)r * stride + k] = pi[(long long)r * stride + p];
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+namespace dustb {
+
+long long csr_scratch_bytes(long long ncell, long long n) {
+  long long nb = (ncell + 1 + kScanTile - 1) / kScanTile;
+  return (long long)(align256(sizeof(int) * (size_t)(n > 0 ? n : 1)) +
+                     align256(sizeof(int) * (size_t)(ncell + 1)) +
+                     align256(sizeof(int) * (size_t)(nb + 1)));
+}
+
+int exclusive_scan(int *a, long long n, int *bsum, cudaStream_t st) {
+  long long nb = (n + kScanTile - 1) / kScanTile;
+  k_scan_reduce<<<(unsigned)nb, kScanT, 0, st>>>(a, n, bsum);
+  k_scan_sums<<<1, kScanT, 0, st>>>(bsum, (int)nb);
+  k_scan_apply<<<(unsigned)nb, kScanT, 0, st>>>(a, n, bsum);
+  return dustb_host::launch_status("exclusive_scan");
+}
+
+// CSR from precomputed keys: key[n] in [0, ncell); cstart must hold ncell + 1 ints and be
+// zero on entry except when counted = true (then cstart[0..ncell) holds the counts).
+int csr_from_keys(const int *key, int n, long long ncell, int *cstart, int *order, void *scratch,
+                  long long bytes, cudaStream_t st) {
+  if (bytes < csr_scratch_bytes(ncell, n)) return DUSTB_ESCRATCH;
+  char *p = (char *)scratch;
+  p += align256(sizeof(int) * (size_t)(n > 0 ? n : 1));   // key slot (unused here)
+  int *cursor = (int *)p; p += align256(sizeof(int) * (size_t)(ncell + 1));
+  int *bsum = (int *)p;
+  int rc = exclusive_scan(cstart, ncell + 1, bsum, st);
+  if (rc) return rc;
+  cudaMemcpyAsync(cursor, cstart, sizeof(int) * (size_t)(ncell + 1), cudaMemcpyDeviceToDevice, st);
+  if (n > 0) k_fill<<<nblk(n), kT, 0, st>>>(key, n, cursor, order);
+  k_sort_runs<<<nblk(ncell), kT, 0, st>>>(cstart, ncell, order);
+  return dustb_host::launch_status("csr_from_keys");
+}
+
+}  // namespace dustb
+
+extern "C" {
+
+long long dustb_sort_scratch_bytes(const dustb_mesh *mesh, int npart) {
+  if (!mesh) return -1;
+  long long ncell = (long long)mesh->nmb * mesh->nx1 * (mesh->multi_d ? mesh->nx2 : 1) *
+                    (mesh->three_d ? mesh->nx3 : 1);
+  // keys + CSR scratch, then order + cstart of dustb_sort_by_cell
+  return csr_scratch_bytes(ncell, npart) +
+         (long long)(align256(sizeof(int) * (size_t)(npart > 0 ? npart : 1)) +
+                     align256(sizeof(int) * (size_t)(ncell + 1)));
+}
+
+int dustb_cell_index(const dustb_ctx *c, int *order, int *cstart, void *scratch,
+                     long long scratch_bytes, void *stream) {
+  if (!c || !order || !cstart || !scratch) return DUSTB_EINVAL;
+  const dustb_mesh &ms = c->mesh;
+  const int nx2 = ms.multi_d ? ms.nx2 : 1, nx3 = ms.three_d ? ms.nx3 : 1;
+  const long long ncell = (long long)ms.nmb * ms.nx1 * nx2 * nx3;
+  if (ncell >= (1LL << 31)) return DUSTB_EUNSUP;
+  const int n = c->part.npart;
+  if (scratch_bytes < csr_scratch_bytes(ncell, n)) return DUSTB_ESCRATCH;
+  cudaStream_t st = (cudaStream_t)stream;
+  int *key = (int *)scratch;
+  cudaMemsetAsync(cstart, 0, sizeof(int) * (size_t)(ncell + 1), st);
+  if (n > 0)
+    k_keys<<<nblk(n), kT, 0, st>>>(c->part.pr, c->part.pi, c->part.stride, n, ms.mb_size, ms.gids,
+                                   ms.nmb, ms.nx1, nx2, nx3, ms.three_d, key, cstart);
+  return csr_from_keys(key, n, ncell, cstart, order, scratch, scratch_bytes, st);
+}
+
+int dustb_sort_by_cell(const dustb_ctx *c, double *spare_pr, int *spare_pi, void *scratch,
+                       long long scratch_bytes, void *stream) {
+  if (!c || !spare_pr || !spare_pi || !scratch) return DUSTB_EINVAL;
+  const dustb_mesh &ms = c->mesh;
+  const int n = c->part.npart;
+  if (scratch_bytes < dustb_sort_scratch_bytes(&ms, n)) return DUSTB_ESCRATCH;
+  const long long ncell = (long long)ms.nmb * ms.nx1 * (ms.multi_d ? ms.nx2 : 1) *
+                          (ms.three_d ? ms.nx3 : 1);
+  const long long base = csr_scratch_bytes(ncell, n);
+  int *order = (int *)((char *)scratch + base);
+  int *cstart = (int *)((char *)scratch + base + align256(sizeof(int) * (size_t)(n > 0 ? n : 1)));
+  int rc = dustb_cell_index(c, order, cstart, scratch, base, stream);
+  if (rc) return rc;
+  if (n > 0)
+    k_move<<<nblk(n), kT, 0, (cudaStream_t)stream>>>(c->part.pr, c->part.pi, c->part.stride, n,
+                                                       order, spare_pr, spare_pi);
+  return dustb_host::launch_status("sort_by_cell");
+}
+
+}  // extern "C"

@@ -1,0 +1,207 @@
+"""Host front end of the drag step: device arrays in the reference layout plus the task
+calls of DustGasDrag, each forwarding to one C-ABI entry point (include/dustb.h).
+
+torch is used only to own device memory and streams; every computation is a kernel of
+libdustb.so.  The task names follow the reference's DustGasDrag members
+(src/dust/dust_pm.cpp, dust_push.cpp, dust_solver.cpp, dust_newdt.cpp).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import capi
+from .inputs import DustState
+
+GAMMA_DEFAULT = 1.707106781186547   # 1 + 1/sqrt(2), src/driver/driver.cpp:201
+
+
+def _stream_ptr(stream) -> int:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream
+
+
+class DeviceDust:
+    """One MeshBlockPack's dust state on the GPU, in the reference layout."""
+
+    def __init__(self, st: DustState, phys: dict, device="cuda", stride=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("the dust drag step runs on a CUDA device only")
+        self.lib = capi.load()
+        self.mesh = st.mesh
+        self.device = torch.device(device)
+        self.npart = st.npart
+        self.nspecies = st.nspecies
+        ms = st.mesh
+        f64 = dict(dtype=torch.float64, device=self.device)
+        self.stride = int(stride or st.stride)
+        pr = torch.zeros((17, self.stride), **f64)
+        pi = torch.zeros((5, self.stride), dtype=torch.int32, device=self.device)
+        pr[:, :st.stride].copy_(torch.from_numpy(st.pr[:, :min(st.stride, self.stride)]))
+        pi[:, :st.stride].copy_(torch.from_numpy(st.pi[:, :min(st.stride, self.stride)]))
+        self.t = {
+            "pr": pr, "pi": pi,
+            "u0": torch.from_numpy(st.u0).to(self.device),
+            "u1": torch.zeros(ms.field_shape(4), **f64),
+            "qdep": torch.zeros(ms.field_shape(5), **f64),
+            "ustar": torch.zeros(ms.field_shape(3), **f64),
+            "dmom": torch.zeros(ms.field_shape(3), **f64),
+            "resid": torch.zeros(ms.field_shape(4), **f64),
+            "work": torch.zeros(ms.field_shape(3), **f64),
+            "mb_size": torch.from_numpy(np.ascontiguousarray(ms.mb_size)).to(self.device),
+            "nghbr": torch.from_numpy(np.ascontiguousarray(ms.nghbr)).to(self.device),
+            "err": torch.zeros(1, dtype=torch.int32, device=self.device),
+            "x3_removed": torch.zeros(2, **f64),
+            "scalar": torch.zeros(2, **f64),
+        }
+        self.phys = dict(phys)
+        self._rebuild_ctx()
+
+    def _rebuild_ctx(self):
+        self.ctx = capi.make_ctx(self.mesh, self.t, self.npart, self.stride, self.phys)
+        self.pctx = C.byref(self.ctx)
+
+    def __getattr__(self, name):
+        t = self.__dict__.get("t")
+        if t is not None and name in t:
+            return t[name]
+        raise AttributeError(name)
+
+    def _call(self, name, *args, stream=None):
+        rc = getattr(self.lib, "dustb_" + name)(self.pctx, *args, _stream_ptr(stream))
+        capi.check(rc, name)
+
+    # ---- tasks (one C-ABI call each) ----
+    def register_copy(self, stream=None):
+        self._call("register_copy", stream=stream)
+
+    def gas_rk_noflux(self, g0, g1, stream=None):
+        self._call("gas_rk_noflux", g0, g1, stream=stream)
+
+    def history_gas(self, atw_dt, stream=None):
+        self._call("history_gas", atw_dt, stream=stream)
+
+    def push_imex(self, gam0, gam1, beta_dt, atw_dt, stream=None):
+        self._call("push_imex", gam0, gam1, beta_dt, atw_dt, stream=stream)
+
+    def route(self, stream=None):
+        self._call("route", self.t["x3_removed"].data_ptr(), stream=stream)
+
+    def deposit_qp(self, a_dt, sh=0.0, stream=None):
+        self._call("deposit_qp", a_dt, sh, stream=stream)
+
+    def ghost_add(self, name, nvar, stream=None):
+        self._call("ghost_add", self.t[name].data_ptr(), nvar, stream=stream)
+
+    def ghost_copy(self, name, nvar, x3_bcs=1, stream=None):
+        self._call("ghost_copy", self.t[name].data_ptr(), nvar, x3_bcs, stream=stream)
+
+    def solve_ustar(self, stream=None):
+        self._call("solve_ustar", stream=stream)
+
+    def dc1_sweep(self, a_dt, sh=0.0, stream=None):
+        self._call("dc1_sweep", a_dt, sh, stream=stream)
+
+    def gather_kick_pmbr(self, a_dt, sh=0.0, stream=None):
+        self._call("gather_kick_pmbr", a_dt, sh, stream=stream)
+
+    def apply_pmbr(self, a_dt, stream=None):
+        self._call("apply_pmbr", a_dt, stream=stream)
+
+    def newdt(self, dt_cfl=1.0, stream=None):
+        out = self.t["scalar"]
+        self._call("newdt", dt_cfl, out.data_ptr(), stream=stream)
+        return out[0]
+
+    def tstop_extrema(self, stream=None):
+        out = self.t["scalar"]
+        self._call("tstop_extrema", out.data_ptr(), stream=stream)
+        return out
+
+    def pc2_predictor(self, dt, rate_dep=1, stream=None):
+        self._call("pc2_predictor", dt, rate_dep, stream=stream)
+
+    def pc2_apply_predictor(self, dt, stream=None):
+        out = self.t["scalar"]
+        self._call("pc2_apply_predictor", dt, out.data_ptr(), stream=stream)
+        return out[0]
+
+    def pc2_midpoint(self, stream=None):
+        self._call("pc2_midpoint", stream=stream)
+
+    def pc2_advance(self, dt, stream=None):
+        self._call("pc2_advance", dt, stream=stream)
+
+    def pc2_commit(self, wpred, stream=None):
+        self._call("pc2_commit", wpred, stream=stream)
+
+    # ---- cycles ----
+    def imex_cycle(self, dt, gamma=GAMMA_DEFAULT, sh=(0.0, 0.0), stream=None):
+        co = capi.DustbImexCoeffs()
+        co.gamma, co.dt = gamma, dt
+        co.sh[0], co.sh[1] = sh
+        rc = self.lib.dustb_imex_cycle(self.pctx, C.byref(co), self.t["x3_removed"].data_ptr(),
+                                       _stream_ptr(stream))
+        capi.check(rc, "imex_cycle")
+
+    def pc2_cycle(self, dt, stream=None):
+        out = self.t["scalar"]
+        rc = self.lib.dustb_pc2_cycle(self.pctx, dt, out.data_ptr(),
+                                      self.t["x3_removed"].data_ptr(), _stream_ptr(stream))
+        capi.check(rc, "pc2_cycle")
+        return out[0]
+
+    # ---- sort ----
+    def _scratch(self):
+        n = int(self.lib.dustb_sort_scratch_bytes(C.byref(self.ctx.mesh), self.npart))
+        s = self.t.get("sort_scratch")
+        if s is None or s.numel() < n:
+            s = torch.empty(n, dtype=torch.uint8, device=self.device)
+            self.t["sort_scratch"] = s
+        return s
+
+    def cell_index(self, stream=None):
+        ms = self.mesh
+        ncell = ms.ncell_active
+        order = torch.empty(max(self.npart, 1), dtype=torch.int32, device=self.device)
+        cstart = torch.empty(ncell + 1, dtype=torch.int32, device=self.device)
+        s = self._scratch()
+        rc = self.lib.dustb_cell_index(self.pctx, order.data_ptr(), cstart.data_ptr(),
+                                       s.data_ptr(), s.numel(), _stream_ptr(stream))
+        capi.check(rc, "cell_index")
+        return order[:self.npart], cstart
+
+    def sort_by_cell(self, stream=None):
+        """SortParticles: sort into spare arrays, then swap them in (as the reference)."""
+        s = self._scratch()
+        spr = torch.empty_like(self.t["pr"])
+        spi = torch.empty_like(self.t["pi"])
+        rc = self.lib.dustb_sort_by_cell(self.pctx, spr.data_ptr(), spi.data_ptr(), s.data_ptr(),
+                                         s.numel(), _stream_ptr(stream))
+        capi.check(rc, "sort_by_cell")
+        self.t["pr"], self.t["pi"] = spr, spi
+        self._rebuild_ctx()
+
+    # ---- host views ----
+    def error_word(self) -> int:
+        return int(self.t["err"].item())
+
+    def host(self, name):
+        a = self.t[name]
+        if name in ("pr", "pi"):
+            a = a[:, :self.npart]
+        return a.detach().cpu().numpy()
+
+    def momentum(self):
+        ms = self.mesh
+        u0 = self.t["u0"]
+        is_, js, ks = ms.starts
+        act = u0[:, 1:4, ks:ks + ms.nx[2], js:js + ms.nx[1], is_:is_ + ms.nx[0]]
+        g = act.sum(dim=(0, 2, 3, 4)) * ms.cell_volume()
+        pr = self.t["pr"][:, :self.npart]
+        m = pr[16]
+        d = torch.stack([(m * pr[1]).sum(), (m * pr[3]).sum(), (m * pr[5]).sum()])
+        return g.cpu().numpy(), d.cpu().numpy()

@@ -1,0 +1,235 @@
+/*
+ * dustb.h -- C ABI of the B200 dust particle-drag step.
+ *
+ * The entry points replace the dust task functions of AthenaK's DustGasDrag one for one
+ * (reference: src/dust/dust_pm.cpp, dust_push.cpp, dust_solver.cpp, dust_newdt.cpp,
+ * src/bvals/bvals_part.cpp, bvals_dep.cpp, dust_cloud_device.cpp).  Every pointer inside
+ * dustb_ctx is a DEVICE pointer to an array the host code already owns, in the host code's
+ * own layout:
+ *
+ *   particles  pr  = prtcl_rdata (17 x stride doubles, row r at pr + r*stride)
+ *              pi  = prtcl_idata ( 5 x stride int32)     (src/particles/particles.cpp:96-113)
+ *   mesh       u0, u1, qdep, ustar, dmom, resid, work:
+ *              (nmb, nvar, n3, n2, n1) row-major doubles, n = nx + 2 ng per active direction
+ *              (src/hydro/hydro.cpp:125, src/dust/dust.cpp:1160-1169)
+ *   mb_size    nmb x 9 doubles {x1min,x2min,x3min,x1max,x2max,x3max,dx1,dx2,dx3}
+ *              (RegionSize, src/mesh/mesh.hpp:25-29)
+ *   nghbr      nmb x 27 int: gid of the same-level neighbour in direction (ox1,ox2,ox3),
+ *              index (ox3+1)*9 + (ox2+1)*3 + (ox1+1), -1 where there is none
+ *              (the first sub-slot NeighborIndex(ox1,ox2,ox3,0,0) of pmb->nghbr,
+ *              src/mesh/nghbr_index.hpp:29)
+ *
+ * Every call takes the CUDA stream the host code runs on (Kokkos' default execution space
+ * stream) as an opaque pointer, queues its kernels there and returns without waiting.
+ * Return value: 0 on success, < 0 for an argument or launch error (DUSTB_E*).  Kernels
+ * never trap: a violated invariant ORs a DUSTB_ERR_* bit into *ctx->err (device uint32) and
+ * the offending particle is skipped, where the reference calls Kokkos::abort.
+ *
+ * No entry point allocates memory: scratch is passed by the caller (dustb_*_bytes).
+ */
+#ifndef DUSTB_H_
+#define DUSTB_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* particle rows (src/athena.hpp:77-80) */
+enum {
+  DUSTB_IPX = 0, DUSTB_IPVX = 1, DUSTB_IPY = 2, DUSTB_IPVY = 3, DUSTB_IPZ = 4, DUSTB_IPVZ = 5,
+  DUSTB_IPX1 = 6, DUSTB_IPVX1 = 7, DUSTB_IPY1 = 8, DUSTB_IPVY1 = 9, DUSTB_IPZ1 = 10,
+  DUSTB_IPVZ1 = 11, DUSTB_IPRX = 12, DUSTB_IPRY = 13, DUSTB_IPRZ = 14, DUSTB_IPTS = 15,
+  DUSTB_IPM = 16, DUSTB_NREAL = 17
+};
+enum { DUSTB_PGID = 0, DUSTB_PTAG = 1, DUSTB_PSP = 2, DUSTB_PLEV = 3, DUSTB_PTAGH = 4,
+       DUSTB_NINT = 5 };
+/* gas conserved variables (src/athena.hpp:52) */
+enum { DUSTB_IDN = 0, DUSTB_IM1 = 1, DUSTB_IM2 = 2, DUSTB_IM3 = 3 };
+/* <dust>/deposit */
+enum { DUSTB_NGP = 0, DUSTB_CIC = 1, DUSTB_TSC = 2 };
+/* <dust>/drag_solver (the point-particle solvers of SolveCoupledStage) */
+enum { DUSTB_SOLVER_LOCAL = 0, DUSTB_SOLVER_APPLYA = 1, DUSTB_SOLVER_DC1 = 2,
+       DUSTB_SOLVER_DC2 = 3 };
+/* x3 physical boundary of the dust (x3bc_dust, src/bvals/bvals.hpp) */
+enum { DUSTB_X3_PERIODIC = 0, DUSTB_X3_REFLECT = 1, DUSTB_X3_OUTFLOW = 2 };
+
+/* device error word bits */
+#define DUSTB_ERR_HALO      0x1u  /* particle outside its block's deposit halo (dust_pm.cpp:241) */
+#define DUSTB_ERR_ROUTE     0x2u  /* particle more than one block away (bvals_part.cpp:245) */
+#define DUSTB_ERR_NGHBR     0x4u  /* no neighbour block covers a crossing (bvals_part.cpp:394) */
+#define DUSTB_ERR_PGID      0x8u  /* PGID outside the pack */
+#define DUSTB_ERR_TSTOP     0x10u /* stopping time not finite and positive (dust_newdt.cpp:53) */
+#define DUSTB_ERR_WINDOW    0x20u /* fused kernels: a particle outside its tile window */
+
+/* host return codes */
+#define DUSTB_OK          0
+#define DUSTB_EINVAL     (-1)
+#define DUSTB_ELAUNCH    (-2)
+#define DUSTB_ESCRATCH   (-3)
+#define DUSTB_EUNSUP     (-4)
+
+typedef struct dustb_mesh {
+  int nmb;                 /* MeshBlocks in the pack (nmb_thispack) */
+  int gids;                /* gid of the pack's first MeshBlock */
+  int nx1, nx2, nx3;       /* active cells per MeshBlock */
+  int ng;                  /* ghost cells (>= 2, src/dust/dust.cpp:325-330) */
+  int multi_d, three_d;
+  int x3bc;                /* DUSTB_X3_* */
+  double x1min, x1max, x2min, x2max, x3min, x3max;   /* mesh_size */
+  const double *mb_size;   /* nmb x 9 */
+  const int *nghbr;        /* nmb x 27 */
+} dustb_mesh;
+
+typedef struct dustb_particles {
+  double *pr;              /* 17 x stride */
+  int *pi;                 /* 5 x stride */
+  long long stride;        /* allocated capacity (row stride) */
+  int npart;               /* live particles (nprtcl_thispack) */
+} dustb_particles;
+
+typedef struct dustb_fields {
+  double *u0, *u1;         /* gas conserved state and its stage register */
+  int nvar_gas;            /* 4 (isothermal) or 5 */
+  double *qdep;            /* 5 vars: Q, P1..P3, pc2 rate */
+  double *ustar;           /* 3 vars */
+  double *dmom;            /* 3 vars */
+  double *resid;           /* 4 vars (imex_resid) */
+  double *work;            /* 3 vars (solver_ap) */
+} dustb_fields;
+
+typedef struct dustb_physics {
+  int scheme;              /* DUSTB_NGP / CIC / TSC */
+  int back_reaction;
+  int consistent_gas;      /* <dust>/imex_consistent_gas (default on) */
+  int drag_solver;         /* DUSTB_SOLVER_* */
+  int shearing_box;        /* rotation and shear terms in the push */
+  int stratified;          /* vertical gravity -Omega^2 z */
+  int pc2_feedback_damping;
+  double qshear, omega0, const_accel_phi;
+} dustb_physics;
+
+typedef struct dustb_ctx {
+  dustb_mesh mesh;
+  dustb_particles part;
+  dustb_fields f;
+  dustb_physics phys;
+  unsigned int *err;       /* device error word */
+} dustb_ctx;
+
+/* ---- library ------------------------------------------------------------------------ */
+int dustb_version(void);
+/* Last CUDA error string of this library's host code (not thread safe). */
+const char *dustb_last_error(void);
+
+/* ---- FP64 per-task entry points (reference layout, straightforward kernels) ---------- */
+
+/* DustGasDrag::FirstTwoImpRK stage 1 (src/dust/dust_push.cpp:63-79): u1 <- u0 (ghosts
+ * included), particle registers (X1,V1) <- (X,V). */
+int dustb_register_copy(const dustb_ctx *ctx, void *stream);
+
+/* Harness stand-in for Hydro::RKUpdate with a zero flux divergence (the gas update is not
+ * part of the drag step): u0 <- gam0 u0 + gam1 u1 over active cells, all gas variables. */
+int dustb_gas_rk_noflux(const dustb_ctx *ctx, double gam0, double gam1, void *stream);
+
+/* DustGasDrag::AddDragHistoryGas (src/dust/dust_pm.cpp:721-742): u0.m += atw_dt dmom. */
+int dustb_history_gas(const dustb_ctx *ctx, double atw_dt, void *stream);
+
+/* DustGasDrag::ExplicitPush, imex branch (src/dust/dust_push.cpp:249-297). */
+int dustb_push_imex(const dustb_ctx *ctx, double gam0, double gam1, double beta_dt,
+                    double atw_dt, void *stream);
+
+/* ParticlesBoundaryValues::SetNewPrtclGID on a single-level mesh (src/bvals/bvals_part.cpp:
+ * 115-429): x3 reflect/outflow, snap into [xmin, xmax), new PGID from the neighbour table,
+ * periodic wrap of X and the RK registers.  x3_removed (2 doubles: mass, count) may be NULL
+ * unless mesh.x3bc == DUSTB_X3_OUTFLOW. */
+int dustb_route(const dustb_ctx *ctx, double *x3_removed, void *stream);
+
+/* DustGasDrag::DepositDrag, imex scatter (src/dust/dust_pm.cpp:197-277): zero qdep, then
+ * Q += m c W/V, P += m c W v/V with c = a_dt/(t_s + a_dt), y weights at y + sh x. */
+int dustb_deposit_qp(const dustb_ctx *ctx, double a_dt, double sh, void *stream);
+
+/* MeshBoundaryValuesDep::PackAndSendDeposit + RecvAndSumDeposit on one device
+ * (src/bvals/bvals_dep.cpp:320-560): the ghost-cell deposits of every block are added into
+ * the active strips of its neighbours, buffers in NeighborIndex order. */
+int dustb_ghost_add(const dustb_ctx *ctx, double *field, int nvar, void *stream);
+
+/* MeshBoundaryValuesCC::PackAndSendCC + RecvAndUnpackCC on one device (same-level copy
+ * exchange), followed by DustGasDrag::UstarX3BCs at physical x3 faces when x3_bcs != 0
+ * (src/dust/dust_tasks.cpp:445-469). */
+int dustb_ghost_copy(const dustb_ctx *ctx, double *field, int nvar, int x3_bcs, void *stream);
+
+/* GasImplicitSolve's per-cell solve (dust_pm.cpp:426-436 and the dc1 local guess,
+ * dust_solver.cpp:643-649): ustar = (u0.m + P)/(rho + Q) over active cells. */
+int dustb_solve_ustar(const dustb_ctx *ctx, void *stream);
+
+/* One ApplyDefectCorrection sweep on ustar (dust_solver.cpp:226-252): ghost fill of ustar,
+ * operator gather/deposit into work, additive ghost exchange of work, per-cell correction. */
+int dustb_dc1_sweep(const dustb_ctx *ctx, double a_dt, double sh, void *stream);
+
+/* DustGasDrag::GatherKickPMBR (dust_pm.cpp:450-568): zero dmom; gather u*, kick, record
+ * R = dv/a_dt, deposit -m W dv / V into dmom with the same weights. */
+int dustb_gather_kick_pmbr(const dustb_ctx *ctx, double a_dt, double sh, void *stream);
+
+/* DustGasDrag::ApplyPMBR imex (dust_pm.cpp:605-711): the consistent point split when
+ * phys.consistent_gas, else u0.m += dmom and dmom /= a_dt. */
+int dustb_apply_pmbr(const dustb_ctx *ctx, double a_dt, void *stream);
+
+/* DustGasDrag::NewTimeStep (src/dust/dust_newdt.cpp:108-149): *dt_out (device double) =
+ * dt_cfl * min over particles of dx/|v| (the y transport velocity includes -q Omega x in
+ * a 3-D shearing box).  Written on the device; no host wait. */
+int dustb_newdt(const dustb_ctx *ctx, double dt_cfl, double *dt_out, void *stream);
+
+/* Stopping-time validation and extrema of RefreshStoppingTimeMaximum
+ * (dust_newdt.cpp:34-98): out[0] = max t_s (DBL_MAX if any is invalid), out[1] = min t_s. */
+int dustb_tstop_extrema(const dustb_ctx *ctx, double *out, void *stream);
+
+/* ---- cell index and sort (src/dust/dust_cloud_device.cpp:1881-1977) ------------------ */
+
+/* Scratch bytes of dustb_cell_index / dustb_sort_by_cell for npart particles. */
+long long dustb_sort_scratch_bytes(const dustb_mesh *mesh, int npart);
+
+/* The particles' cell keys m*ncell + (k nx2 + j) nx1 + i with the floor() cell formula of
+ * SortParticles, and their order: order[0..npart) lists the particles sorted by
+ * (key, index), cstart[0..nmb*ncell] the first position of every cell (a CSR over cells). */
+int dustb_cell_index(const dustb_ctx *ctx, int *order, int *cstart, void *scratch,
+                     long long scratch_bytes, void *stream);
+
+/* DustGasDrag::SortParticles: every particle row moved into the spare arrays (same
+ * stride) in (block, k, j, i, old index) order.  The caller swaps the arrays, as the
+ * reference does with sort_spare_r/i. */
+int dustb_sort_by_cell(const dustb_ctx *ctx, double *spare_pr, int *spare_pi, void *scratch,
+                       long long scratch_bytes, void *stream);
+
+/* ---- pc2 (src/dust/dust_pm.cpp:109-194, :374-405, :585-602; dust_push.cpp:37-61,
+ * :99-247) ---------------------------------------------------------------------------- */
+int dustb_pc2_predictor(const dustb_ctx *ctx, double dt, int rate_dep, void *stream);
+/* chi_max (device double, may be NULL): max over active cells of dt*qdep4/rho
+ * (UpdateStiffness), computed before the damping. */
+int dustb_pc2_apply_predictor(const dustb_ctx *ctx, double dt, double *chi_max, void *stream);
+int dustb_pc2_midpoint(const dustb_ctx *ctx, void *stream);
+int dustb_pc2_advance(const dustb_ctx *ctx, double dt, void *stream);
+int dustb_pc2_commit(const dustb_ctx *ctx, double wpred, void *stream);
+
+/* ---- fused FP64 cycles: the reference's task order for one cycle ----------------------- */
+
+typedef struct dustb_imex_coeffs {
+  double gamma;            /* imex2+ singly-diagonal coefficient (1+1/sqrt 2 or 1/2) */
+  double dt;               /* cycle time step */
+  double sh[2];            /* ImplicitShearShift of working stages 1, 2 */
+} dustb_imex_coeffs;
+
+/* One imex2+ cycle of the drag step (stages 1 and 2; stage 3 is dormant): register copy,
+ * gas stand-in, push, route, deposit, ghost add, solve (+dc1/dc2), ghost copy, gather-kick,
+ * ghost add, apply, history.  x3_removed as in dustb_route. */
+int dustb_imex_cycle(const dustb_ctx *ctx, const dustb_imex_coeffs *c, double *x3_removed,
+                     void *stream);
+
+/* One pc2 cycle (integrator rk2): predictor, apply, gas tail, midpoint, advance, route,
+ * ghost add, commit.  chi_max as in dustb_pc2_apply_predictor. */
+int dustb_pc2_cycle(const dustb_ctx *ctx, double dt, double *chi_max, double *x3_removed,
+                    void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DUSTB_H_ */

@@ -1,0 +1,977 @@
+/*
+ * dust_oracle.c -- CPU oracle of the dust particle-drag step.  TEST INFRASTRUCTURE ONLY:
+ * the tests, the smoke check and the CPU-baseline leg of the benchmark call it as the
+ * checker; the product path (athenak_b200) never links or calls it.
+ *
+ * A plain-C FP64 restatement of the reference kernels, function by function, in the
+ * reference's data layout (dustb.h).  Each function names the file:line it follows.  The
+ * loops run in the reference's iteration order; with one thread the deposits are plain
+ * sums in particle order (Kokkos Serial's DepositAdd, src/dust/dust.hpp:986-998); with
+ * OpenMP threads they are atomic adds (the Kokkos OpenMP backend), which is the form timed
+ * as the CPU baseline.
+ *
+ * Parity pins: the reference ships no golden output files and its Kokkos build cannot be
+ * compiled here (the kokkos submodule is empty), so the oracle is pinned to the
+ * reference's own known-answer tests instead: the dust_damping ODE
+ * (src/pgen/tests/dust_damping.cpp:9-16), exact total-momentum conservation
+ * (tst/test_suite/dust/check_cloud_imex3d.py:66-74) and the NSH drift
+ * (src/pgen/dust_amr/dust_setup.hpp:58-65); see tests/test_oracle_kat.py.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/dustb.h"
+
+#define SQR(x) ((x)*(x))
+
+static int g_threads = 1;
+void oracle_set_threads(int n) { g_threads = (n < 1) ? 1 : n; }
+int oracle_get_threads(void) { return g_threads; }
+
+/* ---- layout helpers ------------------------------------------------------------------ */
+typedef struct {
+  int n1, n2, n3, is, ie, js, je, ks, ke;
+} Ind;
+
+static Ind indices(const dustb_mesh *ms) {
+  Ind d;
+  d.n1 = ms->nx1 + 2*ms->ng;
+  d.n2 = ms->multi_d ? ms->nx2 + 2*ms->ng : 1;
+  d.n3 = ms->three_d ? ms->nx3 + 2*ms->ng : 1;
+  d.is = ms->ng; d.ie = d.is + ms->nx1 - 1;
+  d.js = ms->multi_d ? ms->ng : 0; d.je = d.js + (ms->multi_d ? ms->nx2 : 1) - 1;
+  d.ks = ms->three_d ? ms->ng : 0; d.ke = d.ks + (ms->three_d ? ms->nx3 : 1) - 1;
+  return d;
+}
+
+#define A5(arr, nv, d, m, v, k, j, i) \
+  (arr)[((((size_t)(m)*(nv) + (v))*(d).n3 + (k))*(d).n2 + (j))*(d).n1 + (i)]
+#define PR(c, p) pr[(size_t)(c)*stride + (p)]
+#define PI(c, p) pi[(size_t)(c)*stride + (p)]
+#define MB(m, f) ms->mb_size[(size_t)(m)*9 + (f)]
+enum { X1MIN = 0, X2MIN = 1, X3MIN = 2, X1MAX = 3, X2MAX = 4, X3MAX = 5, DX1 = 6, DX2 = 7,
+       DX3 = 8 };
+
+static inline void deposit_add(double *dst, double v) {
+#pragma omp atomic
+  *dst += v;
+}
+
+/* PMWeights, src/dust/dust.hpp:1088-1111 */
+static inline void pm_weights(double x, double xmin, double xmax, int nx, int is, int scheme,
+                              int *ip, double w[3]) {
+  double cell = (x - xmin)*((double)nx/(xmax - xmin));
+  int ig = (int)(cell + 1.0) - 1;
+  double del = cell - ((double)ig + 0.5);
+  *ip = ig + is;
+  if (scheme == 0) {
+    w[0] = 0.0; w[1] = 1.0; w[2] = 0.0;
+  } else if (scheme == 1) {
+    w[0] = fmax(0.0, -del); w[1] = 1.0 - fabs(del); w[2] = fmax(0.0, del);
+  } else {
+    w[0] = 0.5*SQR(0.5 - del); w[1] = 0.75 - SQR(del); w[2] = 0.5*SQR(0.5 + del);
+  }
+}
+
+/* the three weight sets of particle p at (x, y + sh x, z) */
+static inline void particle_weights(const dustb_ctx *c, const Ind *d, int m, double x,
+                                    double y, double z, int *ip, int *jp, int *kp,
+                                    double wx[3], double wy[3], double wz[3]) {
+  const dustb_mesh *ms = &c->mesh;
+  int sch = c->phys.scheme;
+  pm_weights(x, MB(m, X1MIN), MB(m, X1MAX), ms->nx1, d->is, sch, ip, wx);
+  pm_weights(y, MB(m, X2MIN), MB(m, X2MAX), ms->nx2, d->js, sch, jp, wy);
+  if (ms->three_d) {
+    pm_weights(z, MB(m, X3MIN), MB(m, X3MAX), ms->nx3, d->ks, sch, kp, wz);
+  } else {
+    *kp = d->ks; wz[0] = 0.0; wz[1] = 1.0; wz[2] = 0.0;
+  }
+}
+
+static inline double cell_volume(const dustb_mesh *ms, int m) {
+  double vol = MB(m, DX1)*MB(m, DX2);
+  if (ms->three_d) vol *= MB(m, DX3);
+  return vol;
+}
+
+static int halo_ok(const dustb_mesh *ms, const Ind *d, int ip, int jp, int kp) {
+  if (ip < d->is - 1 || ip > d->is + ms->nx1) return 0;
+  if (jp < d->js - 1 || jp > d->js + ms->nx2) return 0;
+  if (ms->three_d && (kp < d->ks - 1 || kp > d->ks + ms->nx3)) return 0;
+  return 1;
+}
+
+static size_t field_size(const dustb_mesh *ms, int nvar) {
+  Ind d = indices(ms);
+  return (size_t)ms->nmb*nvar*d.n3*d.n2*d.n1;
+}
+
+/* ---- FirstTwoImpRK stage 1, src/dust/dust_push.cpp:63-79 ------------------------------ */
+void oracle_register_copy(const dustb_ctx *c) {
+  const dustb_mesh *ms = &c->mesh;
+  memcpy(c->f.u1, c->f.u0, field_size(ms, c->f.nvar_gas)*sizeof(double));
+  double *pr = c->part.pr; long long stride = c->part.stride;
+  for (int p = 0; p < c->part.npart; ++p) {
+    PR(DUSTB_IPX1, p) = PR(DUSTB_IPX, p);
+    PR(DUSTB_IPVX1, p) = PR(DUSTB_IPVX, p);
+    PR(DUSTB_IPY1, p) = PR(DUSTB_IPY, p);
+    PR(DUSTB_IPVY1, p) = PR(DUSTB_IPVY, p);
+    PR(DUSTB_IPZ1, p) = PR(DUSTB_IPZ, p);
+    PR(DUSTB_IPVZ1, p) = PR(DUSTB_IPVZ, p);
+  }
+}
+
+/* stand-in for Hydro::RKUpdate with a zero flux divergence (active cells) */
+void oracle_gas_rk_noflux(const dustb_ctx *c, double gam0, double gam1) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int v = 0; v < nv; ++v)
+      for (int k = d.ks; k <= d.ke; ++k)
+        for (int j = d.js; j <= d.je; ++j)
+          for (int i = d.is; i <= d.ie; ++i)
+            A5(c->f.u0, nv, d, m, v, k, j, i) = gam0*A5(c->f.u0, nv, d, m, v, k, j, i) +
+                                                gam1*A5(c->f.u1, nv, d, m, v, k, j, i);
+}
+
+/* AddDragHistoryGas, src/dust/dust_pm.cpp:721-742 */
+void oracle_history_gas(const dustb_ctx *c, double atw_dt) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = d.ks; k <= d.ke; ++k)
+      for (int j = d.js; j <= d.je; ++j)
+        for (int i = d.is; i <= d.ie; ++i)
+          for (int v = 0; v < 3; ++v)
+            A5(c->f.u0, nv, d, m, 1 + v, k, j, i) += atw_dt*A5(c->f.dmom, 3, d, m, v, k, j, i);
+}
+
+/* ExplicitPush imex branch, src/dust/dust_push.cpp:249-297 */
+void oracle_push_imex(const dustb_ctx *c, double gam0, double gam1, double beta_dt,
+                      double atw_dt) {
+  double *pr = c->part.pr; long long stride = c->part.stride;
+  const int three_d = c->mesh.three_d, sbox = c->phys.shearing_box, strat = c->phys.stratified;
+  const double q = c->phys.qshear, om = c->phys.omega0;
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int p = 0; p < c->part.npart; ++p) {
+    double x_old = PR(DUSTB_IPX, p), y_old = PR(DUSTB_IPY, p), z_old = PR(DUSTB_IPZ, p);
+    double vx_old = PR(DUSTB_IPVX, p), vy_old = PR(DUSTB_IPVY, p), vz_old = PR(DUSTB_IPVZ, p);
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    if (sbox) {
+      if (three_d) {
+        fx = 2.0*om*vy_old;
+        fy = -(2.0 - q)*om*vx_old;
+        if (strat) fz = -SQR(om)*z_old;
+      } else {
+        fx = 2.0*om*vz_old;
+        fz = -(2.0 - q)*om*vx_old;
+      }
+    }
+    PR(DUSTB_IPVX, p) = gam0*vx_old + gam1*PR(DUSTB_IPVX1, p) + beta_dt*fx + atw_dt*PR(DUSTB_IPRX, p);
+    PR(DUSTB_IPVY, p) = gam0*vy_old + gam1*PR(DUSTB_IPVY1, p) + beta_dt*fy + atw_dt*PR(DUSTB_IPRY, p);
+    PR(DUSTB_IPVZ, p) = gam0*vz_old + gam1*PR(DUSTB_IPVZ1, p) + beta_dt*fz + atw_dt*PR(DUSTB_IPRZ, p);
+    double ydot = vy_old;
+    if (sbox && three_d) ydot -= q*om*x_old;
+    PR(DUSTB_IPX, p) = gam0*x_old + gam1*PR(DUSTB_IPX1, p) + beta_dt*vx_old;
+    PR(DUSTB_IPY, p) = gam0*y_old + gam1*PR(DUSTB_IPY1, p) + beta_dt*ydot;
+    if (three_d) PR(DUSTB_IPZ, p) = gam0*z_old + gam1*PR(DUSTB_IPZ1, p) + beta_dt*vz_old;
+  }
+}
+
+/* SetNewPrtclGID, src/bvals/bvals_part.cpp:115-429, single-level mesh without shear-periodic
+ * x1 faces.  Returns the OR of the error bits of the particles it could not route. */
+unsigned oracle_route(const dustb_ctx *c, double *x3_removed) {
+  const dustb_mesh *ms = &c->mesh;
+  double *pr = c->part.pr; int *pi = c->part.pi; long long stride = c->part.stride;
+  unsigned err = 0;
+  const double z3a = ms->x3min, z3b = ms->x3max;
+  for (int p = 0; p < c->part.npart; ++p) {
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    if (m < 0 || m >= ms->nmb) { err |= DUSTB_ERR_PGID; continue; }
+    if (ms->x3bc != 0 && (PR(DUSTB_IPZ, p) < z3a || PR(DUSTB_IPZ, p) >= z3b)) {
+      const int lo = (PR(DUSTB_IPZ, p) < z3a);
+      if (ms->x3bc == 1) {
+        const double zf = lo ? z3a : z3b;
+        double z = 2.0*zf - PR(DUSTB_IPZ, p);
+        if (z >= z3b) z = z3b - 1.0e-12*(z3b - z3a);
+        if (z < z3a) z = z3a;
+        PR(DUSTB_IPZ, p) = z;
+        PR(DUSTB_IPVZ, p) = -PR(DUSTB_IPVZ, p);
+        PR(DUSTB_IPZ1, p) = 2.0*zf - PR(DUSTB_IPZ1, p);
+        PR(DUSTB_IPVZ1, p) = -PR(DUSTB_IPVZ1, p);
+      } else {
+        if (x3_removed) { x3_removed[0] += PR(DUSTB_IPM, p); x3_removed[1] += 1.0; }
+        PR(DUSTB_IPM, p) = 0.0;
+        const double dz = MB(m, DX3);
+        const double z = lo ? (MB(m, X3MIN) + 0.5*dz) : (MB(m, X3MAX) - 0.5*dz);
+        PR(DUSTB_IPZ, p) = z;
+        PR(DUSTB_IPVX, p) = 0.0; PR(DUSTB_IPVY, p) = 0.0; PR(DUSTB_IPVZ, p) = 0.0;
+        PR(DUSTB_IPX1, p) = PR(DUSTB_IPX, p); PR(DUSTB_IPY1, p) = PR(DUSTB_IPY, p);
+        PR(DUSTB_IPZ1, p) = z;
+        PR(DUSTB_IPVX1, p) = 0.0; PR(DUSTB_IPVY1, p) = 0.0; PR(DUSTB_IPVZ1, p) = 0.0;
+      }
+    }
+    double x1 = PR(DUSTB_IPX, p), x2 = PR(DUSTB_IPY, p), x3 = PR(DUSTB_IPZ, p);
+    const double lx = MB(m, X1MAX) - MB(m, X1MIN);
+    const double ly = MB(m, X2MAX) - MB(m, X2MIN);
+    const double lz = MB(m, X3MAX) - MB(m, X3MIN);
+    int ix = (int)((x1 - MB(m, X1MIN) + lx)/lx) - 1;
+    int iy = (int)((x2 - MB(m, X2MIN) + ly)/ly) - 1;
+    int iz = (int)((x3 - MB(m, X3MIN) + lz)/lz) - 1;
+    /* snap (bvals_part.cpp:230-247) */
+#define SNAP(off, x, xa, xb, ipx, irx) do { \
+      if ((off) == 0) { double xs = (x); \
+        if ((x) < (xa)) xs = (xa); else if ((x) >= (xb)) xs = nextafter((xb), (xa)); \
+        if (xs != (x)) { PR(irx, p) += xs - (x); PR(ipx, p) = xs; (x) = xs; } } } while (0)
+    SNAP(ix, x1, MB(m, X1MIN), MB(m, X1MAX), DUSTB_IPX, DUSTB_IPX1);
+    if (ms->multi_d) SNAP(iy, x2, MB(m, X2MIN), MB(m, X2MAX), DUSTB_IPY, DUSTB_IPY1);
+    if (ms->three_d) SNAP(iz, x3, MB(m, X3MIN), MB(m, X3MAX), DUSTB_IPZ, DUSTB_IPZ1);
+#undef SNAP
+    if (!ms->multi_d) iy = 0;
+    if (!ms->three_d) iz = 0;
+    if (abs(ix) > 1 || abs(iy) > 1 || abs(iz) > 1) { err |= DUSTB_ERR_ROUTE; continue; }
+    if (ix == 0 && iy == 0 && iz == 0) continue;
+    const int lo1 = (ix < 0) && (MB(m, X1MIN) < ms->x1min + 0.5*lx);
+    const int hi1 = (ix > 0) && (MB(m, X1MAX) > ms->x1max - 0.5*lx);
+    const int lo2 = (iy < 0) && (MB(m, X2MIN) < ms->x2min + 0.5*ly);
+    const int hi2 = (iy > 0) && (MB(m, X2MAX) > ms->x2max - 0.5*ly);
+    const int lo3 = (iz < 0) && (MB(m, X3MIN) < ms->x3min + 0.5*lz);
+    const int hi3 = (iz > 0) && (MB(m, X3MAX) > ms->x3max - 0.5*lz);
+    const int gid = ms->nghbr[(size_t)m*27 + (iz + 1)*9 + (iy + 1)*3 + (ix + 1)];
+    if (gid < 0) { err |= DUSTB_ERR_NGHBR; continue; }
+    PI(DUSTB_PGID, p) = gid;
+    if (lo1) { PR(DUSTB_IPX, p) += ms->x1max - ms->x1min; PR(DUSTB_IPX1, p) += ms->x1max - ms->x1min; }
+    else if (hi1) { PR(DUSTB_IPX, p) -= ms->x1max - ms->x1min; PR(DUSTB_IPX1, p) -= ms->x1max - ms->x1min; }
+    if (lo2) { PR(DUSTB_IPY, p) += ms->x2max - ms->x2min; PR(DUSTB_IPY1, p) += ms->x2max - ms->x2min; }
+    else if (hi2) { PR(DUSTB_IPY, p) -= ms->x2max - ms->x2min; PR(DUSTB_IPY1, p) -= ms->x2max - ms->x2min; }
+    if (lo3) { PR(DUSTB_IPZ, p) += ms->x3max - ms->x3min; PR(DUSTB_IPZ1, p) += ms->x3max - ms->x3min; }
+    else if (hi3) { PR(DUSTB_IPZ, p) -= ms->x3max - ms->x3min; PR(DUSTB_IPZ1, p) -= ms->x3max - ms->x3min; }
+  }
+  return err;
+}
+
+/* DepositDrag imex scatter, src/dust/dust_pm.cpp:197-277 */
+unsigned oracle_deposit_qp(const dustb_ctx *c, double a_dt, double sh) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  memset(c->f.qdep, 0, field_size(ms, 5)*sizeof(double));
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  unsigned err = 0;
+  const int clo = ms->three_d ? 0 : 1, chi = ms->three_d ? 2 : 1;
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads) reduction(| : err)
+  for (int p = 0; p < c->part.npart; ++p) {
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    int ip, jp, kp; double wx[3], wy[3], wz[3];
+    particle_weights(c, &d, m, PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p),
+                     PR(DUSTB_IPZ, p), &ip, &jp, &kp, wx, wy, wz);
+    if (!halo_ok(ms, &d, ip, jp, kp)) { err |= DUSTB_ERR_HALO; continue; }
+    double vol = cell_volume(ms, m);
+    double cj = a_dt/(PR(DUSTB_IPTS, p) + a_dt);
+    double muc = PR(DUSTB_IPM, p)*cj/vol;
+    double vx = PR(DUSTB_IPVX, p), vy = PR(DUSTB_IPVY, p), vz = PR(DUSTB_IPVZ, p);
+    for (int cc = clo; cc <= chi; ++cc)
+      for (int b = 0; b < 3; ++b) {
+        double wcb = wz[cc]*wy[b]*muc;
+        if (wcb == 0.0) continue;
+        for (int a = 0; a < 3; ++a) {
+          double w = wcb*wx[a];
+          int kk = kp + cc - 1, jj = jp + b - 1, ii = ip + a - 1;
+          deposit_add(&A5(c->f.qdep, 5, d, m, 0, kk, jj, ii), w);
+          deposit_add(&A5(c->f.qdep, 5, d, m, 1, kk, jj, ii), w*vx);
+          deposit_add(&A5(c->f.qdep, 5, d, m, 2, kk, jj, ii), w*vy);
+          deposit_add(&A5(c->f.qdep, 5, d, m, 3, kk, jj, ii), w*vz);
+        }
+      }
+  }
+  return err;
+}
+
+/* the 26 same-level directions in NeighborIndex(ox1,ox2,ox3,0,0) order
+ * (src/mesh/nghbr_index.hpp:29-55), the order RecvAndSumDeposit sums the buffers in */
+static const int kDirOrder[26][3] = {
+  {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0},
+  {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 1, 0},
+  {0, 0, -1}, {0, 0, 1},
+  {-1, 0, -1}, {1, 0, -1}, {-1, 0, 1}, {1, 0, 1},
+  {0, -1, -1}, {0, 1, -1}, {0, -1, 1}, {0, 1, 1},
+  {-1, -1, -1}, {1, -1, -1}, {-1, 1, -1}, {1, 1, -1},
+  {-1, -1, 1}, {1, -1, 1}, {-1, 1, 1}, {1, 1, 1}};
+
+/* PackAndSendDeposit + RecvAndSumDeposit, same-level, one rank (src/bvals/bvals_dep.cpp:
+ * 249-309 indices, :320-560 pack and sum): the sender's ghost strip in direction -ox is added
+ * to the receiver's active strip on side ox, buffer by buffer in NeighborIndex order. */
+void oracle_ghost_add(const dustb_ctx *c, double *a, int nvar) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  const int ng1 = ms->ng - 1;
+  const int ndir = ms->three_d ? 26 : (ms->multi_d ? 8 : 2);
+  /* pack every buffer first (the sends complete before any receive sums) */
+  size_t total = 0;
+  int lo[26][3], hi[26][3];
+  for (int n = 0; n < ndir; ++n) {
+    const int *o = kDirOrder[n];
+    int s[3] = {d.is, d.js, d.ks}, e[3] = {d.ie, d.je, d.ke};
+    for (int ax = 0; ax < 3; ++ax) {
+      lo[n][ax] = (o[ax] > 0) ? (e[ax] - ng1) : s[ax];
+      hi[n][ax] = (o[ax] < 0) ? (s[ax] + ng1) : e[ax];
+    }
+    total += (size_t)(hi[n][0] - lo[n][0] + 1)*(hi[n][1] - lo[n][1] + 1)*(hi[n][2] - lo[n][2] + 1);
+  }
+  double *buf = (double *)malloc(total*(size_t)ms->nmb*nvar*sizeof(double));
+  size_t off = 0;
+  size_t boff[26];
+  const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
+  for (int n = 0; n < ndir; ++n) {
+    boff[n] = off;
+    size_t cnt = (size_t)(hi[n][0] - lo[n][0] + 1)*(hi[n][1] - lo[n][1] + 1)*(hi[n][2] - lo[n][2] + 1);
+    off += cnt*(size_t)ms->nmb*nvar;
+  }
+  /* receiver m, buffer n (neighbour in direction o): values of the neighbour's ghost cells
+   * at receiver index - o*nx */
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int n = 0; n < ndir; ++n) {
+      const int *o = kDirOrder[n];
+      int gid = ms->nghbr[(size_t)m*27 + (o[2] + 1)*9 + (o[1] + 1)*3 + (o[0] + 1)];
+      if (gid < 0) continue;
+      int src = gid - ms->gids;
+      size_t q = boff[n] + (size_t)m*nvar*((hi[n][0]-lo[n][0]+1)*(hi[n][1]-lo[n][1]+1)*(hi[n][2]-lo[n][2]+1));
+      for (int v = 0; v < nvar; ++v)
+        for (int k = lo[n][2]; k <= hi[n][2]; ++k)
+          for (int j = lo[n][1]; j <= hi[n][1]; ++j)
+            for (int i = lo[n][0]; i <= hi[n][0]; ++i)
+              buf[q++] = A5(a, nvar, d, src, v, k - o[2]*nx[2], j - o[1]*nx[1], i - o[0]*nx[0]);
+    }
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int n = 0; n < ndir; ++n) {
+      const int *o = kDirOrder[n];
+      int gid = ms->nghbr[(size_t)m*27 + (o[2] + 1)*9 + (o[1] + 1)*3 + (o[0] + 1)];
+      if (gid < 0) continue;
+      size_t q = boff[n] + (size_t)m*nvar*((hi[n][0]-lo[n][0]+1)*(hi[n][1]-lo[n][1]+1)*(hi[n][2]-lo[n][2]+1));
+      for (int v = 0; v < nvar; ++v)
+        for (int k = lo[n][2]; k <= hi[n][2]; ++k)
+          for (int j = lo[n][1]; j <= hi[n][1]; ++j)
+            for (int i = lo[n][0]; i <= hi[n][0]; ++i)
+              A5(a, nvar, d, m, v, k, j, i) += buf[q++];
+    }
+  free(buf);
+}
+
+/* UstarX3BCs, src/dust/dust_tasks.cpp:445-469 (single level) */
+static void ustar_x3_bcs(const dustb_ctx *c, double *a) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  if (!ms->three_d || ms->x3bc == 0) return;
+  const int refl = (ms->x3bc == 1);
+  for (int m = 0; m < ms->nmb; ++m) {
+    int lo_face = ms->nghbr[(size_t)m*27 + 0*9 + 1*3 + 1] < 0;
+    int hi_face = ms->nghbr[(size_t)m*27 + 2*9 + 1*3 + 1] < 0;
+    for (int g = 0; g < ms->ng; ++g)
+      for (int j = 0; j < d.n2; ++j)
+        for (int i = 0; i < d.n1; ++i) {
+          if (lo_face) {
+            int kg = d.ks - 1 - g, kc = refl ? (d.ks + g) : d.ks;
+            for (int v = 0; v < 3; ++v)
+              A5(a, 3, d, m, v, kg, j, i) = (refl && v == 2) ? -A5(a, 3, d, m, v, kc, j, i)
+                                                             : A5(a, 3, d, m, v, kc, j, i);
+          }
+          if (hi_face) {
+            int kg = d.ke + 1 + g, kc = refl ? (d.ke - g) : d.ke;
+            for (int v = 0; v < 3; ++v)
+              A5(a, 3, d, m, v, kg, j, i) = (refl && v == 2) ? -A5(a, 3, d, m, v, kc, j, i)
+                                                             : A5(a, 3, d, m, v, kc, j, i);
+          }
+        }
+  }
+}
+
+/* MeshBoundaryValuesCC same-level copy exchange: every ghost cell takes the neighbour's
+ * active cell at index - o*nx (InitSendIndices/InitRecvIndices of the CC exchange), then
+ * the x3 physical boundary values when x3_bcs */
+void oracle_ghost_copy(const dustb_ctx *c, double *a, int nvar, int x3_bcs) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = 0; k < d.n3; ++k)
+      for (int j = 0; j < d.n2; ++j)
+        for (int i = 0; i < d.n1; ++i) {
+          int o[3];
+          o[0] = (i < d.is) ? -1 : ((i > d.ie) ? 1 : 0);
+          o[1] = (j < d.js) ? -1 : ((j > d.je) ? 1 : 0);
+          o[2] = (k < d.ks) ? -1 : ((k > d.ke) ? 1 : 0);
+          if (o[0] == 0 && o[1] == 0 && o[2] == 0) continue;
+          int gid = ms->nghbr[(size_t)m*27 + (o[2] + 1)*9 + (o[1] + 1)*3 + (o[0] + 1)];
+          if (gid < 0) continue;
+          int src = gid - ms->gids;
+          for (int v = 0; v < nvar; ++v)
+            A5(a, nvar, d, m, v, k, j, i) =
+                A5(a, nvar, d, src, v, k - o[2]*nx[2], j - o[1]*nx[1], i - o[0]*nx[0]);
+        }
+  if (x3_bcs && nvar == 3) ustar_x3_bcs(c, a);
+}
+
+/* dust_ustar (dust_pm.cpp:426-436) == dust_solver_local_guess (dust_solver.cpp:643-649) */
+void oracle_solve_ustar(const dustb_ctx *c) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  const int br = c->phys.back_reaction;
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = d.ks; k <= d.ke; ++k)
+      for (int j = d.js; j <= d.je; ++j)
+        for (int i = d.is; i <= d.ie; ++i) {
+          double q0 = br ? A5(c->f.qdep, 5, d, m, 0, k, j, i) : 0.0;
+          double denom = 1.0/(A5(c->f.u0, nv, d, m, 0, k, j, i) + q0);
+          for (int v = 0; v < 3; ++v) {
+            double qv = br ? A5(c->f.qdep, 5, d, m, 1 + v, k, j, i) : 0.0;
+            A5(c->f.ustar, 3, d, m, v, k, j, i) = (A5(c->f.u0, nv, d, m, 1 + v, k, j, i) + qv)*denom;
+          }
+        }
+}
+
+/* PointOperatorParticles, src/dust/dust_solver.cpp:126-203 */
+static unsigned operator_particles(const dustb_ctx *c, const double *field, double *result,
+                                   double a_dt, double sh) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  const int clo = ms->three_d ? 0 : 1, chi = ms->three_d ? 2 : 1;
+  unsigned err = 0;
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads) reduction(| : err)
+  for (int p = 0; p < c->part.npart; ++p) {
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    int ip, jp, kp; double wx[3], wy[3], wz[3];
+    particle_weights(c, &d, m, PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p),
+                     PR(DUSTB_IPZ, p), &ip, &jp, &kp, wx, wy, wz);
+    if (!halo_ok(ms, &d, ip, jp, kp)) { err |= DUSTB_ERR_HALO; continue; }
+    double g[3] = {0.0, 0.0, 0.0};
+    for (int cc = clo; cc <= chi; ++cc)
+      for (int b = 0; b < 3; ++b) {
+        double wcb = wz[cc]*wy[b];
+        if (wcb == 0.0) continue;
+        for (int a = 0; a < 3; ++a) {
+          double w = wcb*wx[a];
+          int kk = kp + cc - 1, jj = jp + b - 1, ii = ip + a - 1;
+          g[0] += w*A5(field, 3, d, m, 0, kk, jj, ii);
+          g[1] += w*A5(field, 3, d, m, 1, kk, jj, ii);
+          g[2] += w*A5(field, 3, d, m, 2, kk, jj, ii);
+        }
+      }
+    double vol = cell_volume(ms, m);
+    double cj = a_dt/(PR(DUSTB_IPTS, p) + a_dt);
+    double fac = PR(DUSTB_IPM, p)*cj/vol;
+    for (int cc = clo; cc <= chi; ++cc)
+      for (int b = 0; b < 3; ++b) {
+        double wcb = wz[cc]*wy[b]*fac;
+        if (wcb == 0.0) continue;
+        for (int a = 0; a < 3; ++a) {
+          double w = wcb*wx[a];
+          int kk = kp + cc - 1, jj = jp + b - 1, ii = ip + a - 1;
+          deposit_add(&A5(result, 3, d, m, 0, kk, jj, ii), w*g[0]);
+          deposit_add(&A5(result, 3, d, m, 1, kk, jj, ii), w*g[1]);
+          deposit_add(&A5(result, 3, d, m, 2, kk, jj, ii), w*g[2]);
+        }
+      }
+  }
+  return err;
+}
+
+/* ApplyDefectCorrection -> ApplyCoupledOperatorImpl(correct_field = true),
+ * src/dust/dust_solver.cpp:218-252 */
+unsigned oracle_dc1_sweep(const dustb_ctx *c, double a_dt, double sh) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  double *x = c->f.ustar, *r = c->f.work;
+  oracle_ghost_copy(c, x, 3, 1);
+  memset(r, 0, field_size(ms, 3)*sizeof(double));
+  unsigned err = operator_particles(c, x, r, a_dt, sh);
+  oracle_ghost_add(c, r, 3);
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = d.ks; k <= d.ke; ++k)
+      for (int j = d.js; j <= d.je; ++j)
+        for (int i = d.is; i <= d.ie; ++i) {
+          double rho = A5(c->f.u0, nv, d, m, 0, k, j, i);
+          double pinv = 1.0/(rho + A5(c->f.qdep, 5, d, m, 0, k, j, i));
+          for (int v = 0; v < 3; ++v) {
+            double av = A5(r, 3, d, m, v, k, j, i) + rho*A5(x, 3, d, m, v, k, j, i);
+            double rv = A5(c->f.u0, nv, d, m, 1 + v, k, j, i) +
+                        A5(c->f.qdep, 5, d, m, 1 + v, k, j, i) - av;
+            A5(x, 3, d, m, v, k, j, i) += pinv*rv;
+          }
+        }
+  return err;
+}
+
+/* GatherKickPMBR point particles, src/dust/dust_pm.cpp:450-568 */
+unsigned oracle_gather_kick_pmbr(const dustb_ctx *c, double a_dt, double sh) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  const int br = c->phys.back_reaction;
+  if (br) memset(c->f.dmom, 0, field_size(ms, 3)*sizeof(double));
+  double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  const int clo = ms->three_d ? 0 : 1, chi = ms->three_d ? 2 : 1;
+  unsigned err = 0;
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads) reduction(| : err)
+  for (int p = 0; p < c->part.npart; ++p) {
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    int ip, jp, kp; double wx[3], wy[3], wz[3];
+    particle_weights(c, &d, m, PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p),
+                     PR(DUSTB_IPZ, p), &ip, &jp, &kp, wx, wy, wz);
+    if (!halo_ok(ms, &d, ip, jp, kp)) { err |= DUSTB_ERR_HALO; continue; }
+    double ux = 0.0, uy = 0.0, uz = 0.0;
+    for (int cc = clo; cc <= chi; ++cc)
+      for (int b = 0; b < 3; ++b) {
+        double wcb = wz[cc]*wy[b];
+        if (wcb == 0.0) continue;
+        for (int a = 0; a < 3; ++a) {
+          double w = wcb*wx[a];
+          int kk = kp + cc - 1, jj = jp + b - 1, ii = ip + a - 1;
+          ux += w*A5(c->f.ustar, 3, d, m, 0, kk, jj, ii);
+          uy += w*A5(c->f.ustar, 3, d, m, 1, kk, jj, ii);
+          uz += w*A5(c->f.ustar, 3, d, m, 2, kk, jj, ii);
+        }
+      }
+    double cj = a_dt/(PR(DUSTB_IPTS, p) + a_dt);
+    double dvx = cj*(ux - PR(DUSTB_IPVX, p));
+    double dvy = cj*(uy - PR(DUSTB_IPVY, p));
+    double dvz = cj*(uz - PR(DUSTB_IPVZ, p));
+    PR(DUSTB_IPVX, p) += dvx; PR(DUSTB_IPVY, p) += dvy; PR(DUSTB_IPVZ, p) += dvz;
+    PR(DUSTB_IPRX, p) = dvx/a_dt; PR(DUSTB_IPRY, p) = dvy/a_dt; PR(DUSTB_IPRZ, p) = dvz/a_dt;
+    if (br) {
+      double vol = cell_volume(ms, m);
+      double fac = -PR(DUSTB_IPM, p)/vol;
+      for (int cc = clo; cc <= chi; ++cc)
+        for (int b = 0; b < 3; ++b) {
+          double wcb = wz[cc]*wy[b]*fac;
+          if (wcb == 0.0) continue;
+          for (int a = 0; a < 3; ++a) {
+            double w = wcb*wx[a];
+            int kk = kp + cc - 1, jj = jp + b - 1, ii = ip + a - 1;
+            deposit_add(&A5(c->f.dmom, 3, d, m, 0, kk, jj, ii), w*dvx);
+            deposit_add(&A5(c->f.dmom, 3, d, m, 1, kk, jj, ii), w*dvy);
+            deposit_add(&A5(c->f.dmom, 3, d, m, 2, kk, jj, ii), w*dvz);
+          }
+        }
+    }
+  }
+  return err;
+}
+
+/* ApplyPMBR imex, src/dust/dust_pm.cpp:605-711 (consistent point split :624-697) */
+void oracle_apply_pmbr(const dustb_ctx *c, double a_dt) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  if (!c->phys.back_reaction) return;
+  const double inv_adt = 1.0/a_dt;
+  double *u0 = c->f.u0, *dm = c->f.dmom;
+  if (!c->phys.consistent_gas) {
+    for (int m = 0; m < ms->nmb; ++m)
+      for (int k = d.ks; k <= d.ke; ++k)
+        for (int j = d.js; j <= d.je; ++j)
+          for (int i = d.is; i <= d.ie; ++i)
+            for (int v = 0; v < 3; ++v) {
+              A5(u0, nv, d, m, 1 + v, k, j, i) += A5(dm, 3, d, m, v, k, j, i);
+              A5(dm, 3, d, m, v, k, j, i) *= inv_adt;
+            }
+    return;
+  }
+  double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  double *res = c->f.resid;
+  memset(res, 0, field_size(ms, 4)*sizeof(double));
+  for (int p = 0; p < c->part.npart; ++p) {     /* dust_imex_point_center_mass */
+    if (PR(DUSTB_IPM, p) <= 0.0) continue;
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    int ip, jp, kp; double w[3];
+    pm_weights(PR(DUSTB_IPX, p), MB(m, X1MIN), MB(m, X1MAX), ms->nx1, d.is, c->phys.scheme, &ip, w);
+    pm_weights(PR(DUSTB_IPY, p), MB(m, X2MIN), MB(m, X2MAX), ms->nx2, d.js, c->phys.scheme, &jp, w);
+    if (ms->three_d) pm_weights(PR(DUSTB_IPZ, p), MB(m, X3MIN), MB(m, X3MAX), ms->nx3, d.ks,
+                                c->phys.scheme, &kp, w);
+    else kp = d.ks;
+    double vol = cell_volume(ms, m);
+    deposit_add(&A5(res, 4, d, m, 3, kp, jp, ip),
+                PR(DUSTB_IPM, p)*(a_dt/(PR(DUSTB_IPTS, p) + a_dt))/vol);
+  }
+  for (int m = 0; m < ms->nmb; ++m)              /* dust_imex_point_consistent_gas */
+    for (int k = d.ks; k <= d.ke; ++k)
+      for (int j = d.js; j <= d.je; ++j)
+        for (int i = d.is; i <= d.ie; ++i) {
+          const double rho = A5(u0, nv, d, m, 0, k, j, i), qt = A5(res, 4, d, m, 3, k, j, i);
+          const double q = A5(c->f.qdep, 5, d, m, 0, k, j, i);
+          for (int v = 0; v < 3; ++v) {
+            double dgas = A5(dm, 3, d, m, v, k, j, i);
+            if (qt > 0.0) {
+              const double g = rho*A5(c->f.ustar, 3, d, m, v, k, j, i) - A5(u0, nv, d, m, 1 + v, k, j, i);
+              const double r = (A5(dm, 3, d, m, v, k, j, i) - g)/(rho + q);
+              dgas = g + rho*r;
+              A5(res, 4, d, m, v, k, j, i) = r*q/qt;
+            }
+            A5(u0, nv, d, m, 1 + v, k, j, i) += dgas;
+            A5(dm, 3, d, m, v, k, j, i) = dgas*inv_adt;
+          }
+        }
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int p = 0; p < c->part.npart; ++p) {     /* dust_imex_point_consistent_dust */
+    if (PR(DUSTB_IPM, p) <= 0.0) continue;
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    int ip, jp, kp; double w[3];
+    pm_weights(PR(DUSTB_IPX, p), MB(m, X1MIN), MB(m, X1MAX), ms->nx1, d.is, c->phys.scheme, &ip, w);
+    pm_weights(PR(DUSTB_IPY, p), MB(m, X2MIN), MB(m, X2MAX), ms->nx2, d.js, c->phys.scheme, &jp, w);
+    if (ms->three_d) pm_weights(PR(DUSTB_IPZ, p), MB(m, X3MIN), MB(m, X3MAX), ms->nx3, d.ks,
+                                c->phys.scheme, &kp, w);
+    else kp = d.ks;
+    const double cj = a_dt/(PR(DUSTB_IPTS, p) + a_dt);
+    for (int v = 0; v < 3; ++v) {
+      const double dv = cj*A5(res, 4, d, m, v, kp, jp, ip);
+      PR(DUSTB_IPVX + 2*v, p) += dv;
+      PR(DUSTB_IPRX + v, p) += dv/a_dt;
+    }
+  }
+}
+
+/* NewTimeStep, src/dust/dust_newdt.cpp:108-149 (the particle part, before the CFL factor) */
+double oracle_newdt(const dustb_ctx *c) {
+  const dustb_mesh *ms = &c->mesh;
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  const int shear3d = c->phys.shearing_box && ms->three_d;
+  const double qo = c->phys.qshear*c->phys.omega0;
+  double dtp = (double)FLT_MAX;
+  for (int p = 0; p < c->part.npart; ++p) {
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    double vy = PR(DUSTB_IPVY, p);
+    if (shear3d) vy -= qo*PR(DUSTB_IPX, p);
+    dtp = fmin(MB(m, DX1)/fmax(fabs(PR(DUSTB_IPVX, p)), 1.0e-30), dtp);
+    dtp = fmin(MB(m, DX2)/fmax(fabs(vy), 1.0e-30), dtp);
+    if (ms->three_d) dtp = fmin(MB(m, DX3)/fmax(fabs(PR(DUSTB_IPVZ, p)), 1.0e-30), dtp);
+  }
+  return dtp;
+}
+
+/* RefreshStoppingTimeMaximum (validation + extrema), src/dust/dust_newdt.cpp:34-98 */
+void oracle_tstop_extrema(const dustb_ctx *c, int nspecies, double out[2]) {
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  double mx = 0.0, mn = DBL_MAX;
+  for (int p = 0; p < c->part.npart; ++p) {
+    int s = PI(DUSTB_PSP, p);
+    double ts = PR(DUSTB_IPTS, p);
+    int bad = (s < 0 || (nspecies > 0 && s >= nspecies) || !isfinite(ts) || !(ts > 0.0));
+    mx = fmax(mx, bad ? DBL_MAX : ts);
+    mn = fmin(mn, ts);
+  }
+  out[0] = mx; out[1] = mn;
+}
+
+/* ---- SortParticles, src/dust/dust_cloud_device.cpp:1881-1977 ---------------------------- */
+static int cmp_i64(const void *a, const void *b) {
+  int64_t x = *(const int64_t *)a, y = *(const int64_t *)b;
+  return (x > y) - (x < y);
+}
+
+/* the sort keys (block, k, j, i) of the floor() cell formula and the resulting permutation
+ * (order[k] = old index of the particle that goes to slot k) */
+void oracle_sort_order(const dustb_ctx *c, int *order, int64_t *cellkey) {
+  const dustb_mesh *ms = &c->mesh;
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  const int n = c->part.npart;
+  const int nx1 = ms->nx1, nx2 = ms->nx2, nx3 = ms->three_d ? ms->nx3 : 1;
+  const int64_t ncell = (int64_t)nx1*nx2*nx3, np = n;
+  int64_t *key = (int64_t *)malloc(sizeof(int64_t)*(size_t)(n > 0 ? n : 1));
+  for (int p = 0; p < n; ++p) {
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    m = (m < 0) ? 0 : ((m >= ms->nmb) ? ms->nmb - 1 : m);
+    int i = (int)floor((PR(DUSTB_IPX, p) - MB(m, X1MIN))/MB(m, DX1));
+    int j = (int)floor((PR(DUSTB_IPY, p) - MB(m, X2MIN))/MB(m, DX2));
+    i = (i < 0) ? 0 : ((i >= nx1) ? nx1 - 1 : i);
+    j = (j < 0) ? 0 : ((j >= nx2) ? nx2 - 1 : j);
+    int k = 0;
+    if (ms->three_d) {
+      k = (int)floor((PR(DUSTB_IPZ, p) - MB(m, X3MIN))/MB(m, DX3));
+      k = (k < 0) ? 0 : ((k >= nx3) ? nx3 - 1 : k);
+    }
+    int64_t cell = ((int64_t)k*nx2 + j)*nx1 + i;
+    key[p] = (m*ncell + cell)*np + p;
+    if (cellkey) cellkey[p] = m*ncell + cell;
+  }
+  qsort(key, (size_t)n, sizeof(int64_t), cmp_i64);
+  for (int k = 0; k < n; ++k) order[k] = (int)(key[k] % np);
+  free(key);
+}
+
+void oracle_sort_particles(const dustb_ctx *c, double *spare_pr, int *spare_pi) {
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  const int n = c->part.npart;
+  int *order = (int *)malloc(sizeof(int)*(size_t)(n > 0 ? n : 1));
+  oracle_sort_order(c, order, NULL);
+  for (int k = 0; k < n; ++k) {
+    int p = order[k];
+    for (int r = 0; r < DUSTB_NREAL; ++r) spare_pr[(size_t)r*stride + k] = PR(r, p);
+    for (int r = 0; r < DUSTB_NINT; ++r) spare_pi[(size_t)r*stride + k] = PI(r, p);
+  }
+  free(order);
+}
+
+/* ---- pc2 ------------------------------------------------------------------------------ */
+/* DepositDrag pc2 predictor, src/dust/dust_pm.cpp:109-194 (qdep zeroed first) */
+unsigned oracle_pc2_predictor(const dustb_ctx *c, double dt, int rate_dep) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  memset(c->f.qdep, 0, field_size(ms, 5)*sizeof(double));
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  const double *uold = c->f.u1;
+  const int clo = ms->three_d ? 0 : 1, chi = ms->three_d ? 2 : 1;
+  unsigned err = 0;
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads) reduction(| : err)
+  for (int p = 0; p < c->part.npart; ++p) {
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    int ip, jp, kp; double wx[3], wy[3], wz[3];
+    particle_weights(c, &d, m, PR(DUSTB_IPX, p), PR(DUSTB_IPY, p), PR(DUSTB_IPZ, p),
+                     &ip, &jp, &kp, wx, wy, wz);
+    if (!halo_ok(ms, &d, ip, jp, kp)) { err |= DUSTB_ERR_HALO; continue; }
+    double ugx = 0.0, ugy = 0.0, ugz = 0.0;
+    for (int cc = clo; cc <= chi; ++cc)
+      for (int b = 0; b < 3; ++b) {
+        double wcb = wz[cc]*wy[b];
+        if (wcb == 0.0) continue;
+        for (int a = 0; a < 3; ++a) {
+          double w = wcb*wx[a];
+          int kk = kp + cc - 1, jj = jp + b - 1, ii = ip + a - 1;
+          double invrho = 1.0/A5(uold, nv, d, m, 0, kk, jj, ii);
+          ugx += w*A5(uold, nv, d, m, 1, kk, jj, ii)*invrho;
+          ugy += w*A5(uold, nv, d, m, 2, kk, jj, ii)*invrho;
+          ugz += w*A5(uold, nv, d, m, 3, kk, jj, ii)*invrho;
+        }
+      }
+    double vol = cell_volume(ms, m);
+    double rate = PR(DUSTB_IPM, p)/(PR(DUSTB_IPTS, p)*vol);
+    double gx = -dt*rate*(ugx - PR(DUSTB_IPVX, p));
+    double gy = -dt*rate*(ugy - PR(DUSTB_IPVY, p));
+    double gz = -dt*rate*(ugz - PR(DUSTB_IPVZ, p));
+    for (int cc = clo; cc <= chi; ++cc)
+      for (int b = 0; b < 3; ++b) {
+        double wcb = wz[cc]*wy[b];
+        if (wcb == 0.0) continue;
+        for (int a = 0; a < 3; ++a) {
+          double w = wcb*wx[a];
+          int kk = kp + cc - 1, jj = jp + b - 1, ii = ip + a - 1;
+          deposit_add(&A5(c->f.qdep, 5, d, m, 1, kk, jj, ii), w*gx);
+          deposit_add(&A5(c->f.qdep, 5, d, m, 2, kk, jj, ii), w*gy);
+          deposit_add(&A5(c->f.qdep, 5, d, m, 3, kk, jj, ii), w*gz);
+          if (rate_dep) deposit_add(&A5(c->f.qdep, 5, d, m, 4, kk, jj, ii), w*rate);
+        }
+      }
+  }
+  return err;
+}
+
+/* GasImplicitSolve pc2 stage 1, src/dust/dust_pm.cpp:374-405, with UpdateStiffness's
+ * maximum (dust_pm.cpp:288-300) returned as chi = dt*max(qdep4/rho) */
+double oracle_pc2_apply_predictor(const dustb_ctx *c, double dt) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  double rate = 0.0;
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = d.ks; k <= d.ke; ++k)
+      for (int j = d.js; j <= d.je; ++j)
+        for (int i = d.is; i <= d.ie; ++i)
+          rate = fmax(rate, A5(c->f.qdep, 5, d, m, 4, k, j, i)/A5(c->f.u0, nv, d, m, 0, k, j, i));
+  const int damp = c->phys.pc2_feedback_damping;
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = d.ks; k <= d.ke; ++k)
+      for (int j = d.js; j <= d.je; ++j)
+        for (int i = d.is; i <= d.ie; ++i) {
+          if (damp) {
+            const double chi = dt*A5(c->f.qdep, 5, d, m, 4, k, j, i)/A5(c->f.u0, nv, d, m, 0, k, j, i);
+            if (chi > 1.0) {
+              const double s = 1.0/chi;
+              for (int v = 1; v <= 3; ++v) A5(c->f.qdep, 5, d, m, v, k, j, i) *= s;
+            }
+          }
+          for (int v = 1; v <= 3; ++v)
+            A5(c->f.u0, nv, d, m, v, k, j, i) += A5(c->f.qdep, 5, d, m, v, k, j, i);
+        }
+  return dt*rate;
+}
+
+/* FirstTwoImpRK pc2 stage 2, src/dust/dust_push.cpp:37-61 (ghosts included) */
+void oracle_pc2_midpoint(const dustb_ctx *c) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = 0; k < d.n3; ++k)
+      for (int j = 0; j < d.n2; ++j)
+        for (int i = 0; i < d.n1; ++i) {
+          double inv = 1.0/(A5(c->f.u1, nv, d, m, 0, k, j, i) + A5(c->f.u0, nv, d, m, 0, k, j, i));
+          for (int v = 0; v < 3; ++v)
+            A5(c->f.ustar, 3, d, m, v, k, j, i) =
+                (A5(c->f.u1, nv, d, m, 1 + v, k, j, i) + A5(c->f.u0, nv, d, m, 1 + v, k, j, i))*inv;
+        }
+}
+
+/* ExplicitPush pc2 advance, src/dust/dust_push.cpp:99-247 (dmom zeroed first) */
+unsigned oracle_pc2_advance(const dustb_ctx *c, double dt) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  const int br = c->phys.back_reaction, three_d = ms->three_d;
+  const int sbox = c->phys.shearing_box, strat = c->phys.stratified;
+  const double q = c->phys.qshear, om = c->phys.omega0, aphi = c->phys.const_accel_phi;
+  if (br) memset(c->f.dmom, 0, field_size(ms, 3)*sizeof(double));
+  double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  const int clo = three_d ? 0 : 1, chi = three_d ? 2 : 1;
+  unsigned err = 0;
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads) reduction(| : err)
+  for (int p = 0; p < c->part.npart; ++p) {
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    double x0 = PR(DUSTB_IPX1, p), y0 = PR(DUSTB_IPY1, p), z0 = PR(DUSTB_IPZ1, p);
+    double vx0 = PR(DUSTB_IPVX1, p), vy0 = PR(DUSTB_IPVY1, p), vz0 = PR(DUSTB_IPVZ1, p);
+    double xh = x0 + 0.5*dt*vx0;
+    double yh = y0 + 0.5*dt*(vy0 - ((sbox && three_d) ? q*om*x0 : 0.0));
+    double zh = three_d ? z0 + 0.5*dt*vz0 : z0;
+    double yg = yh + ((sbox && three_d) ? q*om*xh*0.5*dt : 0.0);
+    int ip, jp, kp; double wx[3], wy[3], wz[3];
+    particle_weights(c, &d, m, xh, yg, zh, &ip, &jp, &kp, wx, wy, wz);
+    if (!halo_ok(ms, &d, ip, jp, kp)) { err |= DUSTB_ERR_HALO; continue; }
+    double ugx = 0.0, ugy = 0.0, ugz = 0.0;
+    for (int cc = clo; cc <= chi; ++cc)
+      for (int b = 0; b < 3; ++b) {
+        double wcb = wz[cc]*wy[b];
+        if (wcb == 0.0) continue;
+        for (int a = 0; a < 3; ++a) {
+          double w = wcb*wx[a];
+          int kk = kp + cc - 1, jj = jp + b - 1, ii = ip + a - 1;
+          ugx += w*A5(c->f.ustar, 3, d, m, 0, kk, jj, ii);
+          ugy += w*A5(c->f.ustar, 3, d, m, 1, kk, jj, ii);
+          ugz += w*A5(c->f.ustar, 3, d, m, 2, kk, jj, ii);
+        }
+      }
+    double h = 0.5*dt;
+    double lambda = h/PR(DUSTB_IPTS, p);
+    double aa = 1.0 + lambda;
+    double rx = vx0 + lambda*ugx, ry = vy0 + lambda*ugy, rz = vz0 + lambda*ugz;
+    double vxh, vyh, vzh;
+    if (sbox && three_d) {
+      double cxy = 2.0*h*om, cyx = h*(2.0 - q)*om;
+      double det = aa*aa + cxy*cyx;
+      vxh = (aa*rx + cxy*ry)/det;
+      vyh = (aa*ry - cyx*rx)/det;
+      if (strat) rz -= h*SQR(om)*zh;
+      vzh = rz/aa;
+    } else if (sbox) {
+      double cxz = 2.0*h*om, czx = h*(2.0 - q)*om;
+      double det = aa*aa + cxz*czx;
+      if (aphi != 0.0) rz += h*aphi;
+      vxh = (aa*rx + cxz*rz)/det;
+      vzh = (aa*rz - czx*rx)/det;
+      vyh = ry/aa;
+    } else {
+      vxh = rx/aa; vyh = ry/aa; vzh = rz/aa;
+    }
+    PR(DUSTB_IPVX, p) = 2.0*vxh - vx0;
+    PR(DUSTB_IPVY, p) = 2.0*vyh - vy0;
+    PR(DUSTB_IPVZ, p) = 2.0*vzh - vz0;
+    PR(DUSTB_IPX, p) = x0 + dt*vxh;
+    PR(DUSTB_IPY, p) = y0 + dt*(vyh - ((sbox && three_d) ? q*om*xh : 0.0));
+    if (three_d) PR(DUSTB_IPZ, p) = z0 + dt*vzh;
+    PR(DUSTB_IPX1, p) = xh; PR(DUSTB_IPY1, p) = yh; PR(DUSTB_IPZ1, p) = zh;
+    double dvx = dt*(ugx - vxh)/PR(DUSTB_IPTS, p);
+    double dvy = dt*(ugy - vyh)/PR(DUSTB_IPTS, p);
+    double dvz = dt*(ugz - vzh)/PR(DUSTB_IPTS, p);
+    PR(DUSTB_IPRX, p) = dvx; PR(DUSTB_IPRY, p) = dvy; PR(DUSTB_IPRZ, p) = dvz;
+    if (br) {
+      double vol = cell_volume(ms, m);
+      double fac = -PR(DUSTB_IPM, p)/vol;
+      for (int cc = clo; cc <= chi; ++cc)
+        for (int b = 0; b < 3; ++b) {
+          double wcb = wz[cc]*wy[b]*fac;
+          if (wcb == 0.0) continue;
+          for (int a = 0; a < 3; ++a) {
+            double w = wcb*wx[a];
+            int kk = kp + cc - 1, jj = jp + b - 1, ii = ip + a - 1;
+            deposit_add(&A5(c->f.dmom, 3, d, m, 0, kk, jj, ii), w*dvx);
+            deposit_add(&A5(c->f.dmom, 3, d, m, 1, kk, jj, ii), w*dvy);
+            deposit_add(&A5(c->f.dmom, 3, d, m, 2, kk, jj, ii), w*dvz);
+          }
+        }
+    }
+  }
+  return err;
+}
+
+/* ApplyPMBR pc2 commit, src/dust/dust_pm.cpp:585-602 */
+void oracle_pc2_commit(const dustb_ctx *c, double wpred) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = d.ks; k <= d.ke; ++k)
+      for (int j = d.js; j <= d.je; ++j)
+        for (int i = d.is; i <= d.ie; ++i)
+          for (int v = 0; v < 3; ++v)
+            A5(c->f.u0, nv, d, m, 1 + v, k, j, i) +=
+                A5(c->f.dmom, 3, d, m, v, k, j, i) - wpred*A5(c->f.qdep, 5, d, m, 1 + v, k, j, i);
+}
+
+/* ---- cycle drivers: the task order of src/dust/dust_tasks.cpp:38-120 -------------------- */
+
+/* imex2+ tableau, src/driver/driver.cpp:278-300 */
+void oracle_imex2p_coeffs(double gamma, double gam0[3], double gam1[3], double beta[3],
+                          double *atw22) {
+  gam0[0] = 1.0; gam1[0] = 0.0; beta[0] = gamma;
+  gam0[1] = (2.0*gamma - 1.0)/(2.0*gamma*gamma);
+  gam1[1] = (1.0 - (2.0*gamma - 1.0)/(2.0*gamma*gamma));
+  beta[1] = 1.0/(2.0*gamma);
+  gam0[2] = 1.0; gam1[2] = 0.0; beta[2] = 0.0;
+  *atw22 = (1.0 - 2.0*gamma*gamma)/2.0/gamma;
+}
+
+/* one imex2+ cycle; sh[s] is ImplicitShearShift of working stage s+1 */
+unsigned oracle_imex_cycle(const dustb_ctx *c, double gamma, double dt, const double sh[2],
+                           double *x3_removed) {
+  double gam0[3], gam1[3], beta[3], atw22;
+  oracle_imex2p_coeffs(gamma, gam0, gam1, beta, &atw22);
+  const double a_dt = gamma*dt;
+  unsigned err = 0;
+  for (int stage = 1; stage <= 2; ++stage) {
+    if (stage == 1) oracle_register_copy(c);
+    /* gas chain: RKUpdate stand-in, then the drag history term */
+    oracle_gas_rk_noflux(c, gam0[stage - 1], gam1[stage - 1]);
+    if (stage == 2 && c->phys.back_reaction) oracle_history_gas(c, atw22*dt);
+    /* particle chain */
+    oracle_push_imex(c, gam0[stage - 1], gam1[stage - 1], beta[stage - 1]*dt,
+                     (stage == 2) ? atw22*dt : 0.0);
+    err |= oracle_route(c, x3_removed);
+    const double s = sh[stage - 1];
+    if (c->phys.back_reaction) {
+      err |= oracle_deposit_qp(c, a_dt, s);
+      oracle_ghost_add(c, c->f.qdep, 5);
+    }
+    oracle_solve_ustar(c);
+    if (c->phys.back_reaction && c->phys.drag_solver >= DUSTB_SOLVER_DC1) {
+      int nsweeps = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
+      for (int w = 0; w < nsweeps; ++w) err |= oracle_dc1_sweep(c, a_dt, s);
+    }
+    oracle_ghost_copy(c, c->f.ustar, 3, 1);
+    err |= oracle_gather_kick_pmbr(c, a_dt, s);
+    if (c->phys.back_reaction) {
+      oracle_ghost_add(c, c->f.dmom, 3);
+      oracle_apply_pmbr(c, a_dt);
+    }
+    /* gas tail: the ghost exchange of the conserved state */
+    oracle_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0);
+  }
+  return err;
+}
+
+/* one pc2 cycle (integrator rk2: gam0 = {1, 1/2}, gam1 = {0, 1/2}) */
+unsigned oracle_pc2_cycle(const dustb_ctx *c, double dt, double *chi_out, double *x3_removed) {
+  unsigned err = 0;
+  const int br = c->phys.back_reaction;
+  /* stage 1 */
+  oracle_register_copy(c);
+  oracle_gas_rk_noflux(c, 1.0, 0.0);
+  double chi = 0.0;
+  if (br) {
+    err |= oracle_pc2_predictor(c, dt, 1);
+    oracle_ghost_add(c, c->f.qdep, 5);
+    chi = oracle_pc2_apply_predictor(c, dt);
+  }
+  oracle_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0);
+  /* stage 2 */
+  oracle_pc2_midpoint(c);
+  oracle_gas_rk_noflux(c, 0.5, 0.5);
+  err |= oracle_pc2_advance(c, dt);
+  err |= oracle_route(c, x3_removed);
+  if (br) {
+    oracle_ghost_add(c, c->f.dmom, 3);
+    oracle_pc2_commit(c, 0.5);
+  }
+  oracle_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0);
+  if (chi_out) *chi_out = chi;
+  return err;
+}

@@ -1,0 +1,218 @@
+"""ctypes front end of the CPU oracle (oracle/liboracle_dust.so).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg, as the checker.  The product path never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from athenak_b200 import capi
+from athenak_b200.inputs import DustState
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle_dust.so")
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with the system gcc (OpenMP if available)."""
+    src = os.path.join(HERE, "dust_oracle.c")
+    hdr = os.path.join(HERE, "..", "include", "dustb.h")
+    if (not force and os.path.exists(LIB)
+            and os.path.getmtime(LIB) >= max(os.path.getmtime(src), os.path.getmtime(hdr))):
+        return LIB
+    base = ["gcc", "-O2", "-std=c11", "-fPIC", "-ffp-contract=off", "-shared", "-o", LIB, src, "-lm"]
+    try:
+        subprocess.run(base[:4] + ["-fopenmp"] + base[4:], check=True, capture_output=True)
+    except subprocess.CalledProcessError:
+        subprocess.run(base, check=True, capture_output=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(LIB)
+        P = C.POINTER(capi.DustbCtx)
+        D, VP, I = C.c_double, C.c_void_p, C.c_int
+        sig = {
+            "oracle_set_threads": ([I], None),
+            "oracle_register_copy": ([P], None),
+            "oracle_gas_rk_noflux": ([P, D, D], None),
+            "oracle_history_gas": ([P, D], None),
+            "oracle_push_imex": ([P, D, D, D, D], None),
+            "oracle_route": ([P, VP], C.c_uint),
+            "oracle_deposit_qp": ([P, D, D], C.c_uint),
+            "oracle_ghost_add": ([P, VP, I], None),
+            "oracle_ghost_copy": ([P, VP, I, I], None),
+            "oracle_solve_ustar": ([P], None),
+            "oracle_dc1_sweep": ([P, D, D], C.c_uint),
+            "oracle_gather_kick_pmbr": ([P, D, D], C.c_uint),
+            "oracle_apply_pmbr": ([P, D], None),
+            "oracle_newdt": ([P], D),
+            "oracle_tstop_extrema": ([P, I, VP], None),
+            "oracle_sort_order": ([P, VP, VP], None),
+            "oracle_sort_particles": ([P, VP, VP], None),
+            "oracle_pc2_predictor": ([P, D, I], C.c_uint),
+            "oracle_pc2_apply_predictor": ([P, D], D),
+            "oracle_pc2_midpoint": ([P], None),
+            "oracle_pc2_advance": ([P, D], C.c_uint),
+            "oracle_pc2_commit": ([P, D], None),
+            "oracle_imex_cycle": ([P, D, D, VP, VP], C.c_uint),
+            "oracle_pc2_cycle": ([P, D, VP, VP], C.c_uint),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(_lib, name)
+            f.argtypes = args
+            f.restype = res
+    return _lib
+
+
+def imex2p_coeffs(gamma):
+    """imex2+ tableau (src/driver/driver.cpp:278-300)."""
+    g0 = [1.0, (2.0 * gamma - 1.0) / (2.0 * gamma * gamma), 1.0]
+    g1 = [0.0, 1.0 - (2.0 * gamma - 1.0) / (2.0 * gamma * gamma), 0.0]
+    b = [gamma, 1.0 / (2.0 * gamma), 0.0]
+    atw22 = (1.0 - 2.0 * gamma * gamma) / 2.0 / gamma
+    return g0, g1, b, atw22
+
+
+GAMMA_DEFAULT = 1.707106781186547   # 1 + 1/sqrt(2), driver.cpp:201
+
+
+class Oracle:
+    """The oracle's copy of a DustState (host arrays) and its context."""
+
+    def __init__(self, st: DustState, phys: dict, threads: int = 1):
+        self.st = st.copy()
+        ms = st.mesh
+        self.mesh = ms
+        self.arr = {
+            "pr": self.st.pr, "pi": self.st.pi, "u0": self.st.u0,
+            "u1": np.zeros(ms.field_shape(4)), "qdep": np.zeros(ms.field_shape(5)),
+            "ustar": np.zeros(ms.field_shape(3)), "dmom": np.zeros(ms.field_shape(3)),
+            "resid": np.zeros(ms.field_shape(4)), "work": np.zeros(ms.field_shape(3)),
+            "mb_size": np.ascontiguousarray(ms.mb_size),
+            "nghbr": np.ascontiguousarray(ms.nghbr),
+        }
+        self.phys = dict(phys)
+        self.ctx = capi.make_ctx(ms, self.arr, self.st.npart, self.st.stride, self.phys)
+        self.threads = threads
+        self.x3_removed = np.zeros(2)
+
+    def __getattr__(self, name):
+        arr = self.__dict__.get("arr")
+        if arr is not None and name in arr:
+            return arr[name]
+        raise AttributeError(name)
+
+    def call(self, name, *args):
+        L = lib()
+        L.oracle_set_threads(self.threads)
+        return getattr(L, "oracle_" + name)(C.byref(self.ctx), *args)
+
+    # --- single tasks ---
+    def register_copy(self):
+        self.call("register_copy")
+
+    def push_imex(self, gam0, gam1, beta_dt, atw_dt):
+        self.call("push_imex", gam0, gam1, beta_dt, atw_dt)
+
+    def route(self):
+        return self.call("route", self.x3_removed.ctypes.data)
+
+    def deposit_qp(self, a_dt, sh=0.0):
+        return self.call("deposit_qp", a_dt, sh)
+
+    def ghost_add(self, name, nvar):
+        self.call("ghost_add", self.arr[name].ctypes.data, nvar)
+
+    def ghost_copy(self, name, nvar, x3_bcs=1):
+        self.call("ghost_copy", self.arr[name].ctypes.data, nvar, x3_bcs)
+
+    def solve_ustar(self):
+        self.call("solve_ustar")
+
+    def dc1_sweep(self, a_dt, sh=0.0):
+        return self.call("dc1_sweep", a_dt, sh)
+
+    def gather_kick_pmbr(self, a_dt, sh=0.0):
+        return self.call("gather_kick_pmbr", a_dt, sh)
+
+    def apply_pmbr(self, a_dt):
+        self.call("apply_pmbr", a_dt)
+
+    def history_gas(self, atw_dt):
+        self.call("history_gas", atw_dt)
+
+    def gas_rk_noflux(self, g0, g1):
+        self.call("gas_rk_noflux", g0, g1)
+
+    def newdt(self):
+        return self.call("newdt")
+
+    def tstop_extrema(self, nspecies):
+        out = np.zeros(2)
+        self.call("tstop_extrema", nspecies, out.ctypes.data)
+        return out
+
+    def sort_order(self):
+        n = self.st.npart
+        order = np.zeros(max(n, 1), np.int32)
+        keys = np.zeros(max(n, 1), np.int64)
+        self.call("sort_order", order.ctypes.data, keys.ctypes.data)
+        return order[:n], keys[:n]
+
+    def sort_particles(self):
+        spr = np.zeros_like(self.st.pr)
+        spi = np.zeros_like(self.st.pi)
+        self.call("sort_particles", spr.ctypes.data, spi.ctypes.data)
+        self.st.pr[...] = spr
+        self.st.pi[...] = spi
+
+    # --- pc2 ---
+    def pc2_predictor(self, dt, rate_dep=1):
+        return self.call("pc2_predictor", dt, rate_dep)
+
+    def pc2_apply_predictor(self, dt):
+        return self.call("pc2_apply_predictor", dt)
+
+    def pc2_midpoint(self):
+        self.call("pc2_midpoint")
+
+    def pc2_advance(self, dt):
+        return self.call("pc2_advance", dt)
+
+    def pc2_commit(self, wpred):
+        self.call("pc2_commit", wpred)
+
+    # --- cycles ---
+    def imex_cycle(self, dt, gamma=GAMMA_DEFAULT, sh=(0.0, 0.0)):
+        shv = (C.c_double * 2)(*sh)
+        return self.call("imex_cycle", gamma, dt, C.cast(shv, C.c_void_p),
+                         self.x3_removed.ctypes.data)
+
+    def pc2_cycle(self, dt):
+        chi = C.c_double(0.0)
+        err = self.call("pc2_cycle", dt, C.cast(C.byref(chi), C.c_void_p),
+                        self.x3_removed.ctypes.data)
+        return err, chi.value
+
+    # --- diagnostics ---
+    def momentum(self):
+        """Total (gas, dust) momentum vectors over active cells / live particles."""
+        ms = self.mesh
+        g = ms.active(self.arr["u0"])[:, 1:4].sum(axis=(0, 2, 3, 4)) * ms.cell_volume()
+        n = self.st.npart
+        pr = self.st.pr
+        m = pr[16, :n]
+        d = np.array([(m * pr[1, :n]).sum(), (m * pr[3, :n]).sum(), (m * pr[5, :n]).sum()])
+        return g, d

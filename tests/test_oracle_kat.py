@@ -1,0 +1,242 @@
+"""CPU checks of the oracle against the reference's known-answer tests and against
+independent numpy restatements (no GPU needed).
+
+Pins (the reference ships no golden output files):
+* dust_damping ODE (src/pgen/tests/dust_damping.cpp:9-16): mean gas/dust velocities of the
+  lattice set-up follow the linear ODE; the error must fall by > 2.5 when dt halves and the
+  total momentum must hold to < 1e-12 (tst/test_suite/dust/check_cloud_imex3d.py:66-74,
+  :112-121), for a resolved and a stiff (t_s = 1e-4) species mixture;
+* the committed damping-ODE fixture tests/golden/damping_ode.json (make_golden.py);
+* exact momentum conservation with random placement (dust_pm.cpp:17-21, :545-563);
+* the NSH drift used by the generator solves the steady equations (dust_setup.hpp:58-65).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from athenak_b200.mesh import uniform_mesh
+from athenak_b200.inputs import make_state, nsh_gas, nsh_dust, hash_uniform01
+from oracle.oracle import Oracle, GAMMA_DEFAULT
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def damping_run(dt, taus, eps, vd, tlim, nb=(8, 8, 1), ncells=(16, 16, 1)):
+    ms = uniform_mesh(ncells, nb, 2, (-0.5, -0.5, -0.5), (0.5, 0.5, 0.5))
+    st = make_state(ms, taus, eps, 1, placement="lattice", vd=vd, gas_noise=0.0)
+    o = Oracle(st, dict(scheme=2, drag_solver=2))
+    n = int(round(tlim / dt))
+    g0, d0 = o.momentum()
+    for _ in range(n):
+        assert o.imex_cycle(dt) == 0
+    g1, d1 = o.momentum()
+    u = o.mesh.active(o.u0)[:, 1].mean()
+    pr, sp = o.st.pr, o.st.pi[2, :o.st.npart]
+    v = [pr[1, :o.st.npart][sp == s].mean() for s in range(len(taus))]
+    return np.array([u] + v), np.abs((g1 + d1) - (g0 + d0)).max(), n * dt
+
+
+def ode_solution(taus, eps, vd, t):
+    from scipy.linalg import expm
+    N = len(taus)
+    A = np.zeros((N + 1, N + 1))
+    for s in range(N):
+        A[0, 0] -= eps[s] / taus[s]
+        A[0, 1 + s] += eps[s] / taus[s]
+        A[1 + s, 1 + s] = -1.0 / taus[s]
+        A[1 + s, 0] = 1.0 / taus[s]
+    return expm(A * t) @ np.array([0.0] + list(vd))
+
+
+@pytest.mark.parametrize("stiff", [False, True])
+def test_damping_ode_convergence_and_conservation(stiff):
+    taus = [1e-4 if stiff else 0.1, 0.03, 1.0]
+    eps = [0.2, 0.5, 0.3]
+    vd = [0.01 / 3, 0.02 / 3, 0.01]
+    dt = 0.4 / 16
+    y1, dp1, t1 = damping_run(dt, taus, eps, vd, 0.2)
+    y2, dp2, t2 = damping_run(dt / 2, taus, eps, vd, 0.2)
+    ex = ode_solution(taus, eps, vd, t1)
+    e1 = np.abs(y1 - ex).max()
+    e2 = np.abs(y2 - ex).max()
+    assert dp1 < 1e-12 and dp2 < 1e-12
+    assert e1 / e2 > 2.5, (e1, e2)
+    assert e1 < 1e-4
+
+
+def test_damping_matches_golden_fixture():
+    with open(os.path.join(GOLDEN, "damping_ode.json")) as f:
+        g = json.load(f)
+    for case in g["cases"]:
+        y, dp, t = damping_run(case["dt"], case["taus"], case["eps"], case["vd"], case["tlim"])
+        exact = np.array(case["exact"])
+        assert abs(t - case["t"]) < 1e-14
+        assert np.abs(y - exact).max() < case["max_err"], (y, exact)
+        assert dp < 1e-12
+
+
+def test_ode_fixture_is_the_ode():
+    with open(os.path.join(GOLDEN, "damping_ode.json")) as f:
+        g = json.load(f)
+    for case in g["cases"]:
+        ex = ode_solution(case["taus"], case["eps"], case["vd"], case["t"])
+        np.testing.assert_allclose(ex, case["exact"], rtol=1e-12, atol=1e-15)
+
+
+def test_random_3d_conservation_multiblock():
+    ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3)
+    st = make_state(ms, [0.01, 0.1, 1.0], [0.5, 0.5, 0.5], 1, seed=3, vd=[0.1, -0.2, 0.3],
+                    gas_noise=1e-2, vel_noise=0.05)
+    o = Oracle(st, dict(scheme=2, drag_solver=2))
+    g0, d0 = o.momentum()
+    tot0 = g0 + d0
+    for _ in range(3):
+        assert o.imex_cycle(2e-3) == 0
+    g1, d1 = o.momentum()
+    scale = np.abs(g0).max() + np.abs(d0).max()
+    assert np.abs((g1 + d1) - tot0).max() < 1e-13 * scale
+    # drag moved momentum between the phases
+    assert np.abs(d1 - d0).max() > 1e-6 * scale
+
+
+def test_pc2_conservation():
+    ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3)
+    st = make_state(ms, [0.01, 0.1], [1.0, 0.5], 1, seed=5, vd=[0.1, -0.2], gas_noise=1e-2,
+                    vel_noise=0.05)
+    o = Oracle(st, dict(scheme=2))
+    g0, d0 = o.momentum()
+    for _ in range(2):
+        err, chi = o.pc2_cycle(2e-3)
+        assert err == 0 and chi > 0.0
+    g1, d1 = o.momentum()
+    scale = np.abs(g0).max() + np.abs(d0).max()
+    assert np.abs((g1 + d1) - (g0 + d0)).max() < 1e-13 * scale
+
+
+def test_nsh_drift_is_steady():
+    om, q, ax = 1.0, 1.5, 0.1
+    taus, eps = [0.01, 0.1, 1.0, 10.0], [0.5] * 4
+    ugx, ugp = nsh_gas(om, q, ax, eps, taus)
+    tot_x, tot_p = ugx, ugp
+    for t, e in zip(taus, eps):
+        vx, vp = nsh_dust(om, q, t, ugx, ugp)
+        # dust steady state: 2 Om vp - (vx - ugx)/t = 0, -(2-q) Om vx - (vp - ugp)/t = 0
+        assert abs(2 * om * vp - (vx - ugx) / t) < 1e-12
+        assert abs(-(2 - q) * om * vx - (vp - ugp) / t) < 1e-12
+        tot_x += e * vx
+        tot_p += e * vp
+    # gas steady state with forcing: total radial momentum zero, 2 Om (u_p + sum e v_p) = -ax
+    assert abs(tot_x) < 1e-12 and abs(2 * om * tot_p + ax) < 1e-12
+
+
+def test_hash_uniform_known_values():
+    # SplitMix64 finaliser of key 0 (the published SplitMix64 output for state 0)
+    z = (0x9E3779B97F4A7C15 ^ (0x9E3779B97F4A7C15 >> 30)) * 0xBF58476D1CE4E5B9 % 2**64
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EB % 2**64
+    z ^= z >> 31
+    assert z == 0xE220A8397B1DCDAF
+    assert hash_uniform01(np.array([0], np.uint64))[0] == (z >> 11) / 2.0**53
+
+
+# ---- independent restatements of the exchanges and the sort ---------------------------
+
+def global_fold(ms, a):
+    """Periodic fold of every cell of (nmb, nvar, n3, n2, n1) arrays onto the global mesh."""
+    nb = ms.nblocks
+    N = [ms.nx[i] * nb[i] for i in range(3)]
+    nvar = a.shape[1]
+    n1, n2, n3 = ms.n
+    g = np.zeros((nvar, N[2], N[1], N[0]))
+    is_, js, ks = ms.starts
+    for m in range(ms.nmb):
+        bi, bj, bk = m % nb[0], (m // nb[0]) % nb[1], m // (nb[0] * nb[1])
+        I = (np.arange(n1) - is_ + bi * ms.nx[0]) % N[0]
+        J = (np.arange(n2) - js + bj * ms.nx[1]) % N[1]
+        K = (np.arange(n3) - ks + bk * ms.nx[2]) % N[2]
+        np.add.at(g, (slice(None), K[:, None, None], J[None, :, None], I[None, None, :]), a[m])
+    return g
+
+
+def global_active(ms, a):
+    nb = ms.nblocks
+    N = [ms.nx[i] * nb[i] for i in range(3)]
+    g = np.zeros((a.shape[1], N[2], N[1], N[0]))
+    act = ms.active(a)
+    for m in range(ms.nmb):
+        bi, bj, bk = m % nb[0], (m // nb[0]) % nb[1], m // (nb[0] * nb[1])
+        g[:, bk * ms.nx[2]:(bk + 1) * ms.nx[2], bj * ms.nx[1]:(bj + 1) * ms.nx[1],
+          bi * ms.nx[0]:(bi + 1) * ms.nx[0]] = act[m]
+    return g
+
+
+@pytest.mark.parametrize("shape", [((16, 16, 16), (8, 8, 8)), ((12, 8, 1), (4, 4, 1)),
+                                   ((8, 8, 8), (8, 4, 8))])
+def test_ghost_add_is_periodic_fold(shape):
+    ms = uniform_mesh(shape[0], shape[1], 2)
+    st = make_state(ms, [0.1], [1.0], 1)
+    o = Oracle(st, dict())
+    rng = np.random.default_rng(0)
+    o.qdep[...] = rng.standard_normal(o.qdep.shape)
+    expect = global_fold(ms, o.qdep)
+    o.ghost_add("qdep", 5)
+    np.testing.assert_allclose(global_active(ms, o.qdep), expect, rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.parametrize("shape", [((16, 16, 16), (8, 8, 8)), ((12, 8, 1), (4, 4, 1))])
+def test_ghost_copy_fills_periodic_images(shape):
+    ms = uniform_mesh(shape[0], shape[1], 2)
+    st = make_state(ms, [0.1], [1.0], 1)
+    o = Oracle(st, dict())
+    rng = np.random.default_rng(1)
+    o.ustar[...] = rng.standard_normal(o.ustar.shape)
+    g = global_active(ms, o.ustar)
+    o.ghost_copy("ustar", 3)
+    nb = ms.nblocks
+    N = [ms.nx[i] * nb[i] for i in range(3)]
+    n1, n2, n3 = ms.n
+    is_, js, ks = ms.starts
+    for m in range(ms.nmb):
+        bi, bj, bk = m % nb[0], (m // nb[0]) % nb[1], m // (nb[0] * nb[1])
+        I = (np.arange(n1) - is_ + bi * ms.nx[0]) % N[0]
+        J = (np.arange(n2) - js + bj * ms.nx[1]) % N[1]
+        K = (np.arange(n3) - ks + bk * ms.nx[2]) % N[2]
+        np.testing.assert_array_equal(o.ustar[m], g[:, K[:, None, None], J[None, :, None], I[None, None, :]])
+
+
+def test_sort_order_is_lexicographic():
+    ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2)
+    st = make_state(ms, [0.1, 1.0], [0.5, 0.5], 2, seed=7)
+    o = Oracle(st, dict())
+    order, keys = o.sort_order()
+    n = st.npart
+    pr, pi = st.pr, st.pi
+    mb = ms.mb_size
+    m = pi[0, :n]
+    i = np.clip(np.floor((pr[0, :n] - mb[m, 0]) / mb[m, 6]).astype(np.int64), 0, 7)
+    j = np.clip(np.floor((pr[2, :n] - mb[m, 1]) / mb[m, 7]).astype(np.int64), 0, 7)
+    k = np.clip(np.floor((pr[4, :n] - mb[m, 2]) / mb[m, 8]).astype(np.int64), 0, 7)
+    key = m.astype(np.int64) * 512 + (k * 8 + j) * 8 + i
+    np.testing.assert_array_equal(keys, key)
+    np.testing.assert_array_equal(order, np.lexsort((np.arange(n), key)))
+    o.sort_particles()
+    np.testing.assert_array_equal(o.st.pi[1, :n], st.pi[1, order])
+
+
+def test_route_keeps_particles_in_their_blocks():
+    ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3)
+    st = make_state(ms, [0.1], [1.0], 2, seed=11, vel_noise=0.5)
+    o = Oracle(st, dict())
+    tags0 = o.st.pi[1, :st.npart].copy()
+    # a push of up to ~0.6 cells moves many particles across block faces and the mesh edge
+    o.register_copy()
+    o.push_imex(1.0, 0.0, 2e-3, 0.0)
+    assert o.route() == 0
+    n = st.npart
+    pr, pi, mb = o.st.pr, o.st.pi, ms.mb_size
+    m = pi[0, :n]
+    for a, (lo, hi) in enumerate(((0, 3), (1, 4), (2, 5))):
+        x = pr[2 * a, :n]
+        assert np.all(x >= mb[m, lo]) and np.all(x < mb[m, hi])
+    np.testing.assert_array_equal(pi[1, :n], tags0)
