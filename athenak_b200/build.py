@@ -21,6 +21,7 @@ UNITS = {
     "dustb_fp64.cu": ["--fmad=false"],
     "dustb_sort.cu": [],
     "dustb_mixed.cu": [],
+    "dustb_seed.cu": [],
 }
 
 

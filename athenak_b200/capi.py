@@ -46,6 +46,14 @@ class DustbCtx(C.Structure):
                 ("phys", DustbPhysics), ("err", C.c_void_p)]
 
 
+class DustbSeedDesc(C.Structure):
+    _fields_ = [("seed", C.c_ulonglong), ("nspecies", C.c_int), ("ppc", C.c_int * 8),
+                ("taus", C.c_double * 8), ("mass", C.c_double * 8), ("vx", C.c_double * 8),
+                ("vy", C.c_double * 8), ("vz", C.c_double * 8), ("vel_noise", C.c_double),
+                ("rho0", C.c_double), ("ug", C.c_double * 3), ("gas_noise", C.c_double),
+                ("nb1", C.c_int), ("nb2", C.c_int), ("nb3", C.c_int)]
+
+
 class DustbImexCoeffs(C.Structure):
     _fields_ = [("gamma", C.c_double), ("dt", C.c_double), ("sh", C.c_double * 2)]
 
@@ -141,6 +149,7 @@ SIGNATURES = {
     "dustb_pc2_commit": [CTXP, D, VP],
     "dustb_imex_cycle": [CTXP, C.POINTER(DustbImexCoeffs), VP, VP],
     "dustb_pc2_cycle": [CTXP, D, VP, VP, VP],
+    "dustb_seed_uniform": [CTXP, C.POINTER(DustbSeedDesc), VP],
 }
 RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_last_error": C.c_char_p}
 

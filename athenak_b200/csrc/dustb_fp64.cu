@@ -765,6 +765,33 @@ int launch_status(const char *what) {
 
 using dustb_host::launch_status;
 
+// launchers of the per-cell FP64 kernels, shared with the mixed-precision form
+namespace dustb_cells {
+void gas_rk(const dustb_ctx *c, double g0, double g1, cudaStream_t st) {
+  Ind d = make_ind(c->mesh);
+  k_gas_rk<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.u1, c->f.nvar_gas, g0, g1);
+}
+void history(const dustb_ctx *c, double atw_dt, cudaStream_t st) {
+  Ind d = make_ind(c->mesh);
+  k_history<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, atw_dt);
+}
+void dc_correct(const dustb_ctx *c, cudaStream_t st) {
+  Ind d = make_ind(c->mesh);
+  k_dc_correct<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, c->f.qdep,
+                                                             c->f.work, c->f.ustar);
+}
+void consistent_gas(const dustb_ctx *c, double a_dt, cudaStream_t st) {
+  Ind d = make_ind(c->mesh);
+  k_consistent_gas<<<blocks_for(n_active(d)), kThreads, 0, st>>>(
+      d, c->f.u0, c->f.nvar_gas, c->f.ustar, c->f.qdep, c->f.dmom, c->f.resid, 1.0 / a_dt);
+}
+void pmbr(const dustb_ctx *c, double a_dt, cudaStream_t st) {
+  Ind d = make_ind(c->mesh);
+  k_pmbr<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, 1.0 / a_dt);
+}
+bool ctx_valid(const dustb_ctx *c) { return ctx_ok(c); }
+}  // namespace dustb_cells
+
 #define CHECK_CTX(c) do { if (!ctx_ok(c)) { return DUSTB_EINVAL; } } while (0)
 #define PGRID(c) blocks_for((c)->part.npart), kThreads, 0, S(stream)
 

@@ -122,11 +122,22 @@ __global__ void k_scan_apply(int *a, long long n, const int *bsum) {
   }
 }
 
+// lanes of a warp with the same key take consecutive slots from one atomic (keys of
+// nearly cell-sorted particles come in runs)
 __global__ void k_fill(const int *key, int npart, int *cursor, int *order) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= npart) return;
-  int slot = atomicAdd(&cursor[key[p]], 1);
-  order[slot] = p;
+  const bool live = p < npart;
+  const unsigned act = __ballot_sync(0xffffffffu, live);
+  if (!live) return;
+  const int k = key[p];
+  const unsigned peers = __match_any_sync(act, k);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  const int rank = __popc(peers & ((1u << lane) - 1u));
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&cursor[k], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  order[base + rank] = p;
 }
 
 // order every cell's run by particle index: insertion sort for short runs, heap sort
@@ -196,21 +207,28 @@ int exclusive_scan(int *a, long long n, int *bsum, cudaStream_t st) {
   return dustb_host::launch_status("exclusive_scan");
 }
 
-// CSR from precomputed keys: key[n] in [0, ncell); cstart must hold ncell + 1 ints and be
-// zero on entry except when counted = true (then cstart[0..ncell) holds the counts).
-int csr_from_keys(const int *key, int n, long long ncell, int *cstart, int *order, void *scratch,
-                  long long bytes, cudaStream_t st) {
-  if (bytes < csr_scratch_bytes(ncell, n)) return DUSTB_ESCRATCH;
-  char *p = (char *)scratch;
-  p += align256(sizeof(int) * (size_t)(n > 0 ? n : 1));   // key slot (unused here)
-  int *cursor = (int *)p; p += align256(sizeof(int) * (size_t)(ncell + 1));
-  int *bsum = (int *)p;
+// CSR from precomputed keys: key[n] in [0, ncell); cstart (ncell + 1 ints) holds the
+// per-cell counts on entry; cursor (ncell + 1 ints) and bsum are scratch.
+int csr_build(const int *key, int n, long long ncell, int *cstart, int *order, int *cursor,
+              int *bsum, bool ordered_runs, cudaStream_t st) {
   int rc = exclusive_scan(cstart, ncell + 1, bsum, st);
   if (rc) return rc;
   cudaMemcpyAsync(cursor, cstart, sizeof(int) * (size_t)(ncell + 1), cudaMemcpyDeviceToDevice, st);
   if (n > 0) k_fill<<<nblk(n), kT, 0, st>>>(key, n, cursor, order);
-  k_sort_runs<<<nblk(ncell), kT, 0, st>>>(cstart, ncell, order);
-  return dustb_host::launch_status("csr_from_keys");
+  if (ordered_runs) k_sort_runs<<<nblk(ncell), kT, 0, st>>>(cstart, ncell, order);
+  return dustb_host::launch_status("csr_build");
+}
+
+long long scan_bsum_ints(long long n) { return (n + kScanTile - 1) / kScanTile + 1; }
+
+int csr_from_keys(const int *key, int n, long long ncell, int *cstart, int *order, void *scratch,
+                  long long bytes, cudaStream_t st) {
+  if (bytes < csr_scratch_bytes(ncell, n)) return DUSTB_ESCRATCH;
+  char *p = (char *)scratch;
+  p += align256(sizeof(int) * (size_t)(n > 0 ? n : 1));   // key slot (dustb_cell_index)
+  int *cursor = (int *)p; p += align256(sizeof(int) * (size_t)(ncell + 1));
+  int *bsum = (int *)p;
+  return csr_build(key, n, ncell, cstart, order, cursor, bsum, true, st);
 }
 
 }  // namespace dustb

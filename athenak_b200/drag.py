@@ -60,6 +60,44 @@ class DeviceDust:
         self.phys = dict(phys)
         self._rebuild_ctx()
 
+    @classmethod
+    def empty(cls, mesh, npart, phys, device="cuda", nspecies=1):
+        """Zeroed device arrays for npart particles (filled by seed_uniform)."""
+        from .inputs import DustState
+        st = DustState(mesh, np.zeros((17, 1)), np.zeros((5, 1), np.int32), 0,
+                       np.zeros((mesh.nmb, 4, 1, 1, 1)), nspecies, [], [])
+        self = cls.__new__(cls)
+        self.lib = capi.load()
+        self.mesh = mesh
+        self.device = torch.device(device)
+        self.npart = int(npart)
+        self.nspecies = nspecies
+        self.stride = int(npart)
+        f64 = dict(dtype=torch.float64, device=self.device)
+        self.t = {
+            "pr": torch.zeros((17, self.stride), **f64),
+            "pi": torch.zeros((5, self.stride), dtype=torch.int32, device=self.device),
+            "u0": torch.zeros(mesh.field_shape(4), **f64),
+            "u1": torch.zeros(mesh.field_shape(4), **f64),
+            "qdep": torch.zeros(mesh.field_shape(5), **f64),
+            "ustar": torch.zeros(mesh.field_shape(3), **f64),
+            "dmom": torch.zeros(mesh.field_shape(3), **f64),
+            "resid": torch.zeros(mesh.field_shape(4), **f64),
+            "work": torch.zeros(mesh.field_shape(3), **f64),
+            "mb_size": torch.from_numpy(np.ascontiguousarray(mesh.mb_size)).to(self.device),
+            "nghbr": torch.from_numpy(np.ascontiguousarray(mesh.nghbr)).to(self.device),
+            "err": torch.zeros(1, dtype=torch.int32, device=self.device),
+            "x3_removed": torch.zeros(2, **f64),
+            "scalar": torch.zeros(2, **f64),
+        }
+        self.phys = dict(phys)
+        self._rebuild_ctx()
+        return self
+
+    def seed_uniform(self, desc, stream=None):
+        rc = self.lib.dustb_seed_uniform(self.pctx, C.byref(desc), _stream_ptr(stream))
+        capi.check(rc, "seed_uniform")
+
     def _rebuild_ctx(self):
         self.ctx = capi.make_ctx(self.mesh, self.t, self.npart, self.stride, self.phys)
         self.pctx = C.byref(self.ctx)

@@ -1,0 +1,120 @@
+"""Host front end of the mixed-precision form (include/dustb.h, dustb_mixed_*).
+
+A MixedDust owns a DeviceDust (the reference-layout FP64 particle rows and mesh fields) and
+the caller-side workspace of the compact particle shadow.  import_() builds the shadow from
+the FP64 rows, imex_cycle() advances it (mesh fields in FP64), export() writes it back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import capi
+from .drag import DeviceDust, GAMMA_DEFAULT, _stream_ptr
+
+KERNELS = ["push", "fill", "deposit_qp", "operator", "kick", "consistent", "cells"]
+
+
+class DustbMixedParams(C.Structure):
+    _fields_ = [("dx", C.c_double * 3), ("rows_per_tile", C.c_int), ("chunk", C.c_int)]
+
+
+_declared = False
+
+
+def _declare(lib):
+    global _declared
+    if _declared:
+        return
+    P = C.POINTER(capi.DustbCtx)
+    MP = C.POINTER(DustbMixedParams)
+    VP, LL = C.c_void_p, C.c_longlong
+    for name, args in {
+        "dustb_mixed_import": [P, MP, VP, LL, VP],
+        "dustb_mixed_export": [P, MP, VP, LL, VP],
+        "dustb_mixed_sort": [P, MP, VP, LL, VP],
+        "dustb_mixed_imex_cycle": [P, MP, VP, LL, C.POINTER(capi.DustbImexCoeffs), VP],
+    }.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    lib.dustb_mixed_workspace_bytes.argtypes = [C.POINTER(capi.DustbMesh), C.c_int]
+    lib.dustb_mixed_workspace_bytes.restype = LL
+    lib.dustb_mixed_timing.argtypes = [C.c_int]
+    lib.dustb_mixed_timing.restype = C.c_int
+    lib.dustb_mixed_kernel_times.argtypes = [VP, VP, C.c_int]
+    lib.dustb_mixed_kernel_times.restype = C.c_int
+    _declared = True
+
+
+class MixedDust:
+    """Mixed-precision drag step over a DeviceDust's reference arrays."""
+
+    def __init__(self, st=None, phys=None, dev: DeviceDust | None = None, rows_per_tile=0,
+                 chunk=0, do_import=True):
+        self.dev = dev if dev is not None else DeviceDust(st, phys)
+        self.lib = self.dev.lib
+        _declare(self.lib)
+        ms = self.dev.mesh
+        self.mp = DustbMixedParams()
+        d = ms.mb_size[0]
+        self.mp.dx[0], self.mp.dx[1], self.mp.dx[2] = float(d[6]), float(d[7]), float(d[8])
+        self.mp.rows_per_tile = rows_per_tile
+        self.mp.chunk = chunk
+        nbytes = int(self.lib.dustb_mixed_workspace_bytes(C.byref(self.dev.ctx.mesh), self.dev.npart))
+        self.ws = torch.empty(nbytes, dtype=torch.uint8, device=self.dev.device)
+        if do_import:
+            self.import_()
+
+    def _ws(self):
+        return self.ws.data_ptr(), self.ws.numel()
+
+    def import_(self, stream=None):
+        p, n = self._ws()
+        capi.check(self.lib.dustb_mixed_import(self.dev.pctx, C.byref(self.mp), p, n,
+                                               _stream_ptr(stream)), "mixed_import")
+
+    def export(self, stream=None):
+        p, n = self._ws()
+        capi.check(self.lib.dustb_mixed_export(self.dev.pctx, C.byref(self.mp), p, n,
+                                               _stream_ptr(stream)), "mixed_export")
+
+    def sort(self, stream=None):
+        p, n = self._ws()
+        capi.check(self.lib.dustb_mixed_sort(self.dev.pctx, C.byref(self.mp), p, n,
+                                             _stream_ptr(stream)), "mixed_sort")
+
+    def imex_cycle(self, dt, gamma=GAMMA_DEFAULT, stream=None):
+        co = capi.DustbImexCoeffs()
+        co.gamma, co.dt = gamma, dt
+        co.sh[0] = co.sh[1] = 0.0
+        p, n = self._ws()
+        capi.check(self.lib.dustb_mixed_imex_cycle(self.dev.pctx, C.byref(self.mp), p, n,
+                                                   C.byref(co), _stream_ptr(stream)),
+                   "mixed_imex_cycle")
+
+    def set_tiles(self, rows_per_tile=0, chunk=0):
+        self.mp.rows_per_tile = rows_per_tile
+        self.mp.chunk = chunk
+
+    # ---- timing ----
+    def timing(self, on: bool):
+        self.lib.dustb_mixed_timing(1 if on else 0)
+
+    def kernel_times(self):
+        ms = (C.c_double * 7)()
+        n = (C.c_int * 7)()
+        self.lib.dustb_mixed_kernel_times(C.cast(ms, C.c_void_p), C.cast(n, C.c_void_p), 7)
+        return {KERNELS[k]: (ms[k], n[k]) for k in range(7)}
+
+    # ---- host views ----
+    def export_velocities(self):
+        self.export()
+        torch.cuda.synchronize()
+        pr = self.dev.host("pr")
+        return pr[1], pr[3], pr[5]
+
+    def error_word(self):
+        return self.dev.error_word()

@@ -1,0 +1,447 @@
+#!/usr/bin/env python
+"""Benchmark of the dust drag step: particle-steps/s, mixed precision vs FP64, on one B200.
+
+Workload (the metric's configuration): uniform 256^3 mesh as 64 MeshBlocks of 64^3 (ng = 2),
+4 species tau_s = {0.01, 0.1, 1, 10}/Omega, epsilon 0.5 each, ppc 4 per species
+(268,435,456 particles), uniform-random positions (seeded hash), NSH-drift velocities plus
+Gaussian 1e-3 c_s noise, gas NSH drift plus 1e-3 uniform noise, imex2+ with dc1, TSC,
+consistent point split, dt from CFL 0.3 on a 40 H periodic box so dt/tau_s spans ~4e-3..4.5.
+A step is one imex2+ cycle (two working stages) of every particle; inputs (~20-46 GB) are far
+larger than L2, so no flush is needed between timed steps.
+
+Arms: --impl ours (default) times the FP64 per-task form and the mixed form on the GPU;
+--impl reference times the CPU oracle port (OpenMP, all host threads) on a bounded sample.
+N > 1 GPUs run independent replicas (the step does not shard across GPUs here).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "dust particle-steps/s (gather+kick+deposit), mixed vs FP64 on 1 B200 at err<=1e-6"
+UNIT = "particle-steps/s"
+GAMMA = 1.707106781186547
+
+# per-kernel algorithmic bytes of the mixed form: (bytes per particle, bytes per cell) of
+# one launch, the minimum each kernel must read and write (4-byte particle words, FP64 cells)
+MIXED_BYTES = {
+    "push": (114.0, 0.0),          # stage 1: 28 read + 52 write; stage 2: 96 read + 52 write
+    "fill": (16.0, 20.0),
+    "deposit_qp": (40.0, 40.0),    # order, cell, offsets, v, t_s, m; Q, P (+ centre mass)
+    "operator": (28.0, 48.0),      # order, cell, offsets, t_s, m; u* in, work out
+    "kick": (64.0, 48.0),          # + v in/out, R out; u* in, dmom out
+    "consistent": (56.0, 0.0),     # cell, t_s, v, R, 3 residuals in; v, R out
+}
+
+
+def config(small: bool):
+    if small:
+        return dict(ncells=(64, 64, 64), nblock=(32, 32, 32), ppc=[1, 1, 1, 1])
+    return dict(ncells=(256, 256, 256), nblock=(64, 64, 64), ppc=[4, 4, 4, 4])
+
+
+def build_workload(small, device="cuda"):
+    import numpy as np
+    from athenak_b200 import capi
+    from athenak_b200.drag import DeviceDust
+    from athenak_b200.inputs import nsh_gas, nsh_dust
+    from athenak_b200.mesh import uniform_mesh
+    cf = config(small)
+    L = 40.0
+    ms = uniform_mesh(cf["ncells"], cf["nblock"], 2, (-L / 2,) * 3, (L / 2,) * 3)
+    taus = [0.01, 0.1, 1.0, 10.0]
+    eps = [0.5] * 4
+    ppc = cf["ppc"]
+    ncell = ms.ncell_active
+    npart = ncell * sum(ppc)
+    om, q, etavk = 1.0, 1.5, 0.05
+    ugx, ugp = nsh_gas(om, q, 2 * om * etavk, eps, taus)
+    phys = dict(scheme=2, drag_solver=2, consistent_gas=True, back_reaction=True)
+    dev = DeviceDust.empty(ms, npart, phys, device=device, nspecies=4)
+    d = capi.DustbSeedDesc()
+    d.seed = 1
+    d.nspecies = 4
+    vol = L ** 3
+    for s in range(4):
+        d.ppc[s] = ppc[s]
+        d.taus[s] = taus[s]
+        d.mass[s] = eps[s] * 1.0 * vol / (ncell * ppc[s])
+        vx, vp = nsh_dust(om, q, taus[s], ugx, ugp)
+        d.vx[s], d.vy[s], d.vz[s] = vx, vp, 0.0
+    d.vel_noise = 1e-3
+    d.rho0 = 1.0
+    d.ug[0], d.ug[1], d.ug[2] = ugx, ugp, 0.0
+    d.gas_noise = 1e-3
+    d.nb1, d.nb2, d.nb3 = ms.nblocks
+    dev.seed_uniform(d)
+    dx = L / cf["ncells"][0]
+    vmax = max(abs(ugx), abs(ugp)) + 3e-3
+    dt = 0.3 * dx / (1.0 + vmax)
+    return dev, ms, dict(npart=npart, ncell=ncell, dt=dt, taus=taus, dx=dx, L=L, **cf)
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def timed_cycles(fn, steps, stream):
+    import torch
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for _ in range(steps):
+        fn()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1) / steps
+
+
+def cpu_baseline(threads=None, cycles=2):
+    """The oracle port (OpenMP, atomics: the reference's Kokkos OpenMP form) on a bounded
+    sample of the workload: one 32^3 MeshBlock (periodic onto itself) with the same species
+    and ppc 16, one warm-up cycle and `cycles` timed cycles."""
+    import numpy as np
+    from athenak_b200.inputs import make_state
+    from athenak_b200.mesh import uniform_mesh
+    from oracle.oracle import Oracle
+    threads = threads or os.cpu_count() or 1
+    L = 40.0 * 32 / 256
+    ms = uniform_mesh((32, 32, 32), (32, 32, 32), 2, (-L / 2,) * 3, (L / 2,) * 3)
+    taus = [0.01, 0.1, 1.0, 10.0]
+    st = make_state(ms, taus, [0.5] * 4, 4, seed=1, shearing_box=True, vel_noise=1e-3,
+                    gas_noise=1e-3)
+    o = Oracle(st, dict(scheme=2, drag_solver=2), threads=threads)
+    dx = L / 32
+    dt = 0.3 * dx / 1.05
+    o.imex_cycle(dt)
+    t = time.perf_counter()
+    for _ in range(cycles):
+        o.imex_cycle(dt)
+    el = time.perf_counter() - t
+    return {"value": st.npart * cycles / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"32^3 cells, 1 MeshBlock periodic, 4 species ppc 16 ({st.npart} particles), "
+                      f"{cycles} imex2+/dc1 cycles after 1 warm-up, FP64, OpenMP atomics"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    cb = cpu_baseline(cycles=min(steps, 3))
+    cf = config(False)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": min(steps, 3), "warmup": 1,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded hash)",
+            "config": {"workload": "uniform 256^3 mesh, 64 MeshBlocks of 64^3, 4 species ppc 4 "
+                                   "each (268,435,456 particles), imex2+/dc1 TSC",
+                       "sample": cb["sample"]},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    from athenak_b200.mixed import MixedDust
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    stream = torch.cuda.current_stream()
+    dev, ms, W = build_workload(args.small)
+    npart, dt = W["npart"], W["dt"]
+    torch.cuda.synchronize()
+    res = {}
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def maxall(x):
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([x], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    # snapshot of the initial state (both forms start from it)
+    pr0, pi0, u00 = dev.t["pr"].clone(), dev.t["pi"].clone(), dev.t["u0"].clone()
+    # ---- mixed form ----
+    mx = MixedDust(dev=dev, do_import=False)
+    mx.import_()
+    if args.tune:
+        best = None
+        for rows in (1, 2):
+            for chunk in (512, 1024, 2048):
+                mx.set_tiles(rows, chunk)
+                try:
+                    t = timed_cycles(lambda: mx.imex_cycle(dt), 1, stream)
+                except RuntimeError:
+                    continue
+                if best is None or t < best[0]:
+                    best = (t, rows, chunk)
+        mx.set_tiles(best[1], best[2])
+        res["tuned"] = {"rows_per_tile": best[1], "chunk": best[2]}
+        dev.t["pr"].copy_(pr0); dev.t["pi"].copy_(pi0); dev.t["u0"].copy_(u00)
+        mx.import_()
+    for _ in range(args.warmup):
+        mx.imex_cycle(dt)
+    barrier()
+    clk = Clocks(int(os.environ.get("LOCAL_RANK", 0)))
+    clk.start()
+    mx.timing(True)
+    ms_mixed = timed_cycles(lambda: mx.imex_cycle(dt), args.steps, stream)
+    ktimes = mx.kernel_times()
+    mx.timing(False)
+    clocks = clk.stop()
+    ms_mixed = maxall(ms_mixed)
+    mx.export()
+    torch.cuda.synchronize()
+    err_mixed = dev.error_word()
+    pr_mixed = dev.t["pr"][[1, 3, 5]].clone()
+    u0_mixed = dev.t["u0"][:, 1:4].clone()
+    mom_mixed = [float(x) for x in sum(dev.momentum())]
+    del mx
+    torch.cuda.empty_cache()
+    # ---- FP64 per-task form from the same initial state ----
+    dev.t["pr"].copy_(pr0); dev.t["pi"].copy_(pi0); dev.t["u0"].copy_(u00)
+    mom0 = [float(x) for x in sum(dev.momentum())]
+    del pr0, pi0
+    torch.cuda.empty_cache()
+    for _ in range(args.warmup):
+        dev.imex_cycle(dt)
+    barrier()
+    ms_fp64 = timed_cycles(lambda: dev.imex_cycle(dt), args.steps, stream)
+    ms_fp64 = maxall(ms_fp64)
+    torch.cuda.synchronize()
+    err_fp64 = dev.error_word()
+    # errors of the mixed result against the FP64 result after the same cycles
+    v64 = dev.t["pr"][[1, 3, 5]]
+    dv = (pr_mixed - v64)
+    vscale = float(v64.abs().max())
+    rel_v_max = float(dv.abs().max()) / vscale
+    rel_v_rms = float(torch.sqrt((dv * dv).mean() / (v64 * v64).mean()))
+    mass = dev.t["pr"][16]
+    pd_mixed = (mass * pr_mixed).sum(dim=1)
+    pd_64 = (mass * v64).sum(dim=1)
+    u64 = dev.t["u0"][:, 1:4]
+    rel_gas = float((u0_mixed - u64).abs().max() / u64.abs().max())
+    mom64 = [float(x) for x in sum(dev.momentum())]
+    ptot = max(abs(x) for x in mom0)
+    dust_p_err = float((pd_mixed - pd_64).abs().max() / pd_64.abs().max())
+    errors = {
+        "velocity_max_rel": rel_v_max, "velocity_rms_rel": rel_v_rms,
+        "dust_momentum_rel": dust_p_err, "gas_momentum_field_max_rel": rel_gas,
+        "total_momentum_change_mixed_rel": max(abs(a - b) for a, b in zip(mom_mixed, mom0)) / ptot,
+        "total_momentum_change_fp64_rel": max(abs(a - b) for a, b in zip(mom64, mom0)) / ptot,
+        "error_words": [err_mixed, err_fp64],
+    }
+    # ---- end to end through the C ABI with host buffers (mixed form) ----
+    e2e = None
+    if not args.no_e2e:
+        e2e = measure_e2e(dev, dt, args, stream)
+    # ---- roofline of the dominant kernel ----
+    meas = {k: v for k, v in ktimes.items() if k in MIXED_BYTES and v[1] > 0}
+    dom = max(meas, key=lambda k: meas[k][0]) if meas else None
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        with open(pk) as f:
+            peaks = json.load(f)
+    peak = peaks.get("hbm_gbs", 6650.0)
+    roof = None
+    if dom:
+        bp, bc = MIXED_BYTES[dom]
+        per_launch = bp * npart + bc * W["ncell"]
+        avg_ms = meas[dom][0] / meas[dom][1]
+        ach = per_launch / (avg_ms * 1e-3) / 1e9
+        tr = load_traffic().get(dom)
+        roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(ach / peak, 3),
+                "traffic": tr, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
+                if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": round(avg_ms, 4)}
+    total_ms = sum(v[0] for v in ktimes.values()) or 1.0
+    shares = {k: {"ms_per_step": round(v[0] / args.steps, 3), "launches_per_step": v[1] / args.steps,
+                  "share": round(v[0] / total_ms, 3)} for k, v in ktimes.items() if v[1]}
+    steps_per_s = npart * world / (ms_mixed * 1e-3)
+    fp64_rate = npart * world / (ms_fp64 * 1e-3)
+    launches_mixed = 44 * args.steps      # kernels of ours per cycle (dc1, consistent split)
+    if rank == 0:
+        cb = None if args.no_cpu else cpu_baseline()
+        line = {
+            "metric": METRIC, "value": steps_per_s, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed (f32 particles/weights/kicks, f64 drag factor, accumulators, gas)",
+            "data": "synthetic (seeded hash)",
+            "config": {"workload": "uniform 256^3 mesh, 64 MeshBlocks of 64^3, 4 species "
+                                   "tau_s={0.01,0.1,1,10}, eps 0.5, ppc 4 each, imex2+/dc1 TSC, "
+                                   "consistent split" if not args.small else "small 64^3 test",
+                       "particles": npart, "cells": W["ncell"], "dt": dt,
+                       "l2": "inputs far larger than L2 (no flush)",
+                       "parallelism": f"replicas x{world}"},
+            "fp64": {"value": fp64_rate, "ms_per_step": ms_fp64,
+                     "form": "per-task FP64 kernels (reference layout, FP64 atomics)"},
+            "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
+            "errors_mixed_vs_fp64": errors,
+            "roofline": roof,
+            "kernels": shares,
+            "clocks": clocks,
+            "gpu_launches": launches_mixed,
+            "cpu_baseline": cb,
+            "e2e": e2e,
+        }
+        if res.get("tuned"):
+            line["config"]["tuned"] = res["tuned"]
+        print(json.dumps(line), flush=True)
+
+
+def measure_e2e(dev, dt, args, stream):
+    """Per step through the C ABI with host (pinned) buffers: the FP64 rows the step reads
+    (X, V, t_s, m, PGID) and u0 copied in, import, one mixed cycle, export, the rows the step
+    writes (X, V, X1, V1, R, PGID) and u0 copied out."""
+    import torch
+    from athenak_b200.mixed import MixedDust
+    n = dev.npart
+    rows_in = [0, 1, 2, 3, 4, 5, 15, 16]
+    rows_out = list(range(15))
+    try:
+        h_pr = torch.empty((17, n), dtype=torch.float64, pin_memory=True)
+        h_pi = torch.empty((1, n), dtype=torch.int32, pin_memory=True)
+        h_u0 = torch.empty_like(dev.t["u0"], device="cpu").pin_memory()
+    except RuntimeError as e:
+        return {"value": None, "unit": UNIT, "note": f"pinned host buffers unavailable: {e}"[:200]}
+    h_pr.copy_(dev.t["pr"])
+    h_pi.copy_(dev.t["pi"][:1])
+    h_u0.copy_(dev.t["u0"])
+    mx = MixedDust(dev=dev, do_import=False)
+    bi = (len(rows_in) * 8 + 4) * n + h_u0.numel() * 8
+    bo = (len(rows_out) * 8 + 4) * n + h_u0.numel() * 8
+    steps = min(args.steps, 3)
+
+    def one():
+        for r in rows_in:
+            dev.t["pr"][r].copy_(h_pr[r], non_blocking=True)
+        dev.t["pi"][0].copy_(h_pi[0], non_blocking=True)
+        dev.t["u0"].copy_(h_u0, non_blocking=True)
+        mx.import_()
+        mx.imex_cycle(dt)
+        mx.export()
+        for r in rows_out:
+            h_pr[r].copy_(dev.t["pr"][r], non_blocking=True)
+        h_pi[0].copy_(dev.t["pi"][0], non_blocking=True)
+        h_u0.copy_(dev.t["u0"], non_blocking=True)
+
+    one()
+    ms = timed_cycles(one, steps, stream)
+    del mx
+    return {"value": n / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bi,
+            "d2h_bytes_per_step": bo, "ms_per_step": ms, "steps": steps,
+            "path": "dustb_mixed_import + dustb_mixed_imex_cycle + dustb_mixed_export, pinned host rows"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="a 64^3 test workload")
+    ap.add_argument("--tune", action="store_true", help="autotune the tile shape first")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    rank = int(os.environ.get("RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -229,6 +229,72 @@ int dustb_imex_cycle(const dustb_ctx *ctx, const dustb_imex_coeffs *c, double *x
 int dustb_pc2_cycle(const dustb_ctx *ctx, double dt, double *chi_max, double *x3_removed,
                     void *stream);
 
+/* ---- mixed-precision form ---------------------------------------------------------------
+ * A compact device shadow of the particles, kept between imports and exports: per particle
+ * a packed cell id (block, k, j, i), FP32 offsets inside the cell, FP32 velocity, velocity
+ * register, register displacement x1 - x (cells), drag rate, stopping time and mass.  The
+ * gas and the deposit fields stay the reference's FP64 arrays of dustb_ctx (per-cell
+ * accumulators, solves and the gas update in FP64); weights, gathers and kicks run in FP32
+ * with the drag factor a/(t_s + a) formed in FP64.  Deposits are accumulated per source
+ * cell in registers, summed into an FP64 shared-memory tile and added to the FP64 field
+ * once per tile cell.  All the workspace is the caller's (dustb_mixed_workspace_bytes).
+ * No reference counterpart: the reference keeps only the FP64 SoA. */
+
+typedef struct dustb_mixed_params {
+  double dx[3];            /* uniform cell size (single-level mesh) */
+  int rows_per_tile;       /* 0: chosen by the library; else rows of nx1 cells per CTA tile */
+  int chunk;               /* 0: default; particles staged per CTA pass (<= 2048) */
+} dustb_mixed_params;
+
+long long dustb_mixed_workspace_bytes(const dustb_mesh *mesh, int npart);
+
+/* Builds the shadow of particles 0..npart-1 of ctx->part (positions, velocities, registers,
+ * rates, t_s, m) and sorts it by cell. */
+int dustb_mixed_import(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
+                       long long ws_bytes, void *stream);
+
+/* Writes X, V, X1, V1, R and PGID of every shadow particle back into its reference row. */
+int dustb_mixed_export(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
+                       long long ws_bytes, void *stream);
+
+/* One imex2+ cycle of the drag step on the shadow (the same task sequence as
+ * dustb_imex_cycle; the FP64 mesh fields of ctx are used and updated). */
+int dustb_mixed_imex_cycle(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
+                           long long ws_bytes, const dustb_imex_coeffs *c, void *stream);
+
+/* Re-sorts the shadow by cell (the SortParticles of the shadow; the reference rows keep
+ * their order, export writes each particle back to its own row). */
+int dustb_mixed_sort(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
+                     long long ws_bytes, void *stream);
+
+/* Kernel timing of the mixed cycle: when enabled, the library records CUDA events around
+ * every fused kernel it launches; dustb_mixed_kernel_times sums their durations (ms) and
+ * launch counts per kernel id since the last reset (it synchronises the events). */
+enum { DUSTB_K_PUSH = 0, DUSTB_K_FILL = 1, DUSTB_K_DEPOSIT_QP = 2, DUSTB_K_OPERATOR = 3,
+       DUSTB_K_KICK = 4, DUSTB_K_CONSISTENT = 5, DUSTB_K_CELLS = 6, DUSTB_K_NKERNELS = 7 };
+int dustb_mixed_timing(int enable);
+int dustb_mixed_kernel_times(double *ms, int *launches, int n);
+
+/* ---- seeded synthetic inputs ----------------------------------------------------------- */
+
+/* Parameters of the seeded uniform-random set-up (the hash placement of
+ * src/pgen/dust_amr/dust_setup.hpp:36-50, :114-118; NSH drift dust_setup.hpp:58-65). */
+typedef struct dustb_seed_desc {
+  unsigned long long seed;
+  int nspecies;                 /* <= 8 */
+  int ppc[8];                   /* particles per cell of each species */
+  double taus[8], mass[8];      /* stopping time and particle mass of each species */
+  double vx[8], vy[8], vz[8];   /* mean velocity of each species */
+  double vel_noise;             /* Gaussian sigma (Box-Muller on two hash draws) */
+  double rho0, ug[3], gas_noise;/* gas density, velocity, uniform noise amplitude */
+  int nb1, nb2, nb3;            /* MeshBlocks per direction (gid = (b3*nb2 + b2)*nb1 + b1) */
+} dustb_seed_desc;
+
+/* Fills particles 0..npart-1 (species blocks in order, tag = index) and the gas u0 (ghosts
+ * included).  A test and benchmark input generator; the reference's problem generators are
+ * the host code's own. */
+int dustb_seed_uniform(const dustb_ctx *ctx, const dustb_seed_desc *desc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

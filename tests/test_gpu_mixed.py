@@ -1,0 +1,145 @@
+"""Mixed-precision form (FP32 offsets/velocities/weights/kicks, FP64 drag factor, per-cell
+accumulators and gas) against the FP64 forms on the same seeded inputs.
+
+Stated tolerance of the mixed form: after a few cycles every particle velocity is within
+1e-5 of the FP64 result relative to the largest velocity, every position within 1e-5 cells,
+the gas momentum field within 1e-5 of its scale; total gas + dust momentum is conserved to
+1e-9 of its scale (the FP32 rounding of the stored velocity increments)."""
+import numpy as np
+import pytest
+
+from athenak_b200.mesh import uniform_mesh
+from athenak_b200.inputs import make_state
+from oracle.oracle import Oracle
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+VTOL = 1e-5
+
+CASES = {
+    "3d_random": dict(mesh=((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3),
+                      st=dict(taus=[0.01, 0.1, 1.0], eps=[0.5, 0.5, 0.5], ppc=2, seed=3,
+                              vd=[0.1, -0.2, 0.3], gas_noise=1e-2, vel_noise=0.05),
+                      phys=dict(scheme=2, drag_solver=2), dt=2e-3),
+    "3d_stiff_64": dict(mesh=((64, 32, 32), (64, 16, 16), 2, (-1.0,) * 3, (1.0,) * 3),
+                        st=dict(taus=[0.001, 0.01, 0.1, 1.0], eps=[0.5] * 4, ppc=2, seed=7,
+                                shearing_box=True, vel_noise=1e-3, gas_noise=1e-3),
+                        phys=dict(scheme=2, drag_solver=2, shearing_box=True), dt=0.01),
+    "2d_lattice": dict(mesh=((32, 32, 1), (16, 16, 1), 2, (-0.5,) * 3, (0.5,) * 3),
+                       st=dict(taus=[0.1, 0.03, 1.0], eps=[0.2, 0.5, 0.3], ppc=1,
+                               placement="lattice", vd=[0.01 / 3, 0.02 / 3, 0.01],
+                               gas_noise=0.0),
+                       phys=dict(scheme=2, drag_solver=2), dt=0.0125),
+    "cic_dc2_plain": dict(mesh=((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3),
+                          st=dict(taus=[0.001, 1.0], eps=[2.0, 0.3], ppc=3, seed=9,
+                                  vel_noise=0.02, gas_noise=1e-2),
+                          phys=dict(scheme=1, drag_solver=3, consistent_gas=False), dt=2e-3),
+}
+
+
+def run_pair(name, cycles=3):
+    from athenak_b200.drag import DeviceDust
+    from athenak_b200.mixed import MixedDust
+    c = CASES[name]
+    ms = uniform_mesh(*c["mesh"])
+    st = make_state(ms, **c["st"])
+    ref = DeviceDust(st, c["phys"])
+    mx = MixedDust(st, c["phys"])
+    p0 = sum(ref.momentum())
+    for _ in range(cycles):
+        ref.imex_cycle(c["dt"])
+        mx.imex_cycle(c["dt"])
+    mx.export()
+    torch.cuda.synchronize()
+    return st, ref, mx, p0, c
+
+
+def check(st, ref, mx, c):
+    assert ref.error_word() == 0 and mx.error_word() == 0
+    a, b = mx.dev.host("pr"), ref.host("pr")
+    vscale = np.abs(b[[1, 3, 5]]).max()
+    for r in (1, 3, 5, 7, 9, 11):
+        assert np.abs(a[r] - b[r]).max() < VTOL * vscale, r
+    ms = st.mesh
+    dx = ms.mb_size[0, 6:9]
+    for r, ax in ((0, 0), (2, 1), (4, 2), (6, 0), (8, 1), (10, 2)):
+        if ax == 2 and not ms.three_d:
+            continue
+        assert np.abs(a[r] - b[r]).max() < VTOL * dx[ax], r
+    np.testing.assert_array_equal(mx.dev.host("pi"), ref.host("pi"))
+    ua, ub = mx.dev.host("u0"), ref.host("u0")
+    for v in range(1, 4):
+        sc = np.abs(ub[:, v]).max()
+        if sc > 0:
+            assert np.abs(ua[:, v] - ub[:, v]).max() < VTOL * sc, v
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_mixed_matches_fp64(name):
+    st, ref, mx, p0, c = run_pair(name)
+    check(st, ref, mx, c)
+
+
+@pytest.mark.parametrize("name", ["3d_random", "2d_lattice", "cic_dc2_plain"])
+def test_mixed_conserves_momentum(name):
+    st, ref, mx, p0, c = run_pair(name, cycles=4)
+    g, d = mx.dev.momentum()
+    scale = np.abs(p0).max()
+    assert np.abs(g + d - p0).max() < 1e-9 * scale
+
+
+def test_mixed_matches_oracle():
+    c = CASES["3d_random"]
+    from athenak_b200.mixed import MixedDust
+    ms = uniform_mesh(*c["mesh"])
+    st = make_state(ms, **c["st"])
+    o = Oracle(st, c["phys"])
+    mx = MixedDust(st, c["phys"])
+    for _ in range(2):
+        assert o.imex_cycle(c["dt"]) == 0
+        mx.imex_cycle(c["dt"])
+    mx.export()
+    torch.cuda.synchronize()
+    a = mx.dev.host("pr")
+    n = st.npart
+    vscale = np.abs(o.st.pr[[1, 3, 5], :n]).max()
+    for r in (1, 3, 5):
+        assert np.abs(a[r] - o.st.pr[r, :n]).max() < VTOL * vscale
+    np.testing.assert_array_equal(mx.dev.host("pi")[0], o.st.pi[0, :n])
+
+
+@pytest.mark.parametrize("rows,chunk", [(1, 64), (2, 128), (4, 2048), (8, 512)])
+def test_tile_shapes_agree(rows, chunk):
+    """The autotuner's knobs (rows per tile, particles per pass) change only the order of
+    the FP32 partial sums."""
+    from athenak_b200.mixed import MixedDust
+    c = CASES["3d_random"]
+    ms = uniform_mesh(*c["mesh"])
+    st = make_state(ms, **c["st"])
+    base = MixedDust(st, c["phys"])
+    alt = MixedDust(st, c["phys"], rows_per_tile=rows, chunk=chunk)
+    for _ in range(2):
+        base.imex_cycle(c["dt"])
+        alt.imex_cycle(c["dt"])
+    base.export(); alt.export()
+    torch.cuda.synchronize()
+    a, b = alt.dev.host("pr"), base.dev.host("pr")
+    vs = np.abs(b[[1, 3, 5]]).max()
+    assert np.abs(a[[1, 3, 5]] - b[[1, 3, 5]]).max() < 1e-6 * vs
+
+
+def test_mixed_sort_keeps_rows():
+    from athenak_b200.mixed import MixedDust
+    c = CASES["3d_random"]
+    ms = uniform_mesh(*c["mesh"])
+    st = make_state(ms, **c["st"])
+    mx = MixedDust(st, c["phys"])
+    mx.imex_cycle(c["dt"])
+    mx.export()
+    torch.cuda.synchronize()
+    before = mx.dev.host("pr").copy()
+    mx.sort()
+    mx.export()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(mx.dev.host("pr"), before)
