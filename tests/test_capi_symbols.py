@@ -17,7 +17,8 @@ def declared():
     for fn in os.listdir(os.path.join(ROOT, "include")):
         if fn.endswith(".h"):
             src = open(os.path.join(ROOT, "include", fn)).read()
-            names |= set(re.findall(r"\b(dustb_[a-z0-9_]+)\s*\(", src))
+            names |= set(re.findall(r"^(?:int|long long|const char \*)\s*(dustb_[a-z0-9_]+)\s*\(",
+                                    src, re.M))
     return names
 
 
