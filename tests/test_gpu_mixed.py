@@ -81,12 +81,24 @@ def test_mixed_matches_fp64(name):
     check(st, ref, mx, c)
 
 
+def absolute_momentum(st):
+    """sum of |m v| over particles + sum of |rho u| V over active cells (per component)"""
+    n = st.npart
+    d = np.array([np.abs(st.pr[16, :n] * st.pr[r, :n]).sum() for r in (1, 3, 5)])
+    g = np.abs(st.mesh.active(st.u0)[:, 1:4]).sum(axis=(0, 2, 3, 4)) * st.mesh.cell_volume()
+    return (d + g).max()
+
+
 @pytest.mark.parametrize("name", ["3d_random", "2d_lattice", "cic_dc2_plain"])
 def test_mixed_conserves_momentum(name):
+    """Gas + dust momentum of the mixed form changes by at most 1e-7 of the absolute
+    momentum: the FP32 rounding of the stencil weights (whose sum is 1 only to FP32
+    precision) and of the stored velocity increments; the FP64 form holds 1e-13."""
     st, ref, mx, p0, c = run_pair(name, cycles=4)
     g, d = mx.dev.momentum()
-    scale = np.abs(p0).max()
-    assert np.abs(g + d - p0).max() < 1e-9 * scale
+    assert np.abs(g + d - p0).max() < 1e-7 * absolute_momentum(st)
+    g, d = ref.momentum()
+    assert np.abs(g + d - p0).max() < 1e-13 * absolute_momentum(st)
 
 
 def test_mixed_matches_oracle():
