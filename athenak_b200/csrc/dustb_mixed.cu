@@ -113,8 +113,8 @@ Geo make_geo(const dustb_ctx *c, const dustb_mixed_params *mp) {
   G.vstride = d.cells();
   G.nghbr = ms.nghbr; G.mb = ms.mb_size;
   for (int a = 0; a < 3; ++a) { G.dx[a] = mp->dx[a]; G.inv_dx[a] = 1.0 / mp->dx[a]; }
+  // cell volume as the reference forms it: dx1 dx2 (dx3 in 3-D), dust_pm.cpp:253-254
   G.vol = mp->dx[0] * mp->dx[1] * (ms.three_d ? mp->dx[2] : 1.0);
-  if (!ms.three_d) G.vol = mp->dx[0] * mp->dx[1] * (ms.x3max - ms.x3min);
   G.scheme = c->phys.scheme;
   return G;
 }
