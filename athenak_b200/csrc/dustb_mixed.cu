@@ -46,7 +46,7 @@ namespace {
 
 constexpr int kT = 256;
 constexpr int kMaxTileThreads = 384;
-constexpr int kNFloat = 17;
+constexpr int kNFloat = 18;
 
 inline unsigned nblk(long long n) {
   long long b = (n + kT - 1) / kT;
@@ -57,12 +57,14 @@ inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 struct MState {
   int *cell, *order, *pid;
   float *ox, *oy, *oz, *vx, *vy, *vz, *ax, *ay, *az, *wx, *wy, *wz, *rx, *ry, *rz, *ts, *m;
+  float *cc;                   // drag factor a/(t_s + a) of the cycle (formed in FP64)
   float *tmp;
   int *cstart, *cursor, *bsum;
 };
 
 struct Geo {
   int nmb, nx1, nx2, nx3, three_d, gids;
+  int l1, l2, l3;              // log2 of nx1, nx2, nx3 when all are powers of two, else -1
   int n1, n2, n3, is, js, ks;
   long long vstride;           // cells of one variable of one block
   const int *nghbr;
@@ -71,6 +73,18 @@ struct Geo {
   int scheme;
   __device__ long long at(int m, int nvar, int v, int k, int j, int i) const {
     return (((long long)m * nvar + v) * vstride) + ((long long)k * n2 + j) * n1 + i;
+  }
+  // the owning block and active cell of block-local cell (k, j, i) of block m, which may
+  // lie one cell outside the block (the same-level neighbour across the face); false if
+  // no block owns it
+  __device__ bool owner(int m, int &k, int &j, int &i, int &mo) const {
+    const int o1 = (i < 0) ? -1 : ((i >= nx1) ? 1 : 0);
+    const int o2 = (j < 0) ? -1 : ((j >= nx2) ? 1 : 0);
+    const int o3 = (k < 0) ? -1 : ((k >= nx3) ? 1 : 0);
+    if ((o1 | o2 | o3) == 0) { mo = m; return true; }
+    mo = nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)] - gids;
+    i -= o1 * nx1; j -= o2 * nx2; k -= o3 * nx3;
+    return mo >= 0 && mo < nmb;
   }
 };
 
@@ -97,7 +111,7 @@ bool carve(const dustb_mesh &ms, int n, void *ws, long long bytes, MState &S, lo
   char *b = (char *)ws;
   S.cell = (int *)(b + o_cell); S.order = (int *)(b + o_order); S.pid = (int *)(b + o_pid);
   float **fp[kNFloat] = {&S.ox, &S.oy, &S.oz, &S.vx, &S.vy, &S.vz, &S.ax, &S.ay, &S.az,
-                         &S.wx, &S.wy, &S.wz, &S.rx, &S.ry, &S.rz, &S.ts, &S.m};
+                         &S.wx, &S.wy, &S.wz, &S.rx, &S.ry, &S.rz, &S.ts, &S.m, &S.cc};
   for (int f = 0; f < kNFloat; ++f) *fp[f] = (float *)(b + o_f[f]);
   S.tmp = (float *)(b + o_tmp);
   S.cstart = (int *)(b + o_cs); S.cursor = (int *)(b + o_cur); S.bsum = (int *)(b + o_bs);
@@ -112,6 +126,9 @@ Geo make_geo(const dustb_ctx *c, const dustb_mixed_params *mp) {
   G.gids = ms.gids; G.n1 = d.n1; G.n2 = d.n2; G.n3 = d.n3; G.is = d.is; G.js = d.js; G.ks = d.ks;
   G.vstride = d.cells();
   G.nghbr = ms.nghbr; G.mb = ms.mb_size;
+  auto lg = [](int n) { int l = 0; while ((1 << l) < n) ++l; return ((1 << l) == n) ? l : -1; };
+  G.l1 = lg(G.nx1); G.l2 = lg(G.nx2); G.l3 = lg(G.nx3);
+  if (G.l1 < 0 || G.l2 < 0 || G.l3 < 0) G.l1 = G.l2 = G.l3 = -1;
   for (int a = 0; a < 3; ++a) { G.dx[a] = mp->dx[a]; G.inv_dx[a] = 1.0 / mp->dx[a]; }
   // cell volume as the reference forms it: dx1 dx2 (dx3 in 3-D), dust_pm.cpp:253-254
   G.vol = mp->dx[0] * mp->dx[1] * (ms.three_d ? mp->dx[2] : 1.0);
@@ -120,6 +137,13 @@ Geo make_geo(const dustb_ctx *c, const dustb_mixed_params *mp) {
 }
 
 __device__ __forceinline__ void decode(const Geo &G, int c, int &m, int &k, int &j, int &i) {
+  if (G.l1 >= 0) {
+    i = c & (G.nx1 - 1); c >>= G.l1;
+    j = c & (G.nx2 - 1); c >>= G.l2;
+    k = c & (G.nx3 - 1);
+    m = c >> G.l3;
+    return;
+  }
   i = c % G.nx1; c /= G.nx1;
   j = c % G.nx2; c /= G.nx2;
   k = c % G.nx3;
@@ -259,7 +283,7 @@ __global__ void __launch_bounds__(kT) k_push(MState S, Geo G, int n, PushArgs P)
       rx = S.rx[p]; ry = S.ry[p]; rz = S.rz[p];
       if (P.res && S.m[p] > 0.0f) {
         // dust_imex_point_consistent_dust of stage 1 (src/dust/dust_pm.cpp:686-696)
-        const double cj = P.a_dt / ((double)S.ts[p] + P.a_dt);
+        const double cj = (double)S.cc[p];
         const long long b = G.at(m, 4, 0, k + G.ks, j + G.js, i + G.is);
         const double d0 = cj * P.res[b], d1 = cj * P.res[b + G.vstride], d2 = cj * P.res[b + 2 * G.vstride];
         vx += (float)d0; vy += (float)d1; vz += (float)d2;
@@ -271,6 +295,8 @@ __global__ void __launch_bounds__(kT) k_push(MState S, Geo G, int n, PushArgs P)
       dx1 = 0.0f; dy1 = 0.0f; dz1 = 0.0f;
       rx = 0.0f; ry = 0.0f; rz = 0.0f;
       S.wx[p] = vx; S.wy[p] = vy; S.wz[p] = vz;
+      // the drag factor of this cycle, a/(t_s + a) (dust_pm.cpp:255), formed in FP64 once
+      S.cc[p] = (float)(P.a_dt / ((double)S.ts[p] + P.a_dt));
     }
     // ExplicitPush imex (src/dust/dust_push.cpp:262-297)
     float fx = 0.0f, fy = 0.0f, fz = 0.0f, xsh = 0.0f;
@@ -336,7 +362,7 @@ __global__ void k_consistent_kick(MState S, Geo G, int n, double a_dt, const dou
   if (p >= n || !(S.m[p] > 0.0f)) return;
   int m, k, j, i;
   decode(G, S.cell[p], m, k, j, i);
-  const double cj = a_dt / ((double)S.ts[p] + a_dt);
+  const double cj = (double)S.cc[p];
   const long long b = G.at(m, 4, 0, k + G.ks, j + G.js, i + G.is);
   const double d0 = cj * res[b], d1 = cj * res[b + G.vstride], d2 = cj * res[b + 2 * G.vstride];
   S.vx[p] += (float)d0; S.vy[p] += (float)d1; S.vz[p] += (float)d2;
@@ -386,13 +412,22 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
   const int CH = T.chunk;
 
   for (int x = threadIdx.x; x <= nct; x += blockDim.x) s_cs[x] = S.cstart[c0 + x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
   if (MODE != MODE_QP) {
-    for (int w = threadIdx.x; w < WN; w += blockDim.x) {
-      const int wi = w % WI, wj = (w / WI) % WJ, wk = w / (WI * WJ);
-      const int kb = G.three_d ? (G.ks + k - 1 + wk) : G.ks;
-      const long long b = G.at(m, 3, 0, kb, G.js + j0 - 1 + wj, G.is - 1 + wi);
-      gw[w] = make_float4((float)T.gfield[b], (float)T.gfield[b + G.vstride],
+    // the tile's u* window; cells beyond the block read the owning neighbour's active cell
+    // (the same-level copy exchange of the ghost cells, folded into the load)
+    for (int row = warp; row < WK * WJ; row += nwarp) {
+      const int wk = row / WJ, wj = row - wk * WJ;
+      for (int wi = lane; wi < WI; wi += 32) {
+        int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
+        float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (G.owner(m, kk, jj, ii, mo)) {
+          const long long b = G.at(mo, 3, 0, G.ks + kk, G.js + jj, G.is + ii);
+          g = make_float4((float)T.gfield[b], (float)T.gfield[b + G.vstride],
                           (float)T.gfield[b + 2 * G.vstride], 0.0f);
+        }
+        gw[row * WI + wi] = g;
+      }
     }
   }
   __syncthreads();
@@ -417,9 +452,11 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
     // (a) per particle: load, [gather, kick], the deposited values into shared memory
     for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
       const int p = S.order[cbase + x];
-      int pm, pk, pj, pii;
-      decode(G, S.cell[p], pm, pk, pj, pii);
-      if (pm != m || pk != k || pj < j0 || pj >= j0 + tj) {
+      const int local = S.cell[p] - c0;      // the tile's cells are consecutive ids
+      int pj, pii;
+      if (G.l1 >= 0) { pj = j0 + (local >> G.l1); pii = local & (nx1 - 1); }
+      else { pj = j0 + local / nx1; pii = local - (pj - j0) * nx1; }
+      if (local < 0 || local >= nct) {
         // not a particle of this tile: the cell index is stale; contribute nothing
         report(T.err, DUSTB_ERR_WINDOW);
         s_f[x] = 0.5f; s_f[CH + x] = 0.5f; s_f[2 * CH + x] = 0.5f;
@@ -428,11 +465,11 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
         continue;
       }
       const float ox = S.ox[p], oy = S.oy[p], oz = S.oz[p];
-      const double cjd = T.a_dt / ((double)S.ts[p] + T.a_dt);
+      const float c32 = S.cc[p];
       const float mass = S.m[p];
       float qv[NC];
       if (MODE == MODE_QP) {
-        const float mc = mass * (float)cjd * inv_vol;
+        const float mc = mass * c32 * inv_vol;
         qv[0] = mc; qv[1] = mc * S.vx[p]; qv[2] = mc * S.vy[p];
         if (NC > 3) qv[NC - 1] = mc * S.vz[p];
       } else {
@@ -456,11 +493,10 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
           }
         }
         if (MODE == MODE_OP) {
-          const float mc = mass * (float)cjd * inv_vol;
+          const float mc = mass * c32 * inv_vol;
           qv[0] = mc * ux; qv[1] = mc * uy; qv[2] = mc * uz;
         } else {
           // GatherKickPMBR (src/dust/dust_pm.cpp:534-563) with the applied velocity change
-          const float c32 = (float)cjd;
           const float vx = S.vx[p], vy = S.vy[p], vz = S.vz[p];
           const float nx_ = vx + c32 * (ux - vx), ny_ = vy + c32 * (uy - vy), nz_ = vz + c32 * (uz - vz);
           const float dvx = nx_ - vx, dvy = ny_ - vy, dvz = nz_ - vz;
@@ -525,14 +561,18 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
       __syncthreads();
     }
   }
-  // (d) the window into the FP64 field
-  for (int x = threadIdx.x; x < NC * WN; x += blockDim.x) {
-    const double v = dw[x];
-    if (v == 0.0) continue;
-    const int q = x / WN, w = x - q * WN;
-    const int wi = w % WI, wj = (w / WI) % WJ, wk = w / (WI * WJ);
-    const int kb = G.three_d ? (G.ks + k - 1 + wk) : G.ks;
-    atomicAdd(&T.dfield[G.at(m, T.dnvar, q, kb, G.js + j0 - 1 + wj, G.is - 1 + wi)], v);
+  // (d) the window into the FP64 field; window cells beyond the block go straight into the
+  // owning neighbour's active cell (the additive ghost exchange folded into the flush)
+  for (int row = warp; row < NC * WK * WJ; row += nwarp) {
+    const int q = row / (WK * WJ), r2 = row - q * (WK * WJ);
+    const int wk = r2 / WJ, wj = r2 - wk * WJ;
+    for (int wi = lane; wi < WI; wi += 32) {
+      const double v = dw[row * WI + wi];
+      if (v == 0.0) continue;
+      int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
+      if (!G.owner(m, kk, jj, ii, mo)) continue;
+      atomicAdd(&T.dfield[G.at(mo, T.dnvar, q, G.ks + kk, G.js + jj, G.is + ii)], v);
+    }
   }
 }
 
@@ -773,30 +813,24 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       T.dfield = c->f.qdep; T.dnvar = 5; T.res = c->f.resid;
       RUN(launch_tile<MODE_QP>(S, G, cf, T, st));
     }
+    // the deposits go straight into the owners' active cells and the gathers read ghost
+    // cells from their owners, so no ghost exchange of qdep, work, dmom or u* is needed
     {
       Scope sc(DUSTB_K_CELLS, st);
-      if (br) RUN(dustb_ghost_add(c, c->f.qdep, 5, st));
       RUN(dustb_solve_ustar(c, st));
     }
     if (br && c->phys.drag_solver >= DUSTB_SOLVER_DC1) {
       const int nsw = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
       for (int w = 0; w < nsw; ++w) {
-        { Scope sc(DUSTB_K_CELLS, st);
-          RUN(dustb_ghost_copy(c, c->f.ustar, 3, 1, st));
-          cudaMemsetAsync(c->f.work, 0, fbytes * 3, st); }
+        cudaMemsetAsync(c->f.work, 0, fbytes * 3, st);
         { Scope sc(DUSTB_K_OPERATOR, st);
           T.gfield = c->f.ustar; T.dfield = c->f.work; T.dnvar = 3;
           RUN(launch_tile<MODE_OP>(S, G, cf, T, st)); }
         { Scope sc(DUSTB_K_CELLS, st);
-          RUN(dustb_ghost_add(c, c->f.work, 3, st));
           dustb_cells::dc_correct(c, st); }
       }
     }
-    {
-      Scope sc(DUSTB_K_CELLS, st);
-      RUN(dustb_ghost_copy(c, c->f.ustar, 3, 1, st));
-      if (br) cudaMemsetAsync(c->f.dmom, 0, fbytes * 3, st);
-    }
+    if (br) cudaMemsetAsync(c->f.dmom, 0, fbytes * 3, st);
     {
       Scope sc(DUSTB_K_KICK, st);
       T.gfield = c->f.ustar; T.dfield = c->f.dmom; T.dnvar = 3; T.deposit = br;
@@ -804,7 +838,6 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     }
     if (br) {
       { Scope sc(DUSTB_K_CELLS, st);
-        RUN(dustb_ghost_add(c, c->f.dmom, 3, st));
         if (cons) dustb_cells::consistent_gas(c, a_dt, st);
         else dustb_cells::pmbr(c, a_dt, st); }
       if (cons && stage == 2 && n > 0) {
@@ -813,10 +846,12 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
         RUN(dustb_host::launch_status("mixed consistent kick"));
       }
     }
-    {
-      Scope sc(DUSTB_K_CELLS, st);
-      RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, st));
-    }
+  }
+  {
+    // the gas tail's ghost exchange of the conserved state, once per cycle (nothing in the
+    // drag step reads u0's ghost cells between the stages)
+    Scope sc(DUSTB_K_CELLS, st);
+    RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, st));
   }
 #undef RUN
   return DUSTB_OK;

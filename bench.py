@@ -349,7 +349,11 @@ def run_ours(args, rank, world):
                   "share": round(v[0] / total_ms, 3)} for k, v in ktimes.items() if v[1]}
     steps_per_s = npart * world / (ms_mixed * 1e-3)
     fp64_rate = npart * world / (ms_fp64 * 1e-3)
-    launches_mixed = 44 * args.steps      # kernels of ours per cycle (dc1, consistent split)
+    # kernels of ours per mixed cycle (dc1, consistent split): per stage gas update, push,
+    # scan (3), fill, run order, Q/P tile, solve, operator tile, correction, kick tile,
+    # consistent gas = 13, stage 2 adds the history term and the consistent kick, and one
+    # ghost exchange of u0 closes the cycle: 13 + 15 + 1
+    launches_mixed = 29 * args.steps
     if rank == 0:
         cb = None if args.no_cpu else cpu_baseline()
         line = {
@@ -431,7 +435,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="a 64^3 test workload")
-    ap.add_argument("--tune", action="store_true", help="autotune the tile shape first")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="skip the tile-shape autotuner (rows per tile, particles per pass)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cells", type=int, default=0,
