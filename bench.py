@@ -246,7 +246,9 @@ def run_ours(args, rank, world):
     mx.import_()
     if args.tune:
         best = None
-        for rows in (1, 2):
+        nx1, nx2 = ms.nx[0], ms.nx[1]
+        cand = [r for r in (1, 2, 4, 8) if nx2 % r == 0 and 3 * r * nx1 <= 384]
+        for rows in cand:
             for chunk in (512, 1024, 2048):
                 mx.set_tiles(rows, chunk)
                 try:
