@@ -88,6 +88,14 @@ struct Geo {
   }
 };
 
+// every FP32 particle array of the shadow, in one place (carving and permuting use it)
+inline void float_arrays(MState &S, float **fp[kNFloat]) {
+  float **all[kNFloat] = {&S.ox, &S.oy, &S.oz, &S.vx, &S.vy, &S.vz, &S.ax, &S.ay, &S.az,
+                          &S.wx, &S.wy, &S.wz, &S.rx, &S.ry, &S.rz, &S.ts, &S.m, &S.cc};
+  static_assert(sizeof(all) / sizeof(all[0]) == kNFloat, "shadow array list");
+  for (int f = 0; f < kNFloat; ++f) fp[f] = all[f];
+}
+
 long long ncell_of(const dustb_mesh &ms) {
   return (long long)ms.nmb * ms.nx1 * (ms.multi_d ? ms.nx2 : 1) * (ms.three_d ? ms.nx3 : 1);
 }
@@ -110,8 +118,8 @@ bool carve(const dustb_mesh &ms, int n, void *ws, long long bytes, MState &S, lo
   if (!ws || bytes < (long long)off) return false;
   char *b = (char *)ws;
   S.cell = (int *)(b + o_cell); S.order = (int *)(b + o_order); S.pid = (int *)(b + o_pid);
-  float **fp[kNFloat] = {&S.ox, &S.oy, &S.oz, &S.vx, &S.vy, &S.vz, &S.ax, &S.ay, &S.az,
-                         &S.wx, &S.wy, &S.wz, &S.rx, &S.ry, &S.rz, &S.ts, &S.m, &S.cc};
+  float **fp[kNFloat];
+  float_arrays(S, fp);
   for (int f = 0; f < kNFloat; ++f) *fp[f] = (float *)(b + o_f[f]);
   S.tmp = (float *)(b + o_tmp);
   S.cstart = (int *)(b + o_cs); S.cursor = (int *)(b + o_cur); S.bsum = (int *)(b + o_bs);
@@ -658,8 +666,14 @@ int permute(const MState &S, int n, cudaStream_t st) {
   cudaMemcpyAsync(S.cell, ti, 4 * (size_t)n, cudaMemcpyDeviceToDevice, st);
   k_gather_i<<<nblk(n), kT, 0, st>>>(S.pid, S.order, n, ti);
   cudaMemcpyAsync(S.pid, ti, 4 * (size_t)n, cudaMemcpyDeviceToDevice, st);
-  float *fs[kNFloat] = {S.ox, S.oy, S.oz, S.vx, S.vy, S.vz, S.ax, S.ay, S.az,
-                        S.wx, S.wy, S.wz, S.rx, S.ry, S.rz, S.ts, S.m};
+  MState T = S;
+  float **fp[kNFloat];
+  float_arrays(T, fp);
+  float *fs[kNFloat];
+  for (int f = 0; f < kNFloat; ++f) {
+    fs[f] = *fp[f];
+    if (!fs[f]) return DUSTB_EINVAL;
+  }
   for (int f = 0; f < kNFloat; ++f) {
     k_gather_f<<<nblk(n), kT, 0, st>>>(fs[f], S.order, n, S.tmp);
     cudaMemcpyAsync(fs[f], S.tmp, 4 * (size_t)n, cudaMemcpyDeviceToDevice, st);
