@@ -174,6 +174,15 @@ __device__ __forceinline__ void wts(int scheme, float o, float w[3]) {
   }
 }
 
+// 4-byte asynchronous global -> shared copy (completion: cp_async_wait_all)
+__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
+}
+
 __device__ __forceinline__ void warp_hist(int *count, int key, bool live) {
   const unsigned act = __ballot_sync(0xffffffffu, live);
   if (!live) return;
@@ -418,6 +427,16 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
   float *s_f = (float *)(smem + off);            // [3 + NC][chunk]
   double *dw = (double *)(smem + off);           // [NC][WN] after the chunks
   const int CH = T.chunk;
+  {
+    const size_t a = (size_t)(3 + NC) * CH * 4, b = (size_t)NC * WN * 8;
+    off += ((a > b ? a : b) + 15) & ~(size_t)15;
+  }
+  // staging of the chunk's particle fields (cp.async gathers through the cell order)
+  int *s_p = (int *)(smem + off);
+  int *s_cell = s_p + CH;
+  float *s_cc = (float *)(s_cell + CH);
+  float *s_m = s_cc + CH;
+  float *s_v = s_m + CH;                         // [3][chunk], Q/P and kick only
 
   for (int x = threadIdx.x; x <= nct; x += blockDim.x) s_cs[x] = S.cstart[c0 + x];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
@@ -457,10 +476,29 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
 
   for (int cbase = P0; cbase < P1; cbase += CH) {
     const int cnt = min(CH, P1 - cbase);
-    // (a) per particle: load, [gather, kick], the deposited values into shared memory
+    // (a0) the chunk's particle ids; (a1) their fields, copied asynchronously into shared
+    // memory so that a thread's gathers are in flight together; (a2) per particle
+    // [gather, kick] and the deposited values.  A thread computes exactly the entries
+    // whose copies it issued, so no barrier separates (a1) and (a2).
+    for (int x = threadIdx.x; x < cnt; x += blockDim.x) s_p[x] = S.order[cbase + x];
     for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
-      const int p = S.order[cbase + x];
-      const int local = S.cell[p] - c0;      // the tile's cells are consecutive ids
+      const int p = s_p[x];
+      cp_async4(&s_cell[x], &S.cell[p]);
+      cp_async4(&s_f[x], &S.ox[p]);
+      cp_async4(&s_f[CH + x], &S.oy[p]);
+      cp_async4(&s_f[2 * CH + x], &S.oz[p]);
+      cp_async4(&s_cc[x], &S.cc[p]);
+      cp_async4(&s_m[x], &S.m[p]);
+      if (MODE != MODE_OP) {
+        cp_async4(&s_v[x], &S.vx[p]);
+        cp_async4(&s_v[CH + x], &S.vy[p]);
+        cp_async4(&s_v[2 * CH + x], &S.vz[p]);
+      }
+    }
+    cp_async_wait_all();
+    for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
+      const int p = s_p[x];
+      const int local = s_cell[x] - c0;      // the tile's cells are consecutive ids
       int pj, pii;
       if (G.l1 >= 0) { pj = j0 + (local >> G.l1); pii = local & (nx1 - 1); }
       else { pj = j0 + local / nx1; pii = local - (pj - j0) * nx1; }
@@ -472,14 +510,14 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
         for (int q = 0; q < NC; ++q) s_f[(3 + q) * CH + x] = 0.0f;
         continue;
       }
-      const float ox = S.ox[p], oy = S.oy[p], oz = S.oz[p];
-      const float c32 = S.cc[p];
-      const float mass = S.m[p];
+      const float ox = s_f[x], oy = s_f[CH + x], oz = s_f[2 * CH + x];
+      const float c32 = s_cc[x];
+      const float mass = s_m[x];
       float qv[NC];
       if (MODE == MODE_QP) {
         const float mc = mass * c32 * inv_vol;
-        qv[0] = mc; qv[1] = mc * S.vx[p]; qv[2] = mc * S.vy[p];
-        if (NC > 3) qv[NC - 1] = mc * S.vz[p];
+        qv[0] = mc; qv[1] = mc * s_v[x]; qv[2] = mc * s_v[CH + x];
+        if (NC > 3) qv[NC - 1] = mc * s_v[2 * CH + x];
       } else {
         float wx_[3], wy_[3], wz_[3];
         wts(G.scheme, ox, wx_); wts(G.scheme, oy, wy_);
@@ -505,7 +543,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
           qv[0] = mc * ux; qv[1] = mc * uy; qv[2] = mc * uz;
         } else {
           // GatherKickPMBR (src/dust/dust_pm.cpp:534-563) with the applied velocity change
-          const float vx = S.vx[p], vy = S.vy[p], vz = S.vz[p];
+          const float vx = s_v[x], vy = s_v[CH + x], vz = s_v[2 * CH + x];
           const float nx_ = vx + c32 * (ux - vx), ny_ = vy + c32 * (uy - vy), nz_ = vz + c32 * (uz - vz);
           const float dvx = nx_ - vx, dvy = ny_ - vy, dvz = nz_ - vz;
           S.vx[p] = nx_; S.vy[p] = ny_; S.vz[p] = nz_;
@@ -591,7 +629,9 @@ size_t tile_smem(int mode, int tj, int nx1, int three_d, int chunk) {
   size_t s = ((size_t)(nct + 1) * 4 + 15) & ~(size_t)15;
   if (mode != MODE_QP) s += (size_t)WN * 16;
   size_t a = (size_t)(3 + NC) * chunk * 4, b = (size_t)NC * WN * 8;
-  return s + (a > b ? a : b);
+  s += ((a > b ? a : b) + 15) & ~(size_t)15;
+  s += (size_t)7 * chunk * 4;                    // staging: id, cell, c, m, v (3)
+  return s;
 }
 
 // ---- kernel timing ------------------------------------------------------------------------
