@@ -174,15 +174,6 @@ __device__ __forceinline__ void wts(int scheme, float o, float w[3]) {
   }
 }
 
-// 4-byte asynchronous global -> shared copy (completion: cp_async_wait_all)
-__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
-}
-
 __device__ __forceinline__ void warp_hist(int *count, int key, bool live) {
   const unsigned act = __ballot_sync(0xffffffffu, live);
   if (!live) return;
@@ -424,19 +415,9 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
   size_t off = ((size_t)(nct + 1) * 4 + 15) & ~(size_t)15;
   float4 *gw = (float4 *)(smem + off);
   if (MODE != MODE_QP) off += (size_t)WN * 16;
-  float *s_f = (float *)(smem + off);            // [3 + NC][chunk]
+  float *s_f = (float *)(smem + off);            // [9 weights + NC values][chunk]
   double *dw = (double *)(smem + off);           // [NC][WN] after the chunks
   const int CH = T.chunk;
-  {
-    const size_t a = (size_t)(3 + NC) * CH * 4, b = (size_t)NC * WN * 8;
-    off += ((a > b ? a : b) + 15) & ~(size_t)15;
-  }
-  // staging of the chunk's particle fields (cp.async gathers through the cell order)
-  int *s_p = (int *)(smem + off);
-  int *s_cell = s_p + CH;
-  float *s_cc = (float *)(s_cell + CH);
-  float *s_m = s_cc + CH;
-  float *s_v = s_m + CH;                         // [3][chunk], Q/P and kick only
 
   for (int x = threadIdx.x; x <= nct; x += blockDim.x) s_cs[x] = S.cstart[c0 + x];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
@@ -476,52 +457,32 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
 
   for (int cbase = P0; cbase < P1; cbase += CH) {
     const int cnt = min(CH, P1 - cbase);
-    // (a0) the chunk's particle ids; (a1) their fields, copied asynchronously into shared
-    // memory so that a thread's gathers are in flight together; (a2) per particle
-    // [gather, kick] and the deposited values.  A thread computes exactly the entries
-    // whose copies it issued, so no barrier separates (a1) and (a2).
-    for (int x = threadIdx.x; x < cnt; x += blockDim.x) s_p[x] = S.order[cbase + x];
+    // (a) per particle: load, the 9 stencil weights, [gather, kick], the deposited values;
+    // weights and values go to shared memory once, for the 3 z-offset threads of the cell
     for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
-      const int p = s_p[x];
-      cp_async4(&s_cell[x], &S.cell[p]);
-      cp_async4(&s_f[x], &S.ox[p]);
-      cp_async4(&s_f[CH + x], &S.oy[p]);
-      cp_async4(&s_f[2 * CH + x], &S.oz[p]);
-      cp_async4(&s_cc[x], &S.cc[p]);
-      cp_async4(&s_m[x], &S.m[p]);
-      if (MODE != MODE_OP) {
-        cp_async4(&s_v[x], &S.vx[p]);
-        cp_async4(&s_v[CH + x], &S.vy[p]);
-        cp_async4(&s_v[2 * CH + x], &S.vz[p]);
-      }
-    }
-    cp_async_wait_all();
-    for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
-      const int p = s_p[x];
-      const int local = s_cell[x] - c0;      // the tile's cells are consecutive ids
+      const int p = S.order[cbase + x];
+      const int local = S.cell[p] - c0;      // the tile's cells are consecutive ids
       int pj, pii;
       if (G.l1 >= 0) { pj = j0 + (local >> G.l1); pii = local & (nx1 - 1); }
       else { pj = j0 + local / nx1; pii = local - (pj - j0) * nx1; }
       if (local < 0 || local >= nct) {
         // not a particle of this tile: the cell index is stale; contribute nothing
         report(T.err, DUSTB_ERR_WINDOW);
-        s_f[x] = 0.5f; s_f[CH + x] = 0.5f; s_f[2 * CH + x] = 0.5f;
 #pragma unroll
-        for (int q = 0; q < NC; ++q) s_f[(3 + q) * CH + x] = 0.0f;
+        for (int q = 0; q < 9 + NC; ++q) s_f[q * CH + x] = 0.0f;
         continue;
       }
-      const float ox = s_f[x], oy = s_f[CH + x], oz = s_f[2 * CH + x];
-      const float c32 = s_cc[x];
-      const float mass = s_m[x];
+      const float c32 = S.cc[p];
+      const float mass = S.m[p];
+      float wx_[3], wy_[3], wz_[3];
+      wts(G.scheme, S.ox[p], wx_); wts(G.scheme, S.oy[p], wy_);
+      if (G.three_d) wts(G.scheme, S.oz[p], wz_); else { wz_[0] = 0.0f; wz_[1] = 1.0f; wz_[2] = 0.0f; }
       float qv[NC];
       if (MODE == MODE_QP) {
         const float mc = mass * c32 * inv_vol;
-        qv[0] = mc; qv[1] = mc * s_v[x]; qv[2] = mc * s_v[CH + x];
-        if (NC > 3) qv[NC - 1] = mc * s_v[2 * CH + x];
+        qv[0] = mc; qv[1] = mc * S.vx[p]; qv[2] = mc * S.vy[p];
+        if (NC > 3) qv[NC - 1] = mc * S.vz[p];
       } else {
-        float wx_[3], wy_[3], wz_[3];
-        wts(G.scheme, ox, wx_); wts(G.scheme, oy, wy_);
-        if (G.three_d) wts(G.scheme, oz, wz_); else { wz_[0] = 0.0f; wz_[1] = 1.0f; wz_[2] = 0.0f; }
         const int jl = pj - j0;
         float ux = 0.0f, uy = 0.0f, uz = 0.0f;
         for (int c = 0; c < 3; ++c) {
@@ -543,7 +504,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
           qv[0] = mc * ux; qv[1] = mc * uy; qv[2] = mc * uz;
         } else {
           // GatherKickPMBR (src/dust/dust_pm.cpp:534-563) with the applied velocity change
-          const float vx = s_v[x], vy = s_v[CH + x], vz = s_v[2 * CH + x];
+          const float vx = S.vx[p], vy = S.vy[p], vz = S.vz[p];
           const float nx_ = vx + c32 * (ux - vx), ny_ = vy + c32 * (uy - vy), nz_ = vz + c32 * (uz - vz);
           const float dvx = nx_ - vx, dvy = ny_ - vy, dvz = nz_ - vz;
           S.vx[p] = nx_; S.vy[p] = ny_; S.vz[p] = nz_;
@@ -552,24 +513,26 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
           qv[0] = fac * dvx; qv[1] = fac * dvy; qv[2] = fac * dvz;
         }
       }
-      s_f[x] = ox; s_f[CH + x] = oy; s_f[2 * CH + x] = oz;
 #pragma unroll
-      for (int q = 0; q < NC; ++q) s_f[(3 + q) * CH + x] = qv[q];
+      for (int a = 0; a < 3; ++a) {
+        s_f[a * CH + x] = wx_[a]; s_f[(3 + a) * CH + x] = wy_[a]; s_f[(6 + a) * CH + x] = wz_[a];
+      }
+#pragma unroll
+      for (int q = 0; q < NC; ++q) s_f[(9 + q) * CH + x] = qv[q];
     }
     __syncthreads();
     // (b) per source cell and z offset: the 9 stencil sums of the cell's particles
     if (T.deposit && cz < WK) {
       const int lo = max(s_cs[cl], cbase) - cbase;
       const int hi = min(s_cs[cl + 1], cbase + cnt) - cbase;
+      const int zrow = (G.three_d ? 6 + cz : 7) * CH;
       for (int r = lo; r < hi; ++r) {
-        float wx_[3], wy_[3];
-        wts(G.scheme, s_f[r], wx_);
-        wts(G.scheme, s_f[CH + r], wy_);
-        float wzc = 1.0f;
-        if (G.three_d) { float wz_[3]; wts(G.scheme, s_f[2 * CH + r], wz_); wzc = wz_[cz]; }
+        const float wx_[3] = {s_f[r], s_f[CH + r], s_f[2 * CH + r]};
+        const float wy_[3] = {s_f[3 * CH + r], s_f[4 * CH + r], s_f[5 * CH + r]};
+        const float wzc = s_f[zrow + r];
         float qv[NC];
 #pragma unroll
-        for (int q = 0; q < NC; ++q) qv[q] = s_f[(3 + q) * CH + r];
+        for (int q = 0; q < NC; ++q) qv[q] = s_f[(9 + q) * CH + r];
         if (MODE == MODE_QP && cz == (G.three_d ? 1 : 0)) qt += qv[0];
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
@@ -628,10 +591,8 @@ size_t tile_smem(int mode, int tj, int nx1, int three_d, int chunk) {
   const int NC = tile_ncomp(mode);
   size_t s = ((size_t)(nct + 1) * 4 + 15) & ~(size_t)15;
   if (mode != MODE_QP) s += (size_t)WN * 16;
-  size_t a = (size_t)(3 + NC) * chunk * 4, b = (size_t)NC * WN * 8;
-  s += ((a > b ? a : b) + 15) & ~(size_t)15;
-  s += (size_t)7 * chunk * 4;                    // staging: id, cell, c, m, v (3)
-  return s;
+  size_t a = (size_t)(9 + NC) * chunk * 4, b = (size_t)NC * WN * 8;
+  return s + (a > b ? a : b);
 }
 
 // ---- kernel timing ------------------------------------------------------------------------
