@@ -396,6 +396,7 @@ __host__ __device__ inline int tile_ncomp(int mode) { return mode == MODE_QP ? 4
 template <int MODE>
 __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, TileArgs T) {
   constexpr int NC = (MODE == MODE_QP) ? 4 : 3;
+  constexpr int B = 4;                           // particles per thread loaded together
   extern __shared__ __align__(16) unsigned char smem[];
   const int nx1 = G.nx1, tj = T.tj;
   const int nct = tj * nx1;                      // source cells of the tile
@@ -410,13 +411,14 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
   const int k = t / T.tpp;
   const int j0 = (t - k * T.tpp) * tj;
   const int c0 = encode(G, m, k, j0, 0);
-  // shared layout: cstart | gather window (float4) | chunk SoA / deposit window
+  // shared layout: cstart | gather window (float4) | deposit window (FP64) | chunk SoA
   int *s_cs = (int *)smem;
   size_t off = ((size_t)(nct + 1) * 4 + 15) & ~(size_t)15;
   float4 *gw = (float4 *)(smem + off);
   if (MODE != MODE_QP) off += (size_t)WN * 16;
+  double *dw = (double *)(smem + off);           // [NC][WN]
+  off += (size_t)NC * WN * 8;
   float *s_f = (float *)(smem + off);            // [9 weights + NC values][chunk]
-  double *dw = (double *)(smem + off);           // [NC][WN] after the chunks
   const int CH = T.chunk;
 
   for (int x = threadIdx.x; x <= nct; x += blockDim.x) s_cs[x] = S.cstart[c0 + x];
@@ -438,91 +440,112 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
       }
     }
   }
+  if (T.deposit)
+    for (int w = threadIdx.x; w < NC * WN; w += blockDim.x) dw[w] = 0.0;
   __syncthreads();
   const int P0 = s_cs[0], P1 = s_cs[nct];
   // thread role in the accumulation: source cell cl, z offset cz
   const int cl = threadIdx.x % nct;
   const int cz = threadIdx.x / nct;              // 0..WK-1
   const int cj_l = cl / nx1, ci_l = cl - cj_l * nx1;
-  float acc[3][3][NC];
-#pragma unroll
-  for (int b = 0; b < 3; ++b)
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int q = 0; q < NC; ++q) acc[b][a][q] = 0.0f;
   float qt = 0.0f;
   const float inv_vol = (float)(1.0 / G.vol);
   const float inv_adt = (float)(1.0 / T.a_dt);
 
   for (int cbase = P0; cbase < P1; cbase += CH) {
     const int cnt = min(CH, P1 - cbase);
-    // (a) per particle: load, the 9 stencil weights, [gather, kick], the deposited values;
-    // weights and values go to shared memory once, for the 3 z-offset threads of the cell
-    for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
-      const int p = S.order[cbase + x];
-      const int local = S.cell[p] - c0;      // the tile's cells are consecutive ids
-      int pj, pii;
-      if (G.l1 >= 0) { pj = j0 + (local >> G.l1); pii = local & (nx1 - 1); }
-      else { pj = j0 + local / nx1; pii = local - (pj - j0) * nx1; }
-      if (local < 0 || local >= nct) {
-        // not a particle of this tile: the cell index is stale; contribute nothing
-        report(T.err, DUSTB_ERR_WINDOW);
+    // (a) per particle: the 9 stencil weights, [gather, kick] and the deposited values into
+    // shared memory (once, for the 3 z-offset threads of the cell); the loads of B particles
+    // per thread are issued together
+    for (int x0 = threadIdx.x; x0 < cnt; x0 += B * blockDim.x) {
+      int pb[B];
 #pragma unroll
-        for (int q = 0; q < 9 + NC; ++q) s_f[q * CH + x] = 0.0f;
-        continue;
+      for (int u = 0; u < B; ++u) pb[u] = S.order[cbase + min(x0 + u * (int)blockDim.x, cnt - 1)];
+      int lc[B];
+      float fo[B][3], fc[B], fmass[B], fv[B][3];
+#pragma unroll
+      for (int u = 0; u < B; ++u) {
+        const int p = pb[u];
+        lc[u] = S.cell[p] - c0;
+        fo[u][0] = S.ox[p]; fo[u][1] = S.oy[p]; fo[u][2] = S.oz[p];
+        fc[u] = S.cc[p]; fmass[u] = S.m[p];
+        if (MODE != MODE_OP) { fv[u][0] = S.vx[p]; fv[u][1] = S.vy[p]; fv[u][2] = S.vz[p]; }
       }
-      const float c32 = S.cc[p];
-      const float mass = S.m[p];
-      float wx_[3], wy_[3], wz_[3];
-      wts(G.scheme, S.ox[p], wx_); wts(G.scheme, S.oy[p], wy_);
-      if (G.three_d) wts(G.scheme, S.oz[p], wz_); else { wz_[0] = 0.0f; wz_[1] = 1.0f; wz_[2] = 0.0f; }
-      float qv[NC];
-      if (MODE == MODE_QP) {
-        const float mc = mass * c32 * inv_vol;
-        qv[0] = mc; qv[1] = mc * S.vx[p]; qv[2] = mc * S.vy[p];
-        if (NC > 3) qv[NC - 1] = mc * S.vz[p];
-      } else {
-        const int jl = pj - j0;
-        float ux = 0.0f, uy = 0.0f, uz = 0.0f;
-        for (int c = 0; c < 3; ++c) {
-          if (!G.three_d && c != 1) continue;
-          const int wk = G.three_d ? c : 0;
-          for (int b = 0; b < 3; ++b) {
-            const float wzy = wz_[c] * wy_[b];
-            const float4 *row = gw + (wk * WJ + jl + b) * WI + pii;
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-              const float w = wzy * wx_[a];
-              const float4 g = row[a];
-              ux += w * g.x; uy += w * g.y; uz += w * g.z;
+      for (int u = 0; u < B; ++u) {
+        const int x = x0 + u * blockDim.x;
+        if (x >= cnt) break;
+        const int local = lc[u];               // the tile's cells are consecutive ids
+        if (local < 0 || local >= nct) {
+          // not a particle of this tile: the cell index is stale; contribute nothing
+          report(T.err, DUSTB_ERR_WINDOW);
+#pragma unroll
+          for (int q = 0; q < 9 + NC; ++q) s_f[q * CH + x] = 0.0f;
+          continue;
+        }
+        int jl, pii;
+        if (G.l1 >= 0) { jl = local >> G.l1; pii = local & (nx1 - 1); }
+        else { jl = local / nx1; pii = local - jl * nx1; }
+        const float c32 = fc[u], mass = fmass[u];
+        float wx_[3], wy_[3], wz_[3];
+        wts(G.scheme, fo[u][0], wx_); wts(G.scheme, fo[u][1], wy_);
+        if (G.three_d) wts(G.scheme, fo[u][2], wz_); else { wz_[0] = 0.0f; wz_[1] = 1.0f; wz_[2] = 0.0f; }
+        float qv[NC];
+        if (MODE == MODE_QP) {
+          const float mc = mass * c32 * inv_vol;
+          qv[0] = mc; qv[1] = mc * fv[u][0]; qv[2] = mc * fv[u][1];
+          if (NC > 3) qv[NC - 1] = mc * fv[u][2];
+        } else {
+          float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            if (!G.three_d && c != 1) continue;
+            const int wk = G.three_d ? c : 0;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+              const float wzy = wz_[c] * wy_[b];
+              const float4 *row = gw + (wk * WJ + jl + b) * WI + pii;
+#pragma unroll
+              for (int a = 0; a < 3; ++a) {
+                const float w = wzy * wx_[a];
+                const float4 g = row[a];
+                ux = fmaf(w, g.x, ux); uy = fmaf(w, g.y, uy); uz = fmaf(w, g.z, uz);
+              }
             }
           }
+          if (MODE == MODE_OP) {
+            const float mc = mass * c32 * inv_vol;
+            qv[0] = mc * ux; qv[1] = mc * uy; qv[2] = mc * uz;
+          } else {
+            // GatherKickPMBR (src/dust/dust_pm.cpp:534-563) with the applied velocity change
+            const float vx = fv[u][0], vy = fv[u][1], vz = fv[u][2];
+            const float nx_ = vx + c32 * (ux - vx), ny_ = vy + c32 * (uy - vy), nz_ = vz + c32 * (uz - vz);
+            const float dvx = nx_ - vx, dvy = ny_ - vy, dvz = nz_ - vz;
+            const int p = pb[u];
+            S.vx[p] = nx_; S.vy[p] = ny_; S.vz[p] = nz_;
+            S.rx[p] = dvx * inv_adt; S.ry[p] = dvy * inv_adt; S.rz[p] = dvz * inv_adt;
+            const float fac = -mass * inv_vol;
+            qv[0] = fac * dvx; qv[1] = fac * dvy; qv[2] = fac * dvz;
+          }
         }
-        if (MODE == MODE_OP) {
-          const float mc = mass * c32 * inv_vol;
-          qv[0] = mc * ux; qv[1] = mc * uy; qv[2] = mc * uz;
-        } else {
-          // GatherKickPMBR (src/dust/dust_pm.cpp:534-563) with the applied velocity change
-          const float vx = S.vx[p], vy = S.vy[p], vz = S.vz[p];
-          const float nx_ = vx + c32 * (ux - vx), ny_ = vy + c32 * (uy - vy), nz_ = vz + c32 * (uz - vz);
-          const float dvx = nx_ - vx, dvy = ny_ - vy, dvz = nz_ - vz;
-          S.vx[p] = nx_; S.vy[p] = ny_; S.vz[p] = nz_;
-          S.rx[p] = dvx * inv_adt; S.ry[p] = dvy * inv_adt; S.rz[p] = dvz * inv_adt;
-          const float fac = -mass * inv_vol;
-          qv[0] = fac * dvx; qv[1] = fac * dvy; qv[2] = fac * dvz;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          s_f[a * CH + x] = wx_[a]; s_f[(3 + a) * CH + x] = wy_[a]; s_f[(6 + a) * CH + x] = wz_[a];
         }
-      }
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        s_f[a * CH + x] = wx_[a]; s_f[(3 + a) * CH + x] = wy_[a]; s_f[(6 + a) * CH + x] = wz_[a];
+        for (int q = 0; q < NC; ++q) s_f[(9 + q) * CH + x] = qv[q];
       }
-#pragma unroll
-      for (int q = 0; q < NC; ++q) s_f[(9 + q) * CH + x] = qv[q];
     }
     __syncthreads();
-    // (b) per source cell and z offset: the 9 stencil sums of the cell's particles
-    if (T.deposit && cz < WK) {
+    if (T.deposit) {
+      // (b) per source cell and z offset: the 9 stencil sums of the cell's particles
+      float acc[3][3][NC];
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int q = 0; q < NC; ++q) acc[b][a][q] = 0.0f;
       const int lo = max(s_cs[cl], cbase) - cbase;
       const int hi = min(s_cs[cl + 1], cbase + cnt) - cbase;
       const int zrow = (G.three_d ? 6 + cz : 7) * CH;
@@ -545,8 +568,19 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
           }
         }
       }
+      // (c) into the FP64 window: 9 passes, one (y, x) offset each; within a pass every
+      // thread writes a different window cell
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const int w = (cz * WJ + cj_l + b) * WI + ci_l + a;
+#pragma unroll
+          for (int q = 0; q < NC; ++q) dw[q * WN + w] += (double)acc[b][a][q];
+          __syncthreads();
+        }
+      }
     }
-    __syncthreads();
   }
   if (MODE == MODE_QP && cz == (G.three_d ? 1 : 0)) {
     // centre mass m c / V of the cell (dust_imex_point_center_mass): only this tile's
@@ -554,22 +588,6 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
     T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj_l, G.is + ci_l)] = (double)qt;
   }
   if (!T.deposit || P1 == P0) return;
-  // (c) the window: 9 passes, one (y, x) offset each; within a pass every thread writes a
-  // different window cell
-  for (int w = threadIdx.x; w < NC * WN; w += blockDim.x) dw[w] = 0.0;
-  __syncthreads();
-#pragma unroll
-  for (int b = 0; b < 3; ++b) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      if (cz < WK) {
-        const int w = (cz * WJ + cj_l + b) * WI + ci_l + a;
-#pragma unroll
-        for (int q = 0; q < NC; ++q) dw[q * WN + w] += (double)acc[b][a][q];
-      }
-      __syncthreads();
-    }
-  }
   // (d) the window into the FP64 field; window cells beyond the block go straight into the
   // owning neighbour's active cell (the additive ghost exchange folded into the flush)
   for (int row = warp; row < NC * WK * WJ; row += nwarp) {
@@ -591,8 +609,9 @@ size_t tile_smem(int mode, int tj, int nx1, int three_d, int chunk) {
   const int NC = tile_ncomp(mode);
   size_t s = ((size_t)(nct + 1) * 4 + 15) & ~(size_t)15;
   if (mode != MODE_QP) s += (size_t)WN * 16;
-  size_t a = (size_t)(9 + NC) * chunk * 4, b = (size_t)NC * WN * 8;
-  return s + (a > b ? a : b);
+  s += (size_t)NC * WN * 8;
+  s += (size_t)(9 + NC) * chunk * 4;
+  return s;
 }
 
 // ---- kernel timing ------------------------------------------------------------------------
