@@ -614,6 +614,176 @@ size_t tile_smem(int mode, int tj, int nx1, int three_d, int chunk) {
   return s;
 }
 
+// One thread per source cell: the thread walks its cell's particles (cell order) straight
+// from global memory, forms the 27 stencil weights and the deposited values of each,
+// accumulates the 27 x NC sums in registers and adds them to the tile's FP64 shared window
+// with shared-memory atomics (native FP64 on this GPU); the window is added to the FP64
+// field once per cell.  Three barriers per tile.
+template <int MODE>
+__global__ void __launch_bounds__(256, 1) k_cellacc(MState S, Geo G, TileArgs T) {
+  constexpr int NC = (MODE == MODE_QP) ? 4 : 3;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nx1 = G.nx1, tj = T.tj;
+  const int nct = tj * nx1;                      // source cells of the tile (= threads)
+  const int WK = G.three_d ? 3 : 1;
+  const int WJ = tj + 2, WI = nx1 + 2;
+  const int WN = WK * WJ * WI;
+  int t = blockIdx.x;
+  const int per_block = G.nx3 * T.tpp;
+  const int m = t / per_block;
+  t -= m * per_block;
+  const int k = t / T.tpp;
+  const int j0 = (t - k * T.tpp) * tj;
+  const int c0 = encode(G, m, k, j0, 0);
+  // shared layout: gather window (float4) | deposit window (FP64)
+  size_t off = 0;
+  float4 *gw = (float4 *)smem;
+  if (MODE != MODE_QP) off += (size_t)WN * 16;
+  double *dw = (double *)(smem + off);           // [NC][WN]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
+  if (MODE != MODE_QP) {
+    for (int row = warp; row < WK * WJ; row += nwarp) {
+      const int wk = row / WJ, wj = row - wk * WJ;
+      for (int wi = lane; wi < WI; wi += 32) {
+        int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
+        float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (G.owner(m, kk, jj, ii, mo)) {
+          const long long b = G.at(mo, 3, 0, G.ks + kk, G.js + jj, G.is + ii);
+          g = make_float4((float)T.gfield[b], (float)T.gfield[b + G.vstride],
+                          (float)T.gfield[b + 2 * G.vstride], 0.0f);
+        }
+        gw[row * WI + wi] = g;
+      }
+    }
+  }
+  if (T.deposit)
+    for (int w = threadIdx.x; w < NC * WN; w += blockDim.x) dw[w] = 0.0;
+  __syncthreads();
+  const int cl = threadIdx.x;                    // the thread's source cell in the tile
+  int jl, il;
+  if (G.l1 >= 0) { jl = cl >> G.l1; il = cl & (nx1 - 1); }
+  else { jl = cl / nx1; il = cl - jl * nx1; }
+  const int lo = S.cstart[c0 + cl], hi = S.cstart[c0 + cl + 1];
+  const float inv_vol = (float)(1.0 / G.vol);
+  const float inv_adt = (float)(1.0 / T.a_dt);
+  float acc[3][3][3][NC];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int q = 0; q < NC; ++q) acc[c][b][a][q] = 0.0f;
+  float qt = 0.0f;
+  for (int r = lo; r < hi; ++r) {
+    const int p = S.order[r];
+    const float c32 = S.cc[p], mass = S.m[p];
+    float wx_[3], wy_[3], wz_[3];
+    wts(G.scheme, S.ox[p], wx_);
+    wts(G.scheme, S.oy[p], wy_);
+    if (G.three_d) wts(G.scheme, S.oz[p], wz_); else { wz_[0] = 0.0f; wz_[1] = 1.0f; wz_[2] = 0.0f; }
+    float qv[NC];
+    if (MODE == MODE_QP) {
+      const float mc = mass * c32 * inv_vol;
+      qt += mc;
+      qv[0] = mc; qv[1] = mc * S.vx[p]; qv[2] = mc * S.vy[p];
+      if (NC > 3) qv[NC - 1] = mc * S.vz[p];
+    } else {
+      float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (!G.three_d && c != 1) continue;
+        const int wk = G.three_d ? c : 0;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          const float wzy = wz_[c] * wy_[b];
+          const float4 *row = gw + (wk * WJ + jl + b) * WI + il;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const float w = wzy * wx_[a];
+            const float4 g = row[a];
+            ux = fmaf(w, g.x, ux); uy = fmaf(w, g.y, uy); uz = fmaf(w, g.z, uz);
+          }
+        }
+      }
+      if (MODE == MODE_OP) {
+        const float mc = mass * c32 * inv_vol;
+        qv[0] = mc * ux; qv[1] = mc * uy; qv[2] = mc * uz;
+      } else {
+        // GatherKickPMBR (src/dust/dust_pm.cpp:534-563) with the applied velocity change
+        const float vx = S.vx[p], vy = S.vy[p], vz = S.vz[p];
+        const float nx_ = vx + c32 * (ux - vx), ny_ = vy + c32 * (uy - vy), nz_ = vz + c32 * (uz - vz);
+        const float dvx = nx_ - vx, dvy = ny_ - vy, dvz = nz_ - vz;
+        S.vx[p] = nx_; S.vy[p] = ny_; S.vz[p] = nz_;
+        S.rx[p] = dvx * inv_adt; S.ry[p] = dvy * inv_adt; S.rz[p] = dvz * inv_adt;
+        const float fac = -mass * inv_vol;
+        qv[0] = fac * dvx; qv[1] = fac * dvy; qv[2] = fac * dvz;
+      }
+    }
+    if (T.deposit) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (!G.three_d && c != 1) continue;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          const float wzy = wz_[c] * wy_[b];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const float w = wzy * wx_[a];
+#pragma unroll
+            for (int q = 0; q < NC; ++q) acc[c][b][a][q] = fmaf(w, qv[q], acc[c][b][a][q]);
+          }
+        }
+      }
+    }
+  }
+  if (MODE == MODE_QP) {
+    // centre mass m c / V of the cell (dust_imex_point_center_mass): only this thread's
+    // particles have this cell as their centre, so it is stored, not added
+    T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + jl, G.is + il)] = (double)qt;
+  }
+  if (!T.deposit) return;
+  if (hi > lo) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (!G.three_d && c != 1) continue;
+      const int wk = G.three_d ? c : 0;
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const int w = (wk * WJ + jl + b) * WI + il + a;
+#pragma unroll
+          for (int q = 0; q < NC; ++q) atomicAdd(&dw[q * WN + w], (double)acc[c][b][a][q]);
+        }
+    }
+  }
+  __syncthreads();
+  // the window into the FP64 field; window cells beyond the block go straight into the
+  // owning neighbour's active cell (the additive ghost exchange folded into the flush)
+  for (int row = warp; row < NC * WK * WJ; row += nwarp) {
+    const int q = row / (WK * WJ), r2 = row - q * (WK * WJ);
+    const int wk = r2 / WJ, wj = r2 - wk * WJ;
+    for (int wi = lane; wi < WI; wi += 32) {
+      const double v = dw[row * WI + wi];
+      if (v == 0.0) continue;
+      int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
+      if (!G.owner(m, kk, jj, ii, mo)) continue;
+      atomicAdd(&T.dfield[G.at(mo, T.dnvar, q, G.ks + kk, G.js + jj, G.is + ii)], v);
+    }
+  }
+}
+
+size_t cellacc_smem(int mode, int tj, int nx1, int three_d) {
+  const int WN = (three_d ? 3 : 1) * (tj + 2) * (nx1 + 2);
+  size_t s = 0;
+  if (mode != MODE_QP) s += (size_t)WN * 16;
+  s += (size_t)tile_ncomp(mode) * WN * 8;
+  return s;
+}
+
+
 // ---- kernel timing ------------------------------------------------------------------------
 struct Timing {
   bool on = false;
@@ -640,19 +810,30 @@ struct Scope {
 };
 
 struct Cfg {
-  int tj, chunk, tpp;
+  int tj, chunk, tpp, variant;
 };
 
 bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   const int nx1 = ms.nx1, nx2 = ms.multi_d ? ms.nx2 : 1;
   const int wk = ms.three_d ? 3 : 1;
+  cf.variant = mp->variant;
   int tj = mp->rows_per_tile;
-  if (tj <= 0) {
-    tj = 1;
-    for (int t = nx2; t >= 1; --t)
-      if (nx2 % t == 0 && wk * t * nx1 <= 384 && t * nx1 <= 128 * (ms.three_d ? 1 : 3)) { tj = t; break; }
+  if (cf.variant == 0) {
+    // one thread per source cell: tiles of up to 256 cells
+    if (tj <= 0) {
+      tj = 1;
+      for (int t = nx2; t >= 1; --t)
+        if (nx2 % t == 0 && t * nx1 <= 256) { tj = t; break; }
+    }
+    if (nx2 % tj != 0 || tj * nx1 > 256) return false;
+  } else {
+    if (tj <= 0) {
+      tj = 1;
+      for (int t = nx2; t >= 1; --t)
+        if (nx2 % t == 0 && wk * t * nx1 <= 384 && t * nx1 <= 128 * (ms.three_d ? 1 : 3)) { tj = t; break; }
+    }
+    if (nx2 % tj != 0 || wk * tj * nx1 > kMaxTileThreads) return false;
   }
-  if (nx2 % tj != 0 || wk * tj * nx1 > kMaxTileThreads) return false;
   cf.tj = tj;
   cf.chunk = mp->chunk > 0 ? mp->chunk : 1024;
   if (cf.chunk > 2048) return false;
@@ -662,15 +843,25 @@ bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
 
 template <int MODE>
 int launch_tile(const MState &S, const Geo &G, const Cfg &cf, TileArgs T, cudaStream_t st) {
+  T.tj = cf.tj; T.chunk = cf.chunk; T.tpp = cf.tpp;
+  const long long tiles = (long long)G.nmb * G.nx3 * cf.tpp;
+  if (cf.variant == 0) {
+    const size_t sm = cellacc_smem(MODE, cf.tj, G.nx1, G.three_d);
+    static size_t configured0 = 0;
+    if (sm > 48 * 1024 && sm > configured0) {
+      cudaFuncSetAttribute(k_cellacc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      configured0 = sm;
+    }
+    k_cellacc<MODE><<<(unsigned)tiles, cf.tj * G.nx1, sm, st>>>(S, G, T);
+    return dustb_host::launch_status("mixed cell tile");
+  }
   const size_t sm = tile_smem(MODE, cf.tj, G.nx1, G.three_d, cf.chunk);
   static size_t configured = 0;
   if (sm > 48 * 1024 && sm > configured) {
     cudaFuncSetAttribute(k_tile<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     configured = sm;
   }
-  T.tj = cf.tj; T.chunk = cf.chunk; T.tpp = cf.tpp;
   const int threads = (G.three_d ? 3 : 1) * cf.tj * G.nx1;
-  const long long tiles = (long long)G.nmb * G.nx3 * cf.tpp;
   k_tile<MODE><<<(unsigned)tiles, threads, sm, st>>>(S, G, T);
   return dustb_host::launch_status("mixed tile");
 }

@@ -18,7 +18,8 @@ KERNELS = ["push", "fill", "deposit_qp", "operator", "kick", "consistent", "cell
 
 
 class DustbMixedParams(C.Structure):
-    _fields_ = [("dx", C.c_double * 3), ("rows_per_tile", C.c_int), ("chunk", C.c_int)]
+    _fields_ = [("dx", C.c_double * 3), ("rows_per_tile", C.c_int), ("chunk", C.c_int),
+                ("variant", C.c_int)]
 
 
 _declared = False
@@ -53,7 +54,7 @@ class MixedDust:
     """Mixed-precision drag step over a DeviceDust's reference arrays."""
 
     def __init__(self, st=None, phys=None, dev: DeviceDust | None = None, rows_per_tile=0,
-                 chunk=0, do_import=True):
+                 chunk=0, do_import=True, variant=0):
         self.dev = dev if dev is not None else DeviceDust(st, phys)
         self.lib = self.dev.lib
         _declare(self.lib)
@@ -63,6 +64,7 @@ class MixedDust:
         self.mp.dx[0], self.mp.dx[1], self.mp.dx[2] = float(d[6]), float(d[7]), float(d[8])
         self.mp.rows_per_tile = rows_per_tile
         self.mp.chunk = chunk
+        self.mp.variant = variant
         nbytes = int(self.lib.dustb_mixed_workspace_bytes(C.byref(self.dev.ctx.mesh), self.dev.npart))
         self.ws = torch.empty(nbytes, dtype=torch.uint8, device=self.dev.device)
         if do_import:
@@ -95,9 +97,11 @@ class MixedDust:
                                                    C.byref(co), _stream_ptr(stream)),
                    "mixed_imex_cycle")
 
-    def set_tiles(self, rows_per_tile=0, chunk=0):
+    def set_tiles(self, rows_per_tile=0, chunk=0, variant=None):
         self.mp.rows_per_tile = rows_per_tile
         self.mp.chunk = chunk
+        if variant is not None:
+            self.mp.variant = variant
 
     # ---- timing ----
     def timing(self, on: bool):

@@ -247,18 +247,22 @@ def run_ours(args, rank, world):
     if args.tune:
         best = None
         nx1, nx2 = ms.nx[0], ms.nx[1]
-        cand = [r for r in (1, 2, 4, 8) if nx2 % r == 0 and 3 * r * nx1 <= 384]
-        for rows in cand:
-            for chunk in (512, 1024, 2048):
-                mx.set_tiles(rows, chunk)
-                try:
-                    t = timed_cycles(lambda: mx.imex_cycle(dt), 1, stream)
-                except RuntimeError:
-                    continue
-                if best is None or t < best[0]:
-                    best = (t, rows, chunk)
-        mx.set_tiles(best[1], best[2])
-        res["tuned"] = {"rows_per_tile": best[1], "chunk": best[2]}
+        # (variant, rows per tile, particles per pass): one thread per source cell with
+        # tiles of up to 256 cells, or the staged tiles of up to 384 threads
+        cands = [(0, r, 0) for r in (1, 2, 4, 8) if nx2 % r == 0 and r * nx1 <= 256]
+        cands += [(1, r, ch) for r in (1, 2) if nx2 % r == 0 and 3 * r * nx1 <= 384
+                  for ch in (1024, 2048)]
+        for var, rows, chunk in cands:
+            mx.set_tiles(rows, chunk, var)
+            try:
+                t = timed_cycles(lambda: mx.imex_cycle(dt), 1, stream)
+            except RuntimeError:
+                continue
+            if best is None or t < best[0]:
+                best = (t, rows, chunk, var)
+        mx.set_tiles(best[1], best[2], best[3])
+        res["tuned"] = {"variant": best[3], "rows_per_tile": best[1], "chunk": best[2],
+                        "cycle_ms": round(best[0], 3)}
         dev.t["pr"].copy_(pr0); dev.t["pi"].copy_(pi0); dev.t["u0"].copy_(u00)
         mx.import_()
     for _ in range(args.warmup):

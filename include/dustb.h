@@ -244,6 +244,8 @@ typedef struct dustb_mixed_params {
   double dx[3];            /* uniform cell size (single-level mesh) */
   int rows_per_tile;       /* 0: chosen by the library; else rows of nx1 cells per CTA tile */
   int chunk;               /* 0: default; particles staged per CTA pass (<= 2048) */
+  int variant;             /* deposit kernels: 0 one thread per source cell (default),
+                              1 particles staged in shared memory per tile */
 } dustb_mixed_params;
 
 long long dustb_mixed_workspace_bytes(const dustb_mesh *mesh, int npart);

@@ -124,16 +124,17 @@ def test_mixed_matches_oracle():
     np.testing.assert_array_equal(mx.dev.host("pi")[0], o.st.pi[0, :n])
 
 
-@pytest.mark.parametrize("rows,chunk", [(1, 64), (2, 128), (4, 2048), (8, 512)])
-def test_tile_shapes_agree(rows, chunk):
-    """The autotuner's knobs (rows per tile, particles per pass) change only the order of
-    the FP32 partial sums."""
+@pytest.mark.parametrize("variant,rows,chunk", [(1, 1, 64), (1, 2, 128), (1, 4, 2048), (1, 8, 512),
+                                                (0, 1, 0), (0, 2, 0), (0, 8, 0)])
+def test_tile_shapes_agree(variant, rows, chunk):
+    """The autotuner's knobs (kernel variant, rows per tile, particles per pass) change only
+    the order of the FP32 partial sums."""
     from athenak_b200.mixed import MixedDust
     c = CASES["3d_random"]
     ms = uniform_mesh(*c["mesh"])
     st = make_state(ms, **c["st"])
     base = MixedDust(st, c["phys"])
-    alt = MixedDust(st, c["phys"], rows_per_tile=rows, chunk=chunk)
+    alt = MixedDust(st, c["phys"], rows_per_tile=rows, chunk=chunk, variant=variant)
     for _ in range(2):
         base.imex_cycle(c["dt"])
         alt.imex_cycle(c["dt"])
