@@ -423,12 +423,14 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
 
   for (int x = threadIdx.x; x <= nct; x += blockDim.x) s_cs[x] = S.cstart[c0 + x];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
+  // threads of this warp (the last warp of a block of 8-cell rows can be partial)
+  const int wlanes = min(32, (int)blockDim.x - 32 * warp);
   if (MODE != MODE_QP) {
     // the tile's u* window; cells beyond the block read the owning neighbour's active cell
     // (the same-level copy exchange of the ghost cells, folded into the load)
     for (int row = warp; row < WK * WJ; row += nwarp) {
       const int wk = row / WJ, wj = row - wk * WJ;
-      for (int wi = lane; wi < WI; wi += 32) {
+      for (int wi = lane; wi < WI; wi += wlanes) {
         int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
         float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (G.owner(m, kk, jj, ii, mo)) {
@@ -593,7 +595,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
   for (int row = warp; row < NC * WK * WJ; row += nwarp) {
     const int q = row / (WK * WJ), r2 = row - q * (WK * WJ);
     const int wk = r2 / WJ, wj = r2 - wk * WJ;
-    for (int wi = lane; wi < WI; wi += 32) {
+    for (int wi = lane; wi < WI; wi += wlanes) {
       const double v = dw[row * WI + wi];
       if (v == 0.0) continue;
       int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
@@ -641,10 +643,12 @@ __global__ void __launch_bounds__(256, 1) k_cellacc(MState S, Geo G, TileArgs T)
   if (MODE != MODE_QP) off += (size_t)WN * 16;
   double *dw = (double *)(smem + off);           // [NC][WN]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
+  // threads of this warp (the last warp of a block of 8-cell rows can be partial)
+  const int wlanes = min(32, (int)blockDim.x - 32 * warp);
   if (MODE != MODE_QP) {
     for (int row = warp; row < WK * WJ; row += nwarp) {
       const int wk = row / WJ, wj = row - wk * WJ;
-      for (int wi = lane; wi < WI; wi += 32) {
+      for (int wi = lane; wi < WI; wi += wlanes) {
         int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
         float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (G.owner(m, kk, jj, ii, mo)) {
@@ -765,7 +769,7 @@ __global__ void __launch_bounds__(256, 1) k_cellacc(MState S, Geo G, TileArgs T)
   for (int row = warp; row < NC * WK * WJ; row += nwarp) {
     const int q = row / (WK * WJ), r2 = row - q * (WK * WJ);
     const int wk = r2 / WJ, wj = r2 - wk * WJ;
-    for (int wi = lane; wi < WI; wi += 32) {
+    for (int wi = lane; wi < WI; wi += wlanes) {
       const double v = dw[row * WI + wi];
       if (v == 0.0) continue;
       int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
