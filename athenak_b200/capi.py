@@ -150,6 +150,7 @@ SIGNATURES = {
     "dustb_imex_cycle": [CTXP, C.POINTER(DustbImexCoeffs), VP, VP],
     "dustb_pc2_cycle": [CTXP, D, VP, VP, VP],
     "dustb_seed_uniform": [CTXP, C.POINTER(DustbSeedDesc), VP],
+    "dustb_cell_index_static": [CTXP, VP, VP, VP],
 }
 RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_last_error": C.c_char_p}
 # declared by athenak_b200.mixed (they take its DustbMixedParams struct)

@@ -77,5 +77,6 @@ __host__ __device__ inline int dir_slot(int o1, int o2, int o3) {
 // host-side error bookkeeping shared by the translation units
 namespace dustb_host {
 void set_error(const char *what, cudaError_t e);
+void set_message(const char *what);
 int launch_status(const char *what);
 }  // namespace dustb_host

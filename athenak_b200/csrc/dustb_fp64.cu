@@ -756,6 +756,7 @@ static char g_err[256] = "";
 void set_error(const char *what, cudaError_t e) {
   snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
 }
+void set_message(const char *what) { snprintf(g_err, sizeof(g_err), "%s", what); }
 int launch_status(const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { set_error(what, e); return DUSTB_ELAUNCH; }

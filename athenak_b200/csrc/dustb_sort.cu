@@ -8,6 +8,7 @@
 // scatter of the particle indices with per-cell cursors, per-cell sort of the (short)
 // index runs.  Every result is deterministic.
 #include <cstdint>
+#include <cstdio>
 
 #include "dustb_common.cuh"
 #include "dustb_sort.cuh"
@@ -283,3 +284,56 @@ int dustb_sort_by_cell(const dustb_ctx *c, double *spare_pr, int *spare_pi, void
 }
 
 }  // extern "C"
+
+// ---- cell index without any allocation ---------------------------------------------------
+// For host codes that cannot allocate device memory at the point of the call (a code whose
+// device memory all comes from its own pool reserved at start-up, or one that must not make
+// the synchronising cudaMalloc/cudaFree calls inside its time step): the scratch of the cell
+// index lives in this file-scope device array instead of a caller buffer.  Every GPU that
+// loads the library holds it until the process exits.
+static __device__ __align__(256) unsigned char g_cell_index_scratch[DUSTB_STATIC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+// the array's device address on each device.  The name g_cell_index_scratch in host code is
+// only a host-side handle, so the address is asked from the runtime, once per device, with
+// that device current.
+void *g_cell_index_scratch_ptr[kMaxDevices] = {nullptr};
+}  // namespace
+
+extern "C" int dustb_cell_index_static(const dustb_ctx *c, int *order, int *cstart,
+                                       void *stream) {
+  if (!c || !order || !cstart) return DUSTB_EINVAL;
+  const dustb_mesh &ms = c->mesh;
+  const long long ncell = (long long)ms.nmb * ms.nx1 * (ms.multi_d ? ms.nx2 : 1) *
+                          (ms.three_d ? ms.nx3 : 1);
+  if (ncell >= (1LL << 31)) return DUSTB_EUNSUP;
+  const long long need = csr_scratch_bytes(ncell, c->part.npart);
+  if (need > (long long)DUSTB_STATIC_SCRATCH_BYTES) {
+    char msg[160];
+    snprintf(msg, sizeof(msg),
+             "dustb_cell_index_static: %lld particles and %lld cells need %lld scratch bytes, "
+             "more than the fixed %lld",
+             (long long)c->part.npart, ncell, need, (long long)DUSTB_STATIC_SCRATCH_BYTES);
+    dustb_host::set_message(msg);
+    return DUSTB_ESCRATCH;
+  }
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { dustb_host::set_error("dustb_cell_index_static: cudaGetDevice", e); return DUSTB_ELAUNCH; }
+  if (dev < 0 || dev >= kMaxDevices) return DUSTB_EUNSUP;
+  if (!g_cell_index_scratch_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_cell_index_scratch);
+    if (e != cudaSuccess || !p) {
+      dustb_host::set_error("dustb_cell_index_static: cudaGetSymbolAddress", e);
+      return DUSTB_ELAUNCH;
+    }
+    g_cell_index_scratch_ptr[dev] = p;
+  }
+  // nothing in the array needs to start at zero: the keys, the cursors and the scan sums are
+  // all written before they are read, and the per-cell counts are kept in the caller's
+  // cstart, which dustb_cell_index clears
+  return dustb_cell_index(c, order, cstart, g_cell_index_scratch_ptr[dev],
+                          (long long)DUSTB_STATIC_SCRATCH_BYTES, stream);
+}

@@ -200,6 +200,27 @@ int dustb_cell_index(const dustb_ctx *ctx, int *order, int *cstart, void *scratc
 int dustb_sort_by_cell(const dustb_ctx *ctx, double *spare_pr, int *spare_pi, void *scratch,
                        long long scratch_bytes, void *stream);
 
+/* Fixed size of the device array behind dustb_cell_index_static. */
+#define DUSTB_STATIC_SCRATCH_BYTES (32ll << 20)
+
+/* dustb_cell_index for callers that cannot allocate device memory when they call it: a host
+ * code whose device memory all comes from its own pool reserved at start-up, or one that
+ * must not make the synchronising cudaMalloc / cudaFree calls inside its time step.  The
+ * outputs are those of dustb_cell_index; the scratch is a file-scope device array of
+ * DUSTB_STATIC_SCRATCH_BYTES (32 MiB), which every GPU that loads the library holds until the
+ * process exits.  No counterpart in the reference (its sort allocates through Kokkos and
+ * thrust).
+ *  - Inputs that need more scratch than the array (4 bytes per particle plus 4 per cell plus
+ *    a little) are rejected with DUSTB_ESCRATCH before anything runs; dustb_last_error()
+ *    names the sizes.
+ *  - The first call on a device looks up the array's device address (cudaGetSymbolAddress,
+ *    with that device current); make that first call before any stream capture.
+ *  - Every call shares the one array: calls that may overlap on the GPU (on different
+ *    streams without ordering between them) race and must not be issued.  Nothing in the
+ *    array needs to start at zero; each call writes what it reads.
+ *  - It calls no cudaMalloc, cudaFree or allocating library routine. */
+int dustb_cell_index_static(const dustb_ctx *ctx, int *order, int *cstart, void *stream);
+
 /* ---- pc2 (src/dust/dust_pm.cpp:109-194, :374-405, :585-602; dust_push.cpp:37-61,
  * :99-247) ---------------------------------------------------------------------------- */
 int dustb_pc2_predictor(const dustb_ctx *ctx, double dt, int rate_dep, void *stream);
