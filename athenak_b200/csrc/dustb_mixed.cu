@@ -1,30 +1,36 @@
 // dustb_mixed.cu -- the mixed-precision form of the imex2+ drag step.
 //
-// Particle shadow (structure of arrays, 4-byte words): packed cell id (block, k, j, i),
-// FP32 offsets inside the cell, velocity, velocity register, register displacement x1 - x
-// in cells, drag rate, stopping time, mass, and the particle's row in the reference SoA.
+// Particle shadow (structure of arrays, 4-byte words, two copies A and B): packed cell id
+// (block, k, j, i), FP32 offsets inside the cell, velocity, velocity register, register
+// displacement x1 - x in cells, drag rate, stopping time, mass, the cycle's drag factor
+// a/(t_s + a) (formed in FP64), and the particle's row in the reference SoA.  The shadow is
+// kept sorted by cell at every stage, so the particles of a tile of cells are one contiguous
+// range, which the Tensor Memory Accelerator copies into shared memory with bulk copies.
 // The mesh fields are the reference's FP64 arrays.
 //
 // One stage (the task order of src/dust/dust_tasks.cpp:56-107):
-//   push      per particle: [stage 2: the stage-1 consistent dust kick], register copy,
-//             the explicit push, the cell/block carry that replaces SetNewPrtclGID, and the
-//             per-cell histogram of the new cells
-//   csr       scan of the histogram and the cell -> particles order (dustb_sort.cu)
-//   deposit   per CTA a tile of rows of cells; every thread owns one source cell and one z
-//             offset, sums the 9 (y, x) stencil weights times the deposited values of its
-//             cell's particles in registers, adds them into an FP64 shared-memory window in 9
-//             conflict-free passes, and the window is added to the FP64 field once per cell
-//             (global FP64 atomics only across tile borders).  Three forms: Q/P + centre mass
-//             (DepositDrag), the dc1 operator gather/deposit (PointOperatorParticles) and
-//             the gather-kick-deposit (GatherKickPMBR), the gathers reading an FP32 copy of the
-//             tile's u* window from shared memory.
-//   cells     the FP64 per-cell solves and exchanges of dustb_fp64.cu
+//   count     per particle: [stage 2: the stage-1 consistent dust kick] and the push of the
+//             position; the new cell and a per-cell histogram
+//   scan      of the histogram: the cell ranges of the new order
+//   move      per particle: the whole push (register copy, velocity, position, the cell carry
+//             that replaces SetNewPrtclGID), written to the particle's slot in the other copy
+//   deposit   per CTA a tile of rows of cells of one plane, one thread per source cell; the
+//             tile's particle range is bulk-copied (one copy per field) into shared memory in
+//             passes; each thread walks its cell's particles: the 27 stencil weights,
+//             [the gather of u* from the 27 cells around its cell, held in registers, the
+//             kick] and the 27 x NC deposits accumulated in registers over all passes.  At the
+//             end the threads of a row combine the x-offset contributions that land on the
+//             same cell (warp shuffles) and add the sums to the FP64 field; cells beyond the
+//             block go straight into the owning neighbour.  Three forms: Q/P + centre mass
+//             (DepositDrag), the dc1 operator (PointOperatorParticles), the
+//             gather-kick-deposit (GatherKickPMBR).
+//   cells     the FP64 per-cell solves of dustb_fp64.cu
 //   kick      [stage 2] the consistent dust kick (stage 1's is folded into stage 2's push)
 // Weights, gathers and kicks are FP32; the drag factor a/(t_s + a) is formed in FP64; every
-// deposit is accumulated into FP64.  The kick deposits the velocity change the particle
-// actually received (v_new - v in FP32), so gas + dust momentum is conserved to the FP64
-// round-off of the accumulation.
+// deposit sum is added into FP64.  The kick deposits the velocity change the particle
+// actually received (v_new - v in FP32).
 #include <cfloat>
+#include <cstdint>
 #include <cstdio>
 #include <vector>
 
@@ -45,8 +51,12 @@ using namespace dustb;
 namespace {
 
 constexpr int kT = 256;
-constexpr int kMaxTileThreads = 384;
-constexpr int kNFloat = 18;
+constexpr int kMaxTileThreads = 256;             // one thread per source cell of a tile
+constexpr int kNF = 18;                          // FP32 arrays per copy
+
+// FP32 array slots of a copy
+enum { F_OX = 0, F_OY, F_OZ, F_VX, F_VY, F_VZ, F_AX, F_AY, F_AZ, F_WX, F_WY, F_WZ,
+       F_RX, F_RY, F_RZ, F_TS, F_M, F_CC };
 
 inline unsigned nblk(long long n) {
   long long b = (n + kT - 1) / kT;
@@ -54,11 +64,14 @@ inline unsigned nblk(long long n) {
 }
 inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+struct PBuf {                    // one copy of the shadow
+  int *cell, *pid;
+  float *f[kNF];
+};
+
 struct MState {
-  int *cell, *order, *pid;
-  float *ox, *oy, *oz, *vx, *vy, *vz, *ax, *ay, *az, *wx, *wy, *wz, *rx, *ry, *rz, *ts, *m;
-  float *cc;                   // drag factor a/(t_s + a) of the cycle (formed in FP64)
-  float *tmp;
+  PBuf A, B;                     // A holds the shadow between cycles
+  int *key;                      // new cell of each particle (count -> move)
   int *cstart, *cursor, *bsum;
 };
 
@@ -88,14 +101,6 @@ struct Geo {
   }
 };
 
-// every FP32 particle array of the shadow, in one place (carving and permuting use it)
-inline void float_arrays(MState &S, float **fp[kNFloat]) {
-  float **all[kNFloat] = {&S.ox, &S.oy, &S.oz, &S.vx, &S.vy, &S.vz, &S.ax, &S.ay, &S.az,
-                          &S.wx, &S.wy, &S.wz, &S.rx, &S.ry, &S.rz, &S.ts, &S.m, &S.cc};
-  static_assert(sizeof(all) / sizeof(all[0]) == kNFloat, "shadow array list");
-  for (int f = 0; f < kNFloat; ++f) fp[f] = all[f];
-}
-
 long long ncell_of(const dustb_mesh &ms) {
   return (long long)ms.nmb * ms.nx1 * (ms.multi_d ? ms.nx2 : 1) * (ms.three_d ? ms.nx3 : 1);
 }
@@ -103,25 +108,25 @@ long long ncell_of(const dustb_mesh &ms) {
 // workspace carving (the same order in every call)
 bool carve(const dustb_mesh &ms, int n, void *ws, long long bytes, MState &S, long long *need) {
   const long long ncell = ncell_of(ms);
-  size_t N = (size_t)(n > 0 ? n : 1);
+  const size_t N = (size_t)(n > 0 ? n : 1);
   size_t off = 0;
-  size_t o_cell = off; off += al256(4 * N);
-  size_t o_order = off; off += al256(4 * N);
-  size_t o_pid = off; off += al256(4 * N);
-  size_t o_f[kNFloat];
-  for (int f = 0; f < kNFloat; ++f) { o_f[f] = off; off += al256(4 * N); }
-  size_t o_tmp = off; off += al256(4 * N);
-  size_t o_cs = off; off += al256(4 * (size_t)(ncell + 1));
-  size_t o_cur = off; off += al256(4 * (size_t)(ncell + 1));
-  size_t o_bs = off; off += al256(4 * (size_t)scan_bsum_ints(ncell + 1));
+  size_t o_buf[2][2 + kNF];
+  for (int b = 0; b < 2; ++b)
+    for (int f = 0; f < 2 + kNF; ++f) { o_buf[b][f] = off; off += al256(4 * N); }
+  const size_t o_key = off; off += al256(4 * N);
+  const size_t o_cs = off; off += al256(4 * (size_t)(ncell + 1));
+  const size_t o_cur = off; off += al256(4 * (size_t)(ncell + 1));
+  const size_t o_bs = off; off += al256(4 * (size_t)scan_bsum_ints(ncell + 1));
   if (need) *need = (long long)off;
   if (!ws || bytes < (long long)off) return false;
   char *b = (char *)ws;
-  S.cell = (int *)(b + o_cell); S.order = (int *)(b + o_order); S.pid = (int *)(b + o_pid);
-  float **fp[kNFloat];
-  float_arrays(S, fp);
-  for (int f = 0; f < kNFloat; ++f) *fp[f] = (float *)(b + o_f[f]);
-  S.tmp = (float *)(b + o_tmp);
+  PBuf *bufs[2] = {&S.A, &S.B};
+  for (int q = 0; q < 2; ++q) {
+    bufs[q]->cell = (int *)(b + o_buf[q][0]);
+    bufs[q]->pid = (int *)(b + o_buf[q][1]);
+    for (int f = 0; f < kNF; ++f) bufs[q]->f[f] = (float *)(b + o_buf[q][2 + f]);
+  }
+  S.key = (int *)(b + o_key);
   S.cstart = (int *)(b + o_cs); S.cursor = (int *)(b + o_cur); S.bsum = (int *)(b + o_bs);
   return true;
 }
@@ -174,95 +179,151 @@ __device__ __forceinline__ void wts(int scheme, float o, float w[3]) {
   }
 }
 
-__device__ __forceinline__ void warp_hist(int *count, int key, bool live) {
-  const unsigned act = __ballot_sync(0xffffffffu, live);
-  if (!live) return;
+// lanes of a warp with the same key take consecutive slots from one atomic add on
+// counter[key]; returns this lane's slot (keys of nearly cell-sorted particles come in runs)
+__device__ __forceinline__ int warp_slot(int *counter, int key, unsigned act) {
   const unsigned peers = __match_any_sync(act, key);
   const int lane = threadIdx.x & 31;
-  if (lane == __ffs(peers) - 1) atomicAdd(&count[key], __popc(peers));
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&counter[key], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+__device__ __forceinline__ void warp_count(int *counter, int key, unsigned act) {
+  const unsigned peers = __match_any_sync(act, key);
+  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counter[key], __popc(peers));
 }
 
-// ---- import / export ------------------------------------------------------------------
-__global__ void k_import(const double *pr, const int *pi, long long stride, int n, MState S,
-                         Geo G, unsigned *err) {
+// ---- Tensor Memory Accelerator bulk copies and their barrier ------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+               ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+               " selp.u32 %0, 1, 0, p;\n}\n"
+               : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+// one contiguous global range into shared memory; both addresses and the size are
+// multiples of 16 bytes (the caller rounds the particle range out to whole 16-byte groups)
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// orders this thread's earlier ordinary shared-memory accesses before later bulk copies
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+// bounded wait for the barrier's phase; false (and the error bit) if it never completes
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned *err) {
+  for (int it = 0; it < (1 << 22); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  report(err, DUSTB_ERR_TIMEOUT);
+  return false;
+}
+
+// ---- import / export / sort ----------------------------------------------------------------
+// the reference rows of particle p into copy B (unsorted) and the histogram of its cells
+__global__ void k_import(const double *pr, const int *pi, long long stride, int n, PBuf B,
+                         int *count, Geo G, unsigned *err) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
-  bool live = p < n;
-  int key = 0;
-  if (live) {
-    auto R = [&](int r) { return pr[(long long)r * stride + p]; };
-    int m = pi[(long long)DUSTB_PGID * stride + p] - G.gids;
-    if (m < 0 || m >= G.nmb) { report(err, DUSTB_ERR_PGID); m = m < 0 ? 0 : G.nmb - 1; }
-    const double *sz = G.mb + (long long)m * 9;
-    const int nx[3] = {G.nx1, G.nx2, G.nx3};
-    const double x[3] = {R(DUSTB_IPX), R(DUSTB_IPY), R(DUSTB_IPZ)};
-    const double x1[3] = {R(DUSTB_IPX1), R(DUSTB_IPY1), R(DUSTB_IPZ1)};
-    int ic[3];
-    float of[3], dd[3];
-    for (int a = 0; a < 3; ++a) {
-      if (a == 2 && !G.three_d) { ic[2] = 0; of[2] = 0.5f; dd[2] = 0.0f; break; }
-      double cell = (x[a] - sz[a]) * ((double)nx[a] / (sz[3 + a] - sz[a]));
-      int ig = (int)(cell + 1.0) - 1;
-      if (ig < 0 || ig >= nx[a]) { report(err, DUSTB_ERR_HALO); ig = ig < 0 ? 0 : nx[a] - 1; }
-      double o = cell - (double)ig;
-      float fo = (float)o;
-      if (!(fo >= 0.0f)) fo = 0.0f;
-      if (fo >= 1.0f) fo = 0.99999994f;
-      ic[a] = ig; of[a] = fo;
-      dd[a] = (float)((x1[a] - x[a]) * G.inv_dx[a]);
-    }
-    key = encode(G, m, ic[2], ic[1], ic[0]);
-    S.cell[p] = key; S.pid[p] = p;
-    S.ox[p] = of[0]; S.oy[p] = of[1]; S.oz[p] = of[2];
-    S.vx[p] = (float)R(DUSTB_IPVX); S.vy[p] = (float)R(DUSTB_IPVY); S.vz[p] = (float)R(DUSTB_IPVZ);
-    S.ax[p] = dd[0]; S.ay[p] = dd[1]; S.az[p] = dd[2];
-    S.wx[p] = (float)R(DUSTB_IPVX1); S.wy[p] = (float)R(DUSTB_IPVY1); S.wz[p] = (float)R(DUSTB_IPVZ1);
-    S.rx[p] = (float)R(DUSTB_IPRX); S.ry[p] = (float)R(DUSTB_IPRY); S.rz[p] = (float)R(DUSTB_IPRZ);
-    S.ts[p] = (float)R(DUSTB_IPTS); S.m[p] = (float)R(DUSTB_IPM);
+  const bool live = p < n;
+  const unsigned act = __ballot_sync(0xffffffffu, live);
+  if (!live) return;
+  auto R = [&](int r) { return pr[(long long)r * stride + p]; };
+  int m = pi[(long long)DUSTB_PGID * stride + p] - G.gids;
+  if (m < 0 || m >= G.nmb) { report(err, DUSTB_ERR_PGID); m = m < 0 ? 0 : G.nmb - 1; }
+  const double *sz = G.mb + (long long)m * 9;
+  const int nx[3] = {G.nx1, G.nx2, G.nx3};
+  const double x[3] = {R(DUSTB_IPX), R(DUSTB_IPY), R(DUSTB_IPZ)};
+  const double x1[3] = {R(DUSTB_IPX1), R(DUSTB_IPY1), R(DUSTB_IPZ1)};
+  int ic[3] = {0, 0, 0};
+  float of[3] = {0.5f, 0.5f, 0.5f}, dd[3] = {0.0f, 0.0f, 0.0f};
+  for (int a = 0; a < (G.three_d ? 3 : 2); ++a) {
+    const double cell = (x[a] - sz[a]) * ((double)nx[a] / (sz[3 + a] - sz[a]));
+    int ig = (int)(cell + 1.0) - 1;
+    if (ig < 0 || ig >= nx[a]) { report(err, DUSTB_ERR_HALO); ig = ig < 0 ? 0 : nx[a] - 1; }
+    float fo = (float)(cell - (double)ig);
+    if (!(fo >= 0.0f)) fo = 0.0f;
+    if (fo >= 1.0f) fo = 0.99999994f;
+    ic[a] = ig; of[a] = fo;
+    dd[a] = (float)((x1[a] - x[a]) * G.inv_dx[a]);
   }
-  warp_hist(S.cstart, key, live);
+  const int key = encode(G, m, ic[2], ic[1], ic[0]);
+  B.cell[p] = key; B.pid[p] = p;
+  B.f[F_OX][p] = of[0]; B.f[F_OY][p] = of[1]; B.f[F_OZ][p] = of[2];
+  B.f[F_VX][p] = (float)R(DUSTB_IPVX); B.f[F_VY][p] = (float)R(DUSTB_IPVY); B.f[F_VZ][p] = (float)R(DUSTB_IPVZ);
+  B.f[F_AX][p] = dd[0]; B.f[F_AY][p] = dd[1]; B.f[F_AZ][p] = dd[2];
+  B.f[F_WX][p] = (float)R(DUSTB_IPVX1); B.f[F_WY][p] = (float)R(DUSTB_IPVY1); B.f[F_WZ][p] = (float)R(DUSTB_IPVZ1);
+  B.f[F_RX][p] = (float)R(DUSTB_IPRX); B.f[F_RY][p] = (float)R(DUSTB_IPRY); B.f[F_RZ][p] = (float)R(DUSTB_IPRZ);
+  B.f[F_TS][p] = (float)R(DUSTB_IPTS); B.f[F_M][p] = (float)R(DUSTB_IPM);
+  B.f[F_CC][p] = 0.0f;
+  warp_count(count, key, act);
 }
 
-__global__ void k_export(double *pr, int *pi, long long stride, int n, MState S, Geo G) {
+__global__ void k_hist(const int *cell, int n, int *count) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = p < n;
+  const unsigned act = __ballot_sync(0xffffffffu, live);
+  if (live) warp_count(count, cell[p], act);
+}
+
+// every particle of src into its slot of dst (cells as they are): the sort of the shadow
+__global__ void k_sortmove(PBuf src, PBuf dst, int n, int *cursor) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = p < n;
+  const unsigned act = __ballot_sync(0xffffffffu, live);
+  if (!live) return;
+  const int key = src.cell[p];
+  const int q = warp_slot(cursor, key, act);
+  dst.cell[q] = key; dst.pid[q] = src.pid[p];
+#pragma unroll
+  for (int f = 0; f < kNF; ++f) dst.f[f][q] = src.f[f][p];
+}
+
+__global__ void k_export(double *pr, int *pi, long long stride, int n, PBuf A, Geo G) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   int m, k, j, i;
-  decode(G, S.cell[q], m, k, j, i);
-  const int p = S.pid[q];
+  decode(G, A.cell[q], m, k, j, i);
+  const int p = A.pid[q];
   auto W = [&](int r, double v) { pr[(long long)r * stride + p] = v; };
   const double *sz = G.mb + (long long)m * 9;
-  const double x = sz[X1MIN] + ((double)i + (double)S.ox[q]) * G.dx[0];
-  const double y = sz[X2MIN] + ((double)j + (double)S.oy[q]) * G.dx[1];
+  const double x = sz[X1MIN] + ((double)i + (double)A.f[F_OX][q]) * G.dx[0];
+  const double y = sz[X2MIN] + ((double)j + (double)A.f[F_OY][q]) * G.dx[1];
   W(DUSTB_IPX, x); W(DUSTB_IPY, y);
-  W(DUSTB_IPX1, x + (double)S.ax[q] * G.dx[0]);
-  W(DUSTB_IPY1, y + (double)S.ay[q] * G.dx[1]);
+  W(DUSTB_IPX1, x + (double)A.f[F_AX][q] * G.dx[0]);
+  W(DUSTB_IPY1, y + (double)A.f[F_AY][q] * G.dx[1]);
   if (G.three_d) {
-    const double z = sz[X3MIN] + ((double)k + (double)S.oz[q]) * G.dx[2];
+    const double z = sz[X3MIN] + ((double)k + (double)A.f[F_OZ][q]) * G.dx[2];
     W(DUSTB_IPZ, z);
-    W(DUSTB_IPZ1, z + (double)S.az[q] * G.dx[2]);
+    W(DUSTB_IPZ1, z + (double)A.f[F_AZ][q] * G.dx[2]);
   }
-  W(DUSTB_IPVX, S.vx[q]); W(DUSTB_IPVY, S.vy[q]); W(DUSTB_IPVZ, S.vz[q]);
-  W(DUSTB_IPVX1, S.wx[q]); W(DUSTB_IPVY1, S.wy[q]); W(DUSTB_IPVZ1, S.wz[q]);
-  W(DUSTB_IPRX, S.rx[q]); W(DUSTB_IPRY, S.ry[q]); W(DUSTB_IPRZ, S.rz[q]);
+  W(DUSTB_IPVX, A.f[F_VX][q]); W(DUSTB_IPVY, A.f[F_VY][q]); W(DUSTB_IPVZ, A.f[F_VZ][q]);
+  W(DUSTB_IPVX1, A.f[F_WX][q]); W(DUSTB_IPVY1, A.f[F_WY][q]); W(DUSTB_IPVZ1, A.f[F_WZ][q]);
+  W(DUSTB_IPRX, A.f[F_RX][q]); W(DUSTB_IPRY, A.f[F_RY][q]); W(DUSTB_IPRZ, A.f[F_RZ][q]);
   pi[(long long)DUSTB_PGID * stride + p] = m + G.gids;
 }
 
-// histogram of the current cells (sort)
-__global__ void k_hist(const int *cell, int n, int *count) {
+__global__ void k_copy_buf(PBuf src, PBuf dst, int n) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
-  bool live = p < n;
-  warp_hist(count, live ? cell[p] : 0, live);
+  if (p >= n) return;
+  dst.cell[p] = src.cell[p]; dst.pid[p] = src.pid[p];
+#pragma unroll
+  for (int f = 0; f < kNF; ++f) dst.f[f][p] = src.f[f][p];
 }
 
-__global__ void k_gather_i(const int *src, const int *order, int n, int *dst) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) dst[q] = src[order[q]];
-}
-__global__ void k_gather_f(const float *src, const int *order, int n, float *dst) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) dst[q] = src[order[q]];
-}
-
-// ---- push + carry + histogram ----------------------------------------------------------
+// ---- push: count and move ------------------------------------------------------------------
 struct PushArgs {
   float gam0, gam1, atw_dt;
   float bdt;                  // beta*dt (velocity kick)
@@ -275,114 +336,169 @@ struct PushArgs {
   unsigned *err;
 };
 
-__global__ void __launch_bounds__(kT) k_push(MState S, Geo G, int n, PushArgs P) {
+// dust_imex_point_consistent_dust of stage 1 (src/dust/dust_pm.cpp:686-696): the velocity
+// change of the particle (c times the FP64 residual of its cell), explicitly rounded so that
+// the count and the move kernel form bit-identical results
+__device__ __forceinline__ void consistent_dv(const Geo &G, const PushArgs &P, float cc,
+                                              int m, int k, int j, int i, double d[3]) {
+  const long long b = G.at(m, 4, 0, k + G.ks, j + G.js, i + G.is);
+  const double cj = (double)cc;
+  d[0] = __dmul_rn(cj, P.res[b]);
+  d[1] = __dmul_rn(cj, P.res[b + G.vstride]);
+  d[2] = __dmul_rn(cj, P.res[b + 2 * G.vstride]);
+}
+
+// the new position: the drift of ExplicitPush (src/dust/dust_push.cpp:289-296) in cell units,
+// x <- x + gam1 (x1 - x) + beta dt xdot (gam0 + gam1 = 1), and the cell carry that replaces
+// SetNewPrtclGID (the neighbour in the crossing direction; periodic images are neighbours).
+// Every operation is explicitly rounded: count and move must agree bit for bit.
+__device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, int &k, int &j,
+                                       int &i, float o[3], float d1[3], const float v[3]) {
+  float xsh = 0.0f;
+  if (P.sbox && G.three_d) {
+    const double *sz = G.mb + (long long)m * 9;
+    const double x = __dadd_rn(sz[X1MIN], __dmul_rn(__dadd_rn((double)i, (double)o[0]), G.dx[0]));
+    xsh = __fmul_rn(__fmul_rn(P.q, P.om), __double2float_rn(x));
+  }
+  const float xdot[3] = {v[0], __fsub_rn(v[1], xsh), v[2]};
+  const int nax = G.three_d ? 3 : 2;
+  int c[3] = {0, 0, 0};
+  for (int a = 0; a < nax; ++a) {
+    const float s = __fmaf_rn(P.bdx[a], xdot[a], __fmul_rn(P.gam1, d1[a]));
+    o[a] = __fadd_rn(o[a], s);
+    d1[a] = __fsub_rn(d1[a], s);
+    int ci = (int)floorf(o[a]);
+    o[a] = __fsub_rn(o[a], (float)ci);
+    if (o[a] >= 1.0f) { o[a] = __fsub_rn(o[a], 1.0f); ++ci; }
+    c[a] = ci;
+  }
+  i += c[0]; j += c[1]; k += c[2];
+  const int o1 = (i < 0) ? -1 : ((i >= G.nx1) ? 1 : 0);
+  const int o2 = (j < 0) ? -1 : ((j >= G.nx2) ? 1 : 0);
+  const int o3 = (k < 0) ? -1 : ((k >= G.nx3) ? 1 : 0);
+  if (o1 | o2 | o3) {
+    const int g = G.nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)] - G.gids;
+    if (g < 0 || g >= G.nmb) {
+      report(P.err, DUSTB_ERR_NGHBR);
+    } else {
+      m = g; i -= o1 * G.nx1; j -= o2 * G.nx2; k -= o3 * G.nx3;
+    }
+    if (i < 0 || i >= G.nx1 || j < 0 || j >= G.nx2 || k < 0 || k >= G.nx3) {
+      report(P.err, DUSTB_ERR_ROUTE);
+      i = min(max(i, 0), G.nx1 - 1); j = min(max(j, 0), G.nx2 - 1); k = min(max(k, 0), G.nx3 - 1);
+    }
+  }
+  return encode(G, m, k, j, i);
+}
+
+// count: the new cell of every particle and the per-cell histogram
+__global__ void __launch_bounds__(kT) k_count(PBuf S, int *key_out, int *count, Geo G, int n,
+                                              PushArgs P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
-  bool live = p < n;
-  int key = 0;
-  if (live) {
-    int m, k, j, i;
-    decode(G, S.cell[p], m, k, j, i);
-    float ox = S.ox[p], oy = S.oy[p], oz = S.oz[p];
-    float vx = S.vx[p], vy = S.vy[p], vz = S.vz[p];
-    float v1x, v1y, v1z, dx1, dy1, dz1, rx, ry, rz;
-    if (P.stage2) {
-      v1x = S.wx[p]; v1y = S.wy[p]; v1z = S.wz[p];
-      dx1 = S.ax[p]; dy1 = S.ay[p]; dz1 = S.az[p];
-      rx = S.rx[p]; ry = S.ry[p]; rz = S.rz[p];
-      if (P.res && S.m[p] > 0.0f) {
-        // dust_imex_point_consistent_dust of stage 1 (src/dust/dust_pm.cpp:686-696)
-        const double cj = (double)S.cc[p];
-        const long long b = G.at(m, 4, 0, k + G.ks, j + G.js, i + G.is);
-        const double d0 = cj * P.res[b], d1 = cj * P.res[b + G.vstride], d2 = cj * P.res[b + 2 * G.vstride];
-        vx += (float)d0; vy += (float)d1; vz += (float)d2;
-        rx += (float)(d0 / P.a_dt); ry += (float)(d1 / P.a_dt); rz += (float)(d2 / P.a_dt);
+  const bool live = p < n;
+  const unsigned act = __ballot_sync(0xffffffffu, live);
+  if (!live) return;
+  int m, k, j, i;
+  decode(G, S.cell[p], m, k, j, i);
+  float o[3] = {S.f[F_OX][p], S.f[F_OY][p], S.f[F_OZ][p]};
+  float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
+  float d1[3] = {0.0f, 0.0f, 0.0f};
+  if (P.stage2) {
+    d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p];
+    if (P.res && S.f[F_M][p] > 0.0f) {
+      double d[3];
+      consistent_dv(G, P, S.f[F_CC][p], m, k, j, i, d);
+      for (int a = 0; a < 3; ++a) v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
+    }
+  }
+  const int key = advance(G, P, m, k, j, i, o, d1, v);
+  key_out[p] = key;
+  warp_count(count, key, act);
+}
+
+// move: the whole push of every particle, written to its slot in dst
+__global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, int *cursor,
+                                             Geo G, int n, PushArgs P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = p < n;
+  const unsigned act = __ballot_sync(0xffffffffu, live);
+  if (!live) return;
+  const int key = key_in[p];
+  const int q = warp_slot(cursor, key, act);
+  int m, k, j, i;
+  decode(G, S.cell[p], m, k, j, i);
+  float o[3] = {S.f[F_OX][p], S.f[F_OY][p], S.f[F_OZ][p]};
+  float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
+  const float ts = S.f[F_TS][p], mass = S.f[F_M][p];
+  float cc = S.f[F_CC][p];
+  float v1[3], d1[3], r[3] = {S.f[F_RX][p], S.f[F_RY][p], S.f[F_RZ][p]};
+  if (P.stage2) {
+    v1[0] = S.f[F_WX][p]; v1[1] = S.f[F_WY][p]; v1[2] = S.f[F_WZ][p];
+    d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p];
+    if (P.res && mass > 0.0f) {
+      double d[3];
+      consistent_dv(G, P, cc, m, k, j, i, d);
+      for (int a = 0; a < 3; ++a) {
+        v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
+        r[a] += (float)(d[a] / P.a_dt);
+      }
+    }
+  } else {
+    // FirstTwoImpRK: (x1, v1) <- (x, v); the drag factor of the cycle, formed in FP64
+    v1[0] = v[0]; v1[1] = v[1]; v1[2] = v[2];
+    d1[0] = d1[1] = d1[2] = 0.0f;
+    cc = (float)(P.a_dt / ((double)ts + P.a_dt));
+  }
+  // ExplicitPush imex (src/dust/dust_push.cpp:262-288): forces from the pre-stage velocity
+  float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+  if (P.sbox) {
+    if (G.three_d) {
+      fx = 2.0f * P.om * v[1];
+      fy = -(2.0f - P.q) * P.om * v[0];
+      if (P.strat) {
+        const double *sz = G.mb + (long long)m * 9;
+        fz = -(P.om * P.om) * (float)(sz[X3MIN] + ((double)k + o[2]) * G.dx[2]);
       }
     } else {
-      // FirstTwoImpRK: (x1, v1) <- (x, v)
-      v1x = vx; v1y = vy; v1z = vz;
-      dx1 = 0.0f; dy1 = 0.0f; dz1 = 0.0f;
-      rx = 0.0f; ry = 0.0f; rz = 0.0f;
-      S.wx[p] = vx; S.wy[p] = vy; S.wz[p] = vz;
-      // the drag factor of this cycle, a/(t_s + a) (dust_pm.cpp:255), formed in FP64 once
-      S.cc[p] = (float)(P.a_dt / ((double)S.ts[p] + P.a_dt));
+      fx = 2.0f * P.om * v[2];
+      fz = -(2.0f - P.q) * P.om * v[0];
     }
-    // ExplicitPush imex (src/dust/dust_push.cpp:262-297)
-    float fx = 0.0f, fy = 0.0f, fz = 0.0f, xsh = 0.0f;
-    if (P.sbox) {
-      const double *sz = G.mb + (long long)m * 9;
-      if (G.three_d) {
-        fx = 2.0f * P.om * vy;
-        fy = -(2.0f - P.q) * P.om * vx;
-        if (P.strat) fz = -(P.om * P.om) * (float)(sz[X3MIN] + ((double)k + oz) * G.dx[2]);
-        xsh = P.q * P.om * (float)(sz[X1MIN] + ((double)i + ox) * G.dx[0]);
-      } else {
-        fx = 2.0f * P.om * vz;
-        fz = -(2.0f - P.q) * P.om * vx;
-      }
-    }
-    const float nvx = P.gam0 * vx + P.gam1 * v1x + P.bdt * fx + P.atw_dt * rx;
-    const float nvy = P.gam0 * vy + P.gam1 * v1y + P.bdt * fy + P.atw_dt * ry;
-    const float nvz = P.gam0 * vz + P.gam1 * v1z + P.bdt * fz + P.atw_dt * rz;
-    // drift in cell units: x <- x + gam1 (x1 - x) + beta dt xdot (gam0 + gam1 = 1)
-    const float sx = P.gam1 * dx1 + P.bdx[0] * vx;
-    const float sy = P.gam1 * dy1 + P.bdx[1] * (vy - xsh);
-    ox += sx; dx1 -= sx;
-    oy += sy; dy1 -= sy;
-    if (G.three_d) {
-      const float sz_ = P.gam1 * dz1 + P.bdx[2] * vz;
-      oz += sz_; dz1 -= sz_;
-    }
-    // cell carry (the integer part of the new offsets)
-    int ci = (int)floorf(ox); ox -= (float)ci; if (ox >= 1.0f) { ox -= 1.0f; ++ci; }
-    int cj = (int)floorf(oy); oy -= (float)cj; if (oy >= 1.0f) { oy -= 1.0f; ++cj; }
-    int ck = 0;
-    if (G.three_d) { ck = (int)floorf(oz); oz -= (float)ck; if (oz >= 1.0f) { oz -= 1.0f; ++ck; } }
-    i += ci; j += cj; k += ck;
-    // block crossing: the neighbour in the crossing direction (periodic images are neighbours)
-    const int o1 = (i < 0) ? -1 : ((i >= G.nx1) ? 1 : 0);
-    const int o2 = (j < 0) ? -1 : ((j >= G.nx2) ? 1 : 0);
-    const int o3 = (k < 0) ? -1 : ((k >= G.nx3) ? 1 : 0);
-    if (o1 | o2 | o3) {
-      const int g = G.nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)] - G.gids;
-      if (g < 0 || g >= G.nmb) {
-        report(P.err, DUSTB_ERR_NGHBR);
-      } else {
-        m = g; i -= o1 * G.nx1; j -= o2 * G.nx2; k -= o3 * G.nx3;
-      }
-      if (i < 0 || i >= G.nx1 || j < 0 || j >= G.nx2 || k < 0 || k >= G.nx3) {
-        report(P.err, DUSTB_ERR_ROUTE);
-        i = min(max(i, 0), G.nx1 - 1); j = min(max(j, 0), G.nx2 - 1); k = min(max(k, 0), G.nx3 - 1);
-      }
-    }
-    key = encode(G, m, k, j, i);
-    S.cell[p] = key;
-    S.ox[p] = ox; S.oy[p] = oy; S.oz[p] = oz;
-    S.vx[p] = nvx; S.vy[p] = nvy; S.vz[p] = nvz;
-    S.ax[p] = dx1; S.ay[p] = dy1; S.az[p] = dz1;
-    if (P.stage2) { S.rx[p] = rx; S.ry[p] = ry; S.rz[p] = rz; }
   }
-  warp_hist(S.cstart, key, live);
+  const float atw = P.stage2 ? P.atw_dt : 0.0f;
+  const float nv[3] = {P.gam0 * v[0] + P.gam1 * v1[0] + P.bdt * fx + atw * r[0],
+                       P.gam0 * v[1] + P.gam1 * v1[1] + P.bdt * fy + atw * r[1],
+                       P.gam0 * v[2] + P.gam1 * v1[2] + P.bdt * fz + atw * r[2]};
+  const int key2 = advance(G, P, m, k, j, i, o, d1, v);
+  if (key2 != key) report(P.err, DUSTB_ERR_WINDOW);   // count and move disagree: never expected
+  D.cell[q] = key; D.pid[q] = S.pid[p];
+  D.f[F_OX][q] = o[0]; D.f[F_OY][q] = o[1]; D.f[F_OZ][q] = o[2];
+  D.f[F_VX][q] = nv[0]; D.f[F_VY][q] = nv[1]; D.f[F_VZ][q] = nv[2];
+  D.f[F_AX][q] = d1[0]; D.f[F_AY][q] = d1[1]; D.f[F_AZ][q] = d1[2];
+  D.f[F_WX][q] = v1[0]; D.f[F_WY][q] = v1[1]; D.f[F_WZ][q] = v1[2];
+  D.f[F_RX][q] = r[0]; D.f[F_RY][q] = r[1]; D.f[F_RZ][q] = r[2];
+  D.f[F_TS][q] = ts; D.f[F_M][q] = mass; D.f[F_CC][q] = cc;
 }
 
 // ---- stage-2 consistent dust kick ------------------------------------------------------
-__global__ void k_consistent_kick(MState S, Geo G, int n, double a_dt, const double *res) {
+__global__ void k_consistent_kick(PBuf S, Geo G, int n, double a_dt, const double *res) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n || !(S.m[p] > 0.0f)) return;
+  if (p >= n || !(S.f[F_M][p] > 0.0f)) return;
   int m, k, j, i;
   decode(G, S.cell[p], m, k, j, i);
-  const double cj = (double)S.cc[p];
+  const double cj = (double)S.f[F_CC][p];
   const long long b = G.at(m, 4, 0, k + G.ks, j + G.js, i + G.is);
   const double d0 = cj * res[b], d1 = cj * res[b + G.vstride], d2 = cj * res[b + 2 * G.vstride];
-  S.vx[p] += (float)d0; S.vy[p] += (float)d1; S.vz[p] += (float)d2;
-  S.rx[p] += (float)(d0 / a_dt); S.ry[p] += (float)(d1 / a_dt); S.rz[p] += (float)(d2 / a_dt);
+  S.f[F_VX][p] += (float)d0; S.f[F_VY][p] += (float)d1; S.f[F_VZ][p] += (float)d2;
+  S.f[F_RX][p] += (float)(d0 / a_dt); S.f[F_RY][p] += (float)(d1 / a_dt); S.f[F_RZ][p] += (float)(d2 / a_dt);
 }
 
-// ---- tile deposit kernels ---------------------------------------------------------------
+// ---- tile deposit kernels -------------------------------------------------------------------
 enum { MODE_QP = 0, MODE_OP = 1, MODE_KICK = 2 };
 
 struct TileArgs {
-  int tj, chunk, tpp;          // rows per tile, particles per pass, tiles per (block, plane)
+  int tj, chunk, tpp;          // rows per tile, buffer columns, tiles per (block, plane)
   double a_dt;
+  const int *cstart;           // cell -> particle ranges of the sorted shadow
   const double *gfield;        // gather field (3 vars), MODE_OP / MODE_KICK
   double *dfield;              // deposit field
   int dnvar;
@@ -391,19 +507,27 @@ struct TileArgs {
   unsigned *err;
 };
 
-__host__ __device__ inline int tile_ncomp(int mode) { return mode == MODE_QP ? 4 : 3; }
+__host__ __device__ inline int tile_nfield(int mode) { return mode == MODE_OP ? 5 : 8; }
 
-template <int MODE>
-__global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, TileArgs T) {
-  constexpr int NC = (MODE == MODE_QP) ? 4 : 3;
-  constexpr int B = 4;                           // particles per thread loaded together
-  extern __shared__ __align__(16) unsigned char smem[];
+// the index of variable 0 of block-local cell (kk, jj, ii) of block m in a field of nvar
+// variables, or -1 if no block owns it; a cell one beyond the block maps to the owning
+// neighbour's active cell (the ghost exchanges folded into the index)
+__device__ __forceinline__ long long cell_at(const Geo &G, int m, int nvar, int kk, int jj, int ii) {
+  int mo;
+  if (!G.owner(m, kk, jj, ii, mo)) return -1;
+  return G.at(mo, nvar, 0, G.ks + kk, G.js + jj, G.is + ii);
+}
+__device__ __forceinline__ float2 dup(float x) { return make_float2(x, x); }
+
+template <int MODE, int D3>
+__global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, TileArgs T) {
+  constexpr int NC = (MODE == MODE_QP) ? 4 : 3;    // deposited values per particle
+  constexpr int NF = (MODE == MODE_OP) ? 5 : 8;    // fields copied: ox oy oz cc m [vx vy vz]
+  constexpr int WK = D3 ? 3 : 1;                   // z planes of the stencil
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
   const int nx1 = G.nx1, tj = T.tj;
-  const int nct = tj * nx1;                      // source cells of the tile
-  const int WK = G.three_d ? 3 : 1;
-  const int WJ = tj + 2, WI = nx1 + 2;
-  const int WN = WK * WJ * WI;
-  // tile coordinates
+  const int nct = tj * nx1;                        // source cells of the tile = threads
   int t = blockIdx.x;
   const int per_block = G.nx3 * T.tpp;
   const int m = t / per_block;
@@ -411,382 +535,213 @@ __global__ void __launch_bounds__(kMaxTileThreads, 2) k_tile(MState S, Geo G, Ti
   const int k = t / T.tpp;
   const int j0 = (t - k * T.tpp) * tj;
   const int c0 = encode(G, m, k, j0, 0);
-  // shared layout: cstart | gather window (float4) | deposit window (FP64) | chunk SoA
-  int *s_cs = (int *)smem;
-  size_t off = ((size_t)(nct + 1) * 4 + 15) & ~(size_t)15;
-  float4 *gw = (float4 *)(smem + off);
-  if (MODE != MODE_QP) off += (size_t)WN * 16;
-  double *dw = (double *)(smem + off);           // [NC][WN]
-  off += (size_t)NC * WN * 8;
-  float *s_f = (float *)(smem + off);            // [9 weights + NC values][chunk]
-  const int CH = T.chunk;
-
-  for (int x = threadIdx.x; x <= nct; x += blockDim.x) s_cs[x] = S.cstart[c0 + x];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
-  // threads of this warp (the last warp of a block of 8-cell rows can be partial)
-  const int wlanes = min(32, (int)blockDim.x - 32 * warp);
-  if (MODE != MODE_QP) {
-    // the tile's u* window; cells beyond the block read the owning neighbour's active cell
-    // (the same-level copy exchange of the ghost cells, folded into the load)
-    for (int row = warp; row < WK * WJ; row += nwarp) {
-      const int wk = row / WJ, wj = row - wk * WJ;
-      for (int wi = lane; wi < WI; wi += wlanes) {
-        int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
-        float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (G.owner(m, kk, jj, ii, mo)) {
-          const long long b = G.at(mo, 3, 0, G.ks + kk, G.js + jj, G.is + ii);
-          g = make_float4((float)T.gfield[b], (float)T.gfield[b + G.vstride],
-                          (float)T.gfield[b + 2 * G.vstride], 0.0f);
-        }
-        gw[row * WI + wi] = g;
-      }
-    }
-  }
-  if (T.deposit)
-    for (int w = threadIdx.x; w < NC * WN; w += blockDim.x) dw[w] = 0.0;
-  __syncthreads();
-  const int P0 = s_cs[0], P1 = s_cs[nct];
-  // thread role in the accumulation: source cell cl, z offset cz
-  const int cl = threadIdx.x % nct;
-  const int cz = threadIdx.x / nct;              // 0..WK-1
+  const int CH = T.chunk;                          // buffer columns (multiple of 4)
+  int *s_cs = (int *)smem;                         // [nct + 1] cell ranges
+  float *s_f = (float *)(smem + (((size_t)(nct + 1) * 4 + 15) & ~(size_t)15));  // [NF][CH]
+  const int cl = threadIdx.x;                      // this thread's source cell
   const int cj_l = cl / nx1, ci_l = cl - cj_l * nx1;
-  float qt = 0.0f;
-  const float inv_vol = (float)(1.0 / G.vol);
-  const float inv_adt = (float)(1.0 / T.a_dt);
+  const int lane = threadIdx.x & 31;
+  const int wlanes = min(32, nct - (int)(threadIdx.x & ~31u));
 
-  for (int cbase = P0; cbase < P1; cbase += CH) {
-    const int cnt = min(CH, P1 - cbase);
-    // (a) per particle: the 9 stencil weights, [gather, kick] and the deposited values into
-    // shared memory (once, for the 3 z-offset threads of the cell); the loads of B particles
-    // per thread are issued together
-    for (int x0 = threadIdx.x; x0 < cnt; x0 += B * blockDim.x) {
-      int pb[B];
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  for (int x = threadIdx.x; x <= nct; x += blockDim.x) s_cs[x] = T.cstart[c0 + x];
+  // the gather field on the 27 cells around this cell, FP32, in registers; cells beyond the
+  // block read the owning neighbour's active cell (the copy exchange of u*'s ghost cells)
+  // (x, y components as packed FP32 pairs)
+  float2 gxy[WK][3][3];
+  float gz[WK][3][3];
+  if (MODE != MODE_QP) {
 #pragma unroll
-      for (int u = 0; u < B; ++u) pb[u] = S.order[cbase + min(x0 + u * (int)blockDim.x, cnt - 1)];
-      int lc[B];
-      float fo[B][3], fc[B], fmass[B], fv[B][3];
-#pragma unroll
-      for (int u = 0; u < B; ++u) {
-        const int p = pb[u];
-        lc[u] = S.cell[p] - c0;
-        fo[u][0] = S.ox[p]; fo[u][1] = S.oy[p]; fo[u][2] = S.oz[p];
-        fc[u] = S.cc[p]; fmass[u] = S.m[p];
-        if (MODE != MODE_OP) { fv[u][0] = S.vx[p]; fv[u][1] = S.vy[p]; fv[u][2] = S.vz[p]; }
-      }
-#pragma unroll
-      for (int u = 0; u < B; ++u) {
-        const int x = x0 + u * blockDim.x;
-        if (x >= cnt) break;
-        const int local = lc[u];               // the tile's cells are consecutive ids
-        if (local < 0 || local >= nct) {
-          // not a particle of this tile: the cell index is stale; contribute nothing
-          report(T.err, DUSTB_ERR_WINDOW);
-#pragma unroll
-          for (int q = 0; q < 9 + NC; ++q) s_f[q * CH + x] = 0.0f;
-          continue;
-        }
-        int jl, pii;
-        if (G.l1 >= 0) { jl = local >> G.l1; pii = local & (nx1 - 1); }
-        else { jl = local / nx1; pii = local - jl * nx1; }
-        const float c32 = fc[u], mass = fmass[u];
-        float wx_[3], wy_[3], wz_[3];
-        wts(G.scheme, fo[u][0], wx_); wts(G.scheme, fo[u][1], wy_);
-        if (G.three_d) wts(G.scheme, fo[u][2], wz_); else { wz_[0] = 0.0f; wz_[1] = 1.0f; wz_[2] = 0.0f; }
-        float qv[NC];
-        if (MODE == MODE_QP) {
-          const float mc = mass * c32 * inv_vol;
-          qv[0] = mc; qv[1] = mc * fv[u][0]; qv[2] = mc * fv[u][1];
-          if (NC > 3) qv[NC - 1] = mc * fv[u][2];
-        } else {
-          float ux = 0.0f, uy = 0.0f, uz = 0.0f;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            if (!G.three_d && c != 1) continue;
-            const int wk = G.three_d ? c : 0;
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-              const float wzy = wz_[c] * wy_[b];
-              const float4 *row = gw + (wk * WJ + jl + b) * WI + pii;
-#pragma unroll
-              for (int a = 0; a < 3; ++a) {
-                const float w = wzy * wx_[a];
-                const float4 g = row[a];
-                ux = fmaf(w, g.x, ux); uy = fmaf(w, g.y, uy); uz = fmaf(w, g.z, uz);
-              }
-            }
-          }
-          if (MODE == MODE_OP) {
-            const float mc = mass * c32 * inv_vol;
-            qv[0] = mc * ux; qv[1] = mc * uy; qv[2] = mc * uz;
-          } else {
-            // GatherKickPMBR (src/dust/dust_pm.cpp:534-563) with the applied velocity change
-            const float vx = fv[u][0], vy = fv[u][1], vz = fv[u][2];
-            const float nx_ = vx + c32 * (ux - vx), ny_ = vy + c32 * (uy - vy), nz_ = vz + c32 * (uz - vz);
-            const float dvx = nx_ - vx, dvy = ny_ - vy, dvz = nz_ - vz;
-            const int p = pb[u];
-            S.vx[p] = nx_; S.vy[p] = ny_; S.vz[p] = nz_;
-            S.rx[p] = dvx * inv_adt; S.ry[p] = dvy * inv_adt; S.rz[p] = dvz * inv_adt;
-            const float fac = -mass * inv_vol;
-            qv[0] = fac * dvx; qv[1] = fac * dvy; qv[2] = fac * dvz;
-          }
-        }
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          s_f[a * CH + x] = wx_[a]; s_f[(3 + a) * CH + x] = wy_[a]; s_f[(6 + a) * CH + x] = wz_[a];
-        }
-#pragma unroll
-        for (int q = 0; q < NC; ++q) s_f[(9 + q) * CH + x] = qv[q];
-      }
-    }
-    __syncthreads();
-    if (T.deposit) {
-      // (b) per source cell and z offset: the 9 stencil sums of the cell's particles
-      float acc[3][3][NC];
+    for (int c = 0; c < WK; ++c)
 #pragma unroll
       for (int b = 0; b < 3; ++b)
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int q = 0; q < NC; ++q) acc[b][a][q] = 0.0f;
-      const int lo = max(s_cs[cl], cbase) - cbase;
-      const int hi = min(s_cs[cl + 1], cbase + cnt) - cbase;
-      const int zrow = (G.three_d ? 6 + cz : 7) * CH;
-      for (int r = lo; r < hi; ++r) {
-        const float wx_[3] = {s_f[r], s_f[CH + r], s_f[2 * CH + r]};
-        const float wy_[3] = {s_f[3 * CH + r], s_f[4 * CH + r], s_f[5 * CH + r]};
-        const float wzc = s_f[zrow + r];
-        float qv[NC];
-#pragma unroll
-        for (int q = 0; q < NC; ++q) qv[q] = s_f[(9 + q) * CH + r];
-        if (MODE == MODE_QP && cz == (G.three_d ? 1 : 0)) qt += qv[0];
-#pragma unroll
-        for (int b = 0; b < 3; ++b) {
-          const float wzy = wzc * wy_[b];
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const float w = wzy * wx_[a];
-#pragma unroll
-            for (int q = 0; q < NC; ++q) acc[b][a][q] = fmaf(w, qv[q], acc[b][a][q]);
+        for (int a = 0; a < 3; ++a) {
+          const long long at = cell_at(G, m, 3, D3 ? k - 1 + c : 0, j0 + cj_l - 1 + b, ci_l - 1 + a);
+          gxy[c][b][a] = make_float2(0.0f, 0.0f);
+          gz[c][b][a] = 0.0f;
+          if (at >= 0) {
+            gxy[c][b][a] = make_float2((float)T.gfield[at], (float)T.gfield[at + G.vstride]);
+            gz[c][b][a] = (float)T.gfield[at + 2 * G.vstride];
           }
         }
-      }
-      // (c) into the FP64 window: 9 passes, one (y, x) offset each; within a pass every
-      // thread writes a different window cell
-#pragma unroll
-      for (int b = 0; b < 3; ++b) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const int w = (cz * WJ + cj_l + b) * WI + ci_l + a;
-#pragma unroll
-          for (int q = 0; q < NC; ++q) dw[q * WN + w] += (double)acc[b][a][q];
-          __syncthreads();
-        }
-      }
-    }
   }
-  if (MODE == MODE_QP && cz == (G.three_d ? 1 : 0)) {
-    // centre mass m c / V of the cell (dust_imex_point_center_mass): only this tile's
-    // particles have this cell as their centre, so it is stored, not added
-    T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj_l, G.is + ci_l)] = (double)qt;
-  }
-  if (!T.deposit || P1 == P0) return;
-  // (d) the window into the FP64 field; window cells beyond the block go straight into the
-  // owning neighbour's active cell (the additive ghost exchange folded into the flush)
-  for (int row = warp; row < NC * WK * WJ; row += nwarp) {
-    const int q = row / (WK * WJ), r2 = row - q * (WK * WJ);
-    const int wk = r2 / WJ, wj = r2 - wk * WJ;
-    for (int wi = lane; wi < WI; wi += wlanes) {
-      const double v = dw[row * WI + wi];
-      if (v == 0.0) continue;
-      int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
-      if (!G.owner(m, kk, jj, ii, mo)) continue;
-      atomicAdd(&T.dfield[G.at(mo, T.dnvar, q, G.ks + kk, G.js + jj, G.is + ii)], v);
-    }
-  }
-}
-
-size_t tile_smem(int mode, int tj, int nx1, int three_d, int chunk) {
-  const int nct = tj * nx1;
-  const int WN = (three_d ? 3 : 1) * (tj + 2) * (nx1 + 2);
-  const int NC = tile_ncomp(mode);
-  size_t s = ((size_t)(nct + 1) * 4 + 15) & ~(size_t)15;
-  if (mode != MODE_QP) s += (size_t)WN * 16;
-  s += (size_t)NC * WN * 8;
-  s += (size_t)(9 + NC) * chunk * 4;
-  return s;
-}
-
-// One thread per source cell: the thread walks its cell's particles (cell order) straight
-// from global memory, forms the 27 stencil weights and the deposited values of each,
-// accumulates the 27 x NC sums in registers and adds them to the tile's FP64 shared window
-// with shared-memory atomics (native FP64 on this GPU); the window is added to the FP64
-// field once per cell.  Three barriers per tile.
-template <int MODE>
-__global__ void __launch_bounds__(256, 1) k_cellacc(MState S, Geo G, TileArgs T) {
-  constexpr int NC = (MODE == MODE_QP) ? 4 : 3;
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int nx1 = G.nx1, tj = T.tj;
-  const int nct = tj * nx1;                      // source cells of the tile (= threads)
-  const int WK = G.three_d ? 3 : 1;
-  const int WJ = tj + 2, WI = nx1 + 2;
-  const int WN = WK * WJ * WI;
-  int t = blockIdx.x;
-  const int per_block = G.nx3 * T.tpp;
-  const int m = t / per_block;
-  t -= m * per_block;
-  const int k = t / T.tpp;
-  const int j0 = (t - k * T.tpp) * tj;
-  const int c0 = encode(G, m, k, j0, 0);
-  // shared layout: gather window (float4) | deposit window (FP64)
-  size_t off = 0;
-  float4 *gw = (float4 *)smem;
-  if (MODE != MODE_QP) off += (size_t)WN * 16;
-  double *dw = (double *)(smem + off);           // [NC][WN]
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
-  // threads of this warp (the last warp of a block of 8-cell rows can be partial)
-  const int wlanes = min(32, (int)blockDim.x - 32 * warp);
-  if (MODE != MODE_QP) {
-    for (int row = warp; row < WK * WJ; row += nwarp) {
-      const int wk = row / WJ, wj = row - wk * WJ;
-      for (int wi = lane; wi < WI; wi += wlanes) {
-        int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
-        float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (G.owner(m, kk, jj, ii, mo)) {
-          const long long b = G.at(mo, 3, 0, G.ks + kk, G.js + jj, G.is + ii);
-          g = make_float4((float)T.gfield[b], (float)T.gfield[b + G.vstride],
-                          (float)T.gfield[b + 2 * G.vstride], 0.0f);
-        }
-        gw[row * WI + wi] = g;
-      }
-    }
-  }
-  if (T.deposit)
-    for (int w = threadIdx.x; w < NC * WN; w += blockDim.x) dw[w] = 0.0;
   __syncthreads();
-  const int cl = threadIdx.x;                    // the thread's source cell in the tile
-  int jl, il;
-  if (G.l1 >= 0) { jl = cl >> G.l1; il = cl & (nx1 - 1); }
-  else { jl = cl / nx1; il = cl - jl * nx1; }
-  const int lo = S.cstart[c0 + cl], hi = S.cstart[c0 + cl + 1];
-  const float inv_vol = (float)(1.0 / G.vol);
-  const float inv_adt = (float)(1.0 / T.a_dt);
-  float acc[3][3][3][NC];
+  const int P0 = s_cs[0], P1 = s_cs[nct];
+  const int c_lo = s_cs[cl], c_hi = s_cs[cl + 1];  // this cell's particles
+  // the 27-point sums of this cell's particles: values 0, 1 as packed pairs; values 2, 3 as
+  // a pair (Q/P) or value 2 alone (operator, kick)
+  float2 acc01[WK][3][3], acc23[WK][3][3];
+  float acc2[WK][3][3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
+  for (int c = 0; c < WK; ++c)
 #pragma unroll
     for (int b = 0; b < 3; ++b)
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int q = 0; q < NC; ++q) acc[c][b][a][q] = 0.0f;
+      for (int a = 0; a < 3; ++a) {
+        acc01[c][b][a] = make_float2(0.0f, 0.0f);
+        acc23[c][b][a] = make_float2(0.0f, 0.0f);
+        acc2[c][b][a] = 0.0f;
+      }
   float qt = 0.0f;
-  for (int r = lo; r < hi; ++r) {
-    const int p = S.order[r];
-    const float c32 = S.cc[p], mass = S.m[p];
-    float wx_[3], wy_[3], wz_[3];
-    wts(G.scheme, S.ox[p], wx_);
-    wts(G.scheme, S.oy[p], wy_);
-    if (G.three_d) wts(G.scheme, S.oz[p], wz_); else { wz_[0] = 0.0f; wz_[1] = 1.0f; wz_[2] = 0.0f; }
-    float qv[NC];
-    if (MODE == MODE_QP) {
-      const float mc = mass * c32 * inv_vol;
-      qt += mc;
-      qv[0] = mc; qv[1] = mc * S.vx[p]; qv[2] = mc * S.vy[p];
-      if (NC > 3) qv[NC - 1] = mc * S.vz[p];
-    } else {
-      float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+  const float inv_vol = (float)(1.0 / G.vol);
+  const float inv_adt = (float)(1.0 / T.a_dt);
+  const int CHP = CH - 8;                          // particles per pass (room to round out)
+  unsigned parity = 0;
+
+  for (int cb = P0; cb < P1; cb += CHP) {
+    const int ce = min(P1, cb + CHP), cnt = ce - cb;
+    const int a0 = cb & ~3, a1 = (ce + 3) & ~3, sh = cb - a0;
+    if (threadIdx.x == 0) {
+      // the particle range of this pass, field by field, rounded out to 16-byte groups
+      const unsigned bytes = (unsigned)(a1 - a0) * 4u;
+      const int fl[8] = {F_OX, F_OY, F_OZ, F_CC, F_M, F_VX, F_VY, F_VZ};
+      fence_proxy_async();
+      mbar_arrive_tx(&bar, bytes * NF);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (!G.three_d && c != 1) continue;
-        const int wk = G.three_d ? c : 0;
-#pragma unroll
-        for (int b = 0; b < 3; ++b) {
-          const float wzy = wz_[c] * wy_[b];
-          const float4 *row = gw + (wk * WJ + jl + b) * WI + il;
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const float w = wzy * wx_[a];
-            const float4 g = row[a];
-            ux = fmaf(w, g.x, ux); uy = fmaf(w, g.y, uy); uz = fmaf(w, g.z, uz);
-          }
-        }
-      }
-      if (MODE == MODE_OP) {
+      for (int f = 0; f < NF; ++f) bulk_copy(s_f + f * CH, S.f[fl[f]] + a0, bytes, &bar);
+    }
+    const bool ok = mbar_wait(&bar, parity, T.err);
+    parity ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      // the copies never completed: wait once more (bounded) for them, then give up the tile
+      mbar_wait(&bar, parity ^ 1u, T.err);
+      return;
+    }
+    // this cell's particles in the pass, at columns lo..hi of the rows
+    const int lo = max(c_lo, cb) - a0, hi = min(c_hi, ce) - a0;
+    for (int r = lo; r < hi; ++r) {
+      const float c32 = s_f[3 * CH + r], mass = s_f[4 * CH + r];
+      float wx_[3], wy_[3], wz_[3];
+      wts(G.scheme, s_f[r], wx_);
+      wts(G.scheme, s_f[CH + r], wy_);
+      if (D3) wts(G.scheme, s_f[2 * CH + r], wz_);
+      float2 q01, q23 = make_float2(0.0f, 0.0f);   // the deposited values
+      if (MODE == MODE_QP) {
         const float mc = mass * c32 * inv_vol;
-        qv[0] = mc * ux; qv[1] = mc * uy; qv[2] = mc * uz;
+        q01 = make_float2(mc, mc * s_f[5 * CH + r]);
+        q23 = make_float2(mc * s_f[6 * CH + r], mc * s_f[7 * CH + r]);
+        qt += mc;
       } else {
-        // GatherKickPMBR (src/dust/dust_pm.cpp:534-563) with the applied velocity change
-        const float vx = S.vx[p], vy = S.vy[p], vz = S.vz[p];
-        const float nx_ = vx + c32 * (ux - vx), ny_ = vy + c32 * (uy - vy), nz_ = vz + c32 * (uz - vz);
-        const float dvx = nx_ - vx, dvy = ny_ - vy, dvz = nz_ - vz;
-        S.vx[p] = nx_; S.vy[p] = ny_; S.vz[p] = nz_;
-        S.rx[p] = dvx * inv_adt; S.ry[p] = dvy * inv_adt; S.rz[p] = dvz * inv_adt;
-        const float fac = -mass * inv_vol;
-        qv[0] = fac * dvx; qv[1] = fac * dvy; qv[2] = fac * dvz;
-      }
-    }
-    if (T.deposit) {
+        // u = sum over (c, b) of wz_c wy_b (sum over a of wx_a g_cba)
+        float2 uxy = make_float2(0.0f, 0.0f);
+        float uz = 0.0f;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (!G.three_d && c != 1) continue;
+        for (int c = 0; c < WK; ++c) {
+          const float wzc = D3 ? wz_[c] : 1.0f;
 #pragma unroll
-        for (int b = 0; b < 3; ++b) {
-          const float wzy = wz_[c] * wy_[b];
+          for (int b = 0; b < 3; ++b) {
+            float2 txy = __fmul2_rn(dup(wx_[0]), gxy[c][b][0]);
+            float tz = wx_[0] * gz[c][b][0];
 #pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const float w = wzy * wx_[a];
-#pragma unroll
-            for (int q = 0; q < NC; ++q) acc[c][b][a][q] = fmaf(w, qv[q], acc[c][b][a][q]);
+            for (int a = 1; a < 3; ++a) {
+              txy = __ffma2_rn(dup(wx_[a]), gxy[c][b][a], txy);
+              tz = fmaf(wx_[a], gz[c][b][a], tz);
+            }
+            const float wzy = wzc * wy_[b];
+            uxy = __ffma2_rn(dup(wzy), txy, uxy);
+            uz = fmaf(wzy, tz, uz);
           }
         }
+        const float ux = uxy.x, uy = uxy.y;
+        if (MODE == MODE_OP) {
+          const float mc = mass * c32 * inv_vol;
+          q01 = make_float2(mc * ux, mc * uy); q23.x = mc * uz;
+        } else {
+          // GatherKickPMBR (src/dust/dust_pm.cpp:534-563) with the applied velocity change;
+          // the new velocity and the change replace this particle's columns of the rows
+          const float vx = s_f[5 * CH + r], vy = s_f[6 * CH + r], vz = s_f[7 * CH + r];
+          const float nx_ = vx + c32 * (ux - vx), ny_ = vy + c32 * (uy - vy), nz_ = vz + c32 * (uz - vz);
+          const float dvx = nx_ - vx, dvy = ny_ - vy, dvz = nz_ - vz;
+          s_f[5 * CH + r] = nx_; s_f[6 * CH + r] = ny_; s_f[7 * CH + r] = nz_;
+          s_f[r] = dvx; s_f[CH + r] = dvy; s_f[2 * CH + r] = dvz;
+          const float fac = -mass * inv_vol;
+          q01 = make_float2(fac * dvx, fac * dvy); q23.x = fac * dvz;
+        }
       }
-    }
-  }
-  if (MODE == MODE_QP) {
-    // centre mass m c / V of the cell (dust_imex_point_center_mass): only this thread's
-    // particles have this cell as their centre, so it is stored, not added
-    T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + jl, G.is + il)] = (double)qt;
-  }
-  if (!T.deposit) return;
-  if (hi > lo) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (!G.three_d && c != 1) continue;
-      const int wk = G.three_d ? c : 0;
-#pragma unroll
-      for (int b = 0; b < 3; ++b)
+      if (MODE == MODE_QP || T.deposit) {
+        // acc_cba += wz_c wy_b (wx_a q): the x weights folded into the values first
+        float2 s01[3], s23[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          const int w = (wk * WJ + jl + b) * WI + il + a;
-#pragma unroll
-          for (int q = 0; q < NC; ++q) atomicAdd(&dw[q * WN + w], (double)acc[c][b][a][q]);
+          s01[a] = __fmul2_rn(dup(wx_[a]), q01);
+          if (MODE == MODE_QP) s23[a] = __fmul2_rn(dup(wx_[a]), q23);
+          else s23[a].x = wx_[a] * q23.x;
         }
+#pragma unroll
+        for (int c = 0; c < WK; ++c) {
+          const float wzc = D3 ? wz_[c] : 1.0f;
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            const float wzy = wzc * wy_[b];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              acc01[c][b][a] = __ffma2_rn(dup(wzy), s01[a], acc01[c][b][a]);
+              if (MODE == MODE_QP) acc23[c][b][a] = __ffma2_rn(dup(wzy), s23[a], acc23[c][b][a]);
+              else acc2[c][b][a] = fmaf(wzy, s23[a].x, acc2[c][b][a]);
+            }
+          }
+        }
+      }
     }
+    if (MODE == MODE_KICK) {
+      // the kicked velocities and rates of the pass, particle by particle (coalesced)
+      __syncthreads();
+      for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
+        const int s = sh + x, p = cb + x;
+        S.f[F_VX][p] = s_f[5 * CH + s]; S.f[F_VY][p] = s_f[6 * CH + s]; S.f[F_VZ][p] = s_f[7 * CH + s];
+        S.f[F_RX][p] = s_f[s] * inv_adt; S.f[F_RY][p] = s_f[CH + s] * inv_adt;
+        S.f[F_RZ][p] = s_f[2 * CH + s] * inv_adt;
+      }
+    }
+    // the next pass's copies overwrite the rows
+    __syncthreads();
   }
-  __syncthreads();
-  // the window into the FP64 field; window cells beyond the block go straight into the
-  // owning neighbour's active cell (the additive ghost exchange folded into the flush)
-  for (int row = warp; row < NC * WK * WJ; row += nwarp) {
-    const int q = row / (WK * WJ), r2 = row - q * (WK * WJ);
-    const int wk = r2 / WJ, wj = r2 - wk * WJ;
-    for (int wi = lane; wi < WI; wi += wlanes) {
-      const double v = dw[row * WI + wi];
-      if (v == 0.0) continue;
-      int kk = G.three_d ? (k - 1 + wk) : 0, jj = j0 - 1 + wj, ii = wi - 1, mo;
-      if (!G.owner(m, kk, jj, ii, mo)) continue;
-      atomicAdd(&T.dfield[G.at(mo, T.dnvar, q, G.ks + kk, G.js + jj, G.is + ii)], v);
+  if (MODE == MODE_QP) {
+    // centre mass m c / V of the cell (dust_imex_point_center_mass): only this cell's
+    // particles have it as their centre, so it is stored, not added
+    T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj_l, G.is + ci_l)] = (double)qt;
+  }
+  if (MODE != MODE_QP && !T.deposit) return;
+  // the x-offset contributions of neighbouring cells of a row meet in registers: lane L takes
+  // lane L+1's left and lane L-1's right contribution; a row's (or warp's) end lanes add
+  // their outward contribution themselves
+  const unsigned wmask = (wlanes == 32) ? 0xffffffffu : ((1u << wlanes) - 1u);
+  const bool has_left = ci_l > 0 && lane > 0;
+  const bool has_right = ci_l + 1 < nx1 && lane + 1 < wlanes;
+  auto val = [&](int c, int b, int a, int q) {
+    return q == 0 ? acc01[c][b][a].x : q == 1 ? acc01[c][b][a].y
+         : (MODE == MODE_QP ? (q == 2 ? acc23[c][b][a].x : acc23[c][b][a].y) : acc2[c][b][a]);
+  };
+#pragma unroll
+  for (int c = 0; c < WK; ++c) {
+    const int kk = D3 ? k - 1 + c : 0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const int jj = j0 + cj_l - 1 + b;
+      // the row's target cells: this cell's column, and the outward ones of the end lanes
+      const long long bc = cell_at(G, m, T.dnvar, kk, jj, ci_l);
+      const long long bl = has_left ? -1 : cell_at(G, m, T.dnvar, kk, jj, ci_l - 1);
+      const long long bR = has_right ? -1 : cell_at(G, m, T.dnvar, kk, jj, ci_l + 1);
+#pragma unroll
+      for (int q = 0; q < NC; ++q) {
+        const float l = val(c, b, 0, q), mid = val(c, b, 1, q), r = val(c, b, 2, q);
+        const float from_right = __shfl_down_sync(wmask, l, 1);
+        const float from_left = __shfl_up_sync(wmask, r, 1);
+        const float tot = mid + (has_right ? from_right : 0.0f) + (has_left ? from_left : 0.0f);
+        const long long qo = (long long)q * G.vstride;
+        if (bc >= 0 && tot != 0.0f) atomicAdd(&T.dfield[bc + qo], (double)tot);
+        if (bl >= 0 && l != 0.0f) atomicAdd(&T.dfield[bl + qo], (double)l);
+        if (bR >= 0 && r != 0.0f) atomicAdd(&T.dfield[bR + qo], (double)r);
+      }
     }
   }
 }
 
-size_t cellacc_smem(int mode, int tj, int nx1, int three_d) {
-  const int WN = (three_d ? 3 : 1) * (tj + 2) * (nx1 + 2);
-  size_t s = 0;
-  if (mode != MODE_QP) s += (size_t)WN * 16;
-  s += (size_t)tile_ncomp(mode) * WN * 8;
-  return s;
+size_t tile_smem(int mode, int tj, int nx1, int chunk) {
+  const int nct = tj * nx1;
+  return (((size_t)(nct + 1) * 4 + 15) & ~(size_t)15) + (size_t)tile_nfield(mode) * chunk * 4;
 }
-
 
 // ---- kernel timing ------------------------------------------------------------------------
 struct Timing {
@@ -814,96 +769,61 @@ struct Scope {
 };
 
 struct Cfg {
-  int tj, chunk, tpp, variant;
+  int tj, chunk, tpp;
 };
 
 bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   const int nx1 = ms.nx1, nx2 = ms.multi_d ? ms.nx2 : 1;
-  const int wk = ms.three_d ? 3 : 1;
-  cf.variant = mp->variant;
+  if (mp->variant != 0 || nx1 > kMaxTileThreads) return false;
   int tj = mp->rows_per_tile;
-  if (cf.variant == 0) {
-    // one thread per source cell: tiles of up to 256 cells
-    if (tj <= 0) {
-      tj = 1;
-      for (int t = nx2; t >= 1; --t)
-        if (nx2 % t == 0 && t * nx1 <= 256) { tj = t; break; }
-    }
-    if (nx2 % tj != 0 || tj * nx1 > 256) return false;
-  } else {
-    if (tj <= 0) {
-      tj = 1;
-      for (int t = nx2; t >= 1; --t)
-        if (nx2 % t == 0 && wk * t * nx1 <= 384 && t * nx1 <= 128 * (ms.three_d ? 1 : 3)) { tj = t; break; }
-    }
-    if (nx2 % tj != 0 || wk * tj * nx1 > kMaxTileThreads) return false;
+  if (tj <= 0) {
+    tj = 1;
+    for (int t = nx2; t >= 1; --t)
+      if (nx2 % t == 0 && t * nx1 <= 128) { tj = t; break; }
   }
+  if (nx2 % tj != 0 || tj * nx1 > kMaxTileThreads) return false;
   cf.tj = tj;
-  cf.chunk = mp->chunk > 0 ? mp->chunk : 1024;
-  if (cf.chunk > 2048) return false;
+  cf.chunk = mp->chunk > 0 ? mp->chunk : 2048;
+  if (cf.chunk < 64 || cf.chunk > 8192 || (cf.chunk & 3)) return false;
   cf.tpp = nx2 / tj;
+  // every tile form must fit the 227 KiB of shared memory a CTA can have (less the barrier)
+  for (int mode = MODE_QP; mode <= MODE_KICK; ++mode)
+    if (tile_smem(mode, tj, nx1, cf.chunk) > 227 * 1024 - 256) return false;
   return true;
 }
 
-template <int MODE>
-int launch_tile(const MState &S, const Geo &G, const Cfg &cf, TileArgs T, cudaStream_t st) {
-  T.tj = cf.tj; T.chunk = cf.chunk; T.tpp = cf.tpp;
+template <int MODE, int D3>
+int launch_tile_d(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &T, cudaStream_t st) {
   const long long tiles = (long long)G.nmb * G.nx3 * cf.tpp;
-  if (cf.variant == 0) {
-    const size_t sm = cellacc_smem(MODE, cf.tj, G.nx1, G.three_d);
-    static size_t configured0 = 0;
-    if (sm > 48 * 1024 && sm > configured0) {
-      cudaFuncSetAttribute(k_cellacc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      configured0 = sm;
-    }
-    k_cellacc<MODE><<<(unsigned)tiles, cf.tj * G.nx1, sm, st>>>(S, G, T);
-    return dustb_host::launch_status("mixed cell tile");
-  }
-  const size_t sm = tile_smem(MODE, cf.tj, G.nx1, G.three_d, cf.chunk);
+  const size_t sm = tile_smem(MODE, cf.tj, G.nx1, cf.chunk);
   static size_t configured = 0;
   if (sm > 48 * 1024 && sm > configured) {
-    cudaFuncSetAttribute(k_tile<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k_tile<MODE, D3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     configured = sm;
   }
-  const int threads = (G.three_d ? 3 : 1) * cf.tj * G.nx1;
-  k_tile<MODE><<<(unsigned)tiles, threads, sm, st>>>(S, G, T);
+  k_tile<MODE, D3><<<(unsigned)tiles, cf.tj * G.nx1, sm, st>>>(cur, G, T);
   return dustb_host::launch_status("mixed tile");
 }
 
-int build_csr(const MState &S, const dustb_mesh &ms, int n, cudaStream_t st) {
-  return csr_build(S.cell, n, ncell_of(ms), S.cstart, S.order, S.cursor, S.bsum, true, st);
+template <int MODE>
+int launch_tile(const MState &S, const PBuf &cur, const Geo &G, const Cfg &cf, TileArgs T,
+                cudaStream_t st) {
+  T.tj = cf.tj; T.chunk = cf.chunk; T.tpp = cf.tpp; T.cstart = S.cstart;
+  return G.three_d ? launch_tile_d<MODE, 1>(G, cf, cur, T, st)
+                   : launch_tile_d<MODE, 0>(G, cf, cur, T, st);
 }
 
-int permute(const MState &S, int n, cudaStream_t st) {
-  if (n <= 0) return DUSTB_OK;
-  int *ti = (int *)S.tmp;
-  k_gather_i<<<nblk(n), kT, 0, st>>>(S.cell, S.order, n, ti);
-  cudaMemcpyAsync(S.cell, ti, 4 * (size_t)n, cudaMemcpyDeviceToDevice, st);
-  k_gather_i<<<nblk(n), kT, 0, st>>>(S.pid, S.order, n, ti);
-  cudaMemcpyAsync(S.pid, ti, 4 * (size_t)n, cudaMemcpyDeviceToDevice, st);
-  MState T = S;
-  float **fp[kNFloat];
-  float_arrays(T, fp);
-  float *fs[kNFloat];
-  for (int f = 0; f < kNFloat; ++f) {
-    fs[f] = *fp[f];
-    if (!fs[f]) return DUSTB_EINVAL;
-  }
-  for (int f = 0; f < kNFloat; ++f) {
-    k_gather_f<<<nblk(n), kT, 0, st>>>(fs[f], S.order, n, S.tmp);
-    cudaMemcpyAsync(fs[f], S.tmp, 4 * (size_t)n, cudaMemcpyDeviceToDevice, st);
-  }
-  return dustb_host::launch_status("mixed permute");
-}
-
-// sort the shadow by cell: histogram, CSR, permutation
-int sort_shadow(const MState &S, const dustb_mesh &ms, int n, cudaStream_t st) {
+// sort copy src into dst by the cells it holds (histogram, scan, moves)
+int sort_into(const MState &S, const PBuf &src, const PBuf &dst, const dustb_mesh &ms, int n,
+              cudaStream_t st) {
   const long long ncell = ncell_of(ms);
   cudaMemsetAsync(S.cstart, 0, 4 * (size_t)(ncell + 1), st);
-  if (n > 0) k_hist<<<nblk(n), kT, 0, st>>>(S.cell, n, S.cstart);
-  int rc = build_csr(S, ms, n, st);
+  if (n > 0) k_hist<<<nblk(n), kT, 0, st>>>(src.cell, n, S.cstart);
+  int rc = exclusive_scan(S.cstart, ncell + 1, S.bsum, st);
   if (rc) return rc;
-  return permute(S, n, st);
+  cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)(ncell + 1), cudaMemcpyDeviceToDevice, st);
+  if (n > 0) k_sortmove<<<nblk(n), kT, 0, st>>>(src, dst, n, S.cursor);
+  return dustb_host::launch_status("mixed sort");
 }
 
 bool params_ok(const dustb_ctx *c, const dustb_mixed_params *mp) {
@@ -934,11 +854,15 @@ int dustb_mixed_import(const dustb_ctx *c, const dustb_mixed_params *mp, void *w
   cudaStream_t st = (cudaStream_t)stream;
   Geo G = make_geo(c, mp);
   const int n = c->part.npart;
-  cudaMemsetAsync(S.cstart, 0, 4 * (size_t)(ncell_of(c->mesh) + 1), st);
-  if (n > 0) k_import<<<nblk(n), kT, 0, st>>>(c->part.pr, c->part.pi, c->part.stride, n, S, G, c->err);
-  int rc = build_csr(S, c->mesh, n, st);
+  const long long ncell = ncell_of(c->mesh);
+  cudaMemsetAsync(S.cstart, 0, 4 * (size_t)(ncell + 1), st);
+  if (n > 0)
+    k_import<<<nblk(n), kT, 0, st>>>(c->part.pr, c->part.pi, c->part.stride, n, S.B, S.cstart, G, c->err);
+  int rc = exclusive_scan(S.cstart, ncell + 1, S.bsum, st);
   if (rc) return rc;
-  return permute(S, n, st);
+  cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)(ncell + 1), cudaMemcpyDeviceToDevice, st);
+  if (n > 0) k_sortmove<<<nblk(n), kT, 0, st>>>(S.B, S.A, n, S.cursor);
+  return dustb_host::launch_status("mixed_import");
 }
 
 int dustb_mixed_export(const dustb_ctx *c, const dustb_mixed_params *mp, void *ws,
@@ -949,7 +873,7 @@ int dustb_mixed_export(const dustb_ctx *c, const dustb_mixed_params *mp, void *w
   Geo G = make_geo(c, mp);
   const int n = c->part.npart;
   if (n > 0)
-    k_export<<<nblk(n), kT, 0, (cudaStream_t)stream>>>(c->part.pr, c->part.pi, c->part.stride, n, S, G);
+    k_export<<<nblk(n), kT, 0, (cudaStream_t)stream>>>(c->part.pr, c->part.pi, c->part.stride, n, S.A, G);
   return dustb_host::launch_status("mixed_export");
 }
 
@@ -958,7 +882,12 @@ int dustb_mixed_sort(const dustb_ctx *c, const dustb_mixed_params *mp, void *ws,
   if (!params_ok(c, mp)) return DUSTB_EINVAL;
   MState S;
   if (!carve(c->mesh, c->part.npart, ws, bytes, S, nullptr)) return DUSTB_ESCRATCH;
-  return sort_shadow(S, c->mesh, c->part.npart, (cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = c->part.npart;
+  int rc = sort_into(S, S.A, S.B, c->mesh, n, st);
+  if (rc) return rc;
+  if (n > 0) k_copy_buf<<<nblk(n), kT, 0, st>>>(S.B, S.A, n);
+  return dustb_host::launch_status("mixed_sort");
 }
 
 int dustb_mixed_timing(int enable) {
@@ -988,6 +917,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
   if (!params_ok(c, mp) || !co || !(co->dt > 0.0)) return DUSTB_EINVAL;
   if (co->sh[0] != 0.0 || co->sh[1] != 0.0) return DUSTB_EUNSUP;   // shear shift: FP64 form
   if (c->mesh.x3bc != DUSTB_X3_PERIODIC) return DUSTB_EUNSUP;       // physical x3: FP64 form
+  if (!c->mesh.multi_d) return DUSTB_EUNSUP;                        // 1-D: FP64 form
   MState S;
   if (!carve(c->mesh, c->part.npart, ws, bytes, S, nullptr)) return DUSTB_ESCRATCH;
   Cfg cf;
@@ -1008,31 +938,40 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
   int rc;
 #define RUN(x) do { rc = (x); if (rc) return rc; } while (0)
   for (int stage = 1; stage <= 2; ++stage) {
+    // stage 1 moves the shadow from A to B, stage 2 back to A
+    const PBuf &src = (stage == 1) ? S.A : S.B;
+    const PBuf &cur = (stage == 1) ? S.B : S.A;
     {
       Scope sc(DUSTB_K_CELLS, st);
       if (stage == 1) cudaMemcpyAsync(c->f.u1, c->f.u0, fbytes * c->f.nvar_gas, cudaMemcpyDeviceToDevice, st);
       dustb_cells::gas_rk(c, gam0[stage - 1], gam1[stage - 1], st);
       if (stage == 2 && br) dustb_cells::history(c, atw22 * dt, st);
-      cudaMemsetAsync(S.cstart, 0, 4 * (size_t)(ncell + 1), st);
     }
+    PushArgs P;
+    P.gam0 = (float)gam0[stage - 1]; P.gam1 = (float)gam1[stage - 1];
+    P.atw_dt = (stage == 2) ? (float)(atw22 * dt) : 0.0f;
+    P.bdt = (float)(beta[stage - 1] * dt);
+    for (int a = 0; a < 3; ++a) P.bdx[a] = (float)(beta[stage - 1] * dt * G.inv_dx[a]);
+    P.a_dt = a_dt; P.stage2 = (stage == 2);
+    P.sbox = c->phys.shearing_box; P.strat = c->phys.stratified;
+    P.q = (float)c->phys.qshear; P.om = (float)c->phys.omega0;
+    P.res = (stage == 2 && br && cons) ? c->f.resid : nullptr;
+    P.err = c->err;
     {
       Scope sc(DUSTB_K_PUSH, st);
-      PushArgs P;
-      P.gam0 = (float)gam0[stage - 1]; P.gam1 = (float)gam1[stage - 1];
-      P.atw_dt = (stage == 2) ? (float)(atw22 * dt) : 0.0f;
-      P.bdt = (float)(beta[stage - 1] * dt);
-      for (int a = 0; a < 3; ++a) P.bdx[a] = (float)(beta[stage - 1] * dt * G.inv_dx[a]);
-      P.a_dt = a_dt; P.stage2 = (stage == 2);
-      P.sbox = c->phys.shearing_box; P.strat = c->phys.stratified;
-      P.q = (float)c->phys.qshear; P.om = (float)c->phys.omega0;
-      P.res = (stage == 2 && br && cons) ? c->f.resid : nullptr;
-      P.err = c->err;
-      if (n > 0) k_push<<<nblk(n), kT, 0, st>>>(S, G, n, P);
-      RUN(dustb_host::launch_status("mixed push"));
+      cudaMemsetAsync(S.cstart, 0, 4 * (size_t)(ncell + 1), st);
+      if (n > 0) k_count<<<nblk(n), kT, 0, st>>>(src, S.key, S.cstart, G, n, P);
+      RUN(dustb_host::launch_status("mixed count"));
     }
     {
       Scope sc(DUSTB_K_FILL, st);
-      RUN(build_csr(S, c->mesh, n, st));
+      RUN(exclusive_scan(S.cstart, ncell + 1, S.bsum, st));
+      cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)(ncell + 1), cudaMemcpyDeviceToDevice, st);
+    }
+    {
+      Scope sc(DUSTB_K_PUSH, st);
+      if (n > 0) k_move<<<nblk(n), kT, 0, st>>>(src, cur, S.key, S.cursor, G, n, P);
+      RUN(dustb_host::launch_status("mixed move"));
     }
     TileArgs T{};
     T.a_dt = a_dt; T.err = c->err; T.deposit = 1;
@@ -1040,7 +979,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       Scope sc(DUSTB_K_DEPOSIT_QP, st);
       cudaMemsetAsync(c->f.qdep, 0, fbytes * 5, st);
       T.dfield = c->f.qdep; T.dnvar = 5; T.res = c->f.resid;
-      RUN(launch_tile<MODE_QP>(S, G, cf, T, st));
+      RUN(launch_tile<MODE_QP>(S, cur, G, cf, T, st));
     }
     // the deposits go straight into the owners' active cells and the gathers read ghost
     // cells from their owners, so no ghost exchange of qdep, work, dmom or u* is needed
@@ -1054,7 +993,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
         cudaMemsetAsync(c->f.work, 0, fbytes * 3, st);
         { Scope sc(DUSTB_K_OPERATOR, st);
           T.gfield = c->f.ustar; T.dfield = c->f.work; T.dnvar = 3;
-          RUN(launch_tile<MODE_OP>(S, G, cf, T, st)); }
+          RUN(launch_tile<MODE_OP>(S, cur, G, cf, T, st)); }
         { Scope sc(DUSTB_K_CELLS, st);
           dustb_cells::dc_correct(c, st); }
       }
@@ -1063,7 +1002,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     {
       Scope sc(DUSTB_K_KICK, st);
       T.gfield = c->f.ustar; T.dfield = c->f.dmom; T.dnvar = 3; T.deposit = br;
-      RUN(launch_tile<MODE_KICK>(S, G, cf, T, st));
+      RUN(launch_tile<MODE_KICK>(S, cur, G, cf, T, st));
     }
     if (br) {
       { Scope sc(DUSTB_K_CELLS, st);
@@ -1071,7 +1010,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
         else dustb_cells::pmbr(c, a_dt, st); }
       if (cons && stage == 2 && n > 0) {
         Scope sc(DUSTB_K_CONSISTENT, st);
-        k_consistent_kick<<<nblk(n), kT, 0, st>>>(S, G, n, a_dt, c->f.resid);
+        k_consistent_kick<<<nblk(n), kT, 0, st>>>(cur, G, n, a_dt, c->f.resid);
         RUN(dustb_host::launch_status("mixed consistent kick"));
       }
     }

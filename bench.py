@@ -247,11 +247,10 @@ def run_ours(args, rank, world):
     if args.tune:
         best = None
         nx1, nx2 = ms.nx[0], ms.nx[1]
-        # (variant, rows per tile, particles per pass): one thread per source cell with
-        # tiles of up to 256 cells, or the staged tiles of up to 384 threads
-        cands = [(0, r, 0) for r in (1, 2, 4, 8) if nx2 % r == 0 and r * nx1 <= 256]
-        cands += [(1, r, ch) for r in (1, 2) if nx2 % r == 0 and 3 * r * nx1 <= 384
-                  for ch in (1024, 2048)]
+        # (variant, rows per tile, particles per pass): one thread per source cell, tiles
+        # of up to 256 cells, particle ranges copied in passes of 1016..4088
+        cands = [(0, r, ch) for r in (1, 2, 4) if nx2 % r == 0 and r * nx1 <= 256
+                 for ch in (1024, 2048, 4096)]
         for var, rows, chunk in cands:
             mx.set_tiles(rows, chunk, var)
             try:

@@ -60,6 +60,7 @@ enum { DUSTB_X3_PERIODIC = 0, DUSTB_X3_REFLECT = 1, DUSTB_X3_OUTFLOW = 2 };
 #define DUSTB_ERR_PGID      0x8u  /* PGID outside the pack */
 #define DUSTB_ERR_TSTOP     0x10u /* stopping time not finite and positive (dust_newdt.cpp:53) */
 #define DUSTB_ERR_WINDOW    0x20u /* fused kernels: a particle outside its tile window */
+#define DUSTB_ERR_TIMEOUT   0x40u /* a bounded wait on an asynchronous copy ran out */
 
 /* host return codes */
 #define DUSTB_OK          0
@@ -256,17 +257,21 @@ int dustb_pc2_cycle(const dustb_ctx *ctx, double dt, double *chi_max, double *x3
  * register, register displacement x1 - x (cells), drag rate, stopping time and mass.  The
  * gas and the deposit fields stay the reference's FP64 arrays of dustb_ctx (per-cell
  * accumulators, solves and the gas update in FP64); weights, gathers and kicks run in FP32
- * with the drag factor a/(t_s + a) formed in FP64.  Deposits are accumulated per source
- * cell in registers, summed into an FP64 shared-memory tile and added to the FP64 field
- * once per tile cell.  All the workspace is the caller's (dustb_mixed_workspace_bytes).
+ * with the drag factor a/(t_s + a) formed in FP64.  The shadow is kept sorted by cell at
+ * every stage (two copies; the push moves each particle to its slot in the other), so the
+ * particles of a CTA's tile of cells are one contiguous range, copied into shared memory
+ * with bulk copies.  One thread per source cell accumulates its particles' 27-point
+ * deposits in registers; neighbouring threads combine the contributions that land on the
+ * same cell and add them to the FP64 field.  All the workspace is the caller's
+ * (dustb_mixed_workspace_bytes).
  * No reference counterpart: the reference keeps only the FP64 SoA. */
 
 typedef struct dustb_mixed_params {
   double dx[3];            /* uniform cell size (single-level mesh) */
   int rows_per_tile;       /* 0: chosen by the library; else rows of nx1 cells per CTA tile */
-  int chunk;               /* 0: default; particles staged per CTA pass (<= 2048) */
-  int variant;             /* deposit kernels: 0 one thread per source cell (default),
-                              1 particles staged in shared memory per tile */
+  int chunk;               /* 0: default (2048); shared-memory columns per CTA pass, a
+                              multiple of 4 in 64..8192 (chunk - 8 particles per pass) */
+  int variant;             /* deposit kernels: 0 (the only one) */
 } dustb_mixed_params;
 
 long long dustb_mixed_workspace_bytes(const dustb_mesh *mesh, int npart);

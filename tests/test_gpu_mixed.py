@@ -124,11 +124,11 @@ def test_mixed_matches_oracle():
     np.testing.assert_array_equal(mx.dev.host("pi")[0], o.st.pi[0, :n])
 
 
-@pytest.mark.parametrize("variant,rows,chunk", [(1, 1, 64), (1, 2, 128), (1, 4, 2048), (1, 8, 512),
-                                                (0, 1, 0), (0, 2, 0), (0, 8, 0)])
+@pytest.mark.parametrize("variant,rows,chunk", [(0, 1, 64), (0, 2, 128), (0, 4, 2048), (0, 8, 512),
+                                                (0, 1, 0), (0, 2, 68), (0, 1, 6144)])
 def test_tile_shapes_agree(variant, rows, chunk):
-    """The autotuner's knobs (kernel variant, rows per tile, particles per pass) change only
-    the order of the FP32 partial sums."""
+    """The autotuner's knobs (rows per tile, particles per pass) change only the order of the
+    FP32 partial sums (64 columns: 56 particles per pass, many passes per tile)."""
     from athenak_b200.mixed import MixedDust
     c = CASES["3d_random"]
     ms = uniform_mesh(*c["mesh"])
