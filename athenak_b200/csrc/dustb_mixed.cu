@@ -519,7 +519,7 @@ __device__ __forceinline__ long long cell_at(const Geo &G, int m, int nvar, int 
 }
 __device__ __forceinline__ float2 dup(float x) { return make_float2(x, x); }
 
-template <int MODE, int D3>
+template <int MODE, int D3, int SCHEME>
 __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, TileArgs T) {
   constexpr int NC = (MODE == MODE_QP) ? 4 : 3;    // deposited values per particle
   constexpr int NF = (MODE == MODE_OP) ? 5 : 8;    // fields copied: ox oy oz cc m [vx vy vz]
@@ -554,10 +554,15 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
 #pragma unroll
     for (int c = 0; c < WK; ++c)
 #pragma unroll
-      for (int b = 0; b < 3; ++b)
+      for (int b = 0; b < 3; ++b) {
+        // this cell's column of the (c, b) row; its x neighbours are the next words unless
+        // the cell ends the block's row
+        const int kk = D3 ? k - 1 + c : 0, jj = j0 + cj_l - 1 + b;
+        const long long rb = cell_at(G, m, 3, kk, jj, ci_l);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          const long long at = cell_at(G, m, 3, D3 ? k - 1 + c : 0, j0 + cj_l - 1 + b, ci_l - 1 + a);
+          long long at = (rb >= 0) ? rb + (a - 1) : -1;
+          if ((a == 0 && ci_l == 0) || (a == 2 && ci_l == nx1 - 1)) at = cell_at(G, m, 3, kk, jj, ci_l - 1 + a);
           gxy[c][b][a] = make_float2(0.0f, 0.0f);
           gz[c][b][a] = 0.0f;
           if (at >= 0) {
@@ -565,6 +570,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
             gz[c][b][a] = (float)T.gfield[at + 2 * G.vstride];
           }
         }
+      }
   }
   __syncthreads();
   const int P0 = s_cs[0], P1 = s_cs[nct];
@@ -613,9 +619,9 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
     for (int r = lo; r < hi; ++r) {
       const float c32 = s_f[3 * CH + r], mass = s_f[4 * CH + r];
       float wx_[3], wy_[3], wz_[3];
-      wts(G.scheme, s_f[r], wx_);
-      wts(G.scheme, s_f[CH + r], wy_);
-      if (D3) wts(G.scheme, s_f[2 * CH + r], wz_);
+      wts(SCHEME, s_f[r], wx_);
+      wts(SCHEME, s_f[CH + r], wy_);
+      if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
       float2 q01, q23 = make_float2(0.0f, 0.0f);   // the deposited values
       if (MODE == MODE_QP) {
         const float mc = mass * c32 * inv_vol;
@@ -721,8 +727,10 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
       const int jj = j0 + cj_l - 1 + b;
       // the row's target cells: this cell's column, and the outward ones of the end lanes
       const long long bc = cell_at(G, m, T.dnvar, kk, jj, ci_l);
-      const long long bl = has_left ? -1 : cell_at(G, m, T.dnvar, kk, jj, ci_l - 1);
-      const long long bR = has_right ? -1 : cell_at(G, m, T.dnvar, kk, jj, ci_l + 1);
+      const long long bl = has_left ? -1
+                         : (ci_l > 0 ? (bc >= 0 ? bc - 1 : -1) : cell_at(G, m, T.dnvar, kk, jj, -1));
+      const long long bR = has_right ? -1
+                         : (ci_l + 1 < nx1 ? (bc >= 0 ? bc + 1 : -1) : cell_at(G, m, T.dnvar, kk, jj, nx1));
 #pragma unroll
       for (int q = 0; q < NC; ++q) {
         const float l = val(c, b, 0, q), mid = val(c, b, 1, q), r = val(c, b, 2, q);
@@ -792,16 +800,16 @@ bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   return true;
 }
 
-template <int MODE, int D3>
+template <int MODE, int D3, int SCHEME>
 int launch_tile_d(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &T, cudaStream_t st) {
   const long long tiles = (long long)G.nmb * G.nx3 * cf.tpp;
   const size_t sm = tile_smem(MODE, cf.tj, G.nx1, cf.chunk);
   static size_t configured = 0;
   if (sm > 48 * 1024 && sm > configured) {
-    cudaFuncSetAttribute(k_tile<MODE, D3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k_tile<MODE, D3, SCHEME>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     configured = sm;
   }
-  k_tile<MODE, D3><<<(unsigned)tiles, cf.tj * G.nx1, sm, st>>>(cur, G, T);
+  k_tile<MODE, D3, SCHEME><<<(unsigned)tiles, cf.tj * G.nx1, sm, st>>>(cur, G, T);
   return dustb_host::launch_status("mixed tile");
 }
 
@@ -809,8 +817,15 @@ template <int MODE>
 int launch_tile(const MState &S, const PBuf &cur, const Geo &G, const Cfg &cf, TileArgs T,
                 cudaStream_t st) {
   T.tj = cf.tj; T.chunk = cf.chunk; T.tpp = cf.tpp; T.cstart = S.cstart;
-  return G.three_d ? launch_tile_d<MODE, 1>(G, cf, cur, T, st)
-                   : launch_tile_d<MODE, 0>(G, cf, cur, T, st);
+  // one kernel per dimensionality and deposit scheme (no per-particle scheme selection)
+  if (G.three_d) {
+    if (G.scheme == 2) return launch_tile_d<MODE, 1, 2>(G, cf, cur, T, st);
+    if (G.scheme == 1) return launch_tile_d<MODE, 1, 1>(G, cf, cur, T, st);
+    return launch_tile_d<MODE, 1, 0>(G, cf, cur, T, st);
+  }
+  if (G.scheme == 2) return launch_tile_d<MODE, 0, 2>(G, cf, cur, T, st);
+  if (G.scheme == 1) return launch_tile_d<MODE, 0, 1>(G, cf, cur, T, st);
+  return launch_tile_d<MODE, 0, 0>(G, cf, cur, T, st);
 }
 
 // sort copy src into dst by the cells it holds (histogram, scan, moves)

@@ -250,7 +250,7 @@ def run_ours(args, rank, world):
         # (variant, rows per tile, particles per pass): one thread per source cell, tiles
         # of up to 256 cells, particle ranges copied in passes of 1016..4088
         cands = [(0, r, ch) for r in (1, 2, 4) if nx2 % r == 0 and r * nx1 <= 256
-                 for ch in (1024, 2048, 4096)]
+                 for ch in (1024, 1152, 2048, 2176, 2304)]
         for var, rows, chunk in cands:
             mx.set_tiles(rows, chunk, var)
             try:
