@@ -507,7 +507,9 @@ struct TileArgs {
   unsigned *err;
 };
 
-__host__ __device__ inline int tile_nfield(int mode) { return mode == MODE_OP ? 5 : 8; }
+// shared rows of a tile pass: the copied fields, then (operator, kick) the per-particle
+// values of the gather phase in rows 5..7
+constexpr int kTileRows = 8;
 
 // the index of variable 0 of block-local cell (kk, jj, ii) of block m in a field of nvar
 // variables, or -1 if no block owns it; a cell one beyond the block maps to the owning
@@ -519,11 +521,174 @@ __device__ __forceinline__ long long cell_at(const Geo &G, int m, int nvar, int 
 }
 __device__ __forceinline__ float2 dup(float x) { return make_float2(x, x); }
 
+// the 27-point sums of one source cell's particles: values 0, 1 as a packed pair; values 2, 3
+// as a pair (Q/P) or value 2 alone (operator, kick)
+template <int MODE, int D3>
+struct CellSums {
+  static constexpr int WK = D3 ? 3 : 1;
+  float2 a01[WK][3][3], a23[WK][3][3];
+  float a2[WK][3][3];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int c = 0; c < WK; ++c)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          a01[c][b][a] = make_float2(0.0f, 0.0f);
+          if (MODE == MODE_QP) a23[c][b][a] = make_float2(0.0f, 0.0f);
+          else a2[c][b][a] = 0.0f;
+        }
+  }
+  __device__ __forceinline__ float val(int c, int b, int a, int q) const {
+    return q == 0 ? a01[c][b][a].x : q == 1 ? a01[c][b][a].y
+         : (MODE == MODE_QP ? (q == 2 ? a23[c][b][a].x : a23[c][b][a].y) : a2[c][b][a]);
+  }
+  // sum_cba += wz_c wy_b (wx_a q): the x weights folded into the values first
+  __device__ __forceinline__ void add(const float wx[3], const float wy[3], const float wz[3],
+                                      float2 q01, float2 q23) {
+    float2 s01[3], s23[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      s01[a] = __fmul2_rn(dup(wx[a]), q01);
+      if (MODE == MODE_QP) s23[a] = __fmul2_rn(dup(wx[a]), q23);
+      else s23[a].x = wx[a] * q23.x;
+    }
+#pragma unroll
+    for (int c = 0; c < WK; ++c) {
+      const float wzc = D3 ? wz[c] : 1.0f;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const float wzy = wzc * wy[b];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          a01[c][b][a] = __ffma2_rn(dup(wzy), s01[a], a01[c][b][a]);
+          if (MODE == MODE_QP) a23[c][b][a] = __ffma2_rn(dup(wzy), s23[a], a23[c][b][a]);
+          else a2[c][b][a] = fmaf(wzy, s23[a].x, a2[c][b][a]);
+        }
+      }
+    }
+  }
+};
+
+// the gather field on the 27 cells around one source cell, FP32 (x, y as a packed pair);
+// cells beyond the block read the owning neighbour's active cell (the copy exchange of u*'s
+// ghost cells folded into the load)
+template <int D3>
+struct GatherWindow {
+  static constexpr int WK = D3 ? 3 : 1;
+  float2 xy[WK][3][3];
+  float z[WK][3][3];
+  __device__ __forceinline__ void load(const Geo &G, const double *f, int m, int k, int jrow,
+                                       int ci) {
+#pragma unroll
+    for (int c = 0; c < WK; ++c)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        // this cell's column of the (c, b) row; its x neighbours are the next words unless
+        // the cell ends the block's row
+        const int kk = D3 ? k - 1 + c : 0, jj = jrow - 1 + b;
+        const long long rb = cell_at(G, m, 3, kk, jj, ci);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          long long at = (rb >= 0) ? rb + (a - 1) : -1;
+          if ((a == 0 && ci == 0) || (a == 2 && ci == G.nx1 - 1)) at = cell_at(G, m, 3, kk, jj, ci - 1 + a);
+          xy[c][b][a] = make_float2(0.0f, 0.0f);
+          z[c][b][a] = 0.0f;
+          if (at >= 0) {
+            xy[c][b][a] = make_float2((float)f[at], (float)f[at + G.vstride]);
+            z[c][b][a] = (float)f[at + 2 * G.vstride];
+          }
+        }
+      }
+  }
+  // u = sum over (c, b) of wz_c wy_b (sum over a of wx_a g_cba)
+  __device__ __forceinline__ void gather(const float wx[3], const float wy[3], const float wz[3],
+                                         float2 &uxy, float &uz) const {
+    uxy = make_float2(0.0f, 0.0f);
+    uz = 0.0f;
+#pragma unroll
+    for (int c = 0; c < WK; ++c) {
+      const float wzc = D3 ? wz[c] : 1.0f;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        float2 txy = __fmul2_rn(dup(wx[0]), xy[c][b][0]);
+        float tz = wx[0] * z[c][b][0];
+#pragma unroll
+        for (int a = 1; a < 3; ++a) {
+          txy = __ffma2_rn(dup(wx[a]), xy[c][b][a], txy);
+          tz = fmaf(wx[a], z[c][b][a], tz);
+        }
+        const float wzy = wzc * wy[b];
+        uxy = __ffma2_rn(dup(wzy), txy, uxy);
+        uz = fmaf(wzy, tz, uz);
+      }
+    }
+  }
+};
+
+// the sums of every source cell of the tile, staged in shared memory as float4 (values 0..3)
+// at [(c*3 + b)*3 + a][cell], for the window pass below
+template <int MODE, int D3>
+__device__ __forceinline__ void stage_sums(const CellSums<MODE, D3> &A, float4 *s_acc, int cl,
+                                           int nct) {
+  constexpr int WK = D3 ? 3 : 1;
+#pragma unroll
+  for (int c = 0; c < WK; ++c)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        s_acc[((c * 3 + b) * 3 + a) * nct + cl] =
+            make_float4(A.val(c, b, a, 0), A.val(c, b, a, 1), A.val(c, b, a, 2),
+                        MODE == MODE_QP ? A.val(c, b, a, 3) : 0.0f);
+}
+
+// adds the tile's deposit window to the FP64 field, one add per window cell and value: a
+// window cell (z plane c, row wy, column wx) sums the staged contributions of the up to 9
+// source cells of its plane that reach it; window cells beyond the block go to the owning
+// neighbour's active cell (the additive ghost exchange folded into the add)
+template <int MODE, int D3>
+__device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, const TileArgs &T,
+                                           int m, int k, int j0, int tj) {
+  constexpr int NC = (MODE == MODE_QP) ? 4 : 3;
+  constexpr int WK = D3 ? 3 : 1;
+  const int nx1 = G.nx1, nct = tj * nx1;
+  const int WI = nx1 + 2, WJ = tj + 2, nplane = WJ * WI;
+  for (int t = threadIdx.x; t < WK * nplane; t += blockDim.x) {
+    const int c = t / nplane, rem = t - c * nplane;
+    const int wy = rem / WI, wx = rem - wy * WI;
+    const long long at = cell_at(G, m, T.dnvar, D3 ? k - 1 + c : 0, j0 - 1 + wy, wx - 1);
+    if (at < 0) continue;
+    float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const int cj = wy - b;                       // source row reaching this row with offset b
+      if (cj < 0 || cj >= tj) continue;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int ci = wx - a;                     // source column reaching this column
+        if (ci < 0 || ci >= nx1) continue;
+        const float4 v = s_acc[((c * 3 + b) * 3 + a) * nct + cj * nx1 + ci];
+        s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+      }
+    }
+    double *f = T.dfield + at;
+    if (s.x != 0.0f) atomicAdd(f, (double)s.x);
+    if (s.y != 0.0f) atomicAdd(f + G.vstride, (double)s.y);
+    if (s.z != 0.0f) atomicAdd(f + 2 * G.vstride, (double)s.z);
+    if (NC > 3 && s.w != 0.0f) atomicAdd(f + 3 * G.vstride, (double)s.w);
+  }
+}
+
+// One CTA per tile of tj rows of one plane, one thread per source cell.  Q/P: the sums of a
+// cell's particles are kept in registers over all passes.  Operator and kick: per pass, a
+// gather phase (the 27 gather values in registers) writes each particle's deposit value (or
+// velocity change) into its column, then a deposit phase sums them and adds them to the
+// field; the gather values and the sums are never live together.
 template <int MODE, int D3, int SCHEME>
 __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, TileArgs T) {
-  constexpr int NC = (MODE == MODE_QP) ? 4 : 3;    // deposited values per particle
   constexpr int NF = (MODE == MODE_OP) ? 5 : 8;    // fields copied: ox oy oz cc m [vx vy vz]
-  constexpr int WK = D3 ? 3 : 1;                   // z planes of the stencil
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   const int nx1 = G.nx1, tj = T.tj;
@@ -537,58 +702,19 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
   const int c0 = encode(G, m, k, j0, 0);
   const int CH = T.chunk;                          // buffer columns (multiple of 4)
   int *s_cs = (int *)smem;                         // [nct + 1] cell ranges
-  float *s_f = (float *)(smem + (((size_t)(nct + 1) * 4 + 15) & ~(size_t)15));  // [NF][CH]
+  float *s_f = (float *)(smem + (((size_t)(nct + 1) * 4 + 15) & ~(size_t)15));  // [8][CH]
+  float4 *s_acc = (float4 *)s_f;                   // the staged sums, after the rows
   const int cl = threadIdx.x;                      // this thread's source cell
   const int cj_l = cl / nx1, ci_l = cl - cj_l * nx1;
-  const int lane = threadIdx.x & 31;
-  const int wlanes = min(32, nct - (int)(threadIdx.x & ~31u));
+  const int jrow = j0 + cj_l;
 
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   for (int x = threadIdx.x; x <= nct; x += blockDim.x) s_cs[x] = T.cstart[c0 + x];
-  // the gather field on the 27 cells around this cell, FP32, in registers; cells beyond the
-  // block read the owning neighbour's active cell (the copy exchange of u*'s ghost cells)
-  // (x, y components as packed FP32 pairs)
-  float2 gxy[WK][3][3];
-  float gz[WK][3][3];
-  if (MODE != MODE_QP) {
-#pragma unroll
-    for (int c = 0; c < WK; ++c)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        // this cell's column of the (c, b) row; its x neighbours are the next words unless
-        // the cell ends the block's row
-        const int kk = D3 ? k - 1 + c : 0, jj = j0 + cj_l - 1 + b;
-        const long long rb = cell_at(G, m, 3, kk, jj, ci_l);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          long long at = (rb >= 0) ? rb + (a - 1) : -1;
-          if ((a == 0 && ci_l == 0) || (a == 2 && ci_l == nx1 - 1)) at = cell_at(G, m, 3, kk, jj, ci_l - 1 + a);
-          gxy[c][b][a] = make_float2(0.0f, 0.0f);
-          gz[c][b][a] = 0.0f;
-          if (at >= 0) {
-            gxy[c][b][a] = make_float2((float)T.gfield[at], (float)T.gfield[at + G.vstride]);
-            gz[c][b][a] = (float)T.gfield[at + 2 * G.vstride];
-          }
-        }
-      }
-  }
   __syncthreads();
   const int P0 = s_cs[0], P1 = s_cs[nct];
   const int c_lo = s_cs[cl], c_hi = s_cs[cl + 1];  // this cell's particles
-  // the 27-point sums of this cell's particles: values 0, 1 as packed pairs; values 2, 3 as
-  // a pair (Q/P) or value 2 alone (operator, kick)
-  float2 acc01[WK][3][3], acc23[WK][3][3];
-  float acc2[WK][3][3];
-#pragma unroll
-  for (int c = 0; c < WK; ++c)
-#pragma unroll
-    for (int b = 0; b < 3; ++b)
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        acc01[c][b][a] = make_float2(0.0f, 0.0f);
-        acc23[c][b][a] = make_float2(0.0f, 0.0f);
-        acc2[c][b][a] = 0.0f;
-      }
+  CellSums<MODE, D3> qp;                           // Q/P: kept over all passes
+  if (MODE == MODE_QP) qp.zero();
   float qt = 0.0f;
   const float inv_vol = (float)(1.0 / G.vol);
   const float inv_adt = (float)(1.0 / T.a_dt);
@@ -607,6 +733,8 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
 #pragma unroll
       for (int f = 0; f < NF; ++f) bulk_copy(s_f + f * CH, S.f[fl[f]] + a0, bytes, &bar);
     }
+    GatherWindow<D3> win;
+    if (MODE != MODE_QP) win.load(G, T.gfield, m, k, jrow, ci_l);   // while the copies fly
     const bool ok = mbar_wait(&bar, parity, T.err);
     parity ^= 1u;
     if (__syncthreads_or(!ok)) {
@@ -616,88 +744,68 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
     }
     // this cell's particles in the pass, at columns lo..hi of the rows
     const int lo = max(c_lo, cb) - a0, hi = min(c_hi, ce) - a0;
-    for (int r = lo; r < hi; ++r) {
-      const float c32 = s_f[3 * CH + r], mass = s_f[4 * CH + r];
-      float wx_[3], wy_[3], wz_[3];
-      wts(SCHEME, s_f[r], wx_);
-      wts(SCHEME, s_f[CH + r], wy_);
-      if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
-      float2 q01, q23 = make_float2(0.0f, 0.0f);   // the deposited values
-      if (MODE == MODE_QP) {
-        const float mc = mass * c32 * inv_vol;
-        q01 = make_float2(mc, mc * s_f[5 * CH + r]);
-        q23 = make_float2(mc * s_f[6 * CH + r], mc * s_f[7 * CH + r]);
+    if (MODE == MODE_QP) {
+      for (int r = lo; r < hi; ++r) {
+        float wx_[3], wy_[3], wz_[3];
+        wts(SCHEME, s_f[r], wx_);
+        wts(SCHEME, s_f[CH + r], wy_);
+        if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
+        const float mc = s_f[4 * CH + r] * s_f[3 * CH + r] * inv_vol;
         qt += mc;
-      } else {
-        // u = sum over (c, b) of wz_c wy_b (sum over a of wx_a g_cba)
-        float2 uxy = make_float2(0.0f, 0.0f);
-        float uz = 0.0f;
-#pragma unroll
-        for (int c = 0; c < WK; ++c) {
-          const float wzc = D3 ? wz_[c] : 1.0f;
-#pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            float2 txy = __fmul2_rn(dup(wx_[0]), gxy[c][b][0]);
-            float tz = wx_[0] * gz[c][b][0];
-#pragma unroll
-            for (int a = 1; a < 3; ++a) {
-              txy = __ffma2_rn(dup(wx_[a]), gxy[c][b][a], txy);
-              tz = fmaf(wx_[a], gz[c][b][a], tz);
-            }
-            const float wzy = wzc * wy_[b];
-            uxy = __ffma2_rn(dup(wzy), txy, uxy);
-            uz = fmaf(wzy, tz, uz);
-          }
-        }
-        const float ux = uxy.x, uy = uxy.y;
+        qp.add(wx_, wy_, wz_, make_float2(mc, mc * s_f[5 * CH + r]),
+               make_float2(mc * s_f[6 * CH + r], mc * s_f[7 * CH + r]));
+      }
+    } else {
+      // gather phase: the operator's m c u / V, or the kick's velocity change, into rows 5..7
+      for (int r = lo; r < hi; ++r) {
+        float wx_[3], wy_[3], wz_[3];
+        wts(SCHEME, s_f[r], wx_);
+        wts(SCHEME, s_f[CH + r], wy_);
+        if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
+        float2 uxy;
+        float uz;
+        win.gather(wx_, wy_, wz_, uxy, uz);
+        const float c32 = s_f[3 * CH + r];
         if (MODE == MODE_OP) {
-          const float mc = mass * c32 * inv_vol;
-          q01 = make_float2(mc * ux, mc * uy); q23.x = mc * uz;
+          const float mc = s_f[4 * CH + r] * c32 * inv_vol;
+          s_f[5 * CH + r] = mc * uxy.x; s_f[6 * CH + r] = mc * uxy.y; s_f[7 * CH + r] = mc * uz;
         } else {
-          // GatherKickPMBR (src/dust/dust_pm.cpp:534-563) with the applied velocity change;
-          // the new velocity and the change replace this particle's columns of the rows
+          // GatherKickPMBR (src/dust/dust_pm.cpp:534-563): the applied velocity change
           const float vx = s_f[5 * CH + r], vy = s_f[6 * CH + r], vz = s_f[7 * CH + r];
-          const float nx_ = vx + c32 * (ux - vx), ny_ = vy + c32 * (uy - vy), nz_ = vz + c32 * (uz - vz);
-          const float dvx = nx_ - vx, dvy = ny_ - vy, dvz = nz_ - vz;
-          s_f[5 * CH + r] = nx_; s_f[6 * CH + r] = ny_; s_f[7 * CH + r] = nz_;
-          s_f[r] = dvx; s_f[CH + r] = dvy; s_f[2 * CH + r] = dvz;
-          const float fac = -mass * inv_vol;
-          q01 = make_float2(fac * dvx, fac * dvy); q23.x = fac * dvz;
+          s_f[5 * CH + r] = (vx + c32 * (uxy.x - vx)) - vx;
+          s_f[6 * CH + r] = (vy + c32 * (uxy.y - vy)) - vy;
+          s_f[7 * CH + r] = (vz + c32 * (uz - vz)) - vz;
         }
       }
-      if (MODE == MODE_QP || T.deposit) {
-        // acc_cba += wz_c wy_b (wx_a q): the x weights folded into the values first
-        float2 s01[3], s23[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          s01[a] = __fmul2_rn(dup(wx_[a]), q01);
-          if (MODE == MODE_QP) s23[a] = __fmul2_rn(dup(wx_[a]), q23);
-          else s23[a].x = wx_[a] * q23.x;
-        }
-#pragma unroll
-        for (int c = 0; c < WK; ++c) {
-          const float wzc = D3 ? wz_[c] : 1.0f;
-#pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            const float wzy = wzc * wy_[b];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-              acc01[c][b][a] = __ffma2_rn(dup(wzy), s01[a], acc01[c][b][a]);
-              if (MODE == MODE_QP) acc23[c][b][a] = __ffma2_rn(dup(wzy), s23[a], acc23[c][b][a]);
-              else acc2[c][b][a] = fmaf(wzy, s23[a].x, acc2[c][b][a]);
-            }
-          }
+      if (MODE == MODE_KICK) {
+        // the kicked velocities and rates of the pass, particle by particle (coalesced):
+        // v <- v + dv, R <- dv / a_dt
+        __syncthreads();
+        for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
+          const int s = sh + x, p = cb + x;
+          const float dvx = s_f[5 * CH + s], dvy = s_f[6 * CH + s], dvz = s_f[7 * CH + s];
+          S.f[F_VX][p] += dvx; S.f[F_VY][p] += dvy; S.f[F_VZ][p] += dvz;
+          S.f[F_RX][p] = dvx * inv_adt; S.f[F_RY][p] = dvy * inv_adt; S.f[F_RZ][p] = dvz * inv_adt;
         }
       }
-    }
-    if (MODE == MODE_KICK) {
-      // the kicked velocities and rates of the pass, particle by particle (coalesced)
-      __syncthreads();
-      for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
-        const int s = sh + x, p = cb + x;
-        S.f[F_VX][p] = s_f[5 * CH + s]; S.f[F_VY][p] = s_f[6 * CH + s]; S.f[F_VZ][p] = s_f[7 * CH + s];
-        S.f[F_RX][p] = s_f[s] * inv_adt; S.f[F_RY][p] = s_f[CH + s] * inv_adt;
-        S.f[F_RZ][p] = s_f[2 * CH + s] * inv_adt;
+      if (T.deposit) {
+        // deposit phase: the sums of the values of this pass, added to the field
+        CellSums<MODE, D3> sums;
+        sums.zero();
+        for (int r = lo; r < hi; ++r) {
+          float wx_[3], wy_[3], wz_[3];
+          wts(SCHEME, s_f[r], wx_);
+          wts(SCHEME, s_f[CH + r], wy_);
+          if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
+          const float f = (MODE == MODE_OP) ? 1.0f : -s_f[4 * CH + r] * inv_vol;
+          sums.add(wx_, wy_, wz_, make_float2(f * s_f[5 * CH + r], f * s_f[6 * CH + r]),
+                   make_float2(f * s_f[7 * CH + r], 0.0f));
+        }
+        // the rows are read by now: their space takes the staged sums
+        __syncthreads();
+        stage_sums<MODE, D3>(sums, s_acc, cl, nct);
+        __syncthreads();
+        add_window<MODE, D3>(s_acc, G, T, m, k, j0, tj);
       }
     }
     // the next pass's copies overwrite the rows
@@ -706,49 +814,20 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
   if (MODE == MODE_QP) {
     // centre mass m c / V of the cell (dust_imex_point_center_mass): only this cell's
     // particles have it as their centre, so it is stored, not added
-    T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj_l, G.is + ci_l)] = (double)qt;
-  }
-  if (MODE != MODE_QP && !T.deposit) return;
-  // the x-offset contributions of neighbouring cells of a row meet in registers: lane L takes
-  // lane L+1's left and lane L-1's right contribution; a row's (or warp's) end lanes add
-  // their outward contribution themselves
-  const unsigned wmask = (wlanes == 32) ? 0xffffffffu : ((1u << wlanes) - 1u);
-  const bool has_left = ci_l > 0 && lane > 0;
-  const bool has_right = ci_l + 1 < nx1 && lane + 1 < wlanes;
-  auto val = [&](int c, int b, int a, int q) {
-    return q == 0 ? acc01[c][b][a].x : q == 1 ? acc01[c][b][a].y
-         : (MODE == MODE_QP ? (q == 2 ? acc23[c][b][a].x : acc23[c][b][a].y) : acc2[c][b][a]);
-  };
-#pragma unroll
-  for (int c = 0; c < WK; ++c) {
-    const int kk = D3 ? k - 1 + c : 0;
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      const int jj = j0 + cj_l - 1 + b;
-      // the row's target cells: this cell's column, and the outward ones of the end lanes
-      const long long bc = cell_at(G, m, T.dnvar, kk, jj, ci_l);
-      const long long bl = has_left ? -1
-                         : (ci_l > 0 ? (bc >= 0 ? bc - 1 : -1) : cell_at(G, m, T.dnvar, kk, jj, -1));
-      const long long bR = has_right ? -1
-                         : (ci_l + 1 < nx1 ? (bc >= 0 ? bc + 1 : -1) : cell_at(G, m, T.dnvar, kk, jj, nx1));
-#pragma unroll
-      for (int q = 0; q < NC; ++q) {
-        const float l = val(c, b, 0, q), mid = val(c, b, 1, q), r = val(c, b, 2, q);
-        const float from_right = __shfl_down_sync(wmask, l, 1);
-        const float from_left = __shfl_up_sync(wmask, r, 1);
-        const float tot = mid + (has_right ? from_right : 0.0f) + (has_left ? from_left : 0.0f);
-        const long long qo = (long long)q * G.vstride;
-        if (bc >= 0 && tot != 0.0f) atomicAdd(&T.dfield[bc + qo], (double)tot);
-        if (bl >= 0 && l != 0.0f) atomicAdd(&T.dfield[bl + qo], (double)l);
-        if (bR >= 0 && r != 0.0f) atomicAdd(&T.dfield[bR + qo], (double)r);
-      }
-    }
+    T.res[G.at(m, 4, 3, G.ks + k, G.js + jrow, G.is + ci_l)] = (double)qt;
+    stage_sums<MODE, D3>(qp, s_acc, cl, nct);
+    __syncthreads();
+    add_window<MODE, D3>(s_acc, G, T, m, k, j0, tj);
   }
 }
 
-size_t tile_smem(int mode, int tj, int nx1, int chunk) {
+// shared memory of a tile: the cell ranges, then the larger of the pass rows and the staged
+// sums (27 float4 per cell in 3-D, 9 in 2-D)
+size_t tile_smem(int three_d, int tj, int nx1, int chunk) {
   const int nct = tj * nx1;
-  return (((size_t)(nct + 1) * 4 + 15) & ~(size_t)15) + (size_t)tile_nfield(mode) * chunk * 4;
+  const size_t rows = (size_t)kTileRows * chunk * 4;
+  const size_t sums = (size_t)(three_d ? 27 : 9) * nct * 16;
+  return (((size_t)(nct + 1) * 4 + 15) & ~(size_t)15) + (rows > sums ? rows : sums);
 }
 
 // ---- kernel timing ------------------------------------------------------------------------
@@ -795,15 +874,14 @@ bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   if (cf.chunk < 64 || cf.chunk > 8192 || (cf.chunk & 3)) return false;
   cf.tpp = nx2 / tj;
   // every tile form must fit the 227 KiB of shared memory a CTA can have (less the barrier)
-  for (int mode = MODE_QP; mode <= MODE_KICK; ++mode)
-    if (tile_smem(mode, tj, nx1, cf.chunk) > 227 * 1024 - 256) return false;
+  if (tile_smem(ms.three_d, tj, nx1, cf.chunk) > 227 * 1024 - 256) return false;
   return true;
 }
 
 template <int MODE, int D3, int SCHEME>
 int launch_tile_d(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &T, cudaStream_t st) {
   const long long tiles = (long long)G.nmb * G.nx3 * cf.tpp;
-  const size_t sm = tile_smem(MODE, cf.tj, G.nx1, cf.chunk);
+  const size_t sm = tile_smem(D3, cf.tj, G.nx1, cf.chunk);
   static size_t configured = 0;
   if (sm > 48 * 1024 && sm > configured) {
     cudaFuncSetAttribute(k_tile<MODE, D3, SCHEME>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
