@@ -35,12 +35,16 @@ GAMMA = 1.707106781186547
 # per-kernel algorithmic bytes of the mixed form: (bytes per particle, bytes per cell) of
 # one launch, the minimum each kernel must read and write (4-byte particle words, FP64 cells)
 MIXED_BYTES = {
-    "push": (114.0, 0.0),          # stage 1: 28 read + 52 write; stage 2: 96 read + 52 write
-    "fill": (16.0, 20.0),
-    "deposit_qp": (40.0, 40.0),    # order, cell, offsets, v, t_s, m; Q, P (+ centre mass)
-    "operator": (28.0, 48.0),      # order, cell, offsets, t_s, m; u* in, work out
-    "kick": (64.0, 48.0),          # + v in/out, R out; u* in, dmom out
-    "consistent": (56.0, 0.0),     # cell, t_s, v, R, 3 residuals in; v, R out
+    # count (stage 1: cell, offsets, v in, key out = 32; stage 2: + register displacement,
+    # drag factor, m = 52) and move (key + the particle's words in, 20 words out: stage 1
+    # 56 + 80, stage 2 84 + 80): 4 launches per cycle, (32 + 136 + 52 + 164) / 4 = 96 per
+    # particle; the per-cell histogram 8
+    "push": (96.0, 8.0),
+    "fill": (0.0, 16.0),           # scan of the histogram, cursor copy
+    "deposit_qp": (32.0, 40.0),    # offsets, drag factor, m, v in; Q, P, centre mass out
+    "operator": (20.0, 48.0),      # offsets, drag factor, m in; u* in, work out
+    "kick": (56.0, 48.0),          # offsets, drag factor, m, v in, v and R out; u*, dmom
+    "consistent": (60.0, 24.0),    # cell, drag factor, m, v, R in; v, R out; residual in
 }
 
 
@@ -354,11 +358,11 @@ def run_ours(args, rank, world):
                   "share": round(v[0] / total_ms, 3)} for k, v in ktimes.items() if v[1]}
     steps_per_s = npart * world / (ms_mixed * 1e-3)
     fp64_rate = npart * world / (ms_fp64 * 1e-3)
-    # kernels of ours per mixed cycle (dc1, consistent split): per stage gas update, push,
-    # scan (3), fill, run order, Q/P tile, solve, operator tile, correction, kick tile,
-    # consistent gas = 13, stage 2 adds the history term and the consistent kick, and one
-    # ghost exchange of u0 closes the cycle: 13 + 15 + 1
-    launches_mixed = 29 * args.steps
+    # kernels of ours per mixed cycle (dc1, consistent split): per stage gas update, count,
+    # scan (3), move, Q/P tile, solve, operator tile, correction, kick tile, consistent gas
+    # = 12, stage 2 adds the history term and the consistent kick, and one ghost exchange of
+    # u0 closes the cycle: 12 + 14 + 1
+    launches_mixed = 27 * args.steps
     if rank == 0:
         cb = None if args.no_cpu else cpu_baseline()
         line = {
