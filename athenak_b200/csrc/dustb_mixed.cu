@@ -430,9 +430,11 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   float o[3] = {S.f[F_OX][p], S.f[F_OY][p], S.f[F_OZ][p]};
   float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
   const float ts = S.f[F_TS][p], mass = S.f[F_M][p];
-  float cc = S.f[F_CC][p];
-  float v1[3], d1[3], r[3] = {S.f[F_RX][p], S.f[F_RY][p], S.f[F_RZ][p]};
+  // (stage 1 forms the drag factor, and its velocity does not use the rates)
+  float cc = P.stage2 ? S.f[F_CC][p] : 0.0f;
+  float v1[3], d1[3], r[3] = {0.0f, 0.0f, 0.0f};
   if (P.stage2) {
+    r[0] = S.f[F_RX][p]; r[1] = S.f[F_RY][p]; r[2] = S.f[F_RZ][p];
     v1[0] = S.f[F_WX][p]; v1[1] = S.f[F_WY][p]; v1[2] = S.f[F_WZ][p];
     d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p];
     if (P.res && mass > 0.0f) {
@@ -475,7 +477,7 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   D.f[F_VX][q] = nv[0]; D.f[F_VY][q] = nv[1]; D.f[F_VZ][q] = nv[2];
   D.f[F_AX][q] = d1[0]; D.f[F_AY][q] = d1[1]; D.f[F_AZ][q] = d1[2];
   D.f[F_WX][q] = v1[0]; D.f[F_WY][q] = v1[1]; D.f[F_WZ][q] = v1[2];
-  D.f[F_RX][q] = r[0]; D.f[F_RY][q] = r[1]; D.f[F_RZ][q] = r[2];
+  // (no rates: the kick tile of this stage writes every particle's rate)
   D.f[F_TS][q] = ts; D.f[F_M][q] = mass; D.f[F_CC][q] = cc;
 }
 

@@ -36,10 +36,11 @@ GAMMA = 1.707106781186547
 # one launch, the minimum each kernel must read and write (4-byte particle words, FP64 cells)
 MIXED_BYTES = {
     # count (stage 1: cell, offsets, v in, key out = 32; stage 2: + register displacement,
-    # drag factor, m = 52) and move (key + the particle's words in, 20 words out: stage 1
-    # 56 + 80, stage 2 84 + 80): 4 launches per cycle, (32 + 136 + 52 + 164) / 4 = 96 per
-    # particle; the per-cell histogram 8
-    "push": (96.0, 8.0),
+    # drag factor, m = 52) and move (stage 1: key, cell, row, offsets, v, t_s, m in = 44,
+    # stage 2: + velocity register, displacement, rates, drag factor = 84; out: cell, row,
+    # offsets, v, velocity register, displacement, t_s, m, drag factor = 68): 4 launches per
+    # cycle, (32 + 112 + 52 + 152) / 4 = 87 per particle; the per-cell histogram 8
+    "push": (87.0, 8.0),
     "fill": (0.0, 16.0),           # scan of the histogram, cursor copy
     "deposit_qp": (32.0, 40.0),    # offsets, drag factor, m, v in; Q, P, centre mass out
     "operator": (20.0, 48.0),      # offsets, drag factor, m in; u* in, work out
@@ -396,9 +397,15 @@ def run_ours(args, rank, world):
 def measure_e2e(dev, dt, args, stream):
     """Per step through the C ABI with host (pinned) buffers: the FP64 rows the step reads
     (X, V, t_s, m, PGID) and u0 copied in, import, one mixed cycle, export, the rows the step
-    writes (X, V, X1, V1, R, PGID) and u0 copied out."""
+    writes (X, V, X1, V1, R, PGID) and u0 copied out.  The host rows are first put in cell
+    order once (dustb_sort_by_cell, the reference's SortParticles), the order a host code
+    that sorts its particles keeps them in; each step's export writes every particle back to
+    its own row."""
     import torch
     from athenak_b200.mixed import MixedDust
+    dev.sort_by_cell()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     n = dev.npart
     rows_in = [0, 1, 2, 3, 4, 5, 15, 16]
     rows_out = list(range(15))
