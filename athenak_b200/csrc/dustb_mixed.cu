@@ -69,7 +69,17 @@ struct PBuf {                    // one copy of the shadow
   float *f[kNF];
 };
 
+// state kept in the workspace between calls: the stage-2 consistent dust kick of the last
+// cycle is not applied to the shadow by that cycle; the next cycle's stage-1 push applies it
+// (as stage 2's push applies stage 1's), and an export applies it to the rows it writes
+struct MHead {
+  int pending;                   // nonzero: the last cycle's consistent kick is pending
+  int pad;
+  double a_dt;                   // that cycle's a dt (the rate change is dv / a dt)
+};
+
 struct MState {
+  MHead *head;
   PBuf A, B;                     // A holds the shadow between cycles
   int *key;                      // new cell of each particle (count -> move)
   int *cstart, *cursor, *bsum;
@@ -109,7 +119,7 @@ long long ncell_of(const dustb_mesh &ms) {
 bool carve(const dustb_mesh &ms, int n, void *ws, long long bytes, MState &S, long long *need) {
   const long long ncell = ncell_of(ms);
   const size_t N = (size_t)(n > 0 ? n : 1);
-  size_t off = 0;
+  size_t off = al256(sizeof(MHead));
   size_t o_buf[2][2 + kNF];
   for (int b = 0; b < 2; ++b)
     for (int f = 0; f < 2 + kNF; ++f) { o_buf[b][f] = off; off += al256(4 * N); }
@@ -126,6 +136,7 @@ bool carve(const dustb_mesh &ms, int n, void *ws, long long bytes, MState &S, lo
     bufs[q]->pid = (int *)(b + o_buf[q][1]);
     for (int f = 0; f < kNF; ++f) bufs[q]->f[f] = (float *)(b + o_buf[q][2 + f]);
   }
+  S.head = (MHead *)b;
   S.key = (int *)(b + o_key);
   S.cstart = (int *)(b + o_cs); S.cursor = (int *)(b + o_cur); S.bsum = (int *)(b + o_bs);
   return true;
@@ -291,12 +302,26 @@ __global__ void k_sortmove(PBuf src, PBuf dst, int n, int *cursor) {
   for (int f = 0; f < kNF; ++f) dst.f[f][q] = src.f[f][p];
 }
 
-__global__ void k_export(double *pr, int *pi, long long stride, int n, PBuf A, Geo G) {
+// the shadow's particles into their reference rows; a pending consistent kick of the last
+// cycle is applied to the exported velocities and rates (rounded as the next push would)
+__global__ void k_export(double *pr, int *pi, long long stride, int n, PBuf A, Geo G,
+                         const double *res, const MHead *head) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   int m, k, j, i;
   decode(G, A.cell[q], m, k, j, i);
   const int p = A.pid[q];
+  float vel[3] = {A.f[F_VX][q], A.f[F_VY][q], A.f[F_VZ][q]};
+  float rate[3] = {A.f[F_RX][q], A.f[F_RY][q], A.f[F_RZ][q]};
+  if (res && head->pending && A.f[F_M][q] > 0.0f) {
+    const long long b = G.at(m, 4, 0, k + G.ks, j + G.js, i + G.is);
+    const double cj = (double)A.f[F_CC][q];
+    for (int a = 0; a < 3; ++a) {
+      const double d = __dmul_rn(cj, res[b + a * G.vstride]);
+      vel[a] = __fadd_rn(vel[a], __double2float_rn(d));
+      rate[a] += (float)(d / head->a_dt);
+    }
+  }
   auto W = [&](int r, double v) { pr[(long long)r * stride + p] = v; };
   const double *sz = G.mb + (long long)m * 9;
   const double x = sz[X1MIN] + ((double)i + (double)A.f[F_OX][q]) * G.dx[0];
@@ -309,9 +334,9 @@ __global__ void k_export(double *pr, int *pi, long long stride, int n, PBuf A, G
     W(DUSTB_IPZ, z);
     W(DUSTB_IPZ1, z + (double)A.f[F_AZ][q] * G.dx[2]);
   }
-  W(DUSTB_IPVX, A.f[F_VX][q]); W(DUSTB_IPVY, A.f[F_VY][q]); W(DUSTB_IPVZ, A.f[F_VZ][q]);
+  W(DUSTB_IPVX, vel[0]); W(DUSTB_IPVY, vel[1]); W(DUSTB_IPVZ, vel[2]);
   W(DUSTB_IPVX1, A.f[F_WX][q]); W(DUSTB_IPVY1, A.f[F_WY][q]); W(DUSTB_IPVZ1, A.f[F_WZ][q]);
-  W(DUSTB_IPRX, A.f[F_RX][q]); W(DUSTB_IPRY, A.f[F_RY][q]); W(DUSTB_IPRZ, A.f[F_RZ][q]);
+  W(DUSTB_IPRX, rate[0]); W(DUSTB_IPRY, rate[1]); W(DUSTB_IPRZ, rate[2]);
   pi[(long long)DUSTB_PGID * stride + p] = m + G.gids;
 }
 
@@ -332,7 +357,12 @@ struct PushArgs {
   int stage2;
   int sbox, strat;
   float q, om;
-  const double *res;          // stage 2 with the consistent split: stage 1's dust residual
+  // the consistent split's dust kick folded into the push: stage 2 applies stage 1's kick
+  // (res = stage 1's dust residual); stage 1 applies the previous cycle's stage-2 kick when
+  // head->pending is set (res = that residual)
+  const double *res;
+  MHead *head;
+  int set_pending;            // stage 2: record this cycle's stage-2 kick as pending
   unsigned *err;
 };
 
@@ -403,17 +433,16 @@ __global__ void __launch_bounds__(kT) k_count(PBuf S, int *key_out, int *count, 
   float o[3] = {S.f[F_OX][p], S.f[F_OY][p], S.f[F_OZ][p]};
   float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
   float d1[3] = {0.0f, 0.0f, 0.0f};
-  if (P.stage2) {
-    d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p];
-    if (P.res && S.f[F_M][p] > 0.0f) {
-      double d[3];
-      consistent_dv(G, P, S.f[F_CC][p], m, k, j, i, d);
-      for (int a = 0; a < 3; ++a) v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
-    }
+  if (P.stage2) { d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p]; }
+  if (P.res && (P.stage2 || P.head->pending) && S.f[F_M][p] > 0.0f) {
+    double d[3];
+    consistent_dv(G, P, S.f[F_CC][p], m, k, j, i, d);
+    for (int a = 0; a < 3; ++a) v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
   }
   const int key = advance(G, P, m, k, j, i, o, d1, v);
   key_out[p] = key;
   warp_count(count, key, act);
+  if (P.set_pending && p == 0) { P.head->a_dt = P.a_dt; P.head->pending = 1; }
 }
 
 // move: the whole push of every particle, written to its slot in dst
@@ -430,21 +459,22 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   float o[3] = {S.f[F_OX][p], S.f[F_OY][p], S.f[F_OZ][p]};
   float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
   const float ts = S.f[F_TS][p], mass = S.f[F_M][p];
-  // (stage 1 forms the drag factor, and its velocity does not use the rates)
-  float cc = P.stage2 ? S.f[F_CC][p] : 0.0f;
+  // (the rates: stage 1's velocity does not use them and every stage's kick rewrites them)
+  const bool kick = P.res && (P.stage2 || P.head->pending);
+  float cc = (P.stage2 || kick) ? S.f[F_CC][p] : 0.0f;
   float v1[3], d1[3], r[3] = {0.0f, 0.0f, 0.0f};
+  if (P.stage2) { r[0] = S.f[F_RX][p]; r[1] = S.f[F_RY][p]; r[2] = S.f[F_RZ][p]; }
+  if (kick && mass > 0.0f) {
+    double d[3];
+    consistent_dv(G, P, cc, m, k, j, i, d);
+    for (int a = 0; a < 3; ++a) {
+      v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
+      r[a] += (float)(d[a] / P.a_dt);
+    }
+  }
   if (P.stage2) {
-    r[0] = S.f[F_RX][p]; r[1] = S.f[F_RY][p]; r[2] = S.f[F_RZ][p];
     v1[0] = S.f[F_WX][p]; v1[1] = S.f[F_WY][p]; v1[2] = S.f[F_WZ][p];
     d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p];
-    if (P.res && mass > 0.0f) {
-      double d[3];
-      consistent_dv(G, P, cc, m, k, j, i, d);
-      for (int a = 0; a < 3; ++a) {
-        v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
-        r[a] += (float)(d[a] / P.a_dt);
-      }
-    }
   } else {
     // FirstTwoImpRK: (x1, v1) <- (x, v); the drag factor of the cycle, formed in FP64
     v1[0] = v[0]; v1[1] = v[1]; v1[2] = v[2];
@@ -479,19 +509,6 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   D.f[F_WX][q] = v1[0]; D.f[F_WY][q] = v1[1]; D.f[F_WZ][q] = v1[2];
   // (no rates: the kick tile of this stage writes every particle's rate)
   D.f[F_TS][q] = ts; D.f[F_M][q] = mass; D.f[F_CC][q] = cc;
-}
-
-// ---- stage-2 consistent dust kick ------------------------------------------------------
-__global__ void k_consistent_kick(PBuf S, Geo G, int n, double a_dt, const double *res) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n || !(S.f[F_M][p] > 0.0f)) return;
-  int m, k, j, i;
-  decode(G, S.cell[p], m, k, j, i);
-  const double cj = (double)S.f[F_CC][p];
-  const long long b = G.at(m, 4, 0, k + G.ks, j + G.js, i + G.is);
-  const double d0 = cj * res[b], d1 = cj * res[b + G.vstride], d2 = cj * res[b + 2 * G.vstride];
-  S.f[F_VX][p] += (float)d0; S.f[F_VY][p] += (float)d1; S.f[F_VZ][p] += (float)d2;
-  S.f[F_RX][p] += (float)(d0 / a_dt); S.f[F_RY][p] += (float)(d1 / a_dt); S.f[F_RZ][p] += (float)(d2 / a_dt);
 }
 
 // ---- tile deposit kernels -------------------------------------------------------------------
@@ -970,6 +987,7 @@ int dustb_mixed_import(const dustb_ctx *c, const dustb_mixed_params *mp, void *w
   Geo G = make_geo(c, mp);
   const int n = c->part.npart;
   const long long ncell = ncell_of(c->mesh);
+  cudaMemsetAsync(S.head, 0, sizeof(MHead), st);   // the rows carry every kick so far
   cudaMemsetAsync(S.cstart, 0, 4 * (size_t)(ncell + 1), st);
   if (n > 0)
     k_import<<<nblk(n), kT, 0, st>>>(c->part.pr, c->part.pi, c->part.stride, n, S.B, S.cstart, G, c->err);
@@ -988,7 +1006,8 @@ int dustb_mixed_export(const dustb_ctx *c, const dustb_mixed_params *mp, void *w
   Geo G = make_geo(c, mp);
   const int n = c->part.npart;
   if (n > 0)
-    k_export<<<nblk(n), kT, 0, (cudaStream_t)stream>>>(c->part.pr, c->part.pi, c->part.stride, n, S.A, G);
+    k_export<<<nblk(n), kT, 0, (cudaStream_t)stream>>>(c->part.pr, c->part.pi, c->part.stride, n, S.A, G,
+                                                        c->f.resid, S.head);
   return dustb_host::launch_status("mixed_export");
 }
 
@@ -1070,7 +1089,11 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     P.a_dt = a_dt; P.stage2 = (stage == 2);
     P.sbox = c->phys.shearing_box; P.strat = c->phys.stratified;
     P.q = (float)c->phys.qshear; P.om = (float)c->phys.omega0;
-    P.res = (stage == 2 && br && cons) ? c->f.resid : nullptr;
+    // stage 2: stage 1's consistent kick (this cycle's split); stage 1: the previous
+    // cycle's stage-2 kick, if it left one pending
+    P.res = (stage == 1 || (br && cons)) ? c->f.resid : nullptr;
+    P.head = S.head;
+    P.set_pending = (stage == 2 && br && cons);
     P.err = c->err;
     {
       Scope sc(DUSTB_K_PUSH, st);
@@ -1087,6 +1110,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       Scope sc(DUSTB_K_PUSH, st);
       if (n > 0) k_move<<<nblk(n), kT, 0, st>>>(src, cur, S.key, S.cursor, G, n, P);
       RUN(dustb_host::launch_status("mixed move"));
+      if (stage == 1) cudaMemsetAsync(&S.head->pending, 0, sizeof(int), st);   // applied
     }
     TileArgs T{};
     T.a_dt = a_dt; T.err = c->err; T.deposit = 1;
@@ -1123,11 +1147,8 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       { Scope sc(DUSTB_K_CELLS, st);
         if (cons) dustb_cells::consistent_gas(c, a_dt, st);
         else dustb_cells::pmbr(c, a_dt, st); }
-      if (cons && stage == 2 && n > 0) {
-        Scope sc(DUSTB_K_CONSISTENT, st);
-        k_consistent_kick<<<nblk(n), kT, 0, st>>>(cur, G, n, a_dt, c->f.resid);
-        RUN(dustb_host::launch_status("mixed consistent kick"));
-      }
+      // stage 2's consistent dust kick is left pending (recorded by stage 2's count): the
+      // next cycle's stage-1 push, or an export, applies it
     }
   }
   {

@@ -35,17 +35,17 @@ GAMMA = 1.707106781186547
 # per-kernel algorithmic bytes of the mixed form: (bytes per particle, bytes per cell) of
 # one launch, the minimum each kernel must read and write (4-byte particle words, FP64 cells)
 MIXED_BYTES = {
-    # count (stage 1: cell, offsets, v in, key out = 32; stage 2: + register displacement,
-    # drag factor, m = 52) and move (stage 1: key, cell, row, offsets, v, t_s, m in = 44,
-    # stage 2: + velocity register, displacement, rates, drag factor = 84; out: cell, row,
+    # count (stage 1: cell, offsets, v, drag factor, m in, key out = 40; stage 2: + register
+    # displacement = 52) and move (stage 1: key, cell, row, offsets, v, t_s, m, drag factor
+    # in = 48, stage 2: + velocity register, displacement, rates = 84; out: cell, row,
     # offsets, v, velocity register, displacement, t_s, m, drag factor = 68): 4 launches per
-    # cycle, (32 + 112 + 52 + 152) / 4 = 87 per particle; the per-cell histogram 8
-    "push": (87.0, 8.0),
+    # cycle, (40 + 116 + 52 + 152) / 4 = 90 per particle (the consistent kicks folded in: the
+    # residual, per cell); the per-cell histogram 8
+    "push": (90.0, 8.0),
     "fill": (0.0, 16.0),           # scan of the histogram, cursor copy
     "deposit_qp": (32.0, 40.0),    # offsets, drag factor, m, v in; Q, P, centre mass out
     "operator": (20.0, 48.0),      # offsets, drag factor, m in; u* in, work out
     "kick": (56.0, 48.0),          # offsets, drag factor, m, v in, v and R out; u*, dmom
-    "consistent": (60.0, 24.0),    # cell, drag factor, m, v, R in; v, R out; residual in
 }
 
 
@@ -361,9 +361,9 @@ def run_ours(args, rank, world):
     fp64_rate = npart * world / (ms_fp64 * 1e-3)
     # kernels of ours per mixed cycle (dc1, consistent split): per stage gas update, count,
     # scan (3), move, Q/P tile, solve, operator tile, correction, kick tile, consistent gas
-    # = 12, stage 2 adds the history term and the consistent kick, and one ghost exchange of
-    # u0 closes the cycle: 12 + 14 + 1
-    launches_mixed = 27 * args.steps
+    # = 12, stage 2 adds the history term, and one ghost exchange of u0 closes the cycle:
+    # 12 + 13 + 1 (the consistent dust kicks are folded into the next stage's push)
+    launches_mixed = 26 * args.steps
     if rank == 0:
         cb = None if args.no_cpu else cpu_baseline()
         line = {

@@ -281,7 +281,9 @@ long long dustb_mixed_workspace_bytes(const dustb_mesh *mesh, int npart);
 int dustb_mixed_import(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
                        long long ws_bytes, void *stream);
 
-/* Writes X, V, X1, V1, R and PGID of every shadow particle back into its reference row. */
+/* Writes X, V, X1, V1, R and PGID of every shadow particle back into its reference row.
+ * The last cycle's stage-2 consistent dust kick, which the shadow keeps pending until the
+ * next cycle's push, is applied to the V and R written (ctx->f.resid as that cycle left it). */
 int dustb_mixed_export(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
                        long long ws_bytes, void *stream);
 
