@@ -396,11 +396,13 @@ def run_ours(args, rank, world):
 
 def measure_e2e(dev, dt, args, stream):
     """Per step through the C ABI with host (pinned) buffers: the FP64 rows the step reads
-    (X, V, t_s, m, PGID) and u0 copied in, import, one mixed cycle, export, the rows the step
-    writes (X, V, X1, V1, R, PGID) and u0 copied out.  The host rows are first put in cell
-    order once (dustb_sort_by_cell, the reference's SortParticles), the order a host code
-    that sorts its particles keeps them in; each step's export writes every particle back to
-    its own row."""
+    (X, V, t_s, m, PGID) and u0 copied in, import, one mixed cycle, export, and the state the
+    next step reads (X, V, PGID, u0) copied out.  X1, V1 and R are the integrator's stage
+    registers: the export writes them on the device, but the next cycle sets X1, V1 from X, V
+    at its first stage and its first stage does not read R, so they are not copied back.
+    The host rows are first put in cell order once (dustb_sort_by_cell, the reference's
+    SortParticles), the order a host code that sorts its particles keeps them in; each
+    step's export writes every particle back to its own row."""
     import torch
     from athenak_b200.mixed import MixedDust
     dev.sort_by_cell()
@@ -408,7 +410,7 @@ def measure_e2e(dev, dt, args, stream):
     torch.cuda.empty_cache()
     n = dev.npart
     rows_in = [0, 1, 2, 3, 4, 5, 15, 16]
-    rows_out = list(range(15))
+    rows_out = [0, 1, 2, 3, 4, 5]
     try:
         h_pr = torch.empty((17, n), dtype=torch.float64, pin_memory=True)
         h_pi = torch.empty((1, n), dtype=torch.int32, pin_memory=True)
