@@ -38,7 +38,8 @@ class DustbPhysics(C.Structure):
     _fields_ = [("scheme", C.c_int), ("back_reaction", C.c_int), ("consistent_gas", C.c_int),
                 ("drag_solver", C.c_int), ("shearing_box", C.c_int), ("stratified", C.c_int),
                 ("pc2_feedback_damping", C.c_int),
-                ("qshear", C.c_double), ("omega0", C.c_double), ("const_accel_phi", C.c_double)]
+                ("qshear", C.c_double), ("omega0", C.c_double), ("const_accel_phi", C.c_double),
+                ("x3_deposit_drop", C.c_int)]
 
 
 class DustbCtx(C.Structure):
@@ -100,6 +101,7 @@ def make_ctx(mesh, arrays, npart, stride, phys) -> DustbCtx:
     p.qshear = phys.get("qshear", 1.5)
     p.omega0 = phys.get("omega0", 1.0)
     p.const_accel_phi = phys.get("const_accel_phi", 0.0)
+    p.x3_deposit_drop = int(phys.get("x3_deposit_drop", False))
     c.err = ptr(arrays.get("err"))
     return c
 

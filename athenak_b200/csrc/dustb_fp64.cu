@@ -245,7 +245,8 @@ __global__ void k_scatter(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, doub
 // RecvAndSumDeposit (src/bvals/bvals_dep.cpp:457-560): receiver active strips on side o
 // (InitRecvIndices :281-297) += the neighbour's ghost cells at index - o*nx, in
 // NeighborIndex order.
-__global__ void k_ghost_add(Ind d, const int *nghbr, int gids, double *a, int nvar) {
+// fold: fold the ghost deposits beyond physical x3 faces back into the mirrored active cells
+__global__ void k_ghost_add(Ind d, const int *nghbr, int gids, double *a, int nvar, int fold) {
   int m, k, j, i;
   long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   long long ncell = (long long)d.nmb * d.nx3 * d.nx2 * d.nx1;
@@ -270,6 +271,29 @@ __global__ void k_ghost_add(Ind d, const int *nghbr, int gids, double *a, int nv
     const int src = nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)] - gids;
     if (src < 0 || src >= d.nmb) continue;
     val += a[d.at(src, nvar, v, k - o3 * d.nx3, j - o2 * d.nx2, i - o1 * d.nx1)];
+  }
+  if (fold && d.three_d) {
+    // a physical x3 face (no neighbour across it): the ghost plane ks-1-t (ke+1+t) folds into
+    // the active plane ks+t (ke-t); the block's own column, then its x1/x2 neighbours'
+    // ghost strips that face this cell, in NeighborIndex order
+    for (int side = 0; side < 2; ++side) {
+      const int o3 = side ? 1 : -1;
+      if (side == 0 ? (k > d.ks + ng1) : (k < d.ke - ng1)) continue;
+      if (nghbr[(long long)m * 27 + dir_slot(0, 0, o3)] >= 0) continue;
+      const int kg = side ? 2 * d.ke + 1 - k : 2 * d.ks - 1 - k;
+      val += a[d.at(m, nvar, v, kg, j, i)];
+      for (int n = 0; n < ndir; ++n) {
+        const int o1 = kDirOrder[n][0], o2 = kDirOrder[n][1];
+        if (kDirOrder[n][2] != 0) continue;
+        if (o1 > 0 && i < d.ie - ng1) continue;
+        if (o1 < 0 && i > d.is + ng1) continue;
+        if (o2 > 0 && j < d.je - ng1) continue;
+        if (o2 < 0 && j > d.js + ng1) continue;
+        const int src = nghbr[(long long)m * 27 + dir_slot(o1, o2, 0)] - gids;
+        if (src < 0 || src >= d.nmb) continue;
+        val += a[d.at(src, nvar, v, kg, j - o2 * d.nx2, i - o1 * d.nx1)];
+      }
+    }
   }
   a[at] = val;
 }
@@ -856,7 +880,8 @@ int dustb_ghost_add(const dustb_ctx *c, double *field, int nvar, void *stream) {
   CHECK_CTX(c);
   if (!field || nvar <= 0) return DUSTB_EINVAL;
   Ind d = make_ind(c->mesh);
-  k_ghost_add<<<blocks_for(n_active(d) * nvar), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar);
+  const int fold = d.three_d && c->mesh.x3bc != DUSTB_X3_PERIODIC && !c->phys.x3_deposit_drop;
+  k_ghost_add<<<blocks_for(n_active(d) * nvar), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar, fold);
   return launch_status("ghost_add");
 }
 

@@ -107,6 +107,11 @@ typedef struct dustb_physics {
   int stratified;          /* vertical gravity -Omega^2 z */
   int pc2_feedback_damping;
   double qshear, omega0, const_accel_phi;
+  int x3_deposit_drop;     /* physical x3 faces (mesh.x3bc != periodic): 0 folds the ghost-cell
+                              deposits beyond a face back into the mirrored active cells
+                              (<dust>/x3_ghost_deposit = fold, the default), 1 drops them
+                              (= drop); src/dust/dust.cpp:1323-1333,
+                              src/bvals/bvals_dep_general.cpp:130-140 */
 } dustb_physics;
 
 typedef struct dustb_ctx {
@@ -151,7 +156,11 @@ int dustb_deposit_qp(const dustb_ctx *ctx, double a_dt, double sh, void *stream)
 
 /* MeshBoundaryValuesDep::PackAndSendDeposit + RecvAndSumDeposit on one device
  * (src/bvals/bvals_dep.cpp:320-560): the ghost-cell deposits of every block are added into
- * the active strips of its neighbours, buffers in NeighborIndex order. */
+ * the active strips of its neighbours, buffers in NeighborIndex order.  At physical x3 faces
+ * the ghost deposits beyond the face are folded back into the mirrored active cells (ghost
+ * plane ks-1-t into ks+t), those of the block's own column first, then those of its x1/x2
+ * neighbours' ghost strips in NeighborIndex order (the reference's general remap,
+ * DepRemapPlan with x3mode fold, bvals_dep_general.cpp:130-140), or dropped. */
 int dustb_ghost_add(const dustb_ctx *ctx, double *field, int nvar, void *stream);
 
 /* MeshBoundaryValuesCC::PackAndSendCC + RecvAndUnpackCC on one device (same-level copy

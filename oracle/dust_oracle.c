@@ -356,6 +356,39 @@ void oracle_ghost_add(const dustb_ctx *c, double *a, int nvar) {
               A5(a, nvar, d, m, v, k, j, i) += buf[q++];
     }
   free(buf);
+  /* physical x3 faces, fold mode (DepRemapPlan x3mode 1, src/bvals/bvals_dep_general.cpp:
+   * 130-140: a ghost interval beyond the face is mirrored about it): the ghost plane ks-1-t
+   * (ke+1+t) is added into the active plane ks+t (ke-t), the block's own column first, then
+   * the x1/x2 neighbours' ghost strips facing the cell, in NeighborIndex order.  (The
+   * reference sums a target's contributions in (source gid, source cell) order; the sums here
+   * differ from it by rounding only.)  The ghost cells read are untouched by the exchange. */
+  if (!ms->three_d || ms->x3bc == 0 || c->phys.x3_deposit_drop) return;
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int side = 0; side < 2; ++side) {
+      const int o3 = side ? 1 : -1;
+      if (ms->nghbr[(size_t)m*27 + (o3 + 1)*9 + 1*3 + 1] >= 0) continue;
+      for (int t = 0; t < ms->ng; ++t) {
+        const int k = side ? d.ke - t : d.ks + t;
+        const int kg = side ? d.ke + 1 + t : d.ks - 1 - t;
+        for (int v = 0; v < nvar; ++v)
+          for (int j = d.js; j <= d.je; ++j)
+            for (int i = d.is; i <= d.ie; ++i) {
+              double val = A5(a, nvar, d, m, v, k, j, i) + A5(a, nvar, d, m, v, kg, j, i);
+              for (int n = 0; n < ndir; ++n) {
+                const int *o = kDirOrder[n];
+                if (o[2] != 0) continue;
+                if (o[0] > 0 && i < d.ie - ng1) continue;
+                if (o[0] < 0 && i > d.is + ng1) continue;
+                if (o[1] > 0 && j < d.je - ng1) continue;
+                if (o[1] < 0 && j > d.js + ng1) continue;
+                int gid = ms->nghbr[(size_t)m*27 + 1*9 + (o[1] + 1)*3 + (o[0] + 1)];
+                if (gid < 0) continue;
+                val += A5(a, nvar, d, gid - ms->gids, v, kg, j - o[1]*nx[1], i - o[0]*nx[0]);
+              }
+              A5(a, nvar, d, m, v, k, j, i) = val;
+            }
+      }
+    }
 }
 
 /* UstarX3BCs, src/dust/dust_tasks.cpp:445-469 (single level) */

@@ -192,3 +192,48 @@ def test_error_word_on_bad_particles():
     w = g.error_word()
     assert w & capi.ERR_ROUTE
     assert w & capi.ERR_TSTOP
+
+
+@pytest.mark.parametrize("drop", [False, True])
+def test_ghost_add_x3_fold_bit_exact(drop):
+    """Physical x3 faces: the fold of the ghost deposits beyond the faces (or their drop)
+    matches the oracle bit for bit."""
+    ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3, x3bc=1)
+    st = make_state(ms, [0.1], [1.0], 1, seed=4)
+    phys = dict(scheme=2, x3_deposit_drop=drop)
+    from athenak_b200.drag import DeviceDust
+    o, g = Oracle(st, phys), DeviceDust(st, phys)
+    rng = np.random.default_rng(5)
+    q = rng.standard_normal(o.qdep.shape)
+    o.qdep[...] = q
+    g.t["qdep"].copy_(torch.from_numpy(q))
+    o.ghost_add("qdep", 5)
+    g.ghost_add("qdep", 5)
+    np.testing.assert_array_equal(g.host("qdep"), o.qdep)
+
+
+@pytest.mark.parametrize("coupling", ["imex", "pc2"])
+def test_x3_reflect_stratified_cycles_parity(coupling):
+    """A stratified shearing box with reflecting x3 faces (the boundaries of the stratified
+    workload): routing at the faces, the u* x3 boundary values and the deposit fold, over
+    cycles, against the oracle."""
+    ms = uniform_mesh((16, 16, 32), (8, 8, 16), 2, (-0.05, -0.05, -0.1), (0.05, 0.05, 0.1),
+                      x3bc=1)
+    st = make_state(ms, [0.01, 0.1], [0.5, 0.5], 2, seed=17, shearing_box=True,
+                    vel_noise=0.05, gas_noise=1e-2)
+    phys = dict(scheme=2, drag_solver=2, shearing_box=True, stratified=True)
+    from athenak_b200.drag import DeviceDust
+    o, g = Oracle(st, phys), DeviceDust(st, phys)
+    for _ in range(3):
+        if coupling == "imex":
+            assert o.imex_cycle(2e-3) == 0
+            g.imex_cycle(2e-3)
+        else:
+            err, chi_o = o.pc2_cycle(2e-3)
+            assert err == 0
+            chi_g = float(g.pc2_cycle(2e-3).item())
+            assert abs(chi_g - chi_o) <= 1e-12 * chi_o
+    torch.cuda.synchronize()
+    assert g.error_word() == 0
+    compare_particles(o, g)
+    assert fieldwise(g.host("u0"), o.u0) < 1e-11

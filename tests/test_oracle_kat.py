@@ -240,3 +240,24 @@ def test_route_keeps_particles_in_their_blocks():
         x = pr[2 * a, :n]
         assert np.all(x >= mb[m, lo]) and np.all(x < mb[m, hi])
     np.testing.assert_array_equal(pi[1, :n], tags0)
+
+
+@pytest.mark.parametrize("drop", [False, True])
+def test_x3_fold_conserves_the_deposit(drop):
+    """Physical x3 faces: folding the ghost deposits beyond a face back into the mirrored
+    active cells (<dust>/x3_ghost_deposit = fold) keeps every particle's whole deposit
+    (sum of Q over the active cells = sum of m c); dropping them (= drop) loses the part
+    beyond the faces."""
+    ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3, x3bc=1)
+    st = make_state(ms, [0.1, 0.01], [1.0, 0.5], 2, seed=7)
+    o = Oracle(st, dict(scheme=2, x3_deposit_drop=drop))
+    a_dt = 1e-3
+    o.deposit_qp(a_dt)
+    o.ghost_add("qdep", 5)
+    q = ms.active(o.qdep)[:, 0].sum() * ms.cell_volume()
+    n = st.npart
+    expect = (st.pr[16, :n] * a_dt / (st.pr[15, :n] + a_dt)).sum()
+    if drop:
+        assert q < expect * (1.0 - 1e-3)
+    else:
+        assert abs(q - expect) < 1e-13 * expect
