@@ -20,7 +20,9 @@ class DustbMesh(C.Structure):
                 ("x3bc", C.c_int),
                 ("x1min", C.c_double), ("x1max", C.c_double), ("x2min", C.c_double),
                 ("x2max", C.c_double), ("x3min", C.c_double), ("x3max", C.c_double),
-                ("mb_size", C.c_void_p), ("nghbr", C.c_void_p)]
+                ("mb_size", C.c_void_p), ("nghbr", C.c_void_p),
+                ("shear_x1", C.c_int), ("sb_nb2", C.c_int), ("sb_nb3", C.c_int),
+                ("sb_gid", C.c_void_p), ("time", C.c_double)]
 
 
 class DustbParticles(C.Structure):
@@ -83,6 +85,10 @@ def make_ctx(mesh, arrays, npart, stride, phys) -> DustbCtx:
     m.x1max, m.x2max, m.x3max = mesh.hi
     m.mb_size = ptr(arrays["mb_size"])
     m.nghbr = ptr(arrays["nghbr"])
+    m.shear_x1 = int(mesh.shear_x1)
+    m.sb_nb2, m.sb_nb3 = mesh.nblocks[1], mesh.nblocks[2]
+    m.sb_gid = ptr(arrays["sb_gid"]) if mesh.shear_x1 else None
+    m.time = 0.0
     c.part.pr, c.part.pi = ptr(arrays["pr"]), ptr(arrays["pi"])
     c.part.stride, c.part.npart = int(stride), int(npart)
     f = c.f

@@ -141,8 +141,196 @@ __global__ void k_push_imex(PCtx P, int three_d, int sbox, int strat, double q, 
   if (three_d) P.r(DUSTB_IPZ, p) = gam0 * z_old + gam1 * P.r(DUSTB_IPZ1, p) + beta_dt * vz_old;
 }
 
+// ---- shear-periodic x1 faces (3-D shearing box) ------------------------------------------
+// Offsets formed on the host as the reference forms them: the u* / gas remap uses the unfolded
+// q Omega Lx t (ShearingBox::InitRecv, shearing_box_tasks.cpp:147), the particles and the
+// deposit remap the folded fmod(q Omega Lx t, Ly) (bvals_part.cpp:141, bvals_dep_general.cpp:652)
+struct SBox {
+  const int *sb_gid, *nghbr;
+  const double *mb;
+  int on, nb2, nb3, gids, nmb, nx1, nx2, nx3, ng, x3bc, drop;
+  double x1min, x1max, x2min, x2max, x3min, x3max;
+  double yshear, ysh, shR;
+  __device__ double s(int m, int f) const { return mb[(long long)m * 9 + f]; }
+  // faces of block m: bit 1 inner, bit 2 outer (bvals_part.cpp:260-261)
+  __device__ int faces(int m) const {
+    const double lx = s(m, X1MAX) - s(m, X1MIN);
+    int f = 0;
+    if (s(m, X1MIN) < x1min + 0.5 * lx) f |= 1;
+    if (s(m, X1MAX) > x1max - 0.5 * lx) f |= 2;
+    return f;
+  }
+  __device__ void b23(int m, int &b2, int &b3) const {
+    b2 = (int)floor((s(m, X2MIN) - x2min) / ((x2max - x2min) / nb2) + 0.5);
+    b3 = (int)floor((s(m, X3MIN) - x3min) / ((x3max - x3min) / nb3) + 0.5);
+  }
+  __device__ int block(int f, int b3, int b2) const {
+    const int g = sb_gid[((long long)f * nb3 + b3) * nb2 + b2] - gids;
+    return (g >= 0 && g < nmb) ? g : -1;
+  }
+  // whether direction o1 from block m crosses a shear face (remapped, not exchanged plainly)
+  __device__ bool crossing(int m, int o1) const {
+    if (!on || o1 == 0) return false;
+    const int f = faces(m);
+    return (o1 < 0) ? (f & 1) : ((f & 2) != 0);
+  }
+  // the active cell owning active-relative cell (k, j, i) of block m (plain neighbour table)
+  __device__ bool owner(int m, int &k, int &j, int &i, int &mo) const {
+    const int o1 = (i < 0) ? -1 : ((i >= nx1) ? 1 : 0);
+    const int o2 = (j < 0) ? -1 : ((j >= nx2) ? 1 : 0);
+    const int o3 = (k < 0) ? -1 : ((k >= nx3) ? 1 : 0);
+    if ((o1 | o2 | o3) == 0) { mo = m; return true; }
+    const int gid = nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)];
+    if (gid < 0) return false;
+    mo = gid - gids;
+    i -= o1 * nx1; j -= o2 * nx2; k -= o3 * nx3;
+    return true;
+  }
+};
+
+SBox sbview(const dustb_ctx *c) {
+  const dustb_mesh &ms = c->mesh;
+  SBox b{};
+  b.on = ms.shear_x1 && ms.three_d;
+  b.sb_gid = ms.sb_gid; b.nghbr = ms.nghbr; b.mb = ms.mb_size;
+  b.nb2 = ms.sb_nb2; b.nb3 = ms.sb_nb3; b.gids = ms.gids; b.nmb = ms.nmb;
+  b.nx1 = ms.nx1; b.nx2 = ms.nx2; b.nx3 = ms.nx3; b.ng = ms.ng;
+  b.x3bc = ms.x3bc; b.drop = c->phys.x3_deposit_drop;
+  b.x1min = ms.x1min; b.x1max = ms.x1max; b.x2min = ms.x2min; b.x2max = ms.x2max;
+  b.x3min = ms.x3min; b.x3max = ms.x3max;
+  if (b.on) {
+    const double lx = ms.x1max - ms.x1min, ly = ms.x2max - ms.x2min;
+    b.yshear = (c->phys.qshear * c->phys.omega0) * lx * ms.time;
+    b.ysh = fmod(c->phys.qshear * c->phys.omega0 * lx * ms.time, ly);
+    const long long N2 = (long long)ms.sb_nb2 * ms.nx2;
+    b.shR = b.ysh * (double)N2 / ly;
+  }
+  return b;
+}
+
+// PLM_RemapFlx and a - (flx(j+1) - flx(j)) of ShearingBoxCC::PackAndSend at one row, from
+// g[t] = the row's column at rows r - 2 + t (src/shearing_box/remap_fluxes.hpp:30-55)
+__device__ double sb_remap(const double g[5], double eps) {
+  double f[2];
+  for (int h = 0; h < 2; ++h) {
+    const int q = 2 + h;
+    double dql, dqr;
+    if (eps > 0.0) { dql = g[q - 1] - g[q - 2]; dqr = g[q] - g[q - 1]; }
+    else { dql = g[q] - g[q - 1]; dqr = g[q + 1] - g[q]; }
+    const double dq2 = dql * dqr;
+    double dqm = 2.0 * dq2 / (dql + dqr);
+    if (dq2 <= 0.0) dqm = 0.0;
+    f[h] = (eps > 0.0) ? eps * (g[q - 1] + 0.5 * (1.0 - eps) * dqm)
+                       : eps * (g[q] - 0.5 * (1.0 + eps) * dqm);
+  }
+  return g[2] - (f[1] - f[0]);
+}
+
+// ShearingBoxCC::PackAndSend + RecvAndUnpack on one device (shearing_box_cc.cpp:78-197,
+// shearing_box.cpp:260-330): every cell of the x1 ghost strips of the face blocks (their
+// y-ghost rows and x3 ghost planes included) takes the remapped plain-periodic strip of the
+// face block holding row J -/+ joffset.  The periodic strip is read from the active cells the
+// plain copy takes it from, so no cell is both read and written.
+__global__ void k_shear_copy(SBox B, Ind d, double *a, int nvar) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long per = (long long)nvar * d.n3 * d.n2 * B.ng;
+  const long long tot = 2LL * B.nb3 * B.nb2 * per;
+  if (idx >= tot) return;
+  const int fb = (int)(idx / per);
+  long long r = idx - (long long)fb * per;
+  const int i = (int)(r % B.ng); r /= B.ng;
+  const int j = (int)(r % d.n2); r /= d.n2;
+  const int k = (int)(r % d.n3);
+  const int v = (int)(r / d.n3);
+  const int n = fb / (B.nb3 * B.nb2);
+  const int b3 = (fb / B.nb2) % B.nb3, b2 = fb % B.nb2;
+  const int T = B.block(n, b3, b2);
+  if (T < 0) return;
+  const double dy = B.s(T, DX2);
+  const long long joffset = (long long)(B.yshear / dy);
+  double eps = fmod(B.yshear, dy) / dy;
+  if (n == 1) eps *= -1.0;
+  const long long Ny = (long long)B.nb2 * B.nx2;
+  const long long J = (long long)b2 * B.nx2 + (j - d.js);
+  long long R = (n == 0) ? J - joffset : J + joffset;
+  R %= Ny; if (R < 0) R += Ny;
+  const int S = B.block(n, b3, (int)(R / B.nx2));
+  if (S < 0) return;
+  const int rr = (int)(R % B.nx2);
+  const int xr = (n == 0) ? i - B.ng : B.nx1 + i;
+  double g[5];
+  for (int t = 0; t < 5; ++t) {
+    int kk = k - d.ks, jj = rr - 2 + t, ii = xr, mo;
+    if (!B.owner(S, kk, jj, ii, mo)) return;
+    g[t] = a[d.at(mo, nvar, v, d.ks + kk, d.js + jj, d.is + ii)];
+  }
+  a[d.at(T, nvar, v, k, j, (n == 0) ? i : d.ie + 1 + i)] = sb_remap(g, eps);
+}
+
+// The shear part of the deposit remap (DepRemapPlan part 1, bvals_dep_general.cpp:99-240) for
+// active cell (k, j, i) of face block m, summed in the oracle's order (faces, source planes,
+// source blocks along x2, source rows, images): the ghost cells beyond the opposite x1 face,
+// moved by the box length and shifted by +shR (beyond the outer face) or -shR (beyond the inner
+// face) cells, weighted by their overlap with the cell
+__device__ double shear_add_sum(const SBox &B, const Ind &d, const double *a, int nvar, int m,
+                                int v, int k, int j, int i) {
+  const int faces = B.faces(m);
+  const int ng1 = B.ng - 1;
+  const long long N2 = (long long)B.nb2 * B.nx2;
+  int b2, b3;
+  B.b23(m, b2, b3);
+  const long long J = (long long)b2 * B.nx2 + (j - d.js);
+  double sum = 0.0;
+  for (int side = 0; side < 2; ++side) {
+    if (!(faces & (side ? 2 : 1))) continue;
+    const int g = side ? i - (d.ie - ng1) : i - d.is;
+    if (g < 0 || g > ng1) continue;
+    const int sface = side ? 0 : 1;
+    const int si = side ? g : d.ie + 1 + g;
+    const double sh = side ? -B.shR : B.shR;
+    const long long F = (long long)floor((double)J - sh);
+    for (int zc = 0; zc < 3; ++zc) {
+      int sb3 = b3, sk = k;
+      if (zc == 1) {
+        if (k > d.ks + ng1) continue;
+        if (b3 > 0 || B.x3bc == 0) { sb3 = (b3 + B.nb3 - 1) % B.nb3; sk = k + B.nx3; }
+        else if (!B.drop) { sk = 2 * d.ks - 1 - k; }
+        else continue;
+      } else if (zc == 2) {
+        if (k < d.ke - ng1) continue;
+        if (b3 < B.nb3 - 1 || B.x3bc == 0) { sb3 = (b3 + 1) % B.nb3; sk = k - B.nx3; }
+        else if (!B.drop) { sk = 2 * d.ke + 1 - k; }
+        else continue;
+      }
+      const long long Fm = ((F % N2) + N2) % N2;
+      const int bc = (int)(Fm / B.nx2);
+      int seen[3] = {-1, -1, -1};
+      for (int db = -1; db <= 1; ++db) {
+        const int sb2 = ((bc + db) % B.nb2 + B.nb2) % B.nb2;
+        if (sb2 == seen[0] || sb2 == seen[1]) continue;
+        seen[db + 1] = sb2;
+        const int S = B.block(sface, sb3, sb2);
+        if (S < 0) continue;
+        for (long long Yc = F - 1; Yc <= F + 1; ++Yc)
+          for (int q = -1; q <= 1; ++q) {
+            const long long Y = Yc + q * N2;
+            const long long sj = Y - (long long)sb2 * B.nx2 + d.js;
+            if (sj < 0 || sj >= d.n2) continue;
+            const double ya = (double)Y + sh, yb = (double)(Y + 1) + sh;
+            for (int im = -2; im <= 2; ++im) {
+              const double clo = (double)(J + im * N2), chi = clo + 1.0;
+              const double o = fmin(yb, chi) - fmax(ya, clo);
+              if (o > 0.0) sum += o * a[d.at(S, nvar, v, sk, (int)sj, si)];
+            }
+          }
+      }
+    }
+  }
+  return sum;
+}
+
 // ---- SetNewPrtclGID, src/bvals/bvals_part.cpp:159-429 (single level, no shear x1) -------
-__global__ void k_route(PCtx P, MCtx M, Ind d, int x3bc, double *x3rem, unsigned *err) {
+__global__ void k_route(PCtx P, MCtx M, Ind d, int x3bc, double *x3rem, unsigned *err, SBox B) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
   int m = P.i(DUSTB_PGID, p) - M.gids;
@@ -198,6 +386,30 @@ __global__ void k_route(PCtx P, MCtx M, Ind d, int x3bc, double *x3rem, unsigned
   const bool hi2 = (iy > 0) && (M.s(m, X2MAX) > M.x2max - 0.5 * ly);
   const bool lo3 = (iz < 0) && (M.s(m, X3MIN) < M.x3min + 0.5 * lz);
   const bool hi3 = (iz > 0) && (M.s(m, X3MAX) > M.x3max - 0.5 * lz);
+  if (B.on && (lo1 || hi1)) {
+    // a radial face (bvals_part.cpp:266-310): wrap x, shift y by the folded shear offset,
+    // wrap y and z, route to the face block on the other side at the new (y, z)
+    const bool cross_in = lo1;
+    const double lxm = M.x1max - M.x1min;
+    P.r(DUSTB_IPX, p) += cross_in ? lxm : -lxm;
+    P.r(DUSTB_IPX1, p) += cross_in ? lxm : -lxm;
+    const double lym = M.x2max - M.x2min;
+    double ynew = P.r(DUSTB_IPY, p) + (cross_in ? -B.ysh : B.ysh);
+    if (ynew < M.x2min) ynew += lym;
+    if (ynew >= M.x2max) ynew -= lym;
+    const double dy = ynew - P.r(DUSTB_IPY, p);
+    P.r(DUSTB_IPY, p) = ynew;
+    P.r(DUSTB_IPY1, p) += dy;
+    const double lzm = M.x3max - M.x3min;
+    if (lo3) { P.r(DUSTB_IPZ, p) += lzm; P.r(DUSTB_IPZ1, p) += lzm; }
+    else if (hi3) { P.r(DUSTB_IPZ, p) -= lzm; P.r(DUSTB_IPZ1, p) -= lzm; }
+    int b2 = (int)(((P.r(DUSTB_IPY, p) - M.x2min) / lym) * (double)B.nb2);
+    b2 = (b2 < 0) ? 0 : ((b2 > B.nb2 - 1) ? B.nb2 - 1 : b2);
+    int b3 = (int)(((P.r(DUSTB_IPZ, p) - M.x3min) / lzm) * (double)B.nb3);
+    b3 = (b3 < 0) ? 0 : ((b3 > B.nb3 - 1) ? B.nb3 - 1 : b3);
+    P.i(DUSTB_PGID, p) = B.sb_gid[((long long)(cross_in ? 1 : 0) * B.nb3 + b3) * B.nb2 + b2];
+    return;
+  }
   const int gid = M.nghbr[(long long)m * 27 + dir_slot(ix, iy, iz)];
   if (gid < 0) { report(err, DUSTB_ERR_NGHBR); return; }
   P.i(DUSTB_PGID, p) = gid;
@@ -245,8 +457,10 @@ __global__ void k_scatter(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, doub
 // RecvAndSumDeposit (src/bvals/bvals_dep.cpp:457-560): receiver active strips on side o
 // (InitRecvIndices :281-297) += the neighbour's ghost cells at index - o*nx, in
 // NeighborIndex order.
+
 // fold: fold the ghost deposits beyond physical x3 faces back into the mirrored active cells
-__global__ void k_ghost_add(Ind d, const int *nghbr, int gids, double *a, int nvar, int fold) {
+__global__ void k_ghost_add(Ind d, const int *nghbr, int gids, double *a, int nvar, int fold,
+                            SBox B) {
   int m, k, j, i;
   long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   long long ncell = (long long)d.nmb * d.nx3 * d.nx2 * d.nx1;
@@ -269,7 +483,7 @@ __global__ void k_ghost_add(Ind d, const int *nghbr, int gids, double *a, int nv
     if (o3 > 0 && k < d.ke - ng1) continue;
     if (o3 < 0 && k > d.ks + ng1) continue;
     const int src = nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)] - gids;
-    if (src < 0 || src >= d.nmb) continue;
+    if (src < 0 || src >= d.nmb || B.crossing(m, o1)) continue;
     val += a[d.at(src, nvar, v, k - o3 * d.nx3, j - o2 * d.nx2, i - o1 * d.nx1)];
   }
   if (fold && d.three_d) {
@@ -290,11 +504,14 @@ __global__ void k_ghost_add(Ind d, const int *nghbr, int gids, double *a, int nv
         if (o2 > 0 && j < d.je - ng1) continue;
         if (o2 < 0 && j > d.js + ng1) continue;
         const int src = nghbr[(long long)m * 27 + dir_slot(o1, o2, 0)] - gids;
-        if (src < 0 || src >= d.nmb) continue;
+        if (src < 0 || src >= d.nmb || B.crossing(m, o1)) continue;
         val += a[d.at(src, nvar, v, kg, j - o2 * d.nx2, i - o1 * d.nx1)];
       }
     }
   }
+  // shear-periodic x1 faces: the remapped ghost cells beyond them (their sum added as
+  // DepRemapPlan's GeneralApply adds it)
+  if (B.on) val += shear_add_sum(B, d, a, nvar, m, v, k, j, i);
   a[at] = val;
 }
 
@@ -863,7 +1080,9 @@ int dustb_route(const dustb_ctx *c, double *x3_removed, void *stream) {
   if (c->mesh.x3bc == DUSTB_X3_OUTFLOW && !x3_removed) return DUSTB_EINVAL;
   if (c->part.npart == 0) return DUSTB_OK;
   Ind d = make_ind(c->mesh);
-  k_route<<<PGRID(c)>>>(pview(c), mview(c), d, c->mesh.x3bc, x3_removed, c->err);
+  const SBox B = sbview(c);
+  if (B.on && (!B.sb_gid || B.nb2 <= 0 || B.nb3 <= 0)) return DUSTB_EINVAL;
+  k_route<<<PGRID(c)>>>(pview(c), mview(c), d, c->mesh.x3bc, x3_removed, c->err, B);
   return launch_status("route");
 }
 
@@ -881,7 +1100,8 @@ int dustb_ghost_add(const dustb_ctx *c, double *field, int nvar, void *stream) {
   if (!field || nvar <= 0) return DUSTB_EINVAL;
   Ind d = make_ind(c->mesh);
   const int fold = d.three_d && c->mesh.x3bc != DUSTB_X3_PERIODIC && !c->phys.x3_deposit_drop;
-  k_ghost_add<<<blocks_for(n_active(d) * nvar), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar, fold);
+  k_ghost_add<<<blocks_for(n_active(d) * nvar), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar, fold,
+                                                                          sbview(c));
   return launch_status("ghost_add");
 }
 
@@ -890,6 +1110,14 @@ int dustb_ghost_copy(const dustb_ctx *c, double *field, int nvar, int x3_bcs, vo
   if (!field || nvar <= 0) return DUSTB_EINVAL;
   Ind d = make_ind(c->mesh);
   k_ghost_copy<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar);
+  const SBox B = sbview(c);
+  if (B.on) {
+    // the shearing box remap of the x1 ghost strips, after the plain copy and before the
+    // x3 boundary values (RecvUstar -> RecvUstarShr -> FinishUstarGhosts, dust_tasks.cpp)
+    if (!B.sb_gid || B.nb2 <= 0 || B.nb3 <= 0) return DUSTB_EINVAL;
+    k_shear_copy<<<blocks_for(2LL * B.nb3 * B.nb2 * nvar * d.n3 * d.n2 * d.ng), kThreads, 0, S(stream)>>>(
+        B, d, field, nvar);
+  }
   if (x3_bcs && nvar == 3 && d.three_d && c->mesh.x3bc != DUSTB_X3_PERIODIC)
     k_x3_bcs<<<blocks_for((long long)d.ng * d.n2 * d.n1 * d.nmb), kThreads, 0, S(stream)>>>(
         d, c->mesh.nghbr, field, c->mesh.x3bc == DUSTB_X3_REFLECT);

@@ -1052,6 +1052,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
   if (co->sh[0] != 0.0 || co->sh[1] != 0.0) return DUSTB_EUNSUP;   // shear shift: FP64 form
   if (c->mesh.x3bc != DUSTB_X3_PERIODIC) return DUSTB_EUNSUP;       // physical x3: FP64 form
   if (!c->mesh.multi_d) return DUSTB_EUNSUP;                        // 1-D: FP64 form
+  if (c->mesh.shear_x1) return DUSTB_EUNSUP;                        // shearing box: FP64 form
   MState S;
   if (!carve(c->mesh, c->part.npart, ws, bytes, S, nullptr)) return DUSTB_ESCRATCH;
   Cfg cf;

@@ -53,6 +53,7 @@ class DeviceDust:
             "work": torch.zeros(ms.field_shape(3), **f64),
             "mb_size": torch.from_numpy(np.ascontiguousarray(ms.mb_size)).to(self.device),
             "nghbr": torch.from_numpy(np.ascontiguousarray(ms.nghbr)).to(self.device),
+            "sb_gid": torch.from_numpy(np.ascontiguousarray(ms.sb_gid)).to(self.device),
             "err": torch.zeros(1, dtype=torch.int32, device=self.device),
             "x3_removed": torch.zeros(2, **f64),
             "scalar": torch.zeros(2, **f64),
@@ -86,6 +87,7 @@ class DeviceDust:
             "work": torch.zeros(mesh.field_shape(3), **f64),
             "mb_size": torch.from_numpy(np.ascontiguousarray(mesh.mb_size)).to(self.device),
             "nghbr": torch.from_numpy(np.ascontiguousarray(mesh.nghbr)).to(self.device),
+            "sb_gid": torch.from_numpy(np.ascontiguousarray(mesh.sb_gid)).to(self.device),
             "err": torch.zeros(1, dtype=torch.int32, device=self.device),
             "x3_removed": torch.zeros(2, **f64),
             "scalar": torch.zeros(2, **f64),
@@ -100,7 +102,13 @@ class DeviceDust:
 
     def _rebuild_ctx(self):
         self.ctx = capi.make_ctx(self.mesh, self.t, self.npart, self.stride, self.phys)
+        self.ctx.mesh.time = self.__dict__.get("time", 0.0)
         self.pctx = C.byref(self.ctx)
+
+    def set_time(self, t):
+        """The mesh time the next calls use (the shear offset of shear-periodic x1 faces)."""
+        self.time = float(t)
+        self.ctx.mesh.time = self.time
 
     def __getattr__(self, name):
         t = self.__dict__.get("t")

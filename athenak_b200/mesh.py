@@ -35,6 +35,19 @@ class MeshSpec:
     mb_size: np.ndarray = field(repr=False)   # (nmb, 9) float64
     nghbr: np.ndarray = field(repr=False)     # (nmb, 27) int32
     gids: int = 0
+    shear_x1: bool = False                    # shear-periodic x1 faces (3-D shearing box)
+
+    @property
+    def sb_gid(self) -> np.ndarray:
+        """(2, nb3, nb2) int32: gid of the inner (0) and outer (1) x1-face block at (b3, b2)
+        (blocks are numbered (b3*nb2 + b2)*nb1 + b1)."""
+        nb1, nb2, nb3 = self.nblocks
+        t = np.zeros((2, nb3, nb2), np.int32)
+        for b3 in range(nb3):
+            for b2 in range(nb2):
+                t[0, b3, b2] = (b3 * nb2 + b2) * nb1 + self.gids
+                t[1, b3, b2] = (b3 * nb2 + b2) * nb1 + nb1 - 1 + self.gids
+        return t
 
     @property
     def nmb(self) -> int:
@@ -74,9 +87,10 @@ class MeshSpec:
 
 
 def uniform_mesh(ncells=(32, 32, 32), nblock=(16, 16, 16), ng=2,
-                 lo=(-0.5, -0.5, -0.5), hi=(0.5, 0.5, 0.5), x3bc=0) -> MeshSpec:
+                 lo=(-0.5, -0.5, -0.5), hi=(0.5, 0.5, 0.5), x3bc=0,
+                 shear_x1=False) -> MeshSpec:
     """A uniform mesh of ncells cells split into blocks of nblock cells; periodic in x1, x2
-    and, unless x3bc != 0, in x3."""
+    and, unless x3bc != 0, in x3; shear_x1: the x1 faces are shear-periodic (3-D)."""
     three_d = ncells[2] > 1
     multi_d = ncells[1] > 1
     if not multi_d:
@@ -126,5 +140,8 @@ def uniform_mesh(ncells=(32, 32, 32), nblock=(16, 16, 16), ng=2,
         mb[:, X3MIN] = lo[2]
         mb[:, X3MAX] = hi[2]
         mb[:, DX3] = hi[2] - lo[2]
+    if shear_x1 and not three_d:
+        raise ValueError("shear-periodic x1 faces need a 3-D mesh")
     return MeshSpec(nx=tuple(nblock), nblocks=nb, ng=ng, lo=tuple(lo), hi=tuple(hi),
-                    three_d=three_d, multi_d=multi_d, x3bc=x3bc, mb_size=mb, nghbr=ng_tab)
+                    three_d=three_d, multi_d=multi_d, x3bc=x3bc, mb_size=mb, nghbr=ng_tab,
+                    shear_x1=bool(shear_x1))

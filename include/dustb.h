@@ -79,6 +79,15 @@ typedef struct dustb_mesh {
   double x1min, x1max, x2min, x2max, x3min, x3max;   /* mesh_size */
   const double *mb_size;   /* nmb x 9 */
   const int *nghbr;        /* nmb x 27 */
+  /* shear-periodic x1 faces (3-D shearing box, <mesh>/ix1_bc = shear_periodic); 0: off.
+   * nghbr keeps the plain periodic x1 neighbours; the shear maps the faces onto each other
+   * shifted in x2 by the shear offset q Omega Lx time. */
+  int shear_x1;
+  int sb_nb2, sb_nb3;      /* MeshBlocks of one radial face along x2 and x3 */
+  const int *sb_gid;       /* 2 x sb_nb3 x sb_nb2: gid of the face block (0 inner, 1 outer)
+                              at (b3, b2) (the ShearingBox x1 boundary maps, bvals_part.cpp
+                              sgid_map) */
+  double time;             /* mesh time of the cycle (the offset of every stage's remaps) */
 } dustb_mesh;
 
 typedef struct dustb_particles {

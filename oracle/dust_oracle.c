@@ -182,13 +182,19 @@ void oracle_push_imex(const dustb_ctx *c, double gam0, double gam1, double beta_
   }
 }
 
-/* SetNewPrtclGID, src/bvals/bvals_part.cpp:115-429, single-level mesh without shear-periodic
- * x1 faces.  Returns the OR of the error bits of the particles it could not route. */
+/* SetNewPrtclGID, src/bvals/bvals_part.cpp:115-429, single-level mesh (shear-periodic x1 faces
+ * :133-141, :266-310).  Returns the OR of the error bits of the particles it could not route. */
 unsigned oracle_route(const dustb_ctx *c, double *x3_removed) {
   const dustb_mesh *ms = &c->mesh;
   double *pr = c->part.pr; int *pi = c->part.pi; long long stride = c->part.stride;
   unsigned err = 0;
   const double z3a = ms->x3min, z3b = ms->x3max;
+  const int shear_x1 = ms->shear_x1 && ms->three_d;
+  double ysh = 0.0;
+  if (shear_x1) {
+    const double lxm = ms->x1max - ms->x1min, lym = ms->x2max - ms->x2min;
+    ysh = fmod(c->phys.qshear*c->phys.omega0*lxm*(ms->time), lym);
+  }
   for (int p = 0; p < c->part.npart; ++p) {
     int m = PI(DUSTB_PGID, p) - ms->gids;
     if (m < 0 || m >= ms->nmb) { err |= DUSTB_ERR_PGID; continue; }
@@ -241,6 +247,30 @@ unsigned oracle_route(const dustb_ctx *c, double *x3_removed) {
     const int hi2 = (iy > 0) && (MB(m, X2MAX) > ms->x2max - 0.5*ly);
     const int lo3 = (iz < 0) && (MB(m, X3MIN) < ms->x3min + 0.5*lz);
     const int hi3 = (iz > 0) && (MB(m, X3MAX) > ms->x3max - 0.5*lz);
+    if (shear_x1 && (lo1 || hi1)) {
+      /* a radial face: wrap x, shift y by the (folded) shear offset, wrap y and z, route to the
+       * face block on the other side at the new (y, z); the registers move with the position */
+      const int cross_in = lo1;
+      const double lxm = ms->x1max - ms->x1min;
+      PR(DUSTB_IPX, p) += cross_in ? lxm : -lxm;
+      PR(DUSTB_IPX1, p) += cross_in ? lxm : -lxm;
+      const double lym = ms->x2max - ms->x2min;
+      double ynew = PR(DUSTB_IPY, p) + (cross_in ? -ysh : ysh);
+      if (ynew < ms->x2min) ynew += lym;
+      if (ynew >= ms->x2max) ynew -= lym;
+      const double dy = ynew - PR(DUSTB_IPY, p);
+      PR(DUSTB_IPY, p) = ynew;
+      PR(DUSTB_IPY1, p) += dy;
+      const double lzm = ms->x3max - ms->x3min;
+      if (lo3) { PR(DUSTB_IPZ, p) += lzm; PR(DUSTB_IPZ1, p) += lzm; }
+      else if (hi3) { PR(DUSTB_IPZ, p) -= lzm; PR(DUSTB_IPZ1, p) -= lzm; }
+      int b2 = (int)(((PR(DUSTB_IPY, p) - ms->x2min)/lym)*(double)ms->sb_nb2);
+      b2 = (b2 < 0) ? 0 : ((b2 > ms->sb_nb2 - 1) ? ms->sb_nb2 - 1 : b2);
+      int b3 = (int)(((PR(DUSTB_IPZ, p) - ms->x3min)/lzm)*(double)ms->sb_nb3);
+      b3 = (b3 < 0) ? 0 : ((b3 > ms->sb_nb3 - 1) ? ms->sb_nb3 - 1 : b3);
+      PI(DUSTB_PGID, p) = ms->sb_gid[((size_t)(cross_in ? 1 : 0)*ms->sb_nb3 + b3)*ms->sb_nb2 + b2];
+      continue;
+    }
     const int gid = ms->nghbr[(size_t)m*27 + (iz + 1)*9 + (iy + 1)*3 + (ix + 1)];
     if (gid < 0) { err |= DUSTB_ERR_NGHBR; continue; }
     PI(DUSTB_PGID, p) = gid;
@@ -303,6 +333,188 @@ static const int kDirOrder[26][3] = {
 /* PackAndSendDeposit + RecvAndSumDeposit, same-level, one rank (src/bvals/bvals_dep.cpp:
  * 249-309 indices, :320-560 pack and sum): the sender's ghost strip in direction -ox is added
  * to the receiver's active strip on side ox, buffer by buffer in NeighborIndex order. */
+/* ---- shear-periodic x1 faces (3-D shearing box) ------------------------------------------ */
+
+/* faces of block m: bit 1 the inner x1 face, bit 2 the outer (bvals_part.cpp:260-261) */
+static int sb_faces(const dustb_mesh *ms, int m) {
+  const double lx = MB(m, X1MAX) - MB(m, X1MIN);
+  int f = 0;
+  if (MB(m, X1MIN) < ms->x1min + 0.5*lx) f |= 1;
+  if (MB(m, X1MAX) > ms->x1max - 0.5*lx) f |= 2;
+  return f;
+}
+
+/* the x2 and x3 block indices of block m, from its lower corner */
+static void sb_b23(const dustb_mesh *ms, int m, int *b2, int *b3) {
+  *b2 = (int)floor((MB(m, X2MIN) - ms->x2min)/((ms->x2max - ms->x2min)/ms->sb_nb2) + 0.5);
+  *b3 = (int)floor((MB(m, X3MIN) - ms->x3min)/((ms->x3max - ms->x3min)/ms->sb_nb3) + 0.5);
+}
+
+/* local index of the face block (face f, b3, b2), or -1 */
+static int sb_block(const dustb_mesh *ms, int f, int b3, int b2) {
+  const int g = ms->sb_gid[((size_t)f*ms->sb_nb3 + b3)*ms->sb_nb2 + b2] - ms->gids;
+  return (g >= 0 && g < ms->nmb) ? g : -1;
+}
+
+/* the active cell owning cell (k, j, i) of block m, in active-relative indices at most one
+ * block beyond the block (the plain neighbour table); 0 if no block owns it */
+static int owner_cell(const dustb_mesh *ms, int m, int *k, int *j, int *i, int *mo) {
+  const int o1 = (*i < 0) ? -1 : ((*i >= ms->nx1) ? 1 : 0);
+  const int o2 = (*j < 0) ? -1 : ((*j >= ms->nx2) ? 1 : 0);
+  const int o3 = (*k < 0) ? -1 : ((*k >= ms->nx3) ? 1 : 0);
+  if ((o1 | o2 | o3) == 0) { *mo = m; return 1; }
+  const int gid = ms->nghbr[(size_t)m*27 + (o3 + 1)*9 + (o2 + 1)*3 + (o1 + 1)];
+  if (gid < 0) return 0;
+  *mo = gid - ms->gids;
+  *i -= o1*ms->nx1; *j -= o2*ms->nx2; *k -= o3*ms->nx3;
+  return 1;
+}
+
+/* PLM_RemapFlx and the update a - (flx(j+1) - flx(j)) of ShearingBoxCC::PackAndSend
+ * (src/shearing_box/remap_fluxes.hpp:30-55, shearing_box_cc.cpp:118-140) at one row, from
+ * g[t] = the row's column at rows r - 2 + t, t = 0..4 */
+static double sb_remap(const double g[5], double eps) {
+  double f[2];
+  for (int h = 0; h < 2; ++h) {
+    const int q = 2 + h;                 /* face between rows q-1 and q of g */
+    double dql, dqr;
+    if (eps > 0.0) { dql = g[q-1] - g[q-2]; dqr = g[q] - g[q-1]; }
+    else { dql = g[q] - g[q-1]; dqr = g[q+1] - g[q]; }
+    const double dq2 = dql*dqr;
+    double dqm = 2.0*dq2/(dql + dqr);
+    if (dq2 <= 0.0) dqm = 0.0;
+    f[h] = (eps > 0.0) ? eps*(g[q-1] + 0.5*(1.0 - eps)*dqm) : eps*(g[q] - 0.5*(1.0 + eps)*dqm);
+  }
+  return g[2] - (f[1] - f[0]);
+}
+
+/* ShearingBoxCC::PackAndSend + RecvAndUnpack on one device (the conservative PLM remap of the
+ * x1 ghost strips after the plain periodic copy, shearing_box_cc.cpp:78-197, integer pieces
+ * shearing_box.cpp:260-330): the ghost strip of a face block at row J (its y-ghost rows and
+ * x3 ghost planes included) takes the remapped periodic strip of the face block holding row
+ * J - joffset (inner face; + joffset at the outer), joffset + eps = q Omega Lx t / dy.  The
+ * periodic strip is read from the active cells that the plain copy takes it from. */
+static void shear_copy(const dustb_ctx *c, double *a, int nvar) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  if (!ms->shear_x1 || !ms->three_d) return;
+  const double lx = ms->x1max - ms->x1min;
+  const double yshear = (c->phys.qshear*c->phys.omega0)*lx*ms->time;
+  const int nb2 = ms->sb_nb2, nb3 = ms->sb_nb3;
+  const long long Ny = (long long)nb2*ms->nx2;
+  for (int n = 0; n < 2; ++n)
+    for (int b3 = 0; b3 < nb3; ++b3)
+      for (int b2 = 0; b2 < nb2; ++b2) {
+        const int T = sb_block(ms, n, b3, b2);
+        if (T < 0) continue;
+        const double dy = MB(T, DX2);
+        const long long joffset = (long long)(yshear/dy);
+        double eps = fmod(yshear, dy)/dy;
+        if (n == 1) eps *= -1.0;
+        for (int v = 0; v < nvar; ++v)
+          for (int k = 0; k < d.n3; ++k)
+            for (int j = 0; j < d.n2; ++j)
+              for (int i = 0; i < ms->ng; ++i) {
+                const long long J = (long long)b2*ms->nx2 + (j - d.js);
+                long long R = (n == 0) ? J - joffset : J + joffset;
+                R %= Ny; if (R < 0) R += Ny;
+                const int S = sb_block(ms, n, b3, (int)(R/ms->nx2));
+                if (S < 0) continue;
+                const int r = (int)(R % ms->nx2);          /* active-relative row of S */
+                const int xr = (n == 0) ? i - ms->ng : ms->nx1 + i;
+                double g[5];
+                int ok = 1;
+                for (int t = 0; t < 5 && ok; ++t) {
+                  int kk = k - d.ks, jj = r - 2 + t, ii = xr, mo;
+                  ok = owner_cell(ms, S, &kk, &jj, &ii, &mo);
+                  if (ok) g[t] = A5(a, nvar, d, mo, v, d.ks + kk, d.js + jj, d.is + ii);
+                }
+                if (!ok) continue;
+                A5(a, nvar, d, T, v, k, j, (n == 0) ? i : d.ie + 1 + i) = sb_remap(g, eps);
+              }
+      }
+}
+
+/* whether direction o1 from block m crosses a shear-periodic x1 face (those ghost cells are
+ * remapped, not exchanged plainly) */
+static int shear_crossing(const dustb_ctx *c, int m, int o1) {
+  const dustb_mesh *ms = &c->mesh;
+  if (!ms->shear_x1 || !ms->three_d || o1 == 0) return 0;
+  const int f = sb_faces(ms, m);
+  return (o1 < 0) ? (f & 1) : ((f & 2) != 0);
+}
+
+/* The shear part of the deposit remap (DepRemapPlan part 1, bvals_dep_general.cpp:99-240) for
+ * active cell (k, j, i) of face block m: the ghost cells beyond the opposite x1 face, moved by
+ * the box length and shifted in x2 by +shR (beyond the outer face) or -shR (beyond the inner
+ * face) cells, add w * value, w = their overlap with the cell (piecewise-constant remap).
+ * Source ghost planes in x3 reach the cell through the periodic wrap or, at a physical face,
+ * the fold.  Sources in a fixed order: faces (inner-face targets first), source planes (the
+ * cell's plane, then the ghost plane below or folded, then above), source blocks along x2
+ * (offsets -1, 0, 1, each block once), source rows, images. */
+static double shear_add_sum(const dustb_ctx *c, const Ind *d, const double *a, int nvar,
+                            int m, int v, int k, int j, int i) {
+  const dustb_mesh *ms = &c->mesh;
+  const int faces = sb_faces(ms, m);
+  const int ng1 = ms->ng - 1;
+  const double lx = ms->x1max - ms->x1min, ly = ms->x2max - ms->x2min;
+  const double ysh = fmod(c->phys.qshear*c->phys.omega0*lx*ms->time, ly);
+  const long long N2 = (long long)ms->sb_nb2*ms->nx2;
+  const double shR = ysh*(double)N2/ly;
+  int b2, b3;
+  sb_b23(ms, m, &b2, &b3);
+  const int nb2 = ms->sb_nb2, nb3 = ms->sb_nb3;
+  const long long J = (long long)b2*ms->nx2 + (j - d->js);
+  double sum = 0.0;
+  for (int side = 0; side < 2; ++side) {
+    /* side 0: this block at the inner face, sources beyond the outer face (+shR) */
+    if (!(faces & (side ? 2 : 1))) continue;
+    const int g = side ? i - (d->ie - ng1) : i - d->is;
+    if (g < 0 || g > ng1) continue;
+    const int sface = side ? 0 : 1;
+    const int si = side ? g : d->ie + 1 + g;                 /* source ghost column */
+    const double sh = side ? -shR : shR;
+    const long long F = (long long)floor((double)J - sh);
+    for (int zc = 0; zc < 3; ++zc) {
+      int sb3 = b3, sk = k;
+      if (zc == 1) {                                        /* below the cell's plane */
+        if (k > d->ks + ng1) continue;
+        if (b3 > 0 || ms->x3bc == 0) { sb3 = (b3 + nb3 - 1) % nb3; sk = k + ms->nx3; }
+        else if (!c->phys.x3_deposit_drop) { sk = 2*d->ks - 1 - k; }
+        else continue;
+      } else if (zc == 2) {                                 /* above */
+        if (k < d->ke - ng1) continue;
+        if (b3 < nb3 - 1 || ms->x3bc == 0) { sb3 = (b3 + 1) % nb3; sk = k - ms->nx3; }
+        else if (!c->phys.x3_deposit_drop) { sk = 2*d->ke + 1 - k; }
+        else continue;
+      }
+      const long long Fm = ((F % N2) + N2) % N2;
+      const int bc = (int)(Fm/ms->nx2);
+      int seen[3] = {-1, -1, -1};
+      for (int db = -1; db <= 1; ++db) {
+        const int sb2 = ((bc + db) % nb2 + nb2) % nb2;
+        if (sb2 == seen[0] || sb2 == seen[1]) continue;
+        seen[db + 1] = sb2;
+        const int S = sb_block(ms, sface, sb3, sb2);
+        if (S < 0) continue;
+        for (long long Yc = F - 1; Yc <= F + 1; ++Yc)
+          for (int q = -1; q <= 1; ++q) {
+            /* the source row Yc + q N2 of S's strip (its ghost rows included) */
+            const long long Y = Yc + q*N2;
+            const long long sj = Y - (long long)sb2*ms->nx2 + d->js;
+            if (sj < 0 || sj >= d->n2) continue;
+            const double ya = (double)Y + sh, yb = (double)(Y + 1) + sh;
+            for (int im = -2; im <= 2; ++im) {
+              const double clo = (double)(J + im*N2), chi = clo + 1.0;
+              const double o = fmin(yb, chi) - fmax(ya, clo);
+              if (o > 0.0) sum += o*A5(a, nvar, (*d), S, v, sk, (int)sj, si);
+            }
+          }
+      }
+    }
+  }
+  return sum;
+}
+
 void oracle_ghost_add(const dustb_ctx *c, double *a, int nvar) {
   const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
   const int ng1 = ms->ng - 1;
@@ -334,7 +546,7 @@ void oracle_ghost_add(const dustb_ctx *c, double *a, int nvar) {
     for (int n = 0; n < ndir; ++n) {
       const int *o = kDirOrder[n];
       int gid = ms->nghbr[(size_t)m*27 + (o[2] + 1)*9 + (o[1] + 1)*3 + (o[0] + 1)];
-      if (gid < 0) continue;
+      if (gid < 0 || shear_crossing(c, m, o[0])) continue;
       int src = gid - ms->gids;
       size_t q = boff[n] + (size_t)m*nvar*((hi[n][0]-lo[n][0]+1)*(hi[n][1]-lo[n][1]+1)*(hi[n][2]-lo[n][2]+1));
       for (int v = 0; v < nvar; ++v)
@@ -347,7 +559,7 @@ void oracle_ghost_add(const dustb_ctx *c, double *a, int nvar) {
     for (int n = 0; n < ndir; ++n) {
       const int *o = kDirOrder[n];
       int gid = ms->nghbr[(size_t)m*27 + (o[2] + 1)*9 + (o[1] + 1)*3 + (o[0] + 1)];
-      if (gid < 0) continue;
+      if (gid < 0 || shear_crossing(c, m, o[0])) continue;
       size_t q = boff[n] + (size_t)m*nvar*((hi[n][0]-lo[n][0]+1)*(hi[n][1]-lo[n][1]+1)*(hi[n][2]-lo[n][2]+1));
       for (int v = 0; v < nvar; ++v)
         for (int k = lo[n][2]; k <= hi[n][2]; ++k)
@@ -362,7 +574,7 @@ void oracle_ghost_add(const dustb_ctx *c, double *a, int nvar) {
    * the x1/x2 neighbours' ghost strips facing the cell, in NeighborIndex order.  (The
    * reference sums a target's contributions in (source gid, source cell) order; the sums here
    * differ from it by rounding only.)  The ghost cells read are untouched by the exchange. */
-  if (!ms->three_d || ms->x3bc == 0 || c->phys.x3_deposit_drop) return;
+  if (ms->three_d && ms->x3bc != 0 && !c->phys.x3_deposit_drop)
   for (int m = 0; m < ms->nmb; ++m)
     for (int side = 0; side < 2; ++side) {
       const int o3 = side ? 1 : -1;
@@ -382,14 +594,39 @@ void oracle_ghost_add(const dustb_ctx *c, double *a, int nvar) {
                 if (o[1] > 0 && j < d.je - ng1) continue;
                 if (o[1] < 0 && j > d.js + ng1) continue;
                 int gid = ms->nghbr[(size_t)m*27 + 1*9 + (o[1] + 1)*3 + (o[0] + 1)];
-                if (gid < 0) continue;
+                if (gid < 0 || shear_crossing(c, m, o[0])) continue;
                 val += A5(a, nvar, d, gid - ms->gids, v, kg, j - o[1]*nx[1], i - o[0]*nx[0]);
               }
               A5(a, nvar, d, m, v, k, j, i) = val;
             }
       }
     }
+  /* shear-periodic x1 faces: the ghost cells beyond them, remapped (the sums of the sources
+   * are added to the cells as DepRemapPlan adds them, GeneralApply) */
+  if (!ms->shear_x1 || !ms->three_d) return;
+  const size_t ncell = (size_t)d.n1*d.n2*d.n3;
+  double *add = (double *)calloc((size_t)ms->nmb*nvar*ncell, sizeof(double));
+  for (int m = 0; m < ms->nmb; ++m) {
+    if (!sb_faces(ms, m)) continue;
+    for (int v = 0; v < nvar; ++v)
+      for (int k = d.ks; k <= d.ke; ++k)
+        for (int j = d.js; j <= d.je; ++j)
+          for (int i = d.is; i <= d.ie; ++i)
+            add[(((size_t)m*nvar + v)*d.n3 + k)*d.n2*d.n1 + (size_t)j*d.n1 + i] =
+                shear_add_sum(c, &d, a, nvar, m, v, k, j, i);
+  }
+  /* (all sums read the ghost cells before any cell changes: they are never written) */
+  for (int m = 0; m < ms->nmb; ++m) {
+    if (!sb_faces(ms, m)) continue;
+    for (int v = 0; v < nvar; ++v)
+      for (int k = d.ks; k <= d.ke; ++k)
+        for (int j = d.js; j <= d.je; ++j)
+          for (int i = d.is; i <= d.ie; ++i)
+            A5(a, nvar, d, m, v, k, j, i) += add[(((size_t)m*nvar + v)*d.n3 + k)*d.n2*d.n1 + (size_t)j*d.n1 + i];
+  }
+  free(add);
 }
+
 
 /* UstarX3BCs, src/dust/dust_tasks.cpp:445-469 (single level) */
 static void ustar_x3_bcs(const dustb_ctx *c, double *a) {
@@ -440,6 +677,7 @@ void oracle_ghost_copy(const dustb_ctx *c, double *a, int nvar, int x3_bcs) {
             A5(a, nvar, d, m, v, k, j, i) =
                 A5(a, nvar, d, src, v, k - o[2]*nx[2], j - o[1]*nx[1], i - o[0]*nx[0]);
         }
+  shear_copy(c, a, nvar);
   if (x3_bcs && nvar == 3) ustar_x3_bcs(c, a);
 }
 

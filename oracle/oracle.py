@@ -102,11 +102,16 @@ class Oracle:
             "resid": np.zeros(ms.field_shape(4)), "work": np.zeros(ms.field_shape(3)),
             "mb_size": np.ascontiguousarray(ms.mb_size),
             "nghbr": np.ascontiguousarray(ms.nghbr),
+            "sb_gid": np.ascontiguousarray(ms.sb_gid),
         }
         self.phys = dict(phys)
         self.ctx = capi.make_ctx(ms, self.arr, self.st.npart, self.st.stride, self.phys)
         self.threads = threads
         self.x3_removed = np.zeros(2)
+
+    def set_time(self, t):
+        """The mesh time the next calls use (the shear offset of shear-periodic x1 faces)."""
+        self.ctx.mesh.time = float(t)
 
     def __getattr__(self, name):
         arr = self.__dict__.get("arr")

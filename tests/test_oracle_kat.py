@@ -261,3 +261,95 @@ def test_x3_fold_conserves_the_deposit(drop):
         assert q < expect * (1.0 - 1e-3)
     else:
         assert abs(q - expect) < 1e-13 * expect
+
+
+def shear_mesh(x3bc=0):
+    return uniform_mesh((16, 32, 16), (8, 8, 8), 2, (-0.05, -0.1, -0.05), (0.05, 0.1, 0.05),
+                        x3bc=x3bc, shear_x1=True)
+
+
+def test_shear_remap_of_ghost_strips_shifts_the_profile():
+    """Shear-periodic x1 faces: after the plain periodic copy the x1 ghost strips are
+    remapped (PLM) by the shear offset q Omega Lx t: the inner strip holds the outer edge's
+    profile shifted by +offset in x2, the outer strip the inner edge's by -offset."""
+    ms = shear_mesh()
+    st = make_state(ms, [0.1], [1.0], 1, seed=2)
+    o = Oracle(st, dict(scheme=2, shearing_box=True))
+    t = 0.37
+    o.set_time(t)
+    N2 = 32
+    dy = 0.2 / N2
+    s_cells = 1.5 * 1.0 * 0.1 * t / dy                      # q Omega Lx t / dy
+    is_, js, ks = ms.starts
+    u = o.ustar
+    for m in range(ms.nmb):
+        b2 = int(round((ms.mb_size[m, 1] + 0.1) / (0.2 / 4)))
+        rows = b2 * 8 + np.arange(-js, 8 + js)
+        u[m, :, :, :, :] = np.sin(2 * np.pi * (rows + 0.5) / N2)[None, None, :, None]
+    o.ghost_copy("ustar", 3, 0)
+    for m in range(ms.nmb):
+        b2 = int(round((ms.mb_size[m, 1] + 0.1) / (0.2 / 4)))
+        rows = b2 * 8 + np.arange(-js, 8 + js)
+        if ms.mb_size[m, 0] < -0.05 + 0.025:                # inner face: shifted by +s
+            want = np.sin(2 * np.pi * (rows + 0.5 - s_cells) / N2)
+            got = u[m, 0, ks, :, 0]
+        elif ms.mb_size[m, 3] > 0.05 - 0.025:                # outer face: shifted by -s
+            want = np.sin(2 * np.pi * (rows + 0.5 + s_cells) / N2)
+            got = u[m, 0, ks, :, -1]
+        else:
+            continue
+        assert np.abs(got - want).max() < 2e-2
+
+
+@pytest.mark.parametrize("x3bc", [0, 1])
+def test_shear_deposit_remap_conserves(x3bc):
+    """The ghost deposits beyond the shear-periodic x1 faces are moved to the other face and
+    shifted by the particles' shear offset (piecewise-constant overlaps): the total deposit
+    is kept exactly."""
+    ms = shear_mesh(x3bc)
+    st = make_state(ms, [0.1, 0.01], [1.0, 0.5], 2, seed=11)
+    o = Oracle(st, dict(scheme=2, shearing_box=True))
+    o.set_time(0.73)
+    a_dt = 1e-3
+    o.deposit_qp(a_dt)
+    o.ghost_add("qdep", 5)
+    q = ms.active(o.qdep)[:, 0].sum() * ms.cell_volume()
+    n = st.npart
+    expect = (st.pr[16, :n] * a_dt / (st.pr[15, :n] + a_dt)).sum()
+    assert abs(q - expect) < 1e-13 * expect
+
+
+def test_shear_route_shifts_radial_crossers():
+    """A particle leaving through the outer x1 face re-enters at the inner face shifted by
+    +fmod(q Omega Lx t, Ly) in x2 (its register with it), routed to the inner-face block at
+    the new x2; one leaving through the inner face the other way."""
+    ms = shear_mesh()
+    st = make_state(ms, [0.1], [1.0], 1, seed=5)
+    o = Oracle(st, dict(scheme=2, shearing_box=True))
+    t = 2.9
+    o.set_time(t)
+    ysh = np.fmod(1.5 * 1.0 * 0.1 * t, 0.2)
+    n = o.st.npart
+    pr, pi = o.st.pr, o.st.pi
+    # two particles: one just past the outer face of an outer block, one past the inner face
+    outer = [m for m in range(ms.nmb) if ms.mb_size[m, 3] > 0.05 - 0.025]
+    inner = [m for m in range(ms.nmb) if ms.mb_size[m, 0] < -0.05 + 0.025]
+    p0, p1 = 0, 1
+    for p, m, x in ((p0, outer[3], 0.05 + 1e-4), (p1, inner[5], -0.05 - 1e-4)):
+        pi[0, p] = m
+        pr[0, p] = x
+        pr[2, p] = 0.5 * (ms.mb_size[m, 1] + ms.mb_size[m, 4])
+        pr[4, p] = 0.5 * (ms.mb_size[m, 2] + ms.mb_size[m, 5])
+        pr[6, p], pr[8, p], pr[10, p] = pr[0, p], pr[2, p], pr[4, p]
+    y0 = pr[2, [p0, p1]].copy()
+    assert o.route() == 0
+    def wrap(y):
+        return (y + 0.1) % 0.2 - 0.1
+    assert abs(pr[2, p0] - wrap(y0[0] + ysh)) < 1e-12
+    assert abs(pr[2, p1] - wrap(y0[1] - ysh)) < 1e-12
+    assert abs(pr[0, p0] - (0.05 + 1e-4 - 0.1)) < 1e-15 and abs(pr[0, p1] - (-0.05 - 1e-4 + 0.1)) < 1e-15
+    for p in (p0, p1):
+        m = pi[0, p]
+        assert ms.mb_size[m, 0] <= pr[0, p] < ms.mb_size[m, 3]
+        assert ms.mb_size[m, 1] <= pr[2, p] < ms.mb_size[m, 4]
+        assert pr[8, p] - pr[2, p] == 0.0 or abs(pr[8, p] - pr[2, p]) < 1e-12
