@@ -78,6 +78,10 @@ struct MHead {
   double a_dt;                   // that cycle's a dt (the rate change is dv / a dt)
 };
 
+// the bins of the sort: one per active cell, then the edge bin (particles whose pc2 gather
+// position lies beyond a physical x3 face or a shear-periodic x1 face), then the end
+inline long long nbins(long long ncell) { return ncell + 2; }
+
 struct MState {
   MHead *head;
   PBuf A, B;                     // A holds the shadow between cycles
@@ -94,6 +98,17 @@ struct Geo {
   const double *mb;
   double dx[3], inv_dx[3], vol;
   int scheme;
+  // 1: the tiles gather from and deposit into each block's own ghost cells (physical x3
+  // faces or shear-periodic x1 faces; the FP64 ghost exchanges run around the tiles);
+  // 0: cells beyond a block map to the owning neighbour's active cells
+  int ghost;
+  int x3bc;                    // DUSTB_X3_*
+  // shear-periodic x1 faces of a 3-D shearing box (bvals_part.cpp:266-310)
+  int sb_on, sb_nb2, sb_nb3;
+  const int *sb_gid;
+  double mx1min, mx1max, mx2min, mx3min, mly, mlz;   // mesh x1 range, lower y, z, y, z extents
+  double shR;                  // fmod(q Omega Lx t, Ly) in cells of y
+  int ncell;                   // active cells; key ncell = the edge bin (pc2 half step)
   __device__ long long at(int m, int nvar, int v, int k, int j, int i) const {
     return (((long long)m * nvar + v) * vstride) + ((long long)k * n2 + j) * n1 + i;
   }
@@ -123,10 +138,11 @@ bool carve(const dustb_mesh &ms, int n, void *ws, long long bytes, MState &S, lo
   size_t o_buf[2][2 + kNF];
   for (int b = 0; b < 2; ++b)
     for (int f = 0; f < 2 + kNF; ++f) { o_buf[b][f] = off; off += al256(4 * N); }
+  // the cell ranges: ncell cells, the edge bin (key ncell) and the end
   const size_t o_key = off; off += al256(4 * N);
-  const size_t o_cs = off; off += al256(4 * (size_t)(ncell + 1));
-  const size_t o_cur = off; off += al256(4 * (size_t)(ncell + 1));
-  const size_t o_bs = off; off += al256(4 * (size_t)scan_bsum_ints(ncell + 1));
+  const size_t o_cs = off; off += al256(4 * (size_t)(ncell + 2));
+  const size_t o_cur = off; off += al256(4 * (size_t)(ncell + 2));
+  const size_t o_bs = off; off += al256(4 * (size_t)scan_bsum_ints(ncell + 2));
   if (need) *need = (long long)off;
   if (!ws || bytes < (long long)off) return false;
   char *b = (char *)ws;
@@ -157,6 +173,20 @@ Geo make_geo(const dustb_ctx *c, const dustb_mixed_params *mp) {
   // cell volume as the reference forms it: dx1 dx2 (dx3 in 3-D), dust_pm.cpp:253-254
   G.vol = mp->dx[0] * mp->dx[1] * (ms.three_d ? mp->dx[2] : 1.0);
   G.scheme = c->phys.scheme;
+  G.x3bc = ms.three_d ? ms.x3bc : DUSTB_X3_PERIODIC;
+  G.sb_on = (ms.shear_x1 && ms.three_d) ? 1 : 0;
+  G.ghost = (G.x3bc != DUSTB_X3_PERIODIC || G.sb_on) ? 1 : 0;
+  G.sb_nb2 = ms.sb_nb2; G.sb_nb3 = ms.sb_nb3; G.sb_gid = ms.sb_gid;
+  G.mx1min = ms.x1min; G.mx1max = ms.x1max; G.mx2min = ms.x2min; G.mx3min = ms.x3min;
+  G.mly = ms.x2max - ms.x2min; G.mlz = ms.x3max - ms.x3min;
+  G.shR = 0.0;
+  if (G.sb_on) {
+    // the folded offset of the particles' crossing, as dustb_route forms it
+    const double lx = ms.x1max - ms.x1min;
+    const double ysh = fmod(c->phys.qshear * c->phys.omega0 * lx * ms.time, G.mly);
+    G.shR = ysh * (double)((long long)ms.sb_nb2 * ms.nx2) / G.mly;
+  }
+  G.ncell = (int)ncell_of(ms);
   return G;
 }
 
@@ -337,6 +367,8 @@ __global__ void k_export(double *pr, int *pi, long long stride, int n, PBuf A, G
   W(DUSTB_IPVX, vel[0]); W(DUSTB_IPVY, vel[1]); W(DUSTB_IPVZ, vel[2]);
   W(DUSTB_IPVX1, A.f[F_WX][q]); W(DUSTB_IPVY1, A.f[F_WY][q]); W(DUSTB_IPVZ1, A.f[F_WZ][q]);
   W(DUSTB_IPRX, rate[0]); W(DUSTB_IPRY, rate[1]); W(DUSTB_IPRZ, rate[2]);
+  // (the FP64 mass stays, unless an outflow face removed the particle)
+  if (A.f[F_M][q] == 0.0f) W(DUSTB_IPM, 0.0);
   pi[(long long)DUSTB_PGID * stride + p] = m + G.gids;
 }
 
@@ -349,14 +381,26 @@ __global__ void k_copy_buf(PBuf src, PBuf dst, int n) {
 }
 
 // ---- push: count and move ------------------------------------------------------------------
+// what a push does: an imex2+ stage (ExplicitPush imex), the pc2 half step to the gather
+// position (dust_pc2_advance's x_h, y_h + q Omega x_h dt/2), or the pc2 move to the new
+// position that the advance tile left as a displacement
+enum { PK_IMEX = 0, PK_HALF = 1, PK_FULL = 2 };
+// advance() flags
+enum { AF_EDGE = 1, AF_REFLECT = 2, AF_REMOVED = 4 };
+
 struct PushArgs {
+  int kind;
   float gam0, gam1, atw_dt;
   float bdt;                  // beta*dt (velocity kick)
-  float bdx[3];               // beta*dt/dx per axis (drift in cells)
-  double a_dt;
+  float bdx[3];               // beta*dt/dx per axis (drift in cells); pc2 half step: h/dx
+  float gy;                   // pc2 half step: q Omega h / dy (the gather position's y shift
+                              // per unit x of the half-step position)
+  float sdy;                  // pc2 half step: q Omega dt / dy (the new y's shear drift)
+  double a_dt;                // imex: a dt; pc2 half step: h = dt/2
   int stage2;
   int sbox, strat;
   float q, om;
+  double *x3rem;              // (mass, count) removed at outflow x3 faces (move only)
   // the consistent split's dust kick folded into the push: stage 2 applies stage 1's kick
   // (res = stage 1's dust residual); stage 1 applies the previous cycle's stage-2 kick when
   // head->pending is set (res = that residual)
@@ -378,45 +422,127 @@ __device__ __forceinline__ void consistent_dv(const Geo &G, const PushArgs &P, f
   d[2] = __dmul_rn(cj, P.res[b + 2 * G.vstride]);
 }
 
-// the new position: the drift of ExplicitPush (src/dust/dust_push.cpp:289-296) in cell units,
-// x <- x + gam1 (x1 - x) + beta dt xdot (gam0 + gam1 = 1), and the cell carry that replaces
-// SetNewPrtclGID (the neighbour in the crossing direction; periodic images are neighbours).
-// Every operation is explicitly rounded: count and move must agree bit for bit.
+// the new position in cell units, explicitly rounded so that count and move agree bit for
+// bit.  imex: the drift of ExplicitPush (src/dust/dust_push.cpp:289-296),
+// x <- x + gam1 (x1 - x) + beta dt xdot (gam0 + gam1 = 1); pc2 half step: x + h xdot with y
+// shifted by q Omega x_h h (dust_push.cpp:132-140); pc2 move: x + the displacement the
+// advance left in d1.  Then SetNewPrtclGID (src/bvals/bvals_part.cpp:159-429) as a cell
+// carry: a physical x3 face reflects or removes the particle (bvals_part.cpp:167-197), a
+// shear-periodic x1 face moves it to the face block on the other side at y -/+ the folded
+// shear offset (bvals_part.cpp:266-310), any other face hands it to the neighbour across it
+// (periodic images are neighbours).  The pc2 half step routes nothing: a gather position
+// beyond a physical x3 face or a shear face sends the particle, unmoved, to the edge bin.
 __device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, int &k, int &j,
-                                       int &i, float o[3], float d1[3], const float v[3]) {
+                                       int &i, float o[3], float d1[3], const float v[3],
+                                       int &flags, float hpos[2]) {
+  flags = 0;
+  hpos[0] = hpos[1] = 0.0f;
+  const double *sz = G.mb + (long long)m * 9;
   float xsh = 0.0f;
-  if (P.sbox && G.three_d) {
-    const double *sz = G.mb + (long long)m * 9;
+  if (P.sbox && G.three_d && P.kind != PK_FULL) {
     const double x = __dadd_rn(sz[X1MIN], __dmul_rn(__dadd_rn((double)i, (double)o[0]), G.dx[0]));
     xsh = __fmul_rn(__fmul_rn(P.q, P.om), __double2float_rn(x));
   }
   const float xdot[3] = {v[0], __fsub_rn(v[1], xsh), v[2]};
   const int nax = G.three_d ? 3 : 2;
+  float on[3] = {o[0], o[1], o[2]}, dn[3] = {d1[0], d1[1], d1[2]};
   int c[3] = {0, 0, 0};
   for (int a = 0; a < nax; ++a) {
-    const float s = __fmaf_rn(P.bdx[a], xdot[a], __fmul_rn(P.gam1, d1[a]));
-    o[a] = __fadd_rn(o[a], s);
-    d1[a] = __fsub_rn(d1[a], s);
-    int ci = (int)floorf(o[a]);
-    o[a] = __fsub_rn(o[a], (float)ci);
-    if (o[a] >= 1.0f) { o[a] = __fsub_rn(o[a], 1.0f); ++ci; }
+    float s = __fmaf_rn(P.bdx[a], xdot[a], __fmul_rn(P.gam1, d1[a]));
+    // (the gather position's y: + q Omega x_h h, x_h the half-step x in this block's frame)
+    if (a == 1 && P.gy != 0.0f) s = __fmaf_rn(P.gy, hpos[0], s);
+    on[a] = __fadd_rn(on[a], s);
+    dn[a] = __fsub_rn(dn[a], s);
+    if (a != 1 && P.kind == PK_HALF) {
+      // the half-step x and z in this block's frame (before any carry or periodic wrap)
+      const double x = __dadd_rn(sz[a == 0 ? X1MIN : X3MIN],
+                                 __dmul_rn(__dadd_rn((double)(a == 0 ? i : k), (double)on[a]), G.dx[a]));
+      hpos[a == 0 ? 0 : 1] = __double2float_rn(x);
+    }
+    int ci = (int)floorf(on[a]);
+    on[a] = __fsub_rn(on[a], (float)ci);
+    if (on[a] >= 1.0f) { on[a] = __fsub_rn(on[a], 1.0f); ++ci; }
     c[a] = ci;
   }
-  i += c[0]; j += c[1]; k += c[2];
-  const int o1 = (i < 0) ? -1 : ((i >= G.nx1) ? 1 : 0);
-  const int o2 = (j < 0) ? -1 : ((j >= G.nx2) ? 1 : 0);
-  const int o3 = (k < 0) ? -1 : ((k >= G.nx3) ? 1 : 0);
-  if (o1 | o2 | o3) {
+  const int ni = i + c[0], nj = j + c[1], nk = k + c[2];
+  const int o1 = (ni < 0) ? -1 : ((ni >= G.nx1) ? 1 : 0);
+  const int o2 = (nj < 0) ? -1 : ((nj >= G.nx2) ? 1 : 0);
+  int o3 = (nk < 0) ? -1 : ((nk >= G.nx3) ? 1 : 0);
+  const bool x3face = o3 != 0 && G.x3bc != DUSTB_X3_PERIODIC &&
+                      G.nghbr[(long long)m * 27 + dir_slot(0, 0, o3)] < 0;
+  bool sbface = false;
+  if (o1 != 0 && G.sb_on) {
+    // this block's x1 face in the crossing direction lies on the mesh's (bvals_part.cpp:260-261)
+    const double lx = sz[X1MAX] - sz[X1MIN];
+    sbface = (o1 < 0) ? (sz[X1MIN] < G.mx1min + 0.5 * lx) : (sz[X1MAX] > G.mx1max - 0.5 * lx);
+  }
+  if (P.kind == PK_HALF && (x3face || sbface)) {
+    flags = AF_EDGE;                               // position and cell left as they were
+    return G.ncell;
+  }
+  i = ni; j = nj; k = nk;
+  for (int a = 0; a < 3; ++a) { o[a] = on[a]; d1[a] = dn[a]; }
+  if ((o1 | o2 | o3) == 0) return encode(G, m, k, j, i);
+  if (x3face) {
+    if (G.x3bc == DUSTB_X3_REFLECT) {
+      // z <- 2 z_face - z: the offset mirrors, the register displacement changes sign (the
+      // caller turns the z velocities); a particle exactly on the upper face stays just
+      // below it, as the reference's snap
+      float om_ = __fsub_rn(1.0f, o[2]);
+      k = (o3 < 0) ? -k - 1 : 2 * G.nx3 - k - 1;
+      if (om_ >= 1.0f) {
+        if (o3 < 0) { om_ = 0.0f; ++k; } else { om_ = 0.99999994f; }
+      }
+      o[2] = om_;
+      d1[2] = -d1[2];
+      flags |= AF_REFLECT;
+    } else {
+      // outflow: removed (the caller zeroes mass and velocities), placed at the centre of the
+      // block's edge cell with x1 = x
+      k = (o3 < 0) ? 0 : G.nx3 - 1;
+      o[2] = 0.5f;
+      d1[0] = d1[1] = d1[2] = 0.0f;
+      flags |= AF_REMOVED;
+    }
+    if (k < 0 || k >= G.nx3) { report(P.err, DUSTB_ERR_ROUTE); k = min(max(k, 0), G.nx3 - 1); }
+    o3 = 0;
+    if ((o1 | o2) == 0) return encode(G, m, k, j, i);
+  }
+  if (sbface) {
+    // the global y cell coordinate, shifted by -/+ the folded offset and wrapped; the face
+    // block on the other side holding the new (y, z)
+    const int N2 = G.sb_nb2 * G.nx2, N3 = G.sb_nb3 * G.nx3;
+    const int b2 = (int)floor(__dadd_rn(__ddiv_rn(__dsub_rn(sz[X2MIN], G.mx2min),
+                                                  __ddiv_rn(G.mly, (double)G.sb_nb2)), 0.5));
+    const int b3 = (int)floor(__dadd_rn(__ddiv_rn(__dsub_rn(sz[X3MIN], G.mx3min),
+                                                  __ddiv_rn(G.mlz, (double)G.sb_nb3)), 0.5));
+    double Y = __dadd_rn((double)(b2 * G.nx2 + j), (double)o[1]);
+    Y = (o1 < 0) ? __dsub_rn(Y, G.shR) : __dadd_rn(Y, G.shR);
+    if (Y < 0.0) Y = __dadd_rn(Y, (double)N2);
+    if (Y >= (double)N2) Y = __dsub_rn(Y, (double)N2);
+    int Yc = (int)floor(Y);
+    float oy = __double2float_rn(__dsub_rn(Y, (double)Yc));
+    if (oy >= 1.0f) { oy = 0.0f; ++Yc; }
+    Yc = (Yc % N2 + N2) % N2;
+    const int Zc = ((b3 * G.nx3 + k) % N3 + N3) % N3;   // (x3 periodic here, or k inside)
+    const int c2 = Yc / G.nx2, c3 = Zc / G.nx3;
+    const int g = G.sb_gid[((long long)(o1 < 0 ? 1 : 0) * G.sb_nb3 + c3) * G.sb_nb2 + c2] - G.gids;
+    if (g < 0 || g >= G.nmb) {
+      report(P.err, DUSTB_ERR_NGHBR);
+    } else {
+      m = g; i -= o1 * G.nx1; j = Yc - c2 * G.nx2; k = Zc - c3 * G.nx3; o[1] = oy;
+    }
+  } else {
     const int g = G.nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)] - G.gids;
     if (g < 0 || g >= G.nmb) {
       report(P.err, DUSTB_ERR_NGHBR);
     } else {
       m = g; i -= o1 * G.nx1; j -= o2 * G.nx2; k -= o3 * G.nx3;
     }
-    if (i < 0 || i >= G.nx1 || j < 0 || j >= G.nx2 || k < 0 || k >= G.nx3) {
-      report(P.err, DUSTB_ERR_ROUTE);
-      i = min(max(i, 0), G.nx1 - 1); j = min(max(j, 0), G.nx2 - 1); k = min(max(k, 0), G.nx3 - 1);
-    }
+  }
+  if (i < 0 || i >= G.nx1 || j < 0 || j >= G.nx2 || k < 0 || k >= G.nx3) {
+    report(P.err, DUSTB_ERR_ROUTE);
+    i = min(max(i, 0), G.nx1 - 1); j = min(max(j, 0), G.nx2 - 1); k = min(max(k, 0), G.nx3 - 1);
   }
   return encode(G, m, k, j, i);
 }
@@ -433,13 +559,15 @@ __global__ void __launch_bounds__(kT) k_count(PBuf S, int *key_out, int *count, 
   float o[3] = {S.f[F_OX][p], S.f[F_OY][p], S.f[F_OZ][p]};
   float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
   float d1[3] = {0.0f, 0.0f, 0.0f};
-  if (P.stage2) { d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p]; }
+  if (P.stage2 || P.kind == PK_FULL) { d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p]; }
   if (P.res && (P.stage2 || P.head->pending) && S.f[F_M][p] > 0.0f) {
     double d[3];
     consistent_dv(G, P, S.f[F_CC][p], m, k, j, i, d);
     for (int a = 0; a < 3; ++a) v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
   }
-  const int key = advance(G, P, m, k, j, i, o, d1, v);
+  int flags;
+  float hpos[2];
+  const int key = advance(G, P, m, k, j, i, o, d1, v, flags, hpos);
   key_out[p] = key;
   warp_count(count, key, act);
   if (P.set_pending && p == 0) { P.head->a_dt = P.a_dt; P.head->pending = 1; }
@@ -458,71 +586,120 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   decode(G, S.cell[p], m, k, j, i);
   float o[3] = {S.f[F_OX][p], S.f[F_OY][p], S.f[F_OZ][p]};
   float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
-  const float ts = S.f[F_TS][p], mass = S.f[F_M][p];
-  // (the rates: stage 1's velocity does not use them and every stage's kick rewrites them)
-  const bool kick = P.res && (P.stage2 || P.head->pending);
-  float cc = (P.stage2 || kick) ? S.f[F_CC][p] : 0.0f;
-  float v1[3], d1[3], r[3] = {0.0f, 0.0f, 0.0f};
-  if (P.stage2) { r[0] = S.f[F_RX][p]; r[1] = S.f[F_RY][p]; r[2] = S.f[F_RZ][p]; }
-  if (kick && mass > 0.0f) {
-    double d[3];
-    consistent_dv(G, P, cc, m, k, j, i, d);
-    for (int a = 0; a < 3; ++a) {
-      v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
-      r[a] += (float)(d[a] / P.a_dt);
-    }
-  }
-  if (P.stage2) {
+  const float ts = S.f[F_TS][p];
+  float mass = S.f[F_M][p];
+  float v1[3], d1[3], r[3] = {0.0f, 0.0f, 0.0f}, cc;
+  if (P.kind == PK_FULL) {
+    // pc2: the advance left the new velocity, the rate and the displacement to the new
+    // position; the register velocity is v0
     v1[0] = S.f[F_WX][p]; v1[1] = S.f[F_WY][p]; v1[2] = S.f[F_WZ][p];
     d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p];
+    r[0] = S.f[F_RX][p]; r[1] = S.f[F_RY][p]; r[2] = S.f[F_RZ][p];
+    cc = S.f[F_CC][p];
   } else {
-    // FirstTwoImpRK: (x1, v1) <- (x, v); the drag factor of the cycle, formed in FP64
-    v1[0] = v[0]; v1[1] = v[1]; v1[2] = v[2];
-    d1[0] = d1[1] = d1[2] = 0.0f;
-    cc = (float)(P.a_dt / ((double)ts + P.a_dt));
-  }
-  // ExplicitPush imex (src/dust/dust_push.cpp:262-288): forces from the pre-stage velocity
-  float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-  if (P.sbox) {
-    if (G.three_d) {
-      fx = 2.0f * P.om * v[1];
-      fy = -(2.0f - P.q) * P.om * v[0];
-      if (P.strat) {
-        const double *sz = G.mb + (long long)m * 9;
-        fz = -(P.om * P.om) * (float)(sz[X3MIN] + ((double)k + o[2]) * G.dx[2]);
+    // (imex stage 1 and the pc2 half step: the rates are not read; every kick rewrites them)
+    const bool kick = P.res && (P.stage2 || P.head->pending);
+    cc = (P.stage2 || kick) ? S.f[F_CC][p] : 0.0f;
+    if (P.stage2) { r[0] = S.f[F_RX][p]; r[1] = S.f[F_RY][p]; r[2] = S.f[F_RZ][p]; }
+    if (kick && mass > 0.0f) {
+      double d[3];
+      consistent_dv(G, P, cc, m, k, j, i, d);
+      for (int a = 0; a < 3; ++a) {
+        v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
+        r[a] += (float)(d[a] / P.a_dt);
       }
+    }
+    if (P.stage2) {
+      v1[0] = S.f[F_WX][p]; v1[1] = S.f[F_WY][p]; v1[2] = S.f[F_WZ][p];
+      d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p];
     } else {
-      fx = 2.0f * P.om * v[2];
-      fz = -(2.0f - P.q) * P.om * v[0];
+      // FirstTwoImpRK: (x1, v1) <- (x, v); the drag factor of the cycle, formed in FP64
+      // (imex: a/(t_s + a); pc2: h/(t_s + h))
+      v1[0] = v[0]; v1[1] = v[1]; v1[2] = v[2];
+      d1[0] = d1[1] = d1[2] = 0.0f;
+      cc = (float)(P.a_dt / ((double)ts + P.a_dt));
     }
   }
-  const float atw = P.stage2 ? P.atw_dt : 0.0f;
-  const float nv[3] = {P.gam0 * v[0] + P.gam1 * v1[0] + P.bdt * fx + atw * r[0],
-                       P.gam0 * v[1] + P.gam1 * v1[1] + P.bdt * fy + atw * r[1],
-                       P.gam0 * v[2] + P.gam1 * v1[2] + P.bdt * fz + atw * r[2]};
-  const int key2 = advance(G, P, m, k, j, i, o, d1, v);
+  float nv[3] = {v[0], v[1], v[2]};
+  if (P.kind == PK_IMEX) {
+    // ExplicitPush imex (src/dust/dust_push.cpp:262-288): forces from the pre-stage velocity
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    if (P.sbox) {
+      if (G.three_d) {
+        fx = 2.0f * P.om * v[1];
+        fy = -(2.0f - P.q) * P.om * v[0];
+        if (P.strat) {
+          const double *sz = G.mb + (long long)m * 9;
+          fz = -(P.om * P.om) * (float)(sz[X3MIN] + ((double)k + o[2]) * G.dx[2]);
+        }
+      } else {
+        fx = 2.0f * P.om * v[2];
+        fz = -(2.0f - P.q) * P.om * v[0];
+      }
+    }
+    const float atw = P.stage2 ? P.atw_dt : 0.0f;
+    nv[0] = P.gam0 * v[0] + P.gam1 * v1[0] + P.bdt * fx + atw * r[0];
+    nv[1] = P.gam0 * v[1] + P.gam1 * v1[1] + P.bdt * fy + atw * r[1];
+    nv[2] = P.gam0 * v[2] + P.gam1 * v1[2] + P.bdt * fz + atw * r[2];
+  }
+  int flags;
+  float hpos[2];
+  const int key2 = advance(G, P, m, k, j, i, o, d1, v, flags, hpos);
   if (key2 != key) report(P.err, DUSTB_ERR_WINDOW);   // count and move disagree: never expected
-  D.cell[q] = key; D.pid[q] = S.pid[p];
+  if (P.kind == PK_HALF && P.sbox && G.three_d && !(flags & AF_EDGE)) {
+    // the shear drift -q Omega x_h dt of the new y goes into the displacement now, and z_h
+    // (for the vertical gravity) into the rate slot, while x_h and z_h are known in the
+    // frame of the particle's own block (the gather position may be a periodic image)
+    d1[1] = __fsub_rn(d1[1], __fmul_rn(P.sdy, hpos[0]));
+    r[2] = hpos[1];
+  }
+  if (flags & AF_REFLECT) { nv[2] = -nv[2]; v1[2] = -v1[2]; }
+  if (flags & AF_REMOVED) {
+    if (P.x3rem) { atomicAdd(&P.x3rem[0], (double)mass); atomicAdd(&P.x3rem[1], 1.0); }
+    mass = 0.0f;
+    for (int a = 0; a < 3; ++a) { nv[a] = 0.0f; v1[a] = 0.0f; }
+  }
+  // (an edge particle keeps its cell; its slot is in the edge bin)
+  D.cell[q] = (flags & AF_EDGE) ? encode(G, m, k, j, i) : key;
+  D.pid[q] = S.pid[p];
   D.f[F_OX][q] = o[0]; D.f[F_OY][q] = o[1]; D.f[F_OZ][q] = o[2];
   D.f[F_VX][q] = nv[0]; D.f[F_VY][q] = nv[1]; D.f[F_VZ][q] = nv[2];
   D.f[F_AX][q] = d1[0]; D.f[F_AY][q] = d1[1]; D.f[F_AZ][q] = d1[2];
   D.f[F_WX][q] = v1[0]; D.f[F_WY][q] = v1[1]; D.f[F_WZ][q] = v1[2];
-  // (no rates: the kick tile of this stage writes every particle's rate)
+  // (imex, pc2 half step: no rates, the stage's kick or advance writes every particle's;
+  // the half step of a 3-D shearing box keeps z_h in the z rate until the advance)
+  if (P.kind == PK_FULL) { D.f[F_RX][q] = r[0]; D.f[F_RY][q] = r[1]; D.f[F_RZ][q] = r[2]; }
+  else if (P.kind == PK_HALF && P.sbox && G.three_d) D.f[F_RZ][q] = r[2];
   D.f[F_TS][q] = ts; D.f[F_M][q] = mass; D.f[F_CC][q] = cc;
 }
 
 // ---- tile deposit kernels -------------------------------------------------------------------
-enum { MODE_QP = 0, MODE_OP = 1, MODE_KICK = 2 };
+// Q/P + centre mass (imex), the dc1 operator, the gather-kick-deposit (imex), the pc2
+// predictor, the pc2 advance
+enum { MODE_QP = 0, MODE_OP = 1, MODE_KICK = 2, MODE_PRED = 3, MODE_ADV = 4 };
+
+// the pc2 constants of a cycle in FP32 (dust_push.cpp:132-245)
+struct Pc2Args {
+  float dt, h;
+  float cxy, cyx;              // 3-D shearing box: 2 h Omega, h (2 - q) Omega (x-z: cxz, czx)
+  float qom;                   // q Omega (the shear drift of y)
+  float hom2;                  // h Omega^2 (stratified vertical gravity)
+  float haphi;                 // h const_accel_phi (2-D x-z shearing box)
+  float hdx[3];                // h / dx per axis (the half step in cells)
+  float gy;                    // q Omega h / dy (the gather position's y shift per unit x)
+  int sbox, strat;
+};
 
 struct TileArgs {
   int tj, chunk, tpp;          // rows per tile, buffer columns, tiles per (block, plane)
   double a_dt;
   const int *cstart;           // cell -> particle ranges of the sorted shadow
-  const double *gfield;        // gather field (3 vars), MODE_OP / MODE_KICK
-  double *dfield;              // deposit field
+  const double *gfield;        // gather field (3 vars): operator, kick, predictor, advance
+  double *dfield;              // deposit field (the predictor: qdep's variable 1)
   int dnvar;
   double *res;                 // MODE_QP: resid, the centre mass goes to var 3
-  int deposit;                 // 0: kick only (no back-reaction)
+  int deposit;                 // 0: kick or advance only (no back-reaction)
+  Pc2Args pc;
   unsigned *err;
 };
 
@@ -534,6 +711,9 @@ constexpr int kTileRows = 8;
 // variables, or -1 if no block owns it; a cell one beyond the block maps to the owning
 // neighbour's active cell (the ghost exchanges folded into the index)
 __device__ __forceinline__ long long cell_at(const Geo &G, int m, int nvar, int kk, int jj, int ii) {
+  // (ghost mode: the block's own cell, ghost cells included; the window reaches one cell
+  // beyond the block and every block has at least two ghost layers)
+  if (G.ghost) return G.at(m, nvar, 0, G.ks + kk, G.js + jj, G.is + ii);
   int mo;
   if (!G.owner(m, kk, jj, ii, mo)) return -1;
   return G.at(mo, nvar, 0, G.ks + kk, G.js + jj, G.is + ii);
@@ -542,9 +722,14 @@ __device__ __forceinline__ float2 dup(float x) { return make_float2(x, x); }
 
 // the 27-point sums of one source cell's particles: values 0, 1 as a packed pair; values 2, 3
 // as a pair (Q/P) or value 2 alone (operator, kick)
+// (four values: Q/P and the predictor)
+template <int MODE>
+struct FourValues { static constexpr bool value = (MODE == MODE_QP || MODE == MODE_PRED); };
+
 template <int MODE, int D3>
 struct CellSums {
   static constexpr int WK = D3 ? 3 : 1;
+  static constexpr bool V4 = FourValues<MODE>::value;
   float2 a01[WK][3][3], a23[WK][3][3];
   float a2[WK][3][3];
   __device__ __forceinline__ void zero() {
@@ -555,13 +740,13 @@ struct CellSums {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           a01[c][b][a] = make_float2(0.0f, 0.0f);
-          if (MODE == MODE_QP) a23[c][b][a] = make_float2(0.0f, 0.0f);
+          if (V4) a23[c][b][a] = make_float2(0.0f, 0.0f);
           else a2[c][b][a] = 0.0f;
         }
   }
   __device__ __forceinline__ float val(int c, int b, int a, int q) const {
     return q == 0 ? a01[c][b][a].x : q == 1 ? a01[c][b][a].y
-         : (MODE == MODE_QP ? (q == 2 ? a23[c][b][a].x : a23[c][b][a].y) : a2[c][b][a]);
+         : (V4 ? (q == 2 ? a23[c][b][a].x : a23[c][b][a].y) : a2[c][b][a]);
   }
   // sum_cba += wz_c wy_b (wx_a q): the x weights folded into the values first
   __device__ __forceinline__ void add(const float wx[3], const float wy[3], const float wz[3],
@@ -570,7 +755,7 @@ struct CellSums {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       s01[a] = __fmul2_rn(dup(wx[a]), q01);
-      if (MODE == MODE_QP) s23[a] = __fmul2_rn(dup(wx[a]), q23);
+      if (V4) s23[a] = __fmul2_rn(dup(wx[a]), q23);
       else s23[a].x = wx[a] * q23.x;
     }
 #pragma unroll
@@ -582,7 +767,7 @@ struct CellSums {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           a01[c][b][a] = __ffma2_rn(dup(wzy), s01[a], a01[c][b][a]);
-          if (MODE == MODE_QP) a23[c][b][a] = __ffma2_rn(dup(wzy), s23[a], a23[c][b][a]);
+          if (V4) a23[c][b][a] = __ffma2_rn(dup(wzy), s23[a], a23[c][b][a]);
           else a2[c][b][a] = fmaf(wzy, s23[a].x, a2[c][b][a]);
         }
       }
@@ -660,7 +845,7 @@ __device__ __forceinline__ void stage_sums(const CellSums<MODE, D3> &A, float4 *
       for (int a = 0; a < 3; ++a)
         s_acc[((c * 3 + b) * 3 + a) * nct + cl] =
             make_float4(A.val(c, b, a, 0), A.val(c, b, a, 1), A.val(c, b, a, 2),
-                        MODE == MODE_QP ? A.val(c, b, a, 3) : 0.0f);
+                        FourValues<MODE>::value ? A.val(c, b, a, 3) : 0.0f);
 }
 
 // adds the tile's deposit window to the FP64 field, one add per window cell and value: a
@@ -670,7 +855,7 @@ __device__ __forceinline__ void stage_sums(const CellSums<MODE, D3> &A, float4 *
 template <int MODE, int D3>
 __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, const TileArgs &T,
                                            int m, int k, int j0, int tj) {
-  constexpr int NC = (MODE == MODE_QP) ? 4 : 3;
+  constexpr int NC = FourValues<MODE>::value ? 4 : 3;
   constexpr int WK = D3 ? 3 : 1;
   const int nx1 = G.nx1, nct = tj * nx1;
   const int WI = nx1 + 2, WJ = tj + 2, nplane = WJ * WI;
@@ -700,14 +885,60 @@ __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, co
   }
 }
 
+// dust_pc2_advance (src/dust/dust_push.cpp:132-245) of one particle in FP32 from u* gathered
+// at its half-step gather position: the implicit midpoint velocity v_h (the 2x2 Coriolis solve
+// and the vertical gravity of the shearing box), v <- 2 v_h - v0, the displacement dt xdot_h
+// to the new position, and the drag impulse dt (u - v_h) / t_s handed to the gas.  With
+// c = h/(t_s + h) (formed in FP64), 1/(1 + h/t_s) = 1 - c and (h/t_s)/(1 + h/t_s) = c, so the
+// system (1 + l) v_h + K v_h = v0 + l u + G becomes v_h + (1 - c) K v_h = (1 - c)(v0 + G) + c u.
+// The impulse is formed from the velocity change the particle received, less the Coriolis
+// and gravity terms (the same quantity in exact arithmetic): dv = (v - v0) + 2 K v_h - 2 G.
+__device__ __forceinline__ void pc2_particle(const Pc2Args &C, int three_d, float xh, float zh,
+                                             const float v0[3], const float u[3], float c,
+                                             bool shear_drift, float vn[3], float disp[3],
+                                             float dv[3]) {
+  const float s = 1.0f - c;
+  float vh[3], kv[3] = {0.0f, 0.0f, 0.0f}, gv[3] = {0.0f, 0.0f, 0.0f};
+  float r[3] = {s * v0[0] + c * u[0], s * v0[1] + c * u[1], s * v0[2] + c * u[2]};
+  if (C.sbox && three_d) {
+    if (C.strat) { gv[2] = -C.hom2 * zh; r[2] += s * gv[2]; }
+    const float det = 1.0f + C.cxy * C.cyx * s * s;
+    vh[0] = (r[0] + C.cxy * s * r[1]) / det;
+    vh[1] = (r[1] - C.cyx * s * r[0]) / det;
+    vh[2] = r[2];
+    kv[0] = -C.cxy * vh[1]; kv[1] = C.cyx * vh[0];
+  } else if (C.sbox) {
+    // the 2-D (x, z) shearing box: the Coriolis pair is (x, z); const_accel_phi along z
+    gv[2] = C.haphi; r[2] += s * gv[2];
+    const float det = 1.0f + C.cxy * C.cyx * s * s;
+    vh[0] = (r[0] + C.cxy * s * r[2]) / det;
+    vh[2] = (r[2] - C.cyx * s * r[0]) / det;
+    vh[1] = r[1];
+    kv[0] = -C.cxy * vh[2]; kv[2] = C.cyx * vh[0];
+  } else {
+    vh[0] = r[0]; vh[1] = r[1]; vh[2] = r[2];
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    vn[a] = 2.0f * vh[a] - v0[a];
+    dv[a] = (vn[a] - v0[a]) + 2.0f * kv[a] - 2.0f * gv[a];
+  }
+  disp[0] = C.dt * vh[0];
+  disp[1] = C.dt * (vh[1] - ((shear_drift && C.sbox && three_d) ? C.qom * xh : 0.0f));
+  disp[2] = C.dt * vh[2];
+}
+
 // One CTA per tile of tj rows of one plane, one thread per source cell.  Q/P: the sums of a
-// cell's particles are kept in registers over all passes.  Operator and kick: per pass, a
-// gather phase (the 27 gather values in registers) writes each particle's deposit value (or
-// velocity change) into its column, then a deposit phase sums them and adds them to the
-// field; the gather values and the sums are never live together.
+// cell's particles are kept in registers over all passes.  Operator, kick, pc2 predictor and
+// advance: per pass, a gather phase (the 27 gather values in registers) writes each
+// particle's deposit values (the kick: its velocity change; the advance: the gathered u*,
+// which a coalesced per-particle step turns into the new state and the impulse) into its
+// column, then a deposit phase sums them and adds them to the field; the gather values and
+// the sums are never live together.
 template <int MODE, int D3, int SCHEME>
 __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, TileArgs T) {
-  constexpr int NF = (MODE == MODE_OP) ? 5 : 8;    // fields copied: ox oy oz cc m [vx vy vz]
+  // fields copied: ox oy oz cc m [vx vy vz] (the predictor: t_s in place of cc)
+  constexpr int NF = (MODE == MODE_OP) ? 5 : 8;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   const int nx1 = G.nx1, tj = T.tj;
@@ -732,7 +963,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
   auto issue_pass = [&](int cb, int ce) {
     const int a0 = cb & ~3, a1 = (ce + 3) & ~3;
     const unsigned bytes = (unsigned)(a1 - a0) * 4u;
-    const int fl[8] = {F_OX, F_OY, F_OZ, F_CC, F_M, F_VX, F_VY, F_VZ};
+    const int fl[8] = {F_OX, F_OY, F_OZ, (MODE == MODE_PRED) ? F_TS : F_CC, F_M, F_VX, F_VY, F_VZ};
     fence_proxy_async();
     mbar_arrive_tx(&bar, bytes * NF);
 #pragma unroll
@@ -782,7 +1013,8 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
                make_float2(mc * s_f[6 * CH + r], mc * s_f[7 * CH + r]));
       }
     } else {
-      // gather phase: the operator's m c u / V, or the kick's velocity change, into rows 5..7
+      // gather phase: the operator's m c u / V, the kick's velocity change, the predictor's
+      // impulse and rate, or the advance's u*, into rows 5..7 (and 3)
       for (int r = lo; r < hi; ++r) {
         float wx_[3], wy_[3], wz_[3];
         wts(SCHEME, s_f[r], wx_);
@@ -795,6 +1027,17 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
         if (MODE == MODE_OP) {
           const float mc = s_f[4 * CH + r] * c32 * inv_vol;
           s_f[5 * CH + r] = mc * uxy.x; s_f[6 * CH + r] = mc * uxy.y; s_f[7 * CH + r] = mc * uz;
+        } else if (MODE == MODE_PRED) {
+          // dust_pc2_predictor (src/dust/dust_pm.cpp:141-193): rate m/(t_s V), impulse
+          // -dt rate (u - v) from the old gas velocity m/rho of u1
+          const float rate = s_f[4 * CH + r] * inv_vol / c32;
+          const float vx = s_f[5 * CH + r], vy = s_f[6 * CH + r], vz = s_f[7 * CH + r];
+          const float g = -T.pc.dt * rate;
+          s_f[3 * CH + r] = rate;
+          s_f[5 * CH + r] = g * (uxy.x - vx); s_f[6 * CH + r] = g * (uxy.y - vy);
+          s_f[7 * CH + r] = g * (uz - vz);
+        } else if (MODE == MODE_ADV) {
+          s_f[5 * CH + r] = uxy.x; s_f[6 * CH + r] = uxy.y; s_f[7 * CH + r] = uz;
         } else {
           // GatherKickPMBR (src/dust/dust_pm.cpp:534-563): the applied velocity change
           const float vx = s_f[5 * CH + r], vy = s_f[6 * CH + r], vz = s_f[7 * CH + r];
@@ -827,6 +1070,30 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
           }
         }
       }
+      if (MODE == MODE_ADV) {
+        // the advanced particles of the pass, one per thread (coalesced): v, the
+        // displacement to the new position (cells), the rate dv; their impulses -m dv / V
+        // into rows 5..7
+        __syncthreads();
+        for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
+          const int s = sh + x, p = cb + x;
+          const float v0[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
+          const float u[3] = {s_f[5 * CH + s], s_f[6 * CH + s], s_f[7 * CH + s]};
+          // (3-D shearing box: the half step left z_h in the z rate and the shear drift in
+          // the displacement)
+          const float zh = (T.pc.sbox && D3) ? S.f[F_RZ][p] : 0.0f;
+          float vn[3], disp[3], dv[3];
+          pc2_particle(T.pc, D3, 0.0f, zh, v0, u, s_f[3 * CH + s], false, vn, disp, dv);
+          S.f[F_VX][p] = vn[0]; S.f[F_VY][p] = vn[1]; S.f[F_VZ][p] = vn[2];
+          S.f[F_AX][p] += disp[0] * (float)G.inv_dx[0];
+          S.f[F_AY][p] += disp[1] * (float)G.inv_dx[1];
+          if (D3) S.f[F_AZ][p] += disp[2] * (float)G.inv_dx[2];
+          S.f[F_RX][p] = dv[0]; S.f[F_RY][p] = dv[1]; S.f[F_RZ][p] = dv[2];
+          const float f = -s_f[4 * CH + s] * inv_vol;
+          s_f[5 * CH + s] = f * dv[0]; s_f[6 * CH + s] = f * dv[1]; s_f[7 * CH + s] = f * dv[2];
+        }
+        __syncthreads();
+      }
       if (T.deposit) {
         // deposit phase: the sums of the values of this pass, added to the field
         CellSums<MODE, D3> sums;
@@ -836,9 +1103,9 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
           wts(SCHEME, s_f[r], wx_);
           wts(SCHEME, s_f[CH + r], wy_);
           if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
-          const float f = (MODE == MODE_OP) ? 1.0f : -s_f[4 * CH + r] * inv_vol;
+          const float f = (MODE == MODE_KICK) ? -s_f[4 * CH + r] * inv_vol : 1.0f;
           sums.add(wx_, wy_, wz_, make_float2(f * s_f[5 * CH + r], f * s_f[6 * CH + r]),
-                   make_float2(f * s_f[7 * CH + r], 0.0f));
+                   make_float2(f * s_f[7 * CH + r], (MODE == MODE_PRED) ? s_f[3 * CH + r] : 0.0f));
         }
         // the rows are read by now: their space takes the staged sums
         __syncthreads();
@@ -867,6 +1134,89 @@ size_t tile_smem(int three_d, int tj, int nx1, int chunk) {
   const size_t rows = (size_t)kTileRows * chunk * 4;
   const size_t sums = (size_t)(three_d ? 27 : 9) * nct * 16;
   return (((size_t)(nct + 1) * 4 + 15) & ~(size_t)15) + (rows > sums ? rows : sums);
+}
+
+// m/rho of a gas field on every cell, ghosts included: the predictor's gather field
+__global__ void k_gas_velocity(const double *u, int nv, double *out, long long per,
+                               long long total) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const long long m = idx / per, c = idx - m * per;
+  const double inv = 1.0 / u[(m * nv) * per + c];
+  for (int v = 0; v < 3; ++v) out[(m * 3 + v) * per + c] = u[(m * nv + 1 + v) * per + c] * inv;
+}
+
+// The pc2 advance of the edge bin: particles whose gather position lies beyond a physical x3
+// face or a shear-periodic x1 face of their block.  There the gather and the deposit use the
+// block's own ghost cells (u* beyond the face as the FP64 form has it; the deposit's ghost
+// exchange folds, drops or remaps it), as dust_pc2_advance does for every particle.  One
+// thread per particle, the same FP32 arithmetic as the advance tiles, FP64 atomics.  The
+// shadow keeps such a particle at its old position, so its displacement is the whole step.
+template <int SCHEME>
+__global__ void __launch_bounds__(kT) k_pc2_edge(PBuf S, Geo G, TileArgs T) {
+  const int e0 = T.cstart[G.ncell], e1 = T.cstart[G.ncell + 1];
+  const float inv_vol = (float)(1.0 / G.vol);
+  const int nax = G.three_d ? 3 : 2;
+  for (int p = e0 + blockIdx.x * blockDim.x + threadIdx.x; p < e1; p += gridDim.x * blockDim.x) {
+    int m, k, j, i;
+    decode(G, S.cell[p], m, k, j, i);
+    const double *sz = G.mb + (long long)m * 9;
+    const float v0[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
+    const float o[3] = {S.f[F_OX][p], S.f[F_OY][p], S.f[F_OZ][p]};
+    // the gather position in block-local cells, as the half-step push forms it
+    float xsh = 0.0f;
+    if (T.pc.sbox && G.three_d)
+      xsh = T.pc.qom * (float)(sz[X1MIN] + ((double)i + (double)o[0]) * G.dx[0]);
+    const float xdot[3] = {v0[0], v0[1] - xsh, v0[2]};
+    const int idx[3] = {i, j, k}, nx[3] = {G.nx1, G.nx2, G.nx3};
+    float g[3], w[3][3];
+    int ig[3];
+    bool in = true;
+    for (int a = 0; a < 3; ++a) {
+      g[a] = (float)idx[a] + o[a];
+      if (a < nax) g[a] += T.pc.hdx[a] * xdot[a];
+      if (a == 1 && T.pc.gy != 0.0f) g[1] += T.pc.gy * (float)(sz[X1MIN] + (double)g[0] * G.dx[0]);
+      ig[a] = (a < nax) ? (int)floorf(g[a]) : idx[a];
+      wts(SCHEME, (a < nax) ? g[a] - (float)ig[a] : 0.5f, w[a]);
+      if (a < nax && (ig[a] < -1 || ig[a] > nx[a])) in = false;
+    }
+    if (!in) { report(T.err, DUSTB_ERR_HALO); continue; }
+    // the gather from the block's own cells, ghost cells included
+    const int clo = G.three_d ? 0 : 1, chi = G.three_d ? 2 : 1;
+    float u[3] = {0.0f, 0.0f, 0.0f};
+    for (int c = clo; c <= chi; ++c)
+      for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) {
+          const float wt = (G.three_d ? w[2][c] : 1.0f) * w[1][b] * w[0][a];
+          const long long at = G.at(m, 3, 0, G.three_d ? G.ks + ig[2] - 1 + c : G.ks,
+                                    G.js + ig[1] - 1 + b, G.is + ig[0] - 1 + a);
+          u[0] += wt * (float)T.gfield[at];
+          u[1] += wt * (float)T.gfield[at + G.vstride];
+          u[2] += wt * (float)T.gfield[at + 2 * G.vstride];
+        }
+    const float xh = (float)(sz[X1MIN] + (double)g[0] * G.dx[0]);
+    const float zh = G.three_d ? (float)(sz[X3MIN] + (double)g[2] * G.dx[2]) : 0.0f;
+    float vn[3], disp[3], dv[3];
+    pc2_particle(T.pc, G.three_d, xh, zh, v0, u, S.f[F_CC][p], true, vn, disp, dv);
+    S.f[F_VX][p] = vn[0]; S.f[F_VY][p] = vn[1]; S.f[F_VZ][p] = vn[2];
+    S.f[F_AX][p] += disp[0] * (float)G.inv_dx[0];
+    S.f[F_AY][p] += disp[1] * (float)G.inv_dx[1];
+    if (G.three_d) S.f[F_AZ][p] += disp[2] * (float)G.inv_dx[2];
+    S.f[F_RX][p] = dv[0]; S.f[F_RY][p] = dv[1]; S.f[F_RZ][p] = dv[2];
+    if (!T.deposit) continue;
+    const float f = -S.f[F_M][p] * inv_vol;
+    for (int c = clo; c <= chi; ++c)
+      for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) {
+          const float wt = f * (G.three_d ? w[2][c] : 1.0f) * w[1][b] * w[0][a];
+          if (wt == 0.0f) continue;
+          const long long at = G.at(m, 3, 0, G.three_d ? G.ks + ig[2] - 1 + c : G.ks,
+                                    G.js + ig[1] - 1 + b, G.is + ig[0] - 1 + a);
+          atomicAdd(&T.dfield[at], (double)(wt * dv[0]));
+          atomicAdd(&T.dfield[at + G.vstride], (double)(wt * dv[1]));
+          atomicAdd(&T.dfield[at + 2 * G.vstride], (double)(wt * dv[2]));
+        }
+  }
 }
 
 // ---- kernel timing ------------------------------------------------------------------------
@@ -949,11 +1299,11 @@ int launch_tile(const MState &S, const PBuf &cur, const Geo &G, const Cfg &cf, T
 int sort_into(const MState &S, const PBuf &src, const PBuf &dst, const dustb_mesh &ms, int n,
               cudaStream_t st) {
   const long long ncell = ncell_of(ms);
-  cudaMemsetAsync(S.cstart, 0, 4 * (size_t)(ncell + 1), st);
+  cudaMemsetAsync(S.cstart, 0, 4 * (size_t)nbins(ncell), st);
   if (n > 0) k_hist<<<nblk(n), kT, 0, st>>>(src.cell, n, S.cstart);
-  int rc = exclusive_scan(S.cstart, ncell + 1, S.bsum, st);
+  int rc = exclusive_scan(S.cstart, nbins(ncell), S.bsum, st);
   if (rc) return rc;
-  cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)(ncell + 1), cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)nbins(ncell), cudaMemcpyDeviceToDevice, st);
   if (n > 0) k_sortmove<<<nblk(n), kT, 0, st>>>(src, dst, n, S.cursor);
   return dustb_host::launch_status("mixed sort");
 }
@@ -962,8 +1312,59 @@ bool params_ok(const dustb_ctx *c, const dustb_mixed_params *mp) {
   if (!dustb_cells::ctx_valid(c) || !mp) return false;
   for (int a = 0; a < 3; ++a)
     if (!(mp->dx[a] > 0.0)) return false;
-  if (ncell_of(c->mesh) >= (1LL << 31)) return false;
+  if (ncell_of(c->mesh) >= (1LL << 31) - 2) return false;   // (cells and the edge bin)
   return true;
+}
+
+
+// the geometry's tables and outputs are there
+bool geo_ok(const dustb_mixed_params *mp, const Geo &G) {
+  if (G.sb_on && (!G.sb_gid || G.sb_nb2 <= 0 || G.sb_nb3 <= 0)) return false;
+  if (G.x3bc == DUSTB_X3_OUTFLOW && !mp->x3_removed) return false;
+  return true;
+}
+
+// ghost mode: the FP64 exchanges around the tiles (additive: x3 fold or drop and the shear
+// remap included; copy: the shear remap and the x3 boundary values of u*)
+int ghost_add_if(const dustb_ctx *c, const Geo &G, double *f, int nvar, cudaStream_t st) {
+  return G.ghost ? dustb_ghost_add(c, f, nvar, st) : DUSTB_OK;
+}
+int ghost_copy_if(const dustb_ctx *c, const Geo &G, double *f, cudaStream_t st) {
+  return G.ghost ? dustb_ghost_copy(c, f, 3, 1, st) : DUSTB_OK;
+}
+
+// the pc2 constants of a cycle (dust_push.cpp:132-245), rounded once to FP32
+Pc2Args make_pc2(const dustb_ctx *c, const Geo &G, double dt) {
+  Pc2Args a{};
+  const double h = 0.5 * dt, om = c->phys.omega0, q = c->phys.qshear;
+  a.dt = (float)dt; a.h = (float)h;
+  a.cxy = (float)(2.0 * h * om); a.cyx = (float)(h * (2.0 - q) * om);
+  a.qom = (float)(q * om); a.hom2 = (float)(h * om * om);
+  a.haphi = (float)(h * c->phys.const_accel_phi);
+  for (int x = 0; x < 3; ++x) a.hdx[x] = (float)(h * G.inv_dx[x]);
+  a.sbox = c->phys.shearing_box; a.strat = c->phys.stratified;
+  a.gy = (a.sbox && G.three_d) ? (float)(q * om * h * G.inv_dx[1]) : 0.0f;
+  return a;
+}
+
+// one push: count (the new cells and their histogram), the scan of the bins, the moves
+int push_sort(const MState &S, const PBuf &src, const PBuf &dst, const Geo &G, int n,
+              long long ncell, const PushArgs &P, cudaStream_t st) {
+  int rc;
+  {
+    Scope sc(DUSTB_K_PUSH, st);
+    cudaMemsetAsync(S.cstart, 0, 4 * (size_t)nbins(ncell), st);
+    if (n > 0) k_count<<<nblk(n), kT, 0, st>>>(src, S.key, S.cstart, G, n, P);
+    if ((rc = dustb_host::launch_status("mixed count"))) return rc;
+  }
+  {
+    Scope sc(DUSTB_K_FILL, st);
+    if ((rc = exclusive_scan(S.cstart, nbins(ncell), S.bsum, st))) return rc;
+    cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)nbins(ncell), cudaMemcpyDeviceToDevice, st);
+  }
+  Scope sc(DUSTB_K_PUSH, st);
+  if (n > 0) k_move<<<nblk(n), kT, 0, st>>>(src, dst, S.key, S.cursor, G, n, P);
+  return dustb_host::launch_status("mixed move");
 }
 
 }  // namespace
@@ -988,12 +1389,12 @@ int dustb_mixed_import(const dustb_ctx *c, const dustb_mixed_params *mp, void *w
   const int n = c->part.npart;
   const long long ncell = ncell_of(c->mesh);
   cudaMemsetAsync(S.head, 0, sizeof(MHead), st);   // the rows carry every kick so far
-  cudaMemsetAsync(S.cstart, 0, 4 * (size_t)(ncell + 1), st);
+  cudaMemsetAsync(S.cstart, 0, 4 * (size_t)nbins(ncell), st);
   if (n > 0)
     k_import<<<nblk(n), kT, 0, st>>>(c->part.pr, c->part.pi, c->part.stride, n, S.B, S.cstart, G, c->err);
-  int rc = exclusive_scan(S.cstart, ncell + 1, S.bsum, st);
+  int rc = exclusive_scan(S.cstart, nbins(ncell), S.bsum, st);
   if (rc) return rc;
-  cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)(ncell + 1), cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)nbins(ncell), cudaMemcpyDeviceToDevice, st);
   if (n > 0) k_sortmove<<<nblk(n), kT, 0, st>>>(S.B, S.A, n, S.cursor);
   return dustb_host::launch_status("mixed_import");
 }
@@ -1050,15 +1451,14 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
                            long long bytes, const dustb_imex_coeffs *co, void *stream) {
   if (!params_ok(c, mp) || !co || !(co->dt > 0.0)) return DUSTB_EINVAL;
   if (co->sh[0] != 0.0 || co->sh[1] != 0.0) return DUSTB_EUNSUP;   // shear shift: FP64 form
-  if (c->mesh.x3bc != DUSTB_X3_PERIODIC) return DUSTB_EUNSUP;       // physical x3: FP64 form
   if (!c->mesh.multi_d) return DUSTB_EUNSUP;                        // 1-D: FP64 form
-  if (c->mesh.shear_x1) return DUSTB_EUNSUP;                        // shearing box: FP64 form
+  const Geo G = make_geo(c, mp);
+  if (!geo_ok(mp, G)) return DUSTB_EINVAL;
   MState S;
   if (!carve(c->mesh, c->part.npart, ws, bytes, S, nullptr)) return DUSTB_ESCRATCH;
   Cfg cf;
   if (!pick_cfg(c->mesh, mp, cf)) return DUSTB_EUNSUP;
   cudaStream_t st = (cudaStream_t)stream;
-  Geo G = make_geo(c, mp);
   const int n = c->part.npart;
   const long long ncell = ncell_of(c->mesh);
   Ind d = make_ind(c->mesh);
@@ -1082,11 +1482,13 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       dustb_cells::gas_rk(c, gam0[stage - 1], gam1[stage - 1], st);
       if (stage == 2 && br) dustb_cells::history(c, atw22 * dt, st);
     }
-    PushArgs P;
+    PushArgs P{};
+    P.kind = PK_IMEX;
     P.gam0 = (float)gam0[stage - 1]; P.gam1 = (float)gam1[stage - 1];
     P.atw_dt = (stage == 2) ? (float)(atw22 * dt) : 0.0f;
     P.bdt = (float)(beta[stage - 1] * dt);
     for (int a = 0; a < 3; ++a) P.bdx[a] = (float)(beta[stage - 1] * dt * G.inv_dx[a]);
+    P.gy = 0.0f;
     P.a_dt = a_dt; P.stage2 = (stage == 2);
     P.sbox = c->phys.shearing_box; P.strat = c->phys.stratified;
     P.q = (float)c->phys.qshear; P.om = (float)c->phys.omega0;
@@ -1095,34 +1497,24 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     P.res = (stage == 1 || (br && cons)) ? c->f.resid : nullptr;
     P.head = S.head;
     P.set_pending = (stage == 2 && br && cons);
+    P.x3rem = mp->x3_removed;
     P.err = c->err;
-    {
-      Scope sc(DUSTB_K_PUSH, st);
-      cudaMemsetAsync(S.cstart, 0, 4 * (size_t)(ncell + 1), st);
-      if (n > 0) k_count<<<nblk(n), kT, 0, st>>>(src, S.key, S.cstart, G, n, P);
-      RUN(dustb_host::launch_status("mixed count"));
-    }
-    {
-      Scope sc(DUSTB_K_FILL, st);
-      RUN(exclusive_scan(S.cstart, ncell + 1, S.bsum, st));
-      cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)(ncell + 1), cudaMemcpyDeviceToDevice, st);
-    }
-    {
-      Scope sc(DUSTB_K_PUSH, st);
-      if (n > 0) k_move<<<nblk(n), kT, 0, st>>>(src, cur, S.key, S.cursor, G, n, P);
-      RUN(dustb_host::launch_status("mixed move"));
-      if (stage == 1) cudaMemsetAsync(&S.head->pending, 0, sizeof(int), st);   // applied
-    }
+    RUN(push_sort(S, src, cur, G, n, ncell, P, st));
+    if (stage == 1) cudaMemsetAsync(&S.head->pending, 0, sizeof(int), st);   // applied
     TileArgs T{};
     T.a_dt = a_dt; T.err = c->err; T.deposit = 1;
     if (br) {
-      Scope sc(DUSTB_K_DEPOSIT_QP, st);
-      cudaMemsetAsync(c->f.qdep, 0, fbytes * 5, st);
-      T.dfield = c->f.qdep; T.dnvar = 5; T.res = c->f.resid;
-      RUN(launch_tile<MODE_QP>(S, cur, G, cf, T, st));
+      {
+        Scope sc(DUSTB_K_DEPOSIT_QP, st);
+        cudaMemsetAsync(c->f.qdep, 0, fbytes * 5, st);
+        T.dfield = c->f.qdep; T.dnvar = 5; T.res = c->f.resid;
+        RUN(launch_tile<MODE_QP>(S, cur, G, cf, T, st));
+      }
+      Scope sc(DUSTB_K_CELLS, st);
+      RUN(ghost_add_if(c, G, c->f.qdep, 5, st));
     }
-    // the deposits go straight into the owners' active cells and the gathers read ghost
-    // cells from their owners, so no ghost exchange of qdep, work, dmom or u* is needed
+    // periodic meshes: the deposits go straight into the owners' active cells and the
+    // gathers read ghost cells from their owners, so no ghost exchange is needed
     {
       Scope sc(DUSTB_K_CELLS, st);
       RUN(dustb_solve_ustar(c, st));
@@ -1130,13 +1522,20 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     if (br && c->phys.drag_solver >= DUSTB_SOLVER_DC1) {
       const int nsw = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
       for (int w = 0; w < nsw; ++w) {
+        { Scope sc(DUSTB_K_CELLS, st);
+          RUN(ghost_copy_if(c, G, c->f.ustar, st)); }
         cudaMemsetAsync(c->f.work, 0, fbytes * 3, st);
         { Scope sc(DUSTB_K_OPERATOR, st);
           T.gfield = c->f.ustar; T.dfield = c->f.work; T.dnvar = 3;
           RUN(launch_tile<MODE_OP>(S, cur, G, cf, T, st)); }
         { Scope sc(DUSTB_K_CELLS, st);
+          RUN(ghost_add_if(c, G, c->f.work, 3, st));
           dustb_cells::dc_correct(c, st); }
       }
+    }
+    {
+      Scope sc(DUSTB_K_CELLS, st);
+      RUN(ghost_copy_if(c, G, c->f.ustar, st));
     }
     if (br) cudaMemsetAsync(c->f.dmom, 0, fbytes * 3, st);
     {
@@ -1145,9 +1544,10 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       RUN(launch_tile<MODE_KICK>(S, cur, G, cf, T, st));
     }
     if (br) {
-      { Scope sc(DUSTB_K_CELLS, st);
-        if (cons) dustb_cells::consistent_gas(c, a_dt, st);
-        else dustb_cells::pmbr(c, a_dt, st); }
+      Scope sc(DUSTB_K_CELLS, st);
+      RUN(ghost_add_if(c, G, c->f.dmom, 3, st));
+      if (cons) dustb_cells::consistent_gas(c, a_dt, st);
+      else dustb_cells::pmbr(c, a_dt, st);
       // stage 2's consistent dust kick is left pending (recorded by stage 2's count): the
       // next cycle's stage-1 push, or an export, applies it
     }
@@ -1155,6 +1555,103 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
   {
     // the gas tail's ghost exchange of the conserved state, once per cycle (nothing in the
     // drag step reads u0's ghost cells between the stages)
+    Scope sc(DUSTB_K_CELLS, st);
+    RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, st));
+  }
+  return DUSTB_OK;
+}
+
+int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void *ws,
+                          long long bytes, double dt, double *chi_max, void *stream) {
+  if (!params_ok(c, mp) || !(dt > 0.0)) return DUSTB_EINVAL;
+  if (!c->mesh.multi_d) return DUSTB_EUNSUP;                        // 1-D: FP64 form
+  const Geo G = make_geo(c, mp);
+  if (!geo_ok(mp, G)) return DUSTB_EINVAL;
+  MState S;
+  if (!carve(c->mesh, c->part.npart, ws, bytes, S, nullptr)) return DUSTB_ESCRATCH;
+  Cfg cf;
+  if (!pick_cfg(c->mesh, mp, cf)) return DUSTB_EUNSUP;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = c->part.npart;
+  const long long ncell = ncell_of(c->mesh);
+  Ind d = make_ind(c->mesh);
+  const size_t fbytes = (size_t)d.cells() * d.nmb * sizeof(double);
+  const double h = 0.5 * dt;
+  const int br = c->phys.back_reaction;
+  int rc;
+  // FirstTwoImpRK's gas register and the gas stand-in's first stage
+  {
+    Scope sc(DUSTB_K_CELLS, st);
+    cudaMemcpyAsync(c->f.u1, c->f.u0, fbytes * c->f.nvar_gas, cudaMemcpyDeviceToDevice, st);
+    dustb_cells::gas_rk(c, 1.0, 0.0, st);
+  }
+  TileArgs T{};
+  T.a_dt = h; T.err = c->err; T.deposit = 1;
+  T.pc = make_pc2(c, G, dt);
+  if (br) {
+    // the predictor: the old gas velocity m/rho of u1 (work), the tiles' deposits into
+    // qdep 1..4, the exchange, the stiffness damping and the gas update
+    {
+      Scope sc(DUSTB_K_CELLS, st);
+      const long long per = d.cells(), tot = per * d.nmb;
+      k_gas_velocity<<<nblk(tot), kT, 0, st>>>(c->f.u1, c->f.nvar_gas, c->f.work, per, tot);
+      RUN(dustb_host::launch_status("mixed gas velocity"));
+    }
+    {
+      Scope sc(DUSTB_K_DEPOSIT_QP, st);
+      cudaMemsetAsync(c->f.qdep, 0, fbytes * 5, st);
+      T.gfield = c->f.work; T.dfield = c->f.qdep + d.cells(); T.dnvar = 5;
+      RUN(launch_tile<MODE_PRED>(S, S.A, G, cf, T, st));
+    }
+    Scope sc(DUSTB_K_CELLS, st);
+    RUN(ghost_add_if(c, G, c->f.qdep, 5, st));
+    RUN(dustb_pc2_apply_predictor(c, dt, chi_max, st));
+  }
+  {
+    // the gas tail: exchange, the midpoint u* (every cell), the stand-in's second stage
+    Scope sc(DUSTB_K_CELLS, st);
+    RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, st));
+    RUN(dustb_pc2_midpoint(c, st));
+    dustb_cells::gas_rk(c, 0.5, 0.5, st);
+  }
+  // the half step: A -> B sorted by the cell of each particle's gather position
+  PushArgs P{};
+  P.kind = PK_HALF;
+  P.gam0 = 1.0f; P.gam1 = 0.0f; P.atw_dt = 0.0f; P.bdt = 0.0f;
+  for (int a = 0; a < 3; ++a) P.bdx[a] = T.pc.hdx[a];
+  P.gy = T.pc.gy;
+  P.sdy = (float)(c->phys.qshear * c->phys.omega0 * dt * G.inv_dx[1]);
+  P.a_dt = h; P.stage2 = 0;
+  P.sbox = c->phys.shearing_box; P.strat = c->phys.stratified;
+  P.q = (float)c->phys.qshear; P.om = (float)c->phys.omega0;
+  P.res = nullptr; P.head = S.head; P.set_pending = 0;
+  P.x3rem = mp->x3_removed; P.err = c->err;
+  RUN(push_sort(S, S.A, S.B, G, n, ncell, P, st));
+  if (br) cudaMemsetAsync(c->f.dmom, 0, fbytes * 3, st);
+  {
+    Scope sc(DUSTB_K_KICK, st);
+    T.gfield = c->f.ustar; T.dfield = c->f.dmom; T.dnvar = 3; T.deposit = br;
+    RUN(launch_tile<MODE_ADV>(S, S.B, G, cf, T, st));
+    if (G.ghost && n > 0) {
+      T.cstart = S.cstart;
+      if (G.scheme == 2) k_pc2_edge<2><<<148 * 4, kT, 0, st>>>(S.B, G, T);
+      else if (G.scheme == 1) k_pc2_edge<1><<<148 * 4, kT, 0, st>>>(S.B, G, T);
+      else k_pc2_edge<0><<<148 * 4, kT, 0, st>>>(S.B, G, T);
+      RUN(dustb_host::launch_status("mixed pc2 edge"));
+    }
+  }
+  // the move to the new position: B -> A sorted by cell (routing as SetNewPrtclGID)
+  P.kind = PK_FULL;
+  P.gam0 = 0.0f; P.gam1 = 1.0f;
+  for (int a = 0; a < 3; ++a) P.bdx[a] = 0.0f;
+  P.gy = 0.0f;
+  RUN(push_sort(S, S.B, S.A, G, n, ncell, P, st));
+  if (br) {
+    Scope sc(DUSTB_K_CELLS, st);
+    RUN(ghost_add_if(c, G, c->f.dmom, 3, st));
+    RUN(dustb_pc2_commit(c, 0.5, st));
+  }
+  {
     Scope sc(DUSTB_K_CELLS, st);
     RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, st));
   }

@@ -19,7 +19,7 @@ KERNELS = ["push", "fill", "deposit_qp", "operator", "kick", "consistent", "cell
 
 class DustbMixedParams(C.Structure):
     _fields_ = [("dx", C.c_double * 3), ("rows_per_tile", C.c_int), ("chunk", C.c_int),
-                ("variant", C.c_int)]
+                ("variant", C.c_int), ("x3_removed", C.c_void_p)]
 
 
 _declared = False
@@ -37,6 +37,7 @@ def _declare(lib):
         "dustb_mixed_export": [P, MP, VP, LL, VP],
         "dustb_mixed_sort": [P, MP, VP, LL, VP],
         "dustb_mixed_imex_cycle": [P, MP, VP, LL, C.POINTER(capi.DustbImexCoeffs), VP],
+        "dustb_mixed_pc2_cycle": [P, MP, VP, LL, C.c_double, VP, VP],
     }.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -65,6 +66,7 @@ class MixedDust:
         self.mp.rows_per_tile = rows_per_tile
         self.mp.chunk = chunk
         self.mp.variant = variant
+        self.mp.x3_removed = self.dev.t["x3_removed"].data_ptr()
         nbytes = int(self.lib.dustb_mixed_workspace_bytes(C.byref(self.dev.ctx.mesh), self.dev.npart))
         self.ws = torch.empty(nbytes, dtype=torch.uint8, device=self.dev.device)
         if do_import:
@@ -96,6 +98,28 @@ class MixedDust:
         capi.check(self.lib.dustb_mixed_imex_cycle(self.dev.pctx, C.byref(self.mp), p, n,
                                                    C.byref(co), _stream_ptr(stream)),
                    "mixed_imex_cycle")
+
+    def pc2_cycle(self, dt, stream=None):
+        """One pc2 cycle; returns the device scalar chi_max (dt times the largest
+        predicted rate over rho)."""
+        out = self.dev.t["scalar"]
+        p, n = self._ws()
+        capi.check(self.lib.dustb_mixed_pc2_cycle(self.dev.pctx, C.byref(self.mp), p, n, dt,
+                                                  out.data_ptr(), _stream_ptr(stream)),
+                   "mixed_pc2_cycle")
+        return out[0]
+
+    def capture(self, cycle):
+        """Captures one call of `cycle` (a zero-argument function launching one cycle on
+        the current stream, e.g. lambda: mx.imex_cycle(dt)) into a CUDA graph; replay()
+        advances the state by one cycle.  Every kernel argument is fixed at capture (the
+        shadow, the workspace, the reference arrays and dt), so the graph stays valid while
+        none of them is reallocated.  Run one eager cycle of the same shape first (it sets
+        the kernels' shared-memory limits, which a capture does not)."""
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            cycle()
+        return g
 
     def set_tiles(self, rows_per_tile=0, chunk=0, variant=None):
         self.mp.rows_per_tile = rows_per_tile

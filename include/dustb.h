@@ -290,6 +290,9 @@ typedef struct dustb_mixed_params {
   int chunk;               /* 0: default (2048); shared-memory columns per CTA pass, a
                               multiple of 4 in 64..8192 (chunk - 8 particles per pass) */
   int variant;             /* deposit kernels: 0 (the only one) */
+  double *x3_removed;      /* device (mass, count) of the particles removed at outflow x3
+                              faces, accumulated; required when mesh.x3bc is
+                              DUSTB_X3_OUTFLOW, else may be NULL */
 } dustb_mixed_params;
 
 long long dustb_mixed_workspace_bytes(const dustb_mesh *mesh, int npart);
@@ -306,9 +309,32 @@ int dustb_mixed_export(const dustb_ctx *ctx, const dustb_mixed_params *mp, void 
                        long long ws_bytes, void *stream);
 
 /* One imex2+ cycle of the drag step on the shadow (the same task sequence as
- * dustb_imex_cycle; the FP64 mesh fields of ctx are used and updated). */
+ * dustb_imex_cycle; the FP64 mesh fields of ctx are used and updated).  On a periodic mesh
+ * the tiles gather from and deposit into the owning blocks' active cells directly; with
+ * physical x3 faces or shear-periodic x1 faces they use each block's own ghost cells and the
+ * FP64 ghost exchanges (dustb_ghost_add / dustb_ghost_copy: x3 fold or drop, shear remaps)
+ * run around them.  The push routes particles as dustb_route does (x3 reflect / outflow,
+ * shear-periodic crossings).  A 3-D shearing box needs c->sh = 0 here (DUSTB_EUNSUP
+ * otherwise; the FP64 form takes any shift). */
 int dustb_mixed_imex_cycle(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
                            long long ws_bytes, const dustb_imex_coeffs *c, void *stream);
+
+/* One pc2 cycle (integrator rk2) on the shadow, the task sequence of dustb_pc2_cycle: the
+ * predictor tiles gather m/rho of u1 and deposit the predicted impulse and rate into qdep;
+ * the FP64 cell passes apply it and form the midpoint u*; the particles are re-sorted by the
+ * cell of their half-step gather position, where the advance tiles gather u*, solve the
+ * implicit midpoint step (Coriolis, vertical gravity) and deposit the drag impulse into
+ * dmom; particles whose gather position lies beyond a physical x3 face or a shear-periodic
+ * x1 face are advanced by a per-particle kernel on their block's own ghost cells; then
+ * every particle moves to its new position (routing as dustb_route) and is re-sorted.
+ * chi_max as in dustb_pc2_apply_predictor (may be NULL).  The export writes X1 = X (the
+ * half-step position register is not kept; the next cycle's register copy sets it).
+ * On entry u0's ghost cells hold the copy exchange of the active cells (the state every
+ * cycle leaves): on a periodic mesh the tiles read the gas through the owning blocks.
+ * After imex cycles, export and import the shadow before the first pc2 cycle (the export
+ * applies the imex cycle's pending consistent kick). */
+int dustb_mixed_pc2_cycle(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
+                          long long ws_bytes, double dt, double *chi_max, void *stream);
 
 /* Re-sorts the shadow by cell (the SortParticles of the shadow; the reference rows keep
  * their order, export writes each particle back to its own row). */

@@ -159,3 +159,184 @@ def test_mixed_sort_keeps_rows():
     mx.export()
     torch.cuda.synchronize()
     np.testing.assert_array_equal(mx.dev.host("pr"), before)
+
+
+def test_graph_replay_matches_eager():
+    """One mixed imex2+ cycle captured as a CUDA graph and replayed: the same state as the
+    eager calls (up to the order of the FP32 partial sums' atomic adds)."""
+    from athenak_b200.mixed import MixedDust
+    c = CASES["3d_random"]
+    ms = uniform_mesh(*c["mesh"])
+    st = make_state(ms, **c["st"])
+    eager = MixedDust(st, c["phys"])
+    graph = MixedDust(st, c["phys"])
+    for _ in range(3):
+        eager.imex_cycle(c["dt"])
+    graph.imex_cycle(c["dt"])
+    g = graph.capture(lambda: graph.imex_cycle(c["dt"]))
+    for _ in range(2):
+        g.replay()
+    eager.export(); graph.export()
+    torch.cuda.synchronize()
+    assert eager.error_word() == 0 and graph.error_word() == 0
+    a, b = graph.dev.host("pr"), eager.dev.host("pr")
+    vs = np.abs(b[[1, 3, 5]]).max()
+    assert np.abs(a[[1, 3, 5]] - b[[1, 3, 5]]).max() < 1e-6 * vs
+    np.testing.assert_array_equal(graph.dev.host("pi"), eager.dev.host("pi"))
+
+
+# boundaries beyond the periodic box: physical x3 faces (reflect, outflow) and shear-periodic
+# x1 faces.  Large velocity noise so that particles cross the faces every cycle.
+EDGE_MESHES = {
+    "strat_reflect": dict(mesh=((16, 16, 32), (8, 8, 16), 2, (-0.05, -0.05, -0.1), (0.05, 0.05, 0.1)),
+                          kw=dict(x3bc=1), phys=dict(stratified=True)),
+    "strat_outflow": dict(mesh=((16, 16, 32), (8, 8, 16), 2, (-0.05, -0.05, -0.1), (0.05, 0.05, 0.1)),
+                          kw=dict(x3bc=2), phys=dict(stratified=True, x3_deposit_drop=True)),
+    "shear_x1": dict(mesh=((32, 32, 16), (16, 8, 8), 2, (-0.05, -0.1, -0.05), (0.05, 0.1, 0.05)),
+                     kw=dict(shear_x1=True), phys=dict()),
+    "shear_strat_outflow": dict(mesh=((16, 32, 32), (8, 8, 16), 2, (-0.05, -0.1, -0.1), (0.05, 0.1, 0.1)),
+                                kw=dict(x3bc=2, shear_x1=True), phys=dict(stratified=True)),
+}
+
+
+def edge_pair(name, ts_range=None):
+    from athenak_b200.drag import DeviceDust
+    from athenak_b200.mixed import MixedDust
+    e = EDGE_MESHES[name]
+    ms = uniform_mesh(*e["mesh"], **e["kw"])
+    st = make_state(ms, [0.01, 0.1], [0.5, 0.5], 2, seed=17, shearing_box=True, vel_noise=0.3,
+                    gas_noise=1e-2, ts_per_particle=ts_range)
+    phys = dict(scheme=2, drag_solver=2, shearing_box=True, **e["phys"])
+    return st, DeviceDust(st, phys), MixedDust(st, phys)
+
+
+def check_edges(st, ref, mx, x1_rows=True):
+    assert ref.error_word() == 0 and mx.error_word() == 0
+    a, b = mx.dev.host("pr"), ref.host("pr")
+    vscale = np.abs(b[[1, 3, 5]]).max()
+    for r in (1, 3, 5, 7, 9, 11):
+        assert np.abs(a[r] - b[r]).max() < VTOL * vscale, r
+    # the rates (imex dv/(a dt), pc2 dv): FP32 velocity differences, 1e-3 of their scale
+    rscale = np.abs(b[12:15]).max()
+    assert np.abs(a[12:15] - b[12:15]).max() < 1e-3 * rscale
+    # masses: kept, or zeroed by an outflow face in both forms
+    np.testing.assert_array_equal(a[16] == 0.0, b[16] == 0.0)
+    dx = st.mesh.mb_size[0, 6:9]
+    for r, ax in ((0, 0), (2, 1), (4, 2)) + (((6, 0), (8, 1), (10, 2)) if x1_rows else ()):
+        assert np.abs(a[r] - b[r]).max() < VTOL * dx[ax], r
+    np.testing.assert_array_equal(mx.dev.host("pi"), ref.host("pi"))
+    ua, ub = mx.dev.host("u0"), ref.host("u0")
+    ms = st.mesh
+    for v in range(1, 4):
+        sa, sb = ms.active(ua)[:, v], ms.active(ub)[:, v]
+        sc = np.abs(sb).max()
+        assert np.abs(sa - sb).max() < VTOL * sc, v
+    ra, rb = mx.dev.host("x3_removed"), ref.host("x3_removed")
+    assert ra[1] == rb[1] and abs(ra[0] - rb[0]) <= 1e-6 * abs(rb[0])
+
+
+@pytest.mark.parametrize("name", list(EDGE_MESHES))
+def test_mixed_imex_physical_and_shear_faces(name):
+    """The mixed imex2+ cycle on meshes with physical x3 faces or shear-periodic x1 faces (the
+    tiles on each block's own ghost cells with the FP64 exchanges around them; the push's
+    reflect / outflow / shear crossing) against the FP64 form, to the mixed tolerance."""
+    st, ref, mx = edge_pair(name)
+    t, dt = 1.7, 2e-3
+    for _ in range(3):
+        ref.set_time(t); mx.dev.set_time(t)
+        ref.imex_cycle(dt)
+        mx.imex_cycle(dt)
+        t += dt
+    mx.export()
+    torch.cuda.synchronize()
+    check_edges(st, ref, mx)
+
+
+PC2_CASES = {
+    "3d_random": dict(mesh=((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3), kw={},
+                      st=dict(taus=[0.01, 0.1, 1.0], eps=[0.5, 0.5, 0.5], ppc=2, seed=3,
+                              vd=[0.1, -0.2, 0.3], gas_noise=1e-2, vel_noise=0.05),
+                      phys=dict(scheme=2), dt=2e-3),
+    "3d_stiff_sbox": dict(mesh=((64, 32, 32), (64, 16, 16), 2, (-1.0,) * 3, (1.0,) * 3), kw={},
+                          st=dict(taus=[0.001, 0.01, 0.1, 1.0], eps=[0.5] * 4, ppc=2, seed=7,
+                                  shearing_box=True, vel_noise=1e-3, gas_noise=1e-3),
+                          phys=dict(scheme=2, shearing_box=True), dt=0.01),
+    "2d_xz_sbox_cic": dict(mesh=((32, 32, 1), (16, 16, 1), 2, (-0.5,) * 3, (0.5,) * 3), kw={},
+                           st=dict(taus=[0.1, 1.0], eps=[0.5, 0.5], ppc=2, seed=2,
+                                   shearing_box=True, vel_noise=0.01),
+                           phys=dict(scheme=1, shearing_box=True, const_accel_phi=0.05), dt=0.01),
+    "strat_reflect": dict(mesh=((16, 16, 32), (8, 8, 16), 2, (-0.05, -0.05, -0.1), (0.05, 0.05, 0.1)),
+                          kw=dict(x3bc=1),
+                          st=dict(taus=[0.01, 0.1], eps=[0.5, 0.5], ppc=2, seed=17,
+                                  shearing_box=True, vel_noise=0.3, gas_noise=1e-2),
+                          phys=dict(scheme=2, shearing_box=True, stratified=True), dt=2e-3),
+    # the stratified continuous-distribution workload in small: shear-periodic x1, outflow
+    # x3 faces with the deposit fold, per-particle t_s log-uniform over St 1e-3..1
+    "strat_shear_continuous": dict(
+        mesh=((16, 32, 32), (8, 8, 16), 2, (-0.05, -0.1, -0.1), (0.05, 0.1, 0.1)),
+        kw=dict(x3bc=2, shear_x1=True),
+        st=dict(taus=[0.1, 0.1], eps=[0.01, 0.01], ppc=2, seed=5, shearing_box=True,
+                vel_noise=0.3, gas_noise=1e-2, ts_per_particle=(1e-3, 1.0)),
+        phys=dict(scheme=2, shearing_box=True, stratified=True), dt=2e-3),
+}
+
+
+def consistent_ghosts(dev):
+    """The generator draws every cell's gas noise, ghosts included.  A step starts from ghost
+    cells that agree with the cells they stand for (the hydro's exchange and boundary
+    values): one copy exchange, then the planes beyond physical x3 faces copied from the
+    edge plane, x1/x2 ghost columns included (the mixed form reads ghost cells across
+    internal faces through their owners)."""
+    dev.ghost_copy("u0", 4, x3_bcs=0)
+    ms = dev.mesh
+    if not ms.three_d or not ms.x3bc:
+        return
+    u = dev.t["u0"]
+    ng, nx3 = ms.ng, ms.nx[2]
+    nb = np.asarray(ms.nghbr)
+    for m in range(ms.nmb):
+        if nb[m, 4] < 0:                     # no neighbour across the lower x3 face
+            u[m, :, :ng] = u[m, :, ng:ng + 1]
+        if nb[m, 22] < 0:                    # nor across the upper one
+            u[m, :, ng + nx3:] = u[m, :, ng + nx3 - 1:ng + nx3]
+    torch.cuda.synchronize()
+
+
+def pc2_pair(name, cycles=3):
+    from athenak_b200.drag import DeviceDust
+    from athenak_b200.mixed import MixedDust
+    c = PC2_CASES[name]
+    ms = uniform_mesh(*c["mesh"], **c["kw"])
+    st = make_state(ms, **c["st"])
+    ref, mx = DeviceDust(st, c["phys"]), MixedDust(st, c["phys"])
+    consistent_ghosts(ref)
+    consistent_ghosts(mx.dev)
+    p0 = sum(ref.momentum())
+    t = 1.7
+    for _ in range(cycles):
+        ref.set_time(t); mx.dev.set_time(t)
+        chi_r = float(ref.pc2_cycle(c["dt"]).item())
+        chi_m = float(mx.pc2_cycle(c["dt"]).item())
+        assert abs(chi_m - chi_r) <= 1e-5 * chi_r
+        t += c["dt"]
+    mx.export()
+    torch.cuda.synchronize()
+    return st, ref, mx, p0
+
+
+@pytest.mark.parametrize("name", list(PC2_CASES))
+def test_mixed_pc2_matches_fp64(name):
+    """The mixed pc2 cycle (predictor tiles, half-step sort, advance tiles + the edge kernel,
+    the move) against the FP64 pc2 cycle, to the mixed tolerance; X1 is not compared (the
+    mixed form does not keep the half-step register)."""
+    st, ref, mx, _ = pc2_pair(name)
+    check_edges(st, ref, mx, x1_rows=False)
+
+
+def test_mixed_pc2_conserves_momentum():
+    """Without rotation the pc2 impulse handed to the gas is the velocity change the
+    particle received, so gas + dust momentum holds to the FP32 rounding of the deposits."""
+    cycles = 4
+    st, ref, mx, p0 = pc2_pair("3d_random", cycles=cycles)
+    g, d = mx.dev.momentum()
+    assert np.abs(g + d - p0).max() < 1e-7 * cycles * absolute_momentum(st)
