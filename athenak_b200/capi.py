@@ -54,7 +54,10 @@ class DustbSeedDesc(C.Structure):
                 ("taus", C.c_double * 8), ("mass", C.c_double * 8), ("vx", C.c_double * 8),
                 ("vy", C.c_double * 8), ("vz", C.c_double * 8), ("vel_noise", C.c_double),
                 ("rho0", C.c_double), ("ug", C.c_double * 3), ("gas_noise", C.c_double),
-                ("nb1", C.c_int), ("nb2", C.c_int), ("nb3", C.c_int)]
+                ("nb1", C.c_int), ("nb2", C.c_int), ("nb3", C.c_int),
+                ("ts_lo", C.c_double), ("ts_hi", C.c_double), ("mass_slope", C.c_double),
+                ("hp", C.c_double), ("nsh", C.c_int), ("omega0", C.c_double),
+                ("qshear", C.c_double)]
 
 
 class DustbImexCoeffs(C.Structure):

@@ -509,10 +509,31 @@ __global__ void k_ghost_add(Ind d, const int *nghbr, int gids, double *a, int nv
       }
     }
   }
-  // shear-periodic x1 faces: the remapped ghost cells beyond them (their sum added as
-  // DepRemapPlan's GeneralApply adds it)
-  if (B.on) val += shear_add_sum(B, d, a, nvar, m, v, k, j, i);
   a[at] = val;
+}
+
+// shear-periodic x1 faces: the remapped ghost cells beyond them, their sum added as
+// DepRemapPlan's GeneralApply adds it, after the exchange above (a pass of its own over the
+// strips of active cells next to the faces: the exchange reads only ghost cells, this one
+// too, so the order of the additions is that of one pass)
+__global__ void k_shear_add(Ind d, SBox B, double *a, int nvar) {
+  const int ng = d.ng, ng1 = d.ng - 1;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int c = (int)(idx % (2 * ng)); idx /= 2 * ng;
+  const int j = (int)(idx % d.nx2) + d.js; idx /= d.nx2;
+  const int k = (int)(idx % d.nx3) + d.ks; idx /= d.nx3;
+  const int v = (int)(idx % nvar); idx /= nvar;
+  if (idx >= d.nmb) return;
+  const int m = (int)idx;
+  const int faces = B.faces(m);
+  if (!faces) return;
+  // strip column c: the inner strip's is + c, else the outer strip's (once if they overlap)
+  const int i = (c < ng) ? d.is + c : d.ie - ng1 + (c - ng);
+  if (c >= ng && i <= d.is + ng1) return;
+  const bool inner = (faces & 1) && i <= d.is + ng1, outer = (faces & 2) && i >= d.ie - ng1;
+  if (!inner && !outer) return;
+  const long long at = d.at(m, nvar, v, k, j, i);
+  a[at] += shear_add_sum(B, d, a, nvar, m, v, k, j, i);
 }
 
 // copy exchange: every ghost cell <- the neighbour's active cell at index - o*nx
@@ -1100,8 +1121,14 @@ int dustb_ghost_add(const dustb_ctx *c, double *field, int nvar, void *stream) {
   if (!field || nvar <= 0) return DUSTB_EINVAL;
   Ind d = make_ind(c->mesh);
   const int fold = d.three_d && c->mesh.x3bc != DUSTB_X3_PERIODIC && !c->phys.x3_deposit_drop;
+  const SBox B = sbview(c);
   k_ghost_add<<<blocks_for(n_active(d) * nvar), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar, fold,
-                                                                          sbview(c));
+                                                                          B);
+  if (B.on) {
+    if (!B.sb_gid || B.nb2 <= 0 || B.nb3 <= 0) return DUSTB_EINVAL;
+    k_shear_add<<<blocks_for((long long)d.nmb * nvar * d.nx3 * d.nx2 * 2 * d.ng), kThreads, 0, S(stream)>>>(
+        d, B, field, nvar);
+  }
   return launch_status("ghost_add");
 }
 

@@ -432,39 +432,22 @@ __device__ __forceinline__ void consistent_dv(const Geo &G, const PushArgs &P, f
 // shear offset (bvals_part.cpp:266-310), any other face hands it to the neighbour across it
 // (periodic images are neighbours).  The pc2 half step routes nothing: a gather position
 // beyond a physical x3 face or a shear face sends the particle, unmoved, to the edge bin.
-__device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, int &k, int &j,
-                                       int &i, float o[3], float d1[3], const float v[3],
-                                       int &flags, float hpos[2]) {
-  flags = 0;
-  hpos[0] = hpos[1] = 0.0f;
+
+// the carried state of a particle that leaves its block
+struct Carry {
+  int key, m, k, j, i, flags;
+  float o[3], d1[3];
+};
+
+// the face crossings, out of line (few particles take them; the common path stays small).
+// (m, k, j, i) the old cell, (ni, nj, nk) the new block-local cell, on / dn the new offsets
+// and displacement
+__device__ __forceinline__ Carry cross_face(const Geo &G, const PushArgs &P, int m, int k, int j,
+                                         int i, int ni, int nj, int nk, float on0, float on1,
+                                         float on2, float dn0, float dn1, float dn2) {
+  Carry C;
+  C.flags = 0;
   const double *sz = G.mb + (long long)m * 9;
-  float xsh = 0.0f;
-  if (P.sbox && G.three_d && P.kind != PK_FULL) {
-    const double x = __dadd_rn(sz[X1MIN], __dmul_rn(__dadd_rn((double)i, (double)o[0]), G.dx[0]));
-    xsh = __fmul_rn(__fmul_rn(P.q, P.om), __double2float_rn(x));
-  }
-  const float xdot[3] = {v[0], __fsub_rn(v[1], xsh), v[2]};
-  const int nax = G.three_d ? 3 : 2;
-  float on[3] = {o[0], o[1], o[2]}, dn[3] = {d1[0], d1[1], d1[2]};
-  int c[3] = {0, 0, 0};
-  for (int a = 0; a < nax; ++a) {
-    float s = __fmaf_rn(P.bdx[a], xdot[a], __fmul_rn(P.gam1, d1[a]));
-    // (the gather position's y: + q Omega x_h h, x_h the half-step x in this block's frame)
-    if (a == 1 && P.gy != 0.0f) s = __fmaf_rn(P.gy, hpos[0], s);
-    on[a] = __fadd_rn(on[a], s);
-    dn[a] = __fsub_rn(dn[a], s);
-    if (a != 1 && P.kind == PK_HALF) {
-      // the half-step x and z in this block's frame (before any carry or periodic wrap)
-      const double x = __dadd_rn(sz[a == 0 ? X1MIN : X3MIN],
-                                 __dmul_rn(__dadd_rn((double)(a == 0 ? i : k), (double)on[a]), G.dx[a]));
-      hpos[a == 0 ? 0 : 1] = __double2float_rn(x);
-    }
-    int ci = (int)floorf(on[a]);
-    on[a] = __fsub_rn(on[a], (float)ci);
-    if (on[a] >= 1.0f) { on[a] = __fsub_rn(on[a], 1.0f); ++ci; }
-    c[a] = ci;
-  }
-  const int ni = i + c[0], nj = j + c[1], nk = k + c[2];
   const int o1 = (ni < 0) ? -1 : ((ni >= G.nx1) ? 1 : 0);
   const int o2 = (nj < 0) ? -1 : ((nj >= G.nx2) ? 1 : 0);
   int o3 = (nk < 0) ? -1 : ((nk >= G.nx3) ? 1 : 0);
@@ -477,12 +460,14 @@ __device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, 
     sbface = (o1 < 0) ? (sz[X1MIN] < G.mx1min + 0.5 * lx) : (sz[X1MAX] > G.mx1max - 0.5 * lx);
   }
   if (P.kind == PK_HALF && (x3face || sbface)) {
-    flags = AF_EDGE;                               // position and cell left as they were
-    return G.ncell;
+    // position and cell left as they were
+    C.flags = AF_EDGE; C.key = G.ncell;
+    C.m = m; C.k = k; C.j = j; C.i = i;
+    C.o[0] = C.o[1] = C.o[2] = 0.0f; C.d1[0] = C.d1[1] = C.d1[2] = 0.0f;
+    return C;
   }
   i = ni; j = nj; k = nk;
-  for (int a = 0; a < 3; ++a) { o[a] = on[a]; d1[a] = dn[a]; }
-  if ((o1 | o2 | o3) == 0) return encode(G, m, k, j, i);
+  float o[3] = {on0, on1, on2}, d1[3] = {dn0, dn1, dn2};
   if (x3face) {
     if (G.x3bc == DUSTB_X3_REFLECT) {
       // z <- 2 z_face - z: the offset mirrors, the register displacement changes sign (the
@@ -495,20 +480,21 @@ __device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, 
       }
       o[2] = om_;
       d1[2] = -d1[2];
-      flags |= AF_REFLECT;
+      C.flags |= AF_REFLECT;
     } else {
       // outflow: removed (the caller zeroes mass and velocities), placed at the centre of the
       // block's edge cell with x1 = x
       k = (o3 < 0) ? 0 : G.nx3 - 1;
       o[2] = 0.5f;
       d1[0] = d1[1] = d1[2] = 0.0f;
-      flags |= AF_REMOVED;
+      C.flags |= AF_REMOVED;
     }
     if (k < 0 || k >= G.nx3) { report(P.err, DUSTB_ERR_ROUTE); k = min(max(k, 0), G.nx3 - 1); }
     o3 = 0;
-    if ((o1 | o2) == 0) return encode(G, m, k, j, i);
   }
-  if (sbface) {
+  if ((o1 | o2 | o3) == 0) {
+    // (nothing left to cross)
+  } else if (sbface) {
     // the global y cell coordinate, shifted by -/+ the folded offset and wrapped; the face
     // block on the other side holding the new (y, z)
     const int N2 = G.sb_nb2 * G.nx2, N3 = G.sb_nb3 * G.nx3;
@@ -544,10 +530,84 @@ __device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, 
     report(P.err, DUSTB_ERR_ROUTE);
     i = min(max(i, 0), G.nx1 - 1); j = min(max(j, 0), G.nx2 - 1); k = min(max(k, 0), G.nx3 - 1);
   }
-  return encode(G, m, k, j, i);
+  C.m = m; C.k = k; C.j = j; C.i = i;
+  for (int a = 0; a < 3; ++a) { C.o[a] = o[a]; C.d1[a] = d1[a]; }
+  C.key = encode(G, m, k, j, i);
+  return C;
+}
+
+template <int KIND, int SP>
+__device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, int &k, int &j,
+                                       int &i, float o[3], float d1[3], const float v[3],
+                                       int &flags, float hpos[2]) {
+  flags = 0;
+  hpos[0] = hpos[1] = 0.0f;
+  float xsh = 0.0f;
+  if (KIND != PK_FULL && P.sbox && G.three_d) {
+    const double *sz = G.mb + (long long)m * 9;
+    const double x = __dadd_rn(sz[X1MIN], __dmul_rn(__dadd_rn((double)i, (double)o[0]), G.dx[0]));
+    xsh = __fmul_rn(__fmul_rn(P.q, P.om), __double2float_rn(x));
+  }
+  const float xdot[3] = {v[0], __fsub_rn(v[1], xsh), v[2]};
+  const int nax = G.three_d ? 3 : 2;
+  float on[3] = {o[0], o[1], o[2]}, dn[3] = {d1[0], d1[1], d1[2]};
+  int c[3] = {0, 0, 0};
+  for (int a = 0; a < nax; ++a) {
+    float s = __fmaf_rn(P.bdx[a], xdot[a], __fmul_rn(P.gam1, d1[a]));
+    // (the gather position's y: + q Omega x_h h, x_h the half-step x in this block's frame)
+    if (KIND == PK_HALF && a == 1 && P.gy != 0.0f) s = __fmaf_rn(P.gy, hpos[0], s);
+    on[a] = __fadd_rn(on[a], s);
+    dn[a] = __fsub_rn(dn[a], s);
+    if (KIND == PK_HALF && a != 1) {
+      // the half-step x and z in this block's frame (before any carry or periodic wrap)
+      const double *sz = G.mb + (long long)m * 9;
+      const double x = __dadd_rn(sz[a == 0 ? X1MIN : X3MIN],
+                                 __dmul_rn(__dadd_rn((double)(a == 0 ? i : k), (double)on[a]), G.dx[a]));
+      hpos[a == 0 ? 0 : 1] = __double2float_rn(x);
+    }
+    int ci = (int)floorf(on[a]);
+    on[a] = __fsub_rn(on[a], (float)ci);
+    if (on[a] >= 1.0f) { on[a] = __fsub_rn(on[a], 1.0f); ++ci; }
+    c[a] = ci;
+  }
+  const int ni = i + c[0], nj = j + c[1], nk = k + c[2];
+  if ((unsigned)ni < (unsigned)G.nx1 && (unsigned)nj < (unsigned)G.nx2 &&
+      (unsigned)nk < (unsigned)G.nx3) {
+    i = ni; j = nj; k = nk;
+    for (int a = 0; a < 3; ++a) { o[a] = on[a]; d1[a] = dn[a]; }
+    return encode(G, m, k, j, i);
+  }
+  if (!SP) {
+    // a periodic mesh: the neighbour across the face (periodic images are neighbours)
+    const int o1 = (ni < 0) ? -1 : ((ni >= G.nx1) ? 1 : 0);
+    const int o2 = (nj < 0) ? -1 : ((nj >= G.nx2) ? 1 : 0);
+    const int o3 = (nk < 0) ? -1 : ((nk >= G.nx3) ? 1 : 0);
+    i = ni; j = nj; k = nk;
+    for (int a = 0; a < 3; ++a) { o[a] = on[a]; d1[a] = dn[a]; }
+    const int g = G.nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)] - G.gids;
+    if (g < 0 || g >= G.nmb) {
+      report(P.err, DUSTB_ERR_NGHBR);
+    } else {
+      m = g; i -= o1 * G.nx1; j -= o2 * G.nx2; k -= o3 * G.nx3;
+    }
+    if (i < 0 || i >= G.nx1 || j < 0 || j >= G.nx2 || k < 0 || k >= G.nx3) {
+      report(P.err, DUSTB_ERR_ROUTE);
+      i = min(max(i, 0), G.nx1 - 1); j = min(max(j, 0), G.nx2 - 1); k = min(max(k, 0), G.nx3 - 1);
+    }
+    return encode(G, m, k, j, i);
+  }
+  const Carry C = cross_face(G, P, m, k, j, i, ni, nj, nk, on[0], on[1], on[2], dn[0], dn[1], dn[2]);
+  flags = C.flags;
+  if (!(flags & AF_EDGE)) {
+    m = C.m; k = C.k; j = C.j; i = C.i;
+    for (int a = 0; a < 3; ++a) { o[a] = C.o[a]; d1[a] = C.d1[a]; }
+  }
+  return C.key;
 }
 
 // count: the new cell of every particle and the per-cell histogram
+// SP: the mesh has physical x3 or shear-periodic x1 faces
+template <int KIND, int SP>
 __global__ void __launch_bounds__(kT) k_count(PBuf S, int *key_out, int *count, Geo G, int n,
                                               PushArgs P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -559,21 +619,22 @@ __global__ void __launch_bounds__(kT) k_count(PBuf S, int *key_out, int *count, 
   float o[3] = {S.f[F_OX][p], S.f[F_OY][p], S.f[F_OZ][p]};
   float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
   float d1[3] = {0.0f, 0.0f, 0.0f};
-  if (P.stage2 || P.kind == PK_FULL) { d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p]; }
-  if (P.res && (P.stage2 || P.head->pending) && S.f[F_M][p] > 0.0f) {
+  if (P.stage2 || KIND == PK_FULL) { d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p]; }
+  if (KIND != PK_FULL && P.res && (P.stage2 || P.head->pending) && S.f[F_M][p] > 0.0f) {
     double d[3];
     consistent_dv(G, P, S.f[F_CC][p], m, k, j, i, d);
     for (int a = 0; a < 3; ++a) v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
   }
   int flags;
   float hpos[2];
-  const int key = advance(G, P, m, k, j, i, o, d1, v, flags, hpos);
+  const int key = advance<KIND, SP>(G, P, m, k, j, i, o, d1, v, flags, hpos);
   key_out[p] = key;
   warp_count(count, key, act);
   if (P.set_pending && p == 0) { P.head->a_dt = P.a_dt; P.head->pending = 1; }
 }
 
 // move: the whole push of every particle, written to its slot in dst
+template <int KIND, int SP>
 __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, int *cursor,
                                              Geo G, int n, PushArgs P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -589,7 +650,7 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   const float ts = S.f[F_TS][p];
   float mass = S.f[F_M][p];
   float v1[3], d1[3], r[3] = {0.0f, 0.0f, 0.0f}, cc;
-  if (P.kind == PK_FULL) {
+  if (KIND == PK_FULL) {
     // pc2: the advance left the new velocity, the rate and the displacement to the new
     // position; the register velocity is v0
     v1[0] = S.f[F_WX][p]; v1[1] = S.f[F_WY][p]; v1[2] = S.f[F_WZ][p];
@@ -621,7 +682,7 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
     }
   }
   float nv[3] = {v[0], v[1], v[2]};
-  if (P.kind == PK_IMEX) {
+  if (KIND == PK_IMEX) {
     // ExplicitPush imex (src/dust/dust_push.cpp:262-288): forces from the pre-stage velocity
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
     if (P.sbox) {
@@ -644,9 +705,9 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   }
   int flags;
   float hpos[2];
-  const int key2 = advance(G, P, m, k, j, i, o, d1, v, flags, hpos);
+  const int key2 = advance<KIND, SP>(G, P, m, k, j, i, o, d1, v, flags, hpos);
   if (key2 != key) report(P.err, DUSTB_ERR_WINDOW);   // count and move disagree: never expected
-  if (P.kind == PK_HALF && P.sbox && G.three_d && !(flags & AF_EDGE)) {
+  if (KIND == PK_HALF && P.sbox && G.three_d && !(flags & AF_EDGE)) {
     // the shear drift -q Omega x_h dt of the new y goes into the displacement now, and z_h
     // (for the vertical gravity) into the rate slot, while x_h and z_h are known in the
     // frame of the particle's own block (the gather position may be a periodic image)
@@ -668,8 +729,8 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   D.f[F_WX][q] = v1[0]; D.f[F_WY][q] = v1[1]; D.f[F_WZ][q] = v1[2];
   // (imex, pc2 half step: no rates, the stage's kick or advance writes every particle's;
   // the half step of a 3-D shearing box keeps z_h in the z rate until the advance)
-  if (P.kind == PK_FULL) { D.f[F_RX][q] = r[0]; D.f[F_RY][q] = r[1]; D.f[F_RZ][q] = r[2]; }
-  else if (P.kind == PK_HALF && P.sbox && G.three_d) D.f[F_RZ][q] = r[2];
+  if (KIND == PK_FULL) { D.f[F_RX][q] = r[0]; D.f[F_RY][q] = r[1]; D.f[F_RZ][q] = r[2]; }
+  else if (KIND == PK_HALF && P.sbox && G.three_d) D.f[F_RZ][q] = r[2];
   D.f[F_TS][q] = ts; D.f[F_M][q] = mass; D.f[F_CC][q] = cc;
 }
 
@@ -710,10 +771,11 @@ constexpr int kTileRows = 8;
 // the index of variable 0 of block-local cell (kk, jj, ii) of block m in a field of nvar
 // variables, or -1 if no block owns it; a cell one beyond the block maps to the owning
 // neighbour's active cell (the ghost exchanges folded into the index)
+template <int GH>
 __device__ __forceinline__ long long cell_at(const Geo &G, int m, int nvar, int kk, int jj, int ii) {
   // (ghost mode: the block's own cell, ghost cells included; the window reaches one cell
   // beyond the block and every block has at least two ghost layers)
-  if (G.ghost) return G.at(m, nvar, 0, G.ks + kk, G.js + jj, G.is + ii);
+  if (GH) return G.at(m, nvar, 0, G.ks + kk, G.js + jj, G.is + ii);
   int mo;
   if (!G.owner(m, kk, jj, ii, mo)) return -1;
   return G.at(mo, nvar, 0, G.ks + kk, G.js + jj, G.is + ii);
@@ -783,6 +845,7 @@ struct GatherWindow {
   static constexpr int WK = D3 ? 3 : 1;
   float2 xy[WK][3][3];
   float z[WK][3][3];
+  template <int GH>
   __device__ __forceinline__ void load(const Geo &G, const double *f, int m, int k, int jrow,
                                        int ci) {
 #pragma unroll
@@ -792,11 +855,11 @@ struct GatherWindow {
         // this cell's column of the (c, b) row; its x neighbours are the next words unless
         // the cell ends the block's row
         const int kk = D3 ? k - 1 + c : 0, jj = jrow - 1 + b;
-        const long long rb = cell_at(G, m, 3, kk, jj, ci);
+        const long long rb = cell_at<GH>(G, m, 3, kk, jj, ci);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           long long at = (rb >= 0) ? rb + (a - 1) : -1;
-          if ((a == 0 && ci == 0) || (a == 2 && ci == G.nx1 - 1)) at = cell_at(G, m, 3, kk, jj, ci - 1 + a);
+          if ((a == 0 && ci == 0) || (a == 2 && ci == G.nx1 - 1)) at = cell_at<GH>(G, m, 3, kk, jj, ci - 1 + a);
           xy[c][b][a] = make_float2(0.0f, 0.0f);
           z[c][b][a] = 0.0f;
           if (at >= 0) {
@@ -852,7 +915,7 @@ __device__ __forceinline__ void stage_sums(const CellSums<MODE, D3> &A, float4 *
 // window cell (z plane c, row wy, column wx) sums the staged contributions of the up to 9
 // source cells of its plane that reach it; window cells beyond the block go to the owning
 // neighbour's active cell (the additive ghost exchange folded into the add)
-template <int MODE, int D3>
+template <int MODE, int D3, int GH>
 __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, const TileArgs &T,
                                            int m, int k, int j0, int tj) {
   constexpr int NC = FourValues<MODE>::value ? 4 : 3;
@@ -862,7 +925,7 @@ __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, co
   for (int t = threadIdx.x; t < WK * nplane; t += blockDim.x) {
     const int c = t / nplane, rem = t - c * nplane;
     const int wy = rem / WI, wx = rem - wy * WI;
-    const long long at = cell_at(G, m, T.dnvar, D3 ? k - 1 + c : 0, j0 - 1 + wy, wx - 1);
+    const long long at = cell_at<GH>(G, m, T.dnvar, D3 ? k - 1 + c : 0, j0 - 1 + wy, wx - 1);
     if (at < 0) continue;
     float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
@@ -935,7 +998,7 @@ __device__ __forceinline__ void pc2_particle(const Pc2Args &C, int three_d, floa
 // which a coalesced per-particle step turns into the new state and the impulse) into its
 // column, then a deposit phase sums them and adds them to the field; the gather values and
 // the sums are never live together.
-template <int MODE, int D3, int SCHEME>
+template <int MODE, int D3, int SCHEME, int GH>
 __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, TileArgs T) {
   // fields copied: ox oy oz cc m [vx vy vz] (the predictor: t_s in place of cc)
   constexpr int NF = (MODE == MODE_OP) ? 5 : 8;
@@ -991,7 +1054,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
     const int a0 = cb & ~3, sh = cb - a0;
     if (threadIdx.x == 0 && cb != P0) issue_pass(cb, ce);
     GatherWindow<D3> win;
-    if (MODE != MODE_QP) win.load(G, T.gfield, m, k, jrow, ci_l);   // while the copies fly
+    if (MODE != MODE_QP) win.template load<GH>(G, T.gfield, m, k, jrow, ci_l);   // while the copies fly
     const bool ok = mbar_wait(&bar, parity, T.err);
     parity ^= 1u;
     if (__syncthreads_or(!ok)) {
@@ -1111,7 +1174,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
         __syncthreads();
         stage_sums<MODE, D3>(sums, s_acc, cl, nct);
         __syncthreads();
-        add_window<MODE, D3>(s_acc, G, T, m, k, j0, tj);
+        add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj);
       }
     }
     // the next pass's copies overwrite the rows
@@ -1123,7 +1186,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
     T.res[G.at(m, 4, 3, G.ks + k, G.js + jrow, G.is + ci_l)] = (double)qt;
     stage_sums<MODE, D3>(qp, s_acc, cl, nct);
     __syncthreads();
-    add_window<MODE, D3>(s_acc, G, T, m, k, j0, tj);
+    add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj);
   }
 }
 
@@ -1248,6 +1311,19 @@ struct Cfg {
   int tj, chunk, tpp;
 };
 
+// the default particles per pass: the largest multiple of 4 that lets as many CTAs share an
+// SM as their registers allow (about 168 per thread), so that a typical tile's particles
+// fit one pass (a second pass costs a second window flush)
+int default_chunk(int tj, int nx1) {
+  const int nct = tj * nx1;
+  int ctas = 65536 / (168 * nct);
+  ctas = ctas < 1 ? 1 : (ctas > 8 ? 8 : ctas);
+  const long long per = 233472 / ctas - 1024 - 64;     // less the reserve and the barrier
+  long long ch = (per - ((((long long)nct + 1) * 4 + 15) & ~15LL)) / (kTileRows * 4);
+  ch &= ~3LL;
+  return (int)(ch < 64 ? 64 : (ch > 8192 ? 8192 : ch));
+}
+
 bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   const int nx1 = ms.nx1, nx2 = ms.multi_d ? ms.nx2 : 1;
   if (mp->variant != 0 || nx1 > kMaxTileThreads) return false;
@@ -1259,7 +1335,7 @@ bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   }
   if (nx2 % tj != 0 || tj * nx1 > kMaxTileThreads) return false;
   cf.tj = tj;
-  cf.chunk = mp->chunk > 0 ? mp->chunk : 2048;
+  cf.chunk = mp->chunk > 0 ? mp->chunk : default_chunk(tj, nx1);
   if (cf.chunk < 64 || cf.chunk > 8192 || (cf.chunk & 3)) return false;
   cf.tpp = nx2 / tj;
   // every tile form must fit the 227 KiB of shared memory a CTA can have (less the barrier)
@@ -1267,16 +1343,16 @@ bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   return true;
 }
 
-template <int MODE, int D3, int SCHEME>
+template <int MODE, int D3, int SCHEME, int GH>
 int launch_tile_d(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &T, cudaStream_t st) {
   const long long tiles = (long long)G.nmb * G.nx3 * cf.tpp;
   const size_t sm = tile_smem(D3, cf.tj, G.nx1, cf.chunk);
   static size_t configured = 0;
   if (sm > 48 * 1024 && sm > configured) {
-    cudaFuncSetAttribute(k_tile<MODE, D3, SCHEME>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k_tile<MODE, D3, SCHEME, GH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     configured = sm;
   }
-  k_tile<MODE, D3, SCHEME><<<(unsigned)tiles, cf.tj * G.nx1, sm, st>>>(cur, G, T);
+  k_tile<MODE, D3, SCHEME, GH><<<(unsigned)tiles, cf.tj * G.nx1, sm, st>>>(cur, G, T);
   return dustb_host::launch_status("mixed tile");
 }
 
@@ -1286,13 +1362,19 @@ int launch_tile(const MState &S, const PBuf &cur, const Geo &G, const Cfg &cf, T
   T.tj = cf.tj; T.chunk = cf.chunk; T.tpp = cf.tpp; T.cstart = S.cstart;
   // one kernel per dimensionality and deposit scheme (no per-particle scheme selection)
   if (G.three_d) {
-    if (G.scheme == 2) return launch_tile_d<MODE, 1, 2>(G, cf, cur, T, st);
-    if (G.scheme == 1) return launch_tile_d<MODE, 1, 1>(G, cf, cur, T, st);
-    return launch_tile_d<MODE, 1, 0>(G, cf, cur, T, st);
+    // (ghost mode: physical x3 or shear-periodic x1 faces, 3-D only)
+    if (G.ghost) {
+      if (G.scheme == 2) return launch_tile_d<MODE, 1, 2, 1>(G, cf, cur, T, st);
+      if (G.scheme == 1) return launch_tile_d<MODE, 1, 1, 1>(G, cf, cur, T, st);
+      return launch_tile_d<MODE, 1, 0, 1>(G, cf, cur, T, st);
+    }
+    if (G.scheme == 2) return launch_tile_d<MODE, 1, 2, 0>(G, cf, cur, T, st);
+    if (G.scheme == 1) return launch_tile_d<MODE, 1, 1, 0>(G, cf, cur, T, st);
+    return launch_tile_d<MODE, 1, 0, 0>(G, cf, cur, T, st);
   }
-  if (G.scheme == 2) return launch_tile_d<MODE, 0, 2>(G, cf, cur, T, st);
-  if (G.scheme == 1) return launch_tile_d<MODE, 0, 1>(G, cf, cur, T, st);
-  return launch_tile_d<MODE, 0, 0>(G, cf, cur, T, st);
+  if (G.scheme == 2) return launch_tile_d<MODE, 0, 2, 0>(G, cf, cur, T, st);
+  if (G.scheme == 1) return launch_tile_d<MODE, 0, 1, 0>(G, cf, cur, T, st);
+  return launch_tile_d<MODE, 0, 0, 0>(G, cf, cur, T, st);
 }
 
 // sort copy src into dst by the cells it holds (histogram, scan, moves)
@@ -1354,7 +1436,19 @@ int push_sort(const MState &S, const PBuf &src, const PBuf &dst, const Geo &G, i
   {
     Scope sc(DUSTB_K_PUSH, st);
     cudaMemsetAsync(S.cstart, 0, 4 * (size_t)nbins(ncell), st);
-    if (n > 0) k_count<<<nblk(n), kT, 0, st>>>(src, S.key, S.cstart, G, n, P);
+    if (n > 0) {
+#define DUSTB_COUNT(K, SPF) k_count<K, SPF><<<nblk(n), kT, 0, st>>>(src, S.key, S.cstart, G, n, P)
+      if (G.ghost) {
+        if (P.kind == PK_HALF) DUSTB_COUNT(PK_HALF, 1);
+        else if (P.kind == PK_FULL) DUSTB_COUNT(PK_FULL, 1);
+        else DUSTB_COUNT(PK_IMEX, 1);
+      } else {
+        if (P.kind == PK_HALF) DUSTB_COUNT(PK_HALF, 0);
+        else if (P.kind == PK_FULL) DUSTB_COUNT(PK_FULL, 0);
+        else DUSTB_COUNT(PK_IMEX, 0);
+      }
+#undef DUSTB_COUNT
+    }
     if ((rc = dustb_host::launch_status("mixed count"))) return rc;
   }
   {
@@ -1363,7 +1457,19 @@ int push_sort(const MState &S, const PBuf &src, const PBuf &dst, const Geo &G, i
     cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)nbins(ncell), cudaMemcpyDeviceToDevice, st);
   }
   Scope sc(DUSTB_K_PUSH, st);
-  if (n > 0) k_move<<<nblk(n), kT, 0, st>>>(src, dst, S.key, S.cursor, G, n, P);
+  if (n > 0) {
+#define DUSTB_MOVE(K, SPF) k_move<K, SPF><<<nblk(n), kT, 0, st>>>(src, dst, S.key, S.cursor, G, n, P)
+    if (G.ghost) {
+      if (P.kind == PK_HALF) DUSTB_MOVE(PK_HALF, 1);
+      else if (P.kind == PK_FULL) DUSTB_MOVE(PK_FULL, 1);
+      else DUSTB_MOVE(PK_IMEX, 1);
+    } else {
+      if (P.kind == PK_HALF) DUSTB_MOVE(PK_HALF, 0);
+      else if (P.kind == PK_FULL) DUSTB_MOVE(PK_FULL, 0);
+      else DUSTB_MOVE(PK_IMEX, 0);
+    }
+#undef DUSTB_MOVE
+  }
   return dustb_host::launch_status("mixed move");
 }
 

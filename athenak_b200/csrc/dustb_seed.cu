@@ -18,6 +18,8 @@ __device__ __forceinline__ double hash01(uint64_t key) {
 
 constexpr uint64_t KX = 0x632BE59BD9B4E019ull, KY = 0x8CB92BAA3F3D8DD7ull;
 constexpr uint64_t KZ = 0x58F38DED6F7C55B5ull, KG = 0x1D8E4E27C47D124Full;
+// the stopping-time draw of the continuous distribution (dust_setup.cpp:736-745)
+constexpr uint64_t KT = 0xD6E8FEB86659FD93ull;
 
 struct SeedArgs {
   dustb_seed_desc d;
@@ -38,6 +40,15 @@ __global__ void k_seed_particles(double *pr, int *pi, long long stride, int npar
   double x = x1min + hash01(key + KX) * Lx;
   double y = x2min + hash01(key + KY) * Ly;
   double z = three_d ? x3min + hash01(key + KZ) * Lz : 0.5 * (x3min + x3max);
+  if (three_d && a.d.hp > 0.0) {
+    // Gaussian height of scale hp (Box-Muller on two draws), redrawn while outside the mesh
+    for (int r = 0; r < 64; ++r) {
+      const double u1 = fmax(hash01(key + KZ + 0x3333ull * (r + 1)), 1e-300);
+      const double u2 = hash01(key + KZ + 0x4444ull * (r + 1));
+      const double zz = a.d.hp * sqrt(-2.0 * log(u1)) * cos(2.0 * 3.141592653589793 * u2);
+      if (zz >= x3min && zz < x3max) { z = zz; break; }
+    }
+  }
   // block by position, then the block's own half-open box decides
   int b1 = (int)((x - x1min) / Lx * a.d.nb1), b2 = (int)((y - x2min) / Ly * a.d.nb2);
   int b3 = three_d ? (int)((z - x3min) / Lz * a.d.nb3) : 0;
@@ -53,7 +64,21 @@ __global__ void k_seed_particles(double *pr, int *pi, long long stride, int npar
     if (z < sz[2]) m -= a.d.nb1 * a.d.nb2; else if (z >= sz[5]) m += a.d.nb1 * a.d.nb2;
   }
   m = min(max(m, 0), nmb - 1);
+  double ts = a.d.taus[s], mass = a.d.mass[s];
+  if (a.d.ts_lo > 0.0) {
+    // bin s of nspecies equal bins in ln t_s; log-uniform inside it; mass ~ t_s^slope
+    const double lo = log(a.d.ts_lo), w = (log(a.d.ts_hi) - lo) / a.d.nspecies;
+    ts = exp(lo + ((double)s + hash01(key + KT)) * w);
+    mass = a.d.mass[s] * pow(ts / exp(lo + ((double)s + 0.5) * w), a.d.mass_slope);
+  }
   double v[3] = {a.d.vx[s], a.d.vy[s], a.d.vz[s]};
+  if (a.d.nsh) {
+    // the NSH drift of this particle's own stopping time (dust_setup.hpp:58-65)
+    const double T = a.d.omega0 * ts, b = 2.0 - a.d.qshear;
+    const double vx = (a.d.ug[0] + 2.0 * T * a.d.ug[1]) / (1.0 + 2.0 * b * T * T);
+    const double vp = a.d.ug[1] - b * T * vx;
+    v[0] = vx; v[1] = three_d ? vp : 0.0; v[2] = three_d ? 0.0 : vp;
+  }
   if (a.d.vel_noise > 0.0) {
     for (int c = 0; c < 3; ++c) {
       double u1 = fmax(hash01(key + 0x1111ull * (c + 1) + KG), 1e-300);
@@ -67,8 +92,8 @@ __global__ void k_seed_particles(double *pr, int *pi, long long stride, int npar
   R(DUSTB_IPX1) = x; R(DUSTB_IPY1) = y; R(DUSTB_IPZ1) = z;
   R(DUSTB_IPVX1) = v[0]; R(DUSTB_IPVY1) = v[1]; R(DUSTB_IPVZ1) = v[2];
   R(DUSTB_IPRX) = 0.0; R(DUSTB_IPRY) = 0.0; R(DUSTB_IPRZ) = 0.0;
-  R(DUSTB_IPTS) = a.d.taus[s];
-  R(DUSTB_IPM) = a.d.mass[s];
+  R(DUSTB_IPTS) = ts;
+  R(DUSTB_IPM) = mass;
   pi[(long long)DUSTB_PGID * stride + p] = m;
   pi[(long long)DUSTB_PTAG * stride + p] = (int)(uint32_t)(tag & 0xFFFFFFFFull);
   pi[(long long)DUSTB_PSP * stride + p] = s;

@@ -18,6 +18,14 @@ from .inputs import DustState
 GAMMA_DEFAULT = 1.707106781186547   # 1 + 1/sqrt(2), src/driver/driver.cpp:201
 
 
+class _null:
+    def __enter__(self):
+        return None
+
+    def __exit__(self, *a):
+        return False
+
+
 def _stream_ptr(stream) -> int:
     if stream is None:
         stream = torch.cuda.current_stream()
@@ -99,6 +107,26 @@ class DeviceDust:
     def seed_uniform(self, desc, stream=None):
         rc = self.lib.dustb_seed_uniform(self.pctx, C.byref(desc), _stream_ptr(stream))
         capi.check(rc, "seed_uniform")
+
+    def init_gas_ghosts(self, stream=None):
+        """Gives u0's ghost cells the values a step expects (the hydro's exchange and boundary
+        values agree with the cells they stand for): the copy exchange, then the planes
+        beyond physical x3 faces copied from the block's edge plane, ghost columns included.
+        For generated states, whose every cell (ghosts included) is drawn independently."""
+        self.ghost_copy("u0", int(self.t["u0"].shape[1]), x3_bcs=0, stream=stream)
+        ms = self.mesh
+        if not (ms.three_d and ms.x3bc):
+            return
+        u = self.t["u0"]
+        ng, nx3 = ms.ng, ms.nx[2]
+        nb = np.asarray(ms.nghbr)
+        lo = torch.from_numpy(np.nonzero(nb[:, 4] < 0)[0]).to(self.device)    # no block below
+        hi = torch.from_numpy(np.nonzero(nb[:, 22] < 0)[0]).to(self.device)   # none above
+        with torch.cuda.stream(stream) if stream is not None else _null():
+            if lo.numel():
+                u[lo, :, :ng] = u[lo, :, ng:ng + 1].expand(-1, -1, ng, -1, -1)
+            if hi.numel():
+                u[hi, :, ng + nx3:] = u[hi, :, ng + nx3 - 1:ng + nx3].expand(-1, -1, ng, -1, -1)
 
     def _rebuild_ctx(self):
         self.ctx = capi.make_ctx(self.mesh, self.t, self.npart, self.stride, self.phys)

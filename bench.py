@@ -255,7 +255,7 @@ def run_ours(args, rank, world):
         # (variant, rows per tile, particles per pass): one thread per source cell, tiles
         # of up to 256 cells, particle ranges copied in passes of 1016..4088
         cands = [(0, r, ch) for r in (1, 2, 4) if nx2 % r == 0 and r * nx1 <= 256
-                 for ch in (1024, 1152, 2048, 2176, 2304)]
+                 for ch in (1152, 2048, 2176, 2304, 0)]
         for var, rows, chunk in cands:
             mx.set_tiles(rows, chunk, var)
             try:
@@ -271,13 +271,12 @@ def run_ours(args, rank, world):
         mx.import_()
     for _ in range(args.warmup):
         mx.imex_cycle(dt)
+    # the timed steps replay one captured cycle (a CUDA graph of its 26 kernel launches)
+    graph = mx.capture(lambda: mx.imex_cycle(dt))
     barrier()
     clk = Clocks(int(os.environ.get("LOCAL_RANK", 0)))
     clk.start()
-    mx.timing(True)
-    ms_mixed = timed_cycles(lambda: mx.imex_cycle(dt), args.steps, stream)
-    ktimes = mx.kernel_times()
-    mx.timing(False)
+    ms_mixed = timed_cycles(graph.replay, args.steps, stream)
     clocks = clk.stop()
     ms_mixed = maxall(ms_mixed)
     mx.export()
@@ -286,7 +285,14 @@ def run_ours(args, rank, world):
     pr_mixed = dev.t["pr"][[1, 3, 5]].clone()
     u0_mixed = dev.t["u0"][:, 1:4].clone()
     mom_mixed = [float(x) for x in sum(dev.momentum())]
-    del mx
+    # the per-kernel breakdown: eager cycles with CUDA events around every launch (after the
+    # state above was taken; the FP64 form restarts from the initial state)
+    nk = 3
+    mx.timing(True)
+    ms_eager = timed_cycles(lambda: mx.imex_cycle(dt), nk, stream)
+    ktimes = mx.kernel_times()
+    mx.timing(False)
+    del graph, mx
     torch.cuda.empty_cache()
     if args.mixed_only:
         if rank == 0:
@@ -329,6 +335,7 @@ def run_ours(args, rank, world):
         "total_momentum_change_fp64_rel": max(abs(a - b) for a, b in zip(mom64, mom0)) / ptot,
         "error_words": [err_mixed, err_fp64],
     }
+    del v64, dv, mass, pd_mixed, pd_64, u64, pr_mixed, u0_mixed
     # ---- end to end through the C ABI with host buffers (mixed form) ----
     e2e = None
     if not args.no_e2e:
@@ -355,7 +362,7 @@ def run_ours(args, rank, world):
                 if "hbm_gbs" in peaks else "fallback 6650 GB/s",
                 "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": round(avg_ms, 4)}
     total_ms = sum(v[0] for v in ktimes.values()) or 1.0
-    shares = {k: {"ms_per_step": round(v[0] / args.steps, 3), "launches_per_step": v[1] / args.steps,
+    shares = {k: {"ms_per_step": round(v[0] / nk, 3), "launches_per_step": v[1] / nk,
                   "share": round(v[0] / total_ms, 3)} for k, v in ktimes.items() if v[1]}
     steps_per_s = npart * world / (ms_mixed * 1e-3)
     fp64_rate = npart * world / (ms_fp64 * 1e-3)
@@ -364,6 +371,12 @@ def run_ours(args, rank, world):
     # = 12, stage 2 adds the history term, and one ghost exchange of u0 closes the cycle:
     # 12 + 13 + 1 (the consistent dust kicks are folded into the next stage's push)
     launches_mixed = 26 * args.steps
+    # ---- the stratified pc2 workload (mixed pc2 vs FP64 pc2) ----
+    strat = None
+    if not args.no_pc2:
+        del dev
+        torch.cuda.empty_cache()
+        strat = measure_pc2_strat(args, stream, maxall, barrier)
     if rank == 0:
         cb = None if args.no_cpu else cpu_baseline()
         line = {
@@ -380,6 +393,8 @@ def run_ours(args, rank, world):
                        "parallelism": f"replicas x{world}"},
             "fp64": {"value": fp64_rate, "ms_per_step": ms_fp64,
                      "form": "per-task FP64 kernels (reference layout, FP64 atomics)"},
+            "timing": {"timed": "CUDA-graph replay of one captured cycle",
+                       "eager_ms_per_step": ms_eager},
             "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
             "errors_mixed_vs_fp64": errors,
             "roofline": roof,
@@ -388,10 +403,140 @@ def run_ours(args, rank, world):
             "gpu_launches": launches_mixed,
             "cpu_baseline": cb,
             "e2e": e2e,
+            "pc2_stratified": strat,
         }
         if res.get("tuned"):
             line["config"]["tuned"] = res["tuned"]
         print(json.dumps(line), flush=True)
+
+
+def build_strat(small, device="cuda"):
+    """The stratified streaming-instability set-up with a continuous size distribution
+    (inputs/dust_amr/si3d_strat_continuous.athinput at 128x128x256): a 3-D shearing box with
+    shear-periodic x1 faces, vertical gravity and outflow x3 faces, cells of 0.00625 H,
+    MeshBlocks of 64^3; 7 bins of equal width in ln St over St 1e-3..1, 1 particle per bin
+    per cell, each with its own St inside its bin and mass ~ St^0.5, total Z = 0.01 of the
+    gas; Gaussian heights of scale H_p = 0.02 H; NSH drift of each particle's own St plus
+    1e-3 Gaussian noise; gas rho = 1 with the NSH drift of the bins plus 1e-3 noise (the
+    hydro's own stratified gas is outside the drag step); pc2 coupling, TSC."""
+    import math
+    import numpy as np
+    from athenak_b200 import capi
+    from athenak_b200.drag import DeviceDust
+    from athenak_b200.inputs import nsh_gas
+    from athenak_b200.mesh import uniform_mesh
+    cells = (32, 32, 64) if small else (128, 128, 256)
+    nblock = (16, 16, 32) if small else (64, 64, 64)
+    dxc = 0.00625
+    hi = tuple(0.5 * dxc * c for c in cells)
+    ms = uniform_mesh(cells, nblock, 2, tuple(-h for h in hi), hi, x3bc=2, shear_x1=True)
+    nspec, slope, Z, hp = 7, 0.5, 0.01, 0.02
+    lo_t, hi_t = 1e-3, 1.0
+    w = (math.log(hi_t) - math.log(lo_t)) / nspec
+    tmid = [math.exp(math.log(lo_t) + (s + 0.5) * w) for s in range(nspec)]
+    share = np.array([t ** slope for t in tmid])
+    share /= share.sum()
+    ncell = ms.ncell_active
+    npart = ncell * nspec
+    vol = float(np.prod([2 * h for h in hi]))
+    # mean of (t/t_mid)^slope over a log-uniform bin of width w
+    mean_w = math.sinh(slope * w / 2) / (slope * w / 2)
+    om, q, etavk = 1.0, 1.5, 0.05
+    ugx, ugp = nsh_gas(om, q, 2 * om * etavk, list(Z * share), tmid)
+    phys = dict(scheme=2, drag_solver=2, shearing_box=True, stratified=True, back_reaction=True,
+                qshear=q, omega0=om)
+    dev = DeviceDust.empty(ms, npart, phys, device=device, nspecies=nspec)
+    d = capi.DustbSeedDesc()
+    d.seed = 3
+    d.nspecies = nspec
+    for s in range(nspec):
+        d.ppc[s] = 1
+        d.taus[s] = tmid[s]
+        d.mass[s] = Z * vol * share[s] / (ncell * mean_w)
+    d.ts_lo, d.ts_hi, d.mass_slope, d.hp = lo_t, hi_t, slope, hp
+    d.nsh, d.omega0, d.qshear = 1, om, q
+    d.vel_noise = 1e-3
+    d.rho0 = 1.0
+    d.ug[0], d.ug[1], d.ug[2] = ugx, ugp, 0.0
+    d.gas_noise = 1e-3
+    d.nb1, d.nb2, d.nb3 = ms.nblocks
+    dev.seed_uniform(d)
+    t0 = 3.7                                   # a mesh time with a non-zero shear offset
+    dev.set_time(t0)
+    dev.init_gas_ghosts()
+    dt = 0.3 * dxc / (1.0 + q * om * hi[0])
+    return dev, ms, dict(npart=npart, ncell=ncell, dt=dt, t=t0, cells=cells)
+
+
+def measure_pc2_strat(args, stream, maxall, barrier):
+    """Mixed pc2 cycles (CUDA-graph replay) and FP64 pc2 cycles from the same initial state
+    of the stratified workload, and the mixed result's errors against the FP64 one."""
+    import torch
+    from athenak_b200.mixed import MixedDust
+    dev, ms, W = build_strat(args.small)
+    npart, dt = W["npart"], W["dt"]
+    pr0, pi0, u00 = dev.t["pr"].clone(), dev.t["pi"].clone(), dev.t["u0"].clone()
+    mx = MixedDust(dev=dev, do_import=False)
+    mx.import_()
+    steps = args.steps
+    for _ in range(args.warmup):
+        mx.pc2_cycle(dt)
+    graph = mx.capture(lambda: mx.pc2_cycle(dt))
+    barrier()
+    ms_mixed = maxall(timed_cycles(graph.replay, steps, stream))
+    mx.export()
+    torch.cuda.synchronize()
+    err_m = dev.error_word()
+    v_m = dev.t["pr"][[1, 3, 5]].clone()
+    rem_m = dev.t["x3_removed"].clone()
+    # per-kernel breakdown (eager cycles with CUDA events; after the state above was taken)
+    nk = 3
+    mx.timing(True)
+    timed_cycles(lambda: mx.pc2_cycle(dt), nk, stream)
+    kt = mx.kernel_times()
+    mx.timing(False)
+    names = {"deposit_qp": "predictor", "kick": "advance"}
+    tot = sum(v[0] for v in kt.values()) or 1.0
+    shares = {names.get(k, k): {"ms_per_step": round(v[0] / nk, 3), "launches_per_step": v[1] / nk,
+                                "share": round(v[0] / tot, 3)} for k, v in kt.items() if v[1]}
+    del graph, mx
+    torch.cuda.empty_cache()
+    dev.t["pr"].copy_(pr0); dev.t["pi"].copy_(pi0); dev.t["u0"].copy_(u00)
+    dev.t["x3_removed"].zero_()
+    del pr0, pi0, u00
+    for _ in range(args.warmup):
+        dev.pc2_cycle(dt)
+    barrier()
+    ms_64 = maxall(timed_cycles(lambda: dev.pc2_cycle(dt), steps, stream))
+    torch.cuda.synchronize()
+    err_64 = dev.error_word()
+    v64 = dev.t["pr"][[1, 3, 5]]
+    mass = dev.t["pr"][16]
+    dv = v_m - v64
+    pd_m, pd_64 = (mass * v_m).sum(dim=1), (mass * v64).sum(dim=1)
+    rem_64 = dev.t["x3_removed"]
+    out = {
+        "workload": "stratified shearing box 128x128x256 (16 MeshBlocks of 64^3), shear-periodic x1, "
+                    "outflow x3, 7 bins St 1e-3..1 ppc 1 each, mass ~ St^0.5, Z 0.01, H_p 0.02, "
+                    "pc2 TSC" if not args.small else "small 32x32x64 stratified test",
+        "particles": npart, "cells": W["ncell"], "dt": dt, "mesh_time": W["t"],
+        "value": npart / (ms_mixed * 1e-3), "unit": UNIT, "ms_per_step": ms_mixed,
+        "steps": steps, "warmup": args.warmup, "timed": "CUDA-graph replay of one captured cycle",
+        "fp64": {"value": npart / (ms_64 * 1e-3), "ms_per_step": ms_64,
+                 "form": "per-task FP64 kernels (reference layout, FP64 atomics)"},
+        "speedup_mixed_vs_fp64": ms_64 / ms_mixed,
+        "kernels": shares,
+        "errors_mixed_vs_fp64": {
+            "velocity_max_rel": float(dv.abs().max() / v64.abs().max()),
+            "velocity_rms_rel": float(torch.sqrt((dv * dv).mean() / (v64 * v64).mean())),
+            "dust_momentum_rel": float((pd_m - pd_64).abs().max() / pd_64.abs().max()),
+            "x3_removed_mass_rel": float((rem_m[0] - rem_64[0]).abs() / rem_64[0].abs().clamp_min(1e-300)),
+            "x3_removed_count": [float(rem_m[1]), float(rem_64[1])],
+            "error_words": [err_m, err_64]},
+    }
+    del dev
+    torch.cuda.empty_cache()
+    return out
 
 
 def measure_e2e(dev, dt, args, stream):
@@ -460,6 +605,8 @@ def main():
     ap.add_argument("--cells", type=int, default=0,
                     help="a cubic mesh of this many cells per side (profiling cases)")
     ap.add_argument("--mixed-only", action="store_true", help="time the mixed form only")
+    ap.add_argument("--no-pc2", action="store_true",
+                    help="skip the stratified pc2 workload (128x128x256, 29.4 M particles)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", 1))
     rank = int(os.environ.get("RANK", 0))

@@ -287,8 +287,10 @@ int dustb_pc2_cycle(const dustb_ctx *ctx, double dt, double *chi_max, double *x3
 typedef struct dustb_mixed_params {
   double dx[3];            /* uniform cell size (single-level mesh) */
   int rows_per_tile;       /* 0: chosen by the library; else rows of nx1 cells per CTA tile */
-  int chunk;               /* 0: default (2048); shared-memory columns per CTA pass, a
-                              multiple of 4 in 64..8192 (chunk - 8 particles per pass) */
+  int chunk;               /* shared-memory columns per CTA pass (chunk - 8 particles per
+                              pass), a multiple of 4 in 64..8192; 0: the largest that keeps
+                              as many CTAs per SM as their registers allow (2380 for tiles
+                              of 128 cells) */
   int variant;             /* deposit kernels: 0 (the only one) */
   double *x3_removed;      /* device (mass, count) of the particles removed at outflow x3
                               faces, accumulated; required when mesh.x3bc is
@@ -362,6 +364,17 @@ typedef struct dustb_seed_desc {
   double vel_noise;             /* Gaussian sigma (Box-Muller on two hash draws) */
   double rho0, ug[3], gas_noise;/* gas density, velocity, uniform noise amplitude */
   int nb1, nb2, nb3;            /* MeshBlocks per direction (gid = (b3*nb2 + b2)*nb1 + b1) */
+  /* the continuous size distribution (src/pgen/dust_amr/dust_setup.cpp:736-745): with
+   * ts_lo > 0 species s is bin s of nspecies equal bins in ln t_s over [ts_lo, ts_hi], each
+   * particle draws its t_s log-uniform inside its bin (taus[] unused) and weighs
+   * mass[s] (t_s / t_mid)^mass_slope, t_mid the bin's geometric centre */
+  double ts_lo, ts_hi, mass_slope;
+  double hp;                    /* > 0: Gaussian heights of scale hp about x3 = 0 (redrawn
+                                   while outside the mesh) in place of uniform x3 */
+  int nsh;                      /* 1: every particle drifts at the NSH velocity of its own t_s
+                                   (dust_setup.hpp:58-65) about the gas drift (ug[0], ug[1]);
+                                   vx[], vy[] unused */
+  double omega0, qshear;        /* (nsh) */
 } dustb_seed_desc;
 
 /* Fills particles 0..npart-1 (species blocks in order, tag = index) and the gas u0 (ghosts

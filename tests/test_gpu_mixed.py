@@ -281,27 +281,6 @@ PC2_CASES = {
 }
 
 
-def consistent_ghosts(dev):
-    """The generator draws every cell's gas noise, ghosts included.  A step starts from ghost
-    cells that agree with the cells they stand for (the hydro's exchange and boundary
-    values): one copy exchange, then the planes beyond physical x3 faces copied from the
-    edge plane, x1/x2 ghost columns included (the mixed form reads ghost cells across
-    internal faces through their owners)."""
-    dev.ghost_copy("u0", 4, x3_bcs=0)
-    ms = dev.mesh
-    if not ms.three_d or not ms.x3bc:
-        return
-    u = dev.t["u0"]
-    ng, nx3 = ms.ng, ms.nx[2]
-    nb = np.asarray(ms.nghbr)
-    for m in range(ms.nmb):
-        if nb[m, 4] < 0:                     # no neighbour across the lower x3 face
-            u[m, :, :ng] = u[m, :, ng:ng + 1]
-        if nb[m, 22] < 0:                    # nor across the upper one
-            u[m, :, ng + nx3:] = u[m, :, ng + nx3 - 1:ng + nx3]
-    torch.cuda.synchronize()
-
-
 def pc2_pair(name, cycles=3):
     from athenak_b200.drag import DeviceDust
     from athenak_b200.mixed import MixedDust
@@ -309,8 +288,9 @@ def pc2_pair(name, cycles=3):
     ms = uniform_mesh(*c["mesh"], **c["kw"])
     st = make_state(ms, **c["st"])
     ref, mx = DeviceDust(st, c["phys"]), MixedDust(st, c["phys"])
-    consistent_ghosts(ref)
-    consistent_ghosts(mx.dev)
+    # the generator draws every gas cell, ghosts included: the ghost values a step starts from
+    ref.init_gas_ghosts()
+    mx.dev.init_gas_ghosts()
     p0 = sum(ref.momentum())
     t = 1.7
     for _ in range(cycles):
