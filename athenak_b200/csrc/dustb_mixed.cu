@@ -265,10 +265,13 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned b
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
-// bounded wait for the barrier's phase; false (and the error bit) if it never completes
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned *err) {
+// bounded wait for the barrier's phase; false (and the error bit) if it never completes.
+// Warp-uniform: the lanes of mask leave the loop together, so the warp is converged at the
+// CTA barrier that follows (a CTA barrier assumes converged warps)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned *err,
+                                          unsigned mask) {
   for (int it = 0; it < (1 << 22); ++it)
-    if (mbar_try_wait(bar, parity)) return true;
+    if (__all_sync(mask, mbar_try_wait(bar, parity))) return true;
   report(err, DUSTB_ERR_TIMEOUT);
   return false;
 }
@@ -894,8 +897,9 @@ struct GatherWindow {
   }
 };
 
-// the sums of every source cell of the tile, staged in shared memory as float4 (values 0..3)
-// at [(c*3 + b)*3 + a][cell], for the window pass below
+// the sums of a source cell's particles of the pass (or of one slot, when the pass splits
+// cells), staged in shared memory as float4 (values 0..3) at [(c*3 + b)*3 + a][cell or
+// slot], for the window pass below
 template <int MODE, int D3>
 __device__ __forceinline__ void stage_sums(const CellSums<MODE, D3> &A, float4 *s_acc, int cl,
                                            int nct) {
@@ -911,13 +915,21 @@ __device__ __forceinline__ void stage_sums(const CellSums<MODE, D3> &A, float4 *
                         FourValues<MODE>::value ? A.val(c, b, a, 3) : 0.0f);
 }
 
+// zero staged sums for a cell without particles in the pass
+template <int D3>
+__device__ __forceinline__ void stage_zero(float4 *s_acc, int cl, int nct) {
+  constexpr int WK = D3 ? 3 : 1;
+#pragma unroll
+  for (int x = 0; x < WK * 9; ++x) s_acc[x * nct + cl] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
 // adds the tile's deposit window to the FP64 field, one add per window cell and value: a
 // window cell (z plane c, row wy, column wx) sums the staged contributions of the up to 9
 // source cells of its plane that reach it; window cells beyond the block go to the owning
 // neighbour's active cell (the additive ghost exchange folded into the add)
 template <int MODE, int D3, int GH>
 __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, const TileArgs &T,
-                                           int m, int k, int j0, int tj) {
+                                           int m, int k, int j0, int tj, const int *s_ss) {
   constexpr int NC = FourValues<MODE>::value ? 4 : 3;
   constexpr int WK = D3 ? 3 : 1;
   const int nx1 = G.nx1, nct = tj * nx1;
@@ -936,8 +948,17 @@ __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, co
       for (int a = 0; a < 3; ++a) {
         const int ci = wx - a;                     // source column reaching this column
         if (ci < 0 || ci >= nx1) continue;
-        const float4 v = s_acc[((c * 3 + b) * 3 + a) * nct + cj * nx1 + ci];
-        s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+        const int src = cj * nx1 + ci;
+        if (!s_ss) {
+          const float4 v = s_acc[((c * 3 + b) * 3 + a) * nct + src];
+          s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+        } else {
+          // (a pass with split cells: the sums are staged per slot, a cell's slots in a row)
+          for (int q = s_ss[src]; q < s_ss[src + 1]; ++q) {
+            const float4 v = s_acc[((c * 3 + b) * 3 + a) * nct + q];
+            s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+          }
+        }
       }
     }
     double *f = T.dfield + at;
@@ -991,19 +1012,41 @@ __device__ __forceinline__ void pc2_particle(const Pc2Args &C, int three_d, floa
   disp[2] = C.dt * vh[2];
 }
 
-// One CTA per tile of tj rows of one plane, one thread per source cell.  Q/P: the sums of a
-// cell's particles are kept in registers over all passes.  Operator, kick, pc2 predictor and
-// advance: per pass, a gather phase (the 27 gather values in registers) writes each
+// a CTA barrier entered by converged warps (the loops before it end at different iterations
+// in different lanes; the barrier instruction assumes converged warps)
+__device__ __forceinline__ void cta_sync(unsigned wmask) {
+  __syncwarp(wmask);
+  __syncthreads();
+}
+
+// the head of a tile's shared memory: the cell ranges, the slot starts of the pass and the
+// centre mass of each cell (ints, ints, floats), 16-byte aligned
+__host__ __device__ inline size_t tile_head_bytes(int nct) {
+  return (((size_t)(3 * nct + 2) * 4 + 15) & ~(size_t)15);
+}
+
+// One CTA per tile of tj rows of one plane.  The tile's particles (one contiguous range of
+// the sorted shadow) are cut into passes of at most chunk - 8, bulk-copied into shared
+// memory.  In each pass every thread takes a slot: the particles of one source cell in the
+// pass, or an even share of them when the pass covers fewer cells than there are threads
+// (dense, clumped cells are split so that every thread has work).  A thread sums its slot's
+// 27-point deposits in registers; the sums are staged in shared memory per slot and added
+// to the field once per window cell and pass.  Operator, kick, pc2 predictor and advance:
+// a gather phase (the 27 gather values of the slot's cell in registers) first writes each
 // particle's deposit values (the kick: its velocity change; the advance: the gathered u*,
 // which a coalesced per-particle step turns into the new state and the impulse) into its
-// column, then a deposit phase sums them and adds them to the field; the gather values and
-// the sums are never live together.
+// column, then the deposit phase sums them; the gather values and the sums are never live
+// together.
+// (at most 168 registers: three CTAs of 128 threads per SM)
 template <int MODE, int D3, int SCHEME, int GH>
-__global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, TileArgs T) {
+__global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
   // fields copied: ox oy oz cc m [vx vy vz] (the predictor: t_s in place of cc)
   constexpr int NF = (MODE == MODE_OP) ? 5 : 8;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_wsum[kMaxTileThreads / 32];
+  __shared__ int s_wcnt[kMaxTileThreads / 32];
+  __shared__ int s_split;                          // some cell of the pass has several slots
   const int nx1 = G.nx1, tj = T.tj;
   const int nct = tj * nx1;                        // source cells of the tile = threads
   int t = blockIdx.x;
@@ -1015,13 +1058,15 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
   const int c0 = encode(G, m, k, j0, 0);
   const int CH = T.chunk;                          // buffer columns (multiple of 4)
   int *s_cs = (int *)smem;                         // [nct + 1] cell ranges
-  float *s_f = (float *)(smem + (((size_t)(nct + 1) * 4 + 15) & ~(size_t)15));  // [8][CH]
+  int *s_ss = s_cs + (nct + 1);                    // [nct + 1] slot starts of the pass
+  float *s_qt = (float *)(s_ss + (nct + 1));       // [nct] centre mass (Q/P)
+  float *s_f = (float *)(smem + tile_head_bytes(nct));   // [8][CH]
   float4 *s_acc = (float4 *)s_f;                   // the staged sums, after the rows
-  const int cl = threadIdx.x;                      // this thread's source cell
-  const int cj_l = cl / nx1, ci_l = cl - cj_l * nx1;
-  const int jrow = j0 + cj_l;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, wid = tid >> 5;
+  const unsigned wmask = (nct - (wid << 5)) >= 32 ? 0xffffffffu : ((1u << (nct - (wid << 5))) - 1u);
+  const int nwarp = (nct + 31) >> 5;
 
-  const int CHP = CH - 8;                          // particles per pass (room to round out)
   // the particle range [cb, ce) of a pass, field by field, rounded out to 16-byte groups
   auto issue_pass = [&](int cb, int ce) {
     const int a0 = cb & ~3, a1 = (ce + 3) & ~3;
@@ -1032,39 +1077,89 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
 #pragma unroll
     for (int f = 0; f < NF; ++f) bulk_copy(s_f + f * CH, S.f[fl[f]] + a0, bytes, &bar);
   };
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     // the first pass's copies go out before the cell ranges are read
     mbar_init(&bar, 1);
     const int p0 = T.cstart[c0], p1 = T.cstart[c0 + nct];
-    if (p1 > p0) issue_pass(p0, min(p1, p0 + CHP));
+    if (p1 > p0) issue_pass(p0, min(p1, p0 + (CH - 8)));
   }
-  for (int x = threadIdx.x; x <= nct; x += blockDim.x) s_cs[x] = T.cstart[c0 + x];
-  __syncthreads();
+  __syncwarp(wmask);
+  for (int x = tid; x <= nct; x += blockDim.x) s_cs[x] = T.cstart[c0 + x];
+  if (MODE == MODE_QP) s_qt[tid] = 0.0f;
+  cta_sync(wmask);
   const int P0 = s_cs[0], P1 = s_cs[nct];
-  const int c_lo = s_cs[cl], c_hi = s_cs[cl + 1];  // this cell's particles
-  CellSums<MODE, D3> qp;                           // Q/P: kept over all passes
-  if (MODE == MODE_QP) qp.zero();
-  float qt = 0.0f;
   const float inv_vol = (float)(1.0 / G.vol);
   const float inv_adt = (float)(1.0 / T.a_dt);
+  const int CHP = CH - 8;                          // particles per pass (room to round out)
+  const bool single = (P1 - P0) <= CHP;            // the whole tile in one pass
   unsigned parity = 0;
 
   for (int cb = P0; cb < P1; cb += CHP) {
     const int ce = min(P1, cb + CHP), cnt = ce - cb;
     const int a0 = cb & ~3, sh = cb - a0;
-    if (threadIdx.x == 0 && cb != P0) issue_pass(cb, ce);
+    if (tid == 0 && cb != P0) issue_pass(cb, ce);
+    // (the warp reconverges before the barriers of the slot map: thread 0 must not arrive
+    // at them apart from its warp)
+    __syncwarp(wmask);
+    // the slots of the pass: cell c gets q_c = ceil(n_c / R) of them, R the smallest share
+    // with sum q_c <= threads (every cell one slot when the pass covers all the cells).  A
+    // tile of one pass takes thread = cell directly (the uniform case)
+    int cl = -1, lo = 0, hi = 0;
+    if (single) {
+      cl = tid; lo = s_cs[tid] - a0; hi = s_cs[tid + 1] - a0;
+    } else {
+      const int n_c = max(0, min(s_cs[tid + 1], ce) - max(s_cs[tid], cb));
+      // (the cells with particles in the pass: per-warp ballots, summed after a barrier)
+      const unsigned bal = __ballot_sync(wmask, n_c > 0);
+      if (lane == 0) s_wcnt[wid] = __popc(bal);
+      cta_sync(wmask);
+      int ncp = 0;
+      for (int w = 0; w < nwarp; ++w) ncp += s_wcnt[w];
+      const int R = (ncp >= nct) ? cnt : (cnt + (nct - ncp) - 1) / (nct - ncp);
+      const int q_c = (n_c > 0) ? (n_c + R - 1) / R : 0;
+      int inc = q_c;                                 // block-wide inclusive scan of q_c
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(wmask, inc, o);
+        if (lane >= o) inc += y;
+      }
+      if (lane == 31 || tid == nct - 1) s_wsum[wid] = inc;
+      cta_sync(wmask);
+      for (int w = 0; w < wid; ++w) inc += s_wsum[w];
+      s_ss[tid + 1] = inc;
+      if (tid == 0) s_ss[0] = 0;
+      if (tid == nct - 1) s_split = inc > ncp;
+      cta_sync(wmask);
+      // this thread's slot: the last cell whose slots start at or before tid, an even share
+      // of its particles in the pass (columns lo..hi of the rows)
+      if (tid < s_ss[nct]) {
+        int L = 0, H = nct - 1;
+        while (L < H) {
+          const int M = (L + H + 1) >> 1;
+          if (s_ss[M] <= tid) L = M; else H = M - 1;
+        }
+        cl = L;
+        const int qc = s_ss[cl + 1] - s_ss[cl], rk = tid - s_ss[cl];
+        const int b0 = max(s_cs[cl], cb), len = min(s_cs[cl + 1], ce) - b0;
+        lo = b0 + (len * rk) / qc - a0;
+        hi = b0 + (len * (rk + 1)) / qc - a0;
+      }
+    }
+    const int cj_l = (cl >= 0) ? cl / nx1 : 0, ci_l = (cl >= 0) ? cl - cj_l * nx1 : 0;
+    const int jrow = j0 + cj_l;
     GatherWindow<D3> win;
     if (MODE != MODE_QP) win.template load<GH>(G, T.gfield, m, k, jrow, ci_l);   // while the copies fly
-    const bool ok = mbar_wait(&bar, parity, T.err);
+    const bool ok = mbar_wait(&bar, parity, T.err, wmask);
     parity ^= 1u;
     if (__syncthreads_or(!ok)) {
       // the copies never completed: wait once more (bounded) for them, then give up the tile
-      mbar_wait(&bar, parity ^ 1u, T.err);
+      mbar_wait(&bar, parity ^ 1u, T.err, wmask);
       return;
     }
-    // this cell's particles in the pass, at columns lo..hi of the rows
-    const int lo = max(c_lo, cb) - a0, hi = min(c_hi, ce) - a0;
     if (MODE == MODE_QP) {
+      CellSums<MODE, D3> qp;
+      qp.zero();
+      float qt = 0.0f;
       for (int r = lo; r < hi; ++r) {
         float wx_[3], wy_[3], wz_[3];
         wts(SCHEME, s_f[r], wx_);
@@ -1075,6 +1170,15 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
         qp.add(wx_, wy_, wz_, make_float2(mc, mc * s_f[5 * CH + r]),
                make_float2(mc * s_f[6 * CH + r], mc * s_f[7 * CH + r]));
       }
+      if (cl >= 0) atomicAdd(&s_qt[cl], qt);
+      // the rows are read by now: their space takes the staged sums (per cell, or per slot
+      // when the pass splits cells)
+      cta_sync(wmask);
+      const bool split = !single && s_split;
+      if (!single && !split && s_ss[tid + 1] == s_ss[tid]) stage_zero<D3>(s_acc, tid, nct);
+      if (cl >= 0) stage_sums<MODE, D3>(qp, s_acc, split ? tid : cl, nct);
+      cta_sync(wmask);
+      add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
     } else {
       // gather phase: the operator's m c u / V, the kick's velocity change, the predictor's
       // impulse and rate, or the advance's u*, into rows 5..7 (and 3)
@@ -1112,10 +1216,10 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
       if (MODE == MODE_KICK) {
         // the kicked velocities and rates of the pass, particle by particle (coalesced):
         // v <- v + dv, R <- dv / a_dt
-        __syncthreads();
+        cta_sync(wmask);
         // (four particles per thread at a time, their velocity loads issued together)
         constexpr int U = 4;
-        for (int x0 = threadIdx.x; x0 < cnt; x0 += U * blockDim.x) {
+        for (int x0 = tid; x0 < cnt; x0 += U * blockDim.x) {
           float v[U][3];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
@@ -1137,8 +1241,8 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
         // the advanced particles of the pass, one per thread (coalesced): v, the
         // displacement to the new position (cells), the rate dv; their impulses -m dv / V
         // into rows 5..7
-        __syncthreads();
-        for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
+        cta_sync(wmask);
+        for (int x = tid; x < cnt; x += blockDim.x) {
           const int s = sh + x, p = cb + x;
           const float v0[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
           const float u[3] = {s_f[5 * CH + s], s_f[6 * CH + s], s_f[7 * CH + s]};
@@ -1155,7 +1259,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
           const float f = -s_f[4 * CH + s] * inv_vol;
           s_f[5 * CH + s] = f * dv[0]; s_f[6 * CH + s] = f * dv[1]; s_f[7 * CH + s] = f * dv[2];
         }
-        __syncthreads();
+        cta_sync(wmask);
       }
       if (T.deposit) {
         // deposit phase: the sums of the values of this pass, added to the field
@@ -1170,33 +1274,34 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1) k_tile(PBuf S, Geo G, Tile
           sums.add(wx_, wy_, wz_, make_float2(f * s_f[5 * CH + r], f * s_f[6 * CH + r]),
                    make_float2(f * s_f[7 * CH + r], (MODE == MODE_PRED) ? s_f[3 * CH + r] : 0.0f));
         }
-        // the rows are read by now: their space takes the staged sums
-        __syncthreads();
-        stage_sums<MODE, D3>(sums, s_acc, cl, nct);
-        __syncthreads();
-        add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj);
+        // the rows are read by now: their space takes the staged sums (per cell, or per slot
+        // when the pass splits cells)
+        cta_sync(wmask);
+        const bool split = !single && s_split;
+        if (!single && !split && s_ss[tid + 1] == s_ss[tid]) stage_zero<D3>(s_acc, tid, nct);
+        if (cl >= 0) stage_sums<MODE, D3>(sums, s_acc, split ? tid : cl, nct);
+        cta_sync(wmask);
+        add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
       }
     }
-    // the next pass's copies overwrite the rows
-    __syncthreads();
+    // the next pass's copies overwrite the rows (and its slots the slot starts)
+    cta_sync(wmask);
   }
   if (MODE == MODE_QP) {
     // centre mass m c / V of the cell (dust_imex_point_center_mass): only this cell's
     // particles have it as their centre, so it is stored, not added
-    T.res[G.at(m, 4, 3, G.ks + k, G.js + jrow, G.is + ci_l)] = (double)qt;
-    stage_sums<MODE, D3>(qp, s_acc, cl, nct);
-    __syncthreads();
-    add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj);
+    const int cj = tid / nx1, ci = tid - cj * nx1;
+    T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj, G.is + ci)] = (double)s_qt[tid];
   }
 }
 
-// shared memory of a tile: the cell ranges, then the larger of the pass rows and the staged
-// sums (27 float4 per cell in 3-D, 9 in 2-D)
+// shared memory of a tile: the head, then the larger of the pass rows and the staged sums
+// (27 float4 per slot in 3-D, 9 in 2-D)
 size_t tile_smem(int three_d, int tj, int nx1, int chunk) {
   const int nct = tj * nx1;
   const size_t rows = (size_t)kTileRows * chunk * 4;
   const size_t sums = (size_t)(three_d ? 27 : 9) * nct * 16;
-  return (((size_t)(nct + 1) * 4 + 15) & ~(size_t)15) + (rows > sums ? rows : sums);
+  return tile_head_bytes(nct) + (rows > sums ? rows : sums);
 }
 
 // m/rho of a gas field on every cell, ghosts included: the predictor's gather field
@@ -1318,8 +1423,8 @@ int default_chunk(int tj, int nx1) {
   const int nct = tj * nx1;
   int ctas = 65536 / (168 * nct);
   ctas = ctas < 1 ? 1 : (ctas > 8 ? 8 : ctas);
-  const long long per = 233472 / ctas - 1024 - 64;     // less the reserve and the barrier
-  long long ch = (per - ((((long long)nct + 1) * 4 + 15) & ~15LL)) / (kTileRows * 4);
+  const long long per = 233472 / ctas - 2560 - 64;     // less a reserve and the statics
+  long long ch = (per - (long long)tile_head_bytes(nct)) / (kTileRows * 4);
   ch &= ~3LL;
   return (int)(ch < 64 ? 64 : (ch > 8192 ? 8192 : ch));
 }
