@@ -226,6 +226,11 @@ def run_ours(args, rank, world):
     from athenak_b200.mixed import MixedDust
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     stream = torch.cuda.current_stream()
+    if args.pc2_only:
+        out = measure_pc2_strat(args, stream, lambda x: x, lambda: None)
+        if rank == 0:
+            print(json.dumps(dict(out, note="stratified pc2 workload only (profiling case)")), flush=True)
+        return
     dev, ms, W = build_workload(args.small, cells=args.cells)
     npart, dt = W["npart"], W["dt"]
     torch.cuda.synchronize()
@@ -607,6 +612,8 @@ def main():
     ap.add_argument("--mixed-only", action="store_true", help="time the mixed form only")
     ap.add_argument("--no-pc2", action="store_true",
                     help="skip the stratified pc2 workload (128x128x256, 29.4 M particles)")
+    ap.add_argument("--pc2-only", action="store_true",
+                    help="time the stratified pc2 workload only (profiling case)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", 1))
     rank = int(os.environ.get("RANK", 0))
