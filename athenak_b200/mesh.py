@@ -145,3 +145,20 @@ def uniform_mesh(ncells=(32, 32, 32), nblock=(16, 16, 16), ng=2,
     return MeshSpec(nx=tuple(nblock), nblocks=nb, ng=ng, lo=tuple(lo), hi=tuple(hi),
                     three_d=three_d, multi_d=multi_d, x3bc=x3bc, mb_size=mb, nghbr=ng_tab,
                     shear_x1=bool(shear_x1))
+
+
+def box_ensemble_mesh(side: int, nbox: int, ng: int = 2, L: float = 1.0) -> MeshSpec:
+    """nbox independent periodic boxes of side^3 cells as one MeshBlock pack: every block
+    covers the same domain [0, L]^3 and is its own neighbour in all 26 directions (a
+    periodic box of one MeshBlock), so one call of the drag step advances every box."""
+    if ng < 2:
+        raise ValueError("the dust module requires nghost >= 2")
+    mb = np.zeros((nbox, 9), np.float64)
+    mb[:, X1MAX] = mb[:, X2MAX] = mb[:, X3MAX] = L
+    mb[:, DX1] = mb[:, DX2] = mb[:, DX3] = L / side
+    nb = np.full((nbox, 27), -1, np.int32)
+    for d in range(27):
+        if d != dir_index(0, 0, 0):
+            nb[:, d] = np.arange(nbox, dtype=np.int32)
+    return MeshSpec(nx=(side, side, side), nblocks=(nbox, 1, 1), ng=ng, lo=(0.0,) * 3,
+                    hi=(L,) * 3, three_d=True, multi_d=True, x3bc=0, mb_size=mb, nghbr=nb)
