@@ -162,8 +162,11 @@ SIGNATURES = {
     "dustb_pc2_cycle": [CTXP, D, VP, VP, VP],
     "dustb_seed_uniform": [CTXP, C.POINTER(DustbSeedDesc), VP],
     "dustb_cell_index_static": [CTXP, VP, VP, VP],
+    "dustb_phst_scratch_bytes": [MESHP, I],
+    "dustb_phst": [CTXP, VP, VP, VP, LL, VP],
 }
-RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_last_error": C.c_char_p}
+RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_phst_scratch_bytes": LL,
+            "dustb_last_error": C.c_char_p}
 # declared by athenak_b200.mixed (they take its DustbMixedParams struct)
 EXTRA_SIGNATURES = {"dustb_mixed_workspace_bytes", "dustb_mixed_import", "dustb_mixed_export",
                     "dustb_mixed_imex_cycle", "dustb_mixed_sort", "dustb_mixed_timing",

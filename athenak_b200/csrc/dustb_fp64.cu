@@ -994,6 +994,118 @@ __global__ void k_pc2_commit(Ind d, double *u0, int nv, const double *dmom, cons
     u0[d.at(m, nv, 1 + v, k, j, i)] += dmom[d.at(m, 3, v, k, j, i)] - wpred * qdep[d.at(m, 5, 1 + v, k, j, i)];
 }
 
+// ---- ParticleHistory (the phst row), src/dust/dust_science.cpp:391-482 ------------------
+constexpr int kPhstChunk = 4096, kPhstSums = 7;
+
+// the particle sums of one chunk of 4096 particles, in particle order (dust_science.cpp:400-413)
+__global__ void k_phst_chunks(PCtx P, int zc, double *part, int nchunk) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nchunk) return;
+  double a[kPhstSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  const int p0 = c * kPhstChunk, p1 = min(p0 + kPhstChunk, P.npart);
+  for (int p = p0; p < p1; ++p) {
+    const double m = P.r(DUSTB_IPM, p);
+    if (m == 0.0) continue;                        // outflow tombstones
+    const double v1 = P.r(DUSTB_IPVX, p), v2 = P.r(DUSTB_IPVY, p), v3 = P.r(DUSTB_IPVZ, p);
+    const double z = P.r(zc, p);
+    a[0] += 1.0;
+    a[1] += m;
+    a[2] += m * v1; a[3] += m * v2; a[4] += m * v3;
+    a[5] += 0.5 * m * (v1 * v1 + v2 * v2 + v3 * v3);
+    a[6] += m * z * z;
+  }
+  for (int q = 0; q < kPhstSums; ++q) part[(long long)c * kPhstSums + q] = a[q];
+}
+
+// the chunks summed in order (the host loop of dust_science.cpp:415-416), one thread
+__global__ void k_phst_sums(const double *part, int nchunk, const double *chi, int br,
+                            double *row) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double s[kPhstSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int c = 0; c < nchunk; ++c)
+    for (int q = 0; q < kPhstSums; ++q) s[q] += part[(long long)c * kPhstSums + q];
+  for (int q = 0; q < 6; ++q) row[q] = s[q];
+  row[6] = (s[1] > 0.0) ? sqrt(s[6] / s[1]) : 0.0;
+  row[12] = (br && chi) ? *chi : -1.0;
+  row[13] = -1.0;
+  row[14] = 0.0;
+  row[15] = 0.0;
+}
+
+// the mass component of DepositPointScienceFields (src/dust/dust_gravity_points.cpp:277-304):
+// m/V with the deposit weights into the block's cells, ghost cells included
+__global__ void k_mass_deposit(PCtx P, MCtx M, Ind d, double *f, unsigned *err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  const double mass = P.r(DUSTB_IPM, p);
+  if (mass == 0.0) return;
+  const int m = P.i(DUSTB_PGID, p) - M.gids;
+  if (!block_ok(d, m)) { report(err, DUSTB_ERR_PGID); return; }
+  int ip, jp, kp; double wx[3], wy[3], wz[3];
+  weights3(M, d, m, P.r(DUSTB_IPX, p), P.r(DUSTB_IPY, p), P.r(DUSTB_IPZ, p), ip, jp, kp, wx, wy, wz);
+  if (!halo_ok(d, ip, jp, kp)) { report(err, DUSTB_ERR_HALO); return; }
+  const double density = mass / cell_vol(M, d, m);
+  for (int c = 0; c < 3; ++c)
+    for (int b = 0; b < 3; ++b)
+      for (int a = 0; a < 3; ++a) {
+        const double w = density * wz[c] * wy[b] * wx[a];
+        if (w == 0.0) continue;
+        atomicAdd(&f[d.at(m, 1, 0, kp + c - 1, jp + b - 1, ip + a - 1)], w);
+      }
+}
+
+// the densest active cell (dust_science.cpp:428-441): per block of threads the largest value
+// and, among equal values, the smallest cell index q = ((m nx3 + k) nx2 + j) nx1 + i
+__device__ __forceinline__ void better(double &bv, long long &bq, double v, long long q) {
+  if (v > bv || (v == bv && q < bq && bq >= 0)) { bv = v; bq = q; }
+}
+__global__ void k_argmax_blocks(Ind d, const double *f, double *bval, long long *bloc) {
+  __shared__ double sv[256];
+  __shared__ long long sq[256];
+  const long long ncell = (long long)d.nx1 * d.nx2 * d.nx3;
+  double v = 0.0;
+  long long q = -1;
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < ncell * d.nmb;
+       x += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(x / ncell);
+    const long long r = x - (long long)m * ncell;
+    const int k = (int)(r / ((long long)d.nx1 * d.nx2)), j = (int)((r / d.nx1) % d.nx2), i = (int)(r % d.nx1);
+    better(v, q, f[d.at(m, 1, 0, d.ks + k, d.js + j, d.is + i)], x);
+  }
+  sv[threadIdx.x] = v; sq[threadIdx.x] = q;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      double bv = sv[threadIdx.x]; long long bq = sq[threadIdx.x];
+      const double ov = sv[threadIdx.x + o]; const long long oq = sq[threadIdx.x + o];
+      if (oq >= 0) better(bv, bq, ov, oq);
+      sv[threadIdx.x] = bv; sq[threadIdx.x] = bq;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { bval[blockIdx.x] = sv[0]; bloc[blockIdx.x] = sq[0]; }
+}
+__global__ void k_argmax_final(Ind d, MCtx M, const double *bval, const long long *bloc,
+                               int nb, double *row) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double v = 0.0;
+  long long q = -1;
+  for (int b = 0; b < nb; ++b) if (bloc[b] >= 0) better(v, q, bval[b], bloc[b]);
+  row[7] = (q >= 0 && v > 0.0) ? v : 0.0;
+  row[8] = row[9] = row[10] = 0.0;
+  row[11] = -1.0;
+  if (q >= 0 && v > 0.0) {
+    const long long ncell = (long long)d.nx1 * d.nx2 * d.nx3;
+    const int m = (int)(q / ncell);
+    const long long r = q - (long long)m * ncell;
+    const int k = (int)(r / ((long long)d.nx1 * d.nx2)), j = (int)((r / d.nx1) % d.nx2), i = (int)(r % d.nx1);
+    row[8] = M.s(m, X1MIN) + (i + 0.5) * M.s(m, DX1);
+    row[9] = M.s(m, X2MIN) + (j + 0.5) * M.s(m, DX2);
+    row[10] = d.three_d ? M.s(m, X3MIN) + (k + 0.5) * M.s(m, DX3) : 0.0;
+    row[11] = 0.0;                                 // single level: the root
+  }
+}
+
 long long n_active(const Ind &d) { return (long long)d.nmb * d.nx3 * d.nx2 * d.nx1; }
 long long n_all(const Ind &d) { return d.cells() * d.nmb; }
 
@@ -1271,6 +1383,43 @@ int dustb_pc2_commit(const dustb_ctx *c, double wpred, void *stream) {
   k_pc2_commit<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom,
                                                                     c->f.qdep, wpred);
   return launch_status("pc2_commit");
+}
+
+long long dustb_phst_scratch_bytes(const dustb_mesh *mesh, int npart) {
+  if (!mesh) return -1;
+  const Ind d = make_ind(*mesh);
+  const long long nchunk = ((long long)(npart > 0 ? npart : 1) + kPhstChunk - 1) / kPhstChunk;
+  const long long fb = d.cells() * d.nmb * 8;
+  return ((nchunk * kPhstSums * 8 + 255) & ~255LL) + ((fb + 255) & ~255LL) + 1024 * 16;
+}
+
+int dustb_phst(const dustb_ctx *c, const double *chi_max, double *row, void *scratch,
+               long long bytes, void *stream) {
+  CHECK_CTX(c);
+  if (!row) return DUSTB_EINVAL;
+  if (!c->mesh.three_d) return DUSTB_EUNSUP;      // (the densest cell of point particles: 3-D)
+  if (!scratch || bytes < dustb_phst_scratch_bytes(&c->mesh, c->part.npart)) return DUSTB_ESCRATCH;
+  const Ind d = make_ind(c->mesh);
+  const int np = c->part.npart;
+  const int nchunk = (int)(((long long)(np > 0 ? np : 1) + kPhstChunk - 1) / kPhstChunk);
+  char *b = (char *)scratch;
+  double *part = (double *)b;
+  b += ((long long)nchunk * kPhstSums * 8 + 255) & ~255LL;
+  double *field = (double *)b;
+  b += (d.cells() * d.nmb * 8 + 255) & ~255LL;
+  double *bval = (double *)b;
+  long long *bloc = (long long *)(b + 1024 * 8);
+  cudaMemsetAsync(part, 0, (size_t)nchunk * kPhstSums * 8, S(stream));
+  if (np > 0) k_phst_chunks<<<blocks_for(nchunk), kThreads, 0, S(stream)>>>(pview(c), DUSTB_IPZ, part, nchunk);
+  k_phst_sums<<<1, 1, 0, S(stream)>>>(part, nchunk, chi_max, c->phys.back_reaction, row);
+  cudaMemsetAsync(field, 0, (size_t)d.cells() * d.nmb * 8, S(stream));
+  if (np > 0) k_mass_deposit<<<PGRID(c)>>>(pview(c), mview(c), d, field, c->err);
+  int rc = dustb_ghost_add(c, field, 1, stream);
+  if (rc) return rc;
+  const int nb = 1024;
+  k_argmax_blocks<<<nb, 256, 0, S(stream)>>>(d, field, bval, bloc);
+  k_argmax_final<<<1, 1, 0, S(stream)>>>(d, mview(c), bval, bloc, nb, row);
+  return launch_status("phst");
 }
 
 // one imex2+ cycle in the task order of src/dust/dust_tasks.cpp:38-120 (stage 3 dormant,

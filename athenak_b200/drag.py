@@ -228,6 +228,19 @@ class DeviceDust:
         capi.check(rc, "pc2_cycle")
         return out[0]
 
+    def phst(self, chi_max=None, stream=None):
+        """ParticleHistory's row (16 doubles, on the device): particle sums, the densest
+        cell of the mass deposit, chi_max (a device scalar, or None)."""
+        n = int(self.lib.dustb_phst_scratch_bytes(C.byref(self.ctx.mesh), self.npart))
+        s = self.t.get("phst_scratch")
+        if s is None or s.numel() < n:
+            s = torch.empty(n, dtype=torch.uint8, device=self.device)
+            self.t["phst_scratch"] = s
+        row = torch.zeros(16, dtype=torch.float64, device=self.device)
+        chi = 0 if chi_max is None else chi_max.data_ptr()
+        self._call("phst", chi, row.data_ptr(), s.data_ptr(), s.numel(), stream=stream)
+        return row
+
     # ---- sort ----
     def _scratch(self):
         n = int(self.lib.dustb_sort_scratch_bytes(C.byref(self.ctx.mesh), self.npart))

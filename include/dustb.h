@@ -269,6 +269,22 @@ int dustb_imex_cycle(const dustb_ctx *ctx, const dustb_imex_coeffs *c, double *x
 int dustb_pc2_cycle(const dustb_ctx *ctx, double dt, double *chi_max, double *x3_removed,
                     void *stream);
 
+/* DustGasDrag::ParticleHistory (src/dust/dust_science.cpp:391-482), the phst row, on a
+ * single-level 3-D mesh of point particles.  row (device, 16 doubles): [0] particles with
+ * m != 0, [1] mass, [2..4] momentum, [5] kinetic energy, [6] z_rms = sqrt(sum m z^2 / sum m),
+ * each summed as the reference sums them (chunks of 4096 particles in particle order, then
+ * the chunks in order: deterministic); [7] the largest density of the mass deposit on the
+ * active cells (m/V with the deposit weights, the ghost deposits summed into their owners
+ * as dustb_ghost_add sums them; among equal values the first cell in (block, k, j, i)
+ * order), [8..10] that cell's centre, [11] its level above the root (0; with centre 0 and
+ * -1 when the largest density is 0); [12] *chi_max when back_reaction (NULL or none: -1);
+ * [13] -1 (no stiffness threshold); [14], [15] 0 (no coarsening events, no removal
+ * counter).  The particle rows are read as they are (export the mixed shadow first).
+ * Scratch: dustb_phst_scratch_bytes.  2-D meshes: DUSTB_EUNSUP. */
+long long dustb_phst_scratch_bytes(const dustb_mesh *mesh, int npart);
+int dustb_phst(const dustb_ctx *ctx, const double *chi_max, double *row, void *scratch,
+               long long scratch_bytes, void *stream);
+
 /* ---- mixed-precision form ---------------------------------------------------------------
  * A compact device shadow of the particles, kept between imports and exports: per particle
  * a packed cell id (block, k, j, i), FP32 offsets inside the cell, FP32 velocity, velocity

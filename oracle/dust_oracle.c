@@ -1171,6 +1171,91 @@ void oracle_pc2_commit(const dustb_ctx *c, double wpred) {
 /* ---- cycle drivers: the task order of src/dust/dust_tasks.cpp:38-120 -------------------- */
 
 /* imex2+ tableau, src/driver/driver.cpp:278-300 */
+/* ---- ParticleHistory, src/dust/dust_science.cpp:391-482 (3-D point particles) ----------
+ * row[0..6]: the particle sums, chunks of 4096 particles each summed in particle order, the
+ * chunks summed in order (:398-418); row[7..11]: the densest active cell of the mass deposit
+ * (DepositPointScienceFields, src/dust/dust_gravity_points.cpp:277-309: m/V times the deposit
+ * weights, the ghost deposits summed into their owners) and its centre, the first cell in
+ * (block, k, j, i) order among equal values (:428-441); row[12]: *chi (back-reaction) or -1;
+ * row[13] -1, row[14..15] 0.  field: nmb cells of one variable (ghosts included), scratch. */
+unsigned oracle_phst(const dustb_ctx *c, const double *chi, double *field, double row[16]) {
+  const dustb_mesh *ms = &c->mesh;
+  const double *pr = c->part.pr;
+  const int *pi = c->part.pi;
+  const size_t stride = (size_t)c->part.stride;
+  const int np = c->part.npart;
+  const int zc = ms->three_d ? DUSTB_IPZ : DUSTB_IPY;
+  double sums[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int c0 = 0; c0 < np; c0 += 4096) {
+    double a[7] = {0, 0, 0, 0, 0, 0, 0};
+    const int p1 = (c0 + 4096 < np) ? c0 + 4096 : np;
+    for (int p = c0; p < p1; ++p) {
+      const double m = PR(DUSTB_IPM, p);
+      if (m == 0.0) continue;
+      const double v1 = PR(DUSTB_IPVX, p), v2 = PR(DUSTB_IPVY, p), v3 = PR(DUSTB_IPVZ, p);
+      const double z = PR(zc, p);
+      a[0] += 1.0;
+      a[1] += m;
+      a[2] += m*v1; a[3] += m*v2; a[4] += m*v3;
+      a[5] += 0.5*m*(v1*v1 + v2*v2 + v3*v3);
+      a[6] += m*z*z;
+    }
+    for (int q = 0; q < 7; ++q) sums[q] += a[q];
+  }
+  for (int q = 0; q < 6; ++q) row[q] = sums[q];
+  row[6] = (sums[1] > 0.0) ? sqrt(sums[6]/sums[1]) : 0.0;
+  /* the mass deposit */
+  const Ind d = indices(ms);
+  memset(field, 0, field_size(ms, 1)*sizeof(double));
+  unsigned err = 0;
+  for (int p = 0; p < np; ++p) {
+    const double mass = PR(DUSTB_IPM, p);
+    if (mass == 0.0) continue;
+    const int m = PI(DUSTB_PGID, p) - ms->gids;
+    if (m < 0 || m >= ms->nmb) { err |= DUSTB_ERR_PGID; continue; }
+    int ip, jp, kp; double wx[3], wy[3], wz[3];
+    particle_weights(c, &d, m, PR(DUSTB_IPX, p), PR(DUSTB_IPY, p), PR(DUSTB_IPZ, p), &ip, &jp,
+                     &kp, wx, wy, wz);
+    if (!halo_ok(ms, &d, ip, jp, kp)) { err |= DUSTB_ERR_HALO; continue; }
+    const double density = mass/cell_volume(ms, m);
+    for (int cc = 0; cc < 3; ++cc)
+      for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) {
+          const double w = density*wz[cc]*wy[b]*wx[a];
+          if (w == 0.0) continue;
+          A5(field, 1, d, m, 0, kp + cc - 1, jp + b - 1, ip + a - 1) += w;
+        }
+  }
+  oracle_ghost_add(c, field, 1);
+  double best = 0.0;
+  long long loc = -1;
+  const long long ncell = (long long)ms->nx1*ms->nx2*ms->nx3;
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = 0; k < ms->nx3; ++k)
+      for (int j = 0; j < ms->nx2; ++j)
+        for (int i = 0; i < ms->nx1; ++i) {
+          const double v = A5(field, 1, d, m, 0, d.ks + k, d.js + j, d.is + i);
+          if (v > best) { best = v; loc = ((long long)m*ncell + ((long long)k*ms->nx2 + j)*ms->nx1 + i); }
+        }
+  row[7] = best;
+  row[8] = row[9] = row[10] = 0.0;
+  row[11] = -1.0;
+  if (loc >= 0) {
+    const int m = (int)(loc/ncell);
+    const long long r = loc % ncell;
+    const int k = (int)(r/((long long)ms->nx1*ms->nx2)), j = (int)((r/ms->nx1) % ms->nx2), i = (int)(r % ms->nx1);
+    row[8] = MB(m, X1MIN) + (i + 0.5)*MB(m, DX1);
+    row[9] = MB(m, X2MIN) + (j + 0.5)*MB(m, DX2);
+    row[10] = ms->three_d ? MB(m, X3MIN) + (k + 0.5)*MB(m, DX3) : 0.0;
+    row[11] = 0.0;
+  }
+  row[12] = (c->phys.back_reaction && chi) ? *chi : -1.0;
+  row[13] = -1.0;
+  row[14] = 0.0;
+  row[15] = 0.0;
+  return err;
+}
+
 void oracle_imex2p_coeffs(double gamma, double gam0[3], double gam1[3], double beta[3],
                           double *atw22) {
   gam0[0] = 1.0; gam1[0] = 0.0; beta[0] = gamma;

@@ -68,6 +68,7 @@ def lib():
             "oracle_pc2_commit": ([P, D], None),
             "oracle_imex_cycle": ([P, D, D, VP, VP], C.c_uint),
             "oracle_pc2_cycle": ([P, D, VP, VP], C.c_uint),
+            "oracle_phst": ([P, VP, VP, VP], C.c_uint),
         }
         for name, (args, res) in sig.items():
             f = getattr(_lib, name)
@@ -212,6 +213,14 @@ class Oracle:
         return err, chi.value
 
     # --- diagnostics ---
+    def phst(self, chi=None):
+        """ParticleHistory's row (16 doubles) and the error word."""
+        row = np.zeros(16)
+        field = np.zeros(self.mesh.field_shape(1))
+        ch = None if chi is None else np.array([chi], np.float64)
+        err = self.call("phst", capi.ptr(ch), field.ctypes.data, row.ctypes.data)
+        return row, err
+
     def momentum(self):
         """Total (gas, dust) momentum vectors over active cells / live particles."""
         ms = self.mesh
