@@ -62,5 +62,32 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return OUT
 
 
+HOST_SRC = os.path.join(HERE, "host", "dust_gas_drag.cpp")
+HOST_LIB = os.path.join(HERE, "libdustb_host.so")
+
+
+def cuda_home() -> str:
+    return os.path.dirname(os.path.dirname(os.path.realpath(nvcc())))
+
+
+def build_host(force: bool = False) -> str:
+    """The C++ host layer (athenak_b200/host: DustGasDrag's task functions over the C ABI)
+    as libdustb_host.so, linked against libdustb.so."""
+    lib = build(force)
+    hdr = os.path.join(HERE, "host", "dust_gas_drag.hpp")
+    newest = max(os.path.getmtime(p) for p in (HOST_SRC, hdr, lib))
+    if not force and os.path.exists(HOST_LIB) and os.path.getmtime(HOST_LIB) >= newest:
+        return HOST_LIB
+    cu = cuda_home()
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-o", HOST_LIB, HOST_SRC,
+           f"-I{cu}/include", f"-L{HERE}", "-ldustb", f"-L{cu}/lib64", "-lcudart",
+           "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{cu}/lib64"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("host layer build failed")
+    return HOST_LIB
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -1,0 +1,216 @@
+// dust_gas_drag.cpp -- DustGasDrag's task functions forwarding to the C ABI (see the header).
+#include "dust_gas_drag.hpp"
+
+#include <cuda_runtime.h>
+
+namespace athenak_b200 {
+
+void Driver::SetImEx2PlusCoefficients(double gamma_new) {
+  gamma = gamma_new;
+  gam0[0] = 1.0; gam1[0] = 0.0; beta[0] = gamma;
+  gam0[1] = (2.0 * gamma - 1.0) / (2.0 * gamma * gamma);
+  gam1[1] = 1.0 - (2.0 * gamma - 1.0) / (2.0 * gamma * gamma);
+  beta[1] = 1.0 / (2.0 * gamma);
+  gam0[2] = 1.0; gam1[2] = 0.0; beta[2] = 0.0;
+  for (int i = 0; i < 4; ++i)
+    for (int s = 0; s < 4; ++s) a_twid[i][s] = 0.0;
+  a_twid[2][2] = (1.0 - 2.0 * gamma * gamma) / 2.0 / gamma;
+  a_impl = gamma;
+}
+
+DustGasDrag::DustGasDrag(const dustb_ctx &ctx, void *stream, DustCoupling coupling)
+    : ctx_(ctx), stream_(stream), coupling_(coupling) {
+  if (cudaMalloc(&dev_scalars_, 4 * sizeof(double)) != cudaSuccess) {
+    dev_scalars_ = nullptr;
+    last_error_ = "DustGasDrag: device scalars not allocated";
+    return;
+  }
+  cudaMemsetAsync(dev_scalars_, 0, 4 * sizeof(double), (cudaStream_t)stream_);
+}
+
+DustGasDrag::~DustGasDrag() {
+  if (dev_scalars_) cudaFree(dev_scalars_);
+}
+
+TaskStatus DustGasDrag::Check(int rc, const char *task) {
+  if (rc == DUSTB_OK) return TaskStatus::complete;
+  last_error_ = std::string(task) + ": " + dustb_last_error() + " (" + std::to_string(rc) + ")";
+  return TaskStatus::fail;
+}
+
+// the implicit stage's a dt (a_impl dt) and the stage's RK weights, as the reference forms them
+static inline double a_dt(const Driver *d) { return d->a_impl * d->dt; }
+
+TaskStatus DustGasDrag::FirstTwoImpRK(Driver *pdrive, int stage) {
+  // stage 1: the register copies; pc2 stage 2: the midpoint u* from the two gas states,
+  // ghost cells included (dust_push.cpp:53-59)
+  if (stage == 1) return Check(dustb_register_copy(&ctx_, stream_), "FirstTwoImpRK");
+  if (coupling_ == DustCoupling::pc2 && stage == 2)
+    return Check(dustb_pc2_midpoint(&ctx_, stream_), "FirstTwoImpRK");
+  return TaskStatus::complete;
+}
+
+TaskStatus DustGasDrag::RKUpdate(Driver *pdrive, int stage) {
+  const int s = stage - 1;
+  if (coupling_ == DustCoupling::pc2)
+    return Check(dustb_gas_rk_noflux(&ctx_, stage == 1 ? 1.0 : 0.5, stage == 1 ? 0.0 : 0.5, stream_),
+                 "RKUpdate");
+  return Check(dustb_gas_rk_noflux(&ctx_, pdrive->gam0[s], pdrive->gam1[s], stream_), "RKUpdate");
+}
+
+TaskStatus DustGasDrag::AddDragHistoryGas(Driver *pdrive, int stage) {
+  if (coupling_ != DustCoupling::imex || stage != 2 || !ctx_.phys.back_reaction)
+    return TaskStatus::complete;
+  return Check(dustb_history_gas(&ctx_, pdrive->a_twid[stage][stage] * pdrive->dt, stream_),
+               "AddDragHistoryGas");
+}
+
+TaskStatus DustGasDrag::ExplicitPush(Driver *pdrive, int stage) {
+  const int s = stage - 1;
+  if (coupling_ == DustCoupling::pc2) {
+    if (stage != 2) return TaskStatus::complete;   // the advance of the midpoint stage
+    return Check(dustb_pc2_advance(&ctx_, pdrive->dt, stream_), "ExplicitPush");
+  }
+  const double atw = (stage == 2) ? pdrive->a_twid[stage][stage] * pdrive->dt : 0.0;
+  return Check(dustb_push_imex(&ctx_, pdrive->gam0[s], pdrive->gam1[s], pdrive->beta[s] * pdrive->dt,
+                               atw, stream_),
+               "ExplicitPush");
+}
+
+TaskStatus DustGasDrag::UpdateParticleGIDs(Driver *pdrive, int stage) {
+  if (coupling_ == DustCoupling::pc2 && stage != 2) return TaskStatus::complete;
+  return Check(dustb_route(&ctx_, dev_scalars_, stream_), "UpdateParticleGIDs");
+}
+
+TaskStatus DustGasDrag::DepositDrag(Driver *pdrive, int stage) {
+  if (!ctx_.phys.back_reaction) return TaskStatus::complete;
+  if (coupling_ == DustCoupling::pc2) {
+    if (stage != 1) return TaskStatus::complete;   // the predictor
+    return Check(dustb_pc2_predictor(&ctx_, pdrive->dt, 1, stream_), "DepositDrag");
+  }
+  return Check(dustb_deposit_qp(&ctx_, a_dt(pdrive), 0.0, stream_), "DepositDrag");
+}
+
+TaskStatus DustGasDrag::RecvDepQP(Driver *pdrive, int stage) {
+  if (!ctx_.phys.back_reaction) return TaskStatus::complete;
+  if (coupling_ == DustCoupling::pc2 && stage != 1) return TaskStatus::complete;
+  return Check(dustb_ghost_add(&ctx_, ctx_.f.qdep, 5, stream_), "RecvDepQP");
+}
+
+TaskStatus DustGasDrag::GasImplicitSolve(Driver *pdrive, int stage) {
+  if (coupling_ == DustCoupling::pc2) {
+    // the predictor's gas update with the stiffness record (UpdateStiffness, dust_pm.cpp:288-341)
+    if (stage != 1 || !ctx_.phys.back_reaction) return TaskStatus::complete;
+    return Check(dustb_pc2_apply_predictor(&ctx_, pdrive->dt, dev_scalars_ + 2, stream_),
+                 "GasImplicitSolve");
+  }
+  TaskStatus ts = Check(dustb_solve_ustar(&ctx_, stream_), "GasImplicitSolve");
+  if (ts != TaskStatus::complete || !ctx_.phys.back_reaction) return ts;
+  // SolveCoupledStage (dust_solver.cpp:630-724): dc1 / dc2 defect-correction sweeps
+  const int nsw = (ctx_.phys.drag_solver == DUSTB_SOLVER_DC2) ? 2
+                : (ctx_.phys.drag_solver == DUSTB_SOLVER_DC1) ? 1 : 0;
+  for (int w = 0; w < nsw && ts == TaskStatus::complete; ++w)
+    ts = Check(dustb_dc1_sweep(&ctx_, a_dt(pdrive), 0.0, stream_), "SolveCoupledStage");
+  return ts;
+}
+
+TaskStatus DustGasDrag::RecvUstar(Driver *pdrive, int stage) {
+  if (coupling_ == DustCoupling::pc2) return TaskStatus::complete;   // (the midpoint covers ghosts)
+  return Check(dustb_ghost_copy(&ctx_, ctx_.f.ustar, 3, 1, stream_), "RecvUstar");
+}
+
+TaskStatus DustGasDrag::GatherKickPMBR(Driver *pdrive, int stage) {
+  if (coupling_ == DustCoupling::pc2) return TaskStatus::complete;   // (inside the advance)
+  return Check(dustb_gather_kick_pmbr(&ctx_, a_dt(pdrive), 0.0, stream_), "GatherKickPMBR");
+}
+
+TaskStatus DustGasDrag::RecvPMBR(Driver *pdrive, int stage) {
+  if (!ctx_.phys.back_reaction) return TaskStatus::complete;
+  if (coupling_ == DustCoupling::pc2 && stage != 2) return TaskStatus::complete;
+  return Check(dustb_ghost_add(&ctx_, ctx_.f.dmom, 3, stream_), "RecvPMBR");
+}
+
+TaskStatus DustGasDrag::ApplyPMBR(Driver *pdrive, int stage) {
+  if (!ctx_.phys.back_reaction) return TaskStatus::complete;
+  if (coupling_ == DustCoupling::pc2) {
+    if (stage != 2) return TaskStatus::complete;
+    return Check(dustb_pc2_commit(&ctx_, 0.5, stream_), "ApplyPMBR");
+  }
+  return Check(dustb_apply_pmbr(&ctx_, a_dt(pdrive), stream_), "ApplyPMBR");
+}
+
+TaskStatus DustGasDrag::RecvU(Driver *pdrive, int stage) {
+  return Check(dustb_ghost_copy(&ctx_, ctx_.f.u0, ctx_.f.nvar_gas, 0, stream_), "RecvU");
+}
+
+TaskStatus DustGasDrag::NewTimeStep(Driver *pdrive, int stage) {
+  if (stage != pdrive->nexp_stages) return TaskStatus::complete;
+  return Check(dustb_newdt(&ctx_, 1.0, dev_scalars_ + 3, stream_), "NewTimeStep");
+}
+
+TaskStatus DustGasDrag::SortParticles(double *spare_pr, int *spare_pi, void *scratch,
+                                      long long bytes) {
+  TaskStatus ts = Check(dustb_sort_by_cell(&ctx_, spare_pr, spare_pi, scratch, bytes, stream_),
+                        "SortParticles");
+  if (ts != TaskStatus::complete) return ts;
+  // the sorted rows are the spares now (dust_cloud_device.cpp:1951-1954: swap)
+  ctx_.part.pr = spare_pr;
+  ctx_.part.pi = spare_pi;
+  return ts;
+}
+
+TaskStatus DustGasDrag::DoStage(Driver *pdrive, int stage) {
+  // dust_tasks.cpp:56-107 on one rank, in dependency order: the register copy (pc2: the
+  // midpoint), the gas update and the history term, the push and its migration, the deposit
+  // and its exchange, the solve, the u* exchange, the gather-kick, its exchange and the
+  // apply, the gas tail's exchange, the time step.  Each task is a no-op where the
+  // reference's is for this coupling and stage.
+  using Task = TaskStatus (DustGasDrag::*)(Driver *, int);
+  static const Task order[] = {
+      &DustGasDrag::FirstTwoImpRK,   &DustGasDrag::RKUpdate,       &DustGasDrag::AddDragHistoryGas,
+      &DustGasDrag::ExplicitPush,    &DustGasDrag::UpdateParticleGIDs,
+      &DustGasDrag::DepositDrag,     &DustGasDrag::RecvDepQP,      &DustGasDrag::GasImplicitSolve,
+      &DustGasDrag::RecvUstar,       &DustGasDrag::GatherKickPMBR, &DustGasDrag::RecvPMBR,
+      &DustGasDrag::ApplyPMBR,       &DustGasDrag::RecvU,          &DustGasDrag::NewTimeStep};
+  for (Task t : order) {
+    const TaskStatus ts = (this->*t)(pdrive, stage);
+    if (ts != TaskStatus::complete) return ts;
+  }
+  return TaskStatus::complete;
+}
+
+TaskStatus DustGasDrag::DoCycle(Driver *pdrive) {
+  for (int stage = 1; stage <= pdrive->nexp_stages; ++stage) {
+    TaskStatus ts = DoStage(pdrive, stage);
+    if (ts != TaskStatus::complete) return ts;
+  }
+  return TaskStatus::complete;
+}
+
+unsigned DustGasDrag::ErrorWord() {
+  unsigned e = 0;
+  cudaStreamSynchronize((cudaStream_t)stream_);
+  cudaMemcpy(&e, ctx_.err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  return e;
+}
+
+double DustGasDrag::NewDt() {
+  double v = 0.0;
+  cudaStreamSynchronize((cudaStream_t)stream_);
+  cudaMemcpy(&v, dev_scalars_ + 3, sizeof(double), cudaMemcpyDeviceToHost);
+  return v;
+}
+
+double DustGasDrag::ChiMax() {
+  double v = 0.0;
+  cudaStreamSynchronize((cudaStream_t)stream_);
+  cudaMemcpy(&v, dev_scalars_ + 2, sizeof(double), cudaMemcpyDeviceToHost);
+  return v;
+}
+
+void DustGasDrag::X3Removed(double out[2]) {
+  cudaStreamSynchronize((cudaStream_t)stream_);
+  cudaMemcpy(out, dev_scalars_, 2 * sizeof(double), cudaMemcpyDeviceToHost);
+}
+
+}  // namespace athenak_b200

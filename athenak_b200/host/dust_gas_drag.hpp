@@ -1,0 +1,96 @@
+// dust_gas_drag.hpp -- the host side of the drag step in the reference's own terms.
+//
+// A DustGasDrag whose task functions carry the names, arguments and stage logic of the
+// reference's (src/dust/dust_pm.cpp, dust_push.cpp, dust_solver.cpp, dust_newdt.cpp,
+// src/bvals/bvals_part.cpp, src/dust/dust_cloud_device.cpp) and forward one for one to the
+// C ABI of include/dustb.h on the pack's stream, plus the task list of one stage in the order
+// AssembleDustGasDragTasks builds it (src/dust/dust_tasks.cpp:38-120), for one rank: the
+// MPI send/receive pairs of the reference become the single-rank exchanges of the ABI, and
+// the hydro's flux update is the ABI's zero-flux stand-in.  A failing call returns
+// TaskStatus::fail with the library's message in LastError() (the reference aborts).
+#ifndef ATHENAK_B200_DUST_GAS_DRAG_HPP_
+#define ATHENAK_B200_DUST_GAS_DRAG_HPP_
+
+#include <string>
+
+#include "../../include/dustb.h"
+
+namespace athenak_b200 {
+
+// src/tasklist/task_list.hpp:32
+enum class TaskStatus { fail, complete, incomplete };
+
+// <dust>/coupling
+enum class DustCoupling { imex, pc2 };
+
+// The integrator state the drag tasks read: Driver::SetImEx2PlusCoefficients
+// (src/driver/driver.cpp:278-300) and the mesh's time and step.
+struct Driver {
+  double gamma = 0.0;
+  double gam0[3] = {0.0, 0.0, 0.0}, gam1[3] = {0.0, 0.0, 0.0}, beta[3] = {0.0, 0.0, 0.0};
+  double a_twid[4][4] = {};
+  double a_impl = 0.0;
+  int nexp_stages = 2;           // stage 3 of imex2+ is dormant for the drag (dust.cpp:1646)
+  double dt = 0.0, time = 0.0;   // Mesh::dt, Mesh::time
+  void SetImEx2PlusCoefficients(double gamma_new);
+};
+
+class DustGasDrag {
+ public:
+  // ctx: the pack's arrays (device pointers, the reference's layout); stream: the pack's
+  // (Kokkos default execution space) CUDA stream.  Allocates the few device scalars the
+  // tasks write (the x3 outflow tally, the pc2 stiffness record, the new time step).
+  DustGasDrag(const dustb_ctx &ctx, void *stream, DustCoupling coupling = DustCoupling::imex);
+  ~DustGasDrag();
+  DustGasDrag(const DustGasDrag &) = delete;
+  DustGasDrag &operator=(const DustGasDrag &) = delete;
+
+  dustb_ctx &Context() { return ctx_; }
+
+  // ---- tasks of a stage (dust_tasks.cpp:56-107)
+  TaskStatus FirstTwoImpRK(Driver *pdrive, int stage);     // dust_push.cpp:35-80
+  TaskStatus RKUpdate(Driver *pdrive, int stage);          // Hydro::RKUpdate, zero flux
+  TaskStatus AddDragHistoryGas(Driver *pdrive, int stage); // dust_pm.cpp:721-742
+  TaskStatus ExplicitPush(Driver *pdrive, int stage);      // dust_push.cpp:99-297
+  TaskStatus UpdateParticleGIDs(Driver *pdrive, int stage);// bvals_part.cpp:115-471
+  TaskStatus DepositDrag(Driver *pdrive, int stage);       // dust_pm.cpp:104-277
+  TaskStatus RecvDepQP(Driver *pdrive, int stage);         // bvals_dep.cpp:457-560
+  TaskStatus GasImplicitSolve(Driver *pdrive, int stage);  // dust_pm.cpp:372-442
+  TaskStatus RecvUstar(Driver *pdrive, int stage);         // the u* ghost copy (+ shear, x3)
+  TaskStatus GatherKickPMBR(Driver *pdrive, int stage);    // dust_pm.cpp:450-568
+  TaskStatus RecvPMBR(Driver *pdrive, int stage);          // the dmom deposit exchange
+  TaskStatus ApplyPMBR(Driver *pdrive, int stage);         // dust_pm.cpp:576-711
+  TaskStatus RecvU(Driver *pdrive, int stage);             // the hydro tail's u0 exchange
+  TaskStatus NewTimeStep(Driver *pdrive, int stage);       // dust_newdt.cpp:108-149
+
+  // SortParticles (dust_cloud_device.cpp:1881-1977): into the spare arrays, then swapped
+  // in; the spares (same shape as the rows) become the caller's to keep or free.
+  TaskStatus SortParticles(double *spare_pr, int *spare_pi, void *scratch, long long bytes);
+
+  // the stage's drag tasks in dependency order on one rank and one stream
+  TaskStatus DoStage(Driver *pdrive, int stage);
+  // one cycle: every working stage
+  TaskStatus DoCycle(Driver *pdrive);
+
+  // synchronises the stream and reads the device error word (nonzero: a particle the
+  // reference would have aborted on)
+  unsigned ErrorWord();
+  // synchronises and reads the last NewTimeStep result, the pc2 stiffness record chi_max and
+  // the x3 outflow tally (mass, count)
+  double NewDt();
+  double ChiMax();
+  void X3Removed(double out[2]);
+  const std::string &LastError() const { return last_error_; }
+
+ private:
+  TaskStatus Check(int rc, const char *task);
+  dustb_ctx ctx_;
+  void *stream_;
+  DustCoupling coupling_;
+  double *dev_scalars_ = nullptr;   // [0..1] x3 removed, [2] chi_max, [3] dt
+  std::string last_error_;
+};
+
+}  // namespace athenak_b200
+
+#endif  // ATHENAK_B200_DUST_GAS_DRAG_HPP_
