@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 namespace athenak_b200 {
 
 void Driver::SetImEx2PlusCoefficients(double gamma_new) {
@@ -211,6 +213,62 @@ double DustGasDrag::ChiMax() {
 void DustGasDrag::X3Removed(double out[2]) {
   cudaStreamSynchronize((cudaStream_t)stream_);
   cudaMemcpy(out, dev_scalars_, 2 * sizeof(double), cudaMemcpyDeviceToHost);
+}
+
+MixedDustGasDrag::MixedDustGasDrag(const dustb_ctx &ctx, void *stream, const double dx[3],
+                                   int rows_per_tile, int chunk)
+    : ctx_(ctx), stream_(stream) {
+  std::memset(&mp_, 0, sizeof(mp_));
+  for (int a = 0; a < 3; ++a) mp_.dx[a] = dx[a];
+  mp_.rows_per_tile = rows_per_tile;
+  mp_.chunk = chunk;
+  ws_bytes_ = dustb_mixed_workspace_bytes(&ctx_.mesh, ctx_.part.npart);
+  if (ws_bytes_ <= 0 || cudaMalloc(&ws_, (size_t)ws_bytes_) != cudaSuccess ||
+      cudaMalloc(&dev_scalars_, 3 * sizeof(double)) != cudaSuccess) {
+    last_error_ = "MixedDustGasDrag: workspace not allocated";
+    return;
+  }
+  cudaMemsetAsync(dev_scalars_, 0, 3 * sizeof(double), (cudaStream_t)stream_);
+  mp_.x3_removed = dev_scalars_;
+}
+
+MixedDustGasDrag::~MixedDustGasDrag() {
+  if (ws_) cudaFree(ws_);
+  if (dev_scalars_) cudaFree(dev_scalars_);
+}
+
+TaskStatus MixedDustGasDrag::Check(int rc, const char *what) {
+  if (rc == DUSTB_OK) return TaskStatus::complete;
+  last_error_ = std::string(what) + ": " + dustb_last_error() + " (" + std::to_string(rc) + ")";
+  return TaskStatus::fail;
+}
+
+TaskStatus MixedDustGasDrag::Import() {
+  return Check(dustb_mixed_import(&ctx_, &mp_, ws_, ws_bytes_, stream_), "mixed import");
+}
+
+TaskStatus MixedDustGasDrag::Export() {
+  return Check(dustb_mixed_export(&ctx_, &mp_, ws_, ws_bytes_, stream_), "mixed export");
+}
+
+TaskStatus MixedDustGasDrag::ImexCycle(const Driver &drv) {
+  dustb_imex_coeffs co;
+  co.gamma = drv.gamma; co.dt = drv.dt; co.sh[0] = co.sh[1] = 0.0;
+  ctx_.mesh.time = drv.time;
+  return Check(dustb_mixed_imex_cycle(&ctx_, &mp_, ws_, ws_bytes_, &co, stream_), "mixed imex cycle");
+}
+
+TaskStatus MixedDustGasDrag::Pc2Cycle(const Driver &drv) {
+  ctx_.mesh.time = drv.time;
+  return Check(dustb_mixed_pc2_cycle(&ctx_, &mp_, ws_, ws_bytes_, drv.dt, dev_scalars_ + 2, stream_),
+               "mixed pc2 cycle");
+}
+
+double MixedDustGasDrag::ChiMax() {
+  double v = 0.0;
+  cudaStreamSynchronize((cudaStream_t)stream_);
+  cudaMemcpy(&v, dev_scalars_ + 2, sizeof(double), cudaMemcpyDeviceToHost);
+  return v;
 }
 
 }  // namespace athenak_b200

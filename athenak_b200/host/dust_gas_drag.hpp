@@ -91,6 +91,38 @@ class DustGasDrag {
   std::string last_error_;
 };
 
+// The mixed-precision form from the host (dustb_mixed_*): a compact FP32 shadow of the
+// particles kept sorted by cell in a workspace this object allocates; Import after any change
+// of the particle set, cycles, Export before anything reads the particle rows (outputs,
+// restart, the FP64 task functions).  The mesh fields stay the pack's FP64 arrays.
+class MixedDustGasDrag {
+ public:
+  // dx: the uniform cell size; rows_per_tile, chunk: the tile shape (0: the library's)
+  MixedDustGasDrag(const dustb_ctx &ctx, void *stream, const double dx[3],
+                   int rows_per_tile = 0, int chunk = 0);
+  ~MixedDustGasDrag();
+  MixedDustGasDrag(const MixedDustGasDrag &) = delete;
+  MixedDustGasDrag &operator=(const MixedDustGasDrag &) = delete;
+
+  TaskStatus Import();
+  TaskStatus Export();
+  TaskStatus ImexCycle(const Driver &drv);   // imex2+ (no implicit shear shift)
+  TaskStatus Pc2Cycle(const Driver &drv);    // pc2
+  dustb_ctx &Context() { return ctx_; }
+  const std::string &LastError() const { return last_error_; }
+  double ChiMax();                           // synchronises
+
+ private:
+  TaskStatus Check(int rc, const char *what);
+  dustb_ctx ctx_;
+  void *stream_;
+  dustb_mixed_params mp_;
+  void *ws_ = nullptr;
+  long long ws_bytes_ = 0;
+  double *dev_scalars_ = nullptr;            // [0..1] x3 removed, [2] chi_max
+  std::string last_error_;
+};
+
 }  // namespace athenak_b200
 
 #endif  // ATHENAK_B200_DUST_GAS_DRAG_HPP_

@@ -4,7 +4,8 @@
 // infrastructure, oracle/dust_oracle.c) runs the same cycles on a host copy of the same
 // seeded inputs.  imex2+/dc2 and pc2 on a periodic 16^3 mesh of 8^3 MeshBlocks (a 3-D shearing
 // box: rotation, shear drift): positions within 1e-12 of the box, velocities within 1e-12 of
-// their scale, the gas momentum within 1e-11 of its scale, PGID identical, no error bit.
+// their scale, the gas momentum within 1e-11 of its scale, PGID identical, no error bit;
+// then the same cycles in the mixed-precision form (MixedDustGasDrag) at its tolerance.
 // Exit status 0 on agreement.
 #include <cuda_runtime.h>
 
@@ -19,6 +20,7 @@ extern "C" {
 unsigned oracle_imex_cycle(const dustb_ctx *c, double gamma, double dt, const double sh[2],
                            double *x3_removed);
 unsigned oracle_pc2_cycle(const dustb_ctx *c, double dt, double *chi_out, double *x3_removed);
+void oracle_ghost_copy(const dustb_ctx *c, double *a, int nvar, int x3_bcs);
 void oracle_set_threads(int n);
 }
 
@@ -85,7 +87,11 @@ dustb_ctx make_ctx(const Arrays &a, int npart) {
 
 const size_t NF[8] = {4, 4, 5, 3, 3, 4, 3};   // u0 u1 qdep ustar dmom resid work
 
-int run(athenak_b200::DustCoupling coupling, const char *name) {
+// mixed: the mixed-precision form (MixedDustGasDrag) against the oracle at the mixed form's
+// stated tolerance (velocities 1e-5 of their scale, positions 1e-5 of a cell, the gas
+// momentum 1e-5 of its scale); the gas ghost cells first take the copy exchange the mixed
+// form reads through the owning blocks
+int run(athenak_b200::DustCoupling coupling, const char *name, bool mixed = false) {
   const int ppc = 2, nsp = 2;
   const int npart = NMB * NX * NX * NX * ppc * nsp;
   std::vector<double> mb; std::vector<int> ng;
@@ -147,14 +153,32 @@ int run(athenak_b200::DustCoupling coupling, const char *name) {
   const double sh[2] = {0.0, 0.0};
   double x3o[2] = {0.0, 0.0}, chi = 0.0;
   unsigned oerr = 0;
+  const double cell[3] = {(HI - LO) / (NB * NX), (HI - LO) / (NB * NX), (HI - LO) / (NB * NX)};
+  athenak_b200::MixedDustGasDrag mx(dc, nullptr, cell);
+  if (mixed) {
+    dustb_ghost_copy(&dc, d.u0, 4, 0, nullptr);
+    oracle_ghost_copy(&hc, hf[0].data(), 4, 0);
+    if (mx.Import() != athenak_b200::TaskStatus::complete) {
+      std::printf("%s: %s\n", name, mx.LastError().c_str());
+      return 1;
+    }
+  }
   for (int cyc = 0; cyc < 3; ++cyc) {
-    if (drag.DoCycle(&drv) != athenak_b200::TaskStatus::complete) {
-      std::printf("%s: task failed: %s\n", name, drag.LastError().c_str());
+    athenak_b200::TaskStatus ts;
+    if (!mixed) ts = drag.DoCycle(&drv);
+    else if (coupling == athenak_b200::DustCoupling::imex) ts = mx.ImexCycle(drv);
+    else ts = mx.Pc2Cycle(drv);
+    if (ts != athenak_b200::TaskStatus::complete) {
+      std::printf("%s: task failed: %s%s\n", name, drag.LastError().c_str(), mx.LastError().c_str());
       return 1;
     }
     oerr |= (coupling == athenak_b200::DustCoupling::imex)
                 ? oracle_imex_cycle(&hc, drv.gamma, drv.dt, sh, x3o)
                 : oracle_pc2_cycle(&hc, drv.dt, &chi, x3o);
+  }
+  if (mixed && mx.Export() != athenak_b200::TaskStatus::complete) {
+    std::printf("%s: %s\n", name, mx.LastError().c_str());
+    return 1;
   }
   const unsigned gerr = drag.ErrorWord();
   std::vector<double> gpr(hpr.size()), gu0(hf[0].size());
@@ -175,8 +199,9 @@ int run(athenak_b200::DustCoupling coupling, const char *name) {
   }
   bool pgid = true;
   for (int p = 0; p < npart; ++p) pgid = pgid && gpi[p] == hpi[p];
-  const bool ok = gerr == 0 && oerr == 0 && pgid && dx <= 1e-12 * (HI - LO) && dv <= 1e-12 * vs &&
-                  du <= 1e-11 * us;
+  const double tp = mixed ? 1e-5 * cell[0] : 1e-12 * (HI - LO), tv = mixed ? 1e-5 : 1e-12;
+  const double tu = mixed ? 1e-5 : 1e-11;
+  const bool ok = gerr == 0 && oerr == 0 && pgid && dx <= tp && dv <= tv * vs && du <= tu * us;
   std::printf("%s: particles %d, max |dx| %.3e, max |dv| %.3e (scale %.3e), max |du0| %.3e "
               "(scale %.3e), PGID %s, error words %u/%u: %s\n",
               name, npart, dx, dv, vs, du, us, pgid ? "identical" : "DIFFER", gerr, oerr,
@@ -194,5 +219,7 @@ int main() {
   int bad = 0;
   bad += run(athenak_b200::DustCoupling::imex, "imex2+/dc2 cycles");
   bad += run(athenak_b200::DustCoupling::pc2, "pc2 cycles");
+  bad += run(athenak_b200::DustCoupling::imex, "mixed imex2+/dc2 cycles", true);
+  bad += run(athenak_b200::DustCoupling::pc2, "mixed pc2 cycles", true);
   return bad ? 1 : 0;
 }
