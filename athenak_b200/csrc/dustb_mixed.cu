@@ -399,6 +399,8 @@ struct PushArgs {
   float gy;                   // pc2 half step: q Omega h / dy (the gather position's y shift
                               // per unit x of the half-step position)
   float sdy;                  // pc2 half step: q Omega dt / dy (the new y's shear drift)
+  float shy;                  // imex: the stage's implicit shear shift sh / dy (the deposit and
+                              // gather weights sit at y + sh x), 0 outside the 3-D shearing box
   double a_dt;                // imex: a dt; pc2 half step: h = dt/2
   int stage2;
   int sbox, strat;
@@ -423,6 +425,16 @@ __device__ __forceinline__ void consistent_dv(const Geo &G, const PushArgs &P, f
   d[0] = __dmul_rn(cj, P.res[b]);
   d[1] = __dmul_rn(cj, P.res[b + G.vstride]);
   d[2] = __dmul_rn(cj, P.res[b + 2 * G.vstride]);
+}
+
+// the y offset of the implicit stage's weight position y + sh x (ImplicitShearShift,
+// src/dust/dust.hpp:1698-1702) in cells of the particle's own cell; explicitly rounded, so
+// that the push and the tiles form it bit for bit alike
+__device__ __forceinline__ float shifted_oy(const Geo &G, float shy, int m, int i, float ox,
+                                            float oy) {
+  const double *sz = G.mb + (long long)m * 9;
+  const double x = __dadd_rn(sz[X1MIN], __dmul_rn(__dadd_rn((double)i, (double)ox), G.dx[0]));
+  return __fadd_rn(oy, __fmul_rn(shy, __double2float_rn(x)));
 }
 
 // the new position in cell units, explicitly rounded so that count and move agree bit for
@@ -540,9 +552,9 @@ __device__ __forceinline__ Carry cross_face(const Geo &G, const PushArgs &P, int
 }
 
 template <int KIND, int SP>
-__device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, int &k, int &j,
-                                       int &i, float o[3], float d1[3], const float v[3],
-                                       int &flags, float hpos[2]) {
+__device__ __forceinline__ int advance_carry(const Geo &G, const PushArgs &P, int &m, int &k,
+                                             int &j, int &i, float o[3], float d1[3],
+                                             const float v[3], int &flags, float hpos[2]) {
   flags = 0;
   hpos[0] = hpos[1] = 0.0f;
   float xsh = 0.0f;
@@ -606,6 +618,21 @@ __device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, 
     for (int a = 0; a < 3; ++a) { o[a] = C.o[a]; d1[a] = C.d1[a]; }
   }
   return C.key;
+}
+
+// the push of advance_carry; an imex stage with an implicit shear shift sends a particle
+// whose shifted weight position lies in another cell to the edge bin (its true, new cell is
+// kept; per-particle kernels deposit and gather it)
+template <int KIND, int SP>
+__device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, int &k, int &j,
+                                       int &i, float o[3], float d1[3], const float v[3],
+                                       int &flags, float hpos[2]) {
+  const int key = advance_carry<KIND, SP>(G, P, m, k, j, i, o, d1, v, flags, hpos);
+  if (KIND == PK_IMEX && P.shy != 0.0f && !(flags & AF_EDGE)) {
+    const float oy = shifted_oy(G, P.shy, m, i, o[0], o[1]);
+    if (oy < 0.0f || oy >= 1.0f) { flags |= AF_EDGE; return G.ncell; }
+  }
+  return key;
 }
 
 // count: the new cell of every particle and the per-cell histogram
@@ -763,6 +790,7 @@ struct TileArgs {
   int dnvar;
   double *res;                 // MODE_QP: resid, the centre mass goes to var 3
   int deposit;                 // 0: kick or advance only (no back-reaction)
+  float shy;                   // imex: the stage's implicit shear shift sh / dy (0: none)
   Pc2Args pc;
   unsigned *err;
 };
@@ -1147,6 +1175,11 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
     }
     const int cj_l = (cl >= 0) ? cl / nx1 : 0, ci_l = (cl >= 0) ? cl - cj_l * nx1 : 0;
     const int jrow = j0 + cj_l;
+    // the y offset of the weights: the particle's own, or (an imex stage with an implicit
+    // shear shift) that of y + sh x, which the push kept inside the particle's cell
+    auto oy_at = [&](int r) -> float {
+      return (T.shy != 0.0f) ? shifted_oy(G, T.shy, m, ci_l, s_f[r], s_f[CH + r]) : s_f[CH + r];
+    };
     GatherWindow<D3> win;
     if (MODE != MODE_QP) win.template load<GH>(G, T.gfield, m, k, jrow, ci_l);   // while the copies fly
     const bool ok = mbar_wait(&bar, parity, T.err, wmask);
@@ -1163,7 +1196,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       for (int r = lo; r < hi; ++r) {
         float wx_[3], wy_[3], wz_[3];
         wts(SCHEME, s_f[r], wx_);
-        wts(SCHEME, s_f[CH + r], wy_);
+        wts(SCHEME, oy_at(r), wy_);
         if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
         const float mc = s_f[4 * CH + r] * s_f[3 * CH + r] * inv_vol;
         qt += mc;
@@ -1185,7 +1218,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       for (int r = lo; r < hi; ++r) {
         float wx_[3], wy_[3], wz_[3];
         wts(SCHEME, s_f[r], wx_);
-        wts(SCHEME, s_f[CH + r], wy_);
+        wts(SCHEME, oy_at(r), wy_);
         if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
         float2 uxy;
         float uz;
@@ -1268,7 +1301,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
         for (int r = lo; r < hi; ++r) {
           float wx_[3], wy_[3], wz_[3];
           wts(SCHEME, s_f[r], wx_);
-          wts(SCHEME, s_f[CH + r], wy_);
+          wts(SCHEME, oy_at(r), wy_);
           if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
           const float f = (MODE == MODE_KICK) ? -s_f[4 * CH + r] * inv_vol : 1.0f;
           sums.add(wx_, wy_, wz_, make_float2(f * s_f[5 * CH + r], f * s_f[6 * CH + r]),
@@ -1387,6 +1420,82 @@ __global__ void __launch_bounds__(kT) k_pc2_edge(PBuf S, Geo G, TileArgs T) {
   }
 }
 
+// The imex stage's edge bin under an implicit shear shift: particles whose weight position
+// y + sh x lies in a cell next to their own.  One thread per particle with the tiles' FP32
+// arithmetic at the shifted position and FP64 atomics: Q/P with the centre mass into the
+// particle's own cell (after the Q/P tiles stored theirs), the dc1 operator, the
+// gather-kick-deposit.  3-D.
+template <int MODE, int SCHEME, int GH>
+__global__ void __launch_bounds__(kT) k_shift_edge(PBuf S, Geo G, TileArgs T) {
+  const int e0 = T.cstart[G.ncell], e1 = T.cstart[G.ncell + 1];
+  const float inv_vol = (float)(1.0 / G.vol);
+  const float inv_adt = (float)(1.0 / T.a_dt);
+  for (int p = e0 + blockIdx.x * blockDim.x + threadIdx.x; p < e1; p += gridDim.x * blockDim.x) {
+    int m, k, j, i;
+    decode(G, S.cell[p], m, k, j, i);
+    const float ox = S.f[F_OX][p];
+    float oy = shifted_oy(G, T.shy, m, i, ox, S.f[F_OY][p]);
+    const float fl = floorf(oy);
+    const int jc = j + (int)fl;                   // the cell of the shifted position
+    oy = __fsub_rn(oy, fl);
+    if (oy >= 1.0f) oy = 0.99999994f;
+    float wx[3], wy[3], wz[3];
+    wts(SCHEME, ox, wx); wts(SCHEME, oy, wy); wts(SCHEME, S.f[F_OZ][p], wz);
+    const float cc = S.f[F_CC][p], mass = S.f[F_M][p];
+    const float mc = mass * cc * inv_vol;
+    if (MODE == MODE_QP) {
+      const float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
+      for (int c = 0; c < 3; ++c)
+        for (int b = 0; b < 3; ++b)
+          for (int a = 0; a < 3; ++a) {
+            const float w = wz[c] * wy[b] * wx[a] * mc;
+            if (w == 0.0f) continue;
+            const long long at = cell_at<GH>(G, m, T.dnvar, k - 1 + c, jc - 1 + b, i - 1 + a);
+            if (at < 0) continue;
+            atomicAdd(&T.dfield[at], (double)w);
+            atomicAdd(&T.dfield[at + G.vstride], (double)(w * v[0]));
+            atomicAdd(&T.dfield[at + 2 * G.vstride], (double)(w * v[1]));
+            atomicAdd(&T.dfield[at + 3 * G.vstride], (double)(w * v[2]));
+          }
+      atomicAdd(&T.res[G.at(m, 4, 3, G.ks + k, G.js + j, G.is + i)], (double)mc);
+      continue;
+    }
+    float u[3] = {0.0f, 0.0f, 0.0f};
+    for (int c = 0; c < 3; ++c)
+      for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) {
+          const float w = wz[c] * wy[b] * wx[a];
+          const long long at = cell_at<GH>(G, m, 3, k - 1 + c, jc - 1 + b, i - 1 + a);
+          if (at < 0) continue;
+          u[0] += w * (float)T.gfield[at];
+          u[1] += w * (float)T.gfield[at + G.vstride];
+          u[2] += w * (float)T.gfield[at + 2 * G.vstride];
+        }
+    float val[3];
+    if (MODE == MODE_OP) {
+      for (int q = 0; q < 3; ++q) val[q] = mc * u[q];
+    } else {
+      // GatherKickPMBR (src/dust/dust_pm.cpp:534-563): the applied velocity change
+      const float v0[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
+      for (int q = 0; q < 3; ++q) val[q] = (v0[q] + cc * (u[q] - v0[q])) - v0[q];
+      S.f[F_VX][p] = v0[0] + val[0]; S.f[F_VY][p] = v0[1] + val[1]; S.f[F_VZ][p] = v0[2] + val[2];
+      S.f[F_RX][p] = val[0] * inv_adt; S.f[F_RY][p] = val[1] * inv_adt; S.f[F_RZ][p] = val[2] * inv_adt;
+      if (!T.deposit) continue;
+      const float f = -mass * inv_vol;
+      for (int q = 0; q < 3; ++q) val[q] *= f;
+    }
+    for (int c = 0; c < 3; ++c)
+      for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) {
+          const float w = wz[c] * wy[b] * wx[a];
+          if (w == 0.0f) continue;
+          const long long at = cell_at<GH>(G, m, 3, k - 1 + c, jc - 1 + b, i - 1 + a);
+          if (at < 0) continue;
+          for (int q = 0; q < 3; ++q) atomicAdd(&T.dfield[at + q * G.vstride], (double)(w * val[q]));
+        }
+  }
+}
+
 // ---- kernel timing ------------------------------------------------------------------------
 struct Timing {
   bool on = false;
@@ -1480,6 +1589,21 @@ int launch_tile(const MState &S, const PBuf &cur, const Geo &G, const Cfg &cf, T
   if (G.scheme == 2) return launch_tile_d<MODE, 0, 2, 0>(G, cf, cur, T, st);
   if (G.scheme == 1) return launch_tile_d<MODE, 0, 1, 0>(G, cf, cur, T, st);
   return launch_tile_d<MODE, 0, 0, 0>(G, cf, cur, T, st);
+}
+
+// the edge bin of an imex stage with an implicit shear shift (after the mode's tiles)
+template <int MODE>
+int launch_shift_edge(const MState &S, const PBuf &cur, const Geo &G, TileArgs T, cudaStream_t st) {
+  T.cstart = S.cstart;
+  const unsigned nb = 148 * 4;
+#define DUSTB_SE(SC, GHF) k_shift_edge<MODE, SC, GHF><<<nb, kT, 0, st>>>(cur, G, T)
+  if (G.ghost) {
+    if (G.scheme == 2) DUSTB_SE(2, 1); else if (G.scheme == 1) DUSTB_SE(1, 1); else DUSTB_SE(0, 1);
+  } else {
+    if (G.scheme == 2) DUSTB_SE(2, 0); else if (G.scheme == 1) DUSTB_SE(1, 0); else DUSTB_SE(0, 0);
+  }
+#undef DUSTB_SE
+  return dustb_host::launch_status("mixed shear-shift edge");
 }
 
 // sort copy src into dst by the cells it holds (histogram, scan, moves)
@@ -1661,8 +1785,9 @@ int dustb_mixed_kernel_times(double *ms, int *launches, int n) {
 int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void *ws,
                            long long bytes, const dustb_imex_coeffs *co, void *stream) {
   if (!params_ok(c, mp) || !co || !(co->dt > 0.0)) return DUSTB_EINVAL;
-  if (co->sh[0] != 0.0 || co->sh[1] != 0.0) return DUSTB_EUNSUP;   // shear shift: FP64 form
   if (!c->mesh.multi_d) return DUSTB_EUNSUP;                        // 1-D: FP64 form
+  // (the implicit shear shift is the 3-D shearing box's: 2-D meshes take the FP64 form)
+  if ((co->sh[0] != 0.0 || co->sh[1] != 0.0) && !c->mesh.three_d) return DUSTB_EUNSUP;
   const Geo G = make_geo(c, mp);
   if (!geo_ok(mp, G)) return DUSTB_EINVAL;
   MState S;
@@ -1700,6 +1825,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     P.bdt = (float)(beta[stage - 1] * dt);
     for (int a = 0; a < 3; ++a) P.bdx[a] = (float)(beta[stage - 1] * dt * G.inv_dx[a]);
     P.gy = 0.0f;
+    P.shy = (float)(co->sh[stage - 1] * G.inv_dx[1]);
     P.a_dt = a_dt; P.stage2 = (stage == 2);
     P.sbox = c->phys.shearing_box; P.strat = c->phys.stratified;
     P.q = (float)c->phys.qshear; P.om = (float)c->phys.omega0;
@@ -1713,13 +1839,15 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     RUN(push_sort(S, src, cur, G, n, ncell, P, st));
     if (stage == 1) cudaMemsetAsync(&S.head->pending, 0, sizeof(int), st);   // applied
     TileArgs T{};
-    T.a_dt = a_dt; T.err = c->err; T.deposit = 1;
+    T.a_dt = a_dt; T.err = c->err; T.deposit = 1; T.shy = P.shy;
+    const bool shift = P.shy != 0.0f;
     if (br) {
       {
         Scope sc(DUSTB_K_DEPOSIT_QP, st);
         cudaMemsetAsync(c->f.qdep, 0, fbytes * 5, st);
         T.dfield = c->f.qdep; T.dnvar = 5; T.res = c->f.resid;
         RUN(launch_tile<MODE_QP>(S, cur, G, cf, T, st));
+        if (shift) RUN(launch_shift_edge<MODE_QP>(S, cur, G, T, st));
       }
       Scope sc(DUSTB_K_CELLS, st);
       RUN(ghost_add_if(c, G, c->f.qdep, 5, st));
@@ -1738,7 +1866,8 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
         cudaMemsetAsync(c->f.work, 0, fbytes * 3, st);
         { Scope sc(DUSTB_K_OPERATOR, st);
           T.gfield = c->f.ustar; T.dfield = c->f.work; T.dnvar = 3;
-          RUN(launch_tile<MODE_OP>(S, cur, G, cf, T, st)); }
+          RUN(launch_tile<MODE_OP>(S, cur, G, cf, T, st));
+          if (shift) RUN(launch_shift_edge<MODE_OP>(S, cur, G, T, st)); }
         { Scope sc(DUSTB_K_CELLS, st);
           RUN(ghost_add_if(c, G, c->f.work, 3, st));
           dustb_cells::dc_correct(c, st); }
@@ -1753,6 +1882,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       Scope sc(DUSTB_K_KICK, st);
       T.gfield = c->f.ustar; T.dfield = c->f.dmom; T.dnvar = 3; T.deposit = br;
       RUN(launch_tile<MODE_KICK>(S, cur, G, cf, T, st));
+      if (shift) RUN(launch_shift_edge<MODE_KICK>(S, cur, G, T, st));
     }
     if (br) {
       Scope sc(DUSTB_K_CELLS, st);

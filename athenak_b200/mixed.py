@@ -90,10 +90,12 @@ class MixedDust:
         capi.check(self.lib.dustb_mixed_sort(self.dev.pctx, C.byref(self.mp), p, n,
                                              _stream_ptr(stream)), "mixed_sort")
 
-    def imex_cycle(self, dt, gamma=GAMMA_DEFAULT, stream=None):
+    def imex_cycle(self, dt, gamma=GAMMA_DEFAULT, sh=(0.0, 0.0), stream=None):
+        """One imex2+ cycle; sh: the implicit shear shift of stages 1 and 2 (3-D shearing
+        box: the deposit and gather weights sit at y + sh x)."""
         co = capi.DustbImexCoeffs()
         co.gamma, co.dt = gamma, dt
-        co.sh[0] = co.sh[1] = 0.0
+        co.sh[0], co.sh[1] = sh
         p, n = self._ws()
         capi.check(self.lib.dustb_mixed_imex_cycle(self.dev.pctx, C.byref(self.mp), p, n,
                                                    C.byref(co), _stream_ptr(stream)),

@@ -332,8 +332,10 @@ int dustb_mixed_export(const dustb_ctx *ctx, const dustb_mixed_params *mp, void 
  * physical x3 faces or shear-periodic x1 faces they use each block's own ghost cells and the
  * FP64 ghost exchanges (dustb_ghost_add / dustb_ghost_copy: x3 fold or drop, shear remaps)
  * run around them.  The push routes particles as dustb_route does (x3 reflect / outflow,
- * shear-periodic crossings).  A 3-D shearing box needs c->sh = 0 here (DUSTB_EUNSUP
- * otherwise; the FP64 form takes any shift). */
+ * shear-periodic crossings).  With an implicit shear shift (c->sh, 3-D shearing box) the
+ * tiles place the weights at y + sh x; particles whose shifted position lies in the next
+ * cell are sorted into an edge bin that per-particle kernels deposit and gather (2-D meshes
+ * with sh != 0: DUSTB_EUNSUP, the FP64 form). */
 int dustb_mixed_imex_cycle(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
                            long long ws_bytes, const dustb_imex_coeffs *c, void *stream);
 
