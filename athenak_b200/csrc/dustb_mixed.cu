@@ -265,13 +265,23 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned b
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
-// bounded wait for the barrier's phase; false (and the error bit) if it never completes.
-// Warp-uniform: the lanes of mask leave the loop together, so the warp is converged at the
-// CTA barrier that follows (a CTA barrier assumes converged warps)
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait for the barrier's phase: at most 2^22 polls and 0.2 s (a copy of a pass takes
+// microseconds); false (and the error bit) if it never completes.  Warp-uniform: the lanes of
+// mask leave the loop together, so the warp is converged at the CTA barrier that follows (a
+// CTA barrier assumes converged warps)
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned *err,
                                           unsigned mask) {
-  for (int it = 0; it < (1 << 22); ++it)
+  const unsigned long long t0 = global_ns();
+  for (int it = 0; it < (1 << 22); ++it) {
     if (__all_sync(mask, mbar_try_wait(bar, parity))) return true;
+    if (__any_sync(mask, global_ns() - t0 > 200000000ull)) break;
+  }
   report(err, DUSTB_ERR_TIMEOUT);
   return false;
 }
@@ -791,6 +801,7 @@ struct TileArgs {
   double *res;                 // MODE_QP: resid, the centre mass goes to var 3
   int deposit;                 // 0: kick or advance only (no back-reaction)
   float shy;                   // imex: the stage's implicit shear shift sh / dy (0: none)
+  int probe_timeout;           // test hook: tile 0 never issues its first copy
   Pc2Args pc;
   unsigned *err;
 };
@@ -1109,7 +1120,8 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
     // the first pass's copies go out before the cell ranges are read
     mbar_init(&bar, 1);
     const int p0 = T.cstart[c0], p1 = T.cstart[c0 + nct];
-    if (p1 > p0) issue_pass(p0, min(p1, p0 + (CH - 8)));
+    // (the failure-detection hook: tile 0's first copy is never issued, its wait runs out)
+    if (p1 > p0 && !(T.probe_timeout && blockIdx.x == 0)) issue_pass(p0, min(p1, p0 + (CH - 8)));
   }
   __syncwarp(wmask);
   for (int x = tid; x <= nct; x += blockDim.x) s_cs[x] = T.cstart[c0 + x];
@@ -1523,6 +1535,7 @@ struct Scope {
 
 struct Cfg {
   int tj, chunk, tpp;
+  int probe_timeout;
 };
 
 // the default particles per pass: the largest multiple of 4 that lets as many CTAs share an
@@ -1540,7 +1553,8 @@ int default_chunk(int tj, int nx1) {
 
 bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   const int nx1 = ms.nx1, nx2 = ms.multi_d ? ms.nx2 : 1;
-  if (mp->variant != 0 || nx1 > kMaxTileThreads) return false;
+  if ((mp->variant != 0 && mp->variant != DUSTB_MIXED_PROBE_COPY_TIMEOUT) || nx1 > kMaxTileThreads)
+    return false;
   int tj = mp->rows_per_tile;
   if (tj <= 0) {
     tj = 1;
@@ -1552,6 +1566,7 @@ bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   cf.chunk = mp->chunk > 0 ? mp->chunk : default_chunk(tj, nx1);
   if (cf.chunk < 64 || cf.chunk > 8192 || (cf.chunk & 3)) return false;
   cf.tpp = nx2 / tj;
+  cf.probe_timeout = (mp->variant == DUSTB_MIXED_PROBE_COPY_TIMEOUT);
   // every tile form must fit the 227 KiB of shared memory a CTA can have (less the barrier)
   if (tile_smem(ms.three_d, tj, nx1, cf.chunk) > 227 * 1024 - 256) return false;
   return true;
@@ -1574,6 +1589,7 @@ template <int MODE>
 int launch_tile(const MState &S, const PBuf &cur, const Geo &G, const Cfg &cf, TileArgs T,
                 cudaStream_t st) {
   T.tj = cf.tj; T.chunk = cf.chunk; T.tpp = cf.tpp; T.cstart = S.cstart;
+  T.probe_timeout = cf.probe_timeout;
   // one kernel per dimensionality and deposit scheme (no per-particle scheme selection)
   if (G.three_d) {
     // (ghost mode: physical x3 or shear-periodic x1 faces, 3-D only)

@@ -300,6 +300,8 @@ int dustb_phst(const dustb_ctx *ctx, const double *chi_max, double *row, void *s
  * (dustb_mixed_workspace_bytes).
  * No reference counterpart: the reference keeps only the FP64 SoA. */
 
+enum { DUSTB_MIXED_PROBE_COPY_TIMEOUT = 7 };
+
 typedef struct dustb_mixed_params {
   double dx[3];            /* uniform cell size (single-level mesh) */
   int rows_per_tile;       /* 0: chosen by the library; else rows of nx1 cells per CTA tile */
@@ -307,7 +309,10 @@ typedef struct dustb_mixed_params {
                               pass), a multiple of 4 in 64..8192; 0: the largest that keeps
                               as many CTAs per SM as their registers allow (2380 for tiles
                               of 128 cells) */
-  int variant;             /* deposit kernels: 0 (the only one) */
+  int variant;             /* 0; DUSTB_MIXED_PROBE_COPY_TIMEOUT: a failure-detection test
+                              hook (the first tile of every deposit launch never issues its
+                              first copy: its bounded wait runs out, the tile returns and
+                              sets DUSTB_ERR_TIMEOUT) */
   double *x3_removed;      /* device (mass, count) of the particles removed at outflow x3
                               faces, accumulated; required when mesh.x3bc is
                               DUSTB_X3_OUTFLOW, else may be NULL */

@@ -367,3 +367,23 @@ def test_mixed_imex_shear_shift_matches_fp64(mesh):
     mx.export()
     torch.cuda.synchronize()
     check(st, ref, mx, None)
+
+
+def test_copy_wait_timeout_is_reported_and_recoverable():
+    """Failure detection without a fault: the test hook makes the first tile of every deposit
+    launch skip its first bulk copy, so that tile's bounded wait runs out.  The kernels
+    return, the error word carries DUSTB_ERR_TIMEOUT, and the context stays usable: a
+    fresh shadow on the same device runs a clean cycle afterwards."""
+    from athenak_b200.mixed import MixedDust
+    ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3)
+    st = make_state(ms, [0.1], [1.0], 2, seed=2)
+    phys = dict(scheme=2, drag_solver=1)
+    probe = MixedDust(st, phys, variant=7)      # DUSTB_MIXED_PROBE_COPY_TIMEOUT
+    probe.imex_cycle(2e-3)
+    torch.cuda.synchronize()
+    assert probe.error_word() & 0x40             # DUSTB_ERR_TIMEOUT
+    clean = MixedDust(st, phys)
+    clean.imex_cycle(2e-3)
+    clean.export()
+    torch.cuda.synchronize()
+    assert clean.error_word() == 0
