@@ -35,6 +35,14 @@ CASES = {
                           st=dict(taus=[0.001, 1.0], eps=[2.0, 0.3], ppc=3, seed=9,
                                   vel_noise=0.02, gas_noise=1e-2),
                           phys=dict(scheme=1, drag_solver=3, consistent_gas=False), dt=2e-3),
+    "ngp_local": dict(mesh=((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3),
+                      st=dict(taus=[0.01, 0.3], eps=[1.0, 0.5], ppc=2, seed=12,
+                              vel_noise=0.03, gas_noise=1e-2),
+                      phys=dict(scheme=0, drag_solver=0), dt=2e-3),
+    "no_back_reaction": dict(mesh=((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3),
+                             st=dict(taus=[0.01, 0.3], eps=[1.0, 0.5], ppc=2, seed=13,
+                                     vel_noise=0.03, gas_noise=1e-2),
+                             phys=dict(scheme=2, drag_solver=2, back_reaction=False), dt=2e-3),
 }
 
 
