@@ -312,7 +312,7 @@ __device__ double shear_add_sum(const SBox &B, const Ind &d, const double *a, in
         const int S = B.block(sface, sb3, sb2);
         if (S < 0) continue;
         for (long long Yc = F - 1; Yc <= F + 1; ++Yc)
-          for (int q = -1; q <= 1; ++q) {
+          for (int q = -2; q <= 2; ++q) {
             const long long Y = Yc + q * N2;
             const long long sj = Y - (long long)sb2 * B.nx2 + d.js;
             if (sj < 0 || sj >= d.n2) continue;

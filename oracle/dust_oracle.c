@@ -497,7 +497,7 @@ static double shear_add_sum(const dustb_ctx *c, const Ind *d, const double *a, i
         const int S = sb_block(ms, sface, sb3, sb2);
         if (S < 0) continue;
         for (long long Yc = F - 1; Yc <= F + 1; ++Yc)
-          for (int q = -1; q <= 1; ++q) {
+          for (int q = -2; q <= 2; ++q) {
             /* the source row Yc + q N2 of S's strip (its ghost rows included) */
             const long long Y = Yc + q*N2;
             const long long sj = Y - (long long)sb2*ms->nx2 + d->js;
@@ -972,6 +972,33 @@ void oracle_sort_particles(const dustb_ctx *c, double *spare_pr, int *spare_pi) 
     for (int r = 0; r < DUSTB_NINT; ++r) spare_pi[(size_t)r*stride + k] = PI(r, p);
   }
   free(order);
+}
+
+/* ---- the cloud order index, DustGasDrag::UpdateCloudOrder, src/dust/dust_cloud_device.cpp:
+ * 1992-2055: the keys of SortParticles sorted, the particle of each slot and its 64-bit tag
+ * (TagFromWords, src/athena.hpp:85-88) ------------------------------------------------- */
+static uint64_t tag_words(int lo, int hi) {
+  return ((uint64_t)(uint32_t)hi << 32) | (uint64_t)(uint32_t)lo;
+}
+
+void oracle_cloud_order(const dustb_ctx *c, int *ord, uint64_t *tag) {
+  const int *pi = c->part.pi; long long stride = c->part.stride;
+  oracle_sort_order(c, ord, NULL);
+  for (int k = 0; k < c->part.npart; ++k)
+    tag[k] = tag_words(PI(DUSTB_PTAG, ord[k]), PI(DUSTB_PTAGH, ord[k]));
+}
+
+/* the check between rebuilds (:2001-2010): entries whose slot is out of range or holds
+ * another tag */
+int oracle_cloud_order_check(const dustb_ctx *c, const int *ord, const uint64_t *tag, int n) {
+  const int *pi = c->part.pi; long long stride = c->part.stride;
+  int bad = 0;
+  for (int k = 0; k < n; ++k) {
+    const int p = ord[k];
+    if (p < 0 || p >= c->part.npart ||
+        tag_words(PI(DUSTB_PTAG, p), PI(DUSTB_PTAGH, p)) != tag[k]) ++bad;
+  }
+  return bad;
 }
 
 /* ---- pc2 ------------------------------------------------------------------------------ */

@@ -168,6 +168,40 @@ def test_sort_bit_exact_and_cell_index():
     compare_particles(o, g, exact=True)
 
 
+@pytest.mark.parametrize("dims", ["3d", "2d"])
+def test_cloud_order_index_bit_exact(dims):
+    """UpdateCloudOrder's index and tags against the oracle (bit-exact), its check before and
+    after the rows are reordered, and the identity index a sort leaves."""
+    from athenak_b200.drag import DeviceDust
+    if dims == "3d":
+        ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3)
+    else:
+        ms = uniform_mesh((32, 32, 1), (16, 16, 1), 2, (-0.5,) * 3, (0.5,) * 3)
+    st = make_state(ms, [0.01, 0.1], [1.0, 0.5], 3, seed=23, vel_noise=0.05)
+    n = st.npart
+    st.pi[1, :n:3] = -1 - np.arange(len(st.pi[1, :n:3]), dtype=np.int32)
+    st.pi[4, :n:5] = 11
+    o, g = Oracle(st, {}), DeviceDust(st, {})
+    ord_o, tag_o = o.cloud_order()
+    ord_g, tag_g = g.cloud_order()
+    np.testing.assert_array_equal(ord_g.cpu().numpy(), ord_o)
+    np.testing.assert_array_equal(tag_g.cpu().numpy().view(np.uint64), tag_o)
+    assert g.cloud_order_check(ord_g, tag_g) == 0
+    g.sort_by_cell()
+    o.sort_particles()
+    moved = o.cloud_order_check(ord_o, tag_o)
+    assert moved > 0 and g.cloud_order_check(ord_g, tag_g) == moved
+    ord_i, tag_i = g.cloud_order_identity()
+    np.testing.assert_array_equal(ord_i.cpu().numpy(), np.arange(n))
+    np.testing.assert_array_equal(tag_i.cpu().numpy().view(np.uint64), tag_o)
+    assert g.cloud_order_check(ord_i, tag_i) == 0
+    ord_r, tag_r = g.cloud_order()       # a rebuild on sorted rows is the identity
+    np.testing.assert_array_equal(ord_r.cpu().numpy(), np.arange(n))
+    bad = ord_i.clone()
+    bad[:2] = torch.tensor([-1, n], dtype=torch.int32)
+    assert g.cloud_order_check(bad, tag_i) == 2
+
+
 def test_newdt_and_tstop_exact():
     o, g, c = build("sbox_nsh")
     dt_o = o.newdt() * 0.3
@@ -248,7 +282,7 @@ def test_shear_ghost_ops_bit_exact():
     phys = dict(scheme=2, shearing_box=True)
     from athenak_b200.drag import DeviceDust
     o, g = Oracle(st, phys), DeviceDust(st, phys)
-    for t in (0.0, 0.37, 5.3):
+    for t in (0.0, 0.37, 5.3, 1.32):
         o.set_time(t)
         g.set_time(t)
         rng = np.random.default_rng(int(t * 100) + 1)

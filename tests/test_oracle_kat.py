@@ -224,6 +224,37 @@ def test_sort_order_is_lexicographic():
     np.testing.assert_array_equal(o.st.pi[1, :n], st.pi[1, order])
 
 
+def test_cloud_order_index_tags_and_check():
+    """UpdateCloudOrder (src/dust/dust_cloud_device.cpp:1992-2055): the index is the sort's
+    permutation, each slot's tag is TagFromWords(PTAG, PTAGH) (src/athena.hpp:85-88, the words
+    as unsigned 32-bit), and the check counts the slots whose particle changed."""
+    ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2)
+    st = make_state(ms, [0.1, 1.0], [0.5, 0.5], 2, seed=7)
+    n = st.npart
+    # tags beyond 2^31: negative low words and nonzero high words
+    st.pi[1, :n:3] = -1 - np.arange(len(st.pi[1, :n:3]), dtype=np.int32)
+    st.pi[4, :n:5] = 7
+    st.pi[4, 1:n:7] = -2
+    o = Oracle(st, dict())
+    ord_, tag = o.cloud_order()
+    order, _ = o.sort_order()
+    np.testing.assert_array_equal(ord_, order)
+    lo = st.pi[1, :n].astype(np.int64) & 0xFFFFFFFF
+    hi = st.pi[4, :n].astype(np.int64) & 0xFFFFFFFF
+    want = (hi.astype(np.uint64) << np.uint64(32)) | lo.astype(np.uint64)
+    np.testing.assert_array_equal(tag, want[order])
+    assert o.cloud_order_check(ord_, tag) == 0
+    # reordered rows: every slot whose particle moved fails; out-of-range slots fail
+    o.sort_particles()
+    moved = int((order != np.arange(n)).sum())
+    assert moved > 0 and o.cloud_order_check(ord_, tag) == moved
+    # the identity index of the sorted rows carries the same tags (the sort's identity)
+    ident = np.arange(n, dtype=np.int32)
+    assert o.cloud_order_check(ident, tag) == 0
+    ident[:3] = [-1, n, n + 5]
+    assert o.cloud_order_check(ident, tag) == 3
+
+
 def test_route_keeps_particles_in_their_blocks():
     ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3)
     st = make_state(ms, [0.1], [1.0], 2, seed=11, vel_noise=0.5)
@@ -301,15 +332,18 @@ def test_shear_remap_of_ghost_strips_shifts_the_profile():
         assert np.abs(got - want).max() < 2e-2
 
 
+@pytest.mark.parametrize("t", [0.73, 1.32])
 @pytest.mark.parametrize("x3bc", [0, 1])
-def test_shear_deposit_remap_conserves(x3bc):
+def test_shear_deposit_remap_conserves(x3bc, t):
     """The ghost deposits beyond the shear-periodic x1 faces are moved to the other face and
     shifted by the particles' shear offset (piecewise-constant overlaps): the total deposit
-    is kept exactly."""
+    is kept exactly.  t = 1.32 puts the offset 31.68 of 32 cells, within the ghost width of
+    a full period, where the sources of a target cell include the ghost rows of the block
+    column on the far side of the periodic x2 wrap."""
     ms = shear_mesh(x3bc)
     st = make_state(ms, [0.1, 0.01], [1.0, 0.5], 2, seed=11)
     o = Oracle(st, dict(scheme=2, shearing_box=True))
-    o.set_time(0.73)
+    o.set_time(t)
     a_dt = 1e-3
     o.deposit_qp(a_dt)
     o.ghost_add("qdep", 5)
