@@ -164,6 +164,9 @@ SIGNATURES = {
     "dustb_cell_index_static": [CTXP, VP, VP, VP],
     "dustb_phst_scratch_bytes": [MESHP, I],
     "dustb_phst": [CTXP, VP, VP, VP, LL, VP],
+    "dustb_cloud_order": [CTXP, VP, VP, VP, LL, VP],
+    "dustb_cloud_order_identity": [CTXP, VP, VP, VP],
+    "dustb_cloud_order_check": [CTXP, VP, VP, I, VP, VP],
 }
 RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_phst_scratch_bytes": LL,
             "dustb_last_error": C.c_char_p}

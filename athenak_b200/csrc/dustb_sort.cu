@@ -285,6 +285,88 @@ int dustb_sort_by_cell(const dustb_ctx *c, double *spare_pr, int *spare_pi, void
 
 }  // extern "C"
 
+// ---- the cloud order index (DustGasDrag::UpdateCloudOrder) -------------------------------
+namespace {
+
+// the 64-bit tag of particle p: PTAG the low word, PTAGH the high (two's complement words)
+__device__ __forceinline__ unsigned long long tag_of(const int *pi, long long stride, int p) {
+  const unsigned lo = (unsigned)pi[(long long)DUSTB_PTAG * stride + p];
+  const unsigned hi = (unsigned)pi[(long long)DUSTB_PTAGH * stride + p];
+  return ((unsigned long long)hi << 32) | (unsigned long long)lo;
+}
+
+// the tag of the particle each slot k indexes: ord given (the key order), or written as the
+// identity (identity = 1: after a sort in cell order)
+__global__ void k_order_tags(const int *pi, long long stride, int n, int *ord, int identity,
+                             unsigned long long *tag) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int p = k;
+  if (identity) ord[k] = k;
+  else p = ord[k];
+  tag[k] = tag_of(pi, stride, p);
+}
+
+// entries k < n whose slot is out of range or holds another particle than when indexed
+__global__ void k_order_check(const int *pi, long long stride, int npart, const int *ord,
+                              const unsigned long long *tag, int n, int *bad) {
+  int cnt = 0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int p = ord[k];
+    if (p < 0 || p >= npart || tag_of(pi, stride, p) != tag[k]) ++cnt;
+  }
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(bad, cnt);
+}
+
+}  // namespace
+
+extern "C" {
+
+int dustb_cloud_order(const dustb_ctx *c, int *ord, unsigned long long *tag, void *scratch,
+                      long long scratch_bytes, void *stream) {
+  if (!c || !ord || !tag || !scratch) return DUSTB_EINVAL;
+  const dustb_mesh &ms = c->mesh;
+  const int n = c->part.npart;
+  if (scratch_bytes < dustb_sort_scratch_bytes(&ms, n)) return DUSTB_ESCRATCH;
+  const long long ncell = (long long)ms.nmb * ms.nx1 * (ms.multi_d ? ms.nx2 : 1) *
+                          (ms.three_d ? ms.nx3 : 1);
+  const long long base = csr_scratch_bytes(ncell, n);
+  // the per-cell starts are not returned: they sit behind the key scratch
+  int *cstart = (int *)((char *)scratch + base);
+  int rc = dustb_cell_index(c, ord, cstart, scratch, base, stream);
+  if (rc) return rc;
+  if (n > 0)
+    k_order_tags<<<nblk(n), kT, 0, (cudaStream_t)stream>>>(c->part.pi, c->part.stride, n, ord, 0,
+                                                             tag);
+  return dustb_host::launch_status("cloud_order");
+}
+
+int dustb_cloud_order_identity(const dustb_ctx *c, int *ord, unsigned long long *tag,
+                               void *stream) {
+  if (!c || !ord || !tag) return DUSTB_EINVAL;
+  const int n = c->part.npart;
+  if (n > 0)
+    k_order_tags<<<nblk(n), kT, 0, (cudaStream_t)stream>>>(c->part.pi, c->part.stride, n, ord, 1,
+                                                             tag);
+  return dustb_host::launch_status("cloud_order_identity");
+}
+
+int dustb_cloud_order_check(const dustb_ctx *c, const int *ord, const unsigned long long *tag,
+                            int n, int *bad, void *stream) {
+  if (!c || !bad || n < 0 || (n > 0 && (!ord || !tag))) return DUSTB_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(bad, 0, sizeof(int), st);
+  if (n > 0) {
+    const unsigned g = nblk(n) < 148u * 8u ? nblk(n) : 148u * 8u;
+    k_order_check<<<g, kT, 0, st>>>(c->part.pi, c->part.stride, c->part.npart, ord, tag, n, bad);
+  }
+  return dustb_host::launch_status("cloud_order_check");
+}
+
+}  // extern "C"
+
 // ---- cell index without any allocation ---------------------------------------------------
 // For host codes that cannot allocate device memory at the point of the call (a code whose
 // device memory all comes from its own pool reserved at start-up, or one that must not make

@@ -261,6 +261,32 @@ class DeviceDust:
         capi.check(rc, "cell_index")
         return order[:self.npart], cstart
 
+    def cloud_order(self, stream=None):
+        """UpdateCloudOrder's rebuild: the particles in (block, cell, index) order without
+        moving them, and the 64-bit tag of each indexed particle (int32, int64 tensors)."""
+        n = self.npart
+        ord_ = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+        tag = torch.empty(max(n, 1), dtype=torch.int64, device=self.device)
+        s = self._scratch()
+        self._call("cloud_order", ord_.data_ptr(), tag.data_ptr(), s.data_ptr(), s.numel(),
+                   stream=stream)
+        return ord_[:n], tag[:n]
+
+    def cloud_order_identity(self, stream=None):
+        """The index after a sort in cell order: slot k holds particle k."""
+        n = self.npart
+        ord_ = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+        tag = torch.empty(max(n, 1), dtype=torch.int64, device=self.device)
+        self._call("cloud_order_identity", ord_.data_ptr(), tag.data_ptr(), stream=stream)
+        return ord_[:n], tag[:n]
+
+    def cloud_order_check(self, ord_, tag, stream=None) -> int:
+        """The number of index entries whose slot no longer holds the indexed particle."""
+        bad = torch.empty(1, dtype=torch.int32, device=self.device)
+        self._call("cloud_order_check", ord_.data_ptr(), tag.data_ptr(), int(ord_.numel()),
+                   bad.data_ptr(), stream=stream)
+        return int(bad.item())
+
     def sort_by_cell(self, stream=None):
         """SortParticles: sort into spare arrays, then swap them in (as the reference)."""
         s = self._scratch()

@@ -32,6 +32,9 @@ DustGasDrag::DustGasDrag(const dustb_ctx &ctx, void *stream, DustCoupling coupli
 
 DustGasDrag::~DustGasDrag() {
   if (dev_scalars_) cudaFree(dev_scalars_);
+  if (cloud_ord_) cudaFree(cloud_ord_);
+  if (cloud_ord_tag_) cudaFree(cloud_ord_tag_);
+  if (dev_bad_) cudaFree(dev_bad_);
 }
 
 TaskStatus DustGasDrag::Check(int rc, const char *task) {
@@ -151,13 +154,79 @@ TaskStatus DustGasDrag::NewTimeStep(Driver *pdrive, int stage) {
 }
 
 TaskStatus DustGasDrag::SortParticles(double *spare_pr, int *spare_pi, void *scratch,
-                                      long long bytes) {
+                                      long long bytes, int ncycle) {
   TaskStatus ts = Check(dustb_sort_by_cell(&ctx_, spare_pr, spare_pi, scratch, bytes, stream_),
                         "SortParticles");
   if (ts != TaskStatus::complete) return ts;
   // the sorted rows are the spares now (dust_cloud_device.cpp:1951-1954: swap)
   ctx_.part.pr = spare_pr;
   ctx_.part.pi = spare_pi;
+  // after a sort in cell order the cloud order index is the identity (:1956-1975)
+  if (cloud_order_interval_ > 0 && ncycle >= 0) {
+    if ((ts = GrowCloudOrder()) != TaskStatus::complete) return ts;
+    ts = Check(dustb_cloud_order_identity(&ctx_, cloud_ord_, cloud_ord_tag_, stream_),
+               "SortParticles");
+    if (ts != TaskStatus::complete) return ts;
+    cloud_ord_n_ = ctx_.part.npart;
+    cloud_sort_cycle_ = ncycle;
+  }
+  return ts;
+}
+
+// room for npart + npart/4 entries, as the reference allocates
+TaskStatus DustGasDrag::GrowCloudOrder() {
+  const int n = ctx_.part.npart;
+  if (!dev_bad_ && cudaMalloc(&dev_bad_, sizeof(int)) != cudaSuccess) {
+    dev_bad_ = nullptr;
+    last_error_ = "UpdateCloudOrder: device counter not allocated";
+    return TaskStatus::fail;
+  }
+  if (cloud_ord_cap_ >= n) return TaskStatus::complete;
+  if (cloud_ord_) cudaFree(cloud_ord_);
+  if (cloud_ord_tag_) cudaFree(cloud_ord_tag_);
+  cloud_ord_ = nullptr;
+  cloud_ord_tag_ = nullptr;
+  cloud_ord_cap_ = 0;
+  const int cap = n + n / 4;
+  if (cudaMalloc(&cloud_ord_, sizeof(int) * (size_t)cap) != cudaSuccess ||
+      cudaMalloc(&cloud_ord_tag_, sizeof(unsigned long long) * (size_t)cap) != cudaSuccess) {
+    last_error_ = "UpdateCloudOrder: index not allocated";
+    return TaskStatus::fail;
+  }
+  cloud_ord_cap_ = cap;
+  return TaskStatus::complete;
+}
+
+TaskStatus DustGasDrag::UpdateCloudOrder(const Driver &drv, void *scratch, long long bytes) {
+  if (cloud_order_interval_ <= 0) return TaskStatus::complete;
+  const int npart = ctx_.part.npart;
+  // the sort of this cycle left the identity index
+  if (cloud_sort_cycle_ == drv.ncycle && cloud_ord_n_ == npart) return TaskStatus::complete;
+  bool rebuild = (drv.ncycle % cloud_order_interval_ == 0) || cloud_ord_n_ == 0 ||
+                 cloud_ord_n_ > npart;
+  if (!rebuild) {
+    TaskStatus ts = Check(dustb_cloud_order_check(&ctx_, cloud_ord_, cloud_ord_tag_,
+                                                  cloud_ord_n_, dev_bad_, stream_),
+                          "UpdateCloudOrder");
+    if (ts != TaskStatus::complete) return ts;
+    int bad = 0;
+    if (cudaMemcpyAsync(&bad, dev_bad_, sizeof(int), cudaMemcpyDeviceToHost,
+                        (cudaStream_t)stream_) != cudaSuccess ||
+        cudaStreamSynchronize((cudaStream_t)stream_) != cudaSuccess) {
+      last_error_ = "UpdateCloudOrder: check count not read";
+      return TaskStatus::fail;
+    }
+    rebuild = bad > 0;
+  }
+  if (!rebuild) return TaskStatus::complete;
+  if (npart < 2) { cloud_ord_n_ = 0; return TaskStatus::complete; }
+  TaskStatus ts = GrowCloudOrder();
+  if (ts != TaskStatus::complete) return ts;
+  ts = Check(dustb_cloud_order(&ctx_, cloud_ord_, cloud_ord_tag_, scratch, bytes, stream_),
+             "UpdateCloudOrder");
+  if (ts != TaskStatus::complete) return ts;
+  cloud_ord_n_ = npart;
+  ++cloud_ord_builds_;
   return ts;
 }
 

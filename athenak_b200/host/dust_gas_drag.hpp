@@ -32,6 +32,7 @@ struct Driver {
   double a_impl = 0.0;
   int nexp_stages = 2;           // stage 3 of imex2+ is dormant for the drag (dust.cpp:1646)
   double dt = 0.0, time = 0.0;   // Mesh::dt, Mesh::time
+  int ncycle = 0;                // Mesh::ncycle
   void SetImEx2PlusCoefficients(double gamma_new);
 };
 
@@ -64,8 +65,23 @@ class DustGasDrag {
   TaskStatus NewTimeStep(Driver *pdrive, int stage);       // dust_newdt.cpp:108-149
 
   // SortParticles (dust_cloud_device.cpp:1881-1977): into the spare arrays, then swapped
-  // in; the spares (same shape as the rows) become the caller's to keep or free.
-  TaskStatus SortParticles(double *spare_pr, int *spare_pi, void *scratch, long long bytes);
+  // in; the spares (same shape as the rows) become the caller's to keep or free.  With the
+  // cloud order index on, the index becomes the identity, marked with the cycle ncycle.
+  TaskStatus SortParticles(double *spare_pr, int *spare_pi, void *scratch, long long bytes,
+                           int ncycle = -1);
+
+  // UpdateCloudOrder (dust_cloud_device.cpp:1992-2055), <dust>/cloud_order_interval = n > 0:
+  // an index of the particles in (block, cell, index) order without moving them, rebuilt
+  // every n cycles, after a check finds a slot that no longer holds its particle, or when it
+  // is longer than the particle set; kept as it is after a sort of the same cycle; none
+  // below 2 particles.  Synchronises the stream for the check's count.  scratch: at least
+  // dustb_sort_scratch_bytes.
+  void SetCloudOrderInterval(int n) { cloud_order_interval_ = n; }
+  TaskStatus UpdateCloudOrder(const Driver &drv, void *scratch, long long bytes);
+  const int *CloudOrder() const { return cloud_ord_; }
+  const unsigned long long *CloudOrderTags() const { return cloud_ord_tag_; }
+  int CloudOrderLength() const { return cloud_ord_n_; }
+  int CloudOrderBuilds() const { return cloud_ord_builds_; }
 
   // the stage's drag tasks in dependency order on one rank and one stream
   TaskStatus DoStage(Driver *pdrive, int stage);
@@ -89,6 +105,13 @@ class DustGasDrag {
   DustCoupling coupling_;
   double *dev_scalars_ = nullptr;   // [0..1] x3 removed, [2] chi_max, [3] dt
   std::string last_error_;
+  // the cloud order index (cloud_ord, cloud_ord_tag of the reference) and its control
+  TaskStatus GrowCloudOrder();
+  int *cloud_ord_ = nullptr;
+  unsigned long long *cloud_ord_tag_ = nullptr;
+  int *dev_bad_ = nullptr;
+  int cloud_ord_cap_ = 0, cloud_ord_n_ = 0, cloud_sort_cycle_ = -1, cloud_ord_builds_ = 0;
+  int cloud_order_interval_ = 0;
 };
 
 // The mixed-precision form from the host (dustb_mixed_*): a compact FP32 shadow of the

@@ -240,6 +240,25 @@ int dustb_sort_by_cell(const dustb_ctx *ctx, double *spare_pr, int *spare_pi, vo
  *  - It calls no cudaMalloc, cudaFree or allocating library routine. */
 int dustb_cell_index_static(const dustb_ctx *ctx, int *order, int *cstart, void *stream);
 
+/* ---- the cloud order index (DustGasDrag::UpdateCloudOrder, src/dust/dust_cloud_device.cpp:
+ * 1992-2055; the identity after a sort, :1956-1975) -------------------------------------
+ * An index of the particles in (block, k, j, i, index) order without moving them, and the
+ * 64-bit tag (PTAG the low word, PTAGH the high) of the particle each slot indexed, so that a
+ * later check finds any reordering of the rows.  The keys are those of dustb_cell_index.
+ * The host keeps the reference's control (rebuild every cloud_order_interval cycles, after a
+ * failed check, or when the index is longer than the particle set; none after a sort in the
+ * same cycle; no index below 2 particles). */
+/* Rebuild: ord[0..npart), tag[0..npart); scratch as dustb_sort_scratch_bytes. */
+int dustb_cloud_order(const dustb_ctx *ctx, int *ord, unsigned long long *tag, void *scratch,
+                      long long scratch_bytes, void *stream);
+/* After a sort in cell order: ord[k] = k and its tag (:1970-1972). */
+int dustb_cloud_order_identity(const dustb_ctx *ctx, int *ord, unsigned long long *tag,
+                               void *stream);
+/* The check between rebuilds (:2001-2010): *bad (device int) = the entries k < n whose ord[k]
+ * is outside [0, npart) or whose particle's tag is not tag[k]. */
+int dustb_cloud_order_check(const dustb_ctx *ctx, const int *ord, const unsigned long long *tag,
+                            int n, int *bad, void *stream);
+
 /* ---- pc2 (src/dust/dust_pm.cpp:109-194, :374-405, :585-602; dust_push.cpp:37-61,
  * :99-247) ---------------------------------------------------------------------------- */
 int dustb_pc2_predictor(const dustb_ctx *ctx, double dt, int rate_dep, void *stream);

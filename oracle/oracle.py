@@ -61,6 +61,8 @@ def lib():
             "oracle_tstop_extrema": ([P, I, VP], None),
             "oracle_sort_order": ([P, VP, VP], None),
             "oracle_sort_particles": ([P, VP, VP], None),
+            "oracle_cloud_order": ([P, VP, VP], None),
+            "oracle_cloud_order_check": ([P, VP, VP, I], I),
             "oracle_pc2_predictor": ([P, D, I], C.c_uint),
             "oracle_pc2_apply_predictor": ([P, D], D),
             "oracle_pc2_midpoint": ([P], None),
@@ -176,6 +178,19 @@ class Oracle:
         keys = np.zeros(max(n, 1), np.int64)
         self.call("sort_order", order.ctypes.data, keys.ctypes.data)
         return order[:n], keys[:n]
+
+    def cloud_order(self):
+        """UpdateCloudOrder's rebuild: (ord, tag)."""
+        n = self.st.npart
+        ord_ = np.zeros(max(n, 1), np.int32)
+        tag = np.zeros(max(n, 1), np.uint64)
+        self.call("cloud_order", ord_.ctypes.data, tag.ctypes.data)
+        return ord_[:n], tag[:n]
+
+    def cloud_order_check(self, ord_, tag):
+        ord_ = np.ascontiguousarray(ord_, np.int32)
+        tag = np.ascontiguousarray(tag, np.uint64)
+        return self.call("cloud_order_check", ord_.ctypes.data, tag.ctypes.data, len(ord_))
 
     def sort_particles(self):
         spr = np.zeros_like(self.st.pr)

@@ -6,10 +6,12 @@
 // box: rotation, shear drift): positions within 1e-12 of the box, velocities within 1e-12 of
 // their scale, the gas momentum within 1e-11 of its scale, PGID identical, no error bit;
 // then the same cycles in the mixed-precision form (MixedDustGasDrag) at its tolerance.
-// Exit status 0 on agreement.
+// After the FP64 imex2+ cycles the cloud order index (UpdateCloudOrder) runs through its
+// control on the moved rows.  Exit status 0 on agreement.
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -22,6 +24,7 @@ unsigned oracle_imex_cycle(const dustb_ctx *c, double gamma, double dt, const do
 unsigned oracle_pc2_cycle(const dustb_ctx *c, double dt, double *chi_out, double *x3_removed);
 void oracle_ghost_copy(const dustb_ctx *c, double *a, int nvar, int x3_bcs);
 void oracle_set_threads(int n);
+void oracle_cloud_order(const dustb_ctx *c, int *ord, uint64_t *tag);
 }
 
 namespace {
@@ -86,6 +89,79 @@ dustb_ctx make_ctx(const Arrays &a, int npart) {
 }
 
 const size_t NF[8] = {4, 4, 5, 3, 3, 4, 3};   // u0 u1 qdep ustar dmom resid work
+
+// UpdateCloudOrder's control on the pack's rows (cloud_order_interval = 4): the first build
+// equals the oracle's index of the same rows (slots and tags bit-exact); a passing check at
+// the next cycle keeps it; a sort at cycle 3 leaves the identity, which that cycle keeps; the
+// rebuild at the interval (cycle 4) gives the identity again on the sorted rows; a tag
+// changed under the index fails the next check and the rebuilt index holds the new tag.
+// The sort moves the rows into spares this function allocates and frees: call it last.
+bool cloud_order_checks(athenak_b200::DustGasDrag &drag, int npart, std::vector<double> &mb,
+                        std::vector<int> &ng) {
+  using athenak_b200::TaskStatus;
+  athenak_b200::Driver drv;
+  const long long bytes = dustb_sort_scratch_bytes(&drag.Context().mesh, npart);
+  void *scratch = nullptr;
+  double *spr = nullptr;
+  int *spi = nullptr;
+  cudaMalloc(&scratch, (size_t)bytes);
+  cudaMalloc(&spr, sizeof(double) * 17 * npart);
+  cudaMalloc(&spi, sizeof(int) * 5 * npart);
+  std::vector<int> go(npart);
+  std::vector<unsigned long long> gt(npart);
+  auto index = [&]() {
+    cudaMemcpy(go.data(), drag.CloudOrder(), sizeof(int) * npart, cudaMemcpyDeviceToHost);
+    cudaMemcpy(gt.data(), drag.CloudOrderTags(), sizeof(unsigned long long) * npart,
+               cudaMemcpyDeviceToHost);
+  };
+  auto identity = [&]() {
+    index();
+    bool id = true;
+    for (int k = 0; k < npart; ++k) id = id && go[k] == k;
+    return id;
+  };
+  auto update = [&](int cyc) {
+    drv.ncycle = cyc;
+    return drag.UpdateCloudOrder(drv, scratch, bytes) == TaskStatus::complete;
+  };
+  drag.SetCloudOrderInterval(4);
+  bool ok = update(1) && drag.CloudOrderBuilds() == 1 && drag.CloudOrderLength() == npart;
+  // the oracle's index of the same rows
+  std::vector<double> hpr(17 * (size_t)npart);
+  std::vector<int> hpi(5 * (size_t)npart);
+  cudaMemcpy(hpr.data(), drag.Context().part.pr, sizeof(double) * hpr.size(), cudaMemcpyDeviceToHost);
+  cudaMemcpy(hpi.data(), drag.Context().part.pi, sizeof(int) * hpi.size(), cudaMemcpyDeviceToHost);
+  Arrays h{hpr.data(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, mb.data(),
+           hpi.data(), ng.data(), nullptr, nullptr};
+  dustb_ctx hc = make_ctx(h, npart);
+  std::vector<int> oo(npart);
+  std::vector<uint64_t> ot(npart);
+  oracle_cloud_order(&hc, oo.data(), ot.data());
+  index();
+  bool same = true, moved = false;
+  for (int k = 0; k < npart; ++k) {
+    same = same && go[k] == oo[k] && gt[k] == (unsigned long long)ot[k];
+    moved = moved || go[k] != k;
+  }
+  ok = ok && same && moved;
+  ok = ok && update(2) && drag.CloudOrderBuilds() == 1;
+  ok = ok && drag.SortParticles(spr, spi, scratch, bytes, 3) == TaskStatus::complete;
+  ok = ok && update(3) && drag.CloudOrderBuilds() == 1 && identity();
+  ok = ok && update(4) && drag.CloudOrderBuilds() == 2 && identity();
+  // a new tag in slot 5 (PTAG row)
+  const int newtag = 987654321;
+  cudaMemcpy(drag.Context().part.pi + 1 * (size_t)npart + 5, &newtag, sizeof(int),
+             cudaMemcpyHostToDevice);
+  ok = ok && update(5) && drag.CloudOrderBuilds() == 3 && identity() &&
+       (unsigned)(gt[5] & 0xffffffffull) == (unsigned)newtag;
+  std::printf("cloud order index: builds %d, length %d, first build %s the oracle's: %s\n",
+              drag.CloudOrderBuilds(), drag.CloudOrderLength(), same ? "equals" : "DIFFERS FROM",
+              ok ? "ok" : "MISMATCH");
+  cudaFree(scratch);
+  cudaFree(spr);
+  cudaFree(spi);
+  return ok;
+}
 
 // mixed: the mixed-precision form (MixedDustGasDrag) against the oracle at the mixed form's
 // stated tolerance (velocities 1e-5 of their scale, positions 1e-5 of a cell, the gas
@@ -206,10 +282,12 @@ int run(athenak_b200::DustCoupling coupling, const char *name, bool mixed = fals
               "(scale %.3e), PGID %s, error words %u/%u: %s\n",
               name, npart, dx, dv, vs, du, us, pgid ? "identical" : "DIFFER", gerr, oerr,
               ok ? "ok" : "MISMATCH");
+  const bool cord = mixed || coupling != athenak_b200::DustCoupling::imex ||
+                    cloud_order_checks(drag, npart, mb, ng);
   for (int f = 0; f < 7; ++f) cudaFree(*fd[f]);
   cudaFree(d.pr); cudaFree(d.pi); cudaFree(d.mb); cudaFree(d.nghbr); cudaFree(d.sbgid);
   cudaFree(d.err);
-  return ok ? 0 : 1;
+  return ok && cord ? 0 : 1;
 }
 
 }  // namespace
