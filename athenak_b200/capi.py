@@ -12,6 +12,7 @@ DUSTB_NGP, DUSTB_CIC, DUSTB_TSC = 0, 1, 2
 SOLVER_LOCAL, SOLVER_APPLYA, SOLVER_DC1, SOLVER_DC2 = 0, 1, 2, 3
 X3_PERIODIC, X3_REFLECT, X3_OUTFLOW = 0, 1, 2
 ERR_HALO, ERR_ROUTE, ERR_NGHBR, ERR_PGID, ERR_TSTOP, ERR_WINDOW = 1, 2, 4, 8, 16, 32
+ERR_TIMEOUT, ERR_POINT = 64, 128
 
 
 class DustbMesh(C.Structure):
@@ -167,6 +168,9 @@ SIGNATURES = {
     "dustb_cloud_order": [CTXP, VP, VP, VP, LL, VP],
     "dustb_cloud_order_identity": [CTXP, VP, VP, VP],
     "dustb_cloud_order_check": [CTXP, VP, VP, I, VP, VP],
+    "dustb_point_gravity_density": [CTXP, VP, VP, VP],
+    "dustb_point_gravity_gather": [CTXP, VP, VP, VP, LL, VP],
+    "dustb_point_science_fields": [CTXP, VP, VP, I, I, VP],
 }
 RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_phst_scratch_bytes": LL,
             "dustb_last_error": C.c_char_p}

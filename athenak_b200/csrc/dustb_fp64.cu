@@ -1106,6 +1106,183 @@ __global__ void k_argmax_final(Ind d, MCtx M, const double *bval, const long lon
   }
 }
 
+// ---- point-particle fields for self-gravity and outputs, src/dust/dust_gravity_points.cpp --
+// A 3-D point particle the transfers accept (:216-223, :282-287): a finite mass (gravity: also
+// >= 0), an owner block in the pack, a finite position and a stencil inside the padded block.
+// Massless particles (outflow tombstones) contribute nothing; the science fields also skip
+// the particles of other species.  A rejected particle sets DUSTB_ERR_POINT (the reference
+// aborts the run).
+__device__ __forceinline__ bool point_stencil(const PCtx &P, const MCtx &M, const Ind &d, int p,
+                                              int &m, int &ip, int &jp, int &kp, double wx[3],
+                                              double wy[3], double wz[3]) {
+  m = P.i(DUSTB_PGID, p) - M.gids;
+  const double x = P.r(DUSTB_IPX, p), y = P.r(DUSTB_IPY, p), z = P.r(DUSTB_IPZ, p);
+  if (!block_ok(d, m) || !isfinite(x) || !isfinite(y) || !isfinite(z)) return false;
+  weights3(M, d, m, x, y, z, ip, jp, kp, wx, wy, wz);
+  return ip >= 1 && ip < d.n1 - 1 && jp >= 1 && jp < d.n2 - 1 && kp >= 1 && kp < d.n3 - 1;
+}
+
+// DepositPointGravityDensity (:215-245; gravity = 1: density only, mass >= 0) and
+// DepositPointScienceFields (:257-304; ncomp 1 or 4: m/V and m v/V, one species or all):
+// the density with the deposit weights into the owner block's cells, ghost cells included
+__global__ void k_point_deposit(PCtx P, MCtx M, Ind d, double *f, int ncomp, int species,
+                                int gravity, unsigned *err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  const double mass = P.r(DUSTB_IPM, p);
+  if (gravity) {
+    if (!(mass >= 0.0) || !isfinite(mass)) { report(err, DUSTB_ERR_POINT); return; }
+    if (mass == 0.0) return;
+  } else {
+    if (mass == 0.0) return;
+    if (species >= 0 && P.i(DUSTB_PSP, p) != species) return;
+    if (!isfinite(mass)) { report(err, DUSTB_ERR_POINT); return; }
+  }
+  int m, ip, jp, kp; double wx[3], wy[3], wz[3];
+  if (!point_stencil(P, M, d, p, m, ip, jp, kp, wx, wy, wz)) { report(err, DUSTB_ERR_POINT); return; }
+  const double density = mass / (M.s(m, DX1) * M.s(m, DX2) * M.s(m, DX3));
+  const double v1 = P.r(DUSTB_IPVX, p), v2 = P.r(DUSTB_IPVY, p), v3 = P.r(DUSTB_IPVZ, p);
+  for (int c = 0; c < 3; ++c)
+    for (int b = 0; b < 3; ++b)
+      for (int a = 0; a < 3; ++a) {
+        const double w = density * wz[c] * wy[b] * wx[a];
+        if (w == 0.0) continue;
+        const int kk = kp + c - 1, jj = jp + b - 1, ii = ip + a - 1;
+        atomicAdd(&f[d.at(m, ncomp, 0, kk, jj, ii)], w);
+        if (ncomp == 1) continue;
+        atomicAdd(&f[d.at(m, ncomp, 1, kk, jj, ii)], w * v1);
+        atomicAdd(&f[d.at(m, ncomp, 2, kk, jj, ii)], w * v2);
+        atomicAdd(&f[d.at(m, ncomp, 3, kk, jj, ii)], w * v3);
+      }
+}
+
+// the remapped field's active cells, the ghost cells zero (:246-248, :297-304)
+__global__ void k_owned_copy(Ind d, const double *f, double *out, int nvar) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long per = d.cells();
+  if (idx >= per * d.nmb * nvar) return;
+  const long long mv = idx / per;
+  long long r = idx - mv * per;
+  const int i = (int)(r % d.n1); r /= d.n1;
+  const int j = (int)(r % d.n2);
+  const int k = (int)(r / d.n2);
+  const bool act = i >= d.is && i <= d.ie && j >= d.js && j <= d.je && k >= d.ks && k <= d.ke;
+  out[idx] = act ? f[idx] : 0.0;
+}
+
+// The transpose of the shear part of the deposit remap (shear_add_sum) for ghost cell
+// (k, j, i) of face block m beyond the shear-periodic face in direction o1: the active cells
+// its deposit lands in lie in the strip next to the opposite face, in the same x3 plane (or
+// the neighbouring block's across an x3 ghost plane, or the mirrored plane at a physical x3
+// face), in the global rows its interval [Y + sh, Y + 1 + sh) overlaps; the overlaps are the
+// weights, formed as shear_add_sum forms them.
+__device__ double shear_transpose_sum(const SBox &B, const Ind &d, const double *owned, int nvar,
+                                      int m, int v, int k, int j, int i, int o1) {
+  const int ng1 = B.ng - 1;
+  const long long N2 = (long long)B.nb2 * B.nx2;
+  int b2, b3;
+  B.b23(m, b2, b3);
+  const int g = (o1 > 0) ? i - d.ie - 1 : i - (d.is - d.ng);
+  const int tface = (o1 > 0) ? 0 : 1;
+  const int ti = (o1 > 0) ? d.is + g : d.ie - ng1 + g;
+  const double sh = (o1 > 0) ? B.shR : -B.shR;
+  int tb3 = b3, tk = k;
+  if (k > d.ke) {
+    if (b3 < B.nb3 - 1 || B.x3bc == 0) { tb3 = (b3 + 1) % B.nb3; tk = k - B.nx3; }
+    else if (!B.drop) tk = 2 * d.ke + 1 - k;
+    else return 0.0;
+  } else if (k < d.ks) {
+    if (b3 > 0 || B.x3bc == 0) { tb3 = (b3 + B.nb3 - 1) % B.nb3; tk = k + B.nx3; }
+    else if (!B.drop) tk = 2 * d.ks - 1 - k;
+    else return 0.0;
+  }
+  const long long Y = (long long)b2 * B.nx2 + (j - d.js);
+  const double ya = (double)Y + sh, yb = (double)(Y + 1) + sh;
+  const long long F = (long long)floor(ya);
+  double sum = 0.0;
+  for (long long Jg = F; Jg <= F + 1; ++Jg) {
+    const double clo = (double)Jg, chi = clo + 1.0;
+    const double o = fmin(yb, chi) - fmax(ya, clo);
+    if (!(o > 0.0)) continue;
+    const long long J = ((Jg % N2) + N2) % N2;
+    const int tb2 = (int)(J / B.nx2);
+    const int T = B.block(tface, tb3, tb2);
+    if (T < 0) continue;
+    const int tj = (int)(J - (long long)tb2 * B.nx2) + d.js;
+    sum += o * owned[d.at(T, nvar, v, tk, tj, ti)];
+  }
+  return sum;
+}
+
+// GatherPointGravityAcceleration's force field (:325-337, with the transpose of the deposit
+// remap, GatherMap :121-160): the owned values on the active cells, and in every ghost cell the
+// owned values of the active cells a deposit into that ghost cell lands in, times the remap
+// weight -- the same-level neighbour's cell, the mirrored cell behind a physical x3 face (of the
+// block or of its x1/x2 neighbour), or the overlap-weighted cells across a shear-periodic face
+__global__ void k_point_force_field(Ind d, const int *nghbr, int gids, SBox B,
+                                    const double *owned, double *f, int nvar) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long per = d.cells();
+  if (idx >= per * d.nmb) return;
+  const int m = (int)(idx / per);
+  long long r = idx - (long long)m * per;
+  const int i = (int)(r % d.n1); r /= d.n1;
+  const int j = (int)(r % d.n2);
+  const int k = (int)(r / d.n2);
+  const int o1 = (i < d.is) ? -1 : ((i > d.ie) ? 1 : 0);
+  const int o2 = (j < d.js) ? -1 : ((j > d.je) ? 1 : 0);
+  const int o3 = (k < d.ks) ? -1 : ((k > d.ke) ? 1 : 0);
+  if ((o1 | o2 | o3) == 0) {
+    for (int v = 0; v < nvar; ++v) f[d.at(m, nvar, v, k, j, i)] = owned[d.at(m, nvar, v, k, j, i)];
+    return;
+  }
+  if (B.on && B.crossing(m, o1)) {
+    for (int v = 0; v < nvar; ++v)
+      f[d.at(m, nvar, v, k, j, i)] = shear_transpose_sum(B, d, owned, nvar, m, v, k, j, i, o1);
+    return;
+  }
+  int src = -1, sk = k - o3 * d.nx3;
+  if (o3 != 0 && nghbr[(long long)m * 27 + dir_slot(0, 0, o3)] < 0) {
+    // behind a physical x3 face: the fold's mirrored plane, in this block or its x1/x2
+    // neighbour (the deposit is never dropped here)
+    src = (o1 | o2) ? nghbr[(long long)m * 27 + dir_slot(o1, o2, 0)] - gids : m;
+    sk = (o3 < 0) ? 2 * d.ks - 1 - k : 2 * d.ke + 1 - k;
+  } else {
+    src = nghbr[(long long)m * 27 + dir_slot(o1, o2, o3)] - gids;
+  }
+  const bool ok = src >= 0 && src < d.nmb;
+  for (int v = 0; v < nvar; ++v)
+    f[d.at(m, nvar, v, k, j, i)] =
+        ok ? owned[d.at(src, nvar, v, sk, j - o2 * d.nx2, i - o1 * d.nx1)] : 0.0;
+}
+
+// the acceleration at each particle: the TSC weights over the force field (:339-368)
+__global__ void k_point_gather(PCtx P, MCtx M, Ind d, const double *f, double *acc,
+                               long long astride, unsigned *err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  double a[3] = {0.0, 0.0, 0.0};
+  const double mass = P.r(DUSTB_IPM, p);
+  int m, ip, jp, kp; double wx[3], wy[3], wz[3];
+  if (!(mass >= 0.0) || !isfinite(mass)) {
+    report(err, DUSTB_ERR_POINT);
+  } else if (mass != 0.0) {
+    if (!point_stencil(P, M, d, p, m, ip, jp, kp, wx, wy, wz)) {
+      report(err, DUSTB_ERR_POINT);
+    } else {
+      for (int c = 0; c < 3; ++c)
+        for (int b = 0; b < 3; ++b)
+          for (int q = 0; q < 3; ++q) {
+            const double w = wz[c] * wy[b] * wx[q];
+            for (int v = 0; v < 3; ++v)
+              a[v] += w * f[d.at(m, 3, v, kp + c - 1, jp + b - 1, ip + q - 1)];
+          }
+      if (!isfinite(a[0]) || !isfinite(a[1]) || !isfinite(a[2])) report(err, DUSTB_ERR_POINT);
+    }
+  }
+  for (int v = 0; v < 3; ++v) acc[(long long)v * astride + p] = a[v];
+}
+
 long long n_active(const Ind &d) { return (long long)d.nmb * d.nx3 * d.nx2 * d.nx1; }
 long long n_all(const Ind &d) { return d.cells() * d.nmb; }
 
@@ -1420,6 +1597,58 @@ int dustb_phst(const dustb_ctx *c, const double *chi_max, double *row, void *scr
   k_argmax_blocks<<<nb, 256, 0, S(stream)>>>(d, field, bval, bloc);
   k_argmax_final<<<1, 1, 0, S(stream)>>>(d, mview(c), bval, bloc, nb, row);
   return launch_status("phst");
+}
+
+// the point transfers' remap: the drag's, with the ghost deposits behind physical x3 faces
+// always folded (src/dust/dust_gravity_points.cpp:176-178)
+static dustb_ctx fold_ctx(const dustb_ctx *c) {
+  dustb_ctx g = *c;
+  g.phys.x3_deposit_drop = 0;
+  return g;
+}
+
+static int point_deposit(const dustb_ctx *c, double *out, double *halo, int ncomp, int species,
+                         int gravity, void *stream) {
+  const Ind d = make_ind(c->mesh);
+  const dustb_ctx g = fold_ctx(c);
+  cudaMemsetAsync(halo, 0, (size_t)(n_all(d) * ncomp) * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_point_deposit<<<PGRID(c)>>>(pview(c), mview(c), d, halo, ncomp, species, gravity, c->err);
+  int rc = dustb_ghost_add(&g, halo, ncomp, stream);
+  if (rc) return rc;
+  k_owned_copy<<<blocks_for(n_all(d) * ncomp), kThreads, 0, S(stream)>>>(d, halo, out, ncomp);
+  return launch_status("point_deposit");
+}
+
+int dustb_point_gravity_density(const dustb_ctx *c, double *owned, double *halo, void *stream) {
+  CHECK_CTX(c);
+  if (!owned || !halo) return DUSTB_EINVAL;
+  if (!c->mesh.three_d || c->phys.scheme != DUSTB_TSC) return DUSTB_EUNSUP;
+  return point_deposit(c, owned, halo, 1, -1, 1, stream);
+}
+
+int dustb_point_science_fields(const dustb_ctx *c, double *out, double *halo, int mass_only,
+                               int species, void *stream) {
+  CHECK_CTX(c);
+  if (!out || !halo) return DUSTB_EINVAL;
+  if (!c->mesh.three_d) return DUSTB_EUNSUP;
+  return point_deposit(c, out, halo, mass_only ? 1 : 4, species, 0, stream);
+}
+
+int dustb_point_gravity_gather(const dustb_ctx *c, const double *owned, double *halo,
+                               double *acc, long long acc_stride, void *stream) {
+  CHECK_CTX(c);
+  if (!owned || !halo || !acc || acc_stride < c->part.npart) return DUSTB_EINVAL;
+  if (!c->mesh.three_d || c->phys.scheme != DUSTB_TSC) return DUSTB_EUNSUP;
+  const Ind d = make_ind(c->mesh);
+  const dustb_ctx g = fold_ctx(c);
+  const SBox B = sbview(&g);
+  if (B.on && (!B.sb_gid || B.nb2 <= 0 || B.nb3 <= 0)) return DUSTB_EINVAL;
+  k_point_force_field<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(
+      d, c->mesh.nghbr, c->mesh.gids, B, owned, halo, 3);
+  if (c->part.npart > 0)
+    k_point_gather<<<PGRID(c)>>>(pview(c), mview(c), d, halo, acc, acc_stride, c->err);
+  return launch_status("point_gravity_gather");
 }
 
 // one imex2+ cycle in the task order of src/dust/dust_tasks.cpp:38-120 (stage 3 dormant,

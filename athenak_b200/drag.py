@@ -241,6 +241,34 @@ class DeviceDust:
         self._call("phst", chi, row.data_ptr(), s.data_ptr(), s.numel(), stream=stream)
         return row
 
+    # ---- point-particle fields (self-gravity, outputs) ----
+    def _field(self, nvar):
+        return torch.zeros(self.mesh.field_shape(nvar), dtype=torch.float64, device=self.device)
+
+    def point_gravity_density(self, stream=None):
+        """DepositPointGravityDensity: the owned TSC density field (ghost cells zero)."""
+        owned, halo = self._field(1), self._field(1)
+        self._call("point_gravity_density", owned.data_ptr(), halo.data_ptr(), stream=stream)
+        return owned
+
+    def point_gravity_gather(self, owned, stream=None, return_field=False):
+        """GatherPointGravityAcceleration: the (3, npart) acceleration over owned (nmb, 3, ...)
+        (and, with return_field, the force field with its transposed ghost cells)."""
+        n = self.npart
+        halo = self._field(3)
+        acc = torch.empty((3, max(n, 1)), dtype=torch.float64, device=self.device)
+        self._call("point_gravity_gather", owned.data_ptr(), halo.data_ptr(), acc.data_ptr(),
+                   max(n, 1), stream=stream)
+        return (acc[:, :n], halo) if return_field else acc[:, :n]
+
+    def point_science_fields(self, mass_only=False, species=-1, stream=None):
+        """DepositPointScienceFields: m/V and m v/V (or m/V alone) on the active cells."""
+        nv = 1 if mass_only else 4
+        out, halo = self._field(nv), self._field(nv)
+        self._call("point_science_fields", out.data_ptr(), halo.data_ptr(), int(mass_only),
+                   int(species), stream=stream)
+        return out
+
     # ---- sort ----
     def _scratch(self):
         n = int(self.lib.dustb_sort_scratch_bytes(C.byref(self.ctx.mesh), self.npart))

@@ -173,6 +173,29 @@ TaskStatus DustGasDrag::SortParticles(double *spare_pr, int *spare_pi, void *scr
   return ts;
 }
 
+TaskStatus DustGasDrag::DepositPointGravityDensity(double time, double *owned, double *halo) {
+  dustb_ctx c = ctx_;
+  c.mesh.time = time;
+  return Check(dustb_point_gravity_density(&c, owned, halo, stream_), "DepositPointGravityDensity");
+}
+
+TaskStatus DustGasDrag::GatherPointGravityAcceleration(double time, const double *owned,
+                                                       double *halo, double *acc,
+                                                       long long acc_stride) {
+  dustb_ctx c = ctx_;
+  c.mesh.time = time;
+  return Check(dustb_point_gravity_gather(&c, owned, halo, acc, acc_stride, stream_),
+               "GatherPointGravityAcceleration");
+}
+
+TaskStatus DustGasDrag::DepositPointScienceFields(double time, double *out, double *halo,
+                                                  bool mass_only, int species) {
+  dustb_ctx c = ctx_;
+  c.mesh.time = time;
+  return Check(dustb_point_science_fields(&c, out, halo, mass_only ? 1 : 0, species, stream_),
+               "DepositPointScienceFields");
+}
+
 // room for npart + npart/4 entries, as the reference allocates
 TaskStatus DustGasDrag::GrowCloudOrder() {
   const int n = ctx_.part.npart;

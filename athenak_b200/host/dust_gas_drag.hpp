@@ -83,6 +83,16 @@ class DustGasDrag {
   int CloudOrderLength() const { return cloud_ord_n_; }
   int CloudOrderBuilds() const { return cloud_ord_builds_; }
 
+  // Point-particle fields (src/dust/dust_gravity_points.cpp) at the field time `time` (the
+  // shear offset of the remap): the TSC density for self-gravity, the acceleration gathered
+  // from an owned force field (acc row d at acc + d * acc_stride), and the mass and momentum
+  // densities of the outputs.  halo: the caller's scratch field of the output's shape.
+  TaskStatus DepositPointGravityDensity(double time, double *owned, double *halo);
+  TaskStatus GatherPointGravityAcceleration(double time, const double *owned, double *halo,
+                                            double *acc, long long acc_stride);
+  TaskStatus DepositPointScienceFields(double time, double *out, double *halo, bool mass_only,
+                                       int species);
+
   // the stage's drag tasks in dependency order on one rank and one stream
   TaskStatus DoStage(Driver *pdrive, int stage);
   // one cycle: every working stage

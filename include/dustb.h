@@ -61,6 +61,8 @@ enum { DUSTB_X3_PERIODIC = 0, DUSTB_X3_REFLECT = 1, DUSTB_X3_OUTFLOW = 2 };
 #define DUSTB_ERR_TSTOP     0x10u /* stopping time not finite and positive (dust_newdt.cpp:53) */
 #define DUSTB_ERR_WINDOW    0x20u /* fused kernels: a particle outside its tile window */
 #define DUSTB_ERR_TIMEOUT   0x40u /* a bounded wait on an asynchronous copy ran out */
+#define DUSTB_ERR_POINT     0x80u /* point-particle fields: invalid mass, owner, position or
+                                   * TSC support (dust_gravity_points.cpp:29-33) */
 
 /* host return codes */
 #define DUSTB_OK          0
@@ -258,6 +260,27 @@ int dustb_cloud_order_identity(const dustb_ctx *ctx, int *ord, unsigned long lon
  * is outside [0, npart) or whose particle's tag is not tag[k]. */
 int dustb_cloud_order_check(const dustb_ctx *ctx, const int *ord, const unsigned long long *tag,
                             int n, int *bad, void *stream);
+
+/* ---- point-particle fields for self-gravity and outputs (src/dust/dust_gravity_points.cpp)
+ * 3-D point particles on a uniform mesh (PointGravityTransferSupported, :162-167).  Fields
+ * have the mesh layout (nmb, nvar, n3, n2, n1); halo is a scratch field of the same shape.
+ * The ghost deposits are remapped as the drag's are (same-level neighbours, shear-periodic x1
+ * faces), except that at physical x3 faces they are always folded (the transfers' own plans,
+ * :176-178).  A rejected particle sets DUSTB_ERR_POINT and contributes nothing. */
+/* DepositPointGravityDensity (:215-249): owned (nvar 1) = the TSC density m W / V on the
+ * active cells, the ghost cells zero.  Needs scheme TSC (EUNSUP otherwise). */
+int dustb_point_gravity_density(const dustb_ctx *ctx, double *owned, double *halo, void *stream);
+/* GatherPointGravityAcceleration (:316-369): acc[d * acc_stride + p] (d = 0..2, acc_stride >=
+ * npart) = the TSC weights of particle p over the force field, whose active cells are owned
+ * (nvar 3) and whose ghost cells take, by the transpose of the deposit remap (GatherMap
+ * :121-160), the owned values of the cells their deposits land in.  halo: nvar 3. */
+int dustb_point_gravity_gather(const dustb_ctx *ctx, const double *owned, double *halo,
+                               double *acc, long long acc_stride, void *stream);
+/* DepositPointScienceFields (:257-305): out (nvar 4, or 1 with mass_only) = m W / V and
+ * m v W / V with the coupling's weights (ctx scheme) on the active cells, the ghost cells zero;
+ * species >= 0: that species only.  halo: the same nvar. */
+int dustb_point_science_fields(const dustb_ctx *ctx, double *out, double *halo, int mass_only,
+                               int species, void *stream);
 
 /* ---- pc2 (src/dust/dust_pm.cpp:109-194, :374-405, :585-602; dust_push.cpp:37-61,
  * :99-247) ---------------------------------------------------------------------------- */

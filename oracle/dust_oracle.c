@@ -451,8 +451,18 @@ static int shear_crossing(const dustb_ctx *c, int m, int o1) {
  * the fold.  Sources in a fixed order: faces (inner-face targets first), source planes (the
  * cell's plane, then the ghost plane below or folded, then above), source blocks along x2
  * (offsets -1, 0, 1, each block once), source rows, images. */
+static double shear_remap_entries(const dustb_ctx *c, const Ind *d, const double *a, int nvar,
+                                  int m, int v, int k, int j, int i, double *scat,
+                                  double tval);
 static double shear_add_sum(const dustb_ctx *c, const Ind *d, const double *a, int nvar,
                             int m, int v, int k, int j, int i) {
+  return shear_remap_entries(c, d, a, nvar, m, v, k, j, i, NULL, 0.0);
+}
+/* The entries of the cell's remap: with scat == NULL the sum of w * source value, else the
+ * transpose, w * tval added into each source cell of scat (a field of the same shape). */
+static double shear_remap_entries(const dustb_ctx *c, const Ind *d, const double *a, int nvar,
+                                  int m, int v, int k, int j, int i, double *scat,
+                                  double tval) {
   const dustb_mesh *ms = &c->mesh;
   const int faces = sb_faces(ms, m);
   const int ng1 = ms->ng - 1;
@@ -506,7 +516,9 @@ static double shear_add_sum(const dustb_ctx *c, const Ind *d, const double *a, i
             for (int im = -2; im <= 2; ++im) {
               const double clo = (double)(J + im*N2), chi = clo + 1.0;
               const double o = fmin(yb, chi) - fmax(ya, clo);
-              if (o > 0.0) sum += o*A5(a, nvar, (*d), S, v, sk, (int)sj, si);
+              if (!(o > 0.0)) continue;
+              if (scat) A5(scat, nvar, (*d), S, v, sk, (int)sj, si) += o*tval;
+              else sum += o*A5(a, nvar, (*d), S, v, sk, (int)sj, si);
             }
           }
       }
@@ -1205,6 +1217,199 @@ void oracle_pc2_commit(const dustb_ctx *c, double wpred) {
  * weights, the ghost deposits summed into their owners) and its centre, the first cell in
  * (block, k, j, i) order among equal values (:428-441); row[12]: *chi (back-reaction) or -1;
  * row[13] -1, row[14..15] 0.  field: nmb cells of one variable (ghosts included), scratch. */
+/* ---- point-particle fields for self-gravity and outputs, src/dust/dust_gravity_points.cpp ---
+ * A 3-D point particle the transfers accept (:216-223, :282-287): a finite mass (gravity: also
+ * >= 0), an owner block in the pack, a finite position, a stencil inside the padded block.
+ * Massless particles contribute nothing. */
+static int point_stencil(const dustb_ctx *c, const Ind *d, int p, int *m, int *ip, int *jp,
+                         int *kp, double wx[3], double wy[3], double wz[3]) {
+  const dustb_mesh *ms = &c->mesh;
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  *m = PI(DUSTB_PGID, p) - ms->gids;
+  const double x = PR(DUSTB_IPX, p), y = PR(DUSTB_IPY, p), z = PR(DUSTB_IPZ, p);
+  if (*m < 0 || *m >= ms->nmb || !isfinite(x) || !isfinite(y) || !isfinite(z)) return 0;
+  particle_weights(c, d, *m, x, y, z, ip, jp, kp, wx, wy, wz);
+  return *ip >= 1 && *ip < d->n1 - 1 && *jp >= 1 && *jp < d->n2 - 1 && *kp >= 1 &&
+         *kp < d->n3 - 1;
+}
+
+/* DepositPointGravityDensity (:215-249, gravity = 1) and DepositPointScienceFields (:257-305):
+ * the densities into a field with ghosts, the remap with the fold at physical x3 faces (the
+ * transfers' plans, :176-178), the active cells copied out, the ghost cells zero */
+static unsigned point_deposit(const dustb_ctx *c, double *out, int ncomp, int species,
+                              int gravity) {
+  const dustb_mesh *ms = &c->mesh; const Ind d = indices(ms);
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  const size_t nf = field_size(ms, ncomp);
+  double *f = (double *)calloc(nf, sizeof(double));
+  unsigned err = 0;
+  for (int p = 0; p < c->part.npart; ++p) {
+    const double mass = PR(DUSTB_IPM, p);
+    if (gravity) {
+      if (!(mass >= 0.0) || !isfinite(mass)) { err |= DUSTB_ERR_POINT; continue; }
+      if (mass == 0.0) continue;
+    } else {
+      if (mass == 0.0) continue;
+      if (species >= 0 && PI(DUSTB_PSP, p) != species) continue;
+      if (!isfinite(mass)) { err |= DUSTB_ERR_POINT; continue; }
+    }
+    int m, ip, jp, kp; double wx[3], wy[3], wz[3];
+    if (!point_stencil(c, &d, p, &m, &ip, &jp, &kp, wx, wy, wz)) { err |= DUSTB_ERR_POINT; continue; }
+    const double density = mass/(MB(m, DX1)*MB(m, DX2)*MB(m, DX3));
+    const double v[3] = {PR(DUSTB_IPVX, p), PR(DUSTB_IPVY, p), PR(DUSTB_IPVZ, p)};
+    for (int cc = 0; cc < 3; ++cc)
+      for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) {
+          const double w = density*wz[cc]*wy[b]*wx[a];
+          if (w == 0.0) continue;
+          A5(f, ncomp, d, m, 0, kp + cc - 1, jp + b - 1, ip + a - 1) += w;
+          for (int q = 1; q < ncomp; ++q)
+            A5(f, ncomp, d, m, q, kp + cc - 1, jp + b - 1, ip + a - 1) += w*v[q - 1];
+        }
+  }
+  dustb_ctx g = *c;
+  g.phys.x3_deposit_drop = 0;
+  oracle_ghost_add(&g, f, ncomp);
+  memset(out, 0, nf*sizeof(double));
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int q = 0; q < ncomp; ++q)
+      for (int k = d.ks; k <= d.ke; ++k)
+        for (int j = d.js; j <= d.je; ++j)
+          for (int i = d.is; i <= d.ie; ++i)
+            A5(out, ncomp, d, m, q, k, j, i) = A5(f, ncomp, d, m, q, k, j, i);
+  free(f);
+  return err;
+}
+
+unsigned oracle_point_gravity_density(const dustb_ctx *c, double *owned) {
+  return point_deposit(c, owned, 1, -1, 1);
+}
+
+unsigned oracle_point_science_fields(const dustb_ctx *c, double *out, int mass_only,
+                                     int species) {
+  return point_deposit(c, out, mass_only ? 1 : 4, species, 0);
+}
+
+/* The force field of GatherPointGravityAcceleration (:325-337): owned on the active cells, and
+ * the transpose of the deposit remap (GatherMap, :121-160) for the ghost cells: every entry
+ * (target active cell, source ghost cell, weight) of oracle_ghost_add's remap, with the fold at
+ * physical x3 faces, adds weight * owned(target) into the source ghost cell. */
+static void point_force_field(const dustb_ctx *c0, const double *owned, double *f) {
+  dustb_ctx cg = *c0;
+  cg.phys.x3_deposit_drop = 0;
+  const dustb_ctx *c = &cg;
+  const dustb_mesh *ms = &c->mesh; const Ind d = indices(ms);
+  const int nvar = 3, ng1 = ms->ng - 1, ndir = 26;
+  const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
+  memset(f, 0, field_size(ms, nvar)*sizeof(double));
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int v = 0; v < nvar; ++v)
+      for (int k = d.ks; k <= d.ke; ++k)
+        for (int j = d.js; j <= d.je; ++j)
+          for (int i = d.is; i <= d.ie; ++i)
+            A5(f, nvar, d, m, v, k, j, i) = A5(owned, nvar, d, m, v, k, j, i);
+  /* the same-level exchange: receiver m's strip facing direction o took the neighbour's ghost
+   * cells at index - o nx */
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int n = 0; n < ndir; ++n) {
+      const int *o = kDirOrder[n];
+      const int gid = ms->nghbr[(size_t)m*27 + (o[2] + 1)*9 + (o[1] + 1)*3 + (o[0] + 1)];
+      if (gid < 0 || shear_crossing(c, m, o[0])) continue;
+      const int src = gid - ms->gids;
+      int lo[3], hi[3];
+      const int s[3] = {d.is, d.js, d.ks}, e[3] = {d.ie, d.je, d.ke};
+      for (int ax = 0; ax < 3; ++ax) {
+        lo[ax] = (o[ax] > 0) ? (e[ax] - ng1) : s[ax];
+        hi[ax] = (o[ax] < 0) ? (s[ax] + ng1) : e[ax];
+      }
+      for (int v = 0; v < nvar; ++v)
+        for (int k = lo[2]; k <= hi[2]; ++k)
+          for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i)
+              A5(f, nvar, d, src, v, k - o[2]*nx[2], j - o[1]*nx[1], i - o[0]*nx[0]) +=
+                  A5(owned, nvar, d, m, v, k, j, i);
+    }
+  /* the fold behind physical x3 faces */
+  if (ms->x3bc != 0)
+    for (int m = 0; m < ms->nmb; ++m)
+      for (int side = 0; side < 2; ++side) {
+        const int o3 = side ? 1 : -1;
+        if (ms->nghbr[(size_t)m*27 + (o3 + 1)*9 + 1*3 + 1] >= 0) continue;
+        for (int t = 0; t < ms->ng; ++t) {
+          const int k = side ? d.ke - t : d.ks + t;
+          const int kg = side ? d.ke + 1 + t : d.ks - 1 - t;
+          for (int v = 0; v < nvar; ++v)
+            for (int j = d.js; j <= d.je; ++j)
+              for (int i = d.is; i <= d.ie; ++i) {
+                const double val = A5(owned, nvar, d, m, v, k, j, i);
+                A5(f, nvar, d, m, v, kg, j, i) += val;
+                for (int n = 0; n < ndir; ++n) {
+                  const int *o = kDirOrder[n];
+                  if (o[2] != 0) continue;
+                  if (o[0] > 0 && i < d.ie - ng1) continue;
+                  if (o[0] < 0 && i > d.is + ng1) continue;
+                  if (o[1] > 0 && j < d.je - ng1) continue;
+                  if (o[1] < 0 && j > d.js + ng1) continue;
+                  const int gid = ms->nghbr[(size_t)m*27 + 1*9 + (o[1] + 1)*3 + (o[0] + 1)];
+                  if (gid < 0 || shear_crossing(c, m, o[0])) continue;
+                  A5(f, nvar, d, gid - ms->gids, v, kg, j - o[1]*nx[1], i - o[0]*nx[0]) += val;
+                }
+              }
+        }
+      }
+  /* the shear-periodic faces */
+  if (!ms->shear_x1) return;
+  for (int m = 0; m < ms->nmb; ++m) {
+    if (!sb_faces(ms, m)) continue;
+    for (int v = 0; v < nvar; ++v)
+      for (int k = d.ks; k <= d.ke; ++k)
+        for (int j = d.js; j <= d.je; ++j)
+          for (int i = d.is; i <= d.ie; ++i)
+            shear_remap_entries(c, &d, NULL, nvar, m, v, k, j, i, f,
+                                A5(owned, nvar, d, m, v, k, j, i));
+  }
+}
+
+void oracle_point_force_field(const dustb_ctx *c, const double *owned, double *f) {
+  point_force_field(c, owned, f);
+}
+
+/* GatherPointGravityAcceleration (:316-369): acc[v * acc_stride + p] = the TSC weights of the
+ * particle over the force field */
+unsigned oracle_point_gravity_gather(const dustb_ctx *c, const double *owned, double *acc,
+                                     long long acc_stride) {
+  const dustb_mesh *ms = &c->mesh; const Ind d = indices(ms);
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  (void)pi;
+  double *f = (double *)malloc(field_size(ms, 3)*sizeof(double));
+  point_force_field(c, owned, f);
+  unsigned err = 0;
+  for (int p = 0; p < c->part.npart; ++p) {
+    double a[3] = {0.0, 0.0, 0.0};
+    const double mass = PR(DUSTB_IPM, p);
+    int m, ip, jp, kp; double wx[3], wy[3], wz[3];
+    if (!(mass >= 0.0) || !isfinite(mass)) {
+      err |= DUSTB_ERR_POINT;
+    } else if (mass != 0.0) {
+      if (!point_stencil(c, &d, p, &m, &ip, &jp, &kp, wx, wy, wz)) {
+        err |= DUSTB_ERR_POINT;
+      } else {
+        for (int cc = 0; cc < 3; ++cc)
+          for (int b = 0; b < 3; ++b)
+            for (int q = 0; q < 3; ++q) {
+              const double w = wz[cc]*wy[b]*wx[q];
+              for (int v = 0; v < 3; ++v)
+                a[v] += w*A5(f, 3, d, m, v, kp + cc - 1, jp + b - 1, ip + q - 1);
+            }
+        if (!isfinite(a[0]) || !isfinite(a[1]) || !isfinite(a[2])) err |= DUSTB_ERR_POINT;
+      }
+    }
+    for (int v = 0; v < 3; ++v) acc[(size_t)v*acc_stride + p] = a[v];
+  }
+  free(f);
+  return err;
+}
+
 unsigned oracle_phst(const dustb_ctx *c, const double *chi, double *field, double row[16]) {
   const dustb_mesh *ms = &c->mesh;
   const double *pr = c->part.pr;

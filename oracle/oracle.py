@@ -71,6 +71,10 @@ def lib():
             "oracle_imex_cycle": ([P, D, D, VP, VP], C.c_uint),
             "oracle_pc2_cycle": ([P, D, VP, VP], C.c_uint),
             "oracle_phst": ([P, VP, VP, VP], C.c_uint),
+            "oracle_point_gravity_density": ([P, VP], C.c_uint),
+            "oracle_point_gravity_gather": ([P, VP, VP, C.c_longlong], C.c_uint),
+            "oracle_point_science_fields": ([P, VP, I, I], C.c_uint),
+            "oracle_point_force_field": ([P, VP, VP], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(_lib, name)
@@ -235,6 +239,35 @@ class Oracle:
         ch = None if chi is None else np.array([chi], np.float64)
         err = self.call("phst", capi.ptr(ch), field.ctypes.data, row.ctypes.data)
         return row, err
+
+    # --- point-particle fields (self-gravity, outputs) ---
+    def point_gravity_density(self):
+        """DepositPointGravityDensity: (owned density field, error word)."""
+        owned = np.zeros(self.mesh.field_shape(1))
+        err = self.call("point_gravity_density", owned.ctypes.data)
+        return owned, err
+
+    def point_gravity_gather(self, owned):
+        """GatherPointGravityAcceleration over the owned (nmb, 3, ...) field: (3 x npart, err)."""
+        owned = np.ascontiguousarray(owned, np.float64)
+        n = self.st.npart
+        acc = np.zeros((3, max(n, 1)))
+        err = self.call("point_gravity_gather", owned.ctypes.data, acc.ctypes.data, max(n, 1))
+        return acc[:, :n], err
+
+    def point_force_field(self, owned):
+        """The gather's force field: owned on the active cells, the transposed remap in the
+        ghost cells."""
+        owned = np.ascontiguousarray(owned, np.float64)
+        f = np.zeros(self.mesh.field_shape(3))
+        self.call("point_force_field", owned.ctypes.data, f.ctypes.data)
+        return f
+
+    def point_science_fields(self, mass_only=False, species=-1):
+        """DepositPointScienceFields: (out field with 1 or 4 vars, err)."""
+        out = np.zeros(self.mesh.field_shape(1 if mass_only else 4))
+        err = self.call("point_science_fields", out.ctypes.data, int(mass_only), int(species))
+        return out, err
 
     def momentum(self):
         """Total (gas, dust) momentum vectors over active cells / live particles."""
