@@ -1,6 +1,6 @@
 """Build recipe of the CUDA library athenak_b200/libdustb.so (sm_100a, in-tree).
 
-Every .cu under csrc/ is compiled by nvcc for sm_100a and linked into one shared library
+The .cu files under csrc/ (UNITS) are compiled by nvcc for sm_100a and linked into one shared library
 with C linkage entry points (include/dustb.h).  The FP64 translation units are compiled with
 --fmad=false so their per-particle arithmetic rounds as the CPU oracle's does.
 """
@@ -22,6 +22,7 @@ UNITS = {
     "dustb_sort.cu": [],
     "dustb_mixed.cu": [],
     "dustb_seed.cu": [],
+    "dustb_output.cu": [],
 }
 
 
@@ -62,8 +63,16 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return OUT
 
 
-HOST_SRC = os.path.join(HERE, "host", "dust_gas_drag.cpp")
+HOST_SRCS = [os.path.join(HERE, "host", f) for f in ("dust_gas_drag.cpp", "pbin.cpp")]
+HOST_HDRS = [os.path.join(HERE, "host", f) for f in ("dust_gas_drag.hpp", "pbin.hpp")]
 HOST_LIB = os.path.join(HERE, "libdustb_host.so")
+
+
+def have_zlib() -> bool:
+    """zlib (header and library) for the compressed pbin format (version 3)."""
+    return os.path.exists("/usr/include/zlib.h") and any(
+        os.path.exists(os.path.join(d, "libz.so"))
+        for d in ("/usr/lib/x86_64-linux-gnu", "/usr/lib64", "/usr/lib", "/lib/x86_64-linux-gnu"))
 
 
 def cuda_home() -> str:
@@ -74,13 +83,15 @@ def build_host(force: bool = False) -> str:
     """The C++ host layer (athenak_b200/host: DustGasDrag's task functions over the C ABI)
     as libdustb_host.so, linked against libdustb.so."""
     lib = build(force)
-    hdr = os.path.join(HERE, "host", "dust_gas_drag.hpp")
-    newest = max(os.path.getmtime(p) for p in (HOST_SRC, hdr, lib))
+    newest = max(os.path.getmtime(p) for p in (*HOST_SRCS, *HOST_HDRS, lib))
     if not force and os.path.exists(HOST_LIB) and os.path.getmtime(HOST_LIB) >= newest:
         return HOST_LIB
     cu = cuda_home()
-    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-o", HOST_LIB, HOST_SRC,
-           f"-I{cu}/include", f"-L{HERE}", "-ldustb", f"-L{cu}/lib64", "-lcudart",
+    z = have_zlib()
+    zlink = ["-lz"] if z else []
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-o", HOST_LIB, *HOST_SRCS,
+           f"-DATHENAK_B200_HAVE_ZLIB={1 if z else 0}", "-pthread",
+           f"-I{cu}/include", f"-L{HERE}", "-ldustb", f"-L{cu}/lib64", "-lcudart", *zlink,
            "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{cu}/lib64"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

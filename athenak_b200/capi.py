@@ -171,8 +171,13 @@ SIGNATURES = {
     "dustb_point_gravity_density": [CTXP, VP, VP, VP],
     "dustb_point_gravity_gather": [CTXP, VP, VP, VP, LL, VP],
     "dustb_point_science_fields": [CTXP, VP, VP, I, I, VP],
+    "dustb_pbin_scratch_bytes": [I],
+    "dustb_pbin_rows": [CTXP, VP, VP, D, VP, LL, VP],
+    "dustb_pbin_pack": [CTXP, VP, I, I, I, VP, VP],
+    "dustb_pbin_shuffle": [VP, LL, I, LL, VP, VP],
 }
 RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_phst_scratch_bytes": LL,
+            "dustb_pbin_scratch_bytes": LL,
             "dustb_last_error": C.c_char_p}
 # declared by athenak_b200.mixed (they take its DustbMixedParams struct)
 EXTRA_SIGNATURES = {"dustb_mixed_workspace_bytes", "dustb_mixed_import", "dustb_mixed_export",

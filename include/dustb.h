@@ -282,6 +282,37 @@ int dustb_point_gravity_gather(const dustb_ctx *ctx, const double *owned, double
 int dustb_point_science_fields(const dustb_ctx *ctx, double *out, double *halo, int mass_only,
                                int species, void *stream);
 
+/* ---- the particle science file (pbin, src/outputs/pbin.cpp): its device side -----------
+ * The host writes the file (athenak_b200/host/pbin.hpp); these calls find the active rows
+ * and pack their columns. */
+typedef struct dustb_pbin_stats {
+  long long active_rows;        /* mass != 0 (written) */
+  long long zero_mass_rows;     /* mass == 0 (outflow tombstones, left out) */
+  long long invalid_mass_rows;  /* active rows whose mass is not finite or not > 0 */
+  long long negative_tag_rows;  /* active rows with PTAGH < 0 (tags >= 2^63) */
+  long long differ_rows;        /* active rows whose species is not 0 or t_s not ts0 */
+  double mass_min, mass_max;    /* over the active rows (fmin / fmax: NaN skipped) */
+} dustb_pbin_stats;
+/* the particle columns, in the file's order */
+enum { DUSTB_PBIN_ID = 0, DUSTB_PBIN_SPECIES = 1, DUSTB_PBIN_X1 = 2, DUSTB_PBIN_X2 = 3,
+       DUSTB_PBIN_X3 = 4, DUSTB_PBIN_V1 = 5, DUSTB_PBIN_V2 = 6, DUSTB_PBIN_V3 = 7,
+       DUSTB_PBIN_MASS = 8, DUSTB_PBIN_STOPPING_TIME = 9 };
+long long dustb_pbin_scratch_bytes(int npart);
+/* ParticleBinaryOutput::LoadOutputData (:394-420) and the checks of WriteOutputFile
+ * (:526-560): idx[0..active_rows) = the rows with mass != 0 in array order; *stats (device)
+ * the counts and the mass range (ts0: the t_s of species 0 for the constant check). */
+int dustb_pbin_rows(const dustb_ctx *ctx, int *idx, dustb_pbin_stats *stats, double ts0,
+                    void *scratch, long long scratch_bytes, void *stream);
+/* PackParticleColumns (:322-390): column DUSTB_PBIN_* of rows idx[0..n) into out (device):
+ * ID uint64 (PTAG low word, PTAGH high), SPECIES uint32, the reals float64 or, with single,
+ * float32. */
+int dustb_pbin_pack(const dustb_ctx *ctx, const int *idx, int n, int column, int single,
+                    void *out, void *stream);
+/* ShuffleDeflate's byte shuffle (:243-262) of rows values of itemsize bytes, chunk by chunk
+ * of chunk_rows rows: out[chunk + k * rows_c + i] = in[chunk + i * itemsize + k]. */
+int dustb_pbin_shuffle(const void *in, long long rows, int itemsize, long long chunk_rows,
+                       void *out, void *stream);
+
 /* ---- pc2 (src/dust/dust_pm.cpp:109-194, :374-405, :585-602; dust_push.cpp:37-61,
  * :99-247) ---------------------------------------------------------------------------- */
 int dustb_pc2_predictor(const dustb_ctx *ctx, double dt, int rate_dep, void *stream);
