@@ -225,7 +225,8 @@ def test_device_rows_pack_and_shuffle_through_the_c_abi():
     np.testing.assert_array_equal(ids, tag[act])
     capi.check(lib.dustb_pbin_pack(g.pctx, idx.data_ptr(), k, 1, 0, out.data_ptr(), None), "pack")
     np.testing.assert_array_equal(out[:4 * k].cpu().numpy().view(np.uint32), pi[2, act])
-    # the byte shuffle, chunk by chunk (a ragged last chunk)
+    # the byte shuffle of the id column, chunk by chunk (a ragged last chunk)
+    capi.check(lib.dustb_pbin_pack(g.pctx, idx.data_ptr(), k, 0, 0, out.data_ptr(), None), "pack")
     chunk = 1000
     sh = torch.empty_like(out)
     capi.check(lib.dustb_pbin_shuffle(out.data_ptr(), k, 8, chunk, sh.data_ptr(), None), "shuffle")
