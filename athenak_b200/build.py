@@ -63,8 +63,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return OUT
 
 
-HOST_SRCS = [os.path.join(HERE, "host", f) for f in ("dust_gas_drag.cpp", "pbin.cpp")]
-HOST_HDRS = [os.path.join(HERE, "host", f) for f in ("dust_gas_drag.hpp", "pbin.hpp")]
+HOST_SRCS = [os.path.join(HERE, "host", f) for f in ("dust_gas_drag.cpp", "pbin.cpp",
+                                                      "restart.cpp")]
+HOST_HDRS = [os.path.join(HERE, "host", f) for f in ("dust_gas_drag.hpp", "pbin.hpp",
+                                                      "restart.hpp")]
 HOST_LIB = os.path.join(HERE, "libdustb_host.so")
 
 

@@ -1,0 +1,302 @@
+// restart.cpp -- the particle section of the restart file; see restart.hpp.
+#include "restart.hpp"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+namespace athenak_b200 {
+namespace {
+
+const char kMagic[9] = "AKPRST01";
+constexpr std::int32_t kVersion = 2;
+constexpr std::size_t kHeadBytes = 8 + 6 * sizeof(std::int32_t) + sizeof(std::uint64_t);
+constexpr std::size_t kStateMax = 0x7fffffff;   // the dust state's length is an int32
+constexpr int kNReal = 17, kNInt = 5;
+
+void Put(std::vector<char> &b, const void *p, std::size_t n) {
+  const char *c = static_cast<const char *>(p);
+  b.insert(b.end(), c, c + n);
+}
+template <typename T>
+void PutValue(std::vector<char> &b, const T &v) { Put(b, &v, sizeof(T)); }
+void PutRecord(std::vector<char> &b, const char *name, const void *p, std::size_t n) {
+  char key[16] = {0};
+  std::strncpy(key, name, 15);
+  Put(b, key, 16);
+  PutValue(b, static_cast<std::int32_t>(n));
+  Put(b, p, n);
+}
+
+// the dust records in the reference's order (PackRestartState, then the cell-order index)
+void PackState(const ParticleRestartState &s, std::vector<char> &b) {
+  const std::uint64_t ts[3] = {s.next_tag_set ? 1ULL : 0ULL, s.next_tag, s.tag_bound};
+  PutRecord(b, "tag_state", ts, sizeof(ts));
+  const std::int32_t rb[3] = {s.rank, s.gids, s.nmb};
+  PutRecord(b, "rank_blocks", rb, sizeof(rb));
+  PutRecord(b, "merge_pass", &s.merge_pass, sizeof(s.merge_pass));
+  PutRecord(b, "species_table", s.species_table.data(), s.species_table.size());
+  if (!s.mroot.empty()) PutRecord(b, "mroot", s.mroot.data(), s.mroot.size() * sizeof(double));
+  if (!s.imex_mown.empty())
+    PutRecord(b, "imex_mown", s.imex_mown.data(), s.imex_mown.size() * sizeof(double));
+  PutRecord(b, "resample", s.resample, sizeof(s.resample));
+  char clk[sizeof(s.resample_clk_r) + sizeof(s.resample_clk_n)];
+  std::memcpy(clk, s.resample_clk_r, sizeof(s.resample_clk_r));
+  std::memcpy(clk + sizeof(s.resample_clk_r), s.resample_clk_n, sizeof(s.resample_clk_n));
+  PutRecord(b, "resample_clk", clk, sizeof(clk));
+  char mclk[sizeof(s.merge_clk_r) + sizeof(s.merge_clk_n)];
+  std::memcpy(mclk, s.merge_clk_r, sizeof(s.merge_clk_r));
+  std::memcpy(mclk + sizeof(s.merge_clk_r), s.merge_clk_n, sizeof(s.merge_clk_n));
+  PutRecord(b, "merge_clk", mclk, sizeof(mclk));
+  if (!s.amr_state.empty())
+    PutRecord(b, "amr_state", s.amr_state.data(), s.amr_state.size() * sizeof(std::int32_t));
+  PutRecord(b, "split", s.split, sizeof(s.split));
+  PutRecord(b, "coarsen_n", s.coarsen, sizeof(s.coarsen));
+  PutRecord(b, "amr_regrids", &s.amr_regrids, sizeof(s.amr_regrids));
+  PutRecord(b, "regrid_evt", s.regrid_evt, sizeof(s.regrid_evt));
+  PutRecord(b, "regrid_evt_t", s.regrid_evt_t, sizeof(s.regrid_evt_t));
+  std::vector<double> led(5 + s.dropped_sum.size());
+  led[0] = s.x3_outflow_mass; led[1] = s.x3_outflow_count;
+  led[2] = s.x3_removed[0]; led[3] = s.x3_removed[1];
+  led[4] = static_cast<double>(s.dropped_sum.size());
+  for (std::size_t v = 0; v < s.dropped_sum.size(); ++v) led[5 + v] = s.dropped_sum[v];
+  PutRecord(b, "x3_ledger", led.data(), led.size() * sizeof(double));
+  if (s.cloud_ord_status != 0) {
+    const bool stored = s.cloud_ord_status == 1;
+    const std::int32_t info[3] = {s.cloud_ord_status,
+                                  stored ? static_cast<std::int32_t>(s.cloud_ord.size()) : 0,
+                                  s.cloud_ord_sort_cycle};
+    PutRecord(b, "cloud_ord_n", info, sizeof(info));
+    if (stored) {
+      PutRecord(b, "cloud_ord", s.cloud_ord.data(), s.cloud_ord.size() * sizeof(std::int32_t));
+      PutRecord(b, "cloud_ord_tag", s.cloud_ord_tag.data(),
+                s.cloud_ord_tag.size() * sizeof(std::uint64_t));
+    }
+  }
+}
+
+// UnpackRestartState's reading of the records; "" or the error
+std::string UnpackState(const char *p, std::size_t nbytes, ParticleRestartSection &sec) {
+  ParticleRestartState &s = sec.state;
+  bool species_found = false;
+  std::size_t at = 0;
+  while (at + 16 + sizeof(std::int32_t) <= nbytes) {
+    char key[17] = {0};
+    std::memcpy(key, p + at, 16);
+    std::int32_t n = 0;
+    std::memcpy(&n, p + at + 16, sizeof(n));
+    const char *d = p + at + 16 + sizeof(n);
+    if (n < 0 || at + 16 + sizeof(n) + static_cast<std::size_t>(n) > nbytes)
+      return "dust record runs past the end";
+    const std::string name(key);
+    const std::size_t sz = static_cast<std::size_t>(n);
+    auto fixed = [&](void *dst, std::size_t want) {
+      if (sz != want) return false;
+      std::memcpy(dst, d, want);
+      return true;
+    };
+    bool ok = true;
+    if (name == "next_tag") {                    // version 1: int32 counter (-1: not set)
+      std::int32_t v = 0;
+      ok = fixed(&v, sizeof(v));
+      s.next_tag_set = v >= 0;
+      s.next_tag = v >= 0 ? static_cast<std::uint64_t>(v) : 0;
+    } else if (name == "tag_state") {
+      std::uint64_t v[3];
+      ok = fixed(v, sizeof(v));
+      s.next_tag_set = v[0] != 0; s.next_tag = v[1]; s.tag_bound = v[2];
+    } else if (name == "rank_blocks") {
+      std::int32_t v[3];
+      ok = fixed(v, sizeof(v));
+      s.rank = v[0]; s.gids = v[1]; s.nmb = v[2];
+    } else if (name == "merge_pass") {
+      ok = fixed(&s.merge_pass, sizeof(s.merge_pass));
+    } else if (name == "species_table") {
+      species_found = true;
+      s.species_table.assign(d, sz);
+    } else if (name == "mroot" || name == "imex_mown") {
+      ok = sz % sizeof(double) == 0;
+      auto &v = (name == "mroot") ? s.mroot : s.imex_mown;
+      v.resize(sz / sizeof(double));
+      if (ok && sz) std::memcpy(v.data(), d, sz);
+    } else if (name == "resample") {
+      ok = fixed(s.resample, sizeof(s.resample));
+    } else if (name == "resample_clk") {
+      ok = sz == sizeof(s.resample_clk_r) + sizeof(s.resample_clk_n);
+      if (ok) {
+        std::memcpy(s.resample_clk_r, d, sizeof(s.resample_clk_r));
+        std::memcpy(s.resample_clk_n, d + sizeof(s.resample_clk_r), sizeof(s.resample_clk_n));
+      }
+    } else if (name == "merge_clk") {
+      ok = sz == sizeof(s.merge_clk_r) + sizeof(s.merge_clk_n);
+      if (ok) {
+        std::memcpy(s.merge_clk_r, d, sizeof(s.merge_clk_r));
+        std::memcpy(s.merge_clk_n, d + sizeof(s.merge_clk_r), sizeof(s.merge_clk_n));
+      }
+    } else if (name == "amr_state") {
+      ok = sz >= 2 * sizeof(std::int32_t) && sz % sizeof(std::int32_t) == 0;
+      if (ok) {
+        s.amr_state.resize(sz / sizeof(std::int32_t));
+        std::memcpy(s.amr_state.data(), d, sz);
+        ok = static_cast<std::size_t>(s.amr_state[1]) + 2 == s.amr_state.size();
+      }
+    } else if (name == "split") {
+      ok = fixed(s.split, sizeof(s.split));
+    } else if (name == "coarsen_n") {
+      ok = fixed(s.coarsen, sizeof(s.coarsen));
+    } else if (name == "amr_regrids") {
+      ok = fixed(&s.amr_regrids, sizeof(s.amr_regrids));
+    } else if (name == "regrid_evt") {
+      ok = fixed(s.regrid_evt, sizeof(s.regrid_evt));
+    } else if (name == "regrid_evt_t") {
+      ok = fixed(s.regrid_evt_t, sizeof(s.regrid_evt_t));
+    } else if (name == "x3_ledger") {
+      ok = sz >= 5 * sizeof(double) && sz % sizeof(double) == 0;
+      if (ok) {
+        std::vector<double> led(sz / sizeof(double));
+        std::memcpy(led.data(), d, sz);
+        const int nd = static_cast<int>(led[4]);
+        ok = nd >= 0 && static_cast<std::size_t>(5 + nd) == led.size();
+        if (ok) {
+          s.x3_outflow_mass = led[0]; s.x3_outflow_count = led[1];
+          s.x3_removed[0] = led[2]; s.x3_removed[1] = led[3];
+          s.dropped_sum.assign(led.begin() + 5, led.end());
+        }
+      }
+    } else if (name == "cloud_ord_n") {
+      std::int32_t v[3];
+      ok = fixed(v, sizeof(v));
+      s.cloud_ord_status = v[0]; s.cloud_ord_sort_cycle = v[2];
+    } else if (name == "cloud_ord") {
+      ok = sz % sizeof(std::int32_t) == 0;
+      s.cloud_ord.resize(sz / sizeof(std::int32_t));
+      if (ok && sz) std::memcpy(s.cloud_ord.data(), d, sz);
+    } else if (name == "cloud_ord_tag") {
+      ok = sz % sizeof(std::uint64_t) == 0;
+      s.cloud_ord_tag.resize(sz / sizeof(std::uint64_t));
+      if (ok && sz) std::memcpy(s.cloud_ord_tag.data(), d, sz);
+    } else {
+      s.other.emplace_back(name, std::vector<char>(d, d + sz));
+      sec.notes.push_back("record '" + name + "' is not known to this code and is kept as read");
+    }
+    if (!ok) return "dust record " + name + " has an unexpected size";
+    at += 16 + sizeof(n) + sz;
+  }
+  if (!species_found) sec.notes.push_back("no record species_table (an older file)");
+  // the index must be a whole group: stored with both arrays of its length
+  if (s.cloud_ord_status == 1 &&
+      (s.cloud_ord.size() != s.cloud_ord_tag.size() || s.cloud_ord.empty())) {
+    sec.notes.push_back("cloud order records are incomplete: the index is rebuilt");
+    s.cloud_ord_status = 0;
+    s.cloud_ord.clear();
+    s.cloud_ord_tag.clear();
+  }
+  return "";
+}
+
+}  // namespace
+
+std::string PackParticleRestartRows(const double *pr, const int *pi, long long stride,
+                                    std::int64_t np, double dtnew,
+                                    const ParticleRestartState &st, std::vector<char> &buf) {
+  if (np < 0 || stride < np || (np > 0 && (!pr || !pi))) return "restart: bad particle rows";
+  std::vector<char> state;
+  PackState(st, state);
+  if (state.size() > kStateMax) return "restart: the dust records exceed the int32 length";
+  buf.clear();
+  const std::uint64_t rows = static_cast<std::uint64_t>(np) * (kNReal * sizeof(double) +
+                                                               kNInt * sizeof(int));
+  const std::uint64_t total = kHeadBytes + sizeof(std::int64_t) + sizeof(double) +
+                              sizeof(std::int32_t) + state.size() + rows + 8;
+  buf.reserve(total);
+  Put(buf, kMagic, 8);
+  const std::int32_t head[6] = {kVersion, static_cast<std::int32_t>(sizeof(double)),
+                                static_cast<std::int32_t>(sizeof(int)), 1, kNReal, kNInt};
+  Put(buf, head, sizeof(head));
+  PutValue(buf, total);
+  PutValue(buf, np);
+  PutValue(buf, dtnew);
+  PutValue(buf, static_cast<std::int32_t>(state.size()));
+  Put(buf, state.data(), state.size());
+  for (int c = 0; c < kNReal; ++c) Put(buf, pr + (std::size_t)c * stride, (std::size_t)np * sizeof(double));
+  for (int c = 0; c < kNInt; ++c) Put(buf, pi + (std::size_t)c * stride, (std::size_t)np * sizeof(int));
+  Put(buf, kMagic, 8);
+  if (buf.size() != total) return "restart: internal size mismatch";
+  return "";
+}
+
+std::string PackParticleRestart(const dustb_ctx &ctx, void *stream, double dtnew,
+                                const ParticleRestartState &st, std::vector<char> &buf) {
+  const std::int64_t np = ctx.part.npart;
+  std::vector<double> pr((std::size_t)np * kNReal);
+  std::vector<int> pi((std::size_t)np * kNInt);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (int c = 0; c < kNReal && np > 0; ++c)
+    if (cudaMemcpyAsync(pr.data() + (std::size_t)c * np, ctx.part.pr + (std::size_t)c * ctx.part.stride,
+                        (std::size_t)np * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      return "restart: particle rows not copied";
+  for (int c = 0; c < kNInt && np > 0; ++c)
+    if (cudaMemcpyAsync(pi.data() + (std::size_t)c * np, ctx.part.pi + (std::size_t)c * ctx.part.stride,
+                        (std::size_t)np * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      return "restart: particle rows not copied";
+  if (cudaStreamSynchronize(s) != cudaSuccess) return "restart: particle rows not copied";
+  return PackParticleRestartRows(pr.data(), pi.data(), np, np, dtnew, st, buf);
+}
+
+std::string ParseParticleRestart(const std::vector<char> &buf, ParticleRestartSection &out) {
+  out = ParticleRestartSection();
+  if (buf.size() < kHeadBytes + 8 || std::memcmp(buf.data(), kMagic, 8) != 0 ||
+      std::memcmp(buf.data() + buf.size() - 8, kMagic, 8) != 0)
+    return "restart: missing or truncated particle section (no head or end marker)";
+  std::int32_t head[6];
+  std::memcpy(head, buf.data() + 8, sizeof(head));
+  std::uint64_t total = 0;
+  std::memcpy(&total, buf.data() + 8 + sizeof(head), sizeof(total));
+  const bool columns_ok = head[5] == kNInt || (head[0] == 1 && head[5] == kNInt - 1);
+  if ((head[0] != 1 && head[0] != 2) || head[1] != (std::int32_t)sizeof(double) ||
+      head[2] != (std::int32_t)sizeof(int) || head[3] != 1 || head[4] != kNReal || !columns_ok)
+    return "restart: version, type sizes, rank count or particle columns do not match (file: "
+           "version " + std::to_string(head[0]) + ", Real " + std::to_string(head[1]) +
+           " bytes, int " + std::to_string(head[2]) + " bytes, ranks " + std::to_string(head[3]) +
+           ", nrdata " + std::to_string(head[4]) + ", nidata " + std::to_string(head[5]) + ")";
+  out.version = head[0]; out.ranks = head[3]; out.nrdata = head[4]; out.nidata = head[5];
+  std::size_t at = kHeadBytes;
+  std::int32_t nstate = 0;
+  std::memcpy(&out.np, buf.data() + at, sizeof(out.np)); at += sizeof(out.np);
+  std::memcpy(&out.dtnew, buf.data() + at, sizeof(out.dtnew)); at += sizeof(out.dtnew);
+  std::memcpy(&nstate, buf.data() + at, sizeof(nstate)); at += sizeof(nstate);
+  if (out.np < 0 || nstate < 0) return "restart: sizes inside the section are inconsistent";
+  const std::size_t need = at + (std::size_t)nstate +
+                           (std::size_t)out.np * (kNReal * sizeof(double) + out.nidata * sizeof(int)) + 8;
+  if (need != buf.size() || total != buf.size())
+    return "restart: sizes inside the section are inconsistent";
+  std::string err = UnpackState(buf.data() + at, (std::size_t)nstate, out);
+  if (!err.empty()) return "restart: " + err;
+  at += (std::size_t)nstate;
+  const std::size_t n = (std::size_t)out.np;
+  out.pr.resize(n * kNReal);
+  if (n) std::memcpy(out.pr.data(), buf.data() + at, n * kNReal * sizeof(double));
+  at += n * kNReal * sizeof(double);
+  out.pi.assign(n * kNInt, 0);   // version 1: PTAGH (the last row) stays 0
+  if (n) std::memcpy(out.pi.data(), buf.data() + at, n * out.nidata * sizeof(int));
+  return "";
+}
+
+std::string RestoreParticleRows(const ParticleRestartSection &sec, dustb_ctx &ctx, void *stream) {
+  const std::int64_t np = sec.np;
+  if (np > ctx.part.stride) return "restart: the particle arrays cannot hold the section's rows";
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (int c = 0; c < kNReal && np > 0; ++c)
+    if (cudaMemcpyAsync(ctx.part.pr + (std::size_t)c * ctx.part.stride, sec.pr.data() + (std::size_t)c * np,
+                        (std::size_t)np * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return "restart: particle rows not restored";
+  for (int c = 0; c < kNInt && np > 0; ++c)
+    if (cudaMemcpyAsync(ctx.part.pi + (std::size_t)c * ctx.part.stride, sec.pi.data() + (std::size_t)c * np,
+                        (std::size_t)np * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return "restart: particle rows not restored";
+  if (cudaStreamSynchronize(s) != cudaSuccess) return "restart: particle rows not restored";
+  ctx.part.npart = static_cast<int>(np);
+  return "";
+}
+
+}  // namespace athenak_b200
