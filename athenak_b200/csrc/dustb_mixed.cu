@@ -277,10 +277,15 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // CTA barrier assumes converged warps)
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned *err,
                                           unsigned mask) {
-  const unsigned long long t0 = global_ns();
+  // (the clock is read every 1024 polls only: a completed copy costs no clock read)
+  unsigned long long t0 = 0;
   for (int it = 0; it < (1 << 22); ++it) {
     if (__all_sync(mask, mbar_try_wait(bar, parity))) return true;
-    if (__any_sync(mask, global_ns() - t0 > 200000000ull)) break;
+    if ((it & 1023) == 1023) {
+      const unsigned long long t = global_ns();
+      if (it == 1023) t0 = t;
+      else if (__any_sync(mask, t - t0 > 200000000ull)) break;
+    }
   }
   report(err, DUSTB_ERR_TIMEOUT);
   return false;
@@ -813,11 +818,13 @@ constexpr int kTileRows = 8;
 // the index of variable 0 of block-local cell (kk, jj, ii) of block m in a field of nvar
 // variables, or -1 if no block owns it; a cell one beyond the block maps to the owning
 // neighbour's active cell (the ghost exchanges folded into the index)
+// GH: bit 0 ghost mode; (tiles) bit 1 the imex stage's implicit shear shift, compiled in only
+// where it is used
 template <int GH>
 __device__ __forceinline__ long long cell_at(const Geo &G, int m, int nvar, int kk, int jj, int ii) {
   // (ghost mode: the block's own cell, ghost cells included; the window reaches one cell
   // beyond the block and every block has at least two ghost layers)
-  if (GH) return G.at(m, nvar, 0, G.ks + kk, G.js + jj, G.is + ii);
+  if (GH & 1) return G.at(m, nvar, 0, G.ks + kk, G.js + jj, G.is + ii);
   int mo;
   if (!G.owner(m, kk, jj, ii, mo)) return -1;
   return G.at(mo, nvar, 0, G.ks + kk, G.js + jj, G.is + ii);
@@ -1190,7 +1197,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
     // the y offset of the weights: the particle's own, or (an imex stage with an implicit
     // shear shift) that of y + sh x, which the push kept inside the particle's cell
     auto oy_at = [&](int r) -> float {
-      return (T.shy != 0.0f) ? shifted_oy(G, T.shy, m, ci_l, s_f[r], s_f[CH + r]) : s_f[CH + r];
+      return (GH & 2) ? shifted_oy(G, T.shy, m, ci_l, s_f[r], s_f[CH + r]) : s_f[CH + r];
     };
     GatherWindow<D3> win;
     if (MODE != MODE_QP) win.template load<GH>(G, T.gfield, m, k, jrow, ci_l);   // while the copies fly
@@ -1594,6 +1601,13 @@ int launch_tile(const MState &S, const PBuf &cur, const Geo &G, const Cfg &cf, T
   if (G.three_d) {
     // (ghost mode: physical x3 or shear-periodic x1 faces, 3-D only)
     if (G.ghost) {
+      // (an implicit shear shift comes only with shear-periodic faces: ghost mode)
+      constexpr bool kImex = MODE == MODE_QP || MODE == MODE_OP || MODE == MODE_KICK;
+      if (kImex && T.shy != 0.0f) {
+        if (G.scheme == 2) return launch_tile_d<MODE, 1, 2, 3>(G, cf, cur, T, st);
+        if (G.scheme == 1) return launch_tile_d<MODE, 1, 1, 3>(G, cf, cur, T, st);
+        return launch_tile_d<MODE, 1, 0, 3>(G, cf, cur, T, st);
+      }
       if (G.scheme == 2) return launch_tile_d<MODE, 1, 2, 1>(G, cf, cur, T, st);
       if (G.scheme == 1) return launch_tile_d<MODE, 1, 1, 1>(G, cf, cur, T, st);
       return launch_tile_d<MODE, 1, 0, 1>(G, cf, cur, T, st);
