@@ -1592,33 +1592,33 @@ int launch_tile_d(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &
   return dustb_host::launch_status("mixed tile");
 }
 
+// the kernel of one dimensionality, ghost mode (GH bit 0) and implicit-shift form (bit 1)
+template <int MODE, int D3, int GH>
+int launch_tile_s(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &T, cudaStream_t st) {
+  if (G.scheme == 2) return launch_tile_d<MODE, D3, 2, GH>(G, cf, cur, T, st);
+  if (G.scheme == 1) return launch_tile_d<MODE, D3, 1, GH>(G, cf, cur, T, st);
+  return launch_tile_d<MODE, D3, 0, GH>(G, cf, cur, T, st);
+}
+
 template <int MODE>
 int launch_tile(const MState &S, const PBuf &cur, const Geo &G, const Cfg &cf, TileArgs T,
                 cudaStream_t st) {
   T.tj = cf.tj; T.chunk = cf.chunk; T.tpp = cf.tpp; T.cstart = S.cstart;
   T.probe_timeout = cf.probe_timeout;
-  // one kernel per dimensionality and deposit scheme (no per-particle scheme selection)
-  if (G.three_d) {
-    // (ghost mode: physical x3 or shear-periodic x1 faces, 3-D only)
-    if (G.ghost) {
-      // (an implicit shear shift comes only with shear-periodic faces: ghost mode)
-      constexpr bool kImex = MODE == MODE_QP || MODE == MODE_OP || MODE == MODE_KICK;
-      if (kImex && T.shy != 0.0f) {
-        if (G.scheme == 2) return launch_tile_d<MODE, 1, 2, 3>(G, cf, cur, T, st);
-        if (G.scheme == 1) return launch_tile_d<MODE, 1, 1, 3>(G, cf, cur, T, st);
-        return launch_tile_d<MODE, 1, 0, 3>(G, cf, cur, T, st);
-      }
-      if (G.scheme == 2) return launch_tile_d<MODE, 1, 2, 1>(G, cf, cur, T, st);
-      if (G.scheme == 1) return launch_tile_d<MODE, 1, 1, 1>(G, cf, cur, T, st);
-      return launch_tile_d<MODE, 1, 0, 1>(G, cf, cur, T, st);
+  // one kernel per dimensionality and deposit scheme (no per-particle scheme selection); the
+  // weights shifted by an imex stage's implicit shear shift only in the kernels of that form
+  constexpr bool kImex = MODE == MODE_QP || MODE == MODE_OP || MODE == MODE_KICK;
+  if constexpr (kImex) {
+    if (T.shy != 0.0f) {
+      if (!G.three_d) return launch_tile_s<MODE, 0, 2>(G, cf, cur, T, st);
+      return G.ghost ? launch_tile_s<MODE, 1, 3>(G, cf, cur, T, st)
+                     : launch_tile_s<MODE, 1, 2>(G, cf, cur, T, st);
     }
-    if (G.scheme == 2) return launch_tile_d<MODE, 1, 2, 0>(G, cf, cur, T, st);
-    if (G.scheme == 1) return launch_tile_d<MODE, 1, 1, 0>(G, cf, cur, T, st);
-    return launch_tile_d<MODE, 1, 0, 0>(G, cf, cur, T, st);
   }
-  if (G.scheme == 2) return launch_tile_d<MODE, 0, 2, 0>(G, cf, cur, T, st);
-  if (G.scheme == 1) return launch_tile_d<MODE, 0, 1, 0>(G, cf, cur, T, st);
-  return launch_tile_d<MODE, 0, 0, 0>(G, cf, cur, T, st);
+  // (ghost mode: physical x3 or shear-periodic x1 faces, 3-D only)
+  if (!G.three_d) return launch_tile_s<MODE, 0, 0>(G, cf, cur, T, st);
+  return G.ghost ? launch_tile_s<MODE, 1, 1>(G, cf, cur, T, st)
+                 : launch_tile_s<MODE, 1, 0>(G, cf, cur, T, st);
 }
 
 // the edge bin of an imex stage with an implicit shear shift (after the mode's tiles)
