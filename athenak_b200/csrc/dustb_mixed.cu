@@ -311,7 +311,12 @@ __global__ void k_import(const double *pr, const int *pi, long long stride, int 
   for (int a = 0; a < (G.three_d ? 3 : 2); ++a) {
     const double cell = (x[a] - sz[a]) * ((double)nx[a] / (sz[3 + a] - sz[a]));
     int ig = (int)(cell + 1.0) - 1;
-    if (ig < 0 || ig >= nx[a]) { report(err, DUSTB_ERR_HALO); ig = ig < 0 ? 0 : nx[a] - 1; }
+    if (ig < 0 || ig >= nx[a]) {
+      // a position inside the block's box [min, max) whose cell rounded onto the upper face
+      // (one ulp below it) is clamped into the last cell; one outside the box is an error
+      if (!(x[a] >= sz[a] && x[a] < sz[3 + a])) report(err, DUSTB_ERR_HALO);
+      ig = ig < 0 ? 0 : nx[a] - 1;
+    }
     float fo = (float)(cell - (double)ig);
     if (!(fo >= 0.0f)) fo = 0.0f;
     if (fo >= 1.0f) fo = 0.99999994f;
