@@ -220,10 +220,11 @@ def load_traffic():
     return {}
 
 
-def run_ours(args, rank, world):
+def run_ours(args, rep):
     import numpy as np
     import torch
     from athenak_b200.mixed import MixedDust
+    rank, world = rep.rank, rep.world
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     stream = torch.cuda.current_stream()
     if args.pc2_only:
@@ -236,18 +237,7 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     res = {}
 
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def maxall(x):
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([x], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
+    barrier, maxall = rep.barrier, rep.max_over_ranks
 
     # snapshot of the initial state (both forms start from it)
     pr0, pi0, u00 = dev.t["pr"].clone(), dev.t["pi"].clone(), dev.t["u0"].clone()
@@ -301,7 +291,7 @@ def run_ours(args, rank, world):
     torch.cuda.empty_cache()
     if args.mixed_only:
         if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": npart * world / (ms_mixed * 1e-3),
+            print(json.dumps({"metric": METRIC, "value": rep.throughput(npart, ms_mixed),
                               "unit": UNIT, "ms_per_step": ms_mixed, "steps": args.steps,
                               "config": {"cells": W["ncell"], "particles": npart},
                               "kernels": {k: v for k, v in ktimes.items()},
@@ -369,8 +359,8 @@ def run_ours(args, rank, world):
     total_ms = sum(v[0] for v in ktimes.values()) or 1.0
     shares = {k: {"ms_per_step": round(v[0] / nk, 3), "launches_per_step": v[1] / nk,
                   "share": round(v[0] / total_ms, 3)} for k, v in ktimes.items() if v[1]}
-    steps_per_s = npart * world / (ms_mixed * 1e-3)
-    fp64_rate = npart * world / (ms_fp64 * 1e-3)
+    steps_per_s = rep.throughput(npart, ms_mixed)
+    fp64_rate = rep.throughput(npart, ms_fp64)
     # kernels of ours per mixed cycle (dc1, consistent split): per stage gas update, count,
     # scan (3), move, Q/P tile, solve, operator tile, correction, kick tile, consistent gas
     # = 12, stage 2 adds the history term, and one ghost exchange of u0 closes the cycle:
@@ -652,18 +642,12 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    from athenak_b200.replicas import Replicas
+    rep = Replicas(world, rank, backend="nccl", timeout_s=600)
     try:
-        run_ours(args, rank, world)
+        run_ours(args, rep)
     finally:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        rep.close()
 
 
 if __name__ == "__main__":
