@@ -12,7 +12,7 @@ DUSTB_NGP, DUSTB_CIC, DUSTB_TSC = 0, 1, 2
 SOLVER_LOCAL, SOLVER_APPLYA, SOLVER_DC1, SOLVER_DC2 = 0, 1, 2, 3
 X3_PERIODIC, X3_REFLECT, X3_OUTFLOW = 0, 1, 2
 ERR_HALO, ERR_ROUTE, ERR_NGHBR, ERR_PGID, ERR_TSTOP, ERR_WINDOW = 1, 2, 4, 8, 16, 32
-ERR_TIMEOUT, ERR_POINT = 64, 128
+ERR_TIMEOUT, ERR_POINT, ERR_CLOUD = 64, 128, 256
 
 
 class DustbMesh(C.Structure):
@@ -171,13 +171,16 @@ SIGNATURES = {
     "dustb_point_gravity_density": [CTXP, VP, VP, VP],
     "dustb_point_gravity_gather": [CTXP, VP, VP, VP, LL, VP],
     "dustb_point_science_fields": [CTXP, VP, VP, I, I, VP],
+    "dustb_cloud_deposit_qp": [CTXP, D, D, VP],
+    "dustb_cloud_gpack_bytes": [MESHP],
+    "dustb_cloud_gather_kick": [CTXP, D, D, VP, VP],
     "dustb_pbin_scratch_bytes": [I],
     "dustb_pbin_rows": [CTXP, VP, VP, D, VP, LL, VP],
     "dustb_pbin_pack": [CTXP, VP, I, I, I, VP, VP],
     "dustb_pbin_shuffle": [VP, LL, I, LL, VP, VP],
 }
 RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_phst_scratch_bytes": LL,
-            "dustb_pbin_scratch_bytes": LL,
+            "dustb_pbin_scratch_bytes": LL, "dustb_cloud_gpack_bytes": LL,
             "dustb_last_error": C.c_char_p}
 # declared by athenak_b200.mixed (they take its DustbMixedParams struct)
 EXTRA_SIGNATURES = {"dustb_mixed_workspace_bytes", "dustb_mixed_import", "dustb_mixed_export",

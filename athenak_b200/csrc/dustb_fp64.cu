@@ -1283,6 +1283,223 @@ __global__ void k_point_gather(PCtx P, MCtx M, Ind d, const double *f, double *a
   for (int v = 0; v < 3; ++v) acc[(long long)v * astride + p] = a[v];
 }
 
+// ---- refinable clouds on a uniform 3-D mesh: plain P1 hat clouds --------------------------
+// CloudShape1D (src/dust/dust.hpp:240-298; HatCDF / HatMoment :169-182) for a cloud without
+// lobes: along each direction the hat of half-width ell = dx / 2^level about the particle, a
+// cell's weight the difference of the hat CDF at its faces, its first moment about the
+// particle ell times the difference of the moment antiderivative.  LeafTraversal3D::ForEach
+// (src/dust/dust_leaf3d.hpp:368-513) on a uniform mesh: the cells of the block and of its
+// same-level neighbours under the support, each cell's faces from its own block's origin (the
+// neighbour's periodic image next to the block), leaves in the order z, y, x (lower neighbour,
+// block, upper neighbour along each), zero-weight leaves skipped.
+__device__ __forceinline__ double hat_cdf(double s) {
+  if (s <= -1.0) return 0.0;
+  if (s >= 1.0) return 1.0;
+  return (s <= 0.0) ? 0.5 * (1.0 + s) * (1.0 + s) : 1.0 - 0.5 * (1.0 - s) * (1.0 - s);
+}
+__device__ __forceinline__ double hat_moment(double s) {
+  if (s <= -1.0 || s >= 1.0) return 1.0 / 6.0;
+  return (s <= 0.0) ? 0.5 * (s * s) + (s * s) * s / 3.0 : 0.5 * (s * s) - (s * s) * s / 3.0;
+}
+
+struct CloudAxis {
+  int n;
+  int o[6], i[6];
+  double w[6], g[6];
+};
+
+__device__ void cloud_axis(const MCtx &M, const Ind &d, int m, int a, double x, int lev,
+                           double L, CloudAxis &A) {
+  const int nx = (a == 0) ? d.nx1 : ((a == 1) ? d.nx2 : d.nx3);
+  const double dx = M.s(m, DX1 + a), idx = 1.0 / dx;
+  const double ell = ldexp(dx, -lev), inv = ldexp(idx, lev);
+  const double lo = x - ell, hi = x + ell;
+  A.n = 0;
+  for (int o = -1; o <= 1; ++o) {
+    int b = m;
+    if (o != 0) {
+      const int gid = M.nghbr[(long long)m * 27 + dir_slot(a == 0 ? o : 0, a == 1 ? o : 0,
+                                                           a == 2 ? o : 0)];
+      if (gid < 0 || gid - M.gids < 0 || gid - M.gids >= d.nmb) continue;
+      b = gid - M.gids;
+    }
+    double bx0 = M.s(b, X1MIN + a);
+    if (o < 0 && M.s(b, X1MIN + a) >= M.s(m, X1MIN + a)) bx0 -= L;
+    if (o > 0 && M.s(b, X1MIN + a) <= M.s(m, X1MIN + a)) bx0 += L;
+    int i0 = (int)floor((lo - bx0) * idx), i1 = (int)ceil((hi - bx0) * idx) - 1;
+    i0 = (i0 < 0) ? 0 : i0;
+    i1 = (i1 > nx - 1) ? nx - 1 : i1;
+    for (int i = i0; i <= i1 && A.n < 6; ++i) {
+      const double za = (bx0 + i * dx - x) * inv, zb = (bx0 + (i + 1) * dx - x) * inv;
+      A.o[A.n] = o; A.i[A.n] = i;
+      A.w[A.n] = hat_cdf(zb) - hat_cdf(za);
+      A.g[A.n] = ell * (hat_moment(zb) - hat_moment(za));
+      ++A.n;
+    }
+  }
+}
+
+// the cloud's position in the frame of its block (Frame), and whether this build takes it: a
+// level code without lobe bits and a position inside the block
+__device__ bool cloud_load(const PCtx &P, const MCtx &M, const Ind &d, int p, double sh,
+                           const double L[3], int &m, double x[3], int &lev) {
+  m = P.i(DUSTB_PGID, p) - M.gids;
+  lev = P.i(DUSTB_PLEV, p);
+  x[0] = P.r(DUSTB_IPX, p);
+  x[1] = P.r(DUSTB_IPY, p) + sh * P.r(DUSTB_IPX, p);
+  x[2] = P.r(DUSTB_IPZ, p);
+  if (!block_ok(d, m) || (lev & ~15) != 0) return false;
+  const int nx[3] = {d.nx1, d.nx2, d.nx3};
+  for (int a = 0; a < 3; ++a) {
+    const double cx = M.s(m, X1MIN + a) + 0.5 * nx[a] * M.s(m, DX1 + a);
+    x[a] -= L[a] * round((x[a] - cx) * (1.0 / L[a]));
+    if (!(x[a] >= M.s(m, X1MIN + a) && x[a] < M.s(m, X1MAX + a))) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ int cloud_owner(const MCtx &M, const Ind &d, int m, int ox, int oy,
+                                           int oz) {
+  if (!ox && !oy && !oz) return m;
+  const int gid = M.nghbr[(long long)m * 27 + dir_slot(ox, oy, oz)];
+  const int b = gid - M.gids;
+  return (gid < 0 || b < 0 || b >= d.nmb) ? -1 : b;
+}
+
+// CloudDepositImplicitT (src/dust/dust_imex3d.cpp:61-99): Q = m c W / V, P = Q v
+__global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, double sh,
+                                unsigned *err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
+  int m, lev;
+  double x[3];
+  if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
+  const double mass_c = P.r(DUSTB_IPM, p) * a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
+  const double vx = P.r(DUSTB_IPVX, p), vy = P.r(DUSTB_IPVY, p), vz = P.r(DUSTB_IPVZ, p);
+  CloudAxis X, Y, Z;
+  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
+  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
+  cloud_axis(M, d, m, 2, x[2], lev, L[2], Z);
+  for (int kz = 0; kz < Z.n; ++kz) {
+    if (Z.w[kz] == 0.0) continue;
+    for (int jy = 0; jy < Y.n; ++jy) {
+      if (Y.w[jy] == 0.0) continue;
+      const double w23 = Y.w[jy] * Z.w[kz];
+      for (int ix = 0; ix < X.n; ++ix) {
+        const double w = w23 * X.w[ix];
+        if (w == 0.0) continue;
+        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
+        if (b < 0) { report(err, DUSTB_ERR_CLOUD); continue; }
+        const double dw = mass_c * w / (M.s(b, DX1) * M.s(b, DX2) * M.s(b, DX3));
+        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+        atomicAdd(&qdep[d.at(b, 5, 0, k, j, i)], dw);
+        atomicAdd(&qdep[d.at(b, 5, 1, k, j, i)], dw * vx);
+        atomicAdd(&qdep[d.at(b, 5, 2, k, j, i)], dw * vy);
+        atomicAdd(&qdep[d.at(b, 5, 3, k, j, i)], dw * vz);
+      }
+    }
+  }
+}
+
+// PackGatherField3D (src/dust/dust_cloud3d.cpp:1319-1340): the velocity and its central
+// differences, gp(m, k, j, i, 0..11), over the padded interior (the outer layer zero)
+__global__ void k_gather_pack(Ind d, const double *v, double *gp) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long per = d.cells();
+  if (idx >= per * d.nmb) return;
+  const int m = (int)(idx / per);
+  long long r = idx - (long long)m * per;
+  const int i = (int)(r % d.n1); r /= d.n1;
+  const int j = (int)(r % d.n2);
+  const int k = (int)(r / d.n2);
+  double *g = gp + idx * 12;
+  const bool in = i >= 1 && i < d.n1 - 1 && j >= 1 && j < d.n2 - 1 && k >= 1 && k < d.n3 - 1;
+  for (int q = 0; q < 3; ++q) {
+    if (!in) { g[q] = g[3 + q] = g[6 + q] = g[9 + q] = 0.0; continue; }
+    g[q] = v[d.at(m, 3, q, k, j, i)];
+    g[3 + q] = v[d.at(m, 3, q, k, j, i + 1)] - v[d.at(m, 3, q, k, j, i - 1)];
+    g[6 + q] = v[d.at(m, 3, q, k, j + 1, i)] - v[d.at(m, 3, q, k, j - 1, i)];
+    g[9 + q] = v[d.at(m, 3, q, k + 1, j, i)] - v[d.at(m, 3, q, k - 1, j, i)];
+  }
+}
+
+// CloudGatherKickT without the blend (src/dust/dust_imex3d.cpp:114-175; the linear gather of
+// dust_imex3d_gather.hpp and dust_leaf_api.hpp:196-219): ubar = sum w u* + cx du/dx + cy du/dy
+// + cz du/dz, cx = (m1x + MinImage(x - xc) w) / (2 dx); dv = c (ubar - v), v += dv,
+// R = dv / a_dt; with back-reaction -m w dv / V into dmom over the leaves of nonzero weight
+__global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
+                                    double a_dt, double sh, int br, unsigned *err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
+  int m, lev;
+  double x[3];
+  if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
+  CloudAxis X, Y, Z;
+  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
+  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
+  cloud_axis(M, d, m, 2, x[2], lev, L[2], Z);
+  double ug[3] = {0.0, 0.0, 0.0};
+  for (int kz = 0; kz < Z.n; ++kz) {
+    const double w3 = Z.w[kz], g3 = Z.g[kz];
+    if (w3 == 0.0 && g3 == 0.0) continue;
+    for (int jy = 0; jy < Y.n; ++jy) {
+      const double w2 = Y.w[jy], g2 = Y.g[jy];
+      if (w2 == 0.0 && g2 == 0.0) continue;
+      const double w23 = w2 * w3;
+      for (int ix = 0; ix < X.n; ++ix) {
+        const double wa = X.w[ix], ga = X.g[ix];
+        const double w = w23 * wa;
+        const double m1x = w23 * ga, m1y = wa * g2 * w3, m1z = wa * w2 * g3;
+        if (w == 0.0 && m1x == 0.0 && m1y == 0.0 && m1z == 0.0) continue;
+        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
+        if (b < 0) { report(err, DUSTB_ERR_CLOUD); continue; }
+        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+        const double dx1 = M.s(b, DX1), dx2 = M.s(b, DX2), dx3 = M.s(b, DX3);
+        const double xc = M.s(b, X1MIN) + (i - d.is + 0.5) * dx1;
+        const double yc = M.s(b, X2MIN) + (j - d.js + 0.5) * dx2;
+        const double zc = M.s(b, X3MIN) + (k - d.ks + 0.5) * dx3;
+        const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
+        const double cx = 0.5 * (m1x + (ex - L[0] * round(ex / L[0])) * w) / dx1;
+        const double cy = 0.5 * (m1y + (ey - L[1] * round(ey / L[1])) * w) / dx2;
+        const double cz = 0.5 * (m1z + (ez - L[2] * round(ez / L[2])) * w) / dx3;
+        const double *g = gp + ((((long long)b * d.n3 + k) * d.n2 + j) * d.n1 + i) * 12;
+        ug[0] += w * g[0] + cx * g[3] + cy * g[6] + cz * g[9];
+        ug[1] += w * g[1] + cx * g[4] + cy * g[7] + cz * g[10];
+        ug[2] += w * g[2] + cx * g[5] + cy * g[8] + cz * g[11];
+      }
+    }
+  }
+  const double cj = a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
+  const double dvx = cj * (ug[0] - P.r(DUSTB_IPVX, p));
+  const double dvy = cj * (ug[1] - P.r(DUSTB_IPVY, p));
+  const double dvz = cj * (ug[2] - P.r(DUSTB_IPVZ, p));
+  P.r(DUSTB_IPVX, p) += dvx; P.r(DUSTB_IPVY, p) += dvy; P.r(DUSTB_IPVZ, p) += dvz;
+  P.r(DUSTB_IPRX, p) = dvx / a_dt; P.r(DUSTB_IPRY, p) = dvy / a_dt; P.r(DUSTB_IPRZ, p) = dvz / a_dt;
+  if (!br) return;
+  // the impulse with the deposit's leaves (those of nonzero weight, the same as the gather's)
+  const double mass = -P.r(DUSTB_IPM, p);
+  for (int kz = 0; kz < Z.n; ++kz) {
+    if (Z.w[kz] == 0.0) continue;
+    for (int jy = 0; jy < Y.n; ++jy) {
+      if (Y.w[jy] == 0.0) continue;
+      const double w23 = Y.w[jy] * Z.w[kz];
+      for (int ix = 0; ix < X.n; ++ix) {
+        const double w = w23 * X.w[ix];
+        if (w == 0.0) continue;
+        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
+        if (b < 0) continue;
+        const double dw = mass * w / (M.s(b, DX1) * M.s(b, DX2) * M.s(b, DX3));
+        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+        atomicAdd(&dmom[d.at(b, 3, 0, k, j, i)], dw * dvx);
+        atomicAdd(&dmom[d.at(b, 3, 1, k, j, i)], dw * dvy);
+        atomicAdd(&dmom[d.at(b, 3, 2, k, j, i)], dw * dvz);
+      }
+    }
+  }
+}
+
 long long n_active(const Ind &d) { return (long long)d.nmb * d.nx3 * d.nx2 * d.nx1; }
 long long n_all(const Ind &d) { return d.cells() * d.nmb; }
 
@@ -1597,6 +1814,42 @@ int dustb_phst(const dustb_ctx *c, const double *chi_max, double *row, void *scr
   k_argmax_blocks<<<nb, 256, 0, S(stream)>>>(d, field, bval, bloc);
   k_argmax_final<<<1, 1, 0, S(stream)>>>(d, mview(c), bval, bloc, nb, row);
   return launch_status("phst");
+}
+
+// ---- refinable clouds on a uniform 3-D mesh (periodic; plain P1 hat clouds) ---------------
+static int cloud_mesh_ok(const dustb_ctx *c) {
+  const dustb_mesh &ms = c->mesh;
+  return ms.three_d && !ms.shear_x1 && ms.x3bc == DUSTB_X3_PERIODIC;
+}
+
+long long dustb_cloud_gpack_bytes(const dustb_mesh *mesh) {
+  if (!mesh) return -1;
+  const Ind d = make_ind(*mesh);
+  return n_all(d) * 12 * (long long)sizeof(double);
+}
+
+int dustb_cloud_deposit_qp(const dustb_ctx *c, double a_dt, double sh, void *stream) {
+  CHECK_CTX(c);
+  if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
+  const Ind d = make_ind(c->mesh);
+  cudaMemsetAsync(c->f.qdep, 0, (size_t)(n_all(d) * 5) * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_cloud_deposit<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, c->err);
+  return launch_status("cloud_deposit_qp");
+}
+
+int dustb_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, double *gpack,
+                            void *stream) {
+  CHECK_CTX(c);
+  if (!gpack) return DUSTB_EINVAL;
+  if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
+  const Ind d = make_ind(c->mesh);
+  k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
+  cudaMemsetAsync(c->f.dmom, 0, (size_t)(n_all(d) * 3) * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_cloud_gather_kick<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, a_dt, sh,
+                                      c->phys.back_reaction, c->err);
+  return launch_status("cloud_gather_kick");
 }
 
 // the point transfers' remap: the drag's, with the ghost deposits behind physical x3 faces

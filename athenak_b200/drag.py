@@ -241,6 +241,19 @@ class DeviceDust:
         self._call("phst", chi, row.data_ptr(), s.data_ptr(), s.numel(), stream=stream)
         return row
 
+    # ---- refinable clouds on a uniform 3-D mesh ----
+    def cloud_deposit_qp(self, a_dt, sh=0.0, stream=None):
+        self._call("cloud_deposit_qp", a_dt, sh, stream=stream)
+
+    def cloud_gather_kick(self, a_dt, sh=0.0, stream=None):
+        n = int(self.lib.dustb_cloud_gpack_bytes(C.byref(self.ctx.mesh))) // 8
+        gp = self.t.get("gpack")
+        if gp is None or gp.numel() < n:
+            gp = torch.empty(n, dtype=torch.float64, device=self.device)
+            self.t["gpack"] = gp
+        self._call("cloud_gather_kick", a_dt, sh, gp.data_ptr(), stream=stream)
+        return gp
+
     # ---- point-particle fields (self-gravity, outputs) ----
     def _field(self, nvar):
         return torch.zeros(self.mesh.field_shape(nvar), dtype=torch.float64, device=self.device)

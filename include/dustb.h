@@ -63,6 +63,8 @@ enum { DUSTB_X3_PERIODIC = 0, DUSTB_X3_REFLECT = 1, DUSTB_X3_OUTFLOW = 2 };
 #define DUSTB_ERR_TIMEOUT   0x40u /* a bounded wait on an asynchronous copy ran out */
 #define DUSTB_ERR_POINT     0x80u /* point-particle fields: invalid mass, owner, position or
                                    * TSC support (dust_gravity_points.cpp:29-33) */
+#define DUSTB_ERR_CLOUD     0x100u /* refinable clouds: a cloud code with lobe bits (transition
+                                    * clouds of refined meshes) or a cloud outside its block */
 
 /* host return codes */
 #define DUSTB_OK          0
@@ -281,6 +283,23 @@ int dustb_point_gravity_gather(const dustb_ctx *ctx, const double *owned, double
  * species >= 0: that species only.  halo: the same nvar. */
 int dustb_point_science_fields(const dustb_ctx *ctx, double *out, double *halo, int mass_only,
                                int species, void *stream);
+
+/* ---- refinable clouds on a uniform 3-D mesh (src/dust/dust_imex3d.cpp) -----------------
+ * Plain P1 hat clouds: PLEV holds the cloud level L (half-width dx / 2^L along each
+ * direction), integrated exactly over the cells of the block and its same-level neighbours
+ * (CloudShape1D, LeafTraversal3D::ForEach on a uniform mesh).  Periodic meshes (no physical
+ * x3 or shear-periodic faces: EUNSUP).  A cloud code with lobe bits (the transition clouds
+ * of refined meshes) or a cloud outside its block sets DUSTB_ERR_CLOUD and is skipped. */
+/* CloudDepositImplicitT (:61-99): qdep cleared, then Q = m c W / V and P = Q v into the owner
+ * cells (no ghost exchange needed). */
+int dustb_cloud_deposit_qp(const dustb_ctx *ctx, double a_dt, double sh, void *stream);
+/* Bytes of the gather pack (12 doubles per padded cell, PackGatherField3D). */
+long long dustb_cloud_gpack_bytes(const dustb_mesh *mesh);
+/* CloudGatherImplicit3D's plain kernel (CloudGatherKickT, :114-175): u* (ghost cells filled by
+ * the caller's copy exchange) packed with its central differences into gpack, the linear-
+ * moment gather, the kick (v, R), and with back-reaction the impulse into dmom (cleared). */
+int dustb_cloud_gather_kick(const dustb_ctx *ctx, double a_dt, double sh, double *gpack,
+                            void *stream);
 
 /* ---- the particle science file (pbin, src/outputs/pbin.cpp): its device side -----------
  * The host writes the file (athenak_b200/host/pbin.hpp); these calls find the active rows

@@ -986,6 +986,230 @@ void oracle_sort_particles(const dustb_ctx *c, double *spare_pr, int *spare_pi) 
   free(order);
 }
 
+/* ---- refinable clouds on a uniform 3-D mesh: plain P1 hat clouds ---------------------
+ * CloudShape1D (src/dust/dust.hpp:240-298) with HatCDF / HatMoment (:169-182) for a cloud
+ * without lobes: along each direction the hat of half-width ell = dx / 2^level about the
+ * particle; a cell's weight is the difference of the hat CDF at its two faces, its first
+ * moment about the particle ell times the difference of the moment antiderivative.
+ * LeafTraversal3D::ForEach (src/dust/dust_leaf3d.hpp:368-513) on a uniform mesh: the cells of
+ * the block and of its same-level neighbours that the support overlaps, each cell's faces
+ * from its own block's origin (the neighbour's periodic image next to the block), weight w =
+ * w1 w2 w3 and moments (g1 w2 w3, w1 g2 w3, w1 w2 g3).  Leaf order here: z, then y, then x,
+ * each direction from the lower neighbour through the block to the upper one; leaves of zero
+ * weight (and zero moments) are skipped. */
+static double hat_cdf(double s) {
+  if (s <= -1.0) return 0.0;
+  if (s >= 1.0) return 1.0;
+  return (s <= 0.0) ? 0.5*(1.0 + s)*(1.0 + s) : 1.0 - 0.5*(1.0 - s)*(1.0 - s);
+}
+static double hat_moment(double s) {
+  if (s <= -1.0 || s >= 1.0) return 1.0/6.0;
+  return (s <= 0.0) ? 0.5*(s*s) + (s*s)*s/3.0 : 0.5*(s*s) - (s*s)*s/3.0;
+}
+
+typedef struct { int n; int o[6]; int i[6]; double w[6]; double g[6]; } CloudAxis;
+
+/* the cells of one direction a (0..2) for a cloud at x of level lev anchored at block m */
+static void cloud_axis(const dustb_ctx *c, int m, int a, double x, int lev, CloudAxis *A) {
+  const dustb_mesh *ms = &c->mesh;
+  const int nx = (a == 0) ? ms->nx1 : ((a == 1) ? ms->nx2 : ms->nx3);
+  const double L = (a == 0) ? ms->x1max - ms->x1min : ((a == 1) ? ms->x2max - ms->x2min
+                                                                 : ms->x3max - ms->x3min);
+  const double dx = MB(m, DX1 + a), idx = 1.0/dx;
+  const double ell = ldexp(dx, -lev), inv = ldexp(idx, lev);
+  const double lo = x - ell, hi = x + ell;
+  A->n = 0;
+  for (int o = -1; o <= 1; ++o) {
+    int b = m;
+    if (o != 0) {
+      const int oo[3] = {a == 0 ? o : 0, a == 1 ? o : 0, a == 2 ? o : 0};
+      const int gid = ms->nghbr[(size_t)m*27 + (oo[2] + 1)*9 + (oo[1] + 1)*3 + (oo[0] + 1)];
+      if (gid < 0 || gid - ms->gids < 0 || gid - ms->gids >= ms->nmb) continue;
+      b = gid - ms->gids;
+    }
+    double bx0 = MB(b, X1MIN + a);
+    if (o < 0 && MB(b, X1MIN + a) >= MB(m, X1MIN + a)) bx0 -= L;   /* its image below m */
+    if (o > 0 && MB(b, X1MIN + a) <= MB(m, X1MIN + a)) bx0 += L;   /* its image above m */
+    int i0 = (int)floor((lo - bx0)*idx), i1 = (int)ceil((hi - bx0)*idx) - 1;
+    i0 = (i0 < 0) ? 0 : i0;
+    i1 = (i1 > nx - 1) ? nx - 1 : i1;
+    for (int i = i0; i <= i1 && A->n < 6; ++i) {
+      const double za = (bx0 + i*dx - x)*inv, zb = (bx0 + (i + 1)*dx - x)*inv;
+      A->o[A->n] = o; A->i[A->n] = i;
+      A->w[A->n] = hat_cdf(zb) - hat_cdf(za);
+      A->g[A->n] = ell*(hat_moment(zb) - hat_moment(za));
+      ++A->n;
+    }
+  }
+}
+
+/* Frame (dust_leaf3d.hpp): the periodic image of the position next to block m */
+static void cloud_frame(const dustb_ctx *c, int m, double x[3]) {
+  const dustb_mesh *ms = &c->mesh;
+  const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
+  const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
+  for (int a = 0; a < 3; ++a) {
+    const double cx = MB(m, X1MIN + a) + 0.5*nx[a]*MB(m, DX1 + a);
+    x[a] -= L[a]*round((x[a] - cx)*(1.0/L[a]));
+  }
+}
+
+/* a cloud this restatement takes: level code without lobe bits, position inside its block */
+static int cloud_ok(const dustb_ctx *c, int m, const double x[3], int code) {
+  const dustb_mesh *ms = &c->mesh;
+  if (m < 0 || m >= ms->nmb || (code & ~15) != 0) return 0;
+  for (int a = 0; a < 3; ++a)
+    if (!(x[a] >= MB(m, X1MIN + a) && x[a] < MB(m, X1MAX + a))) return 0;
+  return 1;
+}
+
+/* the owner block of a leaf in direction (ox, oy, oz) of m */
+static int cloud_owner(const dustb_ctx *c, int m, int ox, int oy, int oz) {
+  if (!ox && !oy && !oz) return m;
+  const int gid = c->mesh.nghbr[(size_t)m*27 + (oz + 1)*9 + (oy + 1)*3 + (ox + 1)];
+  const int b = gid - c->mesh.gids;
+  return (gid < 0 || b < 0 || b >= c->mesh.nmb) ? -1 : b;
+}
+
+/* CloudDepositImplicitT (src/dust/dust_imex3d.cpp:61-99): Q = m c W / V and P = Q v into
+ * qdep 0-3 of the owner cells (qdep cleared first) */
+unsigned oracle_cloud_deposit_qp(const dustb_ctx *c, double a_dt, double sh) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  memset(c->f.qdep, 0, field_size(ms, 5)*sizeof(double));
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  unsigned err = 0;
+  for (int p = 0; p < c->part.npart; ++p) {
+    const int m = PI(DUSTB_PGID, p) - ms->gids;
+    double x[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p), PR(DUSTB_IPZ, p)};
+    const int code = PI(DUSTB_PLEV, p);
+    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
+    if (!cloud_ok(c, m, x, code)) { err |= DUSTB_ERR_CLOUD; continue; }
+    const double mass_c = PR(DUSTB_IPM, p)*a_dt/(PR(DUSTB_IPTS, p) + a_dt);
+    const double vx = PR(DUSTB_IPVX, p), vy = PR(DUSTB_IPVY, p), vz = PR(DUSTB_IPVZ, p);
+    CloudAxis X, Y, Z;
+    cloud_axis(c, m, 0, x[0], code, &X);
+    cloud_axis(c, m, 1, x[1], code, &Y);
+    cloud_axis(c, m, 2, x[2], code, &Z);
+    for (int kz = 0; kz < Z.n; ++kz) {
+      if (Z.w[kz] == 0.0) continue;
+      for (int jy = 0; jy < Y.n; ++jy) {
+        if (Y.w[jy] == 0.0) continue;
+        const double w23 = Y.w[jy]*Z.w[kz];
+        for (int ix = 0; ix < X.n; ++ix) {
+          const double w = w23*X.w[ix];
+          if (w == 0.0) continue;
+          const int b = cloud_owner(c, m, X.o[ix], Y.o[jy], Z.o[kz]);
+          if (b < 0) { err |= DUSTB_ERR_CLOUD; continue; }
+          const double dw = mass_c*w/(MB(b, DX1)*MB(b, DX2)*MB(b, DX3));
+          const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+          A5(c->f.qdep, 5, d, b, 0, k, j, i) += dw;
+          A5(c->f.qdep, 5, d, b, 1, k, j, i) += dw*vx;
+          A5(c->f.qdep, 5, d, b, 2, k, j, i) += dw*vy;
+          A5(c->f.qdep, 5, d, b, 3, k, j, i) += dw*vz;
+        }
+      }
+    }
+  }
+  return err;
+}
+
+/* PackGatherField3D (src/dust/dust_cloud3d.cpp:1319-1340): gp(m, k, j, i, 0..11) = the
+ * velocity and its central differences along x, y, z, over the padded interior */
+void oracle_gather_pack(const dustb_ctx *c, const double *v, double *gp) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  memset(gp, 0, (size_t)ms->nmb*d.n3*d.n2*d.n1*12*sizeof(double));
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = 1; k < d.n3 - 1; ++k)
+      for (int j = 1; j < d.n2 - 1; ++j)
+        for (int i = 1; i < d.n1 - 1; ++i) {
+          double *g = gp + ((((size_t)m*d.n3 + k)*d.n2 + j)*d.n1 + i)*12;
+          for (int q = 0; q < 3; ++q) {
+            g[q] = A5(v, 3, d, m, q, k, j, i);
+            g[3 + q] = A5(v, 3, d, m, q, k, j, i + 1) - A5(v, 3, d, m, q, k, j, i - 1);
+            g[6 + q] = A5(v, 3, d, m, q, k, j + 1, i) - A5(v, 3, d, m, q, k, j - 1, i);
+            g[9 + q] = A5(v, 3, d, m, q, k + 1, j, i) - A5(v, 3, d, m, q, k - 1, j, i);
+          }
+        }
+}
+
+/* CloudGatherKickT without the blend (src/dust/dust_imex3d.cpp:114-175, the linear gather
+ * CloudLinearGather3D / GatherLinear, src/dust/dust_imex3d_gather.hpp, dust_leaf_api.hpp:
+ * 196-219): ubar = sum over the leaves of w u* + cx du/dx + cy du/dy + cz du/dz with
+ * cx = (m1x + MinImage(x - xc) w) / (2 dx); dv = c (ubar - v), v += dv, R = dv / a_dt; with
+ * back-reaction -m w dv / V into dmom (cleared first) of the same leaves.  gp: the pack of
+ * u* (its ghost cells filled by the caller). */
+unsigned oracle_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, const double *gp) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  memset(c->f.dmom, 0, field_size(ms, 3)*sizeof(double));
+  double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
+  const int br = c->phys.back_reaction;
+  unsigned err = 0;
+  for (int p = 0; p < c->part.npart; ++p) {
+    const int m = PI(DUSTB_PGID, p) - ms->gids;
+    double x[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p), PR(DUSTB_IPZ, p)};
+    const int code = PI(DUSTB_PLEV, p);
+    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
+    if (!cloud_ok(c, m, x, code)) { err |= DUSTB_ERR_CLOUD; continue; }
+    CloudAxis X, Y, Z;
+    cloud_axis(c, m, 0, x[0], code, &X);
+    cloud_axis(c, m, 1, x[1], code, &Y);
+    cloud_axis(c, m, 2, x[2], code, &Z);
+    double ug[3] = {0.0, 0.0, 0.0};
+    int nt = 0, tb[216], tk[216], tj[216], ti[216];
+    double tw[216];
+    for (int kz = 0; kz < Z.n; ++kz) {
+      const double w3 = Z.w[kz], g3 = Z.g[kz];
+      if (w3 == 0.0 && g3 == 0.0) continue;
+      for (int jy = 0; jy < Y.n; ++jy) {
+        const double w2 = Y.w[jy], g2 = Y.g[jy];
+        if (w2 == 0.0 && g2 == 0.0) continue;
+        const double w23 = w2*w3;
+        for (int ix = 0; ix < X.n; ++ix) {
+          const double wa = X.w[ix], ga = X.g[ix];
+          const double w = w23*wa;
+          const double m1x = w23*ga, m1y = wa*g2*w3, m1z = wa*w2*g3;
+          if (w == 0.0 && m1x == 0.0 && m1y == 0.0 && m1z == 0.0) continue;
+          const int b = cloud_owner(c, m, X.o[ix], Y.o[jy], Z.o[kz]);
+          if (b < 0) { err |= DUSTB_ERR_CLOUD; continue; }
+          const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+          const double dx1 = MB(b, DX1), dx2 = MB(b, DX2), dx3 = MB(b, DX3);
+          const double xc = MB(b, X1MIN) + (i - d.is + 0.5)*dx1;
+          const double yc = MB(b, X2MIN) + (j - d.js + 0.5)*dx2;
+          const double zc = MB(b, X3MIN) + (k - d.ks + 0.5)*dx3;
+          const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
+          const double cx = 0.5*(m1x + (ex - L[0]*round(ex/L[0]))*w)/dx1;
+          const double cy = 0.5*(m1y + (ey - L[1]*round(ey/L[1]))*w)/dx2;
+          const double cz = 0.5*(m1z + (ez - L[2]*round(ez/L[2]))*w)/dx3;
+          const double *g = gp + ((((size_t)b*d.n3 + k)*d.n2 + j)*d.n1 + i)*12;
+          ug[0] += w*g[0] + cx*g[3] + cy*g[6] + cz*g[9];
+          ug[1] += w*g[1] + cx*g[4] + cy*g[7] + cz*g[10];
+          ug[2] += w*g[2] + cx*g[5] + cy*g[8] + cz*g[11];
+          tb[nt] = b; tk[nt] = k; tj[nt] = j; ti[nt] = i; tw[nt] = w;
+          ++nt;
+        }
+      }
+    }
+    const double cj = a_dt/(PR(DUSTB_IPTS, p) + a_dt);
+    const double dvx = cj*(ug[0] - PR(DUSTB_IPVX, p));
+    const double dvy = cj*(ug[1] - PR(DUSTB_IPVY, p));
+    const double dvz = cj*(ug[2] - PR(DUSTB_IPVZ, p));
+    PR(DUSTB_IPVX, p) += dvx; PR(DUSTB_IPVY, p) += dvy; PR(DUSTB_IPVZ, p) += dvz;
+    PR(DUSTB_IPRX, p) = dvx/a_dt; PR(DUSTB_IPRY, p) = dvy/a_dt; PR(DUSTB_IPRZ, p) = dvz/a_dt;
+    if (!br) continue;
+    const double mass = -PR(DUSTB_IPM, p);
+    for (int q = 0; q < nt; ++q) {
+      if (tw[q] == 0.0) continue;
+      const int b = tb[q];
+      const double dw = mass*tw[q]/(MB(b, DX1)*MB(b, DX2)*MB(b, DX3));
+      A5(c->f.dmom, 3, d, b, 0, tk[q], tj[q], ti[q]) += dw*dvx;
+      A5(c->f.dmom, 3, d, b, 1, tk[q], tj[q], ti[q]) += dw*dvy;
+      A5(c->f.dmom, 3, d, b, 2, tk[q], tj[q], ti[q]) += dw*dvz;
+    }
+  }
+  return err;
+}
+
 /* ---- the cloud order index, DustGasDrag::UpdateCloudOrder, src/dust/dust_cloud_device.cpp:
  * 1992-2055: the keys of SortParticles sorted, the particle of each slot and its 64-bit tag
  * (TagFromWords, src/athena.hpp:85-88) ------------------------------------------------- */

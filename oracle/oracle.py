@@ -75,6 +75,9 @@ def lib():
             "oracle_point_gravity_gather": ([P, VP, VP, C.c_longlong], C.c_uint),
             "oracle_point_science_fields": ([P, VP, I, I], C.c_uint),
             "oracle_point_force_field": ([P, VP, VP], None),
+            "oracle_cloud_deposit_qp": ([P, D, D], C.c_uint),
+            "oracle_gather_pack": ([P, VP, VP], None),
+            "oracle_cloud_gather_kick": ([P, D, D, VP], C.c_uint),
         }
         for name, (args, res) in sig.items():
             f = getattr(_lib, name)
@@ -262,6 +265,23 @@ class Oracle:
         f = np.zeros(self.mesh.field_shape(3))
         self.call("point_force_field", owned.ctypes.data, f.ctypes.data)
         return f
+
+    # --- refinable clouds on a uniform 3-D mesh (plain P1 hat clouds, PLEV = level) ---
+    def cloud_deposit_qp(self, a_dt, sh=0.0):
+        return self.call("cloud_deposit_qp", a_dt, sh)
+
+    def gather_pack(self, v=None):
+        """PackGatherField3D of v (default u*): (nmb, n3, n2, n1, 12)."""
+        v = self.arr["ustar"] if v is None else np.ascontiguousarray(v, np.float64)
+        ms = self.mesh
+        n1, n2, n3 = ms.n
+        gp = np.zeros((ms.nmb, n3, n2, n1, 12))
+        self.call("gather_pack", v.ctypes.data, gp.ctypes.data)
+        return gp
+
+    def cloud_gather_kick(self, a_dt, sh=0.0, gp=None):
+        gp = self.gather_pack() if gp is None else np.ascontiguousarray(gp, np.float64)
+        return self.call("cloud_gather_kick", a_dt, sh, gp.ctypes.data)
 
     def point_science_fields(self, mass_only=False, species=-1):
         """DepositPointScienceFields: (out field with 1 or 4 vars, err)."""
