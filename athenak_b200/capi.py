@@ -174,6 +174,9 @@ SIGNATURES = {
     "dustb_cloud_deposit_qp": [CTXP, D, D, VP],
     "dustb_cloud_gpack_bytes": [MESHP],
     "dustb_cloud_gather_kick": [CTXP, D, D, VP, VP],
+    "dustb_cloud_dc1_sweep": [CTXP, D, D, VP, VP],
+    "dustb_cloud_apply_pmbr": [CTXP, D, D, VP],
+    "dustb_cloud_imex_cycle": [CTXP, C.POINTER(DustbImexCoeffs), VP, VP, VP],
     "dustb_pbin_scratch_bytes": [I],
     "dustb_pbin_rows": [CTXP, VP, VP, D, VP, LL, VP],
     "dustb_pbin_pack": [CTXP, VP, I, I, I, VP, VP],

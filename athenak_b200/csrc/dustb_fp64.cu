@@ -1500,6 +1500,140 @@ __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, dou
   }
 }
 
+// the clouds' linear gather of the packed field at one cloud (without the blend), in the
+// leaf order of the gather-kick
+__device__ void cloud_gather(const MCtx &M, const Ind &d, int m, const double x[3],
+                             const CloudAxis &X, const CloudAxis &Y, const CloudAxis &Z,
+                             const double L[3], const double *gp, double ug[3], unsigned *err) {
+  ug[0] = ug[1] = ug[2] = 0.0;
+  for (int kz = 0; kz < Z.n; ++kz) {
+    const double w3 = Z.w[kz], g3 = Z.g[kz];
+    if (w3 == 0.0 && g3 == 0.0) continue;
+    for (int jy = 0; jy < Y.n; ++jy) {
+      const double w2 = Y.w[jy], g2 = Y.g[jy];
+      if (w2 == 0.0 && g2 == 0.0) continue;
+      const double w23 = w2 * w3;
+      for (int ix = 0; ix < X.n; ++ix) {
+        const double wa = X.w[ix], ga = X.g[ix];
+        const double w = w23 * wa;
+        const double m1x = w23 * ga, m1y = wa * g2 * w3, m1z = wa * w2 * g3;
+        if (w == 0.0 && m1x == 0.0 && m1y == 0.0 && m1z == 0.0) continue;
+        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
+        if (b < 0) { report(err, DUSTB_ERR_CLOUD); continue; }
+        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+        const double dx1 = M.s(b, DX1), dx2 = M.s(b, DX2), dx3 = M.s(b, DX3);
+        const double xc = M.s(b, X1MIN) + (i - d.is + 0.5) * dx1;
+        const double yc = M.s(b, X2MIN) + (j - d.js + 0.5) * dx2;
+        const double zc = M.s(b, X3MIN) + (k - d.ks + 0.5) * dx3;
+        const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
+        const double cx = 0.5 * (m1x + (ex - L[0] * round(ex / L[0])) * w) / dx1;
+        const double cy = 0.5 * (m1y + (ey - L[1] * round(ey / L[1])) * w) / dx2;
+        const double cz = 0.5 * (m1z + (ez - L[2] * round(ez / L[2])) * w) / dx3;
+        const double *g = gp + ((((long long)b * d.n3 + k) * d.n2 + j) * d.n1 + i) * 12;
+        ug[0] += w * g[0] + cx * g[3] + cy * g[6] + cz * g[9];
+        ug[1] += w * g[1] + cx * g[4] + cy * g[7] + cz * g[10];
+        ug[2] += w * g[2] + cx * g[5] + cy * g[8] + cz * g[11];
+      }
+    }
+  }
+}
+
+// CloudOperatorKernelT (src/dust/dust_cloud_imex_kernels.hpp:20-70): the clouds' m c W ubar / V
+// with ubar their linear gather of the packed field, into result (the operator of dc1 / dc2)
+__global__ void k_cloud_operator(PCtx P, MCtx M, Ind d, const double *gp, double *result,
+                                 double a_dt, double sh, unsigned *err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
+  int m, lev;
+  double x[3];
+  if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
+  CloudAxis X, Y, Z;
+  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
+  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
+  cloud_axis(M, d, m, 2, x[2], lev, L[2], Z);
+  double ug[3];
+  cloud_gather(M, d, m, x, X, Y, Z, L, gp, ug, err);
+  const double mc = P.r(DUSTB_IPM, p) * (a_dt / (P.r(DUSTB_IPTS, p) + a_dt));
+  for (int kz = 0; kz < Z.n; ++kz) {
+    if (Z.w[kz] == 0.0) continue;
+    for (int jy = 0; jy < Y.n; ++jy) {
+      if (Y.w[jy] == 0.0) continue;
+      const double w23 = Y.w[jy] * Z.w[kz];
+      for (int ix = 0; ix < X.n; ++ix) {
+        const double w = w23 * X.w[ix];
+        if (w == 0.0) continue;
+        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
+        if (b < 0) continue;
+        const double dw = mc * w / (M.s(b, DX1) * M.s(b, DX2) * M.s(b, DX3));
+        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+        atomicAdd(&result[d.at(b, 3, 0, k, j, i)], dw * ug[0]);
+        atomicAdd(&result[d.at(b, 3, 1, k, j, i)], dw * ug[1]);
+        atomicAdd(&result[d.at(b, 3, 2, k, j, i)], dw * ug[2]);
+      }
+    }
+  }
+}
+
+// CloudImplicitConsistencyOverlapT (src/dust/dust_imex3d.cpp:669-790), the cells: g = rho u* -
+// M, r = (D - g) / (rho + Q) (by the reciprocal), the gas takes g + rho r, dmom its rate, r
+// into res (vars 0-2 of a 4-variable field)
+__global__ void k_cloud_consistent_gas(Ind d, double *u0, int nv, const double *us,
+                                       const double *qdep, double *dmom, double *res,
+                                       double inv_adt) {
+  int m, k, j, i;
+  if (!active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i)) return;
+  const double rho = u0[d.at(m, nv, 0, k, j, i)];
+  const double q = qdep[d.at(m, 5, 0, k, j, i)];
+  const double inv = 1.0 / (rho + q);
+  for (int v = 0; v < 3; ++v) {
+    const long long a3 = d.at(m, 3, v, k, j, i), au = d.at(m, nv, 1 + v, k, j, i);
+    const double g = rho * us[a3] - u0[au];
+    const double r = (dmom[a3] - g) * inv;
+    const double dgas = g + rho * r;
+    u0[au] += dgas;
+    dmom[a3] = dgas * inv_adt;
+    res[d.at(m, 4, v, k, j, i)] = r;
+  }
+}
+
+// ... the clouds: v += c sum W r, R += c sum W r / a_dt with the deposit's weights
+__global__ void k_cloud_consistent_dust(PCtx P, MCtx M, Ind d, const double *res, double a_dt,
+                                        double sh) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  if (P.r(DUSTB_IPM, p) <= 0.0) return;
+  const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
+  int m, lev;
+  double x[3];
+  if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) return;
+  CloudAxis X, Y, Z;
+  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
+  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
+  cloud_axis(M, d, m, 2, x[2], lev, L[2], Z);
+  double rv[3] = {0.0, 0.0, 0.0};
+  for (int kz = 0; kz < Z.n; ++kz) {
+    if (Z.w[kz] == 0.0) continue;
+    for (int jy = 0; jy < Y.n; ++jy) {
+      if (Y.w[jy] == 0.0) continue;
+      const double w23 = Y.w[jy] * Z.w[kz];
+      for (int ix = 0; ix < X.n; ++ix) {
+        const double w = w23 * X.w[ix];
+        if (w == 0.0) continue;
+        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
+        if (b < 0) continue;
+        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+        for (int v = 0; v < 3; ++v) rv[v] += w * res[d.at(b, 4, v, k, j, i)];
+      }
+    }
+  }
+  const double cj = a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
+  P.r(DUSTB_IPVX, p) += cj * rv[0]; P.r(DUSTB_IPVY, p) += cj * rv[1]; P.r(DUSTB_IPVZ, p) += cj * rv[2];
+  P.r(DUSTB_IPRX, p) += cj * rv[0] / a_dt;
+  P.r(DUSTB_IPRY, p) += cj * rv[1] / a_dt;
+  P.r(DUSTB_IPRZ, p) += cj * rv[2] / a_dt;
+}
+
 long long n_active(const Ind &d) { return (long long)d.nmb * d.nx3 * d.nx2 * d.nx1; }
 long long n_all(const Ind &d) { return d.cells() * d.nmb; }
 
@@ -1852,6 +1986,38 @@ int dustb_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, double *
   return launch_status("cloud_gather_kick");
 }
 
+int dustb_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh, double *gpack,
+                          void *stream) {
+  CHECK_CTX(c);
+  if (!gpack) return DUSTB_EINVAL;
+  if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
+  const Ind d = make_ind(c->mesh);
+  int rc = dustb_ghost_copy(c, c->f.ustar, 3, 1, stream);
+  if (rc) return rc;
+  k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
+  cudaMemsetAsync(c->f.work, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_cloud_operator<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.work, a_dt, sh, c->err);
+  k_dc_correct<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas,
+                                                                    c->f.qdep, c->f.work,
+                                                                    c->f.ustar);
+  return launch_status("cloud_dc1_sweep");
+}
+
+int dustb_cloud_apply_pmbr(const dustb_ctx *c, double a_dt, double sh, void *stream) {
+  CHECK_CTX(c);
+  if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
+  if (!c->phys.back_reaction) return DUSTB_OK;
+  if (!c->phys.consistent_gas) return dustb_apply_pmbr(c, a_dt, stream);
+  const Ind d = make_ind(c->mesh);
+  cudaMemsetAsync(c->f.resid, 0, (size_t)n_all(d) * 4 * sizeof(double), S(stream));
+  k_cloud_consistent_gas<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(
+      d, c->f.u0, c->f.nvar_gas, c->f.ustar, c->f.qdep, c->f.dmom, c->f.resid, 1.0 / a_dt);
+  if (c->part.npart > 0)
+    k_cloud_consistent_dust<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, sh);
+  return launch_status("cloud_apply_pmbr");
+}
+
 // the point transfers' remap: the drag's, with the ghost deposits behind physical x3 faces
 // always folded (src/dust/dust_gravity_points.cpp:176-178)
 static dustb_ctx fold_ctx(const dustb_ctx *c) {
@@ -1942,6 +2108,44 @@ int dustb_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co, double *x3
       RUN(dustb_ghost_add(c, c->f.dmom, 3, stream));
       RUN(dustb_apply_pmbr(c, a_dt, stream));
     }
+    RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, stream));
+  }
+  return DUSTB_OK;
+}
+
+// one imex2+ cycle of refinable clouds on a uniform mesh: the task order of dustb_imex_cycle
+// with the clouds' deposit (into the owner cells: no deposit exchange), dc1 / dc2 sweeps,
+// gather-kick and PMBR split
+int dustb_cloud_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co, double *gpack,
+                           double *x3_removed, void *stream) {
+  CHECK_CTX(c);
+  if (!co || !(co->dt > 0.0) || !gpack) return DUSTB_EINVAL;
+  if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
+  const double g = co->gamma, dt = co->dt;
+  const double gam0[2] = {1.0, (2.0 * g - 1.0) / (2.0 * g * g)};
+  const double gam1[2] = {0.0, 1.0 - (2.0 * g - 1.0) / (2.0 * g * g)};
+  const double beta[2] = {g, 1.0 / (2.0 * g)};
+  const double atw22 = (1.0 - 2.0 * g * g) / 2.0 / g;
+  const double a_dt = g * dt;
+  const int br = c->phys.back_reaction;
+  int rc;
+  for (int stage = 1; stage <= 2; ++stage) {
+    if (stage == 1) RUN(dustb_register_copy(c, stream));
+    RUN(dustb_gas_rk_noflux(c, gam0[stage - 1], gam1[stage - 1], stream));
+    if (stage == 2 && br) RUN(dustb_history_gas(c, atw22 * dt, stream));
+    RUN(dustb_push_imex(c, gam0[stage - 1], gam1[stage - 1], beta[stage - 1] * dt,
+                        (stage == 2) ? atw22 * dt : 0.0, stream));
+    RUN(dustb_route(c, x3_removed, stream));
+    const double sh = co->sh[stage - 1];
+    if (br) RUN(dustb_cloud_deposit_qp(c, a_dt, sh, stream));
+    RUN(dustb_solve_ustar(c, stream));
+    if (br && c->phys.drag_solver >= DUSTB_SOLVER_DC1) {
+      int nsw = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
+      for (int w = 0; w < nsw; ++w) RUN(dustb_cloud_dc1_sweep(c, a_dt, sh, gpack, stream));
+    }
+    RUN(dustb_ghost_copy(c, c->f.ustar, 3, 1, stream));
+    RUN(dustb_cloud_gather_kick(c, a_dt, sh, gpack, stream));
+    if (br) RUN(dustb_cloud_apply_pmbr(c, a_dt, sh, stream));
     RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, stream));
   }
   return DUSTB_OK;

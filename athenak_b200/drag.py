@@ -245,14 +245,31 @@ class DeviceDust:
     def cloud_deposit_qp(self, a_dt, sh=0.0, stream=None):
         self._call("cloud_deposit_qp", a_dt, sh, stream=stream)
 
-    def cloud_gather_kick(self, a_dt, sh=0.0, stream=None):
+    def _gpack(self):
         n = int(self.lib.dustb_cloud_gpack_bytes(C.byref(self.ctx.mesh))) // 8
         gp = self.t.get("gpack")
         if gp is None or gp.numel() < n:
             gp = torch.empty(n, dtype=torch.float64, device=self.device)
             self.t["gpack"] = gp
+        return gp
+
+    def cloud_gather_kick(self, a_dt, sh=0.0, stream=None):
+        gp = self._gpack()
         self._call("cloud_gather_kick", a_dt, sh, gp.data_ptr(), stream=stream)
         return gp
+
+    def cloud_dc1_sweep(self, a_dt, sh=0.0, stream=None):
+        self._call("cloud_dc1_sweep", a_dt, sh, self._gpack().data_ptr(), stream=stream)
+
+    def cloud_apply_pmbr(self, a_dt, sh=0.0, stream=None):
+        self._call("cloud_apply_pmbr", a_dt, sh, stream=stream)
+
+    def cloud_imex_cycle(self, dt, gamma=GAMMA_DEFAULT, sh=(0.0, 0.0), stream=None):
+        co = capi.DustbImexCoeffs()
+        co.gamma, co.dt = gamma, dt
+        co.sh[0], co.sh[1] = sh
+        self._call("cloud_imex_cycle", C.byref(co), self._gpack().data_ptr(),
+                   self.t["x3_removed"].data_ptr(), stream=stream)
 
     # ---- point-particle fields (self-gravity, outputs) ----
     def _field(self, nvar):

@@ -300,6 +300,16 @@ long long dustb_cloud_gpack_bytes(const dustb_mesh *mesh);
  * moment gather, the kick (v, R), and with back-reaction the impulse into dmom (cleared). */
 int dustb_cloud_gather_kick(const dustb_ctx *ctx, double a_dt, double sh, double *gpack,
                             void *stream);
+/* CloudDefectCorrection (src/dust/dust_imex3d_dc.cpp:229-274), one sweep: the u* copy
+ * exchange, its pack, the clouds' operator D M G x (CloudOperatorKernelT) into work, then
+ * x += (rho + Q)^-1 (M + P - rho x - D M G x) on the active cells. */
+int dustb_cloud_dc1_sweep(const dustb_ctx *ctx, double a_dt, double sh, double *gpack,
+                          void *stream);
+/* ApplyPMBR for the clouds: with consistent_gas the overlap split
+ * (CloudImplicitConsistencyOverlapT, src/dust/dust_imex3d.cpp:669-790; the residual in
+ * resid), otherwise the plain PMBR. */
+int dustb_cloud_apply_pmbr(const dustb_ctx *ctx, double a_dt, double sh, void *stream);
+/* (dustb_cloud_imex_cycle: with the fused cycles below) */
 
 /* ---- the particle science file (pbin, src/outputs/pbin.cpp): its device side -----------
  * The host writes the file (athenak_b200/host/pbin.hpp); these calls find the active rows
@@ -349,6 +359,12 @@ typedef struct dustb_imex_coeffs {
   double dt;               /* cycle time step */
   double sh[2];            /* ImplicitShearShift of working stages 1, 2 */
 } dustb_imex_coeffs;
+
+/* One imex2+ cycle of refinable clouds on a uniform 3-D mesh (the task order of
+ * dustb_imex_cycle with dustb_cloud_deposit_qp, dustb_cloud_dc1_sweep, dustb_cloud_gather_kick
+ * and dustb_cloud_apply_pmbr); gpack as dustb_cloud_gpack_bytes. */
+int dustb_cloud_imex_cycle(const dustb_ctx *ctx, const dustb_imex_coeffs *coeffs, double *gpack,
+                           double *x3_removed, void *stream);
 
 /* One imex2+ cycle of the drag step (stages 1 and 2; stage 3 is dormant): register copy,
  * gas stand-in, push, route, deposit, ghost add, solve (+dc1/dc2), ghost copy, gather-kick,

@@ -986,6 +986,9 @@ void oracle_sort_particles(const dustb_ctx *c, double *spare_pr, int *spare_pi) 
   free(order);
 }
 
+void oracle_imex2p_coeffs(double gamma, double gam0[3], double gam1[3], double beta[3],
+                          double *atw22);
+
 /* ---- refinable clouds on a uniform 3-D mesh: plain P1 hat clouds ---------------------
  * CloudShape1D (src/dust/dust.hpp:240-298) with HatCDF / HatMoment (:169-182) for a cloud
  * without lobes: along each direction the hat of half-width ell = dx / 2^level about the
@@ -1207,6 +1210,200 @@ unsigned oracle_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, co
       A5(c->f.dmom, 3, d, b, 2, tk[q], tj[q], ti[q]) += dw*dvz;
     }
   }
+  return err;
+}
+
+/* the clouds' linear gather of the packed field gp at one cloud (CloudLinearGather3D
+ * without the blend): ubar, and the leaves of nonzero weight (owner block, cell, w) */
+static int cloud_gather(const dustb_ctx *c, const Ind *d, int m, const double x[3], int code,
+                        const double *gp, double ug[3], int *tb, int *tk, int *tj, int *ti,
+                        double *tw, unsigned *err) {
+  const dustb_mesh *ms = &c->mesh;
+  const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
+  CloudAxis X, Y, Z;
+  cloud_axis(c, m, 0, x[0], code, &X);
+  cloud_axis(c, m, 1, x[1], code, &Y);
+  cloud_axis(c, m, 2, x[2], code, &Z);
+  ug[0] = ug[1] = ug[2] = 0.0;
+  int nt = 0;
+  for (int kz = 0; kz < Z.n; ++kz) {
+    const double w3 = Z.w[kz], g3 = Z.g[kz];
+    if (w3 == 0.0 && g3 == 0.0) continue;
+    for (int jy = 0; jy < Y.n; ++jy) {
+      const double w2 = Y.w[jy], g2 = Y.g[jy];
+      if (w2 == 0.0 && g2 == 0.0) continue;
+      const double w23 = w2*w3;
+      for (int ix = 0; ix < X.n; ++ix) {
+        const double wa = X.w[ix], ga = X.g[ix];
+        const double w = w23*wa;
+        const double m1x = w23*ga, m1y = wa*g2*w3, m1z = wa*w2*g3;
+        if (w == 0.0 && m1x == 0.0 && m1y == 0.0 && m1z == 0.0) continue;
+        const int b = cloud_owner(c, m, X.o[ix], Y.o[jy], Z.o[kz]);
+        if (b < 0) { *err |= DUSTB_ERR_CLOUD; continue; }
+        const int k = d->ks + Z.i[kz], j = d->js + Y.i[jy], i = d->is + X.i[ix];
+        const double dx1 = MB(b, DX1), dx2 = MB(b, DX2), dx3 = MB(b, DX3);
+        const double xc = MB(b, X1MIN) + (i - d->is + 0.5)*dx1;
+        const double yc = MB(b, X2MIN) + (j - d->js + 0.5)*dx2;
+        const double zc = MB(b, X3MIN) + (k - d->ks + 0.5)*dx3;
+        const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
+        const double cx = 0.5*(m1x + (ex - L[0]*round(ex/L[0]))*w)/dx1;
+        const double cy = 0.5*(m1y + (ey - L[1]*round(ey/L[1]))*w)/dx2;
+        const double cz = 0.5*(m1z + (ez - L[2]*round(ez/L[2]))*w)/dx3;
+        const double *g = gp + ((((size_t)b*d->n3 + k)*d->n2 + j)*d->n1 + i)*12;
+        ug[0] += w*g[0] + cx*g[3] + cy*g[6] + cz*g[9];
+        ug[1] += w*g[1] + cx*g[4] + cy*g[7] + cz*g[10];
+        ug[2] += w*g[2] + cx*g[5] + cy*g[8] + cz*g[11];
+        if (w != 0.0) { tb[nt] = b; tk[nt] = k; tj[nt] = j; ti[nt] = i; tw[nt] = w; ++nt; }
+      }
+    }
+  }
+  return nt;
+}
+
+/* CloudDefectCorrection (src/dust/dust_imex3d_dc.cpp:229-274) with CloudOperatorKernelT
+ * (dust_cloud_imex_kernels.hpp:20-70): one sweep x <- x + (rho + Q)^-1 (M + P - rho x - D M G x)
+ * on u*, the operator D M G x = the clouds' m c W ubar / V with ubar their linear gather of x
+ * (u*'s ghost cells by the copy exchange first; the operator's result in work) */
+unsigned oracle_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  double *x = c->f.ustar, *r = c->f.work;
+  double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  oracle_ghost_copy(c, x, 3, 1);
+  double *gp = (double *)malloc((size_t)ms->nmb*d.n3*d.n2*d.n1*12*sizeof(double));
+  oracle_gather_pack(c, x, gp);
+  memset(r, 0, field_size(ms, 3)*sizeof(double));
+  unsigned err = 0;
+  int tb[216], tk[216], tj[216], ti[216];
+  double tw[216];
+  for (int p = 0; p < c->part.npart; ++p) {
+    const int m = PI(DUSTB_PGID, p) - ms->gids;
+    double xp[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p), PR(DUSTB_IPZ, p)};
+    const int code = PI(DUSTB_PLEV, p);
+    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, xp);
+    if (!cloud_ok(c, m, xp, code)) { err |= DUSTB_ERR_CLOUD; continue; }
+    double ug[3];
+    const int nt = cloud_gather(c, &d, m, xp, code, gp, ug, tb, tk, tj, ti, tw, &err);
+    const double mc = PR(DUSTB_IPM, p)*(a_dt/(PR(DUSTB_IPTS, p) + a_dt));
+    for (int q = 0; q < nt; ++q) {
+      const int b = tb[q];
+      const double dw = mc*tw[q]/(MB(b, DX1)*MB(b, DX2)*MB(b, DX3));
+      A5(r, 3, d, b, 0, tk[q], tj[q], ti[q]) += dw*ug[0];
+      A5(r, 3, d, b, 1, tk[q], tj[q], ti[q]) += dw*ug[1];
+      A5(r, 3, d, b, 2, tk[q], tj[q], ti[q]) += dw*ug[2];
+    }
+  }
+  free(gp);
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = d.ks; k <= d.ke; ++k)
+      for (int j = d.js; j <= d.je; ++j)
+        for (int i = d.is; i <= d.ie; ++i) {
+          const double rho = A5(c->f.u0, nv, d, m, 0, k, j, i);
+          const double pinv = 1.0/(rho + A5(c->f.qdep, 5, d, m, 0, k, j, i));
+          for (int v = 0; v < 3; ++v) {
+            const double av = A5(r, 3, d, m, v, k, j, i) + rho*A5(x, 3, d, m, v, k, j, i);
+            const double rv = A5(c->f.u0, nv, d, m, 1 + v, k, j, i) +
+                              A5(c->f.qdep, 5, d, m, 1 + v, k, j, i) - av;
+            A5(x, 3, d, m, v, k, j, i) += pinv*rv;
+          }
+        }
+  return err;
+}
+
+/* ApplyPMBR for the clouds (src/dust/dust_pm.cpp:576-711): with imex_consistent_gas the
+ * overlap split CloudImplicitConsistencyOverlapT (src/dust/dust_imex3d.cpp:669-790): per cell
+ * g = rho u* - M, r = (D - g) / (rho + Q), the gas takes g + rho r and dmom its rate; every
+ * cloud v += c sum W r, R += c sum W r / a_dt with the deposit's weights.  Otherwise the plain
+ * PMBR of the points. */
+void oracle_cloud_apply_pmbr(const dustb_ctx *c, double a_dt, double sh) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  if (!c->phys.back_reaction) return;
+  if (!c->phys.consistent_gas) { oracle_apply_pmbr(c, a_dt); return; }
+  const double inv_adt = 1.0/a_dt;
+  double *u0 = c->f.u0, *dm = c->f.dmom, *res = c->f.resid;
+  memset(res, 0, field_size(ms, 4)*sizeof(double));
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = d.ks; k <= d.ke; ++k)
+      for (int j = d.js; j <= d.je; ++j)
+        for (int i = d.is; i <= d.ie; ++i) {
+          const double rho = A5(u0, nv, d, m, 0, k, j, i);
+          const double q = A5(c->f.qdep, 5, d, m, 0, k, j, i);
+          const double inv = 1.0/(rho + q);
+          for (int v = 0; v < 3; ++v) {
+            const double g = rho*A5(c->f.ustar, 3, d, m, v, k, j, i) - A5(u0, nv, d, m, 1 + v, k, j, i);
+            const double r = (A5(dm, 3, d, m, v, k, j, i) - g)*inv;
+            const double dgas = g + rho*r;
+            A5(u0, nv, d, m, 1 + v, k, j, i) += dgas;
+            A5(dm, 3, d, m, v, k, j, i) = dgas*inv_adt;
+            A5(res, 4, d, m, v, k, j, i) = r;
+          }
+        }
+  double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  for (int p = 0; p < c->part.npart; ++p) {
+    if (PR(DUSTB_IPM, p) <= 0.0) continue;
+    const int m = PI(DUSTB_PGID, p) - ms->gids;
+    double x[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p), PR(DUSTB_IPZ, p)};
+    const int code = PI(DUSTB_PLEV, p);
+    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
+    if (!cloud_ok(c, m, x, code)) continue;
+    CloudAxis X, Y, Z;
+    cloud_axis(c, m, 0, x[0], code, &X);
+    cloud_axis(c, m, 1, x[1], code, &Y);
+    cloud_axis(c, m, 2, x[2], code, &Z);
+    double rv[3] = {0.0, 0.0, 0.0};
+    for (int kz = 0; kz < Z.n; ++kz) {
+      if (Z.w[kz] == 0.0) continue;
+      for (int jy = 0; jy < Y.n; ++jy) {
+        if (Y.w[jy] == 0.0) continue;
+        const double w23 = Y.w[jy]*Z.w[kz];
+        for (int ix = 0; ix < X.n; ++ix) {
+          const double w = w23*X.w[ix];
+          if (w == 0.0) continue;
+          const int b = cloud_owner(c, m, X.o[ix], Y.o[jy], Z.o[kz]);
+          if (b < 0) continue;
+          const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+          for (int v = 0; v < 3; ++v) rv[v] += w*A5(res, 4, d, b, v, k, j, i);
+        }
+      }
+    }
+    const double cj = a_dt/(PR(DUSTB_IPTS, p) + a_dt);
+    PR(DUSTB_IPVX, p) += cj*rv[0]; PR(DUSTB_IPVY, p) += cj*rv[1]; PR(DUSTB_IPVZ, p) += cj*rv[2];
+    PR(DUSTB_IPRX, p) += cj*rv[0]/a_dt; PR(DUSTB_IPRY, p) += cj*rv[1]/a_dt;
+    PR(DUSTB_IPRZ, p) += cj*rv[2]/a_dt;
+  }
+}
+
+/* one imex2+ cycle of refinable clouds on a uniform mesh: the task order of oracle_imex_cycle
+ * with the clouds' deposit (into the owners: no deposit exchange), their dc1 / dc2 sweeps
+ * (with back-reaction), gather-kick and PMBR split */
+unsigned oracle_cloud_imex_cycle(const dustb_ctx *c, double gamma, double dt, const double sh[2],
+                                 double *x3_removed) {
+  double gam0[3], gam1[3], beta[3], atw22;
+  oracle_imex2p_coeffs(gamma, gam0, gam1, beta, &atw22);
+  const double a_dt = gamma*dt;
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  double *gp = (double *)malloc((size_t)ms->nmb*d.n3*d.n2*d.n1*12*sizeof(double));
+  unsigned err = 0;
+  for (int stage = 1; stage <= 2; ++stage) {
+    if (stage == 1) oracle_register_copy(c);
+    oracle_gas_rk_noflux(c, gam0[stage - 1], gam1[stage - 1]);
+    if (stage == 2 && c->phys.back_reaction) oracle_history_gas(c, atw22*dt);
+    oracle_push_imex(c, gam0[stage - 1], gam1[stage - 1], beta[stage - 1]*dt,
+                     (stage == 2) ? atw22*dt : 0.0);
+    err |= oracle_route(c, x3_removed);
+    const double s = sh[stage - 1];
+    if (c->phys.back_reaction) err |= oracle_cloud_deposit_qp(c, a_dt, s);
+    oracle_solve_ustar(c);
+    if (c->phys.back_reaction && c->phys.drag_solver >= DUSTB_SOLVER_DC1) {
+      int nsweeps = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
+      for (int w = 0; w < nsweeps; ++w) err |= oracle_cloud_dc1_sweep(c, a_dt, s);
+    }
+    oracle_ghost_copy(c, c->f.ustar, 3, 1);
+    oracle_gather_pack(c, c->f.ustar, gp);
+    err |= oracle_cloud_gather_kick(c, a_dt, s, gp);
+    if (c->phys.back_reaction) oracle_cloud_apply_pmbr(c, a_dt, s);
+    oracle_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0);
+  }
+  free(gp);
   return err;
 }
 

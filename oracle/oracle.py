@@ -78,6 +78,9 @@ def lib():
             "oracle_cloud_deposit_qp": ([P, D, D], C.c_uint),
             "oracle_gather_pack": ([P, VP, VP], None),
             "oracle_cloud_gather_kick": ([P, D, D, VP], C.c_uint),
+            "oracle_cloud_dc1_sweep": ([P, D, D], C.c_uint),
+            "oracle_cloud_apply_pmbr": ([P, D, D], None),
+            "oracle_cloud_imex_cycle": ([P, D, D, VP, VP], C.c_uint),
         }
         for name, (args, res) in sig.items():
             f = getattr(_lib, name)
@@ -282,6 +285,17 @@ class Oracle:
     def cloud_gather_kick(self, a_dt, sh=0.0, gp=None):
         gp = self.gather_pack() if gp is None else np.ascontiguousarray(gp, np.float64)
         return self.call("cloud_gather_kick", a_dt, sh, gp.ctypes.data)
+
+    def cloud_dc1_sweep(self, a_dt, sh=0.0):
+        return self.call("cloud_dc1_sweep", a_dt, sh)
+
+    def cloud_apply_pmbr(self, a_dt, sh=0.0):
+        self.call("cloud_apply_pmbr", a_dt, sh)
+
+    def cloud_imex_cycle(self, dt, gamma=GAMMA_DEFAULT, sh=(0.0, 0.0)):
+        shv = (C.c_double * 2)(*sh)
+        return self.call("cloud_imex_cycle", gamma, dt, C.cast(shv, C.c_void_p),
+                         self.x3_removed.ctypes.data)
 
     def point_science_fields(self, mass_only=False, species=-1):
         """DepositPointScienceFields: (out field with 1 or 4 vars, err)."""

@@ -113,3 +113,42 @@ def test_lobed_codes_are_flagged():
     st.pi[3, 5] = 1 | (1 << 6)                 # a lobe along x1: a transition cloud
     o = Oracle(st, dict(scheme=2))
     assert o.cloud_deposit_qp(1e-3) == ERR_CLOUD
+
+
+def lattice_pair():
+    """one particle per cell at its centre, gas and dust of uniform (different) velocities"""
+    ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3)
+    st = make_state(ms, [0.05], [2.0], 1, placement="lattice", vd=[0.03], gas_noise=0.0)
+    return ms, st
+
+
+def test_cloud_cycle_on_a_lattice_is_the_point_cycle():
+    """On a lattice of level-0 clouds every cell gets the same Q and the linear gather of a
+    uniform u* is u*: the cloud cycle (overlap split) equals the point-particle TSC cycle
+    (centre split), whose damping rate the oracle's known-answer tests pin."""
+    ms, st = lattice_pair()
+    phys = dict(scheme=2, drag_solver=2)
+    oc, op = Oracle(st, phys), Oracle(st, phys)
+    for _ in range(4):
+        assert oc.cloud_imex_cycle(0.004) == 0
+        assert op.imex_cycle(0.004) == 0
+    n = st.npart
+    for r in (1, 3, 5, 12, 13, 14):
+        sc = max(np.abs(op.st.pr[r, :n]).max(), 1e-300)
+        assert np.abs(oc.st.pr[r, :n] - op.st.pr[r, :n]).max() < 1e-12 * sc, r
+    for v in range(1, 4):
+        sc = max(np.abs(op.u0[:, v]).max(), 1e-300)
+        assert np.abs(oc.u0[:, v] - op.u0[:, v]).max() < 1e-12 * sc, v
+
+
+@pytest.mark.parametrize("solver", [0, 2, 3])
+def test_cloud_cycles_conserve_momentum(solver):
+    ms, st = setup((0, 1, 2), seed=13)
+    o = Oracle(st, dict(scheme=2, drag_solver=solver))
+    p0 = sum(o.momentum())
+    for _ in range(3):
+        assert o.cloud_imex_cycle(2e-3) == 0
+    p1 = sum(o.momentum())
+    n = st.npart
+    scale = np.abs(st.pr[16, :n] * np.abs(st.pr[[1, 3, 5], :n]).max(axis=0)).sum()
+    assert np.abs(p1 - p0).max() < 1e-13 * scale
