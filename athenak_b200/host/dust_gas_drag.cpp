@@ -35,6 +35,7 @@ DustGasDrag::~DustGasDrag() {
   if (cloud_ord_) cudaFree(cloud_ord_);
   if (cloud_ord_tag_) cudaFree(cloud_ord_tag_);
   if (dev_bad_) cudaFree(dev_bad_);
+  if (gpack_) cudaFree(gpack_);
 }
 
 TaskStatus DustGasDrag::Check(int rc, const char *task) {
@@ -93,12 +94,14 @@ TaskStatus DustGasDrag::DepositDrag(Driver *pdrive, int stage) {
     if (stage != 1) return TaskStatus::complete;   // the predictor
     return Check(dustb_pc2_predictor(&ctx_, pdrive->dt, 1, stream_), "DepositDrag");
   }
+  if (clouds_) return Check(dustb_cloud_deposit_qp(&ctx_, a_dt(pdrive), 0.0, stream_), "DepositDrag");
   return Check(dustb_deposit_qp(&ctx_, a_dt(pdrive), 0.0, stream_), "DepositDrag");
 }
 
 TaskStatus DustGasDrag::RecvDepQP(Driver *pdrive, int stage) {
   if (!ctx_.phys.back_reaction) return TaskStatus::complete;
   if (coupling_ == DustCoupling::pc2 && stage != 1) return TaskStatus::complete;
+  if (clouds_) return TaskStatus::complete;   // (the clouds deposit into the owner cells)
   return Check(dustb_ghost_add(&ctx_, ctx_.f.qdep, 5, stream_), "RecvDepQP");
 }
 
@@ -115,7 +118,9 @@ TaskStatus DustGasDrag::GasImplicitSolve(Driver *pdrive, int stage) {
   const int nsw = (ctx_.phys.drag_solver == DUSTB_SOLVER_DC2) ? 2
                 : (ctx_.phys.drag_solver == DUSTB_SOLVER_DC1) ? 1 : 0;
   for (int w = 0; w < nsw && ts == TaskStatus::complete; ++w)
-    ts = Check(dustb_dc1_sweep(&ctx_, a_dt(pdrive), 0.0, stream_), "SolveCoupledStage");
+    ts = clouds_ ? Check(dustb_cloud_dc1_sweep(&ctx_, a_dt(pdrive), 0.0, gpack_, stream_),
+                         "CloudDefectCorrection")
+                 : Check(dustb_dc1_sweep(&ctx_, a_dt(pdrive), 0.0, stream_), "SolveCoupledStage");
   return ts;
 }
 
@@ -126,12 +131,16 @@ TaskStatus DustGasDrag::RecvUstar(Driver *pdrive, int stage) {
 
 TaskStatus DustGasDrag::GatherKickPMBR(Driver *pdrive, int stage) {
   if (coupling_ == DustCoupling::pc2) return TaskStatus::complete;   // (inside the advance)
+  if (clouds_)   // CloudGatherImplicit3D (dust_imex3d.cpp:181-308)
+    return Check(dustb_cloud_gather_kick(&ctx_, a_dt(pdrive), 0.0, gpack_, stream_),
+                 "GatherKickPMBR");
   return Check(dustb_gather_kick_pmbr(&ctx_, a_dt(pdrive), 0.0, stream_), "GatherKickPMBR");
 }
 
 TaskStatus DustGasDrag::RecvPMBR(Driver *pdrive, int stage) {
   if (!ctx_.phys.back_reaction) return TaskStatus::complete;
   if (coupling_ == DustCoupling::pc2 && stage != 2) return TaskStatus::complete;
+  if (clouds_) return TaskStatus::complete;   // (the impulse went to the owner cells)
   return Check(dustb_ghost_add(&ctx_, ctx_.f.dmom, 3, stream_), "RecvPMBR");
 }
 
@@ -141,7 +150,25 @@ TaskStatus DustGasDrag::ApplyPMBR(Driver *pdrive, int stage) {
     if (stage != 2) return TaskStatus::complete;
     return Check(dustb_pc2_commit(&ctx_, 0.5, stream_), "ApplyPMBR");
   }
+  if (clouds_) return Check(dustb_cloud_apply_pmbr(&ctx_, a_dt(pdrive), 0.0, stream_), "ApplyPMBR");
   return Check(dustb_apply_pmbr(&ctx_, a_dt(pdrive), stream_), "ApplyPMBR");
+}
+
+TaskStatus DustGasDrag::SetRefinableClouds(bool on) {
+  if (on && coupling_ == DustCoupling::pc2) {
+    last_error_ = "SetRefinableClouds: the clouds of this build run the imex coupling";
+    return TaskStatus::fail;
+  }
+  if (on && !gpack_) {
+    const long long bytes = dustb_cloud_gpack_bytes(&ctx_.mesh);
+    if (bytes <= 0 || cudaMalloc(&gpack_, (size_t)bytes) != cudaSuccess) {
+      gpack_ = nullptr;
+      last_error_ = "SetRefinableClouds: gather pack not allocated";
+      return TaskStatus::fail;
+    }
+  }
+  clouds_ = on;
+  return TaskStatus::complete;
 }
 
 TaskStatus DustGasDrag::RecvU(Driver *pdrive, int stage) {

@@ -93,6 +93,12 @@ class DustGasDrag {
   TaskStatus DepositPointScienceFields(double time, double *out, double *halo, bool mass_only,
                                        int species);
 
+  // <dust>/smr_transfer = refinable_cloud on a uniform 3-D mesh (UsesRefinableClouds): the
+  // deposit, the dc1 / dc2 sweeps, the gather-kick and the PMBR split of the tasks run the
+  // clouds' kernels (PLEV = cloud level); their deposits land in the owner cells, so the
+  // deposit exchanges are skipped.  Allocates the gather pack; imex coupling only.
+  TaskStatus SetRefinableClouds(bool on);
+
   // the stage's drag tasks in dependency order on one rank and one stream
   TaskStatus DoStage(Driver *pdrive, int stage);
   // one cycle: every working stage
@@ -122,6 +128,8 @@ class DustGasDrag {
   int *dev_bad_ = nullptr;
   int cloud_ord_cap_ = 0, cloud_ord_n_ = 0, cloud_sort_cycle_ = -1, cloud_ord_builds_ = 0;
   int cloud_order_interval_ = 0;
+  bool clouds_ = false;
+  double *gpack_ = nullptr;   // the clouds' gather pack (12 doubles per padded cell)
 };
 
 // The mixed-precision form from the host (dustb_mixed_*): a compact FP32 shadow of the

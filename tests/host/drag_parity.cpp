@@ -22,6 +22,8 @@ extern "C" {
 unsigned oracle_imex_cycle(const dustb_ctx *c, double gamma, double dt, const double sh[2],
                            double *x3_removed);
 unsigned oracle_pc2_cycle(const dustb_ctx *c, double dt, double *chi_out, double *x3_removed);
+unsigned oracle_cloud_imex_cycle(const dustb_ctx *c, double gamma, double dt, const double sh[2],
+                                 double *x3_removed);
 void oracle_ghost_copy(const dustb_ctx *c, double *a, int nvar, int x3_bcs);
 void oracle_set_threads(int n);
 void oracle_cloud_order(const dustb_ctx *c, int *ord, uint64_t *tag);
@@ -167,7 +169,8 @@ bool cloud_order_checks(athenak_b200::DustGasDrag &drag, int npart, std::vector<
 // stated tolerance (velocities 1e-5 of their scale, positions 1e-5 of a cell, the gas
 // momentum 1e-5 of its scale); the gas ghost cells first take the copy exchange the mixed
 // form reads through the owning blocks
-int run(athenak_b200::DustCoupling coupling, const char *name, bool mixed = false) {
+int run(athenak_b200::DustCoupling coupling, const char *name, bool mixed = false,
+        bool clouds = false) {
   const int ppc = 2, nsp = 2;
   const int npart = NMB * NX * NX * NX * ppc * nsp;
   std::vector<double> mb; std::vector<int> ng;
@@ -226,6 +229,18 @@ int run(athenak_b200::DustCoupling coupling, const char *name, bool mixed = fals
   drv.SetImEx2PlusCoefficients(1.0 + 1.0 / std::sqrt(2.0));
   drv.dt = 2e-3;
   athenak_b200::DustGasDrag drag(dc, nullptr, coupling);
+  if (clouds) {
+    // refinable clouds of levels 0-3 on a periodic box (the shearing box's push terms kept,
+    // its faces plain periodic here)
+    std::vector<int> lev(npart);
+    for (int p = 0; p < npart; ++p) lev[p] = p % 4;
+    cudaMemcpy(d.pi + (size_t)3 * npart, lev.data(), sizeof(int) * npart, cudaMemcpyHostToDevice);
+    std::memcpy(hpi.data() + (size_t)3 * npart, lev.data(), sizeof(int) * npart);
+    if (drag.SetRefinableClouds(true) != athenak_b200::TaskStatus::complete) {
+      std::printf("%s: %s\n", name, drag.LastError().c_str());
+      return 1;
+    }
+  }
   const double sh[2] = {0.0, 0.0};
   double x3o[2] = {0.0, 0.0}, chi = 0.0;
   unsigned oerr = 0;
@@ -248,7 +263,8 @@ int run(athenak_b200::DustCoupling coupling, const char *name, bool mixed = fals
       std::printf("%s: task failed: %s%s\n", name, drag.LastError().c_str(), mx.LastError().c_str());
       return 1;
     }
-    oerr |= (coupling == athenak_b200::DustCoupling::imex)
+    oerr |= clouds ? oracle_cloud_imex_cycle(&hc, drv.gamma, drv.dt, sh, x3o)
+            : (coupling == athenak_b200::DustCoupling::imex)
                 ? oracle_imex_cycle(&hc, drv.gamma, drv.dt, sh, x3o)
                 : oracle_pc2_cycle(&hc, drv.dt, &chi, x3o);
   }
@@ -282,7 +298,7 @@ int run(athenak_b200::DustCoupling coupling, const char *name, bool mixed = fals
               "(scale %.3e), PGID %s, error words %u/%u: %s\n",
               name, npart, dx, dv, vs, du, us, pgid ? "identical" : "DIFFER", gerr, oerr,
               ok ? "ok" : "MISMATCH");
-  const bool cord = mixed || coupling != athenak_b200::DustCoupling::imex ||
+  const bool cord = mixed || clouds || coupling != athenak_b200::DustCoupling::imex ||
                     cloud_order_checks(drag, npart, mb, ng);
   for (int f = 0; f < 7; ++f) cudaFree(*fd[f]);
   cudaFree(d.pr); cudaFree(d.pi); cudaFree(d.mb); cudaFree(d.nghbr); cudaFree(d.sbgid);
@@ -299,5 +315,6 @@ int main() {
   bad += run(athenak_b200::DustCoupling::pc2, "pc2 cycles");
   bad += run(athenak_b200::DustCoupling::imex, "mixed imex2+/dc2 cycles", true);
   bad += run(athenak_b200::DustCoupling::pc2, "mixed pc2 cycles", true);
+  bad += run(athenak_b200::DustCoupling::imex, "refinable-cloud imex2+/dc2 cycles", false, true);
   return bad ? 1 : 0;
 }
