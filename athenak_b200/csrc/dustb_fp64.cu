@@ -1345,17 +1345,31 @@ __device__ bool cloud_load(const PCtx &P, const MCtx &M, const Ind &d, int p, do
                            const double L[3], int &m, double x[3], int &lev) {
   m = P.i(DUSTB_PGID, p) - M.gids;
   lev = P.i(DUSTB_PLEV, p);
+  // (2-D: no orbital-advection shift, no x3, LeafApi<LeafTraversal>::LoadImplicit)
   x[0] = P.r(DUSTB_IPX, p);
-  x[1] = P.r(DUSTB_IPY, p) + sh * P.r(DUSTB_IPX, p);
-  x[2] = P.r(DUSTB_IPZ, p);
+  x[1] = d.three_d ? P.r(DUSTB_IPY, p) + sh * P.r(DUSTB_IPX, p) : P.r(DUSTB_IPY, p);
+  x[2] = d.three_d ? P.r(DUSTB_IPZ, p) : 0.0;
   if (!block_ok(d, m) || (lev & ~15) != 0) return false;
   const int nx[3] = {d.nx1, d.nx2, d.nx3};
-  for (int a = 0; a < 3; ++a) {
+  for (int a = 0; a < (d.three_d ? 3 : 2); ++a) {
     const double cx = M.s(m, X1MIN + a) + 0.5 * nx[a] * M.s(m, DX1 + a);
     x[a] -= L[a] * round((x[a] - cx) * (1.0 / L[a]));
     if (!(x[a] >= M.s(m, X1MIN + a) && x[a] < M.s(m, X1MAX + a))) return false;
   }
   return true;
+}
+
+// the three directions of a cloud; 2-D: a unit z axis (w = w2 w1 and the moments bit for bit)
+__device__ void cloud_axes(const MCtx &M, const Ind &d, int m, const double x[3], int lev,
+                           const double L[3], CloudAxis &X, CloudAxis &Y, CloudAxis &Z) {
+  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
+  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
+  if (d.three_d) { cloud_axis(M, d, m, 2, x[2], lev, L[2], Z); return; }
+  Z.n = 1; Z.o[0] = 0; Z.i[0] = 0; Z.w[0] = 1.0; Z.g[0] = 0.0;
+}
+// the cell measure: the volume, 2-D the area (LeafApi::Measure)
+__device__ __forceinline__ double cloud_measure(const MCtx &M, const Ind &d, int b) {
+  return d.three_d ? M.s(b, DX1) * M.s(b, DX2) * M.s(b, DX3) : M.s(b, DX1) * M.s(b, DX2);
 }
 
 __device__ __forceinline__ int cloud_owner(const MCtx &M, const Ind &d, int m, int ox, int oy,
@@ -1375,12 +1389,11 @@ __global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt
   int m, lev;
   double x[3];
   if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
-  const double mass_c = P.r(DUSTB_IPM, p) * a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
+  const double mass_c = d.three_d ? P.r(DUSTB_IPM, p) * a_dt / (P.r(DUSTB_IPTS, p) + a_dt)
+                                  : P.r(DUSTB_IPM, p) * (a_dt / (P.r(DUSTB_IPTS, p) + a_dt));
   const double vx = P.r(DUSTB_IPVX, p), vy = P.r(DUSTB_IPVY, p), vz = P.r(DUSTB_IPVZ, p);
   CloudAxis X, Y, Z;
-  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
-  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
-  cloud_axis(M, d, m, 2, x[2], lev, L[2], Z);
+  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
   for (int kz = 0; kz < Z.n; ++kz) {
     if (Z.w[kz] == 0.0) continue;
     for (int jy = 0; jy < Y.n; ++jy) {
@@ -1391,7 +1404,7 @@ __global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt
         if (w == 0.0) continue;
         const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
         if (b < 0) { report(err, DUSTB_ERR_CLOUD); continue; }
-        const double dw = mass_c * w / (M.s(b, DX1) * M.s(b, DX2) * M.s(b, DX3));
+        const double dw = mass_c * w / cloud_measure(M, d, b);
         const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
         atomicAdd(&qdep[d.at(b, 5, 0, k, j, i)], dw);
         atomicAdd(&qdep[d.at(b, 5, 1, k, j, i)], dw * vx);
@@ -1414,13 +1427,15 @@ __global__ void k_gather_pack(Ind d, const double *v, double *gp) {
   const int j = (int)(r % d.n2);
   const int k = (int)(r / d.n2);
   double *g = gp + idx * 12;
-  const bool in = i >= 1 && i < d.n1 - 1 && j >= 1 && j < d.n2 - 1 && k >= 1 && k < d.n3 - 1;
+  // (2-D: PackGatherField, src/dust/dust_pm.cpp:81-102: the plane ks, no x3 differences)
+  const bool kin = d.three_d ? (k >= 1 && k < d.n3 - 1) : (k == d.ks);
+  const bool in = i >= 1 && i < d.n1 - 1 && j >= 1 && j < d.n2 - 1 && kin;
   for (int q = 0; q < 3; ++q) {
     if (!in) { g[q] = g[3 + q] = g[6 + q] = g[9 + q] = 0.0; continue; }
     g[q] = v[d.at(m, 3, q, k, j, i)];
     g[3 + q] = v[d.at(m, 3, q, k, j, i + 1)] - v[d.at(m, 3, q, k, j, i - 1)];
     g[6 + q] = v[d.at(m, 3, q, k, j + 1, i)] - v[d.at(m, 3, q, k, j - 1, i)];
-    g[9 + q] = v[d.at(m, 3, q, k + 1, j, i)] - v[d.at(m, 3, q, k - 1, j, i)];
+    g[9 + q] = d.three_d ? v[d.at(m, 3, q, k + 1, j, i)] - v[d.at(m, 3, q, k - 1, j, i)] : 0.0;
   }
 }
 
@@ -1437,9 +1452,7 @@ __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, dou
   double x[3];
   if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
   CloudAxis X, Y, Z;
-  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
-  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
-  cloud_axis(M, d, m, 2, x[2], lev, L[2], Z);
+  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
   double ug[3] = {0.0, 0.0, 0.0};
   for (int kz = 0; kz < Z.n; ++kz) {
     const double w3 = Z.w[kz], g3 = Z.g[kz];
@@ -1463,11 +1476,17 @@ __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, dou
         const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
         const double cx = 0.5 * (m1x + (ex - L[0] * round(ex / L[0])) * w) / dx1;
         const double cy = 0.5 * (m1y + (ey - L[1] * round(ey / L[1])) * w) / dx2;
-        const double cz = 0.5 * (m1z + (ez - L[2] * round(ez / L[2])) * w) / dx3;
         const double *g = gp + ((((long long)b * d.n3 + k) * d.n2 + j) * d.n1 + i) * 12;
-        ug[0] += w * g[0] + cx * g[3] + cy * g[6] + cz * g[9];
-        ug[1] += w * g[1] + cx * g[4] + cy * g[7] + cz * g[10];
-        ug[2] += w * g[2] + cx * g[5] + cy * g[8] + cz * g[11];
+        if (d.three_d) {
+          const double cz = 0.5 * (m1z + (ez - L[2] * round(ez / L[2])) * w) / dx3;
+          ug[0] += w * g[0] + cx * g[3] + cy * g[6] + cz * g[9];
+          ug[1] += w * g[1] + cx * g[4] + cy * g[7] + cz * g[10];
+          ug[2] += w * g[2] + cx * g[5] + cy * g[8] + cz * g[11];
+        } else {
+          ug[0] += w * g[0] + cx * g[3] + cy * g[6];
+          ug[1] += w * g[1] + cx * g[4] + cy * g[7];
+          ug[2] += w * g[2] + cx * g[5] + cy * g[8];
+        }
       }
     }
   }
@@ -1490,7 +1509,7 @@ __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, dou
         if (w == 0.0) continue;
         const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
         if (b < 0) continue;
-        const double dw = mass * w / (M.s(b, DX1) * M.s(b, DX2) * M.s(b, DX3));
+        const double dw = mass * w / cloud_measure(M, d, b);
         const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
         atomicAdd(&dmom[d.at(b, 3, 0, k, j, i)], dw * dvx);
         atomicAdd(&dmom[d.at(b, 3, 1, k, j, i)], dw * dvy);
@@ -1528,11 +1547,17 @@ __device__ void cloud_gather(const MCtx &M, const Ind &d, int m, const double x[
         const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
         const double cx = 0.5 * (m1x + (ex - L[0] * round(ex / L[0])) * w) / dx1;
         const double cy = 0.5 * (m1y + (ey - L[1] * round(ey / L[1])) * w) / dx2;
-        const double cz = 0.5 * (m1z + (ez - L[2] * round(ez / L[2])) * w) / dx3;
         const double *g = gp + ((((long long)b * d.n3 + k) * d.n2 + j) * d.n1 + i) * 12;
-        ug[0] += w * g[0] + cx * g[3] + cy * g[6] + cz * g[9];
-        ug[1] += w * g[1] + cx * g[4] + cy * g[7] + cz * g[10];
-        ug[2] += w * g[2] + cx * g[5] + cy * g[8] + cz * g[11];
+        if (d.three_d) {
+          const double cz = 0.5 * (m1z + (ez - L[2] * round(ez / L[2])) * w) / dx3;
+          ug[0] += w * g[0] + cx * g[3] + cy * g[6] + cz * g[9];
+          ug[1] += w * g[1] + cx * g[4] + cy * g[7] + cz * g[10];
+          ug[2] += w * g[2] + cx * g[5] + cy * g[8] + cz * g[11];
+        } else {
+          ug[0] += w * g[0] + cx * g[3] + cy * g[6];
+          ug[1] += w * g[1] + cx * g[4] + cy * g[7];
+          ug[2] += w * g[2] + cx * g[5] + cy * g[8];
+        }
       }
     }
   }
@@ -1549,9 +1574,7 @@ __global__ void k_cloud_operator(PCtx P, MCtx M, Ind d, const double *gp, double
   double x[3];
   if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
   CloudAxis X, Y, Z;
-  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
-  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
-  cloud_axis(M, d, m, 2, x[2], lev, L[2], Z);
+  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
   double ug[3];
   cloud_gather(M, d, m, x, X, Y, Z, L, gp, ug, err);
   const double mc = P.r(DUSTB_IPM, p) * (a_dt / (P.r(DUSTB_IPTS, p) + a_dt));
@@ -1565,7 +1588,7 @@ __global__ void k_cloud_operator(PCtx P, MCtx M, Ind d, const double *gp, double
         if (w == 0.0) continue;
         const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
         if (b < 0) continue;
-        const double dw = mc * w / (M.s(b, DX1) * M.s(b, DX2) * M.s(b, DX3));
+        const double dw = mc * w / cloud_measure(M, d, b);
         const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
         atomicAdd(&result[d.at(b, 3, 0, k, j, i)], dw * ug[0]);
         atomicAdd(&result[d.at(b, 3, 1, k, j, i)], dw * ug[1]);
@@ -1608,9 +1631,7 @@ __global__ void k_cloud_consistent_dust(PCtx P, MCtx M, Ind d, const double *res
   double x[3];
   if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) return;
   CloudAxis X, Y, Z;
-  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
-  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
-  cloud_axis(M, d, m, 2, x[2], lev, L[2], Z);
+  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
   double rv[3] = {0.0, 0.0, 0.0};
   for (int kz = 0; kz < Z.n; ++kz) {
     if (Z.w[kz] == 0.0) continue;
@@ -1953,7 +1974,7 @@ int dustb_phst(const dustb_ctx *c, const double *chi_max, double *row, void *scr
 // ---- refinable clouds on a uniform 3-D mesh (periodic; plain P1 hat clouds) ---------------
 static int cloud_mesh_ok(const dustb_ctx *c) {
   const dustb_mesh &ms = c->mesh;
-  return ms.three_d && !ms.shear_x1 && ms.x3bc == DUSTB_X3_PERIODIC;
+  return ms.multi_d && !ms.shear_x1 && (!ms.three_d || ms.x3bc == DUSTB_X3_PERIODIC);
 }
 
 long long dustb_cloud_gpack_bytes(const dustb_mesh *mesh) {

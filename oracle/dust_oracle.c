@@ -1051,7 +1051,7 @@ static void cloud_frame(const dustb_ctx *c, int m, double x[3]) {
   const dustb_mesh *ms = &c->mesh;
   const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
   const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
-  for (int a = 0; a < 3; ++a) {
+  for (int a = 0; a < (ms->three_d ? 3 : 2); ++a) {
     const double cx = MB(m, X1MIN + a) + 0.5*nx[a]*MB(m, DX1 + a);
     x[a] -= L[a]*round((x[a] - cx)*(1.0/L[a]));
   }
@@ -1061,9 +1061,33 @@ static void cloud_frame(const dustb_ctx *c, int m, double x[3]) {
 static int cloud_ok(const dustb_ctx *c, int m, const double x[3], int code) {
   const dustb_mesh *ms = &c->mesh;
   if (m < 0 || m >= ms->nmb || (code & ~15) != 0) return 0;
-  for (int a = 0; a < 3; ++a)
+  for (int a = 0; a < (ms->three_d ? 3 : 2); ++a)
     if (!(x[a] >= MB(m, X1MIN + a) && x[a] < MB(m, X1MAX + a))) return 0;
   return 1;
+}
+
+/* the 2-D form (LeafApi<LeafTraversal>, src/dust/dust_leaf_api.hpp:31-146): no x3 direction
+ * (a unit z axis: w = w2 w1, the moments w2 g1 and w1 g2 bit for bit), no orbital-advection
+ * shift of the position, the cell area as the measure, the coupled mass m (a_dt / (t_s +
+ * a_dt)) */
+static void cloud_axes(const dustb_ctx *c, int m, const double x[3], int code, CloudAxis *X,
+                       CloudAxis *Y, CloudAxis *Z) {
+  cloud_axis(c, m, 0, x[0], code, X);
+  cloud_axis(c, m, 1, x[1], code, Y);
+  if (c->mesh.three_d) { cloud_axis(c, m, 2, x[2], code, Z); return; }
+  Z->n = 1; Z->o[0] = 0; Z->i[0] = 0; Z->w[0] = 1.0; Z->g[0] = 0.0;
+}
+static void cloud_position(const dustb_ctx *c, int p, double sh, double x[3]) {
+  const double *pr = c->part.pr; long long stride = c->part.stride;
+  if (c->mesh.three_d) {
+    x[0] = PR(DUSTB_IPX, p); x[1] = PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p); x[2] = PR(DUSTB_IPZ, p);
+  } else {
+    x[0] = PR(DUSTB_IPX, p); x[1] = PR(DUSTB_IPY, p); x[2] = 0.0;
+  }
+}
+static double cloud_measure(const dustb_ctx *c, int b) {
+  const dustb_mesh *ms = &c->mesh;
+  return ms->three_d ? MB(b, DX1)*MB(b, DX2)*MB(b, DX3) : MB(b, DX1)*MB(b, DX2);
 }
 
 /* the owner block of a leaf in direction (ox, oy, oz) of m */
@@ -1083,16 +1107,16 @@ unsigned oracle_cloud_deposit_qp(const dustb_ctx *c, double a_dt, double sh) {
   unsigned err = 0;
   for (int p = 0; p < c->part.npart; ++p) {
     const int m = PI(DUSTB_PGID, p) - ms->gids;
-    double x[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p), PR(DUSTB_IPZ, p)};
+    double x[3];
+    cloud_position(c, p, sh, x);
     const int code = PI(DUSTB_PLEV, p);
     if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
     if (!cloud_ok(c, m, x, code)) { err |= DUSTB_ERR_CLOUD; continue; }
-    const double mass_c = PR(DUSTB_IPM, p)*a_dt/(PR(DUSTB_IPTS, p) + a_dt);
+    const double mass_c = ms->three_d ? PR(DUSTB_IPM, p)*a_dt/(PR(DUSTB_IPTS, p) + a_dt)
+                                      : PR(DUSTB_IPM, p)*(a_dt/(PR(DUSTB_IPTS, p) + a_dt));
     const double vx = PR(DUSTB_IPVX, p), vy = PR(DUSTB_IPVY, p), vz = PR(DUSTB_IPVZ, p);
     CloudAxis X, Y, Z;
-    cloud_axis(c, m, 0, x[0], code, &X);
-    cloud_axis(c, m, 1, x[1], code, &Y);
-    cloud_axis(c, m, 2, x[2], code, &Z);
+    cloud_axes(c, m, x, code, &X, &Y, &Z);
     for (int kz = 0; kz < Z.n; ++kz) {
       if (Z.w[kz] == 0.0) continue;
       for (int jy = 0; jy < Y.n; ++jy) {
@@ -1103,7 +1127,7 @@ unsigned oracle_cloud_deposit_qp(const dustb_ctx *c, double a_dt, double sh) {
           if (w == 0.0) continue;
           const int b = cloud_owner(c, m, X.o[ix], Y.o[jy], Z.o[kz]);
           if (b < 0) { err |= DUSTB_ERR_CLOUD; continue; }
-          const double dw = mass_c*w/(MB(b, DX1)*MB(b, DX2)*MB(b, DX3));
+          const double dw = mass_c*w/cloud_measure(c, b);
           const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
           A5(c->f.qdep, 5, d, b, 0, k, j, i) += dw;
           A5(c->f.qdep, 5, d, b, 1, k, j, i) += dw*vx;
@@ -1121,8 +1145,10 @@ unsigned oracle_cloud_deposit_qp(const dustb_ctx *c, double a_dt, double sh) {
 void oracle_gather_pack(const dustb_ctx *c, const double *v, double *gp) {
   const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
   memset(gp, 0, (size_t)ms->nmb*d.n3*d.n2*d.n1*12*sizeof(double));
+  /* (2-D: PackGatherField, src/dust/dust_pm.cpp:81-102, the plane ks and no x3 differences) */
+  const int k0 = ms->three_d ? 1 : d.ks, k1 = ms->three_d ? d.n3 - 2 : d.ks;
   for (int m = 0; m < ms->nmb; ++m)
-    for (int k = 1; k < d.n3 - 1; ++k)
+    for (int k = k0; k <= k1; ++k)
       for (int j = 1; j < d.n2 - 1; ++j)
         for (int i = 1; i < d.n1 - 1; ++i) {
           double *g = gp + ((((size_t)m*d.n3 + k)*d.n2 + j)*d.n1 + i)*12;
@@ -1130,7 +1156,8 @@ void oracle_gather_pack(const dustb_ctx *c, const double *v, double *gp) {
             g[q] = A5(v, 3, d, m, q, k, j, i);
             g[3 + q] = A5(v, 3, d, m, q, k, j, i + 1) - A5(v, 3, d, m, q, k, j, i - 1);
             g[6 + q] = A5(v, 3, d, m, q, k, j + 1, i) - A5(v, 3, d, m, q, k, j - 1, i);
-            g[9 + q] = A5(v, 3, d, m, q, k + 1, j, i) - A5(v, 3, d, m, q, k - 1, j, i);
+            if (ms->three_d)
+              g[9 + q] = A5(v, 3, d, m, q, k + 1, j, i) - A5(v, 3, d, m, q, k - 1, j, i);
           }
         }
 }
@@ -1150,14 +1177,13 @@ unsigned oracle_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, co
   unsigned err = 0;
   for (int p = 0; p < c->part.npart; ++p) {
     const int m = PI(DUSTB_PGID, p) - ms->gids;
-    double x[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p), PR(DUSTB_IPZ, p)};
+    double x[3];
+    cloud_position(c, p, sh, x);
     const int code = PI(DUSTB_PLEV, p);
     if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
     if (!cloud_ok(c, m, x, code)) { err |= DUSTB_ERR_CLOUD; continue; }
     CloudAxis X, Y, Z;
-    cloud_axis(c, m, 0, x[0], code, &X);
-    cloud_axis(c, m, 1, x[1], code, &Y);
-    cloud_axis(c, m, 2, x[2], code, &Z);
+    cloud_axes(c, m, x, code, &X, &Y, &Z);
     double ug[3] = {0.0, 0.0, 0.0};
     int nt = 0, tb[216], tk[216], tj[216], ti[216];
     double tw[216];
@@ -1183,11 +1209,17 @@ unsigned oracle_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, co
           const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
           const double cx = 0.5*(m1x + (ex - L[0]*round(ex/L[0]))*w)/dx1;
           const double cy = 0.5*(m1y + (ey - L[1]*round(ey/L[1]))*w)/dx2;
-          const double cz = 0.5*(m1z + (ez - L[2]*round(ez/L[2]))*w)/dx3;
           const double *g = gp + ((((size_t)b*d.n3 + k)*d.n2 + j)*d.n1 + i)*12;
-          ug[0] += w*g[0] + cx*g[3] + cy*g[6] + cz*g[9];
-          ug[1] += w*g[1] + cx*g[4] + cy*g[7] + cz*g[10];
-          ug[2] += w*g[2] + cx*g[5] + cy*g[8] + cz*g[11];
+          if (ms->three_d) {
+            const double cz = 0.5*(m1z + (ez - L[2]*round(ez/L[2]))*w)/dx3;
+            ug[0] += w*g[0] + cx*g[3] + cy*g[6] + cz*g[9];
+            ug[1] += w*g[1] + cx*g[4] + cy*g[7] + cz*g[10];
+            ug[2] += w*g[2] + cx*g[5] + cy*g[8] + cz*g[11];
+          } else {
+            ug[0] += w*g[0] + cx*g[3] + cy*g[6];
+            ug[1] += w*g[1] + cx*g[4] + cy*g[7];
+            ug[2] += w*g[2] + cx*g[5] + cy*g[8];
+          }
           tb[nt] = b; tk[nt] = k; tj[nt] = j; ti[nt] = i; tw[nt] = w;
           ++nt;
         }
@@ -1204,7 +1236,7 @@ unsigned oracle_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, co
     for (int q = 0; q < nt; ++q) {
       if (tw[q] == 0.0) continue;
       const int b = tb[q];
-      const double dw = mass*tw[q]/(MB(b, DX1)*MB(b, DX2)*MB(b, DX3));
+      const double dw = mass*tw[q]/cloud_measure(c, b);
       A5(c->f.dmom, 3, d, b, 0, tk[q], tj[q], ti[q]) += dw*dvx;
       A5(c->f.dmom, 3, d, b, 1, tk[q], tj[q], ti[q]) += dw*dvy;
       A5(c->f.dmom, 3, d, b, 2, tk[q], tj[q], ti[q]) += dw*dvz;
@@ -1221,9 +1253,7 @@ static int cloud_gather(const dustb_ctx *c, const Ind *d, int m, const double x[
   const dustb_mesh *ms = &c->mesh;
   const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
   CloudAxis X, Y, Z;
-  cloud_axis(c, m, 0, x[0], code, &X);
-  cloud_axis(c, m, 1, x[1], code, &Y);
-  cloud_axis(c, m, 2, x[2], code, &Z);
+  cloud_axes(c, m, x, code, &X, &Y, &Z);
   ug[0] = ug[1] = ug[2] = 0.0;
   int nt = 0;
   for (int kz = 0; kz < Z.n; ++kz) {
@@ -1248,11 +1278,17 @@ static int cloud_gather(const dustb_ctx *c, const Ind *d, int m, const double x[
         const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
         const double cx = 0.5*(m1x + (ex - L[0]*round(ex/L[0]))*w)/dx1;
         const double cy = 0.5*(m1y + (ey - L[1]*round(ey/L[1]))*w)/dx2;
-        const double cz = 0.5*(m1z + (ez - L[2]*round(ez/L[2]))*w)/dx3;
         const double *g = gp + ((((size_t)b*d->n3 + k)*d->n2 + j)*d->n1 + i)*12;
-        ug[0] += w*g[0] + cx*g[3] + cy*g[6] + cz*g[9];
-        ug[1] += w*g[1] + cx*g[4] + cy*g[7] + cz*g[10];
-        ug[2] += w*g[2] + cx*g[5] + cy*g[8] + cz*g[11];
+        if (ms->three_d) {
+          const double cz = 0.5*(m1z + (ez - L[2]*round(ez/L[2]))*w)/dx3;
+          ug[0] += w*g[0] + cx*g[3] + cy*g[6] + cz*g[9];
+          ug[1] += w*g[1] + cx*g[4] + cy*g[7] + cz*g[10];
+          ug[2] += w*g[2] + cx*g[5] + cy*g[8] + cz*g[11];
+        } else {
+          ug[0] += w*g[0] + cx*g[3] + cy*g[6];
+          ug[1] += w*g[1] + cx*g[4] + cy*g[7];
+          ug[2] += w*g[2] + cx*g[5] + cy*g[8];
+        }
         if (w != 0.0) { tb[nt] = b; tk[nt] = k; tj[nt] = j; ti[nt] = i; tw[nt] = w; ++nt; }
       }
     }
@@ -1277,7 +1313,8 @@ unsigned oracle_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh) {
   double tw[216];
   for (int p = 0; p < c->part.npart; ++p) {
     const int m = PI(DUSTB_PGID, p) - ms->gids;
-    double xp[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p), PR(DUSTB_IPZ, p)};
+    double xp[3];
+    cloud_position(c, p, sh, xp);
     const int code = PI(DUSTB_PLEV, p);
     if (m >= 0 && m < ms->nmb) cloud_frame(c, m, xp);
     if (!cloud_ok(c, m, xp, code)) { err |= DUSTB_ERR_CLOUD; continue; }
@@ -1286,7 +1323,7 @@ unsigned oracle_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh) {
     const double mc = PR(DUSTB_IPM, p)*(a_dt/(PR(DUSTB_IPTS, p) + a_dt));
     for (int q = 0; q < nt; ++q) {
       const int b = tb[q];
-      const double dw = mc*tw[q]/(MB(b, DX1)*MB(b, DX2)*MB(b, DX3));
+      const double dw = mc*tw[q]/cloud_measure(c, b);
       A5(r, 3, d, b, 0, tk[q], tj[q], ti[q]) += dw*ug[0];
       A5(r, 3, d, b, 1, tk[q], tj[q], ti[q]) += dw*ug[1];
       A5(r, 3, d, b, 2, tk[q], tj[q], ti[q]) += dw*ug[2];
@@ -1341,14 +1378,13 @@ void oracle_cloud_apply_pmbr(const dustb_ctx *c, double a_dt, double sh) {
   for (int p = 0; p < c->part.npart; ++p) {
     if (PR(DUSTB_IPM, p) <= 0.0) continue;
     const int m = PI(DUSTB_PGID, p) - ms->gids;
-    double x[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p) + sh*PR(DUSTB_IPX, p), PR(DUSTB_IPZ, p)};
+    double x[3];
+    cloud_position(c, p, sh, x);
     const int code = PI(DUSTB_PLEV, p);
     if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
     if (!cloud_ok(c, m, x, code)) continue;
     CloudAxis X, Y, Z;
-    cloud_axis(c, m, 0, x[0], code, &X);
-    cloud_axis(c, m, 1, x[1], code, &Y);
-    cloud_axis(c, m, 2, x[2], code, &Z);
+    cloud_axes(c, m, x, code, &X, &Y, &Z);
     double rv[3] = {0.0, 0.0, 0.0};
     for (int kz = 0; kz < Z.n; ++kz) {
       if (Z.w[kz] == 0.0) continue;

@@ -152,3 +152,67 @@ def test_cloud_cycles_conserve_momentum(solver):
     n = st.npart
     scale = np.abs(st.pr[16, :n] * np.abs(st.pr[[1, 3, 5], :n]).max(axis=0)).sum()
     assert np.abs(p1 - p0).max() < 1e-13 * scale
+
+
+# ---- 2-D clouds (LeafApi<LeafTraversal>: cell areas, m (a_dt / (t_s + a_dt)), 9-component pack)
+def setup2d(levels=(0,), seed=5, ppc=2):
+    ms = uniform_mesh((32, 32, 1), (16, 16, 1), 2, (-0.5,) * 3, (0.5,) * 3)
+    st = make_state(ms, [0.1, 0.01], [1.0, 0.5], ppc, seed=seed, vel_noise=0.05,
+                    gas_noise=1e-2)
+    n = st.npart
+    st.pi[3, :n] = np.asarray(levels)[np.arange(n) % len(levels)]
+    return ms, st
+
+
+def test_2d_level0_cloud_deposit_is_the_tsc_deposit_and_keeps_the_mass():
+    ms, st = setup2d((0,))
+    oc, op = Oracle(st, dict(scheme=2)), Oracle(st, dict(scheme=2))
+    a_dt = 1.3e-3
+    assert oc.cloud_deposit_qp(a_dt) == 0 and op.deposit_qp(a_dt) == 0
+    op.ghost_add("qdep", 5)
+    qa, qb = ms.active(oc.qdep)[:, :4], ms.active(op.qdep)[:, :4]
+    for v in range(4):
+        assert np.abs(qa[:, v] - qb[:, v]).max() < 1e-13 * np.abs(qb[:, v]).max(), v
+    ms2, st2 = setup2d((0, 1, 2, 3))
+    o = Oracle(st2, dict(scheme=2))
+    assert o.cloud_deposit_qp(a_dt) == 0
+    n = st2.npart
+    want = (st2.pr[16, :n] * (a_dt / (st2.pr[15, :n] + a_dt))).sum()
+    got = ms2.active(o.qdep)[:, 0].sum() * ms2.cell_volume()
+    assert abs(got - want) < 1e-13 * want
+
+
+def test_2d_linear_gather_and_lattice_cycle():
+    ms, st = setup2d((0, 1, 2), seed=9)
+    o = Oracle(st, dict(scheme=2, back_reaction=False))
+    n1, n2, _ = ms.n
+    is_, js, _ = ms.starts
+    us = np.zeros(ms.field_shape(3))
+    coef = np.array([[0.3, 1.5, -2.0], [-0.1, 0.4, 0.9], [0.05, -0.6, 0.2]])
+    for m in range(ms.nmb):
+        mb = ms.mb_size[m]
+        x = mb[0] + (np.arange(n1) - is_ + 0.5) * mb[6]
+        y = mb[1] + (np.arange(n2) - js + 0.5) * mb[7]
+        Y, X = np.meshgrid(y, x, indexing="ij")
+        for c in range(3):
+            us[m, c, 0] = coef[c, 0] + coef[c, 1] * X + coef[c, 2] * Y
+    o.arr["ustar"][...] = us
+    n = st.npart
+    o.st.pr[15, :n] = 1.0
+    assert o.cloud_gather_kick(1e300) == 0
+    xp = st.pr[[0, 2], :n]
+    want = coef[:, :1] + coef[:, 1:] @ xp
+    inner = np.all((xp > -0.5 + 2 / 32) & (xp < 0.5 - 2 / 32), axis=0)
+    assert inner.sum() > 100
+    assert np.abs(o.st.pr[[1, 3, 5], :n][:, inner] - want[:, inner]).max() < 1e-12
+    # the lattice: the cloud cycle is the point cycle
+    ms3 = uniform_mesh((32, 32, 1), (16, 16, 1), 2, (-0.5,) * 3, (0.5,) * 3)
+    st3 = make_state(ms3, [0.05], [2.0], 1, placement="lattice", vd=[0.03], gas_noise=0.0)
+    phys = dict(scheme=2, drag_solver=2)
+    oc, op = Oracle(st3, phys), Oracle(st3, phys)
+    for _ in range(3):
+        assert oc.cloud_imex_cycle(0.01) == 0 and op.imex_cycle(0.01) == 0
+    m3 = st3.npart
+    for r in (1, 3, 12, 13):
+        sc = max(np.abs(op.st.pr[r, :m3]).max(), 1e-300)
+        assert np.abs(oc.st.pr[r, :m3] - op.st.pr[r, :m3]).max() < 1e-12 * sc, r
