@@ -376,6 +376,10 @@ def run_ours(args, rep):
     ens = None
     if not args.no_ensemble:
         ens = measure_ensemble(args)
+    # ---- refinable clouds on the uniform root mesh of config 4 ----
+    clouds = None
+    if not args.no_clouds:
+        clouds = measure_clouds(args)
     if rank == 0:
         cb = None if args.no_cpu else cpu_baseline()
         line = {
@@ -404,6 +408,7 @@ def run_ours(args, rep):
             "e2e": e2e,
             "pc2_stratified": strat,
             "ensemble": ens,
+            "clouds": clouds,
         }
         if res.get("tuned"):
             line["config"]["tuned"] = res["tuned"]
@@ -562,6 +567,78 @@ def measure_ensemble(args):
             "worst_box": worst}
 
 
+def measure_clouds(args):
+    """Refinable clouds on config 4's root mesh without its refinement: 128^3 cells as 512
+    MeshBlocks of 16^3, 2 species tau_s = {0.1, 1}, eps 0.5 each, 8 clouds per cell each
+    (33.5 M level-0 P1 hat clouds), imex2+/dc1 with the overlap split, FP64 (the clouds' reference
+    layout kernels); the point-particle TSC cycle of the same particles beside it, and the
+    total momentum change of the cloud cycles."""
+    import numpy as np
+    import torch
+    from athenak_b200 import capi
+    from athenak_b200.drag import DeviceDust
+    from athenak_b200.mesh import uniform_mesh
+    cells = (32, 32, 32) if args.small else (128, 128, 128)
+    ms = uniform_mesh(cells, (16, 16, 16), 2, (-0.5,) * 3, (0.5,) * 3)
+    ppc, taus, eps = 8, [0.1, 1.0], [0.5, 0.5]
+    ncell = ms.ncell_active
+    npart = ncell * ppc * len(taus)
+    phys = dict(scheme=2, drag_solver=2, back_reaction=True)
+    dev = DeviceDust.empty(ms, npart, phys, nspecies=len(taus))
+    d = capi.DustbSeedDesc()
+    d.seed, d.nspecies = 4, len(taus)
+    for s_, (t, e) in enumerate(zip(taus, eps)):
+        d.ppc[s_], d.taus[s_], d.mass[s_] = ppc, t, e / (ncell * ppc)
+        d.vx[s_], d.vy[s_], d.vz[s_] = 0.01 * (s_ + 1), -0.02, 0.005
+    d.vel_noise, d.rho0, d.gas_noise = 1e-2, 1.0, 1e-3
+    d.nb1, d.nb2, d.nb3 = ms.nblocks
+    dev.seed_uniform(d)
+    dev.init_gas_ghosts()
+    dt = 0.3 / cells[0]
+    pr0, pi0, u00 = dev.t["pr"].clone(), dev.t["pi"].clone(), dev.t["u0"].clone()
+    steps = max(1, min(args.steps, 3))
+
+    def timed(cycle):
+        cycle()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            cycle()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / steps
+
+    def scale():
+        pr = dev.t["pr"][:, :npart]
+        m = pr[16]
+        dsum = torch.stack([(m * pr[r]).abs().sum() for r in (1, 3, 5)])
+        u0 = ms.active(dev.t["u0"])
+        gsum = u0[:, 1:4].abs().sum(dim=(0, 2, 3, 4)) * ms.cell_volume()
+        return float((dsum + gsum).max())
+
+    p0 = sum(dev.momentum())
+    sc = scale()
+    ms_cloud = timed(lambda: dev.cloud_imex_cycle(dt))
+    p1 = sum(dev.momentum())
+    err_cloud = dev.error_word()
+    dev.t["pr"].copy_(pr0); dev.t["pi"].copy_(pi0); dev.t["u0"].copy_(u00)
+    ms_point = timed(lambda: dev.imex_cycle(dt))
+    err_point = dev.error_word()
+    out = {"workload": f"{cells[0]}^3 uniform mesh (config 4's root mesh, no refinement), "
+                       f"{ms.nmb} MeshBlocks of 16^3, 2 species tau_s 0.1, 1, eps 0.5 each, "
+                       f"8 level-0 P1 hat clouds per cell each, imex2+/dc1, overlap split, FP64",
+           "particles": npart, "cells": ncell, "dt": dt, "steps": steps,
+           "value": npart / (ms_cloud * 1e-3), "unit": UNIT, "ms_per_step": ms_cloud,
+           "timed": "CUDA events around eager cycles after one warm-up cycle",
+           "fp64_points_tsc": {"ms_per_step": ms_point, "value": npart / (ms_point * 1e-3)},
+           "momentum_change_rel": float(np.abs(p1 - p0).max() / sc),
+           "error_words": [err_cloud, err_point]}
+    del dev, pr0, pi0, u00
+    torch.cuda.empty_cache()
+    return out
+
+
 def measure_e2e(dev, dt, args, stream):
     """Per step through the C ABI with host (pinned) buffers: the FP64 rows the step reads
     (X, V, t_s, m, PGID) and u0 copied in, import, one mixed cycle, export, and the state the
@@ -634,6 +711,8 @@ def main():
                     help="skip the batched ensemble of 1024 damping boxes")
     ap.add_argument("--ensemble-cycles", type=int, default=20,
                     help="imex2+ cycles of every ensemble box")
+    ap.add_argument("--no-clouds", action="store_true",
+                    help="skip the refinable-cloud workload (128^3, 33.5 M clouds, FP64)")
     ap.add_argument("--pc2-only", action="store_true",
                     help="time the stratified pc2 workload only (profiling case)")
     args = ap.parse_args()
