@@ -177,6 +177,9 @@ SIGNATURES = {
     "dustb_cloud_dc1_sweep": [CTXP, D, D, VP, VP],
     "dustb_cloud_apply_pmbr": [CTXP, D, D, VP],
     "dustb_cloud_imex_cycle": [CTXP, C.POINTER(DustbImexCoeffs), VP, VP, VP],
+    "dustb_cloud_pc2_predictor": [CTXP, D, I, VP, VP],
+    "dustb_cloud_pc2_advance": [CTXP, D, VP, VP],
+    "dustb_cloud_pc2_cycle": [CTXP, D, VP, VP, VP, VP],
     "dustb_pbin_scratch_bytes": [I],
     "dustb_pbin_rows": [CTXP, VP, VP, D, VP, LL, VP],
     "dustb_pbin_pack": [CTXP, VP, I, I, I, VP, VP],

@@ -1341,6 +1341,20 @@ __device__ void cloud_axis(const MCtx &M, const Ind &d, int m, int a, double x, 
 
 // the cloud's position in the frame of its block (Frame), and whether this build takes it: a
 // level code without lobe bits and a position inside the block
+// (the pc2 advance gathers at its midpoint, which may lie within one cell of the block: slack)
+__device__ bool cloud_frame_ok(const MCtx &M, const Ind &d, int m, int lev, const double L[3],
+                               double x[3], double slack) {
+  if (!block_ok(d, m) || (lev & ~15) != 0) return false;
+  const int nx[3] = {d.nx1, d.nx2, d.nx3};
+  for (int a = 0; a < (d.three_d ? 3 : 2); ++a) {
+    const double cx = M.s(m, X1MIN + a) + 0.5 * nx[a] * M.s(m, DX1 + a);
+    x[a] -= L[a] * round((x[a] - cx) * (1.0 / L[a]));
+    const double e = slack * M.s(m, DX1 + a);
+    if (!(x[a] >= M.s(m, X1MIN + a) - e && x[a] < M.s(m, X1MAX + a) + e)) return false;
+  }
+  return true;
+}
+
 __device__ bool cloud_load(const PCtx &P, const MCtx &M, const Ind &d, int p, double sh,
                            const double L[3], int &m, double x[3], int &lev) {
   m = P.i(DUSTB_PGID, p) - M.gids;
@@ -1653,6 +1667,153 @@ __global__ void k_cloud_consistent_dust(PCtx P, MCtx M, Ind d, const double *res
   P.r(DUSTB_IPRX, p) += cj * rv[0] / a_dt;
   P.r(DUSTB_IPRY, p) += cj * rv[1] / a_dt;
   P.r(DUSTB_IPRZ, p) += cj * rv[2] / a_dt;
+}
+
+// ---- the clouds' pc2 (src/dust/dust_cloud3d.cpp:1362-1538, CloudPC2Push :76-150) ----------
+// PackGasGather3D: the gas velocity u1 momentum / density in every cell
+__global__ void k_gas_velocity_all(Ind d, const double *u, int nv, double *uv) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long per = d.cells();
+  if (idx >= per * d.nmb) return;
+  const int m = (int)(idx / per);
+  const long long r = idx - (long long)m * per;
+  const long long base = (long long)m * nv * per;
+  const double invrho = 1.0 / u[base + r];
+  for (int v = 0; v < 3; ++v) uv[((long long)m * 3 + v) * per + r] = u[base + (1 + v) * per + r] * invrho;
+}
+
+// CloudPredictorT: g = -dt (m / t_s) (ubar - v) into qdep 1-3, m / t_s into qdep 4 (rate_dep)
+__global__ void k_cloud_pc2_predictor(PCtx P, MCtx M, Ind d, const double *gp, double *qdep,
+                                      double dt, int rate_dep, unsigned *err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
+  int m, lev;
+  double x[3];
+  if (!cloud_load(P, M, d, p, 0.0, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
+  CloudAxis X, Y, Z;
+  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
+  double ug[3];
+  cloud_gather(M, d, m, x, X, Y, Z, L, gp, ug, err);
+  const double mass_rate = P.r(DUSTB_IPM, p) / P.r(DUSTB_IPTS, p);
+  const double gx = -dt * mass_rate * (ug[0] - P.r(DUSTB_IPVX, p));
+  const double gy = -dt * mass_rate * (ug[1] - P.r(DUSTB_IPVY, p));
+  const double gz = -dt * mass_rate * (ug[2] - P.r(DUSTB_IPVZ, p));
+  for (int kz = 0; kz < Z.n; ++kz) {
+    if (Z.w[kz] == 0.0) continue;
+    for (int jy = 0; jy < Y.n; ++jy) {
+      if (Y.w[jy] == 0.0) continue;
+      const double w23 = Y.w[jy] * Z.w[kz];
+      for (int ix = 0; ix < X.n; ++ix) {
+        const double w = w23 * X.w[ix];
+        if (w == 0.0) continue;
+        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
+        if (b < 0) continue;
+        const double inv_volume = 1.0 / cloud_measure(M, d, b);
+        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+        atomicAdd(&qdep[d.at(b, 5, 1, k, j, i)], inv_volume * w * gx);
+        atomicAdd(&qdep[d.at(b, 5, 2, k, j, i)], inv_volume * w * gy);
+        atomicAdd(&qdep[d.at(b, 5, 3, k, j, i)], inv_volume * w * gz);
+        if (rate_dep) atomicAdd(&qdep[d.at(b, 5, 4, k, j, i)], inv_volume * w * mass_rate);
+      }
+    }
+  }
+}
+
+// CloudAdvanceT with CloudPC2Push's Midpoint / Kick / Drift
+__global__ void k_cloud_pc2_advance(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
+                                    double dt, int br, int sbox, int strat, double q, double om,
+                                    double aphi, unsigned *err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
+  const int m = P.i(DUSTB_PGID, p) - M.gids, lev = P.i(DUSTB_PLEV, p);
+  const double x0[3] = {P.r(DUSTB_IPX1, p), P.r(DUSTB_IPY1, p), d.three_d ? P.r(DUSTB_IPZ1, p) : 0.0};
+  const double v0[3] = {P.r(DUSTB_IPVX1, p), P.r(DUSTB_IPVY1, p), P.r(DUSTB_IPVZ1, p)};
+  double xh[3], xg[3];
+  if (d.three_d) {
+    xh[0] = x0[0] + 0.5 * dt * v0[0];
+    xh[1] = x0[1] + 0.5 * dt * (v0[1] - (sbox ? q * om * x0[0] : 0.0));
+    xh[2] = x0[2] + 0.5 * dt * v0[2];
+    xg[0] = xh[0];
+    xg[1] = xh[1] + (sbox ? q * om * xh[0] * 0.5 * dt : 0.0);
+    xg[2] = xh[2];
+  } else {
+    xh[0] = x0[0] + 0.5 * dt * v0[0];
+    xh[1] = x0[1] + 0.5 * dt * v0[1];
+    xh[2] = x0[2];
+    xg[0] = xh[0]; xg[1] = xh[1]; xg[2] = xh[2];
+  }
+  double x[3] = {xg[0], xg[1], xg[2]};
+  if (!cloud_frame_ok(M, d, m, lev, L, x, 1.0)) { report(err, DUSTB_ERR_CLOUD); return; }
+  CloudAxis X, Y, Z;
+  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
+  double ug[3];
+  cloud_gather(M, d, m, x, X, Y, Z, L, gp, ug, err);
+  const double h = 0.5 * dt;
+  const double lambda = h / P.r(DUSTB_IPTS, p);
+  const double aa = 1.0 + lambda;
+  double r[3] = {v0[0] + lambda * ug[0], v0[1] + lambda * ug[1], v0[2] + lambda * ug[2]};
+  double vh[3];
+  if (d.three_d) {
+    if (sbox) {
+      const double cxy = 2.0 * h * om, cyx = h * (2.0 - q) * om;
+      const double det = aa * aa + cxy * cyx;
+      vh[0] = (aa * r[0] + cxy * r[1]) / det;
+      vh[1] = (aa * r[1] - cyx * r[0]) / det;
+      if (strat) r[2] -= h * (om * om) * xh[2];
+      vh[2] = r[2] / aa;
+    } else {
+      vh[0] = r[0] / aa; vh[1] = r[1] / aa; vh[2] = r[2] / aa;
+    }
+  } else {
+    if (sbox) {
+      const double cxz = 2.0 * h * om, czx = h * (2.0 - q) * om;
+      const double det = aa * aa + cxz * czx;
+      if (aphi != 0.0) r[2] += h * aphi;
+      vh[0] = (aa * r[0] + cxz * r[2]) / det;
+      vh[2] = (aa * r[2] - czx * r[0]) / det;
+      vh[1] = r[1] / aa;
+    } else {
+      vh[0] = r[0] / aa; vh[1] = r[1] / aa; vh[2] = r[2] / aa;
+    }
+  }
+  P.r(DUSTB_IPVX, p) = 2.0 * vh[0] - v0[0];
+  P.r(DUSTB_IPVY, p) = 2.0 * vh[1] - v0[1];
+  P.r(DUSTB_IPVZ, p) = 2.0 * vh[2] - v0[2];
+  P.r(DUSTB_IPX, p) = x0[0] + dt * vh[0];
+  if (d.three_d) {
+    P.r(DUSTB_IPY, p) = x0[1] + dt * (vh[1] - (sbox ? q * om * xh[0] : 0.0));
+    P.r(DUSTB_IPZ, p) = x0[2] + dt * vh[2];
+  } else {
+    P.r(DUSTB_IPY, p) = x0[1] + dt * vh[1];
+  }
+  P.r(DUSTB_IPX1, p) = xh[0]; P.r(DUSTB_IPY1, p) = xh[1];
+  if (d.three_d) P.r(DUSTB_IPZ1, p) = xh[2];
+  const double dvx = dt * (ug[0] - vh[0]) / P.r(DUSTB_IPTS, p);
+  const double dvy = dt * (ug[1] - vh[1]) / P.r(DUSTB_IPTS, p);
+  const double dvz = dt * (ug[2] - vh[2]) / P.r(DUSTB_IPTS, p);
+  P.r(DUSTB_IPRX, p) = dvx; P.r(DUSTB_IPRY, p) = dvy; P.r(DUSTB_IPRZ, p) = dvz;
+  if (!br) return;
+  const double mass = -P.r(DUSTB_IPM, p);
+  for (int kz = 0; kz < Z.n; ++kz) {
+    if (Z.w[kz] == 0.0) continue;
+    for (int jy = 0; jy < Y.n; ++jy) {
+      if (Y.w[jy] == 0.0) continue;
+      const double w23 = Y.w[jy] * Z.w[kz];
+      for (int ix = 0; ix < X.n; ++ix) {
+        const double w = w23 * X.w[ix];
+        if (w == 0.0) continue;
+        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
+        if (b < 0) continue;
+        const double dw = mass * w / cloud_measure(M, d, b);
+        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
+        atomicAdd(&dmom[d.at(b, 3, 0, k, j, i)], dw * dvx);
+        atomicAdd(&dmom[d.at(b, 3, 1, k, j, i)], dw * dvy);
+        atomicAdd(&dmom[d.at(b, 3, 2, k, j, i)], dw * dvz);
+      }
+    }
+  }
 }
 
 long long n_active(const Ind &d) { return (long long)d.nmb * d.nx3 * d.nx2 * d.nx1; }
@@ -2039,6 +2200,38 @@ int dustb_cloud_apply_pmbr(const dustb_ctx *c, double a_dt, double sh, void *str
   return launch_status("cloud_apply_pmbr");
 }
 
+int dustb_cloud_pc2_predictor(const dustb_ctx *c, double dt, int rate_dep, double *gpack,
+                              void *stream) {
+  CHECK_CTX(c);
+  if (!gpack) return DUSTB_EINVAL;
+  if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
+  const Ind d = make_ind(c->mesh);
+  cudaMemsetAsync(c->f.qdep, 0, (size_t)(n_all(d) * 5) * sizeof(double), S(stream));
+  // the step-start gas velocity in work, packed with its central differences
+  k_gas_velocity_all<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.u1, c->f.nvar_gas,
+                                                                        c->f.work);
+  k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.work, gpack);
+  if (c->part.npart > 0)
+    k_cloud_pc2_predictor<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.qdep, dt, rate_dep,
+                                        c->err);
+  return launch_status("cloud_pc2_predictor");
+}
+
+int dustb_cloud_pc2_advance(const dustb_ctx *c, double dt, double *gpack, void *stream) {
+  CHECK_CTX(c);
+  if (!gpack) return DUSTB_EINVAL;
+  if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
+  const Ind d = make_ind(c->mesh);
+  const dustb_physics &ph = c->phys;
+  k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
+  cudaMemsetAsync(c->f.dmom, 0, (size_t)(n_all(d) * 3) * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_cloud_pc2_advance<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, dt,
+                                      ph.back_reaction, ph.shearing_box, ph.stratified,
+                                      ph.qshear, ph.omega0, ph.const_accel_phi, c->err);
+  return launch_status("cloud_pc2_advance");
+}
+
 // the point transfers' remap: the drag's, with the ghost deposits behind physical x3 faces
 // always folded (src/dust/dust_gravity_points.cpp:176-178)
 static dustb_ctx fold_ctx(const dustb_ctx *c) {
@@ -2169,6 +2362,31 @@ int dustb_cloud_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co, doub
     if (br) RUN(dustb_cloud_apply_pmbr(c, a_dt, sh, stream));
     RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, stream));
   }
+  return DUSTB_OK;
+}
+
+// one pc2 cycle of the clouds: the order of dustb_pc2_cycle with the clouds' predictor and
+// advance (their deposits in the owner cells: no deposit exchanges)
+int dustb_cloud_pc2_cycle(const dustb_ctx *c, double dt, double *chi_max, double *gpack,
+                          double *x3_removed, void *stream) {
+  CHECK_CTX(c);
+  if (!(dt > 0.0) || !gpack) return DUSTB_EINVAL;
+  if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
+  const int br = c->phys.back_reaction;
+  int rc;
+  RUN(dustb_register_copy(c, stream));
+  RUN(dustb_gas_rk_noflux(c, 1.0, 0.0, stream));
+  if (br) {
+    RUN(dustb_cloud_pc2_predictor(c, dt, 1, gpack, stream));
+    RUN(dustb_pc2_apply_predictor(c, dt, chi_max, stream));
+  }
+  RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, stream));
+  RUN(dustb_pc2_midpoint(c, stream));
+  RUN(dustb_gas_rk_noflux(c, 0.5, 0.5, stream));
+  RUN(dustb_cloud_pc2_advance(c, dt, gpack, stream));
+  RUN(dustb_route(c, x3_removed, stream));
+  if (br) RUN(dustb_pc2_commit(c, 0.5, stream));
+  RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, stream));
   return DUSTB_OK;
 }
 

@@ -271,6 +271,12 @@ class DeviceDust:
         self._call("cloud_imex_cycle", C.byref(co), self._gpack().data_ptr(),
                    self.t["x3_removed"].data_ptr(), stream=stream)
 
+    def cloud_pc2_cycle(self, dt, stream=None):
+        chi = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self._call("cloud_pc2_cycle", dt, chi.data_ptr(), self._gpack().data_ptr(),
+                   self.t["x3_removed"].data_ptr(), stream=stream)
+        return chi
+
     # ---- point-particle fields (self-gravity, outputs) ----
     def _field(self, nvar):
         return torch.zeros(self.mesh.field_shape(nvar), dtype=torch.float64, device=self.device)

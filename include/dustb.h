@@ -310,7 +310,15 @@ int dustb_cloud_dc1_sweep(const dustb_ctx *ctx, double a_dt, double sh, double *
  * (CloudImplicitConsistencyOverlapT, src/dust/dust_imex3d.cpp:669-790; the residual in
  * resid), otherwise the plain PMBR. */
 int dustb_cloud_apply_pmbr(const dustb_ctx *ctx, double a_dt, double sh, void *stream);
-/* (dustb_cloud_imex_cycle: with the fused cycles below) */
+/* The clouds' pc2 (src/dust/dust_cloud3d.cpp:1362-1538): CloudPredictorT (qdep cleared, the
+ * step-start gas velocity m / rho of u1 put in work and packed, the linear gather, the drag
+ * impulse -dt (m / t_s)(ubar - v) into qdep 1-3 and, with rate_dep, m / t_s into qdep 4 of the
+ * owner cells) and CloudAdvanceT (u* packed, the midpoint gather from the registers X1, V1,
+ * the implicit-midpoint kick and drift of CloudPC2Push, the impulse into dmom, cleared). */
+int dustb_cloud_pc2_predictor(const dustb_ctx *ctx, double dt, int rate_dep, double *gpack,
+                              void *stream);
+int dustb_cloud_pc2_advance(const dustb_ctx *ctx, double dt, double *gpack, void *stream);
+/* (dustb_cloud_imex_cycle, dustb_cloud_pc2_cycle: with the fused cycles below) */
 
 /* ---- the particle science file (pbin, src/outputs/pbin.cpp): its device side -----------
  * The host writes the file (athenak_b200/host/pbin.hpp); these calls find the active rows
@@ -366,6 +374,10 @@ typedef struct dustb_imex_coeffs {
  * and dustb_cloud_apply_pmbr); gpack as dustb_cloud_gpack_bytes. */
 int dustb_cloud_imex_cycle(const dustb_ctx *ctx, const dustb_imex_coeffs *coeffs, double *gpack,
                            double *x3_removed, void *stream);
+/* One pc2 cycle of the clouds (the order of dustb_pc2_cycle with the cloud predictor and
+ * advance; chi_max as there). */
+int dustb_cloud_pc2_cycle(const dustb_ctx *ctx, double dt, double *chi_max, double *gpack,
+                          double *x3_removed, void *stream);
 
 /* One imex2+ cycle of the drag step (stages 1 and 2; stage 3 is dormant): register copy,
  * gas stand-in, push, route, deposit, ghost add, solve (+dc1/dc2), ghost copy, gather-kick,

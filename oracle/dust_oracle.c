@@ -1057,13 +1057,20 @@ static void cloud_frame(const dustb_ctx *c, int m, double x[3]) {
   }
 }
 
-/* a cloud this restatement takes: level code without lobe bits, position inside its block */
-static int cloud_ok(const dustb_ctx *c, int m, const double x[3], int code) {
+/* a cloud this restatement takes: level code without lobe bits, position inside its block
+ * (or, slack = 1, within one cell of it: the pc2 midpoint, whose support then stays in the
+ * same-level neighbours) */
+static int cloud_ok_slack(const dustb_ctx *c, int m, const double x[3], int code, double slack) {
   const dustb_mesh *ms = &c->mesh;
   if (m < 0 || m >= ms->nmb || (code & ~15) != 0) return 0;
-  for (int a = 0; a < (ms->three_d ? 3 : 2); ++a)
-    if (!(x[a] >= MB(m, X1MIN + a) && x[a] < MB(m, X1MAX + a))) return 0;
+  for (int a = 0; a < (ms->three_d ? 3 : 2); ++a) {
+    const double e = slack*MB(m, DX1 + a);
+    if (!(x[a] >= MB(m, X1MIN + a) - e && x[a] < MB(m, X1MAX + a) + e)) return 0;
+  }
   return 1;
+}
+static int cloud_ok(const dustb_ctx *c, int m, const double x[3], int code) {
+  return cloud_ok_slack(c, m, x, code, 0.0);
 }
 
 /* the 2-D form (LeafApi<LeafTraversal>, src/dust/dust_leaf_api.hpp:31-146): no x3 direction
@@ -1406,6 +1413,180 @@ void oracle_cloud_apply_pmbr(const dustb_ctx *c, double a_dt, double sh) {
     PR(DUSTB_IPRX, p) += cj*rv[0]/a_dt; PR(DUSTB_IPRY, p) += cj*rv[1]/a_dt;
     PR(DUSTB_IPRZ, p) += cj*rv[2]/a_dt;
   }
+}
+
+/* ---- the clouds' pc2 (src/dust/dust_cloud3d.cpp:1362-1538, CloudPC2Push :76-150) ------- */
+/* CloudPredictorT: the step-start gas velocity (PackGasGather3D: u1 momentum over density in
+ * every cell, then packed) gathered linearly over the cloud; g = -dt (m / t_s) (ubar - v) into
+ * qdep 1-3 and, with rate_dep, m / t_s into qdep 4, with the cloud's weights (qdep cleared) */
+unsigned oracle_cloud_pc2_predictor(const dustb_ctx *c, double dt, int rate_dep) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
+  memset(c->f.qdep, 0, field_size(ms, 5)*sizeof(double));
+  double *uv = (double *)malloc(field_size(ms, 3)*sizeof(double));
+  for (int m = 0; m < ms->nmb; ++m)
+    for (int k = 0; k < d.n3; ++k)
+      for (int j = 0; j < d.n2; ++j)
+        for (int i = 0; i < d.n1; ++i) {
+          const double invrho = 1.0/A5(c->f.u1, nv, d, m, 0, k, j, i);
+          for (int v = 0; v < 3; ++v)
+            A5(uv, 3, d, m, v, k, j, i) = A5(c->f.u1, nv, d, m, 1 + v, k, j, i)*invrho;
+        }
+  double *gp = (double *)malloc((size_t)ms->nmb*d.n3*d.n2*d.n1*12*sizeof(double));
+  oracle_gather_pack(c, uv, gp);
+  const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  unsigned err = 0;
+  int tb[216], tk[216], tj[216], ti[216];
+  double tw[216];
+  for (int p = 0; p < c->part.npart; ++p) {
+    const int m = PI(DUSTB_PGID, p) - ms->gids;
+    double x[3];
+    cloud_position(c, p, 0.0, x);
+    const int code = PI(DUSTB_PLEV, p);
+    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
+    if (!cloud_ok(c, m, x, code)) { err |= DUSTB_ERR_CLOUD; continue; }
+    double ug[3];
+    const int nt = cloud_gather(c, &d, m, x, code, gp, ug, tb, tk, tj, ti, tw, &err);
+    const double mass_rate = PR(DUSTB_IPM, p)/PR(DUSTB_IPTS, p);
+    const double gx = -dt*mass_rate*(ug[0] - PR(DUSTB_IPVX, p));
+    const double gy = -dt*mass_rate*(ug[1] - PR(DUSTB_IPVY, p));
+    const double gz = -dt*mass_rate*(ug[2] - PR(DUSTB_IPVZ, p));
+    for (int q = 0; q < nt; ++q) {
+      const int b = tb[q];
+      const double inv_volume = 1.0/cloud_measure(c, b);
+      A5(c->f.qdep, 5, d, b, 1, tk[q], tj[q], ti[q]) += inv_volume*tw[q]*gx;
+      A5(c->f.qdep, 5, d, b, 2, tk[q], tj[q], ti[q]) += inv_volume*tw[q]*gy;
+      A5(c->f.qdep, 5, d, b, 3, tk[q], tj[q], ti[q]) += inv_volume*tw[q]*gz;
+      if (rate_dep) A5(c->f.qdep, 5, d, b, 4, tk[q], tj[q], ti[q]) += inv_volume*tw[q]*mass_rate;
+    }
+  }
+  free(gp); free(uv);
+  return err;
+}
+
+/* CloudAdvanceT: from the stage-start registers (X1, V1) the midpoint xh and the gather
+ * position xg (CloudPC2Push::Midpoint), ubar = the linear gather of u* (ghost cells filled by the
+ * caller) at xg, the implicit-midpoint kick (Kick: the 2x2 Coriolis solve, vertical gravity),
+ * v = 2 vh - v0, the drift, X1 = xh, R = dt (ubar - vh) / t_s, and with back-reaction -m W R / V
+ * into dmom (cleared) */
+unsigned oracle_cloud_pc2_advance(const dustb_ctx *c, double dt) {
+  const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
+  memset(c->f.dmom, 0, field_size(ms, 3)*sizeof(double));
+  double *gp = (double *)malloc((size_t)ms->nmb*d.n3*d.n2*d.n1*12*sizeof(double));
+  oracle_gather_pack(c, c->f.ustar, gp);
+  double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
+  const int br = c->phys.back_reaction, sbox = c->phys.shearing_box, strat = c->phys.stratified;
+  const double q = c->phys.qshear, om = c->phys.omega0, aphi = c->phys.const_accel_phi;
+  unsigned err = 0;
+  int tb[216], tk[216], tj[216], ti[216];
+  double tw[216];
+  for (int p = 0; p < c->part.npart; ++p) {
+    const int m = PI(DUSTB_PGID, p) - ms->gids;
+    const double x0[3] = {PR(DUSTB_IPX1, p), PR(DUSTB_IPY1, p), ms->three_d ? PR(DUSTB_IPZ1, p) : 0.0};
+    const double v0[3] = {PR(DUSTB_IPVX1, p), PR(DUSTB_IPVY1, p), PR(DUSTB_IPVZ1, p)};
+    double xh[3], xg[3];
+    if (ms->three_d) {
+      xh[0] = x0[0] + 0.5*dt*v0[0];
+      xh[1] = x0[1] + 0.5*dt*(v0[1] - (sbox ? q*om*x0[0] : 0.0));
+      xh[2] = x0[2] + 0.5*dt*v0[2];
+      xg[0] = xh[0];
+      xg[1] = xh[1] + (sbox ? q*om*xh[0]*0.5*dt : 0.0);
+      xg[2] = xh[2];
+    } else {
+      xh[0] = x0[0] + 0.5*dt*v0[0];
+      xh[1] = x0[1] + 0.5*dt*v0[1];
+      xh[2] = x0[2];
+      xg[0] = xh[0]; xg[1] = xh[1]; xg[2] = xh[2];
+    }
+    const int code = PI(DUSTB_PLEV, p);
+    double xf[3] = {xg[0], xg[1], xg[2]};
+    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, xf);
+    if (!cloud_ok_slack(c, m, xf, code, 1.0)) { err |= DUSTB_ERR_CLOUD; continue; }
+    double ug[3];
+    const int nt = cloud_gather(c, &d, m, xf, code, gp, ug, tb, tk, tj, ti, tw, &err);
+    const double h = 0.5*dt;
+    const double lambda = h/PR(DUSTB_IPTS, p);
+    const double aa = 1.0 + lambda;
+    double r[3] = {v0[0] + lambda*ug[0], v0[1] + lambda*ug[1], v0[2] + lambda*ug[2]};
+    double vh[3];
+    if (ms->three_d) {
+      if (sbox) {
+        const double cxy = 2.0*h*om, cyx = h*(2.0 - q)*om;
+        const double det = aa*aa + cxy*cyx;
+        vh[0] = (aa*r[0] + cxy*r[1])/det;
+        vh[1] = (aa*r[1] - cyx*r[0])/det;
+        if (strat) r[2] -= h*(om*om)*xh[2];
+        vh[2] = r[2]/aa;
+      } else {
+        vh[0] = r[0]/aa; vh[1] = r[1]/aa; vh[2] = r[2]/aa;
+      }
+    } else {
+      if (sbox) {
+        const double cxz = 2.0*h*om, czx = h*(2.0 - q)*om;
+        const double det = aa*aa + cxz*czx;
+        if (aphi != 0.0) r[2] += h*aphi;
+        vh[0] = (aa*r[0] + cxz*r[2])/det;
+        vh[2] = (aa*r[2] - czx*r[0])/det;
+        vh[1] = r[1]/aa;
+      } else {
+        vh[0] = r[0]/aa; vh[1] = r[1]/aa; vh[2] = r[2]/aa;
+      }
+    }
+    PR(DUSTB_IPVX, p) = 2.0*vh[0] - v0[0];
+    PR(DUSTB_IPVY, p) = 2.0*vh[1] - v0[1];
+    PR(DUSTB_IPVZ, p) = 2.0*vh[2] - v0[2];
+    PR(DUSTB_IPX, p) = x0[0] + dt*vh[0];
+    if (ms->three_d) {
+      PR(DUSTB_IPY, p) = x0[1] + dt*(vh[1] - (sbox ? q*om*xh[0] : 0.0));
+      PR(DUSTB_IPZ, p) = x0[2] + dt*vh[2];
+    } else {
+      PR(DUSTB_IPY, p) = x0[1] + dt*vh[1];
+    }
+    PR(DUSTB_IPX1, p) = xh[0]; PR(DUSTB_IPY1, p) = xh[1];
+    if (ms->three_d) PR(DUSTB_IPZ1, p) = xh[2];
+    const double dvx = dt*(ug[0] - vh[0])/PR(DUSTB_IPTS, p);
+    const double dvy = dt*(ug[1] - vh[1])/PR(DUSTB_IPTS, p);
+    const double dvz = dt*(ug[2] - vh[2])/PR(DUSTB_IPTS, p);
+    PR(DUSTB_IPRX, p) = dvx; PR(DUSTB_IPRY, p) = dvy; PR(DUSTB_IPRZ, p) = dvz;
+    if (!br) continue;
+    const double mass = -PR(DUSTB_IPM, p);
+    for (int qq = 0; qq < nt; ++qq) {
+      const int b = tb[qq];
+      const double dw = mass*tw[qq]/cloud_measure(c, b);
+      A5(c->f.dmom, 3, d, b, 0, tk[qq], tj[qq], ti[qq]) += dw*dvx;
+      A5(c->f.dmom, 3, d, b, 1, tk[qq], tj[qq], ti[qq]) += dw*dvy;
+      A5(c->f.dmom, 3, d, b, 2, tk[qq], tj[qq], ti[qq]) += dw*dvz;
+    }
+  }
+  free(gp);
+  return err;
+}
+
+double oracle_pc2_apply_predictor(const dustb_ctx *c, double dt);
+void oracle_pc2_midpoint(const dustb_ctx *c);
+void oracle_pc2_commit(const dustb_ctx *c, double wpred);
+
+/* one pc2 cycle of the clouds: the order of oracle_pc2_cycle with the clouds' predictor and
+ * advance (their deposits in the owner cells: no deposit exchanges) */
+unsigned oracle_cloud_pc2_cycle(const dustb_ctx *c, double dt, double *chi_out,
+                                double *x3_removed) {
+  unsigned err = 0;
+  const int br = c->phys.back_reaction;
+  oracle_register_copy(c);
+  oracle_gas_rk_noflux(c, 1.0, 0.0);
+  double chi = 0.0;
+  if (br) {
+    err |= oracle_cloud_pc2_predictor(c, dt, 1);
+    chi = oracle_pc2_apply_predictor(c, dt);
+  }
+  oracle_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0);
+  oracle_pc2_midpoint(c);
+  oracle_gas_rk_noflux(c, 0.5, 0.5);
+  err |= oracle_cloud_pc2_advance(c, dt);
+  err |= oracle_route(c, x3_removed);
+  if (br) oracle_pc2_commit(c, 0.5);
+  oracle_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0);
+  if (chi_out) *chi_out = chi;
+  return err;
 }
 
 /* one imex2+ cycle of refinable clouds on a uniform mesh: the task order of oracle_imex_cycle

@@ -81,6 +81,7 @@ def lib():
             "oracle_cloud_dc1_sweep": ([P, D, D], C.c_uint),
             "oracle_cloud_apply_pmbr": ([P, D, D], None),
             "oracle_cloud_imex_cycle": ([P, D, D, VP, VP], C.c_uint),
+            "oracle_cloud_pc2_cycle": ([P, D, VP, VP], C.c_uint),
         }
         for name, (args, res) in sig.items():
             f = getattr(_lib, name)
@@ -296,6 +297,12 @@ class Oracle:
         shv = (C.c_double * 2)(*sh)
         return self.call("cloud_imex_cycle", gamma, dt, C.cast(shv, C.c_void_p),
                          self.x3_removed.ctypes.data)
+
+    def cloud_pc2_cycle(self, dt):
+        chi = C.c_double(0.0)
+        err = self.call("cloud_pc2_cycle", dt, C.cast(C.byref(chi), C.c_void_p),
+                        self.x3_removed.ctypes.data)
+        return err, chi.value
 
     def point_science_fields(self, mass_only=False, species=-1):
         """DepositPointScienceFields: (out field with 1 or 4 vars, err)."""

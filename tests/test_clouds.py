@@ -216,3 +216,38 @@ def test_2d_linear_gather_and_lattice_cycle():
     for r in (1, 3, 12, 13):
         sc = max(np.abs(op.st.pr[r, :m3]).max(), 1e-300)
         assert np.abs(oc.st.pr[r, :m3] - op.st.pr[r, :m3]).max() < 1e-12 * sc, r
+
+
+# ---- the clouds' pc2 (CloudPredictorT / CloudAdvanceT) ----
+@pytest.mark.parametrize("dims", [3, 2])
+def test_cloud_pc2_cycle_on_a_lattice_is_the_point_pc2_cycle(dims):
+    if dims == 3:
+        ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3)
+        dt = 0.004
+    else:
+        ms = uniform_mesh((32, 32, 1), (16, 16, 1), 2, (-0.5,) * 3, (0.5,) * 3)
+        dt = 0.01
+    st = make_state(ms, [0.05], [2.0], 1, placement="lattice", vd=[0.03], gas_noise=0.0)
+    phys = dict(scheme=2)
+    oc, op = Oracle(st, phys), Oracle(st, phys)
+    for _ in range(3):
+        assert oc.cloud_pc2_cycle(dt)[0] == 0 and op.pc2_cycle(dt)[0] == 0
+    n = st.npart
+    for r in (0, 1, 2, 3, 12, 13):
+        sc = max(np.abs(op.st.pr[r, :n]).max(), 1e-300)
+        assert np.abs(oc.st.pr[r, :n] - op.st.pr[r, :n]).max() < 1e-12 * sc, r
+    for v in range(1, 3):
+        sc = max(np.abs(op.u0[:, v]).max(), 1e-300)
+        assert np.abs(oc.u0[:, v] - op.u0[:, v]).max() < 1e-12 * sc, v
+
+
+def test_cloud_pc2_cycles_conserve_momentum():
+    ms, st = setup((0, 1, 2), seed=21)
+    o = Oracle(st, dict(scheme=2, pc2_feedback_damping=False))
+    p0 = sum(o.momentum())
+    for _ in range(3):
+        assert o.cloud_pc2_cycle(2e-3)[0] == 0
+    p1 = sum(o.momentum())
+    n = st.npart
+    scale = np.abs(st.pr[16, :n] * np.abs(st.pr[[1, 3, 5], :n]).max(axis=0)).sum()
+    assert np.abs(p1 - p0).max() < 1e-12 * scale
