@@ -75,6 +75,8 @@ TaskStatus DustGasDrag::ExplicitPush(Driver *pdrive, int stage) {
   const int s = stage - 1;
   if (coupling_ == DustCoupling::pc2) {
     if (stage != 2) return TaskStatus::complete;   // the advance of the midpoint stage
+    if (clouds_)   // CloudAdvanceT (dust_cloud3d.cpp:1442-1536)
+      return Check(dustb_cloud_pc2_advance(&ctx_, pdrive->dt, gpack_, stream_), "ExplicitPush");
     return Check(dustb_pc2_advance(&ctx_, pdrive->dt, stream_), "ExplicitPush");
   }
   const double atw = (stage == 2) ? pdrive->a_twid[stage][stage] * pdrive->dt : 0.0;
@@ -92,6 +94,8 @@ TaskStatus DustGasDrag::DepositDrag(Driver *pdrive, int stage) {
   if (!ctx_.phys.back_reaction) return TaskStatus::complete;
   if (coupling_ == DustCoupling::pc2) {
     if (stage != 1) return TaskStatus::complete;   // the predictor
+    if (clouds_)   // CloudPredictorT (dust_cloud3d.cpp:1362-1436)
+      return Check(dustb_cloud_pc2_predictor(&ctx_, pdrive->dt, 1, gpack_, stream_), "DepositDrag");
     return Check(dustb_pc2_predictor(&ctx_, pdrive->dt, 1, stream_), "DepositDrag");
   }
   if (clouds_) return Check(dustb_cloud_deposit_qp(&ctx_, a_dt(pdrive), 0.0, stream_), "DepositDrag");
@@ -155,10 +159,6 @@ TaskStatus DustGasDrag::ApplyPMBR(Driver *pdrive, int stage) {
 }
 
 TaskStatus DustGasDrag::SetRefinableClouds(bool on) {
-  if (on && coupling_ == DustCoupling::pc2) {
-    last_error_ = "SetRefinableClouds: the clouds of this build run the imex coupling";
-    return TaskStatus::fail;
-  }
   if (on && !gpack_) {
     const long long bytes = dustb_cloud_gpack_bytes(&ctx_.mesh);
     if (bytes <= 0 || cudaMalloc(&gpack_, (size_t)bytes) != cudaSuccess) {

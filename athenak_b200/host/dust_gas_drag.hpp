@@ -93,10 +93,11 @@ class DustGasDrag {
   TaskStatus DepositPointScienceFields(double time, double *out, double *halo, bool mass_only,
                                        int species);
 
-  // <dust>/smr_transfer = refinable_cloud on a uniform 3-D mesh (UsesRefinableClouds): the
-  // deposit, the dc1 / dc2 sweeps, the gather-kick and the PMBR split of the tasks run the
-  // clouds' kernels (PLEV = cloud level); their deposits land in the owner cells, so the
-  // deposit exchanges are skipped.  Allocates the gather pack; imex coupling only.
+  // <dust>/smr_transfer = refinable_cloud on a uniform 2-D or 3-D mesh (UsesRefinableClouds):
+  // the deposit, the dc1 / dc2 sweeps, the gather-kick and the PMBR split of the imex tasks,
+  // and the predictor and advance of pc2, run the clouds' kernels (PLEV = cloud level); their
+  // deposits land in the owner cells, so the deposit exchanges are skipped.  Allocates the
+  // gather pack.
   TaskStatus SetRefinableClouds(bool on);
 
   // the stage's drag tasks in dependency order on one rank and one stream

@@ -24,6 +24,7 @@ unsigned oracle_imex_cycle(const dustb_ctx *c, double gamma, double dt, const do
 unsigned oracle_pc2_cycle(const dustb_ctx *c, double dt, double *chi_out, double *x3_removed);
 unsigned oracle_cloud_imex_cycle(const dustb_ctx *c, double gamma, double dt, const double sh[2],
                                  double *x3_removed);
+unsigned oracle_cloud_pc2_cycle(const dustb_ctx *c, double dt, double *chi_out, double *x3_removed);
 void oracle_ghost_copy(const dustb_ctx *c, double *a, int nvar, int x3_bcs);
 void oracle_set_threads(int n);
 void oracle_cloud_order(const dustb_ctx *c, int *ord, uint64_t *tag);
@@ -263,7 +264,9 @@ int run(athenak_b200::DustCoupling coupling, const char *name, bool mixed = fals
       std::printf("%s: task failed: %s%s\n", name, drag.LastError().c_str(), mx.LastError().c_str());
       return 1;
     }
-    oerr |= clouds ? oracle_cloud_imex_cycle(&hc, drv.gamma, drv.dt, sh, x3o)
+    oerr |= clouds ? ((coupling == athenak_b200::DustCoupling::imex)
+                          ? oracle_cloud_imex_cycle(&hc, drv.gamma, drv.dt, sh, x3o)
+                          : oracle_cloud_pc2_cycle(&hc, drv.dt, &chi, x3o))
             : (coupling == athenak_b200::DustCoupling::imex)
                 ? oracle_imex_cycle(&hc, drv.gamma, drv.dt, sh, x3o)
                 : oracle_pc2_cycle(&hc, drv.dt, &chi, x3o);
@@ -316,5 +319,6 @@ int main() {
   bad += run(athenak_b200::DustCoupling::imex, "mixed imex2+/dc2 cycles", true);
   bad += run(athenak_b200::DustCoupling::pc2, "mixed pc2 cycles", true);
   bad += run(athenak_b200::DustCoupling::imex, "refinable-cloud imex2+/dc2 cycles", false, true);
+  bad += run(athenak_b200::DustCoupling::pc2, "refinable-cloud pc2 cycles", false, true);
   return bad ? 1 : 0;
 }

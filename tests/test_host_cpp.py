@@ -37,4 +37,4 @@ def test_host_task_list_matches_oracle():
     r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.count(": ok") == 6
+    assert r.stdout.count(": ok") == 7
