@@ -1283,15 +1283,17 @@ __global__ void k_point_gather(PCtx P, MCtx M, Ind d, const double *f, double *a
   for (int v = 0; v < 3; ++v) acc[(long long)v * astride + p] = a[v];
 }
 
-// ---- refinable clouds on a uniform 3-D mesh: plain P1 hat clouds --------------------------
+// ---- refinable clouds on a uniform mesh: plain P1 hat clouds ------------------------------
 // CloudShape1D (src/dust/dust.hpp:240-298; HatCDF / HatMoment :169-182) for a cloud without
 // lobes: along each direction the hat of half-width ell = dx / 2^level about the particle, a
 // cell's weight the difference of the hat CDF at its faces, its first moment about the
 // particle ell times the difference of the moment antiderivative.  LeafTraversal3D::ForEach
 // (src/dust/dust_leaf3d.hpp:368-513) on a uniform mesh: the cells of the block and of its
 // same-level neighbours under the support, each cell's faces from its own block's origin (the
-// neighbour's periodic image next to the block), leaves in the order z, y, x (lower neighbour,
-// block, upper neighbour along each), zero-weight leaves skipped.
+// neighbour's periodic image next to the block); across a physical x3 face a second part, the
+// cloud mirrored about the face, whose x3 moments are taken about the particle; leaves in the
+// order part, z, y, x (lower neighbour, block, upper neighbour along each), zero-weight leaves
+// skipped.  2-D (LeafTraversal::ForEach): no x3 direction.
 __device__ __forceinline__ double hat_cdf(double s) {
   if (s <= -1.0) return 0.0;
   if (s >= 1.0) return 1.0;
@@ -1305,7 +1307,7 @@ __device__ __forceinline__ double hat_moment(double s) {
 struct CloudAxis {
   int n;
   int o[6], i[6];
-  double w[6], g[6];
+  double w[6], g[6], org[6];   // weight, moment, the origin of the cell's block image
 };
 
 __device__ void cloud_axis(const MCtx &M, const Ind &d, int m, int a, double x, int lev,
@@ -1331,7 +1333,7 @@ __device__ void cloud_axis(const MCtx &M, const Ind &d, int m, int a, double x, 
     i1 = (i1 > nx - 1) ? nx - 1 : i1;
     for (int i = i0; i <= i1 && A.n < 6; ++i) {
       const double za = (bx0 + i * dx - x) * inv, zb = (bx0 + (i + 1) * dx - x) * inv;
-      A.o[A.n] = o; A.i[A.n] = i;
+      A.o[A.n] = o; A.i[A.n] = i; A.org[A.n] = bx0;
       A.w[A.n] = hat_cdf(zb) - hat_cdf(za);
       A.g[A.n] = ell * (hat_moment(zb) - hat_moment(za));
       ++A.n;
@@ -1339,9 +1341,8 @@ __device__ void cloud_axis(const MCtx &M, const Ind &d, int m, int a, double x, 
   }
 }
 
-// the cloud's position in the frame of its block (Frame), and whether this build takes it: a
-// level code without lobe bits and a position inside the block
-// (the pc2 advance gathers at its midpoint, which may lie within one cell of the block: slack)
+// the position of a cloud in the frame of block m; true if this build takes it: a level code
+// without lobe bits, a position inside the block (slack: within that many cells of it)
 __device__ bool cloud_frame_ok(const MCtx &M, const Ind &d, int m, int lev, const double L[3],
                                double x[3], double slack) {
   if (!block_ok(d, m) || (lev & ~15) != 0) return false;
@@ -1355,35 +1356,15 @@ __device__ bool cloud_frame_ok(const MCtx &M, const Ind &d, int m, int lev, cons
   return true;
 }
 
+// the stage position (3-D: y + sh x, the gas in its orbital-advection frame; 2-D: no shift)
 __device__ bool cloud_load(const PCtx &P, const MCtx &M, const Ind &d, int p, double sh,
                            const double L[3], int &m, double x[3], int &lev) {
   m = P.i(DUSTB_PGID, p) - M.gids;
   lev = P.i(DUSTB_PLEV, p);
-  // (2-D: no orbital-advection shift, no x3, LeafApi<LeafTraversal>::LoadImplicit)
   x[0] = P.r(DUSTB_IPX, p);
   x[1] = d.three_d ? P.r(DUSTB_IPY, p) + sh * P.r(DUSTB_IPX, p) : P.r(DUSTB_IPY, p);
   x[2] = d.three_d ? P.r(DUSTB_IPZ, p) : 0.0;
-  if (!block_ok(d, m) || (lev & ~15) != 0) return false;
-  const int nx[3] = {d.nx1, d.nx2, d.nx3};
-  for (int a = 0; a < (d.three_d ? 3 : 2); ++a) {
-    const double cx = M.s(m, X1MIN + a) + 0.5 * nx[a] * M.s(m, DX1 + a);
-    x[a] -= L[a] * round((x[a] - cx) * (1.0 / L[a]));
-    if (!(x[a] >= M.s(m, X1MIN + a) && x[a] < M.s(m, X1MAX + a))) return false;
-  }
-  return true;
-}
-
-// the three directions of a cloud; 2-D: a unit z axis (w = w2 w1 and the moments bit for bit)
-__device__ void cloud_axes(const MCtx &M, const Ind &d, int m, const double x[3], int lev,
-                           const double L[3], CloudAxis &X, CloudAxis &Y, CloudAxis &Z) {
-  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
-  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
-  if (d.three_d) { cloud_axis(M, d, m, 2, x[2], lev, L[2], Z); return; }
-  Z.n = 1; Z.o[0] = 0; Z.i[0] = 0; Z.w[0] = 1.0; Z.g[0] = 0.0;
-}
-// the cell measure: the volume, 2-D the area (LeafApi::Measure)
-__device__ __forceinline__ double cloud_measure(const MCtx &M, const Ind &d, int b) {
-  return d.three_d ? M.s(b, DX1) * M.s(b, DX2) * M.s(b, DX3) : M.s(b, DX1) * M.s(b, DX2);
+  return cloud_frame_ok(M, d, m, lev, L, x, 0.0);
 }
 
 __device__ __forceinline__ int cloud_owner(const MCtx &M, const Ind &d, int m, int ox, int oy,
@@ -1394,9 +1375,111 @@ __device__ __forceinline__ int cloud_owner(const MCtx &M, const Ind &d, int m, i
   return (gid < 0 || b < 0 || b >= d.nmb) ? -1 : b;
 }
 
+// the cell measure: the volume, 2-D the area (LeafApi::Measure)
+__device__ __forceinline__ double cloud_measure(const MCtx &M, const Ind &d, int b) {
+  return d.three_d ? M.s(b, DX1) * M.s(b, DX2) * M.s(b, DX3) : M.s(b, DX1) * M.s(b, DX2);
+}
+
+struct CloudLeaf {
+  int b, k, j, i;              // owner block, padded cell
+  double w, m1x, m1y, m1z;
+};
+
+// every leaf of the cloud at x (level lev, anchored at block m): f(leaf); with kMoments the
+// moment traversal (a leaf with zero weight but a moment visited), else the weight traversal
+template <bool kMoments, typename F>
+__device__ void cloud_leaves(const MCtx &M, const Ind &d, int m, const double x[3], int lev,
+                             const double L[3], int x3phys, F &&f, unsigned *err) {
+  CloudAxis X, Y, Z;
+  cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
+  cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
+  if (d.three_d) {
+    cloud_axis(M, d, m, 2, x[2], lev, L[2], Z);
+  } else {
+    Z.n = 1; Z.o[0] = 0; Z.i[0] = 0; Z.w[0] = 1.0; Z.g[0] = 0.0; Z.org[0] = 0.0;
+  }
+  int npz = 1;
+  double zp = x[2];
+  if (x3phys && d.three_d) {
+    const double ell = ldexp(M.s(m, DX3), -lev);
+    const double lo = x[2] - ell, hi = x[2] + ell;
+    if (lo < M.x3min || hi > M.x3max) {
+      npz = 2;
+      zp = 2.0 * ((hi > M.x3max) ? M.x3max : M.x3min) - x[2];
+    }
+  }
+  for (int part = 0; part < npz; ++part) {
+    if (part == 1) cloud_axis(M, d, m, 2, zp, lev, L[2], Z);
+    for (int kz = 0; kz < Z.n; ++kz) {
+      const double w3 = Z.w[kz], g3 = Z.g[kz];
+      if (w3 == 0.0 && (!kMoments || g3 == 0.0)) continue;
+      double czk = 0.0;
+      if (kMoments && part == 1) {
+        const double zc = Z.org[kz] + (Z.i[kz] + 0.5) * M.s(m, DX3);
+        const double ez = x[2] - zc;
+        czk = (zp - zc) - (ez - L[2] * round(ez / L[2]));
+      }
+      for (int jy = 0; jy < Y.n; ++jy) {
+        const double w2 = Y.w[jy], g2 = Y.g[jy];
+        if (w2 == 0.0 && (!kMoments || g2 == 0.0)) continue;
+        const double w23 = w2 * w3;
+        for (int ix = 0; ix < X.n; ++ix) {
+          const double wa = X.w[ix];
+          CloudLeaf lf;
+          lf.w = w23 * wa;
+          lf.m1x = lf.m1y = lf.m1z = 0.0;
+          if (kMoments) {
+            lf.m1x = w23 * X.g[ix];
+            lf.m1y = wa * g2 * w3;
+            lf.m1z = wa * w2 * g3;
+            if (part == 1) lf.m1z += czk * lf.w;
+            if (lf.w == 0.0 && lf.m1x == 0.0 && lf.m1y == 0.0 && lf.m1z == 0.0) continue;
+          } else if (lf.w == 0.0) {
+            continue;
+          }
+          lf.b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
+          if (lf.b < 0) { if (err) report(err, DUSTB_ERR_CLOUD); continue; }
+          lf.k = d.ks + Z.i[kz]; lf.j = d.js + Y.i[jy]; lf.i = d.is + X.i[ix];
+          f(lf);
+        }
+      }
+    }
+  }
+}
+
+// the clouds' linear gather of the packed field at x (CloudLinearGather3D without the blend)
+__device__ void cloud_gather(const MCtx &M, const Ind &d, int m, const double x[3], int lev,
+                             const double L[3], int x3phys, const double *gp, double ug[3],
+                             unsigned *err) {
+  ug[0] = ug[1] = ug[2] = 0.0;
+  cloud_leaves<true>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+    const int b = lf.b;
+    const double w = lf.w;
+    const double dx1 = M.s(b, DX1), dx2 = M.s(b, DX2), dx3 = M.s(b, DX3);
+    const double xc = M.s(b, X1MIN) + (lf.i - d.is + 0.5) * dx1;
+    const double yc = M.s(b, X2MIN) + (lf.j - d.js + 0.5) * dx2;
+    const double ex = x[0] - xc, ey = x[1] - yc;
+    const double cx = 0.5 * (lf.m1x + (ex - L[0] * round(ex / L[0])) * w) / dx1;
+    const double cy = 0.5 * (lf.m1y + (ey - L[1] * round(ey / L[1])) * w) / dx2;
+    const double *g = gp + ((((long long)b * d.n3 + lf.k) * d.n2 + lf.j) * d.n1 + lf.i) * 12;
+    if (d.three_d) {
+      const double zc = M.s(b, X3MIN) + (lf.k - d.ks + 0.5) * dx3;
+      const double ez = x[2] - zc;
+      const double cz = 0.5 * (lf.m1z + (ez - L[2] * round(ez / L[2])) * w) / dx3;
+      ug[0] += w * g[0] + cx * g[3] + cy * g[6] + cz * g[9];
+      ug[1] += w * g[1] + cx * g[4] + cy * g[7] + cz * g[10];
+      ug[2] += w * g[2] + cx * g[5] + cy * g[8] + cz * g[11];
+    } else {
+      ug[0] += w * g[0] + cx * g[3] + cy * g[6];
+      ug[1] += w * g[1] + cx * g[4] + cy * g[7];
+      ug[2] += w * g[2] + cx * g[5] + cy * g[8];
+    }
+  }, err);
+}
+
 // CloudDepositImplicitT (src/dust/dust_imex3d.cpp:61-99): Q = m c W / V, P = Q v
 __global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, double sh,
-                                unsigned *err) {
+                                int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
   const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
@@ -1406,31 +1489,18 @@ __global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt
   const double mass_c = d.three_d ? P.r(DUSTB_IPM, p) * a_dt / (P.r(DUSTB_IPTS, p) + a_dt)
                                   : P.r(DUSTB_IPM, p) * (a_dt / (P.r(DUSTB_IPTS, p) + a_dt));
   const double vx = P.r(DUSTB_IPVX, p), vy = P.r(DUSTB_IPVY, p), vz = P.r(DUSTB_IPVZ, p);
-  CloudAxis X, Y, Z;
-  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
-  for (int kz = 0; kz < Z.n; ++kz) {
-    if (Z.w[kz] == 0.0) continue;
-    for (int jy = 0; jy < Y.n; ++jy) {
-      if (Y.w[jy] == 0.0) continue;
-      const double w23 = Y.w[jy] * Z.w[kz];
-      for (int ix = 0; ix < X.n; ++ix) {
-        const double w = w23 * X.w[ix];
-        if (w == 0.0) continue;
-        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
-        if (b < 0) { report(err, DUSTB_ERR_CLOUD); continue; }
-        const double dw = mass_c * w / cloud_measure(M, d, b);
-        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-        atomicAdd(&qdep[d.at(b, 5, 0, k, j, i)], dw);
-        atomicAdd(&qdep[d.at(b, 5, 1, k, j, i)], dw * vx);
-        atomicAdd(&qdep[d.at(b, 5, 2, k, j, i)], dw * vy);
-        atomicAdd(&qdep[d.at(b, 5, 3, k, j, i)], dw * vz);
-      }
-    }
-  }
+  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+    const double dw = mass_c * lf.w / cloud_measure(M, d, lf.b);
+    atomicAdd(&qdep[d.at(lf.b, 5, 0, lf.k, lf.j, lf.i)], dw);
+    atomicAdd(&qdep[d.at(lf.b, 5, 1, lf.k, lf.j, lf.i)], dw * vx);
+    atomicAdd(&qdep[d.at(lf.b, 5, 2, lf.k, lf.j, lf.i)], dw * vy);
+    atomicAdd(&qdep[d.at(lf.b, 5, 3, lf.k, lf.j, lf.i)], dw * vz);
+  }, err);
 }
 
 // PackGatherField3D (src/dust/dust_cloud3d.cpp:1319-1340): the velocity and its central
-// differences, gp(m, k, j, i, 0..11), over the padded interior (the outer layer zero)
+// differences, gp(m, k, j, i, 0..11), over the padded interior (the outer layer zero); 2-D
+// (PackGatherField, src/dust/dust_pm.cpp:81-102): the plane ks, no x3 differences
 __global__ void k_gather_pack(Ind d, const double *v, double *gp) {
   const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = d.cells();
@@ -1441,7 +1511,6 @@ __global__ void k_gather_pack(Ind d, const double *v, double *gp) {
   const int j = (int)(r % d.n2);
   const int k = (int)(r / d.n2);
   double *g = gp + idx * 12;
-  // (2-D: PackGatherField, src/dust/dust_pm.cpp:81-102: the plane ks, no x3 differences)
   const bool kin = d.three_d ? (k >= 1 && k < d.n3 - 1) : (k == d.ks);
   const bool in = i >= 1 && i < d.n1 - 1 && j >= 1 && j < d.n2 - 1 && kin;
   for (int q = 0; q < 3; ++q) {
@@ -1458,52 +1527,15 @@ __global__ void k_gather_pack(Ind d, const double *v, double *gp) {
 // + cz du/dz, cx = (m1x + MinImage(x - xc) w) / (2 dx); dv = c (ubar - v), v += dv,
 // R = dv / a_dt; with back-reaction -m w dv / V into dmom over the leaves of nonzero weight
 __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
-                                    double a_dt, double sh, int br, unsigned *err) {
+                                    double a_dt, double sh, int br, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
   const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
   int m, lev;
   double x[3];
   if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
-  CloudAxis X, Y, Z;
-  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
-  double ug[3] = {0.0, 0.0, 0.0};
-  for (int kz = 0; kz < Z.n; ++kz) {
-    const double w3 = Z.w[kz], g3 = Z.g[kz];
-    if (w3 == 0.0 && g3 == 0.0) continue;
-    for (int jy = 0; jy < Y.n; ++jy) {
-      const double w2 = Y.w[jy], g2 = Y.g[jy];
-      if (w2 == 0.0 && g2 == 0.0) continue;
-      const double w23 = w2 * w3;
-      for (int ix = 0; ix < X.n; ++ix) {
-        const double wa = X.w[ix], ga = X.g[ix];
-        const double w = w23 * wa;
-        const double m1x = w23 * ga, m1y = wa * g2 * w3, m1z = wa * w2 * g3;
-        if (w == 0.0 && m1x == 0.0 && m1y == 0.0 && m1z == 0.0) continue;
-        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
-        if (b < 0) { report(err, DUSTB_ERR_CLOUD); continue; }
-        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-        const double dx1 = M.s(b, DX1), dx2 = M.s(b, DX2), dx3 = M.s(b, DX3);
-        const double xc = M.s(b, X1MIN) + (i - d.is + 0.5) * dx1;
-        const double yc = M.s(b, X2MIN) + (j - d.js + 0.5) * dx2;
-        const double zc = M.s(b, X3MIN) + (k - d.ks + 0.5) * dx3;
-        const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
-        const double cx = 0.5 * (m1x + (ex - L[0] * round(ex / L[0])) * w) / dx1;
-        const double cy = 0.5 * (m1y + (ey - L[1] * round(ey / L[1])) * w) / dx2;
-        const double *g = gp + ((((long long)b * d.n3 + k) * d.n2 + j) * d.n1 + i) * 12;
-        if (d.three_d) {
-          const double cz = 0.5 * (m1z + (ez - L[2] * round(ez / L[2])) * w) / dx3;
-          ug[0] += w * g[0] + cx * g[3] + cy * g[6] + cz * g[9];
-          ug[1] += w * g[1] + cx * g[4] + cy * g[7] + cz * g[10];
-          ug[2] += w * g[2] + cx * g[5] + cy * g[8] + cz * g[11];
-        } else {
-          ug[0] += w * g[0] + cx * g[3] + cy * g[6];
-          ug[1] += w * g[1] + cx * g[4] + cy * g[7];
-          ug[2] += w * g[2] + cx * g[5] + cy * g[8];
-        }
-      }
-    }
-  }
+  double ug[3];
+  cloud_gather(M, d, m, x, lev, L, x3phys, gp, ug, err);
   const double cj = a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
   const double dvx = cj * (ug[0] - P.r(DUSTB_IPVX, p));
   const double dvy = cj * (ug[1] - P.r(DUSTB_IPVY, p));
@@ -1511,105 +1543,34 @@ __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, dou
   P.r(DUSTB_IPVX, p) += dvx; P.r(DUSTB_IPVY, p) += dvy; P.r(DUSTB_IPVZ, p) += dvz;
   P.r(DUSTB_IPRX, p) = dvx / a_dt; P.r(DUSTB_IPRY, p) = dvy / a_dt; P.r(DUSTB_IPRZ, p) = dvz / a_dt;
   if (!br) return;
-  // the impulse with the deposit's leaves (those of nonzero weight, the same as the gather's)
   const double mass = -P.r(DUSTB_IPM, p);
-  for (int kz = 0; kz < Z.n; ++kz) {
-    if (Z.w[kz] == 0.0) continue;
-    for (int jy = 0; jy < Y.n; ++jy) {
-      if (Y.w[jy] == 0.0) continue;
-      const double w23 = Y.w[jy] * Z.w[kz];
-      for (int ix = 0; ix < X.n; ++ix) {
-        const double w = w23 * X.w[ix];
-        if (w == 0.0) continue;
-        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
-        if (b < 0) continue;
-        const double dw = mass * w / cloud_measure(M, d, b);
-        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-        atomicAdd(&dmom[d.at(b, 3, 0, k, j, i)], dw * dvx);
-        atomicAdd(&dmom[d.at(b, 3, 1, k, j, i)], dw * dvy);
-        atomicAdd(&dmom[d.at(b, 3, 2, k, j, i)], dw * dvz);
-      }
-    }
-  }
-}
-
-// the clouds' linear gather of the packed field at one cloud (without the blend), in the
-// leaf order of the gather-kick
-__device__ void cloud_gather(const MCtx &M, const Ind &d, int m, const double x[3],
-                             const CloudAxis &X, const CloudAxis &Y, const CloudAxis &Z,
-                             const double L[3], const double *gp, double ug[3], unsigned *err) {
-  ug[0] = ug[1] = ug[2] = 0.0;
-  for (int kz = 0; kz < Z.n; ++kz) {
-    const double w3 = Z.w[kz], g3 = Z.g[kz];
-    if (w3 == 0.0 && g3 == 0.0) continue;
-    for (int jy = 0; jy < Y.n; ++jy) {
-      const double w2 = Y.w[jy], g2 = Y.g[jy];
-      if (w2 == 0.0 && g2 == 0.0) continue;
-      const double w23 = w2 * w3;
-      for (int ix = 0; ix < X.n; ++ix) {
-        const double wa = X.w[ix], ga = X.g[ix];
-        const double w = w23 * wa;
-        const double m1x = w23 * ga, m1y = wa * g2 * w3, m1z = wa * w2 * g3;
-        if (w == 0.0 && m1x == 0.0 && m1y == 0.0 && m1z == 0.0) continue;
-        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
-        if (b < 0) { report(err, DUSTB_ERR_CLOUD); continue; }
-        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-        const double dx1 = M.s(b, DX1), dx2 = M.s(b, DX2), dx3 = M.s(b, DX3);
-        const double xc = M.s(b, X1MIN) + (i - d.is + 0.5) * dx1;
-        const double yc = M.s(b, X2MIN) + (j - d.js + 0.5) * dx2;
-        const double zc = M.s(b, X3MIN) + (k - d.ks + 0.5) * dx3;
-        const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
-        const double cx = 0.5 * (m1x + (ex - L[0] * round(ex / L[0])) * w) / dx1;
-        const double cy = 0.5 * (m1y + (ey - L[1] * round(ey / L[1])) * w) / dx2;
-        const double *g = gp + ((((long long)b * d.n3 + k) * d.n2 + j) * d.n1 + i) * 12;
-        if (d.three_d) {
-          const double cz = 0.5 * (m1z + (ez - L[2] * round(ez / L[2])) * w) / dx3;
-          ug[0] += w * g[0] + cx * g[3] + cy * g[6] + cz * g[9];
-          ug[1] += w * g[1] + cx * g[4] + cy * g[7] + cz * g[10];
-          ug[2] += w * g[2] + cx * g[5] + cy * g[8] + cz * g[11];
-        } else {
-          ug[0] += w * g[0] + cx * g[3] + cy * g[6];
-          ug[1] += w * g[1] + cx * g[4] + cy * g[7];
-          ug[2] += w * g[2] + cx * g[5] + cy * g[8];
-        }
-      }
-    }
-  }
+  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+    const double dw = mass * lf.w / cloud_measure(M, d, lf.b);
+    atomicAdd(&dmom[d.at(lf.b, 3, 0, lf.k, lf.j, lf.i)], dw * dvx);
+    atomicAdd(&dmom[d.at(lf.b, 3, 1, lf.k, lf.j, lf.i)], dw * dvy);
+    atomicAdd(&dmom[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * dvz);
+  }, nullptr);
 }
 
 // CloudOperatorKernelT (src/dust/dust_cloud_imex_kernels.hpp:20-70): the clouds' m c W ubar / V
 // with ubar their linear gather of the packed field, into result (the operator of dc1 / dc2)
 __global__ void k_cloud_operator(PCtx P, MCtx M, Ind d, const double *gp, double *result,
-                                 double a_dt, double sh, unsigned *err) {
+                                 double a_dt, double sh, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
   const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
   int m, lev;
   double x[3];
   if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
-  CloudAxis X, Y, Z;
-  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
   double ug[3];
-  cloud_gather(M, d, m, x, X, Y, Z, L, gp, ug, err);
+  cloud_gather(M, d, m, x, lev, L, x3phys, gp, ug, err);
   const double mc = P.r(DUSTB_IPM, p) * (a_dt / (P.r(DUSTB_IPTS, p) + a_dt));
-  for (int kz = 0; kz < Z.n; ++kz) {
-    if (Z.w[kz] == 0.0) continue;
-    for (int jy = 0; jy < Y.n; ++jy) {
-      if (Y.w[jy] == 0.0) continue;
-      const double w23 = Y.w[jy] * Z.w[kz];
-      for (int ix = 0; ix < X.n; ++ix) {
-        const double w = w23 * X.w[ix];
-        if (w == 0.0) continue;
-        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
-        if (b < 0) continue;
-        const double dw = mc * w / cloud_measure(M, d, b);
-        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-        atomicAdd(&result[d.at(b, 3, 0, k, j, i)], dw * ug[0]);
-        atomicAdd(&result[d.at(b, 3, 1, k, j, i)], dw * ug[1]);
-        atomicAdd(&result[d.at(b, 3, 2, k, j, i)], dw * ug[2]);
-      }
-    }
-  }
+  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+    const double dw = mc * lf.w / cloud_measure(M, d, lf.b);
+    atomicAdd(&result[d.at(lf.b, 3, 0, lf.k, lf.j, lf.i)], dw * ug[0]);
+    atomicAdd(&result[d.at(lf.b, 3, 1, lf.k, lf.j, lf.i)], dw * ug[1]);
+    atomicAdd(&result[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * ug[2]);
+  }, nullptr);
 }
 
 // CloudImplicitConsistencyOverlapT (src/dust/dust_imex3d.cpp:669-790), the cells: g = rho u* -
@@ -1636,7 +1597,7 @@ __global__ void k_cloud_consistent_gas(Ind d, double *u0, int nv, const double *
 
 // ... the clouds: v += c sum W r, R += c sum W r / a_dt with the deposit's weights
 __global__ void k_cloud_consistent_dust(PCtx P, MCtx M, Ind d, const double *res, double a_dt,
-                                        double sh) {
+                                        double sh, int x3phys) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
   if (P.r(DUSTB_IPM, p) <= 0.0) return;
@@ -1644,24 +1605,10 @@ __global__ void k_cloud_consistent_dust(PCtx P, MCtx M, Ind d, const double *res
   int m, lev;
   double x[3];
   if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) return;
-  CloudAxis X, Y, Z;
-  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
   double rv[3] = {0.0, 0.0, 0.0};
-  for (int kz = 0; kz < Z.n; ++kz) {
-    if (Z.w[kz] == 0.0) continue;
-    for (int jy = 0; jy < Y.n; ++jy) {
-      if (Y.w[jy] == 0.0) continue;
-      const double w23 = Y.w[jy] * Z.w[kz];
-      for (int ix = 0; ix < X.n; ++ix) {
-        const double w = w23 * X.w[ix];
-        if (w == 0.0) continue;
-        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
-        if (b < 0) continue;
-        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-        for (int v = 0; v < 3; ++v) rv[v] += w * res[d.at(b, 4, v, k, j, i)];
-      }
-    }
-  }
+  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+    for (int v = 0; v < 3; ++v) rv[v] += lf.w * res[d.at(lf.b, 4, v, lf.k, lf.j, lf.i)];
+  }, nullptr);
   const double cj = a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
   P.r(DUSTB_IPVX, p) += cj * rv[0]; P.r(DUSTB_IPVY, p) += cj * rv[1]; P.r(DUSTB_IPVZ, p) += cj * rv[2];
   P.r(DUSTB_IPRX, p) += cj * rv[0] / a_dt;
@@ -1684,46 +1631,32 @@ __global__ void k_gas_velocity_all(Ind d, const double *u, int nv, double *uv) {
 
 // CloudPredictorT: g = -dt (m / t_s) (ubar - v) into qdep 1-3, m / t_s into qdep 4 (rate_dep)
 __global__ void k_cloud_pc2_predictor(PCtx P, MCtx M, Ind d, const double *gp, double *qdep,
-                                      double dt, int rate_dep, unsigned *err) {
+                                      double dt, int rate_dep, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
   const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
   int m, lev;
   double x[3];
   if (!cloud_load(P, M, d, p, 0.0, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
-  CloudAxis X, Y, Z;
-  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
   double ug[3];
-  cloud_gather(M, d, m, x, X, Y, Z, L, gp, ug, err);
+  cloud_gather(M, d, m, x, lev, L, x3phys, gp, ug, err);
   const double mass_rate = P.r(DUSTB_IPM, p) / P.r(DUSTB_IPTS, p);
   const double gx = -dt * mass_rate * (ug[0] - P.r(DUSTB_IPVX, p));
   const double gy = -dt * mass_rate * (ug[1] - P.r(DUSTB_IPVY, p));
   const double gz = -dt * mass_rate * (ug[2] - P.r(DUSTB_IPVZ, p));
-  for (int kz = 0; kz < Z.n; ++kz) {
-    if (Z.w[kz] == 0.0) continue;
-    for (int jy = 0; jy < Y.n; ++jy) {
-      if (Y.w[jy] == 0.0) continue;
-      const double w23 = Y.w[jy] * Z.w[kz];
-      for (int ix = 0; ix < X.n; ++ix) {
-        const double w = w23 * X.w[ix];
-        if (w == 0.0) continue;
-        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
-        if (b < 0) continue;
-        const double inv_volume = 1.0 / cloud_measure(M, d, b);
-        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-        atomicAdd(&qdep[d.at(b, 5, 1, k, j, i)], inv_volume * w * gx);
-        atomicAdd(&qdep[d.at(b, 5, 2, k, j, i)], inv_volume * w * gy);
-        atomicAdd(&qdep[d.at(b, 5, 3, k, j, i)], inv_volume * w * gz);
-        if (rate_dep) atomicAdd(&qdep[d.at(b, 5, 4, k, j, i)], inv_volume * w * mass_rate);
-      }
-    }
-  }
+  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+    const double inv_volume = 1.0 / cloud_measure(M, d, lf.b);
+    atomicAdd(&qdep[d.at(lf.b, 5, 1, lf.k, lf.j, lf.i)], inv_volume * lf.w * gx);
+    atomicAdd(&qdep[d.at(lf.b, 5, 2, lf.k, lf.j, lf.i)], inv_volume * lf.w * gy);
+    atomicAdd(&qdep[d.at(lf.b, 5, 3, lf.k, lf.j, lf.i)], inv_volume * lf.w * gz);
+    if (rate_dep) atomicAdd(&qdep[d.at(lf.b, 5, 4, lf.k, lf.j, lf.i)], inv_volume * lf.w * mass_rate);
+  }, nullptr);
 }
 
 // CloudAdvanceT with CloudPC2Push's Midpoint / Kick / Drift
 __global__ void k_cloud_pc2_advance(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
                                     double dt, int br, int sbox, int strat, double q, double om,
-                                    double aphi, unsigned *err) {
+                                    double aphi, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
   const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
@@ -1746,10 +1679,8 @@ __global__ void k_cloud_pc2_advance(PCtx P, MCtx M, Ind d, const double *gp, dou
   }
   double x[3] = {xg[0], xg[1], xg[2]};
   if (!cloud_frame_ok(M, d, m, lev, L, x, 1.0)) { report(err, DUSTB_ERR_CLOUD); return; }
-  CloudAxis X, Y, Z;
-  cloud_axes(M, d, m, x, lev, L, X, Y, Z);
   double ug[3];
-  cloud_gather(M, d, m, x, X, Y, Z, L, gp, ug, err);
+  cloud_gather(M, d, m, x, lev, L, x3phys, gp, ug, err);
   const double h = 0.5 * dt;
   const double lambda = h / P.r(DUSTB_IPTS, p);
   const double aa = 1.0 + lambda;
@@ -1796,24 +1727,12 @@ __global__ void k_cloud_pc2_advance(PCtx P, MCtx M, Ind d, const double *gp, dou
   P.r(DUSTB_IPRX, p) = dvx; P.r(DUSTB_IPRY, p) = dvy; P.r(DUSTB_IPRZ, p) = dvz;
   if (!br) return;
   const double mass = -P.r(DUSTB_IPM, p);
-  for (int kz = 0; kz < Z.n; ++kz) {
-    if (Z.w[kz] == 0.0) continue;
-    for (int jy = 0; jy < Y.n; ++jy) {
-      if (Y.w[jy] == 0.0) continue;
-      const double w23 = Y.w[jy] * Z.w[kz];
-      for (int ix = 0; ix < X.n; ++ix) {
-        const double w = w23 * X.w[ix];
-        if (w == 0.0) continue;
-        const int b = cloud_owner(M, d, m, X.o[ix], Y.o[jy], Z.o[kz]);
-        if (b < 0) continue;
-        const double dw = mass * w / cloud_measure(M, d, b);
-        const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-        atomicAdd(&dmom[d.at(b, 3, 0, k, j, i)], dw * dvx);
-        atomicAdd(&dmom[d.at(b, 3, 1, k, j, i)], dw * dvy);
-        atomicAdd(&dmom[d.at(b, 3, 2, k, j, i)], dw * dvz);
-      }
-    }
-  }
+  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+    const double dw = mass * lf.w / cloud_measure(M, d, lf.b);
+    atomicAdd(&dmom[d.at(lf.b, 3, 0, lf.k, lf.j, lf.i)], dw * dvx);
+    atomicAdd(&dmom[d.at(lf.b, 3, 1, lf.k, lf.j, lf.i)], dw * dvy);
+    atomicAdd(&dmom[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * dvz);
+  }, nullptr);
 }
 
 long long n_active(const Ind &d) { return (long long)d.nmb * d.nx3 * d.nx2 * d.nx1; }
@@ -2133,9 +2052,14 @@ int dustb_phst(const dustb_ctx *c, const double *chi_max, double *row, void *scr
 }
 
 // ---- refinable clouds on a uniform 3-D mesh (periodic; plain P1 hat clouds) ---------------
+// (physical x3 faces: the mirrored part of the clouds that reach beyond them; shear-periodic x1
+// faces, whose translated parts need the shear images of the neighbours, are not supported)
 static int cloud_mesh_ok(const dustb_ctx *c) {
   const dustb_mesh &ms = c->mesh;
-  return ms.multi_d && !ms.shear_x1 && (!ms.three_d || ms.x3bc == DUSTB_X3_PERIODIC);
+  return ms.multi_d && !ms.shear_x1;
+}
+static int cloud_x3phys(const dustb_ctx *c) {
+  return c->mesh.three_d && c->mesh.x3bc != DUSTB_X3_PERIODIC;
 }
 
 long long dustb_cloud_gpack_bytes(const dustb_mesh *mesh) {
@@ -2150,7 +2074,7 @@ int dustb_cloud_deposit_qp(const dustb_ctx *c, double a_dt, double sh, void *str
   const Ind d = make_ind(c->mesh);
   cudaMemsetAsync(c->f.qdep, 0, (size_t)(n_all(d) * 5) * sizeof(double), S(stream));
   if (c->part.npart > 0)
-    k_cloud_deposit<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, c->err);
+    k_cloud_deposit<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, cloud_x3phys(c), c->err);
   return launch_status("cloud_deposit_qp");
 }
 
@@ -2164,7 +2088,7 @@ int dustb_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, double *
   cudaMemsetAsync(c->f.dmom, 0, (size_t)(n_all(d) * 3) * sizeof(double), S(stream));
   if (c->part.npart > 0)
     k_cloud_gather_kick<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, a_dt, sh,
-                                      c->phys.back_reaction, c->err);
+                                      c->phys.back_reaction, cloud_x3phys(c), c->err);
   return launch_status("cloud_gather_kick");
 }
 
@@ -2179,7 +2103,8 @@ int dustb_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh, double *gp
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
   cudaMemsetAsync(c->f.work, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
   if (c->part.npart > 0)
-    k_cloud_operator<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.work, a_dt, sh, c->err);
+    k_cloud_operator<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.work, a_dt, sh,
+                                   cloud_x3phys(c), c->err);
   k_dc_correct<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas,
                                                                     c->f.qdep, c->f.work,
                                                                     c->f.ustar);
@@ -2196,7 +2121,8 @@ int dustb_cloud_apply_pmbr(const dustb_ctx *c, double a_dt, double sh, void *str
   k_cloud_consistent_gas<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(
       d, c->f.u0, c->f.nvar_gas, c->f.ustar, c->f.qdep, c->f.dmom, c->f.resid, 1.0 / a_dt);
   if (c->part.npart > 0)
-    k_cloud_consistent_dust<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, sh);
+    k_cloud_consistent_dust<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, sh,
+                                          cloud_x3phys(c));
   return launch_status("cloud_apply_pmbr");
 }
 
@@ -2213,7 +2139,7 @@ int dustb_cloud_pc2_predictor(const dustb_ctx *c, double dt, int rate_dep, doubl
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.work, gpack);
   if (c->part.npart > 0)
     k_cloud_pc2_predictor<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.qdep, dt, rate_dep,
-                                        c->err);
+                                        cloud_x3phys(c), c->err);
   return launch_status("cloud_pc2_predictor");
 }
 
@@ -2228,7 +2154,7 @@ int dustb_cloud_pc2_advance(const dustb_ctx *c, double dt, double *gpack, void *
   if (c->part.npart > 0)
     k_cloud_pc2_advance<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, dt,
                                       ph.back_reaction, ph.shearing_box, ph.stratified,
-                                      ph.qshear, ph.omega0, ph.const_accel_phi, c->err);
+                                      ph.qshear, ph.omega0, ph.const_accel_phi, cloud_x3phys(c), c->err);
   return launch_status("cloud_pc2_advance");
 }
 

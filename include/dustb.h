@@ -288,9 +288,10 @@ int dustb_point_science_fields(const dustb_ctx *ctx, double *out, double *halo, 
  * Plain P1 hat clouds: PLEV holds the cloud level L (half-width dx / 2^L along each
  * direction), integrated exactly over the cells of the block and its same-level neighbours
  * (CloudShape1D, LeafTraversal3D::ForEach / LeafTraversal::ForEach on a uniform mesh; 2-D:
- * the LeafApi<LeafTraversal> forms).  Periodic meshes (no physical x3 or shear-periodic
- * faces: EUNSUP).  A cloud code with lobe bits (the transition clouds of refined meshes) or
- * a cloud outside its block sets DUSTB_ERR_CLOUD and is skipped. */
+ * the LeafApi<LeafTraversal> forms).  At physical x3 faces the part of a cloud beyond the face
+ * comes back mirrored about it; shear-periodic x1 faces: EUNSUP.  A cloud code with lobe bits
+ * (the transition clouds of refined meshes) or a cloud outside its block sets DUSTB_ERR_CLOUD
+ * and is skipped. */
 /* CloudDepositImplicitT (:61-99): qdep cleared, then Q = m c W / V and P = Q v into the owner
  * cells (no ghost exchange needed). */
 int dustb_cloud_deposit_qp(const dustb_ctx *ctx, double a_dt, double sh, void *stream);

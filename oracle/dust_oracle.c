@@ -989,7 +989,7 @@ void oracle_sort_particles(const dustb_ctx *c, double *spare_pr, int *spare_pi) 
 void oracle_imex2p_coeffs(double gamma, double gam0[3], double gam1[3], double beta[3],
                           double *atw22);
 
-/* ---- refinable clouds on a uniform 3-D mesh: plain P1 hat clouds ---------------------
+/* ---- refinable clouds on a uniform mesh: plain P1 hat clouds ------------------------
  * CloudShape1D (src/dust/dust.hpp:240-298) with HatCDF / HatMoment (:169-182) for a cloud
  * without lobes: along each direction the hat of half-width ell = dx / 2^level about the
  * particle; a cell's weight is the difference of the hat CDF at its two faces, its first
@@ -997,9 +997,13 @@ void oracle_imex2p_coeffs(double gamma, double gam0[3], double gam1[3], double b
  * LeafTraversal3D::ForEach (src/dust/dust_leaf3d.hpp:368-513) on a uniform mesh: the cells of
  * the block and of its same-level neighbours that the support overlaps, each cell's faces
  * from its own block's origin (the neighbour's periodic image next to the block), weight w =
- * w1 w2 w3 and moments (g1 w2 w3, w1 g2 w3, w1 w2 g3).  Leaf order here: z, then y, then x,
- * each direction from the lower neighbour through the block to the upper one; leaves of zero
- * weight (and zero moments) are skipped. */
+ * w1 w2 w3 and moments (g1 w2 w3, w1 g2 w3, w1 w2 g3); across a physical x3 face a second
+ * part, the cloud mirrored about the face, its x3 moments taken about the particle (zcorr).
+ * Leaf order here: part, z, y, x, each direction from the lower neighbour through the block to
+ * the upper one; leaves of zero weight (and zero moments) are skipped.  2-D
+ * (LeafTraversal::ForEach and LeafApi<LeafTraversal>, src/dust/dust_leaf_api.hpp:31-146): no x3
+ * direction (a unit z axis: w = w2 w1 and the moments bit for bit), no orbital-advection
+ * shift, the cell area as the measure, the coupled mass m (a_dt / (t_s + a_dt)). */
 static double hat_cdf(double s) {
   if (s <= -1.0) return 0.0;
   if (s >= 1.0) return 1.0;
@@ -1010,7 +1014,7 @@ static double hat_moment(double s) {
   return (s <= 0.0) ? 0.5*(s*s) + (s*s)*s/3.0 : 0.5*(s*s) - (s*s)*s/3.0;
 }
 
-typedef struct { int n; int o[6]; int i[6]; double w[6]; double g[6]; } CloudAxis;
+typedef struct { int n; int o[6]; int i[6]; double w[6]; double g[6]; double org[6]; } CloudAxis;
 
 /* the cells of one direction a (0..2) for a cloud at x of level lev anchored at block m */
 static void cloud_axis(const dustb_ctx *c, int m, int a, double x, int lev, CloudAxis *A) {
@@ -1038,7 +1042,7 @@ static void cloud_axis(const dustb_ctx *c, int m, int a, double x, int lev, Clou
     i1 = (i1 > nx - 1) ? nx - 1 : i1;
     for (int i = i0; i <= i1 && A->n < 6; ++i) {
       const double za = (bx0 + i*dx - x)*inv, zb = (bx0 + (i + 1)*dx - x)*inv;
-      A->o[A->n] = o; A->i[A->n] = i;
+      A->o[A->n] = o; A->i[A->n] = i; A->org[A->n] = bx0;
       A->w[A->n] = hat_cdf(zb) - hat_cdf(za);
       A->g[A->n] = ell*(hat_moment(zb) - hat_moment(za));
       ++A->n;
@@ -1046,44 +1050,24 @@ static void cloud_axis(const dustb_ctx *c, int m, int a, double x, int lev, Clou
   }
 }
 
-/* Frame (dust_leaf3d.hpp): the periodic image of the position next to block m */
-static void cloud_frame(const dustb_ctx *c, int m, double x[3]) {
+/* Frame: the periodic image of the position next to block m; then whether this restatement
+ * takes the cloud: a level code without lobe bits and a position inside the block (slack: within
+ * that many cells of it, the pc2 midpoint) */
+static int cloud_frame_ok(const dustb_ctx *c, int m, double x[3], int code, double slack) {
   const dustb_mesh *ms = &c->mesh;
+  if (m < 0 || m >= ms->nmb || (code & ~15) != 0) return 0;
   const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
   const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
   for (int a = 0; a < (ms->three_d ? 3 : 2); ++a) {
     const double cx = MB(m, X1MIN + a) + 0.5*nx[a]*MB(m, DX1 + a);
     x[a] -= L[a]*round((x[a] - cx)*(1.0/L[a]));
-  }
-}
-
-/* a cloud this restatement takes: level code without lobe bits, position inside its block
- * (or, slack = 1, within one cell of it: the pc2 midpoint, whose support then stays in the
- * same-level neighbours) */
-static int cloud_ok_slack(const dustb_ctx *c, int m, const double x[3], int code, double slack) {
-  const dustb_mesh *ms = &c->mesh;
-  if (m < 0 || m >= ms->nmb || (code & ~15) != 0) return 0;
-  for (int a = 0; a < (ms->three_d ? 3 : 2); ++a) {
     const double e = slack*MB(m, DX1 + a);
     if (!(x[a] >= MB(m, X1MIN + a) - e && x[a] < MB(m, X1MAX + a) + e)) return 0;
   }
   return 1;
 }
-static int cloud_ok(const dustb_ctx *c, int m, const double x[3], int code) {
-  return cloud_ok_slack(c, m, x, code, 0.0);
-}
 
-/* the 2-D form (LeafApi<LeafTraversal>, src/dust/dust_leaf_api.hpp:31-146): no x3 direction
- * (a unit z axis: w = w2 w1, the moments w2 g1 and w1 g2 bit for bit), no orbital-advection
- * shift of the position, the cell area as the measure, the coupled mass m (a_dt / (t_s +
- * a_dt)) */
-static void cloud_axes(const dustb_ctx *c, int m, const double x[3], int code, CloudAxis *X,
-                       CloudAxis *Y, CloudAxis *Z) {
-  cloud_axis(c, m, 0, x[0], code, X);
-  cloud_axis(c, m, 1, x[1], code, Y);
-  if (c->mesh.three_d) { cloud_axis(c, m, 2, x[2], code, Z); return; }
-  Z->n = 1; Z->o[0] = 0; Z->i[0] = 0; Z->w[0] = 1.0; Z->g[0] = 0.0;
-}
+/* the stage position (3-D: y + sh x; 2-D: no shift) */
 static void cloud_position(const dustb_ctx *c, int p, double sh, double x[3]) {
   const double *pr = c->part.pr; long long stride = c->part.stride;
   if (c->mesh.three_d) {
@@ -1096,13 +1080,140 @@ static double cloud_measure(const dustb_ctx *c, int b) {
   const dustb_mesh *ms = &c->mesh;
   return ms->three_d ? MB(b, DX1)*MB(b, DX2)*MB(b, DX3) : MB(b, DX1)*MB(b, DX2);
 }
-
 /* the owner block of a leaf in direction (ox, oy, oz) of m */
 static int cloud_owner(const dustb_ctx *c, int m, int ox, int oy, int oz) {
   if (!ox && !oy && !oz) return m;
   const int gid = c->mesh.nghbr[(size_t)m*27 + (oz + 1)*9 + (oy + 1)*3 + (ox + 1)];
   const int b = gid - c->mesh.gids;
   return (gid < 0 || b < 0 || b >= c->mesh.nmb) ? -1 : b;
+}
+
+typedef struct { int b, k, j, i; double w, m1x, m1y, m1z; } CloudLeaf;
+typedef void (*CloudLeafFn)(void *ctx, const CloudLeaf *lf);
+
+/* every leaf of the cloud at x (level code, anchored at block m): f(ctx, leaf); with moments the
+ * moment traversal, else the weight traversal */
+static void cloud_leaves(const dustb_ctx *c, const Ind *d, int m, const double x[3], int code,
+                         int moments, CloudLeafFn f, void *ctx, unsigned *err) {
+  const dustb_mesh *ms = &c->mesh;
+  const double Lz = ms->x3max - ms->x3min;
+  CloudAxis X, Y, Z;
+  cloud_axis(c, m, 0, x[0], code, &X);
+  cloud_axis(c, m, 1, x[1], code, &Y);
+  if (ms->three_d) cloud_axis(c, m, 2, x[2], code, &Z);
+  else { Z.n = 1; Z.o[0] = 0; Z.i[0] = 0; Z.w[0] = 1.0; Z.g[0] = 0.0; Z.org[0] = 0.0; }
+  int npz = 1;
+  double zp = x[2];
+  if (ms->three_d && ms->x3bc != 0) {
+    const double ell = ldexp(MB(m, DX3), -code);
+    const double lo = x[2] - ell, hi = x[2] + ell;
+    if (lo < ms->x3min || hi > ms->x3max) {
+      npz = 2;
+      zp = 2.0*((hi > ms->x3max) ? ms->x3max : ms->x3min) - x[2];
+    }
+  }
+  for (int part = 0; part < npz; ++part) {
+    if (part == 1) cloud_axis(c, m, 2, zp, code, &Z);
+    for (int kz = 0; kz < Z.n; ++kz) {
+      const double w3 = Z.w[kz], g3 = Z.g[kz];
+      if (w3 == 0.0 && (!moments || g3 == 0.0)) continue;
+      double czk = 0.0;
+      if (moments && part == 1) {
+        const double zc = Z.org[kz] + (Z.i[kz] + 0.5)*MB(m, DX3);
+        const double ez = x[2] - zc;
+        czk = (zp - zc) - (ez - Lz*round(ez/Lz));
+      }
+      for (int jy = 0; jy < Y.n; ++jy) {
+        const double w2 = Y.w[jy], g2 = Y.g[jy];
+        if (w2 == 0.0 && (!moments || g2 == 0.0)) continue;
+        const double w23 = w2*w3;
+        for (int ix = 0; ix < X.n; ++ix) {
+          const double wa = X.w[ix];
+          CloudLeaf lf;
+          lf.w = w23*wa;
+          lf.m1x = lf.m1y = lf.m1z = 0.0;
+          if (moments) {
+            lf.m1x = w23*X.g[ix];
+            lf.m1y = wa*g2*w3;
+            lf.m1z = wa*w2*g3;
+            if (part == 1) lf.m1z += czk*lf.w;
+            if (lf.w == 0.0 && lf.m1x == 0.0 && lf.m1y == 0.0 && lf.m1z == 0.0) continue;
+          } else if (lf.w == 0.0) {
+            continue;
+          }
+          lf.b = cloud_owner(c, m, X.o[ix], Y.o[jy], Z.o[kz]);
+          if (lf.b < 0) { if (err) *err |= DUSTB_ERR_CLOUD; continue; }
+          lf.k = d->ks + Z.i[kz]; lf.j = d->js + Y.i[jy]; lf.i = d->is + X.i[ix];
+          f(ctx, &lf);
+        }
+      }
+    }
+  }
+}
+
+/* ---- the linear gather and the deposits, as callbacks ---- */
+typedef struct {
+  const dustb_ctx *c; const Ind *d; const double *x; const double *gp; double ug[3];
+} GatherCtx;
+static void gather_leaf(void *vctx, const CloudLeaf *lf) {
+  GatherCtx *g = (GatherCtx *)vctx;
+  const dustb_ctx *c = g->c; const dustb_mesh *ms = &c->mesh; const Ind *d = g->d;
+  const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
+  const int b = lf->b;
+  const double w = lf->w;
+  const double dx1 = MB(b, DX1), dx2 = MB(b, DX2), dx3 = MB(b, DX3);
+  const double xc = MB(b, X1MIN) + (lf->i - d->is + 0.5)*dx1;
+  const double yc = MB(b, X2MIN) + (lf->j - d->js + 0.5)*dx2;
+  const double ex = g->x[0] - xc, ey = g->x[1] - yc;
+  const double cx = 0.5*(lf->m1x + (ex - L[0]*round(ex/L[0]))*w)/dx1;
+  const double cy = 0.5*(lf->m1y + (ey - L[1]*round(ey/L[1]))*w)/dx2;
+  const double *gp = g->gp + ((((size_t)b*d->n3 + lf->k)*d->n2 + lf->j)*d->n1 + lf->i)*12;
+  if (ms->three_d) {
+    const double zc = MB(b, X3MIN) + (lf->k - d->ks + 0.5)*dx3;
+    const double ez = g->x[2] - zc;
+    const double cz = 0.5*(lf->m1z + (ez - L[2]*round(ez/L[2]))*w)/dx3;
+    g->ug[0] += w*gp[0] + cx*gp[3] + cy*gp[6] + cz*gp[9];
+    g->ug[1] += w*gp[1] + cx*gp[4] + cy*gp[7] + cz*gp[10];
+    g->ug[2] += w*gp[2] + cx*gp[5] + cy*gp[8] + cz*gp[11];
+  } else {
+    g->ug[0] += w*gp[0] + cx*gp[3] + cy*gp[6];
+    g->ug[1] += w*gp[1] + cx*gp[4] + cy*gp[7];
+    g->ug[2] += w*gp[2] + cx*gp[5] + cy*gp[8];
+  }
+}
+/* the clouds' linear gather of the packed field gp at one cloud (CloudLinearGather3D without
+ * the blend) */
+static void cloud_gather(const dustb_ctx *c, const Ind *d, int m, const double x[3], int code,
+                         const double *gp, double ug[3], unsigned *err) {
+  GatherCtx g = {c, d, x, gp, {0.0, 0.0, 0.0}};
+  cloud_leaves(c, d, m, x, code, 1, gather_leaf, &g, err);
+  ug[0] = g.ug[0]; ug[1] = g.ug[1]; ug[2] = g.ug[2];
+}
+
+/* s * w / V * v[q] into f(b, nvar, c0 + q) for q < n: the deposits of the cloud kernels */
+typedef struct {
+  const dustb_ctx *c; const Ind *d; double *f; int nvar, c0, n; double s; double v[4];
+  int inv_first;   /* 1: (1 / V) w v (the pc2 predictor's product order), 0: s w / V v */
+} DepositCtx;
+static void deposit_leaf(void *vctx, const CloudLeaf *lf) {
+  DepositCtx *q = (DepositCtx *)vctx;
+  const Ind *d = q->d;
+  if (q->inv_first) {
+    const double inv_volume = 1.0/cloud_measure(q->c, lf->b);
+    for (int t = 0; t < q->n; ++t)
+      A5(q->f, q->nvar, (*d), lf->b, q->c0 + t, lf->k, lf->j, lf->i) += inv_volume*lf->w*q->v[t];
+  } else {
+    const double dw = q->s*lf->w/cloud_measure(q->c, lf->b);
+    for (int t = 0; t < q->n; ++t)
+      A5(q->f, q->nvar, (*d), lf->b, q->c0 + t, lf->k, lf->j, lf->i) += dw*q->v[t];
+  }
+}
+static void cloud_deposit(const dustb_ctx *c, const Ind *d, int m, const double x[3], int code,
+                          double *f, int nvar, int c0, int n, double s, const double *v,
+                          int inv_first, unsigned *err) {
+  DepositCtx q = {c, d, f, nvar, c0, n, s, {0.0, 0.0, 0.0, 0.0}, inv_first};
+  for (int t = 0; t < n; ++t) q.v[t] = v[t];
+  cloud_leaves(c, d, m, x, code, 0, deposit_leaf, &q, err);
 }
 
 /* CloudDepositImplicitT (src/dust/dust_imex3d.cpp:61-99): Q = m c W / V and P = Q v into
@@ -1114,45 +1225,25 @@ unsigned oracle_cloud_deposit_qp(const dustb_ctx *c, double a_dt, double sh) {
   unsigned err = 0;
   for (int p = 0; p < c->part.npart; ++p) {
     const int m = PI(DUSTB_PGID, p) - ms->gids;
+    const int code = PI(DUSTB_PLEV, p);
     double x[3];
     cloud_position(c, p, sh, x);
-    const int code = PI(DUSTB_PLEV, p);
-    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
-    if (!cloud_ok(c, m, x, code)) { err |= DUSTB_ERR_CLOUD; continue; }
+    if (!cloud_frame_ok(c, m, x, code, 0.0)) { err |= DUSTB_ERR_CLOUD; continue; }
     const double mass_c = ms->three_d ? PR(DUSTB_IPM, p)*a_dt/(PR(DUSTB_IPTS, p) + a_dt)
                                       : PR(DUSTB_IPM, p)*(a_dt/(PR(DUSTB_IPTS, p) + a_dt));
-    const double vx = PR(DUSTB_IPVX, p), vy = PR(DUSTB_IPVY, p), vz = PR(DUSTB_IPVZ, p);
-    CloudAxis X, Y, Z;
-    cloud_axes(c, m, x, code, &X, &Y, &Z);
-    for (int kz = 0; kz < Z.n; ++kz) {
-      if (Z.w[kz] == 0.0) continue;
-      for (int jy = 0; jy < Y.n; ++jy) {
-        if (Y.w[jy] == 0.0) continue;
-        const double w23 = Y.w[jy]*Z.w[kz];
-        for (int ix = 0; ix < X.n; ++ix) {
-          const double w = w23*X.w[ix];
-          if (w == 0.0) continue;
-          const int b = cloud_owner(c, m, X.o[ix], Y.o[jy], Z.o[kz]);
-          if (b < 0) { err |= DUSTB_ERR_CLOUD; continue; }
-          const double dw = mass_c*w/cloud_measure(c, b);
-          const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-          A5(c->f.qdep, 5, d, b, 0, k, j, i) += dw;
-          A5(c->f.qdep, 5, d, b, 1, k, j, i) += dw*vx;
-          A5(c->f.qdep, 5, d, b, 2, k, j, i) += dw*vy;
-          A5(c->f.qdep, 5, d, b, 3, k, j, i) += dw*vz;
-        }
-      }
-    }
+    const double v[4] = {1.0, PR(DUSTB_IPVX, p), PR(DUSTB_IPVY, p), PR(DUSTB_IPVZ, p)};
+    /* (dw = m c w / V, then dw, dw vx, dw vy, dw vz: the factor 1 keeps dw itself) */
+    cloud_deposit(c, &d, m, x, code, c->f.qdep, 5, 0, 4, mass_c, v, 0, &err);
   }
   return err;
 }
 
 /* PackGatherField3D (src/dust/dust_cloud3d.cpp:1319-1340): gp(m, k, j, i, 0..11) = the
- * velocity and its central differences along x, y, z, over the padded interior */
+ * velocity and its central differences along x, y, z, over the padded interior; 2-D
+ * (PackGatherField, src/dust/dust_pm.cpp:81-102): the plane ks, no x3 differences */
 void oracle_gather_pack(const dustb_ctx *c, const double *v, double *gp) {
   const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
   memset(gp, 0, (size_t)ms->nmb*d.n3*d.n2*d.n1*12*sizeof(double));
-  /* (2-D: PackGatherField, src/dust/dust_pm.cpp:81-102, the plane ks and no x3 differences) */
   const int k0 = ms->three_d ? 1 : d.ks, k1 = ms->three_d ? d.n3 - 2 : d.ks;
   for (int m = 0; m < ms->nmb; ++m)
     for (int k = k0; k <= k1; ++k)
@@ -1173,65 +1264,22 @@ void oracle_gather_pack(const dustb_ctx *c, const double *v, double *gp) {
  * CloudLinearGather3D / GatherLinear, src/dust/dust_imex3d_gather.hpp, dust_leaf_api.hpp:
  * 196-219): ubar = sum over the leaves of w u* + cx du/dx + cy du/dy + cz du/dz with
  * cx = (m1x + MinImage(x - xc) w) / (2 dx); dv = c (ubar - v), v += dv, R = dv / a_dt; with
- * back-reaction -m w dv / V into dmom (cleared first) of the same leaves.  gp: the pack of
- * u* (its ghost cells filled by the caller). */
+ * back-reaction -m w dv / V into dmom (cleared first) of the leaves of nonzero weight.  gp: the
+ * pack of u* (its ghost cells filled by the caller). */
 unsigned oracle_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, const double *gp) {
   const dustb_mesh *ms = &c->mesh; Ind d = indices(ms);
   memset(c->f.dmom, 0, field_size(ms, 3)*sizeof(double));
   double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
-  const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
   const int br = c->phys.back_reaction;
   unsigned err = 0;
   for (int p = 0; p < c->part.npart; ++p) {
     const int m = PI(DUSTB_PGID, p) - ms->gids;
+    const int code = PI(DUSTB_PLEV, p);
     double x[3];
     cloud_position(c, p, sh, x);
-    const int code = PI(DUSTB_PLEV, p);
-    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
-    if (!cloud_ok(c, m, x, code)) { err |= DUSTB_ERR_CLOUD; continue; }
-    CloudAxis X, Y, Z;
-    cloud_axes(c, m, x, code, &X, &Y, &Z);
-    double ug[3] = {0.0, 0.0, 0.0};
-    int nt = 0, tb[216], tk[216], tj[216], ti[216];
-    double tw[216];
-    for (int kz = 0; kz < Z.n; ++kz) {
-      const double w3 = Z.w[kz], g3 = Z.g[kz];
-      if (w3 == 0.0 && g3 == 0.0) continue;
-      for (int jy = 0; jy < Y.n; ++jy) {
-        const double w2 = Y.w[jy], g2 = Y.g[jy];
-        if (w2 == 0.0 && g2 == 0.0) continue;
-        const double w23 = w2*w3;
-        for (int ix = 0; ix < X.n; ++ix) {
-          const double wa = X.w[ix], ga = X.g[ix];
-          const double w = w23*wa;
-          const double m1x = w23*ga, m1y = wa*g2*w3, m1z = wa*w2*g3;
-          if (w == 0.0 && m1x == 0.0 && m1y == 0.0 && m1z == 0.0) continue;
-          const int b = cloud_owner(c, m, X.o[ix], Y.o[jy], Z.o[kz]);
-          if (b < 0) { err |= DUSTB_ERR_CLOUD; continue; }
-          const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-          const double dx1 = MB(b, DX1), dx2 = MB(b, DX2), dx3 = MB(b, DX3);
-          const double xc = MB(b, X1MIN) + (i - d.is + 0.5)*dx1;
-          const double yc = MB(b, X2MIN) + (j - d.js + 0.5)*dx2;
-          const double zc = MB(b, X3MIN) + (k - d.ks + 0.5)*dx3;
-          const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
-          const double cx = 0.5*(m1x + (ex - L[0]*round(ex/L[0]))*w)/dx1;
-          const double cy = 0.5*(m1y + (ey - L[1]*round(ey/L[1]))*w)/dx2;
-          const double *g = gp + ((((size_t)b*d.n3 + k)*d.n2 + j)*d.n1 + i)*12;
-          if (ms->three_d) {
-            const double cz = 0.5*(m1z + (ez - L[2]*round(ez/L[2]))*w)/dx3;
-            ug[0] += w*g[0] + cx*g[3] + cy*g[6] + cz*g[9];
-            ug[1] += w*g[1] + cx*g[4] + cy*g[7] + cz*g[10];
-            ug[2] += w*g[2] + cx*g[5] + cy*g[8] + cz*g[11];
-          } else {
-            ug[0] += w*g[0] + cx*g[3] + cy*g[6];
-            ug[1] += w*g[1] + cx*g[4] + cy*g[7];
-            ug[2] += w*g[2] + cx*g[5] + cy*g[8];
-          }
-          tb[nt] = b; tk[nt] = k; tj[nt] = j; ti[nt] = i; tw[nt] = w;
-          ++nt;
-        }
-      }
-    }
+    if (!cloud_frame_ok(c, m, x, code, 0.0)) { err |= DUSTB_ERR_CLOUD; continue; }
+    double ug[3];
+    cloud_gather(c, &d, m, x, code, gp, ug, &err);
     const double cj = a_dt/(PR(DUSTB_IPTS, p) + a_dt);
     const double dvx = cj*(ug[0] - PR(DUSTB_IPVX, p));
     const double dvy = cj*(ug[1] - PR(DUSTB_IPVY, p));
@@ -1239,68 +1287,10 @@ unsigned oracle_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, co
     PR(DUSTB_IPVX, p) += dvx; PR(DUSTB_IPVY, p) += dvy; PR(DUSTB_IPVZ, p) += dvz;
     PR(DUSTB_IPRX, p) = dvx/a_dt; PR(DUSTB_IPRY, p) = dvy/a_dt; PR(DUSTB_IPRZ, p) = dvz/a_dt;
     if (!br) continue;
-    const double mass = -PR(DUSTB_IPM, p);
-    for (int q = 0; q < nt; ++q) {
-      if (tw[q] == 0.0) continue;
-      const int b = tb[q];
-      const double dw = mass*tw[q]/cloud_measure(c, b);
-      A5(c->f.dmom, 3, d, b, 0, tk[q], tj[q], ti[q]) += dw*dvx;
-      A5(c->f.dmom, 3, d, b, 1, tk[q], tj[q], ti[q]) += dw*dvy;
-      A5(c->f.dmom, 3, d, b, 2, tk[q], tj[q], ti[q]) += dw*dvz;
-    }
+    const double v[3] = {dvx, dvy, dvz};
+    cloud_deposit(c, &d, m, x, code, c->f.dmom, 3, 0, 3, -PR(DUSTB_IPM, p), v, 0, NULL);
   }
   return err;
-}
-
-/* the clouds' linear gather of the packed field gp at one cloud (CloudLinearGather3D
- * without the blend): ubar, and the leaves of nonzero weight (owner block, cell, w) */
-static int cloud_gather(const dustb_ctx *c, const Ind *d, int m, const double x[3], int code,
-                        const double *gp, double ug[3], int *tb, int *tk, int *tj, int *ti,
-                        double *tw, unsigned *err) {
-  const dustb_mesh *ms = &c->mesh;
-  const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
-  CloudAxis X, Y, Z;
-  cloud_axes(c, m, x, code, &X, &Y, &Z);
-  ug[0] = ug[1] = ug[2] = 0.0;
-  int nt = 0;
-  for (int kz = 0; kz < Z.n; ++kz) {
-    const double w3 = Z.w[kz], g3 = Z.g[kz];
-    if (w3 == 0.0 && g3 == 0.0) continue;
-    for (int jy = 0; jy < Y.n; ++jy) {
-      const double w2 = Y.w[jy], g2 = Y.g[jy];
-      if (w2 == 0.0 && g2 == 0.0) continue;
-      const double w23 = w2*w3;
-      for (int ix = 0; ix < X.n; ++ix) {
-        const double wa = X.w[ix], ga = X.g[ix];
-        const double w = w23*wa;
-        const double m1x = w23*ga, m1y = wa*g2*w3, m1z = wa*w2*g3;
-        if (w == 0.0 && m1x == 0.0 && m1y == 0.0 && m1z == 0.0) continue;
-        const int b = cloud_owner(c, m, X.o[ix], Y.o[jy], Z.o[kz]);
-        if (b < 0) { *err |= DUSTB_ERR_CLOUD; continue; }
-        const int k = d->ks + Z.i[kz], j = d->js + Y.i[jy], i = d->is + X.i[ix];
-        const double dx1 = MB(b, DX1), dx2 = MB(b, DX2), dx3 = MB(b, DX3);
-        const double xc = MB(b, X1MIN) + (i - d->is + 0.5)*dx1;
-        const double yc = MB(b, X2MIN) + (j - d->js + 0.5)*dx2;
-        const double zc = MB(b, X3MIN) + (k - d->ks + 0.5)*dx3;
-        const double ex = x[0] - xc, ey = x[1] - yc, ez = x[2] - zc;
-        const double cx = 0.5*(m1x + (ex - L[0]*round(ex/L[0]))*w)/dx1;
-        const double cy = 0.5*(m1y + (ey - L[1]*round(ey/L[1]))*w)/dx2;
-        const double *g = gp + ((((size_t)b*d->n3 + k)*d->n2 + j)*d->n1 + i)*12;
-        if (ms->three_d) {
-          const double cz = 0.5*(m1z + (ez - L[2]*round(ez/L[2]))*w)/dx3;
-          ug[0] += w*g[0] + cx*g[3] + cy*g[6] + cz*g[9];
-          ug[1] += w*g[1] + cx*g[4] + cy*g[7] + cz*g[10];
-          ug[2] += w*g[2] + cx*g[5] + cy*g[8] + cz*g[11];
-        } else {
-          ug[0] += w*g[0] + cx*g[3] + cy*g[6];
-          ug[1] += w*g[1] + cx*g[4] + cy*g[7];
-          ug[2] += w*g[2] + cx*g[5] + cy*g[8];
-        }
-        if (w != 0.0) { tb[nt] = b; tk[nt] = k; tj[nt] = j; ti[nt] = i; tw[nt] = w; ++nt; }
-      }
-    }
-  }
-  return nt;
 }
 
 /* CloudDefectCorrection (src/dust/dust_imex3d_dc.cpp:229-274) with CloudOperatorKernelT
@@ -1316,25 +1306,16 @@ unsigned oracle_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh) {
   oracle_gather_pack(c, x, gp);
   memset(r, 0, field_size(ms, 3)*sizeof(double));
   unsigned err = 0;
-  int tb[216], tk[216], tj[216], ti[216];
-  double tw[216];
   for (int p = 0; p < c->part.npart; ++p) {
     const int m = PI(DUSTB_PGID, p) - ms->gids;
+    const int code = PI(DUSTB_PLEV, p);
     double xp[3];
     cloud_position(c, p, sh, xp);
-    const int code = PI(DUSTB_PLEV, p);
-    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, xp);
-    if (!cloud_ok(c, m, xp, code)) { err |= DUSTB_ERR_CLOUD; continue; }
+    if (!cloud_frame_ok(c, m, xp, code, 0.0)) { err |= DUSTB_ERR_CLOUD; continue; }
     double ug[3];
-    const int nt = cloud_gather(c, &d, m, xp, code, gp, ug, tb, tk, tj, ti, tw, &err);
+    cloud_gather(c, &d, m, xp, code, gp, ug, &err);
     const double mc = PR(DUSTB_IPM, p)*(a_dt/(PR(DUSTB_IPTS, p) + a_dt));
-    for (int q = 0; q < nt; ++q) {
-      const int b = tb[q];
-      const double dw = mc*tw[q]/cloud_measure(c, b);
-      A5(r, 3, d, b, 0, tk[q], tj[q], ti[q]) += dw*ug[0];
-      A5(r, 3, d, b, 1, tk[q], tj[q], ti[q]) += dw*ug[1];
-      A5(r, 3, d, b, 2, tk[q], tj[q], ti[q]) += dw*ug[2];
-    }
+    cloud_deposit(c, &d, m, xp, code, r, 3, 0, 3, mc, ug, 0, NULL);
   }
   free(gp);
   for (int m = 0; m < ms->nmb; ++m)
@@ -1351,6 +1332,13 @@ unsigned oracle_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh) {
           }
         }
   return err;
+}
+
+/* the overlap split's particle part: rv = sum over the leaves of w res */
+typedef struct { const Ind *d; const double *res; double rv[3]; } ResCtx;
+static void res_leaf(void *vctx, const CloudLeaf *lf) {
+  ResCtx *q = (ResCtx *)vctx;
+  for (int v = 0; v < 3; ++v) q->rv[v] += lf->w*A5(q->res, 4, (*q->d), lf->b, v, lf->k, lf->j, lf->i);
 }
 
 /* ApplyPMBR for the clouds (src/dust/dust_pm.cpp:576-711): with imex_consistent_gas the
@@ -1385,33 +1373,16 @@ void oracle_cloud_apply_pmbr(const dustb_ctx *c, double a_dt, double sh) {
   for (int p = 0; p < c->part.npart; ++p) {
     if (PR(DUSTB_IPM, p) <= 0.0) continue;
     const int m = PI(DUSTB_PGID, p) - ms->gids;
+    const int code = PI(DUSTB_PLEV, p);
     double x[3];
     cloud_position(c, p, sh, x);
-    const int code = PI(DUSTB_PLEV, p);
-    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
-    if (!cloud_ok(c, m, x, code)) continue;
-    CloudAxis X, Y, Z;
-    cloud_axes(c, m, x, code, &X, &Y, &Z);
-    double rv[3] = {0.0, 0.0, 0.0};
-    for (int kz = 0; kz < Z.n; ++kz) {
-      if (Z.w[kz] == 0.0) continue;
-      for (int jy = 0; jy < Y.n; ++jy) {
-        if (Y.w[jy] == 0.0) continue;
-        const double w23 = Y.w[jy]*Z.w[kz];
-        for (int ix = 0; ix < X.n; ++ix) {
-          const double w = w23*X.w[ix];
-          if (w == 0.0) continue;
-          const int b = cloud_owner(c, m, X.o[ix], Y.o[jy], Z.o[kz]);
-          if (b < 0) continue;
-          const int k = d.ks + Z.i[kz], j = d.js + Y.i[jy], i = d.is + X.i[ix];
-          for (int v = 0; v < 3; ++v) rv[v] += w*A5(res, 4, d, b, v, k, j, i);
-        }
-      }
-    }
+    if (!cloud_frame_ok(c, m, x, code, 0.0)) continue;
+    ResCtx q = {&d, res, {0.0, 0.0, 0.0}};
+    cloud_leaves(c, &d, m, x, code, 0, res_leaf, &q, NULL);
     const double cj = a_dt/(PR(DUSTB_IPTS, p) + a_dt);
-    PR(DUSTB_IPVX, p) += cj*rv[0]; PR(DUSTB_IPVY, p) += cj*rv[1]; PR(DUSTB_IPVZ, p) += cj*rv[2];
-    PR(DUSTB_IPRX, p) += cj*rv[0]/a_dt; PR(DUSTB_IPRY, p) += cj*rv[1]/a_dt;
-    PR(DUSTB_IPRZ, p) += cj*rv[2]/a_dt;
+    PR(DUSTB_IPVX, p) += cj*q.rv[0]; PR(DUSTB_IPVY, p) += cj*q.rv[1]; PR(DUSTB_IPVZ, p) += cj*q.rv[2];
+    PR(DUSTB_IPRX, p) += cj*q.rv[0]/a_dt; PR(DUSTB_IPRY, p) += cj*q.rv[1]/a_dt;
+    PR(DUSTB_IPRZ, p) += cj*q.rv[2]/a_dt;
   }
 }
 
@@ -1435,29 +1406,19 @@ unsigned oracle_cloud_pc2_predictor(const dustb_ctx *c, double dt, int rate_dep)
   oracle_gather_pack(c, uv, gp);
   const double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
   unsigned err = 0;
-  int tb[216], tk[216], tj[216], ti[216];
-  double tw[216];
   for (int p = 0; p < c->part.npart; ++p) {
     const int m = PI(DUSTB_PGID, p) - ms->gids;
+    const int code = PI(DUSTB_PLEV, p);
     double x[3];
     cloud_position(c, p, 0.0, x);
-    const int code = PI(DUSTB_PLEV, p);
-    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, x);
-    if (!cloud_ok(c, m, x, code)) { err |= DUSTB_ERR_CLOUD; continue; }
+    if (!cloud_frame_ok(c, m, x, code, 0.0)) { err |= DUSTB_ERR_CLOUD; continue; }
     double ug[3];
-    const int nt = cloud_gather(c, &d, m, x, code, gp, ug, tb, tk, tj, ti, tw, &err);
+    cloud_gather(c, &d, m, x, code, gp, ug, &err);
     const double mass_rate = PR(DUSTB_IPM, p)/PR(DUSTB_IPTS, p);
-    const double gx = -dt*mass_rate*(ug[0] - PR(DUSTB_IPVX, p));
-    const double gy = -dt*mass_rate*(ug[1] - PR(DUSTB_IPVY, p));
-    const double gz = -dt*mass_rate*(ug[2] - PR(DUSTB_IPVZ, p));
-    for (int q = 0; q < nt; ++q) {
-      const int b = tb[q];
-      const double inv_volume = 1.0/cloud_measure(c, b);
-      A5(c->f.qdep, 5, d, b, 1, tk[q], tj[q], ti[q]) += inv_volume*tw[q]*gx;
-      A5(c->f.qdep, 5, d, b, 2, tk[q], tj[q], ti[q]) += inv_volume*tw[q]*gy;
-      A5(c->f.qdep, 5, d, b, 3, tk[q], tj[q], ti[q]) += inv_volume*tw[q]*gz;
-      if (rate_dep) A5(c->f.qdep, 5, d, b, 4, tk[q], tj[q], ti[q]) += inv_volume*tw[q]*mass_rate;
-    }
+    const double v[4] = {-dt*mass_rate*(ug[0] - PR(DUSTB_IPVX, p)),
+                         -dt*mass_rate*(ug[1] - PR(DUSTB_IPVY, p)),
+                         -dt*mass_rate*(ug[2] - PR(DUSTB_IPVZ, p)), mass_rate};
+    cloud_deposit(c, &d, m, x, code, c->f.qdep, 5, 1, rate_dep ? 4 : 3, 1.0, v, 1, NULL);
   }
   free(gp); free(uv);
   return err;
@@ -1477,8 +1438,6 @@ unsigned oracle_cloud_pc2_advance(const dustb_ctx *c, double dt) {
   const int br = c->phys.back_reaction, sbox = c->phys.shearing_box, strat = c->phys.stratified;
   const double q = c->phys.qshear, om = c->phys.omega0, aphi = c->phys.const_accel_phi;
   unsigned err = 0;
-  int tb[216], tk[216], tj[216], ti[216];
-  double tw[216];
   for (int p = 0; p < c->part.npart; ++p) {
     const int m = PI(DUSTB_PGID, p) - ms->gids;
     const double x0[3] = {PR(DUSTB_IPX1, p), PR(DUSTB_IPY1, p), ms->three_d ? PR(DUSTB_IPZ1, p) : 0.0};
@@ -1499,10 +1458,9 @@ unsigned oracle_cloud_pc2_advance(const dustb_ctx *c, double dt) {
     }
     const int code = PI(DUSTB_PLEV, p);
     double xf[3] = {xg[0], xg[1], xg[2]};
-    if (m >= 0 && m < ms->nmb) cloud_frame(c, m, xf);
-    if (!cloud_ok_slack(c, m, xf, code, 1.0)) { err |= DUSTB_ERR_CLOUD; continue; }
+    if (!cloud_frame_ok(c, m, xf, code, 1.0)) { err |= DUSTB_ERR_CLOUD; continue; }
     double ug[3];
-    const int nt = cloud_gather(c, &d, m, xf, code, gp, ug, tb, tk, tj, ti, tw, &err);
+    cloud_gather(c, &d, m, xf, code, gp, ug, &err);
     const double h = 0.5*dt;
     const double lambda = h/PR(DUSTB_IPTS, p);
     const double aa = 1.0 + lambda;
@@ -1543,19 +1501,12 @@ unsigned oracle_cloud_pc2_advance(const dustb_ctx *c, double dt) {
     }
     PR(DUSTB_IPX1, p) = xh[0]; PR(DUSTB_IPY1, p) = xh[1];
     if (ms->three_d) PR(DUSTB_IPZ1, p) = xh[2];
-    const double dvx = dt*(ug[0] - vh[0])/PR(DUSTB_IPTS, p);
-    const double dvy = dt*(ug[1] - vh[1])/PR(DUSTB_IPTS, p);
-    const double dvz = dt*(ug[2] - vh[2])/PR(DUSTB_IPTS, p);
-    PR(DUSTB_IPRX, p) = dvx; PR(DUSTB_IPRY, p) = dvy; PR(DUSTB_IPRZ, p) = dvz;
+    const double dv[3] = {dt*(ug[0] - vh[0])/PR(DUSTB_IPTS, p),
+                          dt*(ug[1] - vh[1])/PR(DUSTB_IPTS, p),
+                          dt*(ug[2] - vh[2])/PR(DUSTB_IPTS, p)};
+    PR(DUSTB_IPRX, p) = dv[0]; PR(DUSTB_IPRY, p) = dv[1]; PR(DUSTB_IPRZ, p) = dv[2];
     if (!br) continue;
-    const double mass = -PR(DUSTB_IPM, p);
-    for (int qq = 0; qq < nt; ++qq) {
-      const int b = tb[qq];
-      const double dw = mass*tw[qq]/cloud_measure(c, b);
-      A5(c->f.dmom, 3, d, b, 0, tk[qq], tj[qq], ti[qq]) += dw*dvx;
-      A5(c->f.dmom, 3, d, b, 1, tk[qq], tj[qq], ti[qq]) += dw*dvy;
-      A5(c->f.dmom, 3, d, b, 2, tk[qq], tj[qq], ti[qq]) += dw*dvz;
-    }
+    cloud_deposit(c, &d, m, xf, code, c->f.dmom, 3, 0, 3, -PR(DUSTB_IPM, p), dv, 0, NULL);
   }
   free(gp);
   return err;

@@ -13,7 +13,7 @@ that pin it without the reference binary:
 import numpy as np
 import pytest
 
-from athenak_b200.inputs import make_state
+from athenak_b200.inputs import _block_of, make_state
 from athenak_b200.mesh import uniform_mesh
 from oracle.oracle import Oracle
 
@@ -251,3 +251,44 @@ def test_cloud_pc2_cycles_conserve_momentum():
     n = st.npart
     scale = np.abs(st.pr[16, :n] * np.abs(st.pr[[1, 3, 5], :n]).max(axis=0)).sum()
     assert np.abs(p1 - p0).max() < 1e-12 * scale
+
+
+# ---- clouds at physical x3 faces: the mirrored part ----
+def setup_x3(levels=(0, 1), seed=7, x3bc=1):
+    ms = uniform_mesh((16, 16, 16), (8, 8, 8), 2, (-0.05,) * 3, (0.05,) * 3, x3bc=x3bc)
+    st = make_state(ms, [0.1, 0.01], [1.0, 0.5], 2, seed=seed, vel_noise=0.05, gas_noise=1e-2)
+    n = st.npart
+    st.pi[3, :n] = np.asarray(levels)[np.arange(n) % len(levels)]
+    # a share of the clouds within a cell of the x3 faces
+    st.pr[4, :n:5] = np.where(np.arange(len(st.pr[4, :n:5])) % 2, 0.05 - 0.004, -0.05 + 0.003)
+    st.pr[10, :n] = st.pr[4, :n]
+    st.pi[0, :n] = _block_of(ms, st.pr[0, :n], st.pr[2, :n], st.pr[4, :n])
+    return ms, st
+
+
+@pytest.mark.parametrize("x3bc", [1, 2])
+def test_clouds_at_physical_x3_faces_keep_their_mass(x3bc):
+    """The part of a cloud beyond a physical x3 face comes back as the mirrored part: the
+    deposit holds every cloud's whole coupled mass, and nothing lands in a ghost cell."""
+    ms, st = setup_x3(x3bc=x3bc)
+    o = Oracle(st, dict(scheme=2))
+    a_dt = 1.5e-3
+    assert o.cloud_deposit_qp(a_dt) == 0
+    n = st.npart
+    want = (st.pr[16, :n] * a_dt / (st.pr[15, :n] + a_dt)).sum()
+    got = ms.active(o.qdep)[:, 0].sum() * ms.cell_volume()
+    assert abs(got - want) < 1e-13 * want
+    assert np.abs(o.qdep[:, 0]).sum() * ms.cell_volume() == pytest.approx(got, rel=1e-14)
+
+
+def test_cloud_cycles_at_a_reflecting_face_conserve_momentum():
+    ms, st = setup_x3((0, 1, 2), seed=8)
+    o = Oracle(st, dict(scheme=2, drag_solver=2))
+    p0 = sum(o.momentum())
+    for _ in range(3):
+        assert o.cloud_imex_cycle(2e-3) == 0
+    p1 = sum(o.momentum())
+    n = o.st.npart
+    scale = np.abs(st.pr[16, :n] * np.abs(st.pr[[1, 3, 5], :n]).max(axis=0)).sum()
+    # (x1, x2: exact; x3: the reflections of crossing particles change p_z)
+    assert np.abs(p1[:2] - p0[:2]).max() < 1e-12 * scale

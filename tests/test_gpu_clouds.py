@@ -172,3 +172,36 @@ def test_cloud_pc2_cycles_match_oracle(dims):
     for v in range(4):
         sc = max(np.abs(o.u0[:, v]).max(), 1e-300)
         assert np.abs(gu[:, v] - o.u0[:, v]).max() <= 1e-11 * sc, v
+
+
+@pytest.mark.parametrize("coupling", ["imex", "pc2"])
+def test_cloud_cycles_at_physical_x3_faces_match_oracle(coupling):
+    """Clouds within a cell of reflecting x3 faces (their mirrored parts) through three imex2+
+    or pc2 cycles of a stratified box: particles within 1e-12, the gas within 1e-11."""
+    from athenak_b200.drag import DeviceDust
+    from tests.test_clouds import setup_x3
+    ms, st = setup_x3((0, 1, 2), seed=31)
+    phys = dict(scheme=2, drag_solver=2, stratified=True)
+    o, g = Oracle(st, phys), DeviceDust(st, phys)
+    g.init_gas_ghosts()
+    u = g.host("u0")
+    o.u0[...] = u
+    for _ in range(3):
+        if coupling == "imex":
+            assert o.cloud_imex_cycle(2e-3) == 0
+            g.cloud_imex_cycle(2e-3)
+        else:
+            assert o.cloud_pc2_cycle(2e-3)[0] == 0
+            g.cloud_pc2_cycle(2e-3)
+    torch.cuda.synchronize()
+    assert g.error_word() == 0
+    n = o.st.npart
+    gp, gi = g.host("pr"), g.host("pi")
+    np.testing.assert_array_equal(gi, o.st.pi[:, :n])
+    for r in range(17):
+        sc = max(np.abs(o.st.pr[r, :n]).max(), 1e-300)
+        assert np.abs(gp[r] - o.st.pr[r, :n]).max() <= 1e-12 * sc, r
+    gu = g.host("u0")
+    for v in range(4):
+        sc = max(np.abs(o.u0[:, v]).max(), 1e-300)
+        assert np.abs(gu[:, v] - o.u0[:, v]).max() <= 1e-11 * sc, v
