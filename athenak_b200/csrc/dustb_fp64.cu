@@ -458,19 +458,74 @@ __global__ void k_scatter(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, doub
 // (InitRecvIndices :281-297) += the neighbour's ghost cells at index - o*nx, in
 // NeighborIndex order.
 
+// The active cells within ng of a face of their block (the only ones a neighbour's ghost
+// cells reach), enumerated per block: the near x3 planes whole (zn of them), then in each of
+// the zin inner planes its near x2 rows whole (yn) and, in each of its yin inner rows, the xn
+// cells near the x1 faces.  A dimension the mesh lacks has no near part (zn = 0, zin = nx3).
+struct Shell { int zn, zin, yn, yin, xn, xin, zoff, yoff; long long per; };
+
+__host__ __device__ inline Shell make_shell(const Ind &d) {
+  Shell h;
+  const int g2 = 2 * d.ng;
+  h.xn = d.nx1 < g2 ? d.nx1 : g2;
+  h.xin = d.nx1 - h.xn;
+  h.yn = d.multi_d ? (d.nx2 < g2 ? d.nx2 : g2) : 0;
+  h.yin = d.nx2 - h.yn;
+  h.zn = d.three_d ? (d.nx3 < g2 ? d.nx3 : g2) : 0;
+  h.zin = d.nx3 - h.zn;
+  h.yoff = d.multi_d ? d.ng : 0;
+  h.zoff = d.three_d ? d.ng : 0;
+  h.per = (long long)h.zn * d.nx2 * d.nx1 +
+          (long long)h.zin * ((long long)h.yn * d.nx1 + (long long)h.yin * h.xn);
+  return h;
+}
+
+// t in [0, per) -> the cell's offsets from (ks, js, is)
+__device__ __forceinline__ void shell_cell(const Ind &d, const Shell &h, long long t, int &k,
+                                           int &j, int &i) {
+  const long long plane = (long long)d.nx2 * d.nx1;
+  if (t < (long long)h.zn * plane) {
+    const int z = (int)(t / plane);
+    const long long r = t - z * plane;
+    k = z < d.ng ? z : z + h.zin;
+    j = (int)(r / d.nx1);
+    i = (int)(r - (long long)j * d.nx1);
+    return;
+  }
+  t -= (long long)h.zn * plane;
+  const long long inner = (long long)h.yn * d.nx1 + (long long)h.yin * h.xn;
+  const int z = (int)(t / inner);
+  long long r = t - z * inner;
+  k = h.zoff + z;
+  if (r < (long long)h.yn * d.nx1) {
+    const int y = (int)(r / d.nx1);
+    j = y < d.ng ? y : y + h.yin;
+    i = (int)(r - (long long)y * d.nx1);
+    return;
+  }
+  r -= (long long)h.yn * d.nx1;
+  const int y = (int)(r / h.xn);
+  const int u = (int)(r - (long long)y * h.xn);
+  j = h.yoff + y;
+  i = u < d.ng ? u : u + h.xin;
+}
+
 // fold: fold the ghost deposits beyond physical x3 faces back into the mirrored active cells
 __global__ void k_ghost_add(Ind d, const int *nghbr, int gids, double *a, int nvar, int fold,
                             SBox B) {
   int m, k, j, i;
+  const Shell sh = make_shell(d);
   long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  long long ncell = (long long)d.nmb * d.nx3 * d.nx2 * d.nx1;
+  const long long ncell = (long long)d.nmb * sh.per;
   int v = (int)(idx / ncell);
   if (v >= nvar) return;
-  if (!active_cell(d, idx - (long long)v * ncell, m, k, j, i)) return;
+  {
+    const long long r = idx - (long long)v * ncell;
+    m = (int)(r / sh.per);
+    shell_cell(d, sh, r - (long long)m * sh.per, k, j, i);
+    k += d.ks; j += d.js; i += d.is;
+  }
   const int ng1 = d.ng - 1;
-  const bool near = (i <= d.is + ng1) || (i >= d.ie - ng1) || (j <= d.js + ng1 && d.multi_d) ||
-                    (j >= d.je - ng1 && d.multi_d) || (d.three_d && (k <= d.ks + ng1 || k >= d.ke - ng1));
-  if (!near) return;
   const int ndir = d.three_d ? 26 : (d.multi_d ? 8 : 2);
   const long long at = d.at(m, nvar, v, k, j, i);
   double val = a[at];
@@ -1863,7 +1918,7 @@ int dustb_ghost_add(const dustb_ctx *c, double *field, int nvar, void *stream) {
   Ind d = make_ind(c->mesh);
   const int fold = d.three_d && c->mesh.x3bc != DUSTB_X3_PERIODIC && !c->phys.x3_deposit_drop;
   const SBox B = sbview(c);
-  k_ghost_add<<<blocks_for(n_active(d) * nvar), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar, fold,
+  k_ghost_add<<<blocks_for(make_shell(d).per * d.nmb * nvar), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar, fold,
                                                                           B);
   if (B.on) {
     if (!B.sb_gid || B.nb2 <= 0 || B.nb3 <= 0) return DUSTB_EINVAL;
