@@ -692,26 +692,29 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   const unsigned act = __ballot_sync(0xffffffffu, live);
   if (!live) return;
   const int key = key_in[p];
-  const int q = warp_slot(cursor, key, act);
+  // the source copy is only read here: its loads go through the read-only path and are all
+  // issued before the slot's atomic, whose round trip then overlaps theirs
+  const float *const *sf = S.f;
   int m, k, j, i;
-  decode(G, S.cell[p], m, k, j, i);
-  float o[3] = {S.f[F_OX][p], S.f[F_OY][p], S.f[F_OZ][p]};
-  float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
-  const float ts = S.f[F_TS][p];
-  float mass = S.f[F_M][p];
+  decode(G, __ldg(S.cell + p), m, k, j, i);
+  float o[3] = {__ldg(sf[F_OX] + p), __ldg(sf[F_OY] + p), __ldg(sf[F_OZ] + p)};
+  float v[3] = {__ldg(sf[F_VX] + p), __ldg(sf[F_VY] + p), __ldg(sf[F_VZ] + p)};
+  const float ts = __ldg(sf[F_TS] + p);
+  float mass = __ldg(sf[F_M] + p);
+  const int pid = __ldg(S.pid + p);
   float v1[3], d1[3], r[3] = {0.0f, 0.0f, 0.0f}, cc;
-  if (KIND == PK_FULL) {
+  const bool kick = KIND != PK_FULL && P.res && (P.stage2 || P.head->pending);
+  if (KIND == PK_FULL || P.stage2) {
     // pc2: the advance left the new velocity, the rate and the displacement to the new
-    // position; the register velocity is v0
-    v1[0] = S.f[F_WX][p]; v1[1] = S.f[F_WY][p]; v1[2] = S.f[F_WZ][p];
-    d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p];
-    r[0] = S.f[F_RX][p]; r[1] = S.f[F_RY][p]; r[2] = S.f[F_RZ][p];
-    cc = S.f[F_CC][p];
-  } else {
-    // (imex stage 1 and the pc2 half step: the rates are not read; every kick rewrites them)
-    const bool kick = P.res && (P.stage2 || P.head->pending);
-    cc = (P.stage2 || kick) ? S.f[F_CC][p] : 0.0f;
-    if (P.stage2) { r[0] = S.f[F_RX][p]; r[1] = S.f[F_RY][p]; r[2] = S.f[F_RZ][p]; }
+    // position; the register velocity is v0.  imex stage 2: the stage registers and rates
+    v1[0] = __ldg(sf[F_WX] + p); v1[1] = __ldg(sf[F_WY] + p); v1[2] = __ldg(sf[F_WZ] + p);
+    d1[0] = __ldg(sf[F_AX] + p); d1[1] = __ldg(sf[F_AY] + p); d1[2] = __ldg(sf[F_AZ] + p);
+    r[0] = __ldg(sf[F_RX] + p); r[1] = __ldg(sf[F_RY] + p); r[2] = __ldg(sf[F_RZ] + p);
+  }
+  // (imex stage 1 and the pc2 half step: the rates are not read; every kick rewrites them)
+  cc = (KIND == PK_FULL || P.stage2 || kick) ? __ldg(sf[F_CC] + p) : 0.0f;
+  const int q = warp_slot(cursor, key, act);
+  if (KIND != PK_FULL) {
     if (kick && mass > 0.0f) {
       double d[3];
       consistent_dv(G, P, cc, m, k, j, i, d);
@@ -720,10 +723,7 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
         r[a] += (float)(d[a] / P.a_dt);
       }
     }
-    if (P.stage2) {
-      v1[0] = S.f[F_WX][p]; v1[1] = S.f[F_WY][p]; v1[2] = S.f[F_WZ][p];
-      d1[0] = S.f[F_AX][p]; d1[1] = S.f[F_AY][p]; d1[2] = S.f[F_AZ][p];
-    } else {
+    if (!P.stage2) {
       // FirstTwoImpRK: (x1, v1) <- (x, v); the drag factor of the cycle, formed in FP64
       // (imex: a/(t_s + a); pc2: h/(t_s + h))
       v1[0] = v[0]; v1[1] = v[1]; v1[2] = v[2];
@@ -772,7 +772,7 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   }
   // (an edge particle keeps its cell; its slot is in the edge bin)
   D.cell[q] = (flags & AF_EDGE) ? encode(G, m, k, j, i) : key;
-  D.pid[q] = S.pid[p];
+  D.pid[q] = pid;
   D.f[F_OX][q] = o[0]; D.f[F_OY][q] = o[1]; D.f[F_OZ][q] = o[2];
   D.f[F_VX][q] = nv[0]; D.f[F_VY][q] = nv[1]; D.f[F_VZ][q] = nv[2];
   D.f[F_AX][q] = d1[0]; D.f[F_AY][q] = d1[1]; D.f[F_AZ][q] = d1[2];
