@@ -3,7 +3,8 @@
 
 Workload (the metric's configuration): uniform 256^3 mesh as 64 MeshBlocks of 64^3 (ng = 2),
 4 species tau_s = {0.01, 0.1, 1, 10}/Omega, epsilon 0.5 each, ppc 4 per species
-(268,435,456 particles), uniform-random positions (seeded hash), NSH-drift velocities plus
+(268,435,456 particles), uniform-random positions (seeded hash; the rows then put in cell
+order once, as the reference's SortParticles keeps them), NSH-drift velocities plus
 Gaussian 1e-3 c_s noise, gas NSH drift plus 1e-3 uniform noise, imex2+ with dc1, TSC,
 consistent point split, dt from CFL 0.3 on a 40 H periodic box so dt/tau_s spans ~4e-3..4.5.
 A step is one imex2+ cycle (two working stages) of every particle; inputs (~20-46 GB) are far
@@ -234,6 +235,9 @@ def run_ours(args, rep):
         return
     dev, ms, W = build_workload(args.small, cells=args.cells)
     npart, dt = W["npart"], W["dt"]
+    # the rows in cell order (SortParticles, which the reference runs every sort interval so
+    # that its particles stay close to cell order), as both forms find them in a run
+    dev.sort_by_cell()
     torch.cuda.synchronize()
     res = {}
 
@@ -480,6 +484,7 @@ def measure_pc2_strat(args, stream, maxall, barrier):
     from athenak_b200.mixed import MixedDust
     dev, ms, W = build_strat(args.small)
     npart, dt = W["npart"], W["dt"]
+    dev.sort_by_cell()                        # the rows in cell order (SortParticles)
     pr0, pi0, u00 = dev.t["pr"].clone(), dev.t["pi"].clone(), dev.t["u0"].clone()
     mx = MixedDust(dev=dev, do_import=False)
     mx.import_()
@@ -594,6 +599,7 @@ def measure_clouds(args):
     d.nb1, d.nb2, d.nb3 = ms.nblocks
     dev.seed_uniform(d)
     dev.init_gas_ghosts()
+    dev.sort_by_cell()                        # the rows in cell order (SortParticles)
     dt = 0.3 / cells[0]
     pr0, pi0, u00 = dev.t["pr"].clone(), dev.t["pi"].clone(), dev.t["u0"].clone()
     steps = max(1, min(args.steps, 3))
