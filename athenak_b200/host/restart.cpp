@@ -109,6 +109,7 @@ std::string UnpackState(const char *p, std::size_t nbytes, ParticleRestartSectio
       std::int32_t v[3];
       ok = fixed(v, sizeof(v));
       s.rank = v[0]; s.gids = v[1]; s.nmb = v[2];
+      s.rank_blocks_read = ok;
     } else if (name == "merge_pass") {
       ok = fixed(&s.merge_pass, sizeof(s.merge_pass));
     } else if (name == "species_table") {
@@ -200,6 +201,8 @@ std::string PackParticleRestartRows(const double *pr, const int *pi, long long s
                                     std::int64_t np, double dtnew,
                                     const ParticleRestartState &st, std::vector<char> &buf) {
   if (np < 0 || stride < np || (np > 0 && (!pr || !pi))) return "restart: bad particle rows";
+  if (st.nranks < 1 || st.rank < 0 || st.rank >= st.nranks)
+    return "restart: the writing rank or the rank count is out of range";
   std::vector<char> state;
   PackState(st, state);
   if (state.size() > kStateMax) return "restart: the dust records exceed the int32 length";
@@ -211,7 +214,7 @@ std::string PackParticleRestartRows(const double *pr, const int *pi, long long s
   buf.reserve(total);
   Put(buf, kMagic, 8);
   const std::int32_t head[6] = {kVersion, static_cast<std::int32_t>(sizeof(double)),
-                                static_cast<std::int32_t>(sizeof(int)), 1, kNReal, kNInt};
+                                static_cast<std::int32_t>(sizeof(int)), st.nranks, kNReal, kNInt};
   Put(buf, head, sizeof(head));
   PutValue(buf, total);
   PutValue(buf, np);
@@ -243,8 +246,10 @@ std::string PackParticleRestart(const dustb_ctx &ctx, void *stream, double dtnew
   return PackParticleRestartRows(pr.data(), pi.data(), np, np, dtnew, st, buf);
 }
 
-std::string ParseParticleRestart(const std::vector<char> &buf, ParticleRestartSection &out) {
+std::string ParseParticleRestart(const std::vector<char> &buf, ParticleRestartSection &out,
+                                 int nsec) {
   out = ParticleRestartSection();
+  if (nsec < 1) return "restart: no particle section";
   if (buf.size() < kHeadBytes + 8 || std::memcmp(buf.data(), kMagic, 8) != 0 ||
       std::memcmp(buf.data() + buf.size() - 8, kMagic, 8) != 0)
     return "restart: missing or truncated particle section (no head or end marker)";
@@ -254,7 +259,7 @@ std::string ParseParticleRestart(const std::vector<char> &buf, ParticleRestartSe
   std::memcpy(&total, buf.data() + 8 + sizeof(head), sizeof(total));
   const bool columns_ok = head[5] == kNInt || (head[0] == 1 && head[5] == kNInt - 1);
   if ((head[0] != 1 && head[0] != 2) || head[1] != (std::int32_t)sizeof(double) ||
-      head[2] != (std::int32_t)sizeof(int) || head[3] != 1 || head[4] != kNReal || !columns_ok)
+      head[2] != (std::int32_t)sizeof(int) || head[3] != nsec || head[4] != kNReal || !columns_ok)
     return "restart: version, type sizes, rank count or particle columns do not match (file: "
            "version " + std::to_string(head[0]) + ", Real " + std::to_string(head[1]) +
            " bytes, int " + std::to_string(head[2]) + " bytes, ranks " + std::to_string(head[3]) +
@@ -272,6 +277,7 @@ std::string ParseParticleRestart(const std::vector<char> &buf, ParticleRestartSe
     return "restart: sizes inside the section are inconsistent";
   std::string err = UnpackState(buf.data() + at, (std::size_t)nstate, out);
   if (!err.empty()) return "restart: " + err;
+  out.state.nranks = head[3];
   at += (std::size_t)nstate;
   const std::size_t n = (std::size_t)out.np;
   out.pr.resize(n * kNReal);
@@ -296,6 +302,97 @@ std::string RestoreParticleRows(const ParticleRestartSection &sec, dustb_ctx &ct
       return "restart: particle rows not restored";
   if (cudaStreamSynchronize(s) != cudaSuccess) return "restart: particle rows not restored";
   ctx.part.npart = static_cast<int>(np);
+  return "";
+}
+
+std::string SplitParticleRestart(const std::vector<char> &file, std::size_t at,
+                                 std::vector<std::vector<char>> &sections) {
+  sections.clear();
+  while (at < file.size()) {
+    if (file.size() - at < kHeadBytes + 8 || std::memcmp(file.data() + at, kMagic, 8) != 0)
+      return "restart: particle section " + std::to_string(sections.size()) +
+             " has no head at byte " + std::to_string(at);
+    std::uint64_t total = 0;
+    std::memcpy(&total, file.data() + at + 8 + 6 * sizeof(std::int32_t), sizeof(total));
+    if (total < kHeadBytes + 8 || total > file.size() - at)
+      return "restart: particle section " + std::to_string(sections.size()) +
+             " runs past the end of the file";
+    sections.emplace_back(file.begin() + (std::ptrdiff_t)at,
+                          file.begin() + (std::ptrdiff_t)(at + total));
+    at += total;
+  }
+  if (sections.empty()) return "restart: no particle section";
+  return "";
+}
+
+std::string ParticleRestartOwnSectionMatches(const std::vector<std::vector<char>> &sections,
+                                             int me, int nranks, int gids, int nmb,
+                                             bool &match) {
+  match = false;
+  const int nsec = static_cast<int>(sections.size());
+  if (nsec < 1) return "restart: no particle section";
+  if (nranks < 1 || me < 0 || me >= nranks || nmb < 0) return "restart: bad rank or blocks";
+  if (nsec != nranks) return "";
+  ParticleRestartSection own;
+  std::string err = ParseParticleRestart(sections[me], own, nsec);
+  if (!err.empty()) return err;
+  // one rank: also sections written before the rank_blocks record existed
+  match = nranks == 1 || (own.state.rank_blocks_read && own.state.rank == me &&
+                          own.state.gids == gids && own.state.nmb == nmb);
+  return "";
+}
+
+std::string SelectParticleRestart(const std::vector<std::vector<char>> &sections, int me,
+                                  int gids, int nmb, bool exact, ParticleRestartSection &out) {
+  out = ParticleRestartSection();
+  const int nsec = static_cast<int>(sections.size());
+  if (nsec < 1) return "restart: no particle section";
+  if (me < 0 || nmb < 0 || (exact && me >= nsec)) return "restart: bad rank or blocks";
+  auto mine = [&](int gid) { return gid >= gids && gid < gids + nmb; };
+  if (exact) {
+    std::string err = ParseParticleRestart(sections[me], out, nsec);
+    if (!err.empty()) return err;
+    for (std::int64_t p = 0; p < out.np; ++p)
+      if (!mine(out.pi[(std::size_t)p]))
+        return "restart: a particle names a MeshBlock that does not exist (particle " +
+               std::to_string(p) + ", block " + std::to_string(out.pi[(std::size_t)p]) + ")";
+    return "";
+  }
+  // the rows kept, row by row, then packed into the section's layout (row r at r * np)
+  std::vector<std::vector<double>> rc(kNReal);
+  std::vector<std::vector<int>> ic(kNInt);
+  for (int k = 0; k < nsec; ++k) {
+    ParticleRestartSection s;
+    std::string err = ParseParticleRestart(sections[k], s, nsec);
+    if (!err.empty()) return "restart: section " + std::to_string(k) + ": " + err;
+    if (k == 0) {
+      out.version = s.version; out.ranks = s.ranks; out.nrdata = s.nrdata;
+      out.nidata = s.nidata; out.dtnew = s.dtnew;
+      out.state = s.state;
+      out.notes = s.notes;
+    }
+    const std::size_t n = (std::size_t)s.np;
+    for (std::size_t p = 0; p < n; ++p) {
+      if (!mine(s.pi[p])) continue;   // PGID is row 0 of the integers
+      for (int c = 0; c < kNReal; ++c) rc[c].push_back(s.pr[(std::size_t)c * n + p]);
+      for (int c = 0; c < kNInt; ++c) ic[c].push_back(s.pi[(std::size_t)c * n + p]);
+    }
+  }
+  const std::size_t np = rc[0].size();
+  out.np = static_cast<std::int64_t>(np);
+  out.pr.resize(np * kNReal);
+  out.pi.resize(np * kNInt);
+  for (int c = 0; c < kNReal; ++c)
+    std::copy(rc[c].begin(), rc[c].end(), out.pr.begin() + (std::ptrdiff_t)(c * np));
+  for (int c = 0; c < kNInt; ++c)
+    std::copy(ic[c].begin(), ic[c].end(), out.pi.begin() + (std::ptrdiff_t)(c * np));
+  // the sections' tag counters were per rank: the counter starts again; the cell-order index
+  // of another layout is rebuilt
+  out.state.next_tag_set = false;
+  out.state.next_tag = 0;
+  out.state.cloud_ord_status = 0;
+  out.state.cloud_ord.clear();
+  out.state.cloud_ord_tag.clear();
   return "";
 }
 

@@ -15,6 +15,7 @@
 #ifndef ATHENAK_B200_RESTART_HPP_
 #define ATHENAK_B200_RESTART_HPP_
 
+#include <cstddef>
 #include <cstdint>
 #include <string>
 #include <utility>
@@ -28,8 +29,11 @@ struct ParticleRestartState {
   // tag_state: {counter set, next tag of this rank, bound above every tag issued}
   bool next_tag_set = false;
   std::uint64_t next_tag = 0, tag_bound = 0;
-  // rank_blocks: {rank, first gid, blocks}
+  // rank_blocks: {rank, first gid, blocks} (rank_blocks_read: the record was in the section)
   std::int32_t rank = 0, gids = 0, nmb = 0;
+  bool rank_blocks_read = false;
+  // the head's "ranks written": the number of sections of the file, one per writing rank
+  std::int32_t nranks = 1;
   std::int32_t merge_pass = 0;
   std::string species_table;              // the resolved species table, ASCII lines
   std::vector<double> mroot, imex_mown;   // written when not empty
@@ -77,8 +81,35 @@ struct ParticleRestartSection {
   std::vector<std::string> notes;   // unknown records, missing species table
 };
 
-// checks the section (magic at both ends, version, type sizes, columns, sizes) and parses it
-std::string ParseParticleRestart(const std::vector<char> &buf, ParticleRestartSection &out);
+// checks the section (magic at both ends, version, type sizes, a rank count of nsec, columns,
+// sizes) and parses it (ParseSection + UnpackRestartState, src/dust/dust_restart.cpp)
+std::string ParseParticleRestart(const std::vector<char> &buf, ParticleRestartSection &out,
+                                 int nsec = 1);
+
+// The particle sections of a restart file: a run on several ranks appends one section per
+// rank, in rank order, each with "ranks written" in its head.  Splits file[at, end) into them
+// by the byte count of each head (magic and size checked; the restart reader's section
+// offsets, src/gravity/restart.cpp).
+std::string SplitParticleRestart(const std::vector<char> &file, std::size_t at,
+                                 std::vector<std::vector<char>> &sections);
+
+// Whether rank `me` of a run on `nranks` ranks, holding blocks [gids, gids + nmb), can take
+// its own section back exactly (UnpackParticleRestart, src/dust/dust_restart.cpp): as many
+// sections as ranks and, with more than one, the section's rank_blocks record names this rank
+// and these blocks.  A run on several ranks takes the exact path only when every rank's
+// answer is yes (the reference reduces it with a logical and over the ranks).
+std::string ParticleRestartOwnSectionMatches(const std::vector<std::vector<char>> &sections,
+                                             int me, int nranks, int gids, int nmb,
+                                             bool &match);
+
+// The particles (and dust records) of rank `me`: exact (all ranks matched) -- its own
+// section as written, every particle's PGID within its blocks (else an error: a particle
+// names a MeshBlock that does not exist); otherwise the particles of its blocks from every
+// section in section order, the records and dtnew of section 0, the tag counter unset (it
+// starts again at the bound of all tags issued) and the cloud order index dropped (another
+// layout: it is rebuilt).
+std::string SelectParticleRestart(const std::vector<std::vector<char>> &sections, int me,
+                                  int gids, int nmb, bool exact, ParticleRestartSection &out);
 
 // the parsed rows into the device arrays of ctx (npart set to the section's; the capacity
 // ctx.part.stride must hold them); synchronises

@@ -5,6 +5,10 @@
 //                              bit for bit), a version-1 section built here byte by byte and
 //                              parsed (the high tag words 0, the int32 counter), and damaged
 //                              sections rejected; writes <dir>/host.rst and <dir>/host.rows
+//   restart_tool ranks <dir>   a file of two ranks' sections: split, each rank's own section
+//                              taken back exactly, the particles of other block layouts
+//                              gathered from every section, damaged files rejected; writes
+//                              <dir>/ranks.rst (the two sections)
 //   restart_tool device <dir>  rows seeded on the GPU, packed from the device, restored into
 //                              arrays of another capacity and compared bit for bit
 //
@@ -212,14 +216,123 @@ int device_checks() {
   return bad;
 }
 
+// the rows of one writing rank: n particles of blocks [gids, gids + nmb), tags from tag0
+void rank_rows(int n, int gids, int nmb, int tag0, std::vector<double> &pr, std::vector<int> &pi) {
+  make_rows(n, n, pr, pi);
+  for (int p = 0; p < n; ++p) {
+    pi[p] = gids + (p * 7) % nmb;
+    pi[(std::size_t)1 * n + p] = tag0 + p;
+    pr[p] += 100.0 * gids;                   // rows told apart by rank
+  }
+}
+
+// one particle of a parsed section (rows r * np + p) against one of the writer's rows
+bool same_particle(const ParticleRestartSection &s, std::int64_t p, const std::vector<double> &pr,
+                   const std::vector<int> &pi, int n, int q) {
+  bool ok = true;
+  for (int r = 0; r < 17; ++r) ok = ok && s.pr[(std::size_t)r * s.np + p] == pr[(std::size_t)r * n + q];
+  for (int r = 0; r < 5; ++r) ok = ok && s.pi[(std::size_t)r * s.np + p] == pi[(std::size_t)r * n + q];
+  return ok;
+}
+
+// a file of two sections (ranks 0 and 1 of a run on two ranks, blocks [0, 4) and [4, 8)) after
+// other bytes; read back on two ranks with the same blocks (each its own section exactly), on
+// one rank (every particle, the records of section 0, a new tag counter, no cloud order), on
+// two ranks with other blocks (the particles of each rank's blocks from both sections, in
+// section order); damaged files and a rank count that does not match rejected
+int rank_checks(const std::string &dir) {
+  const int n0 = 10, n1 = 7;
+  std::vector<double> pr0, pr1;
+  std::vector<int> pi0, pi1;
+  rank_rows(n0, 0, 4, 1000, pr0, pi0);
+  rank_rows(n1, 4, 4, 2000, pr1, pi1);
+  ParticleRestartState s0 = make_state(), s1 = make_state();
+  s0.nranks = s1.nranks = 2;
+  s0.rank = 0; s0.gids = 0; s0.nmb = 4; s0.next_tag = 1010; s0.merge_pass = 3;
+  s1.rank = 1; s1.gids = 4; s1.nmb = 4; s1.next_tag = 2007; s1.merge_pass = 5;
+  std::vector<char> b0, b1, file(100, 'm');   // (the mesh data before the sections)
+  std::string err = athenak_b200::PackParticleRestartRows(pr0.data(), pi0.data(), n0, n0, 0.25, s0, b0);
+  err += athenak_b200::PackParticleRestartRows(pr1.data(), pi1.data(), n1, n1, 0.5, s1, b1);
+  check(err.empty(), "two ranks' sections packed");
+  file.insert(file.end(), b0.begin(), b0.end());
+  file.insert(file.end(), b1.begin(), b1.end());
+  std::vector<std::vector<char>> secs;
+  err = athenak_b200::SplitParticleRestart(file, 100, secs);
+  check(err.empty() && secs.size() == 2 && secs[0] == b0 && secs[1] == b1, "file split into its sections");
+  ParticleRestartSection one;
+  check(!athenak_b200::ParseParticleRestart(secs[0], one).empty() &&
+        athenak_b200::ParseParticleRestart(secs[0], one, 2).empty() && one.state.nranks == 2,
+        "a section's rank count is checked");
+  // two ranks, the writer's blocks: exact
+  bool m0 = false, m1 = false;
+  err = athenak_b200::ParticleRestartOwnSectionMatches(secs, 0, 2, 0, 4, m0);
+  err += athenak_b200::ParticleRestartOwnSectionMatches(secs, 1, 2, 4, 4, m1);
+  check(err.empty() && m0 && m1, "own sections match on the writer's layout");
+  ParticleRestartSection e0, e1;
+  err = athenak_b200::SelectParticleRestart(secs, 0, 0, 4, true, e0);
+  err += athenak_b200::SelectParticleRestart(secs, 1, 4, 4, true, e1);
+  bool ok = err.empty() && e0.np == n0 && e1.np == n1 && e0.dtnew == 0.25 && e1.dtnew == 0.5 &&
+            e0.state.next_tag == 1010 && e1.state.next_tag == 2007 && e1.state.merge_pass == 5 &&
+            e1.state.cloud_ord == s1.cloud_ord;
+  for (int p = 0; p < n0 && ok; ++p) ok = same_particle(e0, p, pr0, pi0, n0, p);
+  for (int p = 0; p < n1 && ok; ++p) ok = same_particle(e1, p, pr1, pi1, n1, p);
+  check(ok, "exact: each rank its own section, rows and records bit for bit");
+  // one rank: no match (two sections), everything gathered
+  bool m = true;
+  err = athenak_b200::ParticleRestartOwnSectionMatches(secs, 0, 1, 0, 8, m);
+  ParticleRestartSection all;
+  err += athenak_b200::SelectParticleRestart(secs, 0, 0, 8, m, all);
+  ok = err.empty() && !m && all.np == n0 + n1 && all.dtnew == 0.25 && all.state.merge_pass == 3 &&
+       !all.state.next_tag_set && all.state.next_tag == 0 && all.state.cloud_ord.empty() &&
+       all.state.cloud_ord_tag.empty() && all.state.cloud_ord_status == 0;
+  for (int p = 0; p < n0 && ok; ++p) ok = same_particle(all, p, pr0, pi0, n0, p);
+  for (int p = 0; p < n1 && ok; ++p) ok = same_particle(all, n0 + p, pr1, pi1, n1, p);
+  check(ok, "one rank: every particle in section order, section 0's records, tag counter anew");
+  // two ranks, blocks [0, 3) and [3, 8): no match, each rank its blocks from both sections
+  err = athenak_b200::ParticleRestartOwnSectionMatches(secs, 0, 2, 0, 3, m0);
+  err += athenak_b200::ParticleRestartOwnSectionMatches(secs, 1, 2, 3, 5, m1);
+  ParticleRestartSection g0, g1;
+  err += athenak_b200::SelectParticleRestart(secs, 0, 0, 3, m0 && m1, g0);
+  err += athenak_b200::SelectParticleRestart(secs, 1, 3, 5, m0 && m1, g1);
+  std::vector<std::pair<int, int>> want0, want1;   // (section, particle)
+  for (int p = 0; p < n0; ++p) (pi0[p] < 3 ? want0 : want1).emplace_back(0, p);
+  for (int p = 0; p < n1; ++p) (pi1[p] < 3 ? want0 : want1).emplace_back(1, p);
+  ok = err.empty() && !m0 && !m1 && g0.np == (std::int64_t)want0.size() &&
+       g1.np == (std::int64_t)want1.size() && g1.state.merge_pass == 3 && !g1.state.next_tag_set;
+  for (std::size_t q = 0; q < want0.size() && ok; ++q)
+    ok = want0[q].first == 0 ? same_particle(g0, q, pr0, pi0, n0, want0[q].second)
+                             : same_particle(g0, q, pr1, pi1, n1, want0[q].second);
+  for (std::size_t q = 0; q < want1.size() && ok; ++q)
+    ok = want1[q].first == 0 ? same_particle(g1, q, pr0, pi0, n0, want1[q].second)
+                             : same_particle(g1, q, pr1, pi1, n1, want1[q].second);
+  check(ok && !want0.empty() && !want1.empty(), "other blocks: each rank's particles from both sections");
+  // a particle outside the blocks on the exact path, a truncated file, a section too many
+  std::vector<char> bad0;
+  pi0[3] = 6;
+  athenak_b200::PackParticleRestartRows(pr0.data(), pi0.data(), n0, n0, 0.25, s0, bad0);
+  std::vector<std::vector<char>> badsecs = {bad0, b1};
+  ParticleRestartSection x;
+  check(!athenak_b200::SelectParticleRestart(badsecs, 0, 0, 4, true, x).empty(),
+        "exact: a particle of another block rejected");
+  std::vector<char> cut(file.begin(), file.end() - 9);
+  std::vector<std::vector<char>> cs;
+  check(!athenak_b200::SplitParticleRestart(cut, 100, cs).empty(), "truncated file rejected");
+  std::vector<std::vector<char>> three = {b0, b1, b1};
+  ParticleRestartSection y;
+  check(!athenak_b200::SelectParticleRestart(three, 0, 0, 8, false, y).empty(),
+        "sections whose rank count is not their number rejected");
+  return write_file(dir + "/ranks.rst", file.data() + 100, file.size() - 100) ? bad : bad + 1;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
   if (argc < 3) {
-    std::printf("usage: restart_tool host|device <dir>\n");
+    std::printf("usage: restart_tool host|ranks|device <dir>\n");
     return 2;
   }
   const std::string mode = argv[1];
-  const int b = (mode == "host") ? host_checks(argv[2]) : device_checks();
+  const int b = (mode == "host") ? host_checks(argv[2])
+              : (mode == "ranks") ? rank_checks(argv[2]) : device_checks();
   return b ? 1 : 0;
 }

@@ -85,6 +85,28 @@ def test_host_sections(tmp_path):
     np.testing.assert_array_equal(pi, rpi[:, :n])
 
 
+def test_rank_sections(tmp_path):
+    """A run on several ranks appends one section per rank in rank order (src/dust/
+    dust_restart.cpp): the tool's checks (split, exact own sections, other block layouts
+    gathered from every section, damaged files rejected), and the file read here: two
+    sections, each with ranks written = 2 in its head and its own rank_blocks record."""
+    exe = build_tool()
+    r = subprocess.run([exe, "ranks", str(tmp_path)], capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.count(": ok") == 10
+    raw = (tmp_path / "ranks.rst").read_bytes()
+    total0 = int(np.frombuffer(raw[32:40], "<u8")[0])
+    blocks = []
+    for sec, n in ((raw[:total0], 10), (raw[total0:], 7)):
+        head, np_, dtnew, recs, pr, pi = read_section(sec)
+        assert list(head) == [2, 8, 4, 2, 17, 5] and np_ == n
+        blocks.append(list(np.frombuffer(dict(recs)["rank_blocks"], "<i4")))
+        lo, nb = blocks[-1][1], blocks[-1][2]
+        assert np.all((pi[0] >= lo) & (pi[0] < lo + nb))
+    assert blocks == [[0, 0, 4], [1, 4, 4]]
+
+
 @pytest.mark.gpu
 def test_device_round_trip(tmp_path):
     exe = build_tool()
