@@ -170,7 +170,8 @@ def timed_cycles(fn, steps, stream):
 def cpu_baseline(threads=None, cycles=2):
     """The oracle port (OpenMP, atomics: the reference's Kokkos OpenMP form) on a bounded
     sample of the workload: one 32^3 MeshBlock (periodic onto itself) with the same species
-    and ppc 16, one warm-up cycle and `cycles` timed cycles."""
+    and ppc 16, the rows put in cell order (the oracle's SortParticles), one warm-up cycle and
+    `cycles` timed cycles."""
     import numpy as np
     from athenak_b200.inputs import make_state
     from athenak_b200.mesh import uniform_mesh
@@ -182,6 +183,7 @@ def cpu_baseline(threads=None, cycles=2):
     st = make_state(ms, taus, [0.5] * 4, 4, seed=1, shearing_box=True, vel_noise=1e-3,
                     gas_noise=1e-3)
     o = Oracle(st, dict(scheme=2, drag_solver=2), threads=threads)
+    o.sort_particles()                        # the rows in cell order, as the GPU arms
     dx = L / 32
     dt = 0.3 * dx / 1.05
     o.imex_cycle(dt)
@@ -190,8 +192,9 @@ def cpu_baseline(threads=None, cycles=2):
         o.imex_cycle(dt)
     el = time.perf_counter() - t
     return {"value": st.npart * cycles / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"32^3 cells, 1 MeshBlock periodic, 4 species ppc 16 ({st.npart} particles), "
-                      f"{cycles} imex2+/dc1 cycles after 1 warm-up, FP64, OpenMP atomics"}
+            "sample": f"32^3 cells, 1 MeshBlock periodic, 4 species ppc 16 ({st.npart} particles, "
+                      f"in cell order), {cycles} imex2+/dc1 cycles after 1 warm-up, FP64, "
+                      f"OpenMP atomics"}
 
 
 def run_reference(args, rank, world):
