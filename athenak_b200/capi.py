@@ -163,6 +163,7 @@ SIGNATURES = {
     "dustb_pc2_cycle": [CTXP, D, VP, VP, VP],
     "dustb_seed_uniform": [CTXP, C.POINTER(DustbSeedDesc), VP],
     "dustb_cell_index_static": [CTXP, VP, VP, VP],
+    "dustb_cell_index_static_reset": [],
     "dustb_phst_scratch_bytes": [MESHP, I],
     "dustb_phst": [CTXP, VP, VP, VP, LL, VP],
     "dustb_cloud_order": [CTXP, VP, VP, VP, LL, VP],

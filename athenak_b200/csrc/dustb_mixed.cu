@@ -1698,7 +1698,7 @@ int push_sort(const MState &S, const PBuf &src, const PBuf &dst, const Geo &G, i
               long long ncell, const PushArgs &P, cudaStream_t st) {
   int rc;
   {
-    Scope sc(DUSTB_K_PUSH, st);
+    Scope sc(DUSTB_K_COUNT, st);
     cudaMemsetAsync(S.cstart, 0, 4 * (size_t)nbins(ncell), st);
     if (n > 0) {
 #define DUSTB_COUNT(K, SPF) k_count<K, SPF><<<nblk(n), kT, 0, st>>>(src, S.key, S.cstart, G, n, P)
@@ -1720,7 +1720,7 @@ int push_sort(const MState &S, const PBuf &src, const PBuf &dst, const Geo &G, i
     if ((rc = exclusive_scan(S.cstart, nbins(ncell), S.bsum, st))) return rc;
     cudaMemcpyAsync(S.cursor, S.cstart, 4 * (size_t)nbins(ncell), cudaMemcpyDeviceToDevice, st);
   }
-  Scope sc(DUSTB_K_PUSH, st);
+  Scope sc(DUSTB_K_MOVE, st);
   if (n > 0) {
 #define DUSTB_MOVE(K, SPF) k_move<K, SPF><<<nblk(n), kT, 0, st>>>(src, dst, S.key, S.cursor, G, n, P)
     if (G.ghost) {

@@ -7,6 +7,7 @@
 // Steps: key + histogram (atomics on the cell counters), exclusive scan of the counters,
 // scatter of the particle indices with per-cell cursors, per-cell sort of the (short)
 // index runs.  Every result is deterministic.
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 
@@ -379,8 +380,11 @@ namespace {
 constexpr int kMaxDevices = 64;
 // the array's device address on each device.  The name g_cell_index_scratch in host code is
 // only a host-side handle, so the address is asked from the runtime, once per device, with
-// that device current.
-void *g_cell_index_scratch_ptr[kMaxDevices] = {nullptr};
+// that device current.  Atomic slots: host threads making their first call on one device at
+// the same time may both look the address up (the same value) and store it without a race.
+// A cudaDeviceReset unloads the module, so the cached address is stale after it:
+// dustb_cell_index_static_reset() clears the slots for such a caller.
+std::atomic<void *> g_cell_index_scratch_ptr[kMaxDevices];
 }  // namespace
 
 extern "C" int dustb_cell_index_static(const dustb_ctx *c, int *order, int *cstart,
@@ -403,19 +407,29 @@ extern "C" int dustb_cell_index_static(const dustb_ctx *c, int *order, int *csta
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) { dustb_host::set_error("dustb_cell_index_static: cudaGetDevice", e); return DUSTB_ELAUNCH; }
-  if (dev < 0 || dev >= kMaxDevices) return DUSTB_EUNSUP;
-  if (!g_cell_index_scratch_ptr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_cell_index_scratch);
-    if (e != cudaSuccess || !p) {
+  if (dev < 0 || dev >= kMaxDevices) {
+    char msg[128];
+    snprintf(msg, sizeof(msg), "dustb_cell_index_static: device ordinal %d is not below the %d "
+             "devices the address cache holds", dev, kMaxDevices);
+    dustb_host::set_message(msg);
+    return DUSTB_EUNSUP;
+  }
+  void *ptr = g_cell_index_scratch_ptr[dev].load(std::memory_order_acquire);
+  if (!ptr) {
+    e = cudaGetSymbolAddress(&ptr, g_cell_index_scratch);
+    if (e != cudaSuccess || !ptr) {
       dustb_host::set_error("dustb_cell_index_static: cudaGetSymbolAddress", e);
       return DUSTB_ELAUNCH;
     }
-    g_cell_index_scratch_ptr[dev] = p;
+    g_cell_index_scratch_ptr[dev].store(ptr, std::memory_order_release);
   }
   // nothing in the array needs to start at zero: the keys, the cursors and the scan sums are
   // all written before they are read, and the per-cell counts are kept in the caller's
   // cstart, which dustb_cell_index clears
-  return dustb_cell_index(c, order, cstart, g_cell_index_scratch_ptr[dev],
-                          (long long)DUSTB_STATIC_SCRATCH_BYTES, stream);
+  return dustb_cell_index(c, order, cstart, ptr, (long long)DUSTB_STATIC_SCRATCH_BYTES, stream);
+}
+
+extern "C" int dustb_cell_index_static_reset(void) {
+  for (int d = 0; d < kMaxDevices; ++d) g_cell_index_scratch_ptr[d].store(nullptr);
+  return DUSTB_OK;
 }

@@ -14,7 +14,7 @@ import torch
 from . import capi
 from .drag import DeviceDust, GAMMA_DEFAULT, _stream_ptr
 
-KERNELS = ["push", "fill", "deposit_qp", "operator", "kick", "consistent", "cells"]
+KERNELS = ["count", "fill", "deposit_qp", "operator", "kick", "consistent", "cells", "move"]
 
 
 class DustbMixedParams(C.Structure):
@@ -134,10 +134,11 @@ class MixedDust:
         self.lib.dustb_mixed_timing(1 if on else 0)
 
     def kernel_times(self):
-        ms = (C.c_double * 7)()
-        n = (C.c_int * 7)()
-        self.lib.dustb_mixed_kernel_times(C.cast(ms, C.c_void_p), C.cast(n, C.c_void_p), 7)
-        return {KERNELS[k]: (ms[k], n[k]) for k in range(7)}
+        nk = len(KERNELS)
+        ms = (C.c_double * nk)()
+        n = (C.c_int * nk)()
+        self.lib.dustb_mixed_kernel_times(C.cast(ms, C.c_void_p), C.cast(n, C.c_void_p), nk)
+        return {KERNELS[k]: (ms[k], n[k]) for k in range(nk)}
 
     # ---- host views ----
     def export_velocities(self):

@@ -25,7 +25,10 @@
  * never trap: a violated invariant ORs a DUSTB_ERR_* bit into *ctx->err (device uint32) and
  * the offending particle is skipped, where the reference calls Kokkos::abort.
  *
- * No entry point allocates memory: scratch is passed by the caller (dustb_*_bytes).
+ * No entry point allocates memory: scratch is passed by the caller (dustb_*_bytes).  The one
+ * exception is dustb_cell_index_static, whose scratch is a fixed device array of the library
+ * (DUSTB_STATIC_SCRATCH_BYTES on every GPU that loads it); its calls must not overlap on the
+ * GPU.
  */
 #ifndef DUSTB_H_
 #define DUSTB_H_
@@ -60,7 +63,12 @@ enum { DUSTB_X3_PERIODIC = 0, DUSTB_X3_REFLECT = 1, DUSTB_X3_OUTFLOW = 2 };
 #define DUSTB_ERR_PGID      0x8u  /* PGID outside the pack */
 #define DUSTB_ERR_TSTOP     0x10u /* stopping time not finite and positive (dust_newdt.cpp:53) */
 #define DUSTB_ERR_WINDOW    0x20u /* fused kernels: a particle outside its tile window */
-#define DUSTB_ERR_TIMEOUT   0x40u /* a bounded wait on an asynchronous copy ran out */
+#define DUSTB_ERR_TIMEOUT   0x40u /* a bounded wait on an asynchronous copy ran out.  The CTA
+                                   * that gave up may leave a copy in flight into shared memory
+                                   * that a later CTA on the same SM then uses: every output of
+                                   * that launch and of the launches after it on the stream is
+                                   * untrusted, and the host must discard the step (restore the
+                                   * last good state) rather than continue from it */
 #define DUSTB_ERR_POINT     0x80u /* point-particle fields: invalid mass, owner, position or
                                    * TSC support (dust_gravity_points.cpp:29-33) */
 #define DUSTB_ERR_CLOUD     0x100u /* refinable clouds: a cloud code with lobe bits (transition
@@ -241,8 +249,13 @@ int dustb_sort_by_cell(const dustb_ctx *ctx, double *spare_pr, int *spare_pi, vo
  *  - Every call shares the one array: calls that may overlap on the GPU (on different
  *    streams without ordering between them) race and must not be issued.  Nothing in the
  *    array needs to start at zero; each call writes what it reads.
- *  - It calls no cudaMalloc, cudaFree or allocating library routine. */
+ *  - It calls no cudaMalloc, cudaFree or allocating library routine.
+ *  - The looked-up address does not survive cudaDeviceReset (which unloads the module): a
+ *    caller that resets a device calls dustb_cell_index_static_reset() before its next call. */
 int dustb_cell_index_static(const dustb_ctx *ctx, int *order, int *cstart, void *stream);
+/* Forgets the device addresses dustb_cell_index_static looked up (after a cudaDeviceReset);
+ * the next call on each device looks its address up again.  Not while calls are running. */
+int dustb_cell_index_static_reset(void);
 
 /* ---- the cloud order index (DustGasDrag::UpdateCloudOrder, src/dust/dust_cloud_device.cpp:
  * 1992-2055; the identity after a sort, :1956-1975) -------------------------------------
@@ -490,9 +503,13 @@ int dustb_mixed_sort(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *w
 
 /* Kernel timing of the mixed cycle: when enabled, the library records CUDA events around
  * every fused kernel it launches; dustb_mixed_kernel_times sums their durations (ms) and
- * launch counts per kernel id since the last reset (it synchronises the events). */
-enum { DUSTB_K_PUSH = 0, DUSTB_K_FILL = 1, DUSTB_K_DEPOSIT_QP = 2, DUSTB_K_OPERATOR = 3,
-       DUSTB_K_KICK = 4, DUSTB_K_CONSISTENT = 5, DUSTB_K_CELLS = 6, DUSTB_K_NKERNELS = 7 };
+ * launch counts per kernel id since the last reset (it synchronises the events).  The push
+ * is two kernels: DUSTB_K_COUNT (the new cells and their histogram) and DUSTB_K_MOVE (the
+ * push written to each particle's slot); DUSTB_K_CELLS holds the FP64 per-cell kernels and
+ * exchanges, DUSTB_K_FILL the scan of the histogram. */
+enum { DUSTB_K_COUNT = 0, DUSTB_K_FILL = 1, DUSTB_K_DEPOSIT_QP = 2, DUSTB_K_OPERATOR = 3,
+       DUSTB_K_KICK = 4, DUSTB_K_CONSISTENT = 5, DUSTB_K_CELLS = 6, DUSTB_K_MOVE = 7,
+       DUSTB_K_NKERNELS = 8 };
 int dustb_mixed_timing(int enable);
 int dustb_mixed_kernel_times(double *ms, int *launches, int n);
 
