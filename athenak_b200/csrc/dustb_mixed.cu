@@ -87,7 +87,15 @@ struct MState {
   PBuf A, B;                     // A holds the shadow between cycles
   int *key;                      // new cell of each particle (count -> move)
   int *cstart, *cursor, *bsum;
+  float4 *win;                   // 3-D: the gather window (k_gather_window)
 };
+
+// cells of the gather window of a 3-D mesh: every block's active cells and one layer around
+// them, (nx1 + 2)(nx2 + 2)(nx3 + 2) per block; 0 in 2-D (the 2-D tiles read the FP64 field)
+long long nwin(const dustb_mesh &ms) {
+  if (!ms.three_d) return 0;
+  return (long long)ms.nmb * (ms.nx1 + 2) * (ms.nx2 + 2) * (ms.nx3 + 2);
+}
 
 struct Geo {
   int nmb, nx1, nx2, nx3, three_d, gids;
@@ -109,6 +117,7 @@ struct Geo {
   double mx1min, mx1max, mx2min, mx3min, mly, mlz;   // mesh x1 range, lower y, z, y, z extents
   double shR;                  // fmod(q Omega Lx t, Ly) in cells of y
   int ncell;                   // active cells; key ncell = the edge bin (pc2 half step)
+  int W1, W2, W3;              // 3-D: the gather window's cells per row, rows, planes of a block
   __device__ long long at(int m, int nvar, int v, int k, int j, int i) const {
     return (((long long)m * nvar + v) * vstride) + ((long long)k * n2 + j) * n1 + i;
   }
@@ -143,6 +152,7 @@ bool carve(const dustb_mesh &ms, int n, void *ws, long long bytes, MState &S, lo
   const size_t o_cs = off; off += al256(4 * (size_t)(ncell + 2));
   const size_t o_cur = off; off += al256(4 * (size_t)(ncell + 2));
   const size_t o_bs = off; off += al256(4 * (size_t)scan_bsum_ints(ncell + 2));
+  const size_t o_win = off; off += al256(16 * (size_t)nwin(ms));
   if (need) *need = (long long)off;
   if (!ws || bytes < (long long)off) return false;
   char *b = (char *)ws;
@@ -155,6 +165,7 @@ bool carve(const dustb_mesh &ms, int n, void *ws, long long bytes, MState &S, lo
   S.head = (MHead *)b;
   S.key = (int *)(b + o_key);
   S.cstart = (int *)(b + o_cs); S.cursor = (int *)(b + o_cur); S.bsum = (int *)(b + o_bs);
+  S.win = (float4 *)(b + o_win);
   return true;
 }
 
@@ -187,6 +198,7 @@ Geo make_geo(const dustb_ctx *c, const dustb_mixed_params *mp) {
     G.shR = ysh * (double)((long long)ms.sb_nb2 * ms.nx2) / G.mly;
   }
   G.ncell = (int)ncell_of(ms);
+  G.W1 = G.nx1 + 2; G.W2 = G.nx2 + 2; G.W3 = G.nx3 + 2;
   return G;
 }
 
@@ -806,6 +818,7 @@ struct TileArgs {
   double a_dt;
   const int *cstart;           // cell -> particle ranges of the sorted shadow
   const double *gfield;        // gather field (3 vars): operator, kick, predictor, advance
+  const float4 *win4;          // 3-D: the gather field's window (k_gather_window)
   double *dfield;              // deposit field (the predictor: qdep's variable 1)
   int dnvar;
   double *res;                 // MODE_QP: resid, the centre mass goes to var 3
@@ -835,6 +848,30 @@ __device__ __forceinline__ long long cell_at(const Geo &G, int m, int nvar, int 
   return G.at(mo, nvar, 0, G.ks + kk, G.js + jj, G.is + ii);
 }
 __device__ __forceinline__ float2 dup(float x) { return make_float2(x, x); }
+
+// The 3-D tiles' gather window: the gather field (3 FP64 variables) on every block's active
+// cells and one layer of cells around them, rounded to FP32 (x, y, z, 0) per cell, cell
+// (k, j, i) at window index (k + 1, j + 1, i + 1).  GH = 1: the cells around a block are its
+// own ghost cells (the FP64 copy exchange fills them); GH = 0: the owning neighbour's active
+// cells (the exchange folded into the read).  Written once per gather, it replaces the 27
+// owner lookups and 81 FP64 loads each tile thread made per cell.
+template <int GH>
+__global__ void __launch_bounds__(256) k_gather_window(const double *f, float4 *win, Geo G) {
+  const long long total = (long long)G.W1 * G.W2 * G.W3 * G.nmb;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    long long r = idx;
+    const int ii = (int)(r % G.W1); r /= G.W1;
+    const int jj = (int)(r % G.W2); r /= G.W2;
+    const int kk = (int)(r % G.W3);
+    const int m = (int)(r / G.W3);
+    const long long at = cell_at<GH>(G, m, 3, kk - 1, jj - 1, ii - 1);
+    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (at >= 0)
+      v = make_float4((float)f[at], (float)f[at + G.vstride], (float)f[at + 2 * G.vstride], 0.0f);
+    win[idx] = v;
+  }
+}
 
 // the 27-point sums of one source cell's particles: values 0, 1 as a packed pair; values 2, 3
 // as a pair (Q/P) or value 2 alone (operator, kick)
@@ -922,6 +959,23 @@ struct GatherWindow {
           }
         }
       }
+  }
+  // 3-D: the 27 cells from the gather window (cell + 1 in each direction: the stencil's
+  // lowest cell, one below, is window index k, jrow, ci); consecutive threads read
+  // consecutive cells, so every load of a warp is one coalesced 16-byte-per-lane access
+  __device__ __forceinline__ void load4(const Geo &G, const float4 *W, int m, int k, int jrow,
+                                        int ci) {
+    const float4 *p = W + (((long long)m * G.W3 + k) * G.W2 + jrow) * G.W1 + ci;
+#pragma unroll
+    for (int c = 0; c < WK; ++c)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float4 v = __ldg(p + ((long long)c * G.W2 + b) * G.W1 + a);
+          xy[c][b][a] = make_float2(v.x, v.y);
+          z[c][b][a] = v.z;
+        }
   }
   // u = sum over (c, b) of wz_c wy_b (sum over a of wx_a g_cba)
   __device__ __forceinline__ void gather(const float wx[3], const float wy[3], const float wz[3],
@@ -1205,7 +1259,10 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       return (GH & 2) ? shifted_oy(G, T.shy, m, ci_l, s_f[r], s_f[CH + r]) : s_f[CH + r];
     };
     GatherWindow<D3> win;
-    if (MODE != MODE_QP) win.template load<GH>(G, T.gfield, m, k, jrow, ci_l);   // while the copies fly
+    if constexpr (MODE != MODE_QP) {                 // (the loads fly with the copies)
+      if constexpr (D3) win.load4(G, T.win4, m, k, jrow, ci_l);
+      else win.template load<GH>(G, T.gfield, m, k, jrow, ci_l);
+    }
     const bool ok = mbar_wait(&bar, parity, T.err, wmask);
     parity ^= 1u;
     if (__syncthreads_or(!ok)) {
@@ -1641,6 +1698,20 @@ int launch_shift_edge(const MState &S, const PBuf &cur, const Geo &G, TileArgs T
   return dustb_host::launch_status("mixed shear-shift edge");
 }
 
+// the gather window of a 3-D mesh from the FP64 gather field f (after its ghost exchange in
+// ghost mode); nothing in 2-D
+int gather_window(const MState &S, const Geo &G, const dustb_mesh &ms, const double *f,
+                  TileArgs &T, cudaStream_t st) {
+  T.win4 = S.win;
+  if (!ms.three_d) return DUSTB_OK;
+  Scope sc(DUSTB_K_WINDOW, st);
+  const long long n = nwin(ms);
+  const unsigned nb = (unsigned)((n + 255) / 256 < 148LL * 16 ? (n + 255) / 256 : 148LL * 16);
+  if (G.ghost) k_gather_window<1><<<nb, 256, 0, st>>>(f, S.win, G);
+  else k_gather_window<0><<<nb, 256, 0, st>>>(f, S.win, G);
+  return dustb_host::launch_status("mixed gather window");
+}
+
 // sort copy src into dst by the cells it holds (histogram, scan, moves)
 int sort_into(const MState &S, const PBuf &src, const PBuf &dst, const dustb_mesh &ms, int n,
               cudaStream_t st) {
@@ -1899,6 +1970,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
         { Scope sc(DUSTB_K_CELLS, st);
           RUN(ghost_copy_if(c, G, c->f.ustar, st)); }
         cudaMemsetAsync(c->f.work, 0, fbytes * 3, st);
+        RUN(gather_window(S, G, c->mesh, c->f.ustar, T, st));
         { Scope sc(DUSTB_K_OPERATOR, st);
           T.gfield = c->f.ustar; T.dfield = c->f.work; T.dnvar = 3;
           RUN(launch_tile<MODE_OP>(S, cur, G, cf, T, st));
@@ -1913,6 +1985,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       RUN(ghost_copy_if(c, G, c->f.ustar, st));
     }
     if (br) cudaMemsetAsync(c->f.dmom, 0, fbytes * 3, st);
+    RUN(gather_window(S, G, c->mesh, c->f.ustar, T, st));
     {
       Scope sc(DUSTB_K_KICK, st);
       T.gfield = c->f.ustar; T.dfield = c->f.dmom; T.dnvar = 3; T.deposit = br;
@@ -1973,6 +2046,7 @@ int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void
       k_gas_velocity<<<nblk(tot), kT, 0, st>>>(c->f.u1, c->f.nvar_gas, c->f.work, per, tot);
       RUN(dustb_host::launch_status("mixed gas velocity"));
     }
+    RUN(gather_window(S, G, c->mesh, c->f.work, T, st));
     {
       Scope sc(DUSTB_K_DEPOSIT_QP, st);
       cudaMemsetAsync(c->f.qdep, 0, fbytes * 5, st);
@@ -2004,6 +2078,7 @@ int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void
   P.x3rem = mp->x3_removed; P.err = c->err;
   RUN(push_sort(S, S.A, S.B, G, n, ncell, P, st));
   if (br) cudaMemsetAsync(c->f.dmom, 0, fbytes * 3, st);
+  RUN(gather_window(S, G, c->mesh, c->f.ustar, T, st));
   {
     Scope sc(DUSTB_K_KICK, st);
     T.gfield = c->f.ustar; T.dfield = c->f.dmom; T.dnvar = 3; T.deposit = br;

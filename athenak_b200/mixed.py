@@ -14,7 +14,8 @@ import torch
 from . import capi
 from .drag import DeviceDust, GAMMA_DEFAULT, _stream_ptr
 
-KERNELS = ["count", "fill", "deposit_qp", "operator", "kick", "consistent", "cells", "move"]
+KERNELS = ["count", "fill", "deposit_qp", "operator", "kick", "consistent", "cells", "move",
+           "window"]
 
 
 class DustbMixedParams(C.Structure):

@@ -47,7 +47,10 @@ GAMMA = 1.707106781186547
 #   operator: offsets, drag factor, mass in (20 B); u* in, work out (48 B per cell)
 #   kick:  offsets, drag factor, mass, velocity in, velocity and rate out (56 B); u* in, dmom
 #          out (48 B per cell)
+#   window: the FP64 u* of every active cell and of the one-cell layer around each block in,
+#          the FP32 window out: (24 + 16) B times (66/64)^3
 MIXED_BYTES = {
+    "window": (0.0, 44.0),
     "count": (46.0, 8.0),
     "move": (134.0, 0.0),
     "fill": (0.0, 16.0),

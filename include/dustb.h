@@ -506,10 +506,11 @@ int dustb_mixed_sort(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *w
  * launch counts per kernel id since the last reset (it synchronises the events).  The push
  * is two kernels: DUSTB_K_COUNT (the new cells and their histogram) and DUSTB_K_MOVE (the
  * push written to each particle's slot); DUSTB_K_CELLS holds the FP64 per-cell kernels and
- * exchanges, DUSTB_K_FILL the scan of the histogram. */
+ * exchanges, DUSTB_K_FILL the scan of the histogram, DUSTB_K_WINDOW the FP32 gather window
+ * of a 3-D mesh written before each gathering tile launch. */
 enum { DUSTB_K_COUNT = 0, DUSTB_K_FILL = 1, DUSTB_K_DEPOSIT_QP = 2, DUSTB_K_OPERATOR = 3,
        DUSTB_K_KICK = 4, DUSTB_K_CONSISTENT = 5, DUSTB_K_CELLS = 6, DUSTB_K_MOVE = 7,
-       DUSTB_K_NKERNELS = 8 };
+       DUSTB_K_WINDOW = 8, DUSTB_K_NKERNELS = 9 };
 int dustb_mixed_timing(int enable);
 int dustb_mixed_kernel_times(double *ms, int *launches, int n);
 
