@@ -1074,6 +1074,62 @@ __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, co
   }
 }
 
+// The window add of a 3-D tile in one pass whose threads are its cells (thread (cj, ci) holds
+// cell (cj, ci)'s staged sums): thread (cj, ci) adds the window cells of its own column ci --
+// target rows wy = cj + 1, and also row 0 (cj = 0) and row tj + 1 (cj = tj - 1) -- in the three
+// planes, each the sum of the up to 9 staged contributions of source rows wy - b and columns
+// ci + 1 - a; the threads of columns 0 and nx1 - 1 also add the halo columns x = -1 and x = nx1.
+// Every thread has a fixed set of targets (no index division), a warp's loads of one
+// contribution are consecutive in shared memory, and a target inside the block is indexed
+// directly (cell_at only beyond the block's faces).  One FP64 add per window cell and value,
+// as add_window.
+template <int MODE, int GH>
+__device__ __forceinline__ void add_window_cells(const float4 *s_acc, const Geo &G,
+                                                 const TileArgs &T, int m, int k, int j0, int tj,
+                                                 int cj, int ci) {
+  constexpr bool V4 = FourValues<MODE>::value;
+  const int nx1 = G.nx1, nct = tj * nx1;
+  auto put = [&](const float4 &v, int kt, int jt, int it) {
+    long long at;
+    if ((unsigned)kt < (unsigned)G.nx3 && (unsigned)jt < (unsigned)G.nx2 &&
+        (unsigned)it < (unsigned)nx1)
+      at = G.at(m, T.dnvar, 0, G.ks + kt, G.js + jt, G.is + it);
+    else
+      at = cell_at<GH>(G, m, T.dnvar, kt, jt, it);
+    if (at < 0) return;
+    double *f = T.dfield + at;
+    if (v.x != 0.0f) atomicAdd(f, (double)v.x);
+    if (v.y != 0.0f) atomicAdd(f + G.vstride, (double)v.y);
+    if (v.z != 0.0f) atomicAdd(f + 2 * G.vstride, (double)v.z);
+    if (V4 && v.w != 0.0f) atomicAdd(f + 3 * G.vstride, (double)v.w);
+  };
+  auto acc = [](float4 &s, const float4 &v) { s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w; };
+  const int wy_lo = (cj == 0) ? 0 : cj + 1, wy_hi = (cj == tj - 1) ? tj + 1 : cj + 1;
+  for (int wy = wy_lo; wy <= wy_hi; ++wy) {
+    const int jt = j0 - 1 + wy;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float4 sm = make_float4(0.0f, 0.0f, 0.0f, 0.0f), sl = sm, sr = sm;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const int sj = wy - b;
+        if (sj < 0 || sj >= tj) continue;
+        const float4 *row = s_acc + (size_t)((c * 3 + b) * 3) * nct + sj * nx1;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const int si = ci + 1 - a;
+          if (si >= 0 && si < nx1) acc(sm, row[(size_t)a * nct + si]);
+        }
+        if (ci == 0) acc(sl, row[ci]);                              // a = 0 -> x = -1
+        if (ci == nx1 - 1) acc(sr, row[(size_t)2 * nct + ci]);      // a = 2 -> x = nx1
+      }
+      put(sm, k - 1 + c, jt, ci);
+      if (ci == 0) put(sl, k - 1 + c, jt, -1);
+      if (ci == nx1 - 1) put(sr, k - 1 + c, jt, nx1);
+    }
+  }
+}
+
 // dust_pc2_advance (src/dust/dust_push.cpp:132-245) of one particle in FP32 from u* gathered
 // at its half-step gather position: the implicit midpoint velocity v_h (the 2x2 Coriolis solve
 // and the vertical gravity of the shearing box), v <- 2 v_h - v0, the displacement dt xdot_h
@@ -1292,7 +1348,8 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       if (!single && !split && s_ss[tid + 1] == s_ss[tid]) stage_zero<D3>(s_acc, tid, nct);
       if (cl >= 0) stage_sums<MODE, D3>(qp, s_acc, split ? tid : cl, nct);
       cta_sync(wmask);
-      add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
+      if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l);
+      else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
     } else {
       // gather phase: the operator's m c u / V, the kick's velocity change, the predictor's
       // impulse and rate, or the advance's u*, into rows 5..7 (and 3)
@@ -1395,7 +1452,8 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
         if (!single && !split && s_ss[tid + 1] == s_ss[tid]) stage_zero<D3>(s_acc, tid, nct);
         if (cl >= 0) stage_sums<MODE, D3>(sums, s_acc, split ? tid : cl, nct);
         cta_sync(wmask);
-        add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
+        if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l);
+        else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
       }
     }
     // the next pass's copies overwrite the rows (and its slots the slot starts)
