@@ -28,7 +28,7 @@ constexpr std::uint64_t kAlign = 64, kPreamble = 64, kFooter = 16;
 std::uint64_t Align(std::uint64_t a) { return a + (kAlign - a % kAlign) % kAlign; }
 
 struct Col {
-  std::string table, name, dtype, meaning;
+  std::string table, name, dtype;
   std::uint64_t itemsize = 0, count = 0, offset = 0, bytes = 0;
   int pcol = -1;                       // DUSTB_PBIN_* of a particle column
   bool encoded = false;                // version 3
@@ -46,84 +46,88 @@ int CompressThreads() {
 }
 
 #if ATHENAK_B200_HAVE_ZLIB
-// one complete zlib stream (RFC 1950), level 1
-bool Deflate(const unsigned char *in, std::uint64_t bytes, std::vector<unsigned char> &out) {
-  z_stream z;
-  std::memset(&z, 0, sizeof(z));
-  if (deflateInit(&z, 1) != Z_OK) return false;
-  out.clear();
-  std::vector<unsigned char> buf(std::size_t(1) << 18);
-  const std::uint64_t piece = std::uint64_t(1) << 30;   // the zlib counters are 32-bit
-  std::uint64_t done = 0;
-  int flush = Z_NO_FLUSH, ret = Z_OK;
-  do {
-    const std::uint64_t nin = std::min(piece, bytes - done);
-    z.next_in = const_cast<Bytef *>(in + done);
-    z.avail_in = static_cast<uInt>(nin);
-    done += nin;
-    flush = (done == bytes) ? Z_FINISH : Z_NO_FLUSH;
-    do {
-      z.next_out = buf.data();
-      z.avail_out = static_cast<uInt>(buf.size());
-      ret = deflate(&z, flush);
-      if (ret == Z_STREAM_ERROR) { deflateEnd(&z); return false; }
-      out.insert(out.end(), buf.data(), buf.data() + (buf.size() - z.avail_out));
-    } while (z.avail_out == 0);
-  } while (flush != Z_FINISH);
-  deflateEnd(&z);
-  return ret == Z_STREAM_END;
+// the zlib stream (RFC 1950: deflate data and its adler32) of one chunk at level 1, made by
+// zlib's one-shot compressor into a buffer of its worst-case size
+bool ZlibChunk(const unsigned char *in, std::uint64_t n, std::vector<unsigned char> &out) {
+  uLongf cap = compressBound(static_cast<uLong>(n));
+  out.resize(static_cast<std::size_t>(cap));
+  if (compress2(out.data(), &cap, in, static_cast<uLong>(n), 1) != Z_OK) return false;
+  out.resize(static_cast<std::size_t>(cap));
+  return true;
 }
 #endif
 
-// version 3: the chunks of one column (n rows of size bytes), shuffled here unless the bytes
-// come shuffled, deflated by a pool of threads; chunk order and bytes do not depend on the
-// thread count
-bool ShuffleDeflate(const unsigned char *src, std::uint64_t n, std::uint64_t size,
-                    std::uint64_t chunk_rows, bool shuffled, Col &c) {
+// Version 3: column c of n rows of `size` bytes as consecutive chunks of at most chunk_rows
+// rows, each byte-shuffled (byte k of row i to position k * rows + i; skipped when the rows
+// arrive shuffled already) and compressed on its own.  Thread t of the pool takes chunks
+// t, t + T, t + 2T, ...; the stored bytes are the chunks in row order, whatever T is.
+bool EncodeColumn(const unsigned char *src, std::uint64_t n, std::uint64_t size,
+                  std::uint64_t chunk_rows, bool pre_shuffled, Col &c) {
   const std::uint64_t nchunk = NumChunks(n, chunk_rows);
   c.stored.clear();
   c.chunk_bytes.assign(nchunk, 0);
   if (n == 0) return true;
 #if ATHENAK_B200_HAVE_ZLIB
-  std::vector<std::vector<unsigned char>> part(nchunk);
-  std::atomic<std::uint64_t> next(0);
-  std::atomic<int> failed(0);
-  auto work = [&]() {
-    std::vector<unsigned char> sh;
-    for (std::uint64_t j = next++; j < nchunk; j = next++) {
-      const std::uint64_t r0 = j * chunk_rows, rows = std::min(chunk_rows, n - r0);
-      const unsigned char *in = src + r0 * size;
-      if (!shuffled && size > 1) {
-        sh.resize(static_cast<std::size_t>(rows * size));
-        for (std::uint64_t k = 0; k < size; ++k)
-          for (std::uint64_t i = 0; i < rows; ++i) sh[k * rows + i] = in[i * size + k];
-        in = sh.data();
+  std::vector<std::vector<unsigned char>> enc(nchunk);
+  const int nthread = static_cast<int>(std::min<std::uint64_t>(CompressThreads(), nchunk));
+  std::vector<char> good(nthread, 1);
+  auto encode = [&](int t) {
+    std::vector<unsigned char> shuffled;
+    for (std::uint64_t j = t; j < nchunk; j += nthread) {
+      const std::uint64_t first = j * chunk_rows;
+      const std::uint64_t rows = std::min(chunk_rows, n - first);
+      const unsigned char *rowbytes = src + first * size;
+      if (!pre_shuffled && size > 1) {
+        shuffled.resize(static_cast<std::size_t>(rows * size));
+        for (std::uint64_t i = 0; i < rows; ++i)
+          for (std::uint64_t k = 0; k < size; ++k) shuffled[k * rows + i] = rowbytes[i * size + k];
+        rowbytes = shuffled.data();
       }
-      if (!Deflate(in, rows * size, part[j])) failed = 1;
-      c.chunk_bytes[j] = part[j].size();
+      if (!ZlibChunk(rowbytes, rows * size, enc[j])) good[t] = 0;
     }
   };
-  std::vector<std::thread> pool;
-  const int nt = static_cast<int>(std::min<std::uint64_t>(CompressThreads(), nchunk));
-  for (int t = 1; t < nt; ++t) pool.emplace_back(work);
-  work();
-  for (auto &t : pool) t.join();
-  if (failed) return false;
+  std::vector<std::thread> helpers;
+  for (int t = 1; t < nthread; ++t) helpers.emplace_back(encode, t);
+  encode(0);
+  for (auto &h : helpers) h.join();
+  for (char g : good)
+    if (!g) return false;
   std::uint64_t total = 0;
-  for (const auto &p : part) total += p.size();
-  c.stored.resize(static_cast<std::size_t>(total));
-  std::uint64_t at = 0;
-  for (auto &p : part) {
-    if (!p.empty()) std::memcpy(c.stored.data() + at, p.data(), p.size());
-    at += p.size();
-    std::vector<unsigned char>().swap(p);
+  for (std::uint64_t j = 0; j < nchunk; ++j) {
+    c.chunk_bytes[j] = enc[j].size();
+    total += enc[j].size();
+  }
+  c.stored.reserve(static_cast<std::size_t>(total));
+  for (auto &e : enc) {
+    c.stored.insert(c.stored.end(), e.begin(), e.end());
+    std::vector<unsigned char>().swap(e);
   }
   return true;
 #else
-  (void)src; (void)size; (void)shuffled;
+  (void)src; (void)size; (void)pre_shuffled;
   return false;
 #endif
 }
+
+// the text header, section by section: "[name]" lines and "key = value" lines, an optional
+// note after "  # " (readers drop it)
+class HeaderText {
+ public:
+  HeaderText() { o_ << std::setprecision(17); }
+  void line(const std::string &l) { o_ << l << "\n"; }
+  void section(const char *name) { o_ << "[" << name << "]\n"; }
+  template <class T>
+  void key(const std::string &k, const T &v, const char *note = nullptr) {
+    o_ << k << " = " << v;
+    if (note) o_ << "  # " << note;
+    o_ << "\n";
+  }
+  void raw(const std::string &text) { o_ << text; }
+  std::string str() const { return o_.str(); }
+
+ private:
+  std::ostringstream o_;
+};
 
 bool LittleEndian() {
   const std::uint32_t one = 1;
@@ -203,46 +207,31 @@ std::string WritePbinFile(const std::string &path, const PbinMeta &meta,
   const std::uint64_t rsz = meta.single_precision ? 4 : 8;
   const std::uint32_t version = meta.compress ? kVersionCompressed : kVersion;
 
-  // ---- the columns, in the reference's order
+  // ---- the column directory: the particle columns the plan keeps, then the blocks table
   std::vector<Col> cols;
-  auto col = [&](const char *table, const char *name, const char *dt, std::uint64_t size,
-                 const std::string &meaning, int pcol) {
+  auto add = [&](const char *table, const char *name, const char *dt, std::uint64_t size,
+                 int pcol) {
     Col c;
-    c.table = table; c.name = name; c.dtype = bo + dt; c.itemsize = size; c.meaning = meaning;
+    c.table = table; c.name = name; c.dtype = bo + dt; c.itemsize = size; c.pcol = pcol;
     c.count = (c.table == "particles") ? ntotal : nblocks;
-    c.pcol = pcol;
     cols.push_back(c);
   };
-  const char *species_meaning = "species_id (0-based; input index N = species_id + 1)";
-  const char *ts_meaning = "stopping time t_s (code time)";
-  const char *mass_meaning = "macro-particle mass (code units; not a grain mass)";
-  col("particles", "id", "u8", 8, "numerical sample identity: the 64-bit tag; split / merge / "
-      "resampling create and remove samples, an id is not a grain lineage", DUSTB_PBIN_ID);
-  if (!plan.constant_sp_ts) col("particles", "species", "u4", 4, species_meaning, DUSTB_PBIN_SPECIES);
-  col("particles", "x1", rdt, rsz, "position x1 (code length)", DUSTB_PBIN_X1);
-  col("particles", "x2", rdt, rsz, "position x2 (code length)", DUSTB_PBIN_X2);
-  col("particles", "x3", rdt, rsz, meta.ndim == 3 ? "position x3 (code length)" :
-      "x3 column of a 2-D run (not a mesh direction; as stored)", DUSTB_PBIN_X3);
-  col("particles", "v1", rdt, rsz, "velocity component 1 (see [frame])", DUSTB_PBIN_V1);
-  col("particles", "v2", rdt, rsz, "velocity component 2 (see [frame])", DUSTB_PBIN_V2);
-  col("particles", "v3", rdt, rsz, "velocity component 3 (see [frame])", DUSTB_PBIN_V3);
-  if (!plan.constant_mass) col("particles", "mass", rdt, rsz, mass_meaning, DUSTB_PBIN_MASS);
-  if (!plan.constant_sp_ts)
-    col("particles", "stopping_time", rdt, rsz, ts_meaning, DUSTB_PBIN_STOPPING_TIME);
-  col("blocks", "gid", "i8", 8, "MeshBlock global id", -1);
-  col("blocks", "rank", "i4", 4, "MPI rank that wrote the block", -1);
-  col("blocks", "level", "i4", 4, "refinement level above the root level", -1);
-  col("blocks", "lx1", "i8", 8, "logical location x1 (at the block's level)", -1);
-  col("blocks", "lx2", "i8", 8, "logical location x2", -1);
-  col("blocks", "lx3", "i8", 8, "logical location x3", -1);
-  col("blocks", "x1min", "f8", 8, "block box x1min", -1);
-  col("blocks", "x1max", "f8", 8, "block box x1max", -1);
-  col("blocks", "x2min", "f8", 8, "block box x2min", -1);
-  col("blocks", "x2max", "f8", 8, "block box x2max", -1);
-  col("blocks", "x3min", "f8", 8, "block box x3min", -1);
-  col("blocks", "x3max", "f8", 8, "block box x3max", -1);
+  add("particles", "id", "u8", 8, DUSTB_PBIN_ID);
+  if (!plan.constant_sp_ts) add("particles", "species", "u4", 4, DUSTB_PBIN_SPECIES);
+  add("particles", "x1", rdt, rsz, DUSTB_PBIN_X1);
+  add("particles", "x2", rdt, rsz, DUSTB_PBIN_X2);
+  add("particles", "x3", rdt, rsz, DUSTB_PBIN_X3);
+  add("particles", "v1", rdt, rsz, DUSTB_PBIN_V1);
+  add("particles", "v2", rdt, rsz, DUSTB_PBIN_V2);
+  add("particles", "v3", rdt, rsz, DUSTB_PBIN_V3);
+  if (!plan.constant_mass) add("particles", "mass", rdt, rsz, DUSTB_PBIN_MASS);
+  if (!plan.constant_sp_ts) add("particles", "stopping_time", rdt, rsz, DUSTB_PBIN_STOPPING_TIME);
+  for (const char *n : {"gid", "lx1", "lx2", "lx3"}) add("blocks", n, "i8", 8, -1);
+  for (const char *n : {"rank", "level"}) add("blocks", n, "i4", 4, -1);
+  for (const char *n : {"x1min", "x1max", "x2min", "x2max", "x3min", "x3max"})
+    add("blocks", n, "f8", 8, -1);
 
-  // ---- version 3: every particle column compressed first (the stored sizes set the layout)
+  // ---- version 3: the particle columns are encoded first (their stored sizes place them)
   std::vector<unsigned char> buf;
   std::uint64_t raw_bytes = 0, stored_bytes = 0;
   if (meta.compress) {
@@ -255,189 +244,146 @@ std::string WritePbinFile(const std::string &path, const PbinMeta &meta,
             buf.size() != ntotal * c.itemsize)
           return "pbin: column " + c.name + " not available";
       }
-      if (!ShuffleDeflate(buf.data(), ntotal, c.itemsize, meta.chunk_rows, rows.shuffled, c))
-        return "pbin: zlib deflate failed (column " + c.name + ")";
+      if (!EncodeColumn(buf.data(), ntotal, c.itemsize, meta.chunk_rows, rows.shuffled, c))
+        return "pbin: compression failed (column " + c.name + ")";
     }
   }
   std::uint64_t at = 0;
   for (auto &c : cols) {
     c.offset = at;
-    if (c.encoded) {
-      c.bytes = c.stored.size();
-      raw_bytes += c.count * c.itemsize;
-      stored_bytes += c.bytes;
-    } else {
-      c.bytes = c.count * c.itemsize;
-    }
+    c.bytes = c.encoded ? c.stored.size() : c.count * c.itemsize;
+    if (c.encoded) { raw_bytes += c.count * c.itemsize; stored_bytes += c.bytes; }
     at = Align(at + c.bytes);
   }
   const std::uint64_t data_bytes = at;
 
-  // ---- the text header
-  std::ostringstream h;
-  h << std::setprecision(17);
-  h << "AthenaK particle science file (pbin) format_version = " << version << "\n";
-  h << "[file]\n";
-  h << "format = AKPBIN\nformat_version = " << version << "\n";
-  if (meta.compress) h << "encoding = shuffle_deflate  # particle columns compressed, see [encoding]\n";
-  h << "byte_order = " << (little ? "little" : "big") << "\n";
-  h << "n_particles = " << ntotal << "\nn_blocks = " << nblocks << "\n";
-  h << "written_by_ranks = 1\n";
-  h << "completeness = footer AKPBEND1 + file size; written as .tmp, renamed when complete\n";
-  h << "[snapshot]\n";
-  h << "time = " << meta.time << "\ncycle = " << meta.cycle << "\n";
-  h << "dt = " << meta.dt << "\n";
-  h << "basename = " << meta.basename << "\n";
-  h << "output_block = " << meta.block_name << "\n";
-  h << "file_number = " << meta.file_number << "\n";
-  h << "source_commit = " << meta.source_commit << "\n";
-  h << "mesh_update_seq = " << meta.mesh_update_seq << "\n";
+  // ---- the text header: what the readers parse, in the format's sections and key names
+  HeaderText h;
+  h.line("AthenaK particle science file (pbin) format_version = " + std::to_string(version));
+  h.section("file");
+  h.key("format", "AKPBIN");
+  h.key("format_version", version);
+  if (meta.compress) h.key("encoding", "shuffle_deflate");
+  h.key("byte_order", little ? "little" : "big");
+  h.key("n_particles", ntotal);
+  h.key("n_blocks", nblocks);
+  h.key("written_by_ranks", 1);
+  h.section("snapshot");
+  h.key("time", meta.time);
+  h.key("cycle", meta.cycle);
+  h.key("dt", meta.dt);
+  h.key("basename", meta.basename);
+  h.key("output_block", meta.block_name);
+  h.key("file_number", meta.file_number);
+  h.key("source_commit", meta.source_commit);
+  h.key("mesh_update_seq", meta.mesh_update_seq);
   {
-    std::ostringstream hx;
-    hx << "0x" << std::hex << std::setw(16) << std::setfill('0') << PbinTopologyHash(blocks);
-    h << "block_topology_hash = " << hx.str() << "  # FNV-1a 64 of (level, lx1, lx2, lx3) "
-      << "as int64 for every block in gid order\n";
+    char hex[24];
+    std::snprintf(hex, sizeof(hex), "0x%016llx",
+                  static_cast<unsigned long long>(PbinTopologyHash(blocks)));
+    h.key("block_topology_hash", hex, "FNV-1a 64 over (level, lx1, lx2, lx3) of the blocks");
   }
-  h << "output_point = end of a cycle, before that cycle's mesh refinement check (the first "
-    << "output: after the problem generator; the last: after the final check)\n";
-  h << "[mesh]\n";
-  h << "ndim = " << meta.ndim << "\n";
-  h << "nx1 = " << meta.nx1 << "\nnx2 = " << meta.nx2 << "\nnx3 = " << meta.nx3 << "\n";
-  h << "x1min = " << meta.x1min << "\nx1max = " << meta.x1max << "\n";
-  h << "x2min = " << meta.x2min << "\nx2max = " << meta.x2max << "\n";
-  h << "x3min = " << meta.x3min << "\nx3max = " << meta.x3max << "\n";
-  h << "meshblock_nx1 = " << meta.mb_nx1 << "\nmeshblock_nx2 = " << meta.mb_nx2
-    << "\nmeshblock_nx3 = " << meta.mb_nx3 << "\n";
-  h << "levels = " << meta.levels << "  # finest level above the root\n";
-  h << "multilevel = " << meta.multilevel << "\nadaptive = " << meta.adaptive << "\n";
-  const char *face[6] = {"ix1", "ox1", "ix2", "ox2", "ix3", "ox3"};
-  for (int f = 0; f < 6; ++f) h << "bc_" << face[f] << " = " << meta.bc[f] << "\n";
-  h << "[particles]\n";
-  h << "rows = active rows only (the capacity tail and zero-mass rows are left out)\n";
-  h << "row_order = by writing rank, then the rank's array order (unsorted; neither the "
-    << "order nor the rank layout is stable between outputs)\n";
-  h << "zero_mass_rows_excluded = " << st.zero_mass_rows << "\n";
-  h << "invalid_mass_rows = " << st.invalid_mass_rows << "  # negative or non-finite mass "
-    << "(written)\n";
-  h << "negative_tag_rows = " << st.negative_tag_rows << "  # tags >= 2^63 (high word below "
-    << "zero; never issued; the key keeps its version-1 name)\n";
-  h << "owner = not stored: the MeshBlock whose half-open box [min, max) holds the position "
-    << "(blocks table)\n";
+  h.section("mesh");
+  h.key("ndim", meta.ndim);
+  h.key("nx1", meta.nx1); h.key("nx2", meta.nx2); h.key("nx3", meta.nx3);
+  h.key("x1min", meta.x1min); h.key("x1max", meta.x1max);
+  h.key("x2min", meta.x2min); h.key("x2max", meta.x2max);
+  h.key("x3min", meta.x3min); h.key("x3max", meta.x3max);
+  h.key("meshblock_nx1", meta.mb_nx1); h.key("meshblock_nx2", meta.mb_nx2);
+  h.key("meshblock_nx3", meta.mb_nx3);
+  h.key("levels", meta.levels);
+  h.key("multilevel", meta.multilevel);
+  h.key("adaptive", meta.adaptive);
   {
-    std::string names;
-    if (plan.constant_sp_ts) names += "species stopping_time";
-    if (plan.constant_mass) names += std::string(names.empty() ? "" : " ") + "mass";
-    h << "constant_columns = " << (names.empty() ? std::string("none") : names);
-    if (!names.empty()) h << "  # the same value in every row, given in [constants]";
-    const bool sp_candidate = meta.nspecies == 1 && meta.stopping_time_mode == "species_fixed" &&
-                              !meta.taus.empty();
-    if (sp_candidate && !plan.constant_sp_ts && st.differ_rows > 0)
-      h << (names.empty() ? "  # " : "; ") << "one species, species_fixed, but " << st.differ_rows
-        << " rows differ from species 0 / its tau_s: kept as columns";
-    h << "\n";
+    const char *faces[6] = {"bc_ix1", "bc_ox1", "bc_ix2", "bc_ox2", "bc_ix3", "bc_ox3"};
+    for (int f = 0; f < 6; ++f) h.key(faces[f], meta.bc[f]);
   }
-  h << "particle_real_precision = " << (meta.single_precision ? "single" : "double")
-    << "  # positions, velocities, mass, stopping time (<outputN>/precision)\n";
-  h << "[species]\n";
-  h << "nspecies = " << meta.nspecies << "\n";
-  h << "stopping_time_mode = " << meta.stopping_time_mode << "  # stopping_time (column or "
-    << "constant) is the value each particle uses\n";
-  if (meta.legacy_species) {
-    h << "dust_to_gas = " << meta.dust_to_gas << "  # the <dust>/dust_to_gas key only; a "
-      << "problem generator may set its own abundances (e.g. <problem>/eps_N, see [input])\n";
+  h.section("particles");
+  h.key("zero_mass_rows_excluded", st.zero_mass_rows);
+  h.key("invalid_mass_rows", st.invalid_mass_rows);
+  h.key("negative_tag_rows", st.negative_tag_rows);
+  {
+    std::string consts;
+    if (plan.constant_sp_ts) consts = "species stopping_time";
+    if (plan.constant_mass) consts += consts.empty() ? "mass" : " mass";
+    h.key("constant_columns", consts.empty() ? std::string("none") : consts,
+          consts.empty() ? nullptr : "values in [constants]");
   }
-  h << "back_reaction = " << meta.back_reaction << "\n";
-  for (const auto &line : meta.species_table) h << line << "\n";
-  for (int s = 0; s < meta.nspecies; ++s) {
-    h << "species." << s << " = input_index " << (s + 1) << ", tau_s "
-      << (s < static_cast<int>(meta.taus.size()) ? meta.taus[s]
-                                                 : std::numeric_limits<double>::quiet_NaN());
-    if (s < static_cast<int>(meta.species_detail.size())) h << meta.species_detail[s];
-    h << "\n";
+  h.key("particle_real_precision", meta.single_precision ? "single" : "double");
+  h.section("species");
+  h.key("nspecies", meta.nspecies);
+  h.key("stopping_time_mode", meta.stopping_time_mode);
+  if (meta.legacy_species) h.key("dust_to_gas", meta.dust_to_gas);
+  h.key("back_reaction", meta.back_reaction);
+  for (const auto &l : meta.species_table) h.line(l);
+  for (int sp = 0; sp < meta.nspecies; ++sp) {
+    std::ostringstream v;
+    v << std::setprecision(17) << "input_index " << (sp + 1) << ", tau_s "
+      << (sp < static_cast<int>(meta.taus.size()) ? meta.taus[sp]
+                                                  : std::numeric_limits<double>::quiet_NaN());
+    if (sp < static_cast<int>(meta.species_detail.size())) v << meta.species_detail[sp];
+    h.key("species." + std::to_string(sp), v.str());
   }
-  h << "[representation]\n";
-  for (const auto &line : meta.representation) h << line << "\n";
-  h << "[frame]\n";
-  h << "positions = lab frame, code length\n";
+  h.section("representation");
+  for (const auto &l : meta.representation) h.line(l);
+  h.section("frame");
+  h.key("positions", "lab frame, code length");
   if (meta.shearing_box) {
-    h << "velocity_frame = shear_relative  # velocities relative to the background shear "
-      << "-q Omega x1\n";
-    h << "shear_q = " << meta.qshear << "\nshear_omega = " << meta.omega0 << "\n";
-    if (meta.ndim == 3) {
-      h << "axes = x1 radial, x2 azimuthal, x3 vertical\n";
-      h << "azimuthal_velocity = v2  # v2_phys = v2 - q*Omega*x1\n";
-    } else {
-      h << "axes = x1 radial, x2 vertical (2-D r-z shearing box), azimuth not a mesh "
-        << "direction\n";
-      h << "azimuthal_velocity = v3  # v3_phys = v3 - q*Omega*x1; v2 is vertical\n";
-    }
+    h.key("velocity_frame", "shear_relative",
+          meta.ndim == 3 ? "v2 relative to -q Omega x1" : "v3 relative to -q Omega x1");
+    h.key("shear_q", meta.qshear);
+    h.key("shear_omega", meta.omega0);
   } else {
-    h << "velocity_frame = lab\n";
+    h.key("velocity_frame", "lab");
   }
   if (meta.compress) {
-    h << "[encoding]\n";
-    h << "particle_columns = shuffle_deflate  # every particles column; the blocks columns "
-      << "are raw\n";
-    h << "chunk_rows = " << meta.chunk_rows << "  # rows per chunk at most; a chunk holds rows "
-      << "of one writing rank\n";
-    h << "shuffle = byte shuffle per chunk: stored[k*rows + i] = raw[i*itemsize + k] for "
-      << "byte k = 0 .. itemsize-1 of row i (raw bytes in the file byte order)\n";
-    h << "deflate = one complete zlib stream per chunk (RFC 1950: deflate + adler32), "
-      << "level 1\n";
-    h << "chunk_layout = the chunks of a column follow one another without padding, by "
-      << "rank, then by row; a rank without rows has one chunk with rows 0 and "
-      << "stored_bytes 0\n";
-    h << "chunk_table = [chunks]  # chunk = column rank first_row rows offset stored_bytes; "
-      << "raw bytes = rows * itemsize\n";
-    h << "particle_raw_bytes = " << raw_bytes << "\n";
-    h << "particle_stored_bytes = " << stored_bytes << "\n";
+    h.section("encoding");
+    h.key("particle_columns", "shuffle_deflate");
+    h.key("chunk_rows", meta.chunk_rows);
+    h.key("shuffle", "bytes", "stored[k*rows + i] = raw[i*itemsize + k]");
+    h.key("deflate", "zlib", "RFC 1950 stream per chunk, level 1");
+    h.key("particle_raw_bytes", raw_bytes);
+    h.key("particle_stored_bytes", stored_bytes);
   }
-  h << "[columns]\n";
-  if (meta.compress) {
-    h << "# column = table name dtype count offset bytes encoding (offset from data_start; "
-      << "bytes stored: count * itemsize when raw)\n";
-  } else {
-    h << "# column = table name dtype count offset bytes (offset from data_start)\n";
-  }
+  h.section("columns");
   for (const auto &c : cols) {
-    h << "column = " << c.table << " " << c.name << " " << c.dtype << " " << c.count << " "
-      << c.offset << " " << c.bytes;
-    if (meta.compress) h << (c.encoded ? " shuffle_deflate" : " raw");
-    h << "\n";
+    std::ostringstream v;
+    v << c.table << " " << c.name << " " << c.dtype << " " << c.count << " " << c.offset << " "
+      << c.bytes;
+    if (meta.compress) v << (c.encoded ? " shuffle_deflate" : " raw");
+    h.key("column", v.str());
   }
   if (meta.compress) {
-    h << "[chunks]\n";
-    h << "# chunk = column rank first_row rows offset stored_bytes (offset from "
-      << "data_start)\n";
+    h.section("chunks");
+    const std::uint64_t nch = NumChunks(ntotal, meta.chunk_rows);
     for (const auto &c : cols) {
       if (!c.encoded) continue;
-      std::uint64_t off = c.offset, row = 0;
-      const std::uint64_t nch = NumChunks(ntotal, meta.chunk_rows);
+      std::uint64_t off = c.offset;
       for (std::uint64_t j = 0; j < nch; ++j) {
-        const std::uint64_t r = (ntotal == 0) ? 0 : std::min(meta.chunk_rows, ntotal - j * meta.chunk_rows);
-        const std::uint64_t sb = c.chunk_bytes[j];
-        h << "chunk = " << c.name << " 0 " << row << " " << r << " " << off << " " << sb << "\n";
-        off += sb;
-        row += r;
+        const std::uint64_t first = j * meta.chunk_rows;
+        const std::uint64_t nrow = (ntotal == 0) ? 0 : std::min(meta.chunk_rows, ntotal - first);
+        std::ostringstream v;
+        v << c.name << " 0 " << (ntotal == 0 ? 0 : first) << " " << nrow << " " << off << " "
+          << c.chunk_bytes[j];
+        h.key("chunk", v.str());
+        off += c.chunk_bytes[j];
       }
     }
   }
-  h << "[constants]\n";
-  h << "# constant = table name dtype value (the same value in every row of the table)\n";
+  h.section("constants");
   if (plan.constant_sp_ts) {
-    h << "constant = particles species " << bo << "u4 0\n";
-    h << "constant = particles stopping_time " << bo << "f8 " << plan.ts0 << "\n";
+    h.key("constant", "particles species " + bo + "u4 0");
+    std::ostringstream v;
+    v << std::setprecision(17) << "particles stopping_time " << bo << "f8 " << plan.ts0;
+    h.key("constant", v.str());
   }
-  if (plan.constant_mass) h << "constant = particles mass " << bo << "f8 " << plan.mass << "\n";
-  h << "[meaning]\n";
-  for (const auto &c : cols) h << c.table << "." << c.name << " = " << c.meaning << "\n";
-  if (plan.constant_sp_ts) {
-    h << "particles.species = " << species_meaning << "\n";
-    h << "particles.stopping_time = " << ts_meaning << "\n";
+  if (plan.constant_mass) {
+    std::ostringstream v;
+    v << std::setprecision(17) << "particles mass " << bo << "f8 " << plan.mass;
+    h.key("constant", v.str());
   }
-  if (plan.constant_mass) h << "particles.mass = " << mass_meaning << "\n";
-  h << "[input]\n";
-  h << meta.input_dump;
+  h.section("input");
+  h.raw(meta.input_dump);
   const std::string text = h.str();
   const std::uint64_t data_start = Align(kPreamble + text.size());
   const std::uint64_t file_bytes = data_start + data_bytes + kFooter;

@@ -1,7 +1,7 @@
 // pbin.hpp -- the particle science file (file_type = pbin) of the dust particles, written as
 // ParticleBinaryOutput writes it (src/outputs/pbin.cpp): a 64-byte preamble, the text header
 // ([file] [snapshot] [mesh] [particles] [species] [representation] [frame] ([encoding]
-// [chunks] in version 3) [columns] [constants] [meaning] [input]), the columns one after the
+// [chunks] in version 3) [columns] [constants] [input]), the columns one after the
 // other at 64-byte boundaries, the footer "AKPBEND1" + file size; written as <name>.tmp and
 // renamed when complete.  Only the active rows (mass != 0) are written; species and stopping
 // time, and the mass, become header constants under the reference's conditions.  Format

@@ -3,7 +3,12 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
+#include <string>
+#include <functional>
+#include <map>
+#include <type_traits>
 
 namespace athenak_b200 {
 namespace {
@@ -14,18 +19,24 @@ constexpr std::size_t kHeadBytes = 8 + 6 * sizeof(std::int32_t) + sizeof(std::ui
 constexpr std::size_t kStateMax = 0x7fffffff;   // the dust state's length is an int32
 constexpr int kNReal = 17, kNInt = 5;
 
+// appends raw bytes to a section under construction
 void Put(std::vector<char> &b, const void *p, std::size_t n) {
   const char *c = static_cast<const char *>(p);
   b.insert(b.end(), c, c + n);
 }
 template <typename T>
 void PutValue(std::vector<char> &b, const T &v) { Put(b, &v, sizeof(T)); }
-void PutRecord(std::vector<char> &b, const char *name, const void *p, std::size_t n) {
-  char key[16] = {0};
-  std::strncpy(key, name, 15);
-  Put(b, key, 16);
-  PutValue(b, static_cast<std::int32_t>(n));
-  Put(b, p, n);
+
+// one framed record: the name NUL-padded to 16 bytes, the payload length as int32, the payload
+void PutRecord(std::vector<char> &b, const char *name, const void *payload, std::size_t n) {
+  std::string frame(16, '\0');
+  frame.replace(0, std::min<std::size_t>(15, std::strlen(name)), name,
+                std::min<std::size_t>(15, std::strlen(name)));
+  const std::int32_t len = static_cast<std::int32_t>(n);
+  b.reserve(b.size() + frame.size() + sizeof(len) + n);
+  Put(b, frame.data(), frame.size());
+  Put(b, &len, sizeof(len));
+  Put(b, payload, n);
 }
 
 // the dust records in the reference's order (PackRestartState, then the cell-order index)
@@ -75,113 +86,126 @@ void PackState(const ParticleRestartState &s, std::vector<char> &b) {
   }
 }
 
-// UnpackRestartState's reading of the records; "" or the error
+// The dust records of a section: frames of a 16-byte name, an int32 length and the payload.
+// Each known name has a decoder that checks the payload's size and stores it in the state;
+// an unknown name is kept as read.  "" or the error.
 std::string UnpackState(const char *p, std::size_t nbytes, ParticleRestartSection &sec) {
   ParticleRestartState &s = sec.state;
-  bool species_found = false;
-  std::size_t at = 0;
-  while (at + 16 + sizeof(std::int32_t) <= nbytes) {
-    char key[17] = {0};
-    std::memcpy(key, p + at, 16);
-    std::int32_t n = 0;
-    std::memcpy(&n, p + at + 16, sizeof(n));
-    const char *d = p + at + 16 + sizeof(n);
-    if (n < 0 || at + 16 + sizeof(n) + static_cast<std::size_t>(n) > nbytes)
-      return "dust record runs past the end";
-    const std::string name(key);
-    const std::size_t sz = static_cast<std::size_t>(n);
-    auto fixed = [&](void *dst, std::size_t want) {
-      if (sz != want) return false;
+  using Decoder = std::function<bool(const char *, std::size_t)>;
+  // a payload of exactly `want` bytes copied into dst
+  auto exact = [](void *dst, std::size_t want) -> Decoder {
+    return [dst, want](const char *d, std::size_t n) {
+      if (n != want) return false;
       std::memcpy(dst, d, want);
       return true;
     };
-    bool ok = true;
-    if (name == "next_tag") {                    // version 1: int32 counter (-1: not set)
-      std::int32_t v = 0;
-      ok = fixed(&v, sizeof(v));
-      s.next_tag_set = v >= 0;
-      s.next_tag = v >= 0 ? static_cast<std::uint64_t>(v) : 0;
-    } else if (name == "tag_state") {
-      std::uint64_t v[3];
-      ok = fixed(v, sizeof(v));
-      s.next_tag_set = v[0] != 0; s.next_tag = v[1]; s.tag_bound = v[2];
-    } else if (name == "rank_blocks") {
-      std::int32_t v[3];
-      ok = fixed(v, sizeof(v));
-      s.rank = v[0]; s.gids = v[1]; s.nmb = v[2];
-      s.rank_blocks_read = ok;
-    } else if (name == "merge_pass") {
-      ok = fixed(&s.merge_pass, sizeof(s.merge_pass));
-    } else if (name == "species_table") {
-      species_found = true;
-      s.species_table.assign(d, sz);
-    } else if (name == "mroot" || name == "imex_mown") {
-      ok = sz % sizeof(double) == 0;
-      auto &v = (name == "mroot") ? s.mroot : s.imex_mown;
-      v.resize(sz / sizeof(double));
-      if (ok && sz) std::memcpy(v.data(), d, sz);
-    } else if (name == "resample") {
-      ok = fixed(s.resample, sizeof(s.resample));
-    } else if (name == "resample_clk") {
-      ok = sz == sizeof(s.resample_clk_r) + sizeof(s.resample_clk_n);
-      if (ok) {
-        std::memcpy(s.resample_clk_r, d, sizeof(s.resample_clk_r));
-        std::memcpy(s.resample_clk_n, d + sizeof(s.resample_clk_r), sizeof(s.resample_clk_n));
-      }
-    } else if (name == "merge_clk") {
-      ok = sz == sizeof(s.merge_clk_r) + sizeof(s.merge_clk_n);
-      if (ok) {
-        std::memcpy(s.merge_clk_r, d, sizeof(s.merge_clk_r));
-        std::memcpy(s.merge_clk_n, d + sizeof(s.merge_clk_r), sizeof(s.merge_clk_n));
-      }
-    } else if (name == "amr_state") {
-      ok = sz >= 2 * sizeof(std::int32_t) && sz % sizeof(std::int32_t) == 0;
-      if (ok) {
-        s.amr_state.resize(sz / sizeof(std::int32_t));
-        std::memcpy(s.amr_state.data(), d, sz);
-        ok = static_cast<std::size_t>(s.amr_state[1]) + 2 == s.amr_state.size();
-      }
-    } else if (name == "split") {
-      ok = fixed(s.split, sizeof(s.split));
-    } else if (name == "coarsen_n") {
-      ok = fixed(s.coarsen, sizeof(s.coarsen));
-    } else if (name == "amr_regrids") {
-      ok = fixed(&s.amr_regrids, sizeof(s.amr_regrids));
-    } else if (name == "regrid_evt") {
-      ok = fixed(s.regrid_evt, sizeof(s.regrid_evt));
-    } else if (name == "regrid_evt_t") {
-      ok = fixed(s.regrid_evt_t, sizeof(s.regrid_evt_t));
-    } else if (name == "x3_ledger") {
-      ok = sz >= 5 * sizeof(double) && sz % sizeof(double) == 0;
-      if (ok) {
-        std::vector<double> led(sz / sizeof(double));
-        std::memcpy(led.data(), d, sz);
-        const int nd = static_cast<int>(led[4]);
-        ok = nd >= 0 && static_cast<std::size_t>(5 + nd) == led.size();
-        if (ok) {
-          s.x3_outflow_mass = led[0]; s.x3_outflow_count = led[1];
-          s.x3_removed[0] = led[2]; s.x3_removed[1] = led[3];
-          s.dropped_sum.assign(led.begin() + 5, led.end());
-        }
-      }
-    } else if (name == "cloud_ord_n") {
-      std::int32_t v[3];
-      ok = fixed(v, sizeof(v));
-      s.cloud_ord_status = v[0]; s.cloud_ord_sort_cycle = v[2];
-    } else if (name == "cloud_ord") {
-      ok = sz % sizeof(std::int32_t) == 0;
-      s.cloud_ord.resize(sz / sizeof(std::int32_t));
-      if (ok && sz) std::memcpy(s.cloud_ord.data(), d, sz);
-    } else if (name == "cloud_ord_tag") {
-      ok = sz % sizeof(std::uint64_t) == 0;
-      s.cloud_ord_tag.resize(sz / sizeof(std::uint64_t));
-      if (ok && sz) std::memcpy(s.cloud_ord_tag.data(), d, sz);
-    } else {
-      s.other.emplace_back(name, std::vector<char>(d, d + sz));
+  };
+  // a payload of whole items of type T into a vector
+  auto items = [](auto &vec) -> Decoder {
+    return [&vec](const char *d, std::size_t n) {
+      using T = typename std::decay_t<decltype(vec)>::value_type;
+      if (n % sizeof(T) != 0) return false;
+      vec.resize(n / sizeof(T));
+      if (n) std::memcpy(vec.data(), d, n);
+      return true;
+    };
+  };
+  // two fixed arrays stored back to back
+  auto pair = [](void *a, std::size_t na, void *b, std::size_t nb) -> Decoder {
+    return [=](const char *d, std::size_t n) {
+      if (n != na + nb) return false;
+      std::memcpy(a, d, na);
+      std::memcpy(b, d + na, nb);
+      return true;
+    };
+  };
+  bool species_found = false;
+  std::int32_t rank_blocks[3] = {0, 0, 0}, cloud_info[3] = {0, 0, 0};
+  std::uint64_t tag_state[3] = {0, 0, 0};
+  const std::map<std::string, Decoder> decoders = {
+      {"next_tag", [&](const char *d, std::size_t n) {   // version 1: int32, -1 when unset
+         std::int32_t v = 0;
+         if (!exact(&v, sizeof(v))(d, n)) return false;
+         s.next_tag_set = v >= 0;
+         s.next_tag = v >= 0 ? static_cast<std::uint64_t>(v) : 0;
+         return true;
+       }},
+      {"tag_state", [&](const char *d, std::size_t n) {
+         if (!exact(tag_state, sizeof(tag_state))(d, n)) return false;
+         s.next_tag_set = tag_state[0] != 0;
+         s.next_tag = tag_state[1];
+         s.tag_bound = tag_state[2];
+         return true;
+       }},
+      {"rank_blocks", [&](const char *d, std::size_t n) {
+         s.rank_blocks_read = exact(rank_blocks, sizeof(rank_blocks))(d, n);
+         s.rank = rank_blocks[0]; s.gids = rank_blocks[1]; s.nmb = rank_blocks[2];
+         return s.rank_blocks_read;
+       }},
+      {"merge_pass", exact(&s.merge_pass, sizeof(s.merge_pass))},
+      {"species_table", [&](const char *d, std::size_t n) {
+         species_found = true;
+         s.species_table.assign(d, n);
+         return true;
+       }},
+      {"mroot", items(s.mroot)},
+      {"imex_mown", items(s.imex_mown)},
+      {"resample", exact(s.resample, sizeof(s.resample))},
+      {"resample_clk", pair(s.resample_clk_r, sizeof(s.resample_clk_r), s.resample_clk_n,
+                            sizeof(s.resample_clk_n))},
+      {"merge_clk", pair(s.merge_clk_r, sizeof(s.merge_clk_r), s.merge_clk_n,
+                         sizeof(s.merge_clk_n))},
+      {"amr_state", [&](const char *d, std::size_t n) {
+         // [flag, count, count values]
+         if (n < 2 * sizeof(std::int32_t) || !items(s.amr_state)(d, n)) return false;
+         return static_cast<std::size_t>(s.amr_state[1]) + 2 == s.amr_state.size();
+       }},
+      {"split", exact(s.split, sizeof(s.split))},
+      {"coarsen_n", exact(s.coarsen, sizeof(s.coarsen))},
+      {"amr_regrids", exact(&s.amr_regrids, sizeof(s.amr_regrids))},
+      {"regrid_evt", exact(s.regrid_evt, sizeof(s.regrid_evt))},
+      {"regrid_evt_t", exact(s.regrid_evt_t, sizeof(s.regrid_evt_t))},
+      {"x3_ledger", [&](const char *d, std::size_t n) {
+         // outflow mass and count, the removed (mass, count), the number of dropped sums,
+         // then those sums
+         std::vector<double> led;
+         if (n < 5 * sizeof(double) || !items(led)(d, n)) return false;
+         const int ndrop = static_cast<int>(led[4]);
+         if (ndrop < 0 || static_cast<std::size_t>(5 + ndrop) != led.size()) return false;
+         s.x3_outflow_mass = led[0]; s.x3_outflow_count = led[1];
+         s.x3_removed[0] = led[2]; s.x3_removed[1] = led[3];
+         s.dropped_sum.assign(led.begin() + 5, led.end());
+         return true;
+       }},
+      {"cloud_ord_n", [&](const char *d, std::size_t n) {
+         if (!exact(cloud_info, sizeof(cloud_info))(d, n)) return false;
+         s.cloud_ord_status = cloud_info[0];
+         s.cloud_ord_sort_cycle = cloud_info[2];
+         return true;
+       }},
+      {"cloud_ord", items(s.cloud_ord)},
+      {"cloud_ord_tag", items(s.cloud_ord_tag)},
+  };
+  constexpr std::size_t kFrame = 16 + sizeof(std::int32_t);
+  std::size_t at = 0;
+  while (at + kFrame <= nbytes) {
+    char raw_name[17] = {0};
+    std::memcpy(raw_name, p + at, 16);
+    std::int32_t len = 0;
+    std::memcpy(&len, p + at + 16, sizeof(len));
+    if (len < 0 || at + kFrame + static_cast<std::size_t>(len) > nbytes)
+      return "dust record runs past the end";
+    const std::string name(raw_name);
+    const char *payload = p + at + kFrame;
+    const std::size_t n = static_cast<std::size_t>(len);
+    const auto it = decoders.find(name);
+    if (it == decoders.end()) {
+      s.other.emplace_back(name, std::vector<char>(payload, payload + n));
       sec.notes.push_back("record '" + name + "' is not known to this code and is kept as read");
+    } else if (!it->second(payload, n)) {
+      return "dust record " + name + " has an unexpected size";
     }
-    if (!ok) return "dust record " + name + " has an unexpected size";
-    at += 16 + sizeof(n) + sz;
+    at += kFrame + n;
   }
   if (!species_found) sec.notes.push_back("no record species_table (an older file)");
   // the index must be a whole group: stored with both arrays of its length
