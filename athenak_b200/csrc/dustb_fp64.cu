@@ -1806,6 +1806,18 @@ bool ctx_ok(const dustb_ctx *c) {
   return true;
 }
 
+// the context of a task that reads no particle row (the per-cell solves and exchanges, the
+// mixed form's cycles): the particle rows may be detached (pr = pi = NULL, npart kept)
+bool ctx_cells_ok(const dustb_ctx *c) {
+  if (!c) return false;
+  if (!c->part.pr && !c->part.pi && c->part.npart >= 0) {
+    dustb_ctx d = *c;
+    d.part.npart = 0;
+    return ctx_ok(&d);
+  }
+  return ctx_ok(c);
+}
+
 }  // namespace
 
 // ---- host error bookkeeping --------------------------------------------------------------
@@ -1848,10 +1860,11 @@ void pmbr(const dustb_ctx *c, double a_dt, cudaStream_t st) {
   Ind d = make_ind(c->mesh);
   k_pmbr<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, 1.0 / a_dt);
 }
-bool ctx_valid(const dustb_ctx *c) { return ctx_ok(c); }
+bool ctx_valid(const dustb_ctx *c) { return ctx_cells_ok(c); }
 }  // namespace dustb_cells
 
 #define CHECK_CTX(c) do { if (!ctx_ok(c)) { return DUSTB_EINVAL; } } while (0)
+#define CHECK_CELLS(c) do { if (!ctx_cells_ok(c)) { return DUSTB_EINVAL; } } while (0)
 #define PGRID(c) blocks_for((c)->part.npart), kThreads, 0, S(stream)
 
 extern "C" {
@@ -1870,14 +1883,14 @@ int dustb_register_copy(const dustb_ctx *c, void *stream) {
 }
 
 int dustb_gas_rk_noflux(const dustb_ctx *c, double gam0, double gam1, void *stream) {
-  CHECK_CTX(c);
+  CHECK_CELLS(c);
   Ind d = make_ind(c->mesh);
   k_gas_rk<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.u1, c->f.nvar_gas, gam0, gam1);
   return launch_status("gas_rk_noflux");
 }
 
 int dustb_history_gas(const dustb_ctx *c, double atw_dt, void *stream) {
-  CHECK_CTX(c);
+  CHECK_CELLS(c);
   Ind d = make_ind(c->mesh);
   k_history<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, atw_dt);
   return launch_status("history_gas");
@@ -1913,7 +1926,7 @@ int dustb_deposit_qp(const dustb_ctx *c, double a_dt, double sh, void *stream) {
 }
 
 int dustb_ghost_add(const dustb_ctx *c, double *field, int nvar, void *stream) {
-  CHECK_CTX(c);
+  CHECK_CELLS(c);
   if (!field || nvar <= 0) return DUSTB_EINVAL;
   Ind d = make_ind(c->mesh);
   const int fold = d.three_d && c->mesh.x3bc != DUSTB_X3_PERIODIC && !c->phys.x3_deposit_drop;
@@ -1929,7 +1942,7 @@ int dustb_ghost_add(const dustb_ctx *c, double *field, int nvar, void *stream) {
 }
 
 int dustb_ghost_copy(const dustb_ctx *c, double *field, int nvar, int x3_bcs, void *stream) {
-  CHECK_CTX(c);
+  CHECK_CELLS(c);
   if (!field || nvar <= 0) return DUSTB_EINVAL;
   Ind d = make_ind(c->mesh);
   k_ghost_copy<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar);
@@ -1948,7 +1961,7 @@ int dustb_ghost_copy(const dustb_ctx *c, double *field, int nvar, int x3_bcs, vo
 }
 
 int dustb_solve_ustar(const dustb_ctx *c, void *stream) {
-  CHECK_CTX(c);
+  CHECK_CELLS(c);
   Ind d = make_ind(c->mesh);
   k_solve_ustar<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.qdep,
                                                                      c->f.ustar, c->phys.back_reaction);
@@ -2030,7 +2043,7 @@ int dustb_pc2_predictor(const dustb_ctx *c, double dt, int rate_dep, void *strea
 }
 
 int dustb_pc2_apply_predictor(const dustb_ctx *c, double dt, double *chi_max, void *stream) {
-  CHECK_CTX(c);
+  CHECK_CELLS(c);
   Ind d = make_ind(c->mesh);
   if (chi_max) {
     k_set<<<1, 1, 0, S(stream)>>>(chi_max, 0.0, 0, 0.0);
@@ -2043,7 +2056,7 @@ int dustb_pc2_apply_predictor(const dustb_ctx *c, double dt, double *chi_max, vo
 }
 
 int dustb_pc2_midpoint(const dustb_ctx *c, void *stream) {
-  CHECK_CTX(c);
+  CHECK_CELLS(c);
   Ind d = make_ind(c->mesh);
   k_pc2_midpoint<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.u1, c->f.nvar_gas, c->f.ustar);
   return launch_status("pc2_midpoint");
@@ -2062,7 +2075,7 @@ int dustb_pc2_advance(const dustb_ctx *c, double dt, void *stream) {
 }
 
 int dustb_pc2_commit(const dustb_ctx *c, double wpred, void *stream) {
-  CHECK_CTX(c);
+  CHECK_CELLS(c);
   Ind d = make_ind(c->mesh);
   k_pc2_commit<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom,
                                                                     c->f.qdep, wpred);

@@ -1783,6 +1783,11 @@ int sort_into(const MState &S, const PBuf &src, const PBuf &dst, const dustb_mes
   return dustb_host::launch_status("mixed sort");
 }
 
+// import and export read and write the reference rows: they must be attached
+bool rows_attached(const dustb_ctx *c) {
+  return c->part.npart == 0 || (c->part.pr && c->part.pi);
+}
+
 bool params_ok(const dustb_ctx *c, const dustb_mixed_params *mp) {
   if (!dustb_cells::ctx_valid(c) || !mp) return false;
   for (int a = 0; a < 3; ++a)
@@ -1880,7 +1885,7 @@ long long dustb_mixed_workspace_bytes(const dustb_mesh *mesh, int npart) {
 
 int dustb_mixed_import(const dustb_ctx *c, const dustb_mixed_params *mp, void *ws,
                        long long bytes, void *stream) {
-  if (!params_ok(c, mp)) return DUSTB_EINVAL;
+  if (!params_ok(c, mp) || !rows_attached(c)) return DUSTB_EINVAL;
   MState S;
   if (!carve(c->mesh, c->part.npart, ws, bytes, S, nullptr)) return DUSTB_ESCRATCH;
   cudaStream_t st = (cudaStream_t)stream;
@@ -1900,7 +1905,7 @@ int dustb_mixed_import(const dustb_ctx *c, const dustb_mixed_params *mp, void *w
 
 int dustb_mixed_export(const dustb_ctx *c, const dustb_mixed_params *mp, void *ws,
                        long long bytes, void *stream) {
-  if (!params_ok(c, mp)) return DUSTB_EINVAL;
+  if (!params_ok(c, mp) || !rows_attached(c)) return DUSTB_EINVAL;
   MState S;
   if (!carve(c->mesh, c->part.npart, ws, bytes, S, nullptr)) return DUSTB_ESCRATCH;
   Geo G = make_geo(c, mp);

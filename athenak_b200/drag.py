@@ -133,6 +133,19 @@ class DeviceDust:
         self.ctx.mesh.time = self.__dict__.get("time", 0.0)
         self.pctx = C.byref(self.ctx)
 
+    def detach_rows(self):
+        """Frees the reference rows (pr, pi) and passes them as detached (NULL, npart kept):
+        between a mixed import and export only the shadow and the mesh fields are used."""
+        self.t["pr"] = None
+        self.t["pi"] = None
+        self._rebuild_ctx()
+
+    def attach_rows(self, pr, pi):
+        """Attaches reference rows (17 x stride float64, 5 x stride int32 device tensors)."""
+        self.t["pr"], self.t["pi"] = pr, pi
+        self.stride = int(pr.shape[1])
+        self._rebuild_ctx()
+
     def set_time(self, t):
         """The mesh time the next calls use (the shear offset of shear-periodic x1 faces)."""
         self.time = float(t)

@@ -23,7 +23,8 @@ from .mesh import box_ensemble_mesh
 from .mixed import MixedDust
 from .inputs import IPX, IPVX, IPY, IPZ, IPX1, IPY1, IPZ1, IPVX1, IPTS, IPM, PGID, PTAG, PSP
 
-__all__ = ["Box", "draw_boxes", "damping_solution", "EnsemblePack", "run_ensemble"]
+__all__ = ["Box", "draw_boxes", "damping_solution", "EnsemblePack", "run_ensemble",
+           "run_ensemble_one_launch"]
 
 
 @dataclass
@@ -72,7 +73,9 @@ class EnsemblePack:
     """The boxes of one side as one MeshBlock pack on the device, in the reference layout,
     advanced by the mixed-precision imex2+ cycle."""
 
-    def __init__(self, side, boxes, v0=0.1, device="cuda"):
+    def __init__(self, side, boxes, v0=0.1, device="cuda", detach=False):
+        """detach: free the reference rows after the import (the cycles advance the shadow
+        alone; check() rebuilds the rows before its export)."""
         self.side, self.boxes, self.v0 = side, list(boxes), v0
         self.ms = box_ensemble_mesh(side, len(self.boxes))
         ncell = side ** 3
@@ -80,6 +83,28 @@ class EnsemblePack:
         self.npart = int(sum(counts))
         phys = dict(scheme=2, drag_solver=2, consistent_gas=True, back_reaction=True)
         self.dev = DeviceDust.empty(self.ms, self.npart, phys, device=device, nspecies=4)
+        self._fill_rows()
+        u0 = self.dev.t["u0"]
+        u0.zero_()
+        u0[:, 0] = 1.0                               # gas at rest, density 1
+        dx = 1.0 / side
+        self.dt = 0.3 * dx / (1.0 + v0)
+        self.mx = MixedDust(dev=self.dev, do_import=False)
+        self.mx.import_()
+        if detach:
+            self.dev.detach_rows()
+        self.cycles = 0
+        self.graph = None
+
+    def _fill_rows(self):
+        """The initial reference rows: ppc particles of every species at every cell centre
+        of every box (the damping test's lattice), moving at v0 through gas at rest."""
+        side, v0 = self.side, self.v0
+        ncell = side ** 3
+        if self.dev.t.get("pr") is None:
+            self.dev.attach_rows(
+                torch.zeros((17, self.npart), dtype=torch.float64, device=self.dev.device),
+                torch.zeros((5, self.npart), dtype=torch.int32, device=self.dev.device))
         pr, pi = self.dev.t["pr"], self.dev.t["pi"]
         f64 = dict(dtype=torch.float64, device=self.dev.device)
         dx = 1.0 / side
@@ -102,14 +127,6 @@ class EnsemblePack:
                 pi[PSP, sl] = s
                 pi[PTAG, sl] = torch.arange(p0, p0 + n, dtype=torch.int32, device=self.dev.device)
                 p0 += n
-        u0 = self.dev.t["u0"]
-        u0.zero_()
-        u0[:, 0] = 1.0                               # gas at rest, density 1
-        self.dt = 0.3 * dx / (1.0 + v0)
-        self.mx = MixedDust(dev=self.dev, do_import=False)
-        self.mx.import_()
-        self.cycles = 0
-        self.graph = None
 
     def step(self, n, stream=None):
         """n imex2+ cycles of every box (the first call runs one eager cycle and captures
@@ -125,7 +142,11 @@ class EnsemblePack:
     def check(self):
         """Per box: the largest deviation of the gas and species mean velocities from the
         exact damping solution, relative to v0, and the change of total momentum relative
-        to the initial dust momentum (per-box sums formed on the device)."""
+        to the initial dust momentum (per-box sums formed on the device).  Detached rows are
+        rebuilt first (the export writes positions, velocities, registers and rates; species,
+        tags and masses are the initial ones)."""
+        if self.dev.t.get("pr") is None:
+            self._fill_rows()
         self.mx.export()
         pr, pi = self.dev.t["pr"], self.dev.t["pi"]
         nb = len(self.boxes)
@@ -156,6 +177,53 @@ class EnsemblePack:
         self.graph = None
         del self.mx, self.dev
         torch.cuda.empty_cache()
+
+
+def run_ensemble_one_launch(boxes, cycles, v0=0.1):
+    """Every box resident at once, one pack per side with its reference rows detached after
+    the import, and one substep of the whole ensemble as ONE CUDA-graph launch: the cycle of
+    every pack captured on a stream of its own, forked from and joined to the capture stream,
+    so the packs' kernels run side by side (the small packs fill the GPU together).  Returns
+    the device time of cycles 2..cycles (graph replays), the particle-cycles done in them,
+    the per-box checks and the number of packs."""
+    by_side = {}
+    for b in boxes:
+        by_side.setdefault(b.side, []).append(b)
+    packs = [EnsemblePack(side, by_side[side], v0, detach=True) for side in sorted(by_side)]
+    # one eager cycle of every pack: it sets the kernels' shared-memory limits (a capture
+    # does not) and is the untimed first cycle
+    for p in packs:
+        p.mx.imex_cycle(p.dt, GAMMA_DEFAULT)
+        p.cycles += 1
+    torch.cuda.synchronize()
+    streams = [torch.cuda.Stream() for _ in packs]
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        cap = torch.cuda.current_stream()
+        for p, st in zip(packs, streams):
+            st.wait_stream(cap)
+            p.mx.imex_cycle(p.dt, GAMMA_DEFAULT, stream=st)
+        for st in streams:
+            cap.wait_stream(st)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(cycles - 1):
+        g.replay()
+    t1.record()
+    torch.cuda.synchronize()
+    for p in packs:
+        p.cycles += cycles - 1
+    ms = t0.elapsed_time(t1)
+    psteps = sum(p.npart for p in packs) * (cycles - 1)
+    del g
+    checks = []
+    for p in packs:
+        assert p.mx.error_word() == 0, "device error word set"
+        checks += p.check()
+        p.free()
+    return ms, psteps, checks, len(packs)
 
 
 def run_ensemble(boxes, cycles, v0=0.1, stream=None):

@@ -541,11 +541,21 @@ def measure_ensemble(args):
     species, t_s log-uniform in 1e-3..10, eps log-uniform in 0.1..10, ppc 1..8), one
     MeshBlock pack per side, each pack's cycle a replayed CUDA graph; every box checked
     against the exact solution of its damping ODE."""
-    from athenak_b200.ensemble import draw_boxes, run_ensemble
+    import torch
+    from athenak_b200.ensemble import draw_boxes, run_ensemble, run_ensemble_one_launch
     n = 32 if args.small else 1024
     boxes = draw_boxes(n, seed=1, sides=(8, 16) if args.small else (16, 64))
     cycles = args.ensemble_cycles
-    ms, ps, ch = run_ensemble(boxes, cycles)
+    try:
+        # every box resident, one CUDA-graph launch per substep
+        ms, ps, ch, npk = run_ensemble_one_launch(boxes, cycles)
+        timed = (f"cycles 2..{cycles}: one CUDA-graph launch per substep over all {n} boxes "
+                 f"({npk} packs by side as parallel branches, reference rows detached)")
+    except torch.cuda.OutOfMemoryError:
+        torch.cuda.empty_cache()
+        ms, ps, ch = run_ensemble(boxes, cycles)
+        timed = (f"cycles 2..{cycles} of every pack (CUDA-graph replays pack by pack; the "
+                 f"resident ensemble did not fit), device time summed over packs")
     worst = max(ch, key=lambda c: c["err_vs_exact"])
     return {"workload": f"{n} periodic dust_damping boxes, sides log-uniform {boxes and min(b.side for b in boxes)}.."
                         f"{max(b.side for b in boxes)} cells, 1-4 species, t_s 1e-3..10, eps 0.1..10, ppc 1..8, "
@@ -553,7 +563,7 @@ def measure_ensemble(args):
             "boxes": n, "particles": int(sum(b.side ** 3 * b.ppc * len(b.taus) for b in boxes)),
             "cells": int(sum(b.side ** 3 for b in boxes)), "cycles": cycles,
             "value": ps / (ms * 1e-3), "unit": UNIT, "device_ms": ms,
-            "timed": f"cycles 2..{cycles} of every pack (CUDA-graph replays), device time summed over packs",
+            "timed": timed,
             "max_err_vs_exact_rel_v0": max(c["err_vs_exact"] for c in ch),
             "max_momentum_change_rel": max(c["momentum_change"] for c in ch),
             "worst_box": worst}

@@ -455,6 +455,13 @@ typedef struct dustb_mixed_params {
 
 long long dustb_mixed_workspace_bytes(const dustb_mesh *mesh, int npart);
 
+/* Detached rows: between an import and an export the mixed cycles (and the cell tasks they
+ * call: dustb_solve_ustar, dustb_ghost_add, dustb_ghost_copy, dustb_gas_rk_noflux,
+ * dustb_history_gas, dustb_pc2_apply_predictor, dustb_pc2_midpoint, dustb_pc2_commit) read no
+ * particle row, so a host code may free the reference rows and pass ctx->part with
+ * pr = pi = NULL and npart kept, holding only the shadow while the cycles run; import and
+ * export need the rows attached (DUSTB_EINVAL otherwise). */
+
 /* Builds the shadow of particles 0..npart-1 of ctx->part (positions, velocities, registers,
  * rates, t_s, m) and sorts it by cell. */
 int dustb_mixed_import(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
