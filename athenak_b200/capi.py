@@ -192,7 +192,7 @@ RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_phst_scratch_bytes": LL,
 # declared by athenak_b200.mixed (they take its DustbMixedParams struct)
 EXTRA_SIGNATURES = {"dustb_mixed_workspace_bytes", "dustb_mixed_import", "dustb_mixed_export",
                     "dustb_mixed_imex_cycle", "dustb_mixed_sort", "dustb_mixed_timing",
-                    "dustb_mixed_kernel_times", "dustb_mixed_pc2_cycle"}
+                    "dustb_mixed_kernel_times", "dustb_mixed_pc2_cycle", "dustb_mixed_tune"}
 
 
 def _declare(lib):

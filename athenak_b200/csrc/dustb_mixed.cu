@@ -88,7 +88,14 @@ struct MState {
   int *key;                      // new cell of each particle (count -> move)
   int *cstart, *cursor, *bsum;
   float4 *win;                   // 3-D: the gather window (k_gather_window)
+  int *tile_order;               // the tiles heaviest first (the device work queue)
+  int *qhead;                    // kQueues counters: tiles taken by each queued launch
 };
+
+// counters of the queued tile launches of a stage (Q/P, up to two operator sweeps, kick;
+// the pc2 predictor and advance), cleared when the stage's queue is built
+constexpr int kQueues = 8;
+enum { Q_QP = 0, Q_OP = 1, Q_KICK = 4, Q_PRED = 5, Q_ADV = 6 };
 
 // cells of the gather window of a 3-D mesh: every block's active cells and one layer around
 // them, (nx1 + 2)(nx2 + 2)(nx3 + 2) per block; 0 in 2-D (the 2-D tiles read the FP64 field)
@@ -153,6 +160,9 @@ bool carve(const dustb_mesh &ms, int n, void *ws, long long bytes, MState &S, lo
   const size_t o_cur = off; off += al256(4 * (size_t)(ncell + 2));
   const size_t o_bs = off; off += al256(4 * (size_t)scan_bsum_ints(ncell + 2));
   const size_t o_win = off; off += al256(16 * (size_t)nwin(ms));
+  // (tiles of one row each at most: the active rows of the mesh)
+  const size_t o_ord = off; off += al256(4 * (size_t)(ncell / ms.nx1 + 1));
+  const size_t o_qh = off; off += al256(4 * kQueues);
   if (need) *need = (long long)off;
   if (!ws || bytes < (long long)off) return false;
   char *b = (char *)ws;
@@ -166,6 +176,8 @@ bool carve(const dustb_mesh &ms, int n, void *ws, long long bytes, MState &S, lo
   S.key = (int *)(b + o_key);
   S.cstart = (int *)(b + o_cs); S.cursor = (int *)(b + o_cur); S.bsum = (int *)(b + o_bs);
   S.win = (float4 *)(b + o_win);
+  S.tile_order = (int *)(b + o_ord);
+  S.qhead = (int *)(b + o_qh);
   return true;
 }
 
@@ -825,6 +837,11 @@ struct TileArgs {
   int deposit;                 // 0: kick or advance only (no back-reaction)
   float shy;                   // imex: the stage's implicit shear shift sh / dy (0: none)
   int probe_timeout;           // test hook: tile 0 never issues its first copy
+  // the device work queue of a persistent launch: the tiles in the order to take them
+  // (heaviest first) and the launch's counter of tiles taken; order null: one CTA per tile
+  const int *order;
+  int *qhead;
+  int ntiles;
   Pc2Args pc;
   unsigned *err;
 };
@@ -1210,13 +1227,6 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
   __shared__ int s_split;                          // some cell of the pass has several slots
   const int nx1 = G.nx1, tj = T.tj;
   const int nct = tj * nx1;                        // source cells of the tile = threads
-  int t = blockIdx.x;
-  const int per_block = G.nx3 * T.tpp;
-  const int m = t / per_block;
-  t -= m * per_block;
-  const int k = t / T.tpp;
-  const int j0 = (t - k * T.tpp) * tj;
-  const int c0 = encode(G, m, k, j0, 0);
   const int CH = T.chunk;                          // buffer columns (multiple of 4)
   int *s_cs = (int *)smem;                         // [nct + 1] cell ranges
   int *s_ss = s_cs + (nct + 1);                    // [nct + 1] slot starts of the pass
@@ -1238,233 +1248,286 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
 #pragma unroll
     for (int f = 0; f < NF; ++f) bulk_copy(s_f + f * CH, S.f[fl[f]] + a0, bytes, &bar);
   };
-  if (tid == 0) {
-    // the first pass's copies go out before the cell ranges are read
-    mbar_init(&bar, 1);
-    const int p0 = T.cstart[c0], p1 = T.cstart[c0 + nct];
-    // (the failure-detection hook: tile 0's first copy is never issued, its wait runs out)
-    if (p1 > p0 && !(T.probe_timeout && blockIdx.x == 0)) issue_pass(p0, min(p1, p0 + (CH - 8)));
-  }
-  __syncwarp(wmask);
-  for (int x = tid; x <= nct; x += blockDim.x) s_cs[x] = T.cstart[c0 + x];
-  if (MODE == MODE_QP) s_qt[tid] = 0.0f;
-  cta_sync(wmask);
-  const int P0 = s_cs[0], P1 = s_cs[nct];
-  const float inv_vol = (float)(1.0 / G.vol);
-  const float inv_adt = (float)(1.0 / T.a_dt);
-  const int CHP = CH - 8;                          // particles per pass (room to round out)
-  const bool single = (P1 - P0) <= CHP;            // the whole tile in one pass
-  unsigned parity = 0;
-
-  for (int cb = P0; cb < P1; cb += CHP) {
-    const int ce = min(P1, cb + CHP), cnt = ce - cb;
-    const int a0 = cb & ~3, sh = cb - a0;
-    if (tid == 0 && cb != P0) issue_pass(cb, ce);
-    // (the warp reconverges before the barriers of the slot map: thread 0 must not arrive
-    // at them apart from its warp)
+  __shared__ int s_item;
+  if (tid == 0) mbar_init(&bar, 1);
+  unsigned parity = 0;                             // the copies' barrier phase, over all tiles
+  // One tile per CTA (T.order null), or a persistent CTA taking tiles from the device work
+  // queue -- T.order, heaviest first -- until the queue is empty.
+  for (int item = 0;; ++item) {
+    int t;
+    if (!T.order) {
+      if (item > 0) break;
+      t = blockIdx.x;
+    } else {
+      if (tid == 0) s_item = atomicAdd(T.qhead, 1);
+      cta_sync(wmask);
+      const int q = s_item;
+      if (q >= T.ntiles) break;
+      t = T.order[q];
+    }
+    const int per_block = G.nx3 * T.tpp;
+    const int m = t / per_block;
+    t -= m * per_block;
+    const int k = t / T.tpp;
+    const int j0 = (t - k * T.tpp) * tj;
+    const int c0 = encode(G, m, k, j0, 0);
+    if (tid == 0) {
+      // the first pass's copies go out before the cell ranges are read
+      const int p0 = T.cstart[c0], p1 = T.cstart[c0 + nct];
+      // (the failure-detection hook: the first tile of CTA 0 never issues its first copy, its
+      // wait runs out)
+      if (p1 > p0 && !(T.probe_timeout && blockIdx.x == 0 && item == 0))
+        issue_pass(p0, min(p1, p0 + (CH - 8)));
+    }
     __syncwarp(wmask);
-    // the slots of the pass: cell c gets q_c = ceil(n_c / R) of them, R the smallest share
-    // with sum q_c <= threads (every cell one slot when the pass covers all the cells).  A
-    // tile of one pass takes thread = cell directly (the uniform case)
-    int cl = -1, lo = 0, hi = 0;
-    if (single) {
-      cl = tid; lo = s_cs[tid] - a0; hi = s_cs[tid + 1] - a0;
-    } else {
-      const int n_c = max(0, min(s_cs[tid + 1], ce) - max(s_cs[tid], cb));
-      // (the cells with particles in the pass: per-warp ballots, summed after a barrier)
-      const unsigned bal = __ballot_sync(wmask, n_c > 0);
-      if (lane == 0) s_wcnt[wid] = __popc(bal);
-      cta_sync(wmask);
-      int ncp = 0;
-      for (int w = 0; w < nwarp; ++w) ncp += s_wcnt[w];
-      const int R = (ncp >= nct) ? cnt : (cnt + (nct - ncp) - 1) / (nct - ncp);
-      const int q_c = (n_c > 0) ? (n_c + R - 1) / R : 0;
-      int inc = q_c;                                 // block-wide inclusive scan of q_c
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(wmask, inc, o);
-        if (lane >= o) inc += y;
-      }
-      if (lane == 31 || tid == nct - 1) s_wsum[wid] = inc;
-      cta_sync(wmask);
-      for (int w = 0; w < wid; ++w) inc += s_wsum[w];
-      s_ss[tid + 1] = inc;
-      if (tid == 0) s_ss[0] = 0;
-      if (tid == nct - 1) s_split = inc > ncp;
-      cta_sync(wmask);
-      // this thread's slot: the last cell whose slots start at or before tid, an even share
-      // of its particles in the pass (columns lo..hi of the rows)
-      if (tid < s_ss[nct]) {
-        int L = 0, H = nct - 1;
-        while (L < H) {
-          const int M = (L + H + 1) >> 1;
-          if (s_ss[M] <= tid) L = M; else H = M - 1;
-        }
-        cl = L;
-        const int qc = s_ss[cl + 1] - s_ss[cl], rk = tid - s_ss[cl];
-        const int b0 = max(s_cs[cl], cb), len = min(s_cs[cl + 1], ce) - b0;
-        lo = b0 + (len * rk) / qc - a0;
-        hi = b0 + (len * (rk + 1)) / qc - a0;
-      }
-    }
-    const int cj_l = (cl >= 0) ? cl / nx1 : 0, ci_l = (cl >= 0) ? cl - cj_l * nx1 : 0;
-    const int jrow = j0 + cj_l;
-    // the y offset of the weights: the particle's own, or (an imex stage with an implicit
-    // shear shift) that of y + sh x, which the push kept inside the particle's cell
-    auto oy_at = [&](int r) -> float {
-      return (GH & 2) ? shifted_oy(G, T.shy, m, ci_l, s_f[r], s_f[CH + r]) : s_f[CH + r];
-    };
-    GatherWindow<D3> win;
-    if constexpr (MODE != MODE_QP) {                 // (the loads fly with the copies)
-      if constexpr (D3) win.load4(G, T.win4, m, k, jrow, ci_l);
-      else win.template load<GH>(G, T.gfield, m, k, jrow, ci_l);
-    }
-    const bool ok = mbar_wait(&bar, parity, T.err, wmask);
-    parity ^= 1u;
-    if (__syncthreads_or(!ok)) {
-      // the copies never completed: wait once more (bounded) for them, then give up the tile
-      mbar_wait(&bar, parity ^ 1u, T.err, wmask);
-      return;
-    }
-    if (MODE == MODE_QP) {
-      CellSums<MODE, D3> qp;
-      qp.zero();
-      float qt = 0.0f;
-      for (int r = lo; r < hi; ++r) {
-        float wx_[3], wy_[3], wz_[3];
-        wts(SCHEME, s_f[r], wx_);
-        wts(SCHEME, oy_at(r), wy_);
-        if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
-        const float mc = s_f[4 * CH + r] * s_f[3 * CH + r] * inv_vol;
-        qt += mc;
-        qp.add(wx_, wy_, wz_, make_float2(mc, mc * s_f[5 * CH + r]),
-               make_float2(mc * s_f[6 * CH + r], mc * s_f[7 * CH + r]));
-      }
-      if (cl >= 0) atomicAdd(&s_qt[cl], qt);
-      // the rows are read by now: their space takes the staged sums (per cell, or per slot
-      // when the pass splits cells)
-      cta_sync(wmask);
-      const bool split = !single && s_split;
-      if (!single && !split && s_ss[tid + 1] == s_ss[tid]) stage_zero<D3>(s_acc, tid, nct);
-      if (cl >= 0) stage_sums<MODE, D3>(qp, s_acc, split ? tid : cl, nct);
-      cta_sync(wmask);
-      if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l);
-      else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
-    } else {
-      // gather phase: the operator's m c u / V, the kick's velocity change, the predictor's
-      // impulse and rate, or the advance's u*, into rows 5..7 (and 3)
-      for (int r = lo; r < hi; ++r) {
-        float wx_[3], wy_[3], wz_[3];
-        wts(SCHEME, s_f[r], wx_);
-        wts(SCHEME, oy_at(r), wy_);
-        if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
-        float2 uxy;
-        float uz;
-        win.gather(wx_, wy_, wz_, uxy, uz);
-        const float c32 = s_f[3 * CH + r];
-        if (MODE == MODE_OP) {
-          const float mc = s_f[4 * CH + r] * c32 * inv_vol;
-          s_f[5 * CH + r] = mc * uxy.x; s_f[6 * CH + r] = mc * uxy.y; s_f[7 * CH + r] = mc * uz;
-        } else if (MODE == MODE_PRED) {
-          // dust_pc2_predictor (src/dust/dust_pm.cpp:141-193): rate m/(t_s V), impulse
-          // -dt rate (u - v) from the old gas velocity m/rho of u1
-          const float rate = s_f[4 * CH + r] * inv_vol / c32;
-          const float vx = s_f[5 * CH + r], vy = s_f[6 * CH + r], vz = s_f[7 * CH + r];
-          const float g = -T.pc.dt * rate;
-          s_f[3 * CH + r] = rate;
-          s_f[5 * CH + r] = g * (uxy.x - vx); s_f[6 * CH + r] = g * (uxy.y - vy);
-          s_f[7 * CH + r] = g * (uz - vz);
-        } else if (MODE == MODE_ADV) {
-          s_f[5 * CH + r] = uxy.x; s_f[6 * CH + r] = uxy.y; s_f[7 * CH + r] = uz;
-        } else {
-          // GatherKickPMBR (src/dust/dust_pm.cpp:534-563): the applied velocity change
-          const float vx = s_f[5 * CH + r], vy = s_f[6 * CH + r], vz = s_f[7 * CH + r];
-          s_f[5 * CH + r] = (vx + c32 * (uxy.x - vx)) - vx;
-          s_f[6 * CH + r] = (vy + c32 * (uxy.y - vy)) - vy;
-          s_f[7 * CH + r] = (vz + c32 * (uz - vz)) - vz;
-        }
-      }
-      if (MODE == MODE_KICK) {
-        // the kicked velocities and rates of the pass, particle by particle (coalesced):
-        // v <- v + dv, R <- dv / a_dt
+    for (int x = tid; x <= nct; x += blockDim.x) s_cs[x] = T.cstart[c0 + x];
+    if (MODE == MODE_QP) s_qt[tid] = 0.0f;
+    cta_sync(wmask);
+    const int P0 = s_cs[0], P1 = s_cs[nct];
+    const float inv_vol = (float)(1.0 / G.vol);
+    const float inv_adt = (float)(1.0 / T.a_dt);
+    const int CHP = CH - 8;                          // particles per pass (room to round out)
+    const bool single = (P1 - P0) <= CHP;            // the whole tile in one pass
+
+    for (int cb = P0; cb < P1; cb += CHP) {
+      const int ce = min(P1, cb + CHP), cnt = ce - cb;
+      const int a0 = cb & ~3, sh = cb - a0;
+      if (tid == 0 && cb != P0) issue_pass(cb, ce);
+      // (the warp reconverges before the barriers of the slot map: thread 0 must not arrive
+      // at them apart from its warp)
+      __syncwarp(wmask);
+      // the slots of the pass: cell c gets q_c = ceil(n_c / R) of them, R the smallest share
+      // with sum q_c <= threads (every cell one slot when the pass covers all the cells).  A
+      // tile of one pass takes thread = cell directly (the uniform case)
+      int cl = -1, lo = 0, hi = 0;
+      if (single) {
+        cl = tid; lo = s_cs[tid] - a0; hi = s_cs[tid + 1] - a0;
+      } else {
+        const int n_c = max(0, min(s_cs[tid + 1], ce) - max(s_cs[tid], cb));
+        // (the cells with particles in the pass: per-warp ballots, summed after a barrier)
+        const unsigned bal = __ballot_sync(wmask, n_c > 0);
+        if (lane == 0) s_wcnt[wid] = __popc(bal);
         cta_sync(wmask);
-        // (four particles per thread at a time, their velocity loads issued together)
-        constexpr int U = 4;
-        for (int x0 = tid; x0 < cnt; x0 += U * blockDim.x) {
-          float v[U][3];
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int p = cb + min(x0 + u * (int)blockDim.x, cnt - 1);
-            v[u][0] = S.f[F_VX][p]; v[u][1] = S.f[F_VY][p]; v[u][2] = S.f[F_VZ][p];
+        int ncp = 0;
+        for (int w = 0; w < nwarp; ++w) ncp += s_wcnt[w];
+        const int R = (ncp >= nct) ? cnt : (cnt + (nct - ncp) - 1) / (nct - ncp);
+        const int q_c = (n_c > 0) ? (n_c + R - 1) / R : 0;
+        int inc = q_c;                                 // block-wide inclusive scan of q_c
+  #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(wmask, inc, o);
+          if (lane >= o) inc += y;
+        }
+        if (lane == 31 || tid == nct - 1) s_wsum[wid] = inc;
+        cta_sync(wmask);
+        for (int w = 0; w < wid; ++w) inc += s_wsum[w];
+        s_ss[tid + 1] = inc;
+        if (tid == 0) s_ss[0] = 0;
+        if (tid == nct - 1) s_split = inc > ncp;
+        cta_sync(wmask);
+        // this thread's slot: the last cell whose slots start at or before tid, an even share
+        // of its particles in the pass (columns lo..hi of the rows)
+        if (tid < s_ss[nct]) {
+          int L = 0, H = nct - 1;
+          while (L < H) {
+            const int M = (L + H + 1) >> 1;
+            if (s_ss[M] <= tid) L = M; else H = M - 1;
           }
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int x = x0 + u * blockDim.x;
-            if (x >= cnt) break;
-            const int s = sh + x, p = cb + x;
-            const float dvx = s_f[5 * CH + s], dvy = s_f[6 * CH + s], dvz = s_f[7 * CH + s];
-            S.f[F_VX][p] = v[u][0] + dvx; S.f[F_VY][p] = v[u][1] + dvy; S.f[F_VZ][p] = v[u][2] + dvz;
-            S.f[F_RX][p] = dvx * inv_adt; S.f[F_RY][p] = dvy * inv_adt; S.f[F_RZ][p] = dvz * inv_adt;
-          }
+          cl = L;
+          const int qc = s_ss[cl + 1] - s_ss[cl], rk = tid - s_ss[cl];
+          const int b0 = max(s_cs[cl], cb), len = min(s_cs[cl + 1], ce) - b0;
+          lo = b0 + (len * rk) / qc - a0;
+          hi = b0 + (len * (rk + 1)) / qc - a0;
         }
       }
-      if (MODE == MODE_ADV) {
-        // the advanced particles of the pass, one per thread (coalesced): v, the
-        // displacement to the new position (cells), the rate dv; their impulses -m dv / V
-        // into rows 5..7
-        cta_sync(wmask);
-        for (int x = tid; x < cnt; x += blockDim.x) {
-          const int s = sh + x, p = cb + x;
-          const float v0[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
-          const float u[3] = {s_f[5 * CH + s], s_f[6 * CH + s], s_f[7 * CH + s]};
-          // (3-D shearing box: the half step left z_h in the z rate and the shear drift in
-          // the displacement)
-          const float zh = (T.pc.sbox && D3) ? S.f[F_RZ][p] : 0.0f;
-          float vn[3], disp[3], dv[3];
-          pc2_particle(T.pc, D3, 0.0f, zh, v0, u, s_f[3 * CH + s], false, vn, disp, dv);
-          S.f[F_VX][p] = vn[0]; S.f[F_VY][p] = vn[1]; S.f[F_VZ][p] = vn[2];
-          S.f[F_AX][p] += disp[0] * (float)G.inv_dx[0];
-          S.f[F_AY][p] += disp[1] * (float)G.inv_dx[1];
-          if (D3) S.f[F_AZ][p] += disp[2] * (float)G.inv_dx[2];
-          S.f[F_RX][p] = dv[0]; S.f[F_RY][p] = dv[1]; S.f[F_RZ][p] = dv[2];
-          const float f = -s_f[4 * CH + s] * inv_vol;
-          s_f[5 * CH + s] = f * dv[0]; s_f[6 * CH + s] = f * dv[1]; s_f[7 * CH + s] = f * dv[2];
-        }
-        cta_sync(wmask);
+      const int cj_l = (cl >= 0) ? cl / nx1 : 0, ci_l = (cl >= 0) ? cl - cj_l * nx1 : 0;
+      const int jrow = j0 + cj_l;
+      // the y offset of the weights: the particle's own, or (an imex stage with an implicit
+      // shear shift) that of y + sh x, which the push kept inside the particle's cell
+      auto oy_at = [&](int r) -> float {
+        return (GH & 2) ? shifted_oy(G, T.shy, m, ci_l, s_f[r], s_f[CH + r]) : s_f[CH + r];
+      };
+      GatherWindow<D3> win;
+      if constexpr (MODE != MODE_QP) {                 // (the loads fly with the copies)
+        if constexpr (D3) win.load4(G, T.win4, m, k, jrow, ci_l);
+        else win.template load<GH>(G, T.gfield, m, k, jrow, ci_l);
       }
-      if (T.deposit) {
-        // deposit phase: the sums of the values of this pass, added to the field
-        CellSums<MODE, D3> sums;
-        sums.zero();
+      const bool ok = mbar_wait(&bar, parity, T.err, wmask);
+      parity ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        // the copies never completed: wait once more (bounded) for them, then give up the tile
+        mbar_wait(&bar, parity ^ 1u, T.err, wmask);
+        return;
+      }
+      if (MODE == MODE_QP) {
+        CellSums<MODE, D3> qp;
+        qp.zero();
+        float qt = 0.0f;
         for (int r = lo; r < hi; ++r) {
           float wx_[3], wy_[3], wz_[3];
           wts(SCHEME, s_f[r], wx_);
           wts(SCHEME, oy_at(r), wy_);
           if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
-          const float f = (MODE == MODE_KICK) ? -s_f[4 * CH + r] * inv_vol : 1.0f;
-          sums.add(wx_, wy_, wz_, make_float2(f * s_f[5 * CH + r], f * s_f[6 * CH + r]),
-                   make_float2(f * s_f[7 * CH + r], (MODE == MODE_PRED) ? s_f[3 * CH + r] : 0.0f));
+          const float mc = s_f[4 * CH + r] * s_f[3 * CH + r] * inv_vol;
+          qt += mc;
+          qp.add(wx_, wy_, wz_, make_float2(mc, mc * s_f[5 * CH + r]),
+                 make_float2(mc * s_f[6 * CH + r], mc * s_f[7 * CH + r]));
         }
+        if (cl >= 0) atomicAdd(&s_qt[cl], qt);
         // the rows are read by now: their space takes the staged sums (per cell, or per slot
         // when the pass splits cells)
         cta_sync(wmask);
         const bool split = !single && s_split;
         if (!single && !split && s_ss[tid + 1] == s_ss[tid]) stage_zero<D3>(s_acc, tid, nct);
-        if (cl >= 0) stage_sums<MODE, D3>(sums, s_acc, split ? tid : cl, nct);
+        if (cl >= 0) stage_sums<MODE, D3>(qp, s_acc, split ? tid : cl, nct);
         cta_sync(wmask);
         if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l);
         else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
+      } else {
+        // gather phase: the operator's m c u / V, the kick's velocity change, the predictor's
+        // impulse and rate, or the advance's u*, into rows 5..7 (and 3)
+        for (int r = lo; r < hi; ++r) {
+          float wx_[3], wy_[3], wz_[3];
+          wts(SCHEME, s_f[r], wx_);
+          wts(SCHEME, oy_at(r), wy_);
+          if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
+          float2 uxy;
+          float uz;
+          win.gather(wx_, wy_, wz_, uxy, uz);
+          const float c32 = s_f[3 * CH + r];
+          if (MODE == MODE_OP) {
+            const float mc = s_f[4 * CH + r] * c32 * inv_vol;
+            s_f[5 * CH + r] = mc * uxy.x; s_f[6 * CH + r] = mc * uxy.y; s_f[7 * CH + r] = mc * uz;
+          } else if (MODE == MODE_PRED) {
+            // dust_pc2_predictor (src/dust/dust_pm.cpp:141-193): rate m/(t_s V), impulse
+            // -dt rate (u - v) from the old gas velocity m/rho of u1
+            const float rate = s_f[4 * CH + r] * inv_vol / c32;
+            const float vx = s_f[5 * CH + r], vy = s_f[6 * CH + r], vz = s_f[7 * CH + r];
+            const float g = -T.pc.dt * rate;
+            s_f[3 * CH + r] = rate;
+            s_f[5 * CH + r] = g * (uxy.x - vx); s_f[6 * CH + r] = g * (uxy.y - vy);
+            s_f[7 * CH + r] = g * (uz - vz);
+          } else if (MODE == MODE_ADV) {
+            s_f[5 * CH + r] = uxy.x; s_f[6 * CH + r] = uxy.y; s_f[7 * CH + r] = uz;
+          } else {
+            // GatherKickPMBR (src/dust/dust_pm.cpp:534-563): the applied velocity change
+            const float vx = s_f[5 * CH + r], vy = s_f[6 * CH + r], vz = s_f[7 * CH + r];
+            s_f[5 * CH + r] = (vx + c32 * (uxy.x - vx)) - vx;
+            s_f[6 * CH + r] = (vy + c32 * (uxy.y - vy)) - vy;
+            s_f[7 * CH + r] = (vz + c32 * (uz - vz)) - vz;
+          }
+        }
+        if (MODE == MODE_KICK) {
+          // the kicked velocities and rates of the pass, particle by particle (coalesced):
+          // v <- v + dv, R <- dv / a_dt
+          cta_sync(wmask);
+          // (four particles per thread at a time, their velocity loads issued together)
+          constexpr int U = 4;
+          for (int x0 = tid; x0 < cnt; x0 += U * blockDim.x) {
+            float v[U][3];
+  #pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const int p = cb + min(x0 + u * (int)blockDim.x, cnt - 1);
+              v[u][0] = S.f[F_VX][p]; v[u][1] = S.f[F_VY][p]; v[u][2] = S.f[F_VZ][p];
+            }
+  #pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const int x = x0 + u * blockDim.x;
+              if (x >= cnt) break;
+              const int s = sh + x, p = cb + x;
+              const float dvx = s_f[5 * CH + s], dvy = s_f[6 * CH + s], dvz = s_f[7 * CH + s];
+              S.f[F_VX][p] = v[u][0] + dvx; S.f[F_VY][p] = v[u][1] + dvy; S.f[F_VZ][p] = v[u][2] + dvz;
+              S.f[F_RX][p] = dvx * inv_adt; S.f[F_RY][p] = dvy * inv_adt; S.f[F_RZ][p] = dvz * inv_adt;
+            }
+          }
+        }
+        if (MODE == MODE_ADV) {
+          // the advanced particles of the pass, one per thread (coalesced): v, the
+          // displacement to the new position (cells), the rate dv; their impulses -m dv / V
+          // into rows 5..7
+          cta_sync(wmask);
+          for (int x = tid; x < cnt; x += blockDim.x) {
+            const int s = sh + x, p = cb + x;
+            const float v0[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
+            const float u[3] = {s_f[5 * CH + s], s_f[6 * CH + s], s_f[7 * CH + s]};
+            // (3-D shearing box: the half step left z_h in the z rate and the shear drift in
+            // the displacement)
+            const float zh = (T.pc.sbox && D3) ? S.f[F_RZ][p] : 0.0f;
+            float vn[3], disp[3], dv[3];
+            pc2_particle(T.pc, D3, 0.0f, zh, v0, u, s_f[3 * CH + s], false, vn, disp, dv);
+            S.f[F_VX][p] = vn[0]; S.f[F_VY][p] = vn[1]; S.f[F_VZ][p] = vn[2];
+            S.f[F_AX][p] += disp[0] * (float)G.inv_dx[0];
+            S.f[F_AY][p] += disp[1] * (float)G.inv_dx[1];
+            if (D3) S.f[F_AZ][p] += disp[2] * (float)G.inv_dx[2];
+            S.f[F_RX][p] = dv[0]; S.f[F_RY][p] = dv[1]; S.f[F_RZ][p] = dv[2];
+            const float f = -s_f[4 * CH + s] * inv_vol;
+            s_f[5 * CH + s] = f * dv[0]; s_f[6 * CH + s] = f * dv[1]; s_f[7 * CH + s] = f * dv[2];
+          }
+          cta_sync(wmask);
+        }
+        if (T.deposit) {
+          // deposit phase: the sums of the values of this pass, added to the field
+          CellSums<MODE, D3> sums;
+          sums.zero();
+          for (int r = lo; r < hi; ++r) {
+            float wx_[3], wy_[3], wz_[3];
+            wts(SCHEME, s_f[r], wx_);
+            wts(SCHEME, oy_at(r), wy_);
+            if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
+            const float f = (MODE == MODE_KICK) ? -s_f[4 * CH + r] * inv_vol : 1.0f;
+            sums.add(wx_, wy_, wz_, make_float2(f * s_f[5 * CH + r], f * s_f[6 * CH + r]),
+                     make_float2(f * s_f[7 * CH + r], (MODE == MODE_PRED) ? s_f[3 * CH + r] : 0.0f));
+          }
+          // the rows are read by now: their space takes the staged sums (per cell, or per slot
+          // when the pass splits cells)
+          cta_sync(wmask);
+          const bool split = !single && s_split;
+          if (!single && !split && s_ss[tid + 1] == s_ss[tid]) stage_zero<D3>(s_acc, tid, nct);
+          if (cl >= 0) stage_sums<MODE, D3>(sums, s_acc, split ? tid : cl, nct);
+          cta_sync(wmask);
+          if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l);
+          else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
+        }
       }
+      // the next pass's copies overwrite the rows (and its slots the slot starts)
+      cta_sync(wmask);
     }
-    // the next pass's copies overwrite the rows (and its slots the slot starts)
+    if (MODE == MODE_QP) {
+      // centre mass m c / V of the cell (dust_imex_point_center_mass): only this cell's
+      // particles have it as their centre, so it is stored, not added
+      const int cj = tid / nx1, ci = tid - cj * nx1;
+      T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj, G.is + ci)] = (double)s_qt[tid];
+    }
+    // (every thread is done with this tile's shared memory before the next tile's copies)
     cta_sync(wmask);
   }
-  if (MODE == MODE_QP) {
-    // centre mass m c / V of the cell (dust_imex_point_center_mass): only this cell's
-    // particles have it as their centre, so it is stored, not added
-    const int cj = tid / nx1, ci = tid - cj * nx1;
-    T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj, G.is + ci)] = (double)s_qt[tid];
+}
+
+// The device work queue of a stage: every tile of the mesh ordered by its particle count,
+// heaviest first (buckets of equal log2 count, in descending order; a tile's place inside its
+// bucket does not matter), so that the persistent tile launches start the long tiles first
+// and finish on short ones.  One CTA; also clears the stage's queue counters.
+__global__ void __launch_bounds__(1024) k_tile_order(const int *cstart, Geo G, int tj, int tpp,
+                                                     int ntiles, int *order, int *qhead) {
+  __shared__ int hist[33], base[33];
+  const int nct = tj * G.nx1, per_block = G.nx3 * tpp;
+  auto bucket = [&](int t) {
+    const int m = t / per_block, r = t - m * per_block, k = r / tpp, j0 = (r - k * tpp) * tj;
+    const int c0 = encode(G, m, k, j0, 0);
+    const int cost = cstart[c0 + nct] - cstart[c0];
+    return cost > 0 ? __clz(cost) : 32;           // 32 - log2 size: heavy tiles first
+  };
+  for (int b = threadIdx.x; b < 33; b += blockDim.x) hist[b] = 0;
+  if (threadIdx.x < kQueues) qhead[threadIdx.x] = 0;
+  __syncthreads();
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) atomicAdd(&hist[bucket(t)], 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int b = 0; b < 33; ++b) { base[b] = run; run += hist[b]; }
   }
+  __syncthreads();
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) order[atomicAdd(&base[bucket(t)], 1)] = t;
 }
 
 // shared memory of a tile: the head, then the larger of the pass rows and the staged sums
@@ -1663,6 +1726,7 @@ struct Scope {
 struct Cfg {
   int tj, chunk, tpp;
   int probe_timeout;
+  int grid;                      // 1: one CTA per tile; 0: persistent CTAs on the work queue
 };
 
 // the default particles per pass: the largest multiple of 4 that lets as many CTAs share an
@@ -1680,8 +1744,10 @@ int default_chunk(int tj, int nx1) {
 
 bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   const int nx1 = ms.nx1, nx2 = ms.multi_d ? ms.nx2 : 1;
-  if ((mp->variant != 0 && mp->variant != DUSTB_MIXED_PROBE_COPY_TIMEOUT) || nx1 > kMaxTileThreads)
+  const int base = mp->variant & ~DUSTB_MIXED_GRID_TILES;
+  if ((base != 0 && base != DUSTB_MIXED_PROBE_COPY_TIMEOUT) || nx1 > kMaxTileThreads)
     return false;
+  cf.grid = (mp->variant & DUSTB_MIXED_GRID_TILES) ? 1 : 0;
   int tj = mp->rows_per_tile;
   if (tj <= 0) {
     tj = 1;
@@ -1693,7 +1759,7 @@ bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   cf.chunk = mp->chunk > 0 ? mp->chunk : default_chunk(tj, nx1);
   if (cf.chunk < 64 || cf.chunk > 8192 || (cf.chunk & 3)) return false;
   cf.tpp = nx2 / tj;
-  cf.probe_timeout = (mp->variant == DUSTB_MIXED_PROBE_COPY_TIMEOUT);
+  cf.probe_timeout = (base == DUSTB_MIXED_PROBE_COPY_TIMEOUT);
   // every tile form must fit the 227 KiB of shared memory a CTA can have (less the barrier)
   if (tile_smem(ms.three_d, tj, nx1, cf.chunk) > 227 * 1024 - 256) return false;
   return true;
@@ -1703,13 +1769,42 @@ template <int MODE, int D3, int SCHEME, int GH>
 int launch_tile_d(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &T, cudaStream_t st) {
   const long long tiles = (long long)G.nmb * G.nx3 * cf.tpp;
   const size_t sm = tile_smem(D3, cf.tj, G.nx1, cf.chunk);
+  const int threads = cf.tj * G.nx1;
   static size_t configured = 0;
+  // the CTAs of this kernel one SM holds at this shared-memory size and block (for the
+  // persistent launch), looked up once per size
+  static size_t occ_sm = 0;
+  static int occ_threads = 0, occ = 0, nsm = 0;
   if (sm > 48 * 1024 && sm > configured) {
     cudaFuncSetAttribute(k_tile<MODE, D3, SCHEME, GH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     configured = sm;
   }
-  k_tile<MODE, D3, SCHEME, GH><<<(unsigned)tiles, cf.tj * G.nx1, sm, st>>>(cur, G, T);
+  long long grid = tiles;
+  if (T.order) {
+    if (occ_sm != sm || occ_threads != threads || nsm == 0) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile<MODE, D3, SCHEME, GH>, threads, sm);
+      occ_sm = sm; occ_threads = threads;
+    }
+    const long long resident = (long long)(occ > 0 ? occ : 1) * (nsm > 0 ? nsm : 1);
+    grid = tiles < resident ? tiles : resident;
+  }
+  k_tile<MODE, D3, SCHEME, GH><<<(unsigned)grid, threads, sm, st>>>(cur, G, T);
   return dustb_host::launch_status("mixed tile");
+}
+
+// the stage's work queue (the tiles of the sorted copy heaviest first) unless the
+// configuration asks for one CTA per tile
+int build_queue(const MState &S, const Geo &G, const Cfg &cf, TileArgs &T, cudaStream_t st) {
+  T.order = nullptr; T.qhead = nullptr;
+  if (cf.grid) return DUSTB_OK;
+  T.ntiles = G.nmb * G.nx3 * cf.tpp;
+  k_tile_order<<<1, 1024, 0, st>>>(S.cstart, G, cf.tj, cf.tpp, T.ntiles, S.tile_order, S.qhead);
+  T.order = S.tile_order;
+  T.qhead = S.qhead;
+  return dustb_host::launch_status("mixed tile queue");
 }
 
 // the kernel of one dimensionality, ghost mode (GH bit 0) and implicit-shift form (bit 1)
@@ -1722,8 +1817,9 @@ int launch_tile_s(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &
 
 template <int MODE>
 int launch_tile(const MState &S, const PBuf &cur, const Geo &G, const Cfg &cf, TileArgs T,
-                cudaStream_t st) {
+                cudaStream_t st, int qslot) {
   T.tj = cf.tj; T.chunk = cf.chunk; T.tpp = cf.tpp; T.cstart = S.cstart;
+  if (T.qhead) T.qhead = S.qhead + qslot;
   T.probe_timeout = cf.probe_timeout;
   // one kernel per dimensionality and deposit scheme (no per-particle scheme selection); the
   // weights shifted by an imex stage's implicit shear shift only in the kernels of that form
@@ -1929,6 +2025,75 @@ int dustb_mixed_sort(const dustb_ctx *c, const dustb_mixed_params *mp, void *ws,
   return dustb_host::launch_status("mixed_sort");
 }
 
+int dustb_mixed_tune(const dustb_ctx *c, dustb_mixed_params *mp, void *ws, long long bytes,
+                     double a_dt, double *best_ms, void *stream) {
+  if (!params_ok(c, mp) || !(a_dt > 0.0)) return DUSTB_EINVAL;
+  if (!c->mesh.multi_d) return DUSTB_EUNSUP;
+  const Geo G = make_geo(c, mp);
+  if (!geo_ok(mp, G)) return DUSTB_EINVAL;
+  MState S;
+  if (!carve(c->mesh, c->part.npart, ws, bytes, S, nullptr)) return DUSTB_ESCRATCH;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (g_timing.on) return DUSTB_EUNSUP;          // (its events would interleave)
+  const int nx1 = c->mesh.nx1, nx2 = c->mesh.nx2;
+  const int keep = mp->variant & ~DUSTB_MIXED_GRID_TILES;
+  // the candidates: rows per tile (tiles of at most 256 cells), particles per pass (the
+  // default, or passes sized for 2.25, 4 and 4.5 thousand particles), persistent CTAs on the
+  // work queue or one CTA per tile
+  struct Cand { int rows, chunk, grid; };
+  std::vector<Cand> cands;
+  for (int r : {1, 2, 4, 8})
+    if (nx2 % r == 0 && r * nx1 <= kMaxTileThreads)
+      for (int ch : {0, 2304, 4096, 4608})
+        for (int g : {0, 1}) cands.push_back({r, ch, g});
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    return DUSTB_ELAUNCH;
+  float best = -1.0f;
+  Cand pick{mp->rows_per_tile, mp->chunk, (mp->variant & DUSTB_MIXED_GRID_TILES) ? 1 : 0};
+  int rc = DUSTB_OK;
+  TileArgs base{};
+  base.a_dt = a_dt; base.err = c->err; base.deposit = 1;
+  rc = gather_window(S, G, c->mesh, c->f.ustar, base, st);
+  for (size_t q = 0; q < cands.size() && rc == DUSTB_OK; ++q) {
+    dustb_mixed_params t = *mp;
+    t.rows_per_tile = cands[q].rows;
+    t.chunk = cands[q].chunk;
+    t.variant = keep | (cands[q].grid ? DUSTB_MIXED_GRID_TILES : 0);
+    Cfg cf;
+    if (!pick_cfg(c->mesh, &t, cf)) continue;     // (the shape does not fit shared memory)
+    // the Q/P and operator tiles on the shadow as it stands: they write only the stage's
+    // scratch fields (qdep, the centre mass, work), which every cycle rewrites before use
+    auto trial = [&]() {
+      TileArgs T = base;
+      int r = build_queue(S, G, cf, T, st);
+      if (r) return r;
+      T.dfield = c->f.qdep; T.dnvar = 5; T.res = c->f.resid;
+      if ((r = launch_tile<MODE_QP>(S, S.A, G, cf, T, st, Q_QP))) return r;
+      T.gfield = c->f.ustar; T.dfield = c->f.work; T.dnvar = 3;
+      return launch_tile<MODE_OP>(S, S.A, G, cf, T, st, Q_OP);
+    };
+    if ((rc = trial())) break;                     // warm-up (kernel attributes, caches)
+    cudaEventRecord(e0, st);
+    for (int rep = 0; rep < 2 && rc == DUSTB_OK; ++rep) rc = trial();
+    cudaEventRecord(e1, st);
+    if (rc) break;
+    if (cudaEventSynchronize(e1) != cudaSuccess) { rc = DUSTB_ELAUNCH; break; }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (best < 0.0f || ms < best) { best = ms; pick = cands[q]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (best < 0.0f) return DUSTB_EUNSUP;
+  mp->rows_per_tile = pick.rows;
+  mp->chunk = pick.chunk;
+  mp->variant = keep | (pick.grid ? DUSTB_MIXED_GRID_TILES : 0);
+  if (best_ms) *best_ms = 0.5 * best;
+  return DUSTB_OK;
+}
+
 int dustb_mixed_timing(int enable) {
   g_timing.on = enable != 0;
   for (int k = 0; k < DUSTB_K_NKERNELS; ++k) g_timing.used[k] = 0;
@@ -2009,13 +2174,14 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     if (stage == 1) cudaMemsetAsync(&S.head->pending, 0, sizeof(int), st);   // applied
     TileArgs T{};
     T.a_dt = a_dt; T.err = c->err; T.deposit = 1; T.shy = P.shy;
+    RUN(build_queue(S, G, cf, T, st));                // the stage's tiles, heaviest first
     const bool shift = P.shy != 0.0f;
     if (br) {
       {
         Scope sc(DUSTB_K_DEPOSIT_QP, st);
         cudaMemsetAsync(c->f.qdep, 0, fbytes * 5, st);
         T.dfield = c->f.qdep; T.dnvar = 5; T.res = c->f.resid;
-        RUN(launch_tile<MODE_QP>(S, cur, G, cf, T, st));
+        RUN(launch_tile<MODE_QP>(S, cur, G, cf, T, st, Q_QP));
         if (shift) RUN(launch_shift_edge<MODE_QP>(S, cur, G, T, st));
       }
       Scope sc(DUSTB_K_CELLS, st);
@@ -2036,7 +2202,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
         RUN(gather_window(S, G, c->mesh, c->f.ustar, T, st));
         { Scope sc(DUSTB_K_OPERATOR, st);
           T.gfield = c->f.ustar; T.dfield = c->f.work; T.dnvar = 3;
-          RUN(launch_tile<MODE_OP>(S, cur, G, cf, T, st));
+          RUN(launch_tile<MODE_OP>(S, cur, G, cf, T, st, Q_OP + w));
           if (shift) RUN(launch_shift_edge<MODE_OP>(S, cur, G, T, st)); }
         { Scope sc(DUSTB_K_CELLS, st);
           RUN(ghost_add_if(c, G, c->f.work, 3, st));
@@ -2052,7 +2218,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     {
       Scope sc(DUSTB_K_KICK, st);
       T.gfield = c->f.ustar; T.dfield = c->f.dmom; T.dnvar = 3; T.deposit = br;
-      RUN(launch_tile<MODE_KICK>(S, cur, G, cf, T, st));
+      RUN(launch_tile<MODE_KICK>(S, cur, G, cf, T, st, Q_KICK));
       if (shift) RUN(launch_shift_edge<MODE_KICK>(S, cur, G, T, st));
     }
     if (br) {
@@ -2114,7 +2280,8 @@ int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void
       Scope sc(DUSTB_K_DEPOSIT_QP, st);
       cudaMemsetAsync(c->f.qdep, 0, fbytes * 5, st);
       T.gfield = c->f.work; T.dfield = c->f.qdep + d.cells(); T.dnvar = 5;
-      RUN(launch_tile<MODE_PRED>(S, S.A, G, cf, T, st));
+      RUN(build_queue(S, G, cf, T, st));             // the tiles of copy A
+      RUN(launch_tile<MODE_PRED>(S, S.A, G, cf, T, st, Q_PRED));
     }
     Scope sc(DUSTB_K_CELLS, st);
     RUN(ghost_add_if(c, G, c->f.qdep, 5, st));
@@ -2145,7 +2312,8 @@ int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void
   {
     Scope sc(DUSTB_K_KICK, st);
     T.gfield = c->f.ustar; T.dfield = c->f.dmom; T.dnvar = 3; T.deposit = br;
-    RUN(launch_tile<MODE_ADV>(S, S.B, G, cf, T, st));
+    RUN(build_queue(S, G, cf, T, st));               // the tiles of copy B (half step)
+    RUN(launch_tile<MODE_ADV>(S, S.B, G, cf, T, st, Q_ADV));
     if (G.ghost && n > 0) {
       T.cstart = S.cstart;
       if (G.scheme == 2) k_pc2_edge<2><<<148 * 4, kT, 0, st>>>(S.B, G, T);

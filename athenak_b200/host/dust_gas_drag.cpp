@@ -341,6 +341,7 @@ MixedDustGasDrag::MixedDustGasDrag(const dustb_ctx &ctx, void *stream, const dou
   for (int a = 0; a < 3; ++a) mp_.dx[a] = dx[a];
   mp_.rows_per_tile = rows_per_tile;
   mp_.chunk = chunk;
+  tuned_ = rows_per_tile > 0 || chunk > 0;    // a given tile shape is kept
   ws_bytes_ = dustb_mixed_workspace_bytes(&ctx_.mesh, ctx_.part.npart);
   if (ws_bytes_ <= 0 || cudaMalloc(&ws_, (size_t)ws_bytes_) != cudaSuccess ||
       cudaMalloc(&dev_scalars_, 3 * sizeof(double)) != cudaSuccess) {
@@ -370,7 +371,14 @@ TaskStatus MixedDustGasDrag::Export() {
   return Check(dustb_mixed_export(&ctx_, &mp_, ws_, ws_bytes_, stream_), "mixed export");
 }
 
+TaskStatus MixedDustGasDrag::Tune(double a_dt) {
+  tuned_ = true;
+  return Check(dustb_mixed_tune(&ctx_, &mp_, ws_, ws_bytes_, a_dt, nullptr, stream_),
+               "mixed tune");
+}
+
 TaskStatus MixedDustGasDrag::ImexCycle(const Driver &drv) {
+  if (!tuned_ && Tune(drv.gamma * drv.dt) != TaskStatus::complete) return TaskStatus::fail;
   dustb_imex_coeffs co;
   co.gamma = drv.gamma; co.dt = drv.dt; co.sh[0] = co.sh[1] = 0.0;
   ctx_.mesh.time = drv.time;
@@ -378,6 +386,7 @@ TaskStatus MixedDustGasDrag::ImexCycle(const Driver &drv) {
 }
 
 TaskStatus MixedDustGasDrag::Pc2Cycle(const Driver &drv) {
+  if (!tuned_ && Tune(0.5 * drv.dt) != TaskStatus::complete) return TaskStatus::fail;
   ctx_.mesh.time = drv.time;
   return Check(dustb_mixed_pc2_cycle(&ctx_, &mp_, ws_, ws_bytes_, drv.dt, dev_scalars_ + 2, stream_),
                "mixed pc2 cycle");

@@ -148,6 +148,9 @@ class MixedDustGasDrag {
 
   TaskStatus Import();
   TaskStatus Export();
+  // the library's autotuner on this workspace (after Import; synchronous, outside any stream
+  // capture); ImexCycle and Pc2Cycle call it once themselves unless the tile shape was given
+  TaskStatus Tune(double a_dt);
   TaskStatus ImexCycle(const Driver &drv);   // imex2+ (no implicit shear shift)
   TaskStatus Pc2Cycle(const Driver &drv);    // pc2
   dustb_ctx &Context() { return ctx_; }
@@ -159,6 +162,7 @@ class MixedDustGasDrag {
   dustb_ctx ctx_;
   void *stream_;
   dustb_mixed_params mp_;
+  bool tuned_ = false;
   void *ws_ = nullptr;
   long long ws_bytes_ = 0;
   double *dev_scalars_ = nullptr;            // [0..1] x3 removed, [2] chi_max

@@ -39,6 +39,7 @@ def _declare(lib):
         "dustb_mixed_sort": [P, MP, VP, LL, VP],
         "dustb_mixed_imex_cycle": [P, MP, VP, LL, C.POINTER(capi.DustbImexCoeffs), VP],
         "dustb_mixed_pc2_cycle": [P, MP, VP, LL, C.c_double, VP, VP],
+        "dustb_mixed_tune": [P, MP, VP, LL, C.c_double, VP, VP],
     }.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -123,6 +124,15 @@ class MixedDust:
         with torch.cuda.graph(g):
             cycle()
         return g
+
+    def tune(self, a_dt, stream=None):
+        """The library's autotuner (dustb_mixed_tune): picks rows per tile, particles per pass
+        and the launch form on this workspace; returns (rows_per_tile, chunk, grid, ms)."""
+        p, n = self._ws()
+        ms = C.c_double(0.0)
+        capi.check(self.lib.dustb_mixed_tune(self.dev.pctx, C.byref(self.mp), p, n, a_dt,
+                                             C.byref(ms), _stream_ptr(stream)), "mixed_tune")
+        return (self.mp.rows_per_tile, self.mp.chunk, int(bool(self.mp.variant & 8)), ms.value)
 
     def set_tiles(self, rows_per_tile=0, chunk=0, variant=None):
         self.mp.rows_per_tile = rows_per_tile

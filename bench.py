@@ -272,25 +272,12 @@ def run_ours(args, rep):
     mx = MixedDust(dev=dev, do_import=False)
     mx.import_()
     if args.tune:
-        best = None
-        nx1, nx2 = ms.nx[0], ms.nx[1]
-        # (variant, rows per tile, particles per pass): one thread per source cell, tiles
-        # of up to 256 cells, particle ranges copied in passes of 1016..4088
-        cands = [(0, r, ch) for r in (1, 2, 4) if nx2 % r == 0 and r * nx1 <= 256
-                 for ch in (1152, 2048, 2176, 2304, 0)]
-        for var, rows, chunk in cands:
-            mx.set_tiles(rows, chunk, var)
-            try:
-                t = timed_cycles(lambda: mx.imex_cycle(dt), 1, stream)
-            except RuntimeError:
-                continue
-            if best is None or t < best[0]:
-                best = (t, rows, chunk, var)
-        mx.set_tiles(best[1], best[2], best[3])
-        res["tuned"] = {"variant": best[3], "rows_per_tile": best[1], "chunk": best[2],
-                        "cycle_ms": round(best[0], 3)}
-        restore(dev, snap)
-        mx.import_()
+        # the library's autotuner (dustb_mixed_tune) on this workspace: rows per tile,
+        # particles per pass, persistent work-queue CTAs or one CTA per tile
+        rows, chunk, grid, tms = mx.tune(GAMMA * dt)
+        res["tuned"] = {"rows_per_tile": rows, "chunk": chunk,
+                        "launch": "one CTA per tile" if grid else "persistent CTAs, work queue",
+                        "qp_plus_operator_ms": round(tms, 3), "by": "dustb_mixed_tune"}
     for _ in range(args.warmup):
         mx.imex_cycle(dt)
     # the timed steps replay one captured cycle (a CUDA graph of its kernel launches)

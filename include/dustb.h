@@ -436,6 +436,9 @@ int dustb_phst(const dustb_ctx *ctx, const double *chi_max, double *row, void *s
  * No reference counterpart: the reference keeps only the FP64 SoA. */
 
 enum { DUSTB_MIXED_PROBE_COPY_TIMEOUT = 7 };
+/* variant flag: the tile kernels as one CTA per tile instead of persistent CTAs taking the
+ * tiles, heaviest first, from a device work queue (the default) */
+#define DUSTB_MIXED_GRID_TILES 8
 
 typedef struct dustb_mixed_params {
   double dx[3];            /* uniform cell size (single-level mesh) */
@@ -444,10 +447,11 @@ typedef struct dustb_mixed_params {
                               pass), a multiple of 4 in 64..8192; 0: the largest that keeps
                               as many CTAs per SM as their registers allow (2380 for tiles
                               of 128 cells) */
-  int variant;             /* 0; DUSTB_MIXED_PROBE_COPY_TIMEOUT: a failure-detection test
-                              hook (the first tile of every deposit launch never issues its
-                              first copy: its bounded wait runs out, the tile returns and
-                              sets DUSTB_ERR_TIMEOUT) */
+  int variant;             /* 0, or DUSTB_MIXED_GRID_TILES; DUSTB_MIXED_PROBE_COPY_TIMEOUT (with
+                              or without the flag): a failure-detection test
+                              hook (the first tile CTA 0 takes in every deposit launch never
+                              issues its first copy: its bounded wait runs out, the CTA returns
+                              and sets DUSTB_ERR_TIMEOUT) */
   double *x3_removed;      /* device (mass, count) of the particles removed at outflow x3
                               faces, accumulated; required when mesh.x3bc is
                               DUSTB_X3_OUTFLOW, else may be NULL */
@@ -502,6 +506,21 @@ int dustb_mixed_imex_cycle(const dustb_ctx *ctx, const dustb_mixed_params *mp, v
  * applies the imex cycle's pending consistent kick). */
 int dustb_mixed_pc2_cycle(const dustb_ctx *ctx, const dustb_mixed_params *mp, void *ws,
                           long long ws_bytes, double dt, double *chi_max, void *stream);
+
+/* The autotuner of the tile kernels: times the candidate tile shapes -- rows per tile (1,
+ * 2, 4, 8 where they divide nx2 and give at most 256 cells), particles per pass (the default,
+ * 2304, 4096, 4608) and the launch form (persistent CTAs on the device work queue or one CTA
+ * per tile) -- with the Q/P and dc1 operator tiles on the caller's shadow and workspace as
+ * they stand (after an import or a cycle), and writes the fastest into mp (rows_per_tile,
+ * chunk, the DUSTB_MIXED_GRID_TILES flag of variant; *best_ms, if given, its time per Q/P +
+ * operator pair).  It changes no particle or gas state: the tiles write only the stage
+ * scratch fields qdep, the centre mass of imex_resid and work, which every cycle rewrites
+ * before reading them.  Synchronous (it waits for its events); not inside a stream capture
+ * and not while dustb_mixed_timing is on (DUSTB_EUNSUP).  The reference has no counterpart
+ * (its kernels take Kokkos' default launch shapes); the counting sort has one bucket per
+ * cell, so there is no sort-bucket width to tune. */
+int dustb_mixed_tune(const dustb_ctx *ctx, dustb_mixed_params *mp, void *ws, long long ws_bytes,
+                     double a_dt, double *best_ms, void *stream);
 
 /* Re-sorts the shadow by cell (the SortParticles of the shadow; the reference rows keep
  * their order, export writes each particle back to its own row). */

@@ -398,3 +398,67 @@ def test_copy_wait_timeout_is_reported_and_recoverable():
     clean.export()
     torch.cuda.synchronize()
     assert clean.error_word() == 0
+
+
+def test_uneven_blocks_from_the_work_queue():
+    """Four MeshBlocks stacked in x3 around a Gaussian particle layer (scale 0.009 of a box
+    of 0.1): the inner blocks hold more than 100 times the particles of the outer ones and
+    the midplane cells ~70 each (tiles of several passes, split cells).  The persistent
+    tile launches taking the tiles heaviest first from the device work queue match the FP64
+    form to the per-particle tolerance (the plain back-reaction: a step continuous in the
+    positions, so the bar holds for every one of the 1,048,576 particles), and the
+    one-CTA-per-tile launches to FP32 rounding."""
+    from athenak_b200.drag import DeviceDust
+    from athenak_b200.mixed import MixedDust
+    ms = uniform_mesh((32, 32, 64), (32, 32, 16), 2, (-0.05,) * 3, (0.05,) * 3)
+    st = make_state(ms, [0.01, 0.3], [1.0, 0.5], 8, seed=21, hp=0.009, vel_noise=0.03,
+                    gas_noise=1e-2)
+    counts = np.bincount(st.pi[0, :st.npart], minlength=ms.nmb)
+    assert counts.min() > 0 and counts.max() > 100 * counts.min(), counts
+    phys = dict(scheme=2, drag_solver=2, consistent_gas=False)
+    ref = DeviceDust(st, phys)
+    mq = MixedDust(st, phys)                    # the work queue (default)
+    mg = MixedDust(st, phys, variant=8)         # DUSTB_MIXED_GRID_TILES: one CTA per tile
+    dt = 2e-3
+    for _ in range(3):
+        ref.imex_cycle(dt)
+        mq.imex_cycle(dt)
+        mg.imex_cycle(dt)
+    mq.export()
+    mg.export()
+    torch.cuda.synchronize()
+    check(st, ref, mq, None)
+    a, b = mq.dev.host("pr"), mg.dev.host("pr")
+    vscale = np.abs(b[[1, 3, 5]]).max()
+    for r in (1, 3, 5):
+        assert np.abs(a[r] - b[r]).max() < 1e-6 * vscale, r
+    assert mg.error_word() == 0
+
+
+def test_library_autotuner_keeps_the_results():
+    """dustb_mixed_tune picks a tile shape and launch form on the caller's workspace without
+    changing the state: cycles after tuning match cycles with the default shape to FP32
+    rounding of the sums' order, and match the FP64 form."""
+    from athenak_b200.mixed import MixedDust
+    c = CASES["3d_random"]
+    ms = uniform_mesh(*c["mesh"])
+    st = make_state(ms, **c["st"])
+    a = MixedDust(st, c["phys"])
+    b = MixedDust(st, c["phys"])
+    rows, chunk, grid, tms = a.tune(1.7 * c["dt"])
+    assert rows in (1, 2, 4, 8) and tms > 0.0
+    from athenak_b200.drag import DeviceDust
+    ref = DeviceDust(st, c["phys"])
+    for _ in range(3):
+        a.imex_cycle(c["dt"])
+        b.imex_cycle(c["dt"])
+        ref.imex_cycle(c["dt"])
+    a.export()
+    b.export()
+    torch.cuda.synchronize()
+    assert a.error_word() == 0 and b.error_word() == 0
+    pa, pb = a.dev.host("pr"), b.dev.host("pr")
+    vscale = np.abs(pb[[1, 3, 5]]).max()
+    for r in (1, 3, 5):
+        assert np.abs(pa[r] - pb[r]).max() < 1e-6 * vscale, r
+    check(st, ref, a, c)
