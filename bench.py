@@ -271,6 +271,8 @@ def run_ours(args, rep):
     # ---- mixed form ----
     mx = MixedDust(dev=dev, do_import=False)
     mx.import_()
+    if args.grid_tiles:
+        mx.set_tiles(0, 0, 8)                   # DUSTB_MIXED_GRID_TILES
     if args.tune:
         # the library's autotuner (dustb_mixed_tune) on this workspace: rows per tile,
         # particles per pass, persistent work-queue CTAs or one CTA per tile
@@ -777,6 +779,8 @@ def main():
     ap.add_argument("--small", action="store_true", help="a 64^3 test workload")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="skip the tile-shape autotuner (rows per tile, particles per pass)")
+    ap.add_argument("--grid-tiles", action="store_true",
+                    help="one CTA per tile instead of the work queue (profiling cases)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cells", type=int, default=0,
