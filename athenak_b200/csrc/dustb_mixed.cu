@@ -994,14 +994,17 @@ struct GatherWindow {
           z[c][b][a] = v.z;
         }
   }
-  // u = sum over (c, b) of wz_c wy_b (sum over a of wx_a g_cba)
+  // u = sum over c of wz_c (sum over b of wy_b (sum over a of wx_a g_cba)): the three
+  // directions one after the other, so the dependent chains are three FMAs long and the
+  // planes' partial sums are independent of one another
   __device__ __forceinline__ void gather(const float wx[3], const float wy[3], const float wz[3],
                                          float2 &uxy, float &uz) const {
-    uxy = make_float2(0.0f, 0.0f);
-    uz = 0.0f;
+    float2 pxy[WK];
+    float pz[WK];
 #pragma unroll
     for (int c = 0; c < WK; ++c) {
-      const float wzc = D3 ? wz[c] : 1.0f;
+      float2 sxy = make_float2(0.0f, 0.0f);
+      float sz = 0.0f;
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
         float2 txy = __fmul2_rn(dup(wx[0]), xy[c][b][0]);
@@ -1011,10 +1014,23 @@ struct GatherWindow {
           txy = __ffma2_rn(dup(wx[a]), xy[c][b][a], txy);
           tz = fmaf(wx[a], z[c][b][a], tz);
         }
-        const float wzy = wzc * wy[b];
-        uxy = __ffma2_rn(dup(wzy), txy, uxy);
-        uz = fmaf(wzy, tz, uz);
+        sxy = __ffma2_rn(dup(wy[b]), txy, sxy);
+        sz = fmaf(wy[b], tz, sz);
       }
+      pxy[c] = sxy;
+      pz[c] = sz;
+    }
+    if (D3) {
+      uxy = __fmul2_rn(dup(wz[0]), pxy[0]);
+      uz = wz[0] * pz[0];
+#pragma unroll
+      for (int c = 1; c < WK; ++c) {
+        uxy = __ffma2_rn(dup(wz[c]), pxy[c], uxy);
+        uz = fmaf(wz[c], pz[c], uz);
+      }
+    } else {
+      uxy = pxy[0];
+      uz = pz[0];
     }
   }
 };
