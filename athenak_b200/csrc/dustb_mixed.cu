@@ -414,8 +414,9 @@ __global__ void k_export(double *pr, int *pi, long long stride, int n, PBuf A, G
   W(DUSTB_IPVX, vel[0]); W(DUSTB_IPVY, vel[1]); W(DUSTB_IPVZ, vel[2]);
   W(DUSTB_IPVX1, A.f[F_WX][q]); W(DUSTB_IPVY1, A.f[F_WY][q]); W(DUSTB_IPVZ1, A.f[F_WZ][q]);
   W(DUSTB_IPRX, rate[0]); W(DUSTB_IPRY, rate[1]); W(DUSTB_IPRZ, rate[2]);
-  // (the FP64 mass stays, unless an outflow face removed the particle)
-  if (A.f[F_M][q] == 0.0f) W(DUSTB_IPM, 0.0);
+  // the mass as the mixed form carries it (FP32; 0 for a particle an outflow face removed),
+  // so that the rows' momentum is the momentum the cycles exchanged with the gas
+  W(DUSTB_IPM, (double)A.f[F_M][q]);
   pi[(long long)DUSTB_PGID * stride + p] = m + G.gids;
 }
 
@@ -1072,6 +1073,7 @@ __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, co
   constexpr int WK = D3 ? 3 : 1;
   const int nx1 = G.nx1, nct = tj * nx1;
   const int WI = nx1 + 2, WJ = tj + 2, nplane = WJ * WI;
+  const double vinv = 1.0 / G.vol;                 // (every deposited value is per unit volume)
   for (int t = threadIdx.x; t < WK * nplane; t += blockDim.x) {
     const int c = t / nplane, rem = t - c * nplane;
     const int wy = rem / WI, wx = rem - wy * WI;
@@ -1100,10 +1102,10 @@ __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, co
       }
     }
     double *f = T.dfield + at;
-    if (s.x != 0.0f) atomicAdd(f, (double)s.x);
-    if (s.y != 0.0f) atomicAdd(f + G.vstride, (double)s.y);
-    if (s.z != 0.0f) atomicAdd(f + 2 * G.vstride, (double)s.z);
-    if (NC > 3 && s.w != 0.0f) atomicAdd(f + 3 * G.vstride, (double)s.w);
+    if (s.x != 0.0f) atomicAdd(f, (double)s.x * vinv);
+    if (s.y != 0.0f) atomicAdd(f + G.vstride, (double)s.y * vinv);
+    if (s.z != 0.0f) atomicAdd(f + 2 * G.vstride, (double)s.z * vinv);
+    if (NC > 3 && s.w != 0.0f) atomicAdd(f + 3 * G.vstride, (double)s.w * vinv);
   }
 }
 
@@ -1122,6 +1124,7 @@ __device__ __forceinline__ void add_window_cells(const float4 *s_acc, const Geo 
                                                  int cj, int ci) {
   constexpr bool V4 = FourValues<MODE>::value;
   const int nx1 = G.nx1, nct = tj * nx1;
+  const double vinv = 1.0 / G.vol;                 // (every deposited value is per unit volume)
   auto put = [&](const float4 &v, int kt, int jt, int it) {
     long long at;
     if ((unsigned)kt < (unsigned)G.nx3 && (unsigned)jt < (unsigned)G.nx2 &&
@@ -1131,10 +1134,10 @@ __device__ __forceinline__ void add_window_cells(const float4 *s_acc, const Geo 
       at = cell_at<GH>(G, m, T.dnvar, kt, jt, it);
     if (at < 0) return;
     double *f = T.dfield + at;
-    if (v.x != 0.0f) atomicAdd(f, (double)v.x);
-    if (v.y != 0.0f) atomicAdd(f + G.vstride, (double)v.y);
-    if (v.z != 0.0f) atomicAdd(f + 2 * G.vstride, (double)v.z);
-    if (V4 && v.w != 0.0f) atomicAdd(f + 3 * G.vstride, (double)v.w);
+    if (v.x != 0.0f) atomicAdd(f, (double)v.x * vinv);
+    if (v.y != 0.0f) atomicAdd(f + G.vstride, (double)v.y * vinv);
+    if (v.z != 0.0f) atomicAdd(f + 2 * G.vstride, (double)v.z * vinv);
+    if (V4 && v.w != 0.0f) atomicAdd(f + 3 * G.vstride, (double)v.w * vinv);
   };
   auto acc = [](float4 &s, const float4 &v) { s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w; };
   const int wy_lo = (cj == 0) ? 0 : cj + 1, wy_hi = (cj == tj - 1) ? tj + 1 : cj + 1;
@@ -1300,7 +1303,6 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
     if (MODE == MODE_QP) s_qt[tid] = 0.0f;
     cta_sync(wmask);
     const int P0 = s_cs[0], P1 = s_cs[nct];
-    const float inv_vol = (float)(1.0 / G.vol);
     const float inv_adt = (float)(1.0 / T.a_dt);
     const int CHP = CH - 8;                          // particles per pass (room to round out)
     const bool single = (P1 - P0) <= CHP;            // the whole tile in one pass
@@ -1384,7 +1386,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
           wts(SCHEME, s_f[r], wx_);
           wts(SCHEME, oy_at(r), wy_);
           if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
-          const float mc = s_f[4 * CH + r] * s_f[3 * CH + r] * inv_vol;
+          const float mc = s_f[4 * CH + r] * s_f[3 * CH + r];
           qt += mc;
           qp.add(wx_, wy_, wz_, make_float2(mc, mc * s_f[5 * CH + r]),
                  make_float2(mc * s_f[6 * CH + r], mc * s_f[7 * CH + r]));
@@ -1412,12 +1414,12 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
           win.gather(wx_, wy_, wz_, uxy, uz);
           const float c32 = s_f[3 * CH + r];
           if (MODE == MODE_OP) {
-            const float mc = s_f[4 * CH + r] * c32 * inv_vol;
+            const float mc = s_f[4 * CH + r] * c32;
             s_f[5 * CH + r] = mc * uxy.x; s_f[6 * CH + r] = mc * uxy.y; s_f[7 * CH + r] = mc * uz;
           } else if (MODE == MODE_PRED) {
             // dust_pc2_predictor (src/dust/dust_pm.cpp:141-193): rate m/(t_s V), impulse
             // -dt rate (u - v) from the old gas velocity m/rho of u1
-            const float rate = s_f[4 * CH + r] * inv_vol / c32;
+            const float rate = s_f[4 * CH + r] / c32;
             const float vx = s_f[5 * CH + r], vy = s_f[6 * CH + r], vz = s_f[7 * CH + r];
             const float g = -T.pc.dt * rate;
             s_f[3 * CH + r] = rate;
@@ -1476,7 +1478,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
             S.f[F_AY][p] += disp[1] * (float)G.inv_dx[1];
             if (D3) S.f[F_AZ][p] += disp[2] * (float)G.inv_dx[2];
             S.f[F_RX][p] = dv[0]; S.f[F_RY][p] = dv[1]; S.f[F_RZ][p] = dv[2];
-            const float f = -s_f[4 * CH + s] * inv_vol;
+            const float f = -s_f[4 * CH + s];
             s_f[5 * CH + s] = f * dv[0]; s_f[6 * CH + s] = f * dv[1]; s_f[7 * CH + s] = f * dv[2];
           }
           cta_sync(wmask);
@@ -1490,7 +1492,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
             wts(SCHEME, s_f[r], wx_);
             wts(SCHEME, oy_at(r), wy_);
             if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
-            const float f = (MODE == MODE_KICK) ? -s_f[4 * CH + r] * inv_vol : 1.0f;
+            const float f = (MODE == MODE_KICK) ? -s_f[4 * CH + r] : 1.0f;
             sums.add(wx_, wy_, wz_, make_float2(f * s_f[5 * CH + r], f * s_f[6 * CH + r]),
                      make_float2(f * s_f[7 * CH + r], (MODE == MODE_PRED) ? s_f[3 * CH + r] : 0.0f));
           }
@@ -1512,7 +1514,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       // centre mass m c / V of the cell (dust_imex_point_center_mass): only this cell's
       // particles have it as their centre, so it is stored, not added
       const int cj = tid / nx1, ci = tid - cj * nx1;
-      T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj, G.is + ci)] = (double)s_qt[tid];
+      T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj, G.is + ci)] = (double)s_qt[tid] / G.vol;
     }
     // (every thread is done with this tile's shared memory before the next tile's copies)
     cta_sync(wmask);
@@ -1574,7 +1576,7 @@ __global__ void k_gas_velocity(const double *u, int nv, double *out, long long p
 template <int SCHEME>
 __global__ void __launch_bounds__(kT) k_pc2_edge(PBuf S, Geo G, TileArgs T) {
   const int e0 = T.cstart[G.ncell], e1 = T.cstart[G.ncell + 1];
-  const float inv_vol = (float)(1.0 / G.vol);
+  const double vinv = 1.0 / G.vol;
   const int nax = G.three_d ? 3 : 2;
   for (int p = e0 + blockIdx.x * blockDim.x + threadIdx.x; p < e1; p += gridDim.x * blockDim.x) {
     int m, k, j, i;
@@ -1623,7 +1625,7 @@ __global__ void __launch_bounds__(kT) k_pc2_edge(PBuf S, Geo G, TileArgs T) {
     if (G.three_d) S.f[F_AZ][p] += disp[2] * (float)G.inv_dx[2];
     S.f[F_RX][p] = dv[0]; S.f[F_RY][p] = dv[1]; S.f[F_RZ][p] = dv[2];
     if (!T.deposit) continue;
-    const float f = -S.f[F_M][p] * inv_vol;
+    const float f = -S.f[F_M][p];
     for (int c = clo; c <= chi; ++c)
       for (int b = 0; b < 3; ++b)
         for (int a = 0; a < 3; ++a) {
@@ -1631,9 +1633,9 @@ __global__ void __launch_bounds__(kT) k_pc2_edge(PBuf S, Geo G, TileArgs T) {
           if (wt == 0.0f) continue;
           const long long at = G.at(m, 3, 0, G.three_d ? G.ks + ig[2] - 1 + c : G.ks,
                                     G.js + ig[1] - 1 + b, G.is + ig[0] - 1 + a);
-          atomicAdd(&T.dfield[at], (double)(wt * dv[0]));
-          atomicAdd(&T.dfield[at + G.vstride], (double)(wt * dv[1]));
-          atomicAdd(&T.dfield[at + 2 * G.vstride], (double)(wt * dv[2]));
+          atomicAdd(&T.dfield[at], (double)(wt * dv[0]) * vinv);
+          atomicAdd(&T.dfield[at + G.vstride], (double)(wt * dv[1]) * vinv);
+          atomicAdd(&T.dfield[at + 2 * G.vstride], (double)(wt * dv[2]) * vinv);
         }
   }
 }
@@ -1646,7 +1648,7 @@ __global__ void __launch_bounds__(kT) k_pc2_edge(PBuf S, Geo G, TileArgs T) {
 template <int MODE, int SCHEME, int GH>
 __global__ void __launch_bounds__(kT) k_shift_edge(PBuf S, Geo G, TileArgs T) {
   const int e0 = T.cstart[G.ncell], e1 = T.cstart[G.ncell + 1];
-  const float inv_vol = (float)(1.0 / G.vol);
+  const double vinv = 1.0 / G.vol;
   const float inv_adt = (float)(1.0 / T.a_dt);
   for (int p = e0 + blockIdx.x * blockDim.x + threadIdx.x; p < e1; p += gridDim.x * blockDim.x) {
     int m, k, j, i;
@@ -1660,7 +1662,7 @@ __global__ void __launch_bounds__(kT) k_shift_edge(PBuf S, Geo G, TileArgs T) {
     float wx[3], wy[3], wz[3];
     wts(SCHEME, ox, wx); wts(SCHEME, oy, wy); wts(SCHEME, S.f[F_OZ][p], wz);
     const float cc = S.f[F_CC][p], mass = S.f[F_M][p];
-    const float mc = mass * cc * inv_vol;
+    const float mc = mass * cc;
     if (MODE == MODE_QP) {
       const float v[3] = {S.f[F_VX][p], S.f[F_VY][p], S.f[F_VZ][p]};
       for (int c = 0; c < 3; ++c)
@@ -1670,12 +1672,12 @@ __global__ void __launch_bounds__(kT) k_shift_edge(PBuf S, Geo G, TileArgs T) {
             if (w == 0.0f) continue;
             const long long at = cell_at<GH>(G, m, T.dnvar, k - 1 + c, jc - 1 + b, i - 1 + a);
             if (at < 0) continue;
-            atomicAdd(&T.dfield[at], (double)w);
-            atomicAdd(&T.dfield[at + G.vstride], (double)(w * v[0]));
-            atomicAdd(&T.dfield[at + 2 * G.vstride], (double)(w * v[1]));
-            atomicAdd(&T.dfield[at + 3 * G.vstride], (double)(w * v[2]));
+            atomicAdd(&T.dfield[at], (double)w * vinv);
+            atomicAdd(&T.dfield[at + G.vstride], (double)(w * v[0]) * vinv);
+            atomicAdd(&T.dfield[at + 2 * G.vstride], (double)(w * v[1]) * vinv);
+            atomicAdd(&T.dfield[at + 3 * G.vstride], (double)(w * v[2]) * vinv);
           }
-      atomicAdd(&T.res[G.at(m, 4, 3, G.ks + k, G.js + j, G.is + i)], (double)mc);
+      atomicAdd(&T.res[G.at(m, 4, 3, G.ks + k, G.js + j, G.is + i)], (double)mc * vinv);
       continue;
     }
     float u[3] = {0.0f, 0.0f, 0.0f};
@@ -1699,7 +1701,7 @@ __global__ void __launch_bounds__(kT) k_shift_edge(PBuf S, Geo G, TileArgs T) {
       S.f[F_VX][p] = v0[0] + val[0]; S.f[F_VY][p] = v0[1] + val[1]; S.f[F_VZ][p] = v0[2] + val[2];
       S.f[F_RX][p] = val[0] * inv_adt; S.f[F_RY][p] = val[1] * inv_adt; S.f[F_RZ][p] = val[2] * inv_adt;
       if (!T.deposit) continue;
-      const float f = -mass * inv_vol;
+      const float f = -mass;
       for (int q = 0; q < 3; ++q) val[q] *= f;
     }
     for (int c = 0; c < 3; ++c)
@@ -1709,7 +1711,7 @@ __global__ void __launch_bounds__(kT) k_shift_edge(PBuf S, Geo G, TileArgs T) {
           if (w == 0.0f) continue;
           const long long at = cell_at<GH>(G, m, 3, k - 1 + c, jc - 1 + b, i - 1 + a);
           if (at < 0) continue;
-          for (int q = 0; q < 3; ++q) atomicAdd(&T.dfield[at + q * G.vstride], (double)(w * val[q]));
+          for (int q = 0; q < 3; ++q) atomicAdd(&T.dfield[at + q * G.vstride], (double)(w * val[q]) * vinv);
         }
   }
 }
