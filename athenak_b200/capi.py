@@ -45,6 +45,11 @@ class DustbPhysics(C.Structure):
                 ("x3_deposit_drop", C.c_int)]
 
 
+class DustbDepPlan(C.Structure):
+    _fields_ = [("nseg", C.c_int), ("seg_tgt", C.c_void_p), ("seg_ptr", C.c_void_p),
+                ("ent_src", C.c_void_p), ("ent_w", C.c_void_p)]
+
+
 class DustbCtx(C.Structure):
     _fields_ = [("mesh", DustbMesh), ("part", DustbParticles), ("f", DustbFields),
                 ("phys", DustbPhysics), ("err", C.c_void_p)]
@@ -145,6 +150,7 @@ SIGNATURES = {
     "dustb_deposit_qp": [CTXP, D, D, VP],
     "dustb_ghost_add": [CTXP, VP, I, VP],
     "dustb_ghost_copy": [CTXP, VP, I, I, VP],
+    "dustb_ghost_add_plan": [CTXP, C.POINTER(DustbDepPlan), VP, I, VP],
     "dustb_solve_ustar": [CTXP, VP],
     "dustb_dc1_sweep": [CTXP, D, D, VP],
     "dustb_gather_kick_pmbr": [CTXP, D, D, VP],

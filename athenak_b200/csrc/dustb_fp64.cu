@@ -591,6 +591,26 @@ __global__ void k_shear_add(Ind d, SBox B, double *a, int nvar) {
   a[at] += shear_add_sum(B, d, a, nvar, m, v, k, j, i);
 }
 
+// the general deposit remap of a refined mesh (GeneralApply, bvals_dep_general.cpp:1135-1175):
+// one thread per (target cell, variable), its sources summed in list order and added once.
+// Sources are ghost cells and targets active cells, so no thread reads what another writes.
+__global__ void k_dep_plan_apply(int nseg, const int *__restrict__ tgt, const int *__restrict__ ptr,
+                                 const int *__restrict__ src, const double *__restrict__ w,
+                                 double *a, int nvar, long long ncell) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nseg * nvar) return;
+  const int s = (int)(t / nvar), v = (int)(t - (long long)s * nvar);
+  double sum = 0.0;
+  for (int e = ptr[s]; e < ptr[s + 1]; ++e) {
+    const long long q = src[e];
+    const long long sm = q / ncell;
+    sum += w[e] * a[(sm * nvar + v) * ncell + (q - sm * ncell)];
+  }
+  const long long c = tgt[s];
+  const long long tm = c / ncell;
+  a[(tm * nvar + v) * ncell + (c - tm * ncell)] += sum;
+}
+
 // copy exchange: every ghost cell <- the neighbour's active cell at index - o*nx
 __global__ void k_ghost_copy(Ind d, const int *nghbr, int gids, double *a, int nvar) {
   long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1939,6 +1959,19 @@ int dustb_ghost_add(const dustb_ctx *c, double *field, int nvar, void *stream) {
         d, B, field, nvar);
   }
   return launch_status("ghost_add");
+}
+
+int dustb_ghost_add_plan(const dustb_ctx *c, const dustb_dep_plan *plan, double *field,
+                         int nvar, void *stream) {
+  CHECK_CELLS(c);
+  if (!plan || !field || nvar <= 0 || plan->nseg < 0 || !c->mesh.three_d) return DUSTB_EINVAL;
+  if (plan->nseg == 0) return DUSTB_OK;
+  if (!plan->seg_tgt || !plan->seg_ptr || !plan->ent_src || !plan->ent_w) return DUSTB_EINVAL;
+  Ind d = make_ind(c->mesh);
+  k_dep_plan_apply<<<blocks_for((long long)plan->nseg * nvar), kThreads, 0, S(stream)>>>(
+      plan->nseg, plan->seg_tgt, plan->seg_ptr, plan->ent_src, plan->ent_w, field, nvar,
+      d.cells());
+  return launch_status("ghost_add_plan");
 }
 
 int dustb_ghost_copy(const dustb_ctx *c, double *field, int nvar, int x3_bcs, void *stream) {

@@ -186,6 +186,25 @@ class DeviceDust:
     def ghost_copy(self, name, nvar, x3_bcs=1, stream=None):
         self._call("ghost_copy", self.t[name].data_ptr(), nvar, x3_bcs, stream=stream)
 
+    def set_dep_plan(self, plan):
+        """The general deposit remap of a refined mesh (athenak_b200.amr.DepPlan), copied to
+        the device; ghost_add_plan applies it."""
+        dev = dict(device=self.device)
+        self.t["plan_tgt"] = torch.from_numpy(plan.seg_tgt).to(**dev)
+        self.t["plan_ptr"] = torch.from_numpy(plan.seg_ptr).to(**dev)
+        self.t["plan_src"] = torch.from_numpy(plan.ent_src).to(**dev)
+        self.t["plan_w"] = torch.from_numpy(plan.ent_w).to(**dev)
+        self.plan = capi.DustbDepPlan(plan.nseg, self.t["plan_tgt"].data_ptr(),
+                                      self.t["plan_ptr"].data_ptr(),
+                                      self.t["plan_src"].data_ptr(),
+                                      self.t["plan_w"].data_ptr())
+
+    def ghost_add_plan(self, name, nvar, stream=None):
+        """MeshBoundaryValuesDep's general path on a refined mesh: the ghost deposits of name
+        remapped by the plan of set_dep_plan (dustb_ghost_add_plan)."""
+        self._call("ghost_add_plan", C.byref(self.plan), self.t[name].data_ptr(), nvar,
+                   stream=stream)
+
     def solve_ustar(self, stream=None):
         self._call("solve_ustar", stream=stream)
 

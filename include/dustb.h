@@ -189,6 +189,27 @@ int dustb_ghost_add(const dustb_ctx *ctx, double *field, int nvar, void *stream)
  * (src/dust/dust_tasks.cpp:445-469). */
 int dustb_ghost_copy(const dustb_ctx *ctx, double *field, int nvar, int x3_bcs, void *stream);
 
+/* The additive ghost-deposit exchange of a 3-D mesh with refinement levels: the static part
+ * of the reference's general remap (DepRemapPlan, src/bvals/bvals_dep_general.cpp:1-35; the
+ * apply is GeneralApply, :1135-1175).  Every ghost cell of every block is given to the active
+ * cells it overlaps, weight = overlap volume / target cell volume measured in finest-level
+ * cells, so the remap conserves the deposit exactly at any level difference; beyond a physical
+ * x3 face a ghost cell is mirrored back (fold) or dropped.  The plan is built on the host (the
+ * C++ host layer's dustb_host_dep_plan, athenak_b200/host/dep_plan.hpp) from the blocks'
+ * logical locations and neighbour slots; its arrays are DEVICE arrays.  Cells are flat indices
+ * m * (n3 n2 n1) + (k n2 + j) n1 + i of the padded block arrays. */
+typedef struct dustb_dep_plan {
+  int nseg;                /* target cells that receive deposits */
+  const int *seg_tgt;      /* nseg target cells, ascending */
+  const int *seg_ptr;      /* nseg + 1: the sources of target s are entries seg_ptr[s] .. */
+  const int *ent_src;      /* source ghost cell of each entry, by (source gid, source cell) */
+  const double *ent_w;     /* overlap volume / target cell volume */
+} dustb_dep_plan;
+/* field (nmb, nvar, n3, n2, n1): target += sum over its entries of w * source, summed in
+ * entry order and added once (the reference's order; FP64, bit-reproducible). */
+int dustb_ghost_add_plan(const dustb_ctx *ctx, const dustb_dep_plan *plan, double *field,
+                         int nvar, void *stream);
+
 /* GasImplicitSolve's per-cell solve (dust_pm.cpp:426-436 and the dc1 local guess,
  * dust_solver.cpp:643-649): ustar = (u0.m + P)/(rho + Q) over active cells. */
 int dustb_solve_ustar(const dustb_ctx *ctx, void *stream);

@@ -2152,3 +2152,133 @@ unsigned oracle_pc2_cycle(const dustb_ctx *c, double dt, double *chi_out, double
   if (chi_out) *chi_out = chi;
   return err;
 }
+
+/* ---- the general deposit remap of a refined 3-D mesh, by brute force ------------------------
+ * The static part of DepRemapPlan (src/bvals/bvals_dep_general.cpp:1-35, :62-160, :383-545):
+ * every ghost cell of every block is given to the active cells it overlaps, weight = overlap
+ * volume / target cell volume in finest-level units, and per target cell its sources ordered by
+ * (source gid, source cell).  The reference intersects intervals direction by direction over a
+ * target's neighbour list; this restatement instead cuts each ghost cell into finest-level unit
+ * cubes and looks each cube's owner up in a finest-level ownership grid, counting the cubes a
+ * (target cell, source cell) pair shares, which checks the neighbour-based build independently.
+ * geo: nx1..3, ng, nmb_root1..3, root_level, max_level, x3mode (0 periodic, 1 fold, 2 drop);
+ * lloc: level, lx1, lx2, lx3 per block.  Returns 0, -1 for invalid input, -3 for small capacities
+ * (the counts are written either way). */
+typedef struct { int tflat, sgid, scell; int cnt; } DepEnt;
+
+static int cmp_depent(const void *a, const void *b) {
+  const DepEnt *x = (const DepEnt *)a, *y = (const DepEnt *)b;
+  if (x->tflat != y->tflat) return x->tflat < y->tflat ? -1 : 1;
+  if (x->sgid != y->sgid) return x->sgid < y->sgid ? -1 : 1;
+  if (x->scell != y->scell) return x->scell < y->scell ? -1 : 1;
+  return 0;
+}
+
+int oracle_dep_plan(const int *geo, int nmb, const int *lloc, int *counts, int *seg_tgt,
+                    int *seg_ptr, int *ent_src, double *ent_w, long long cap_seg,
+                    long long cap_ent) {
+  const int nx[3] = {geo[0], geo[1], geo[2]}, ng = geo[3];
+  const int root = geo[7], R = geo[8], x3mode = geo[9];
+  const int nc[3] = {nx[0] + 2*ng, nx[1] + 2*ng, nx[2] + 2*ng};
+  const int ncell = nc[0]*nc[1]*nc[2];
+  long long N[3];
+  for (int d = 0; d < 3; ++d) N[d] = (long long)geo[4 + d]*nx[d]*(1LL << (R - root));
+  const long long nunit = N[0]*N[1]*N[2];
+  if (nunit <= 0 || nunit > (1LL << 28)) return -1;
+  int *own = (int *)malloc((size_t)nunit*sizeof(int));
+  for (long long u = 0; u < nunit; ++u) own[u] = -1;
+  for (int m = 0; m < nmb; ++m) {
+    const long long sc = 1LL << (R - lloc[4*m]);
+    long long lo[3];
+    for (int d = 0; d < 3; ++d) lo[d] = (long long)lloc[4*m + 1 + d]*nx[d]*sc;
+    for (long long z = lo[2]; z < lo[2] + nx[2]*sc; ++z)
+      for (long long y = lo[1]; y < lo[1] + nx[1]*sc; ++y)
+        for (long long x = lo[0]; x < lo[0] + nx[0]*sc; ++x) own[(z*N[1] + y)*N[0] + x] = m;
+  }
+  size_t cap = 1 << 20, n = 0;
+  DepEnt *e = (DepEnt *)malloc(cap*sizeof(DepEnt));
+  int rc = 0;
+  for (int m = 0; m < nmb && rc == 0; ++m) {
+    const long long sc = 1LL << (R - lloc[4*m]);
+    long long lo[3];
+    for (int d = 0; d < 3; ++d) lo[d] = (long long)lloc[4*m + 1 + d]*nx[d]*sc;
+    for (int k = 0; k < nc[2]; ++k)
+      for (int j = 0; j < nc[1]; ++j)
+        for (int i = 0; i < nc[0]; ++i) {
+          if (i >= ng && i < nc[0] - ng && j >= ng && j < nc[1] - ng && k >= ng && k < nc[2] - ng)
+            continue;
+          const int scell = (k*nc[1] + j)*nc[0] + i;
+          const long long a0[3] = {lo[0] + (i - ng)*sc, lo[1] + (j - ng)*sc, lo[2] + (k - ng)*sc};
+          for (long long dz = 0; dz < sc; ++dz)
+            for (long long dy = 0; dy < sc; ++dy)
+              for (long long dx = 0; dx < sc; ++dx) {
+                long long u[3] = {a0[0] + dx, a0[1] + dy, a0[2] + dz};
+                int drop = 0;
+                for (int d = 0; d < 3; ++d) {
+                  if (u[d] >= 0 && u[d] < N[d]) continue;
+                  if (d == 2 && x3mode != 0) {
+                    if (x3mode == 2) { drop = 1; break; }
+                    u[2] = (u[2] < 0) ? -u[2] - 1 : 2*N[2] - 1 - u[2];   /* mirror */
+                  } else {
+                    u[d] = (u[d] < 0) ? u[d] + N[d] : u[d] - N[d];
+                  }
+                }
+                if (drop) continue;
+                const int t = own[(u[2]*N[1] + u[1])*N[0] + u[0]];
+                if (t < 0) { rc = -1; continue; }
+                const long long tsc = 1LL << (R - lloc[4*t]);
+                int tc[3];
+                for (int d = 0; d < 3; ++d)
+                  tc[d] = (int)((u[d] - (long long)lloc[4*t + 1 + d]*nx[d]*tsc)/tsc) + ng;
+                if (n == cap) { cap *= 2; e = (DepEnt *)realloc(e, cap*sizeof(DepEnt)); }
+                e[n].tflat = t*ncell + (tc[2]*nc[1] + tc[1])*nc[0] + tc[0];
+                e[n].sgid = m; e[n].scell = scell; e[n].cnt = 1;
+                ++n;
+              }
+        }
+  }
+  free(own);
+  if (rc) { free(e); return rc; }
+  qsort(e, n, sizeof(DepEnt), cmp_depent);
+  /* merge the unit cubes of each (target cell, source cell) pair */
+  size_t ne = 0;
+  for (size_t q = 0; q < n; ++q) {
+    if (ne > 0 && cmp_depent(&e[ne - 1], &e[q]) == 0) { e[ne - 1].cnt += 1; continue; }
+    e[ne++] = e[q];
+  }
+  long long nseg = 0;
+  for (size_t q = 0; q < ne; ++q) if (q == 0 || e[q].tflat != e[q - 1].tflat) ++nseg;
+  counts[0] = (int)nseg; counts[1] = (int)ne; counts[2] = 0;
+  if (seg_tgt && seg_ptr && ent_src && ent_w) {
+    if (cap_seg < nseg || cap_ent < (long long)ne) { free(e); return -3; }
+    long long s = 0;
+    for (size_t q = 0; q < ne; ++q) {
+      if (q == 0 || e[q].tflat != e[q - 1].tflat) { seg_tgt[s] = e[q].tflat; seg_ptr[s] = (int)q; ++s; }
+      const int t = e[q].tflat/ncell;
+      const double tsc = (double)(1LL << (R - lloc[4*t]));
+      ent_src[q] = e[q].sgid*ncell + e[q].scell;
+      ent_w[q] = (double)e[q].cnt/(tsc*tsc*tsc);
+    }
+    seg_ptr[nseg] = (int)ne;
+  }
+  free(e);
+  return 0;
+}
+
+/* GeneralApply (src/bvals/bvals_dep_general.cpp:1135-1175): per target cell and variable the
+ * weighted sum of its sources in list order, added once; a is (nmb, nvar, n3, n2, n1) with
+ * ncell = n3 n2 n1 cells per block and variable. */
+void oracle_dep_apply(int nseg, const int *seg_tgt, const int *seg_ptr, const int *ent_src,
+                      const double *ent_w, double *a, int nvar, int ncell) {
+  for (int s = 0; s < nseg; ++s) {
+    const int tm = seg_tgt[s]/ncell, tc = seg_tgt[s] - tm*ncell;
+    for (int v = 0; v < nvar; ++v) {
+      double sum = 0.0;
+      for (int q = seg_ptr[s]; q < seg_ptr[s + 1]; ++q) {
+        const int sm = ent_src[q]/ncell, sc = ent_src[q] - sm*ncell;
+        sum += ent_w[q]*a[((size_t)sm*nvar + v)*ncell + sc];
+      }
+      a[((size_t)tm*nvar + v)*ncell + tc] += sum;
+    }
+  }
+}

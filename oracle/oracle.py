@@ -82,6 +82,8 @@ def lib():
             "oracle_cloud_apply_pmbr": ([P, D, D], None),
             "oracle_cloud_imex_cycle": ([P, D, D, VP, VP], C.c_uint),
             "oracle_cloud_pc2_cycle": ([P, D, VP, VP], C.c_uint),
+            "oracle_dep_plan": ([VP, I, VP, VP, VP, VP, VP, VP, C.c_longlong, C.c_longlong], I),
+            "oracle_dep_apply": ([I, VP, VP, VP, VP, VP, I, I], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(_lib, name)
@@ -319,3 +321,39 @@ class Oracle:
         m = pr[16, :n]
         d = np.array([(m * pr[1, :n]).sum(), (m * pr[3, :n]).sum(), (m * pr[5, :n]).sum()])
         return g, d
+
+
+def dep_plan(ms, x3mode=0):
+    """The general deposit remap of a refined 3-D mesh by the oracle's brute-force build
+    (finest-level unit cubes): an athenak_b200.amr.DepPlan."""
+    from athenak_b200.amr import DepPlan, plan_geometry
+    L = lib()
+    geo = plan_geometry(ms, x3mode)
+    lloc = np.ascontiguousarray(ms.lloc, np.int32)
+    counts = np.zeros(3, np.int32)
+    rc = L.oracle_dep_plan(geo.ctypes.data, ms.nmb, lloc.ctypes.data, counts.ctypes.data,
+                           None, None, None, None, 0, 0)
+    if rc != 0:
+        raise RuntimeError(f"oracle_dep_plan failed ({rc})")
+    nseg, nent = int(counts[0]), int(counts[1])
+    seg_tgt = np.zeros(max(nseg, 1), np.int32)
+    seg_ptr = np.zeros(nseg + 1, np.int32)
+    ent_src = np.zeros(max(nent, 1), np.int32)
+    ent_w = np.zeros(max(nent, 1), np.float64)
+    rc = L.oracle_dep_plan(geo.ctypes.data, ms.nmb, lloc.ctypes.data, counts.ctypes.data,
+                           seg_tgt.ctypes.data, seg_ptr.ctypes.data, ent_src.ctypes.data,
+                           ent_w.ctypes.data, nseg, nent)
+    if rc != 0:
+        raise RuntimeError(f"oracle_dep_plan failed ({rc})")
+    return DepPlan(seg_tgt[:nseg], seg_ptr, ent_src[:nent], ent_w[:nent])
+
+
+def dep_apply(plan, a):
+    """GeneralApply of plan to the (nmb, nvar, n3, n2, n1) array a, in place."""
+    a = np.ascontiguousarray(a) if not a.flags.c_contiguous else a
+    nvar = int(a.shape[1])
+    ncell = int(a.shape[2] * a.shape[3] * a.shape[4])
+    lib().oracle_dep_apply(plan.nseg, plan.seg_tgt.ctypes.data, plan.seg_ptr.ctypes.data,
+                           plan.ent_src.ctypes.data, plan.ent_w.ctypes.data, a.ctypes.data,
+                           nvar, ncell)
+    return a

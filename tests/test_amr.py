@@ -1,0 +1,114 @@
+"""Refined (multi-level) 3-D meshes and the general deposit remap, on the CPU.
+
+The block tree and its 56 neighbour slots follow MeshBlock::SetNeighbors
+(src/mesh/meshblock.cpp:142-420); the remap plan built by the C++ host layer
+(dustb_host_dep_plan: interval overlaps over each target's neighbour list, as
+DepRemapPlan does, src/bvals/bvals_dep_general.cpp:62-545) must equal the oracle's
+brute-force plan (finest-level unit cubes looked up in an ownership grid) entry for entry,
+and applying it must conserve the deposit exactly.
+"""
+import numpy as np
+import pytest
+
+from athenak_b200.amr import (build_dep_plan, neighbor_index, refined_mesh, refined_state,
+                              sphere_refine, X3_FOLD, X3_DROP)
+from oracle import oracle
+
+MESHES = {
+    "sphere_2lev": dict(nmbroot=(4, 4, 4), nx=(8, 8, 8), refine=sphere_refine((0.1, 0.05, -0.02),
+                                                                             (0.3, 0.15))),
+    "offcentre_4x2x2": dict(nmbroot=(4, 2, 2), nx=(8, 8, 8), lo=(-1.0, -0.5, -0.5),
+                            hi=(1.0, 0.5, 0.5), refine=sphere_refine((0.9, 0.4, 0.45), (0.4, 0.2))),
+}
+
+
+def mesh(name, x3bc=0):
+    return refined_mesh(x3bc=x3bc, **MESHES[name])
+
+
+@pytest.mark.parametrize("name", sorted(MESHES))
+def test_tree_is_balanced_and_neighbour_slots_symmetric(name):
+    ms = mesh(name)
+    assert ms.max_level == ms.root_level + 2
+    lev = ms.lloc[:, 0]
+    for m in range(ms.nmb):
+        nb = ms.nghbr56[m]
+        for s in range(56):
+            g = nb[s]
+            if g < 0:
+                continue
+            assert ms.nlev56[m, s] == lev[g]
+            assert abs(int(lev[g]) - int(lev[m])) <= 1
+            # adjacency is symmetric: the neighbour lists this block in one of its slots
+            assert m in set(ms.nghbr56[g]), (m, s, g)
+    # every face of every block is covered: the same-level slot, or four finer ones, or the
+    # coarser neighbour in this block's own sub-slot
+    for m in range(ms.nmb):
+        for o in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+            slots = [neighbor_index(*o, a, b) for b in (0, 1) for a in (0, 1)]
+            assert (ms.nghbr56[m, slots] >= 0).any()
+
+
+@pytest.mark.parametrize("x3mode", [0, X3_FOLD, X3_DROP])
+@pytest.mark.parametrize("name", sorted(MESHES))
+def test_plan_equals_the_bruteforce_oracle(name, x3mode):
+    ms = mesh(name, x3bc=0 if x3mode == 0 else 1)
+    p = build_dep_plan(ms, x3mode)
+    q = oracle.dep_plan(ms, x3mode)
+    assert p.nbad == 0
+    assert p.nseg > 0
+    for f in ("seg_tgt", "seg_ptr", "ent_src"):
+        np.testing.assert_array_equal(getattr(p, f), getattr(q, f), err_msg=f)
+    np.testing.assert_array_equal(p.ent_w, q.ent_w)
+
+
+def _field(ms, nvar, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal(ms.field_shape(nvar))
+
+
+def _integrals(ms, a):
+    """(active, ghost) integrals of every variable: sum of value times cell volume."""
+    n1, n2, n3 = ms.n
+    g = ms.ng
+    vol = (ms.mb_size[:, 6] * ms.mb_size[:, 7] * ms.mb_size[:, 8])[:, None, None, None, None]
+    act = np.zeros(a.shape, bool)
+    act[:, :, g:n3 - g, g:n2 - g, g:n1 - g] = True
+    w = a * vol
+    return (w * act).sum(axis=(0, 2, 3, 4)), (w * ~act).sum(axis=(0, 2, 3, 4))
+
+
+@pytest.mark.parametrize("x3mode", [0, X3_FOLD, X3_DROP])
+def test_remap_conserves_the_deposit(x3mode):
+    ms = mesh("sphere_2lev", x3bc=0 if x3mode == 0 else 1)
+    p = build_dep_plan(ms, x3mode)
+    a = _field(ms, 3, 5)
+    if x3mode == X3_DROP:
+        # the ghost cells beyond the physical x3 faces carry nothing (they would be dropped)
+        g, n3 = ms.ng, ms.n[2]
+        lo_face = ms.mb_size[:, 2] == ms.lo[2]
+        hi_face = ms.mb_size[:, 5] == ms.hi[2]
+        a[lo_face, :, :g] = 0.0
+        a[hi_face, :, n3 - g:] = 0.0
+    act0, gh0 = _integrals(ms, a)
+    b = oracle.dep_apply(p, a.copy())
+    act1, _ = _integrals(ms, b)
+    scale = np.abs(a).max() * ms.mb_size[:, 6:9].prod(axis=1).max() * a[0, 0].size * ms.nmb
+    np.testing.assert_allclose(act1, act0 + gh0, rtol=0, atol=1e-12 * scale)
+
+
+def test_plan_on_a_mesh_without_refinement_is_the_same_level_exchange():
+    """One level, 2x2x2 root blocks (their Z order is the lexicographic order): the general
+    remap adds the same ghost deposits as the same-level exchange, in another order."""
+    ms = refined_mesh((2, 2, 2), (8, 8, 8), 2, refine=None)
+    p = build_dep_plan(ms, 0)
+    st = refined_state(ms, [0.1], [1.0], 1, seed=3)
+    o = oracle.Oracle(st, dict(scheme=2))
+    a = _field(ms, 3, 11)
+    o.arr["work"][...] = a
+    o.ghost_add("work", 3)
+    b = oracle.dep_apply(p, a.copy())
+    g = ms.ng
+    n1, n2, n3 = ms.n
+    sl = (slice(None), slice(None), slice(g, n3 - g), slice(g, n2 - g), slice(g, n1 - g))
+    np.testing.assert_allclose(b[sl], o.arr["work"][sl], rtol=0, atol=1e-13 * np.abs(a).max())
