@@ -23,7 +23,8 @@ class DustbMesh(C.Structure):
                 ("x2max", C.c_double), ("x3min", C.c_double), ("x3max", C.c_double),
                 ("mb_size", C.c_void_p), ("nghbr", C.c_void_p),
                 ("shear_x1", C.c_int), ("sb_nb2", C.c_int), ("sb_nb3", C.c_int),
-                ("sb_gid", C.c_void_p), ("time", C.c_double)]
+                ("sb_gid", C.c_void_p), ("time", C.c_double),
+                ("mb_lev", C.c_void_p), ("nghbr_ml", C.c_void_p)]
 
 
 class DustbParticles(C.Structure):
@@ -98,6 +99,10 @@ def make_ctx(mesh, arrays, npart, stride, phys) -> DustbCtx:
     m.sb_nb2, m.sb_nb3 = mesh.nblocks[1], mesh.nblocks[2]
     m.sb_gid = ptr(arrays["sb_gid"]) if mesh.shear_x1 else None
     m.time = 0.0
+    # refined meshes: the block levels and the 56 neighbour slots
+    if arrays.get("nghbr_ml") is not None:
+        m.mb_lev = ptr(arrays["mb_lev"])
+        m.nghbr_ml = ptr(arrays["nghbr_ml"])
     c.part.pr, c.part.pi = ptr(arrays["pr"]), ptr(arrays["pi"])
     c.part.stride, c.part.npart = int(stride), int(npart)
     f = c.f

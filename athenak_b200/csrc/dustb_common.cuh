@@ -72,6 +72,19 @@ __host__ __device__ inline int dir_slot(int o1, int o2, int o3) {
   return (o3 + 1) * 9 + (o2 + 1) * 3 + (o1 + 1);
 }
 
+// the slot of direction (ix, iy, iz) and sub-slot (n1, n2) among the 56 neighbours of a block of
+// a refined 3-D mesh (NeighborIndex, src/mesh/nghbr_index.hpp:29-60): x1 faces 0-7, x2 faces
+// 8-15, x1x2 edges 16-23, x3 faces 24-31, x3x1 edges 32-39, x2x3 edges 40-47, corners 48-55
+__host__ __device__ inline int nbr_slot(int ix, int iy, int iz, int n1, int n2) {
+  const int ax = ix < 0 ? -ix : ix, ay = iy < 0 ? -iy : iy;
+  if (iz == 0) {
+    if (ix * iy == 0) return ax * 2 * (ix + 1) + ay * 2 * (iy + 5) + n1 + 2 * n2;
+    return 16 + (ix + 1) + 2 * (iy + 1) + n1;
+  }
+  if (ix * iy == 0) return 24 + ax * (ix + 9) + ay * (iy + 17) + 2 * (iz + 1) + n1 + 2 * n2;
+  return 48 + (ix + 1) / 2 + (iy + 1) + 2 * (iz + 1);
+}
+
 }  // namespace dustb
 
 // host-side error bookkeeping shared by the translation units

@@ -35,6 +35,7 @@ struct MCtx {            // mesh view
   const int *nghbr;
   int gids, scheme, three_d, multi_d;
   double x1min, x1max, x2min, x2max, x3min, x3max;
+  const int *blev, *nml;   // refined meshes: block levels and the 56 neighbour slots (or NULL)
   __device__ double s(int m, int f) const { return mb[(long long)m * 9 + f]; }
 };
 
@@ -44,7 +45,8 @@ PCtx pview(const dustb_ctx *c) {
 MCtx mview(const dustb_ctx *c) {
   const dustb_mesh &ms = c->mesh;
   return MCtx{ms.mb_size, ms.nghbr, ms.gids, c->phys.scheme, ms.three_d, ms.multi_d,
-              ms.x1min, ms.x1max, ms.x2min, ms.x2max, ms.x3min, ms.x3max};
+              ms.x1min, ms.x1max, ms.x2min, ms.x2max, ms.x3min, ms.x3max, ms.mb_lev,
+              ms.nghbr_ml};
 }
 
 __device__ __forceinline__ void weights3(const MCtx &M, const Ind &d, int m, double x,
@@ -329,7 +331,78 @@ __device__ double shear_add_sum(const SBox &B, const Ind &d, const double *a, in
   return sum;
 }
 
-// ---- SetNewPrtclGID, src/bvals/bvals_part.cpp:159-429 (single level, no shear x1) -------
+// SetNewPrtclGID's neighbour on a refined mesh (src/bvals/bvals_part.cpp:312-394): the slot of
+// the crossing direction (ix, iy, iz); a finer neighbour's sub-slot from the half (fx, fy, fz)
+// of the block the particle leaves from; the first filled sub-slot of the direction; an empty
+// edge or corner is covered by a coarser block stored under the lower-dimensional direction
+// that keeps the components leaving this block's parent.  -1 if no slot holds a block.
+__device__ int route_slot_ml(const MCtx &M, int m, int ix, int iy, int iz, int fx, int fy,
+                             int fz) {
+  const int *nb = M.nml + (long long)m * 56;
+  const int mylevel = M.blev[m];
+  auto lev_of = [&](int slot) {
+    const int g = nb[slot] - M.gids;
+    return (nb[slot] >= 0 && g >= 0) ? M.blev[g] : -1;
+  };
+  auto filled = [&](int jx, int jy, int jz, int k) {
+    const int nd = abs(jx) + abs(jy) + abs(jz);
+    const int end = nbr_slot(jx, jy, jz, 0, 0) + ((nd == 1) ? 4 : ((nd == 2) ? 2 : 1));
+    for (; k < end; ++k)
+      if (nb[k] >= 0) return k;
+    return -1;
+  };
+  auto coarse_cover = [&](int jx, int jy, int jz) {
+    const double lx = M.s(m, X1MAX) - M.s(m, X1MIN), ly = M.s(m, X2MAX) - M.s(m, X2MIN);
+    const double lz = M.s(m, X3MAX) - M.s(m, X3MIN);
+    const int l1 = (int)floor((M.s(m, X1MIN) - M.x1min) / lx + 0.5);
+    const int l2 = (int)floor((M.s(m, X2MIN) - M.x2min) / ly + 0.5);
+    const int l3 = (int)floor((M.s(m, X3MIN) - M.x3min) / lz + 0.5);
+    const int kx = (jx == 0 || ((l1 & 1) == ((jx > 0) ? 1 : 0))) ? jx : 0;
+    const int ky = (jy == 0 || ((l2 & 1) == ((jy > 0) ? 1 : 0))) ? jy : 0;
+    const int kz = (jz == 0 || ((l3 & 1) == ((jz > 0) ? 1 : 0))) ? jz : 0;
+    if (abs(kx) + abs(ky) + abs(kz) == 0 || (kx == jx && ky == jy && kz == jz)) return -1;
+    return filled(kx, ky, kz, nbr_slot(kx, ky, kz, 0, 0));
+  };
+  int s;
+  if (iz == 0) {
+    if (iy == 0) {                                          // x1 face
+      s = nbr_slot(ix, 0, 0, 0, 0);
+      if (lev_of(s) > mylevel) s = nbr_slot(ix, 0, 0, fy, fz);
+      s = filled(ix, 0, 0, s);
+    } else if (ix == 0) {                                   // x2 face
+      s = nbr_slot(0, iy, 0, 0, 0);
+      if (lev_of(s) > mylevel) s = nbr_slot(0, iy, 0, fx, fz);
+      s = filled(0, iy, 0, s);
+    } else {                                                // x1x2 edge
+      s = nbr_slot(ix, iy, 0, 0, 0);
+      if (lev_of(s) > mylevel) s = nbr_slot(ix, iy, 0, fz, 0);
+      s = filled(ix, iy, 0, s);
+      if (s < 0) s = coarse_cover(ix, iy, 0);
+    }
+  } else if (iy == 0) {
+    if (ix == 0) {                                          // x3 face
+      s = nbr_slot(0, 0, iz, 0, 0);
+      if (lev_of(s) > mylevel) s = nbr_slot(0, 0, iz, fx, fy);
+      s = filled(0, 0, iz, s);
+    } else {                                                // x3x1 edge
+      s = nbr_slot(ix, 0, iz, 0, 0);
+      if (lev_of(s) > mylevel) s = nbr_slot(ix, 0, iz, fy, 0);
+      s = filled(ix, 0, iz, s);
+      if (s < 0) s = coarse_cover(ix, 0, iz);
+    }
+  } else if (ix == 0) {                                     // x2x3 edge
+    s = nbr_slot(0, iy, iz, 0, 0);
+    if (lev_of(s) > mylevel) s = nbr_slot(0, iy, iz, fx, 0);
+    s = filled(0, iy, iz, s);
+    if (s < 0) s = coarse_cover(0, iy, iz);
+  } else {                                                  // corner
+    s = filled(ix, iy, iz, nbr_slot(ix, iy, iz, 0, 0));
+    if (s < 0) s = coarse_cover(ix, iy, iz);
+  }
+  return s;
+}
+
+// ---- SetNewPrtclGID, src/bvals/bvals_part.cpp:159-429 (any levels with M.nml) -------------
 __global__ void k_route(PCtx P, MCtx M, Ind d, int x3bc, double *x3rem, unsigned *err, SBox B) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
@@ -410,7 +483,17 @@ __global__ void k_route(PCtx P, MCtx M, Ind d, int x3bc, double *x3rem, unsigned
     P.i(DUSTB_PGID, p) = B.sb_gid[((long long)(cross_in ? 1 : 0) * B.nb3 + b3) * B.nb2 + b2];
     return;
   }
-  const int gid = M.nghbr[(long long)m * 27 + dir_slot(ix, iy, iz)];
+  int gid;
+  if (M.nml) {
+    // (the half of the block the particle leaves from: sub-slots of finer neighbours)
+    const int fx = (x1 < 0.5 * (M.s(m, X1MIN) + M.s(m, X1MAX))) ? 0 : 1;
+    const int fy = (x2 < 0.5 * (M.s(m, X2MIN) + M.s(m, X2MAX))) ? 0 : 1;
+    const int fz = (x3 < 0.5 * (M.s(m, X3MIN) + M.s(m, X3MAX))) ? 0 : 1;
+    const int s = route_slot_ml(M, m, ix, iy, iz, fx, fy, fz);
+    gid = (s < 0) ? -1 : M.nml[(long long)m * 56 + s];
+  } else {
+    gid = M.nghbr[(long long)m * 27 + dir_slot(ix, iy, iz)];
+  }
   if (gid < 0) { report(err, DUSTB_ERR_NGHBR); return; }
   P.i(DUSTB_PGID, p) = gid;
   const double Lx = M.x1max - M.x1min, Ly = M.x2max - M.x2min, Lz = M.x3max - M.x3min;
@@ -1932,6 +2015,9 @@ int dustb_route(const dustb_ctx *c, double *x3_removed, void *stream) {
   Ind d = make_ind(c->mesh);
   const SBox B = sbview(c);
   if (B.on && (!B.sb_gid || B.nb2 <= 0 || B.nb3 <= 0)) return DUSTB_EINVAL;
+  // refined meshes: 3-D, both tables, no shear-periodic faces (their maps are single-level)
+  if ((c->mesh.nghbr_ml != nullptr) != (c->mesh.mb_lev != nullptr)) return DUSTB_EINVAL;
+  if (c->mesh.nghbr_ml && (!c->mesh.three_d || B.on)) return DUSTB_EUNSUP;
   k_route<<<PGRID(c)>>>(pview(c), mview(c), d, c->mesh.x3bc, x3_removed, c->err, B);
   return launch_status("route");
 }
@@ -1948,6 +2034,7 @@ int dustb_deposit_qp(const dustb_ctx *c, double a_dt, double sh, void *stream) {
 int dustb_ghost_add(const dustb_ctx *c, double *field, int nvar, void *stream) {
   CHECK_CELLS(c);
   if (!field || nvar <= 0) return DUSTB_EINVAL;
+  if (c->mesh.nghbr_ml) return DUSTB_EUNSUP;        // refined: dustb_ghost_add_plan
   Ind d = make_ind(c->mesh);
   const int fold = d.three_d && c->mesh.x3bc != DUSTB_X3_PERIODIC && !c->phys.x3_deposit_drop;
   const SBox B = sbview(c);
@@ -1977,6 +2064,7 @@ int dustb_ghost_add_plan(const dustb_ctx *c, const dustb_dep_plan *plan, double 
 int dustb_ghost_copy(const dustb_ctx *c, double *field, int nvar, int x3_bcs, void *stream) {
   CHECK_CELLS(c);
   if (!field || nvar <= 0) return DUSTB_EINVAL;
+  if (c->mesh.nghbr_ml) return DUSTB_EUNSUP;        // (no prolongation across levels)
   Ind d = make_ind(c->mesh);
   k_ghost_copy<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->mesh.nghbr, c->mesh.gids, field, nvar);
   const SBox B = sbview(c);

@@ -1904,6 +1904,7 @@ bool rows_attached(const dustb_ctx *c) {
 
 bool params_ok(const dustb_ctx *c, const dustb_mixed_params *mp) {
   if (!dustb_cells::ctx_valid(c) || !mp) return false;
+  if (c->mesh.nghbr_ml) return false;                // (single-level meshes only)
   for (int a = 0; a < 3; ++a)
     if (!(mp->dx[a] > 0.0)) return false;
   if (ncell_of(c->mesh) >= (1LL << 31) - 2) return false;   // (cells and the edge bin)

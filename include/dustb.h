@@ -100,6 +100,14 @@ typedef struct dustb_mesh {
                               at (b3, b2) (the ShearingBox x1 boundary maps, bvals_part.cpp
                               sgid_map) */
   double time;             /* mesh time of the cycle (the offset of every stage's remaps) */
+  /* refined meshes (blocks of several levels, 3-D); both NULL on a single-level mesh.  With
+   * them dustb_route hands particles to neighbours of any level, the deposits are exchanged by
+   * dustb_ghost_add_plan, and the entry points that assume one level (dustb_ghost_add,
+   * dustb_ghost_copy, the cycles, the mixed form) return DUSTB_EUNSUP. */
+  const int *mb_lev;       /* nmb: level of each block (pmb->mb_lev) */
+  const int *nghbr_ml;     /* nmb x 56: gid in every NeighborIndex slot of pmb->nghbr (four
+                              sub-slots per face, two per edge, one per corner;
+                              src/mesh/nghbr_index.hpp:20-60), -1 where the slot is empty */
 } dustb_mesh;
 
 typedef struct dustb_particles {

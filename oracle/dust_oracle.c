@@ -271,15 +271,29 @@ unsigned oracle_route(const dustb_ctx *c, double *x3_removed) {
       PI(DUSTB_PGID, p) = ms->sb_gid[((size_t)(cross_in ? 1 : 0)*ms->sb_nb3 + b3)*ms->sb_nb2 + b2];
       continue;
     }
-    const int gid = ms->nghbr[(size_t)m*27 + (iz + 1)*9 + (iy + 1)*3 + (ix + 1)];
+    int gid = -1;
+    if (!ms->nghbr_ml) gid = ms->nghbr[(size_t)m*27 + (iz + 1)*9 + (iy + 1)*3 + (ix + 1)];
+    else if (ms->mb_lev) gid = 0;   /* refined mesh: found below from the new position */
     if (gid < 0) { err |= DUSTB_ERR_NGHBR; continue; }
-    PI(DUSTB_PGID, p) = gid;
     if (lo1) { PR(DUSTB_IPX, p) += ms->x1max - ms->x1min; PR(DUSTB_IPX1, p) += ms->x1max - ms->x1min; }
     else if (hi1) { PR(DUSTB_IPX, p) -= ms->x1max - ms->x1min; PR(DUSTB_IPX1, p) -= ms->x1max - ms->x1min; }
     if (lo2) { PR(DUSTB_IPY, p) += ms->x2max - ms->x2min; PR(DUSTB_IPY1, p) += ms->x2max - ms->x2min; }
     else if (hi2) { PR(DUSTB_IPY, p) -= ms->x2max - ms->x2min; PR(DUSTB_IPY1, p) -= ms->x2max - ms->x2min; }
     if (lo3) { PR(DUSTB_IPZ, p) += ms->x3max - ms->x3min; PR(DUSTB_IPZ1, p) += ms->x3max - ms->x3min; }
     else if (hi3) { PR(DUSTB_IPZ, p) -= ms->x3max - ms->x3min; PR(DUSTB_IPZ1, p) -= ms->x3max - ms->x3min; }
+    if (ms->nghbr_ml) {
+      /* a refined mesh: the reference searches the 56 neighbour slots of the block
+       * (bvals_part.cpp:312-394); this restatement finds the block whose half-open box holds
+       * the (wrapped) position instead, by a search over every block, which is where that slot
+       * search must lead on a valid tree */
+      const double q1 = PR(DUSTB_IPX, p), q2 = PR(DUSTB_IPY, p), q3 = PR(DUSTB_IPZ, p);
+      gid = -1;
+      for (int b = 0; b < ms->nmb; ++b)
+        if (q1 >= MB(b, X1MIN) && q1 < MB(b, X1MAX) && q2 >= MB(b, X2MIN) && q2 < MB(b, X2MAX) &&
+            q3 >= MB(b, X3MIN) && q3 < MB(b, X3MAX)) { gid = b + ms->gids; break; }
+      if (gid < 0) { err |= DUSTB_ERR_NGHBR; continue; }
+    }
+    PI(DUSTB_PGID, p) = gid;
   }
   return err;
 }

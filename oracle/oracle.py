@@ -120,6 +120,9 @@ class Oracle:
             "nghbr": np.ascontiguousarray(ms.nghbr),
             "sb_gid": np.ascontiguousarray(ms.sb_gid),
         }
+        if getattr(ms, "nghbr56", None) is not None:
+            self.arr["mb_lev"] = np.ascontiguousarray(ms.lloc[:, 0])
+            self.arr["nghbr_ml"] = np.ascontiguousarray(ms.nghbr56)
         self.phys = dict(phys)
         self.ctx = capi.make_ctx(ms, self.arr, self.st.npart, self.st.stride, self.phys)
         self.threads = threads

@@ -112,3 +112,88 @@ def test_plan_on_a_mesh_without_refinement_is_the_same_level_exchange():
     n1, n2, n3 = ms.n
     sl = (slice(None), slice(None), slice(g, n3 - g), slice(g, n2 - g), slice(g, n1 - g))
     np.testing.assert_allclose(b[sl], o.arr["work"][sl], rtol=0, atol=1e-13 * np.abs(a).max())
+
+
+def _slot_search(ms, m, ix, iy, iz, fx, fy, fz):
+    """The neighbour-slot search of SetNewPrtclGID on a refined mesh
+    (src/bvals/bvals_part.cpp:312-394), restated as the device kernel route_slot_ml does it."""
+    nb = ms.nghbr56[m]
+    lev = ms.lloc[:, 0]
+    mylevel = lev[m]
+
+    def lev_of(s):
+        return lev[nb[s]] if nb[s] >= 0 else -1
+
+    def filled(jx, jy, jz, k):
+        nd = abs(jx) + abs(jy) + abs(jz)
+        end = neighbor_index(jx, jy, jz) + (4 if nd == 1 else (2 if nd == 2 else 1))
+        for q in range(k, end):
+            if nb[q] >= 0:
+                return q
+        return -1
+
+    def coarse_cover(jx, jy, jz):
+        mb = ms.mb_size[m]
+        lx, ly, lz = mb[3] - mb[0], mb[4] - mb[1], mb[5] - mb[2]
+        l1 = int(np.floor((mb[0] - ms.lo[0]) / lx + 0.5))
+        l2 = int(np.floor((mb[1] - ms.lo[1]) / ly + 0.5))
+        l3 = int(np.floor((mb[2] - ms.lo[2]) / lz + 0.5))
+        kx = jx if (jx == 0 or (l1 & 1) == (1 if jx > 0 else 0)) else 0
+        ky = jy if (jy == 0 or (l2 & 1) == (1 if jy > 0 else 0)) else 0
+        kz = jz if (jz == 0 or (l3 & 1) == (1 if jz > 0 else 0)) else 0
+        if abs(kx) + abs(ky) + abs(kz) == 0 or (kx, ky, kz) == (jx, jy, jz):
+            return -1
+        return filled(kx, ky, kz, neighbor_index(kx, ky, kz))
+
+    nd = abs(ix) + abs(iy) + abs(iz)
+    s = neighbor_index(ix, iy, iz)
+    if nd == 1:
+        if lev_of(s) > mylevel:
+            sub = {0: (fy, fz), 1: (fx, fz), 2: (fx, fy)}[[ix, iy, iz].index(next(v for v in (ix, iy, iz) if v))]
+            s = neighbor_index(ix, iy, iz, *sub)
+        return filled(ix, iy, iz, s)
+    if nd == 2:
+        if lev_of(s) > mylevel:
+            free = [a for a, v in enumerate((ix, iy, iz)) if v == 0][0]
+            s = neighbor_index(ix, iy, iz, (fx, fy, fz)[free], 0)
+        s = filled(ix, iy, iz, s)
+        return s if s >= 0 else coarse_cover(ix, iy, iz)
+    s = filled(ix, iy, iz, s)
+    return s if s >= 0 else coarse_cover(ix, iy, iz)
+
+
+def test_slot_search_finds_the_block_that_holds_the_position():
+    """For points just beyond every face, edge and corner of every block (both halves of each
+    transverse direction), the slot search of the route lands in the block whose box holds the
+    point (periodic wrap), at every level difference."""
+    ms = mesh("sphere_2lev")
+    mb = ms.mb_size
+    L = [ms.hi[a] - ms.lo[a] for a in range(3)]
+    rng = np.random.default_rng(1)
+    checked = 0
+    for m in range(ms.nmb):
+        lo, hi = mb[m, :3], mb[m, 3:6]
+        dx = mb[m, 6:9]
+        for o in [(a, b, c) for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1)
+                  if (a, b, c) != (0, 0, 0)]:
+            for _ in range(4):
+                x = np.empty(3)
+                for a in range(3):
+                    if o[a] < 0:
+                        x[a] = lo[a] - rng.uniform(0.05, 0.9) * dx[a]
+                    elif o[a] > 0:
+                        x[a] = hi[a] + rng.uniform(0.05, 0.9) * dx[a]
+                    else:
+                        x[a] = lo[a] + rng.uniform(0.02, 0.98) * (hi[a] - lo[a])
+                ix, iy, iz = [int((x[a] - lo[a] + (hi[a] - lo[a])) // (hi[a] - lo[a])) - 1
+                              for a in range(3)]
+                assert (ix, iy, iz) == o
+                f = [0 if x[a] < 0.5 * (lo[a] + hi[a]) else 1 for a in range(3)]
+                s = _slot_search(ms, m, ix, iy, iz, *f)
+                assert s >= 0, (m, o)
+                g = ms.nghbr56[m, s]
+                w = [(x[a] - ms.lo[a]) % L[a] + ms.lo[a] for a in range(3)]
+                own = np.nonzero(np.all((mb[:, :3] <= w) & (w < mb[:, 3:6]), axis=1))[0]
+                assert own.tolist() == [g], (m, o, s, g, own)
+                checked += 1
+    assert checked == ms.nmb * 26 * 4

@@ -70,3 +70,41 @@ def test_deposit_and_remap_on_a_refined_mesh(scheme):
     c = a_dt / (st.pr[15, :n] + a_dt)
     want = (st.pr[16, :n] * c).sum()
     assert abs(total - want) <= 1e-12 * want
+
+
+def test_route_across_levels_matches_the_oracle():
+    """SetNewPrtclGID on a refined mesh (src/bvals/bvals_part.cpp:115-471): after a drift of up
+    to 0.9 of each particle's own cell width, every particle that left its block is handed to
+    the neighbour of whatever level holds it (the device searches the 56 neighbour slots, the
+    oracle searches the block boxes), positions wrapped across periodic faces bit for bit."""
+    ms = _mesh()
+    st = refined_state(ms, [0.1], [1.0], 2, seed=9, vel_noise=0.0)
+    n = st.npart
+    rng = np.random.default_rng(3)
+    m = st.pi[0, :n]
+    dx = ms.mb_size[m, 6:9]
+    dt = 0.01
+    for a, r in enumerate((1, 3, 5)):
+        st.pr[r, :n] = rng.uniform(-0.9, 0.9, n) * dx[:, a] / dt
+    phys = dict(scheme=2, drag_solver=0)
+    g = DeviceDust(st, phys)
+    o = oracle.Oracle(st, phys)
+    for obj in (g, o):
+        obj.register_copy()
+        obj.push_imex(1.0, 0.0, dt, 0.0)
+        obj.route()
+    torch.cuda.synchronize()
+    assert g.error_word() == 0
+    pi = g.t["pi"].cpu().numpy()[:, :n]
+    pr = g.t["pr"].cpu().numpy()[:, :n]
+    moved = (pi[0] != st.pi[0, :n]).sum()
+    assert moved > n // 20
+    np.testing.assert_array_equal(pi[0], o.arr["pi"][0, :n])
+    np.testing.assert_array_equal(pr, o.arr["pr"][:, :n])
+    # every particle inside its new block's box
+    mb = ms.mb_size[pi[0]]
+    for a, r in enumerate((0, 2, 4)):
+        assert ((pr[r] >= mb[:, a]) & (pr[r] < mb[:, 3 + a])).all()
+    # and the levels differ where particles changed blocks
+    lev = ms.lloc[:, 0]
+    assert (lev[pi[0]] != lev[st.pi[0, :n]]).sum() > 0
