@@ -1949,6 +1949,11 @@ void history(const dustb_ctx *c, double atw_dt, cudaStream_t st) {
   Ind d = make_ind(c->mesh);
   k_history<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, atw_dt);
 }
+// u0.m += atw_dt f for a 3-variable field f (the mixed form's rate ledger)
+void history_field(const dustb_ctx *c, const double *f, double atw_dt, cudaStream_t st) {
+  Ind d = make_ind(c->mesh);
+  k_history<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, f, atw_dt);
+}
 void dc_correct(const dustb_ctx *c, cudaStream_t st) {
   Ind d = make_ind(c->mesh);
   k_dc_correct<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, c->f.qdep,

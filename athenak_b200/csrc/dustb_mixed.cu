@@ -40,6 +40,7 @@
 namespace dustb_cells {
 void gas_rk(const dustb_ctx *c, double g0, double g1, cudaStream_t st);
 void history(const dustb_ctx *c, double atw_dt, cudaStream_t st);
+void history_field(const dustb_ctx *c, const double *f, double atw_dt, cudaStream_t st);
 void dc_correct(const dustb_ctx *c, cudaStream_t st);
 void consistent_gas(const dustb_ctx *c, double a_dt, cudaStream_t st);
 void pmbr(const dustb_ctx *c, double a_dt, cudaStream_t st);
@@ -255,6 +256,18 @@ __device__ __forceinline__ int warp_slot(int *counter, int key, unsigned act) {
   base = __shfl_sync(peers, base, leader);
   return base + __popc(peers & ((1u << lane) - 1u));
 }
+// the sum of v over the lanes of mask (FP64), in lane 0; mask is a prefix of the warp's lanes
+// (the threads of a CTA whose size is not a multiple of 32): a lane adds only what a lane of
+// the mask sent it
+__device__ __forceinline__ double warp_sum(unsigned mask, double v) {
+  const int nl = 32 - __clz(mask), lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double y = __shfl_down_sync(mask, v, o);
+    if (lane + o < nl) v += y;
+  }
+  return v;
+}
 __device__ __forceinline__ void warp_count(int *counter, int key, unsigned act) {
   const unsigned peers = __match_any_sync(act, key);
   if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counter[key], __popc(peers));
@@ -380,7 +393,8 @@ __global__ void k_sortmove(PBuf src, PBuf dst, int n, int *cursor) {
 }
 
 // the shadow's particles into their reference rows; a pending consistent kick of the last
-// cycle is applied to the exported velocities and rates (rounded as the next push would)
+// cycle is applied to the exported velocities and rates in FP64 (the kick the gas's split
+// gave them, exactly: the rows' momentum is the one the cycles exchanged)
 __global__ void k_export(double *pr, int *pi, long long stride, int n, PBuf A, Geo G,
                          const double *res, const MHead *head) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -388,15 +402,15 @@ __global__ void k_export(double *pr, int *pi, long long stride, int n, PBuf A, G
   int m, k, j, i;
   decode(G, A.cell[q], m, k, j, i);
   const int p = A.pid[q];
-  float vel[3] = {A.f[F_VX][q], A.f[F_VY][q], A.f[F_VZ][q]};
-  float rate[3] = {A.f[F_RX][q], A.f[F_RY][q], A.f[F_RZ][q]};
+  double vel[3] = {A.f[F_VX][q], A.f[F_VY][q], A.f[F_VZ][q]};
+  double rate[3] = {A.f[F_RX][q], A.f[F_RY][q], A.f[F_RZ][q]};
   if (res && head->pending && A.f[F_M][q] > 0.0f) {
     const long long b = G.at(m, 4, 0, k + G.ks, j + G.js, i + G.is);
     const double cj = (double)A.f[F_CC][q];
     for (int a = 0; a < 3; ++a) {
       const double d = __dmul_rn(cj, res[b + a * G.vstride]);
-      vel[a] = __fadd_rn(vel[a], __double2float_rn(d));
-      rate[a] += (float)(d / head->a_dt);
+      vel[a] += d;
+      rate[a] += d / head->a_dt;
     }
   }
   auto W = [&](int r, double v) { pr[(long long)r * stride + p] = v; };
@@ -458,6 +472,14 @@ struct PushArgs {
   MHead *head;
   int set_pending;            // stage 2: record this cycle's stage-2 kick as pending
   unsigned *err;
+  // imex: the momentum ledger of the push.  The FP32 velocity a particle stores differs from
+  // the FP64 value of the same update (the RK combination g0 v + g1 v1 of the gas's own FP64
+  // coefficients, the folded consistent kick, the history term); m times the difference is
+  // added to the gas momentum (u0, and at stage 1 also its register u1, which the push's
+  // register copy pairs with) at the cell of each CTA's first particle.  Null: no ledger
+  double *u0, *u1;
+  int nvg;
+  double g0, g1, atw, inv_adt;
 };
 
 // dust_imex_point_consistent_dust of stage 1 (src/dust/dust_pm.cpp:686-696): the velocity
@@ -708,14 +730,12 @@ __global__ void __launch_bounds__(kT) k_count(PBuf S, int *key_out, int *count, 
   if (P.set_pending && p == 0) { P.head->a_dt = P.a_dt; P.head->pending = 1; }
 }
 
-// move: the whole push of every particle, written to its slot in dst
+// move: the whole push of every particle, written to its slot in dst; comp receives
+// m (v_FP64 - v_stored) of the imex ledger
 template <int KIND, int SP>
-__global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, int *cursor,
-                                             Geo G, int n, PushArgs P) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = p < n;
-  const unsigned act = __ballot_sync(0xffffffffu, live);
-  if (!live) return;
+__device__ __forceinline__ void move_particle(const PBuf &S, const PBuf &D, const int *key_in,
+                                              int *cursor, const Geo &G, const PushArgs &P,
+                                              int p, unsigned act, double comp[3]) {
   const int key = key_in[p];
   // the source copy is only read here: its loads go through the read-only path and are all
   // issued before the slot's atomic, whose round trip then overlaps theirs
@@ -739,6 +759,9 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   // (imex stage 1 and the pc2 half step: the rates are not read; every kick rewrites them)
   cc = (KIND == PK_FULL || P.stage2 || kick) ? __ldg(sf[F_CC] + p) : 0.0f;
   const int q = warp_slot(cursor, key, act);
+  // (the ledger's inputs: the velocity and rate before the folded kick, the kick in FP64)
+  const float vb[3] = {v[0], v[1], v[2]}, rb[3] = {r[0], r[1], r[2]};
+  double dk[3] = {0.0, 0.0, 0.0};
   if (KIND != PK_FULL) {
     if (kick && mass > 0.0f) {
       double d[3];
@@ -746,6 +769,7 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
       for (int a = 0; a < 3; ++a) {
         v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
         r[a] += (float)(d[a] / P.a_dt);
+        dk[a] = d[a];
       }
     }
     if (!P.stage2) {
@@ -777,6 +801,25 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
     nv[0] = P.gam0 * v[0] + P.gam1 * v1[0] + P.bdt * fx + atw * r[0];
     nv[1] = P.gam0 * v[1] + P.gam1 * v1[1] + P.bdt * fy + atw * r[1];
     nv[2] = P.gam0 * v[2] + P.gam1 * v1[2] + P.bdt * fz + atw * r[2];
+    if (P.u0 && mass > 0.0f) {
+      // the same update in FP64 from the stored inputs: the gas's coefficients, the exact kick
+      // (c times the FP64 residual) in the velocity and, over a dt, in the rate; the ledger
+      // takes m times what the stored FP32 velocity left out.  Stage 1 (g0 = 1, g1 = 0, no
+      // history term) has only the kick; its register copy v1 is the stored velocity (no
+      // forces) or carries the forces' own rounding (the shearing box, which does not
+      // conserve momentum)
+      const float fv[3] = {P.bdt * fx, P.bdt * fy, P.bdt * fz};
+      const double mm = (double)mass;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const double base = (double)vb[a] + dk[a];
+        double want = base;
+        if (P.stage2)
+          want = fma(P.atw, fma(dk[a], P.inv_adt, (double)rb[a]), fma(P.g1, (double)v1[a], P.g0 * base));
+        if (P.sbox) want += (double)fv[a];
+        comp[a] = mm * (want - (double)nv[a]);
+      }
+    }
   }
   int flags;
   float hpos[2];
@@ -809,6 +852,33 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   D.f[F_TS][q] = ts; D.f[F_M][q] = mass; D.f[F_CC][q] = cc;
 }
 
+template <int KIND, int SP>
+__global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, int *cursor,
+                                             Geo G, int n, PushArgs P) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = p < n;
+  const unsigned act = __ballot_sync(0xffffffffu, live);
+  double comp[3] = {0.0, 0.0, 0.0};
+  if (live) move_particle<KIND, SP>(S, D, key_in, cursor, G, P, p, act, comp);
+  if (KIND != PK_IMEX || !P.u0) return;
+  // the warp's ledger, added to the gas at its first particle's (old) cell: the particles of
+  // a warp are consecutive in cell order, one or two cells
+  double w[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) w[a] = warp_sum(0xffffffffu, comp[a]);
+  if ((threadIdx.x & 31) == 0 && live) {
+    int m, k, j, i;
+    decode(G, S.cell[p], m, k, j, i);
+    const double vinv = 1.0 / G.vol;
+    for (int a = 0; a < 3; ++a) {
+      if (w[a] == 0.0) continue;
+      const long long at = G.at(m, P.nvg, 1 + a, G.ks + k, G.js + j, G.is + i);
+      atomicAdd(&P.u0[at], w[a] * vinv);
+      if (!P.stage2 && P.u1) atomicAdd(&P.u1[at], w[a] * vinv);
+    }
+  }
+}
+
 // ---- tile deposit kernels -------------------------------------------------------------------
 // Q/P + centre mass (imex), the dc1 operator, the gather-kick-deposit (imex), the pc2
 // predictor, the pc2 advance
@@ -835,6 +905,7 @@ struct TileArgs {
   double *dfield;              // deposit field (the predictor: qdep's variable 1)
   int dnvar;
   double *res;                 // MODE_QP: resid, the centre mass goes to var 3
+  double *hfield;              // MODE_KICK: the rate's rounding for the history term (or null)
   int deposit;                 // 0: kick or advance only (no back-reaction)
   float shy;                   // imex: the stage's implicit shear shift sh / dy (0: none)
   int probe_timeout;           // test hook: tile 0 never issues its first copy
@@ -1066,9 +1137,12 @@ __device__ __forceinline__ void stage_zero(float4 *s_acc, int cl, int nct) {
 // window cell (z plane c, row wy, column wx) sums the staged contributions of the up to 9
 // source cells of its plane that reach it; window cells beyond the block go to the owning
 // neighbour's active cell (the additive ghost exchange folded into the add)
+// gs (the kick): this thread's FP64 sums of the values it adds (before the 1/V), the gas side
+// of the tile's momentum ledger
 template <int MODE, int D3, int GH>
 __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, const TileArgs &T,
-                                           int m, int k, int j0, int tj, const int *s_ss) {
+                                           int m, int k, int j0, int tj, const int *s_ss,
+                                           double *gs) {
   constexpr int NC = FourValues<MODE>::value ? 4 : 3;
   constexpr int WK = D3 ? 3 : 1;
   const int nx1 = G.nx1, nct = tj * nx1;
@@ -1106,6 +1180,7 @@ __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, co
     if (s.y != 0.0f) atomicAdd(f + G.vstride, (double)s.y * vinv);
     if (s.z != 0.0f) atomicAdd(f + 2 * G.vstride, (double)s.z * vinv);
     if (NC > 3 && s.w != 0.0f) atomicAdd(f + 3 * G.vstride, (double)s.w * vinv);
+    if (MODE == MODE_KICK && gs) { gs[0] += (double)s.x; gs[1] += (double)s.y; gs[2] += (double)s.z; }
   }
 }
 
@@ -1121,7 +1196,7 @@ __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, co
 template <int MODE, int GH>
 __device__ __forceinline__ void add_window_cells(const float4 *s_acc, const Geo &G,
                                                  const TileArgs &T, int m, int k, int j0, int tj,
-                                                 int cj, int ci) {
+                                                 int cj, int ci, double *gs) {
   constexpr bool V4 = FourValues<MODE>::value;
   const int nx1 = G.nx1, nct = tj * nx1;
   const double vinv = 1.0 / G.vol;                 // (every deposited value is per unit volume)
@@ -1138,6 +1213,7 @@ __device__ __forceinline__ void add_window_cells(const float4 *s_acc, const Geo 
     if (v.y != 0.0f) atomicAdd(f + G.vstride, (double)v.y * vinv);
     if (v.z != 0.0f) atomicAdd(f + 2 * G.vstride, (double)v.z * vinv);
     if (V4 && v.w != 0.0f) atomicAdd(f + 3 * G.vstride, (double)v.w * vinv);
+    if (MODE == MODE_KICK && gs) { gs[0] += (double)v.x; gs[1] += (double)v.y; gs[2] += (double)v.z; }
   };
   auto acc = [](float4 &s, const float4 &v) { s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w; };
   const int wy_lo = (cj == 0) ? 0 : cj + 1, wy_hi = (cj == tj - 1) ? tj + 1 : cj + 1;
@@ -1216,11 +1292,13 @@ __device__ __forceinline__ void cta_sync(unsigned wmask) {
   __syncthreads();
 }
 
-// the head of a tile's shared memory: the cell ranges, the slot starts of the pass and the
-// centre mass of each cell (ints, ints, floats), 16-byte aligned
+// the head of a tile's shared memory: the cell ranges, the slot starts of the pass (ints) and
+// the centre mass of each cell (doubles, 8-byte aligned after the two int arrays), 16-byte
+// aligned
 __host__ __device__ inline size_t tile_head_bytes(int nct) {
-  return (((size_t)(3 * nct + 2) * 4 + 15) & ~(size_t)15);
+  return (((size_t)(2 * nct + 2) * 4 + (size_t)nct * 8 + 15) & ~(size_t)15);
 }
+
 
 // One CTA per tile of tj rows of one plane.  The tile's particles (one contiguous range of
 // the sorted shadow) are cut into passes of at most chunk - 8, bulk-copied into shared
@@ -1244,12 +1322,13 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
   __shared__ int s_wsum[kMaxTileThreads / 32];
   __shared__ int s_wcnt[kMaxTileThreads / 32];
   __shared__ int s_split;                          // some cell of the pass has several slots
+  __shared__ double s_ledger[9];                   // the kick tile's momentum ledger (FP64)
   const int nx1 = G.nx1, tj = T.tj;
   const int nct = tj * nx1;                        // source cells of the tile = threads
   const int CH = T.chunk;                          // buffer columns (multiple of 4)
   int *s_cs = (int *)smem;                         // [nct + 1] cell ranges
   int *s_ss = s_cs + (nct + 1);                    // [nct + 1] slot starts of the pass
-  float *s_qt = (float *)(s_ss + (nct + 1));       // [nct] centre mass (Q/P)
+  double *s_qt = (double *)(s_ss + (nct + 1));     // [nct] centre mass (Q/P), FP64
   float *s_f = (float *)(smem + tile_head_bytes(nct));   // [8][CH]
   float4 *s_acc = (float4 *)s_f;                   // the staged sums, after the rows
   const int tid = threadIdx.x;
@@ -1300,7 +1379,8 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
     }
     __syncwarp(wmask);
     for (int x = tid; x <= nct; x += blockDim.x) s_cs[x] = T.cstart[c0 + x];
-    if (MODE == MODE_QP) s_qt[tid] = 0.0f;
+    if (MODE == MODE_QP) s_qt[tid] = 0.0;
+    for (int x = tid; x < 9; x += blockDim.x) s_ledger[x] = 0.0;   // (tiles of fewer threads)
     cta_sync(wmask);
     const int P0 = s_cs[0], P1 = s_cs[nct];
     const float inv_adt = (float)(1.0 / T.a_dt);
@@ -1380,14 +1460,16 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       if (MODE == MODE_QP) {
         CellSums<MODE, D3> qp;
         qp.zero();
-        float qt = 0.0f;
+        // (the centre mass m c summed in FP64 from the FP32 m and c the consistent kick uses:
+        // exact products, so the dust share r q / qt of a cell sums to r q V over its particles)
+        double qt = 0.0;
         for (int r = lo; r < hi; ++r) {
           float wx_[3], wy_[3], wz_[3];
           wts(SCHEME, s_f[r], wx_);
           wts(SCHEME, oy_at(r), wy_);
           if (D3) wts(SCHEME, s_f[2 * CH + r], wz_);
           const float mc = s_f[4 * CH + r] * s_f[3 * CH + r];
-          qt += mc;
+          qt += (double)s_f[4 * CH + r] * (double)s_f[3 * CH + r];
           qp.add(wx_, wy_, wz_, make_float2(mc, mc * s_f[5 * CH + r]),
                  make_float2(mc * s_f[6 * CH + r], mc * s_f[7 * CH + r]));
         }
@@ -1399,8 +1481,8 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
         if (!single && !split && s_ss[tid + 1] == s_ss[tid]) stage_zero<D3>(s_acc, tid, nct);
         if (cl >= 0) stage_sums<MODE, D3>(qp, s_acc, split ? tid : cl, nct);
         cta_sync(wmask);
-        if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l);
-        else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
+        if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l, nullptr);
+        else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr, nullptr);
       } else {
         // gather phase: the operator's m c u / V, the kick's velocity change, the predictor's
         // impulse and rate, or the advance's u*, into rows 5..7 (and 3)
@@ -1441,6 +1523,11 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
           cta_sync(wmask);
           // (four particles per thread at a time, their velocity loads issued together)
           constexpr int U = 4;
+          // the dust side of the tile's momentum ledger (FP64): the momentum m (v' - v) the
+          // particles received, v' the stored FP32 velocity, and the part m (v' - v)/(a dt) - m R
+          // of the rate that the FP32 rate R leaves out (the history term reads R)
+          double le[3] = {0.0, 0.0, 0.0}, lr[3] = {0.0, 0.0, 0.0};
+          const double inv_adt64 = 1.0 / T.a_dt;
           for (int x0 = tid; x0 < cnt; x0 += U * blockDim.x) {
             float v[U][3];
   #pragma unroll
@@ -1453,9 +1540,32 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
               const int x = x0 + u * blockDim.x;
               if (x >= cnt) break;
               const int s = sh + x, p = cb + x;
-              const float dvx = s_f[5 * CH + s], dvy = s_f[6 * CH + s], dvz = s_f[7 * CH + s];
-              S.f[F_VX][p] = v[u][0] + dvx; S.f[F_VY][p] = v[u][1] + dvy; S.f[F_VZ][p] = v[u][2] + dvz;
-              S.f[F_RX][p] = dvx * inv_adt; S.f[F_RY][p] = dvy * inv_adt; S.f[F_RZ][p] = dvz * inv_adt;
+              const float dv[3] = {s_f[5 * CH + s], s_f[6 * CH + s], s_f[7 * CH + s]};
+              float vn[3], rn[3];
+#pragma unroll
+              for (int a = 0; a < 3; ++a) { vn[a] = v[u][a] + dv[a]; rn[a] = dv[a] * inv_adt; }
+              S.f[F_VX][p] = vn[0]; S.f[F_VY][p] = vn[1]; S.f[F_VZ][p] = vn[2];
+              S.f[F_RX][p] = rn[0]; S.f[F_RY][p] = rn[1]; S.f[F_RZ][p] = rn[2];
+              if (T.deposit) {
+                const double mp = (double)s_f[4 * CH + s];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                  const double act = (double)vn[a] - (double)v[u][a];
+                  le[a] += mp * act;
+                  if (T.hfield) lr[a] += mp * (act * inv_adt64 - (double)rn[a]);
+                }
+              }
+            }
+          }
+          if (T.deposit) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              const double e = warp_sum(wmask, le[a]);
+              if (lane == 0) atomicAdd(&s_ledger[a], e);
+              if (T.hfield) {
+                const double r = warp_sum(wmask, lr[a]);
+                if (lane == 0) atomicAdd(&s_ledger[3 + a], r);
+              }
             }
           }
         }
@@ -1503,18 +1613,46 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
           if (!single && !split && s_ss[tid + 1] == s_ss[tid]) stage_zero<D3>(s_acc, tid, nct);
           if (cl >= 0) stage_sums<MODE, D3>(sums, s_acc, split ? tid : cl, nct);
           cta_sync(wmask);
-          if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l);
-          else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr);
+          double gs[3] = {0.0, 0.0, 0.0};
+          if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l, gs);
+          else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr, gs);
+          if (MODE == MODE_KICK) {
+            // the gas side of the tile's ledger: what this pass added, summed over the CTA
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              const double w = warp_sum(wmask, gs[a]);
+              if (lane == 0) atomicAdd(&s_ledger[6 + a], w);
+            }
+          }
         }
       }
       // the next pass's copies overwrite the rows (and its slots the slot starts)
       cta_sync(wmask);
     }
+    if (MODE == MODE_KICK && T.deposit && P1 > P0) {
+      // the tile's momentum ledger closed: what the gas received from the FP32 sums and what
+      // the particles received differ by the FP32 rounding of weights, products and sums; the
+      // difference goes to the gas, spread evenly over the tile's cells, so that gas and dust
+      // exchange exactly opposite momenta (FP64 round-off) and no cell takes a tile's worth of
+      // rounding.  The rate's rounding goes to the history field the same way (the next
+      // stage's history term adds it to the gas as it adds the gas rate)
+      cta_sync(wmask);
+      const double share = 1.0 / (G.vol * (double)nct);
+      const int cj = tid / nx1, ci = tid - cj * nx1;
+      const long long at = G.at(m, 3, 0, G.ks + k, G.js + j0 + cj, G.is + ci);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const double r = -(s_ledger[a] + s_ledger[6 + a]);
+        if (r != 0.0) atomicAdd(&T.dfield[at + a * G.vstride], r * share);
+        if (T.hfield && s_ledger[3 + a] != 0.0)
+          atomicAdd(&T.hfield[at + a * G.vstride], s_ledger[3 + a] * share);
+      }
+    }
     if (MODE == MODE_QP) {
       // centre mass m c / V of the cell (dust_imex_point_center_mass): only this cell's
       // particles have it as their centre, so it is stored, not added
       const int cj = tid / nx1, ci = tid - cj * nx1;
-      T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj, G.is + ci)] = (double)s_qt[tid] / G.vol;
+      T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj, G.is + ci)] = s_qt[tid] / G.vol;
     }
     // (every thread is done with this tile's shared memory before the next tile's copies)
     cta_sync(wmask);
@@ -2169,7 +2307,11 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       Scope sc(DUSTB_K_CELLS, st);
       if (stage == 1) cudaMemcpyAsync(c->f.u1, c->f.u0, fbytes * c->f.nvar_gas, cudaMemcpyDeviceToDevice, st);
       dustb_cells::gas_rk(c, gam0[stage - 1], gam1[stage - 1], st);
-      if (stage == 2 && br) dustb_cells::history(c, atw22 * dt, st);
+      if (stage == 2 && br) {
+        dustb_cells::history(c, atw22 * dt, st);
+        // the rate's FP32 rounding the stage-1 kick tiles recorded (the momentum ledger)
+        dustb_cells::history_field(c, c->f.work, atw22 * dt, st);
+      }
     }
     PushArgs P{};
     P.kind = PK_IMEX;
@@ -2189,6 +2331,12 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     P.set_pending = (stage == 2 && br && cons);
     P.x3rem = mp->x3_removed;
     P.err = c->err;
+    if (br) {
+      // the push's momentum ledger (FP64 coefficients of the gas's own RK combination)
+      P.u0 = c->f.u0; P.u1 = c->f.u1; P.nvg = c->f.nvar_gas;
+      P.g0 = gam0[stage - 1]; P.g1 = gam1[stage - 1];
+      P.atw = (stage == 2) ? atw22 * dt : 0.0; P.inv_adt = 1.0 / a_dt;
+    }
     RUN(push_sort(S, src, cur, G, n, ncell, P, st));
     if (stage == 1) cudaMemsetAsync(&S.head->pending, 0, sizeof(int), st);   // applied
     TileArgs T{};
@@ -2233,10 +2381,14 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       RUN(ghost_copy_if(c, G, c->f.ustar, st));
     }
     if (br) cudaMemsetAsync(c->f.dmom, 0, fbytes * 3, st);
+    // stage 1: the kick tiles record the rate's rounding in work for stage 2's history term
+    // (work is free from here: the operator sweeps are done)
+    if (br && stage == 1) cudaMemsetAsync(c->f.work, 0, fbytes * 3, st);
     RUN(gather_window(S, G, c->mesh, c->f.ustar, T, st));
     {
       Scope sc(DUSTB_K_KICK, st);
       T.gfield = c->f.ustar; T.dfield = c->f.dmom; T.dnvar = 3; T.deposit = br;
+      T.hfield = (br && stage == 1) ? c->f.work : nullptr;
       RUN(launch_tile<MODE_KICK>(S, cur, G, cf, T, st, Q_KICK));
       if (shift) RUN(launch_shift_edge<MODE_KICK>(S, cur, G, T, st));
     }

@@ -4,8 +4,9 @@ accumulators and gas) against the FP64 forms on the same seeded inputs.
 Stated tolerance of the mixed form on these small cases (a few cycles, a few thousand
 particles): every particle velocity is within 1e-5 of the FP64 result relative to the largest
 velocity, every position within 1e-5 cells, the gas momentum field within 1e-5 of its scale;
-total gas + dust momentum changes by at most 1e-7 of the absolute momentum per cycle (the
-FP32 rounding of the deposited values and weights).  The benchmark-shaped case and the
+total gas + dust momentum of the mixed form's own state changes by at most 1e-12 of the
+absolute momentum per cycle (the momentum ledgers of the kick tiles and the push return every
+FP32 rounding of the exchange to the gas).  The benchmark-shaped case and the
 tolerance with the consistent split on large particle counts are in
 test_gpu_mixed_config2.py."""
 import numpy as np
@@ -100,17 +101,33 @@ def absolute_momentum(st):
     return (d + g).max()
 
 
-@pytest.mark.parametrize("name", ["3d_random", "2d_lattice", "cic_dc2_plain"])
+@pytest.mark.parametrize("name", ["3d_random", "2d_lattice", "cic_dc2_plain", "ngp_local"])
 def test_mixed_conserves_momentum(name):
-    """Gas + dust momentum of the mixed form changes by at most 1e-7 of the absolute
-    momentum per cycle: the FP32 rounding (2^-24 ~ 6e-8) of the deposited values, of the
-    stencil weights (whose sum is 1 only to FP32 precision) and of the stored velocity
-    increments -- systematic, not random, when all particles are alike (the lattice case);
-    the FP64 form holds 1e-13."""
-    cycles = 4
-    st, ref, mx, p0, c = run_pair(name, cycles=cycles)
-    g, d = mx.dev.momentum()
-    assert np.abs(g + d - p0).max() < 1e-7 * cycles * absolute_momentum(st)
+    """Gas + dust momentum of the mixed form is conserved to FP64 round-off: from its own
+    initial state (the import rounds m and v to FP32; an export before the first cycle writes
+    that state to the rows), every cycle changes the total by at most 1e-12 of the absolute
+    momentum.  The kick tiles return the FP32 rounding of their deposits (weights whose sum is 1
+    only to FP32 precision, FP32 products and per-cell sums) and of the stored velocities and
+    rates to the gas, the push returns the rounding of the FP32 RK combination and of the folded
+    consistent kick, and the centre mass is summed in FP64, so that the dust share of a cell
+    sums to what the gas gave up.  The FP64 form holds 1e-13."""
+    from athenak_b200.mixed import MixedDust
+    c = CASES[name]
+    ms = uniform_mesh(*c["mesh"])
+    st = make_state(ms, **c["st"])
+    absm = absolute_momentum(st)
+    mx = MixedDust(st, c["phys"])
+    mx.export()
+    torch.cuda.synchronize()
+    p0 = sum(mx.dev.momentum())
+    for cyc in range(1, 5):
+        mx.imex_cycle(c["dt"])
+        mx.export()
+        torch.cuda.synchronize()
+        p = sum(mx.dev.momentum())
+        assert np.abs(p - p0).max() <= 1e-12 * cyc * absm, (cyc, np.abs(p - p0).max() / absm)
+    assert mx.error_word() == 0
+    st, ref, mx, p0, c = run_pair(name, cycles=4)
     g, d = ref.momentum()
     assert np.abs(g + d - p0).max() < 1e-13 * absolute_momentum(st)
 
