@@ -907,6 +907,7 @@ struct TileArgs {
   double *res;                 // MODE_QP: resid, the centre mass goes to var 3
   double *hfield;              // MODE_KICK: the rate's rounding for the history term (or null)
   int deposit;                 // 0: kick or advance only (no back-reaction)
+  int ledger;                  // MODE_KICK: keep the tile's momentum ledger
   float shy;                   // imex: the stage's implicit shear shift sh / dy (0: none)
   int probe_timeout;           // test hook: tile 0 never issues its first copy
   // the device work queue of a persistent launch: the tiles in the order to take them
@@ -1546,7 +1547,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
               for (int a = 0; a < 3; ++a) { vn[a] = v[u][a] + dv[a]; rn[a] = dv[a] * inv_adt; }
               S.f[F_VX][p] = vn[0]; S.f[F_VY][p] = vn[1]; S.f[F_VZ][p] = vn[2];
               S.f[F_RX][p] = rn[0]; S.f[F_RY][p] = rn[1]; S.f[F_RZ][p] = rn[2];
-              if (T.deposit) {
+              if (T.ledger) {
                 const double mp = (double)s_f[4 * CH + s];
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
@@ -1557,7 +1558,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
               }
             }
           }
-          if (T.deposit) {
+          if (T.ledger) {
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
               const double e = warp_sum(wmask, le[a]);
@@ -1616,7 +1617,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
           double gs[3] = {0.0, 0.0, 0.0};
           if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l, gs);
           else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr, gs);
-          if (MODE == MODE_KICK) {
+          if (MODE == MODE_KICK && T.ledger) {
             // the gas side of the tile's ledger: what this pass added, summed over the CTA
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
@@ -1629,7 +1630,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       // the next pass's copies overwrite the rows (and its slots the slot starts)
       cta_sync(wmask);
     }
-    if (MODE == MODE_KICK && T.deposit && P1 > P0) {
+    if (MODE == MODE_KICK && T.ledger && P1 > P0) {
       // the tile's momentum ledger closed: what the gas received from the FP32 sums and what
       // the particles received differ by the FP32 rounding of weights, products and sums; the
       // difference goes to the gas, spread evenly over the tile's cells, so that gas and dust
@@ -1900,7 +1901,7 @@ int default_chunk(int tj, int nx1) {
 
 bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   const int nx1 = ms.nx1, nx2 = ms.multi_d ? ms.nx2 : 1;
-  const int base = mp->variant & ~DUSTB_MIXED_GRID_TILES;
+  const int base = mp->variant & ~(DUSTB_MIXED_GRID_TILES | DUSTB_MIXED_NO_LEDGER);
   if ((base != 0 && base != DUSTB_MIXED_PROBE_COPY_TIMEOUT) || nx1 > kMaxTileThreads)
     return false;
   cf.grid = (mp->variant & DUSTB_MIXED_GRID_TILES) ? 1 : 0;
@@ -2193,7 +2194,7 @@ int dustb_mixed_tune(const dustb_ctx *c, dustb_mixed_params *mp, void *ws, long 
   cudaStream_t st = (cudaStream_t)stream;
   if (g_timing.on) return DUSTB_EUNSUP;          // (its events would interleave)
   const int nx1 = c->mesh.nx1, nx2 = c->mesh.nx2;
-  const int keep = mp->variant & ~DUSTB_MIXED_GRID_TILES;
+  const int keep = mp->variant & ~DUSTB_MIXED_GRID_TILES;   // (the probe hook, the ledger flag)
   // the candidates: rows per tile (tiles of at most 256 cells), particles per pass (the
   // default, or passes sized for 2.25, 4 and 4.5 thousand particles), persistent CTAs on the
   // work queue or one CTA per tile
@@ -2310,7 +2311,8 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       if (stage == 2 && br) {
         dustb_cells::history(c, atw22 * dt, st);
         // the rate's FP32 rounding the stage-1 kick tiles recorded (the momentum ledger)
-        dustb_cells::history_field(c, c->f.work, atw22 * dt, st);
+        if (!(mp->variant & DUSTB_MIXED_NO_LEDGER))
+          dustb_cells::history_field(c, c->f.work, atw22 * dt, st);
       }
     }
     PushArgs P{};
@@ -2331,7 +2333,8 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     P.set_pending = (stage == 2 && br && cons);
     P.x3rem = mp->x3_removed;
     P.err = c->err;
-    if (br) {
+    const bool ledger = br && !(mp->variant & DUSTB_MIXED_NO_LEDGER);
+    if (ledger) {
       // the push's momentum ledger (FP64 coefficients of the gas's own RK combination)
       P.u0 = c->f.u0; P.u1 = c->f.u1; P.nvg = c->f.nvar_gas;
       P.g0 = gam0[stage - 1]; P.g1 = gam1[stage - 1];
@@ -2383,12 +2386,13 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     if (br) cudaMemsetAsync(c->f.dmom, 0, fbytes * 3, st);
     // stage 1: the kick tiles record the rate's rounding in work for stage 2's history term
     // (work is free from here: the operator sweeps are done)
-    if (br && stage == 1) cudaMemsetAsync(c->f.work, 0, fbytes * 3, st);
+    if (ledger && stage == 1) cudaMemsetAsync(c->f.work, 0, fbytes * 3, st);
     RUN(gather_window(S, G, c->mesh, c->f.ustar, T, st));
     {
       Scope sc(DUSTB_K_KICK, st);
       T.gfield = c->f.ustar; T.dfield = c->f.dmom; T.dnvar = 3; T.deposit = br;
-      T.hfield = (br && stage == 1) ? c->f.work : nullptr;
+      T.ledger = ledger;
+      T.hfield = (ledger && stage == 1) ? c->f.work : nullptr;
       RUN(launch_tile<MODE_KICK>(S, cur, G, cf, T, st, Q_KICK));
       if (shift) RUN(launch_shift_edge<MODE_KICK>(S, cur, G, T, st));
     }

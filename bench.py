@@ -312,6 +312,14 @@ def run_ours(args, rep):
     ms_dev_rt = timed_cycles(lambda: (mx.import_(), mx.imex_cycle(dt), mx.export()),
                              min(args.steps, 3), stream)
     del graph
+    # the cost of the momentum ledgers (exact conservation): the same cycle with them off
+    # (DUSTB_MIXED_NO_LEDGER), timed the same way
+    mx.mp.variant |= 16
+    mx.imex_cycle(dt)
+    graph = mx.capture(lambda: mx.imex_cycle(dt))
+    ms_no_ledger = maxall(timed_cycles(graph.replay, args.steps, stream))
+    del graph
+    mx.mp.variant &= ~16
     if args.mixed_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": rep.throughput(npart, ms_mixed),
@@ -319,6 +327,7 @@ def run_ours(args, rep):
                               "config": {"cells": ncell, "particles": npart},
                               "kernels": {k: v for k, v in ktimes.items()},
                               "roofline": roofline(ktimes, nk, npart, ncell, ms_mixed),
+                              "ms_per_step_without_momentum_ledger": ms_no_ledger,
                               "note": "mixed form only (profiling case)"}), flush=True)
         return
     # ---- the storage twin: FP64 cycles with the state rounded to the mixed form's layout
@@ -420,7 +429,9 @@ def run_ours(args, rep):
             "fp64_seeded_order": fp64_seeded,
             "timing": {"timed": "CUDA-graph replay of one captured cycle",
                        "eager_ms_per_step": ms_eager,
-                       "device_import_cycle_export_ms_per_step": ms_dev_rt},
+                       "device_import_cycle_export_ms_per_step": ms_dev_rt,
+                       "momentum_ledger": "on (gas + dust momentum to FP64 round-off)",
+                       "ms_per_step_without_momentum_ledger": ms_no_ledger},
             "speedup_mixed_vs_fp64": fp64_best / ms_mixed,
             "speedup_basis": "the faster of the FP64 form's two row orders",
             "errors_mixed_vs_fp64": errors,
