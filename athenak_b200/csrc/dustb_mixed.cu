@@ -802,12 +802,11 @@ __device__ __forceinline__ void move_particle(const PBuf &S, const PBuf &D, cons
     nv[1] = P.gam0 * v[1] + P.gam1 * v1[1] + P.bdt * fy + atw * r[1];
     nv[2] = P.gam0 * v[2] + P.gam1 * v1[2] + P.bdt * fz + atw * r[2];
     if (P.u0 && mass > 0.0f) {
-      // the same update in FP64 from the stored inputs: the gas's coefficients, the exact kick
-      // (c times the FP64 residual) in the velocity and, over a dt, in the rate; the ledger
-      // takes m times what the stored FP32 velocity left out.  Stage 1 (g0 = 1, g1 = 0, no
-      // history term) has only the kick; its register copy v1 is the stored velocity (no
-      // forces) or carries the forces' own rounding (the shearing box, which does not
-      // conserve momentum)
+      // the same update in FP64 from the stored inputs (the gas's coefficients, the exact kick
+      // -- c times the FP64 residual -- in the velocity and, over a dt, in the rate), stored
+      // rounded once to FP32 (half an ulp, where the FP32 chain leaves up to two); the ledger
+      // takes m times what the rounding left out.  Stage 1 (g0 = 1, g1 = 0, no history term)
+      // has only the kick, and its register copy is the kicked velocity rounded the same way
       const float fv[3] = {P.bdt * fx, P.bdt * fy, P.bdt * fz};
       const double mm = (double)mass;
 #pragma unroll
@@ -816,7 +815,10 @@ __device__ __forceinline__ void move_particle(const PBuf &S, const PBuf &D, cons
         double want = base;
         if (P.stage2)
           want = fma(P.atw, fma(dk[a], P.inv_adt, (double)rb[a]), fma(P.g1, (double)v1[a], P.g0 * base));
+        else
+          v1[a] = __double2float_rn(base);
         if (P.sbox) want += (double)fv[a];
+        nv[a] = __double2float_rn(want);
         comp[a] = mm * (want - (double)nv[a]);
       }
     }
@@ -1524,11 +1526,15 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
           cta_sync(wmask);
           // (four particles per thread at a time, their velocity loads issued together)
           constexpr int U = 4;
-          // the dust side of the tile's momentum ledger (FP64): the momentum m (v' - v) the
-          // particles received, v' the stored FP32 velocity, and the part m (v' - v)/(a dt) - m R
-          // of the rate that the FP32 rate R leaves out (the history term reads R)
-          double le[3] = {0.0, 0.0, 0.0}, lr[3] = {0.0, 0.0, 0.0};
-          const double inv_adt64 = 1.0 / T.a_dt;
+          // the dust side of the tile's momentum ledger: the momentum m (v' - v) the particles
+          // received (v' the stored FP32 velocity) and the part m (v' - v)/(a dt) - m R of the
+          // rate that the FP32 rate R leaves out (the history term reads R).  With
+          // v' = v + dv - err (err the exact error of the FP32 sum) and m dv = pm + em (pm the
+          // FP32 product, em its exact error), m (v' - v) = pm + em - m err: the large part pm
+          // summed in FP64, the small ones (of order 1e-8 of it) in FP32
+          double le[3] = {0.0, 0.0, 0.0};
+          float ls[3] = {0.0f, 0.0f, 0.0f}, lr[3] = {0.0f, 0.0f, 0.0f};
+          const float dinv = (float)(1.0 / T.a_dt - (double)inv_adt);   // 1/(a dt) - FP32 1/(a dt)
           for (int x0 = tid; x0 < cnt; x0 += U * blockDim.x) {
             float v[U][3];
   #pragma unroll
@@ -1548,12 +1554,18 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
               S.f[F_VX][p] = vn[0]; S.f[F_VY][p] = vn[1]; S.f[F_VZ][p] = vn[2];
               S.f[F_RX][p] = rn[0]; S.f[F_RY][p] = rn[1]; S.f[F_RZ][p] = rn[2];
               if (T.ledger) {
-                const double mp = (double)s_f[4 * CH + s];
+                const float mf = s_f[4 * CH + s];
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
-                  const double act = (double)vn[a] - (double)v[u][a];
-                  le[a] += mp * act;
-                  if (T.hfield) lr[a] += mp * (act * inv_adt64 - (double)rn[a]);
+                  const float bb = __fsub_rn(vn[a], v[u][a]);
+                  const float err = __fadd_rn(__fsub_rn(v[u][a], __fsub_rn(vn[a], bb)),
+                                              __fsub_rn(dv[a], bb));   // v + dv = vn + err
+                  const float pm = __fmul_rn(mf, dv[a]);
+                  const float em = fmaf(mf, dv[a], -pm);                // m dv = pm + em
+                  le[a] += (double)pm;
+                  ls[a] += em - mf * err;
+                  // (m (v' - v)/(a dt) - m R = m (dv inv - R + dv dinv - err / (a dt)))
+                  if (T.hfield) lr[a] += mf * (fmaf(dv[a], inv_adt, -rn[a]) + dv[a] * dinv - err * inv_adt);
                 }
               }
             }
@@ -1561,10 +1573,10 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
           if (T.ledger) {
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-              const double e = warp_sum(wmask, le[a]);
+              const double e = warp_sum(wmask, le[a] + (double)ls[a]);
               if (lane == 0) atomicAdd(&s_ledger[a], e);
               if (T.hfield) {
-                const double r = warp_sum(wmask, lr[a]);
+                const double r = warp_sum(wmask, (double)lr[a]);
                 if (lane == 0) atomicAdd(&s_ledger[3 + a], r);
               }
             }
@@ -1633,20 +1645,22 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
     if (MODE == MODE_KICK && T.ledger && P1 > P0) {
       // the tile's momentum ledger closed: what the gas received from the FP32 sums and what
       // the particles received differ by the FP32 rounding of weights, products and sums; the
-      // difference goes to the gas, spread evenly over the tile's cells, so that gas and dust
-      // exchange exactly opposite momenta (FP64 round-off) and no cell takes a tile's worth of
-      // rounding.  The rate's rounding goes to the history field the same way (the next
-      // stage's history term adds it to the gas as it adds the gas rate)
+      // difference goes to the gas in equal parts at the first cell of each warp's cells, so
+      // that gas and dust exchange exactly opposite momenta (FP64 round-off) and no cell takes
+      // a tile's worth of rounding.  The rate's rounding goes to the history field the same
+      // way (the next stage's history term adds it to the gas as it adds the gas rate)
       cta_sync(wmask);
-      const double share = 1.0 / (G.vol * (double)nct);
-      const int cj = tid / nx1, ci = tid - cj * nx1;
-      const long long at = G.at(m, 3, 0, G.ks + k, G.js + j0 + cj, G.is + ci);
+      if (lane == 0) {
+        const double share = 1.0 / (G.vol * (double)nwarp);
+        const int cj = tid / nx1, ci = tid - cj * nx1;
+        const long long at = G.at(m, 3, 0, G.ks + k, G.js + j0 + cj, G.is + ci);
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const double r = -(s_ledger[a] + s_ledger[6 + a]);
-        if (r != 0.0) atomicAdd(&T.dfield[at + a * G.vstride], r * share);
-        if (T.hfield && s_ledger[3 + a] != 0.0)
-          atomicAdd(&T.hfield[at + a * G.vstride], s_ledger[3 + a] * share);
+        for (int a = 0; a < 3; ++a) {
+          const double r = -(s_ledger[a] + s_ledger[6 + a]);
+          if (r != 0.0) atomicAdd(&T.dfield[at + a * G.vstride], r * share);
+          if (T.hfield && s_ledger[3 + a] != 0.0)
+            atomicAdd(&T.hfield[at + a * G.vstride], s_ledger[3 + a] * share);
+        }
       }
     }
     if (MODE == MODE_QP) {
