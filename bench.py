@@ -314,12 +314,14 @@ def run_ours(args, rep):
     del graph
     # the cost of the momentum ledgers (exact conservation): the same cycle with them off
     # (DUSTB_MIXED_NO_LEDGER), timed the same way
-    mx.mp.variant |= 16
-    mx.imex_cycle(dt)
-    graph = mx.capture(lambda: mx.imex_cycle(dt))
-    ms_no_ledger = maxall(timed_cycles(graph.replay, args.steps, stream))
-    del graph
-    mx.mp.variant &= ~16
+    ms_no_ledger = None
+    if args.ledger_timing:
+        mx.mp.variant |= 16
+        mx.imex_cycle(dt)
+        graph = mx.capture(lambda: mx.imex_cycle(dt))
+        ms_no_ledger = maxall(timed_cycles(graph.replay, args.steps, stream))
+        del graph
+        mx.mp.variant &= ~16
     if args.mixed_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": rep.throughput(npart, ms_mixed),
@@ -804,6 +806,8 @@ def main():
     ap.add_argument("--cells", type=int, default=0,
                     help="a cubic mesh of this many cells per side (profiling cases)")
     ap.add_argument("--mixed-only", action="store_true", help="time the mixed form only")
+    ap.add_argument("--no-ledger-timing", dest="ledger_timing", action="store_false",
+                    help="skip the timing of the cycle without the momentum ledgers")
     ap.add_argument("--no-pc2", action="store_true",
                     help="skip the stratified pc2 workload (128x128x256, 29.4 M particles)")
     ap.add_argument("--no-ensemble", action="store_true",
