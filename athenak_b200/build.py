@@ -23,6 +23,7 @@ UNITS = {
     "dustb_mixed.cu": [],
     "dustb_seed.cu": [],
     "dustb_output.cu": [],
+    "dustb_amr.cu": ["--fmad=false"],
 }
 
 

@@ -156,6 +156,8 @@ SIGNATURES = {
     "dustb_ghost_add": [CTXP, VP, I, VP],
     "dustb_ghost_copy": [CTXP, VP, I, I, VP],
     "dustb_ghost_add_plan": [CTXP, C.POINTER(DustbDepPlan), VP, I, VP],
+    "dustb_ghost_copy_ml_bytes": [MESHP, I],
+    "dustb_ghost_copy_ml": [CTXP, VP, I, VP, LL, VP],
     "dustb_solve_ustar": [CTXP, VP],
     "dustb_dc1_sweep": [CTXP, D, D, VP],
     "dustb_gather_kick_pmbr": [CTXP, D, D, VP],
@@ -197,7 +199,7 @@ SIGNATURES = {
     "dustb_pbin_pack": [CTXP, VP, I, I, I, VP, VP],
     "dustb_pbin_shuffle": [VP, LL, I, LL, VP, VP],
 }
-RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_phst_scratch_bytes": LL,
+RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_ghost_copy_ml_bytes": LL, "dustb_phst_scratch_bytes": LL,
             "dustb_pbin_scratch_bytes": LL, "dustb_cloud_gpack_bytes": LL,
             "dustb_last_error": C.c_char_p}
 # declared by athenak_b200.mixed (they take its DustbMixedParams struct)

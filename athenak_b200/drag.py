@@ -203,6 +203,18 @@ class DeviceDust:
                                       self.t["plan_src"].data_ptr(),
                                       self.t["plan_w"].data_ptr())
 
+    def ghost_copy_ml(self, name, nvar, stream=None):
+        """The copy exchange of a refined mesh (dustb_ghost_copy_ml) with its coarse-array
+        scratch."""
+        nb = int(self.lib.dustb_ghost_copy_ml_bytes(C.byref(self.ctx.mesh), nvar))
+        if nb <= 0:
+            raise RuntimeError("dustb_ghost_copy_ml_bytes rejected the mesh")
+        ca = self.t.get("coarse")
+        if ca is None or ca.numel() * 8 < nb:
+            ca = self.t["coarse"] = torch.empty(nb // 8, dtype=torch.float64, device=self.device)
+        self._call("ghost_copy_ml", self.t[name].data_ptr(), nvar, ca.data_ptr(), nb,
+                   stream=stream)
+
     def ghost_add_plan(self, name, nvar, stream=None):
         """MeshBoundaryValuesDep's general path on a refined mesh: the ghost deposits of name
         remapped by the plan of set_dep_plan (dustb_ghost_add_plan)."""

@@ -218,6 +218,19 @@ typedef struct dustb_dep_plan {
 int dustb_ghost_add_plan(const dustb_ctx *ctx, const dustb_dep_plan *plan, double *field,
                          int nvar, void *stream);
 
+/* The copy exchange of a cell-centred field on a refined 3-D mesh (ctx->mesh.nghbr_ml and
+ * mb_lev set; periodic; even nx and ng, nx >= 2 ng): AthenaK's multilevel boundary values as
+ * the dust module's u* exchange uses them (DustGasDrag::SendUstar / RecvUstar /
+ * FinishUstarGhosts, src/dust/dust_tasks.cpp:262-442): restriction into every block's coarse
+ * array (MeshRefinement::RestrictCC), the exchange with same-level, coarser and finer
+ * neighbours in the index boxes of MeshBoundaryValuesCC::InitSendIndices / InitRecvIndices
+ * (src/bvals/buffs_cc.cpp), FillCoarseInBndryCC and the min-mod ProlongateCC
+ * (src/bvals/prolongation.cpp, src/mesh/prolongation.hpp).  coarse: device scratch of
+ * dustb_ghost_copy_ml_bytes (the coarse arrays, cleared at every call). */
+long long dustb_ghost_copy_ml_bytes(const dustb_mesh *mesh, int nvar);
+int dustb_ghost_copy_ml(const dustb_ctx *ctx, double *field, int nvar, double *coarse,
+                        long long coarse_bytes, void *stream);
+
 /* GasImplicitSolve's per-cell solve (dust_pm.cpp:426-436 and the dc1 local guess,
  * dust_solver.cpp:643-649): ustar = (u0.m + P)/(rho + Q) over active cells. */
 int dustb_solve_ustar(const dustb_ctx *ctx, void *stream);

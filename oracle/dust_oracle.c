@@ -2296,3 +2296,211 @@ void oracle_dep_apply(int nseg, const int *seg_tgt, const int *seg_ptr, const in
     }
   }
 }
+
+/* ---- the copy exchange of a cell-centred field on a refined 3-D mesh ------------------------
+ * AthenaK's multilevel cell-centred boundary values as the u* exchange uses them
+ * (src/dust/dust_tasks.cpp:262-442): RestrictCC (src/mesh/mesh_refinement.cpp:1829-1880),
+ * PackAndSendCC / RecvAndUnpackCC with the boxes of InitSendIndices / InitRecvIndices
+ * (src/bvals/bvals_cc.cpp:53-460, src/bvals/buffs_cc.cpp:28-410), FillCoarseInBndryCC and
+ * ProlongateCC with ProlongCC's min-mod slopes (src/bvals/prolongation.cpp:29-230,
+ * src/mesh/prolongation.hpp:21-80).  The exchange runs as the reference's does, sender by
+ * sender: every block packs the box of each slot and it lands in the receiver's buffer of the
+ * slot the neighbour table names as its destination (MeshBlock::SetNeighbors' dest,
+ * src/mesh/meshblock.cpp:142-420).  ca: nmb x nvar x (nx/2 + 2 ng)^3 scratch (cleared). */
+static int nbr_index(int ix, int iy, int iz, int n1, int n2) {
+  const int ax = ix < 0 ? -ix : ix, ay = iy < 0 ? -iy : iy;
+  if (iz == 0) {
+    if (ix*iy == 0) return ax*2*(ix + 1) + ay*2*(iy + 5) + n1 + 2*n2;
+    return 16 + (ix + 1) + 2*(iy + 1) + n1;
+  }
+  if (ix*iy == 0) return 24 + ax*(ix + 9) + ay*(iy + 17) + 2*(iz + 1) + n1 + 2*n2;
+  return 48 + (ix + 1)/2 + (iy + 1) + 2*(iz + 1);
+}
+
+typedef struct { int lo[3], hi[3]; } MlBox;
+typedef struct { int nx[3], cnx[3], ng, is[3], ie[3], cis[3], cie[3], n[3], cn[3]; } MlGeo;
+
+static void ml_slots(int tab[56][5]) {
+  int s;
+#define PUT(ix, iy, iz, a, b) do { s = nbr_index(ix, iy, iz, a, b); tab[s][0] = ix; \
+    tab[s][1] = iy; tab[s][2] = iz; tab[s][3] = a; tab[s][4] = b; } while (0)
+  for (int n = -1; n <= 1; n += 2) for (int fz = 0; fz < 2; ++fz) for (int fy = 0; fy < 2; ++fy) PUT(n, 0, 0, fy, fz);
+  for (int m = -1; m <= 1; m += 2) for (int fz = 0; fz < 2; ++fz) for (int fx = 0; fx < 2; ++fx) PUT(0, m, 0, fx, fz);
+  for (int m = -1; m <= 1; m += 2) for (int n = -1; n <= 1; n += 2) for (int fz = 0; fz < 2; ++fz) PUT(n, m, 0, fz, 0);
+  for (int l = -1; l <= 1; l += 2) for (int fy = 0; fy < 2; ++fy) for (int fx = 0; fx < 2; ++fx) PUT(0, 0, l, fx, fy);
+  for (int l = -1; l <= 1; l += 2) for (int n = -1; n <= 1; n += 2) for (int fy = 0; fy < 2; ++fy) PUT(n, 0, l, fy, 0);
+  for (int l = -1; l <= 1; l += 2) for (int m = -1; m <= 1; m += 2) for (int fx = 0; fx < 2; ++fx) PUT(0, m, l, fx, 0);
+  for (int l = -1; l <= 1; l += 2) for (int m = -1; m <= 1; m += 2) for (int n = -1; n <= 1; n += 2) PUT(n, m, l, 0, 0);
+#undef PUT
+}
+
+/* InitSendIndices (3-D): kind 0 isame, 1 icoar (to a coarser neighbour), 2 ifine (to a finer) */
+static MlBox ml_send(const MlGeo *g, const int *t, int kind) {
+  MlBox b;
+  const int ox1 = t[0], ox2 = t[1], ox3 = t[2], f1 = t[3], f2 = t[4], ng1 = g->ng - 1;
+  const int o[3] = {ox1, ox2, ox3};
+  for (int d = 0; d < 3; ++d) {
+    const int s = (kind == 1) ? g->cis[d] : g->is[d], e = (kind == 1) ? g->cie[d] : g->ie[d];
+    b.lo[d] = (o[d] > 0) ? (e - ng1) : s;
+    b.hi[d] = (o[d] < 0) ? (s + ng1) : e;
+  }
+  if (kind == 2) {
+    if (ox1 == 0) { if (f1 == 1) b.lo[0] += g->cnx[0] - g->ng; else b.hi[0] -= g->cnx[0] - g->ng; }
+    if (ox2 == 0) {
+      const int f = (ox1 != 0) ? f1 : f2;
+      if (f == 1) b.lo[1] += g->cnx[1] - g->ng; else b.hi[1] -= g->cnx[1] - g->ng;
+    }
+    if (ox3 == 0) {
+      const int f = (ox1 != 0 && ox2 != 0) ? f1 : f2;
+      if (f == 1) b.lo[2] += g->cnx[2] - g->ng; else b.hi[2] -= g->cnx[2] - g->ng;
+    }
+  }
+  return b;
+}
+
+/* InitRecvIndices (3-D): kind 0 isame, 1 icoar (from a coarser neighbour, into the coarse
+ * array), 2 ifine (from a finer neighbour), 3 iprol (coarse cells to prolongate) */
+static MlBox ml_recv(const MlGeo *g, const int *t, int kind) {
+  MlBox b;
+  const int o[3] = {t[0], t[1], t[2]}, f1 = t[3], f2 = t[4];
+  const int w = (kind == 3) ? g->ng/2 : g->ng;
+  for (int d = 0; d < 3; ++d) {
+    const int coarse = (kind == 1 || kind == 3);
+    const int s = coarse ? g->cis[d] : g->is[d], e = coarse ? g->cie[d] : g->ie[d];
+    if (o[d] > 0) { b.lo[d] = e + 1; b.hi[d] = e + w; continue; }
+    if (o[d] < 0) { b.lo[d] = s - w; b.hi[d] = s - 1; continue; }
+    b.lo[d] = s; b.hi[d] = e;
+    const int f = (d == 0) ? f1 : ((d == 1) ? ((o[0] != 0) ? f1 : f2)
+                                            : ((o[0] != 0 && o[1] != 0) ? f1 : f2));
+    if (kind == 1 || kind == 3) { if (f == 0) b.hi[d] += w; else b.lo[d] -= w; }
+    else if (kind == 2) { if (f == 1) b.lo[d] += g->cnx[d]; else b.hi[d] -= g->cnx[d]; }
+  }
+  return b;
+}
+
+#define ML_F(m, v, k, j, i) a[((((size_t)(m)*nvar + (v))*g.n[2] + (k))*g.n[1] + (j))*g.n[0] + (i)]
+#define ML_C(m, v, k, j, i) ca[((((size_t)(m)*nvar + (v))*g.cn[2] + (k))*g.cn[1] + (j))*g.cn[0] + (i)]
+
+void oracle_ghost_copy_ml(const dustb_ctx *c, double *a, int nvar, double *ca) {
+  const dustb_mesh *ms = &c->mesh;
+  MlGeo g;
+  const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
+  g.ng = ms->ng;
+  for (int d = 0; d < 3; ++d) {
+    g.nx[d] = nx[d]; g.cnx[d] = nx[d]/2; g.is[d] = ms->ng; g.ie[d] = ms->ng + nx[d] - 1;
+    g.cis[d] = ms->ng; g.cie[d] = ms->ng + nx[d]/2 - 1;
+    g.n[d] = nx[d] + 2*ms->ng; g.cn[d] = nx[d]/2 + 2*ms->ng;
+  }
+  int tab[56][5];
+  ml_slots(tab);
+  const int nmb = ms->nmb;
+  memset(ca, 0, (size_t)nmb*nvar*g.cn[0]*g.cn[1]*g.cn[2]*sizeof(double));
+  /* RestrictCC */
+  for (int m = 0; m < nmb; ++m)
+    for (int v = 0; v < nvar; ++v)
+      for (int k = g.cis[2]; k <= g.cie[2]; ++k)
+        for (int j = g.cis[1]; j <= g.cie[1]; ++j)
+          for (int i = g.cis[0]; i <= g.cie[0]; ++i) {
+            const int fi = (i - g.cis[0])*2 + g.is[0], fj = (j - g.cis[1])*2 + g.is[1];
+            const int fk = (k - g.cis[2])*2 + g.is[2];
+            ML_C(m, v, k, j, i) = 0.125*(ML_F(m, v, fk, fj, fi) + ML_F(m, v, fk, fj, fi + 1)
+                + ML_F(m, v, fk, fj + 1, fi) + ML_F(m, v, fk, fj + 1, fi + 1)
+                + ML_F(m, v, fk + 1, fj, fi) + ML_F(m, v, fk + 1, fj, fi + 1)
+                + ML_F(m, v, fk + 1, fj + 1, fi) + ML_F(m, v, fk + 1, fj + 1, fi + 1));
+          }
+  /* the exchange, sender by sender (every block's active or coarse cells are read, only
+   * ghost cells are written, so the order does not matter) */
+  for (int s = 0; s < nmb; ++s) {
+    const int lev_s = ms->mb_lev[s];
+    int myf[3];
+    for (int d = 0; d < 3; ++d) {
+      const double lo = (d == 0) ? ms->x1min : ((d == 1) ? ms->x2min : ms->x3min);
+      const double l = MB(s, X1MAX + d) - MB(s, X1MIN + d);
+      myf[d] = ((int)floor((MB(s, X1MIN + d) - lo)/l + 0.5)) & 1;
+    }
+    for (int n = 0; n < 56; ++n) {
+      const int gr = ms->nghbr_ml[(size_t)s*56 + n];
+      if (gr < 0) continue;
+      const int r = gr - ms->gids;
+      const int lev_r = ms->mb_lev[r];
+      const int *t = tab[n];
+      const int kind = (lev_r < lev_s) ? 1 : ((lev_r == lev_s) ? 0 : 2);
+      const MlBox sb = ml_send(&g, t, kind);
+      /* the receiver's slot pointing back (SetNeighbors' dest) */
+      const int nd = abs(t[0]) + abs(t[1]) + abs(t[2]);
+      int dn;
+      if (lev_r == lev_s || nd == 3) dn = nbr_index(-t[0], -t[1], -t[2], 0, 0);
+      else if (lev_r > lev_s) dn = nbr_index(-t[0], -t[1], -t[2], t[3], nd == 1 ? t[4] : 0);
+      else if (nd == 1) {
+        if (t[0] != 0) dn = nbr_index(-t[0], 0, 0, myf[1], myf[2]);
+        else if (t[1] != 0) dn = nbr_index(0, -t[1], 0, myf[0], myf[2]);
+        else dn = nbr_index(0, 0, -t[2], myf[0], myf[1]);
+      } else {
+        const int fd = (t[0] == 0) ? 0 : ((t[1] == 0) ? 1 : 2);
+        dn = nbr_index(-t[0], -t[1], -t[2], myf[fd], 0);
+      }
+      /* the receiver's box for the sender's level */
+      const int rkind = (lev_s < lev_r) ? 1 : ((lev_s == lev_r) ? 0 : 2);
+      const MlBox rb = ml_recv(&g, tab[dn], rkind);
+      const int ni = sb.hi[0] - sb.lo[0] + 1, nj = sb.hi[1] - sb.lo[1] + 1;
+      const int nk = sb.hi[2] - sb.lo[2] + 1;
+      for (int v = 0; v < nvar; ++v)
+        for (int dk = 0; dk < nk; ++dk)
+          for (int dj = 0; dj < nj; ++dj)
+            for (int di = 0; di < ni; ++di) {
+              const double val = (kind == 1) ? ML_C(s, v, sb.lo[2] + dk, sb.lo[1] + dj, sb.lo[0] + di)
+                                             : ML_F(s, v, sb.lo[2] + dk, sb.lo[1] + dj, sb.lo[0] + di);
+              if (rkind == 1) ML_C(r, v, rb.lo[2] + dk, rb.lo[1] + dj, rb.lo[0] + di) = val;
+              else ML_F(r, v, rb.lo[2] + dk, rb.lo[1] + dj, rb.lo[0] + di) = val;
+            }
+    }
+  }
+  /* FillCoarseInBndryCC: the coarse ghost cells next to same-level neighbours */
+  for (int m = 0; m < nmb; ++m)
+    for (int n = 0; n < 56; ++n) {
+      const int gs = ms->nghbr_ml[(size_t)m*56 + n];
+      if (gs < 0 || ms->mb_lev[gs - ms->gids] != ms->mb_lev[m]) continue;
+      const MlBox fb = ml_recv(&g, tab[n], 0);
+      for (int v = 0; v < nvar; ++v)
+        for (int k = (fb.lo[2] + g.cis[2])/2; k <= (fb.hi[2] + g.cis[2])/2; ++k)
+          for (int j = (fb.lo[1] + g.cis[1])/2; j <= (fb.hi[1] + g.cis[1])/2; ++j)
+            for (int i = (fb.lo[0] + g.cis[0])/2; i <= (fb.hi[0] + g.cis[0])/2; ++i) {
+              const int fi = (i - g.cis[0])*2 + g.is[0], fj = (j - g.cis[1])*2 + g.is[1];
+              const int fk = (k - g.cis[2])*2 + g.is[2];
+              ML_C(m, v, k, j, i) = 0.125*(ML_F(m, v, fk, fj, fi) + ML_F(m, v, fk, fj, fi + 1)
+                  + ML_F(m, v, fk, fj + 1, fi) + ML_F(m, v, fk, fj + 1, fi + 1)
+                  + ML_F(m, v, fk + 1, fj, fi) + ML_F(m, v, fk + 1, fj, fi + 1)
+                  + ML_F(m, v, fk + 1, fj + 1, fi) + ML_F(m, v, fk + 1, fj + 1, fi + 1));
+            }
+    }
+  /* ProlongateCC: the fine ghost cells next to coarser neighbours */
+  for (int m = 0; m < nmb; ++m)
+    for (int n = 0; n < 56; ++n) {
+      const int gs = ms->nghbr_ml[(size_t)m*56 + n];
+      if (gs < 0 || ms->mb_lev[gs - ms->gids] >= ms->mb_lev[m]) continue;
+      const MlBox pb = ml_recv(&g, tab[n], 3);
+      for (int v = 0; v < nvar; ++v)
+        for (int k = pb.lo[2]; k <= pb.hi[2]; ++k)
+          for (int j = pb.lo[1]; j <= pb.hi[1]; ++j)
+            for (int i = pb.lo[0]; i <= pb.hi[0]; ++i) {
+#define SLOPE(dl, dr) (0.125*((((dl) < 0.0) ? -1.0 : 1.0) + (((dr) < 0.0) ? -1.0 : 1.0))*fmin(fabs(dl), fabs(dr)))
+              const double cc = ML_C(m, v, k, j, i);
+              const double d1 = SLOPE(cc - ML_C(m, v, k, j, i - 1), ML_C(m, v, k, j, i + 1) - cc);
+              const double d2 = SLOPE(cc - ML_C(m, v, k, j - 1, i), ML_C(m, v, k, j + 1, i) - cc);
+              const double d3 = SLOPE(cc - ML_C(m, v, k - 1, j, i), ML_C(m, v, k + 1, j, i) - cc);
+#undef SLOPE
+              const int fi = (i - g.cis[0])*2 + g.is[0], fj = (j - g.cis[1])*2 + g.is[1];
+              const int fk = (k - g.cis[2])*2 + g.is[2];
+              ML_F(m, v, fk, fj, fi) = cc - d1 - d2 - d3;
+              ML_F(m, v, fk, fj, fi + 1) = cc + d1 - d2 - d3;
+              ML_F(m, v, fk, fj + 1, fi) = cc - d1 + d2 - d3;
+              ML_F(m, v, fk, fj + 1, fi + 1) = cc + d1 + d2 - d3;
+              ML_F(m, v, fk + 1, fj, fi) = cc - d1 - d2 + d3;
+              ML_F(m, v, fk + 1, fj, fi + 1) = cc + d1 - d2 + d3;
+              ML_F(m, v, fk + 1, fj + 1, fi) = cc - d1 + d2 + d3;
+              ML_F(m, v, fk + 1, fj + 1, fi + 1) = cc + d1 + d2 + d3;
+            }
+    }
+}
+#undef ML_F
+#undef ML_C

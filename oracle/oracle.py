@@ -84,6 +84,7 @@ def lib():
             "oracle_cloud_pc2_cycle": ([P, D, VP, VP], C.c_uint),
             "oracle_dep_plan": ([VP, I, VP, VP, VP, VP, VP, VP, C.c_longlong, C.c_longlong], I),
             "oracle_dep_apply": ([I, VP, VP, VP, VP, VP, I, I], None),
+            "oracle_ghost_copy_ml": ([P, VP, I, VP], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(_lib, name)
@@ -161,6 +162,14 @@ class Oracle:
 
     def ghost_copy(self, name, nvar, x3_bcs=1):
         self.call("ghost_copy", self.arr[name].ctypes.data, nvar, x3_bcs)
+
+    def ghost_copy_ml(self, name, nvar):
+        """The copy exchange of a refined mesh (restriction, same / coarser / finer neighbours,
+        prolongation)."""
+        ms = self.mesh
+        cn = [ms.nx[a] // 2 + 2 * ms.ng for a in range(3)]
+        ca = np.zeros(ms.nmb * nvar * cn[0] * cn[1] * cn[2])
+        self.call("ghost_copy_ml", self.arr[name].ctypes.data, nvar, ca.ctypes.data)
 
     def solve_ustar(self):
         self.call("solve_ustar")

@@ -197,3 +197,63 @@ def test_slot_search_finds_the_block_that_holds_the_position():
                 assert own.tolist() == [g], (m, o, s, g, own)
                 checked += 1
     assert checked == ms.nmb * 26 * 4
+
+
+def _linear_field(ms, nvar, sentinel):
+    """A field linear in the position of every cell centre (f_v = 1 + v + 0.3 x - 0.7 y + 1.1 z),
+    with the ghost cells set to sentinel."""
+    n1, n2, n3 = ms.n
+    g = ms.ng
+    a = np.full(ms.field_shape(nvar), sentinel)
+    cen = []
+    for m in range(ms.nmb):
+        mb = ms.mb_size[m]
+        xs = [mb[d] + (np.arange(ms.n[d]) - g + 0.5) * mb[6 + d] for d in range(3)]
+        Z, Y, X = np.meshgrid(xs[2], xs[1], xs[0], indexing="ij")
+        cen.append((X, Y, Z))
+        for v in range(nvar):
+            f = 1.0 + v + 0.3 * X - 0.7 * Y + 1.1 * Z
+            a[m, v, g:n3 - g, g:n2 - g, g:n1 - g] = f[g:n3 - g, g:n2 - g, g:n1 - g]
+    return a, cen
+
+
+def test_refined_copy_exchange_is_exact_for_a_linear_field():
+    """The oracle's copy exchange of a refined mesh fills every ghost cell of a block away from
+    the domain faces with the value of a linear field there: same-level copies, restrictions
+    (the mean of 8 cells is the centre value) and min-mod prolongation (equal one-sided
+    slopes) are all exact for it, at every level difference."""
+    ms = mesh("sphere_2lev")
+    st = refined_state(ms, [0.1], [1.0], 1, seed=3)
+    o = oracle.Oracle(st, dict(scheme=2))
+    a, cen = _linear_field(ms, 3, 1e30)
+    o.arr["work"][...] = a
+    o.ghost_copy_ml("work", 3)
+    b = o.arr["work"]
+    span = [ms.hi[d] - ms.lo[d] for d in range(3)]
+    checked = 0
+    for m in range(ms.nmb):
+        mb = ms.mb_size[m]
+        # (blocks whose ghost zone stays inside the domain: no periodic image)
+        if any(mb[d] - 3 * ms.ng * mb[6 + d] < ms.lo[d] or mb[3 + d] + 3 * ms.ng * mb[6 + d] > ms.hi[d]
+               for d in range(3)):
+            continue
+        X, Y, Z = cen[m]
+        for v in range(3):
+            f = 1.0 + v + 0.3 * X - 0.7 * Y + 1.1 * Z
+            assert np.abs(b[m, v] - f).max() < 1e-12 * max(span), (m, v)
+        checked += 1
+    assert checked > 20
+    assert not np.any(b >= 1e29)
+
+
+def test_refined_copy_exchange_keeps_a_constant():
+    ms = mesh("offcentre_4x2x2")
+    st = refined_state(ms, [0.1], [1.0], 1, seed=3)
+    o = oracle.Oracle(st, dict(scheme=2))
+    a = np.full(ms.field_shape(3), np.nan)
+    g = ms.ng
+    n1, n2, n3 = ms.n
+    a[:, :, g:n3 - g, g:n2 - g, g:n1 - g] = 2.5
+    o.arr["work"][...] = a
+    o.ghost_copy_ml("work", 3)
+    np.testing.assert_array_equal(o.arr["work"], np.full(a.shape, 2.5))
