@@ -173,6 +173,8 @@ SIGNATURES = {
     "dustb_pc2_advance": [CTXP, D, VP],
     "dustb_pc2_commit": [CTXP, D, VP],
     "dustb_imex_cycle": [CTXP, C.POINTER(DustbImexCoeffs), VP, VP],
+    "dustb_refined_imex_cycle": [CTXP, C.POINTER(DustbDepPlan), C.POINTER(DustbImexCoeffs), VP,
+                                 LL, VP, VP],
     "dustb_pc2_cycle": [CTXP, D, VP, VP, VP],
     "dustb_seed_uniform": [CTXP, C.POINTER(DustbSeedDesc), VP],
     "dustb_cell_index_static": [CTXP, VP, VP, VP],

@@ -2447,6 +2447,60 @@ int dustb_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co, double *x3
   return DUSTB_OK;
 }
 
+// one imex2+ cycle on a refined mesh: the task order of dustb_imex_cycle with the deposits
+// exchanged by the general remap and u*, the operator's field and the gas state by the
+// multilevel copy exchange
+int dustb_refined_imex_cycle(const dustb_ctx *c, const dustb_dep_plan *plan,
+                             const dustb_imex_coeffs *co, double *coarse, long long coarse_bytes,
+                             double *x3_removed, void *stream) {
+  CHECK_CTX(c);
+  if (!co || !(co->dt > 0.0) || !plan || !c->mesh.nghbr_ml) return DUSTB_EINVAL;
+  if (co->sh[0] != 0.0 || co->sh[1] != 0.0) return DUSTB_EUNSUP;    // (no shearing box)
+  const double g = co->gamma, dt = co->dt;
+  const double gam0[2] = {1.0, (2.0 * g - 1.0) / (2.0 * g * g)};
+  const double gam1[2] = {0.0, 1.0 - (2.0 * g - 1.0) / (2.0 * g * g)};
+  const double beta[2] = {g, 1.0 / (2.0 * g)};
+  const double atw22 = (1.0 - 2.0 * g * g) / 2.0 / g;
+  const double a_dt = g * dt;
+  const int br = c->phys.back_reaction;
+  Ind d = make_ind(c->mesh);
+  int rc;
+  for (int stage = 1; stage <= 2; ++stage) {
+    if (stage == 1) RUN(dustb_register_copy(c, stream));
+    RUN(dustb_gas_rk_noflux(c, gam0[stage - 1], gam1[stage - 1], stream));
+    if (stage == 2 && br) RUN(dustb_history_gas(c, atw22 * dt, stream));
+    RUN(dustb_push_imex(c, gam0[stage - 1], gam1[stage - 1], beta[stage - 1] * dt,
+                        (stage == 2) ? atw22 * dt : 0.0, stream));
+    RUN(dustb_route(c, x3_removed, stream));
+    if (br) {
+      RUN(dustb_deposit_qp(c, a_dt, 0.0, stream));
+      RUN(dustb_ghost_add_plan(c, plan, c->f.qdep, 5, stream));
+    }
+    RUN(dustb_solve_ustar(c, stream));
+    if (br && c->phys.drag_solver >= DUSTB_SOLVER_DC1) {
+      const int nsw = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
+      for (int w = 0; w < nsw; ++w) {
+        // ApplyDefectCorrection (dust_solver.cpp:226-252) with the refined exchanges
+        RUN(dustb_ghost_copy_ml(c, c->f.ustar, 3, coarse, coarse_bytes, stream));
+        cudaMemsetAsync(c->f.work, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
+        if (c->part.npart > 0)
+          k_operator<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.ustar, c->f.work, a_dt, 0.0, c->err);
+        RUN(dustb_ghost_add_plan(c, plan, c->f.work, 3, stream));
+        k_dc_correct<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(
+            d, c->f.u0, c->f.nvar_gas, c->f.qdep, c->f.work, c->f.ustar);
+      }
+    }
+    RUN(dustb_ghost_copy_ml(c, c->f.ustar, 3, coarse, coarse_bytes, stream));
+    RUN(dustb_gather_kick_pmbr(c, a_dt, 0.0, stream));
+    if (br) {
+      RUN(dustb_ghost_add_plan(c, plan, c->f.dmom, 3, stream));
+      RUN(dustb_apply_pmbr(c, a_dt, stream));
+    }
+    RUN(dustb_ghost_copy_ml(c, c->f.u0, c->f.nvar_gas, coarse, coarse_bytes, stream));
+  }
+  return launch_status("refined_imex_cycle");
+}
+
 // one imex2+ cycle of refinable clouds on a uniform mesh: the task order of dustb_imex_cycle
 // with the clouds' deposit (into the owner cells: no deposit exchange), dc1 / dc2 sweeps,
 // gather-kick and PMBR split

@@ -269,6 +269,21 @@ class DeviceDust:
                                        _stream_ptr(stream))
         capi.check(rc, "imex_cycle")
 
+    def refined_imex_cycle(self, dt, gamma=GAMMA_DEFAULT, stream=None):
+        """One imex2+ cycle on a refined mesh (dustb_refined_imex_cycle) with the plan of
+        set_dep_plan."""
+        co = capi.DustbImexCoeffs()
+        co.gamma, co.dt = gamma, dt
+        nb = int(self.lib.dustb_ghost_copy_ml_bytes(C.byref(self.ctx.mesh),
+                                                    int(self.t["u0"].shape[1])))
+        ca = self.t.get("coarse")
+        if ca is None or ca.numel() * 8 < nb:
+            ca = self.t["coarse"] = torch.empty(nb // 8, dtype=torch.float64, device=self.device)
+        rc = self.lib.dustb_refined_imex_cycle(self.pctx, C.byref(self.plan), C.byref(co),
+                                               ca.data_ptr(), nb, self.t["x3_removed"].data_ptr(),
+                                               _stream_ptr(stream))
+        capi.check(rc, "refined_imex_cycle")
+
     def pc2_cycle(self, dt, stream=None):
         out = self.t["scalar"]
         rc = self.lib.dustb_pc2_cycle(self.pctx, dt, out.data_ptr(),

@@ -441,6 +441,16 @@ int dustb_cloud_pc2_cycle(const dustb_ctx *ctx, double dt, double *chi_max, doub
 int dustb_imex_cycle(const dustb_ctx *ctx, const dustb_imex_coeffs *c, double *x3_removed,
                      void *stream);
 
+/* One imex2+ cycle of the point-particle drag step on a refined 3-D mesh (ctx->mesh.nghbr_ml
+ * and mb_lev set): the task order of dustb_imex_cycle with the deposits exchanged by
+ * dustb_ghost_add_plan (plan: the mesh's general remap) and u*, the dc1 / dc2 operator's field
+ * and the gas state by dustb_ghost_copy_ml (coarse: its scratch, sized for the gas state's
+ * nvar_gas variables).  Periodic meshes, no implicit shear shift; the reference runs point
+ * particles on refined 3-D meshes with amr_pic = instant_switch (src/dust/dust.cpp:1301-1340). */
+int dustb_refined_imex_cycle(const dustb_ctx *ctx, const dustb_dep_plan *plan,
+                             const dustb_imex_coeffs *c, double *coarse, long long coarse_bytes,
+                             double *x3_removed, void *stream);
+
 /* One pc2 cycle (integrator rk2): predictor, apply, gas tail, midpoint, advance, route,
  * ghost add, commit.  chi_max as in dustb_pc2_apply_predictor. */
 int dustb_pc2_cycle(const dustb_ctx *ctx, double dt, double *chi_max, double *x3_removed,

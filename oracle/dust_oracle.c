@@ -770,15 +770,11 @@ static unsigned operator_particles(const dustb_ctx *c, const double *field, doub
   return err;
 }
 
-/* ApplyDefectCorrection -> ApplyCoupledOperatorImpl(correct_field = true),
- * src/dust/dust_solver.cpp:218-252 */
-unsigned oracle_dc1_sweep(const dustb_ctx *c, double a_dt, double sh) {
+/* the per-cell correction of ApplyCoupledOperatorImpl (dust_solver.cpp:240-252):
+ * u* += (rho + Q)^-1 (rho u + P - rho u* - result), result = work */
+void oracle_dc_correct(const dustb_ctx *c) {
   const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
   double *x = c->f.ustar, *r = c->f.work;
-  oracle_ghost_copy(c, x, 3, 1);
-  memset(r, 0, field_size(ms, 3)*sizeof(double));
-  unsigned err = operator_particles(c, x, r, a_dt, sh);
-  oracle_ghost_add(c, r, 3);
   for (int m = 0; m < ms->nmb; ++m)
     for (int k = d.ks; k <= d.ke; ++k)
       for (int j = d.js; j <= d.je; ++j)
@@ -792,6 +788,23 @@ unsigned oracle_dc1_sweep(const dustb_ctx *c, double a_dt, double sh) {
             A5(x, 3, d, m, v, k, j, i) += pinv*rv;
           }
         }
+}
+
+/* PointOperatorParticles of u* into work (work not cleared; sh = 0) */
+unsigned oracle_operator_particles(const dustb_ctx *c, double a_dt) {
+  return operator_particles(c, c->f.ustar, c->f.work, a_dt, 0.0);
+}
+
+/* ApplyDefectCorrection -> ApplyCoupledOperatorImpl(correct_field = true),
+ * src/dust/dust_solver.cpp:218-252 */
+unsigned oracle_dc1_sweep(const dustb_ctx *c, double a_dt, double sh) {
+  const dustb_mesh *ms = &c->mesh;
+  double *x = c->f.ustar, *r = c->f.work;
+  oracle_ghost_copy(c, x, 3, 1);
+  memset(r, 0, field_size(ms, 3)*sizeof(double));
+  unsigned err = operator_particles(c, x, r, a_dt, sh);
+  oracle_ghost_add(c, r, 3);
+  oracle_dc_correct(c);
   return err;
 }
 

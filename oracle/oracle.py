@@ -85,6 +85,8 @@ def lib():
             "oracle_dep_plan": ([VP, I, VP, VP, VP, VP, VP, VP, C.c_longlong, C.c_longlong], I),
             "oracle_dep_apply": ([I, VP, VP, VP, VP, VP, I, I], None),
             "oracle_ghost_copy_ml": ([P, VP, I, VP], None),
+            "oracle_operator_particles": ([P, D], C.c_uint),
+            "oracle_dc_correct": ([P], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(_lib, name)

@@ -7,6 +7,8 @@ deposits with its own cell size) followed by the remap must match the oracle's t
 field's scale (the deposits are atomic sums), and put the particles' whole coupled mass into
 active cells.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 import torch
@@ -211,3 +213,67 @@ def test_refined_imex_cycles_match_the_oracle():
     p1 = _total_momentum(ms, pr, u, n)
     absm = np.abs(st.pr[16, :n] * np.abs(st.pr[[1, 3, 5], :n])).sum()
     assert np.abs(p1 - p0).max() <= 1e-12 * absm
+
+
+@pytest.mark.parametrize("solver", [0, 2])
+def test_fused_refined_cycle_equals_the_task_sequence(solver):
+    """dustb_refined_imex_cycle (one launch sequence per cycle) gives what the task sequence
+    gives, for the local solver and dc1 (its sweeps exchange u* and the operator's deposits
+    across levels), and the FP64 dc1 cycle matches the oracle's task sequence with dc1."""
+    ms = _mesh()
+    plan = build_dep_plan(ms, 0)
+    st = refined_state(ms, [0.01, 0.3], [0.5, 1.0], 2, seed=8, vd=[0.8, -0.5],
+                       vel_noise=0.2, gas_noise=0.05)
+    phys = dict(scheme=2, drag_solver=solver, consistent_gas=True)
+    a = DeviceDust(st, phys)
+    a.set_dep_plan(plan)
+    dxmin = ms.mb_size[:, 6].min()
+    dt = 0.3 * dxmin / np.abs(st.pr[[1, 3, 5], :st.npart]).max()
+    for _ in range(2):
+        a.refined_imex_cycle(dt)
+    torch.cuda.synchronize()
+    assert a.error_word() == 0
+    if solver == 0:
+        b = DeviceDust(st, phys)
+        b.set_dep_plan(plan)
+        for _ in range(2):
+            _refined_cycle(b, plan, dt, True)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(a.host("pi")[0], b.host("pi")[0])
+        for r in range(16):
+            sc = max(np.abs(b.host("pr")[r]).max(), 1e-300)
+            assert np.abs(a.host("pr")[r] - b.host("pr")[r]).max() <= 1e-12 * sc, r
+        return
+    # dc1 against the oracle's tasks with the refined exchanges around its operator
+    o = oracle.Oracle(st, phys)
+    g0, g1, beta, atw22 = oracle.imex2p_coeffs(oracle.GAMMA_DEFAULT)
+    a_dt = oracle.GAMMA_DEFAULT * dt
+    L = oracle.lib()
+    for _ in range(2):
+        for stage in (1, 2):
+            if stage == 1:
+                o.register_copy()
+            o.gas_rk_noflux(g0[stage - 1], g1[stage - 1])
+            if stage == 2:
+                o.history_gas(atw22 * dt)
+            o.push_imex(g0[stage - 1], g1[stage - 1], beta[stage - 1] * dt,
+                        atw22 * dt if stage == 2 else 0.0)
+            assert o.route() == 0
+            assert o.deposit_qp(a_dt) == 0
+            oracle.dep_apply(plan, o.arr["qdep"])
+            o.solve_ustar()
+            o.ghost_copy_ml("ustar", 3)
+            o.arr["work"][...] = 0.0
+            assert L.oracle_operator_particles(C.byref(o.ctx), a_dt) == 0
+            oracle.dep_apply(plan, o.arr["work"])
+            L.oracle_dc_correct(C.byref(o.ctx))
+            o.ghost_copy_ml("ustar", 3)
+            assert o.gather_kick_pmbr(a_dt) == 0
+            oracle.dep_apply(plan, o.arr["dmom"])
+            o.apply_pmbr(a_dt)
+            o.ghost_copy_ml("u0", 4)
+    n = st.npart
+    np.testing.assert_array_equal(a.host("pi")[0], o.arr["pi"][0, :n])
+    for r in range(16):
+        sc = max(np.abs(o.arr["pr"][r, :n]).max(), 1e-300)
+        assert np.abs(a.host("pr")[r] - o.arr["pr"][r, :n]).max() <= 1e-12 * sc, r
