@@ -131,3 +131,94 @@ def stratified_box(small=False, device="cuda"):
     dev.init_gas_ghosts()
     dt = 0.3 * dxc / (1.0 + q * om * hi[0])
     return dev, ms, dict(npart=npart, ncell=ncell, dt=dt, t=t0, cells=cells)
+
+
+def clump_refined(small=False, peak_ppc=150, seed=4, device="cuda"):
+    """The refined-mesh workload of the SMR/AMR configuration with point particles: a 128^3 root
+    mesh (8^3 MeshBlocks of 16^3) with two more levels around a Gaussian dust clump at the
+    centre (peak eps = 100, sigma = 0.05 L; the root blocks within 0.33 L of the clump refined
+    once, the level-1 blocks within 0.16 L once more: 1520 blocks, 424 / 648 / 448 per level),
+    2 species t_s = {0.1, 1}/Omega.  Every cell of every block holds 1 + floor(peak_ppc *
+    exp(-r^2 / 2 sigma^2)) particles of each species (in the clump's centre blocks more than 100
+    times as many per block as far from it), placed uniformly in the cell, of mass
+    eps(x) rho V / n / 2 with eps = 0.01 + 100 exp(-r^2 / 2 sigma^2); velocities 1e-2 Gaussian
+    noise, gas rho = 1 at rest plus 1e-3 noise; the rows in cell order (as the sort keeps
+    them); dt from a CFL of 0.3 on the finest cells.  Generated on the device (torch's
+    seeded Philox stream: the placement only sets where the work lies).  small: a 32^3 root of
+    16^3 blocks refined the same way.  Returns (DeviceDust, MeshSpec, info)."""
+    import torch
+    from .amr import refined_mesh, build_dep_plan
+    from .drag import DeviceDust
+    L, sigma, peak_eps, eps_bg = 1.0, 0.05, 100.0, 0.01
+    taus = [0.1, 1.0]
+    nroot = (2, 2, 2) if small else (8, 8, 8)
+
+    def refine(e, c):
+        r = math.sqrt(sum(x * x for x in c))
+        return r < (0.33 * L if e == 0 else 0.16 * L)
+
+    ms = refined_mesh(nroot, (16, 16, 16), 2, (-L / 2,) * 3, (L / 2,) * 3, refine=refine)
+    dev_ = torch.device(device)
+    gen = torch.Generator(device=dev_)
+    gen.manual_seed(seed)
+    nx = 16
+    mb = torch.from_numpy(ms.mb_size).to(dev_)
+    nmb = ms.nmb
+    # every active cell: block, (k, j, i), centre, volume
+    kk, jj, ii = torch.meshgrid(torch.arange(nx, device=dev_), torch.arange(nx, device=dev_),
+                                torch.arange(nx, device=dev_), indexing="ij")
+    cm = torch.arange(nmb, device=dev_).repeat_interleave(nx ** 3)
+    ck, cj, ci = (t.reshape(-1).repeat(nmb) for t in (kk, jj, ii))
+    dx = mb[cm, 6:9]
+    cen = mb[cm, 0:3] + (torch.stack([ci, cj, ck], 1).double() + 0.5) * dx
+    r2 = (cen ** 2).sum(1)
+    g = torch.exp(-r2 / (2.0 * sigma ** 2))
+    ncell_p = 1 + torch.floor(peak_ppc * g).long()            # per species
+    vol = dx.prod(1)
+    eps = eps_bg + peak_eps * g
+    nper = int(ncell_p.sum().item())
+    npart = 2 * nper
+    phys = dict(scheme=2, drag_solver=0, consistent_gas=True, back_reaction=True)
+    dev = DeviceDust.empty(ms, npart, phys, device=device, nspecies=2)
+    pr, pi = dev.t["pr"], dev.t["pi"]
+    # cell of every particle of one species (cell order), then the two species cell by cell
+    cid = torch.repeat_interleave(torch.arange(cm.numel(), device=dev_), ncell_p)
+    cell2 = torch.repeat_interleave(torch.arange(cm.numel() * 2, device=dev_),
+                                    ncell_p.repeat_interleave(2))
+    c = cell2 // 2
+    sp = (cell2 % 2).int()
+    u = torch.rand((npart, 3), generator=gen, device=dev_, dtype=torch.float64)
+    lo = mb[cm[c], 0:3] + torch.stack([ci[c], cj[c], ck[c]], 1).double() * dx[c]
+    pos = lo + u * dx[c]
+    for a, (rx, rx1) in enumerate(((0, 6), (2, 8), (4, 10))):
+        pr[rx] = pos[:, a]
+        pr[rx1] = pos[:, a]
+    vel = 1e-2 * torch.randn((npart, 3), generator=gen, device=dev_, dtype=torch.float64)
+    for a, (rv, rv1) in enumerate(((1, 7), (3, 9), (5, 11))):
+        pr[rv] = vel[:, a]
+        pr[rv1] = vel[:, a]
+    pr[15] = torch.tensor(taus, device=dev_, dtype=torch.float64)[sp.long()]
+    pr[16] = 0.5 * eps[c] * vol[c] / ncell_p[c].double()
+    pi[0] = cm[c].int()
+    tag = torch.arange(npart, device=dev_, dtype=torch.int64)
+    pi[1] = (tag & 0xFFFFFFFF).int()            # PTAG the low word, PTAGH the high
+    pi[2] = sp
+    pi[4] = (tag >> 32).int()
+    u0 = dev.t["u0"]
+    u0[:, 0] = 1.0
+    u0[:, 1:4] = 1e-3 * (2.0 * torch.rand(u0[:, 1:4].shape, generator=gen, device=dev_,
+                                           dtype=torch.float64) - 1.0)
+    del cid, cell2, u, lo, pos, vel, c, sp
+    torch.cuda.synchronize()
+    plan = build_dep_plan(ms, 0)
+    dev.set_dep_plan(plan)
+    counts = torch.zeros(nmb, device=dev_, dtype=torch.long)
+    counts.index_add_(0, cm, 2 * ncell_p)
+    counts = counts.cpu().numpy()
+    dxmin = float(ms.mb_size[:, 6].min())
+    dt = 0.3 * dxmin / (1.0 + 0.05)
+    info = dict(npart=npart, ncell=int(cm.numel()), nmb=nmb, dt=dt,
+                levels=np.bincount(ms.lloc[:, 0])[ms.root_level:].tolist(),
+                block_particles_max_over_min=float(counts.max() / counts.min()),
+                plan_entries=int(plan.ent_src.size))
+    return dev, ms, info

@@ -249,6 +249,11 @@ def run_ours(args, rep):
     rank, world = rep.rank, rep.world
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     stream = torch.cuda.current_stream()
+    if args.refined_only:
+        out = measure_refined(args)
+        if rank == 0:
+            print(json.dumps(dict(out, note="refined-mesh workload only")), flush=True)
+        return
     if args.pc2_only:
         out = measure_pc2_strat(args, stream, lambda x: x, lambda: None)
         if rank == 0:
@@ -407,6 +412,10 @@ def run_ours(args, rep):
     clouds = None
     if not args.no_clouds:
         clouds = measure_clouds(args)
+    # ---- point particles on the refined mesh of config 4 ----
+    refined = None
+    if not args.no_refined:
+        refined = measure_refined(args)
     if rank == 0:
         cb = None if args.no_cpu else cpu_baseline()
         line = {
@@ -450,6 +459,7 @@ def run_ours(args, rep):
             "pc2_stratified": strat,
             "ensemble": ens,
             "clouds": clouds,
+            "refined": refined,
         }
         if res.get("tuned"):
             line["config"]["tuned"] = res["tuned"]
@@ -648,6 +658,61 @@ def measure_clouds(args):
     return out
 
 
+def measure_refined(args):
+    """The SMR/AMR configuration's mesh with point particles (athenak_b200/workloads.py
+    clump_refined): a 128^3 root with two more levels around a Gaussian clump, 1520 MeshBlocks
+    of 16^3, per-block particle counts over 100 times apart, the FP64 imex2+ cycle on the
+    refined mesh (dustb_refined_imex_cycle: the general deposit remap, the multilevel copy
+    exchange, particles routed across levels, local solver, consistent split), eager cycles
+    after one warm-up cycle, and the total momentum change (per-block cell volumes)."""
+    import numpy as np
+    import torch
+    from athenak_b200.workloads import clump_refined
+    dev, ms, info = clump_refined(small=args.small)
+    npart, dt = info["npart"], info["dt"]
+    vol = torch.from_numpy(ms.mb_size[:, 6] * ms.mb_size[:, 7] * ms.mb_size[:, 8]).to(dev.device)
+    g_ = ms.ng
+    n1, n2, n3 = ms.n
+
+    def momentum():
+        u0 = dev.t["u0"][:, 1:4, g_:n3 - g_, g_:n2 - g_, g_:n1 - g_].sum(dim=(2, 3, 4))
+        gas = (u0 * vol[:, None]).sum(0)
+        pr = dev.t["pr"][:, :npart]
+        m = pr[16]
+        dust = torch.stack([(m * pr[r]).sum() for r in (1, 3, 5)])
+        absm = float(torch.stack([(m * pr[r]).abs().sum() for r in (1, 3, 5)]).max())
+        return (gas + dust).cpu().numpy(), absm
+
+    p0, absm = momentum()
+    steps = max(1, min(args.steps, 3))
+    dev.refined_imex_cycle(dt)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        dev.refined_imex_cycle(dt)
+    b.record()
+    torch.cuda.synchronize()
+    ms_cyc = a.elapsed_time(b) / steps
+    p1, _ = momentum()
+    out = {"workload": "128^3 root mesh of 16^3 MeshBlocks with two more levels around a Gaussian "
+                       "dust clump (peak eps 100, sigma 0.05 L): point particles, 2 species "
+                       "tau_s 0.1, 1, 1 + floor(150 exp(-r^2/2 sigma^2)) per species per cell, "
+                       "imex2+ / local solver, consistent split, TSC, FP64 (refinable clouds on "
+                       "refined meshes are not built)",
+           "meshblocks": info["nmb"], "blocks_per_level": info["levels"],
+           "block_particles_max_over_min": info["block_particles_max_over_min"],
+           "particles": npart, "cells": info["ncell"], "dt": dt, "steps": steps,
+           "value": npart / (ms_cyc * 1e-3), "unit": UNIT, "ms_per_step": ms_cyc,
+           "timed": "CUDA events around eager dustb_refined_imex_cycle calls after one warm-up",
+           "deposit_remap_entries": info["plan_entries"],
+           "momentum_change_rel": float(np.abs(p1 - p0).max() / absm),
+           "error_word": dev.error_word()}
+    del dev
+    torch.cuda.empty_cache()
+    return out
+
+
 E2E_ROWS_IN = [0, 1, 2, 3, 4, 5, 15, 16]     # X, V, t_s, m
 E2E_ROWS_OUT = [0, 1, 2, 3, 4, 5]            # X, V
 
@@ -806,6 +871,10 @@ def main():
     ap.add_argument("--cells", type=int, default=0,
                     help="a cubic mesh of this many cells per side (profiling cases)")
     ap.add_argument("--mixed-only", action="store_true", help="time the mixed form only")
+    ap.add_argument("--no-refined", action="store_true",
+                    help="skip the refined-mesh (SMR/AMR) point-particle workload")
+    ap.add_argument("--refined-only", action="store_true",
+                    help="run the refined-mesh workload alone and print its object")
     ap.add_argument("--no-ledger-timing", dest="ledger_timing", action="store_false",
                     help="skip the timing of the cycle without the momentum ledgers")
     ap.add_argument("--no-pc2", action="store_true",
