@@ -104,6 +104,10 @@ class DeviceDust:
             "x3_removed": torch.zeros(2, **f64),
             "scalar": torch.zeros(2, **f64),
         }
+        if getattr(mesh, "nghbr56", None) is not None:
+            # a refined mesh: block levels and the 56 neighbour slots
+            self.t["mb_lev"] = torch.from_numpy(np.ascontiguousarray(mesh.lloc[:, 0])).to(self.device)
+            self.t["nghbr_ml"] = torch.from_numpy(np.ascontiguousarray(mesh.nghbr56)).to(self.device)
         self.phys = dict(phys)
         self._rebuild_ctx()
         return self
