@@ -85,6 +85,77 @@ __host__ __device__ inline int nbr_slot(int ix, int iy, int iz, int n1, int n2) 
   return 48 + (ix + 1) / 2 + (iy + 1) + 2 * (iz + 1);
 }
 
+
+// SetNewPrtclGID's neighbour slot on a refined mesh (src/bvals/bvals_part.cpp:312-394): the slot
+// of the crossing direction (ix, iy, iz); a finer neighbour's sub-slot from the half (fx, fy,
+// fz) of the block the particle leaves from; the first filled sub-slot of the direction; an
+// empty edge or corner is covered by a coarser block stored under the lower-dimensional
+// direction that keeps the components leaving this block's parent.  nb: the block's 56 slot
+// gids, lev: block levels (by gid - gids), mb: the block's RegionSize, x?min: the mesh's
+// lower corner.  -1 if no slot holds a block.
+__device__ inline int ml_route_slot(const int *nb, const int *lev, int gids, int mylevel,
+                                    const double *mb, double x1min, double x2min, double x3min,
+                                    int ix, int iy, int iz, int fx, int fy, int fz) {
+  auto lev_of = [&](int slot) {
+    const int g = nb[slot] - gids;
+    return (nb[slot] >= 0 && g >= 0) ? lev[g] : -1;
+  };
+  auto filled = [&](int jx, int jy, int jz, int k) {
+    const int nd = abs(jx) + abs(jy) + abs(jz);
+    const int end = nbr_slot(jx, jy, jz, 0, 0) + ((nd == 1) ? 4 : ((nd == 2) ? 2 : 1));
+    for (; k < end; ++k)
+      if (nb[k] >= 0) return k;
+    return -1;
+  };
+  auto coarse_cover = [&](int jx, int jy, int jz) {
+    const double lx = mb[X1MAX] - mb[X1MIN], ly = mb[X2MAX] - mb[X2MIN], lz = mb[X3MAX] - mb[X3MIN];
+    const int l1 = (int)floor((mb[X1MIN] - x1min) / lx + 0.5);
+    const int l2 = (int)floor((mb[X2MIN] - x2min) / ly + 0.5);
+    const int l3 = (int)floor((mb[X3MIN] - x3min) / lz + 0.5);
+    const int kx = (jx == 0 || ((l1 & 1) == ((jx > 0) ? 1 : 0))) ? jx : 0;
+    const int ky = (jy == 0 || ((l2 & 1) == ((jy > 0) ? 1 : 0))) ? jy : 0;
+    const int kz = (jz == 0 || ((l3 & 1) == ((jz > 0) ? 1 : 0))) ? jz : 0;
+    if (abs(kx) + abs(ky) + abs(kz) == 0 || (kx == jx && ky == jy && kz == jz)) return -1;
+    return filled(kx, ky, kz, nbr_slot(kx, ky, kz, 0, 0));
+  };
+  int s;
+  if (iz == 0) {
+    if (iy == 0) {                                          // x1 face
+      s = nbr_slot(ix, 0, 0, 0, 0);
+      if (lev_of(s) > mylevel) s = nbr_slot(ix, 0, 0, fy, fz);
+      s = filled(ix, 0, 0, s);
+    } else if (ix == 0) {                                   // x2 face
+      s = nbr_slot(0, iy, 0, 0, 0);
+      if (lev_of(s) > mylevel) s = nbr_slot(0, iy, 0, fx, fz);
+      s = filled(0, iy, 0, s);
+    } else {                                                // x1x2 edge
+      s = nbr_slot(ix, iy, 0, 0, 0);
+      if (lev_of(s) > mylevel) s = nbr_slot(ix, iy, 0, fz, 0);
+      s = filled(ix, iy, 0, s);
+      if (s < 0) s = coarse_cover(ix, iy, 0);
+    }
+  } else if (iy == 0) {
+    if (ix == 0) {                                          // x3 face
+      s = nbr_slot(0, 0, iz, 0, 0);
+      if (lev_of(s) > mylevel) s = nbr_slot(0, 0, iz, fx, fy);
+      s = filled(0, 0, iz, s);
+    } else {                                                // x3x1 edge
+      s = nbr_slot(ix, 0, iz, 0, 0);
+      if (lev_of(s) > mylevel) s = nbr_slot(ix, 0, iz, fy, 0);
+      s = filled(ix, 0, iz, s);
+      if (s < 0) s = coarse_cover(ix, 0, iz);
+    }
+  } else if (ix == 0) {                                     // x2x3 edge
+    s = nbr_slot(0, iy, iz, 0, 0);
+    if (lev_of(s) > mylevel) s = nbr_slot(0, iy, iz, fx, 0);
+    s = filled(0, iy, iz, s);
+    if (s < 0) s = coarse_cover(0, iy, iz);
+  } else {                                                  // corner
+    s = filled(ix, iy, iz, nbr_slot(ix, iy, iz, 0, 0));
+    if (s < 0) s = coarse_cover(ix, iy, iz);
+  }
+  return s;
+}
 }  // namespace dustb
 
 // host-side error bookkeeping shared by the translation units

@@ -96,6 +96,7 @@ struct MState {
 // counters of the queued tile launches of a stage (Q/P, up to two operator sweeps, kick;
 // the pc2 predictor and advance), cleared when the stage's queue is built
 constexpr int kQueues = 8;
+constexpr int kMaxLevels = 8;                    // refined meshes: levels above the root
 enum { Q_QP = 0, Q_OP = 1, Q_KICK = 4, Q_PRED = 5, Q_ADV = 6 };
 
 // cells of the gather window of a 3-D mesh: every block's active cells and one layer around
@@ -126,6 +127,20 @@ struct Geo {
   double shR;                  // fmod(q Omega Lx t, Ly) in cells of y
   int ncell;                   // active cells; key ncell = the edge bin (pc2 half step)
   int W1, W2, W3;              // 3-D: the gather window's cells per row, rows, planes of a block
+  // refined meshes (ml = 1): every block's level (lev, by block, root_level first), the cell
+  // size and volume per level above the root, the 56 neighbour slots, the root blocks per
+  // direction; ml = 0 on a single-level mesh (one level: dx, vol)
+  int ml, root;
+  const int *lev, *nml;
+  double dxl[kMaxLevels][3], voll[kMaxLevels];
+  int nmbroot[3];
+  __device__ int lv(int m) const {
+    if (!ml) return 0;
+    const int l = lev[m] - root;
+    return l < 0 ? 0 : (l >= kMaxLevels ? kMaxLevels - 1 : l);
+  }
+  __device__ double dxm(int m, int a) const { return ml ? dxl[lv(m)][a] : dx[a]; }
+  __device__ double volm(int m) const { return ml ? voll[lv(m)] : vol; }
   __device__ long long at(int m, int nvar, int v, int k, int j, int i) const {
     return (((long long)m * nvar + v) * vstride) + ((long long)k * n2 + j) * n1 + i;
   }
@@ -212,6 +227,18 @@ Geo make_geo(const dustb_ctx *c, const dustb_mixed_params *mp) {
   }
   G.ncell = (int)ncell_of(ms);
   G.W1 = G.nx1 + 2; G.W2 = G.nx2 + 2; G.W3 = G.nx3 + 2;
+  G.ml = (ms.nghbr_ml && ms.mb_lev) ? 1 : 0;
+  G.root = mp->root_level;
+  G.lev = ms.mb_lev; G.nml = ms.nghbr_ml;
+  for (int l = 0; l < kMaxLevels; ++l) {
+    const double s = 1.0 / (double)(1 << l);
+    for (int a = 0; a < 3; ++a) G.dxl[l][a] = mp->dx[a] * s;
+    G.voll[l] = G.dxl[l][0] * G.dxl[l][1] * (ms.three_d ? G.dxl[l][2] : 1.0);
+  }
+  const double ext[3] = {ms.x1max - ms.x1min, ms.x2max - ms.x2min, ms.x3max - ms.x3min};
+  const int nxs[3] = {d.nx1, d.nx2, d.nx3};
+  for (int a = 0; a < 3; ++a) G.nmbroot[a] = (int)floor(ext[a] / (nxs[a] * mp->dx[a]) + 0.5);
+  if (G.ml) G.ghost = 1;      // (the tiles on each block's own ghost cells, exchanged around them)
   return G;
 }
 
@@ -358,7 +385,7 @@ __global__ void k_import(const double *pr, const int *pi, long long stride, int 
     if (!(fo >= 0.0f)) fo = 0.0f;
     if (fo >= 1.0f) fo = 0.99999994f;
     ic[a] = ig; of[a] = fo;
-    dd[a] = (float)((x1[a] - x[a]) * G.inv_dx[a]);
+    dd[a] = (float)((x1[a] - x[a]) / G.dxm(m, a));
   }
   const int key = encode(G, m, ic[2], ic[1], ic[0]);
   B.cell[p] = key; B.pid[p] = p;
@@ -415,15 +442,16 @@ __global__ void k_export(double *pr, int *pi, long long stride, int n, PBuf A, G
   }
   auto W = [&](int r, double v) { pr[(long long)r * stride + p] = v; };
   const double *sz = G.mb + (long long)m * 9;
-  const double x = sz[X1MIN] + ((double)i + (double)A.f[F_OX][q]) * G.dx[0];
-  const double y = sz[X2MIN] + ((double)j + (double)A.f[F_OY][q]) * G.dx[1];
+  const double dxm[3] = {G.dxm(m, 0), G.dxm(m, 1), G.dxm(m, 2)};
+  const double x = sz[X1MIN] + ((double)i + (double)A.f[F_OX][q]) * dxm[0];
+  const double y = sz[X2MIN] + ((double)j + (double)A.f[F_OY][q]) * dxm[1];
   W(DUSTB_IPX, x); W(DUSTB_IPY, y);
-  W(DUSTB_IPX1, x + (double)A.f[F_AX][q] * G.dx[0]);
-  W(DUSTB_IPY1, y + (double)A.f[F_AY][q] * G.dx[1]);
+  W(DUSTB_IPX1, x + (double)A.f[F_AX][q] * dxm[0]);
+  W(DUSTB_IPY1, y + (double)A.f[F_AY][q] * dxm[1]);
   if (G.three_d) {
-    const double z = sz[X3MIN] + ((double)k + (double)A.f[F_OZ][q]) * G.dx[2];
+    const double z = sz[X3MIN] + ((double)k + (double)A.f[F_OZ][q]) * dxm[2];
     W(DUSTB_IPZ, z);
-    W(DUSTB_IPZ1, z + (double)A.f[F_AZ][q] * G.dx[2]);
+    W(DUSTB_IPZ1, z + (double)A.f[F_AZ][q] * dxm[2]);
   }
   W(DUSTB_IPVX, vel[0]); W(DUSTB_IPVY, vel[1]); W(DUSTB_IPVZ, vel[2]);
   W(DUSTB_IPVX1, A.f[F_WX][q]); W(DUSTB_IPVY1, A.f[F_WY][q]); W(DUSTB_IPVZ1, A.f[F_WZ][q]);
@@ -454,7 +482,8 @@ struct PushArgs {
   int kind;
   float gam0, gam1, atw_dt;
   float bdt;                  // beta*dt (velocity kick)
-  float bdx[3];               // beta*dt/dx per axis (drift in cells); pc2 half step: h/dx
+  float bdx[kMaxLevels][3];   // beta*dt/dx per level and axis (drift in cells; one level on a
+                              // single-level mesh); pc2 half step: h/dx
   float gy;                   // pc2 half step: q Omega h / dy (the gather position's y shift
                               // per unit x of the half-step position)
   float sdy;                  // pc2 half step: q Omega dt / dy (the new y's shear drift)
@@ -618,6 +647,58 @@ __device__ __forceinline__ Carry cross_face(const Geo &G, const PushArgs &P, int
   return C;
 }
 
+// A particle leaving block m of a refined (periodic) mesh at block-local cell (ni, nj, nk) with
+// offsets o and register displacement d1 (cells of m's level): the block that holds it (the
+// slot search of SetNewPrtclGID, ml_route_slot, with the halves the new position lies in) and
+// its cell, offset and displacement in that block's cells.  The position is carried as cells
+// of the mesh at m's level (the block's logical location times its cells plus the local
+// coordinate), scaled by 2 or 1/2 to the neighbour's level (exact in FP64), wrapped across
+// the periodic faces and taken relative to the neighbour's origin; the displacement scales the
+// same way.  Count and move take the same steps, so they agree bit for bit.
+__device__ __noinline__ int ml_carry(const Geo &G, const PushArgs &P, int &m, int &k, int &j,
+                                     int &i, int ni, int nj, int nk, float o[3], float d1[3]) {
+  const int nxs[3] = {G.nx1, G.nx2, G.nx3};
+  const int nn[3] = {ni, nj, nk};
+  int oc[3], f[3];
+  for (int a = 0; a < 3; ++a) {
+    oc[a] = (nn[a] < 0) ? -1 : ((nn[a] >= nxs[a]) ? 1 : 0);
+    f[a] = (oc[a] != 0) ? (oc[a] > 0 ? 1 : 0) : (nn[a] >= nxs[a] / 2 ? 1 : 0);
+  }
+  const double *mbm = G.mb + (long long)m * 9;
+  const int s = ml_route_slot(G.nml + (long long)m * 56, G.lev, G.gids, G.lev[m], mbm, G.mx1min,
+                              G.mx2min, G.mx3min, oc[0], oc[1], oc[2], f[0], f[1], f[2]);
+  const int t = (s < 0) ? -1 : G.nml[(long long)m * 56 + s] - G.gids;
+  if (t < 0 || t >= G.nmb) {
+    report(P.err, DUSTB_ERR_NGHBR);
+    i = min(max(ni, 0), G.nx1 - 1); j = min(max(nj, 0), G.nx2 - 1); k = min(max(nk, 0), G.nx3 - 1);
+    for (int a = 0; a < 3; ++a) o[a] = min(max(o[a], 0.0f), 0.99999994f);
+    return encode(G, m, k, j, i);
+  }
+  const int rel = G.lev[t] - G.lev[m];
+  const double sc = (rel > 0) ? 2.0 : ((rel < 0) ? 0.5 : 1.0);
+  const double *mbt = G.mb + (long long)t * 9;
+  const double mlo[3] = {G.mx1min, G.mx2min, G.mx3min};
+  int c[3];
+  for (int a = 0; a < 3; ++a) {
+    const double lm = mbm[3 + a] - mbm[a], lt = mbt[3 + a] - mbt[a];
+    const double lxm = floor((mbm[a] - mlo[a]) / lm + 0.5), lxt = floor((mbt[a] - mlo[a]) / lt + 0.5);
+    // the mesh's extent in cells of the neighbour's level
+    const double nt = (double)G.nmbroot[a] * nxs[a] * (double)(1 << (G.lev[t] - G.root));
+    double x = (lxm * nxs[a] + (double)nn[a] + (double)o[a]) * sc;
+    if (x < 0.0) x += nt; else if (x >= nt) x -= nt;
+    const double loc = x - lxt * nxs[a];
+    int ci = (int)floor(loc);
+    float fo = (float)(loc - (double)ci);
+    if (fo >= 1.0f) { fo = 0.0f; ++ci; }
+    if (ci < 0 || ci >= nxs[a]) { report(P.err, DUSTB_ERR_ROUTE); ci = min(max(ci, 0), nxs[a] - 1); }
+    c[a] = ci;
+    o[a] = fo;
+    d1[a] = (float)((double)d1[a] * sc);
+  }
+  m = t; i = c[0]; j = c[1]; k = c[2];
+  return encode(G, m, k, j, i);
+}
+
 template <int KIND, int SP>
 __device__ __forceinline__ int advance_carry(const Geo &G, const PushArgs &P, int &m, int &k,
                                              int &j, int &i, float o[3], float d1[3],
@@ -635,7 +716,7 @@ __device__ __forceinline__ int advance_carry(const Geo &G, const PushArgs &P, in
   float on[3] = {o[0], o[1], o[2]}, dn[3] = {d1[0], d1[1], d1[2]};
   int c[3] = {0, 0, 0};
   for (int a = 0; a < nax; ++a) {
-    float s = __fmaf_rn(P.bdx[a], xdot[a], __fmul_rn(P.gam1, d1[a]));
+    float s = __fmaf_rn(P.bdx[G.lv(m)][a], xdot[a], __fmul_rn(P.gam1, d1[a]));
     // (the gather position's y: + q Omega x_h h, x_h the half-step x in this block's frame)
     if (KIND == PK_HALF && a == 1 && P.gy != 0.0f) s = __fmaf_rn(P.gy, hpos[0], s);
     on[a] = __fadd_rn(on[a], s);
@@ -658,6 +739,10 @@ __device__ __forceinline__ int advance_carry(const Geo &G, const PushArgs &P, in
     i = ni; j = nj; k = nk;
     for (int a = 0; a < 3; ++a) { o[a] = on[a]; d1[a] = dn[a]; }
     return encode(G, m, k, j, i);
+  }
+  if (!SP && G.ml) {
+    for (int a = 0; a < 3; ++a) { o[a] = on[a]; d1[a] = dn[a]; }
+    return ml_carry(G, P, m, k, j, i, ni, nj, nk, o, d1);
   }
   if (!SP) {
     // a periodic mesh: the neighbour across the face (periodic images are neighbours)
@@ -871,7 +956,7 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   if ((threadIdx.x & 31) == 0 && live) {
     int m, k, j, i;
     decode(G, S.cell[p], m, k, j, i);
-    const double vinv = 1.0 / G.vol;
+    const double vinv = 1.0 / G.volm(m);
     for (int a = 0; a < 3; ++a) {
       if (w[a] == 0.0) continue;
       const long long at = G.at(m, P.nvg, 1 + a, G.ks + k, G.js + j, G.is + i);
@@ -1150,7 +1235,7 @@ __device__ __forceinline__ void add_window(const float4 *s_acc, const Geo &G, co
   constexpr int WK = D3 ? 3 : 1;
   const int nx1 = G.nx1, nct = tj * nx1;
   const int WI = nx1 + 2, WJ = tj + 2, nplane = WJ * WI;
-  const double vinv = 1.0 / G.vol;                 // (every deposited value is per unit volume)
+  const double vinv = 1.0 / G.volm(m);             // (every deposited value is per unit volume)
   for (int t = threadIdx.x; t < WK * nplane; t += blockDim.x) {
     const int c = t / nplane, rem = t - c * nplane;
     const int wy = rem / WI, wx = rem - wy * WI;
@@ -1202,7 +1287,7 @@ __device__ __forceinline__ void add_window_cells(const float4 *s_acc, const Geo 
                                                  int cj, int ci, double *gs) {
   constexpr bool V4 = FourValues<MODE>::value;
   const int nx1 = G.nx1, nct = tj * nx1;
-  const double vinv = 1.0 / G.vol;                 // (every deposited value is per unit volume)
+  const double vinv = 1.0 / G.volm(m);             // (every deposited value is per unit volume)
   auto put = [&](const float4 &v, int kt, int jt, int it) {
     long long at;
     if ((unsigned)kt < (unsigned)G.nx3 && (unsigned)jt < (unsigned)G.nx2 &&
@@ -1651,7 +1736,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       // way (the next stage's history term adds it to the gas as it adds the gas rate)
       cta_sync(wmask);
       if (lane == 0) {
-        const double share = 1.0 / (G.vol * (double)nwarp);
+        const double share = 1.0 / (G.volm(m) * (double)nwarp);
         const int cj = tid / nx1, ci = tid - cj * nx1;
         const long long at = G.at(m, 3, 0, G.ks + k, G.js + j0 + cj, G.is + ci);
 #pragma unroll
@@ -1667,7 +1752,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       // centre mass m c / V of the cell (dust_imex_point_center_mass): only this cell's
       // particles have it as their centre, so it is stored, not added
       const int cj = tid / nx1, ci = tid - cj * nx1;
-      T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj, G.is + ci)] = s_qt[tid] / G.vol;
+      T.res[G.at(m, 4, 3, G.ks + k, G.js + j0 + cj, G.is + ci)] = s_qt[tid] / G.volm(m);
     }
     // (every thread is done with this tile's shared memory before the next tile's copies)
     cta_sync(wmask);
@@ -2057,7 +2142,12 @@ bool rows_attached(const dustb_ctx *c) {
 
 bool params_ok(const dustb_ctx *c, const dustb_mixed_params *mp) {
   if (!dustb_cells::ctx_valid(c) || !mp) return false;
-  if (c->mesh.nghbr_ml) return false;                // (single-level meshes only)
+  if (c->mesh.nghbr_ml) {
+    // a refined mesh: periodic, 3-D, with its deposit remap and copy-exchange scratch
+    const dustb_mesh &ms = c->mesh;
+    if (!ms.mb_lev || !ms.three_d || ms.x3bc != DUSTB_X3_PERIODIC || ms.shear_x1) return false;
+    if (!mp->plan || !mp->coarse || mp->root_level < 0) return false;
+  }
   for (int a = 0; a < 3; ++a)
     if (!(mp->dx[a] > 0.0)) return false;
   if (ncell_of(c->mesh) >= (1LL << 31) - 2) return false;   // (cells and the edge bin)
@@ -2074,10 +2164,15 @@ bool geo_ok(const dustb_mixed_params *mp, const Geo &G) {
 
 // ghost mode: the FP64 exchanges around the tiles (additive: x3 fold or drop and the shear
 // remap included; copy: the shear remap and the x3 boundary values of u*)
-int ghost_add_if(const dustb_ctx *c, const Geo &G, double *f, int nvar, cudaStream_t st) {
+// (a refined mesh: the general deposit remap and the multilevel copy exchange)
+int ghost_add_if(const dustb_ctx *c, const Geo &G, double *f, int nvar, cudaStream_t st,
+                 const dustb_mixed_params *mp) {
+  if (G.ml) return dustb_ghost_add_plan(c, mp->plan, f, nvar, st);
   return G.ghost ? dustb_ghost_add(c, f, nvar, st) : DUSTB_OK;
 }
-int ghost_copy_if(const dustb_ctx *c, const Geo &G, double *f, cudaStream_t st) {
+int ghost_copy_if(const dustb_ctx *c, const Geo &G, double *f, cudaStream_t st,
+                  const dustb_mixed_params *mp) {
+  if (G.ml) return dustb_ghost_copy_ml(c, f, 3, mp->coarse, mp->coarse_bytes, st);
   return G.ghost ? dustb_ghost_copy(c, f, 3, 1, st) : DUSTB_OK;
 }
 
@@ -2104,7 +2199,8 @@ int push_sort(const MState &S, const PBuf &src, const PBuf &dst, const Geo &G, i
     cudaMemsetAsync(S.cstart, 0, 4 * (size_t)nbins(ncell), st);
     if (n > 0) {
 #define DUSTB_COUNT(K, SPF) k_count<K, SPF><<<nblk(n), kT, 0, st>>>(src, S.key, S.cstart, G, n, P)
-      if (G.ghost) {
+      // (physical x3 or shear faces; a refined mesh carries its crossings in the periodic form)
+      if (G.ghost && !G.ml) {
         if (P.kind == PK_HALF) DUSTB_COUNT(PK_HALF, 1);
         else if (P.kind == PK_FULL) DUSTB_COUNT(PK_FULL, 1);
         else DUSTB_COUNT(PK_IMEX, 1);
@@ -2125,7 +2221,7 @@ int push_sort(const MState &S, const PBuf &src, const PBuf &dst, const Geo &G, i
   Scope sc(DUSTB_K_MOVE, st);
   if (n > 0) {
 #define DUSTB_MOVE(K, SPF) k_move<K, SPF><<<nblk(n), kT, 0, st>>>(src, dst, S.key, S.cursor, G, n, P)
-    if (G.ghost) {
+    if (G.ghost && !G.ml) {
       if (P.kind == PK_HALF) DUSTB_MOVE(PK_HALF, 1);
       else if (P.kind == PK_FULL) DUSTB_MOVE(PK_FULL, 1);
       else DUSTB_MOVE(PK_IMEX, 1);
@@ -2334,7 +2430,10 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     P.gam0 = (float)gam0[stage - 1]; P.gam1 = (float)gam1[stage - 1];
     P.atw_dt = (stage == 2) ? (float)(atw22 * dt) : 0.0f;
     P.bdt = (float)(beta[stage - 1] * dt);
-    for (int a = 0; a < 3; ++a) P.bdx[a] = (float)(beta[stage - 1] * dt * G.inv_dx[a]);
+    for (int l = 0; l < kMaxLevels; ++l)
+      for (int a = 0; a < 3; ++a) P.bdx[l][a] = (float)(beta[stage - 1] * dt / G.dxl[l][a]);
+    if (!G.ml)
+      for (int a = 0; a < 3; ++a) P.bdx[0][a] = (float)(beta[stage - 1] * dt * G.inv_dx[a]);
     P.gy = 0.0f;
     P.shy = (float)(co->sh[stage - 1] * G.inv_dx[1]);
     P.a_dt = a_dt; P.stage2 = (stage == 2);
@@ -2369,7 +2468,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
         if (shift) RUN(launch_shift_edge<MODE_QP>(S, cur, G, T, st));
       }
       Scope sc(DUSTB_K_CELLS, st);
-      RUN(ghost_add_if(c, G, c->f.qdep, 5, st));
+      RUN(ghost_add_if(c, G, c->f.qdep, 5, st, mp));
     }
     // periodic meshes: the deposits go straight into the owners' active cells and the
     // gathers read ghost cells from their owners, so no ghost exchange is needed
@@ -2381,7 +2480,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       const int nsw = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
       for (int w = 0; w < nsw; ++w) {
         { Scope sc(DUSTB_K_CELLS, st);
-          RUN(ghost_copy_if(c, G, c->f.ustar, st)); }
+          RUN(ghost_copy_if(c, G, c->f.ustar, st, mp)); }
         cudaMemsetAsync(c->f.work, 0, fbytes * 3, st);
         RUN(gather_window(S, G, c->mesh, c->f.ustar, T, st));
         { Scope sc(DUSTB_K_OPERATOR, st);
@@ -2389,13 +2488,13 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
           RUN(launch_tile<MODE_OP>(S, cur, G, cf, T, st, Q_OP + w));
           if (shift) RUN(launch_shift_edge<MODE_OP>(S, cur, G, T, st)); }
         { Scope sc(DUSTB_K_CELLS, st);
-          RUN(ghost_add_if(c, G, c->f.work, 3, st));
+          RUN(ghost_add_if(c, G, c->f.work, 3, st, mp));
           dustb_cells::dc_correct(c, st); }
       }
     }
     {
       Scope sc(DUSTB_K_CELLS, st);
-      RUN(ghost_copy_if(c, G, c->f.ustar, st));
+      RUN(ghost_copy_if(c, G, c->f.ustar, st, mp));
     }
     if (br) cudaMemsetAsync(c->f.dmom, 0, fbytes * 3, st);
     // stage 1: the kick tiles record the rate's rounding in work for stage 2's history term
@@ -2412,7 +2511,7 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     }
     if (br) {
       Scope sc(DUSTB_K_CELLS, st);
-      RUN(ghost_add_if(c, G, c->f.dmom, 3, st));
+      RUN(ghost_add_if(c, G, c->f.dmom, 3, st, mp));
       if (cons) dustb_cells::consistent_gas(c, a_dt, st);
       else dustb_cells::pmbr(c, a_dt, st);
       // stage 2's consistent dust kick is left pending (recorded by stage 2's count): the
@@ -2423,7 +2522,8 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     // the gas tail's ghost exchange of the conserved state, once per cycle (nothing in the
     // drag step reads u0's ghost cells between the stages)
     Scope sc(DUSTB_K_CELLS, st);
-    RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, st));
+    if (G.ml) RUN(dustb_ghost_copy_ml(c, c->f.u0, c->f.nvar_gas, mp->coarse, mp->coarse_bytes, st));
+    else RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, st));
   }
   return DUSTB_OK;
 }
@@ -2432,6 +2532,7 @@ int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void
                           long long bytes, double dt, double *chi_max, void *stream) {
   if (!params_ok(c, mp) || !(dt > 0.0)) return DUSTB_EINVAL;
   if (!c->mesh.multi_d) return DUSTB_EUNSUP;                        // 1-D: FP64 form
+  if (c->mesh.nghbr_ml) return DUSTB_EUNSUP;                        // (refined: imex only)
   const Geo G = make_geo(c, mp);
   if (!geo_ok(mp, G)) return DUSTB_EINVAL;
   MState S;
@@ -2473,7 +2574,7 @@ int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void
       RUN(launch_tile<MODE_PRED>(S, S.A, G, cf, T, st, Q_PRED));
     }
     Scope sc(DUSTB_K_CELLS, st);
-    RUN(ghost_add_if(c, G, c->f.qdep, 5, st));
+    RUN(ghost_add_if(c, G, c->f.qdep, 5, st, mp));
     RUN(dustb_pc2_apply_predictor(c, dt, chi_max, st));
   }
   {
@@ -2487,7 +2588,7 @@ int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void
   PushArgs P{};
   P.kind = PK_HALF;
   P.gam0 = 1.0f; P.gam1 = 0.0f; P.atw_dt = 0.0f; P.bdt = 0.0f;
-  for (int a = 0; a < 3; ++a) P.bdx[a] = T.pc.hdx[a];
+  for (int a = 0; a < 3; ++a) P.bdx[0][a] = T.pc.hdx[a];
   P.gy = T.pc.gy;
   P.sdy = (float)(c->phys.qshear * c->phys.omega0 * dt * G.inv_dx[1]);
   P.a_dt = h; P.stage2 = 0;
@@ -2514,12 +2615,12 @@ int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void
   // the move to the new position: B -> A sorted by cell (routing as SetNewPrtclGID)
   P.kind = PK_FULL;
   P.gam0 = 0.0f; P.gam1 = 1.0f;
-  for (int a = 0; a < 3; ++a) P.bdx[a] = 0.0f;
+  for (int a = 0; a < 3; ++a) P.bdx[0][a] = 0.0f;
   P.gy = 0.0f;
   RUN(push_sort(S, S.B, S.A, G, n, ncell, P, st));
   if (br) {
     Scope sc(DUSTB_K_CELLS, st);
-    RUN(ghost_add_if(c, G, c->f.dmom, 3, st));
+    RUN(ghost_add_if(c, G, c->f.dmom, 3, st, mp));
     RUN(dustb_pc2_commit(c, 0.5, st));
   }
   {

@@ -20,7 +20,8 @@ KERNELS = ["count", "fill", "deposit_qp", "operator", "kick", "consistent", "cel
 
 class DustbMixedParams(C.Structure):
     _fields_ = [("dx", C.c_double * 3), ("rows_per_tile", C.c_int), ("chunk", C.c_int),
-                ("variant", C.c_int), ("x3_removed", C.c_void_p)]
+                ("variant", C.c_int), ("x3_removed", C.c_void_p), ("root_level", C.c_int),
+                ("plan", C.c_void_p), ("coarse", C.c_void_p), ("coarse_bytes", C.c_longlong)]
 
 
 _declared = False
@@ -69,6 +70,25 @@ class MixedDust:
         self.mp.chunk = chunk
         self.mp.variant = variant
         self.mp.x3_removed = self.dev.t["x3_removed"].data_ptr()
+        if getattr(ms, "nghbr56", None) is not None:
+            # a refined mesh: the root level's cell size, the deposit remap set on the device
+            # arrays (DeviceDust.set_dep_plan) and the copy exchange's scratch for the gas state
+            root = int(ms.root_level)
+            lev0 = int(ms.lloc[0, 0])
+            for a in range(3):
+                self.mp.dx[a] = float(ms.mb_size[0, 6 + a]) * float(2 ** (lev0 - root))
+            self.mp.root_level = root
+            if getattr(self.dev, "plan", None) is None:
+                raise RuntimeError("a refined mesh needs DeviceDust.set_dep_plan first")
+            self.mp.plan = C.addressof(self.dev.plan)
+            nvg = int(self.dev.t["u0"].shape[1])
+            nb = int(self.lib.dustb_ghost_copy_ml_bytes(C.byref(self.dev.ctx.mesh), nvg))
+            ca = self.dev.t.get("coarse")
+            if ca is None or ca.numel() * 8 < nb:
+                ca = self.dev.t["coarse"] = torch.empty(nb // 8, dtype=torch.float64,
+                                                        device=self.dev.device)
+            self.mp.coarse = ca.data_ptr()
+            self.mp.coarse_bytes = nb
         nbytes = int(self.lib.dustb_mixed_workspace_bytes(C.byref(self.dev.ctx.mesh), self.dev.npart))
         self.ws = torch.empty(nbytes, dtype=torch.uint8, device=self.dev.device)
         if do_import:

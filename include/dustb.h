@@ -514,6 +514,15 @@ typedef struct dustb_mixed_params {
   double *x3_removed;      /* device (mass, count) of the particles removed at outflow x3
                               faces, accumulated; required when mesh.x3bc is
                               DUSTB_X3_OUTFLOW, else may be NULL */
+  /* refined meshes (ctx->mesh.nghbr_ml set; periodic, imex2+ cycles): dx above is then the
+   * root level's cell size, root_level the root level's number (the levels of mb_lev count
+   * from it, at most 7 above it); plan the mesh's general deposit remap (dustb_ghost_add_plan)
+   * and coarse / coarse_bytes the scratch of dustb_ghost_copy_ml for ctx->f.nvar_gas
+   * variables.  All zero on a single-level mesh. */
+  int root_level;
+  const dustb_dep_plan *plan;
+  double *coarse;
+  long long coarse_bytes;
 } dustb_mixed_params;
 
 long long dustb_mixed_workspace_bytes(const dustb_mesh *mesh, int npart);
