@@ -349,7 +349,62 @@ def _host_lib():
     f.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong]
     f.restype = C.c_int
+    f = lib.dustb_host_leaf_tables
+    f.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_void_p] * 9
+    f.restype = C.c_int
     return lib
+
+
+def leaf_geometry(ms: MeshSpec) -> np.ndarray:
+    """The geometry vector of dustb_host_leaf_tables: nx1..3, nmb_root1..3, root_level,
+    max_level, x3per."""
+    return np.array([*ms.nx, *ms.nmbroot, ms.root_level, ms.max_level, int(ms.x3bc == 0)],
+                    np.int32)
+
+
+class LeafTables:
+    """The leaf traversal's block geometry of a refined 3-D mesh (dustb_leaf_tables): host
+    arrays, the finest grid's levels and extent, the root cell size."""
+
+    KEYS = ("fbox", "blev", "nnb", "nb", "nbs", "nbmax", "safe", "lockey", "locblk")
+
+    def __init__(self, arrays: dict, nlev: int, nfine, root_dx, nunsafe: int = 0):
+        self.arrays = arrays
+        self.nlev = int(nlev)
+        self.nfine = tuple(int(v) for v in nfine)
+        self.root_dx = tuple(float(v) for v in root_dx)
+        self.nunsafe = int(nunsafe)
+
+
+def empty_leaf_arrays(nmb: int) -> dict:
+    mx = 64
+    return dict(fbox=np.zeros((nmb, 6), np.int32), blev=np.zeros(nmb, np.int32),
+                nnb=np.zeros(nmb, np.int32), nb=np.full((nmb, mx), -1, np.int32),
+                nbs=np.zeros((nmb, mx, 3), np.int32), nbmax=np.zeros(nmb, np.int32),
+                safe=np.zeros((nmb, 3), np.int32), lockey=np.zeros(nmb, np.int64),
+                locblk=np.zeros(nmb, np.int32))
+
+
+def root_cell_size(ms: MeshSpec):
+    return tuple((ms.hi[a] - ms.lo[a]) / (ms.nmbroot[a] * ms.nx[a]) for a in range(3))
+
+
+def leaf_tables(ms: MeshSpec, builder=None) -> LeafTables:
+    """The tables of a refined 3-D mesh from the C++ host layer (dustb_host_leaf_tables), or
+    from builder (a function of the same signature: the oracle's own build in the tests)."""
+    if builder is None:
+        lib = _host_lib()
+        builder = lib.dustb_host_leaf_tables
+    geo = leaf_geometry(ms)
+    lloc = np.ascontiguousarray(ms.lloc, np.int32)
+    ng56 = np.ascontiguousarray(ms.nghbr56, np.int32)
+    arr = empty_leaf_arrays(ms.nmb)
+    info = np.zeros(5, np.int32)
+    rc = builder(geo.ctypes.data, ms.nmb, lloc.ctypes.data, ng56.ctypes.data, info.ctypes.data,
+                 *(arr[k].ctypes.data for k in LeafTables.KEYS))
+    if rc != 0:
+        raise RuntimeError(f"leaf tables: the build failed ({rc})")
+    return LeafTables(arr, info[0], info[1:4], root_cell_size(ms), info[4])
 
 
 class DepPlan:

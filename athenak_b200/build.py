@@ -65,9 +65,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 
 HOST_SRCS = [os.path.join(HERE, "host", f) for f in ("dust_gas_drag.cpp", "pbin.cpp",
-                                                      "restart.cpp", "dep_plan.cpp")]
+                                                      "restart.cpp", "dep_plan.cpp",
+                                                      "leaf_tables.cpp")]
 HOST_HDRS = [os.path.join(HERE, "host", f) for f in ("dust_gas_drag.hpp", "pbin.hpp",
-                                                      "restart.hpp", "dep_plan.hpp")]
+                                                      "restart.hpp", "dep_plan.hpp",
+                                                      "leaf_tables.hpp")]
 HOST_LIB = os.path.join(HERE, "libdustb_host.so")
 
 

@@ -9,6 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdustb.so")
 
 DUSTB_NGP, DUSTB_CIC, DUSTB_TSC = 0, 1, 2
+DUSTB_ESCRATCH = -3
 SOLVER_LOCAL, SOLVER_APPLYA, SOLVER_DC1, SOLVER_DC2 = 0, 1, 2, 3
 X3_PERIODIC, X3_REFLECT, X3_OUTFLOW = 0, 1, 2
 ERR_HALO, ERR_ROUTE, ERR_NGHBR, ERR_PGID, ERR_TSTOP, ERR_WINDOW = 1, 2, 4, 8, 16, 32
@@ -24,7 +25,49 @@ class DustbMesh(C.Structure):
                 ("mb_size", C.c_void_p), ("nghbr", C.c_void_p),
                 ("shear_x1", C.c_int), ("sb_nb2", C.c_int), ("sb_nb3", C.c_int),
                 ("sb_gid", C.c_void_p), ("time", C.c_double),
-                ("mb_lev", C.c_void_p), ("nghbr_ml", C.c_void_p)]
+                ("mb_lev", C.c_void_p), ("nghbr_ml", C.c_void_p), ("leaf", C.c_void_p)]
+
+
+LEAF_MAXNB = 64
+
+
+class DustbLeafTables(C.Structure):
+    _fields_ = [("nlev", C.c_int), ("nfine", C.c_int * 3), ("root_dx", C.c_double * 3),
+                ("fbox", C.c_void_p), ("blev", C.c_void_p), ("nnb", C.c_void_p),
+                ("nb", C.c_void_p), ("nbs", C.c_void_p), ("nbmax", C.c_void_p),
+                ("safe", C.c_void_p), ("lockey", C.c_void_p), ("locblk", C.c_void_p),
+                ("coarse", C.c_void_p), ("coarse_bytes", C.c_longlong)]
+
+
+class DustbCloudSplit(C.Structure):
+    _fields_ = [("max_level", C.c_int), ("split_everywhere", C.c_int),
+                ("split_overlap", C.c_int), ("split_buffer", C.c_int), ("slack", C.c_double)]
+
+
+def split_params(max_level, everywhere=False, overlap=True, buffer=0,
+                 slack=0.02) -> DustbCloudSplit:
+    """The split's controls (<dust>/cloud_split_*; slack: cloud_split_slack, 0.02)."""
+    sp = DustbCloudSplit()
+    sp.max_level, sp.split_everywhere = int(max_level), int(everywhere)
+    sp.split_overlap, sp.split_buffer, sp.slack = int(overlap), int(buffer), float(slack)
+    return sp
+
+
+def leaf_tables_struct(tabs: dict, nlev: int, nfine, root_dx) -> DustbLeafTables:
+    """A DustbLeafTables over the arrays of tabs (numpy for the oracle, torch CUDA tensors for
+    the library; the keys of athenak_b200.amr.leaf_tables)."""
+    t = DustbLeafTables()
+    t.nlev = int(nlev)
+    for a in range(3):
+        t.nfine[a] = int(nfine[a])
+        t.root_dx[a] = float(root_dx[a])
+    for k in ("fbox", "blev", "nnb", "nb", "nbs", "nbmax", "safe", "lockey", "locblk"):
+        setattr(t, k, ptr(tabs[k]))
+    if tabs.get("coarse") is not None:
+        t.coarse = ptr(tabs["coarse"])
+        t.coarse_bytes = int(tabs["coarse"].numel() * 8) if hasattr(tabs["coarse"], "numel") \
+            else int(tabs["coarse"].nbytes)
+    return t
 
 
 class DustbParticles(C.Structure):
@@ -193,6 +236,11 @@ SIGNATURES = {
     "dustb_cloud_dc1_sweep": [CTXP, D, D, VP, VP],
     "dustb_cloud_apply_pmbr": [CTXP, D, D, VP],
     "dustb_cloud_imex_cycle": [CTXP, C.POINTER(DustbImexCoeffs), VP, VP, VP],
+    "dustb_cloud_refined_imex_cycle": [CTXP, C.POINTER(DustbImexCoeffs), VP, VP, LL, VP, VP],
+    "dustb_cloud_instant_switch": [CTXP, I, C.POINTER(C.c_int), VP, VP],
+    "dustb_cloud_split_scratch_bytes": [I],
+    "dustb_cloud_split_p1": [CTXP, C.POINTER(DustbCloudSplit), C.c_ulonglong,
+                             C.POINTER(C.c_int), VP, LL, VP],
     "dustb_cloud_pc2_predictor": [CTXP, D, I, VP, VP],
     "dustb_cloud_pc2_advance": [CTXP, D, VP, VP],
     "dustb_cloud_pc2_cycle": [CTXP, D, VP, VP, VP, VP],
@@ -203,6 +251,7 @@ SIGNATURES = {
 }
 RESTYPES = {"dustb_sort_scratch_bytes": LL, "dustb_ghost_copy_ml_bytes": LL, "dustb_phst_scratch_bytes": LL,
             "dustb_pbin_scratch_bytes": LL, "dustb_cloud_gpack_bytes": LL,
+            "dustb_cloud_split_scratch_bytes": LL,
             "dustb_last_error": C.c_char_p}
 # declared by athenak_b200.mixed (they take its DustbMixedParams struct)
 EXTRA_SIGNATURES = {"dustb_mixed_workspace_bytes", "dustb_mixed_import", "dustb_mixed_export",

@@ -8,6 +8,7 @@
 #include <cstring>
 
 #include "dustb_common.cuh"
+#include "dustb_sort.cuh"
 
 using namespace dustb;
 
@@ -30,12 +31,22 @@ struct PCtx {            // particle view passed by value into kernels
   __device__ int &i(int c, int p) const { return pi[(long long)c * stride + p]; }
 };
 
+// the refinable clouds' leaf traversal on a refined mesh (dustb_leaf_tables); on = 0: none
+struct LTab {
+  int on, nlev, nmb, x3per;
+  int nf[3];
+  double rdx[3], irdx[3], fdx[3];
+  const int *fbox, *blev, *nnb, *nb, *nbs, *nbmax, *safe, *locblk;
+  const long long *lockey;
+};
+
 struct MCtx {            // mesh view
   const double *mb;
   const int *nghbr;
   int gids, scheme, three_d, multi_d;
   double x1min, x1max, x2min, x2max, x3min, x3max;
   const int *blev, *nml;   // refined meshes: block levels and the 56 neighbour slots (or NULL)
+  LTab lt;
   __device__ double s(int m, int f) const { return mb[(long long)m * 9 + f]; }
 };
 
@@ -44,9 +55,22 @@ PCtx pview(const dustb_ctx *c) {
 }
 MCtx mview(const dustb_ctx *c) {
   const dustb_mesh &ms = c->mesh;
-  return MCtx{ms.mb_size, ms.nghbr, ms.gids, c->phys.scheme, ms.three_d, ms.multi_d,
-              ms.x1min, ms.x1max, ms.x2min, ms.x2max, ms.x3min, ms.x3max, ms.mb_lev,
-              ms.nghbr_ml};
+  MCtx M{ms.mb_size, ms.nghbr, ms.gids, c->phys.scheme, ms.three_d, ms.multi_d,
+         ms.x1min, ms.x1max, ms.x2min, ms.x2max, ms.x3min, ms.x3max, ms.mb_lev,
+         ms.nghbr_ml, LTab{}};
+  if (const dustb_leaf_tables *t = ms.leaf) {
+    LTab &L = M.lt;
+    L.on = 1; L.nlev = t->nlev; L.nmb = ms.nmb; L.x3per = ms.x3bc == DUSTB_X3_PERIODIC;
+    for (int a = 0; a < 3; ++a) {
+      L.nf[a] = t->nfine[a];
+      L.rdx[a] = t->root_dx[a];
+      L.irdx[a] = 1.0 / t->root_dx[a];
+      L.fdx[a] = t->root_dx[a] / (double)(1 << t->nlev);
+    }
+    L.fbox = t->fbox; L.blev = t->blev; L.nnb = t->nnb; L.nb = t->nb; L.nbs = t->nbs;
+    L.nbmax = t->nbmax; L.safe = t->safe; L.locblk = t->locblk; L.lockey = t->lockey;
+  }
+  return M;
 }
 
 __device__ __forceinline__ void weights3(const MCtx &M, const Ind &d, int m, double x,
@@ -1398,6 +1422,10 @@ __device__ __forceinline__ double hat_moment(double s) {
   return (s <= 0.0) ? 0.5 * (s * s) + (s * s) * s / 3.0 : 0.5 * (s * s) - (s * s) * s / 3.0;
 }
 
+// cloud code bits (CloudGeometry, src/dust/dust.hpp:101-125)
+constexpr int kCodeLevel = 15, kCodeLobe2 = 4, kCodeLobe1 = 6, kCodeLobe3 = 9;
+constexpr int kCodeBits = 15 | (3 << 4) | (3 << 6) | (3 << 9);
+
 struct CloudAxis {
   int n;
   int o[6], i[6];
@@ -1439,7 +1467,7 @@ __device__ void cloud_axis(const MCtx &M, const Ind &d, int m, int a, double x, 
 // without lobe bits, a position inside the block (slack: within that many cells of it)
 __device__ bool cloud_frame_ok(const MCtx &M, const Ind &d, int m, int lev, const double L[3],
                                double x[3], double slack) {
-  if (!block_ok(d, m) || (lev & ~15) != 0) return false;
+  if (!block_ok(d, m) || (lev & ~(M.lt.on ? kCodeBits : kCodeLevel)) != 0) return false;
   const int nx[3] = {d.nx1, d.nx2, d.nx3};
   for (int a = 0; a < (d.three_d ? 3 : 2); ++a) {
     const double cx = M.s(m, X1MIN + a) + 0.5 * nx[a] * M.s(m, DX1 + a);
@@ -1479,11 +1507,582 @@ struct CloudLeaf {
   double w, m1x, m1y, m1z;
 };
 
+// ---- refinable clouds on a refined 3-D mesh: the leaf traversal -------------------------
+// LeafTraversal3D (src/dust/dust_leaf3d.hpp), one rank, no shear: a cloud anchored at block m
+// is integrated over the leaf cells of every block its support meets, each cell's weight the
+// product of the three 1-D integrals of the cloud shape (CloudShape1D with transition lobes,
+// src/dust/dust.hpp:240-298) between the cell's faces.  Candidates: m alone when the support
+// lies inside it; m and its distinct neighbours when the safe ring or the band scan shows they
+// cover the support (NeedGlobal / Covered); otherwise every block and periodic image that
+// meets it.  Leaves in the order part, candidate, runs of 4 cells in x, z, y, x.
+
+
+struct Shape1 {
+  double x, ell, inv, sl, lo, hi;
+  int lobe;
+  bool both, point;
+};
+__device__ __forceinline__ Shape1 make_shape(double x, double ell_in, double inv_in,
+                                             int lobe_in, bool point) {
+  Shape1 s;
+  s.both = (lobe_in == 3);
+  s.ell = s.both ? 2.0 * ell_in : ell_in;
+  s.lobe = s.both ? 0 : lobe_in;
+  s.sl = (s.lobe == 1) ? -s.ell : s.ell;
+  s.lo = (s.lobe == 1) ? x - 2.0 * s.ell : x - s.ell;
+  s.hi = (s.lobe == 2) ? x + 2.0 * s.ell : x + s.ell;
+  s.x = x;
+  s.point = point;
+  s.inv = s.both ? 0.5 * inv_in : inv_in;
+  return s;
+}
+struct Face1 { double c, cl, h, hl; };
+template <bool kM>
+__device__ __forceinline__ Face1 face_at(const Shape1 &s, double z) {
+  Face1 f{0.0, 0.0, 0.0, 0.0};
+  const double sz = (z - s.x) * s.inv;
+  f.c = hat_cdf(sz);
+  if (kM) f.h = hat_moment(sz);
+  if (s.lobe) {
+    const double tz = (z - s.x - s.sl) * s.inv;
+    f.cl = hat_cdf(tz);
+    if (kM) f.hl = hat_moment(tz);
+  }
+  return f;
+}
+template <bool kM>
+__device__ __forceinline__ void cell_1d(const Shape1 &s, const Face1 &a, const Face1 &b,
+                                        double &w, double &g) {
+  w = b.c - a.c;
+  g = 0.0;
+  if (kM) g = (s.both && s.point) ? 0.0 : s.ell * (b.h - a.h);
+  if (s.lobe) {
+    const double wl = b.cl - a.cl;
+    w = (2.0 / 3.0) * w + (1.0 / 3.0) * wl;
+    if (kM) g = s.point ? 0.0 : (2.0 / 3.0) * g + (1.0 / 3.0) * (s.ell * (b.hl - a.hl) + s.sl * wl);
+  }
+}
+
+__device__ __forceinline__ int floor_div(int a, int n) {
+  int q = a / n;
+  if ((a % n != 0) && ((a < 0) != (n < 0))) --q;
+  return q;
+}
+// the periodic images k0..k1 of [c0 - r, c1 + r) that meet [a, b] (LeafTraversal::ImageRange)
+__device__ __forceinline__ void image_range(int c0, int c1, int r, int n, int a, int b, int &k0,
+                                            int &k1) {
+  k0 = floor_div(a - (c1 + r), n) + 1;
+  k1 = floor_div(b - (c0 - r), n);
+}
+
+// ForCandidates (src/dust/dust_leaf3d.hpp:142-180): f(b, sx, sy, sz), block b moved by
+// -(sx, sy, sz) domain lengths; local: m, then its neighbours; global: every block's images
+// that meet the finest-cell box [ia, ib] x [ja, jb] x [ka, kb] widened by r.  f returns false
+// to stop.
+template <typename F>
+__device__ void for_candidates(const LTab &T, int m, bool global, int ia, int ib, int ja,
+                               int jb, int ka, int kb, int r, F &&f) {
+  if (!global) {
+    if (!f(m, 0, 0, 0)) return;
+    const int n = T.nnb[m];
+    for (int k = 0; k < n; ++k) {
+      const int *s = T.nbs + ((long long)m * DUSTB_LEAF_MAXNB + k) * 3;
+      if (!f(T.nb[(long long)m * DUSTB_LEAF_MAXNB + k], s[0], s[1], s[2])) return;
+    }
+    return;
+  }
+  for (int b = 0; b < T.nmb; ++b) {
+    const int *fb = T.fbox + 6 * (long long)b;
+    int kx0, kx1, ky0, ky1, kz0, kz1;
+    image_range(fb[0], fb[1], r, T.nf[0], ia, ib, kx0, kx1);
+    image_range(fb[2], fb[3], r, T.nf[1], ja, jb, ky0, ky1);
+    image_range(fb[4], fb[5], r, T.nf[2], ka, kb, kz0, kz1);
+    if (!T.x3per) {
+      if (kz0 > 0 || kz1 < 0) continue;
+      kz0 = 0; kz1 = 0;
+    }
+    for (int kz = kz0; kz <= kz1; ++kz)
+      for (int ky = ky0; ky <= ky1; ++ky)
+        for (int kx = kx0; kx <= kx1; ++kx)
+          if (!f(b, -kx, -ky, -kz)) return;
+  }
+}
+// the finest-cell box of block b's image (sx, sy, sz) widened by r: [x0, x1) ...
+__device__ __forceinline__ void image_rect(const LTab &T, int b, int sx, int sy, int sz, int r,
+                                           int q[6]) {
+  const int *fb = T.fbox + 6 * (long long)b;
+  q[0] = fb[0] - sx * T.nf[0] - r; q[1] = fb[1] - sx * T.nf[0] + r;
+  q[2] = fb[2] - sy * T.nf[1] - r; q[3] = fb[3] - sy * T.nf[1] + r;
+  q[4] = fb[4] - sz * T.nf[2] - r; q[5] = fb[5] - sz * T.nf[2] + r;
+}
+// Meets (:181-197): a candidate of level >= minlev, widened by r, meets the box
+__device__ bool leaf_meets(const LTab &T, int m, int ia, int ib, int ja, int jb, int ka, int kb,
+                           int minlev, int r, bool global) {
+  bool hit = false;
+  for_candidates(T, m, global, ia, ib, ja, jb, ka, kb, r, [&](int b, int sx, int sy, int sz) {
+    if (T.blev[b] < minlev) return true;
+    int q[6];
+    image_rect(T, b, sx, sy, sz, r, q);
+    if (ib < q[0] || ia >= q[1] || jb < q[2] || ja >= q[3] || kb < q[4] || ka >= q[5]) return true;
+    hit = true;
+    return false;
+  });
+  return hit;
+}
+// Covered (:198-238): the band scan, slab by slab in z; every box taken holds the cell it was
+// taken for
+__device__ bool leaf_covered(const LTab &T, int m, int ia, int ib, int ja, int jb, int ka, int kb,
+                             int minlev, int r, bool global) {
+  int z = ka;
+  while (z <= kb) {
+    int ztop = kb + 1;
+    int y = ja;
+    while (y <= jb) {
+      int x = ia, top = jb + 1;
+      while (x <= ib) {
+        int xe = x, ye = y, ze = z;
+        for_candidates(T, m, global, x, x, y, y, z, z, r, [&](int b, int sx, int sy, int sz) {
+          if (T.blev[b] < minlev) return true;
+          int q[6];
+          image_rect(T, b, sx, sy, sz, r, q);
+          if (x < q[0] || x >= q[1] || y < q[2] || y >= q[3] || z < q[4] || z >= q[5]) return true;
+          if (q[1] > xe || (q[1] == xe && q[3] > ye) || (q[1] == xe && q[3] == ye && q[5] > ze)) {
+            xe = q[1]; ye = q[3]; ze = q[5];
+          }
+          return true;
+        });
+        if (xe == x) return false;
+        top = (ye < top) ? ye : top;
+        ztop = (ze < ztop) ? ze : ztop;
+        x = xe;
+      }
+      y = top;
+    }
+    z = ztop;
+  }
+  return true;
+}
+__device__ __forceinline__ void clip_z(const LTab &T, int &ka, int &kb) {
+  if (T.x3per) return;
+  ka = (ka < 0) ? 0 : ka;
+  kb = (kb > T.nf[2] - 1) ? T.nf[2] - 1 : kb;
+}
+// NeedGlobal (:253-272): the box widened by r is not inside the safe ring of m nor covered by m
+// and its neighbours
+__device__ bool leaf_need_global(const LTab &T, int m, int ia, int ib, int ja, int jb, int ka,
+                                 int kb, int r) {
+  const int a1 = ia - r, b1 = ib + r;
+  int c1 = ka - r, d1 = kb + r;
+  clip_z(T, c1, d1);
+  int q[6];
+  image_rect(T, m, 0, 0, 0, 0, q);
+  const int *sf = T.safe + 3 * (long long)m;
+  if (q[0] - sf[0] <= a1 && q[1] + sf[0] > b1 && q[2] - sf[1] <= ja - r && q[3] + sf[1] > jb + r &&
+      q[4] - sf[2] <= c1 && q[5] + sf[2] > d1)
+    return false;
+  return !leaf_covered(T, m, a1, b1, ja - r, jb + r, c1, d1, 0, 0, false);
+}
+
+// ForEach (:368-513) without shear: f(leaf) for every leaf under the cloud `code` at the framed
+// position x (anchor m); kM: the moment traversal of the gathers (GatherCode: the point rule
+// along lobed directions)
+template <bool kM, typename F>
+__device__ void leaf_foreach(const MCtx &M, const Ind &d, int m, const double x[3], int code,
+                             F &&f) {
+  const LTab &T = M.lt;
+  const double Lz = M.x3max - M.x3min;
+  const int lev = code & kCodeLevel;
+  const int lb1 = (code >> kCodeLobe1) & 3, lb2 = (code >> kCodeLobe2) & 3;
+  const int lb3 = (code >> kCodeLobe3) & 3;
+  const bool point = kM;
+  const double h1 = ldexp(T.rdx[0], -lev), ih1 = ldexp(T.irdx[0], lev);
+  const double h2 = ldexp(T.rdx[1], -lev), ih2 = ldexp(T.irdx[1], lev);
+  const double h3 = ldexp(T.rdx[2], -lev), ih3 = ldexp(T.irdx[2], lev);
+  const Shape1 s1 = make_shape(x[0], h1, ih1, lb1, point);
+  const Shape1 s2 = make_shape(x[1], h2, ih2, lb2, point);
+  Shape1 s3 = make_shape(x[2], h3, ih3, lb3, point);
+  int npz = 1, zside = 0;
+  if (!T.x3per && (s3.lo < M.x3min || s3.hi > M.x3max)) { npz = 2; zside = (s3.hi > M.x3max) ? 1 : 0; }
+  const double Lx = M.x1max - M.x1min, Ly = M.x2max - M.x2min;
+#pragma unroll 1
+  for (int part = 0; part < npz; ++part) {
+    double zp = x[2];
+    if (part == 1) {
+      zp = 2.0 * ((zside == 1) ? M.x3max : M.x3min) - x[2];
+      s3 = make_shape(zp, h3, ih3, (lb3 == 1 || lb3 == 2) ? 3 - lb3 : lb3, point);
+    }
+    const bool zcorr = kM && part == 1;
+    const double ax0 = M.s(m, X1MIN), ay0 = M.s(m, X2MIN), az0 = M.s(m, X3MIN);
+    const bool inside = s1.lo >= ax0 && s1.hi <= ax0 + d.nx1 * M.s(m, DX1) && s2.lo >= ay0 &&
+                        s2.hi <= ay0 + d.nx2 * M.s(m, DX2) && s3.lo >= az0 &&
+                        s3.hi <= az0 + d.nx3 * M.s(m, DX3);
+    // one candidate: its cells under the support
+    auto visit = [&](int b, int sx, int sy, int sz) {
+      const double dx = M.s(b, DX1), dy = M.s(b, DX2), dz = M.s(b, DX3);
+      const double bx0 = M.s(b, X1MIN) - sx * Lx, by0 = M.s(b, X2MIN) - sy * Ly;
+      const double bz0 = M.s(b, X3MIN) - sz * Lz;
+      const double idx = 1.0 / dx, idy = 1.0 / dy, idz = 1.0 / dz;
+      int i0 = (int)floor((s1.lo - bx0) * idx), i1 = (int)ceil((s1.hi - bx0) * idx) - 1;
+      int j0 = (int)floor((s2.lo - by0) * idy), j1 = (int)ceil((s2.hi - by0) * idy) - 1;
+      int k0 = (int)floor((s3.lo - bz0) * idz), k1 = (int)ceil((s3.hi - bz0) * idz) - 1;
+      i0 = (i0 < 0) ? 0 : i0; i1 = (i1 > d.nx1 - 1) ? d.nx1 - 1 : i1;
+      j0 = (j0 < 0) ? 0 : j0; j1 = (j1 > d.nx2 - 1) ? d.nx2 - 1 : j1;
+      k0 = (k0 < 0) ? 0 : k0; k1 = (k1 > d.nx3 - 1) ? d.nx3 - 1 : k1;
+#pragma unroll 1
+      for (int ic = i0; ic <= i1; ic += 4) {
+        const int nr = (i1 - ic + 1 < 4) ? i1 - ic + 1 : 4;
+        double w1[4], g1[4];
+        Face1 f1 = face_at<kM>(s1, bx0 + ic * dx);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          w1[a] = 0.0; g1[a] = 0.0;
+          if (a < nr) {
+            const Face1 fn = face_at<kM>(s1, bx0 + (ic + a + 1) * dx);
+            cell_1d<kM>(s1, f1, fn, w1[a], g1[a]);
+            f1 = fn;
+          }
+        }
+        Face1 f3 = face_at<kM>(s3, bz0 + k0 * dz);
+#pragma unroll 1
+        for (int k = k0; k <= k1; ++k) {
+          const Face1 fn3 = face_at<kM>(s3, bz0 + (k + 1) * dz);
+          double w3, g3;
+          cell_1d<kM>(s3, f3, fn3, w3, g3);
+          f3 = fn3;
+          if (w3 == 0.0 && (!kM || g3 == 0.0)) continue;
+          double czk = 0.0;
+          if (zcorr) {
+            const double zc = bz0 + (k + 0.5) * dz;
+            const double e = x[2] - zc;
+            czk = (zp - zc) - (e - Lz * round(e / Lz));
+          }
+          Face1 f2 = face_at<kM>(s2, by0 + j0 * dy);
+#pragma unroll 1
+          for (int j = j0; j <= j1; ++j) {
+            const Face1 fn2 = face_at<kM>(s2, by0 + (j + 1) * dy);
+            double w2, g2;
+            cell_1d<kM>(s2, f2, fn2, w2, g2);
+            f2 = fn2;
+            if (w2 == 0.0 && (!kM || g2 == 0.0)) continue;
+            const double w23 = w2 * w3;
+#pragma unroll 1
+            for (int a = 0; a < nr; ++a) {
+              CloudLeaf lf;
+              lf.w = w23 * w1[a];
+              lf.m1x = lf.m1y = lf.m1z = 0.0;
+              if (kM) {
+                lf.m1x = w23 * g1[a];
+                lf.m1y = w1[a] * g2 * w3;
+                lf.m1z = w1[a] * w2 * g3;
+                if (zcorr) lf.m1z += czk * lf.w;
+                if (lf.w == 0.0 && lf.m1x == 0.0 && lf.m1y == 0.0 && lf.m1z == 0.0) continue;
+              } else if (lf.w == 0.0) {
+                continue;
+              }
+              lf.b = b; lf.k = d.ks + k; lf.j = d.js + j; lf.i = d.is + ic + a;
+              f(lf);
+            }
+          }
+        }
+      }
+    };
+    if (inside) {
+      visit(m, 0, 0, 0);
+      continue;
+    }
+    // Candidates (:319-366): the support's finest-cell box
+    const int ia = (int)floor((s1.lo - M.x1min) / T.fdx[0]);
+    const int ib = (int)ceil((s1.hi - M.x1min) / T.fdx[0]) - 1;
+    const int ja = (int)floor((s2.lo - M.x2min) / T.fdx[1]);
+    const int jb = (int)ceil((s2.hi - M.x2min) / T.fdx[1]) - 1;
+    int ka = (int)floor((s3.lo - M.x3min) / T.fdx[2]);
+    int kb = (int)ceil((s3.hi - M.x3min) / T.fdx[2]) - 1;
+    clip_z(T, ka, kb);
+    auto meets = [&](int b, int sx, int sy, int sz) {
+      const double bx0 = M.s(b, X1MIN) - sx * Lx, by0 = M.s(b, X2MIN) - sy * Ly;
+      const double bz0 = M.s(b, X3MIN) - sz * Lz;
+      return !(s1.hi <= bx0 || s1.lo >= bx0 + d.nx1 * M.s(b, DX1) || s2.hi <= by0 ||
+               s2.lo >= by0 + d.nx2 * M.s(b, DX2) || s3.hi <= bz0 ||
+               s3.lo >= bz0 + d.nx3 * M.s(b, DX3));
+    };
+    const bool global = leaf_need_global(T, m, ia, ib, ja, jb, ka, kb, 0);
+    for_candidates(T, m, global, ia - 1, ib + 1, ja - 1, jb + 1, ka - 1, kb + 1, 0,
+                   [&](int b, int sx, int sy, int sz) {
+      if (meets(b, sx, sy, sz)) visit(b, sx, sy, sz);
+      return true;
+    });
+  }
+}
+
+// ---- the owner leaf, the instant switch and the P1 split ----------------------------------
+// the periodic image of a point next to block m (LeafTraversal3D::Frame without shear)
+__device__ __forceinline__ void leaf_frame(const MCtx &M, const Ind &d, int m, double x[3]) {
+  const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
+  const int nx[3] = {d.nx1, d.nx2, d.nx3};
+  for (int a = 0; a < 3; ++a) {
+    if (a == 2 && !M.lt.x3per) break;
+    const double c = M.s(m, X1MIN + a) + 0.5 * nx[a] * M.s(m, DX1 + a);
+    x[a] -= L[a] * round((x[a] - c) * (1.0 / L[a]));
+  }
+}
+// Locate (:515-533): the block holding the finest cell (ic, jc, kc), -1 if none
+__device__ int leaf_locate(const LTab &T, const Ind &d, int ic, int jc, int kc) {
+  ic = ((ic % T.nf[0]) + T.nf[0]) % T.nf[0];
+  jc = ((jc % T.nf[1]) + T.nf[1]) % T.nf[1];
+  if (!T.x3per && (kc < 0 || kc >= T.nf[2])) return -1;
+  kc = ((kc % T.nf[2]) + T.nf[2]) % T.nf[2];
+  for (int l = 0; l <= T.nlev; ++l) {
+    const int sh = T.nlev - l;
+    const long long key = ((long long)l << 57) | ((long long)(kc / (d.nx3 << sh)) << 38) |
+                          ((long long)(jc / (d.nx2 << sh)) << 19) | (long long)(ic / (d.nx1 << sh));
+    int lo = 0, hi = T.nmb;
+    while (lo < hi) {
+      const int mid = (lo + hi) / 2;
+      if (T.lockey[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    if (lo < T.nmb && T.lockey[lo] == key) return T.locblk[lo];
+  }
+  return -1;
+}
+// Owner (:534-595) without shear: the block whose leaf holds the point, searched from block m
+// (m and its neighbours, then the location index); -1 if none
+__device__ int leaf_owner(const MCtx &M, const Ind &d, const double px[3], int m) {
+  const LTab &T = M.lt;
+  const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
+  double x[3] = {px[0], px[1], px[2]};
+  leaf_frame(M, d, m, x);
+  if (!T.x3per) {
+    if (x[2] < M.x3min) x[2] = 2.0 * M.x3min - x[2];
+    if (x[2] >= M.x3max) x[2] = fmin(2.0 * M.x3max - x[2], M.x3max - 1.0e-12 * L[2]);
+  }
+  const int ic = (int)floor((x[0] - M.x1min) / T.fdx[0]);
+  const int jc = (int)floor((x[1] - M.x2min) / T.fdx[1]);
+  const int kc = (int)floor((x[2] - M.x3min) / T.fdx[2]);
+  int res = -1;
+  for_candidates(T, m, false, 0, 0, 0, 0, 0, 0, 0, [&](int b, int sx, int sy, int sz) {
+    const double fi = (x[0] - (M.s(b, X1MIN) - sx * L[0])) / M.s(b, DX1);
+    const double fj = (x[1] - (M.s(b, X2MIN) - sy * L[1])) / M.s(b, DX2);
+    const double fk = (x[2] - (M.s(b, X3MIN) - sz * L[2])) / M.s(b, DX3);
+    if (!(fi >= 0.0 && fi < d.nx1 && fj >= 0.0 && fj < d.nx2 && fk >= 0.0 && fk < d.nx3))
+      return true;
+    res = b;
+    return false;
+  });
+  return (res >= 0) ? res : leaf_locate(T, d, ic, jc, kc);
+}
+
+__device__ __forceinline__ int leaf_anchor(const MCtx &M, const Ind &d, int pgid) {
+  const int m = pgid - M.gids;
+  return (m >= 0 && m < d.nmb) ? m : 0;
+}
+
+// CloudInstantSwitch's kernel (InstantSwitchLevels, src/dust/dust_cloud.cpp:1023-1045)
+__global__ void k_cloud_instant_switch(PCtx P, MCtx M, Ind d, int L, int *nchange) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  const int code = P.i(DUSTB_PLEV, p);
+  if ((code & ~kCodeLevel) != 0 || code < L) return;
+  const double x[3] = {P.r(DUSTB_IPX, p), P.r(DUSTB_IPY, p), P.r(DUSTB_IPZ, p)};
+  const int b = leaf_owner(M, d, x, leaf_anchor(M, d, P.i(DUSTB_PGID, p)));
+  if (b < 0) return;
+  const int lev = (M.lt.blev[b] > L) ? M.lt.blev[b] : L;
+  if (lev != code) {
+    P.i(DUSTB_PLEV, p) = lev;
+    atomicAdd(nchange, 1);
+  }
+}
+
+struct SplitCtl {
+  int max_level, everywhere, overlap;
+  int rdil[18];
+  double slack;
+};
+
+// AnyAbove / AllAbove (:596-622): a leaf above lev meets (all) or covers the box
+__device__ bool leaf_above(const LTab &T, const SplitCtl &C, int m, int ia, int ib, int ja,
+                           int jb, int ka, int kb, int lev, bool all) {
+  if (lev + 1 > T.nlev) return false;
+  const int r = C.rdil[lev + 1];
+  const bool g = leaf_need_global(T, m, ia, ib, ja, jb, ka, kb, r);
+  if (!g && m < T.nmb && lev + 1 > T.nbmax[m] && ia <= ib && ja <= jb && ka <= kb) return false;
+  return all ? leaf_covered(T, m, ia, ib, ja, jb, ka, kb, lev + 1, r, g)
+             : leaf_meets(T, m, ia, ib, ja, jb, ka, kb, lev + 1, r, g);
+}
+// InsideFiner (:668-681) with SupportBox (:653-666): the plain level-lev cloud's support, shrunk
+// by the slack, meets (split_overlap) or lies on leaves finer than lev
+__device__ bool leaf_inside_finer(const MCtx &M, const Ind &d, const SplitCtl &C, double px,
+                                  double py, double pz, int lev, int m) {
+  const LTab &T = M.lt;
+  if (lev >= T.nlev || lev >= C.max_level) return false;
+  if (C.everywhere) return true;
+  double x[3] = {px, py, pz};
+  leaf_frame(M, d, m, x);
+  const double f = 1.0 - C.slack;
+  const double r1 = f * T.rdx[0] / (double)(1 << lev), r2 = f * T.rdx[1] / (double)(1 << lev);
+  const double r3 = f * T.rdx[2] / (double)(1 << lev);
+  const int ia = (int)floor((x[0] - r1 - M.x1min) / T.fdx[0]);
+  const int ib = (int)ceil((x[0] + r1 - M.x1min) / T.fdx[0]) - 1;
+  const int ja = (int)floor((x[1] - r2 - M.x2min) / T.fdx[1]);
+  const int jb = (int)ceil((x[1] + r2 - M.x2min) / T.fdx[1]) - 1;
+  int ka = (int)floor((x[2] - r3 - M.x3min) / T.fdx[2]);
+  int kb = (int)ceil((x[2] + r3 - M.x3min) / T.fdx[2]) - 1;
+  clip_z(T, ka, kb);
+  return leaf_above(T, C, m, ia, ib, ja, jb, ka, kb, lev, !C.overlap);
+}
+__device__ __forceinline__ double half_width(const LTab &T, int lev, int a) {
+  return T.rdx[a] / (double)(1 << (lev & kCodeLevel));
+}
+// P1FlagT (src/dust/dust_cloud3d.cpp:188-210): is the cloud split (or a lobe released) now?
+__device__ bool p1_flag(const MCtx &M, const Ind &d, const SplitCtl &C, int m, int code,
+                        const double x[3]) {
+  const int lev = code & kCodeLevel;
+  const int l1 = (code >> kCodeLobe1) & 3, l2 = (code >> kCodeLobe2) & 3;
+  const int l3 = (code >> kCodeLobe3) & 3;
+  if (l1 == 0 && l2 == 0 && l3 == 0) return leaf_inside_finer(M, d, C, x[0], x[1], x[2], lev, m);
+  if (lev > 0 && leaf_inside_finer(M, d, C, x[0], x[1], x[2], lev - 1, m)) {
+    const double h1 = half_width(M.lt, lev - 1, 0), h2 = half_width(M.lt, lev - 1, 1);
+    const double h3 = half_width(M.lt, lev - 1, 2);
+    return ((l1 & 1) && leaf_inside_finer(M, d, C, x[0] - h1, x[1], x[2], lev - 1, m)) ||
+           ((l1 & 2) && leaf_inside_finer(M, d, C, x[0] + h1, x[1], x[2], lev - 1, m)) ||
+           ((l2 & 1) && leaf_inside_finer(M, d, C, x[0], x[1] - h2, x[2], lev - 1, m)) ||
+           ((l2 & 2) && leaf_inside_finer(M, d, C, x[0], x[1] + h2, x[2], lev - 1, m)) ||
+           ((l3 & 1) && leaf_inside_finer(M, d, C, x[0], x[1], x[2] - h3, lev - 1, m)) ||
+           ((l3 & 2) && leaf_inside_finer(M, d, C, x[0], x[1], x[2] + h3, lev - 1, m));
+  }
+  return false;
+}
+// P1SepT (:229-250): bit 2a (2a + 1) when the lower (upper) side along a lies on finer leaves
+__device__ int p1_sep(const MCtx &M, const Ind &d, const SplitCtl &C, int m, int code,
+                      const double x[3]) {
+  const int lev = code & kCodeLevel;
+  const bool plain = (code & ~kCodeLevel) == 0;
+  const int l = plain ? lev : lev - 1;
+  const double h1 = half_width(M.lt, l, 0), h2 = half_width(M.lt, l, 1);
+  const double h3 = half_width(M.lt, l, 2);
+  return (leaf_inside_finer(M, d, C, x[0] - h1, x[1], x[2], l, m) ? 1 : 0) |
+         (leaf_inside_finer(M, d, C, x[0] + h1, x[1], x[2], l, m) ? 2 : 0) |
+         (leaf_inside_finer(M, d, C, x[0], x[1] - h2, x[2], l, m) ? 4 : 0) |
+         (leaf_inside_finer(M, d, C, x[0], x[1] + h2, x[2], l, m) ? 8 : 0) |
+         (leaf_inside_finer(M, d, C, x[0], x[1], x[2] - h3, l, m) ? 16 : 0) |
+         (leaf_inside_finer(M, d, C, x[0], x[1], x[2] + h3, l, m) ? 32 : 0);
+}
+struct Piece { double off, frac; int lobe; };
+// P1Pieces3 (:52-65): the pieces of a cloud along one direction
+__device__ __forceinline__ int p1_pieces(int lobe_old, bool sep_lo, bool sep_hi, Piece out[3]) {
+  int n = 0;
+  const double total = 0.5 + 0.25 * ((lobe_old & 1) ? 1 : 0) + 0.25 * ((lobe_old & 2) ? 1 : 0);
+  const bool lo = (lobe_old & 1) && sep_lo, hi = (lobe_old & 2) && sep_hi;
+  const int lobe_new = lobe_old & ~((lo ? 1 : 0) | (hi ? 2 : 0));
+  const double keep = 0.5 + 0.25 * ((lobe_new & 1) ? 1 : 0) + 0.25 * ((lobe_new & 2) ? 1 : 0);
+  out[n].off = 0.0; out[n].frac = keep / total; out[n].lobe = lobe_new; ++n;
+  if (lo) { out[n].off = -1.0; out[n].frac = 0.25 / total; out[n].lobe = 0; ++n; }
+  if (hi) { out[n].off = 1.0; out[n].frac = 0.25 / total; out[n].lobe = 0; ++n; }
+  return n;
+}
+// P1BuildT<3> (:268-281)
+__device__ __forceinline__ void p1_build(int code, int sep, Piece pc[3][3], int n[3], int &clev) {
+  const int lev = code & kCodeLevel;
+  const int l1 = (code >> kCodeLobe1) & 3, l2 = (code >> kCodeLobe2) & 3;
+  const int l3 = (code >> kCodeLobe3) & 3;
+  const bool plain = (l1 == 0 && l2 == 0 && l3 == 0);
+  n[0] = p1_pieces(plain ? 3 : l1, (sep & 1) != 0, (sep & 2) != 0, pc[0]);
+  n[1] = p1_pieces(plain ? 3 : l2, (sep & 4) != 0, (sep & 8) != 0, pc[1]);
+  n[2] = p1_pieces(plain ? 3 : l3, (sep & 16) != 0, (sep & 32) != 0, pc[2]);
+  clev = plain ? lev + 1 : lev;
+}
+
+// the split's count pass: the pieces of every flagged cloud (np) and its separation flags
+__global__ void k_split_count(PCtx P, MCtx M, Ind d, SplitCtl C, int *np, int *sep) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.npart) return;
+  const int code = P.i(DUSTB_PLEV, p);
+  const double x[3] = {P.r(DUSTB_IPX, p), P.r(DUSTB_IPY, p), P.r(DUSTB_IPZ, p)};
+  const int m = leaf_anchor(M, d, P.i(DUSTB_PGID, p));
+  int n = 0, s = 0;
+  if ((code & ~kCodeBits) == 0 && p1_flag(M, d, C, m, code, x)) {
+    s = p1_sep(M, d, C, m, code, x);
+    Piece pc[3][3]; int nn[3], clev;
+    p1_build(code, s, pc, nn, clev);
+    n = nn[0] * nn[1] * nn[2];
+  }
+  np[p] = (n > 0) ? n - 1 : 0;
+  sep[p] = (n > 0) ? (s | 64) : 0;
+}
+
+// WrapPos (:119-136) without shear: a piece into the domain; 1 if a physical x3 face mirrored it
+__device__ __forceinline__ int leaf_wrap_pos(const MCtx &M, double c[3]) {
+  const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
+  auto wrap = [](double x, double lo, double hi) {
+    const double len = hi - lo;
+    while (x < lo) x += len;
+    while (x >= hi) x -= len;
+    return x;
+  };
+  c[0] = wrap(c[0], M.x1min, M.x1max);
+  c[1] = wrap(c[1], M.x2min, M.x2max);
+  if (M.lt.x3per) { c[2] = wrap(c[2], M.x3min, M.x3max); return 0; }
+  if (c[2] < M.x3min) { c[2] = 2.0 * M.x3min - c[2]; return 1; }
+  if (c[2] >= M.x3max) {
+    c[2] = 2.0 * M.x3max - c[2];
+    if (c[2] >= M.x3max) c[2] = M.x3max - 1.0e-12 * L[2];
+    return 1;
+  }
+  return 0;
+}
+
+// the split's fill (:1185-1243): the pieces, the parent's slot written last; off: the exclusive
+// scan of the appended pieces
+__global__ void k_split_fill(PCtx P, MCtx M, Ind d, const int *sep, const int *off,
+                             unsigned long long tag0, int npart, int x3reflect) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npart || sep[p] == 0) return;
+  const int code = P.i(DUSTB_PLEV, p);
+  const double x[3] = {P.r(DUSTB_IPX, p), P.r(DUSTB_IPY, p), P.r(DUSTB_IPZ, p)};
+  const double mass = P.r(DUSTB_IPM, p);
+  Piece pc[3][3]; int n[3], clev;
+  p1_build(code, sep[p] & 63, pc, n, clev);
+  double e[3];
+  for (int a = 0; a < 3; ++a) e[a] = half_width(M.lt, clev, a);
+  const int n12 = n[0] * n[1];
+  for (int k = n12 * n[2] - 1; k >= 0; --k) {
+    const int ia[3] = {k % n[0], (k / n[0]) % n[1], k / n12};
+    const int s = (k == 0) ? p : npart + off[p] + k - 1;
+    double c[3];
+    for (int a = 0; a < 3; ++a) c[a] = x[a] + pc[a][ia[a]].off * e[a];
+    const int zmir = leaf_wrap_pos(M, c);
+    if (k > 0) {
+      for (int q = 0; q < DUSTB_NREAL; ++q) P.r(q, s) = P.r(q, p);
+      for (int q = 0; q < DUSTB_NINT; ++q) P.i(q, s) = P.i(q, p);
+      const unsigned long long t = tag0 + (unsigned long long)(off[p] + k - 1);
+      P.i(DUSTB_PTAG, s) = (int)(unsigned)(t & 0xffffffffULL);
+      P.i(DUSTB_PTAGH, s) = (int)(unsigned)(t >> 32);
+    }
+    P.r(DUSTB_IPX, s) = c[0]; P.r(DUSTB_IPX1, s) = c[0];
+    P.r(DUSTB_IPY, s) = c[1]; P.r(DUSTB_IPY1, s) = c[1];
+    P.r(DUSTB_IPZ, s) = c[2]; P.r(DUSTB_IPZ1, s) = c[2];
+    const double mp = mass * pc[0][ia[0]].frac * pc[1][ia[1]].frac * pc[2][ia[2]].frac;
+    const int l3 = pc[2][ia[2]].lobe;
+    const int code_s = clev | (pc[0][ia[0]].lobe << kCodeLobe1) | (pc[1][ia[1]].lobe << kCodeLobe2) |
+                       ((zmir ? ((l3 == 1 || l3 == 2) ? 3 - l3 : l3) : l3) << kCodeLobe3);
+    P.r(DUSTB_IPM, s) = mp;
+    P.i(DUSTB_PLEV, s) = code_s;
+    if (zmir && x3reflect) { P.r(DUSTB_IPVZ, s) = -P.r(DUSTB_IPVZ, s); P.r(DUSTB_IPVZ1, s) = -P.r(DUSTB_IPVZ1, s); }
+    const int am = leaf_anchor(M, d, P.i(DUSTB_PGID, s));
+    const int b = leaf_owner(M, d, c, am);
+    P.i(DUSTB_PGID, s) = M.gids + ((b >= 0 && b < d.nmb) ? b : am);
+  }
+}
+
+
 // every leaf of the cloud at x (level lev, anchored at block m): f(leaf); with kMoments the
 // moment traversal (a leaf with zero weight but a moment visited), else the weight traversal
 template <bool kMoments, typename F>
 __device__ void cloud_leaves(const MCtx &M, const Ind &d, int m, const double x[3], int lev,
                              const double L[3], int x3phys, F &&f, unsigned *err) {
+  if (M.lt.on) {
+    leaf_foreach<kMoments>(M, d, m, x, lev, f);
+    return;
+  }
   CloudAxis X, Y, Z;
   cloud_axis(M, d, m, 0, x[0], lev, L[0], X);
   cloud_axis(M, d, m, 1, x[1], lev, L[1], Y);
@@ -2184,9 +2783,24 @@ int dustb_phst(const dustb_ctx *c, const double *chi_max, double *row, void *scr
 // ---- refinable clouds on a uniform 3-D mesh (periodic; plain P1 hat clouds) ---------------
 // (physical x3 faces: the mirrored part of the clouds that reach beyond them; shear-periodic x1
 // faces, whose translated parts need the shear images of the neighbours, are not supported)
+// (a refined mesh needs the leaf tables; with them a uniform 3-D mesh takes the leaf traversal
+// too)
 static int cloud_mesh_ok(const dustb_ctx *c) {
   const dustb_mesh &ms = c->mesh;
+  if (ms.nghbr_ml || ms.leaf) {
+    const dustb_leaf_tables *t = ms.leaf;
+    return ms.three_d && !ms.shear_x1 && t && t->fbox && t->blev && t->nnb && t->nb && t->nbs &&
+           t->nbmax && t->safe && t->lockey && t->locblk && t->nlev >= 0 && t->nlev <= 16 &&
+           t->root_dx[0] > 0.0 && t->root_dx[1] > 0.0 && t->root_dx[2] > 0.0;
+  }
   return ms.multi_d && !ms.shear_x1;
+}
+// the clouds' u* copy exchange: the multilevel one on a refined mesh (leaf->coarse)
+static int cloud_ustar_exchange(const dustb_ctx *c, void *stream) {
+  if (c->mesh.nghbr_ml)
+    return dustb_ghost_copy_ml(c, c->f.ustar, 3, c->mesh.leaf->coarse,
+                               c->mesh.leaf->coarse_bytes, stream);
+  return dustb_ghost_copy(c, c->f.ustar, 3, 1, stream);
 }
 static int cloud_x3phys(const dustb_ctx *c) {
   return c->mesh.three_d && c->mesh.x3bc != DUSTB_X3_PERIODIC;
@@ -2228,7 +2842,7 @@ int dustb_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh, double *gp
   if (!gpack) return DUSTB_EINVAL;
   if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
   const Ind d = make_ind(c->mesh);
-  int rc = dustb_ghost_copy(c, c->f.ustar, 3, 1, stream);
+  int rc = cloud_ustar_exchange(c, stream);
   if (rc) return rc;
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
   cudaMemsetAsync(c->f.work, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
@@ -2286,6 +2900,77 @@ int dustb_cloud_pc2_advance(const dustb_ctx *c, double dt, double *gpack, void *
                                       ph.back_reaction, ph.shearing_box, ph.stratified,
                                       ph.qshear, ph.omega0, ph.const_accel_phi, cloud_x3phys(c), c->err);
   return launch_status("cloud_pc2_advance");
+}
+
+// ---- cloud management on a refined mesh: the instant switch and the P1 split -------------
+int dustb_cloud_instant_switch(const dustb_ctx *c, int level_cap, int *nchange, void *scratch,
+                               void *stream) {
+  CHECK_CTX(c);
+  if (!nchange || !scratch) return DUSTB_EINVAL;
+  if (!cloud_mesh_ok(c) || !c->mesh.leaf) return DUSTB_EUNSUP;
+  *nchange = 0;
+  if (level_cap < 0 || level_cap >= c->mesh.leaf->nlev || c->part.npart == 0) return DUSTB_OK;
+  const Ind d = make_ind(c->mesh);
+  int *cnt = (int *)scratch;
+  cudaMemsetAsync(cnt, 0, sizeof(int), S(stream));
+  k_cloud_instant_switch<<<PGRID(c)>>>(pview(c), mview(c), d, level_cap, cnt);
+  int rc = launch_status("cloud_instant_switch");
+  if (rc) return rc;
+  cudaMemcpyAsync(nchange, cnt, sizeof(int), cudaMemcpyDeviceToHost, S(stream));
+  cudaStreamSynchronize(S(stream));
+  return launch_status("cloud_instant_switch");
+}
+
+long long dustb_cloud_split_scratch_bytes(int npart) {
+  if (npart < 0) return -1;
+  const long long n = (long long)npart + 1;
+  return ((2 * n * 4 + 255) & ~255LL) + ((scan_bsum_ints(n) * 4 + 255) & ~255LL);
+}
+
+int dustb_cloud_split_p1(const dustb_ctx *c, const dustb_cloud_split *sp,
+                         unsigned long long tag0, int *nnew, void *scratch, long long bytes,
+                         void *stream) {
+  CHECK_CTX(c);
+  if (!sp || !nnew || !(sp->slack >= 0.0 && sp->slack < 1.0) || sp->split_buffer < 0)
+    return DUSTB_EINVAL;
+  if (!cloud_mesh_ok(c) || !c->mesh.leaf) return DUSTB_EUNSUP;
+  *nnew = 0;
+  const int np = c->part.npart;
+  if (np == 0) return DUSTB_OK;
+  if (!scratch || bytes < dustb_cloud_split_scratch_bytes(np)) return DUSTB_ESCRATCH;
+  const Ind d = make_ind(c->mesh);
+  SplitCtl C{};
+  C.max_level = sp->max_level;
+  C.everywhere = sp->split_everywhere;
+  C.overlap = sp->split_overlap;
+  C.slack = sp->slack;
+  const int nlev = c->mesh.leaf->nlev;
+  for (int l = 0; l <= 17; ++l)
+    C.rdil[l] = (sp->split_buffer > 0 && l >= 1 && l <= nlev) ? (sp->split_buffer << (nlev - l + 1))
+                                                             : 0;
+  const long long n1 = (long long)np + 1;
+  int *off = (int *)scratch;
+  int *sep = off + n1;
+  int *bsum = (int *)((char *)scratch + ((2 * n1 * 4 + 255) & ~255LL));
+  cudaMemsetAsync(off + np, 0, sizeof(int), S(stream));
+  k_split_count<<<PGRID(c)>>>(pview(c), mview(c), d, C, off, sep);
+  int rc = launch_status("cloud_split_p1");
+  if (rc) return rc;
+  rc = exclusive_scan(off, n1, bsum, S(stream));
+  if (rc) return rc;
+  int total = 0;
+  cudaMemcpyAsync(&total, off + np, sizeof(int), cudaMemcpyDeviceToHost, S(stream));
+  cudaStreamSynchronize(S(stream));
+  rc = launch_status("cloud_split_p1");
+  if (rc) return rc;
+  *nnew = total;
+  if ((long long)np + total > c->part.stride) {
+    dustb_host::set_message("cloud_split_p1: the pieces exceed the particle capacity");
+    return DUSTB_ESCRATCH;
+  }
+  const int x3reflect = c->mesh.three_d && c->mesh.x3bc == DUSTB_X3_REFLECT;
+  k_split_fill<<<PGRID(c)>>>(pview(c), mview(c), d, sep, off, tag0, np, x3reflect);
+  return launch_status("cloud_split_p1");
 }
 
 // the point transfers' remap: the drag's, with the ghost deposits behind physical x3 faces
@@ -2440,11 +3125,15 @@ int dustb_refined_imex_cycle(const dustb_ctx *c, const dustb_dep_plan *plan,
 // one imex2+ cycle of refinable clouds on a uniform mesh: the task order of dustb_imex_cycle
 // with the clouds' deposit (into the owner cells: no deposit exchange), dc1 / dc2 sweeps,
 // gather-kick and PMBR split
-int dustb_cloud_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co, double *gpack,
-                           double *x3_removed, void *stream) {
-  CHECK_CTX(c);
-  if (!co || !(co->dt > 0.0) || !gpack) return DUSTB_EINVAL;
-  if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
+static int cloud_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co, double *gpack,
+                            double *coarse, long long coarse_bytes, double *x3_removed,
+                            void *stream) {
+  // the gas state's copy exchange: the multilevel one on a refined mesh
+  auto gas_exchange = [&]() {
+    return c->mesh.nghbr_ml
+               ? dustb_ghost_copy_ml(c, c->f.u0, c->f.nvar_gas, coarse, coarse_bytes, stream)
+               : dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, stream);
+  };
   const double g = co->gamma, dt = co->dt;
   const double gam0[2] = {1.0, (2.0 * g - 1.0) / (2.0 * g * g)};
   const double gam1[2] = {0.0, 1.0 - (2.0 * g - 1.0) / (2.0 * g * g)};
@@ -2467,12 +3156,30 @@ int dustb_cloud_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co, doub
       int nsw = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
       for (int w = 0; w < nsw; ++w) RUN(dustb_cloud_dc1_sweep(c, a_dt, sh, gpack, stream));
     }
-    RUN(dustb_ghost_copy(c, c->f.ustar, 3, 1, stream));
+    RUN(cloud_ustar_exchange(c, stream));
     RUN(dustb_cloud_gather_kick(c, a_dt, sh, gpack, stream));
     if (br) RUN(dustb_cloud_apply_pmbr(c, a_dt, sh, stream));
-    RUN(dustb_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0, stream));
+    RUN(gas_exchange());
   }
   return DUSTB_OK;
+}
+
+int dustb_cloud_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co, double *gpack,
+                           double *x3_removed, void *stream) {
+  CHECK_CTX(c);
+  if (!co || !(co->dt > 0.0) || !gpack) return DUSTB_EINVAL;
+  if (!cloud_mesh_ok(c) || c->mesh.nghbr_ml) return DUSTB_EUNSUP;
+  return cloud_imex_cycle(c, co, gpack, nullptr, 0, x3_removed, stream);
+}
+
+int dustb_cloud_refined_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co,
+                                   double *gpack, double *coarse, long long coarse_bytes,
+                                   double *x3_removed, void *stream) {
+  CHECK_CTX(c);
+  if (!co || !(co->dt > 0.0) || !gpack || !c->mesh.leaf) return DUSTB_EINVAL;
+  if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
+  if (co->sh[0] != 0.0 || co->sh[1] != 0.0) return DUSTB_EUNSUP;    // (no shearing box)
+  return cloud_imex_cycle(c, co, gpack, coarse, coarse_bytes, x3_removed, stream);
 }
 
 // one pc2 cycle of the clouds: the order of dustb_pc2_cycle with the clouds' predictor and

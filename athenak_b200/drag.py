@@ -139,7 +139,22 @@ class DeviceDust:
     def _rebuild_ctx(self):
         self.ctx = capi.make_ctx(self.mesh, self.t, self.npart, self.stride, self.phys)
         self.ctx.mesh.time = self.__dict__.get("time", 0.0)
+        if self.__dict__.get("leaf") is not None:
+            self.ctx.mesh.leaf = C.addressof(self.leaf)
         self.pctx = C.byref(self.ctx)
+
+    def ensure_capacity(self, n):
+        """Grows the particle rows to hold n particles (a quarter more), live rows kept."""
+        if n <= self.stride:
+            return
+        cap = int(n + n // 4)
+        pr = torch.zeros((17, cap), dtype=torch.float64, device=self.device)
+        pi = torch.zeros((5, cap), dtype=torch.int32, device=self.device)
+        pr[:, :self.npart].copy_(self.t["pr"][:, :self.npart])
+        pi[:, :self.npart].copy_(self.t["pi"][:, :self.npart])
+        self.t["pr"], self.t["pi"] = pr, pi
+        self.stride = cap
+        self._rebuild_ctx()
 
     def detach_rows(self):
         """Frees the reference rows (pr, pi) and passes them as detached (NULL, npart kept):
@@ -337,6 +352,62 @@ class DeviceDust:
         co.sh[0], co.sh[1] = sh
         self._call("cloud_imex_cycle", C.byref(co), self._gpack().data_ptr(),
                    self.t["x3_removed"].data_ptr(), stream=stream)
+
+    # ---- refinable clouds on a refined 3-D mesh ----
+    def set_leaf_tables(self, lt):
+        """The leaf traversal's block geometry (athenak_b200.amr.LeafTables) copied to the
+        device and set in the mesh: the cloud calls then integrate over the actual leaves."""
+        tabs = {k: torch.from_numpy(np.ascontiguousarray(v)).to(self.device)
+                for k, v in lt.arrays.items()}
+        if self.t.get("nghbr_ml") is not None:
+            nb = int(self.lib.dustb_ghost_copy_ml_bytes(C.byref(self.ctx.mesh), 3))
+            tabs["coarse"] = torch.empty(nb // 8, dtype=torch.float64, device=self.device)
+        for k, v in tabs.items():
+            self.t["leaf_" + k] = v
+        self.leaf = capi.leaf_tables_struct(tabs, lt.nlev, lt.nfine, lt.root_dx)
+        self._rebuild_ctx()
+
+    def cloud_refined_imex_cycle(self, dt, gamma=GAMMA_DEFAULT, stream=None):
+        """One imex2+ cycle of the clouds on a refined mesh (dustb_cloud_refined_imex_cycle)."""
+        co = capi.DustbImexCoeffs()
+        co.gamma, co.dt = gamma, dt
+        nb = int(self.lib.dustb_ghost_copy_ml_bytes(C.byref(self.ctx.mesh),
+                                                    int(self.t["u0"].shape[1])))
+        ca = self.t.get("coarse")
+        if ca is None or ca.numel() * 8 < nb:
+            ca = self.t["coarse"] = torch.empty(nb // 8, dtype=torch.float64, device=self.device)
+        self._call("cloud_refined_imex_cycle", C.byref(co), self._gpack().data_ptr(),
+                   ca.data_ptr(), nb, self.t["x3_removed"].data_ptr(), stream=stream)
+
+    def cloud_instant_switch(self, level_cap, stream=None) -> int:
+        """CloudInstantSwitch (dustb_cloud_instant_switch); returns the clouds changed."""
+        n = C.c_int(0)
+        s = self.t.get("switch_scratch")
+        if s is None:
+            s = self.t["switch_scratch"] = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._call("cloud_instant_switch", int(level_cap), C.byref(n), s.data_ptr(),
+                   stream=stream)
+        return int(n.value)
+
+    def cloud_split_p1(self, split, tag0, stream=None) -> int:
+        """The moving P1 split (dustb_cloud_split_p1) with new tags from tag0; the rows grow when
+        the pieces need room.  Returns the pieces appended (npart grows by them)."""
+        nb = int(self.lib.dustb_cloud_split_scratch_bytes(self.npart))
+        s = self.t.get("split_scratch")
+        if s is None or s.numel() < nb:
+            s = self.t["split_scratch"] = torch.empty(nb, dtype=torch.uint8, device=self.device)
+        n = C.c_int(0)
+        rc = self.lib.dustb_cloud_split_p1(self.pctx, C.byref(split), C.c_ulonglong(tag0),
+                                           C.byref(n), s.data_ptr(), s.numel(), _stream_ptr(stream))
+        if rc == capi.DUSTB_ESCRATCH and self.npart + n.value > self.stride:
+            self.ensure_capacity(self.npart + n.value)
+            rc = self.lib.dustb_cloud_split_p1(self.pctx, C.byref(split), C.c_ulonglong(tag0),
+                                               C.byref(n), s.data_ptr(), s.numel(),
+                                               _stream_ptr(stream))
+        capi.check(rc, "cloud_split_p1")
+        self.npart += int(n.value)
+        self._rebuild_ctx()
+        return int(n.value)
 
     def cloud_pc2_cycle(self, dt, stream=None):
         chi = torch.zeros(1, dtype=torch.float64, device=self.device)

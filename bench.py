@@ -675,6 +675,9 @@ def measure_refined(args):
     n1, n2, n3 = ms.n
 
     def momentum():
+        return momentum_n(npart)
+
+    def momentum_n(npart):
         u0 = dev.t["u0"][:, 1:4, g_:n3 - g_, g_:n2 - g_, g_:n1 - g_].sum(dim=(2, 3, 4))
         gas = (u0 * vol[:, None]).sum(0)
         pr = dev.t["pr"][:, :npart]
@@ -685,21 +688,67 @@ def measure_refined(args):
 
     p0, absm = momentum()
     steps = max(1, min(args.steps, 3))
-    dev.refined_imex_cycle(dt)
+    snap = (dev.t["pr"].clone(), dev.t["pi"].clone(), dev.t["u0"].clone())
+
+    def timed(cycle):
+        cycle()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            cycle()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / steps
+
+    ms_cyc = timed(lambda: dev.refined_imex_cycle(dt))
+    p1, _ = momentum()
+    err_fp64 = dev.error_word()
+    v64 = dev.t["pr"][[1, 3, 5], :npart].clone()
+    # the mixed form on the same mesh from the same state (its tiles from the device work queue,
+    # heaviest first: the blocks' particle counts are 125x apart)
+    from athenak_b200.mixed import MixedDust
+    dev.t["pr"].copy_(snap[0]); dev.t["pi"].copy_(snap[1]); dev.t["u0"].copy_(snap[2])
+    mx = MixedDust(dev=dev)
+    mx.export()
+    pm0, _ = momentum()
+    ms_mixed = timed(lambda: mx.imex_cycle(dt))
+    mx.export()
     torch.cuda.synchronize()
+    pm1, _ = momentum()
+    vm = dev.t["pr"][[1, 3, 5], :npart]
+    vscale = float(v64.abs().max())
+    dv = float((vm - v64).abs().max()) / vscale
+    err_mixed = dev.error_word()
+    del mx, v64
+    torch.cuda.empty_cache()
+    # refinable clouds on the same mesh from the same state: every cloud takes the level of its
+    # leaf (the instant switch at level 0), one P1 split pass turns the clouds whose support
+    # meets finer leaves into lobed transition clouds and their separated pieces, then imex2+
+    # cycles of the clouds over the actual leaves (dustb_cloud_refined_imex_cycle)
+    from athenak_b200 import capi
+    from athenak_b200.amr import leaf_tables
+    dev.t["pr"].copy_(snap[0]); dev.t["pi"].copy_(snap[1]); dev.t["u0"].copy_(snap[2])
+    del snap
+    torch.cuda.empty_cache()
+    lt = leaf_tables(ms)
+    dev.set_leaf_tables(lt)
+    nsw = dev.cloud_instant_switch(0)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
-    for _ in range(steps):
-        dev.refined_imex_cycle(dt)
+    nsplit = dev.cloud_split_p1(capi.split_params(max_level=lt.nlev), int(npart))
     b.record()
     torch.cuda.synchronize()
-    ms_cyc = a.elapsed_time(b) / steps
-    p1, _ = momentum()
+    ms_split = a.elapsed_time(b)
+    ncl = dev.npart
+    pc0, absc = momentum_n(ncl)
+    ms_cloud = timed(lambda: dev.cloud_refined_imex_cycle(dt))
+    pc1, _ = momentum_n(ncl)
+    err_cloud = dev.error_word()
     out = {"workload": "128^3 root mesh of 16^3 MeshBlocks with two more levels around a Gaussian "
                        "dust clump (peak eps 100, sigma 0.05 L): point particles, 2 species "
                        "tau_s 0.1, 1, 1 + floor(150 exp(-r^2/2 sigma^2)) per species per cell, "
-                       "imex2+ / local solver, consistent split, TSC, FP64 (refinable clouds on "
-                       "refined meshes are not built)",
+                       "imex2+ / local solver, consistent split, TSC, FP64",
            "meshblocks": info["nmb"], "blocks_per_level": info["levels"],
            "block_particles_max_over_min": info["block_particles_max_over_min"],
            "particles": npart, "cells": info["ncell"], "dt": dt, "steps": steps,
@@ -707,7 +756,19 @@ def measure_refined(args):
            "timed": "CUDA events around eager dustb_refined_imex_cycle calls after one warm-up",
            "deposit_remap_entries": info["plan_entries"],
            "momentum_change_rel": float(np.abs(p1 - p0).max() / absm),
-           "error_word": dev.error_word()}
+           "mixed": {"ms_per_step": ms_mixed, "value": npart / (ms_mixed * 1e-3),
+                     "speedup_vs_fp64": ms_cyc / ms_mixed,
+                     "momentum_change_rel": float(np.abs(pm1 - pm0).max() / absm),
+                     "velocity_max_rel_vs_fp64_after_same_cycles": dv,
+                     "note": "the FP64 form ran 1 + steps cycles, the mixed form the same number "
+                             "from the same state"},
+           "clouds": {"ms_per_step": ms_cloud, "value": ncl / (ms_cloud * 1e-3),
+                      "clouds": ncl, "switched_to_leaf_level": nsw,
+                      "split_pieces_appended": nsplit, "split_pass_ms": ms_split,
+                      "momentum_change_rel": float(np.abs(pc1 - pc0).max() / absc),
+                      "timed": "CUDA events around eager dustb_cloud_refined_imex_cycle calls "
+                               "after one warm-up (FP64 refinable clouds over the actual leaves)"},
+           "error_words": [err_fp64, err_mixed, err_cloud]}
     del dev
     torch.cuda.empty_cache()
     return out

@@ -108,7 +108,37 @@ typedef struct dustb_mesh {
   const int *nghbr_ml;     /* nmb x 56: gid in every NeighborIndex slot of pmb->nghbr (four
                               sub-slots per face, two per edge, one per corner;
                               src/mesh/nghbr_index.hpp:20-60), -1 where the slot is empty */
+  /* refinable clouds on a refined 3-D mesh: the leaf traversal's block geometry (a host struct
+   * of device arrays, below); NULL: the clouds' uniform-mesh traversal */
+  const struct dustb_leaf_tables *leaf;
 } dustb_mesh;
+
+/* The block geometry of the refinable clouds' leaf traversal on a refined 3-D mesh
+ * (DustGasDrag::BuildLeafTraversal3D, src/dust/dust_cloud3d.cpp:357-860, one rank: block slot =
+ * gid - gids), built on the host by dustb_host_leaf_tables (athenak_b200/host/leaf_tables.hpp).
+ * Every pointer is a device array.  A uniform mesh is the case nlev = 0. */
+#define DUSTB_LEAF_MAXNB 64
+typedef struct dustb_leaf_tables {
+  int nlev;                /* max_level - root_level */
+  int nfine[3];            /* the domain in cells of the finest level */
+  double root_dx[3];       /* the root level's cell size (mesh extent / mesh cells): a level-L
+                              cloud's half-width is root_dx / 2^L */
+  const int *fbox;         /* nmb x 6: [x0, x1) x [y0, y1) x [z0, z1) in finest cells */
+  const int *blev;         /* nmb: level above the root */
+  const int *nnb;          /* nmb: distinct neighbours */
+  const int *nb;           /* nmb x 64: their block slots, in NeighborIndex slot order */
+  const int *nbs;          /* nmb x 64 x 3: the shift (in domain lengths) of each: the
+                              neighbour's image next to the block is the block moved by -shift */
+  const int *nbmax;        /* nmb: the finest level among a block and its neighbours */
+  const int *safe;         /* nmb x 3: the ring (finest cells) the neighbours certainly hold */
+  const long long *lockey; /* nmb: logical-location keys (level << 57 | lx3 << 38 | lx2 << 19 |
+                              lx1), ascending */
+  const int *locblk;       /* nmb: the block of each key */
+  /* the scratch of the clouds' multilevel u* copy exchange (dustb_ghost_copy_ml for 3
+   * variables: dustb_ghost_copy_ml_bytes) used by the cloud calls that exchange u* */
+  double *coarse;
+  long long coarse_bytes;
+} dustb_leaf_tables;
 
 typedef struct dustb_particles {
   double *pr;              /* 17 x stride */
@@ -376,6 +406,50 @@ int dustb_cloud_pc2_predictor(const dustb_ctx *ctx, double dt, int rate_dep, dou
 int dustb_cloud_pc2_advance(const dustb_ctx *ctx, double dt, double *gpack, void *stream);
 /* (dustb_cloud_imex_cycle, dustb_cloud_pc2_cycle: with the fused cycles below) */
 
+/* ---- refinable clouds on a refined 3-D mesh (mesh.leaf set) ---------------------------
+ * The calls above then integrate every cloud over the actual leaves (LeafTraversal3D::ForEach,
+ * src/dust/dust_leaf3d.hpp:368-513): the half-width root_dx / 2^L of its level L, the transition
+ * lobes of its code (bits 6-7 x1, 4-5 x2, 9-10 x3: CloudShape1D, src/dust/dust.hpp:240-298), the
+ * cells of its block when the support lies inside it, else of the block and its distinct
+ * neighbours when they cover the support (the safe ring or the band scan, NeedGlobal / Covered),
+ * else of every block whose periodic image meets it; gathers with the point rule along lobed
+ * directions (GatherCode).  Periodic x1 and x2; x3 periodic or physical (the mirrored part);
+ * u* exchanges by dustb_ghost_copy_ml with leaf->coarse.
+ *
+ * The split's controls (<dust>/cloud_split_*, src/dust/dust_cloud.cpp:140-270). */
+typedef struct dustb_cloud_split {
+  int max_level;           /* clouds are never split beyond this level (cloud_max_level: nlev, or
+                              cloud_split_max_level when that is lower) */
+  int split_everywhere;    /* test_cloud_split_everywhere: split regardless of the mesh */
+  int split_overlap;       /* 1 (default): split once the shrunk support meets finer leaves; 0:
+                              once it lies entirely on them */
+  int split_buffer;        /* test_cloud_split_buffer: the finer leaves of level l dilated by
+                              buffer << (nlev - l + 1) finest cells (0: none) */
+  double slack;            /* cloud_split_slack (0.02): the support shrunk by this fraction */
+} dustb_cloud_split;
+/* CloudInstantSwitch (src/dust/dust_cloud.cpp:1023-1085): every plain cloud of level >= L takes
+ * the level max(L, level of the leaf holding its centre); lobed clouds and clouds whose leaf is
+ * not found keep theirs.  *nchange (host) receives the clouds changed (the call synchronizes
+ * the stream).  scratch: 4 bytes. */
+int dustb_cloud_instant_switch(const dustb_ctx *ctx, int level_cap, int *nchange, void *scratch,
+                               void *stream);
+/* Bytes of scratch for dustb_cloud_split_p1 with npart particles. */
+long long dustb_cloud_split_scratch_bytes(int npart);
+/* SplitCloudsP1DeviceT (src/dust/dust_cloud3d.cpp:1005-1310) without the budget, the split
+ * velocity and the block marks: a plain cloud whose (shrunk) support meets (or lies on) finer
+ * leaves, or a lobed cloud whose lobe side became eligible, is split along each direction into
+ * the P1 pieces of its separation flags (centre child with the lobes kept, edge children at
+ * +-half-width with a quarter of the parent's shape each); pieces other than the centre are
+ * appended after the live particles with the parent's rows, tags tag0, tag0 + 1, ... in the
+ * order of the exclusive scan; each piece's position (wrapped; mirrored with its x3 lobe at a
+ * physical x3 face, vz flipped at a reflecting one), mass, code and block (its owner leaf's, or
+ * the parent's when none is found).  *nnew (host) receives the pieces appended (the call
+ * synchronizes); the caller adds them to npart.  DUSTB_ESCRATCH when npart + new pieces exceed
+ * the particle capacity (nothing written; *nnew holds the count). */
+int dustb_cloud_split_p1(const dustb_ctx *ctx, const dustb_cloud_split *split,
+                         unsigned long long tag0, int *nnew, void *scratch, long long bytes,
+                         void *stream);
+
 /* ---- the particle science file (pbin, src/outputs/pbin.cpp): its device side -----------
  * The host writes the file (athenak_b200/host/pbin.hpp); these calls find the active rows
  * and pack their columns. */
@@ -430,6 +504,12 @@ typedef struct dustb_imex_coeffs {
  * and dustb_cloud_apply_pmbr); gpack as dustb_cloud_gpack_bytes. */
 int dustb_cloud_imex_cycle(const dustb_ctx *ctx, const dustb_imex_coeffs *coeffs, double *gpack,
                            double *x3_removed, void *stream);
+/* One imex2+ cycle of refinable clouds on a refined 3-D mesh (mesh.leaf set): the order of
+ * dustb_cloud_imex_cycle with the clouds' leaf deposits, the gas state exchanged by
+ * dustb_ghost_copy_ml (coarse: its scratch for ctx->f.nvar_gas) and u* with leaf->coarse. */
+int dustb_cloud_refined_imex_cycle(const dustb_ctx *ctx, const dustb_imex_coeffs *coeffs,
+                                   double *gpack, double *coarse, long long coarse_bytes,
+                                   double *x3_removed, void *stream);
 /* One pc2 cycle of the clouds (the order of dustb_pc2_cycle with the cloud predictor and
  * advance; chi_max as there). */
 int dustb_cloud_pc2_cycle(const dustb_ctx *ctx, double dt, double *chi_max, double *gpack,

@@ -1082,7 +1082,8 @@ static void cloud_axis(const dustb_ctx *c, int m, int a, double x, int lev, Clou
  * that many cells of it, the pc2 midpoint) */
 static int cloud_frame_ok(const dustb_ctx *c, int m, double x[3], int code, double slack) {
   const dustb_mesh *ms = &c->mesh;
-  if (m < 0 || m >= ms->nmb || (code & ~15) != 0) return 0;
+  const int bits = ms->leaf ? (15 | (3 << 4) | (3 << 6) | (3 << 9)) : 15;
+  if (m < 0 || m >= ms->nmb || (code & ~bits) != 0) return 0;
   const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
   const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
   for (int a = 0; a < (ms->three_d ? 3 : 2); ++a) {
@@ -1118,11 +1119,665 @@ static int cloud_owner(const dustb_ctx *c, int m, int ox, int oy, int oz) {
 typedef struct { int b, k, j, i; double w, m1x, m1y, m1z; } CloudLeaf;
 typedef void (*CloudLeafFn)(void *ctx, const CloudLeaf *lf);
 
+/* ---- refinable clouds on a refined 3-D mesh: the leaf traversal (test restatement) ------
+ * LeafTraversal3D (src/dust/dust_leaf3d.hpp), one rank, no shear.  The cloud shape along one
+ * direction (CloudShape1D, src/dust/dust.hpp:240-298): a hat of half-width ell = root_dx /
+ * 2^level about the particle, or with a transition lobe on one side (2/3) S_ell(x - xp) + (1/3)
+ * S_ell(x - xp -/+ ell), or with both lobes the parent hat of half-width 2 ell; the weight of a
+ * cell is the integral between its faces, its moment about the particle the integral of (x -
+ * xp) (zero along lobed directions for gathers: the point rule of GatherCode).  The cells are
+ * those of every candidate block under the support: the anchor alone when the support lies
+ * inside it (ForEach :409-423), else the anchor and its distinct neighbours when they cover it
+ * (NeedGlobal :253-272: the safe ring, else the band scan Covered :198-238), else every block
+ * and periodic image (ForCandidates :142-180) that meets it; cells in the order part,
+ * candidate, runs of four in x, z, y, x (:426-500).  Leaf tables: oracle_leaf_tables. */
+typedef struct { double x, ell, inv, sl, lo, hi; int lobe, both, point; } Shape1;
+static Shape1 make_shape(double x, double ell_in, double inv_in, int lobe_in, int point) {
+  Shape1 s;
+  s.both = (lobe_in == 3);
+  s.ell = s.both ? 2.0*ell_in : ell_in;
+  s.lobe = s.both ? 0 : lobe_in;
+  s.sl = (s.lobe == 1) ? -s.ell : s.ell;
+  s.lo = (s.lobe == 1) ? x - 2.0*s.ell : x - s.ell;
+  s.hi = (s.lobe == 2) ? x + 2.0*s.ell : x + s.ell;
+  s.x = x;
+  s.point = point;
+  s.inv = s.both ? 0.5*inv_in : inv_in;
+  return s;
+}
+typedef struct { double c, cl, h, hl; } Face1;
+static Face1 face_at(const Shape1 *s, double z, int mom) {
+  Face1 f = {0.0, 0.0, 0.0, 0.0};
+  const double sz = (z - s->x)*s->inv;
+  f.c = hat_cdf(sz);
+  if (mom) f.h = hat_moment(sz);
+  if (s->lobe) {
+    const double tz = (z - s->x - s->sl)*s->inv;
+    f.cl = hat_cdf(tz);
+    if (mom) f.hl = hat_moment(tz);
+  }
+  return f;
+}
+static void cell_1d(const Shape1 *s, const Face1 *a, const Face1 *b, int mom, double *w,
+                    double *g) {
+  *w = b->c - a->c;
+  *g = 0.0;
+  if (mom) *g = (s->both && s->point) ? 0.0 : s->ell*(b->h - a->h);
+  if (s->lobe) {
+    const double wl = b->cl - a->cl;
+    *w = (2.0/3.0)*(*w) + (1.0/3.0)*wl;
+    if (mom) *g = s->point ? 0.0 : (2.0/3.0)*(*g) + (1.0/3.0)*(s->ell*(b->hl - a->hl) + s->sl*wl);
+  }
+}
+
+/* a candidate: block b moved by -(sx, sy, sz) domain lengths */
+typedef struct { int b, s[3]; } Cand;
+typedef struct { Cand *v; int n, cap; } CandList;
+static void cand_push(CandList *L, int b, int sx, int sy, int sz) {
+  if (L->n == L->cap) {
+    L->cap = L->cap ? 2*L->cap : 128;
+    L->v = (Cand *)realloc(L->v, (size_t)L->cap*sizeof(Cand));
+  }
+  Cand c = {b, {sx, sy, sz}};
+  L->v[L->n++] = c;
+}
+static int fdiv(int a, int n) { return (int)floor((double)a/(double)n); }
+/* the candidates of ForCandidates: local (m, then its neighbours) or global (every block's
+ * periodic images meeting the finest-cell box widened by r), appended to L */
+static void candidates(const dustb_ctx *c, int m, int global, const int box[6], int r,
+                       CandList *L) {
+  const dustb_leaf_tables *T = c->mesh.leaf;
+  L->n = 0;
+  if (!global) {
+    cand_push(L, m, 0, 0, 0);
+    for (int k = 0; k < T->nnb[m]; ++k) {
+      const int *s = &T->nbs[((size_t)m*DUSTB_LEAF_MAXNB + k)*3];
+      cand_push(L, T->nb[(size_t)m*DUSTB_LEAF_MAXNB + k], s[0], s[1], s[2]);
+    }
+    return;
+  }
+  const int x3per = c->mesh.x3bc == 0;
+  for (int b = 0; b < c->mesh.nmb; ++b) {
+    int k0[3], k1[3];
+    for (int a = 0; a < 3; ++a) {
+      const int c0 = T->fbox[6*b + 2*a], c1 = T->fbox[6*b + 2*a + 1], n = T->nfine[a];
+      k0[a] = fdiv(box[2*a] - (c1 + r), n) + 1;
+      k1[a] = fdiv(box[2*a + 1] - (c0 - r), n);
+    }
+    if (!x3per) {
+      if (k0[2] > 0 || k1[2] < 0) continue;
+      k0[2] = k1[2] = 0;
+    }
+    for (int kz = k0[2]; kz <= k1[2]; ++kz)
+      for (int ky = k0[1]; ky <= k1[1]; ++ky)
+        for (int kx = k0[0]; kx <= k1[0]; ++kx) cand_push(L, b, -kx, -ky, -kz);
+  }
+}
+static void cand_rect(const dustb_leaf_tables *T, const Cand *q, int r, int out[6]) {
+  for (int a = 0; a < 3; ++a) {
+    out[2*a] = T->fbox[6*q->b + 2*a] - q->s[a]*T->nfine[a] - r;
+    out[2*a + 1] = T->fbox[6*q->b + 2*a + 1] - q->s[a]*T->nfine[a] + r;
+  }
+}
+/* Meets: a candidate of level >= minlev, widened by r, meets the box */
+static int leaf_meets(const dustb_ctx *c, int m, const int box[6], int minlev, int r,
+                      int global) {
+  const dustb_leaf_tables *T = c->mesh.leaf;
+  CandList L = {NULL, 0, 0};
+  candidates(c, m, global, box, r, &L);
+  int hit = 0;
+  for (int k = 0; k < L.n && !hit; ++k) {
+    if (T->blev[L.v[k].b] < minlev) continue;
+    int q[6];
+    cand_rect(T, &L.v[k], r, q);
+    hit = !(box[1] < q[0] || box[0] >= q[1] || box[3] < q[2] || box[2] >= q[3] ||
+            box[5] < q[4] || box[4] >= q[5]);
+  }
+  free(L.v);
+  return hit;
+}
+/* Covered: the band scan; each step takes, among the candidates holding the cell, the box
+ * reaching furthest in x, then y, then z */
+static int leaf_covered(const dustb_ctx *c, int m, const int box[6], int minlev, int r,
+                        int global) {
+  const dustb_leaf_tables *T = c->mesh.leaf;
+  CandList L = {NULL, 0, 0};
+  int ok = 1;
+  int z = box[4];
+  while (ok && z <= box[5]) {
+    int ztop = box[5] + 1, y = box[2];
+    while (ok && y <= box[3]) {
+      int x = box[0], top = box[3] + 1;
+      while (ok && x <= box[1]) {
+        const int cell[6] = {x, x, y, y, z, z};
+        candidates(c, m, global, cell, r, &L);
+        int xe = x, ye = y, ze = z;
+        for (int k = 0; k < L.n; ++k) {
+          if (T->blev[L.v[k].b] < minlev) continue;
+          int q[6];
+          cand_rect(T, &L.v[k], r, q);
+          if (x < q[0] || x >= q[1] || y < q[2] || y >= q[3] || z < q[4] || z >= q[5]) continue;
+          if (q[1] > xe || (q[1] == xe && q[3] > ye) || (q[1] == xe && q[3] == ye && q[5] > ze)) {
+            xe = q[1]; ye = q[3]; ze = q[5];
+          }
+        }
+        if (xe == x) { ok = 0; break; }
+        if (ye < top) top = ye;
+        if (ze < ztop) ztop = ze;
+        x = xe;
+      }
+      y = top;
+    }
+    z = ztop;
+  }
+  free(L.v);
+  return ok;
+}
+static void leaf_clip_z(const dustb_ctx *c, int *ka, int *kb) {
+  if (c->mesh.x3bc == 0) return;
+  const int n = c->mesh.leaf->nfine[2];
+  if (*ka < 0) *ka = 0;
+  if (*kb > n - 1) *kb = n - 1;
+}
+static int leaf_need_global(const dustb_ctx *c, int m, const int box[6], int r) {
+  const dustb_leaf_tables *T = c->mesh.leaf;
+  int w[6] = {box[0] - r, box[1] + r, box[2] - r, box[3] + r, box[4] - r, box[5] + r};
+  leaf_clip_z(c, &w[4], &w[5]);
+  const int *f = &T->fbox[6*m], *sf = &T->safe[3*m];
+  if (f[0] - sf[0] <= w[0] && f[1] + sf[0] > w[1] && f[2] - sf[1] <= w[2] &&
+      f[3] + sf[1] > w[3] && f[4] - sf[2] <= w[4] && f[5] + sf[2] > w[5])
+    return 0;
+  return !leaf_covered(c, m, w, 0, 0, 0);
+}
+
+/* every leaf under the cloud `code` at the framed position x (anchor m) */
+static void leaf_foreach(const dustb_ctx *c, const Ind *d, int m, const double x[3], int code,
+                         int mom, CloudLeafFn f, void *ctx) {
+  const dustb_mesh *ms = &c->mesh;
+  const dustb_leaf_tables *T = ms->leaf;
+  const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
+  const int lev = code & 15, lb1 = (code >> 6) & 3, lb2 = (code >> 4) & 3, lb3 = (code >> 9) & 3;
+  double h[3], ih[3];
+  for (int a = 0; a < 3; ++a) { h[a] = ldexp(T->root_dx[a], -lev); ih[a] = ldexp(1.0/T->root_dx[a], lev); }
+  Shape1 S[3];
+  S[0] = make_shape(x[0], h[0], ih[0], lb1, mom);
+  S[1] = make_shape(x[1], h[1], ih[1], lb2, mom);
+  S[2] = make_shape(x[2], h[2], ih[2], lb3, mom);
+  int npz = 1, zside = 0;
+  if (ms->x3bc != 0 && (S[2].lo < ms->x3min || S[2].hi > ms->x3max)) {
+    npz = 2; zside = S[2].hi > ms->x3max;
+  }
+  double fdx[3];
+  for (int a = 0; a < 3; ++a) fdx[a] = T->root_dx[a]/(double)(1 << T->nlev);
+  const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
+  CandList CL = {NULL, 0, 0};
+  for (int part = 0; part < npz; ++part) {
+    double zp = x[2];
+    if (part == 1) {
+      zp = 2.0*(zside ? ms->x3max : ms->x3min) - x[2];
+      S[2] = make_shape(zp, h[2], ih[2], (lb3 == 1 || lb3 == 2) ? 3 - lb3 : lb3, mom);
+    }
+    int inside = 1;
+    for (int a = 0; a < 3; ++a)
+      inside = inside && S[a].lo >= MB(m, X1MIN + a) && S[a].hi <= MB(m, X1MIN + a) + nx[a]*MB(m, DX1 + a);
+    CL.n = 0;
+    if (inside) {
+      cand_push(&CL, m, 0, 0, 0);
+    } else {
+      const double xmin[3] = {ms->x1min, ms->x2min, ms->x3min};
+      int box[6];
+      for (int a = 0; a < 3; ++a) {
+        box[2*a] = (int)floor((S[a].lo - xmin[a])/fdx[a]);
+        box[2*a + 1] = (int)ceil((S[a].hi - xmin[a])/fdx[a]) - 1;
+      }
+      leaf_clip_z(c, &box[4], &box[5]);
+      const int global = leaf_need_global(c, m, box, 0);
+      const int wide[6] = {box[0] - 1, box[1] + 1, box[2] - 1, box[3] + 1, box[4] - 1, box[5] + 1};
+      CandList all = {NULL, 0, 0};
+      candidates(c, m, global, wide, 0, &all);
+      for (int k = 0; k < all.n; ++k) {
+        const Cand *q = &all.v[k];
+        int meets = 1;
+        for (int a = 0; a < 3; ++a) {
+          const double b0 = MB(q->b, X1MIN + a) - q->s[a]*L[a];
+          meets = meets && !(S[a].hi <= b0 || S[a].lo >= b0 + nx[a]*MB(q->b, DX1 + a));
+        }
+        if (meets) cand_push(&CL, q->b, q->s[0], q->s[1], q->s[2]);
+      }
+      free(all.v);
+    }
+    for (int t = 0; t < CL.n; ++t) {
+      const int b = CL.v[t].b;
+      double o[3], dd[3];
+      int lo[3], hi[3];
+      for (int a = 0; a < 3; ++a) {
+        dd[a] = MB(b, DX1 + a);
+        o[a] = MB(b, X1MIN + a) - CL.v[t].s[a]*L[a];
+        const double id = 1.0/dd[a];
+        lo[a] = (int)floor((S[a].lo - o[a])*id);
+        hi[a] = (int)ceil((S[a].hi - o[a])*id) - 1;
+        if (lo[a] < 0) lo[a] = 0;
+        if (hi[a] > nx[a] - 1) hi[a] = nx[a] - 1;
+      }
+      for (int ic = lo[0]; ic <= hi[0]; ic += 4) {
+        const int nr = (hi[0] - ic + 1 < 4) ? hi[0] - ic + 1 : 4;
+        double w1[4] = {0.0, 0.0, 0.0, 0.0}, g1[4] = {0.0, 0.0, 0.0, 0.0};
+        Face1 f1 = face_at(&S[0], o[0] + ic*dd[0], mom);
+        for (int a = 0; a < nr; ++a) {
+          const Face1 fn = face_at(&S[0], o[0] + (ic + a + 1)*dd[0], mom);
+          cell_1d(&S[0], &f1, &fn, mom, &w1[a], &g1[a]);
+          f1 = fn;
+        }
+        Face1 f3 = face_at(&S[2], o[2] + lo[2]*dd[2], mom);
+        for (int k = lo[2]; k <= hi[2]; ++k) {
+          const Face1 fn3 = face_at(&S[2], o[2] + (k + 1)*dd[2], mom);
+          double w3, g3;
+          cell_1d(&S[2], &f3, &fn3, mom, &w3, &g3);
+          f3 = fn3;
+          if (w3 == 0.0 && (!mom || g3 == 0.0)) continue;
+          double czk = 0.0;
+          if (mom && part == 1) {
+            const double zc = o[2] + (k + 0.5)*dd[2];
+            const double e = x[2] - zc;
+            czk = (zp - zc) - (e - L[2]*round(e/L[2]));
+          }
+          Face1 f2 = face_at(&S[1], o[1] + lo[1]*dd[1], mom);
+          for (int j = lo[1]; j <= hi[1]; ++j) {
+            const Face1 fn2 = face_at(&S[1], o[1] + (j + 1)*dd[1], mom);
+            double w2, g2;
+            cell_1d(&S[1], &f2, &fn2, mom, &w2, &g2);
+            f2 = fn2;
+            if (w2 == 0.0 && (!mom || g2 == 0.0)) continue;
+            const double w23 = w2*w3;
+            for (int a = 0; a < nr; ++a) {
+              CloudLeaf lf;
+              lf.w = w23*w1[a];
+              lf.m1x = lf.m1y = lf.m1z = 0.0;
+              if (mom) {
+                lf.m1x = w23*g1[a];
+                lf.m1y = w1[a]*g2*w3;
+                lf.m1z = w1[a]*w2*g3;
+                if (part == 1) lf.m1z += czk*lf.w;
+                if (lf.w == 0.0 && lf.m1x == 0.0 && lf.m1y == 0.0 && lf.m1z == 0.0) continue;
+              } else if (lf.w == 0.0) {
+                continue;
+              }
+              lf.b = b; lf.k = d->ks + k; lf.j = d->js + j; lf.i = d->is + ic + a;
+              f(ctx, &lf);
+            }
+          }
+        }
+      }
+    }
+  }
+  free(CL.v);
+}
+
+/* the leaf tables (DustGasDrag::BuildLeafTraversal3D, src/dust/dust_cloud3d.cpp:604-793), the
+ * oracle's own build: geo nx1..3, nmb_root1..3, root_level, max_level, x3per; outputs as
+ * dustb_host_leaf_tables.  The periodic shift of a neighbour: lround of the gap between the
+ * facing sides across the slot's direction, of the centre offset along it, in domain lengths. */
+int oracle_leaf_tables(const int *geo, int nmb, const int *lloc, const int *nghbr56, int *info,
+                       int *fbox, int *blev, int *nnb, int *nb, int *nbs, int *nbmax, int *safe,
+                       long long *lockey, int *locblk) {
+  const int nlev = geo[7] - geo[6], x3per = geo[8];
+  int nf[3];
+  for (int a = 0; a < 3; ++a) nf[a] = (geo[3 + a]*geo[a]) << nlev;
+  info[0] = nlev; info[1] = nf[0]; info[2] = nf[1]; info[3] = nf[2]; info[4] = 0;
+  for (int b = 0; b < nmb; ++b) {
+    blev[b] = lloc[4*b] - geo[6];
+    for (int a = 0; a < 3; ++a) {
+      fbox[6*b + 2*a] = (lloc[4*b + 1 + a]*geo[a]) << (nlev - blev[b]);
+      fbox[6*b + 2*a + 1] = fbox[6*b + 2*a] + (geo[a] << (nlev - blev[b]));
+    }
+  }
+  /* the direction of every slot, from the slot index formula of NeighborIndex */
+  int dir[56][3];
+  memset(dir, 0, sizeof(dir));
+  for (int iz = -1; iz <= 1; ++iz)
+    for (int iy = -1; iy <= 1; ++iy)
+      for (int ix = -1; ix <= 1; ++ix) {
+        const int nd = abs(ix) + abs(iy) + abs(iz);
+        if (!nd) continue;
+        for (int n2 = 0; n2 < 2; ++n2)
+          for (int n1 = 0; n1 < 2; ++n1) {
+            if ((nd >= 2 && n2) || (nd == 3 && n1)) continue;
+            int s;
+            if (iz == 0 && ix*iy == 0) s = abs(ix)*2*(ix + 1) + abs(iy)*2*(iy + 5) + n1 + 2*n2;
+            else if (iz == 0) s = 16 + (ix + 1) + 2*(iy + 1) + n1;
+            else if (ix*iy == 0) s = 24 + abs(ix)*(ix + 9) + abs(iy)*(iy + 17) + 2*(iz + 1) + n1 + 2*n2;
+            else s = 48 + (ix + 1)/2 + (iy + 1) + 2*(iz + 1);
+            dir[s][0] = ix; dir[s][1] = iy; dir[s][2] = iz;
+          }
+      }
+  for (int m = 0; m < nmb; ++m) {
+    int cnt = 0;
+    for (int n = 0; n < 56; ++n) {
+      const int b = nghbr56[56*m + n];
+      if (b < 0) continue;
+      int s[3];
+      for (int a = 0; a < 3; ++a) {
+        const double lo_b = fbox[6*b + 2*a], hi_b = fbox[6*b + 2*a + 1];
+        const double lo_m = fbox[6*m + 2*a], hi_m = fbox[6*m + 2*a + 1];
+        const double gap = dir[n][a] > 0 ? lo_b - hi_m
+                         : (dir[n][a] < 0 ? hi_b - lo_m : 0.5*(lo_b + hi_b - lo_m - hi_m));
+        s[a] = (int)lround(gap/nf[a]);
+      }
+      int seen = (b == m && !s[0] && !s[1] && !s[2]);
+      for (int k = 0; k < cnt && !seen; ++k)
+        seen = nb[m*DUSTB_LEAF_MAXNB + k] == b && nbs[(m*DUSTB_LEAF_MAXNB + k)*3] == s[0] &&
+               nbs[(m*DUSTB_LEAF_MAXNB + k)*3 + 1] == s[1] && nbs[(m*DUSTB_LEAF_MAXNB + k)*3 + 2] == s[2];
+      if (seen) continue;
+      if (cnt >= DUSTB_LEAF_MAXNB) return -1;
+      nb[m*DUSTB_LEAF_MAXNB + cnt] = b;
+      for (int a = 0; a < 3; ++a) nbs[(m*DUSTB_LEAF_MAXNB + cnt)*3 + a] = s[a];
+      ++cnt;
+    }
+    nnb[m] = cnt;
+    for (int k = cnt; k < DUSTB_LEAF_MAXNB; ++k) {
+      nb[m*DUSTB_LEAF_MAXNB + k] = -1;
+      for (int a = 0; a < 3; ++a) nbs[(m*DUSTB_LEAF_MAXNB + k)*3 + a] = 0;
+    }
+  }
+  for (int m = 0; m < nmb; ++m) {
+    int mx = blev[m], w[3] = {0, 0, 0};
+    for (int k = 0; k < nnb[m]; ++k) {
+      const int b = nb[m*DUSTB_LEAF_MAXNB + k];
+      if (blev[b] > mx) mx = blev[b];
+      for (int a = 0; a < 3; ++a) {
+        const int wd = fbox[6*b + 2*a + 1] - fbox[6*b + 2*a];
+        if (k == 0 || wd < w[a]) w[a] = wd;
+      }
+    }
+    nbmax[m] = mx;
+    const int *f = &fbox[6*m];
+    int ok = w[0] > 0 && w[1] > 0 && w[2] > 0;
+    for (int a = 0; a < 3 && ok; ++a) ok = (f[2*a + 1] - f[2*a]) % w[a] == 0;
+    for (int cz = f[4] - w[2]; ok && cz < f[5] + w[2]; cz += w[2])
+      for (int cy = f[2] - w[1]; ok && cy < f[3] + w[1]; cy += w[1])
+        for (int cx = f[0] - w[0]; ok && cx < f[1] + w[0]; cx += w[0]) {
+          if (cx >= f[0] && cx < f[1] && cy >= f[2] && cy < f[3] && cz >= f[4] && cz < f[5]) continue;
+          if (!x3per && (cz < 0 || cz >= nf[2])) continue;
+          int held = 0;
+          for (int k = 0; k < nnb[m] && !held; ++k) {
+            const int b = nb[m*DUSTB_LEAF_MAXNB + k];
+            const int *s = &nbs[(m*DUSTB_LEAF_MAXNB + k)*3];
+            const int c3[3] = {cx, cy, cz};
+            held = 1;
+            for (int a = 0; a < 3; ++a)
+              held = held && fbox[6*b + 2*a] - s[a]*nf[a] <= c3[a] &&
+                     c3[a] + w[a] <= fbox[6*b + 2*a + 1] - s[a]*nf[a];
+          }
+          ok = held;
+        }
+    if (!ok) { w[0] = w[1] = w[2] = 0; ++info[4]; }
+    for (int a = 0; a < 3; ++a) safe[3*m + a] = w[a];
+  }
+  /* the location index: keys ascending (insertion sort; the tests' meshes are small) */
+  for (int b = 0; b < nmb; ++b) {
+    const int sh = nlev - blev[b];
+    const long long key = ((long long)blev[b] << 57) | ((long long)(fbox[6*b + 4]/(geo[2] << sh)) << 38) |
+                          ((long long)(fbox[6*b + 2]/(geo[1] << sh)) << 19) |
+                          (long long)(fbox[6*b]/(geo[0] << sh));
+    int k = b;
+    while (k > 0 && lockey[k - 1] > key) { lockey[k] = lockey[k - 1]; locblk[k] = locblk[k - 1]; --k; }
+    lockey[k] = key; locblk[k] = b;
+  }
+  return 0;
+}
+
+/* Owner (src/dust/dust_leaf3d.hpp:534-595) without shear: the point framed next to block m (and
+ * mirrored into the domain at a physical x3 face); the first of m and its neighbours whose box
+ * holds it, else the block of Locate (:515-533, the location index level by level) */
+static int leaf_owner(const dustb_ctx *c, const double px[3], int m) {
+  const dustb_mesh *ms = &c->mesh;
+  const dustb_leaf_tables *T = ms->leaf;
+  const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
+  const double xmin[3] = {ms->x1min, ms->x2min, ms->x3min};
+  const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
+  double x[3] = {px[0], px[1], px[2]};
+  for (int a = 0; a < (ms->x3bc == 0 ? 3 : 2); ++a) {
+    const double cx = MB(m, X1MIN + a) + 0.5*nx[a]*MB(m, DX1 + a);
+    x[a] -= L[a]*round((x[a] - cx)*(1.0/L[a]));
+  }
+  if (ms->x3bc != 0) {
+    if (x[2] < ms->x3min) x[2] = 2.0*ms->x3min - x[2];
+    if (x[2] >= ms->x3max) x[2] = fmin(2.0*ms->x3max - x[2], ms->x3max - 1.0e-12*L[2]);
+  }
+  CandList CL = {NULL, 0, 0};
+  const int none[6] = {0, 0, 0, 0, 0, 0};
+  candidates(c, m, 0, none, 0, &CL);
+  int res = -1;
+  for (int k = 0; k < CL.n && res < 0; ++k) {
+    const int b = CL.v[k].b;
+    int in = 1;
+    for (int a = 0; a < 3; ++a) {
+      const double fi = (x[a] - (MB(b, X1MIN + a) - CL.v[k].s[a]*L[a]))/MB(b, DX1 + a);
+      in = in && fi >= 0.0 && fi < nx[a];
+    }
+    if (in) res = b;
+  }
+  free(CL.v);
+  if (res >= 0) return res;
+  int cc[3];
+  for (int a = 0; a < 3; ++a) {
+    const double fdx = T->root_dx[a]/(double)(1 << T->nlev);
+    cc[a] = (int)floor((x[a] - xmin[a])/fdx);
+    if (a == 2 && ms->x3bc != 0 && (cc[a] < 0 || cc[a] >= T->nfine[a])) return -1;
+    cc[a] = ((cc[a] % T->nfine[a]) + T->nfine[a]) % T->nfine[a];
+  }
+  for (int l = 0; l <= T->nlev; ++l) {
+    const int sh = T->nlev - l;
+    const long long key = ((long long)l << 57) | ((long long)(cc[2]/(nx[2] << sh)) << 38) |
+                          ((long long)(cc[1]/(nx[1] << sh)) << 19) | (long long)(cc[0]/(nx[0] << sh));
+    for (int k = 0; k < ms->nmb; ++k)
+      if (T->lockey[k] == key) return T->locblk[k];
+  }
+  return -1;
+}
+
+/* CloudInstantSwitch (src/dust/dust_cloud.cpp:1023-1085): every plain cloud of level >= L
+ * takes max(L, the level of the block holding its centre); returns the clouds changed */
+int oracle_cloud_instant_switch(const dustb_ctx *c, int L) {
+  const dustb_mesh *ms = &c->mesh;
+  if (L < 0 || L >= ms->leaf->nlev) return 0;
+  const double *pr = c->part.pr; int *pi = c->part.pi; long long stride = c->part.stride;
+  int n = 0;
+  for (int p = 0; p < c->part.npart; ++p) {
+    const int code = PI(DUSTB_PLEV, p);
+    if ((code & ~15) != 0 || code < L) continue;
+    const double x[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p), PR(DUSTB_IPZ, p)};
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    if (m < 0 || m >= ms->nmb) m = 0;
+    const int b = leaf_owner(c, x, m);
+    if (b < 0) continue;
+    const int lev = ms->leaf->blev[b] > L ? ms->leaf->blev[b] : L;
+    if (lev != code) { PI(DUSTB_PLEV, p) = lev; ++n; }
+  }
+  return n;
+}
+
+/* the split's eligibility (AnyAbove / AllAbove :596-622, SupportBox :653-666, InsideFiner
+ * :668-681): the support of a plain level-lev cloud shrunk by the slack meets (overlap) or lies
+ * on leaves above lev, the leaves of level l dilated by buffer << (nlev - l + 1) finest cells */
+static int leaf_inside_finer(const dustb_ctx *c, const dustb_cloud_split *sp, double px,
+                             double py, double pz, int lev, int m) {
+  const dustb_mesh *ms = &c->mesh;
+  const dustb_leaf_tables *T = ms->leaf;
+  if (lev >= T->nlev || lev >= sp->max_level) return 0;
+  if (sp->split_everywhere) return 1;
+  const double L[3] = {ms->x1max - ms->x1min, ms->x2max - ms->x2min, ms->x3max - ms->x3min};
+  const double xmin[3] = {ms->x1min, ms->x2min, ms->x3min};
+  const int nx[3] = {ms->nx1, ms->nx2, ms->nx3};
+  double x[3] = {px, py, pz};
+  for (int a = 0; a < (ms->x3bc == 0 ? 3 : 2); ++a) {
+    const double cx = MB(m, X1MIN + a) + 0.5*nx[a]*MB(m, DX1 + a);
+    x[a] -= L[a]*round((x[a] - cx)*(1.0/L[a]));
+  }
+  int box[6];
+  for (int a = 0; a < 3; ++a) {
+    const double r = (1.0 - sp->slack)*T->root_dx[a]/(double)(1 << lev);
+    const double fdx = T->root_dx[a]/(double)(1 << T->nlev);
+    box[2*a] = (int)floor((x[a] - r - xmin[a])/fdx);
+    box[2*a + 1] = (int)ceil((x[a] + r - xmin[a])/fdx) - 1;
+  }
+  leaf_clip_z(c, &box[4], &box[5]);
+  const int l1 = lev + 1;
+  if (l1 > T->nlev) return 0;
+  const int r = (sp->split_buffer > 0 && l1 >= 1 && l1 <= T->nlev) ? sp->split_buffer << (T->nlev - l1 + 1) : 0;
+  const int g = leaf_need_global(c, m, box, r);
+  if (!g && l1 > T->nbmax[m] && box[0] <= box[1] && box[2] <= box[3] && box[4] <= box[5]) return 0;
+  return sp->split_overlap ? leaf_meets(c, m, box, l1, r, g) : leaf_covered(c, m, box, l1, r, g);
+}
+static double half_width(const dustb_leaf_tables *T, int lev, int a) {
+  return T->root_dx[a]/(double)(1 << (lev & 15));
+}
+/* P1FlagT / P1SepT<LeafTraversal3D> (src/dust/dust_cloud3d.cpp:188-250) */
+static int p1_flag(const dustb_ctx *c, const dustb_cloud_split *sp, int m, int code, const double x[3]) {
+  const dustb_leaf_tables *T = c->mesh.leaf;
+  const int lev = code & 15, l1 = (code >> 6) & 3, l2 = (code >> 4) & 3, l3 = (code >> 9) & 3;
+  if (!l1 && !l2 && !l3) return leaf_inside_finer(c, sp, x[0], x[1], x[2], lev, m);
+  if (lev > 0 && leaf_inside_finer(c, sp, x[0], x[1], x[2], lev - 1, m)) {
+    const double h1 = half_width(T, lev - 1, 0), h2 = half_width(T, lev - 1, 1), h3 = half_width(T, lev - 1, 2);
+    return ((l1 & 1) && leaf_inside_finer(c, sp, x[0] - h1, x[1], x[2], lev - 1, m)) ||
+           ((l1 & 2) && leaf_inside_finer(c, sp, x[0] + h1, x[1], x[2], lev - 1, m)) ||
+           ((l2 & 1) && leaf_inside_finer(c, sp, x[0], x[1] - h2, x[2], lev - 1, m)) ||
+           ((l2 & 2) && leaf_inside_finer(c, sp, x[0], x[1] + h2, x[2], lev - 1, m)) ||
+           ((l3 & 1) && leaf_inside_finer(c, sp, x[0], x[1], x[2] - h3, lev - 1, m)) ||
+           ((l3 & 2) && leaf_inside_finer(c, sp, x[0], x[1], x[2] + h3, lev - 1, m));
+  }
+  return 0;
+}
+static int p1_sep(const dustb_ctx *c, const dustb_cloud_split *sp, int m, int code, const double x[3]) {
+  const dustb_leaf_tables *T = c->mesh.leaf;
+  const int lev = code & 15;
+  const int l = ((code & ~15) == 0) ? lev : lev - 1;
+  int s = 0;
+  for (int a = 0; a < 3; ++a) {
+    const double h = half_width(T, l, a);
+    double lo[3] = {x[0], x[1], x[2]}, hi[3] = {x[0], x[1], x[2]};
+    lo[a] -= h; hi[a] += h;
+    if (leaf_inside_finer(c, sp, lo[0], lo[1], lo[2], l, m)) s |= 1 << (2*a);
+    if (leaf_inside_finer(c, sp, hi[0], hi[1], hi[2], l, m)) s |= 2 << (2*a);
+  }
+  return s;
+}
+typedef struct { double off, frac; int lobe; } P1Piece;
+/* P1Pieces3 (:52-65) */
+static int p1_pieces(int lobe_old, int sep_lo, int sep_hi, P1Piece out[3]) {
+  int n = 0;
+  const double total = 0.5 + 0.25*((lobe_old & 1) ? 1 : 0) + 0.25*((lobe_old & 2) ? 1 : 0);
+  const int lo = (lobe_old & 1) && sep_lo, hi = (lobe_old & 2) && sep_hi;
+  const int lobe_new = lobe_old & ~((lo ? 1 : 0) | (hi ? 2 : 0));
+  const double keep = 0.5 + 0.25*((lobe_new & 1) ? 1 : 0) + 0.25*((lobe_new & 2) ? 1 : 0);
+  out[n].off = 0.0; out[n].frac = keep/total; out[n].lobe = lobe_new; ++n;
+  if (lo) { out[n].off = -1.0; out[n].frac = 0.25/total; out[n].lobe = 0; ++n; }
+  if (hi) { out[n].off = 1.0; out[n].frac = 0.25/total; out[n].lobe = 0; ++n; }
+  return n;
+}
+static double wrap_pos(double x, double lo, double hi) {
+  const double len = hi - lo;
+  while (x < lo) x += len;
+  while (x >= hi) x -= len;
+  return x;
+}
+/* SplitCloudsP1DeviceT (src/dust/dust_cloud3d.cpp:1005-1310) without the budget, the split
+ * velocity and the block marks: the count pass, the exclusive scan of the appended pieces, the
+ * fill (pieces last to first, the parent's slot last).  The arrays must hold npart + the pieces;
+ * returns the pieces appended (npart is not changed), or -1 when they exceed the capacity. */
+int oracle_cloud_split_p1(const dustb_ctx *c, const dustb_cloud_split *sp, unsigned long long tag0) {
+  const dustb_mesh *ms = &c->mesh;
+  const dustb_leaf_tables *T = ms->leaf;
+  double *pr = c->part.pr; int *pi = c->part.pi; long long stride = c->part.stride;
+  const int np = c->part.npart;
+  int *sep = (int *)calloc((size_t)np + 1, sizeof(int));
+  int *off = (int *)calloc((size_t)np + 1, sizeof(int));
+  int total = 0;
+  for (int p = 0; p < np; ++p) {
+    const int code = PI(DUSTB_PLEV, p);
+    const double x[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p), PR(DUSTB_IPZ, p)};
+    int m = PI(DUSTB_PGID, p) - ms->gids;
+    if (m < 0 || m >= ms->nmb) m = 0;
+    off[p] = total;
+    if ((code & ~(15 | (3 << 4) | (3 << 6) | (3 << 9))) != 0 || !p1_flag(c, sp, m, code, x)) continue;
+    const int s = p1_sep(c, sp, m, code, x);
+    const int plain = (code & ~15) == 0;
+    P1Piece pc[3][3];
+    int n = 1;
+    for (int a = 0; a < 3; ++a) {
+      const int lobe = plain ? 3 : ((a == 0) ? (code >> 6) & 3 : ((a == 1) ? (code >> 4) & 3 : (code >> 9) & 3));
+      n *= p1_pieces(lobe, (s >> (2*a)) & 1, (s >> (2*a + 1)) & 1, pc[a]);
+    }
+    sep[p] = s | 64;
+    total += n - 1;
+  }
+  if ((long long)np + total > stride) { free(sep); free(off); return -1; }
+  const int reflect = ms->x3bc == 1;
+  for (int p = 0; p < np; ++p) {
+    if (!sep[p]) continue;
+    const int code = PI(DUSTB_PLEV, p);
+    const int lev = code & 15, plain = (code & ~15) == 0;
+    const double x[3] = {PR(DUSTB_IPX, p), PR(DUSTB_IPY, p), PR(DUSTB_IPZ, p)};
+    const double mass = PR(DUSTB_IPM, p);
+    P1Piece pc[3][3];
+    int n[3];
+    for (int a = 0; a < 3; ++a) {
+      const int lobe = plain ? 3 : ((a == 0) ? (code >> 6) & 3 : ((a == 1) ? (code >> 4) & 3 : (code >> 9) & 3));
+      n[a] = p1_pieces(lobe, (sep[p] >> (2*a)) & 1, (sep[p] >> (2*a + 1)) & 1, pc[a]);
+    }
+    const int clev = plain ? lev + 1 : lev;
+    double e[3];
+    for (int a = 0; a < 3; ++a) e[a] = half_width(T, clev, a);
+    const int n12 = n[0]*n[1];
+    for (int k = n12*n[2] - 1; k >= 0; --k) {
+      const int ia[3] = {k % n[0], (k/n[0]) % n[1], k/n12};
+      const int s = (k == 0) ? p : np + off[p] + k - 1;
+      double cpos[3];
+      for (int a = 0; a < 3; ++a) cpos[a] = x[a] + pc[a][ia[a]].off*e[a];
+      int zmir = 0;
+      cpos[0] = wrap_pos(cpos[0], ms->x1min, ms->x1max);
+      cpos[1] = wrap_pos(cpos[1], ms->x2min, ms->x2max);
+      if (ms->x3bc == 0) {
+        cpos[2] = wrap_pos(cpos[2], ms->x3min, ms->x3max);
+      } else if (cpos[2] < ms->x3min) {
+        cpos[2] = 2.0*ms->x3min - cpos[2]; zmir = 1;
+      } else if (cpos[2] >= ms->x3max) {
+        cpos[2] = 2.0*ms->x3max - cpos[2]; zmir = 1;
+        if (cpos[2] >= ms->x3max) cpos[2] = ms->x3max - 1.0e-12*(ms->x3max - ms->x3min);
+      }
+      if (k > 0) {
+        for (int q = 0; q < DUSTB_NREAL; ++q) PR(q, s) = PR(q, p);
+        for (int q = 0; q < DUSTB_NINT; ++q) PI(q, s) = PI(q, p);
+        const unsigned long long t = tag0 + (unsigned long long)(off[p] + k - 1);
+        PI(DUSTB_PTAG, s) = (int)(unsigned)(t & 0xffffffffULL);
+        PI(DUSTB_PTAGH, s) = (int)(unsigned)(t >> 32);
+      }
+      PR(DUSTB_IPX, s) = cpos[0]; PR(DUSTB_IPX1, s) = cpos[0];
+      PR(DUSTB_IPY, s) = cpos[1]; PR(DUSTB_IPY1, s) = cpos[1];
+      PR(DUSTB_IPZ, s) = cpos[2]; PR(DUSTB_IPZ1, s) = cpos[2];
+      double mp = mass*pc[0][ia[0]].frac*pc[1][ia[1]].frac;
+      mp = mp*pc[2][ia[2]].frac;
+      const int l3 = pc[2][ia[2]].lobe;
+      PR(DUSTB_IPM, s) = mp;
+      PI(DUSTB_PLEV, s) = clev | (pc[0][ia[0]].lobe << 6) | (pc[1][ia[1]].lobe << 4) |
+                          ((zmir && (l3 == 1 || l3 == 2) ? 3 - l3 : l3) << 9);
+      if (zmir && reflect) { PR(DUSTB_IPVZ, s) = -PR(DUSTB_IPVZ, s); PR(DUSTB_IPVZ1, s) = -PR(DUSTB_IPVZ1, s); }
+      int am = PI(DUSTB_PGID, s) - ms->gids;
+      if (am < 0 || am >= ms->nmb) am = 0;
+      const int b = leaf_owner(c, cpos, am);
+      PI(DUSTB_PGID, s) = ms->gids + ((b >= 0 && b < ms->nmb) ? b : am);
+    }
+  }
+  free(sep); free(off);
+  return total;
+}
+
 /* every leaf of the cloud at x (level code, anchored at block m): f(ctx, leaf); with moments the
  * moment traversal, else the weight traversal */
 static void cloud_leaves(const dustb_ctx *c, const Ind *d, int m, const double x[3], int code,
                          int moments, CloudLeafFn f, void *ctx, unsigned *err) {
   const dustb_mesh *ms = &c->mesh;
+  if (ms->leaf) { leaf_foreach(c, d, m, x, code, moments, f, ctx); return; }
   const double Lz = ms->x3max - ms->x3min;
   CloudAxis X, Y, Z;
   cloud_axis(c, m, 0, x[0], code, &X);
@@ -1320,6 +1975,19 @@ unsigned oracle_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, co
   return err;
 }
 
+/* the clouds' copy exchanges: on a refined mesh the multilevel one (its coarse arrays
+ * allocated here) */
+void oracle_ghost_copy_ml(const dustb_ctx *c, double *a, int nvar, double *ca);
+static void cloud_copy_exchange(const dustb_ctx *c, double *a, int nvar, int x3_bcs) {
+  const dustb_mesh *ms = &c->mesh;
+  if (!ms->nghbr_ml) { oracle_ghost_copy(c, a, nvar, x3_bcs); return; }
+  const size_t n = (size_t)ms->nmb*nvar*(ms->nx1/2 + 2*ms->ng)*(ms->nx2/2 + 2*ms->ng)*
+                   (ms->nx3/2 + 2*ms->ng);
+  double *ca = (double *)malloc(n*sizeof(double));
+  oracle_ghost_copy_ml(c, a, nvar, ca);
+  free(ca);
+}
+
 /* CloudDefectCorrection (src/dust/dust_imex3d_dc.cpp:229-274) with CloudOperatorKernelT
  * (dust_cloud_imex_kernels.hpp:20-70): one sweep x <- x + (rho + Q)^-1 (M + P - rho x - D M G x)
  * on u*, the operator D M G x = the clouds' m c W ubar / V with ubar their linear gather of x
@@ -1328,7 +1996,7 @@ unsigned oracle_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh) {
   const dustb_mesh *ms = &c->mesh; Ind d = indices(ms); int nv = c->f.nvar_gas;
   double *x = c->f.ustar, *r = c->f.work;
   double *pr = c->part.pr; const int *pi = c->part.pi; long long stride = c->part.stride;
-  oracle_ghost_copy(c, x, 3, 1);
+  cloud_copy_exchange(c, x, 3, 1);
   double *gp = (double *)malloc((size_t)ms->nmb*d.n3*d.n2*d.n1*12*sizeof(double));
   oracle_gather_pack(c, x, gp);
   memset(r, 0, field_size(ms, 3)*sizeof(double));
@@ -1592,11 +2260,11 @@ unsigned oracle_cloud_imex_cycle(const dustb_ctx *c, double gamma, double dt, co
       int nsweeps = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
       for (int w = 0; w < nsweeps; ++w) err |= oracle_cloud_dc1_sweep(c, a_dt, s);
     }
-    oracle_ghost_copy(c, c->f.ustar, 3, 1);
+    cloud_copy_exchange(c, c->f.ustar, 3, 1);
     oracle_gather_pack(c, c->f.ustar, gp);
     err |= oracle_cloud_gather_kick(c, a_dt, s, gp);
     if (c->phys.back_reaction) oracle_cloud_apply_pmbr(c, a_dt, s);
-    oracle_ghost_copy(c, c->f.u0, c->f.nvar_gas, 0);
+    cloud_copy_exchange(c, c->f.u0, c->f.nvar_gas, 0);
   }
   free(gp);
   return err;

@@ -87,6 +87,9 @@ def lib():
             "oracle_ghost_copy_ml": ([P, VP, I, VP], None),
             "oracle_operator_particles": ([P, D], C.c_uint),
             "oracle_dc_correct": ([P], None),
+            "oracle_leaf_tables": ([VP, I, VP, VP, VP] + [VP] * 9, I),
+            "oracle_cloud_instant_switch": ([P, I], I),
+            "oracle_cloud_split_p1": ([P, C.POINTER(capi.DustbCloudSplit), C.c_ulonglong], I),
         }
         for name, (args, res) in sig.items():
             f = getattr(_lib, name)
@@ -319,6 +322,43 @@ class Oracle:
         err = self.call("cloud_pc2_cycle", dt, C.cast(C.byref(chi), C.c_void_p),
                         self.x3_removed.ctypes.data)
         return err, chi.value
+
+    # --- refinable clouds on a refined 3-D mesh ---
+    def set_leaf_tables(self, lt):
+        """The leaf tables (athenak_b200.amr.LeafTables, host arrays): the cloud calls then
+        take the leaf traversal."""
+        self.leaf_arrays = {k: np.ascontiguousarray(v) for k, v in lt.arrays.items()}
+        self.leaf = capi.leaf_tables_struct(self.leaf_arrays, lt.nlev, lt.nfine, lt.root_dx)
+        self.ctx.mesh.leaf = C.addressof(self.leaf)
+
+    def ensure_capacity(self, n):
+        """Grows the particle rows to hold n particles (a quarter more)."""
+        st = self.st
+        if n <= st.stride:
+            return
+        cap = int(n + n // 4)
+        pr = np.zeros((17, cap))
+        pi = np.zeros((5, cap), np.int32)
+        pr[:, :st.npart] = st.pr[:, :st.npart]
+        pi[:, :st.npart] = st.pi[:, :st.npart]
+        st.pr, st.pi = pr, pi
+        self.arr["pr"], self.arr["pi"] = pr, pi
+        self.ctx.part.pr, self.ctx.part.pi = pr.ctypes.data, pi.ctypes.data
+        self.ctx.part.stride = cap
+
+    def cloud_instant_switch(self, level_cap):
+        return self.call("cloud_instant_switch", int(level_cap))
+
+    def cloud_split_p1(self, split, tag0):
+        """The moving P1 split; returns the pieces appended (npart grows by them)."""
+        n = self.call("cloud_split_p1", C.byref(split), C.c_ulonglong(tag0))
+        if n < 0:
+            # the count alone: make room for every cloud's at most 26 pieces, then split
+            self.ensure_capacity(self.st.npart * 27)
+            n = self.call("cloud_split_p1", C.byref(split), C.c_ulonglong(tag0))
+        self.st.npart += n
+        self.ctx.part.npart = self.st.npart
+        return n
 
     def point_science_fields(self, mass_only=False, species=-1):
         """DepositPointScienceFields: (out field with 1 or 4 vars, err)."""
