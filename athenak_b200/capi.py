@@ -216,6 +216,7 @@ SIGNATURES = {
     "dustb_pc2_advance": [CTXP, D, VP],
     "dustb_pc2_commit": [CTXP, D, VP],
     "dustb_imex_cycle": [CTXP, C.POINTER(DustbImexCoeffs), VP, VP],
+    "dustb_dc1_sweep_plan": [CTXP, C.POINTER(DustbDepPlan), D, VP, LL, VP],
     "dustb_refined_imex_cycle": [CTXP, C.POINTER(DustbDepPlan), C.POINTER(DustbImexCoeffs), VP,
                                  LL, VP, VP],
     "dustb_pc2_cycle": [CTXP, D, VP, VP, VP],

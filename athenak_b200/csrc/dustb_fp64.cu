@@ -3071,6 +3071,25 @@ int dustb_imex_cycle(const dustb_ctx *c, const dustb_imex_coeffs *co, double *x3
 // one imex2+ cycle on a refined mesh: the task order of dustb_imex_cycle with the deposits
 // exchanged by the general remap and u*, the operator's field and the gas state by the
 // multilevel copy exchange
+// ApplyDefectCorrection (dust_solver.cpp:226-252), one sweep on a refined mesh: u*'s ghost
+// cells by the multilevel copy exchange, the operator's ghost deposits by the general remap
+int dustb_dc1_sweep_plan(const dustb_ctx *c, const dustb_dep_plan *plan, double a_dt,
+                         double *coarse, long long coarse_bytes, void *stream) {
+  CHECK_CTX(c);
+  if (!plan || !c->mesh.nghbr_ml) return DUSTB_EINVAL;
+  const Ind d = make_ind(c->mesh);
+  int rc = dustb_ghost_copy_ml(c, c->f.ustar, 3, coarse, coarse_bytes, stream);
+  if (rc) return rc;
+  cudaMemsetAsync(c->f.work, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
+  if (c->part.npart > 0)
+    k_operator<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.ustar, c->f.work, a_dt, 0.0, c->err);
+  rc = dustb_ghost_add_plan(c, plan, c->f.work, 3, stream);
+  if (rc) return rc;
+  k_dc_correct<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(
+      d, c->f.u0, c->f.nvar_gas, c->f.qdep, c->f.work, c->f.ustar);
+  return launch_status("dc1_sweep_plan");
+}
+
 int dustb_refined_imex_cycle(const dustb_ctx *c, const dustb_dep_plan *plan,
                              const dustb_imex_coeffs *co, double *coarse, long long coarse_bytes,
                              double *x3_removed, void *stream) {
@@ -3100,16 +3119,8 @@ int dustb_refined_imex_cycle(const dustb_ctx *c, const dustb_dep_plan *plan,
     RUN(dustb_solve_ustar(c, stream));
     if (br && c->phys.drag_solver >= DUSTB_SOLVER_DC1) {
       const int nsw = (c->phys.drag_solver == DUSTB_SOLVER_DC2) ? 2 : 1;
-      for (int w = 0; w < nsw; ++w) {
-        // ApplyDefectCorrection (dust_solver.cpp:226-252) with the refined exchanges
-        RUN(dustb_ghost_copy_ml(c, c->f.ustar, 3, coarse, coarse_bytes, stream));
-        cudaMemsetAsync(c->f.work, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
-        if (c->part.npart > 0)
-          k_operator<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.ustar, c->f.work, a_dt, 0.0, c->err);
-        RUN(dustb_ghost_add_plan(c, plan, c->f.work, 3, stream));
-        k_dc_correct<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(
-            d, c->f.u0, c->f.nvar_gas, c->f.qdep, c->f.work, c->f.ustar);
-      }
+      for (int w = 0; w < nsw; ++w)
+        RUN(dustb_dc1_sweep_plan(c, plan, a_dt, coarse, coarse_bytes, stream));
     }
     RUN(dustb_ghost_copy_ml(c, c->f.ustar, 3, coarse, coarse_bytes, stream));
     RUN(dustb_gather_kick_pmbr(c, a_dt, 0.0, stream));

@@ -36,6 +36,86 @@ DustGasDrag::~DustGasDrag() {
   if (cloud_ord_tag_) cudaFree(cloud_ord_tag_);
   if (dev_bad_) cudaFree(dev_bad_);
   if (gpack_) cudaFree(gpack_);
+  if (coarse_) cudaFree(coarse_);
+  if (leaf_.coarse) cudaFree(leaf_.coarse);
+  if (dev_count_) cudaFree(dev_count_);
+}
+
+// the copy exchange of a field: the multilevel one on a refined mesh
+TaskStatus DustGasDrag::CopyExchange(double *field, int nvar, int x3_bcs, const char *task) {
+  if (refined_) return Check(dustb_ghost_copy_ml(&ctx_, field, nvar, coarse_, coarse_bytes_, stream_), task);
+  return Check(dustb_ghost_copy(&ctx_, field, nvar, x3_bcs, stream_), task);
+}
+
+TaskStatus DustGasDrag::SetRefinedMesh(const dustb_dep_plan &plan) {
+  if (!ctx_.mesh.nghbr_ml || !ctx_.mesh.mb_lev) {
+    last_error_ = "SetRefinedMesh: the mesh has no refinement tables (nghbr_ml, mb_lev)";
+    return TaskStatus::fail;
+  }
+  const int nv = ctx_.f.nvar_gas > 5 ? ctx_.f.nvar_gas : 5;
+  const long long bytes = dustb_ghost_copy_ml_bytes(&ctx_.mesh, nv);
+  if (bytes <= 0) return Check(DUSTB_EINVAL, "SetRefinedMesh");
+  if (!coarse_ || coarse_bytes_ < bytes) {
+    if (coarse_) cudaFree(coarse_);
+    if (cudaMalloc(&coarse_, (size_t)bytes) != cudaSuccess) {
+      coarse_ = nullptr;
+      last_error_ = "SetRefinedMesh: exchange scratch not allocated";
+      return TaskStatus::fail;
+    }
+    coarse_bytes_ = bytes;
+  }
+  plan_ = plan;
+  refined_ = true;
+  return TaskStatus::complete;
+}
+
+TaskStatus DustGasDrag::SetLeafTables(const dustb_leaf_tables &tables) {
+  leaf_ = tables;
+  leaf_.coarse = nullptr;
+  leaf_.coarse_bytes = 0;
+  if (ctx_.mesh.nghbr_ml) {
+    const long long bytes = dustb_ghost_copy_ml_bytes(&ctx_.mesh, 3);
+    if (bytes <= 0 || cudaMalloc(&leaf_.coarse, (size_t)bytes) != cudaSuccess) {
+      leaf_.coarse = nullptr;
+      last_error_ = "SetLeafTables: exchange scratch not allocated";
+      return TaskStatus::fail;
+    }
+    leaf_.coarse_bytes = bytes;
+  }
+  ctx_.mesh.leaf = &leaf_;
+  return SetRefinableClouds(true);
+}
+
+void DustGasDrag::SetCloudSplit(const dustb_cloud_split &split, bool enable, int split_max_level,
+                                unsigned long long next_tag) {
+  split_ = split;
+  split_enable_ = enable;
+  split_max_level_ = split_max_level;
+  next_tag_ = next_tag;
+}
+
+TaskStatus DustGasDrag::RefineClouds(Driver *pdrive, void *scratch, long long bytes) {
+  if (!clouds_ || !ctx_.mesh.leaf) return TaskStatus::complete;
+  last_split_ = last_switch_ = 0;
+  if (split_enable_) {
+    int nnew = 0;
+    const int rc = dustb_cloud_split_p1(&ctx_, &split_, next_tag_, &nnew, scratch, bytes, stream_);
+    last_split_ = nnew;
+    if (rc != DUSTB_OK) return Check(rc, "RefineClouds");
+    ctx_.part.npart += nnew;
+    next_tag_ += (unsigned long long)nnew;
+  }
+  if (split_max_level_ >= 0) {
+    if (!dev_count_ && cudaMalloc(&dev_count_, sizeof(int)) != cudaSuccess) {
+      dev_count_ = nullptr;
+      last_error_ = "RefineClouds: device counter not allocated";
+      return TaskStatus::fail;
+    }
+    return Check(dustb_cloud_instant_switch(&ctx_, split_max_level_, &last_switch_, dev_count_,
+                                            stream_),
+                 "RefineClouds");
+  }
+  return TaskStatus::complete;
 }
 
 TaskStatus DustGasDrag::Check(int rc, const char *task) {
@@ -106,6 +186,7 @@ TaskStatus DustGasDrag::RecvDepQP(Driver *pdrive, int stage) {
   if (!ctx_.phys.back_reaction) return TaskStatus::complete;
   if (coupling_ == DustCoupling::pc2 && stage != 1) return TaskStatus::complete;
   if (clouds_) return TaskStatus::complete;   // (the clouds deposit into the owner cells)
+  if (refined_) return Check(dustb_ghost_add_plan(&ctx_, &plan_, ctx_.f.qdep, 5, stream_), "RecvDepQP");
   return Check(dustb_ghost_add(&ctx_, ctx_.f.qdep, 5, stream_), "RecvDepQP");
 }
 
@@ -124,13 +205,15 @@ TaskStatus DustGasDrag::GasImplicitSolve(Driver *pdrive, int stage) {
   for (int w = 0; w < nsw && ts == TaskStatus::complete; ++w)
     ts = clouds_ ? Check(dustb_cloud_dc1_sweep(&ctx_, a_dt(pdrive), 0.0, gpack_, stream_),
                          "CloudDefectCorrection")
-                 : Check(dustb_dc1_sweep(&ctx_, a_dt(pdrive), 0.0, stream_), "SolveCoupledStage");
+       : refined_ ? Check(dustb_dc1_sweep_plan(&ctx_, &plan_, a_dt(pdrive), coarse_,
+                                               coarse_bytes_, stream_), "SolveCoupledStage")
+                  : Check(dustb_dc1_sweep(&ctx_, a_dt(pdrive), 0.0, stream_), "SolveCoupledStage");
   return ts;
 }
 
 TaskStatus DustGasDrag::RecvUstar(Driver *pdrive, int stage) {
   if (coupling_ == DustCoupling::pc2) return TaskStatus::complete;   // (the midpoint covers ghosts)
-  return Check(dustb_ghost_copy(&ctx_, ctx_.f.ustar, 3, 1, stream_), "RecvUstar");
+  return CopyExchange(ctx_.f.ustar, 3, 1, "RecvUstar");
 }
 
 TaskStatus DustGasDrag::GatherKickPMBR(Driver *pdrive, int stage) {
@@ -145,6 +228,7 @@ TaskStatus DustGasDrag::RecvPMBR(Driver *pdrive, int stage) {
   if (!ctx_.phys.back_reaction) return TaskStatus::complete;
   if (coupling_ == DustCoupling::pc2 && stage != 2) return TaskStatus::complete;
   if (clouds_) return TaskStatus::complete;   // (the impulse went to the owner cells)
+  if (refined_) return Check(dustb_ghost_add_plan(&ctx_, &plan_, ctx_.f.dmom, 3, stream_), "RecvPMBR");
   return Check(dustb_ghost_add(&ctx_, ctx_.f.dmom, 3, stream_), "RecvPMBR");
 }
 
@@ -172,7 +256,7 @@ TaskStatus DustGasDrag::SetRefinableClouds(bool on) {
 }
 
 TaskStatus DustGasDrag::RecvU(Driver *pdrive, int stage) {
-  return Check(dustb_ghost_copy(&ctx_, ctx_.f.u0, ctx_.f.nvar_gas, 0, stream_), "RecvU");
+  return CopyExchange(ctx_.f.u0, ctx_.f.nvar_gas, 0, "RecvU");
 }
 
 TaskStatus DustGasDrag::NewTimeStep(Driver *pdrive, int stage) {

@@ -100,6 +100,31 @@ class DustGasDrag {
   // gather pack.
   TaskStatus SetRefinableClouds(bool on);
 
+  // A refined 3-D mesh (ctx.mesh.nghbr_ml and mb_lev set): the deposit exchanges by the general
+  // remap of plan (MeshBoundaryValuesDep's general path; the plan's arrays stay the caller's),
+  // the u* and gas-state copy exchanges by the multilevel exchange (RestrictCC, the 56-slot
+  // boxes, ProlongCC) with scratch allocated here, the dc1 / dc2 sweeps with both.
+  TaskStatus SetRefinedMesh(const dustb_dep_plan &plan);
+  // Refinable clouds on a refined 3-D mesh: the leaf traversal's block geometry (a copy of the
+  // struct, its device arrays the caller's; the u* exchange scratch allocated here), then
+  // SetRefinableClouds(true).
+  TaskStatus SetLeafTables(const dustb_leaf_tables &tables);
+  // <dust>/cloud_split_*: the split's controls, cloud_split_enable (the P1 split of
+  // RefineClouds), cloud_split_max_level = L (>= 0: the instant switch above L; the split
+  // stops at L), and the next 64-bit tag of this rank (IssueTags' counter).
+  void SetCloudSplit(const dustb_cloud_split &split, bool enable, int split_max_level,
+                     unsigned long long next_tag);
+  // RefineClouds (src/dust/dust_cloud.cpp:615-720), the task at the start of a cycle:
+  // SplitAndMergeClouds (:984-988) -- the P1 split (pieces appended, npart and the tag counter
+  // advanced), then the instant switch above cloud_split_max_level.  scratch: at least
+  // dustb_cloud_split_scratch_bytes(npart).  The particle rows are the caller's: when the
+  // pieces do not fit their capacity the task fails with the pieces' count in
+  // LastSplitPieces(); the caller grows the rows (Context().part) and runs it again.
+  TaskStatus RefineClouds(Driver *pdrive, void *scratch, long long bytes);
+  unsigned long long NextTag() const { return next_tag_; }
+  int LastSplitPieces() const { return last_split_; }
+  int LastSwitched() const { return last_switch_; }
+
   // the stage's drag tasks in dependency order on one rank and one stream
   TaskStatus DoStage(Driver *pdrive, int stage);
   // one cycle: every working stage
@@ -131,6 +156,19 @@ class DustGasDrag {
   int cloud_order_interval_ = 0;
   bool clouds_ = false;
   double *gpack_ = nullptr;   // the clouds' gather pack (12 doubles per padded cell)
+  // a refined mesh: the deposit remap and the copy exchange's scratch
+  bool refined_ = false;
+  dustb_dep_plan plan_{};
+  double *coarse_ = nullptr;
+  long long coarse_bytes_ = 0;
+  // refinable clouds on a refined mesh: the leaf tables and the split's controls
+  dustb_leaf_tables leaf_{};
+  dustb_cloud_split split_{};
+  bool split_enable_ = false;
+  int split_max_level_ = -1, last_split_ = 0, last_switch_ = 0;
+  unsigned long long next_tag_ = 0;
+  int *dev_count_ = nullptr;
+  TaskStatus CopyExchange(double *field, int nvar, int x3_bcs, const char *task);
 };
 
 // The mixed-precision form from the host (dustb_mixed_*): a compact FP32 shadow of the

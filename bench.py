@@ -705,6 +705,7 @@ def measure_refined(args):
     p1, _ = momentum()
     err_fp64 = dev.error_word()
     v64 = dev.t["pr"][[1, 3, 5], :npart].clone()
+    gid64 = dev.t["pi"][0, :npart].clone()
     # the mixed form on the same mesh from the same state (its tiles from the device work queue,
     # heaviest first: the blocks' particle counts are 125x apart)
     from athenak_b200.mixed import MixedDust
@@ -718,9 +719,19 @@ def measure_refined(args):
     pm1, _ = momentum()
     vm = dev.t["pr"][[1, 3, 5], :npart]
     vscale = float(v64.abs().max())
-    dv = float((vm - v64).abs().max()) / vscale
+    dvp = (vm - v64).abs().amax(dim=0)
+    dv = float(dvp.max()) / vscale
+    # where the largest deviations sit: particles whose block differs between the two forms
+    # (a position within FP32 round-off of a block face), and the worst particle's block level
+    gidm = dev.t["pi"][0, :npart]
+    nmis = int((gidm != gid64).sum())
+    pw = int(dvp.argmax())
+    lev_w = int(ms.lloc[int(gid64[pw]), 0] - ms.root_level)
+    same = gidm == gid64
+    dv_same = float(dvp[same].max()) / vscale if bool(same.any()) else 0.0
+    del gidm, same, dvp
     err_mixed = dev.error_word()
-    del mx, v64
+    del mx, v64, gid64
     torch.cuda.empty_cache()
     # refinable clouds on the same mesh from the same state: every cloud takes the level of its
     # leaf (the instant switch at level 0), one P1 split pass turns the clouds whose support
@@ -760,6 +771,9 @@ def measure_refined(args):
                      "speedup_vs_fp64": ms_cyc / ms_mixed,
                      "momentum_change_rel": float(np.abs(pm1 - pm0).max() / absm),
                      "velocity_max_rel_vs_fp64_after_same_cycles": dv,
+                     "velocity_max_rel_same_block": dv_same,
+                     "particles_in_another_block": nmis,
+                     "worst_particle_level": lev_w,
                      "note": "the FP64 form ran 1 + steps cycles, the mixed form the same number "
                              "from the same state"},
            "clouds": {"ms_per_step": ms_cloud, "value": ncl / (ms_cloud * 1e-3),

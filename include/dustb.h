@@ -521,6 +521,12 @@ int dustb_cloud_pc2_cycle(const dustb_ctx *ctx, double dt, double *chi_max, doub
 int dustb_imex_cycle(const dustb_ctx *ctx, const dustb_imex_coeffs *c, double *x3_removed,
                      void *stream);
 
+/* ApplyDefectCorrection (src/dust/dust_solver.cpp:226-252), one dc1 sweep on a refined mesh:
+ * u* exchanged by dustb_ghost_copy_ml (coarse: its scratch for 3 variables), the operator
+ * D M G x of the point particles into work, its ghost deposits remapped by the plan
+ * (dustb_ghost_add_plan), x += (rho + Q)^-1 (M + P - rho x - D M G x). */
+int dustb_dc1_sweep_plan(const dustb_ctx *ctx, const dustb_dep_plan *plan, double a_dt,
+                         double *coarse, long long coarse_bytes, void *stream);
 /* One imex2+ cycle of the point-particle drag step on a refined 3-D mesh (ctx->mesh.nghbr_ml
  * and mb_lev set): the task order of dustb_imex_cycle with the deposits exchanged by
  * dustb_ghost_add_plan (plan: the mesh's general remap) and u*, the dc1 / dc2 operator's field
