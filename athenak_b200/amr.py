@@ -389,6 +389,27 @@ def root_cell_size(ms: MeshSpec):
     return tuple((ms.hi[a] - ms.lo[a]) / (ms.nmbroot[a] * ms.nx[a]) for a in range(3))
 
 
+def uniform_leaf_spec(ms: MeshSpec):
+    """A uniform 3-D mesh (blocks numbered (b3 nb2 + b2) nb1 + b1) in the terms of the leaf
+    tables: every block at the root level, its same-level neighbours in the first sub-slot of
+    each NeighborIndex direction."""
+    from types import SimpleNamespace
+    nb1, nb2, nb3 = ms.nblocks
+    root = max(int(np.ceil(np.log2(n))) if n > 1 else 0 for n in ms.nblocks)
+    lloc = np.zeros((ms.nmb, 4), np.int32)
+    ng56 = np.full((ms.nmb, 56), -1, np.int32)
+    for m in range(ms.nmb):
+        b1, b2, b3 = m % nb1, (m // nb1) % nb2, m // (nb1 * nb2)
+        lloc[m] = (root, b1, b2, b3)
+        for o3 in (-1, 0, 1):
+            for o2 in (-1, 0, 1):
+                for o1 in (-1, 0, 1):
+                    if o1 or o2 or o3:
+                        ng56[m, neighbor_index(o1, o2, o3, 0, 0)] = ms.nghbr[m, dir_index(o1, o2, o3)]
+    return SimpleNamespace(nx=ms.nx, nmbroot=tuple(ms.nblocks), root_level=root, max_level=root,
+                           x3bc=ms.x3bc, lloc=lloc, nghbr56=ng56, nmb=ms.nmb, lo=ms.lo, hi=ms.hi)
+
+
 def leaf_tables(ms: MeshSpec, builder=None) -> LeafTables:
     """The tables of a refined 3-D mesh from the C++ host layer (dustb_host_leaf_tables), or
     from builder (a function of the same signature: the oracle's own build in the tests)."""

@@ -2076,10 +2076,10 @@ __global__ void k_split_fill(PCtx P, MCtx M, Ind d, const int *sep, const int *o
 
 // every leaf of the cloud at x (level lev, anchored at block m): f(leaf); with kMoments the
 // moment traversal (a leaf with zero weight but a moment visited), else the weight traversal
-template <bool kMoments, typename F>
+template <bool kMoments, int LF, typename F>
 __device__ void cloud_leaves(const MCtx &M, const Ind &d, int m, const double x[3], int lev,
                              const double L[3], int x3phys, F &&f, unsigned *err) {
-  if (M.lt.on) {
+  if constexpr (LF != 0) {
     leaf_foreach<kMoments>(M, d, m, x, lev, f);
     return;
   }
@@ -2141,11 +2141,12 @@ __device__ void cloud_leaves(const MCtx &M, const Ind &d, int m, const double x[
 }
 
 // the clouds' linear gather of the packed field at x (CloudLinearGather3D without the blend)
+template <int LF>
 __device__ void cloud_gather(const MCtx &M, const Ind &d, int m, const double x[3], int lev,
                              const double L[3], int x3phys, const double *gp, double ug[3],
                              unsigned *err) {
   ug[0] = ug[1] = ug[2] = 0.0;
-  cloud_leaves<true>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+  cloud_leaves<true, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const int b = lf.b;
     const double w = lf.w;
     const double dx1 = M.s(b, DX1), dx2 = M.s(b, DX2), dx3 = M.s(b, DX3);
@@ -2170,7 +2171,37 @@ __device__ void cloud_gather(const MCtx &M, const Ind &d, int m, const double x[
   }, err);
 }
 
+// The clouds' deposits: f[key + c stride] += v[c] for c < N, where the lanes of a warp that add
+// to the same cell (the same key) combine first.  The lanes sharing a key (match_any) sum in a
+// binary tree over their ranks among those peers (round s: the peer of rank r, r a multiple of
+// 2s, takes the partial sum of the peer of rank r + s, the (r + s)-th set bit of the peer mask),
+// and the peer of rank 0 issues the N atomics: in cell order the clouds of a cell hit the same
+// leaves, so a warp issues about one atomic per distinct leaf instead of one per lane.
+template <int N>
+__device__ __forceinline__ void warp_add(double *f, long long key, long long stride,
+                                         double (&v)[N]) {
+  const unsigned act = __activemask();
+  const unsigned peers = __match_any_sync(act, key);
+  const unsigned lane = threadIdx.x & 31u;
+  const int rank = __popc(peers & ((1u << lane) - 1u));
+  const int cnt = __popc(peers);
+  for (int s = 1; __any_sync(act, s < cnt); s <<= 1) {
+    const bool take = (rank % (2 * s)) == 0 && rank + s < cnt;
+    const int src = take ? (int)__fns(peers, 0u, rank + s + 1) : (int)lane;
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+      const double t = __shfl_sync(act, v[c], src);
+      if (take) v[c] += t;
+    }
+  }
+  if (rank == 0) {
+#pragma unroll
+    for (int c = 0; c < N; ++c) atomicAdd(f + key + c * stride, v[c]);
+  }
+}
+
 // CloudDepositImplicitT (src/dust/dust_imex3d.cpp:61-99): Q = m c W / V, P = Q v
+template <int LF>
 __global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, double sh,
                                 int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2182,12 +2213,10 @@ __global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt
   const double mass_c = d.three_d ? P.r(DUSTB_IPM, p) * a_dt / (P.r(DUSTB_IPTS, p) + a_dt)
                                   : P.r(DUSTB_IPM, p) * (a_dt / (P.r(DUSTB_IPTS, p) + a_dt));
   const double vx = P.r(DUSTB_IPVX, p), vy = P.r(DUSTB_IPVY, p), vz = P.r(DUSTB_IPVZ, p);
-  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+  cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const double dw = mass_c * lf.w / cloud_measure(M, d, lf.b);
-    atomicAdd(&qdep[d.at(lf.b, 5, 0, lf.k, lf.j, lf.i)], dw);
-    atomicAdd(&qdep[d.at(lf.b, 5, 1, lf.k, lf.j, lf.i)], dw * vx);
-    atomicAdd(&qdep[d.at(lf.b, 5, 2, lf.k, lf.j, lf.i)], dw * vy);
-    atomicAdd(&qdep[d.at(lf.b, 5, 3, lf.k, lf.j, lf.i)], dw * vz);
+    double v[4] = {dw, dw * vx, dw * vy, dw * vz};
+    warp_add(qdep, d.at(lf.b, 5, 0, lf.k, lf.j, lf.i), d.cells(), v);
   }, err);
 }
 
@@ -2219,6 +2248,7 @@ __global__ void k_gather_pack(Ind d, const double *v, double *gp) {
 // dust_imex3d_gather.hpp and dust_leaf_api.hpp:196-219): ubar = sum w u* + cx du/dx + cy du/dy
 // + cz du/dz, cx = (m1x + MinImage(x - xc) w) / (2 dx); dv = c (ubar - v), v += dv,
 // R = dv / a_dt; with back-reaction -m w dv / V into dmom over the leaves of nonzero weight
+template <int LF>
 __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
                                     double a_dt, double sh, int br, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2228,7 +2258,7 @@ __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, dou
   double x[3];
   if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
   double ug[3];
-  cloud_gather(M, d, m, x, lev, L, x3phys, gp, ug, err);
+  cloud_gather<LF>(M, d, m, x, lev, L, x3phys, gp, ug, err);
   const double cj = a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
   const double dvx = cj * (ug[0] - P.r(DUSTB_IPVX, p));
   const double dvy = cj * (ug[1] - P.r(DUSTB_IPVY, p));
@@ -2237,16 +2267,16 @@ __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, dou
   P.r(DUSTB_IPRX, p) = dvx / a_dt; P.r(DUSTB_IPRY, p) = dvy / a_dt; P.r(DUSTB_IPRZ, p) = dvz / a_dt;
   if (!br) return;
   const double mass = -P.r(DUSTB_IPM, p);
-  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+  cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const double dw = mass * lf.w / cloud_measure(M, d, lf.b);
-    atomicAdd(&dmom[d.at(lf.b, 3, 0, lf.k, lf.j, lf.i)], dw * dvx);
-    atomicAdd(&dmom[d.at(lf.b, 3, 1, lf.k, lf.j, lf.i)], dw * dvy);
-    atomicAdd(&dmom[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * dvz);
+    double v[3] = {dw * dvx, dw * dvy, dw * dvz};
+    warp_add(dmom, d.at(lf.b, 3, 0, lf.k, lf.j, lf.i), d.cells(), v);
   }, nullptr);
 }
 
 // CloudOperatorKernelT (src/dust/dust_cloud_imex_kernels.hpp:20-70): the clouds' m c W ubar / V
 // with ubar their linear gather of the packed field, into result (the operator of dc1 / dc2)
+template <int LF>
 __global__ void k_cloud_operator(PCtx P, MCtx M, Ind d, const double *gp, double *result,
                                  double a_dt, double sh, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2256,13 +2286,12 @@ __global__ void k_cloud_operator(PCtx P, MCtx M, Ind d, const double *gp, double
   double x[3];
   if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
   double ug[3];
-  cloud_gather(M, d, m, x, lev, L, x3phys, gp, ug, err);
+  cloud_gather<LF>(M, d, m, x, lev, L, x3phys, gp, ug, err);
   const double mc = P.r(DUSTB_IPM, p) * (a_dt / (P.r(DUSTB_IPTS, p) + a_dt));
-  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+  cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const double dw = mc * lf.w / cloud_measure(M, d, lf.b);
-    atomicAdd(&result[d.at(lf.b, 3, 0, lf.k, lf.j, lf.i)], dw * ug[0]);
-    atomicAdd(&result[d.at(lf.b, 3, 1, lf.k, lf.j, lf.i)], dw * ug[1]);
-    atomicAdd(&result[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * ug[2]);
+    double v[3] = {dw * ug[0], dw * ug[1], dw * ug[2]};
+    warp_add(result, d.at(lf.b, 3, 0, lf.k, lf.j, lf.i), d.cells(), v);
   }, nullptr);
 }
 
@@ -2289,6 +2318,7 @@ __global__ void k_cloud_consistent_gas(Ind d, double *u0, int nv, const double *
 }
 
 // ... the clouds: v += c sum W r, R += c sum W r / a_dt with the deposit's weights
+template <int LF>
 __global__ void k_cloud_consistent_dust(PCtx P, MCtx M, Ind d, const double *res, double a_dt,
                                         double sh, int x3phys) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2299,7 +2329,7 @@ __global__ void k_cloud_consistent_dust(PCtx P, MCtx M, Ind d, const double *res
   double x[3];
   if (!cloud_load(P, M, d, p, sh, L, m, x, lev)) return;
   double rv[3] = {0.0, 0.0, 0.0};
-  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+  cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     for (int v = 0; v < 3; ++v) rv[v] += lf.w * res[d.at(lf.b, 4, v, lf.k, lf.j, lf.i)];
   }, nullptr);
   const double cj = a_dt / (P.r(DUSTB_IPTS, p) + a_dt);
@@ -2323,6 +2353,7 @@ __global__ void k_gas_velocity_all(Ind d, const double *u, int nv, double *uv) {
 }
 
 // CloudPredictorT: g = -dt (m / t_s) (ubar - v) into qdep 1-3, m / t_s into qdep 4 (rate_dep)
+template <int LF>
 __global__ void k_cloud_pc2_predictor(PCtx P, MCtx M, Ind d, const double *gp, double *qdep,
                                       double dt, int rate_dep, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2332,21 +2363,27 @@ __global__ void k_cloud_pc2_predictor(PCtx P, MCtx M, Ind d, const double *gp, d
   double x[3];
   if (!cloud_load(P, M, d, p, 0.0, L, m, x, lev)) { report(err, DUSTB_ERR_CLOUD); return; }
   double ug[3];
-  cloud_gather(M, d, m, x, lev, L, x3phys, gp, ug, err);
+  cloud_gather<LF>(M, d, m, x, lev, L, x3phys, gp, ug, err);
   const double mass_rate = P.r(DUSTB_IPM, p) / P.r(DUSTB_IPTS, p);
   const double gx = -dt * mass_rate * (ug[0] - P.r(DUSTB_IPVX, p));
   const double gy = -dt * mass_rate * (ug[1] - P.r(DUSTB_IPVY, p));
   const double gz = -dt * mass_rate * (ug[2] - P.r(DUSTB_IPVZ, p));
-  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+  cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const double inv_volume = 1.0 / cloud_measure(M, d, lf.b);
-    atomicAdd(&qdep[d.at(lf.b, 5, 1, lf.k, lf.j, lf.i)], inv_volume * lf.w * gx);
-    atomicAdd(&qdep[d.at(lf.b, 5, 2, lf.k, lf.j, lf.i)], inv_volume * lf.w * gy);
-    atomicAdd(&qdep[d.at(lf.b, 5, 3, lf.k, lf.j, lf.i)], inv_volume * lf.w * gz);
-    if (rate_dep) atomicAdd(&qdep[d.at(lf.b, 5, 4, lf.k, lf.j, lf.i)], inv_volume * lf.w * mass_rate);
+    const long long key = d.at(lf.b, 5, 1, lf.k, lf.j, lf.i);
+    if (rate_dep) {
+      double v[4] = {inv_volume * lf.w * gx, inv_volume * lf.w * gy, inv_volume * lf.w * gz,
+                     inv_volume * lf.w * mass_rate};
+      warp_add(qdep, key, d.cells(), v);
+    } else {
+      double v[3] = {inv_volume * lf.w * gx, inv_volume * lf.w * gy, inv_volume * lf.w * gz};
+      warp_add(qdep, key, d.cells(), v);
+    }
   }, nullptr);
 }
 
 // CloudAdvanceT with CloudPC2Push's Midpoint / Kick / Drift
+template <int LF>
 __global__ void k_cloud_pc2_advance(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
                                     double dt, int br, int sbox, int strat, double q, double om,
                                     double aphi, int x3phys, unsigned *err) {
@@ -2373,7 +2410,7 @@ __global__ void k_cloud_pc2_advance(PCtx P, MCtx M, Ind d, const double *gp, dou
   double x[3] = {xg[0], xg[1], xg[2]};
   if (!cloud_frame_ok(M, d, m, lev, L, x, 1.0)) { report(err, DUSTB_ERR_CLOUD); return; }
   double ug[3];
-  cloud_gather(M, d, m, x, lev, L, x3phys, gp, ug, err);
+  cloud_gather<LF>(M, d, m, x, lev, L, x3phys, gp, ug, err);
   const double h = 0.5 * dt;
   const double lambda = h / P.r(DUSTB_IPTS, p);
   const double aa = 1.0 + lambda;
@@ -2420,11 +2457,10 @@ __global__ void k_cloud_pc2_advance(PCtx P, MCtx M, Ind d, const double *gp, dou
   P.r(DUSTB_IPRX, p) = dvx; P.r(DUSTB_IPRY, p) = dvy; P.r(DUSTB_IPRZ, p) = dvz;
   if (!br) return;
   const double mass = -P.r(DUSTB_IPM, p);
-  cloud_leaves<false>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
+  cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const double dw = mass * lf.w / cloud_measure(M, d, lf.b);
-    atomicAdd(&dmom[d.at(lf.b, 3, 0, lf.k, lf.j, lf.i)], dw * dvx);
-    atomicAdd(&dmom[d.at(lf.b, 3, 1, lf.k, lf.j, lf.i)], dw * dvy);
-    atomicAdd(&dmom[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * dvz);
+    double v[3] = {dw * dvx, dw * dvy, dw * dvz};
+    warp_add(dmom, d.at(lf.b, 3, 0, lf.k, lf.j, lf.i), d.cells(), v);
   }, nullptr);
 }
 
@@ -2817,8 +2853,10 @@ int dustb_cloud_deposit_qp(const dustb_ctx *c, double a_dt, double sh, void *str
   if (!cloud_mesh_ok(c)) return DUSTB_EUNSUP;
   const Ind d = make_ind(c->mesh);
   cudaMemsetAsync(c->f.qdep, 0, (size_t)(n_all(d) * 5) * sizeof(double), S(stream));
-  if (c->part.npart > 0)
-    k_cloud_deposit<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, cloud_x3phys(c), c->err);
+  if (c->part.npart > 0) {
+    if (c->mesh.leaf) k_cloud_deposit<1><<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, cloud_x3phys(c), c->err);
+    else k_cloud_deposit<0><<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, cloud_x3phys(c), c->err);
+  }
   return launch_status("cloud_deposit_qp");
 }
 
@@ -2830,9 +2868,12 @@ int dustb_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, double *
   const Ind d = make_ind(c->mesh);
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
   cudaMemsetAsync(c->f.dmom, 0, (size_t)(n_all(d) * 3) * sizeof(double), S(stream));
-  if (c->part.npart > 0)
-    k_cloud_gather_kick<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, a_dt, sh,
+  if (c->part.npart > 0) {
+    if (c->mesh.leaf) k_cloud_gather_kick<1><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, a_dt, sh,
                                       c->phys.back_reaction, cloud_x3phys(c), c->err);
+    else k_cloud_gather_kick<0><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, a_dt, sh,
+                                      c->phys.back_reaction, cloud_x3phys(c), c->err);
+  }
   return launch_status("cloud_gather_kick");
 }
 
@@ -2846,9 +2887,12 @@ int dustb_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh, double *gp
   if (rc) return rc;
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
   cudaMemsetAsync(c->f.work, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
-  if (c->part.npart > 0)
-    k_cloud_operator<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.work, a_dt, sh,
+  if (c->part.npart > 0) {
+    if (c->mesh.leaf) k_cloud_operator<1><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.work, a_dt, sh,
                                    cloud_x3phys(c), c->err);
+    else k_cloud_operator<0><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.work, a_dt, sh,
+                                   cloud_x3phys(c), c->err);
+  }
   k_dc_correct<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas,
                                                                     c->f.qdep, c->f.work,
                                                                     c->f.ustar);
@@ -2864,9 +2908,12 @@ int dustb_cloud_apply_pmbr(const dustb_ctx *c, double a_dt, double sh, void *str
   cudaMemsetAsync(c->f.resid, 0, (size_t)n_all(d) * 4 * sizeof(double), S(stream));
   k_cloud_consistent_gas<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(
       d, c->f.u0, c->f.nvar_gas, c->f.ustar, c->f.qdep, c->f.dmom, c->f.resid, 1.0 / a_dt);
-  if (c->part.npart > 0)
-    k_cloud_consistent_dust<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, sh,
+  if (c->part.npart > 0) {
+    if (c->mesh.leaf) k_cloud_consistent_dust<1><<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, sh,
                                           cloud_x3phys(c));
+    else k_cloud_consistent_dust<0><<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, sh,
+                                          cloud_x3phys(c));
+  }
   return launch_status("cloud_apply_pmbr");
 }
 
@@ -2881,9 +2928,12 @@ int dustb_cloud_pc2_predictor(const dustb_ctx *c, double dt, int rate_dep, doubl
   k_gas_velocity_all<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.u1, c->f.nvar_gas,
                                                                         c->f.work);
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.work, gpack);
-  if (c->part.npart > 0)
-    k_cloud_pc2_predictor<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.qdep, dt, rate_dep,
+  if (c->part.npart > 0) {
+    if (c->mesh.leaf) k_cloud_pc2_predictor<1><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.qdep, dt, rate_dep,
                                         cloud_x3phys(c), c->err);
+    else k_cloud_pc2_predictor<0><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.qdep, dt, rate_dep,
+                                        cloud_x3phys(c), c->err);
+  }
   return launch_status("cloud_pc2_predictor");
 }
 
@@ -2895,10 +2945,14 @@ int dustb_cloud_pc2_advance(const dustb_ctx *c, double dt, double *gpack, void *
   const dustb_physics &ph = c->phys;
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
   cudaMemsetAsync(c->f.dmom, 0, (size_t)(n_all(d) * 3) * sizeof(double), S(stream));
-  if (c->part.npart > 0)
-    k_cloud_pc2_advance<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, dt,
+  if (c->part.npart > 0) {
+    if (c->mesh.leaf) k_cloud_pc2_advance<1><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, dt,
                                       ph.back_reaction, ph.shearing_box, ph.stratified,
                                       ph.qshear, ph.omega0, ph.const_accel_phi, cloud_x3phys(c), c->err);
+    else k_cloud_pc2_advance<0><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, dt,
+                                      ph.back_reaction, ph.shearing_box, ph.stratified,
+                                      ph.qshear, ph.omega0, ph.const_accel_phi, cloud_x3phys(c), c->err);
+  }
   return launch_status("cloud_pc2_advance");
 }
 

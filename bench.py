@@ -254,6 +254,12 @@ def run_ours(args, rep):
         if rank == 0:
             print(json.dumps(dict(out, note="refined-mesh workload only")), flush=True)
         return
+    if args.clouds_only:
+        out = measure_clouds(args)
+        if rank == 0:
+            print(json.dumps(dict(out, note="refinable-cloud workload only (profiling case)")),
+                  flush=True)
+        return
     if args.pc2_only:
         out = measure_pc2_strat(args, stream, lambda x: x, lambda: None)
         if rank == 0:
@@ -644,6 +650,12 @@ def measure_clouds(args):
     dev.t["pr"].copy_(pr0); dev.t["pi"].copy_(pi0); dev.t["u0"].copy_(u00)
     ms_point = timed(lambda: dev.imex_cycle(dt))
     err_point = dev.error_word()
+    # the same clouds through the leaf traversal of refined meshes (the mesh as one level)
+    from athenak_b200.amr import leaf_tables, uniform_leaf_spec
+    dev.t["pr"].copy_(pr0); dev.t["pi"].copy_(pi0); dev.t["u0"].copy_(u00)
+    dev.set_leaf_tables(leaf_tables(uniform_leaf_spec(ms)))
+    ms_leaf = timed(lambda: dev.cloud_imex_cycle(dt))
+    err_leaf = dev.error_word()
     out = {"workload": f"{cells[0]}^3 uniform mesh (config 4's root mesh, no refinement), "
                        f"{ms.nmb} MeshBlocks of 16^3, 2 species tau_s 0.1, 1, eps 0.5 each, "
                        f"8 level-0 P1 hat clouds per cell each, imex2+/dc1, overlap split, FP64",
@@ -651,8 +663,11 @@ def measure_clouds(args):
            "value": npart / (ms_cloud * 1e-3), "unit": UNIT, "ms_per_step": ms_cloud,
            "timed": "CUDA events around eager cycles after one warm-up cycle",
            "fp64_points_tsc": {"ms_per_step": ms_point, "value": npart / (ms_point * 1e-3)},
+           "leaf_traversal": {"ms_per_step": ms_leaf, "value": npart / (ms_leaf * 1e-3),
+                              "note": "the same clouds through the refined-mesh leaf traversal "
+                                      "(the mesh as one level of leaf tables)"},
            "momentum_change_rel": float(np.abs(p1 - p0).max() / sc),
-           "error_words": [err_cloud, err_point]}
+           "error_words": [err_cloud, err_point, err_leaf]}
     del dev, pr0, pi0, u00
     torch.cuda.empty_cache()
     return out
@@ -962,6 +977,8 @@ def main():
                     help="skip the refinable-cloud workload (128^3, 33.5 M clouds, FP64)")
     ap.add_argument("--no-seeded", action="store_true",
                     help="skip the FP64 form's timing in the seeded row order")
+    ap.add_argument("--clouds-only", action="store_true",
+                    help="time the uniform refinable-cloud workload only (profiling case)")
     ap.add_argument("--pc2-only", action="store_true",
                     help="time the stratified pc2 workload only (profiling case)")
     args = ap.parse_args()
