@@ -102,8 +102,10 @@ typedef struct dustb_mesh {
   double time;             /* mesh time of the cycle (the offset of every stage's remaps) */
   /* refined meshes (blocks of several levels, 3-D); both NULL on a single-level mesh.  With
    * them dustb_route hands particles to neighbours of any level, the deposits are exchanged by
-   * dustb_ghost_add_plan, and the entry points that assume one level (dustb_ghost_add,
-   * dustb_ghost_copy, the cycles, the mixed form) return DUSTB_EUNSUP. */
+   * dustb_ghost_add_plan, the gathered fields by dustb_ghost_copy_ml, the mixed form takes the
+   * plan and the coarse scratch in dustb_mixed_params, and the entry points that assume one
+   * level (dustb_ghost_add, dustb_ghost_copy, dustb_dc1_sweep, the single-level cycles) return
+   * DUSTB_EUNSUP. */
   const int *mb_lev;       /* nmb: level of each block (pmb->mb_lev) */
   const int *nghbr_ml;     /* nmb x 56: gid in every NeighborIndex slot of pmb->nghbr (four
                               sub-slots per face, two per edge, one per corner;
