@@ -77,12 +77,14 @@ def test_leaf_deposit_and_gather_kick_match_the_oracle(mode, x3bc):
 
 
 def test_split_and_instant_switch_match_the_oracle():
-    ms = _mesh(1)
-    st = refined_state(ms, [0.1, 1.0], [0.5, 1.0], 1, seed=12, vel_noise=0.2)
+    # 2^3 root blocks refined twice (levels 1 and 2), root clouds split pass by pass
+    ms = refined_mesh((2, 2, 2), (8, 8, 8), 2, refine=sphere_refine((0.1, 0.05, -0.02), (0.45, 0.2)),
+                      x3bc=1)
+    st = refined_state(ms, [0.1], [0.5], 1, seed=12, vel_noise=0.2)
     st.pi[3, :st.npart] = 0
     phys = dict(scheme=2)
     g, o = _pair(ms, st, phys)
-    sp = capi.split_params(max_level=2)
+    sp = capi.split_params(max_level=1)       # the split stops at level 1
     tag = st.npart
     for _ in range(4):
         n_g = g.cloud_split_p1(sp, tag)
@@ -107,22 +109,18 @@ def test_split_and_instant_switch_match_the_oracle():
 
 @pytest.mark.parametrize("solver", [0, 2])
 def test_refined_cloud_cycles_match_the_oracle(solver):
-    """Root clouds split down to the leaves (lobed transition clouds between levels), then two
-    imex2+ cycles of the clouds on the refined mesh in both forms."""
+    """Clouds at the level of their leaves, one split pass (lobed transition clouds where a
+    support meets finer leaves), then two imex2+ cycles of the clouds on the refined mesh in both
+    forms."""
     ms = _mesh()
     st = refined_state(ms, [0.02, 0.5], [1.0, 0.5], 1, seed=21, vel_noise=0.3, gas_noise=0.05,
                        vd=[0.5, -0.3])
-    st.pi[3, :st.npart] = 0
+    _codes(st, leaf_tables(ms), "block")
     phys = dict(scheme=2, drag_solver=solver, consistent_gas=True)
     g, o = _pair(ms, st, phys)
     sp = capi.split_params(max_level=2)
-    tag = st.npart
-    for _ in range(4):
-        n = g.cloud_split_p1(sp, tag)
-        assert o.cloud_split_p1(sp, tag) == n
-        tag += n
-        if n == 0:
-            break
+    n = g.cloud_split_p1(sp, st.npart)
+    assert o.cloud_split_p1(sp, st.npart) == n > 0
     dt = 0.2 * ms.mb_size[:, 6].min() / np.abs(st.pr[[1, 3, 5], :st.npart]).max()
     for _ in range(2):
         g.cloud_refined_imex_cycle(dt)

@@ -102,7 +102,7 @@ def test_host_layer_on_a_refined_mesh(clouds):
     lt = leaf_tables(ms)
     st = refined_state(ms, [0.02, 0.5], [1.0, 0.5], 1, seed=31, vel_noise=0.3, gas_noise=0.05,
                        vd=[0.5, -0.3])
-    st.pi[3, :st.npart] = 0
+    st.pi[3, :st.npart] = lt.arrays["blev"][st.pi[0, :st.npart]]   # clouds at their leaf's level
     phys = dict(scheme=2, drag_solver=2, consistent_gas=True)
     dt = 0.2 * ms.mb_size[:, 6].min() / np.abs(st.pr[[1, 3, 5], :st.npart]).max()
     ncyc = 2
