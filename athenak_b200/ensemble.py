@@ -73,9 +73,10 @@ class EnsemblePack:
     """The boxes of one side as one MeshBlock pack on the device, in the reference layout,
     advanced by the mixed-precision imex2+ cycle."""
 
-    def __init__(self, side, boxes, v0=0.1, device="cuda", detach=False):
+    def __init__(self, side, boxes, v0=0.1, device="cuda", detach=False, mixed=True):
         """detach: free the reference rows after the import (the cycles advance the shadow
-        alone; check() rebuilds the rows before its export)."""
+        alone; check() rebuilds the rows before its export).  mixed False: no mixed-precision
+        shadow (the FP64 form advances the reference rows)."""
         self.side, self.boxes, self.v0 = side, list(boxes), v0
         self.ms = box_ensemble_mesh(side, len(self.boxes))
         ncell = side ** 3
@@ -89,10 +90,12 @@ class EnsemblePack:
         u0[:, 0] = 1.0                               # gas at rest, density 1
         dx = 1.0 / side
         self.dt = 0.3 * dx / (1.0 + v0)
-        self.mx = MixedDust(dev=self.dev, do_import=False)
-        self.mx.import_()
-        if detach:
-            self.dev.detach_rows()
+        self.mx = None
+        if mixed:
+            self.mx = MixedDust(dev=self.dev, do_import=False)
+            self.mx.import_()
+            if detach:
+                self.dev.detach_rows()
         self.cycles = 0
         self.graph = None
 
@@ -224,6 +227,58 @@ def run_ensemble_one_launch(boxes, cycles, v0=0.1):
         checks += p.check()
         p.free()
     return ms, psteps, checks, len(packs)
+
+
+def run_ensemble_fp64(boxes, cycles=3, v0=0.1):
+    """The FP64 per-task form (dustb_imex_cycle on the reference rows, the comparator of the
+    mixed form) on the same boxes, every pack resident and one substep of the whole ensemble
+    as one CUDA-graph launch whose branches are the packs' cycles, as the mixed arm runs.
+    Returns the device time of cycles 2..cycles, the particle-cycles done in them and the
+    largest relative deviation of any box from its exact damping solution."""
+    by_side = {}
+    for b in boxes:
+        by_side.setdefault(b.side, []).append(b)
+    packs = [EnsemblePack(side, by_side[side], v0, mixed=False) for side in sorted(by_side)]
+    for p in packs:
+        p.dev.imex_cycle(p.dt, GAMMA_DEFAULT)
+    torch.cuda.synchronize()
+    streams = [torch.cuda.Stream() for _ in packs]
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        cap = torch.cuda.current_stream()
+        for p, st in zip(packs, streams):
+            st.wait_stream(cap)
+            p.dev.imex_cycle(p.dt, GAMMA_DEFAULT, stream=st)
+        for st in streams:
+            cap.wait_stream(st)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(cycles - 1):
+        g.replay()
+    t1.record()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    del g, streams
+    psteps = sum(p.npart for p in packs) * (cycles - 1)
+    worst = 0.0
+    for p in packs:
+        assert p.dev.error_word() == 0, "device error word set"
+        pr, pi = p.dev.t["pr"], p.dev.t["pi"]
+        key = pi[PGID].long() * 4 + pi[PSP].long()
+        f64 = dict(dtype=torch.float64, device=pr.device)
+        nb = len(p.boxes)
+        vs = torch.zeros(nb * 4, **f64).index_add_(0, key, pr[IPVX]).cpu().numpy()
+        cnt = torch.zeros(nb * 4, **f64).index_add_(0, key, torch.ones_like(pr[IPVX])).cpu().numpy()
+        t = cycles * p.dt
+        for k, b in enumerate(p.boxes):
+            ex = damping_solution(b.taus, b.eps, v0, t)
+            for s_ in range(len(b.taus)):
+                worst = max(worst, abs(vs[4 * k + s_] / cnt[4 * k + s_] - ex[1 + s_]) / v0)
+        del p.dev
+    torch.cuda.empty_cache()
+    return ms, psteps, worst
 
 
 def run_ensemble(boxes, cycles, v0=0.1, stream=None):

@@ -579,6 +579,23 @@ def measure_ensemble(args):
         timed = (f"cycles 2..{cycles} of every pack (CUDA-graph replays pack by pack; the "
                  f"resident ensemble did not fit), device time summed over packs")
     worst = max(ch, key=lambda c: c["err_vs_exact"])
+    # the FP64 per-task form on the same boxes, launched the same way (3 cycles: it is slow)
+    from athenak_b200.ensemble import run_ensemble_fp64
+    torch.cuda.empty_cache()
+    try:
+        ms64, ps64, err64 = run_ensemble_fp64(boxes, 3)
+        fp64 = {"device_ms": ms64, "value": ps64 / (ms64 * 1e-3), "cycles": 3,
+                "max_err_vs_exact_rel_v0": err64,
+                "timed": "cycles 2..3: one CUDA-graph launch per substep over all boxes, the "
+                         "packs' FP64 dustb_imex_cycle as parallel branches (rows in the "
+                         "lattice order they are built in)"}
+    except torch.cuda.OutOfMemoryError:
+        torch.cuda.empty_cache()
+        fp64 = {"unavailable": "the FP64 reference rows of every pack do not fit at once"}
+    except RuntimeError as e:          # (a failed capture of the FP64 cycles)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        fp64 = {"unavailable": f"the FP64 arm failed: {str(e)[:200]}"}
     return {"workload": f"{n} periodic dust_damping boxes, sides log-uniform {boxes and min(b.side for b in boxes)}.."
                         f"{max(b.side for b in boxes)} cells, 1-4 species, t_s 1e-3..10, eps 0.1..10, ppc 1..8, "
                         f"imex2+/dc1 TSC, one pack per side ({len(set(b.side for b in boxes))} packs)",
@@ -588,7 +605,8 @@ def measure_ensemble(args):
             "timed": timed,
             "max_err_vs_exact_rel_v0": max(c["err_vs_exact"] for c in ch),
             "max_momentum_change_rel": max(c["momentum_change"] for c in ch),
-            "worst_box": worst}
+            "worst_box": worst, "fp64": fp64,
+            "speedup_mixed_vs_fp64": (ps / (ms * 1e-3)) / fp64["value"] if "value" in fp64 else None}
 
 
 def measure_clouds(args):
