@@ -2171,35 +2171,6 @@ __device__ void cloud_gather(const MCtx &M, const Ind &d, int m, const double x[
   }, err);
 }
 
-// The clouds' deposits: f[key + c stride] += v[c] for c < N, where the lanes of a warp that add
-// to the same cell (the same key) combine first.  The lanes sharing a key (match_any) sum in a
-// binary tree over their ranks among those peers (round s: the peer of rank r, r a multiple of
-// 2s, takes the partial sum of the peer of rank r + s, the (r + s)-th set bit of the peer mask),
-// and the peer of rank 0 issues the N atomics: in cell order the clouds of a cell hit the same
-// leaves, so a warp issues about one atomic per distinct leaf instead of one per lane.
-template <int N>
-__device__ __forceinline__ void warp_add(double *f, long long key, long long stride,
-                                         double (&v)[N]) {
-  const unsigned act = __activemask();
-  const unsigned peers = __match_any_sync(act, key);
-  const unsigned lane = threadIdx.x & 31u;
-  const int rank = __popc(peers & ((1u << lane) - 1u));
-  const int cnt = __popc(peers);
-  for (int s = 1; __any_sync(act, s < cnt); s <<= 1) {
-    const bool take = (rank % (2 * s)) == 0 && rank + s < cnt;
-    const int src = take ? (int)__fns(peers, 0u, rank + s + 1) : (int)lane;
-#pragma unroll
-    for (int c = 0; c < N; ++c) {
-      const double t = __shfl_sync(act, v[c], src);
-      if (take) v[c] += t;
-    }
-  }
-  if (rank == 0) {
-#pragma unroll
-    for (int c = 0; c < N; ++c) atomicAdd(f + key + c * stride, v[c]);
-  }
-}
-
 // CloudDepositImplicitT (src/dust/dust_imex3d.cpp:61-99): Q = m c W / V, P = Q v
 template <int LF>
 __global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, double sh,
@@ -2215,8 +2186,10 @@ __global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt
   const double vx = P.r(DUSTB_IPVX, p), vy = P.r(DUSTB_IPVY, p), vz = P.r(DUSTB_IPVZ, p);
   cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const double dw = mass_c * lf.w / cloud_measure(M, d, lf.b);
-    double v[4] = {dw, dw * vx, dw * vy, dw * vz};
-    warp_add(qdep, d.at(lf.b, 5, 0, lf.k, lf.j, lf.i), d.cells(), v);
+    atomicAdd(&qdep[d.at(lf.b, 5, 0, lf.k, lf.j, lf.i)], dw);
+    atomicAdd(&qdep[d.at(lf.b, 5, 1, lf.k, lf.j, lf.i)], dw * vx);
+    atomicAdd(&qdep[d.at(lf.b, 5, 2, lf.k, lf.j, lf.i)], dw * vy);
+    atomicAdd(&qdep[d.at(lf.b, 5, 3, lf.k, lf.j, lf.i)], dw * vz);
   }, err);
 }
 
@@ -2269,8 +2242,9 @@ __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, dou
   const double mass = -P.r(DUSTB_IPM, p);
   cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const double dw = mass * lf.w / cloud_measure(M, d, lf.b);
-    double v[3] = {dw * dvx, dw * dvy, dw * dvz};
-    warp_add(dmom, d.at(lf.b, 3, 0, lf.k, lf.j, lf.i), d.cells(), v);
+    atomicAdd(&dmom[d.at(lf.b, 3, 0, lf.k, lf.j, lf.i)], dw * dvx);
+    atomicAdd(&dmom[d.at(lf.b, 3, 1, lf.k, lf.j, lf.i)], dw * dvy);
+    atomicAdd(&dmom[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * dvz);
   }, nullptr);
 }
 
@@ -2290,8 +2264,9 @@ __global__ void k_cloud_operator(PCtx P, MCtx M, Ind d, const double *gp, double
   const double mc = P.r(DUSTB_IPM, p) * (a_dt / (P.r(DUSTB_IPTS, p) + a_dt));
   cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const double dw = mc * lf.w / cloud_measure(M, d, lf.b);
-    double v[3] = {dw * ug[0], dw * ug[1], dw * ug[2]};
-    warp_add(result, d.at(lf.b, 3, 0, lf.k, lf.j, lf.i), d.cells(), v);
+    atomicAdd(&result[d.at(lf.b, 3, 0, lf.k, lf.j, lf.i)], dw * ug[0]);
+    atomicAdd(&result[d.at(lf.b, 3, 1, lf.k, lf.j, lf.i)], dw * ug[1]);
+    atomicAdd(&result[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * ug[2]);
   }, nullptr);
 }
 
@@ -2370,15 +2345,10 @@ __global__ void k_cloud_pc2_predictor(PCtx P, MCtx M, Ind d, const double *gp, d
   const double gz = -dt * mass_rate * (ug[2] - P.r(DUSTB_IPVZ, p));
   cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const double inv_volume = 1.0 / cloud_measure(M, d, lf.b);
-    const long long key = d.at(lf.b, 5, 1, lf.k, lf.j, lf.i);
-    if (rate_dep) {
-      double v[4] = {inv_volume * lf.w * gx, inv_volume * lf.w * gy, inv_volume * lf.w * gz,
-                     inv_volume * lf.w * mass_rate};
-      warp_add(qdep, key, d.cells(), v);
-    } else {
-      double v[3] = {inv_volume * lf.w * gx, inv_volume * lf.w * gy, inv_volume * lf.w * gz};
-      warp_add(qdep, key, d.cells(), v);
-    }
+    atomicAdd(&qdep[d.at(lf.b, 5, 1, lf.k, lf.j, lf.i)], inv_volume * lf.w * gx);
+    atomicAdd(&qdep[d.at(lf.b, 5, 2, lf.k, lf.j, lf.i)], inv_volume * lf.w * gy);
+    atomicAdd(&qdep[d.at(lf.b, 5, 3, lf.k, lf.j, lf.i)], inv_volume * lf.w * gz);
+    if (rate_dep) atomicAdd(&qdep[d.at(lf.b, 5, 4, lf.k, lf.j, lf.i)], inv_volume * lf.w * mass_rate);
   }, nullptr);
 }
 
@@ -2459,8 +2429,9 @@ __global__ void k_cloud_pc2_advance(PCtx P, MCtx M, Ind d, const double *gp, dou
   const double mass = -P.r(DUSTB_IPM, p);
   cloud_leaves<false, LF>(M, d, m, x, lev, L, x3phys, [&](const CloudLeaf &lf) {
     const double dw = mass * lf.w / cloud_measure(M, d, lf.b);
-    double v[3] = {dw * dvx, dw * dvy, dw * dvz};
-    warp_add(dmom, d.at(lf.b, 3, 0, lf.k, lf.j, lf.i), d.cells(), v);
+    atomicAdd(&dmom[d.at(lf.b, 3, 0, lf.k, lf.j, lf.i)], dw * dvx);
+    atomicAdd(&dmom[d.at(lf.b, 3, 1, lf.k, lf.j, lf.i)], dw * dvy);
+    atomicAdd(&dmom[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * dvz);
   }, nullptr);
 }
 
