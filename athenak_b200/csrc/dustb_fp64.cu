@@ -2171,9 +2171,14 @@ __device__ void cloud_gather(const MCtx &M, const Ind &d, int m, const double x[
   }, err);
 }
 
+// Every cloud kernel below is a body templated on the traversal form and two kernels: _u over
+// the uniform-mesh traversal (no launch bounds: the compiler keeps it near 120 registers and 16
+// warps per SM), _l over the leaf tables of refined meshes (held to 128 registers, 2 CTAs of 256
+// threads per SM: about 15 % faster than its unbounded 230 registers, which allow one CTA).
+
 // CloudDepositImplicitT (src/dust/dust_imex3d.cpp:61-99): Q = m c W / V, P = Q v
 template <int LF>
-__global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, double sh,
+__device__ __forceinline__ void k_cloud_deposit_body(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, double sh,
                                 int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
@@ -2192,6 +2197,10 @@ __global__ void k_cloud_deposit(PCtx P, MCtx M, Ind d, double *qdep, double a_dt
     atomicAdd(&qdep[d.at(lf.b, 5, 3, lf.k, lf.j, lf.i)], dw * vz);
   }, err);
 }
+__global__ void k_cloud_deposit_u(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, double sh,
+                                int x3phys, unsigned *err) { k_cloud_deposit_body<0>(P, M, d, qdep, a_dt, sh, x3phys, err); }
+__global__ void __launch_bounds__(kThreads, 2) k_cloud_deposit_l(PCtx P, MCtx M, Ind d, double *qdep, double a_dt, double sh,
+                                int x3phys, unsigned *err) { k_cloud_deposit_body<1>(P, M, d, qdep, a_dt, sh, x3phys, err); }
 
 // PackGatherField3D (src/dust/dust_cloud3d.cpp:1319-1340): the velocity and its central
 // differences, gp(m, k, j, i, 0..11), over the padded interior (the outer layer zero); 2-D
@@ -2222,7 +2231,7 @@ __global__ void k_gather_pack(Ind d, const double *v, double *gp) {
 // + cz du/dz, cx = (m1x + MinImage(x - xc) w) / (2 dx); dv = c (ubar - v), v += dv,
 // R = dv / a_dt; with back-reaction -m w dv / V into dmom over the leaves of nonzero weight
 template <int LF>
-__global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
+__device__ __forceinline__ void k_cloud_gather_kick_body(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
                                     double a_dt, double sh, int br, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
@@ -2247,11 +2256,15 @@ __global__ void k_cloud_gather_kick(PCtx P, MCtx M, Ind d, const double *gp, dou
     atomicAdd(&dmom[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * dvz);
   }, nullptr);
 }
+__global__ void k_cloud_gather_kick_u(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
+                                    double a_dt, double sh, int br, int x3phys, unsigned *err) { k_cloud_gather_kick_body<0>(P, M, d, gp, dmom, a_dt, sh, br, x3phys, err); }
+__global__ void __launch_bounds__(kThreads, 2) k_cloud_gather_kick_l(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
+                                    double a_dt, double sh, int br, int x3phys, unsigned *err) { k_cloud_gather_kick_body<1>(P, M, d, gp, dmom, a_dt, sh, br, x3phys, err); }
 
 // CloudOperatorKernelT (src/dust/dust_cloud_imex_kernels.hpp:20-70): the clouds' m c W ubar / V
 // with ubar their linear gather of the packed field, into result (the operator of dc1 / dc2)
 template <int LF>
-__global__ void k_cloud_operator(PCtx P, MCtx M, Ind d, const double *gp, double *result,
+__device__ __forceinline__ void k_cloud_operator_body(PCtx P, MCtx M, Ind d, const double *gp, double *result,
                                  double a_dt, double sh, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
@@ -2269,6 +2282,10 @@ __global__ void k_cloud_operator(PCtx P, MCtx M, Ind d, const double *gp, double
     atomicAdd(&result[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * ug[2]);
   }, nullptr);
 }
+__global__ void k_cloud_operator_u(PCtx P, MCtx M, Ind d, const double *gp, double *result,
+                                 double a_dt, double sh, int x3phys, unsigned *err) { k_cloud_operator_body<0>(P, M, d, gp, result, a_dt, sh, x3phys, err); }
+__global__ void __launch_bounds__(kThreads, 2) k_cloud_operator_l(PCtx P, MCtx M, Ind d, const double *gp, double *result,
+                                 double a_dt, double sh, int x3phys, unsigned *err) { k_cloud_operator_body<1>(P, M, d, gp, result, a_dt, sh, x3phys, err); }
 
 // CloudImplicitConsistencyOverlapT (src/dust/dust_imex3d.cpp:669-790), the cells: g = rho u* -
 // M, r = (D - g) / (rho + Q) (by the reciprocal), the gas takes g + rho r, dmom its rate, r
@@ -2294,7 +2311,7 @@ __global__ void k_cloud_consistent_gas(Ind d, double *u0, int nv, const double *
 
 // ... the clouds: v += c sum W r, R += c sum W r / a_dt with the deposit's weights
 template <int LF>
-__global__ void k_cloud_consistent_dust(PCtx P, MCtx M, Ind d, const double *res, double a_dt,
+__device__ __forceinline__ void k_cloud_consistent_dust_body(PCtx P, MCtx M, Ind d, const double *res, double a_dt,
                                         double sh, int x3phys) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
@@ -2313,6 +2330,10 @@ __global__ void k_cloud_consistent_dust(PCtx P, MCtx M, Ind d, const double *res
   P.r(DUSTB_IPRY, p) += cj * rv[1] / a_dt;
   P.r(DUSTB_IPRZ, p) += cj * rv[2] / a_dt;
 }
+__global__ void k_cloud_consistent_dust_u(PCtx P, MCtx M, Ind d, const double *res, double a_dt,
+                                        double sh, int x3phys) { k_cloud_consistent_dust_body<0>(P, M, d, res, a_dt, sh, x3phys); }
+__global__ void __launch_bounds__(kThreads, 2) k_cloud_consistent_dust_l(PCtx P, MCtx M, Ind d, const double *res, double a_dt,
+                                        double sh, int x3phys) { k_cloud_consistent_dust_body<1>(P, M, d, res, a_dt, sh, x3phys); }
 
 // ---- the clouds' pc2 (src/dust/dust_cloud3d.cpp:1362-1538, CloudPC2Push :76-150) ----------
 // PackGasGather3D: the gas velocity u1 momentum / density in every cell
@@ -2329,7 +2350,7 @@ __global__ void k_gas_velocity_all(Ind d, const double *u, int nv, double *uv) {
 
 // CloudPredictorT: g = -dt (m / t_s) (ubar - v) into qdep 1-3, m / t_s into qdep 4 (rate_dep)
 template <int LF>
-__global__ void k_cloud_pc2_predictor(PCtx P, MCtx M, Ind d, const double *gp, double *qdep,
+__device__ __forceinline__ void k_cloud_pc2_predictor_body(PCtx P, MCtx M, Ind d, const double *gp, double *qdep,
                                       double dt, int rate_dep, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.npart) return;
@@ -2351,10 +2372,14 @@ __global__ void k_cloud_pc2_predictor(PCtx P, MCtx M, Ind d, const double *gp, d
     if (rate_dep) atomicAdd(&qdep[d.at(lf.b, 5, 4, lf.k, lf.j, lf.i)], inv_volume * lf.w * mass_rate);
   }, nullptr);
 }
+__global__ void k_cloud_pc2_predictor_u(PCtx P, MCtx M, Ind d, const double *gp, double *qdep,
+                                      double dt, int rate_dep, int x3phys, unsigned *err) { k_cloud_pc2_predictor_body<0>(P, M, d, gp, qdep, dt, rate_dep, x3phys, err); }
+__global__ void __launch_bounds__(kThreads, 2) k_cloud_pc2_predictor_l(PCtx P, MCtx M, Ind d, const double *gp, double *qdep,
+                                      double dt, int rate_dep, int x3phys, unsigned *err) { k_cloud_pc2_predictor_body<1>(P, M, d, gp, qdep, dt, rate_dep, x3phys, err); }
 
 // CloudAdvanceT with CloudPC2Push's Midpoint / Kick / Drift
 template <int LF>
-__global__ void k_cloud_pc2_advance(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
+__device__ __forceinline__ void k_cloud_pc2_advance_body(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
                                     double dt, int br, int sbox, int strat, double q, double om,
                                     double aphi, int x3phys, unsigned *err) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2434,6 +2459,12 @@ __global__ void k_cloud_pc2_advance(PCtx P, MCtx M, Ind d, const double *gp, dou
     atomicAdd(&dmom[d.at(lf.b, 3, 2, lf.k, lf.j, lf.i)], dw * dvz);
   }, nullptr);
 }
+__global__ void k_cloud_pc2_advance_u(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
+                                    double dt, int br, int sbox, int strat, double q, double om,
+                                    double aphi, int x3phys, unsigned *err) { k_cloud_pc2_advance_body<0>(P, M, d, gp, dmom, dt, br, sbox, strat, q, om, aphi, x3phys, err); }
+__global__ void __launch_bounds__(kThreads, 2) k_cloud_pc2_advance_l(PCtx P, MCtx M, Ind d, const double *gp, double *dmom,
+                                    double dt, int br, int sbox, int strat, double q, double om,
+                                    double aphi, int x3phys, unsigned *err) { k_cloud_pc2_advance_body<1>(P, M, d, gp, dmom, dt, br, sbox, strat, q, om, aphi, x3phys, err); }
 
 long long n_active(const Ind &d) { return (long long)d.nmb * d.nx3 * d.nx2 * d.nx1; }
 long long n_all(const Ind &d) { return d.cells() * d.nmb; }
@@ -2825,8 +2856,8 @@ int dustb_cloud_deposit_qp(const dustb_ctx *c, double a_dt, double sh, void *str
   const Ind d = make_ind(c->mesh);
   cudaMemsetAsync(c->f.qdep, 0, (size_t)(n_all(d) * 5) * sizeof(double), S(stream));
   if (c->part.npart > 0) {
-    if (c->mesh.leaf) k_cloud_deposit<1><<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, cloud_x3phys(c), c->err);
-    else k_cloud_deposit<0><<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, cloud_x3phys(c), c->err);
+    if (c->mesh.leaf) k_cloud_deposit_l<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, cloud_x3phys(c), c->err);
+    else k_cloud_deposit_u<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.qdep, a_dt, sh, cloud_x3phys(c), c->err);
   }
   return launch_status("cloud_deposit_qp");
 }
@@ -2840,9 +2871,9 @@ int dustb_cloud_gather_kick(const dustb_ctx *c, double a_dt, double sh, double *
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
   cudaMemsetAsync(c->f.dmom, 0, (size_t)(n_all(d) * 3) * sizeof(double), S(stream));
   if (c->part.npart > 0) {
-    if (c->mesh.leaf) k_cloud_gather_kick<1><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, a_dt, sh,
+    if (c->mesh.leaf) k_cloud_gather_kick_l<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, a_dt, sh,
                                       c->phys.back_reaction, cloud_x3phys(c), c->err);
-    else k_cloud_gather_kick<0><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, a_dt, sh,
+    else k_cloud_gather_kick_u<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, a_dt, sh,
                                       c->phys.back_reaction, cloud_x3phys(c), c->err);
   }
   return launch_status("cloud_gather_kick");
@@ -2859,9 +2890,9 @@ int dustb_cloud_dc1_sweep(const dustb_ctx *c, double a_dt, double sh, double *gp
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
   cudaMemsetAsync(c->f.work, 0, (size_t)n_all(d) * 3 * sizeof(double), S(stream));
   if (c->part.npart > 0) {
-    if (c->mesh.leaf) k_cloud_operator<1><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.work, a_dt, sh,
+    if (c->mesh.leaf) k_cloud_operator_l<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.work, a_dt, sh,
                                    cloud_x3phys(c), c->err);
-    else k_cloud_operator<0><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.work, a_dt, sh,
+    else k_cloud_operator_u<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.work, a_dt, sh,
                                    cloud_x3phys(c), c->err);
   }
   k_dc_correct<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas,
@@ -2880,9 +2911,9 @@ int dustb_cloud_apply_pmbr(const dustb_ctx *c, double a_dt, double sh, void *str
   k_cloud_consistent_gas<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(
       d, c->f.u0, c->f.nvar_gas, c->f.ustar, c->f.qdep, c->f.dmom, c->f.resid, 1.0 / a_dt);
   if (c->part.npart > 0) {
-    if (c->mesh.leaf) k_cloud_consistent_dust<1><<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, sh,
+    if (c->mesh.leaf) k_cloud_consistent_dust_l<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, sh,
                                           cloud_x3phys(c));
-    else k_cloud_consistent_dust<0><<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, sh,
+    else k_cloud_consistent_dust_u<<<PGRID(c)>>>(pview(c), mview(c), d, c->f.resid, a_dt, sh,
                                           cloud_x3phys(c));
   }
   return launch_status("cloud_apply_pmbr");
@@ -2900,9 +2931,9 @@ int dustb_cloud_pc2_predictor(const dustb_ctx *c, double dt, int rate_dep, doubl
                                                                         c->f.work);
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.work, gpack);
   if (c->part.npart > 0) {
-    if (c->mesh.leaf) k_cloud_pc2_predictor<1><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.qdep, dt, rate_dep,
+    if (c->mesh.leaf) k_cloud_pc2_predictor_l<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.qdep, dt, rate_dep,
                                         cloud_x3phys(c), c->err);
-    else k_cloud_pc2_predictor<0><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.qdep, dt, rate_dep,
+    else k_cloud_pc2_predictor_u<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.qdep, dt, rate_dep,
                                         cloud_x3phys(c), c->err);
   }
   return launch_status("cloud_pc2_predictor");
@@ -2917,10 +2948,10 @@ int dustb_cloud_pc2_advance(const dustb_ctx *c, double dt, double *gpack, void *
   k_gather_pack<<<blocks_for(n_all(d)), kThreads, 0, S(stream)>>>(d, c->f.ustar, gpack);
   cudaMemsetAsync(c->f.dmom, 0, (size_t)(n_all(d) * 3) * sizeof(double), S(stream));
   if (c->part.npart > 0) {
-    if (c->mesh.leaf) k_cloud_pc2_advance<1><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, dt,
+    if (c->mesh.leaf) k_cloud_pc2_advance_l<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, dt,
                                       ph.back_reaction, ph.shearing_box, ph.stratified,
                                       ph.qshear, ph.omega0, ph.const_accel_phi, cloud_x3phys(c), c->err);
-    else k_cloud_pc2_advance<0><<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, dt,
+    else k_cloud_pc2_advance_u<<<PGRID(c)>>>(pview(c), mview(c), d, gpack, c->f.dmom, dt,
                                       ph.back_reaction, ph.shearing_box, ph.stratified,
                                       ph.qshear, ph.omega0, ph.const_accel_phi, cloud_x3phys(c), c->err);
   }
