@@ -127,20 +127,21 @@ struct Geo {
   double shR;                  // fmod(q Omega Lx t, Ly) in cells of y
   int ncell;                   // active cells; key ncell = the edge bin (pc2 half step)
   int W1, W2, W3;              // 3-D: the gather window's cells per row, rows, planes of a block
-  // refined meshes (ml = 1): every block's level (lev, by block, root_level first), the cell
-  // size and volume per level above the root, the 56 neighbour slots, the root blocks per
-  // direction; ml = 0 on a single-level mesh (one level: dx, vol)
+  // refined meshes (ml = 1): every block's level (lev, by block, root_level first), the 56
+  // neighbour slots, the root blocks per direction; dx and vol are the root level's, a block
+  // of level l above the root has cells of dx / 2^l and volume vol / 8^l (exact: powers of
+  // two; no per-level table, whose run-time index would make every thread copy this struct
+  // out of the kernel's parameters); ml = 0 on a single-level mesh
   int ml, root;
   const int *lev, *nml;
-  double dxl[kMaxLevels][3], voll[kMaxLevels];
   int nmbroot[3];
   __device__ int lv(int m) const {
     if (!ml) return 0;
     const int l = lev[m] - root;
     return l < 0 ? 0 : (l >= kMaxLevels ? kMaxLevels - 1 : l);
   }
-  __device__ double dxm(int m, int a) const { return ml ? dxl[lv(m)][a] : dx[a]; }
-  __device__ double volm(int m) const { return ml ? voll[lv(m)] : vol; }
+  __device__ double dxm(int m, int a) const { return ml ? ldexp(dx[a], -lv(m)) : dx[a]; }
+  __device__ double volm(int m) const { return ml ? ldexp(vol, -3 * lv(m)) : vol; }
   __device__ long long at(int m, int nvar, int v, int k, int j, int i) const {
     return (((long long)m * nvar + v) * vstride) + ((long long)k * n2 + j) * n1 + i;
   }
@@ -230,11 +231,6 @@ Geo make_geo(const dustb_ctx *c, const dustb_mixed_params *mp) {
   G.ml = (ms.nghbr_ml && ms.mb_lev) ? 1 : 0;
   G.root = mp->root_level;
   G.lev = ms.mb_lev; G.nml = ms.nghbr_ml;
-  for (int l = 0; l < kMaxLevels; ++l) {
-    const double s = 1.0 / (double)(1 << l);
-    for (int a = 0; a < 3; ++a) G.dxl[l][a] = mp->dx[a] * s;
-    G.voll[l] = G.dxl[l][0] * G.dxl[l][1] * (ms.three_d ? G.dxl[l][2] : 1.0);
-  }
   const double ext[3] = {ms.x1max - ms.x1min, ms.x2max - ms.x2min, ms.x3max - ms.x3min};
   const int nxs[3] = {d.nx1, d.nx2, d.nx3};
   for (int a = 0; a < 3; ++a) G.nmbroot[a] = (int)floor(ext[a] / (nxs[a] * mp->dx[a]) + 0.5);
@@ -482,8 +478,8 @@ struct PushArgs {
   int kind;
   float gam0, gam1, atw_dt;
   float bdt;                  // beta*dt (velocity kick)
-  float bdx[kMaxLevels][3];   // beta*dt/dx per level and axis (drift in cells; one level on a
-                              // single-level mesh); pc2 half step: h/dx
+  float bdx[3];               // beta*dt/dx per axis (drift in cells; on a refined mesh the root
+                              // level's, 2^l times it in a block of level l); pc2 half step: h/dx
   float gy;                   // pc2 half step: q Omega h / dy (the gather position's y shift
                               // per unit x of the half-step position)
   float sdy;                  // pc2 half step: q Omega dt / dy (the new y's shear drift)
@@ -716,7 +712,8 @@ __device__ __forceinline__ int advance_carry(const Geo &G, const PushArgs &P, in
   float on[3] = {o[0], o[1], o[2]}, dn[3] = {d1[0], d1[1], d1[2]};
   int c[3] = {0, 0, 0};
   for (int a = 0; a < nax; ++a) {
-    float s = __fmaf_rn(P.bdx[G.lv(m)][a], xdot[a], __fmul_rn(P.gam1, d1[a]));
+    const float bdx = G.ml ? ldexpf(P.bdx[a], G.lv(m)) : P.bdx[a];
+    float s = __fmaf_rn(bdx, xdot[a], __fmul_rn(P.gam1, d1[a]));
     // (the gather position's y: + q Omega x_h h, x_h the half-step x in this block's frame)
     if (KIND == PK_HALF && a == 1 && P.gy != 0.0f) s = __fmaf_rn(P.gy, hpos[0], s);
     on[a] = __fadd_rn(on[a], s);
@@ -790,8 +787,9 @@ __device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, 
 // count: the new cell of every particle and the per-cell histogram
 // SP: the mesh has physical x3 or shear-periodic x1 faces
 template <int KIND, int SP>
-__global__ void __launch_bounds__(kT) k_count(PBuf S, int *key_out, int *count, Geo G, int n,
-                                              PushArgs P) {
+__global__ void __launch_bounds__(kT) k_count(PBuf S, int *key_out, int *count,
+                                              const __grid_constant__ Geo G, int n,
+                                              const __grid_constant__ PushArgs P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = p < n;
   const unsigned act = __ballot_sync(0xffffffffu, live);
@@ -941,7 +939,8 @@ __device__ __forceinline__ void move_particle(const PBuf &S, const PBuf &D, cons
 
 template <int KIND, int SP>
 __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, int *cursor,
-                                             Geo G, int n, PushArgs P) {
+                                             const __grid_constant__ Geo G, int n,
+                                             const __grid_constant__ PushArgs P) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = p < n;
   const unsigned act = __ballot_sync(0xffffffffu, live);
@@ -2430,10 +2429,9 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
     P.gam0 = (float)gam0[stage - 1]; P.gam1 = (float)gam1[stage - 1];
     P.atw_dt = (stage == 2) ? (float)(atw22 * dt) : 0.0f;
     P.bdt = (float)(beta[stage - 1] * dt);
-    for (int l = 0; l < kMaxLevels; ++l)
-      for (int a = 0; a < 3; ++a) P.bdx[l][a] = (float)(beta[stage - 1] * dt / G.dxl[l][a]);
-    if (!G.ml)
-      for (int a = 0; a < 3; ++a) P.bdx[0][a] = (float)(beta[stage - 1] * dt * G.inv_dx[a]);
+    for (int a = 0; a < 3; ++a)
+      P.bdx[a] = G.ml ? (float)(beta[stage - 1] * dt / G.dx[a])
+                      : (float)(beta[stage - 1] * dt * G.inv_dx[a]);
     P.gy = 0.0f;
     P.shy = (float)(co->sh[stage - 1] * G.inv_dx[1]);
     P.a_dt = a_dt; P.stage2 = (stage == 2);
@@ -2588,7 +2586,7 @@ int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void
   PushArgs P{};
   P.kind = PK_HALF;
   P.gam0 = 1.0f; P.gam1 = 0.0f; P.atw_dt = 0.0f; P.bdt = 0.0f;
-  for (int a = 0; a < 3; ++a) P.bdx[0][a] = T.pc.hdx[a];
+  for (int a = 0; a < 3; ++a) P.bdx[a] = T.pc.hdx[a];
   P.gy = T.pc.gy;
   P.sdy = (float)(c->phys.qshear * c->phys.omega0 * dt * G.inv_dx[1]);
   P.a_dt = h; P.stage2 = 0;
@@ -2615,7 +2613,7 @@ int dustb_mixed_pc2_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, void
   // the move to the new position: B -> A sorted by cell (routing as SetNewPrtclGID)
   P.kind = PK_FULL;
   P.gam0 = 0.0f; P.gam1 = 1.0f;
-  for (int a = 0; a < 3; ++a) P.bdx[0][a] = 0.0f;
+  for (int a = 0; a < 3; ++a) P.bdx[a] = 0.0f;
   P.gy = 0.0f;
   RUN(push_sort(S, S.B, S.A, G, n, ncell, P, st));
   if (br) {
