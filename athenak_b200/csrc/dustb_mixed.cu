@@ -650,9 +650,22 @@ __device__ __forceinline__ Carry cross_face(const Geo &G, const PushArgs &P, int
 // of the mesh at m's level (the block's logical location times its cells plus the local
 // coordinate), scaled by 2 or 1/2 to the neighbour's level (exact in FP64), wrapped across
 // the periodic faces and taken relative to the neighbour's origin; the displacement scales the
-// same way.  Count and move take the same steps, so they agree bit for bit.
-__device__ __noinline__ int ml_carry(const Geo &G, const PushArgs &P, int &m, int &k, int &j,
-                                     int &i, int ni, int nj, int nk, float o[3], float d1[3]) {
+// same way.  Count and move take the same steps, so they agree bit for bit.  Values in and
+// out, no addresses: a caller's variable whose address reached this (not inlined) function
+// would live in local memory on every path of the push.
+struct MlCarry {
+  int m, k, j, i, key;
+  float o[3], d1[3];
+};
+__device__ __noinline__ MlCarry ml_carry(const Geo &G, const PushArgs &P, int m_in, int ni,
+                                         int nj, int nk, float o0, float o1, float o2,
+                                         float e0, float e1, float e2) {
+  MlCarry r;
+  int &m = r.m, &k = r.k, &j = r.j, &i = r.i;
+  float *o = r.o, *d1 = r.d1;
+  m = m_in;
+  o[0] = o0; o[1] = o1; o[2] = o2;
+  d1[0] = e0; d1[1] = e1; d1[2] = e2;
   const int nxs[3] = {G.nx1, G.nx2, G.nx3};
   const int nn[3] = {ni, nj, nk};
   int oc[3], f[3];
@@ -668,7 +681,8 @@ __device__ __noinline__ int ml_carry(const Geo &G, const PushArgs &P, int &m, in
     report(P.err, DUSTB_ERR_NGHBR);
     i = min(max(ni, 0), G.nx1 - 1); j = min(max(nj, 0), G.nx2 - 1); k = min(max(nk, 0), G.nx3 - 1);
     for (int a = 0; a < 3; ++a) o[a] = min(max(o[a], 0.0f), 0.99999994f);
-    return encode(G, m, k, j, i);
+    r.key = encode(G, m, k, j, i);
+    return r;
   }
   const int rel = G.lev[t] - G.lev[m];
   const double sc = (rel > 0) ? 2.0 : ((rel < 0) ? 0.5 : 1.0);
@@ -692,7 +706,8 @@ __device__ __noinline__ int ml_carry(const Geo &G, const PushArgs &P, int &m, in
     d1[a] = (float)((double)d1[a] * sc);
   }
   m = t; i = c[0]; j = c[1]; k = c[2];
-  return encode(G, m, k, j, i);
+  r.key = encode(G, m, k, j, i);
+  return r;
 }
 
 template <int KIND, int SP>
@@ -712,7 +727,7 @@ __device__ __forceinline__ int advance_carry(const Geo &G, const PushArgs &P, in
   float on[3] = {o[0], o[1], o[2]}, dn[3] = {d1[0], d1[1], d1[2]};
   int c[3] = {0, 0, 0};
   for (int a = 0; a < nax; ++a) {
-    const float bdx = G.ml ? ldexpf(P.bdx[a], G.lv(m)) : P.bdx[a];
+    const float bdx = (SP == 2) ? ldexpf(P.bdx[a], G.lv(m)) : P.bdx[a];
     float s = __fmaf_rn(bdx, xdot[a], __fmul_rn(P.gam1, d1[a]));
     // (the gather position's y: + q Omega x_h h, x_h the half-step x in this block's frame)
     if (KIND == PK_HALF && a == 1 && P.gy != 0.0f) s = __fmaf_rn(P.gy, hpos[0], s);
@@ -737,11 +752,13 @@ __device__ __forceinline__ int advance_carry(const Geo &G, const PushArgs &P, in
     for (int a = 0; a < 3; ++a) { o[a] = on[a]; d1[a] = dn[a]; }
     return encode(G, m, k, j, i);
   }
-  if (!SP && G.ml) {
-    for (int a = 0; a < 3; ++a) { o[a] = on[a]; d1[a] = dn[a]; }
-    return ml_carry(G, P, m, k, j, i, ni, nj, nk, o, d1);
+  if constexpr (SP == 2) {
+    const MlCarry r = ml_carry(G, P, m, ni, nj, nk, on[0], on[1], on[2], dn[0], dn[1], dn[2]);
+    m = r.m; k = r.k; j = r.j; i = r.i;
+    for (int a = 0; a < 3; ++a) { o[a] = r.o[a]; d1[a] = r.d1[a]; }
+    return r.key;
   }
-  if (!SP) {
+  if (SP == 0) {
     // a periodic mesh: the neighbour across the face (periodic images are neighbours)
     const int o1 = (ni < 0) ? -1 : ((ni >= G.nx1) ? 1 : 0);
     const int o2 = (nj < 0) ? -1 : ((nj >= G.nx2) ? 1 : 0);
@@ -785,7 +802,8 @@ __device__ __forceinline__ int advance(const Geo &G, const PushArgs &P, int &m, 
 }
 
 // count: the new cell of every particle and the per-cell histogram
-// SP: the mesh has physical x3 or shear-periodic x1 faces
+// SP: 0 a periodic single-level mesh, 1 physical x3 or shear-periodic x1 faces, 2 a refined
+// (periodic) mesh
 template <int KIND, int SP>
 __global__ void __launch_bounds__(kT) k_count(PBuf S, int *key_out, int *count,
                                               const __grid_constant__ Geo G, int n,
@@ -955,7 +973,7 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   if ((threadIdx.x & 31) == 0 && live) {
     int m, k, j, i;
     decode(G, S.cell[p], m, k, j, i);
-    const double vinv = 1.0 / G.volm(m);
+    const double vinv = 1.0 / ((SP == 2) ? G.volm(m) : G.vol);
     for (int a = 0; a < 3; ++a) {
       if (w[a] == 0.0) continue;
       const long long at = G.at(m, P.nvg, 1 + a, G.ks + k, G.js + j, G.is + i);
@@ -2199,7 +2217,11 @@ int push_sort(const MState &S, const PBuf &src, const PBuf &dst, const Geo &G, i
     if (n > 0) {
 #define DUSTB_COUNT(K, SPF) k_count<K, SPF><<<nblk(n), kT, 0, st>>>(src, S.key, S.cstart, G, n, P)
       // (physical x3 or shear faces; a refined mesh carries its crossings in the periodic form)
-      if (G.ghost && !G.ml) {
+      if (G.ml) {
+        if (P.kind == PK_HALF) DUSTB_COUNT(PK_HALF, 2);
+        else if (P.kind == PK_FULL) DUSTB_COUNT(PK_FULL, 2);
+        else DUSTB_COUNT(PK_IMEX, 2);
+      } else if (G.ghost) {
         if (P.kind == PK_HALF) DUSTB_COUNT(PK_HALF, 1);
         else if (P.kind == PK_FULL) DUSTB_COUNT(PK_FULL, 1);
         else DUSTB_COUNT(PK_IMEX, 1);
@@ -2220,7 +2242,11 @@ int push_sort(const MState &S, const PBuf &src, const PBuf &dst, const Geo &G, i
   Scope sc(DUSTB_K_MOVE, st);
   if (n > 0) {
 #define DUSTB_MOVE(K, SPF) k_move<K, SPF><<<nblk(n), kT, 0, st>>>(src, dst, S.key, S.cursor, G, n, P)
-    if (G.ghost && !G.ml) {
+    if (G.ml) {
+      if (P.kind == PK_HALF) DUSTB_MOVE(PK_HALF, 2);
+      else if (P.kind == PK_FULL) DUSTB_MOVE(PK_FULL, 2);
+      else DUSTB_MOVE(PK_IMEX, 2);
+    } else if (G.ghost) {
       if (P.kind == PK_HALF) DUSTB_MOVE(PK_HALF, 1);
       else if (P.kind == PK_FULL) DUSTB_MOVE(PK_FULL, 1);
       else DUSTB_MOVE(PK_IMEX, 1);
