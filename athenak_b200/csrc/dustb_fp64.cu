@@ -1786,31 +1786,74 @@ __device__ void leaf_foreach(const MCtx &M, const Ind &d, int m, const double x[
         }
       }
     };
-    if (inside) {
-      visit(m, 0, 0, 0);
-      continue;
+    // Candidates (:319-366): the support's finest-cell box (not needed when it lies inside m)
+    bool global = false;
+    int box[6] = {0, 0, 0, 0, 0, 0};
+    if (!inside) {
+      box[0] = (int)floor((s1.lo - M.x1min) / T.fdx[0]);
+      box[1] = (int)ceil((s1.hi - M.x1min) / T.fdx[0]) - 1;
+      box[2] = (int)floor((s2.lo - M.x2min) / T.fdx[1]);
+      box[3] = (int)ceil((s2.hi - M.x2min) / T.fdx[1]) - 1;
+      box[4] = (int)floor((s3.lo - M.x3min) / T.fdx[2]);
+      box[5] = (int)ceil((s3.hi - M.x3min) / T.fdx[2]) - 1;
+      clip_z(T, box[4], box[5]);
+      global = leaf_need_global(T, m, box[0], box[1], box[2], box[3], box[4], box[5], 0);
     }
-    // Candidates (:319-366): the support's finest-cell box
-    const int ia = (int)floor((s1.lo - M.x1min) / T.fdx[0]);
-    const int ib = (int)ceil((s1.hi - M.x1min) / T.fdx[0]) - 1;
-    const int ja = (int)floor((s2.lo - M.x2min) / T.fdx[1]);
-    const int jb = (int)ceil((s2.hi - M.x2min) / T.fdx[1]) - 1;
-    int ka = (int)floor((s3.lo - M.x3min) / T.fdx[2]);
-    int kb = (int)ceil((s3.hi - M.x3min) / T.fdx[2]) - 1;
-    clip_z(T, ka, kb);
-    auto meets = [&](int b, int sx, int sy, int sz) {
-      const double bx0 = M.s(b, X1MIN) - sx * Lx, by0 = M.s(b, X2MIN) - sy * Ly;
-      const double bz0 = M.s(b, X3MIN) - sz * Lz;
-      return !(s1.hi <= bx0 || s1.lo >= bx0 + d.nx1 * M.s(b, DX1) || s2.hi <= by0 ||
-               s2.lo >= by0 + d.nx2 * M.s(b, DX2) || s3.hi <= bz0 ||
-               s3.lo >= bz0 + d.nx3 * M.s(b, DX3));
-    };
-    const bool global = leaf_need_global(T, m, ia, ib, ja, jb, ka, kb, 0);
-    for_candidates(T, m, global, ia - 1, ib + 1, ja - 1, jb + 1, ka - 1, kb + 1, 0,
-                   [&](int b, int sx, int sy, int sz) {
-      if (meets(b, sx, sy, sz)) visit(b, sx, sy, sz);
-      return true;
-    });
+    // one loop over the candidates in ForCandidates' order with a single visit: m alone when
+    // inside; m then its neighbours (local); every block and its periodic images meeting the box
+    // widened by one finest cell (global); each taken only when its box meets the support.
+    // (One call site keeps the kernel's code small: two made it stall on instruction fetch.)
+    const int nloc = inside ? 0 : T.nnb[m];
+    int c = global ? 0 : -1;                       // local: -1 is m; global: the next block
+    int cur = 0, img = 0, nimg = 0, kx0 = 0, nx = 1, ky0 = 0, ny = 1, kz0 = 0;
+#pragma unroll 1
+    while (true) {
+      int b, sx, sy, sz;
+      if (!global) {
+        if (c >= nloc) break;
+        if (c < 0) {
+          b = m; sx = sy = sz = 0;
+        } else {
+          const int *sh = T.nbs + ((long long)m * DUSTB_LEAF_MAXNB + c) * 3;
+          b = T.nb[(long long)m * DUSTB_LEAF_MAXNB + c]; sx = sh[0]; sy = sh[1]; sz = sh[2];
+        }
+        ++c;
+      } else {
+        if (img >= nimg) {
+          if (c >= T.nmb) break;
+          const int *fb = T.fbox + 6 * (long long)c;
+          int kx1, ky1, kz1, kz0_;
+          image_range(fb[0], fb[1], 0, T.nf[0], box[0] - 1, box[1] + 1, kx0, kx1);
+          image_range(fb[2], fb[3], 0, T.nf[1], box[2] - 1, box[3] + 1, ky0, ky1);
+          image_range(fb[4], fb[5], 0, T.nf[2], box[4] - 1, box[5] + 1, kz0_, kz1);
+          kz0 = kz0_;
+          if (!T.x3per) {
+            if (kz0 > 0 || kz1 < 0) { kz0 = 0; kz1 = -1; } else { kz0 = 0; kz1 = 0; }
+          }
+          nx = kx1 - kx0 + 1; ny = ky1 - ky0 + 1;
+          const int nz = kz1 - kz0 + 1;
+          nimg = (nx > 0 && ny > 0 && nz > 0) ? nx * ny * nz : 0;
+          img = 0;
+          cur = c++;
+          continue;
+        }
+        // images in the order kz, ky, kx (kx fastest)
+        b = cur;
+        sx = -(kx0 + img % nx);
+        sy = -(ky0 + (img / nx) % ny);
+        sz = -(kz0 + img / (nx * ny));
+        ++img;
+      }
+      bool take = inside;
+      if (!take) {
+        const double bx0 = M.s(b, X1MIN) - sx * Lx, by0 = M.s(b, X2MIN) - sy * Ly;
+        const double bz0 = M.s(b, X3MIN) - sz * Lz;
+        take = !(s1.hi <= bx0 || s1.lo >= bx0 + d.nx1 * M.s(b, DX1) || s2.hi <= by0 ||
+                 s2.lo >= by0 + d.nx2 * M.s(b, DX2) || s3.hi <= bz0 ||
+                 s3.lo >= bz0 + d.nx3 * M.s(b, DX3));
+      }
+      if (take) visit(b, sx, sy, sz);
+    }
   }
 }
 
