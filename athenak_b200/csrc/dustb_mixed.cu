@@ -32,7 +32,11 @@
 #include <cfloat>
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 #include <vector>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include "dustb_common.cuh"
 #include "dustb_sort.cuh"
@@ -320,6 +324,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
 __device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
                ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// one box of a 4-D tensor (the tensor map) into shared memory at dst (128-byte aligned); the
+// innermost coordinate c0 is 0 (the box starts on a 16-byte boundary); no multicast
+__device__ __forceinline__ void tensor_copy_4d(void *dst, const CUtensorMap *map, int c0, int c1,
+                                               int c2, int c3, uint64_t *bar) {
+  asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+               " [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
+               ::"r"(smem_u32(dst)), "l"((unsigned long long)map), "r"(c0), "r"(c1), "r"(c2),
+                 "r"(c3), "r"(smem_u32(bar)) : "memory");
 }
 // orders this thread's earlier ordinary shared-memory accesses before later bulk copies
 __device__ __forceinline__ void fence_proxy_async() {
@@ -1171,6 +1184,21 @@ struct GatherWindow {
           z[c][b][a] = v.z;
         }
   }
+  // 3-D, the window staged in shared memory (sw: the tile's rows plus one layer around them,
+  // three planes, W1 cells per row); consecutive threads read consecutive 16-byte cells
+  __device__ __forceinline__ void load4s(const float4 *sw, int W1, int rows, int cj, int ci) {
+    const float4 *p = sw + cj * W1 + ci;
+#pragma unroll
+    for (int c = 0; c < WK; ++c)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float4 v = p[(c * rows + b) * W1 + a];
+          xy[c][b][a] = make_float2(v.x, v.y);
+          z[c][b][a] = v.z;
+        }
+  }
   // u = sum over c of wz_c (sum over b of wy_b (sum over a of wx_a g_cba)): the three
   // directions one after the other, so the dependent chains are three FMAs long and the
   // planes' partial sums are independent of one another
@@ -1404,6 +1432,21 @@ __host__ __device__ inline size_t tile_head_bytes(int nct) {
   return (((size_t)(2 * nct + 2) * 4 + (size_t)nct * 8 + 15) & ~(size_t)15);
 }
 
+// shared memory of a tile: the head, then the larger of the pass rows and the staged sums
+// (27 float4 per slot in 3-D, 9 in 2-D)
+__host__ __device__ inline size_t tile_smem(int three_d, int tj, int nx1, int chunk) {
+  const int nct = tj * nx1;
+  const size_t rows = (size_t)kTileRows * chunk * 4;
+  const size_t sums = (size_t)(three_d ? 27 : 9) * nct * 16;
+  return tile_head_bytes(nct) + (rows > sums ? rows : sums);
+}
+// the staged window of a 3-D tile: its tj rows plus one row on each side, three planes, nx1 + 2
+// cells of 16 bytes per row (after the rest, on a 128-byte boundary)
+__host__ __device__ inline size_t tile_window_bytes(int tj, int nx1) {
+  return (size_t)3 * (tj + 2) * (nx1 + 2) * 16;
+}
+
+
 
 // One CTA per tile of tj rows of one plane.  The tile's particles (one contiguous range of
 // the sorted shadow) are cut into passes of at most chunk - 8, bulk-copied into shared
@@ -1419,7 +1462,8 @@ __host__ __device__ inline size_t tile_head_bytes(int nct) {
 // together.
 // (at most 168 registers: three CTAs of 128 threads per SM)
 template <int MODE, int D3, int SCHEME, int GH>
-__global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
+__global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T,
+                                        const __grid_constant__ CUtensorMap wmap) {
   // fields copied: ox oy oz cc m [vx vy vz] (the predictor: t_s in place of cc)
   constexpr int NF = (MODE == MODE_OP) ? 5 : 8;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1436,20 +1480,30 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
   double *s_qt = (double *)(s_ss + (nct + 1));     // [nct] centre mass (Q/P), FP64
   float *s_f = (float *)(smem + tile_head_bytes(nct));   // [8][CH]
   float4 *s_acc = (float4 *)s_f;                   // the staged sums, after the rows
+  // (GH bit 2, the gathering tiles of a 3-D mesh) the tile's gather window staged by a tensor
+  // copy, after the rest on a 128-byte boundary
+  constexpr bool kWin = D3 && MODE != MODE_QP && (GH & 4);
+  float4 *s_win = (float4 *)(((uintptr_t)(smem + tile_smem(D3, tj, nx1, CH)) + 127) &
+                             ~(uintptr_t)127);
   const int tid = threadIdx.x;
   const int lane = tid & 31, wid = tid >> 5;
   const unsigned wmask = (nct - (wid << 5)) >= 32 ? 0xffffffffu : ((1u << (nct - (wid << 5))) - 1u);
   const int nwarp = (nct + 31) >> 5;
 
-  // the particle range [cb, ce) of a pass, field by field, rounded out to 16-byte groups
-  auto issue_pass = [&](int cb, int ce) {
+  // the particle range [cb, ce) of a pass, field by field, rounded out to 16-byte groups; with
+  // wz >= 0 (the first pass of a tile, kWin) also the tile's window: rows wj .. wj + tj + 1,
+  // planes wz .. wz + 2 of the window tensor
+  auto issue_pass = [&](int cb, int ce, int wj, int wz) {
     const int a0 = cb & ~3, a1 = (ce + 3) & ~3;
     const unsigned bytes = (unsigned)(a1 - a0) * 4u;
     const int fl[8] = {F_OX, F_OY, F_OZ, (MODE == MODE_PRED) ? F_TS : F_CC, F_M, F_VX, F_VY, F_VZ};
+    const unsigned wbytes = (kWin && wz >= 0) ? (unsigned)tile_window_bytes(tj, nx1) : 0u;
     fence_proxy_async();
-    mbar_arrive_tx(&bar, bytes * NF);
+    mbar_arrive_tx(&bar, bytes * NF + wbytes);
 #pragma unroll
     for (int f = 0; f < NF; ++f) bulk_copy(s_f + f * CH, S.f[fl[f]] + a0, bytes, &bar);
+    if constexpr (kWin)
+      if (wbytes) tensor_copy_4d(s_win, &wmap, 0, 0, wj, wz, &bar);
   };
   __shared__ int s_item;
   if (tid == 0) mbar_init(&bar, 1);
@@ -1480,7 +1534,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       // (the failure-detection hook: the first tile of CTA 0 never issues its first copy, its
       // wait runs out)
       if (p1 > p0 && !(T.probe_timeout && blockIdx.x == 0 && item == 0))
-        issue_pass(p0, min(p1, p0 + (CH - 8)));
+        issue_pass(p0, min(p1, p0 + (CH - 8)), j0, kWin ? m * G.W3 + k : -1);
     }
     __syncwarp(wmask);
     for (int x = tid; x <= nct; x += blockDim.x) s_cs[x] = T.cstart[c0 + x];
@@ -1495,7 +1549,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
     for (int cb = P0; cb < P1; cb += CHP) {
       const int ce = min(P1, cb + CHP), cnt = ce - cb;
       const int a0 = cb & ~3, sh = cb - a0;
-      if (tid == 0 && cb != P0) issue_pass(cb, ce);
+      if (tid == 0 && cb != P0) issue_pass(cb, ce, 0, -1);
       // (the warp reconverges before the barriers of the slot map: thread 0 must not arrive
       // at them apart from its warp)
       __syncwarp(wmask);
@@ -1552,8 +1606,11 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
       };
       GatherWindow<D3> win;
       if constexpr (MODE != MODE_QP) {                 // (the loads fly with the copies)
-        if constexpr (D3) win.load4(G, T.win4, m, k, jrow, ci_l);
-        else win.template load<GH>(G, T.gfield, m, k, jrow, ci_l);
+        if constexpr (D3) {
+          if constexpr (!kWin) win.load4(G, T.win4, m, k, jrow, ci_l);
+        } else {
+          win.template load<GH>(G, T.gfield, m, k, jrow, ci_l);
+        }
       }
       const bool ok = mbar_wait(&bar, parity, T.err, wmask);
       parity ^= 1u;
@@ -1562,6 +1619,8 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T) {
         mbar_wait(&bar, parity ^ 1u, T.err, wmask);
         return;
       }
+      // (kWin: the staged window, complete with the first pass's copies)
+      if constexpr (kWin) win.load4s(s_win, G.W1, tj + 2, cj_l, ci_l);
       if (MODE == MODE_QP) {
         CellSums<MODE, D3> qp;
         qp.zero();
@@ -1803,15 +1862,6 @@ __global__ void __launch_bounds__(1024) k_tile_order(const int *cstart, Geo G, i
   for (int t = threadIdx.x; t < ntiles; t += blockDim.x) order[atomicAdd(&base[bucket(t)], 1)] = t;
 }
 
-// shared memory of a tile: the head, then the larger of the pass rows and the staged sums
-// (27 float4 per slot in 3-D, 9 in 2-D)
-size_t tile_smem(int three_d, int tj, int nx1, int chunk) {
-  const int nct = tj * nx1;
-  const size_t rows = (size_t)kTileRows * chunk * 4;
-  const size_t sums = (size_t)(three_d ? 27 : 9) * nct * 16;
-  return tile_head_bytes(nct) + (rows > sums ? rows : sums);
-}
-
 // m/rho of a gas field on every cell, ghosts included: the predictor's gather field
 __global__ void k_gas_velocity(const double *u, int nv, double *out, long long per,
                                long long total) {
@@ -2000,27 +2050,32 @@ struct Cfg {
   int tj, chunk, tpp;
   int probe_timeout;
   int grid;                      // 1: one CTA per tile; 0: persistent CTAs on the work queue
+  int wtma;                      // 3-D: the gathering tiles stage their window by a tensor copy
 };
 
 // the default particles per pass: the largest multiple of 4 that lets as many CTAs share an
 // SM as their registers allow (about 168 per thread), so that a typical tile's particles
 // fit one pass (a second pass costs a second window flush)
-int default_chunk(int tj, int nx1) {
+// (extra: shared memory a CTA needs beyond the head and the rows: the staged window)
+int default_chunk(int tj, int nx1, long long extra = 0) {
   const int nct = tj * nx1;
   int ctas = 65536 / (168 * nct);
   ctas = ctas < 1 ? 1 : (ctas > 8 ? 8 : ctas);
   const long long per = 233472 / ctas - 2560 - 64;     // less a reserve and the statics
-  long long ch = (per - (long long)tile_head_bytes(nct)) / (kTileRows * 4);
+  long long ch = (per - (long long)tile_head_bytes(nct) - extra) / (kTileRows * 4);
   ch &= ~3LL;
   return (int)(ch < 64 ? 64 : (ch > 8192 ? 8192 : ch));
 }
 
 bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   const int nx1 = ms.nx1, nx2 = ms.multi_d ? ms.nx2 : 1;
-  const int base = mp->variant & ~(DUSTB_MIXED_GRID_TILES | DUSTB_MIXED_NO_LEDGER);
+  const int base = mp->variant & ~(DUSTB_MIXED_GRID_TILES | DUSTB_MIXED_NO_LEDGER |
+                                   DUSTB_MIXED_WINDOW_TMA);
   if ((base != 0 && base != DUSTB_MIXED_PROBE_COPY_TIMEOUT) || nx1 > kMaxTileThreads)
     return false;
   cf.grid = (mp->variant & DUSTB_MIXED_GRID_TILES) ? 1 : 0;
+  // (a box row of the window tensor holds at most 256 cells)
+  cf.wtma = ((mp->variant & DUSTB_MIXED_WINDOW_TMA) && ms.three_d && nx1 + 2 <= 256) ? 1 : 0;
   int tj = mp->rows_per_tile;
   if (tj <= 0) {
     tj = 1;
@@ -2029,19 +2084,60 @@ bool pick_cfg(const dustb_mesh &ms, const dustb_mixed_params *mp, Cfg &cf) {
   }
   if (nx2 % tj != 0 || tj * nx1 > kMaxTileThreads) return false;
   cf.tj = tj;
-  cf.chunk = mp->chunk > 0 ? mp->chunk : default_chunk(tj, nx1);
+  cf.chunk = mp->chunk > 0 ? mp->chunk
+                           : default_chunk(tj, nx1, cf.wtma ? 128 + (long long)tile_window_bytes(tj, nx1) : 0);
   if (cf.chunk < 64 || cf.chunk > 8192 || (cf.chunk & 3)) return false;
   cf.tpp = nx2 / tj;
   cf.probe_timeout = (base == DUSTB_MIXED_PROBE_COPY_TIMEOUT);
   // every tile form must fit the 227 KiB of shared memory a CTA can have (less the barrier)
-  if (tile_smem(ms.three_d, tj, nx1, cf.chunk) > 227 * 1024 - 256) return false;
+  const size_t extra = cf.wtma ? 128 + tile_window_bytes(tj, nx1) : 0;
+  if (tile_smem(ms.three_d, tj, nx1, cf.chunk) + extra > 227 * 1024 - 256) return false;
   return true;
 }
 
+// the tensor map of the gather window (float4 cells, W1 x W2 x W3 per block): 4-D as (the four
+// floats of a cell, x, y, z over all blocks), a box of one tile's window (all W1 cells of tj + 2
+// rows in 3 planes); false when the driver's encoder is not available or refuses the map
+bool window_map(const Geo &G, const float4 *win, int tj, CUtensorMap &map) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  }
+  if (!win || ((uintptr_t)win & 15) || G.W1 > 256 || tj + 2 > 256) return false;
+  const cuuint64_t dims[4] = {4, (cuuint64_t)G.W1, (cuuint64_t)G.W2,
+                              (cuuint64_t)G.W3 * (cuuint64_t)G.nmb};
+  const cuuint64_t strides[3] = {16, 16ull * G.W1, 16ull * G.W1 * G.W2};
+  const cuuint32_t box[4] = {4, (cuuint32_t)G.W1, (cuuint32_t)(tj + 2), 3};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)win, dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+// GH bit 2: the form that stages the window (wm its tensor map), chosen here when the
+// configuration asks for it and the map can be made
 template <int MODE, int D3, int SCHEME, int GH>
-int launch_tile_d(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &T, cudaStream_t st) {
+int launch_tile_d(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &T, cudaStream_t st,
+                  const CUtensorMap *wm = nullptr) {
+  if constexpr (D3 && MODE != MODE_QP && !(GH & 4)) {
+    if (cf.wtma) {
+      CUtensorMap m4;
+      if (window_map(G, T.win4, cf.tj, m4))
+        return launch_tile_d<MODE, D3, SCHEME, GH | 4>(G, cf, cur, T, st, &m4);
+    }
+  }
+  CUtensorMap wmap;
+  std::memset(&wmap, 0, sizeof(wmap));
+  if (wm) wmap = *wm;
   const long long tiles = (long long)G.nmb * G.nx3 * cf.tpp;
-  const size_t sm = tile_smem(D3, cf.tj, G.nx1, cf.chunk);
+  const size_t sm = tile_smem(D3, cf.tj, G.nx1, cf.chunk) +
+                    ((GH & 4) ? 128 + tile_window_bytes(cf.tj, G.nx1) : 0);
   const int threads = cf.tj * G.nx1;
   static size_t configured = 0;
   // the CTAs of this kernel one SM holds at this shared-memory size and block (for the
@@ -2064,7 +2160,7 @@ int launch_tile_d(const Geo &G, const Cfg &cf, const PBuf &cur, const TileArgs &
     const long long resident = (long long)(occ > 0 ? occ : 1) * (nsm > 0 ? nsm : 1);
     grid = tiles < resident ? tiles : resident;
   }
-  k_tile<MODE, D3, SCHEME, GH><<<(unsigned)grid, threads, sm, st>>>(cur, G, T);
+  k_tile<MODE, D3, SCHEME, GH><<<(unsigned)grid, threads, sm, st>>>(cur, G, T, wmap);
   return dustb_host::launch_status("mixed tile");
 }
 

@@ -288,6 +288,8 @@ def run_ours(args, rep):
     mom0_mixed = [float(x) for x in sum(dev.momentum())]
     if args.grid_tiles:
         mx.set_tiles(0, 0, 8)                   # DUSTB_MIXED_GRID_TILES
+    if args.window_tma:
+        mx.mp.variant |= 32                     # DUSTB_MIXED_WINDOW_TMA
     if args.tune:
         # the library's autotuner (dustb_mixed_tune) on this workspace: rows per tile,
         # particles per pass, persistent work-queue CTAs or one CTA per tile
@@ -469,6 +471,8 @@ def run_ours(args, rep):
         }
         if res.get("tuned"):
             line["config"]["tuned"] = res["tuned"]
+        line["config"]["gather_window"] = ("staged in shared memory by one tensor copy per tile"
+                                           if args.window_tma else "loaded per thread (L1)")
         print(json.dumps(line), flush=True)
 
 
@@ -995,6 +999,8 @@ def main():
                     help="skip the refinable-cloud workload (128^3, 33.5 M clouds, FP64)")
     ap.add_argument("--no-seeded", action="store_true",
                     help="skip the FP64 form's timing in the seeded row order")
+    ap.add_argument("--window-tma", action="store_true",
+                    help="the gathering tiles stage their gas window by a tensor copy per tile")
     ap.add_argument("--clouds-only", action="store_true",
                     help="time the uniform refinable-cloud workload only (profiling case)")
     ap.add_argument("--pc2-only", action="store_true",

@@ -585,6 +585,13 @@ enum { DUSTB_MIXED_PROBE_COPY_TIMEOUT = 7 };
  * conserved to the FP32 rounding of the exchange (about 1e-8 of the exchanged momentum per
  * cycle) and a cycle takes about 8 % less time */
 #define DUSTB_MIXED_NO_LEDGER 16
+/* variant flag (3-D): the gathering tiles (operator, kick, pc2 predictor and advance) stage
+ * their gas window -- the tile's rows and one layer around them in three planes of the FP32
+ * gather window -- in shared memory by one tensor copy (TMA) per tile, instead of every thread
+ * loading its 27 cells from global memory.  Same results; off by default: on the 256^3
+ * benchmark workload the per-thread loads (L1 hits, issued while the particle copies fly) are
+ * faster (operator tile 5.7 against 7.1 ms, kick tile 8.3 against 10.0 ms per launch) */
+#define DUSTB_MIXED_WINDOW_TMA 32
 
 typedef struct dustb_mixed_params {
   double dx[3];            /* uniform cell size (single-level mesh) */
@@ -593,7 +600,8 @@ typedef struct dustb_mixed_params {
                               pass), a multiple of 4 in 64..8192; 0: the largest that keeps
                               as many CTAs per SM as their registers allow (2380 for tiles
                               of 128 cells) */
-  int variant;             /* 0, or DUSTB_MIXED_GRID_TILES and / or DUSTB_MIXED_NO_LEDGER;
+  int variant;             /* 0, or any of DUSTB_MIXED_GRID_TILES, DUSTB_MIXED_NO_LEDGER,
+                              DUSTB_MIXED_WINDOW_TMA;
                               DUSTB_MIXED_PROBE_COPY_TIMEOUT (with
                               or without the flag): a failure-detection test
                               hook (the first tile CTA 0 takes in every deposit launch never

@@ -479,3 +479,40 @@ def test_library_autotuner_keeps_the_results():
     for r in (1, 3, 5):
         assert np.abs(pa[r] - pb[r]).max() < 1e-6 * vscale, r
     check(st, ref, a, c)
+
+
+def _window_pair(st, phys, variant, cycles, pc2=False, dt=None, **kw):
+    from athenak_b200.mixed import MixedDust
+    a = MixedDust(st, phys, variant=32 | variant, **kw)
+    b = MixedDust(st, phys, variant=variant, **kw)
+    for _ in range(cycles):
+        for mx in (a, b):
+            if pc2:
+                mx.pc2_cycle(dt)
+            else:
+                mx.imex_cycle(dt)
+    a.export()
+    b.export()
+    torch.cuda.synchronize()
+    assert a.error_word() == 0 and b.error_word() == 0
+    pa, pb = a.dev.host("pr"), b.dev.host("pr")
+    vscale = np.abs(pb[[1, 3, 5]]).max()
+    for r in (1, 3, 5):
+        assert np.abs(pa[r] - pb[r]).max() < 1e-6 * vscale, (variant, r)
+    np.testing.assert_array_equal(a.dev.host("pi")[0], b.dev.host("pi")[0])
+
+
+@pytest.mark.parametrize("case", ["3d_random", "cic_dc2_plain"])
+def test_window_staged_by_tensor_copy_keeps_the_results(case):
+    """DUSTB_MIXED_WINDOW_TMA: the gathering tiles take their gas window from shared memory,
+    staged by one tensor copy per tile, instead of loading it per thread: the same window
+    values in the same order, so the cycles match the default form to the FP32 rounding of
+    the deposits' order -- imex2+ with one CTA per tile and on the work queue, pc2 (predictor
+    and advance tiles), and tiles of several passes (the window kept across them)."""
+    c = CASES[case]
+    ms = uniform_mesh(*c["mesh"])
+    st = make_state(ms, **c["st"])
+    for grid in (0, 8):
+        _window_pair(st, c["phys"], grid, 3, dt=c["dt"])
+    _window_pair(st, c["phys"], 0, 2, pc2=True, dt=c["dt"])
+    _window_pair(st, c["phys"], 0, 2, dt=c["dt"], rows_per_tile=2, chunk=68)
