@@ -41,15 +41,18 @@ class DustbLeafTables(C.Structure):
 
 class DustbCloudSplit(C.Structure):
     _fields_ = [("max_level", C.c_int), ("split_everywhere", C.c_int),
-                ("split_overlap", C.c_int), ("split_buffer", C.c_int), ("slack", C.c_double)]
+                ("split_overlap", C.c_int), ("split_buffer", C.c_int), ("slack", C.c_double),
+                ("budget", C.c_longlong)]
 
 
-def split_params(max_level, everywhere=False, overlap=True, buffer=0,
-                 slack=0.02) -> DustbCloudSplit:
-    """The split's controls (<dust>/cloud_split_*; slack: cloud_split_slack, 0.02)."""
+def split_params(max_level, everywhere=False, overlap=True, buffer=0, slack=0.02,
+                 budget=0) -> DustbCloudSplit:
+    """The split's controls (<dust>/cloud_split_*; slack: cloud_split_slack, 0.02; budget:
+    cloud_split_budget, 0 for none)."""
     sp = DustbCloudSplit()
     sp.max_level, sp.split_everywhere = int(max_level), int(everywhere)
     sp.split_overlap, sp.split_buffer, sp.slack = int(overlap), int(buffer), float(slack)
+    sp.budget = int(budget)
     return sp
 
 

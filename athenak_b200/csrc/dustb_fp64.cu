@@ -2052,6 +2052,16 @@ __global__ void k_split_count(PCtx P, MCtx M, Ind d, SplitCtl C, int *np, int *s
   sep[p] = (n > 0) ? (s | 64) : 0;
 }
 
+// the split budget (:1062-1111): an event whose pieces start at or beyond the budget waits
+// (its flags cleared, so the fill skips it); *taken receives the smallest such start, the
+// pieces of the events taken (left as is when no event waits)
+__global__ void k_split_budget(int *sep, const int *off, int n, long long budget, int *taken) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n || sep[p] == 0 || (long long)off[p] < budget) return;
+  sep[p] = 0;
+  atomicMin(taken, off[p]);
+}
+
 // WrapPos (:119-136) without shear: a piece into the domain; 1 if a physical x3 face mirrored it
 __device__ __forceinline__ int leaf_wrap_pos(const MCtx &M, double c[3]) {
   const double L[3] = {M.x1max - M.x1min, M.x2max - M.x2min, M.x3max - M.x3min};
@@ -3023,14 +3033,15 @@ int dustb_cloud_instant_switch(const dustb_ctx *c, int level_cap, int *nchange, 
 long long dustb_cloud_split_scratch_bytes(int npart) {
   if (npart < 0) return -1;
   const long long n = (long long)npart + 1;
-  return ((2 * n * 4 + 255) & ~255LL) + ((scan_bsum_ints(n) * 4 + 255) & ~255LL);
+  return ((2 * n * 4 + 255) & ~255LL) + ((scan_bsum_ints(n) * 4 + 255) & ~255LL) + 256;
 }
 
 int dustb_cloud_split_p1(const dustb_ctx *c, const dustb_cloud_split *sp,
                          unsigned long long tag0, int *nnew, void *scratch, long long bytes,
                          void *stream) {
   CHECK_CTX(c);
-  if (!sp || !nnew || !(sp->slack >= 0.0 && sp->slack < 1.0) || sp->split_buffer < 0)
+  if (!sp || !nnew || !(sp->slack >= 0.0 && sp->slack < 1.0) || sp->split_buffer < 0 ||
+      sp->budget < 0)
     return DUSTB_EINVAL;
   if (!cloud_mesh_ok(c) || !c->mesh.leaf) return DUSTB_EUNSUP;
   *nnew = 0;
@@ -3051,6 +3062,7 @@ int dustb_cloud_split_p1(const dustb_ctx *c, const dustb_cloud_split *sp,
   int *off = (int *)scratch;
   int *sep = off + n1;
   int *bsum = (int *)((char *)scratch + ((2 * n1 * 4 + 255) & ~255LL));
+  int *taken = (int *)((char *)bsum + ((scan_bsum_ints(n1) * 4 + 255) & ~255LL));
   cudaMemsetAsync(off + np, 0, sizeof(int), S(stream));
   k_split_count<<<PGRID(c)>>>(pview(c), mview(c), d, C, off, sep);
   int rc = launch_status("cloud_split_p1");
@@ -3062,6 +3074,15 @@ int dustb_cloud_split_p1(const dustb_ctx *c, const dustb_cloud_split *sp,
   cudaStreamSynchronize(S(stream));
   rc = launch_status("cloud_split_p1");
   if (rc) return rc;
+  if (sp->budget > 0 && (long long)total > sp->budget) {
+    // the events beyond the budget wait; the pieces of those taken
+    cudaMemcpyAsync(taken, off + np, sizeof(int), cudaMemcpyDeviceToDevice, S(stream));
+    k_split_budget<<<PGRID(c)>>>(sep, off, np, sp->budget, taken);
+    cudaMemcpyAsync(&total, taken, sizeof(int), cudaMemcpyDeviceToHost, S(stream));
+    cudaStreamSynchronize(S(stream));
+    rc = launch_status("cloud_split_p1");
+    if (rc) return rc;
+  }
   *nnew = total;
   if ((long long)np + total > c->part.stride) {
     dustb_host::set_message("cloud_split_p1: the pieces exceed the particle capacity");

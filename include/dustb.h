@@ -428,6 +428,10 @@ typedef struct dustb_cloud_split {
   int split_buffer;        /* test_cloud_split_buffer: the finer leaves of level l dilated by
                               buffer << (nlev - l + 1) finest cells (0: none) */
   double slack;            /* cloud_split_slack (0.02): the support shrunk by this fraction */
+  long long budget;        /* cloud_split_budget (0: none): the split events are taken in
+                              particle order while the pieces appended before them stay below
+                              the budget (the first is always taken, so at most 26 pieces
+                              beyond it); the later events wait for a later call */
 } dustb_cloud_split;
 /* CloudInstantSwitch (src/dust/dust_cloud.cpp:1023-1085): every plain cloud of level >= L takes
  * the level max(L, level of the leaf holding its centre); lobed clouds and clouds whose leaf is
@@ -437,8 +441,8 @@ int dustb_cloud_instant_switch(const dustb_ctx *ctx, int level_cap, int *nchange
                                void *stream);
 /* Bytes of scratch for dustb_cloud_split_p1 with npart particles. */
 long long dustb_cloud_split_scratch_bytes(int npart);
-/* SplitCloudsP1DeviceT (src/dust/dust_cloud3d.cpp:1005-1310) without the budget, the split
- * velocity and the block marks: a plain cloud whose (shrunk) support meets (or lies on) finer
+/* SplitCloudsP1DeviceT (src/dust/dust_cloud3d.cpp:1005-1310) without the split velocity and
+ * the block marks: a plain cloud whose (shrunk) support meets (or lies on) finer
  * leaves, or a lobed cloud whose lobe side became eligible, is split along each direction into
  * the P1 pieces of its separation flags (centre child with the lobes kept, edge children at
  * +-half-width with a quarter of the parent's shape each); pieces other than the centre are

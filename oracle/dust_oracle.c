@@ -1681,8 +1681,8 @@ static double wrap_pos(double x, double lo, double hi) {
   while (x >= hi) x -= len;
   return x;
 }
-/* SplitCloudsP1DeviceT (src/dust/dust_cloud3d.cpp:1005-1310) without the budget, the split
- * velocity and the block marks: the count pass, the exclusive scan of the appended pieces, the
+/* SplitCloudsP1DeviceT (src/dust/dust_cloud3d.cpp:1005-1310) without the split velocity and
+ * the block marks: the count pass, the exclusive scan of the appended pieces, the
  * fill (pieces last to first, the parent's slot last).  The arrays must hold npart + the pieces;
  * returns the pieces appended (npart is not changed), or -1 when they exceed the capacity. */
 int oracle_cloud_split_p1(const dustb_ctx *c, const dustb_cloud_split *sp, unsigned long long tag0) {
@@ -1710,6 +1710,16 @@ int oracle_cloud_split_p1(const dustb_ctx *c, const dustb_cloud_split *sp, unsig
     }
     sep[p] = s | 64;
     total += n - 1;
+  }
+  if (sp->budget > 0 && (long long)total > sp->budget) {
+    /* the split budget (:1062-1111): events whose pieces start at or beyond it wait */
+    int taken = total;
+    for (int p = 0; p < np; ++p)
+      if (sep[p] && (long long)off[p] >= sp->budget) {
+        sep[p] = 0;
+        if (off[p] < taken) taken = off[p];
+      }
+    total = taken;
   }
   if ((long long)np + total > stride) { free(sep); free(off); return -1; }
   const int reflect = ms->x3bc == 1;

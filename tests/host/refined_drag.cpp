@@ -139,6 +139,7 @@ int main(int argc, char **argv) {
   if (ts == TaskStatus::complete && clouds) {
     ts = drag.SetLeafTables(lt);
     dustb_cloud_split sp_ctl;
+    std::memset(&sp_ctl, 0, sizeof(sp_ctl));
     // the split stops at cloud_split_max_level when that is set below the finest level
     sp_ctl.max_level = (h[21] >= 0 && h[21] < lt.nlev) ? (int)h[21] : lt.nlev;
     sp_ctl.split_everywhere = 0;

@@ -173,3 +173,32 @@ def test_split_conserves_mass_and_momentum(x3bc):
     assert o.cloud_deposit_qp(0.05) == 0
     want = (pr[16] * 0.05 / (pr[15] + 0.05)).sum()
     assert abs(_deposited_mass(o, ms) - want) <= 1e-12 * want
+
+
+def test_split_budget_takes_the_first_events():
+    """cloud_split_budget: the split events are taken in particle order while the pieces
+    appended before them stay below the budget; the pieces appended are the first ones of the
+    unbudgeted split (the same tags and rows), at least the budget and at most 26 beyond it,
+    and mass and momentum are kept."""
+    ms = _mesh()
+    st = refined_state(ms, [0.1], [0.5], 1, seed=14, vel_noise=0.2)
+    lt = _oracle_tables(ms)
+    st.pi[3, :st.npart] = 0
+    n0 = st.npart
+    full = oracle.Oracle(st, dict(scheme=2))
+    full.set_leaf_tables(lt)
+    nf = full.cloud_split_p1(capi.split_params(max_level=1), n0)
+    budget = 5000
+    assert nf > 2 * budget
+    o = oracle.Oracle(st, dict(scheme=2))
+    o.set_leaf_tables(lt)
+    nb = o.cloud_split_p1(capi.split_params(max_level=1, budget=budget), n0)
+    assert budget <= nb <= budget + 26
+    np.testing.assert_array_equal(o.st.pr[:, n0:n0 + nb], full.st.pr[:, n0:n0 + nb])
+    np.testing.assert_array_equal(o.st.pi[:, n0:n0 + nb], full.st.pi[:, n0:n0 + nb])
+    m0 = st.pr[16, :n0].sum()
+    assert abs(o.st.pr[16, :n0 + nb].sum() - m0) <= 1e-13 * m0
+    # the waiting clouds are untouched
+    changed = (o.st.pi[3, :n0] != st.pi[3, :n0]) | (o.st.pr[16, :n0] != st.pr[16, :n0])
+    last = int(np.nonzero(changed)[0].max())
+    np.testing.assert_array_equal(o.st.pr[:, last + 1:n0], st.pr[:, last + 1:n0])

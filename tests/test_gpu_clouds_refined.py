@@ -138,3 +138,17 @@ def test_refined_cloud_cycles_match_the_oracle(solver):
     for v in range(4):
         sc = np.abs(ub[:, v]).max()
         assert np.abs(ms.active(ua)[:, v] - ms.active(ub)[:, v]).max() <= 1e-12 * sc, v
+
+
+def test_split_budget_matches_the_oracle():
+    ms = _mesh()
+    st = refined_state(ms, [0.1], [0.5], 1, seed=14, vel_noise=0.2)
+    st.pi[3, :st.npart] = 0
+    g, o = _pair(ms, st, dict(scheme=2))
+    sp = capi.split_params(max_level=1, budget=5000)
+    n_g = g.cloud_split_p1(sp, st.npart)
+    assert n_g == o.cloud_split_p1(sp, st.npart) and 5000 <= n_g <= 5026
+    torch.cuda.synchronize()
+    n = g.npart
+    np.testing.assert_array_equal(g.host("pr")[:, :n], o.st.pr[:, :n])
+    np.testing.assert_array_equal(g.host("pi")[:, :n], o.st.pi[:, :n])
