@@ -977,21 +977,28 @@ __global__ void __launch_bounds__(kT) k_move(PBuf S, PBuf D, const int *key_in, 
   const unsigned act = __ballot_sync(0xffffffffu, live);
   double comp[3] = {0.0, 0.0, 0.0};
   if (live) move_particle<KIND, SP>(S, D, key_in, cursor, G, P, p, act, comp);
-  if (KIND != PK_IMEX || !P.u0) return;
-  // the warp's ledger, added to the gas at its first particle's (old) cell: the particles of
-  // a warp are consecutive in cell order, one or two cells
-  double w[3];
+  if constexpr (KIND == PK_IMEX) {
+    if (!P.u0) return;
+    // the CTA's ledger, added to the gas at its first particle's (old) cell: the particles of
+    // a CTA are consecutive in cell order.  Staged in shared memory and summed by three warps,
+    // one per direction (a warp sum per warp would cost every thread the shuffles)
+    __shared__ double s_comp[3][kT];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) w[a] = warp_sum(0xffffffffu, comp[a]);
-  if ((threadIdx.x & 31) == 0 && live) {
-    int m, k, j, i;
-    decode(G, S.cell[p], m, k, j, i);
-    const double vinv = 1.0 / ((SP == 2) ? G.volm(m) : G.vol);
-    for (int a = 0; a < 3; ++a) {
-      if (w[a] == 0.0) continue;
-      const long long at = G.at(m, P.nvg, 1 + a, G.ks + k, G.js + j, G.is + i);
-      atomicAdd(&P.u0[at], w[a] * vinv);
-      if (!P.stage2 && P.u1) atomicAdd(&P.u1[at], w[a] * vinv);
+    for (int a = 0; a < 3; ++a) s_comp[a][threadIdx.x] = comp[a];
+    __syncthreads();
+    const int a = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (a < 3) {
+      double t = 0.0;
+      for (int x = lane; x < kT; x += 32) t += s_comp[a][x];
+      t = warp_sum(0xffffffffu, t);
+      if (lane == 0 && t != 0.0) {
+        int m, k, j, i;
+        decode(G, S.cell[blockIdx.x * kT], m, k, j, i);
+        const double vinv = 1.0 / ((SP == 2) ? G.volm(m) : G.vol);
+        const long long at = G.at(m, P.nvg, 1 + a, G.ks + k, G.js + j, G.is + i);
+        atomicAdd(&P.u0[at], t * vinv);
+        if (!P.stage2 && P.u1) atomicAdd(&P.u1[at], t * vinv);
+      }
     }
   }
 }
@@ -1689,13 +1696,10 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T,
           constexpr int U = 4;
           // the dust side of the tile's momentum ledger: the momentum m (v' - v) the particles
           // received (v' the stored FP32 velocity) and the part m (v' - v)/(a dt) - m R of the
-          // rate that the FP32 rate R leaves out (the history term reads R).  With
-          // v' = v + dv - err (err the exact error of the FP32 sum) and m dv = pm + em (pm the
-          // FP32 product, em its exact error), m (v' - v) = pm + em - m err: the large part pm
-          // summed in FP64, the small ones (of order 1e-8 of it) in FP32
-          double le[3] = {0.0, 0.0, 0.0};
-          float ls[3] = {0.0f, 0.0f, 0.0f}, lr[3] = {0.0f, 0.0f, 0.0f};
-          const float dinv = (float)(1.0 / T.a_dt - (double)inv_adt);   // 1/(a dt) - FP32 1/(a dt)
+          // rate that the FP32 rate R leaves out (the history term reads R).  v' - v is exact
+          // in FP64 (two FP32 values), so each particle adds m (v' - v) and m R rounded once
+          // in FP64; the rate part is formed from the thread's two sums at the end
+          double le[3] = {0.0, 0.0, 0.0}, lm[3] = {0.0, 0.0, 0.0};
           for (int x0 = tid; x0 < cnt; x0 += U * blockDim.x) {
             float v[U][3];
   #pragma unroll
@@ -1715,29 +1719,24 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T,
               S.f[F_VX][p] = vn[0]; S.f[F_VY][p] = vn[1]; S.f[F_VZ][p] = vn[2];
               S.f[F_RX][p] = rn[0]; S.f[F_RY][p] = rn[1]; S.f[F_RZ][p] = rn[2];
               if (T.ledger) {
-                const float mf = s_f[4 * CH + s];
+                const double md = (double)s_f[4 * CH + s];
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
-                  const float bb = __fsub_rn(vn[a], v[u][a]);
-                  const float err = __fadd_rn(__fsub_rn(v[u][a], __fsub_rn(vn[a], bb)),
-                                              __fsub_rn(dv[a], bb));   // v + dv = vn + err
-                  const float pm = __fmul_rn(mf, dv[a]);
-                  const float em = fmaf(mf, dv[a], -pm);                // m dv = pm + em
-                  le[a] += (double)pm;
-                  ls[a] += em - mf * err;
-                  // (m (v' - v)/(a dt) - m R = m (dv inv - R + dv dinv - err / (a dt)))
-                  if (T.hfield) lr[a] += mf * (fmaf(dv[a], inv_adt, -rn[a]) + dv[a] * dinv - err * inv_adt);
+                  le[a] = fma(md, __dsub_rn((double)vn[a], (double)v[u][a]), le[a]);
+                  if (T.hfield) lm[a] = fma(md, (double)rn[a], lm[a]);
                 }
               }
             }
           }
           if (T.ledger) {
+            const double iadt = 1.0 / T.a_dt;
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-              const double e = warp_sum(wmask, le[a] + (double)ls[a]);
+              const double e = warp_sum(wmask, le[a]);
               if (lane == 0) atomicAdd(&s_ledger[a], e);
               if (T.hfield) {
-                const double r = warp_sum(wmask, (double)lr[a]);
+                // (sum of m (v' - v)/(a dt) - m R over the thread's particles)
+                const double r = warp_sum(wmask, fma(le[a], iadt, -lm[a]));
                 if (lane == 0) atomicAdd(&s_ledger[3 + a], r);
               }
             }
