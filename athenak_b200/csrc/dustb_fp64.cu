@@ -133,10 +133,17 @@ __global__ void k_gas_rk(Ind d, double *u0, const double *u1, int nv, double g0,
   }
 }
 
-__global__ void k_history(Ind d, double *u0, int nv, const double *dmom, double atw_dt) {
+// (f2: a second 3-variable rate field added after dmom, in the same pass; null: none)
+__global__ void k_history(Ind d, double *u0, int nv, const double *dmom, const double *f2,
+                          double atw_dt) {
   int m, k, j, i;
   if (!active_cell(d, blockIdx.x * (long long)blockDim.x + threadIdx.x, m, k, j, i)) return;
-  for (int v = 0; v < 3; ++v) u0[d.at(m, nv, 1 + v, k, j, i)] += atw_dt * dmom[d.at(m, 3, v, k, j, i)];
+  for (int v = 0; v < 3; ++v) {
+    const long long a = d.at(m, nv, 1 + v, k, j, i), b = d.at(m, 3, v, k, j, i);
+    double u = u0[a] + atw_dt * dmom[b];
+    if (f2) u = u + atw_dt * f2[b];
+    u0[a] = u;
+  }
 }
 
 // ---- ExplicitPush imex, src/dust/dust_push.cpp:262-297 ----------------------------------
@@ -2573,12 +2580,15 @@ void gas_rk(const dustb_ctx *c, double g0, double g1, cudaStream_t st) {
 }
 void history(const dustb_ctx *c, double atw_dt, cudaStream_t st) {
   Ind d = make_ind(c->mesh);
-  k_history<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, atw_dt);
+  k_history<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom,
+                                                          nullptr, atw_dt);
 }
-// u0.m += atw_dt f for a 3-variable field f (the mixed form's rate ledger)
+// u0.m += atw_dt dmom, then u0.m += atw_dt f for a 3-variable field f (the mixed form's rate
+// ledger), in one pass: the same sums as two history launches
 void history_field(const dustb_ctx *c, const double *f, double atw_dt, cudaStream_t st) {
   Ind d = make_ind(c->mesh);
-  k_history<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, f, atw_dt);
+  k_history<<<blocks_for(n_active(d)), kThreads, 0, st>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, f,
+                                                          atw_dt);
 }
 void dc_correct(const dustb_ctx *c, cudaStream_t st) {
   Ind d = make_ind(c->mesh);
@@ -2626,7 +2636,7 @@ int dustb_gas_rk_noflux(const dustb_ctx *c, double gam0, double gam1, void *stre
 int dustb_history_gas(const dustb_ctx *c, double atw_dt, void *stream) {
   CHECK_CELLS(c);
   Ind d = make_ind(c->mesh);
-  k_history<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, atw_dt);
+  k_history<<<blocks_for(n_active(d)), kThreads, 0, S(stream)>>>(d, c->f.u0, c->f.nvar_gas, c->f.dmom, nullptr, atw_dt);
   return launch_status("history_gas");
 }
 

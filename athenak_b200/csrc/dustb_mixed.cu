@@ -2539,10 +2539,12 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       if (stage == 1) cudaMemcpyAsync(c->f.u1, c->f.u0, fbytes * c->f.nvar_gas, cudaMemcpyDeviceToDevice, st);
       dustb_cells::gas_rk(c, gam0[stage - 1], gam1[stage - 1], st);
       if (stage == 2 && br) {
-        dustb_cells::history(c, atw22 * dt, st);
-        // the rate's FP32 rounding the stage-1 kick tiles recorded (the momentum ledger)
+        // with the ledger, the rate's FP32 rounding the stage-1 kick tiles recorded follows the
+        // gas rate in the same pass
         if (!(mp->variant & DUSTB_MIXED_NO_LEDGER))
           dustb_cells::history_field(c, c->f.work, atw22 * dt, st);
+        else
+          dustb_cells::history(c, atw22 * dt, st);
       }
     }
     PushArgs P{};
