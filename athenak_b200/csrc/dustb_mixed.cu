@@ -517,7 +517,8 @@ struct PushArgs {
   // register copy pairs with) at the cell of each CTA's first particle.  Null: no ledger
   double *u0, *u1;
   int nvg;
-  double g0, g1, atw, inv_adt;
+  double g0, g1, atw;
+  double inv_adt;              // 1/(a dt) (imex: the kick's share of the rate)
 };
 
 // dust_imex_point_consistent_dust of stage 1 (src/dust/dust_pm.cpp:686-696): the velocity
@@ -882,7 +883,8 @@ __device__ __forceinline__ void move_particle(const PBuf &S, const PBuf &D, cons
       consistent_dv(G, P, cc, m, k, j, i, d);
       for (int a = 0; a < 3; ++a) {
         v[a] = __fadd_rn(v[a], __double2float_rn(d[a]));
-        r[a] += (float)(d[a] / P.a_dt);
+        // (imex: the rate takes the kick in the FP32 update below, the only reader of r)
+        if (KIND != PK_IMEX) r[a] += (float)(d[a] / P.a_dt);
         dk[a] = d[a];
       }
     }
@@ -911,11 +913,15 @@ __device__ __forceinline__ void move_particle(const PBuf &S, const PBuf &D, cons
         fz = -(2.0f - P.q) * P.om * v[0];
       }
     }
-    const float atw = P.stage2 ? P.atw_dt : 0.0f;
-    nv[0] = P.gam0 * v[0] + P.gam1 * v1[0] + P.bdt * fx + atw * r[0];
-    nv[1] = P.gam0 * v[1] + P.gam1 * v1[1] + P.bdt * fy + atw * r[1];
-    nv[2] = P.gam0 * v[2] + P.gam1 * v1[2] + P.bdt * fz + atw * r[2];
-    if (P.u0 && mass > 0.0f) {
+    if (!(P.u0 && mass > 0.0f)) {
+      // the FP32 update (no ledger)
+      if (kick && mass > 0.0f)
+        for (int a = 0; a < 3; ++a) r[a] += (float)(dk[a] * P.inv_adt);
+      const float atw = P.stage2 ? P.atw_dt : 0.0f;
+      nv[0] = P.gam0 * v[0] + P.gam1 * v1[0] + P.bdt * fx + atw * r[0];
+      nv[1] = P.gam0 * v[1] + P.gam1 * v1[1] + P.bdt * fy + atw * r[1];
+      nv[2] = P.gam0 * v[2] + P.gam1 * v1[2] + P.bdt * fz + atw * r[2];
+    } else {
       // the same update in FP64 from the stored inputs (the gas's coefficients, the exact kick
       // -- c times the FP64 residual -- in the velocity and, over a dt, in the rate), stored
       // rounded once to FP32 (half an ulp, where the FP32 chain leaves up to two); the ledger
@@ -2572,8 +2578,9 @@ int dustb_mixed_imex_cycle(const dustb_ctx *c, const dustb_mixed_params *mp, voi
       // the push's momentum ledger (FP64 coefficients of the gas's own RK combination)
       P.u0 = c->f.u0; P.u1 = c->f.u1; P.nvg = c->f.nvar_gas;
       P.g0 = gam0[stage - 1]; P.g1 = gam1[stage - 1];
-      P.atw = (stage == 2) ? atw22 * dt : 0.0; P.inv_adt = 1.0 / a_dt;
+      P.atw = (stage == 2) ? atw22 * dt : 0.0;
     }
+    P.inv_adt = 1.0 / a_dt;
     RUN(push_sort(S, src, cur, G, n, ncell, P, st));
     if (stage == 1) cudaMemsetAsync(&S.head->pending, 0, sizeof(int), st);   // applied
     TileArgs T{};

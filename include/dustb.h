@@ -587,7 +587,7 @@ enum { DUSTB_MIXED_PROBE_COPY_TIMEOUT = 7 };
  * FP32 rounding of the gas-dust momentum exchange to the gas in FP64 (per tile, per CTA), so
  * that total gas + dust momentum is conserved to FP64 round-off; with this flag it is
  * conserved to the FP32 rounding of the exchange (about 1e-8 of the exchanged momentum per
- * cycle) and a cycle takes about 6 % less time */
+ * cycle) and a cycle takes about 5 % less time */
 #define DUSTB_MIXED_NO_LEDGER 16
 /* variant flag (3-D): the gathering tiles (operator, kick, pc2 predictor and advance) stage
  * their gas window -- the tile's rows and one layer around them in three planes of the FP32
