@@ -1484,7 +1484,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T,
   __shared__ int s_wsum[kMaxTileThreads / 32];
   __shared__ int s_wcnt[kMaxTileThreads / 32];
   __shared__ int s_split;                          // some cell of the pass has several slots
-  __shared__ double s_ledger[9];                   // the kick tile's momentum ledger (FP64)
+  __shared__ double s_ledger[6];                   // the kick tile's momentum ledger (FP64)
   const int nx1 = G.nx1, tj = T.tj;
   const int nct = tj * nx1;                        // source cells of the tile = threads
   const int CH = T.chunk;                          // buffer columns (multiple of 4)
@@ -1552,7 +1552,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T,
     __syncwarp(wmask);
     for (int x = tid; x <= nct; x += blockDim.x) s_cs[x] = T.cstart[c0 + x];
     if (MODE == MODE_QP) s_qt[tid] = 0.0;
-    for (int x = tid; x < 9; x += blockDim.x) s_ledger[x] = 0.0;   // (tiles of fewer threads)
+    for (int x = tid; x < 6; x += blockDim.x) s_ledger[x] = 0.0;   // (tiles of fewer threads)
     cta_sync(wmask);
     const int P0 = s_cs[0], P1 = s_cs[nct];
     const float inv_adt = (float)(1.0 / T.a_dt);
@@ -1694,6 +1694,9 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T,
             s_f[7 * CH + r] = (vz + c32 * (uz - vz)) - vz;
           }
         }
+        // the kick's dust-side ledger of the pass, per thread: summed with the gas side of the
+        // deposit phase in one warp sum (only their sum is used)
+        double lk[3] = {0.0, 0.0, 0.0};
         if (MODE == MODE_KICK) {
           // the kicked velocities and rates of the pass, particle by particle (coalesced):
           // v <- v + dv, R <- dv / a_dt
@@ -1738,8 +1741,12 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T,
             const double iadt = 1.0 / T.a_dt;
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-              const double e = warp_sum(wmask, le[a]);
-              if (lane == 0) atomicAdd(&s_ledger[a], e);
+              if (T.deposit) {
+                lk[a] = le[a];
+              } else {
+                const double e = warp_sum(wmask, le[a]);
+                if (lane == 0) atomicAdd(&s_ledger[a], e);
+              }
               if (T.hfield) {
                 // (sum of m (v' - v)/(a dt) - m R over the thread's particles)
                 const double r = warp_sum(wmask, fma(le[a], iadt, -lm[a]));
@@ -1796,11 +1803,12 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T,
           if (D3 && single) add_window_cells<MODE, GH>(s_acc, G, T, m, k, j0, tj, cj_l, ci_l, gs);
           else add_window<MODE, D3, GH>(s_acc, G, T, m, k, j0, tj, split ? s_ss : nullptr, gs);
           if (MODE == MODE_KICK && T.ledger) {
-            // the gas side of the tile's ledger: what this pass added, summed over the CTA
+            // the gas side of the tile's ledger: what this pass added, with the dust side,
+            // summed over the CTA
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-              const double w = warp_sum(wmask, gs[a]);
-              if (lane == 0) atomicAdd(&s_ledger[6 + a], w);
+              const double w = warp_sum(wmask, gs[a] + lk[a]);
+              if (lane == 0) atomicAdd(&s_ledger[a], w);
             }
           }
         }
@@ -1822,7 +1830,7 @@ __global__ void __maxnreg__(168) k_tile(PBuf S, Geo G, TileArgs T,
         const long long at = G.at(m, 3, 0, G.ks + k, G.js + j0 + cj, G.is + ci);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          const double r = -(s_ledger[a] + s_ledger[6 + a]);
+          const double r = -s_ledger[a];
           if (r != 0.0) atomicAdd(&T.dfield[at + a * G.vstride], r * share);
           if (T.hfield && s_ledger[3 + a] != 0.0)
             atomicAdd(&T.hfield[at + a * G.vstride], s_ledger[3 + a] * share);
